@@ -1,0 +1,231 @@
+/*
+ * phieng_sph.h — C ABI of the B200 SPH fluid library (libphieng_sph.so).
+ *
+ * The first block re-exports the PhiEng engine's 2D world/fluid entry points
+ * with identical signatures and semantics, so a host that drives the
+ * reference through its C ABI (crates/engine/src/ffi.rs) can link this
+ * library instead for the fluid step. Each declaration cites the reference
+ * entry point it replaces. The second block (phieng_sph_*) is additive.
+ *
+ * World model: the world owns a set of static rigid bodies (walls: boxes and
+ * circles) and an SPH fluid whose particle state lives on the GPU. Every
+ * entry point tolerates null pointers (no-op / error code), never aborts,
+ * and copies caller buffers in or out; no allocation crosses the boundary.
+ * Stepping is asynchronous on the world's CUDA stream; every call that
+ * returns particle data synchronises that stream first, so observable
+ * semantics are synchronous, like the reference's.
+ *
+ * Not supported by this library (the call fails cleanly instead):
+ *  - dynamic bodies (phieng_world_add_body with is_static = 0 returns -1);
+ *  - adaptive resolution and boundary ghost particles (the config is
+ *    accepted as the reference accepts it, but phieng_world_step then
+ *    leaves the world unchanged and phieng_sph_status reports
+ *    PHIENG_SPH_E_UNSUPPORTED).
+ */
+#ifndef PHIENG_SPH_H
+#define PHIENG_SPH_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Opaque world handle (reference: Box<World2>, ffi.rs:51-54). */
+typedef struct World2 World2;
+
+/* Shape tags (ffi.rs:26-28). */
+#define PHIENG_SHAPE_CIRCLE 0u
+#define PHIENG_SHAPE_BOX 1u
+
+/* 2D SPH fluid config, #[repr(C)] mirror of FluidConfig2Ffi (ffi.rs:712-739).
+ * Rust `bool` fields are one byte (0 or 1). Size 112, align 4. */
+typedef struct FluidConfig2Ffi {
+  float particle_mass;        /* 0   */
+  float rest_density;         /* 4   */
+  float smoothing_length;     /* 8   */
+  float stiffness;            /* 12  */
+  float gamma;                /* 16  */
+  float artificial_viscosity; /* 20  */
+  float surface_tension;      /* 24  */
+  float cfl;                  /* 28  */
+  uint32_t max_substeps;      /* 32  */
+  uint8_t adaptive_resolution;/* 36  */
+  float split_density_ratio;  /* 40  */
+  float merge_density_ratio;  /* 44  */
+  uint8_t boundary_particles; /* 48  */
+  float viscosity;            /* 52  */
+  float drag;                 /* 56  */
+  float wall_friction;        /* 60  */
+  uint8_t phase_count;        /* 64  */
+  float phase_rest_density[4];/* 68  */
+  float phase_mass[4];        /* 84  */
+  float max_velocity;         /* 100 */
+  float particle_radius;      /* 104 */
+  uint8_t enabled;            /* 108 */
+} FluidConfig2Ffi;
+
+#ifdef __cplusplus
+static_assert(sizeof(FluidConfig2Ffi) == 112, "FluidConfig2Ffi must match ffi.rs:712-739");
+static_assert(offsetof(FluidConfig2Ffi, max_substeps) == 32, "layout");
+static_assert(offsetof(FluidConfig2Ffi, split_density_ratio) == 40, "layout");
+static_assert(offsetof(FluidConfig2Ffi, viscosity) == 52, "layout");
+static_assert(offsetof(FluidConfig2Ffi, phase_count) == 64, "layout");
+static_assert(offsetof(FluidConfig2Ffi, phase_rest_density) == 68, "layout");
+static_assert(offsetof(FluidConfig2Ffi, phase_mass) == 84, "layout");
+static_assert(offsetof(FluidConfig2Ffi, enabled) == 108, "layout");
+#endif
+
+/* ---------------- reference entry points (ffi.rs) ---------------- */
+
+/* ffi.rs:51 phieng_world_new — never returns null. No GPU work happens here;
+ * device memory is acquired on first use. */
+World2* phieng_world_new(void);
+
+/* ffi.rs:62 phieng_world_free — null is a no-op. */
+void phieng_world_free(World2* world);
+
+/* ffi.rs:76 phieng_world_step — null, non-finite or non-positive dt is a
+ * no-op; dt is clamped to <= 1/15 s. Runs ceil-CFL fluid substeps
+ * (fluid.rs:541-588) on the GPU and advances the world clock. */
+void phieng_world_step(World2* world, float dt);
+
+/* ffi.rs:89 phieng_world_set_gravity — non-finite components are ignored. */
+void phieng_world_set_gravity(World2* world, float gx, float gy);
+
+/* ffi.rs:1067 / 1079 world clock. 1 ok, 0 null or non-finite. */
+int32_t phieng_world_set_time(World2* world, float t);
+int32_t phieng_world_get_time(World2* world, float* out);
+
+/* ffi.rs:1123 body count, -1 for null. */
+int32_t phieng_world_body_count(World2* world);
+
+/* ffi.rs:1159 phieng_world_add_body — shape_tag PHIENG_SHAPE_CIRCLE
+ * (a = radius) or PHIENG_SHAPE_BOX (a, b = half extents), unrotated.
+ * Returns the body id, or -1 on invalid input. Static bodies only: a
+ * dynamic body (is_static == 0) returns -1 here. friction and restitution
+ * are accepted and sanitised as the reference does; the fluid does not
+ * read them. */
+int32_t phieng_world_add_body(World2* world, float pos_x, float pos_y, uint32_t shape_tag, float a,
+                              float b, float density, uint8_t is_static, float friction,
+                              float restitution);
+
+/* ffi.rs:999 / 1017 fluid config. set: 1 ok, 0 null or invalid (the
+ * validation of fluid2_from_ffi, ffi.rs:773-855; world unchanged on
+ * reject). get: 1 ok, 0 null. */
+int32_t phieng_world_set_fluid_config(World2* world, const FluidConfig2Ffi* cfg);
+int32_t phieng_world_get_fluid_config(World2* world, FluidConfig2Ffi* out);
+
+/* ffi.rs:2486 phieng_world_fluid_add — interleaved [x0,y0,x1,y1,...]; count
+ * capped at 1,000,000 per call and by the fluid's particle cap (4096 by
+ * default, as MAX_PARTICLES_2D, fluid.rs:30; see phieng_sph_set_particle_cap).
+ * Any non-finite input adds nothing (returns 0). Returns the number added. */
+uint32_t phieng_world_fluid_add(World2* world, const float* positions, uint32_t count);
+
+/* ffi.rs:2515 phieng_world_fluid_add_phase — as fluid_add, with a phase
+ * (0..=3, clamped for the mass/rest-density lookup) per particle. */
+uint32_t phieng_world_fluid_add_phase(World2* world, const float* positions, const uint8_t* phases,
+                                      uint32_t count);
+
+/* ffi.rs:2546 particle count (0 for null). */
+uint32_t phieng_world_fluid_count(const World2* world);
+
+/* ffi.rs:2559 remove all particles; 1 ok, 0 null. */
+int32_t phieng_world_fluid_clear(World2* world);
+
+/* ffi.rs:2575 copy out up to `max` quads [x, y, vx, vy] in insertion order;
+ * returns the number written (0 on null). Synchronises the world stream. */
+uint32_t phieng_world_fluid_get(const World2* world, float* out, uint32_t max);
+
+/* ---------------- extension (no reference counterpart) ---------------- */
+
+/* Error codes reported by phieng_sph_status().error. */
+#define PHIENG_SPH_OK 0
+#define PHIENG_SPH_E_NO_DEVICE 1   /* no usable CUDA device */
+#define PHIENG_SPH_E_CUDA 2        /* a CUDA call failed */
+#define PHIENG_SPH_E_UNSUPPORTED 3 /* config enables a feature this library lacks */
+#define PHIENG_SPH_E_ARG 4         /* invalid argument */
+
+typedef struct PhiengSphStatus {
+  int32_t error;          /* last error (sticky until phieng_sph_clear_error) */
+  uint32_t particles;     /* particle count */
+  uint64_t substeps;      /* fluid substeps run since creation */
+  uint32_t grid_log2_w;   /* bucket grid: columns = 1 << grid_log2_w */
+  uint32_t grid_log2_h;   /* rows = 1 << grid_log2_h */
+  uint32_t sort_passes;   /* radix digit passes per substep */
+  int32_t grid_cx0;       /* bucket grid origin cell: bucket = ((cy - grid_cy0) mod H) * W */
+  int32_t grid_cy0;       /*   + ((cx - grid_cx0) mod W), cx = floor(x / h) as i32 */
+  uint32_t reserved;
+} PhiengSphStatus;
+
+/* Fill *out; 1 ok, 0 null. Does not synchronise. */
+int32_t phieng_sph_status(const World2* world, PhiengSphStatus* out);
+/* Reset the sticky error; 1 ok, 0 null. */
+int32_t phieng_sph_clear_error(World2* world);
+/* Human-readable text for the last error (static storage; never null). */
+const char* phieng_sph_error_string(const World2* world);
+
+/* Raise (or lower) the fluid's particle cap (default 4096). Particles beyond
+ * a lowered cap are kept. 1 ok, 0 null or cap == 0. */
+int32_t phieng_sph_set_particle_cap(World2* world, uint32_t cap);
+
+/* Run `steps` world steps of `dt` each (the same as calling
+ * phieng_world_step `steps` times) without host round trips; replays a
+ * captured CUDA graph when the CFL substep count is fixed. 1 ok, 0 error. */
+int32_t phieng_sph_step_n(World2* world, float dt, uint32_t steps);
+
+/* Bind the world to a caller CUDA stream (cudaStream_t passed as void*;
+ * null selects the world's own stream). 1 ok, 0 null world. */
+int32_t phieng_sph_set_stream(World2* world, void* stream);
+/* Block until the world's queued GPU work is done. 1 ok, 0 error. */
+int32_t phieng_sph_sync(World2* world);
+
+/* Overwrite position and velocity of the first n particles from quads
+ * [x, y, vx, vy] (n <= count). Non-finite input is rejected. 1 ok, 0 error. */
+int32_t phieng_sph_set_state(World2* world, const float* xyvv, uint32_t n);
+
+/* Copy out density and pressure of the last substep (insertion order; either
+ * pointer may be null). Returns the number written. Synchronises. */
+uint32_t phieng_sph_get_density_pressure(const World2* world, float* density, float* pressure,
+                                         uint32_t max);
+
+/* Recompute the bucket grid from the current particle bounding box. */
+int32_t phieng_sph_replan(World2* world);
+
+/* max_i x_i and max_i |v_i| over the fluid (the per-step readings of the
+ * reference's fluid_dam example, fluid_dam.rs:46-52) into out[0], out[1];
+ * reduced on the GPU, 8 bytes copied back. 1 ok, 0 error. Synchronises. */
+int32_t phieng_sph_front_metrics(World2* world, float* out);
+
+/* Record CUDA events between the substep phases (sort + ranges, density,
+ * force + integrate) of every following substep. 1 ok, 0 error. */
+int32_t phieng_sph_set_profiling(World2* world, int32_t on);
+/* Milliseconds of each phase of the most recent substep (3 values);
+ * returns the count written, 0 if profiling is off. Synchronises. */
+uint32_t phieng_sph_phase_times(World2* world, float* ms, uint32_t max);
+
+/* ---- diagnostics used by the parity tests ---- */
+
+/* Run the density + force passes of one substep on the current state without
+ * integrating; write per-particle force [fx, fy] (insertion order, the
+ * scratch forces of fluid.rs:942-997) and refresh density/pressure.
+ * Returns the number written. */
+uint32_t phieng_sph_debug_forces(World2* world, float* fxy, uint32_t max);
+
+/* Rebuild the grid from the current state and write the sorted order:
+ * ids[s] = particle id at sorted slot s, keys[s] = its bucket key (either may
+ * be null). Returns n. */
+uint32_t phieng_sph_debug_sorted(World2* world, uint32_t* ids, uint32_t* keys, uint32_t max);
+
+/* Rebuild the grid and write each particle's neighbour list in visit order
+ * (fluid.rs:368-386): counts[i] (total found) and lists[i*max_per + k] for
+ * k < min(counts[i], max_per). Returns n. */
+uint32_t phieng_sph_debug_neighbors(World2* world, uint32_t* counts, uint32_t* lists,
+                                    uint32_t max_per, uint32_t max);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PHIENG_SPH_H */

@@ -1,0 +1,257 @@
+"""ORACLE — TEST INFRASTRUCTURE ONLY.
+
+ctypes wrapper of oracle/liboracle.so, the C++ restatement of the reference
+2D SPH step (crates/dynamics/src/fluid.rs). Only tests/, the smoke check and
+the CPU-baseline leg of bench.py import this module; the product library
+never does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+from phi_eng_b200._abi import FluidConfig2Ffi, default_config
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+
+REF_SEQ = 0
+JACOBI = 1
+
+_lib = None
+
+
+def build() -> None:
+    subprocess.run(["make", "-s", "-C", HERE, "liboracle.so"], check=True)
+
+
+def _load():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        build()
+    lib = C.CDLL(LIB_PATH)
+    P, F, D, U32, U8 = C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_double), C.POINTER(C.c_uint32), C.POINTER(C.c_uint8)
+    I32 = C.POINTER(C.c_int32)
+    sig = {
+        "orc_new": (P, [C.c_int]),
+        "orc_free": (None, [P]),
+        "orc_set_config": (None, [P, C.POINTER(FluidConfig2Ffi)]),
+        "orc_get_config": (None, [P, C.POINTER(FluidConfig2Ffi)]),
+        "orc_set_gravity": (None, [P, C.c_float, C.c_float]),
+        "orc_set_cap": (None, [P, C.c_uint32]),
+        "orc_add_body": (None, [P, C.c_int, C.c_float, C.c_float, C.c_float, C.c_float,
+                                C.c_float, C.c_float, C.c_float, C.c_float]),
+        "orc_add_particles": (C.c_uint32, [P, F, U8, C.c_uint32]),
+        "orc_count": (C.c_uint32, [P]),
+        "orc_clear": (None, [P]),
+        "orc_set_state": (None, [P, F, C.c_uint32]),
+        "orc_set_density_pressure": (None, [P, F, F, C.c_uint32]),
+        "orc_get_state": (C.c_uint32, [P, F, C.c_uint32]),
+        "orc_get_state64": (C.c_uint32, [P, D, C.c_uint32]),
+        "orc_get_density_pressure": (C.c_uint32, [P, F, F, C.c_uint32]),
+        "orc_get_density_pressure64": (C.c_uint32, [P, D, D, C.c_uint32]),
+        "orc_step": (None, [P, C.c_float, C.c_int]),
+        "orc_steps": (C.c_double, [P, C.c_float, C.c_int, C.c_uint32]),
+        "orc_substep": (None, [P, C.c_float, C.c_int]),
+        "orc_pass_density": (None, [P]),
+        "orc_pass_forces": (None, [P]),
+        "orc_get_forces": (C.c_uint32, [P, F, C.c_uint32]),
+        "orc_get_forces64": (C.c_uint32, [P, D, C.c_uint32]),
+        "orc_neighbors": (C.c_uint32, [P, C.c_uint32, U32, C.c_uint32]),
+        "orc_all_neighbors": (None, [P, U32, U32, C.c_uint32]),
+        "orc_cells": (None, [P, I32, I32]),
+        "orc_cfl_substeps": (C.c_uint32, [P, C.c_float]),
+        "orc_poly6": (C.c_float, [C.c_float, C.c_float]),
+        "orc_spiky": (None, [C.c_float, C.c_float, C.c_float, C.c_float, F]),
+        "orc_pressure": (C.c_float, [C.c_float, C.c_float, C.c_float, C.c_float]),
+        "orc_artificial_pressure": (C.c_float, [C.c_float] * 9),
+        "orc_cohesion": (C.c_float, [C.c_float, C.c_float]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _fp(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+def lib():
+    return _load()
+
+
+class OracleWorld:
+    """A World2-shaped CPU world: static bodies + one SPH fluid.
+
+    mode: REF_SEQ (the reference's in-place integrate) or JACOBI.
+    fp64: run the same algorithm in double precision.
+    """
+
+    def __init__(self, fp64: bool = False, cap: int = 4096):
+        self._l = _load()
+        self._h = self._l.orc_new(1 if fp64 else 0)
+        self.fp64 = fp64
+        self._l.orc_set_cap(self._h, cap)
+
+    def __del__(self):
+        try:
+            if self._h:
+                self._l.orc_free(self._h)
+                self._h = None
+        except Exception:
+            pass
+
+    # ---- setup ----
+    def set_config(self, cfg: FluidConfig2Ffi) -> None:
+        self._l.orc_set_config(self._h, C.byref(cfg))
+
+    def get_config(self) -> FluidConfig2Ffi:
+        c = FluidConfig2Ffi()
+        self._l.orc_get_config(self._h, C.byref(c))
+        return c
+
+    def set_gravity(self, gx: float, gy: float) -> None:
+        self._l.orc_set_gravity(self._h, gx, gy)
+
+    def set_cap(self, cap: int) -> None:
+        self._l.orc_set_cap(self._h, cap)
+
+    def add_box(self, px, py, hx, hy, rot=(1.0, 0.0, 0.0, 1.0)) -> None:
+        """Static box; rot = (x_axis.x, x_axis.y, y_axis.x, y_axis.y)."""
+        self._l.orc_add_body(self._h, 1, px, py, hx, hy, *rot)
+
+    def add_circle(self, px, py, r, rot=(1.0, 0.0, 0.0, 1.0)) -> None:
+        self._l.orc_add_body(self._h, 0, px, py, r, 0.0, *rot)
+
+    def add_particles(self, xy, phases=None) -> int:
+        xy = np.ascontiguousarray(xy, dtype=np.float32).reshape(-1, 2)
+        n = xy.shape[0]
+        ph = None
+        if phases is not None:
+            ph = np.ascontiguousarray(phases, dtype=np.uint8)
+            ph_p = ph.ctypes.data_as(C.POINTER(C.c_uint8))
+        else:
+            ph_p = None
+        return int(self._l.orc_add_particles(self._h, _fp(xy), ph_p, n))
+
+    @property
+    def count(self) -> int:
+        return int(self._l.orc_count(self._h))
+
+    def set_state(self, xyvv) -> None:
+        a = np.ascontiguousarray(xyvv, dtype=np.float32).reshape(-1, 4)
+        self._l.orc_set_state(self._h, _fp(a), a.shape[0])
+
+    def set_density_pressure(self, d, p) -> None:
+        d = np.ascontiguousarray(d, dtype=np.float32)
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        self._l.orc_set_density_pressure(self._h, _fp(d), _fp(p), d.shape[0])
+
+    # ---- readback ----
+    def state(self) -> np.ndarray:
+        n = self.count
+        if self.fp64:
+            out = np.zeros((n, 4), np.float64)
+            self._l.orc_get_state64(self._h, out.ctypes.data_as(C.POINTER(C.c_double)), n)
+        else:
+            out = np.zeros((n, 4), np.float32)
+            self._l.orc_get_state(self._h, _fp(out), n)
+        return out
+
+    def density_pressure(self):
+        n = self.count
+        if self.fp64:
+            d = np.zeros(n, np.float64)
+            p = np.zeros(n, np.float64)
+            D = C.POINTER(C.c_double)
+            self._l.orc_get_density_pressure64(self._h, d.ctypes.data_as(D), p.ctypes.data_as(D), n)
+        else:
+            d = np.zeros(n, np.float32)
+            p = np.zeros(n, np.float32)
+            self._l.orc_get_density_pressure(self._h, _fp(d), _fp(p), n)
+        return d, p
+
+    def forces(self) -> np.ndarray:
+        n = self.count
+        if self.fp64:
+            out = np.zeros((n, 2), np.float64)
+            self._l.orc_get_forces64(self._h, out.ctypes.data_as(C.POINTER(C.c_double)), n)
+        else:
+            out = np.zeros((n, 2), np.float32)
+            self._l.orc_get_forces(self._h, _fp(out), n)
+        return out
+
+    def neighbors(self, i: int, max_n: int = 256) -> np.ndarray:
+        out = np.zeros(max_n, np.uint32)
+        k = self._l.orc_neighbors(self._h, i, out.ctypes.data_as(C.POINTER(C.c_uint32)), max_n)
+        return out[: min(k, max_n)].copy()
+
+    def all_neighbors(self, max_per: int = 64):
+        n = self.count
+        counts = np.zeros(n, np.uint32)
+        lists = np.zeros(n * max_per, np.uint32)
+        U = C.POINTER(C.c_uint32)
+        self._l.orc_all_neighbors(self._h, counts.ctypes.data_as(U), lists.ctypes.data_as(U), max_per)
+        return counts, lists.reshape(n, max_per)
+
+    def cells(self):
+        n = self.count
+        cx = np.zeros(n, np.int32)
+        cy = np.zeros(n, np.int32)
+        I = C.POINTER(C.c_int32)
+        self._l.orc_cells(self._h, cx.ctypes.data_as(I), cy.ctypes.data_as(I))
+        return cx, cy
+
+    # ---- stepping ----
+    def step(self, dt: float, mode: int = REF_SEQ) -> None:
+        self._l.orc_step(self._h, dt, mode)
+
+    def steps(self, dt: float, k: int, mode: int = REF_SEQ) -> float:
+        """k world steps; returns the wall seconds spent inside C++."""
+        return float(self._l.orc_steps(self._h, dt, mode, k))
+
+    def substep(self, dt: float, mode: int = REF_SEQ) -> None:
+        self._l.orc_substep(self._h, dt, mode)
+
+    def pass_density(self) -> None:
+        self._l.orc_pass_density(self._h)
+
+    def pass_forces(self) -> None:
+        self._l.orc_pass_forces(self._h)
+
+    def cfl_substeps(self, dt: float) -> int:
+        return int(self._l.orc_cfl_substeps(self._h, dt))
+
+
+# scalar kernels (f32) for the reference's kernel-sanity checks
+def poly6(r2: float, h: float) -> float:
+    return float(_load().orc_poly6(r2, h))
+
+
+def spiky_grad(rx: float, ry: float, r: float, h: float):
+    out = np.zeros(2, np.float32)
+    _load().orc_spiky(rx, ry, r, h, _fp(out))
+    return float(out[0]), float(out[1])
+
+
+def pressure(d: float, rho0: float, k: float, gamma: float) -> float:
+    return float(_load().orc_pressure(d, rho0, k, gamma))
+
+
+def artificial_pressure(dx, dy, vrx, vry, r_sq, h, rho_bar, c, alpha) -> float:
+    return float(_load().orc_artificial_pressure(dx, dy, vrx, vry, r_sq, h, rho_bar, c, alpha))
+
+
+def cohesion(dist: float, h: float) -> float:
+    return float(_load().orc_cohesion(dist, h))
+
+
+__all__ = ["OracleWorld", "REF_SEQ", "JACOBI", "default_config", "build", "lib"]

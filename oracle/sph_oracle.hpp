@@ -1,0 +1,532 @@
+// ORACLE — TEST INFRASTRUCTURE ONLY.
+//
+// CPU restatement of the reference 2D SPH fluid step (PhiEng
+// `crates/dynamics/src/fluid.rs`, `FluidState2::step_fluid` -> `substep`).
+// It is the numeric ground truth for the CUDA path: only the tests, the
+// smoke check and the CPU-baseline leg of the benchmark may link it. The
+// product library never calls into this file.
+//
+// Parity status: the reference's Rust step cannot be compiled in this
+// environment (no cargo/rustc) and its own tests pin no numeric results of
+// the SPH step, so this restatement is pinned by (a) the reference's
+// behavioural tests re-run on it (tests/test_oracle.py), (b) the one
+// bit-pinned arithmetic identity of the reference (linear EOS,
+// fluid.rs:1326-1329), and (c) an FP64 twin that bounds its f32 error.
+//
+// Arithmetic contract: every expression keeps the reference's evaluation
+// order (glam 0.29 Vec2 ops are component-wise IEEE f32; Rust never
+// contracts a*b+c into an FMA). Build with -ffp-contract=off and without
+// -ffast-math. `powf` is the platform libm one, as Rust's `f32::powf` is.
+//
+// Two integrate modes:
+//   REF_SEQ  the reference's in-place Gauss-Seidel sweep (fluid.rs:1003-1050:
+//            particle i reads the already-advected state of every j < i);
+//   JACOBI   every read comes from the pre-integrate state (what a parallel
+//            GPU integrate computes; the CUDA path is bit-exact to this).
+#pragma once
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <unordered_map>
+#include <vector>
+
+namespace oracle {
+
+enum Mode { REF_SEQ = 0, JACOBI = 1 };
+
+// crates/math/src/math.rs:3-4
+constexpr float kEps = 1e-6f;
+constexpr float kEpsSq = 1e-12f;
+
+// FluidConfig2 (fluid.rs:54-140) with its Default (fluid.rs:142-169).
+struct Config {
+  float particle_mass = 0.0625f;
+  float rest_density = 1.0f;
+  float smoothing_length = 0.5f;
+  float stiffness = 100.0f;
+  float gamma = 1.0f;
+  float artificial_viscosity = 0.0f;
+  float surface_tension = 0.0f;
+  float cfl = 0.0f;
+  uint32_t max_substeps = 1;
+  bool adaptive_resolution = false;
+  float split_density_ratio = 0.5f;
+  float merge_density_ratio = 1.6f;
+  bool boundary_particles = false;
+  float viscosity = 0.3f;
+  float drag = 4.0f;
+  float wall_friction = 0.0f;
+  uint8_t phase_count = 1;
+  float phase_rest_density[4] = {1.0f, 1.0f, 1.0f, 1.0f};
+  float phase_mass[4] = {0.0625f, 0.0625f, 0.0625f, 0.0625f};
+  float max_velocity = 30.0f;
+  float particle_radius = 0.125f;
+  bool enabled = true;
+};
+
+// A static rigid body as the fluid sees it (body.rs:573-607): a circle or a
+// box with a Transform2 (math.rs:34-60: position + glam Mat2 columns).
+struct Body {
+  int shape = 1;  // 0 = circle (a = radius), 1 = box (a, b = half extents)
+  float px = 0, py = 0;
+  float xax = 1, xay = 0, yax = 0, yay = 1;  // rotation columns x_axis, y_axis
+  float a = 0, b = 0;
+};
+
+template <class R>
+struct Particle {
+  R x, y, vx, vy;
+  R density, pressure, mass;
+  uint8_t phase;
+};
+
+template <class R>
+struct Consts;
+template <>
+struct Consts<float> {
+  // std::f32::consts::PI
+  static float pi() { return 3.14159265358979323846f; }
+};
+template <>
+struct Consts<double> {
+  static double pi() { return 3.14159265358979323846; }
+};
+
+// `f32 as i32` / `f64 as i32`: saturating, NaN -> 0 (Rust semantics).
+template <class R>
+inline int32_t sat_i32(R v) {
+  if (v != v) return 0;
+  if (v >= (R)2147483648.0) return INT32_MAX;
+  if (v <= (R)-2147483648.0) return INT32_MIN;
+  return (int32_t)v;
+}
+
+template <class R>
+inline bool finite(R v) {
+  return std::isfinite(v);
+}
+
+// Rust f32::max / f32::min ignore a NaN operand.
+template <class R>
+inline R rmax(R a, R b) {
+  if (a != a) return b;
+  if (b != b) return a;
+  return a > b ? a : b;
+}
+// Rust f32::clamp (NaN passes through).
+template <class R>
+inline R rclamp(R x, R lo, R hi) {
+  if (x < lo) x = lo;
+  if (x > hi) x = hi;
+  return x;
+}
+
+template <class R>
+inline R rpow(R a, R b);
+template <>
+inline float rpow<float>(float a, float b) {
+  return powf(a, b);
+}
+template <>
+inline double rpow<double>(double a, double b) {
+  return pow(a, b);
+}
+
+template <class R>
+class Fluid {
+ public:
+  Config cfg;
+  std::vector<Particle<R>> particles;
+  std::vector<Body> bodies;
+  R gx = (R)0.0f, gy = (R)-9.81f;  // World2::new gravity (world.rs:338)
+  R time = 0;
+  size_t cap = 4096;  // MAX_PARTICLES_2D (fluid.rs:30); lifted by the caller
+
+  // last-substep scratch exposed for per-pass parity dumps
+  std::vector<R> fx, fy;
+
+  // ---- kernels (fluid.rs:265-326) ----
+  // poly6: 4/(pi h^8)(h^2-r^2)^3, zero beyond h (fluid.rs:265-273)
+  static R poly6(R r2, R h) {
+    if (r2 >= h * h || r2 < (R)0) return (R)0;
+    R h2 = h * h;
+    R t = h2 - r2;
+    return (R)4.0 / (Consts<R>::pi() * h2 * h2 * h2 * h2) * t * t * t;
+  }
+  // spiky gradient (fluid.rs:278-285)
+  static void spiky_grad(R rx, R ry, R r, R h, R& gxo, R& gyo) {
+    if (r >= h || r < (R)kEps) {
+      gxo = 0;
+      gyo = 0;
+      return;
+    }
+    R s = (R)-30.0 / (Consts<R>::pi() * h * h * h * h * h) * (h - r) * (h - r);
+    gxo = rx / r * s;
+    gyo = ry / r * s;
+  }
+  // equation of state (fluid.rs:290-297)
+  static R pressure(R density, R rest_density, R stiffness, R gamma) {
+    if (gamma == (R)1.0) {
+      return rmax(stiffness * (density - rest_density), (R)0);
+    }
+    R rho0 = rmax(rest_density, (R)kEps);
+    return rmax(stiffness * rho0 * (rpow(density / rho0, gamma) - (R)1.0), (R)0);
+  }
+  // Monaghan artificial viscosity (fluid.rs:302-317)
+  static R artificial_pressure(R dx, R dy, R vrx, R vry, R r_sq, R h, R rho_bar, R c, R alpha) {
+    R vd = vrx * dx + vry * dy;
+    if (vd >= (R)0) return (R)0;
+    R mu = h * vd / (r_sq + (R)0.01f * h * h);
+    return -alpha * c * mu / rmax(rho_bar, (R)kEps);
+  }
+  // cohesion (fluid.rs:320-326)
+  static R cohesion(R dist, R h) { return dist >= h ? (R)0 : (R)1.0 - dist / h; }
+
+  // ---- insert (fluid.rs:232-257) ----
+  size_t add_particles_phase(const float* xy, const uint8_t* ph, size_t n_in) {
+    size_t room = cap > particles.size() ? cap - particles.size() : 0;
+    size_t n = std::min(room, n_in);
+    for (size_t i = 0; i < n; i++) {
+      uint8_t p = ph ? ph[i] : 0;
+      size_t k = std::min<size_t>(p, 3);
+      Particle<R> q;
+      q.x = (R)xy[2 * i];
+      q.y = (R)xy[2 * i + 1];
+      q.vx = 0;
+      q.vy = 0;
+      q.density = (R)cfg.phase_rest_density[k];
+      q.pressure = 0;
+      q.mass = rmax((R)cfg.phase_mass[k], (R)0);
+      q.phase = p;
+      particles.push_back(q);
+    }
+    return n;
+  }
+
+  // ---- grid (fluid.rs:330-386) ----
+  static uint64_t cell_key(int32_t cx, int32_t cy) {
+    return ((uint64_t)(uint32_t)cx << 32) | (uint64_t)(uint32_t)cy;
+  }
+  std::unordered_map<uint64_t, std::vector<uint32_t>> grid;
+
+  void cell_of(R x, R y, int32_t& cx, int32_t& cy) const {
+    R hg = (R)cfg.smoothing_length;  // rebuild_grid / neighbors use the raw h
+    cx = sat_i32(std::floor(x / hg));
+    cy = sat_i32(std::floor(y / hg));
+  }
+
+  void rebuild_grid() {
+    for (auto& kv : grid) kv.second.clear();
+    for (size_t i = 0; i < particles.size(); i++) {
+      const auto& p = particles[i];
+      if (!finite(p.x) || !finite(p.y)) continue;
+      int32_t cx, cy;
+      cell_of(p.x, p.y, cx, cy);
+      grid[cell_key(cx, cy)].push_back((uint32_t)i);
+    }
+  }
+
+  // neighbours of the point (px, py) against the positions in `ps`
+  // (fluid.rs:368-386): oy outer, ox inner, in-cell ids ascending, kept
+  // when |x_j - x|^2 < h*h. Cells beyond the i32 range cannot exist.
+  void neighbors_of(R px, R py, const std::vector<Particle<R>>& ps, std::vector<uint32_t>& out) const {
+    out.clear();
+    R hg = (R)cfg.smoothing_length;
+    int32_t cx, cy;
+    cell_of(px, py, cx, cy);
+    for (int oy = -1; oy <= 1; oy++) {
+      int64_t yy = (int64_t)cy + oy;
+      if (yy < INT32_MIN || yy > INT32_MAX) continue;
+      for (int ox = -1; ox <= 1; ox++) {
+        int64_t xx = (int64_t)cx + ox;
+        if (xx < INT32_MIN || xx > INT32_MAX) continue;
+        auto it = grid.find(cell_key((int32_t)xx, (int32_t)yy));
+        if (it == grid.end()) continue;
+        for (uint32_t j : it->second) {
+          R dx = ps[j].x - px;
+          R dy = ps[j].y - py;
+          R d2 = dx * dx + dy * dy;
+          if (d2 < hg * hg) out.push_back(j);
+        }
+      }
+    }
+  }
+
+  // ---- density + pressure (fluid.rs:592-611) ----
+  void compute_density_pressure(R h) {
+    std::vector<uint32_t> nb;
+    R rho_cap = (R)3.0 * rmax((R)cfg.rest_density, (R)kEps);
+    for (size_t i = 0; i < particles.size(); i++) {
+      neighbors_of(particles[i].x, particles[i].y, particles, nb);
+      R pix = particles[i].x, piy = particles[i].y;
+      R rho = 0;
+      for (uint32_t j : nb) {
+        R dx = particles[j].x - pix;
+        R dy = particles[j].y - piy;
+        R r2 = dx * dx + dy * dy;
+        rho += particles[j].mass * poly6(r2, h);
+      }
+      particles[i].density = rclamp(rho, (R)0, rho_cap);
+    }
+    for (auto& p : particles) {
+      R rho0 = (R)cfg.phase_rest_density[std::min<int>(p.phase, 3)];
+      p.pressure = pressure(p.density, rho0, (R)cfg.stiffness, (R)cfg.gamma);
+    }
+  }
+
+  // ---- pressure force (+AV, cohesion) (fluid.rs:942-997) ----
+  void compute_forces(R h) {
+    std::vector<uint32_t> nb;
+    size_t n = particles.size();
+    fx.assign(n, (R)0);
+    fy.assign(n, (R)0);
+    R c_s = std::sqrt(rmax((R)cfg.stiffness, (R)0));
+    for (size_t i = 0; i < n; i++) {
+      neighbors_of(particles[i].x, particles[i].y, particles, nb);
+      R pix = particles[i].x, piy = particles[i].y;
+      R vix = particles[i].vx, viy = particles[i].vy;
+      R rho_i = rmax(particles[i].density, (R)kEps);
+      R p_i = particles[i].pressure;
+      R fxi = 0, fyi = 0;
+      for (uint32_t j : nb) {
+        if (j == i) continue;
+        const auto& pj = particles[j];
+        R rho_j = rmax(pj.density, (R)kEps);
+        R dx = pix - pj.x;
+        R dy = piy - pj.y;
+        R dist = std::sqrt(dx * dx + dy * dy);
+        R gxx, gyy;
+        spiky_grad(dx, dy, dist, h, gxx, gyy);
+        R term = p_i / (rho_i * rho_i) + pj.pressure / (rho_j * rho_j);
+        if ((R)cfg.artificial_viscosity > (R)0 && dist > (R)kEps) {
+          R rho_bar = (R)0.5 * (rho_i + rho_j);
+          term += artificial_pressure(dx, dy, vix - pj.vx, viy - pj.vy, dist * dist, h, rho_bar, c_s,
+                                      (R)cfg.artificial_viscosity);
+        }
+        R mt = pj.mass * term;
+        fxi -= gxx * mt;
+        fyi -= gyy * mt;
+        if ((R)cfg.surface_tension > (R)0 && dist > (R)kEps) {
+          R coh = cohesion(dist, h);
+          if (coh > (R)0) {
+            R s = (R)cfg.surface_tension * particles[i].mass * pj.mass * coh;
+            fxi -= dx / dist * s;
+            fyi -= dy / dist * s;
+          }
+        }
+      }
+      fx[i] = fxi;
+      fy[i] = fyi;
+    }
+  }
+
+  // ---- integrate: gravity + pressure, XSPH, cap, advect (fluid.rs:1003-1050) ----
+  void integrate(R h, R dt, Mode mode) {
+    std::vector<uint32_t> nb;
+    size_t n = particles.size();
+    std::vector<Particle<R>> snap;
+    if (mode == JACOBI) snap = particles;
+    const std::vector<Particle<R>>& src = (mode == JACOBI) ? snap : particles;
+    R visc = (R)cfg.viscosity;
+    R vmax = (R)cfg.max_velocity;
+    for (size_t i = 0; i < n; i++) {
+      // REF_SEQ reads the live array: j < i are already advected.
+      neighbors_of(src[i].x, src[i].y, src, nb);
+      R rho_i = rmax(src[i].density, (R)kEps);
+      R ax = gx + fx[i] / rho_i;
+      R ay = gy + fy[i] / rho_i;
+      R vx = src[i].vx + ax * dt;
+      R vy = src[i].vy + ay * dt;
+      if (visc > (R)0) {
+        R pix = src[i].x, piy = src[i].y;
+        R sx = 0, sy = 0;
+        for (uint32_t j : nb) {
+          if (j == i) continue;
+          const auto& pj = src[j];
+          R rho_bar = (R)0.5 * (rho_i + rmax(pj.density, (R)kEps));
+          R dx = pj.x - pix;
+          R dy = pj.y - piy;
+          R w = poly6(dx * dx + dy * dy, h);
+          R mr = pj.mass / rho_bar;
+          sx += (pj.vx - src[i].vx) * mr * w;
+          sy += (pj.vy - src[i].vy) * mr * w;
+        }
+        vx += sx * visc;
+        vy += sy * visc;
+      }
+      R speed = std::sqrt(vx * vx + vy * vy);
+      if (speed > vmax) {
+        R sc = vmax / speed;
+        vx *= sc;
+        vy *= sc;
+      }
+      if (!finite(vx) || !finite(vy)) {
+        vx = 0;
+        vy = 0;
+      }
+      R nx = src[i].x + vx * dt;
+      R ny = src[i].y + vy * dt;
+      if (!finite(nx) || !finite(ny)) {
+        nx = src[i].x;
+        ny = src[i].y;
+      }
+      particles[i].vx = vx;
+      particles[i].vy = vy;
+      particles[i].x = nx;
+      particles[i].y = ny;
+    }
+  }
+
+  // ---- particle vs static body (fluid.rs:463-533, circle + box) ----
+  // Returns false when separated; else the normal and depth.
+  static bool collide(R px, R py, R pr, const Body& b, R& nx, R& ny, R& depth) {
+    if (b.shape == 0) {
+      R dx = px - (R)b.px;
+      R dy = py - (R)b.py;
+      R dist = std::sqrt(dx * dx + dy * dy);
+      R radius = (R)b.a;
+      if (dist >= radius + pr) return false;
+      if (dist > (R)kEps) {
+        nx = dx / dist;
+        ny = dy / dist;
+      } else {
+        nx = 1;
+        ny = 0;
+      }
+      depth = radius + pr - dist;
+      return true;
+    }
+    R hx = (R)b.a, hy = (R)b.b;
+    R rx = px - (R)b.px;
+    R ry = py - (R)b.py;
+    R xax = (R)b.xax, xay = (R)b.xay, yax = (R)b.yax, yay = (R)b.yay;
+    // fluid.rs:483-489 literally: x_axis.x*rel.x + y_axis.x*rel.y (this is
+    // R*rel, not R^T*rel as its comment says; identical for unrotated walls).
+    R lx = xax * rx + yax * ry;
+    R ly = xay * rx + yay * ry;
+    R cxl = rclamp(lx, -hx, hx);
+    R cyl = rclamp(ly, -hy, hy);
+    R ddx = lx - cxl;
+    R ddy = ly - cyl;
+    if (ddx * ddx + ddy * ddy > (R)kEpsSq) {
+      R dist = std::sqrt(ddx * ddx + ddy * ddy);
+      if (dist >= pr) return false;
+      R lnx = ddx / dist, lny = ddy / dist;
+      // glam Mat2 * Vec2: x_axis * v.x + y_axis * v.y
+      nx = xax * lnx + yax * lny;
+      ny = xay * lnx + yay * lny;
+      depth = pr - dist;
+      return true;
+    }
+    R dxp = hx - std::fabs(lx);
+    R dyp = hy - std::fabs(ly);
+    // `signum().copysign(1.0)` is always +1 (NaN keeps a NaN): the eject
+    // normal is always +x or +y in the box frame (fluid.rs:504-516).
+    R lnx, lny;
+    if (dxp < dyp) {
+      lnx = (lx != lx) ? lx : (R)1;
+      lny = 0;
+      depth = pr + dxp;
+    } else {
+      lnx = 0;
+      lny = (ly != ly) ? ly : (R)1;
+      depth = pr + dyp;
+    }
+    if (lnx != lnx) lnx = std::fabs(lnx);
+    if (lny != lny) lny = std::fabs(lny);
+    nx = xax * lnx + yax * lny;
+    ny = xay * lnx + yay * lny;
+    return true;
+  }
+
+  // boundary pass (fluid.rs:1056-1094); statics take no impulse
+  // (body.rs:675-687), so only the particle side changes. Static walls
+  // have zero velocity, which the friction branch reads.
+  void boundaries() {
+    R pr = rmax((R)cfg.particle_radius, (R)0);
+    for (auto& p : particles) {
+      for (const Body& b : bodies) {
+        R nx, ny, depth;
+        if (!collide(p.x, p.y, pr, b, nx, ny, depth)) continue;
+        if (depth <= (R)0) continue;
+        p.x = p.x + nx * depth;
+        p.y = p.y + ny * depth;
+        R vn = p.vx * nx + p.vy * ny;
+        if (vn < (R)0) {
+          p.vx -= nx * vn;
+          p.vy -= ny * vn;
+          if ((R)cfg.wall_friction > (R)0) {
+            R mu = rclamp((R)cfg.wall_friction, (R)0, (R)1);
+            R vtx = p.vx, vty = p.vy;
+            R wvx = 0, wvy = 0;
+            R wdot = wvx * nx + wvy * ny;
+            R wtx = wvx - nx * wdot;
+            R wty = wvy - ny * wdot;
+            R dvx = (wtx - vtx) * mu;
+            R dvy = (wty - vty) * mu;
+            p.vx += dvx;
+            p.vy += dvy;
+          }
+        }
+      }
+    }
+  }
+
+  // ---- CFL substeps (fluid.rs:562-588) ----
+  uint32_t cfl_substeps(R dt) const {
+    uint32_t mx = std::max<uint32_t>(cfg.max_substeps, 1);
+    if ((R)cfg.cfl <= (R)0 || mx <= 1) return 1;
+    R h = rmax((R)cfg.smoothing_length, (R)kEps);
+    R rho0 = rmax((R)cfg.rest_density, (R)kEps);
+    R c0;
+    if ((R)cfg.gamma == (R)1.0)
+      c0 = std::sqrt(rmax((R)cfg.stiffness, (R)0));
+    else
+      c0 = std::sqrt((R)cfg.gamma * rmax((R)cfg.stiffness, (R)0) * rho0);
+    R vm = 0;
+    for (const auto& p : particles) vm = rmax(vm, std::sqrt(p.vx * p.vx + p.vy * p.vy));
+    R speed = c0 + vm;
+    if (!finite(speed) || speed <= (R)kEps) return 1;
+    R dt_max = (R)cfg.cfl * h / speed;
+    if (!finite(dt_max) || dt_max <= (R)0) return 1;
+    R q = std::ceil(dt / dt_max);
+    int64_t k;
+    if (q != q)
+      k = 0;
+    else if (q >= (R)9.2233720368547758e18)
+      k = INT64_MAX;
+    else if (q <= (R)-9.2233720368547758e18)
+      k = INT64_MIN;
+    else
+      k = (int64_t)q;
+    if (k < 1) k = 1;
+    if (k > (int64_t)mx) k = mx;
+    return (uint32_t)k;
+  }
+
+  // ---- one substep (fluid.rs:898-1136) for the dam-break feature set ----
+  void substep(R dt, Mode mode) {
+    R h = rmax((R)cfg.smoothing_length, (R)kEps);
+    rebuild_grid();
+    compute_density_pressure(h);
+    compute_forces(h);
+    integrate(h, dt, mode);
+    boundaries();
+    // The trailing rebuild_grid + buoyancy pass (fluid.rs:1102-1135) acts
+    // on dynamic bodies only and leaves particle state unchanged.
+  }
+
+  // ---- step_fluid (fluid.rs:541-557) inside World2::step (world.rs:706-732) ----
+  void world_step(R dt, Mode mode) {
+    if (cfg.enabled && !particles.empty() && dt > (R)0) {
+      uint32_t n = cfl_substeps(dt);
+      R sub = dt / (R)n;
+      for (uint32_t k = 0; k < n; k++) substep(sub, mode);
+    }
+    time += dt;
+  }
+};
+
+}  // namespace oracle

@@ -1,0 +1,371 @@
+// ORACLE — TEST INFRASTRUCTURE ONLY (see sph_oracle.hpp).
+//
+// Flat C API over oracle::Fluid<float> / oracle::Fluid<double> so the Python
+// tests, the smoke check and the CPU-baseline leg of the benchmark can drive
+// the CPU restatement through ctypes. Nothing in the product library links
+// this file.
+#include <chrono>
+#include <cstdint>
+#include <cstring>
+
+#include "../include/phieng_sph.h"
+#include "sph_oracle.hpp"
+
+using oracle::Fluid;
+
+namespace {
+
+struct Orc {
+  int fp64;
+  Fluid<float> f32;
+  Fluid<double> f64;
+};
+
+template <class F>
+void apply_config(F& f, const FluidConfig2Ffi* c) {
+  auto& d = f.cfg;
+  d.particle_mass = c->particle_mass;
+  d.rest_density = c->rest_density;
+  d.smoothing_length = c->smoothing_length;
+  d.stiffness = c->stiffness;
+  d.gamma = c->gamma;
+  d.artificial_viscosity = c->artificial_viscosity;
+  d.surface_tension = c->surface_tension;
+  d.cfl = c->cfl;
+  d.max_substeps = c->max_substeps;
+  d.adaptive_resolution = c->adaptive_resolution != 0;
+  d.split_density_ratio = c->split_density_ratio;
+  d.merge_density_ratio = c->merge_density_ratio;
+  d.boundary_particles = c->boundary_particles != 0;
+  d.viscosity = c->viscosity;
+  d.drag = c->drag;
+  d.wall_friction = c->wall_friction;
+  d.phase_count = c->phase_count;
+  for (int k = 0; k < 4; k++) {
+    d.phase_rest_density[k] = c->phase_rest_density[k];
+    d.phase_mass[k] = c->phase_mass[k];
+  }
+  d.max_velocity = c->max_velocity;
+  d.particle_radius = c->particle_radius;
+  d.enabled = c->enabled != 0;
+}
+
+template <class F>
+void read_config(const F& f, FluidConfig2Ffi* c) {
+  std::memset(c, 0, sizeof(*c));
+  const auto& d = f.cfg;
+  c->particle_mass = d.particle_mass;
+  c->rest_density = d.rest_density;
+  c->smoothing_length = d.smoothing_length;
+  c->stiffness = d.stiffness;
+  c->gamma = d.gamma;
+  c->artificial_viscosity = d.artificial_viscosity;
+  c->surface_tension = d.surface_tension;
+  c->cfl = d.cfl;
+  c->max_substeps = d.max_substeps;
+  c->adaptive_resolution = d.adaptive_resolution;
+  c->split_density_ratio = d.split_density_ratio;
+  c->merge_density_ratio = d.merge_density_ratio;
+  c->boundary_particles = d.boundary_particles;
+  c->viscosity = d.viscosity;
+  c->drag = d.drag;
+  c->wall_friction = d.wall_friction;
+  c->phase_count = d.phase_count;
+  for (int k = 0; k < 4; k++) {
+    c->phase_rest_density[k] = d.phase_rest_density[k];
+    c->phase_mass[k] = d.phase_mass[k];
+  }
+  c->max_velocity = d.max_velocity;
+  c->particle_radius = d.particle_radius;
+  c->enabled = d.enabled;
+}
+
+#define DISPATCH(o, expr)     \
+  do {                        \
+    if ((o)->fp64) {          \
+      auto& F = (o)->f64;     \
+      expr;                   \
+    } else {                  \
+      auto& F = (o)->f32;     \
+      expr;                   \
+    }                         \
+  } while (0)
+
+}  // namespace
+
+extern "C" {
+
+void* orc_new(int fp64) {
+  Orc* o = new Orc();
+  o->fp64 = fp64 ? 1 : 0;
+  return o;
+}
+
+void orc_free(void* h) { delete static_cast<Orc*>(h); }
+
+void orc_set_config(void* h, const FluidConfig2Ffi* c) {
+  Orc* o = static_cast<Orc*>(h);
+  DISPATCH(o, apply_config(F, c));
+}
+
+void orc_get_config(void* h, FluidConfig2Ffi* c) {
+  Orc* o = static_cast<Orc*>(h);
+  DISPATCH(o, read_config(F, c));
+}
+
+void orc_set_gravity(void* h, float gx, float gy) {
+  Orc* o = static_cast<Orc*>(h);
+  o->f32.gx = gx;
+  o->f32.gy = gy;
+  o->f64.gx = (double)gx;
+  o->f64.gy = (double)gy;
+}
+
+void orc_set_cap(void* h, uint32_t cap) {
+  Orc* o = static_cast<Orc*>(h);
+  o->f32.cap = cap;
+  o->f64.cap = cap;
+}
+
+// shape 0 = circle (a = radius), 1 = box (a, b = half extents); rotation
+// columns x_axis = (xax, xay), y_axis = (yax, yay).
+void orc_add_body(void* h, int shape, float px, float py, float a, float b, float xax, float xay,
+                  float yax, float yay) {
+  Orc* o = static_cast<Orc*>(h);
+  oracle::Body bd;
+  bd.shape = shape;
+  bd.px = px;
+  bd.py = py;
+  bd.a = a;
+  bd.b = b;
+  bd.xax = xax;
+  bd.xay = xay;
+  bd.yax = yax;
+  bd.yay = yay;
+  o->f32.bodies.push_back(bd);
+  o->f64.bodies.push_back(bd);
+}
+
+uint32_t orc_add_particles(void* h, const float* xy, const uint8_t* phases, uint32_t n) {
+  Orc* o = static_cast<Orc*>(h);
+  uint32_t r = 0;
+  DISPATCH(o, r = (uint32_t)F.add_particles_phase(xy, phases, n));
+  return r;
+}
+
+uint32_t orc_count(void* h) {
+  Orc* o = static_cast<Orc*>(h);
+  uint32_t r = 0;
+  DISPATCH(o, r = (uint32_t)F.particles.size());
+  return r;
+}
+
+void orc_clear(void* h) {
+  Orc* o = static_cast<Orc*>(h);
+  o->f32.particles.clear();
+  o->f64.particles.clear();
+}
+
+// position + velocity of the first n particles from quads
+void orc_set_state(void* h, const float* xyvv, uint32_t n) {
+  Orc* o = static_cast<Orc*>(h);
+  DISPATCH(o, {
+    for (uint32_t i = 0; i < n && i < F.particles.size(); i++) {
+      F.particles[i].x = xyvv[4 * i];
+      F.particles[i].y = xyvv[4 * i + 1];
+      F.particles[i].vx = xyvv[4 * i + 2];
+      F.particles[i].vy = xyvv[4 * i + 3];
+    }
+  });
+}
+
+void orc_set_density_pressure(void* h, const float* d, const float* p, uint32_t n) {
+  Orc* o = static_cast<Orc*>(h);
+  DISPATCH(o, {
+    for (uint32_t i = 0; i < n && i < F.particles.size(); i++) {
+      if (d) F.particles[i].density = d[i];
+      if (p) F.particles[i].pressure = p[i];
+    }
+  });
+}
+
+uint32_t orc_get_state(void* h, float* out, uint32_t max) {
+  Orc* o = static_cast<Orc*>(h);
+  uint32_t n = 0;
+  DISPATCH(o, {
+    n = (uint32_t)std::min<size_t>(max, F.particles.size());
+    for (uint32_t i = 0; i < n; i++) {
+      out[4 * i] = (float)F.particles[i].x;
+      out[4 * i + 1] = (float)F.particles[i].y;
+      out[4 * i + 2] = (float)F.particles[i].vx;
+      out[4 * i + 3] = (float)F.particles[i].vy;
+    }
+  });
+  return n;
+}
+
+uint32_t orc_get_state64(void* h, double* out, uint32_t max) {
+  Orc* o = static_cast<Orc*>(h);
+  uint32_t n = 0;
+  DISPATCH(o, {
+    n = (uint32_t)std::min<size_t>(max, F.particles.size());
+    for (uint32_t i = 0; i < n; i++) {
+      out[4 * i] = (double)F.particles[i].x;
+      out[4 * i + 1] = (double)F.particles[i].y;
+      out[4 * i + 2] = (double)F.particles[i].vx;
+      out[4 * i + 3] = (double)F.particles[i].vy;
+    }
+  });
+  return n;
+}
+
+uint32_t orc_get_density_pressure(void* h, float* d, float* p, uint32_t max) {
+  Orc* o = static_cast<Orc*>(h);
+  uint32_t n = 0;
+  DISPATCH(o, {
+    n = (uint32_t)std::min<size_t>(max, F.particles.size());
+    for (uint32_t i = 0; i < n; i++) {
+      if (d) d[i] = (float)F.particles[i].density;
+      if (p) p[i] = (float)F.particles[i].pressure;
+    }
+  });
+  return n;
+}
+
+uint32_t orc_get_density_pressure64(void* h, double* d, double* p, uint32_t max) {
+  Orc* o = static_cast<Orc*>(h);
+  uint32_t n = 0;
+  DISPATCH(o, {
+    n = (uint32_t)std::min<size_t>(max, F.particles.size());
+    for (uint32_t i = 0; i < n; i++) {
+      if (d) d[i] = (double)F.particles[i].density;
+      if (p) p[i] = (double)F.particles[i].pressure;
+    }
+  });
+  return n;
+}
+
+// World2::step (world.rs:706-732) with step_fluid (fluid.rs:541-557).
+void orc_step(void* h, float dt, int mode) {
+  Orc* o = static_cast<Orc*>(h);
+  DISPATCH(o, F.world_step(dt, (oracle::Mode)mode));
+}
+
+// k world steps; returns wall seconds spent (for the CPU baseline).
+double orc_steps(void* h, float dt, int mode, uint32_t k) {
+  Orc* o = static_cast<Orc*>(h);
+  auto t0 = std::chrono::steady_clock::now();
+  for (uint32_t s = 0; s < k; s++) DISPATCH(o, F.world_step(dt, (oracle::Mode)mode));
+  auto t1 = std::chrono::steady_clock::now();
+  return std::chrono::duration<double>(t1 - t0).count();
+}
+
+void orc_substep(void* h, float dt, int mode) {
+  Orc* o = static_cast<Orc*>(h);
+  DISPATCH(o, F.substep(dt, (oracle::Mode)mode));
+}
+
+// Pass-level hooks for "from identical state" parity checks.
+void orc_pass_density(void* h) {
+  Orc* o = static_cast<Orc*>(h);
+  DISPATCH(o, {
+    F.rebuild_grid();
+    F.compute_density_pressure(oracle::rmax((decltype(F.time))F.cfg.smoothing_length,
+                                            (decltype(F.time))oracle::kEps));
+  });
+}
+
+void orc_pass_forces(void* h) {
+  Orc* o = static_cast<Orc*>(h);
+  DISPATCH(o, {
+    F.rebuild_grid();
+    F.compute_forces(oracle::rmax((decltype(F.time))F.cfg.smoothing_length,
+                                  (decltype(F.time))oracle::kEps));
+  });
+}
+
+uint32_t orc_get_forces(void* h, float* fxy, uint32_t max) {
+  Orc* o = static_cast<Orc*>(h);
+  uint32_t n = 0;
+  DISPATCH(o, {
+    n = (uint32_t)std::min<size_t>(max, F.fx.size());
+    for (uint32_t i = 0; i < n; i++) {
+      fxy[2 * i] = (float)F.fx[i];
+      fxy[2 * i + 1] = (float)F.fy[i];
+    }
+  });
+  return n;
+}
+
+uint32_t orc_get_forces64(void* h, double* fxy, uint32_t max) {
+  Orc* o = static_cast<Orc*>(h);
+  uint32_t n = 0;
+  DISPATCH(o, {
+    n = (uint32_t)std::min<size_t>(max, F.fx.size());
+    for (uint32_t i = 0; i < n; i++) {
+      fxy[2 * i] = (double)F.fx[i];
+      fxy[2 * i + 1] = (double)F.fy[i];
+    }
+  });
+  return n;
+}
+
+// Neighbour list of particle i in visit order against the current state
+// (rebuilds the grid first). Returns the total count (may exceed max).
+uint32_t orc_neighbors(void* h, uint32_t i, uint32_t* out, uint32_t max) {
+  Orc* o = static_cast<Orc*>(h);
+  uint32_t n = 0;
+  DISPATCH(o, {
+    if (i < F.particles.size()) {
+      F.rebuild_grid();
+      std::vector<uint32_t> nb;
+      F.neighbors_of(F.particles[i].x, F.particles[i].y, F.particles, nb);
+      n = (uint32_t)nb.size();
+      for (uint32_t k = 0; k < n && k < max; k++) out[k] = nb[k];
+    }
+  });
+  return n;
+}
+
+// All neighbour lists at once: counts[i], lists[i*max_per + k].
+void orc_all_neighbors(void* h, uint32_t* counts, uint32_t* lists, uint32_t max_per) {
+  Orc* o = static_cast<Orc*>(h);
+  DISPATCH(o, {
+    F.rebuild_grid();
+    std::vector<uint32_t> nb;
+    for (size_t i = 0; i < F.particles.size(); i++) {
+      F.neighbors_of(F.particles[i].x, F.particles[i].y, F.particles, nb);
+      counts[i] = (uint32_t)nb.size();
+      for (uint32_t k = 0; k < nb.size() && k < max_per; k++) lists[i * max_per + k] = nb[k];
+    }
+  });
+}
+
+// Cell of every particle (cx, cy) as rebuild_grid computes it (fluid.rs:350-356).
+void orc_cells(void* h, int32_t* cx, int32_t* cy) {
+  Orc* o = static_cast<Orc*>(h);
+  DISPATCH(o, {
+    for (size_t i = 0; i < F.particles.size(); i++) F.cell_of(F.particles[i].x, F.particles[i].y, cx[i], cy[i]);
+  });
+}
+
+uint32_t orc_cfl_substeps(void* h, float dt) {
+  Orc* o = static_cast<Orc*>(h);
+  uint32_t r = 1;
+  DISPATCH(o, r = F.cfl_substeps(dt));
+  return r;
+}
+
+// scalar kernels for the reference's kernel-sanity tests (f32)
+float orc_poly6(float r2, float h) { return Fluid<float>::poly6(r2, h); }
+void orc_spiky(float rx, float ry, float r, float h, float* out2) {
+  Fluid<float>::spiky_grad(rx, ry, r, h, out2[0], out2[1]);
+}
+float orc_pressure(float d, float rho0, float k, float g) { return Fluid<float>::pressure(d, rho0, k, g); }
+float orc_artificial_pressure(float dx, float dy, float vrx, float vry, float r_sq, float h, float rho_bar,
+                              float c, float alpha) {
+  return Fluid<float>::artificial_pressure(dx, dy, vrx, vry, r_sq, h, rho_bar, c, alpha);
+}
+float orc_cohesion(float dist, float h) { return Fluid<float>::cohesion(dist, h); }
+
+}  // extern "C"

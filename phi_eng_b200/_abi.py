@@ -1,0 +1,163 @@
+"""ctypes binding of the C ABI in include/phieng_sph.h (libphieng_sph.so).
+
+The library is built in-tree by ``phi_eng_b200.build`` (nvcc, sm_100a). There
+is no fallback: if the shared object is missing or fails to load, importing
+the product API raises, so nothing can silently run a CPU path instead.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libphieng_sph.so")
+
+SHAPE_CIRCLE = 0
+SHAPE_BOX = 1
+
+OK = 0
+E_NO_DEVICE = 1
+E_CUDA = 2
+E_UNSUPPORTED = 3
+E_ARG = 4
+
+
+class FluidConfig2Ffi(C.Structure):
+    """#[repr(C)] FluidConfig2Ffi (crates/engine/src/ffi.rs:712-739), 112 bytes."""
+
+    _fields_ = [
+        ("particle_mass", C.c_float),
+        ("rest_density", C.c_float),
+        ("smoothing_length", C.c_float),
+        ("stiffness", C.c_float),
+        ("gamma", C.c_float),
+        ("artificial_viscosity", C.c_float),
+        ("surface_tension", C.c_float),
+        ("cfl", C.c_float),
+        ("max_substeps", C.c_uint32),
+        ("adaptive_resolution", C.c_uint8),
+        ("split_density_ratio", C.c_float),
+        ("merge_density_ratio", C.c_float),
+        ("boundary_particles", C.c_uint8),
+        ("viscosity", C.c_float),
+        ("drag", C.c_float),
+        ("wall_friction", C.c_float),
+        ("phase_count", C.c_uint8),
+        ("phase_rest_density", C.c_float * 4),
+        ("phase_mass", C.c_float * 4),
+        ("max_velocity", C.c_float),
+        ("particle_radius", C.c_float),
+        ("enabled", C.c_uint8),
+    ]
+
+
+assert C.sizeof(FluidConfig2Ffi) == 112
+
+
+def default_config() -> FluidConfig2Ffi:
+    """FluidConfig2::default() (crates/dynamics/src/fluid.rs:142-169)."""
+    c = FluidConfig2Ffi()
+    c.particle_mass = 0.0625
+    c.rest_density = 1.0
+    c.smoothing_length = 0.5
+    c.stiffness = 100.0
+    c.gamma = 1.0
+    c.artificial_viscosity = 0.0
+    c.surface_tension = 0.0
+    c.cfl = 0.0
+    c.max_substeps = 1
+    c.adaptive_resolution = 0
+    c.split_density_ratio = 0.5
+    c.merge_density_ratio = 1.6
+    c.boundary_particles = 0
+    c.viscosity = 0.3
+    c.drag = 4.0
+    c.wall_friction = 0.0
+    c.phase_count = 1
+    for k in range(4):
+        c.phase_rest_density[k] = 1.0
+        c.phase_mass[k] = 0.0625
+    c.max_velocity = 30.0
+    c.particle_radius = 0.125
+    c.enabled = 1
+    return c
+
+
+class PhiengSphStatus(C.Structure):
+    _fields_ = [
+        ("error", C.c_int32),
+        ("particles", C.c_uint32),
+        ("substeps", C.c_uint64),
+        ("grid_log2_w", C.c_uint32),
+        ("grid_log2_h", C.c_uint32),
+        ("sort_passes", C.c_uint32),
+        ("grid_cx0", C.c_int32),
+        ("grid_cy0", C.c_int32),
+        ("reserved", C.c_uint32),
+    ]
+
+
+_P = C.c_void_p
+_F = C.POINTER(C.c_float)
+_U32P = C.POINTER(C.c_uint32)
+_U8P = C.POINTER(C.c_uint8)
+
+# name -> (restype, argtypes); the exact set declared in include/phieng_sph.h
+SIGNATURES = {
+    "phieng_world_new": (_P, []),
+    "phieng_world_free": (None, [_P]),
+    "phieng_world_step": (None, [_P, C.c_float]),
+    "phieng_world_set_gravity": (None, [_P, C.c_float, C.c_float]),
+    "phieng_world_set_time": (C.c_int32, [_P, C.c_float]),
+    "phieng_world_get_time": (C.c_int32, [_P, _F]),
+    "phieng_world_body_count": (C.c_int32, [_P]),
+    "phieng_world_add_body": (
+        C.c_int32,
+        [_P, C.c_float, C.c_float, C.c_uint32, C.c_float, C.c_float, C.c_float, C.c_uint8,
+         C.c_float, C.c_float],
+    ),
+    "phieng_world_set_fluid_config": (C.c_int32, [_P, C.POINTER(FluidConfig2Ffi)]),
+    "phieng_world_get_fluid_config": (C.c_int32, [_P, C.POINTER(FluidConfig2Ffi)]),
+    "phieng_world_fluid_add": (C.c_uint32, [_P, _F, C.c_uint32]),
+    "phieng_world_fluid_add_phase": (C.c_uint32, [_P, _F, _U8P, C.c_uint32]),
+    "phieng_world_fluid_count": (C.c_uint32, [_P]),
+    "phieng_world_fluid_clear": (C.c_int32, [_P]),
+    "phieng_world_fluid_get": (C.c_uint32, [_P, _F, C.c_uint32]),
+    "phieng_sph_status": (C.c_int32, [_P, C.POINTER(PhiengSphStatus)]),
+    "phieng_sph_clear_error": (C.c_int32, [_P]),
+    "phieng_sph_error_string": (C.c_char_p, [_P]),
+    "phieng_sph_set_particle_cap": (C.c_int32, [_P, C.c_uint32]),
+    "phieng_sph_step_n": (C.c_int32, [_P, C.c_float, C.c_uint32]),
+    "phieng_sph_set_stream": (C.c_int32, [_P, _P]),
+    "phieng_sph_sync": (C.c_int32, [_P]),
+    "phieng_sph_set_state": (C.c_int32, [_P, _F, C.c_uint32]),
+    "phieng_sph_get_density_pressure": (C.c_uint32, [_P, _F, _F, C.c_uint32]),
+    "phieng_sph_replan": (C.c_int32, [_P]),
+    "phieng_sph_front_metrics": (C.c_int32, [_P, _F]),
+    "phieng_sph_set_profiling": (C.c_int32, [_P, C.c_int32]),
+    "phieng_sph_phase_times": (C.c_uint32, [_P, _F, C.c_uint32]),
+    "phieng_sph_debug_forces": (C.c_uint32, [_P, _F, C.c_uint32]),
+    "phieng_sph_debug_sorted": (C.c_uint32, [_P, _U32P, _U32P, C.c_uint32]),
+    "phieng_sph_debug_neighbors": (C.c_uint32, [_P, _U32P, _U32P, C.c_uint32, C.c_uint32]),
+}
+
+_lib = None
+
+
+def load(path: str = LIB_PATH) -> C.CDLL:
+    """Load libphieng_sph.so and bind every declared symbol; raise if absent."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(
+            f"{path} is missing: build it with `python -m phi_eng_b200.build` "
+            "(the SPH step has no CPU fallback)"
+        )
+    lib = C.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib

@@ -1,0 +1,214 @@
+// Device-side definitions shared by the SPH kernels.
+//
+// Arithmetic contract: this translation unit is compiled with --fmad=false
+// and IEEE division / square root (no fast-math), and every expression keeps
+// the evaluation order of the reference (crates/dynamics/src/fluid.rs), so
+// per-pair arithmetic is bit-identical to the reference's f32 arithmetic.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace phieng {
+
+// crates/math/src/math.rs:3-4
+constexpr float kEps = 1e-6f;
+constexpr float kEpsSq = 1e-12f;
+
+// Bucket grid. A particle's cell (cx, cy) = (floor(x/h), floor(y/h)) as
+// saturating i32 (fluid.rs:350-356) maps to bucket
+//   bx = (cx - cx0) mod W, by = (cy - cy0) mod H, key = by * W + bx,
+// W = 2^log2w, H = 2^log2h, both >= 4. Particles with a non-finite position
+// get key = nbuckets (sorted last, never visited), as rebuild_grid skips
+// them (fluid.rs:347-349). Cells that alias into one bucket are at least
+// (W - 2) cells apart, so the distance test (d2 < h*h) rejects every aliased
+// candidate and the per-particle visit order stays the reference's.
+struct GridPlan {
+  int32_t cx0, cy0;
+  uint32_t log2w, log2h;
+  uint32_t maskw, maskh;
+  uint32_t nbuckets;
+  float hg;  // config.smoothing_length (the raw value rebuild_grid uses)
+};
+
+enum StepFlags : uint32_t {
+  F_VISC = 1u << 0,      // XSPH (viscosity > 0)
+  F_AV = 1u << 1,        // Monaghan artificial viscosity (alpha > 0)
+  F_COHESION = 1u << 2,  // surface tension > 0
+  F_FRICTION = 1u << 3,  // wall friction > 0
+  F_TAIT = 1u << 4,      // gamma != 1
+  F_MASS = 1u << 5,      // per-particle mass array (non-uniform)
+  F_PHASE = 1u << 6,     // per-particle phase array (non-uniform rest density)
+};
+
+struct StepParams {
+  GridPlan grid;
+  float hg2;       // hg*hg: neighbour filter (fluid.rs:383)
+  float hk;        // max(h, EPS): kernel support (fluid.rs:908)
+  float hk2;       // hk*hk
+  float c_poly6;   // 4/(PI*h2*h2*h2*h2), f32, as fluid.rs:272 evaluates it
+  float c_spiky;   // -30/(PI*h*h*h*h*h), as fluid.rs:283
+  float rho_cap;   // 3*max(rest_density, EPS) (fluid.rs:605)
+  float stiffness;
+  float gamma;
+  float rest[4];   // phase_rest_density
+  float mass;      // uniform particle mass when !F_MASS
+  float visc;      // XSPH factor
+  float vmax;      // max_velocity
+  float dt;
+  float gx, gy;
+  float pr;        // max(particle_radius, 0)
+  float mu;        // clamp(wall_friction, 0, 1)
+  float av_alpha;
+  float c_s;       // sqrt(max(stiffness, 0))
+  float surface_tension;
+  uint32_t flags;
+  uint32_t nbodies;
+  uint32_t uniform_phase;  // phase used for every particle when !F_PHASE
+};
+
+// Static body as the fluid sees it: shape 0 = circle (a = radius), 1 = box
+// (a, b = half extents); rotation columns x_axis = (xax, xay), y_axis =
+// (yax, yay) (crates/math/src/math.rs:34-60).
+struct DevBody {
+  int32_t shape;
+  float px, py;
+  float xax, xay, yax, yay;
+  float a, b;
+};
+
+__device__ __forceinline__ bool finitef(float v) { return isfinite(v); }
+
+__device__ __forceinline__ uint32_t bucket_of_cell(int32_t cx, int32_t cy, const GridPlan& g) {
+  uint32_t bx = ((uint32_t)cx - (uint32_t)g.cx0) & g.maskw;
+  uint32_t by = ((uint32_t)cy - (uint32_t)g.cy0) & g.maskh;
+  return (by << g.log2w) | bx;
+}
+
+// cvt.rmi.s32.f32 = floor then saturating conversion with NaN -> 0, the
+// semantics of `(x / h).floor() as i32` (fluid.rs:351-354).
+__device__ __forceinline__ uint32_t bucket_key(float x, float y, const GridPlan& g) {
+  if (!finitef(x) || !finitef(y)) return g.nbuckets;
+  int32_t cx = __float2int_rd(__fdiv_rn(x, g.hg));
+  int32_t cy = __float2int_rd(__fdiv_rn(y, g.hg));
+  return bucket_of_cell(cx, cy, g);
+}
+
+// poly6 (fluid.rs:265-273) with the constant factor precomputed in f32 by
+// the same expression; (((c * t) * t) * t) keeps the reference order.
+__device__ __forceinline__ float poly6(float r2, const StepParams& P) {
+  if (r2 >= P.hk2 || r2 < 0.0f) return 0.0f;
+  float t = __fsub_rn(P.hk2, r2);
+  return __fmul_rn(__fmul_rn(__fmul_rn(P.c_poly6, t), t), t);
+}
+
+// equation of state (fluid.rs:290-297). powf is evaluated as a double pow
+// rounded once to f32, which is the correctly rounded x^gamma except in
+// double-rounding corner cases; glibc's powf is correctly rounded in
+// practice, so the two agree bit for bit almost always.
+__device__ __forceinline__ float eos(float density, float rho0, const StepParams& P) {
+  if (!(P.flags & F_TAIT)) {
+    return fmaxf(__fmul_rn(P.stiffness, __fsub_rn(density, rho0)), 0.0f);
+  }
+  float r0 = fmaxf(rho0, kEps);
+  float ratio = __fdiv_rn(density, r0);
+  float pw = (float)pow((double)ratio, (double)P.gamma);
+  return fmaxf(__fmul_rn(__fmul_rn(P.stiffness, r0), __fsub_rn(pw, 1.0f)), 0.0f);
+}
+
+// Particle vs static body (fluid.rs:463-533, circle and box branches).
+// Returns false when separated.
+__device__ __forceinline__ bool collide(float px, float py, float pr, const DevBody& b, float& nx,
+                                        float& ny, float& depth) {
+  if (b.shape == 0) {
+    float dx = __fsub_rn(px, b.px);
+    float dy = __fsub_rn(py, b.py);
+    float dist = __fsqrt_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)));
+    float rr = __fadd_rn(b.a, pr);
+    if (dist >= rr) return false;
+    if (dist > kEps) {
+      nx = __fdiv_rn(dx, dist);
+      ny = __fdiv_rn(dy, dist);
+    } else {
+      nx = 1.0f;
+      ny = 0.0f;
+    }
+    depth = __fsub_rn(rr, dist);
+    return true;
+  }
+  float rx = __fsub_rn(px, b.px);
+  float ry = __fsub_rn(py, b.py);
+  // fluid.rs:483-489 literally: x_axis.x*rel.x + y_axis.x*rel.y, ...
+  float lx = __fadd_rn(__fmul_rn(b.xax, rx), __fmul_rn(b.yax, ry));
+  float ly = __fadd_rn(__fmul_rn(b.xay, rx), __fmul_rn(b.yay, ry));
+  float hx = b.a, hy = b.b;
+  // f32::clamp: NaN passes through
+  float cxl = lx;
+  if (cxl < -hx) cxl = -hx;
+  if (cxl > hx) cxl = hx;
+  float cyl = ly;
+  if (cyl < -hy) cyl = -hy;
+  if (cyl > hy) cyl = hy;
+  float ddx = __fsub_rn(lx, cxl);
+  float ddy = __fsub_rn(ly, cyl);
+  float l2 = __fadd_rn(__fmul_rn(ddx, ddx), __fmul_rn(ddy, ddy));
+  float lnx, lny;
+  if (l2 > kEpsSq) {
+    float dist = __fsqrt_rn(l2);
+    if (dist >= pr) return false;
+    lnx = __fdiv_rn(ddx, dist);
+    lny = __fdiv_rn(ddy, dist);
+    depth = __fsub_rn(pr, dist);
+  } else {
+    float dxp = __fsub_rn(hx, fabsf(lx));
+    float dyp = __fsub_rn(hy, fabsf(ly));
+    // signum().copysign(1.0) is +1 (a NaN stays a positive NaN): the eject
+    // normal is always +x or +y in the box frame (fluid.rs:504-516).
+    if (dxp < dyp) {
+      lnx = (lx != lx) ? fabsf(lx) : 1.0f;
+      lny = 0.0f;
+      depth = __fadd_rn(pr, dxp);
+    } else {
+      lnx = 0.0f;
+      lny = (ly != ly) ? fabsf(ly) : 1.0f;
+      depth = __fadd_rn(pr, dyp);
+    }
+  }
+  // glam Mat2 * Vec2 = x_axis * v.x + y_axis * v.y
+  nx = __fadd_rn(__fmul_rn(b.xax, lnx), __fmul_rn(b.yax, lny));
+  ny = __fadd_rn(__fmul_rn(b.xay, lnx), __fmul_rn(b.yay, lny));
+  return true;
+}
+
+// Boundary response for one particle against every body in order
+// (fluid.rs:1056-1094). Statics take no impulse (body.rs:675-687) and have
+// zero velocity, which the no-slip branch reads.
+__device__ __forceinline__ void walls(float& x, float& y, float& vx, float& vy,
+                                      const DevBody* __restrict__ bodies, const StepParams& P) {
+  for (uint32_t k = 0; k < P.nbodies; k++) {
+    DevBody b = bodies[k];
+    float nx, ny, depth;
+    if (!collide(x, y, P.pr, b, nx, ny, depth)) continue;
+    if (depth <= 0.0f) continue;
+    x = __fadd_rn(x, __fmul_rn(nx, depth));
+    y = __fadd_rn(y, __fmul_rn(ny, depth));
+    float vn = __fadd_rn(__fmul_rn(vx, nx), __fmul_rn(vy, ny));
+    if (vn < 0.0f) {
+      vx = __fsub_rn(vx, __fmul_rn(nx, vn));
+      vy = __fsub_rn(vy, __fmul_rn(ny, vn));
+      if (P.flags & F_FRICTION) {
+        float vtx = vx, vty = vy;
+        float wvx = 0.0f, wvy = 0.0f;
+        float wdot = __fadd_rn(__fmul_rn(wvx, nx), __fmul_rn(wvy, ny));
+        float wtx = __fsub_rn(wvx, __fmul_rn(nx, wdot));
+        float wty = __fsub_rn(wvy, __fmul_rn(ny, wdot));
+        float dvx = __fmul_rn(__fsub_rn(wtx, vtx), P.mu);
+        float dvy = __fmul_rn(__fsub_rn(wty, vty), P.mu);
+        vx = __fadd_rn(vx, dvx);
+        vy = __fadd_rn(vy, dvy);
+      }
+    }
+  }
+}
+
+}  // namespace phieng

@@ -1,0 +1,80 @@
+// Host-side interface of the SPH kernel chain (sph_kernels.cu).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "sph_device.cuh"
+
+namespace phieng {
+
+constexpr uint32_t kSortThreads = 256;
+constexpr uint32_t kSortItems = 8;
+constexpr uint32_t kSortTile = kSortThreads * kSortItems;  // keys per sort tile
+
+// Device arrays of one fluid. "id order" = insertion order (the reference's
+// particle index); "sorted order" = (bucket key, id) order of the last sort.
+struct FluidBufs {
+  uint32_t cap = 0;          // particle capacity of every per-particle array
+  float4* state = nullptr;   // id order: (x, y, vx, vy)
+  float* mass = nullptr;     // id order (used when F_MASS)
+  uint8_t* phase = nullptr;  // id order (used when F_PHASE)
+  uint32_t* key = nullptr;   // id order: bucket key for the next sort
+  uint32_t* ka = nullptr;    // radix ping-pong
+  uint32_t* va = nullptr;
+  uint32_t* kb = nullptr;
+  uint32_t* vb = nullptr;
+  uint32_t* skey = nullptr;  // sorted keys
+  uint32_t* sid = nullptr;   // sorted slot -> particle id
+  float2* spos = nullptr;    // sorted (x, y)
+  float2* svel = nullptr;    // sorted (vx, vy)
+  float* smass = nullptr;    // sorted mass (F_MASS)
+  uint8_t* sphase = nullptr; // sorted phase (F_PHASE)
+  float2* sdq = nullptr;     // sorted (density, pressure / max(density,EPS)^2)
+  float* spres = nullptr;    // sorted pressure
+  uint32_t* hist = nullptr;  // radix tile histograms, [digit][tile]
+  uint32_t hist_len = 0;
+  int2* range = nullptr;     // per bucket [start, end) in sorted order
+  uint32_t range_cap = 0;    // buckets allocated
+  DevBody* bodies = nullptr;
+  uint32_t bodies_cap = 0;
+  unsigned int* scalar = nullptr;  // small device scratch (vmax etc.)
+};
+
+struct SortPlan {
+  uint32_t passes;   // digit passes
+  uint32_t bits;     // digit width
+};
+
+SortPlan sort_plan(uint32_t nbuckets);
+
+// K1: bucket key of every particle from its position (id order).
+void enqueue_keys(const FluidBufs& b, uint32_t n, const GridPlan& g, cudaStream_t st);
+
+// K2+K4: stable LSD radix sort of (key, id) pairs, the last pass gathering
+// the particle state into sorted order. K3: per-bucket ranges.
+void enqueue_sort_and_ranges(const FluidBufs& b, uint32_t n, const StepParams& P, cudaStream_t st);
+
+// K5: density + EOS in sorted order.
+void enqueue_density(const FluidBufs& b, uint32_t n, const StepParams& P, cudaStream_t st);
+
+// K6: pressure force + XSPH + integrate + walls; writes state and next keys
+// in id order. With dbg_force != nullptr it only writes the forces (id
+// order) and leaves the state untouched.
+void enqueue_force_integrate(const FluidBufs& b, uint32_t n, const StepParams& P, float2* dbg_force,
+                             cudaStream_t st);
+
+// Scatter the sorted density / pressure back to id order.
+void enqueue_unsort_dp(const FluidBufs& b, uint32_t n, float* dens, float* pres, cudaStream_t st);
+
+// Neighbour lists in visit order (id order), for the parity tests.
+void enqueue_debug_neighbors(const FluidBufs& b, uint32_t n, const StepParams& P, uint32_t* counts,
+                             uint32_t* lists, uint32_t max_per, cudaStream_t st);
+
+// max_i |v_i| (f32::max semantics, NaN ignored) as float bits in b.scalar[0].
+void enqueue_vmax(const FluidBufs& b, uint32_t n, cudaStream_t st);
+
+// b.scalar[2] = order-preserving bits of max_i x_i, b.scalar[3] = bits of max_i |v_i|.
+void enqueue_front_metrics(const FluidBufs& b, uint32_t n, cudaStream_t st);
+
+}  // namespace phieng

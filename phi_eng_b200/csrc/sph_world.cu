@@ -1,0 +1,964 @@
+// World2 and the C ABI of libphieng_sph.so (include/phieng_sph.h).
+//
+// The world mirrors the slice of the reference's World2 that the fluid step
+// reads (crates/dynamics/src/world.rs: gravity, time, static bodies, the
+// FluidState2) and keeps the particle state resident on the GPU. Host
+// mirrors of the state exist only to serve the copy-in / copy-out entry
+// points; a validity flag on each side says which copy is current.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/phieng_sph.h"
+#include "sph_kernels.h"
+
+using namespace phieng;
+
+namespace {
+
+constexpr uint32_t kMaxParticles2D = 4096;      // MAX_PARTICLES_2D (fluid.rs:30)
+constexpr uint32_t kMaxAddPerCall = 1000000;    // ffi.rs:2493
+constexpr float kMaxDt = 1.0f / 15.0f;          // ffi.rs:80
+
+inline float rmaxf(float a, float b) {  // f32::max: a NaN operand loses
+  if (a != a) return b;
+  if (b != b) return a;
+  return a > b ? a : b;
+}
+
+inline int32_t sat_floor_i32(float v) {  // `v.floor() as i32`
+  float f = std::floor(v);
+  if (f != f) return 0;
+  if (f >= 2147483648.0f) return INT32_MAX;
+  if (f <= -2147483648.0f) return INT32_MIN;
+  return (int32_t)f;
+}
+
+inline uint32_t next_pow2(uint64_t v) {
+  uint32_t p = 1;
+  while (p < v && p < (1u << 31)) p <<= 1;
+  return p;
+}
+
+inline uint32_t log2u(uint32_t v) {
+  uint32_t l = 0;
+  while ((1u << l) < v) l++;
+  return l;
+}
+
+FluidConfig2Ffi default_config() {  // FluidConfig2::default (fluid.rs:142-169)
+  FluidConfig2Ffi c;
+  std::memset(&c, 0, sizeof(c));
+  c.particle_mass = 0.0625f;
+  c.rest_density = 1.0f;
+  c.smoothing_length = 0.5f;
+  c.stiffness = 100.0f;
+  c.gamma = 1.0f;
+  c.artificial_viscosity = 0.0f;
+  c.surface_tension = 0.0f;
+  c.cfl = 0.0f;
+  c.max_substeps = 1;
+  c.adaptive_resolution = 0;
+  c.split_density_ratio = 0.5f;
+  c.merge_density_ratio = 1.6f;
+  c.boundary_particles = 0;
+  c.viscosity = 0.3f;
+  c.drag = 4.0f;
+  c.wall_friction = 0.0f;
+  c.phase_count = 1;
+  for (int k = 0; k < 4; k++) {
+    c.phase_rest_density[k] = 1.0f;
+    c.phase_mass[k] = 0.0625f;
+  }
+  c.max_velocity = 30.0f;
+  c.particle_radius = 0.125f;
+  c.enabled = 1;
+  return c;
+}
+
+// fluid2_from_ffi validation (ffi.rs:773-855).
+bool valid_config(const FluidConfig2Ffi& c) {
+  const float fs[] = {c.particle_mass,         c.rest_density,          c.smoothing_length,
+                      c.stiffness,             c.gamma,                 c.artificial_viscosity,
+                      c.surface_tension,       c.cfl,                   c.split_density_ratio,
+                      c.merge_density_ratio,   c.viscosity,             c.drag,
+                      c.wall_friction,         c.max_velocity,          c.particle_radius,
+                      c.phase_rest_density[0], c.phase_rest_density[1], c.phase_rest_density[2],
+                      c.phase_rest_density[3], c.phase_mass[0],         c.phase_mass[1],
+                      c.phase_mass[2],         c.phase_mass[3]};
+  for (float v : fs)
+    if (!std::isfinite(v)) return false;
+  if (c.particle_mass <= 0.0f || c.rest_density <= 0.0f || c.smoothing_length <= 0.0f || c.stiffness < 0.0f ||
+      c.gamma < 1.0f || c.artificial_viscosity < 0.0f || c.artificial_viscosity > 2.0f ||
+      c.surface_tension < 0.0f || c.cfl < 0.0f || c.cfl > 1.0f || c.max_substeps < 1 ||
+      c.split_density_ratio <= 0.0f || c.merge_density_ratio <= 1.0f || c.viscosity < 0.0f ||
+      c.viscosity > 1.0f || c.drag < 0.0f || c.wall_friction < 0.0f || c.wall_friction > 1.0f ||
+      c.phase_count < 1 || c.phase_count > 4 || c.max_velocity < 0.0f || c.particle_radius < 0.0f)
+    return false;
+  for (int k = 0; k < 4; k++)
+    if (c.phase_rest_density[k] <= 0.0f || c.phase_mass[k] <= 0.0f) return false;
+  return true;
+}
+
+const char* error_text(int32_t e) {
+  switch (e) {
+    case PHIENG_SPH_OK:
+      return "ok";
+    case PHIENG_SPH_E_NO_DEVICE:
+      return "no usable CUDA device";
+    case PHIENG_SPH_E_CUDA:
+      return "a CUDA call failed";
+    case PHIENG_SPH_E_UNSUPPORTED:
+      return "the fluid config enables adaptive resolution or boundary particles, which this library does not "
+             "implement";
+    case PHIENG_SPH_E_ARG:
+      return "invalid argument";
+    default:
+      return "unknown error";
+  }
+}
+
+}  // namespace
+
+struct World2 {
+  FluidConfig2Ffi cfg = default_config();
+  float gx = 0.0f, gy = -9.81f;  // World2::new (world.rs:338)
+  float time = 0.0f;
+  std::vector<DevBody> bodies;
+  bool bodies_dirty = true;
+  uint32_t cap = kMaxParticles2D;
+
+  // particles (host mirror); mass and phase are fixed at insertion
+  uint32_t n = 0;
+  std::vector<float4> h_state;
+  std::vector<float> h_mass;
+  std::vector<uint8_t> h_phase;
+  std::vector<float> h_dens, h_pres;
+  bool mass_uniform = true;
+  float mass_value = 0.0f;
+  bool phase_uniform = true;
+  uint32_t phase_value = 0;
+
+  bool host_state_valid = true;
+  bool dev_state_valid = false;
+  bool dev_aux_valid = false;
+  bool dp_on_device = false;
+  bool keys_valid = false;
+  bool plan_valid = false;
+  GridPlan plan{};
+
+  int device = -1;
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  bool user_stream = false;
+  FluidBufs d;
+  float* d_tmp = nullptr;
+  size_t d_tmp_bytes = 0;
+  unsigned int* h_pinned = nullptr;
+
+  cudaGraphExec_t gexec = nullptr;
+  std::string gsig;
+
+  // phase timing: events recorded between the phases of every substep
+  bool profiling = false;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+
+  int32_t error = PHIENG_SPH_OK;
+  uint64_t substeps = 0;
+};
+
+namespace {
+
+void set_error(World2* w, int32_t e, const char* what) {
+  if (w->error == PHIENG_SPH_OK) {
+    w->error = e;
+    std::fprintf(stderr, "phieng_sph: %s (%s)\n", error_text(e), what ? what : "");
+  }
+}
+
+bool cuda_ok(World2* w, cudaError_t r, const char* what) {
+  if (r == cudaSuccess) return true;
+  cudaGetLastError();
+  if (w->error == PHIENG_SPH_OK) {
+    w->error = PHIENG_SPH_E_CUDA;
+    std::fprintf(stderr, "phieng_sph: %s failed: %s\n", what, cudaGetErrorString(r));
+  }
+  return false;
+}
+
+template <class T>
+void dfree(T*& p) {
+  if (p) cudaFree(p);
+  p = nullptr;
+}
+
+void free_particle_buffers(FluidBufs& d) {
+  dfree(d.state);
+  dfree(d.mass);
+  dfree(d.phase);
+  dfree(d.key);
+  dfree(d.ka);
+  dfree(d.va);
+  dfree(d.kb);
+  dfree(d.vb);
+  dfree(d.skey);
+  dfree(d.sid);
+  dfree(d.spos);
+  dfree(d.svel);
+  dfree(d.smass);
+  dfree(d.sphase);
+  dfree(d.sdq);
+  dfree(d.spres);
+  dfree(d.hist);
+  d.cap = 0;
+  d.hist_len = 0;
+}
+
+void release_graph(World2* w) {
+  if (w->gexec) cudaGraphExecDestroy(w->gexec);
+  w->gexec = nullptr;
+  w->gsig.clear();
+}
+
+bool ensure_device(World2* w) {
+  if (w->device >= 0) return true;
+  int count = 0;
+  cudaError_t r = cudaGetDeviceCount(&count);
+  if (r != cudaSuccess || count == 0) {
+    cudaGetLastError();
+    set_error(w, PHIENG_SPH_E_NO_DEVICE, "cudaGetDeviceCount");
+    return false;
+  }
+  int dev = 0;
+  if (!cuda_ok(w, cudaGetDevice(&dev), "cudaGetDevice")) return false;
+  if (!cuda_ok(w, cudaStreamCreateWithFlags(&w->own_stream, cudaStreamNonBlocking), "cudaStreamCreate"))
+    return false;
+  if (!w->user_stream) w->stream = w->own_stream;
+  if (!cuda_ok(w, cudaMalloc(&w->d.scalar, 64), "cudaMalloc(scalar)")) return false;
+  if (!cuda_ok(w, cudaMallocHost(&w->h_pinned, 64), "cudaMallocHost")) return false;
+  w->device = dev;
+  return true;
+}
+
+template <class T>
+bool dalloc(World2* w, T*& p, size_t count) {
+  return cuda_ok(w, cudaMalloc(&p, sizeof(T) * std::max<size_t>(count, 1)), "cudaMalloc");
+}
+
+bool ensure_capacity(World2* w, uint32_t need) {
+  FluidBufs& d = w->d;
+  if (need <= d.cap && d.state) return true;
+  cudaStreamSynchronize(w->stream);
+  free_particle_buffers(d);
+  release_graph(w);
+  uint32_t c = std::max<uint32_t>(need, 1024);
+  bool ok = dalloc(w, d.state, c) && dalloc(w, d.mass, c) && dalloc(w, d.phase, c) && dalloc(w, d.key, c) &&
+            dalloc(w, d.ka, c) && dalloc(w, d.va, c) && dalloc(w, d.kb, c) && dalloc(w, d.vb, c) &&
+            dalloc(w, d.skey, c) && dalloc(w, d.sid, c) && dalloc(w, d.spos, c) && dalloc(w, d.svel, c) &&
+            dalloc(w, d.smass, c) && dalloc(w, d.sphase, c) && dalloc(w, d.sdq, c) && dalloc(w, d.spres, c);
+  uint32_t ntiles = (c + kSortTile - 1) / kSortTile;
+  ok = ok && dalloc(w, d.hist, (size_t)256 * ntiles);
+  if (!ok) {
+    free_particle_buffers(d);
+    return false;
+  }
+  d.cap = c;
+  d.hist_len = 256 * ntiles;
+  w->dev_state_valid = false;
+  w->dev_aux_valid = false;
+  w->dp_on_device = false;
+  w->keys_valid = false;
+  return true;
+}
+
+bool ensure_tmp(World2* w, size_t bytes) {
+  if (bytes <= w->d_tmp_bytes && w->d_tmp) return true;
+  dfree(w->d_tmp);
+  w->d_tmp_bytes = 0;
+  if (!cuda_ok(w, cudaMalloc(&w->d_tmp, bytes), "cudaMalloc(tmp)")) return false;
+  w->d_tmp_bytes = bytes;
+  return true;
+}
+
+// Download the particle state if the device copy is the current one.
+bool ensure_host_state(World2* w) {
+  if (w->host_state_valid) return true;
+  if (!cuda_ok(w, cudaMemcpyAsync(w->h_state.data(), w->d.state, sizeof(float4) * w->n, cudaMemcpyDeviceToHost,
+                                  w->stream),
+               "download state"))
+    return false;
+  if (!cuda_ok(w, cudaStreamSynchronize(w->stream), "sync")) return false;
+  w->host_state_valid = true;
+  return true;
+}
+
+bool ensure_host_dp(World2* w) {
+  if (!w->dp_on_device) return true;
+  if (w->n == 0) {
+    w->dp_on_device = false;
+    return true;
+  }
+  if (!ensure_tmp(w, sizeof(float) * 2 * (size_t)w->n)) return false;
+  enqueue_unsort_dp(w->d, w->n, w->d_tmp, w->d_tmp + w->n, w->stream);
+  if (!cuda_ok(w, cudaGetLastError(), "unsort")) return false;
+  cudaMemcpyAsync(w->h_dens.data(), w->d_tmp, sizeof(float) * w->n, cudaMemcpyDeviceToHost, w->stream);
+  cudaMemcpyAsync(w->h_pres.data(), w->d_tmp + w->n, sizeof(float) * w->n, cudaMemcpyDeviceToHost, w->stream);
+  if (!cuda_ok(w, cudaStreamSynchronize(w->stream), "sync")) return false;
+  w->dp_on_device = false;
+  return true;
+}
+
+// Bucket grid from the particle bounding box (host copy must be current).
+void plan_grid(World2* w) {
+  const float hg = w->cfg.smoothing_length;
+  int64_t x0 = INT64_MAX, x1 = INT64_MIN, y0 = INT64_MAX, y1 = INT64_MIN;
+  for (uint32_t i = 0; i < w->n; i++) {
+    float4 s = w->h_state[i];
+    if (!std::isfinite(s.x) || !std::isfinite(s.y)) continue;
+    int32_t cx = sat_floor_i32(s.x / hg), cy = sat_floor_i32(s.y / hg);
+    x0 = std::min<int64_t>(x0, cx);
+    x1 = std::max<int64_t>(x1, cx);
+    y0 = std::min<int64_t>(y0, cy);
+    y1 = std::max<int64_t>(y1, cy);
+  }
+  if (x0 > x1) x0 = x1 = y0 = y1 = 0;
+  const int64_t sx = x1 - x0 + 1, sy = y1 - y0 + 1;
+  const int64_t mx = std::max<int64_t>(2, sx / 8), my = std::max<int64_t>(2, sy / 8);
+  uint32_t W = std::max<uint32_t>(4, next_pow2((uint64_t)(sx + 2 * mx)));
+  uint32_t H = std::max<uint32_t>(4, next_pow2((uint64_t)(sy + 2 * my)));
+  // bucket budget: ~2 buckets per particle (the range table costs 8 B each)
+  const uint64_t budget = std::min<uint64_t>(1ull << 24, std::max<uint64_t>(1ull << 12, next_pow2(2ull * w->n)));
+  while ((uint64_t)W * H > budget) {
+    if (W >= H && W > 4)
+      W >>= 1;
+    else if (H > 4)
+      H >>= 1;
+    else
+      break;
+  }
+  GridPlan g;
+  g.log2w = log2u(W);
+  g.log2h = log2u(H);
+  g.maskw = W - 1;
+  g.maskh = H - 1;
+  g.nbuckets = W * H;
+  g.cx0 = (int32_t)std::max<int64_t>(INT32_MIN, x0 - mx);
+  g.cy0 = (int32_t)std::max<int64_t>(INT32_MIN, y0 - my);
+  g.hg = hg;
+  w->plan = g;
+  w->plan_valid = true;
+  w->keys_valid = false;
+}
+
+bool ensure_range(World2* w) {
+  FluidBufs& d = w->d;
+  if (d.range && d.range_cap >= w->plan.nbuckets) return true;
+  cudaStreamSynchronize(w->stream);
+  dfree(d.range);
+  d.range_cap = 0;
+  release_graph(w);
+  if (!dalloc(w, d.range, w->plan.nbuckets)) return false;
+  d.range_cap = w->plan.nbuckets;
+  return true;
+}
+
+bool ensure_bodies(World2* w) {
+  if (!w->bodies_dirty) return true;
+  FluidBufs& d = w->d;
+  uint32_t nb = (uint32_t)w->bodies.size();
+  if (nb > d.bodies_cap || !d.bodies) {
+    cudaStreamSynchronize(w->stream);
+    dfree(d.bodies);
+    release_graph(w);
+    uint32_t c = std::max<uint32_t>(16, nb);
+    if (!dalloc(w, d.bodies, c)) return false;
+    d.bodies_cap = c;
+  }
+  if (nb && !cuda_ok(w, cudaMemcpyAsync(d.bodies, w->bodies.data(), sizeof(DevBody) * nb, cudaMemcpyHostToDevice,
+                                        w->stream),
+                     "upload bodies"))
+    return false;
+  w->bodies_dirty = false;
+  return true;
+}
+
+// Everything a substep needs: device, buffers, current state on the device,
+// a bucket grid, the bodies and valid keys.
+bool prepare(World2* w) {
+  if (w->error != PHIENG_SPH_OK) return false;
+  if (!ensure_device(w)) return false;
+  if (!w->dev_state_valid) {
+    if (!ensure_capacity(w, w->n)) return false;
+    if (!w->plan_valid) plan_grid(w);
+    if (w->n && !cuda_ok(w, cudaMemcpyAsync(w->d.state, w->h_state.data(), sizeof(float4) * w->n,
+                                            cudaMemcpyHostToDevice, w->stream),
+                         "upload state"))
+      return false;
+    w->dev_state_valid = true;
+    w->keys_valid = false;
+  }
+  if (!w->dev_aux_valid && (!w->mass_uniform || !w->phase_uniform) && w->n) {
+    cudaMemcpyAsync(w->d.mass, w->h_mass.data(), sizeof(float) * w->n, cudaMemcpyHostToDevice, w->stream);
+    cudaMemcpyAsync(w->d.phase, w->h_phase.data(), w->n, cudaMemcpyHostToDevice, w->stream);
+    w->dev_aux_valid = true;
+  }
+  if (!w->plan_valid) {
+    if (!ensure_host_state(w)) return false;
+    plan_grid(w);
+  }
+  if (!ensure_range(w)) return false;
+  if (!ensure_bodies(w)) return false;
+  if (!w->keys_valid) {
+    enqueue_keys(w->d, w->n, w->plan, w->stream);
+    w->keys_valid = true;
+  }
+  return cuda_ok(w, cudaGetLastError(), "prepare");
+}
+
+StepParams make_params(const World2* w, float dt) {
+  const FluidConfig2Ffi& c = w->cfg;
+  StepParams P;
+  std::memset(&P, 0, sizeof(P));
+  P.grid = w->plan;
+  const float hg = c.smoothing_length;
+  P.hg2 = hg * hg;
+  const float h = rmaxf(hg, kEps);  // substep's h (fluid.rs:908)
+  P.hk = h;
+  const float h2 = h * h;
+  P.hk2 = h2;
+  const float pi = 3.14159265358979323846f;  // std::f32::consts::PI
+  P.c_poly6 = 4.0f / (pi * h2 * h2 * h2 * h2);
+  P.c_spiky = -30.0f / (pi * h * h * h * h * h);
+  P.rho_cap = 3.0f * rmaxf(c.rest_density, kEps);
+  P.stiffness = c.stiffness;
+  P.gamma = c.gamma;
+  for (int k = 0; k < 4; k++) P.rest[k] = c.phase_rest_density[k];
+  P.mass = w->mass_value;
+  P.visc = c.viscosity;
+  P.vmax = c.max_velocity;
+  P.dt = dt;
+  P.gx = w->gx;
+  P.gy = w->gy;
+  P.pr = rmaxf(c.particle_radius, 0.0f);
+  float mu = c.wall_friction;
+  if (mu < 0.0f) mu = 0.0f;
+  if (mu > 1.0f) mu = 1.0f;
+  P.mu = mu;
+  P.av_alpha = c.artificial_viscosity;
+  P.c_s = std::sqrt(rmaxf(c.stiffness, 0.0f));
+  P.surface_tension = c.surface_tension;
+  uint32_t f = 0;
+  if (c.viscosity > 0.0f) f |= F_VISC;
+  if (c.artificial_viscosity > 0.0f) f |= F_AV;
+  if (c.surface_tension > 0.0f) f |= F_COHESION;
+  if (c.wall_friction > 0.0f) f |= F_FRICTION;
+  if (c.gamma != 1.0f) f |= F_TAIT;
+  if (!w->mass_uniform) f |= F_MASS;
+  if (!w->phase_uniform) f |= F_PHASE;
+  P.flags = f;
+  P.nbodies = (uint32_t)w->bodies.size();
+  P.uniform_phase = w->phase_value;
+  return P;
+}
+
+void enqueue_substep_body(World2* w, const StepParams& P, cudaStream_t st) {
+  if (w->profiling) cudaEventRecordWithFlags(w->ev[0], st, cudaEventRecordExternal);
+  enqueue_sort_and_ranges(w->d, w->n, P, st);
+  if (w->profiling) cudaEventRecordWithFlags(w->ev[1], st, cudaEventRecordExternal);
+  enqueue_density(w->d, w->n, P, st);
+  if (w->profiling) cudaEventRecordWithFlags(w->ev[2], st, cudaEventRecordExternal);
+  enqueue_force_integrate(w->d, w->n, P, nullptr, st);
+  if (w->profiling) cudaEventRecordWithFlags(w->ev[3], st, cudaEventRecordExternal);
+}
+
+// One substep, replayed from a cached CUDA graph while the launch
+// parameters stay the same.
+bool run_substep(World2* w, const StepParams& P) {
+  // Buffer reallocations release the graph, so the parameters and the
+  // particle count identify it.
+  std::string sig((const char*)&P, sizeof(P));
+  sig.append((const char*)&w->n, sizeof(w->n));
+  sig.push_back(w->profiling ? 'p' : '-');
+  if (!w->gexec || sig != w->gsig) {
+    release_graph(w);
+    cudaGraph_t g = nullptr;
+    if (!cuda_ok(w, cudaStreamBeginCapture(w->own_stream, cudaStreamCaptureModeThreadLocal), "begin capture"))
+      return false;
+    enqueue_substep_body(w, P, w->own_stream);
+    cudaError_t r = cudaStreamEndCapture(w->own_stream, &g);
+    if (!cuda_ok(w, r, "end capture")) return false;
+    r = cudaGraphInstantiate(&w->gexec, g, 0);
+    cudaGraphDestroy(g);
+    if (!cuda_ok(w, r, "graph instantiate")) {
+      w->gexec = nullptr;
+      return false;
+    }
+    w->gsig = sig;
+  }
+  if (!cuda_ok(w, cudaGraphLaunch(w->gexec, w->stream), "graph launch")) return false;
+  w->substeps++;
+  w->host_state_valid = false;
+  w->dp_on_device = true;
+  w->keys_valid = true;
+  return true;
+}
+
+// cfl_substeps (fluid.rs:562-588); vmax from the current state.
+bool cfl_substeps(World2* w, float dt, uint32_t* out) {
+  const FluidConfig2Ffi& c = w->cfg;
+  uint32_t mx = std::max<uint32_t>(c.max_substeps, 1);
+  *out = 1;
+  if (c.cfl <= 0.0f || mx <= 1) return true;
+  const float h = rmaxf(c.smoothing_length, kEps);
+  const float rho0 = rmaxf(c.rest_density, kEps);
+  const float c0 = (c.gamma == 1.0f) ? std::sqrt(rmaxf(c.stiffness, 0.0f))
+                                     : std::sqrt(c.gamma * rmaxf(c.stiffness, 0.0f) * rho0);
+  float vmax = 0.0f;
+  if (w->host_state_valid) {
+    for (uint32_t i = 0; i < w->n; i++) {
+      float4 s = w->h_state[i];
+      vmax = rmaxf(vmax, std::sqrt(s.z * s.z + s.w * s.w));
+    }
+  } else {
+    enqueue_vmax(w->d, w->n, w->stream);
+    if (!cuda_ok(w, cudaMemcpyAsync(w->h_pinned, w->d.scalar, 4, cudaMemcpyDeviceToHost, w->stream), "vmax"))
+      return false;
+    if (!cuda_ok(w, cudaStreamSynchronize(w->stream), "sync")) return false;
+    std::memcpy(&vmax, w->h_pinned, 4);
+  }
+  const float speed = c0 + vmax;
+  if (!std::isfinite(speed) || speed <= kEps) return true;
+  const float dt_max = c.cfl * h / speed;
+  if (!std::isfinite(dt_max) || dt_max <= 0.0f) return true;
+  const float q = std::ceil(dt / dt_max);
+  int64_t k;
+  if (q != q)
+    k = 0;
+  else if (q >= 9.2233720368547758e18f)
+    k = INT64_MAX;
+  else
+    k = (int64_t)q;
+  k = std::max<int64_t>(1, std::min<int64_t>(k, mx));
+  *out = (uint32_t)k;
+  return true;
+}
+
+bool unsupported(World2* w) {
+  if (w->cfg.adaptive_resolution || w->cfg.boundary_particles) {
+    set_error(w, PHIENG_SPH_E_UNSUPPORTED, "step");
+    return true;
+  }
+  return false;
+}
+
+// World2::step (world.rs:706-732) restricted to the fluid phase (1b).
+bool world_step(World2* w, float dt) {
+  if (w->cfg.enabled && w->n > 0 && dt > 0.0f) {  // step_fluid guards (fluid.rs:550-552)
+    if (unsupported(w)) return false;
+    if (!prepare(w)) return false;
+    uint32_t ns = 1;
+    if (!cfl_substeps(w, dt, &ns)) return false;
+    const float sub = dt / (float)ns;
+    const StepParams P = make_params(w, sub);
+    for (uint32_t k = 0; k < ns; k++)
+      if (!run_substep(w, P)) return false;
+  }
+  w->time += dt;
+  return true;
+}
+
+void recompute_uniformity(World2* w) {
+  w->mass_uniform = true;
+  w->phase_uniform = true;
+  if (w->n == 0) {
+    w->mass_value = 0.0f;
+    w->phase_value = 0;
+    return;
+  }
+  uint32_t m0;
+  std::memcpy(&m0, &w->h_mass[0], 4);
+  w->mass_value = w->h_mass[0];
+  w->phase_value = std::min<uint32_t>(w->h_phase[0], 3);
+  for (uint32_t i = 1; i < w->n; i++) {
+    uint32_t mi;
+    std::memcpy(&mi, &w->h_mass[i], 4);
+    if (mi != m0) w->mass_uniform = false;
+    if (std::min<uint32_t>(w->h_phase[i], 3) != w->phase_value) w->phase_uniform = false;
+  }
+}
+
+// add_particles_phase (fluid.rs:241-257) behind the FFI checks (ffi.rs:2486-2539).
+uint32_t add_particles(World2* w, const float* xy, const uint8_t* phases, uint32_t count) {
+  uint32_t n = std::min(count, kMaxAddPerCall);
+  for (uint64_t i = 0; i < 2ull * n; i++)
+    if (!std::isfinite(xy[i])) return 0;
+  uint32_t room = w->cap > w->n ? w->cap - w->n : 0;
+  n = std::min(n, room);
+  if (n == 0) return 0;
+  if (!ensure_host_state(w) || !ensure_host_dp(w)) return 0;
+  for (uint32_t i = 0; i < n; i++) {
+    uint8_t ph = phases ? phases[i] : 0;
+    uint32_t k = std::min<uint32_t>(ph, 3);
+    w->h_state.push_back(make_float4(xy[2 * i], xy[2 * i + 1], 0.0f, 0.0f));
+    w->h_dens.push_back(w->cfg.phase_rest_density[k]);
+    w->h_pres.push_back(0.0f);
+    w->h_mass.push_back(rmaxf(w->cfg.phase_mass[k], 0.0f));
+    w->h_phase.push_back(ph);
+  }
+  w->n += n;
+  recompute_uniformity(w);
+  w->dev_state_valid = false;
+  w->dev_aux_valid = false;
+  w->plan_valid = false;
+  w->keys_valid = false;
+  return n;
+}
+
+}  // namespace
+
+// =====================================================================
+// C ABI
+// =====================================================================
+extern "C" {
+
+World2* phieng_world_new(void) { return new (std::nothrow) World2(); }
+
+void phieng_world_free(World2* w) {
+  if (!w) return;
+  if (w->device >= 0) {
+    cudaStreamSynchronize(w->stream);
+    release_graph(w);
+    free_particle_buffers(w->d);
+    dfree(w->d.range);
+    dfree(w->d.bodies);
+    dfree(w->d.scalar);
+    dfree(w->d_tmp);
+    for (auto& e : w->ev)
+      if (e) cudaEventDestroy(e);
+    if (w->h_pinned) cudaFreeHost(w->h_pinned);
+    if (w->own_stream) cudaStreamDestroy(w->own_stream);
+  }
+  delete w;
+}
+
+void phieng_world_step(World2* w, float dt) {
+  if (!w || !std::isfinite(dt) || dt <= 0.0f) return;
+  world_step(w, std::min(dt, kMaxDt));
+}
+
+void phieng_world_set_gravity(World2* w, float gx, float gy) {
+  if (!w || !std::isfinite(gx) || !std::isfinite(gy)) return;
+  w->gx = gx;
+  w->gy = gy;
+}
+
+int32_t phieng_world_set_time(World2* w, float t) {
+  if (!w || !std::isfinite(t)) return 0;
+  w->time = t;
+  return 1;
+}
+
+int32_t phieng_world_get_time(World2* w, float* out) {
+  if (!w || !out) return 0;
+  *out = w->time;
+  return 1;
+}
+
+int32_t phieng_world_body_count(World2* w) {
+  if (!w) return -1;
+  return (int32_t)w->bodies.size();
+}
+
+int32_t phieng_world_add_body(World2* w, float px, float py, uint32_t shape_tag, float a, float b, float density,
+                              uint8_t is_static, float friction, float restitution) {
+  (void)friction;
+  (void)restitution;
+  if (!w || !std::isfinite(px) || !std::isfinite(py)) return -1;
+  DevBody bd;
+  std::memset(&bd, 0, sizeof(bd));
+  auto pos = [](float v) { return std::isfinite(v) && v > 0.0f; };
+  if (shape_tag == PHIENG_SHAPE_CIRCLE && pos(a)) {
+    bd.shape = 0;
+    bd.a = a;
+  } else if (shape_tag == PHIENG_SHAPE_BOX && pos(a) && pos(b)) {
+    bd.shape = 1;
+    bd.a = a;
+    bd.b = b;
+  } else {
+    return -1;
+  }
+  if (!pos(density)) return -1;
+  if (!is_static) return -1;  // dynamic bodies are not part of this library
+  bd.px = px;
+  bd.py = py;
+  // Transform2::from_position_angle(p, 0.0) (ffi.rs:1184): Mat2::from_angle(0)
+  // = columns (cos, sin), (-sin, cos) = (1, 0), (-0, 1).
+  bd.xax = 1.0f;
+  bd.xay = 0.0f;
+  bd.yax = -0.0f;
+  bd.yay = 1.0f;
+  if (w->bodies.size() >= 0x7FFFFFFF) return -1;
+  w->bodies.push_back(bd);
+  w->bodies_dirty = true;
+  return (int32_t)(w->bodies.size() - 1);
+}
+
+int32_t phieng_world_set_fluid_config(World2* w, const FluidConfig2Ffi* cfg) {
+  if (!w || !cfg) return 0;
+  if (!valid_config(*cfg)) return 0;
+  FluidConfig2Ffi c = *cfg;
+  c.adaptive_resolution = c.adaptive_resolution ? 1 : 0;
+  c.boundary_particles = c.boundary_particles ? 1 : 0;
+  c.enabled = c.enabled ? 1 : 0;
+  bool regrid = c.smoothing_length != w->cfg.smoothing_length;
+  w->cfg = c;
+  if (regrid) {
+    w->plan_valid = false;
+    w->keys_valid = false;
+  }
+  return 1;
+}
+
+int32_t phieng_world_get_fluid_config(World2* w, FluidConfig2Ffi* out) {
+  if (!w || !out) return 0;
+  *out = w->cfg;
+  return 1;
+}
+
+uint32_t phieng_world_fluid_add(World2* w, const float* positions, uint32_t count) {
+  if (!w || !positions) return 0;
+  return add_particles(w, positions, nullptr, count);
+}
+
+uint32_t phieng_world_fluid_add_phase(World2* w, const float* positions, const uint8_t* phases, uint32_t count) {
+  if (!w || !positions || !phases) return 0;
+  return add_particles(w, positions, phases, count);
+}
+
+uint32_t phieng_world_fluid_count(const World2* w) {
+  if (!w) return 0;
+  return w->n;
+}
+
+int32_t phieng_world_fluid_clear(World2* w) {
+  if (!w) return 0;
+  if (w->device >= 0) cudaStreamSynchronize(w->stream);
+  w->n = 0;
+  w->h_state.clear();
+  w->h_mass.clear();
+  w->h_phase.clear();
+  w->h_dens.clear();
+  w->h_pres.clear();
+  recompute_uniformity(w);
+  w->host_state_valid = true;
+  w->dev_state_valid = false;
+  w->dev_aux_valid = false;
+  w->dp_on_device = false;
+  w->plan_valid = false;
+  w->keys_valid = false;
+  return 1;
+}
+
+uint32_t phieng_world_fluid_get(const World2* cw, float* out, uint32_t max) {
+  if (!cw || !out) return 0;
+  World2* w = const_cast<World2*>(cw);
+  uint32_t n = std::min(max, w->n);
+  if (n == 0) return 0;
+  if (!ensure_host_state(w)) return 0;
+  std::memcpy(out, w->h_state.data(), sizeof(float4) * n);
+  return n;
+}
+
+// ---------------------------------------------------------------- extension
+int32_t phieng_sph_status(const World2* w, PhiengSphStatus* out) {
+  if (!w || !out) return 0;
+  std::memset(out, 0, sizeof(*out));
+  out->error = w->error;
+  out->particles = w->n;
+  out->substeps = w->substeps;
+  out->grid_log2_w = w->plan_valid ? w->plan.log2w : 0;
+  out->grid_log2_h = w->plan_valid ? w->plan.log2h : 0;
+  out->sort_passes = w->plan_valid ? sort_plan(w->plan.nbuckets).passes : 0;
+  out->grid_cx0 = w->plan_valid ? w->plan.cx0 : 0;
+  out->grid_cy0 = w->plan_valid ? w->plan.cy0 : 0;
+  return 1;
+}
+
+int32_t phieng_sph_clear_error(World2* w) {
+  if (!w) return 0;
+  w->error = PHIENG_SPH_OK;
+  return 1;
+}
+
+const char* phieng_sph_error_string(const World2* w) { return error_text(w ? w->error : PHIENG_SPH_E_ARG); }
+
+int32_t phieng_sph_set_particle_cap(World2* w, uint32_t cap) {
+  if (!w || cap == 0) return 0;
+  w->cap = cap;
+  return 1;
+}
+
+int32_t phieng_sph_step_n(World2* w, float dt, uint32_t steps) {
+  if (!w) return 0;
+  if (!std::isfinite(dt) || dt <= 0.0f) return 1;
+  const float d = std::min(dt, kMaxDt);
+  for (uint32_t s = 0; s < steps; s++)
+    if (!world_step(w, d)) return 0;
+  return 1;
+}
+
+int32_t phieng_sph_set_stream(World2* w, void* stream) {
+  if (!w) return 0;
+  if (w->device >= 0) cudaStreamSynchronize(w->stream);
+  if (stream) {
+    w->stream = (cudaStream_t)stream;
+    w->user_stream = true;
+  } else {
+    w->stream = w->own_stream;
+    w->user_stream = false;
+  }
+  return 1;
+}
+
+int32_t phieng_sph_sync(World2* w) {
+  if (!w) return 0;
+  if (w->device < 0) return w->error == PHIENG_SPH_OK ? 1 : 0;
+  return cuda_ok(w, cudaStreamSynchronize(w->stream), "sync") ? 1 : 0;
+}
+
+int32_t phieng_sph_set_state(World2* w, const float* xyvv, uint32_t n) {
+  if (!w || !xyvv || n > w->n) return 0;
+  for (uint64_t i = 0; i < 4ull * n; i++)
+    if (!std::isfinite(xyvv[i])) return 0;
+  if (!ensure_host_state(w)) return 0;
+  std::memcpy(w->h_state.data(), xyvv, sizeof(float4) * n);
+  w->dev_state_valid = false;
+  w->keys_valid = false;
+  w->plan_valid = false;
+  return 1;
+}
+
+uint32_t phieng_sph_get_density_pressure(const World2* cw, float* dens, float* pres, uint32_t max) {
+  if (!cw) return 0;
+  World2* w = const_cast<World2*>(cw);
+  uint32_t n = std::min(max, w->n);
+  if (n == 0) return 0;
+  if (!ensure_host_dp(w)) return 0;
+  if (dens) std::memcpy(dens, w->h_dens.data(), sizeof(float) * n);
+  if (pres) std::memcpy(pres, w->h_pres.data(), sizeof(float) * n);
+  return n;
+}
+
+int32_t phieng_sph_replan(World2* w) {
+  if (!w) return 0;
+  if (!ensure_host_state(w)) return 0;
+  plan_grid(w);
+  return 1;
+}
+
+int32_t phieng_sph_set_profiling(World2* w, int32_t on) {
+  if (!w) return 0;
+  if (on && !w->ev[0]) {
+    if (!ensure_device(w)) return 0;
+    for (auto& e : w->ev)
+      if (!cuda_ok(w, cudaEventCreate(&e), "cudaEventCreate")) return 0;
+  }
+  if (w->device >= 0) cudaStreamSynchronize(w->stream);
+  w->profiling = on != 0;
+  release_graph(w);
+  return 1;
+}
+
+uint32_t phieng_sph_phase_times(World2* w, float* ms, uint32_t max) {
+  if (!w || !ms || !w->profiling || w->substeps == 0) return 0;
+  if (!cuda_ok(w, cudaStreamSynchronize(w->stream), "sync")) return 0;
+  uint32_t k = 0;
+  for (; k < 3 && k < max; k++)
+    if (!cuda_ok(w, cudaEventElapsedTime(&ms[k], w->ev[k], w->ev[k + 1]), "cudaEventElapsedTime")) return 0;
+  return k;
+}
+
+int32_t phieng_sph_front_metrics(World2* w, float* out) {
+  if (!w || !out) return 0;
+  out[0] = -INFINITY;
+  out[1] = 0.0f;
+  if (w->n == 0) return 1;
+  if (w->host_state_valid) {
+    for (uint32_t i = 0; i < w->n; i++) {
+      float4 s = w->h_state[i];
+      out[0] = rmaxf(out[0], s.x);
+      out[1] = rmaxf(out[1], std::sqrt(s.z * s.z + s.w * s.w));
+    }
+    return 1;
+  }
+  if (w->device < 0) return 0;
+  enqueue_front_metrics(w->d, w->n, w->stream);
+  if (!cuda_ok(w, cudaMemcpyAsync(w->h_pinned, w->d.scalar + 2, 8, cudaMemcpyDeviceToHost, w->stream), "metrics"))
+    return 0;
+  if (!cuda_ok(w, cudaStreamSynchronize(w->stream), "sync")) return 0;
+  unsigned int bx = w->h_pinned[0], bv = w->h_pinned[1];
+  unsigned int ux = (bx & 0x80000000u) ? (bx & 0x7FFFFFFFu) : ~bx;  // undo the order-preserving map
+  if (bx == 0u) {
+    out[0] = -INFINITY;
+  } else {
+    std::memcpy(&out[0], &ux, 4);
+  }
+  std::memcpy(&out[1], &bv, 4);
+  return 1;
+}
+
+uint32_t phieng_sph_debug_sorted(World2* w, uint32_t* ids, uint32_t* keys, uint32_t max) {
+  if (!w || w->n == 0) return 0;
+  if (!ensure_host_dp(w)) return 0;  // the re-sort below invalidates the sorted density
+  if (!prepare(w)) return 0;
+  const StepParams P = make_params(w, 0.0f);
+  enqueue_keys(w->d, w->n, w->plan, w->stream);
+  enqueue_sort_and_ranges(w->d, w->n, P, w->stream);
+  uint32_t n = std::min(max, w->n);
+  if (ids) cudaMemcpyAsync(ids, w->d.sid, 4ull * n, cudaMemcpyDeviceToHost, w->stream);
+  if (keys) cudaMemcpyAsync(keys, w->d.skey, 4ull * n, cudaMemcpyDeviceToHost, w->stream);
+  if (!cuda_ok(w, cudaStreamSynchronize(w->stream), "debug_sorted")) return 0;
+  return w->n;
+}
+
+uint32_t phieng_sph_debug_neighbors(World2* w, uint32_t* counts, uint32_t* lists, uint32_t max_per, uint32_t max) {
+  if (!w || !counts || !lists || w->n == 0 || max < w->n) return 0;
+  if (!ensure_host_dp(w)) return 0;
+  if (!prepare(w)) return 0;
+  const StepParams P = make_params(w, 0.0f);
+  enqueue_keys(w->d, w->n, w->plan, w->stream);
+  enqueue_sort_and_ranges(w->d, w->n, P, w->stream);
+  size_t bytes = 4ull * w->n * (1 + (size_t)max_per);
+  if (!ensure_tmp(w, bytes)) return 0;
+  uint32_t* dc = (uint32_t*)w->d_tmp;
+  uint32_t* dl = dc + w->n;
+  enqueue_debug_neighbors(w->d, w->n, P, dc, dl, max_per, w->stream);
+  cudaMemcpyAsync(counts, dc, 4ull * w->n, cudaMemcpyDeviceToHost, w->stream);
+  cudaMemcpyAsync(lists, dl, 4ull * w->n * max_per, cudaMemcpyDeviceToHost, w->stream);
+  if (!cuda_ok(w, cudaStreamSynchronize(w->stream), "debug_neighbors")) return 0;
+  return w->n;
+}
+
+uint32_t phieng_sph_debug_forces(World2* w, float* fxy, uint32_t max) {
+  if (!w || !fxy || w->n == 0 || max < w->n) return 0;
+  if (!ensure_host_dp(w)) return 0;
+  if (!prepare(w)) return 0;
+  const StepParams P = make_params(w, 0.0f);
+  enqueue_keys(w->d, w->n, w->plan, w->stream);
+  enqueue_sort_and_ranges(w->d, w->n, P, w->stream);
+  enqueue_density(w->d, w->n, P, w->stream);
+  if (!ensure_tmp(w, sizeof(float2) * (size_t)w->n)) return 0;
+  enqueue_force_integrate(w->d, w->n, P, (float2*)w->d_tmp, w->stream);
+  cudaMemcpyAsync(fxy, w->d_tmp, sizeof(float2) * w->n, cudaMemcpyDeviceToHost, w->stream);
+  if (!cuda_ok(w, cudaStreamSynchronize(w->stream), "debug_forces")) return 0;
+  w->dp_on_device = true;
+  return w->n;
+}
+
+}  // extern "C"

@@ -1,0 +1,290 @@
+"""Python mirror of the reference's World2 / FluidState2 API over the C ABI.
+
+The reference drives the fluid as
+
+    let mut world = World2::new();
+    world.add_static_body(pos, Shape2::Box { half_extents });
+    world.fluid.config = FluidConfig2 { .. };
+    world.fluid.add_particles(&pts);
+    world.step(dt);
+    for p in world.fluid.particles.iter() { .. }
+
+(crates/engine/examples/fluid_dam.rs:12-61). This module offers the same
+shape in Python — ``World2()``, ``add_static_body``, ``world.fluid.config``,
+``world.fluid.add_particles``, ``world.step`` and ``world.fluid.particles`` —
+with every call going through libphieng_sph.so; the particle state stays on
+the GPU between steps. There is no CPU fallback: constructing a world loads
+the CUDA library or raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _abi
+from ._abi import FluidConfig2Ffi, default_config
+
+
+@dataclass
+class Box:
+    """Shape2::Box { half_extents } (crates/dynamics/src/body.rs)."""
+
+    hx: float
+    hy: float
+
+
+@dataclass
+class Circle:
+    """Shape2::Circle { radius }."""
+
+    radius: float
+
+
+def _fptr(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+class SphError(RuntimeError):
+    pass
+
+
+class FluidState2:
+    """world.fluid: config, particle insertion and read-back."""
+
+    def __init__(self, world: "World2"):
+        self._world = world
+
+    @property
+    def _lib(self):
+        return self._world._lib
+
+    @property
+    def _h(self):
+        return self._world._h
+
+    # config (ffi.rs:999-1026)
+    @property
+    def config(self) -> FluidConfig2Ffi:
+        c = FluidConfig2Ffi()
+        self._lib.phieng_world_get_fluid_config(self._h, C.byref(c))
+        return c
+
+    @config.setter
+    def config(self, cfg: FluidConfig2Ffi) -> None:
+        if self._lib.phieng_world_set_fluid_config(self._h, C.byref(cfg)) != 1:
+            raise ValueError("invalid fluid config (rejected by the validation of ffi.rs:773-855)")
+
+    def set_config(self, cfg: FluidConfig2Ffi) -> bool:
+        return self._lib.phieng_world_set_fluid_config(self._h, C.byref(cfg)) == 1
+
+    def add_particles(self, positions) -> int:
+        """add_particles (fluid.rs:232-236); returns the number added."""
+        xy = np.ascontiguousarray(positions, dtype=np.float32).reshape(-1, 2)
+        total = 0
+        # the C ABI takes at most 1,000,000 per call (ffi.rs:2493)
+        for s in range(0, xy.shape[0], 1_000_000):
+            chunk = np.ascontiguousarray(xy[s:s + 1_000_000])
+            k = int(self._lib.phieng_world_fluid_add(self._h, _fptr(chunk), chunk.shape[0]))
+            total += k
+            if k < chunk.shape[0]:
+                break
+        return total
+
+    def add_particles_phase(self, positions, phases) -> int:
+        xy = np.ascontiguousarray(positions, dtype=np.float32).reshape(-1, 2)
+        ph = np.ascontiguousarray(phases, dtype=np.uint8)
+        if ph.shape[0] != xy.shape[0]:
+            raise ValueError("one phase per particle")
+        return int(self._lib.phieng_world_fluid_add_phase(
+            self._h, _fptr(xy), ph.ctypes.data_as(C.POINTER(C.c_uint8)), xy.shape[0]))
+
+    def clear(self) -> None:
+        self._lib.phieng_world_fluid_clear(self._h)
+
+    def __len__(self) -> int:
+        return int(self._lib.phieng_world_fluid_count(self._h))
+
+    @property
+    def particles(self) -> np.ndarray:
+        """(n, 4) float32 [x, y, vx, vy] in insertion order (ffi.rs:2575)."""
+        n = len(self)
+        out = np.zeros((n, 4), np.float32)
+        if n:
+            k = self._lib.phieng_world_fluid_get(self._h, _fptr(out), n)
+            if k != n:
+                self._world.check()
+        return out
+
+    def set_state(self, xyvv) -> None:
+        a = np.ascontiguousarray(xyvv, dtype=np.float32).reshape(-1, 4)
+        if self._lib.phieng_sph_set_state(self._h, _fptr(a), a.shape[0]) != 1:
+            raise ValueError("set_state rejected (non-finite input or too many particles)")
+
+    def density_pressure(self):
+        n = len(self)
+        d = np.zeros(n, np.float32)
+        p = np.zeros(n, np.float32)
+        if n:
+            self._lib.phieng_sph_get_density_pressure(self._h, _fptr(d), _fptr(p), n)
+        return d, p
+
+    def set_cap(self, cap: int) -> None:
+        """Lift MAX_PARTICLES_2D (fluid.rs:30) for this fluid."""
+        self._lib.phieng_sph_set_particle_cap(self._h, cap)
+
+
+class World2:
+    """A world of static bodies and one GPU-resident SPH fluid."""
+
+    def __init__(self):
+        self._lib = _abi.load()
+        self._h = self._lib.phieng_world_new()
+        if not self._h:
+            raise MemoryError("phieng_world_new returned null")
+        self._gravity = (0.0, -9.81)
+        self.fluid = FluidState2(self)
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.phieng_world_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # ---- world ----
+    @property
+    def gravity(self):
+        return self._gravity
+
+    @gravity.setter
+    def gravity(self, g) -> None:
+        self._lib.phieng_world_set_gravity(self._h, float(g[0]), float(g[1]))
+        self._gravity = (float(g[0]), float(g[1]))
+
+    @property
+    def time(self) -> float:
+        t = C.c_float()
+        self._lib.phieng_world_get_time(self._h, C.byref(t))
+        return float(t.value)
+
+    def add_static_body(self, position, shape) -> int:
+        """World2::add_static_body (world.rs:384-392) through phieng_world_add_body."""
+        px, py = float(position[0]), float(position[1])
+        if isinstance(shape, Box):
+            r = self._lib.phieng_world_add_body(self._h, px, py, _abi.SHAPE_BOX, shape.hx, shape.hy, 1.0, 1, 0.4, 0.1)
+        elif isinstance(shape, Circle):
+            r = self._lib.phieng_world_add_body(self._h, px, py, _abi.SHAPE_CIRCLE, shape.radius, 0.0, 1.0, 1, 0.4, 0.1)
+        else:
+            raise TypeError("shape must be Box or Circle")
+        if r < 0:
+            raise ValueError("invalid static body")
+        return int(r)
+
+    def body_count(self) -> int:
+        return int(self._lib.phieng_world_body_count(self._h))
+
+    def step(self, dt: float) -> None:
+        self._lib.phieng_world_step(self._h, dt)
+        self.check()
+
+    def step_n(self, dt: float, n: int) -> None:
+        if self._lib.phieng_sph_step_n(self._h, dt, n) != 1:
+            self.check()
+
+    def set_stream(self, stream_ptr: int | None) -> None:
+        self._lib.phieng_sph_set_stream(self._h, C.c_void_p(stream_ptr) if stream_ptr else None)
+
+    def sync(self) -> None:
+        if self._lib.phieng_sph_sync(self._h) != 1:
+            self.check()
+
+    def status(self) -> _abi.PhiengSphStatus:
+        s = _abi.PhiengSphStatus()
+        self._lib.phieng_sph_status(self._h, C.byref(s))
+        return s
+
+    def check(self) -> None:
+        s = self.status()
+        if s.error != _abi.OK:
+            msg = self._lib.phieng_sph_error_string(self._h).decode()
+            raise SphError(f"phieng_sph error {s.error}: {msg}")
+
+    def front_metrics(self):
+        """(max x, peak speed) over the fluid, reduced on the GPU."""
+        out = np.zeros(2, np.float32)
+        if self._lib.phieng_sph_front_metrics(self._h, _fptr(out)) != 1:
+            self.check()
+        return float(out[0]), float(out[1])
+
+    def set_profiling(self, on: bool) -> None:
+        if self._lib.phieng_sph_set_profiling(self._h, 1 if on else 0) != 1:
+            self.check()
+
+    def phase_times(self):
+        """ms of (sort + ranges, density, force + integrate) of the last substep."""
+        out = np.zeros(3, np.float32)
+        k = self._lib.phieng_sph_phase_times(self._h, _fptr(out), 3)
+        return out[:k].astype(np.float64)
+
+    # ---- diagnostics ----
+    def debug_sorted(self):
+        n = len(self.fluid)
+        ids = np.zeros(n, np.uint32)
+        keys = np.zeros(n, np.uint32)
+        U = C.POINTER(C.c_uint32)
+        self._lib.phieng_sph_debug_sorted(self._h, ids.ctypes.data_as(U), keys.ctypes.data_as(U), n)
+        self.check()
+        return ids, keys
+
+    def debug_neighbors(self, max_per: int = 64):
+        n = len(self.fluid)
+        counts = np.zeros(n, np.uint32)
+        lists = np.zeros(n * max_per, np.uint32)
+        U = C.POINTER(C.c_uint32)
+        self._lib.phieng_sph_debug_neighbors(self._h, counts.ctypes.data_as(U), lists.ctypes.data_as(U), max_per, n)
+        self.check()
+        return counts, lists.reshape(n, max_per)
+
+    def debug_forces(self) -> np.ndarray:
+        n = len(self.fluid)
+        out = np.zeros((n, 2), np.float32)
+        self._lib.phieng_sph_debug_forces(self._h, _fptr(out), n)
+        self.check()
+        return out
+
+    def replan(self) -> None:
+        self._lib.phieng_sph_replan(self._h)
+
+
+def world_from_scene(scene, cap: int | None = None) -> World2:
+    """Build a World2 from a phi_eng_b200.scenes.Scene."""
+    w = World2()
+    w.gravity = scene.gravity
+    for (px, py, hx, hy) in scene.boxes:
+        w.add_static_body((px, py), Box(hx, hy))
+    for (px, py, r) in scene.circles:
+        w.add_static_body((px, py), Circle(r))
+    w.fluid.config = scene.config
+    w.fluid.set_cap(cap if cap is not None else max(4096, scene.n))
+    if scene.phases is not None:
+        added = w.fluid.add_particles_phase(scene.xy, scene.phases)
+    else:
+        added = w.fluid.add_particles(scene.xy)
+    if added != scene.n:
+        raise RuntimeError(f"added {added} of {scene.n} particles")
+    return w
+
+
+__all__ = ["World2", "FluidState2", "Box", "Circle", "SphError", "world_from_scene", "default_config"]
