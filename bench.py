@@ -127,7 +127,7 @@ def cpu_baseline(sc, budget_s: float = 15.0, max_steps: int = 20):
     """The reference algorithm on one host core (oracle, in-place order)."""
     from oracle import oracle as orc
 
-    o = orc.OracleWorld(cap=sc.n)
+    o = orc.OracleWorld(cap=sc.n, libm_pow=True)
     o.set_gravity(*sc.gravity)
     for (px, py, hx, hy) in sc.boxes:
         o.add_box(px, py, hx, hy, (1.0, 0.0, -0.0, 1.0))
@@ -150,7 +150,7 @@ def run_reference(args, rank: int):
     sc = make_scene(args.workload)
     from oracle import oracle as orc
 
-    o = orc.OracleWorld(cap=sc.n)
+    o = orc.OracleWorld(cap=sc.n, libm_pow=True)
     o.set_gravity(*sc.gravity)
     for (px, py, hx, hy) in sc.boxes:
         o.add_box(px, py, hx, hy, (1.0, 0.0, -0.0, 1.0))

@@ -44,6 +44,7 @@ def _load():
         "orc_get_config": (None, [P, C.POINTER(FluidConfig2Ffi)]),
         "orc_set_gravity": (None, [P, C.c_float, C.c_float]),
         "orc_set_cap": (None, [P, C.c_uint32]),
+        "orc_set_pow_mode": (None, [P, C.c_int]),
         "orc_add_body": (None, [P, C.c_int, C.c_float, C.c_float, C.c_float, C.c_float,
                                 C.c_float, C.c_float, C.c_float, C.c_float]),
         "orc_add_particles": (C.c_uint32, [P, F, U8, C.c_uint32]),
@@ -95,11 +96,14 @@ class OracleWorld:
     fp64: run the same algorithm in double precision.
     """
 
-    def __init__(self, fp64: bool = False, cap: int = 4096):
+    def __init__(self, fp64: bool = False, cap: int = 4096, libm_pow: bool = False):
+        """libm_pow: evaluate the Tait power with the platform powf (as the
+        reference's f32::powf does) instead of the correctly rounded power."""
         self._l = _load()
         self._h = self._l.orc_new(1 if fp64 else 0)
         self.fp64 = fp64
         self._l.orc_set_cap(self._h, cap)
+        self._l.orc_set_pow_mode(self._h, 0 if libm_pow else 1)
 
     def __del__(self):
         try:

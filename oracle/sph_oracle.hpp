@@ -123,14 +123,35 @@ inline R rclamp(R x, R lo, R hi) {
   return x;
 }
 
+// x^g for the Tait EOS (fluid.rs:295: `(density / rho0).powf(gamma)`).
+// pow_mode 1 (default): the correctly rounded f32 power, evaluated in double
+//   (binary exponentiation for an integer g in [1, 64], else double pow) and
+//   rounded once; this is the GPU's arithmetic.
+// pow_mode 0: the platform libm powf, which Rust's f32::powf calls; glibc's
+//   powf is off by one ulp from the correctly rounded result on ~0.07% of
+//   inputs in [0.5, 3) for g = 7.
+inline float powf_cr(float x, float g) {
+  if (g >= 1.0f && g <= 64.0f && g == std::floor(g)) {
+    unsigned e = (unsigned)g;
+    double b = (double)x, r = 1.0;
+    while (e) {
+      if (e & 1u) r = r * b;
+      e >>= 1;
+      if (e) b = b * b;
+    }
+    return (float)r;
+  }
+  return (float)pow((double)x, (double)g);
+}
+
 template <class R>
-inline R rpow(R a, R b);
+inline R rpow(R a, R b, int mode);
 template <>
-inline float rpow<float>(float a, float b) {
-  return powf(a, b);
+inline float rpow<float>(float a, float b, int mode) {
+  return mode == 0 ? powf(a, b) : powf_cr(a, b);
 }
 template <>
-inline double rpow<double>(double a, double b) {
+inline double rpow<double>(double a, double b, int) {
   return pow(a, b);
 }
 
@@ -143,6 +164,7 @@ class Fluid {
   R gx = (R)0.0f, gy = (R)-9.81f;  // World2::new gravity (world.rs:338)
   R time = 0;
   size_t cap = 4096;  // MAX_PARTICLES_2D (fluid.rs:30); lifted by the caller
+  int pow_mode = 1;   // see powf_cr
 
   // last-substep scratch exposed for per-pass parity dumps
   std::vector<R> fx, fy;
@@ -167,12 +189,12 @@ class Fluid {
     gyo = ry / r * s;
   }
   // equation of state (fluid.rs:290-297)
-  static R pressure(R density, R rest_density, R stiffness, R gamma) {
+  static R pressure(R density, R rest_density, R stiffness, R gamma, int pow_mode = 1) {
     if (gamma == (R)1.0) {
       return rmax(stiffness * (density - rest_density), (R)0);
     }
     R rho0 = rmax(rest_density, (R)kEps);
-    return rmax(stiffness * rho0 * (rpow(density / rho0, gamma) - (R)1.0), (R)0);
+    return rmax(stiffness * rho0 * (rpow(density / rho0, gamma, pow_mode) - (R)1.0), (R)0);
   }
   // Monaghan artificial viscosity (fluid.rs:302-317)
   static R artificial_pressure(R dx, R dy, R vrx, R vry, R r_sq, R h, R rho_bar, R c, R alpha) {
@@ -272,7 +294,7 @@ class Fluid {
     }
     for (auto& p : particles) {
       R rho0 = (R)cfg.phase_rest_density[std::min<int>(p.phase, 3)];
-      p.pressure = pressure(p.density, rho0, (R)cfg.stiffness, (R)cfg.gamma);
+      p.pressure = pressure(p.density, rho0, (R)cfg.stiffness, (R)cfg.gamma, pow_mode);
     }
   }
 

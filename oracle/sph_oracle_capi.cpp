@@ -121,6 +121,13 @@ void orc_set_gravity(void* h, float gx, float gy) {
   o->f64.gy = (double)gy;
 }
 
+// 1 = correctly rounded power (the GPU's), 0 = the platform libm powf
+void orc_set_pow_mode(void* h, int mode) {
+  Orc* o = static_cast<Orc*>(h);
+  o->f32.pow_mode = mode;
+  o->f64.pow_mode = mode;
+}
+
 void orc_set_cap(void* h, uint32_t cap) {
   Orc* o = static_cast<Orc*>(h);
   o->f32.cap = cap;
@@ -361,7 +368,7 @@ float orc_poly6(float r2, float h) { return Fluid<float>::poly6(r2, h); }
 void orc_spiky(float rx, float ry, float r, float h, float* out2) {
   Fluid<float>::spiky_grad(rx, ry, r, h, out2[0], out2[1]);
 }
-float orc_pressure(float d, float rho0, float k, float g) { return Fluid<float>::pressure(d, rho0, k, g); }
+float orc_pressure(float d, float rho0, float k, float g) { return Fluid<float>::pressure(d, rho0, k, g, 0); }
 float orc_artificial_pressure(float dx, float dy, float vrx, float vry, float r_sq, float h, float rho_bar,
                               float c, float alpha) {
   return Fluid<float>::artificial_pressure(dx, dy, vrx, vry, r_sq, h, rho_bar, c, alpha);

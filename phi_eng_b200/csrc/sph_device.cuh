@@ -102,17 +102,33 @@ __device__ __forceinline__ float poly6(float r2, const StepParams& P) {
   return __fmul_rn(__fmul_rn(__fmul_rn(P.c_poly6, t), t), t);
 }
 
-// equation of state (fluid.rs:290-297). powf is evaluated as a double pow
-// rounded once to f32, which is the correctly rounded x^gamma except in
-// double-rounding corner cases; glibc's powf is correctly rounded in
-// practice, so the two agree bit for bit almost always.
+// x^g rounded once to f32: for an integer g in [1, 64] by binary
+// exponentiation in double (each product correctly rounded, so the result
+// is the same on any IEEE machine), else via double pow. This is the
+// correctly rounded f32 power except when x^g lies within a few double ulps
+// of an f32 rounding boundary.
+__device__ __forceinline__ float powf_cr(float x, float g) {
+  if (g >= 1.0f && g <= 64.0f && g == floorf(g)) {
+    unsigned e = (unsigned)g;
+    double b = (double)x, r = 1.0;
+    while (e) {
+      if (e & 1u) r = __dmul_rn(r, b);
+      e >>= 1;
+      if (e) b = __dmul_rn(b, b);
+    }
+    return __double2float_rn(r);
+  }
+  return __double2float_rn(pow((double)x, (double)g));
+}
+
+// equation of state (fluid.rs:290-297)
 __device__ __forceinline__ float eos(float density, float rho0, const StepParams& P) {
   if (!(P.flags & F_TAIT)) {
     return fmaxf(__fmul_rn(P.stiffness, __fsub_rn(density, rho0)), 0.0f);
   }
   float r0 = fmaxf(rho0, kEps);
   float ratio = __fdiv_rn(density, r0);
-  float pw = (float)pow((double)ratio, (double)P.gamma);
+  float pw = powf_cr(ratio, P.gamma);
   return fmaxf(__fmul_rn(__fmul_rn(P.stiffness, r0), __fsub_rn(pw, 1.0f)), 0.0f);
 }
 

@@ -62,41 +62,6 @@ __global__ void __launch_bounds__(kSortThreads) k_radix_hist(const uint32_t* __r
   for (uint32_t d = threadIdx.x; d <= mask; d += blockDim.x) hist[d * ntiles + blockIdx.x] = cnt[d];
 }
 
-// Exclusive scan of hist[0..len) in place (digit-major, so the result is
-// each (digit, tile)'s global output offset). One block of 1024 threads.
-__global__ void __launch_bounds__(1024) k_radix_scan(uint32_t* __restrict__ hist, uint32_t len) {
-  __shared__ uint32_t warp_tot[32];
-  const uint32_t tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-  const uint32_t per = (len + 1023) / 1024;
-  const uint32_t b = min(len, tid * per), e = min(len, b + per);
-  uint32_t sum = 0;
-  for (uint32_t i = b; i < e; i++) sum += hist[i];
-  uint32_t x = sum;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
-    if (lane >= (uint32_t)o) x += y;
-  }
-  if (lane == 31) warp_tot[w] = x;
-  __syncthreads();
-  if (w == 0) {
-    uint32_t t = warp_tot[lane];
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      uint32_t y = __shfl_up_sync(0xFFFFFFFFu, t, o);
-      if (lane >= (uint32_t)o) t += y;
-    }
-    warp_tot[lane] = t;
-  }
-  __syncthreads();
-  uint32_t run = x - sum + (w ? warp_tot[w - 1] : 0u);
-  for (uint32_t i = b; i < e; i++) {
-    uint32_t v = hist[i];
-    hist[i] = run;
-    run += v;
-  }
-}
-
 struct GatherArgs {
   const float4* state;
   const float* mass;
@@ -123,6 +88,41 @@ __device__ __forceinline__ uint32_t block_incl_scan_256(uint32_t v, uint32_t* wa
   return x + add;
 }
 
+// Exclusive scan of each digit's row of tile counts, hist[d * ntiles + t],
+// in place (one block per digit; rows are contiguous, so loads coalesce);
+// the row total goes to tot[d]. Output offsets are then
+// sum_{d' < d} tot[d'] + hist[d * ntiles + t], the first term formed by the
+// scatter kernel itself.
+__global__ void __launch_bounds__(256) k_radix_scan_rows(uint32_t* __restrict__ hist, uint32_t ntiles,
+                                                         uint32_t* __restrict__ tot) {
+  __shared__ uint32_t warp_tot[8];
+  __shared__ uint32_t chunk_tot;
+  uint32_t* row = hist + (size_t)blockIdx.x * ntiles;
+  uint32_t carry = 0;
+  for (uint32_t base = 0; base < ntiles; base += 4 * 256) {
+    uint32_t v[4], s = 0;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      uint32_t idx = base + threadIdx.x * 4 + k;
+      v[k] = idx < ntiles ? row[idx] : 0u;
+      s += v[k];
+    }
+    __syncthreads();  // warp_tot / chunk_tot reuse across chunks
+    uint32_t incl = block_incl_scan_256(s, warp_tot);
+    uint32_t run = carry + incl - s;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      uint32_t idx = base + threadIdx.x * 4 + k;
+      if (idx < ntiles) row[idx] = run;
+      run += v[k];
+    }
+    if (threadIdx.x == 255) chunk_tot = incl;
+    __syncthreads();
+    carry += chunk_tot;
+  }
+  if (threadIdx.x == 0) tot[blockIdx.x] = carry;
+}
+
 // Stable scatter of one digit pass. Each warp ranks its 256 keys in 8 rounds
 // of 32 (item order = round-major, lane-minor = index order) with
 // __match_any_sync, per-warp digit counters give the warp-local rank, a
@@ -136,11 +136,13 @@ __global__ void __launch_bounds__(kSortThreads) k_radix_scatter(const uint32_t* 
                                                                 uint32_t* __restrict__ kout,
                                                                 uint32_t* __restrict__ vout, uint32_t n,
                                                                 uint32_t shift, uint32_t mask, uint32_t ntiles,
-                                                                const uint32_t* __restrict__ hist, GatherArgs ga) {
+                                                                const uint32_t* __restrict__ hist,
+                                                                const uint32_t* __restrict__ dtot, GatherArgs ga) {
   __shared__ uint32_t wcnt[8][256];
   __shared__ uint32_t dstart[256];
   __shared__ uint32_t gofs[256];
   __shared__ uint32_t warp_tot[8];
+  __shared__ uint32_t warp_tot2[8];
   __shared__ uint32_t skeys[kSortTile];
   __shared__ uint32_t svals[kSortTile];
   const uint32_t tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
@@ -175,9 +177,11 @@ __global__ void __launch_bounds__(kSortThreads) k_radix_scatter(const uint32_t* 
     }
   }
   uint32_t incl = block_incl_scan_256(tot, warp_tot);
+  const uint32_t dt = tid < nd ? dtot[tid] : 0u;
+  const uint32_t dincl = block_incl_scan_256(dt, warp_tot2);
   if (tid < nd) {
     dstart[tid] = incl - tot;
-    gofs[tid] = hist[tid * ntiles + blockIdx.x];
+    gofs[tid] = (dincl - dt) + hist[tid * ntiles + blockIdx.x];
   }
   __syncthreads();
 #pragma unroll
@@ -505,7 +509,6 @@ void enqueue_sort_and_ranges(const FluidBufs& b, uint32_t n, const StepParams& P
   const SortPlan sp = sort_plan(P.grid.nbuckets);
   const uint32_t ntiles = cdiv(n, kSortTile);
   const uint32_t mask = (1u << sp.bits) - 1u;
-  const uint32_t len = (mask + 1) * ntiles;
   GatherArgs ga;
   ga.state = b.state;
   ga.mass = b.mass;
@@ -523,19 +526,19 @@ void enqueue_sort_and_ranges(const FluidBufs& b, uint32_t n, const StepParams& P
     uint32_t* kout = last ? b.skey : ((pass & 1) ? b.kb : b.ka);
     uint32_t* vout = last ? b.sid : ((pass & 1) ? b.vb : b.va);
     k_radix_hist<<<ntiles, kSortThreads, 0, st>>>(kin, n, shift, mask, ntiles, b.hist);
-    k_radix_scan<<<1, 1024, 0, st>>>(b.hist, len);
+    k_radix_scan_rows<<<mask + 1, 256, 0, st>>>(b.hist, ntiles, b.dtot);
     if (first && last)
       k_radix_scatter<true, true><<<ntiles, kSortThreads, 0, st>>>(kin, vin, kout, vout, n, shift, mask, ntiles,
-                                                                   b.hist, ga);
+                                                                   b.hist, b.dtot, ga);
     else if (first)
       k_radix_scatter<true, false><<<ntiles, kSortThreads, 0, st>>>(kin, vin, kout, vout, n, shift, mask, ntiles,
-                                                                    b.hist, ga);
+                                                                    b.hist, b.dtot, ga);
     else if (last)
       k_radix_scatter<false, true><<<ntiles, kSortThreads, 0, st>>>(kin, vin, kout, vout, n, shift, mask, ntiles,
-                                                                    b.hist, ga);
+                                                                    b.hist, b.dtot, ga);
     else
       k_radix_scatter<false, false><<<ntiles, kSortThreads, 0, st>>>(kin, vin, kout, vout, n, shift, mask, ntiles,
-                                                                     b.hist, ga);
+                                                                     b.hist, b.dtot, ga);
     kin = kout;
     vin = vout;
   }

@@ -33,6 +33,7 @@ struct FluidBufs {
   float2* sdq = nullptr;     // sorted (density, pressure / max(density,EPS)^2)
   float* spres = nullptr;    // sorted pressure
   uint32_t* hist = nullptr;  // radix tile histograms, [digit][tile]
+  uint32_t* dtot = nullptr;  // radix digit totals (256)
   uint32_t hist_len = 0;
   int2* range = nullptr;     // per bucket [start, end) in sorted order
   uint32_t range_cap = 0;    // buckets allocated

@@ -216,6 +216,7 @@ void free_particle_buffers(FluidBufs& d) {
   dfree(d.sdq);
   dfree(d.spres);
   dfree(d.hist);
+  dfree(d.dtot);
   d.cap = 0;
   d.hist_len = 0;
 }
@@ -263,7 +264,7 @@ bool ensure_capacity(World2* w, uint32_t need) {
             dalloc(w, d.skey, c) && dalloc(w, d.sid, c) && dalloc(w, d.spos, c) && dalloc(w, d.svel, c) &&
             dalloc(w, d.smass, c) && dalloc(w, d.sphase, c) && dalloc(w, d.sdq, c) && dalloc(w, d.spres, c);
   uint32_t ntiles = (c + kSortTile - 1) / kSortTile;
-  ok = ok && dalloc(w, d.hist, (size_t)256 * ntiles);
+  ok = ok && dalloc(w, d.hist, (size_t)256 * ntiles) && dalloc(w, d.dtot, 256);
   if (!ok) {
     free_particle_buffers(d);
     return false;

@@ -21,8 +21,8 @@ FFI_ROT = (1.0, 0.0, -0.0, 1.0)
 
 
 class OracleSim:
-    def __init__(self, mode=orc.REF_SEQ, fp64=False, cap=1 << 22):
-        self.w = orc.OracleWorld(fp64=fp64, cap=cap)
+    def __init__(self, mode=orc.REF_SEQ, fp64=False, cap=1 << 22, libm_pow=False):
+        self.w = orc.OracleWorld(fp64=fp64, cap=cap, libm_pow=libm_pow)
         self.mode = mode
 
     def add_box(self, px, py, hx, hy):
