@@ -41,18 +41,21 @@ METRIC = "particle-updates/s"
 HBM_FALLBACK = 6650.0
 
 # Algorithmic bytes per particle of each phase (every array read or written
-# once; neighbour re-reads not counted). P = radix passes, B/N = buckets per
-# particle, c = occupied cells per particle.
-#   sort+ranges: hist 4P + scatter (12 + 16(P-1)) + gather 32 + memset 8B/N + ranges 4 + 8c
-#   density:     read pos 8 + key 4, write (density, q) 8 + pressure 4     = 24
-#   force:       read pos 8, vel 8, (density, q) 8, key 4, id 4;
-#                write state 16 + next key 4                           = 52
+# once; neighbour re-reads not counted). B/N = buckets per particle.
+#   sort:    scan: read counts twice, write start + cursor, clear counts
+#            (20 B per bucket); place: read id 4 + key 4, write (key, id) 8;
+#            fixup: read (key, id) 8 + start 8, write (key, id) 8,
+#            gather state 16 -> write pos 8 + vel 8                = 72 + 20 B/N
+#   density: read pos 8 + key 4, write (density, q) 8 + pressure 4   = 24
+#   force:   read pos 8, vel 8, (density, q) 8, key 4, id 4;
+#            write state 16 + next key 4                             = 52
 DENSITY_BYTES = 24
 FORCE_BYTES = 52
+KERNELS_PER_STEP = 6  # scan reduce, scan down, place, fixup, density, force
 
 
-def sort_bytes(passes: int, buckets_per_particle: float, c: float = 0.25) -> float:
-    return 4 * passes + 12 + 16 * (passes - 1) + 32 + 8 * buckets_per_particle + 4 + 8 * c
+def sort_bytes(buckets_per_particle: float) -> float:
+    return 72 + 20 * buckets_per_particle
 
 
 def hbm_peak():
@@ -200,7 +203,6 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     w.set_profiling(True)
     w.step(sc.dt)  # capture the profiled graph outside the timed region
     st = w.status()
-    passes = st.sort_passes
     buckets = (1 << st.grid_log2_w) * (1 << st.grid_log2_h)
     torch.cuda.synchronize()
     if dist:
@@ -232,7 +234,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     ph = np.array(phases)
     ph_mean = ph.mean(axis=0)
     names = ["sort_ranges", "density", "force_integrate"]
-    bytes_pp = [sort_bytes(passes, buckets / sc.n), DENSITY_BYTES, FORCE_BYTES]
+    bytes_pp = [sort_bytes(buckets / sc.n), DENSITY_BYTES, FORCE_BYTES]
     top = int(np.argmax(ph_mean))
     peak, peak_kind = hbm_peak()
     achieved = bytes_pp[top] * sc.n / (ph_mean[top] / 1000.0) / 1e9
@@ -270,15 +272,14 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         base = cpu_baseline(sc)
 
     if rank == 0:
-        kernels_per_step = 3 * passes + 3
+        kernels_per_step = KERNELS_PER_STEP
         line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
                 "config": {"workload": workload_desc(sc), "particles": sc.n, "parallelism":
                            ("replicas" if world > 1 else "single"),
                            "l2": "flushed between timed steps (256 MiB write, outside the timed events)",
-                           "grid": f"{1 << st.grid_log2_w}x{1 << st.grid_log2_h} buckets",
-                           "sort_passes": passes},
+                           "grid": f"{1 << st.grid_log2_w}x{1 << st.grid_log2_h} buckets"},
                 "roofline": roofline, "whole_step": whole,
                 "phases_ms": {n: float(v) for n, v in zip(names, ph_mean)},
                 "cpu_baseline": base, "e2e": e2e, "gpu_launches": kernels_per_step * args.steps,

@@ -153,7 +153,7 @@ typedef struct PhiengSphStatus {
   uint64_t substeps;      /* fluid substeps run since creation */
   uint32_t grid_log2_w;   /* bucket grid: columns = 1 << grid_log2_w */
   uint32_t grid_log2_h;   /* rows = 1 << grid_log2_h */
-  uint32_t sort_passes;   /* radix digit passes per substep */
+  uint32_t sort_passes;   /* passes of the bucket sort per substep (1) */
   int32_t grid_cx0;       /* bucket grid origin cell: bucket = ((cy - grid_cy0) mod H) * W */
   int32_t grid_cy0;       /*   + ((cx - grid_cx0) mod W), cx = floor(x / h) as i32 */
   uint32_t reserved;

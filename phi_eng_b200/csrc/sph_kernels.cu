@@ -1,10 +1,10 @@
 // SPH fluid step kernels for sm_100a (B200).
 //
 // Chain per substep (the reference's substep, crates/dynamics/src/fluid.rs:898-1136):
-//   K1 keys     bucket key per particle                (rebuild_grid, :330-363)
-//   K2 sort     stable LSD radix sort of (key, id)     (cell lists with ascending ids)
-//   K4 gather   fused into the last sort pass: state -> sorted order
-//   K3 ranges   [start, end) per bucket
+//   K1 keys     bucket key + bucket count per particle (rebuild_grid, :330-363)
+//   K2 sort     counting sort by bucket, in-bucket rank by id = the cell lists
+//               with ascending ids; the scanned counts are the K3 bucket
+//               ranges, and the last kernel is the K4 gather into sorted order
 //   K5 density  poly6 sum + clamp + EOS                (compute_density_pressure, :592-611)
 //   K6 force    spiky pressure force (+AV, cohesion) + XSPH + cap + advect
 //               + wall push-out, Jacobi reads           (:942-1094)
@@ -32,45 +32,23 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
 
 // ---------------------------------------------------------------- K1 keys
 __global__ void __launch_bounds__(256) k_keys(const float4* __restrict__ state, uint32_t n, GridPlan g,
-                                              uint32_t* __restrict__ keys) {
-  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  float4 s = state[i];
-  keys[i] = bucket_key(s.x, s.y, g);
-}
+                                              uint32_t* __restrict__ keys, uint32_t* __restrict__ count);
 
-// ---------------------------------------------------------------- K2 radix sort
-// Tile histogram of one digit: hist[d * ntiles + tile]. Warp-aggregated
-// shared-memory counting (keys are spatially coherent, so digits repeat).
-__global__ void __launch_bounds__(kSortThreads) k_radix_hist(const uint32_t* __restrict__ keys, uint32_t n,
-                                                             uint32_t shift, uint32_t mask, uint32_t ntiles,
-                                                             uint32_t* __restrict__ hist) {
-  __shared__ uint32_t cnt[256];
-  for (uint32_t d = threadIdx.x; d < 256; d += blockDim.x) cnt[d] = 0;
-  __syncthreads();
-  const uint32_t lane = threadIdx.x & 31;
-  const uint32_t base = blockIdx.x * kSortTile;
-#pragma unroll
-  for (uint32_t r = 0; r < kSortItems; r++) {
-    uint32_t idx = base + r * kSortThreads + threadIdx.x;
-    bool valid = idx < n;
-    uint32_t d = valid ? ((keys[idx] >> shift) & mask) : 0xFFFFFFFFu;
-    uint32_t peers = __match_any_sync(0xFFFFFFFFu, d);
-    if (valid && (peers & lanemask_lt()) == 0) atomicAdd(&cnt[d], (uint32_t)__popc(peers));
-  }
-  __syncthreads();
-  for (uint32_t d = threadIdx.x; d <= mask; d += blockDim.x) hist[d * ntiles + blockIdx.x] = cnt[d];
-}
-
-struct GatherArgs {
-  const float4* state;
-  const float* mass;
-  const uint8_t* phase;
-  float2* spos;
-  float2* svel;
-  float* smass;
-  uint8_t* sphase;
-};
+// ---------------------------------------------------------------- K2 bucket sort
+// Counting sort over the whole bucket key (a one-digit radix sort with radix
+// = number of buckets), then an in-bucket rank by id, so the final order is
+// exactly (key, id):
+//   count   K1 / K6 add each particle to count[key] (warp-aggregated)
+//   scan    count -> start (exclusive; start doubles as the bucket range
+//           table: bucket b holds slots [start[b], start[b+1])), and count
+//           becomes the placement cursor
+//   place   each particle takes a slot in its bucket from the cursor
+//           (arrival order inside a bucket is arbitrary)
+//   fixup   each particle's final slot = start[b] + (number of ids in its
+//           bucket smaller than its own); gathers the state into that slot
+// Buckets hold a handful of particles (a cell is h wide, the support radius),
+// so the in-bucket rank is a short loop.
+constexpr uint32_t kScanTile = kBucketScanTile;  // counts per scan block: 256 threads x 16
 
 // Block-wide inclusive scan of one value per thread (256 threads).
 __device__ __forceinline__ uint32_t block_incl_scan_256(uint32_t v, uint32_t* warp_tot) {
@@ -88,167 +66,192 @@ __device__ __forceinline__ uint32_t block_incl_scan_256(uint32_t v, uint32_t* wa
   return x + add;
 }
 
-// Exclusive scan of each digit's row of tile counts, hist[d * ntiles + t],
-// in place (one block per digit; rows are contiguous, so loads coalesce);
-// the row total goes to tot[d]. Output offsets are then
-// sum_{d' < d} tot[d'] + hist[d * ntiles + t], the first term formed by the
-// scatter kernel itself.
-__global__ void __launch_bounds__(256) k_radix_scan_rows(uint32_t* __restrict__ hist, uint32_t ntiles,
-                                                         uint32_t* __restrict__ tot) {
-  __shared__ uint32_t warp_tot[8];
-  __shared__ uint32_t chunk_tot;
-  uint32_t* row = hist + (size_t)blockIdx.x * ntiles;
-  uint32_t carry = 0;
-  for (uint32_t base = 0; base < ntiles; base += 4 * 256) {
-    uint32_t v[4], s = 0;
-#pragma unroll
-    for (int k = 0; k < 4; k++) {
-      uint32_t idx = base + threadIdx.x * 4 + k;
-      v[k] = idx < ntiles ? row[idx] : 0u;
-      s += v[k];
-    }
-    __syncthreads();  // warp_tot / chunk_tot reuse across chunks
-    uint32_t incl = block_incl_scan_256(s, warp_tot);
-    uint32_t run = carry + incl - s;
-#pragma unroll
-    for (int k = 0; k < 4; k++) {
-      uint32_t idx = base + threadIdx.x * 4 + k;
-      if (idx < ntiles) row[idx] = run;
-      run += v[k];
-    }
-    if (threadIdx.x == 255) chunk_tot = incl;
-    __syncthreads();
-    carry += chunk_tot;
-  }
-  if (threadIdx.x == 0) tot[blockIdx.x] = carry;
+// Add a warp's keys to count[] with one atomic per distinct key.
+__device__ __forceinline__ void count_key(uint32_t* __restrict__ count, uint32_t k) {
+  const uint32_t peers = __match_any_sync(__activemask(), k);
+  if ((peers & lanemask_lt()) == 0) atomicAdd(&count[k], (uint32_t)__popc(peers));
 }
 
-// Stable scatter of one digit pass. Each warp ranks its 256 keys in 8 rounds
-// of 32 (item order = round-major, lane-minor = index order) with
-// __match_any_sync, per-warp digit counters give the warp-local rank, a
-// block scan over (digit, warp) gives the tile-local position; keys are
-// staged in shared memory in tile-sorted order and written out so that each
-// digit's run is contiguous. FIRST: values are the indices (ids). GATHER:
-// last pass, also gathers the particle state into sorted order.
-template <bool FIRST, bool GATHER>
-__global__ void __launch_bounds__(kSortThreads) k_radix_scatter(const uint32_t* __restrict__ kin,
-                                                                const uint32_t* __restrict__ vin,
-                                                                uint32_t* __restrict__ kout,
-                                                                uint32_t* __restrict__ vout, uint32_t n,
-                                                                uint32_t shift, uint32_t mask, uint32_t ntiles,
-                                                                const uint32_t* __restrict__ hist,
-                                                                const uint32_t* __restrict__ dtot, GatherArgs ga) {
-  __shared__ uint32_t wcnt[8][256];
-  __shared__ uint32_t dstart[256];
-  __shared__ uint32_t gofs[256];
+// K1: key and bucket count of every particle (id order).
+__global__ void __launch_bounds__(256) k_keys(const float4* __restrict__ state, uint32_t n, GridPlan g,
+                                              uint32_t* __restrict__ keys, uint32_t* __restrict__ count) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float4 s = state[i];
+  const uint32_t k = bucket_key(s.x, s.y, g);
+  keys[i] = k;
+  count_key(count, k);
+}
+
+// Sum each scan tile; the last block to finish turns the tile sums into
+// exclusive tile offsets in place (no block waits on another).
+__global__ void __launch_bounds__(256) k_scan_reduce(const uint32_t* __restrict__ count,
+                                                     uint32_t* __restrict__ tilesum, uint32_t ntiles,
+                                                     uint32_t* __restrict__ done) {
   __shared__ uint32_t warp_tot[8];
-  __shared__ uint32_t warp_tot2[8];
-  __shared__ uint32_t skeys[kSortTile];
-  __shared__ uint32_t svals[kSortTile];
+  __shared__ bool last;
   const uint32_t tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-  const uint32_t nd = mask + 1;
-  for (uint32_t i = tid; i < 8 * 256; i += kSortThreads) (&wcnt[0][0])[i] = 0;
-  __syncthreads();
-  const uint32_t tbase = blockIdx.x * kSortTile;
-  const uint32_t lt = lanemask_lt();
-  uint32_t key[kSortItems], val[kSortItems], rank[kSortItems];
+  const uint4* c4 = reinterpret_cast<const uint4*>(count + (size_t)blockIdx.x * kScanTile);
+  uint32_t sum = 0;
 #pragma unroll
-  for (uint32_t r = 0; r < kSortItems; r++) {
-    uint32_t idx = tbase + w * (32 * kSortItems) + r * 32 + lane;
-    bool valid = idx < n;
-    key[r] = valid ? kin[idx] : 0xFFFFFFFFu;
-    val[r] = FIRST ? idx : (valid ? vin[idx] : 0u);
-    uint32_t d = valid ? ((key[r] >> shift) & mask) : 0xFFFFFFFFu;
-    uint32_t peers = __match_any_sync(0xFFFFFFFFu, d);
-    uint32_t before = valid ? wcnt[w][d] : 0u;
-    __syncwarp();
-    if (valid && (peers & lt) == 0) wcnt[w][d] = before + (uint32_t)__popc(peers);
-    __syncwarp();
-    rank[r] = before + (uint32_t)__popc(peers & lt);
+  for (int r = 0; r < 4; r++) {
+    const uint4 v = c4[r * 256 + tid];
+    sum += v.x + v.y + v.z + v.w;
   }
-  __syncthreads();
-  uint32_t tot = 0;
-  if (tid < nd) {
 #pragma unroll
-    for (int ww = 0; ww < 8; ww++) {
-      uint32_t c = wcnt[ww][tid];
-      wcnt[ww][tid] = tot;
-      tot += c;
-    }
-  }
-  uint32_t incl = block_incl_scan_256(tot, warp_tot);
-  const uint32_t dt = tid < nd ? dtot[tid] : 0u;
-  const uint32_t dincl = block_incl_scan_256(dt, warp_tot2);
-  if (tid < nd) {
-    dstart[tid] = incl - tot;
-    gofs[tid] = (dincl - dt) + hist[tid * ntiles + blockIdx.x];
+  for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xFFFFFFFFu, sum, o);
+  if (lane == 0) warp_tot[w] = sum;
+  __syncthreads();
+  if (tid == 0) {
+    uint32_t t = 0;
+    for (int k = 0; k < 8; k++) t += warp_tot[k];
+    tilesum[blockIdx.x] = t;
+    __threadfence();
+    last = atomicAdd(done, 1u) + 1u == gridDim.x;
   }
   __syncthreads();
+  if (!last) return;
+  __threadfence();
+  uint32_t carry = 0;
+  for (uint32_t base = 0; base < ntiles; base += 256) {
+    const uint32_t i = base + tid;
+    const uint32_t v = i < ntiles ? *((volatile uint32_t*)&tilesum[i]) : 0u;
+    __syncthreads();  // warp_tot reuse
+    uint32_t x = v;
 #pragma unroll
-  for (uint32_t r = 0; r < kSortItems; r++) {
-    uint32_t idx = tbase + w * (32 * kSortItems) + r * 32 + lane;
-    if (idx < n) {
-      uint32_t d = (key[r] >> shift) & mask;
-      uint32_t pos = dstart[d] + wcnt[w][d] + rank[r];
-      skeys[pos] = key[r];
-      svals[pos] = val[r];
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+      if (lane >= (uint32_t)o) x += y;
     }
+    if (lane == 31) warp_tot[w] = x;
+    __syncthreads();
+    uint32_t add = carry;
+    for (uint32_t k = 0; k < w; k++) add += warp_tot[k];
+    if (i < ntiles) tilesum[i] = add + x - v;
+    uint32_t chunk = 0;
+    for (int k = 0; k < 8; k++) chunk += warp_tot[k];
+    carry += chunk;
   }
-  __syncthreads();
-  const uint32_t cnt = min(kSortTile, n - tbase);
-  for (uint32_t p = tid; p < cnt; p += kSortThreads) {
-    uint32_t k = skeys[p];
-    uint32_t d = (k >> shift) & mask;
-    uint32_t g = gofs[d] + (p - dstart[d]);
-    uint32_t v = svals[p];
-    kout[g] = k;
-    vout[g] = v;
-    if (GATHER) {
-      float4 s = ga.state[v];
-      ga.spos[g] = make_float2(s.x, s.y);
-      ga.svel[g] = make_float2(s.z, s.w);
-      if (ga.smass) ga.smass[g] = ga.mass[v];
-      if (ga.sphase) ga.sphase[g] = ga.phase[v];
-    }
-  }
+  if (tid == 0) *done = 0;
 }
 
-// ---------------------------------------------------------------- K3 ranges
-__global__ void __launch_bounds__(256) k_cell_ranges(const uint32_t* __restrict__ skey, uint32_t n, uint32_t nb,
-                                                     int2* __restrict__ range) {
-  uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+// start[i] = exclusive prefix of count[i]; count[i] is overwritten with the
+// same value (the placement cursor). Entries i <= m are written (m = number
+// of keys incl. the sentinel bucket; start[m] = particle count).
+__global__ void __launch_bounds__(256) k_scan_down(uint32_t* __restrict__ count,
+                                                   const uint32_t* __restrict__ tileoff, uint32_t m,
+                                                   uint32_t* __restrict__ start) {
+  __shared__ uint32_t warp_tot[8];
+  const uint32_t tid = threadIdx.x;
+  const uint32_t base = blockIdx.x * kScanTile + tid * 16;
+  uint4* c4 = reinterpret_cast<uint4*>(count + base);
+  uint32_t v[16];
+#pragma unroll
+  for (int r = 0; r < 4; r++) {
+    const uint4 q = c4[r];
+    v[4 * r] = q.x;
+    v[4 * r + 1] = q.y;
+    v[4 * r + 2] = q.z;
+    v[4 * r + 3] = q.w;
+  }
+  uint32_t sum = 0;
+#pragma unroll
+  for (int q = 0; q < 16; q++) sum += v[q];
+  const uint32_t incl = block_incl_scan_256(sum, warp_tot);
+  uint32_t run = tileoff[blockIdx.x] + incl - sum;
+#pragma unroll
+  for (int q = 0; q < 16; q++) {
+    const uint32_t x = v[q];
+    v[q] = run;
+    run += x;
+  }
+#pragma unroll
+  for (int r = 0; r < 4; r++) c4[r] = make_uint4(v[4 * r], v[4 * r + 1], v[4 * r + 2], v[4 * r + 3]);
+#pragma unroll
+  for (int q = 0; q < 16; q++)
+    if (base + q <= m) start[base + q] = v[q];
+}
+
+// Slot in the bucket from the cursor. BY_SLOT walks the previous sort's
+// order (keys nearly sorted: a warp shares few keys, so few atomics);
+// otherwise particles are taken in id order.
+template <bool BY_SLOT>
+__global__ void __launch_bounds__(256) k_place(const uint32_t* __restrict__ key,
+                                               const uint32_t* __restrict__ sid_prev, uint32_t n,
+                                               uint32_t* __restrict__ cursor, uint32_t* __restrict__ tkey,
+                                               uint32_t* __restrict__ tid_out) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n) return;
-  uint32_t k = skey[s];
-  if (k >= nb) return;
-  if (s == 0 || skey[s - 1] != k) range[k].x = (int)s;
-  if (s + 1 == n || skey[s + 1] != k) range[k].y = (int)(s + 1);
+  const uint32_t id = BY_SLOT ? sid_prev[s] : s;
+  const uint32_t k = key[id];
+  const uint32_t peers = __match_any_sync(__activemask(), k);
+  const uint32_t lt = lanemask_lt();
+  const uint32_t leader = __ffs(peers) - 1;
+  uint32_t base = 0;
+  if ((peers & lt) == 0) base = atomicAdd(&cursor[k], (uint32_t)__popc(peers));
+  base = __shfl_sync(peers, base, leader);
+  const uint32_t slot = base + (uint32_t)__popc(peers & lt);
+  tkey[slot] = k;
+  tid_out[slot] = id;
+}
+
+struct GatherArgs {
+  const float4* state;
+  const float* mass;
+  const uint8_t* phase;
+  float2* spos;
+  float2* svel;
+  float* smass;
+  uint8_t* sphase;
+};
+
+// Final slot = bucket start + rank of the id among the bucket's ids; the
+// particle's state is gathered into that slot.
+__global__ void __launch_bounds__(256) k_fixup(const uint32_t* __restrict__ tkey,
+                                               const uint32_t* __restrict__ tid_in,
+                                               const uint32_t* __restrict__ start, uint32_t n,
+                                               uint32_t* __restrict__ skey, uint32_t* __restrict__ sid,
+                                               GatherArgs ga) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  const uint32_t k = tkey[s];
+  const uint32_t id = tid_in[s];
+  const uint32_t lo = start[k], hi = start[k + 1];
+  uint32_t rank = 0;
+  for (uint32_t j = lo; j < hi; j++) rank += __ldg(&tid_in[j]) < id ? 1u : 0u;
+  const uint32_t f = lo + rank;
+  skey[f] = k;
+  sid[f] = id;
+  const float4 st = ga.state[id];
+  ga.spos[f] = make_float2(st.x, st.y);
+  ga.svel[f] = make_float2(st.z, st.w);
+  if (ga.smass) ga.smass[f] = ga.mass[id];
+  if (ga.sphase) ga.sphase[f] = ga.phase[id];
 }
 
 // ---------------------------------------------------------------- neighbour walk
 // Visit every candidate slot j of the particle in bucket `key`, in the
-// reference's order. Away from the wrap seam the three buckets of a row are
-// consecutive keys, hence one contiguous slot range.
+// reference's order (cell rows oy = -1..1, then cells ox = -1..1, then
+// ascending id). Bucket b holds slots [start[b], start[b + 1]); away from
+// the wrap seam the three buckets of a row are consecutive keys, hence one
+// contiguous slot range.
 template <class F>
-__device__ __forceinline__ void for_each_candidate(uint32_t key, const int2* __restrict__ range,
+__device__ __forceinline__ void for_each_candidate(uint32_t key, const uint32_t* __restrict__ start,
                                                    const GridPlan& g, F&& f) {
   const uint32_t bx = key & g.maskw, by = key >> g.log2w;
 #pragma unroll 1
   for (int oy = -1; oy <= 1; oy++) {
     const uint32_t row = ((by + (uint32_t)oy) & g.maskh) << g.log2w;
     if (bx >= 1u && bx < g.maskw) {
-      int2 r0 = __ldg(&range[row + bx - 1]);
-      int2 r1 = __ldg(&range[row + bx]);
-      int2 r2 = __ldg(&range[row + bx + 1]);
-      int s = 0x7FFFFFFF, e = 0;
-      if (r0.x < r0.y) { s = r0.x; e = r0.y; }
-      if (r1.x < r1.y) { s = min(s, r1.x); e = r1.y; }
-      if (r2.x < r2.y) { s = min(s, r2.x); e = r2.y; }
-      for (int j = s; j < e; j++) f(j);
+      const uint32_t b0 = row + bx - 1;
+      const uint32_t e = __ldg(&start[b0 + 3]);
+      for (uint32_t j = __ldg(&start[b0]); j < e; j++) f((int)j);
     } else {
 #pragma unroll 1
       for (int ox = -1; ox <= 1; ox++) {
-        int2 r = __ldg(&range[row + ((bx + (uint32_t)ox) & g.maskw)]);
-        for (int j = r.x; j < r.y; j++) f(j);
+        const uint32_t b = row + ((bx + (uint32_t)ox) & g.maskw);
+        const uint32_t e = __ldg(&start[b + 1]);
+        for (uint32_t j = __ldg(&start[b]); j < e; j++) f((int)j);
       }
     }
   }
@@ -259,7 +262,7 @@ template <bool MASS, bool PHASE>
 __global__ void __launch_bounds__(256) k_density(const float2* __restrict__ spos, const uint32_t* __restrict__ skey,
                                                  const float* __restrict__ smass,
                                                  const uint8_t* __restrict__ sphase, uint32_t n,
-                                                 const int2* __restrict__ range, StepParams P,
+                                                 const uint32_t* __restrict__ range, StepParams P,
                                                  float2* __restrict__ sdq, float* __restrict__ spres) {
   uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n) return;
@@ -290,13 +293,81 @@ __global__ void __launch_bounds__(256) k_density(const float2* __restrict__ spos
 }
 
 // ---------------------------------------------------------------- K6 force + integrate
+// Per-thread neighbour list (slots in sorted order) kept in shared memory,
+// column-major so that lane t uses bank t. Particles with more neighbours
+// than fit are finished by a second candidate walk that skips the listed ones.
+constexpr uint32_t kNbrCap = 32;
+
+// One neighbour pair of the force loop (fluid.rs:947-990) and of the XSPH
+// sum (fluid.rs:1022-1033), accumulated in the reference's order.
+template <bool MASS>
+__device__ __forceinline__ void pair_terms(int j, float2 pi, float2 vi, float rho_i, float q_i, float m_i,
+                                           const float2* __restrict__ spos, const float2* __restrict__ svel,
+                                           const float2* __restrict__ sdq, const float* __restrict__ smass,
+                                           const StepParams& P, float& fx, float& fy, float& sx, float& sy) {
+  const float2 pj = __ldg(&spos[j]);
+  const float2 dqj = __ldg(&sdq[j]);
+  const float2 vj = __ldg(&svel[j]);
+  const float m_j = MASS ? __ldg(&smass[j]) : P.mass;
+  const float rho_j = fmaxf(dqj.x, kEps);
+  // delta = p_i - p_j; |delta|^2 equals the neighbour test's d2 bit for bit
+  const float dx = __fsub_rn(pi.x, pj.x);
+  const float dy = __fsub_rn(pi.y, pj.y);
+  const float d2 = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
+  const float dist = __fsqrt_rn(d2);
+  // spiky gradient (fluid.rs:278-285)
+  float gxx = 0.0f, gyy = 0.0f;
+  if (!(dist >= P.hk || dist < kEps)) {
+    const float hr = __fsub_rn(P.hk, dist);
+    const float sc = __fmul_rn(__fmul_rn(P.c_spiky, hr), hr);
+    gxx = __fmul_rn(__fdiv_rn(dx, dist), sc);
+    gyy = __fmul_rn(__fdiv_rn(dy, dist), sc);
+  }
+  float term = __fadd_rn(q_i, dqj.y);
+  if ((P.flags & F_AV) && dist > kEps) {
+    // Monaghan term (fluid.rs:302-317, called at :963-975)
+    const float rho_bar = __fmul_rn(0.5f, __fadd_rn(rho_i, rho_j));
+    const float vrx = __fsub_rn(vi.x, vj.x), vry = __fsub_rn(vi.y, vj.y);
+    const float vd = __fadd_rn(__fmul_rn(vrx, dx), __fmul_rn(vry, dy));
+    if (!(vd >= 0.0f)) {
+      const float r_sq = __fmul_rn(dist, dist);
+      const float mu =
+          __fdiv_rn(__fmul_rn(P.hk, vd), __fadd_rn(r_sq, __fmul_rn(__fmul_rn(0.01f, P.hk), P.hk)));
+      const float ap = __fdiv_rn(__fmul_rn(__fmul_rn(-P.av_alpha, P.c_s), mu), fmaxf(rho_bar, kEps));
+      term = __fadd_rn(term, ap);
+    }
+  }
+  const float mt = __fmul_rn(m_j, term);
+  fx = __fsub_rn(fx, __fmul_rn(gxx, mt));
+  fy = __fsub_rn(fy, __fmul_rn(gyy, mt));
+  if ((P.flags & F_COHESION) && dist > kEps) {
+    // cohesion (fluid.rs:320-326, applied at :979-985)
+    const float c = dist >= P.hk ? 0.0f : __fsub_rn(1.0f, __fdiv_rn(dist, P.hk));
+    if (c > 0.0f) {
+      const float sc = __fmul_rn(__fmul_rn(__fmul_rn(P.surface_tension, m_i), m_j), c);
+      fx = __fsub_rn(fx, __fmul_rn(__fdiv_rn(dx, dist), sc));
+      fy = __fsub_rn(fy, __fmul_rn(__fdiv_rn(dy, dist), sc));
+    }
+  }
+  if (P.flags & F_VISC) {
+    // XSPH (fluid.rs:1022-1033) against pre-integrate neighbours
+    const float rho_bar = __fmul_rn(0.5f, __fadd_rn(rho_i, rho_j));
+    const float w = poly6(d2, P);
+    const float mr = __fdiv_rn(m_j, rho_bar);
+    sx = __fadd_rn(sx, __fmul_rn(__fmul_rn(__fsub_rn(vj.x, vi.x), mr), w));
+    sy = __fadd_rn(sy, __fmul_rn(__fmul_rn(__fsub_rn(vj.y, vi.y), mr), w));
+  }
+}
+
 template <bool MASS, bool DEBUG>
-__global__ void __launch_bounds__(256) k_force_integrate(
+__global__ void __launch_bounds__(256, 4) k_force_integrate(
     const float2* __restrict__ spos, const float2* __restrict__ svel, const float2* __restrict__ sdq,
     const uint32_t* __restrict__ skey, const uint32_t* __restrict__ sid, const float* __restrict__ smass,
-    uint32_t n, const int2* __restrict__ range, StepParams P, const DevBody* __restrict__ bodies,
-    float4* __restrict__ state_out, uint32_t* __restrict__ key_out, float2* __restrict__ dbg_force) {
-  uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t n, const uint32_t* __restrict__ range, StepParams P, const DevBody* __restrict__ bodies,
+    float4* __restrict__ state_out, uint32_t* __restrict__ key_out, uint32_t* __restrict__ count_out,
+    float2* __restrict__ dbg_force) {
+  __shared__ uint32_t nbr[kNbrCap][256];
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n) return;
   const uint32_t k = skey[s];
   const uint32_t id = sid[s];
@@ -306,68 +377,37 @@ __global__ void __launch_bounds__(256) k_force_integrate(
   const float m_i = MASS ? smass[s] : P.mass;
   const float rho_i = fmaxf(dqi.x, kEps);
   const float q_i = dqi.y;  // p_i / (rho_i * rho_i)
-  const bool visc = (P.flags & F_VISC) != 0;
-  const bool av = (P.flags & F_AV) != 0;
-  const bool coh = (P.flags & F_COHESION) != 0;
   float fx = 0.0f, fy = 0.0f, sx = 0.0f, sy = 0.0f;
   if (k < P.grid.nbuckets) {
+    // pass 1: neighbours j != i (fluid.rs:368-386, :953-955) in visit order
+    uint32_t c = 0;
     for_each_candidate(k, range, P.grid, [&](int j) {
-      float2 pj = __ldg(&spos[j]);
-      float ex = __fsub_rn(pj.x, pi.x);
-      float ey = __fsub_rn(pj.y, pi.y);
-      float d2 = __fadd_rn(__fmul_rn(ex, ex), __fmul_rn(ey, ey));
-      if (!(d2 < P.hg2) || (uint32_t)j == s) return;
-      const float2 dqj = __ldg(&sdq[j]);
-      const float2 vj = __ldg(&svel[j]);
-      const float m_j = MASS ? __ldg(&smass[j]) : P.mass;
-      const float rho_j = fmaxf(dqj.x, kEps);
-      // delta = p_i - p_j; |delta|^2 equals d2 bit for bit (negation is exact)
-      const float dx = __fsub_rn(pi.x, pj.x);
-      const float dy = __fsub_rn(pi.y, pj.y);
-      const float dist = __fsqrt_rn(d2);
-      // spiky gradient (fluid.rs:278-285)
-      float gxx = 0.0f, gyy = 0.0f;
-      if (!(dist >= P.hk || dist < kEps)) {
-        float hr = __fsub_rn(P.hk, dist);
-        float sc = __fmul_rn(__fmul_rn(P.c_spiky, hr), hr);
-        gxx = __fmul_rn(__fdiv_rn(dx, dist), sc);
-        gyy = __fmul_rn(__fdiv_rn(dy, dist), sc);
-      }
-      float term = __fadd_rn(q_i, dqj.y);
-      if (av && dist > kEps) {
-        // Monaghan term (fluid.rs:302-317, called at :963-975)
-        float rho_bar = __fmul_rn(0.5f, __fadd_rn(rho_i, rho_j));
-        float vrx = __fsub_rn(vi.x, vj.x), vry = __fsub_rn(vi.y, vj.y);
-        float vd = __fadd_rn(__fmul_rn(vrx, dx), __fmul_rn(vry, dy));
-        if (!(vd >= 0.0f)) {
-          float r_sq = __fmul_rn(dist, dist);
-          float mu = __fdiv_rn(__fmul_rn(P.hk, vd),
-                               __fadd_rn(r_sq, __fmul_rn(__fmul_rn(0.01f, P.hk), P.hk)));
-          float ap = __fdiv_rn(__fmul_rn(__fmul_rn(-P.av_alpha, P.c_s), mu), fmaxf(rho_bar, kEps));
-          term = __fadd_rn(term, ap);
-        }
-      }
-      const float mt = __fmul_rn(m_j, term);
-      fx = __fsub_rn(fx, __fmul_rn(gxx, mt));
-      fy = __fsub_rn(fy, __fmul_rn(gyy, mt));
-      if (coh && dist > kEps) {
-        // cohesion (fluid.rs:320-326, applied at :979-985)
-        float c = dist >= P.hk ? 0.0f : __fsub_rn(1.0f, __fdiv_rn(dist, P.hk));
-        if (c > 0.0f) {
-          float sc = __fmul_rn(__fmul_rn(__fmul_rn(P.surface_tension, m_i), m_j), c);
-          fx = __fsub_rn(fx, __fmul_rn(__fdiv_rn(dx, dist), sc));
-          fy = __fsub_rn(fy, __fmul_rn(__fdiv_rn(dy, dist), sc));
-        }
-      }
-      if (visc) {
-        // XSPH (fluid.rs:1022-1033) against pre-integrate neighbours
-        float rho_bar = __fmul_rn(0.5f, __fadd_rn(rho_i, rho_j));
-        float w = poly6(d2, P);
-        float mr = __fdiv_rn(m_j, rho_bar);
-        sx = __fadd_rn(sx, __fmul_rn(__fmul_rn(__fsub_rn(vj.x, vi.x), mr), w));
-        sy = __fadd_rn(sy, __fmul_rn(__fmul_rn(__fsub_rn(vj.y, vi.y), mr), w));
+      const float2 pj = __ldg(&spos[j]);
+      const float ex = __fsub_rn(pj.x, pi.x);
+      const float ey = __fsub_rn(pj.y, pi.y);
+      const float d2 = __fadd_rn(__fmul_rn(ex, ex), __fmul_rn(ey, ey));
+      if (d2 < P.hg2 && (uint32_t)j != s) {
+        if (c < kNbrCap) nbr[c][threadIdx.x] = (uint32_t)j;
+        c++;
       }
     });
+    // pass 2: the pair terms, lanes busy together
+    const uint32_t cl = min(c, kNbrCap);
+    for (uint32_t t = 0; t < cl; t++)
+      pair_terms<MASS>((int)nbr[t][threadIdx.x], pi, vi, rho_i, q_i, m_i, spos, svel, sdq, smass, P, fx, fy, sx, sy);
+    if (c > kNbrCap) {
+      uint32_t seen = 0;
+      for_each_candidate(k, range, P.grid, [&](int j) {
+        const float2 pj = __ldg(&spos[j]);
+        const float ex = __fsub_rn(pj.x, pi.x);
+        const float ey = __fsub_rn(pj.y, pi.y);
+        const float d2 = __fadd_rn(__fmul_rn(ex, ex), __fmul_rn(ey, ey));
+        if (d2 < P.hg2 && (uint32_t)j != s) {
+          if (seen >= kNbrCap) pair_terms<MASS>(j, pi, vi, rho_i, q_i, m_i, spos, svel, sdq, smass, P, fx, fy, sx, sy);
+          seen++;
+        }
+      });
+    }
   }
   if (DEBUG) {
     dbg_force[id] = make_float2(fx, fy);
@@ -378,13 +418,13 @@ __global__ void __launch_bounds__(256) k_force_integrate(
   const float ay = __fadd_rn(P.gy, __fdiv_rn(fy, rho_i));
   float vx = __fadd_rn(vi.x, __fmul_rn(ax, P.dt));
   float vy = __fadd_rn(vi.y, __fmul_rn(ay, P.dt));
-  if (visc) {
+  if (P.flags & F_VISC) {
     vx = __fadd_rn(vx, __fmul_rn(sx, P.visc));
     vy = __fadd_rn(vy, __fmul_rn(sy, P.visc));
   }
   const float speed = __fsqrt_rn(__fadd_rn(__fmul_rn(vx, vx), __fmul_rn(vy, vy)));
   if (speed > P.vmax) {
-    float sc = __fdiv_rn(P.vmax, speed);
+    const float sc = __fdiv_rn(P.vmax, speed);
     vx = __fmul_rn(vx, sc);
     vy = __fmul_rn(vy, sc);
   }
@@ -400,7 +440,9 @@ __global__ void __launch_bounds__(256) k_force_integrate(
   }
   walls(x, y, vx, vy, bodies, P);
   state_out[id] = make_float4(x, y, vx, vy);
-  key_out[id] = bucket_key(x, y, P.grid);
+  const uint32_t nk = bucket_key(x, y, P.grid);
+  key_out[id] = nk;
+  count_key(count_out, nk);  // bucket counts of the next substep's sort
 }
 
 // ---------------------------------------------------------------- helpers
@@ -417,7 +459,7 @@ __global__ void __launch_bounds__(256) k_unsort_dp(const float2* __restrict__ sd
 __global__ void __launch_bounds__(256) k_debug_neighbors(const float2* __restrict__ spos,
                                                          const uint32_t* __restrict__ skey,
                                                          const uint32_t* __restrict__ sid, uint32_t n,
-                                                         const int2* __restrict__ range, StepParams P,
+                                                         const uint32_t* __restrict__ range, StepParams P,
                                                          uint32_t* __restrict__ counts, uint32_t* __restrict__ lists,
                                                          uint32_t max_per) {
   uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
@@ -489,26 +531,22 @@ inline uint32_t cdiv(uint32_t a, uint32_t b) { return (a + b - 1) / b; }
 
 }  // namespace
 
-SortPlan sort_plan(uint32_t nbuckets) {
-  // keys are 0..nbuckets (nbuckets = sentinel), nbuckets a power of two
-  uint32_t bits = 1;
-  while ((1ull << bits) <= (uint64_t)nbuckets) bits++;
-  SortPlan p;
-  p.passes = (bits + 7) / 8;
-  p.bits = (bits + p.passes - 1) / p.passes;
-  return p;
-}
-
 void enqueue_keys(const FluidBufs& b, uint32_t n, const GridPlan& g, cudaStream_t st) {
+  cudaMemsetAsync(b.count, 0, sizeof(uint32_t) * b.count_len, st);
   if (n == 0) return;
-  k_keys<<<cdiv(n, 256), 256, 0, st>>>(b.state, n, g, b.key);
+  k_keys<<<cdiv(n, 256), 256, 0, st>>>(b.state, n, g, b.key, b.count);
 }
 
-void enqueue_sort_and_ranges(const FluidBufs& b, uint32_t n, const StepParams& P, cudaStream_t st) {
+void enqueue_sort_and_ranges(const FluidBufs& b, uint32_t n, const StepParams& P, bool by_slot, cudaStream_t st) {
   if (n == 0) return;
-  const SortPlan sp = sort_plan(P.grid.nbuckets);
-  const uint32_t ntiles = cdiv(n, kSortTile);
-  const uint32_t mask = (1u << sp.bits) - 1u;
+  const uint32_t m = P.grid.nbuckets + 1;  // buckets and the non-finite sentinel
+  const uint32_t nt = cdiv(m, kScanTile);
+  k_scan_reduce<<<nt, 256, 0, st>>>(b.count, b.tilesum, nt, b.done);
+  k_scan_down<<<nt, 256, 0, st>>>(b.count, b.tilesum, m, b.start);
+  if (by_slot)
+    k_place<true><<<cdiv(n, 256), 256, 0, st>>>(b.key, b.sid, n, b.count, b.tkey, b.tid);
+  else
+    k_place<false><<<cdiv(n, 256), 256, 0, st>>>(b.key, b.sid, n, b.count, b.tkey, b.tid);
   GatherArgs ga;
   ga.state = b.state;
   ga.mass = b.mass;
@@ -517,33 +555,9 @@ void enqueue_sort_and_ranges(const FluidBufs& b, uint32_t n, const StepParams& P
   ga.svel = b.svel;
   ga.smass = (P.flags & F_MASS) ? b.smass : nullptr;
   ga.sphase = (P.flags & F_PHASE) ? b.sphase : nullptr;
-  const uint32_t* kin = b.key;
-  const uint32_t* vin = nullptr;
-  for (uint32_t pass = 0; pass < sp.passes; pass++) {
-    const uint32_t shift = pass * sp.bits;
-    const bool first = pass == 0;
-    const bool last = pass + 1 == sp.passes;
-    uint32_t* kout = last ? b.skey : ((pass & 1) ? b.kb : b.ka);
-    uint32_t* vout = last ? b.sid : ((pass & 1) ? b.vb : b.va);
-    k_radix_hist<<<ntiles, kSortThreads, 0, st>>>(kin, n, shift, mask, ntiles, b.hist);
-    k_radix_scan_rows<<<mask + 1, 256, 0, st>>>(b.hist, ntiles, b.dtot);
-    if (first && last)
-      k_radix_scatter<true, true><<<ntiles, kSortThreads, 0, st>>>(kin, vin, kout, vout, n, shift, mask, ntiles,
-                                                                   b.hist, b.dtot, ga);
-    else if (first)
-      k_radix_scatter<true, false><<<ntiles, kSortThreads, 0, st>>>(kin, vin, kout, vout, n, shift, mask, ntiles,
-                                                                    b.hist, b.dtot, ga);
-    else if (last)
-      k_radix_scatter<false, true><<<ntiles, kSortThreads, 0, st>>>(kin, vin, kout, vout, n, shift, mask, ntiles,
-                                                                    b.hist, b.dtot, ga);
-    else
-      k_radix_scatter<false, false><<<ntiles, kSortThreads, 0, st>>>(kin, vin, kout, vout, n, shift, mask, ntiles,
-                                                                     b.hist, b.dtot, ga);
-    kin = kout;
-    vin = vout;
-  }
-  cudaMemsetAsync(b.range, 0, sizeof(int2) * (size_t)P.grid.nbuckets, st);
-  k_cell_ranges<<<cdiv(n, 256), 256, 0, st>>>(b.skey, n, P.grid.nbuckets, b.range);
+  k_fixup<<<cdiv(n, 256), 256, 0, st>>>(b.tkey, b.tid, b.start, n, b.skey, b.sid, ga);
+  // the counts of the next sort accumulate from zero (K6)
+  cudaMemsetAsync(b.count, 0, sizeof(uint32_t) * b.count_len, st);
 }
 
 void enqueue_density(const FluidBufs& b, uint32_t n, const StepParams& P, cudaStream_t st) {
@@ -551,13 +565,13 @@ void enqueue_density(const FluidBufs& b, uint32_t n, const StepParams& P, cudaSt
   const bool m = (P.flags & F_MASS) != 0, ph = (P.flags & F_PHASE) != 0;
   const uint32_t g = cdiv(n, 256);
   if (m && ph)
-    k_density<true, true><<<g, 256, 0, st>>>(b.spos, b.skey, b.smass, b.sphase, n, b.range, P, b.sdq, b.spres);
+    k_density<true, true><<<g, 256, 0, st>>>(b.spos, b.skey, b.smass, b.sphase, n, b.start, P, b.sdq, b.spres);
   else if (m)
-    k_density<true, false><<<g, 256, 0, st>>>(b.spos, b.skey, b.smass, b.sphase, n, b.range, P, b.sdq, b.spres);
+    k_density<true, false><<<g, 256, 0, st>>>(b.spos, b.skey, b.smass, b.sphase, n, b.start, P, b.sdq, b.spres);
   else if (ph)
-    k_density<false, true><<<g, 256, 0, st>>>(b.spos, b.skey, b.smass, b.sphase, n, b.range, P, b.sdq, b.spres);
+    k_density<false, true><<<g, 256, 0, st>>>(b.spos, b.skey, b.smass, b.sphase, n, b.start, P, b.sdq, b.spres);
   else
-    k_density<false, false><<<g, 256, 0, st>>>(b.spos, b.skey, b.smass, b.sphase, n, b.range, P, b.sdq, b.spres);
+    k_density<false, false><<<g, 256, 0, st>>>(b.spos, b.skey, b.smass, b.sphase, n, b.start, P, b.sdq, b.spres);
 }
 
 void enqueue_force_integrate(const FluidBufs& b, uint32_t n, const StepParams& P, float2* dbg_force,
@@ -567,18 +581,18 @@ void enqueue_force_integrate(const FluidBufs& b, uint32_t n, const StepParams& P
   const uint32_t g = cdiv(n, 256);
   if (dbg_force) {
     if (m)
-      k_force_integrate<true, true><<<g, 256, 0, st>>>(b.spos, b.svel, b.sdq, b.skey, b.sid, b.smass, n, b.range, P,
-                                                       b.bodies, b.state, b.key, dbg_force);
+      k_force_integrate<true, true><<<g, 256, 0, st>>>(b.spos, b.svel, b.sdq, b.skey, b.sid, b.smass, n, b.start, P,
+                                                       b.bodies, b.state, b.key, b.count, dbg_force);
     else
-      k_force_integrate<false, true><<<g, 256, 0, st>>>(b.spos, b.svel, b.sdq, b.skey, b.sid, b.smass, n, b.range,
-                                                        P, b.bodies, b.state, b.key, dbg_force);
+      k_force_integrate<false, true><<<g, 256, 0, st>>>(b.spos, b.svel, b.sdq, b.skey, b.sid, b.smass, n, b.start,
+                                                        P, b.bodies, b.state, b.key, b.count, dbg_force);
   } else {
     if (m)
-      k_force_integrate<true, false><<<g, 256, 0, st>>>(b.spos, b.svel, b.sdq, b.skey, b.sid, b.smass, n, b.range,
-                                                        P, b.bodies, b.state, b.key, nullptr);
+      k_force_integrate<true, false><<<g, 256, 0, st>>>(b.spos, b.svel, b.sdq, b.skey, b.sid, b.smass, n, b.start,
+                                                        P, b.bodies, b.state, b.key, b.count, nullptr);
     else
       k_force_integrate<false, false><<<g, 256, 0, st>>>(b.spos, b.svel, b.sdq, b.skey, b.sid, b.smass, n,
-                                                         b.range, P, b.bodies, b.state, b.key, nullptr);
+                                                         b.start, P, b.bodies, b.state, b.key, b.count, nullptr);
   }
 }
 
@@ -590,7 +604,7 @@ void enqueue_unsort_dp(const FluidBufs& b, uint32_t n, float* dens, float* pres,
 void enqueue_debug_neighbors(const FluidBufs& b, uint32_t n, const StepParams& P, uint32_t* counts,
                              uint32_t* lists, uint32_t max_per, cudaStream_t st) {
   if (n == 0) return;
-  k_debug_neighbors<<<cdiv(n, 256), 256, 0, st>>>(b.spos, b.skey, b.sid, n, b.range, P, counts, lists, max_per);
+  k_debug_neighbors<<<cdiv(n, 256), 256, 0, st>>>(b.spos, b.skey, b.sid, n, b.start, P, counts, lists, max_per);
 }
 
 void enqueue_front_metrics(const FluidBufs& b, uint32_t n, cudaStream_t st) {

@@ -8,9 +8,6 @@
 
 namespace phieng {
 
-constexpr uint32_t kSortThreads = 256;
-constexpr uint32_t kSortItems = 8;
-constexpr uint32_t kSortTile = kSortThreads * kSortItems;  // keys per sort tile
 
 // Device arrays of one fluid. "id order" = insertion order (the reference's
 // particle index); "sorted order" = (bucket key, id) order of the last sort.
@@ -20,10 +17,8 @@ struct FluidBufs {
   float* mass = nullptr;     // id order (used when F_MASS)
   uint8_t* phase = nullptr;  // id order (used when F_PHASE)
   uint32_t* key = nullptr;   // id order: bucket key for the next sort
-  uint32_t* ka = nullptr;    // radix ping-pong
-  uint32_t* va = nullptr;
-  uint32_t* kb = nullptr;
-  uint32_t* vb = nullptr;
+  uint32_t* tkey = nullptr;  // placed (key, id) before the in-bucket rank
+  uint32_t* tid = nullptr;
   uint32_t* skey = nullptr;  // sorted keys
   uint32_t* sid = nullptr;   // sorted slot -> particle id
   float2* spos = nullptr;    // sorted (x, y)
@@ -32,29 +27,31 @@ struct FluidBufs {
   uint8_t* sphase = nullptr; // sorted phase (F_PHASE)
   float2* sdq = nullptr;     // sorted (density, pressure / max(density,EPS)^2)
   float* spres = nullptr;    // sorted pressure
-  uint32_t* hist = nullptr;  // radix tile histograms, [digit][tile]
-  uint32_t* dtot = nullptr;  // radix digit totals (256)
-  uint32_t hist_len = 0;
-  int2* range = nullptr;     // per bucket [start, end) in sorted order
-  uint32_t range_cap = 0;    // buckets allocated
+  // per bucket grid (sized by the number of buckets B)
+  uint32_t* count = nullptr;    // particles per bucket, then the placement cursor
+  uint32_t count_len = 0;       // B + 1 rounded up to the scan tile
+  uint32_t* start = nullptr;    // bucket b holds sorted slots [start[b], start[b+1])
+  uint32_t* tilesum = nullptr;  // scan tile sums / offsets
+  uint32_t range_cap = 0;       // buckets the arrays above can hold
+  uint32_t* done = nullptr;     // scan blocks finished (zero between scans)
   DevBody* bodies = nullptr;
   uint32_t bodies_cap = 0;
   unsigned int* scalar = nullptr;  // small device scratch (vmax etc.)
 };
 
-struct SortPlan {
-  uint32_t passes;   // digit passes
-  uint32_t bits;     // digit width
-};
+// Scan tile of the bucket counts; count arrays are padded to a multiple.
+constexpr uint32_t kBucketScanTile = 4096;
 
-SortPlan sort_plan(uint32_t nbuckets);
-
-// K1: bucket key of every particle from its position (id order).
+// K1: bucket key of every particle from its position (id order), and the
+// bucket counts the next sort starts from.
 void enqueue_keys(const FluidBufs& b, uint32_t n, const GridPlan& g, cudaStream_t st);
 
-// K2+K4: stable LSD radix sort of (key, id) pairs, the last pass gathering
-// the particle state into sorted order. K3: per-bucket ranges.
-void enqueue_sort_and_ranges(const FluidBufs& b, uint32_t n, const StepParams& P, cudaStream_t st);
+// K2+K3+K4: counting sort of the particles by bucket key, ranked by id
+// inside each bucket (final order = (key, id)); fills the bucket range table
+// and gathers the particle state into sorted order.
+// by_slot: b.sid holds a permutation of [0, n) (the previous sort), walked
+// for locality; otherwise particles are placed in id order.
+void enqueue_sort_and_ranges(const FluidBufs& b, uint32_t n, const StepParams& P, bool by_slot, cudaStream_t st);
 
 // K5: density + EOS in sorted order.
 void enqueue_density(const FluidBufs& b, uint32_t n, const StepParams& P, cudaStream_t st);

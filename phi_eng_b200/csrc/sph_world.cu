@@ -149,8 +149,9 @@ struct World2 {
   bool dev_state_valid = false;
   bool dev_aux_valid = false;
   bool dp_on_device = false;
-  bool keys_valid = false;
+  bool keys_valid = false;   // key[] and the bucket counts match the state
   bool plan_valid = false;
+  uint32_t sid_perm_n = 0;   // d.sid is a permutation of [0, sid_perm_n)
   GridPlan plan{};
 
   int device = -1;
@@ -203,10 +204,8 @@ void free_particle_buffers(FluidBufs& d) {
   dfree(d.mass);
   dfree(d.phase);
   dfree(d.key);
-  dfree(d.ka);
-  dfree(d.va);
-  dfree(d.kb);
-  dfree(d.vb);
+  dfree(d.tkey);
+  dfree(d.tid);
   dfree(d.skey);
   dfree(d.sid);
   dfree(d.spos);
@@ -215,10 +214,7 @@ void free_particle_buffers(FluidBufs& d) {
   dfree(d.sphase);
   dfree(d.sdq);
   dfree(d.spres);
-  dfree(d.hist);
-  dfree(d.dtot);
   d.cap = 0;
-  d.hist_len = 0;
 }
 
 void release_graph(World2* w) {
@@ -242,6 +238,8 @@ bool ensure_device(World2* w) {
     return false;
   if (!w->user_stream) w->stream = w->own_stream;
   if (!cuda_ok(w, cudaMalloc(&w->d.scalar, 64), "cudaMalloc(scalar)")) return false;
+  if (!cuda_ok(w, cudaMemset(w->d.scalar, 0, 64), "cudaMemset(scalar)")) return false;
+  w->d.done = w->d.scalar + 8;
   if (!cuda_ok(w, cudaMallocHost(&w->h_pinned, 64), "cudaMallocHost")) return false;
   w->device = dev;
   return true;
@@ -260,21 +258,19 @@ bool ensure_capacity(World2* w, uint32_t need) {
   release_graph(w);
   uint32_t c = std::max<uint32_t>(need, 1024);
   bool ok = dalloc(w, d.state, c) && dalloc(w, d.mass, c) && dalloc(w, d.phase, c) && dalloc(w, d.key, c) &&
-            dalloc(w, d.ka, c) && dalloc(w, d.va, c) && dalloc(w, d.kb, c) && dalloc(w, d.vb, c) &&
+            dalloc(w, d.tkey, c) && dalloc(w, d.tid, c) &&
             dalloc(w, d.skey, c) && dalloc(w, d.sid, c) && dalloc(w, d.spos, c) && dalloc(w, d.svel, c) &&
             dalloc(w, d.smass, c) && dalloc(w, d.sphase, c) && dalloc(w, d.sdq, c) && dalloc(w, d.spres, c);
-  uint32_t ntiles = (c + kSortTile - 1) / kSortTile;
-  ok = ok && dalloc(w, d.hist, (size_t)256 * ntiles) && dalloc(w, d.dtot, 256);
   if (!ok) {
     free_particle_buffers(d);
     return false;
   }
   d.cap = c;
-  d.hist_len = 256 * ntiles;
   w->dev_state_valid = false;
   w->dev_aux_valid = false;
   w->dp_on_device = false;
   w->keys_valid = false;
+  w->sid_perm_n = 0;
   return true;
 }
 
@@ -333,7 +329,8 @@ void plan_grid(World2* w) {
   const int64_t mx = std::max<int64_t>(2, sx / 8), my = std::max<int64_t>(2, sy / 8);
   uint32_t W = std::max<uint32_t>(4, next_pow2((uint64_t)(sx + 2 * mx)));
   uint32_t H = std::max<uint32_t>(4, next_pow2((uint64_t)(sy + 2 * my)));
-  // bucket budget: ~2 buckets per particle (the range table costs 8 B each)
+  // bucket budget: ~2 buckets per particle (each bucket costs ~20 B of
+  // count / scan / range-table traffic per substep)
   const uint64_t budget = std::min<uint64_t>(1ull << 24, std::max<uint64_t>(1ull << 12, next_pow2(2ull * w->n)));
   while ((uint64_t)W * H > budget) {
     if (W >= H && W > 4)
@@ -357,15 +354,28 @@ void plan_grid(World2* w) {
   w->keys_valid = false;
 }
 
+// Bucket-grid arrays: counts (padded to whole scan tiles), the range table
+// and the scan tile sums.
 bool ensure_range(World2* w) {
   FluidBufs& d = w->d;
-  if (d.range && d.range_cap >= w->plan.nbuckets) return true;
+  const uint32_t m = w->plan.nbuckets + 1;  // buckets + the non-finite sentinel
+  const uint32_t tiles = (m + kBucketScanTile - 1) / kBucketScanTile;
+  if (d.count && d.range_cap >= w->plan.nbuckets) {
+    d.count_len = tiles * kBucketScanTile;
+    return true;
+  }
   cudaStreamSynchronize(w->stream);
-  dfree(d.range);
+  dfree(d.count);
+  dfree(d.start);
+  dfree(d.tilesum);
   d.range_cap = 0;
   release_graph(w);
-  if (!dalloc(w, d.range, w->plan.nbuckets)) return false;
+  const uint32_t len = tiles * kBucketScanTile;
+  if (!dalloc(w, d.count, len) || !dalloc(w, d.start, (size_t)len + 1) || !dalloc(w, d.tilesum, tiles)) return false;
+  if (!cuda_ok(w, cudaMemsetAsync(d.count, 0, sizeof(uint32_t) * len, w->stream), "memset")) return false;
   d.range_cap = w->plan.nbuckets;
+  d.count_len = len;
+  w->keys_valid = false;
   return true;
 }
 
@@ -470,7 +480,7 @@ StepParams make_params(const World2* w, float dt) {
 
 void enqueue_substep_body(World2* w, const StepParams& P, cudaStream_t st) {
   if (w->profiling) cudaEventRecordWithFlags(w->ev[0], st, cudaEventRecordExternal);
-  enqueue_sort_and_ranges(w->d, w->n, P, st);
+  enqueue_sort_and_ranges(w->d, w->n, P, w->sid_perm_n == w->n, st);
   if (w->profiling) cudaEventRecordWithFlags(w->ev[1], st, cudaEventRecordExternal);
   enqueue_density(w->d, w->n, P, st);
   if (w->profiling) cudaEventRecordWithFlags(w->ev[2], st, cudaEventRecordExternal);
@@ -486,6 +496,7 @@ bool run_substep(World2* w, const StepParams& P) {
   std::string sig((const char*)&P, sizeof(P));
   sig.append((const char*)&w->n, sizeof(w->n));
   sig.push_back(w->profiling ? 'p' : '-');
+  sig.push_back(w->sid_perm_n == w->n ? 's' : '-');
   if (!w->gexec || sig != w->gsig) {
     release_graph(w);
     cudaGraph_t g = nullptr;
@@ -503,6 +514,7 @@ bool run_substep(World2* w, const StepParams& P) {
     w->gsig = sig;
   }
   if (!cuda_ok(w, cudaGraphLaunch(w->gexec, w->stream), "graph launch")) return false;
+  w->sid_perm_n = w->n;
   w->substeps++;
   w->host_state_valid = false;
   w->dp_on_device = true;
@@ -636,9 +648,11 @@ void phieng_world_free(World2* w) {
     cudaStreamSynchronize(w->stream);
     release_graph(w);
     free_particle_buffers(w->d);
-    dfree(w->d.range);
     dfree(w->d.bodies);
     dfree(w->d.scalar);
+    dfree(w->d.count);
+    dfree(w->d.start);
+    dfree(w->d.tilesum);
     dfree(w->d_tmp);
     for (auto& e : w->ev)
       if (e) cudaEventDestroy(e);
@@ -785,7 +799,7 @@ int32_t phieng_sph_status(const World2* w, PhiengSphStatus* out) {
   out->substeps = w->substeps;
   out->grid_log2_w = w->plan_valid ? w->plan.log2w : 0;
   out->grid_log2_h = w->plan_valid ? w->plan.log2h : 0;
-  out->sort_passes = w->plan_valid ? sort_plan(w->plan.nbuckets).passes : 0;
+  out->sort_passes = w->plan_valid ? 1 : 0;
   out->grid_cx0 = w->plan_valid ? w->plan.cx0 : 0;
   out->grid_cy0 = w->plan_valid ? w->plan.cy0 : 0;
   return 1;
@@ -830,7 +844,8 @@ int32_t phieng_sph_set_stream(World2* w, void* stream) {
 int32_t phieng_sph_sync(World2* w) {
   if (!w) return 0;
   if (w->device < 0) return w->error == PHIENG_SPH_OK ? 1 : 0;
-  return cuda_ok(w, cudaStreamSynchronize(w->stream), "sync") ? 1 : 0;
+  if (!cuda_ok(w, cudaStreamSynchronize(w->stream), "sync")) return 0;
+  return w->error == PHIENG_SPH_OK ? 1 : 0;
 }
 
 int32_t phieng_sph_set_state(World2* w, const float* xyvv, uint32_t n) {
@@ -920,7 +935,9 @@ uint32_t phieng_sph_debug_sorted(World2* w, uint32_t* ids, uint32_t* keys, uint3
   if (!prepare(w)) return 0;
   const StepParams P = make_params(w, 0.0f);
   enqueue_keys(w->d, w->n, w->plan, w->stream);
-  enqueue_sort_and_ranges(w->d, w->n, P, w->stream);
+  enqueue_sort_and_ranges(w->d, w->n, P, false, w->stream);
+  w->sid_perm_n = w->n;
+  w->keys_valid = false;  // the sort consumed the bucket counts
   uint32_t n = std::min(max, w->n);
   if (ids) cudaMemcpyAsync(ids, w->d.sid, 4ull * n, cudaMemcpyDeviceToHost, w->stream);
   if (keys) cudaMemcpyAsync(keys, w->d.skey, 4ull * n, cudaMemcpyDeviceToHost, w->stream);
@@ -934,7 +951,9 @@ uint32_t phieng_sph_debug_neighbors(World2* w, uint32_t* counts, uint32_t* lists
   if (!prepare(w)) return 0;
   const StepParams P = make_params(w, 0.0f);
   enqueue_keys(w->d, w->n, w->plan, w->stream);
-  enqueue_sort_and_ranges(w->d, w->n, P, w->stream);
+  enqueue_sort_and_ranges(w->d, w->n, P, false, w->stream);
+  w->sid_perm_n = w->n;
+  w->keys_valid = false;  // the sort consumed the bucket counts
   size_t bytes = 4ull * w->n * (1 + (size_t)max_per);
   if (!ensure_tmp(w, bytes)) return 0;
   uint32_t* dc = (uint32_t*)w->d_tmp;
@@ -952,7 +971,9 @@ uint32_t phieng_sph_debug_forces(World2* w, float* fxy, uint32_t max) {
   if (!prepare(w)) return 0;
   const StepParams P = make_params(w, 0.0f);
   enqueue_keys(w->d, w->n, w->plan, w->stream);
-  enqueue_sort_and_ranges(w->d, w->n, P, w->stream);
+  enqueue_sort_and_ranges(w->d, w->n, P, false, w->stream);
+  w->sid_perm_n = w->n;
+  w->keys_valid = false;  // the sort consumed the bucket counts
   enqueue_density(w->d, w->n, P, w->stream);
   if (!ensure_tmp(w, sizeof(float2) * (size_t)w->n)) return 0;
   enqueue_force_integrate(w->d, w->n, P, (float2*)w->d_tmp, w->stream);
