@@ -193,6 +193,12 @@ uint32_t phieng_sph_get_density_pressure(const World2* world, float* density, fl
 /* Recompute the bucket grid from the current particle bounding box. */
 int32_t phieng_sph_replan(World2* world);
 
+/* Fix the bucket grid: 2^log2w x 2^log2h buckets (log2w, log2h >= 2,
+ * log2w + log2h <= 24) with origin cell (cx0, cy0). Cells farther apart than
+ * the grid share buckets; results are unchanged, only the work grows. Stays
+ * in force until phieng_sph_replan. 1 ok, 0 invalid. */
+int32_t phieng_sph_set_grid(World2* world, uint32_t log2w, uint32_t log2h, int32_t cx0, int32_t cy0);
+
 /* max_i x_i and max_i |v_i| over the fluid (the per-step readings of the
  * reference's fluid_dam example, fluid_dam.rs:46-52) into out[0], out[1];
  * reduced on the GPU, 8 bytes copied back. 1 ok, 0 error. Synchronises. */

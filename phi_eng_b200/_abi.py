@@ -133,6 +133,7 @@ SIGNATURES = {
     "phieng_sph_set_state": (C.c_int32, [_P, _F, C.c_uint32]),
     "phieng_sph_get_density_pressure": (C.c_uint32, [_P, _F, _F, C.c_uint32]),
     "phieng_sph_replan": (C.c_int32, [_P]),
+    "phieng_sph_set_grid": (C.c_int32, [_P, C.c_uint32, C.c_uint32, C.c_int32, C.c_int32]),
     "phieng_sph_front_metrics": (C.c_int32, [_P, _F]),
     "phieng_sph_set_profiling": (C.c_int32, [_P, C.c_int32]),
     "phieng_sph_phase_times": (C.c_uint32, [_P, _F, C.c_uint32]),

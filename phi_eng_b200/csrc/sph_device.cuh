@@ -58,6 +58,7 @@ struct StepParams {
   float dt;
   float gx, gy;
   float pr;        // max(particle_radius, 0)
+  float pr_pad;    // pr padded by 0.1% (+1e-30) for the bounding-box reject
   float mu;        // clamp(wall_friction, 0, 1)
   float av_alpha;
   float c_s;       // sqrt(max(stiffness, 0))
@@ -75,6 +76,10 @@ struct DevBody {
   float px, py;
   float xax, xay, yax, yay;
   float a, b;
+  // half extents of the body's world-space bounding box, padded by 0.1%: a
+  // particle farther than this plus its radius from the centre along x or
+  // y cannot touch the body, so the exact test is skipped for it
+  float ex, ey;
 };
 
 __device__ __forceinline__ bool finitef(float v) { return isfinite(v); }
@@ -202,7 +207,8 @@ __device__ __forceinline__ bool collide(float px, float py, float pr, const DevB
 __device__ __forceinline__ void walls(float& x, float& y, float& vx, float& vy,
                                       const DevBody* __restrict__ bodies, const StepParams& P) {
   for (uint32_t k = 0; k < P.nbodies; k++) {
-    DevBody b = bodies[k];
+    const DevBody b = bodies[k];
+    if (fabsf(x - b.px) > b.ex + P.pr_pad || fabsf(y - b.py) > b.ey + P.pr_pad) continue;
     float nx, ny, depth;
     if (!collide(x, y, P.pr, b, nx, ny, depth)) continue;
     if (depth <= 0.0f) continue;

@@ -258,50 +258,89 @@ __device__ __forceinline__ void for_each_candidate(uint32_t key, const uint32_t*
 }
 
 // ---------------------------------------------------------------- K5 density
+// Per-row neighbour masks: for the candidate row oy (0..2 for oy = -1..1) of
+// a particle away from the wrap seam, bit t of nmask[oy * n + s] is set iff
+// slot (row start + t) is a neighbour (d2 < h*h, the particle itself
+// included). A zero mask for the particle's own row (which always holds the
+// particle itself) means "no masks": the row was longer than 64 slots or the
+// particle sits on the seam, and K6 walks the candidates itself.
+constexpr uint32_t kMaskBits = 64;
+
+// Candidate j's density contribution m_j * poly6(d2) when d2 < h*h, else +0
+// (adding +0 to a non-negative sum is exact, so skipping and adding agree).
+__device__ __forceinline__ float density_term(float d2, float m, const StepParams& P) {
+  return d2 < P.hg2 ? __fmul_rn(m, poly6(d2, P)) : 0.0f;
+}
+
 template <bool MASS, bool PHASE>
 __global__ void __launch_bounds__(256) k_density(const float2* __restrict__ spos, const uint32_t* __restrict__ skey,
                                                  const float* __restrict__ smass,
                                                  const uint8_t* __restrict__ sphase, uint32_t n,
-                                                 const uint32_t* __restrict__ range, StepParams P,
-                                                 float2* __restrict__ sdq, float* __restrict__ spres) {
-  uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+                                                 const uint32_t* __restrict__ start, StepParams P,
+                                                 float2* __restrict__ sdq, float* __restrict__ spres,
+                                                 uint64_t* __restrict__ nmask) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n) return;
   const uint32_t k = skey[s];
   const float2 pi = spos[s];
   float rho = 0.0f;
-  if (k < P.grid.nbuckets) {
-    for_each_candidate(k, range, P.grid, [&](int j) {
-      float2 pj = __ldg(&spos[j]);
-      float dx = __fsub_rn(pj.x, pi.x);
-      float dy = __fsub_rn(pj.y, pi.y);
-      float d2 = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
-      if (d2 < P.hg2) {
-        float m = MASS ? __ldg(&smass[j]) : P.mass;
-        rho = __fadd_rn(rho, __fmul_rn(m, poly6(d2, P)));
+  uint64_t mrow[3] = {0, 0, 0};
+  const GridPlan& g = P.grid;
+  if (k < g.nbuckets) {
+    const uint32_t bx = k & g.maskw, by = k >> g.log2w;
+    const bool seam = !(bx >= 1u && bx < g.maskw);
+    bool masks_ok = !seam;
+#pragma unroll
+    for (int oy = 0; oy < 3; oy++) {
+      const uint32_t row = ((by + (uint32_t)oy - 1u) & g.maskh) << g.log2w;
+      if (!seam) {
+        const uint32_t rs = __ldg(&start[row + bx - 1]);
+        const uint32_t re = __ldg(&start[row + bx + 2]);
+        uint64_t m = 0;
+        for (uint32_t j = rs; j < re; j++) {
+          const float2 a = __ldg(&spos[j]);
+          const float dx = __fsub_rn(a.x, pi.x), dy = __fsub_rn(a.y, pi.y);
+          const float d2 = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
+          rho = __fadd_rn(rho, density_term(d2, MASS ? __ldg(&smass[j]) : P.mass, P));
+          if (j - rs < kMaskBits) m |= (uint64_t)(d2 < P.hg2) << (j - rs);
+        }
+        mrow[oy] = m;
+        if (re - rs > kMaskBits) masks_ok = false;
+      } else {
+#pragma unroll 1
+        for (int ox = -1; ox <= 1; ox++) {
+          const uint32_t bb = row + ((bx + (uint32_t)ox) & g.maskw);
+          const uint32_t e = __ldg(&start[bb + 1]);
+          for (uint32_t j = __ldg(&start[bb]); j < e; j++) {
+            const float2 a = __ldg(&spos[j]);
+            const float dx = __fsub_rn(a.x, pi.x), dy = __fsub_rn(a.y, pi.y);
+            const float d2 = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
+            rho = __fadd_rn(rho, density_term(d2, MASS ? __ldg(&smass[j]) : P.mass, P));
+          }
+        }
       }
-    });
+    }
+    if (!masks_ok) mrow[1] = 0;  // K6 walks the candidates itself
   }
+  nmask[s] = mrow[0];
+  nmask[n + s] = mrow[1];
+  nmask[2 * (size_t)n + s] = mrow[2];
   // f32::clamp(0, 3 * max(rest_density, EPS)) (fluid.rs:605)
   float dens = rho;
   if (dens < 0.0f) dens = 0.0f;
   if (dens > P.rho_cap) dens = P.rho_cap;
-  uint32_t ph = PHASE ? min((uint32_t)sphase[s], 3u) : P.uniform_phase;
-  float p = eos(dens, P.rest[ph], P);
-  float rc = fmaxf(dens, kEps);
+  const uint32_t ph = PHASE ? min((uint32_t)sphase[s], 3u) : P.uniform_phase;
+  const float p = eos(dens, P.rest[ph], P);
+  const float rc = fmaxf(dens, kEps);
   sdq[s] = make_float2(dens, __fdiv_rn(p, __fmul_rn(rc, rc)));
   spres[s] = p;
 }
 
 // ---------------------------------------------------------------- K6 force + integrate
-// Per-thread neighbour list (slots in sorted order) kept in shared memory,
-// column-major so that lane t uses bank t. Particles with more neighbours
-// than fit are finished by a second candidate walk that skips the listed ones.
-constexpr uint32_t kNbrCap = 32;
-
 // One neighbour pair of the force loop (fluid.rs:947-990) and of the XSPH
 // sum (fluid.rs:1022-1033), accumulated in the reference's order.
 template <bool MASS>
-__device__ __forceinline__ void pair_terms(int j, float2 pi, float2 vi, float rho_i, float q_i, float m_i,
+__device__ __forceinline__ void pair_terms(uint32_t j, float2 pi, float2 vi, float rho_i, float q_i, float m_i,
                                            const float2* __restrict__ spos, const float2* __restrict__ svel,
                                            const float2* __restrict__ sdq, const float* __restrict__ smass,
                                            const StepParams& P, float& fx, float& fy, float& sx, float& sy) {
@@ -359,14 +398,15 @@ __device__ __forceinline__ void pair_terms(int j, float2 pi, float2 vi, float rh
   }
 }
 
+// The neighbour set comes from K5's row masks (bits in ascending slot order =
+// the reference's visit order); particles without masks walk the candidates.
 template <bool MASS, bool DEBUG>
-__global__ void __launch_bounds__(256, 4) k_force_integrate(
+__global__ void __launch_bounds__(256) k_force_integrate(
     const float2* __restrict__ spos, const float2* __restrict__ svel, const float2* __restrict__ sdq,
     const uint32_t* __restrict__ skey, const uint32_t* __restrict__ sid, const float* __restrict__ smass,
-    uint32_t n, const uint32_t* __restrict__ range, StepParams P, const DevBody* __restrict__ bodies,
-    float4* __restrict__ state_out, uint32_t* __restrict__ key_out, uint32_t* __restrict__ count_out,
-    float2* __restrict__ dbg_force) {
-  __shared__ uint32_t nbr[kNbrCap][256];
+    uint32_t n, const uint32_t* __restrict__ start, StepParams P, const DevBody* __restrict__ bodies,
+    const uint64_t* __restrict__ nmask, float4* __restrict__ state_out, uint32_t* __restrict__ key_out,
+    uint32_t* __restrict__ count_out, float2* __restrict__ dbg_force) {
   const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n) return;
   const uint32_t k = skey[s];
@@ -378,34 +418,38 @@ __global__ void __launch_bounds__(256, 4) k_force_integrate(
   const float rho_i = fmaxf(dqi.x, kEps);
   const float q_i = dqi.y;  // p_i / (rho_i * rho_i)
   float fx = 0.0f, fy = 0.0f, sx = 0.0f, sy = 0.0f;
-  if (k < P.grid.nbuckets) {
-    // pass 1: neighbours j != i (fluid.rs:368-386, :953-955) in visit order
-    uint32_t c = 0;
-    for_each_candidate(k, range, P.grid, [&](int j) {
-      const float2 pj = __ldg(&spos[j]);
-      const float ex = __fsub_rn(pj.x, pi.x);
-      const float ey = __fsub_rn(pj.y, pi.y);
-      const float d2 = __fadd_rn(__fmul_rn(ex, ex), __fmul_rn(ey, ey));
-      if (d2 < P.hg2 && (uint32_t)j != s) {
-        if (c < kNbrCap) nbr[c][threadIdx.x] = (uint32_t)j;
-        c++;
+  const GridPlan& g = P.grid;
+  if (k < g.nbuckets) {
+    const uint32_t bx = k & g.maskw, by = k >> g.log2w;
+    const uint64_t own = nmask[n + s];
+    if (own != 0ull) {
+      // one loop over the three rows' set bits (ascending slots, row by row)
+      const uint32_t rs0 = __ldg(&start[(((by - 1u) & g.maskh) << g.log2w) + bx - 1]);
+      const uint32_t rs1 = __ldg(&start[((by & g.maskh) << g.log2w) + bx - 1]);
+      const uint32_t rs2 = __ldg(&start[(((by + 1u) & g.maskh) << g.log2w) + bx - 1]);
+      const uint64_t m0 = nmask[s], m2 = nmask[2 * (size_t)n + s];
+      uint64_t cur = m0;
+      uint32_t row = 0, base = rs0;
+      for (;;) {
+        while (cur == 0ull && row < 2) {
+          row++;
+          cur = row == 1 ? own : m2;
+          base = row == 1 ? rs1 : rs2;
+        }
+        if (cur == 0ull) break;
+        const uint32_t j = base + (uint32_t)(__ffsll((long long)cur) - 1);
+        cur &= cur - 1ull;
+        if (j != s) pair_terms<MASS>(j, pi, vi, rho_i, q_i, m_i, spos, svel, sdq, smass, P, fx, fy, sx, sy);
       }
-    });
-    // pass 2: the pair terms, lanes busy together
-    const uint32_t cl = min(c, kNbrCap);
-    for (uint32_t t = 0; t < cl; t++)
-      pair_terms<MASS>((int)nbr[t][threadIdx.x], pi, vi, rho_i, q_i, m_i, spos, svel, sdq, smass, P, fx, fy, sx, sy);
-    if (c > kNbrCap) {
-      uint32_t seen = 0;
-      for_each_candidate(k, range, P.grid, [&](int j) {
+    } else {
+      for_each_candidate(k, start, g, [&](int jj) {
+        const uint32_t j = (uint32_t)jj;
         const float2 pj = __ldg(&spos[j]);
         const float ex = __fsub_rn(pj.x, pi.x);
         const float ey = __fsub_rn(pj.y, pi.y);
         const float d2 = __fadd_rn(__fmul_rn(ex, ex), __fmul_rn(ey, ey));
-        if (d2 < P.hg2 && (uint32_t)j != s) {
-          if (seen >= kNbrCap) pair_terms<MASS>(j, pi, vi, rho_i, q_i, m_i, spos, svel, sdq, smass, P, fx, fy, sx, sy);
-          seen++;
-        }
+        if (d2 < P.hg2 && j != s)
+          pair_terms<MASS>(j, pi, vi, rho_i, q_i, m_i, spos, svel, sdq, smass, P, fx, fy, sx, sy);
       });
     }
   }
@@ -565,13 +609,13 @@ void enqueue_density(const FluidBufs& b, uint32_t n, const StepParams& P, cudaSt
   const bool m = (P.flags & F_MASS) != 0, ph = (P.flags & F_PHASE) != 0;
   const uint32_t g = cdiv(n, 256);
   if (m && ph)
-    k_density<true, true><<<g, 256, 0, st>>>(b.spos, b.skey, b.smass, b.sphase, n, b.start, P, b.sdq, b.spres);
+    k_density<true, true><<<g, 256, 0, st>>>(b.spos, b.skey, b.smass, b.sphase, n, b.start, P, b.sdq, b.spres, b.nmask);
   else if (m)
-    k_density<true, false><<<g, 256, 0, st>>>(b.spos, b.skey, b.smass, b.sphase, n, b.start, P, b.sdq, b.spres);
+    k_density<true, false><<<g, 256, 0, st>>>(b.spos, b.skey, b.smass, b.sphase, n, b.start, P, b.sdq, b.spres, b.nmask);
   else if (ph)
-    k_density<false, true><<<g, 256, 0, st>>>(b.spos, b.skey, b.smass, b.sphase, n, b.start, P, b.sdq, b.spres);
+    k_density<false, true><<<g, 256, 0, st>>>(b.spos, b.skey, b.smass, b.sphase, n, b.start, P, b.sdq, b.spres, b.nmask);
   else
-    k_density<false, false><<<g, 256, 0, st>>>(b.spos, b.skey, b.smass, b.sphase, n, b.start, P, b.sdq, b.spres);
+    k_density<false, false><<<g, 256, 0, st>>>(b.spos, b.skey, b.smass, b.sphase, n, b.start, P, b.sdq, b.spres, b.nmask);
 }
 
 void enqueue_force_integrate(const FluidBufs& b, uint32_t n, const StepParams& P, float2* dbg_force,
@@ -582,17 +626,17 @@ void enqueue_force_integrate(const FluidBufs& b, uint32_t n, const StepParams& P
   if (dbg_force) {
     if (m)
       k_force_integrate<true, true><<<g, 256, 0, st>>>(b.spos, b.svel, b.sdq, b.skey, b.sid, b.smass, n, b.start, P,
-                                                       b.bodies, b.state, b.key, b.count, dbg_force);
+                                                       b.bodies, b.nmask, b.state, b.key, b.count, dbg_force);
     else
       k_force_integrate<false, true><<<g, 256, 0, st>>>(b.spos, b.svel, b.sdq, b.skey, b.sid, b.smass, n, b.start,
-                                                        P, b.bodies, b.state, b.key, b.count, dbg_force);
+                                                        P, b.bodies, b.nmask, b.state, b.key, b.count, dbg_force);
   } else {
     if (m)
       k_force_integrate<true, false><<<g, 256, 0, st>>>(b.spos, b.svel, b.sdq, b.skey, b.sid, b.smass, n, b.start,
-                                                        P, b.bodies, b.state, b.key, b.count, nullptr);
+                                                        P, b.bodies, b.nmask, b.state, b.key, b.count, nullptr);
     else
       k_force_integrate<false, false><<<g, 256, 0, st>>>(b.spos, b.svel, b.sdq, b.skey, b.sid, b.smass, n,
-                                                         b.start, P, b.bodies, b.state, b.key, b.count, nullptr);
+                                                         b.start, P, b.bodies, b.nmask, b.state, b.key, b.count, nullptr);
   }
 }
 

@@ -151,6 +151,7 @@ struct World2 {
   bool dp_on_device = false;
   bool keys_valid = false;   // key[] and the bucket counts match the state
   bool plan_valid = false;
+  bool plan_locked = false;  // set by phieng_sph_set_grid: no automatic replan
   uint32_t sid_perm_n = 0;   // d.sid is a permutation of [0, sid_perm_n)
   GridPlan plan{};
 
@@ -214,6 +215,7 @@ void free_particle_buffers(FluidBufs& d) {
   dfree(d.sphase);
   dfree(d.sdq);
   dfree(d.spres);
+  dfree(d.nmask);
   d.cap = 0;
 }
 
@@ -260,7 +262,8 @@ bool ensure_capacity(World2* w, uint32_t need) {
   bool ok = dalloc(w, d.state, c) && dalloc(w, d.mass, c) && dalloc(w, d.phase, c) && dalloc(w, d.key, c) &&
             dalloc(w, d.tkey, c) && dalloc(w, d.tid, c) &&
             dalloc(w, d.skey, c) && dalloc(w, d.sid, c) && dalloc(w, d.spos, c) && dalloc(w, d.svel, c) &&
-            dalloc(w, d.smass, c) && dalloc(w, d.sphase, c) && dalloc(w, d.sdq, c) && dalloc(w, d.spres, c);
+            dalloc(w, d.smass, c) && dalloc(w, d.sphase, c) && dalloc(w, d.sdq, c) && dalloc(w, d.spres, c) &&
+            dalloc(w, d.nmask, 3 * (size_t)c);
   if (!ok) {
     free_particle_buffers(d);
     return false;
@@ -457,6 +460,7 @@ StepParams make_params(const World2* w, float dt) {
   P.gx = w->gx;
   P.gy = w->gy;
   P.pr = rmaxf(c.particle_radius, 0.0f);
+  P.pr_pad = P.pr * 1.001f + 1e-30f;
   float mu = c.wall_friction;
   if (mu < 0.0f) mu = 0.0f;
   if (mu > 1.0f) mu = 1.0f;
@@ -628,7 +632,7 @@ uint32_t add_particles(World2* w, const float* xy, const uint8_t* phases, uint32
   recompute_uniformity(w);
   w->dev_state_valid = false;
   w->dev_aux_valid = false;
-  w->plan_valid = false;
+  if (!w->plan_locked) w->plan_valid = false;
   w->keys_valid = false;
   return n;
 }
@@ -718,6 +722,12 @@ int32_t phieng_world_add_body(World2* w, float px, float py, uint32_t shape_tag,
   bd.xay = 0.0f;
   bd.yax = -0.0f;
   bd.yay = 1.0f;
+  {
+    // world bounding box of the (unrotated) body, padded by 0.1%
+    const float ha = bd.a, hb = bd.shape == 0 ? bd.a : bd.b;
+    bd.ex = (std::fabs(bd.xax) * ha + std::fabs(bd.yax) * hb) * 1.001f + 1e-30f;
+    bd.ey = (std::fabs(bd.xay) * ha + std::fabs(bd.yay) * hb) * 1.001f + 1e-30f;
+  }
   if (w->bodies.size() >= 0x7FFFFFFF) return -1;
   w->bodies.push_back(bd);
   w->bodies_dirty = true;
@@ -734,7 +744,8 @@ int32_t phieng_world_set_fluid_config(World2* w, const FluidConfig2Ffi* cfg) {
   bool regrid = c.smoothing_length != w->cfg.smoothing_length;
   w->cfg = c;
   if (regrid) {
-    w->plan_valid = false;
+    if (w->plan_locked) w->plan.hg = c.smoothing_length;
+    else w->plan_valid = false;
     w->keys_valid = false;
   }
   return 1;
@@ -856,7 +867,7 @@ int32_t phieng_sph_set_state(World2* w, const float* xyvv, uint32_t n) {
   std::memcpy(w->h_state.data(), xyvv, sizeof(float4) * n);
   w->dev_state_valid = false;
   w->keys_valid = false;
-  w->plan_valid = false;
+  if (!w->plan_locked) w->plan_valid = false;
   return 1;
 }
 
@@ -874,7 +885,26 @@ uint32_t phieng_sph_get_density_pressure(const World2* cw, float* dens, float* p
 int32_t phieng_sph_replan(World2* w) {
   if (!w) return 0;
   if (!ensure_host_state(w)) return 0;
+  w->plan_locked = false;
   plan_grid(w);
+  return 1;
+}
+
+int32_t phieng_sph_set_grid(World2* w, uint32_t log2w, uint32_t log2h, int32_t cx0, int32_t cy0) {
+  if (!w || log2w < 2 || log2h < 2 || log2w + log2h > 24) return 0;
+  GridPlan g;
+  g.log2w = log2w;
+  g.log2h = log2h;
+  g.maskw = (1u << log2w) - 1u;
+  g.maskh = (1u << log2h) - 1u;
+  g.nbuckets = 1u << (log2w + log2h);
+  g.cx0 = cx0;
+  g.cy0 = cy0;
+  g.hg = w->cfg.smoothing_length;
+  w->plan = g;
+  w->plan_valid = true;
+  w->plan_locked = true;
+  w->keys_valid = false;
   return 1;
 }
 

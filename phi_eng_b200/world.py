@@ -267,6 +267,11 @@ class World2:
     def replan(self) -> None:
         self._lib.phieng_sph_replan(self._h)
 
+    def set_grid(self, log2w: int, log2h: int, cx0: int = 0, cy0: int = 0) -> None:
+        """Fix the bucket grid (2^log2w x 2^log2h buckets from cell (cx0, cy0))."""
+        if self._lib.phieng_sph_set_grid(self._h, log2w, log2h, cx0, cy0) != 1:
+            raise ValueError("invalid bucket grid")
+
 
 def world_from_scene(scene, cap: int | None = None) -> World2:
     """Build a World2 from a phi_eng_b200.scenes.Scene."""
