@@ -146,6 +146,7 @@ uint32_t phieng_world_fluid_get(const World2* world, float* out, uint32_t max);
 #define PHIENG_SPH_E_CUDA 2        /* a CUDA call failed */
 #define PHIENG_SPH_E_UNSUPPORTED 3 /* config enables a feature this library lacks */
 #define PHIENG_SPH_E_ARG 4         /* invalid argument */
+#define PHIENG_SPH_E_TOO_LARGE 5   /* more particles than phieng_sph_density_noalloc holds */
 
 typedef struct PhiengSphStatus {
   int32_t error;          /* last error (sticky until phieng_sph_clear_error) */
@@ -210,6 +211,24 @@ int32_t phieng_sph_set_profiling(World2* world, int32_t on);
 /* Milliseconds of each phase of the most recent substep (3 values);
  * returns the count written, 0 if profiling is off. Synchronises. */
 uint32_t phieng_sph_phase_times(World2* world, float* ms, uint32_t max);
+
+/* Density and pressure of n particles (phase 0) at the positions xy
+ * (device memory, interleaved [x0, y0, x1, y1, ...]) into density[n] and
+ * pressure[n] (device memory, input order), computed as one density pass of
+ * the fluid step under cfg, on `stream` (a cudaStream_t; null = legacy
+ * default stream). No counterpart in the reference: it exists for callers
+ * that must not allocate GPU memory while they run, such as a game engine's
+ * simulation thread, where cudaMalloc can synchronise the device and stall
+ * the frame, or a host that reserves all its GPU memory up front. It
+ * allocates nothing: all scratch lives in one fixed device array of about
+ * 6 MiB inside this library (held on every GPU that loads it until exit),
+ * which limits n to 65536 (more returns PHIENG_SPH_E_TOO_LARGE). The first
+ * call on a device resolves that array's address; make it before any stream
+ * capture. Calls share the array, so calls whose GPU work overlaps race:
+ * order them on the device. Synchronises the stream once (to read the
+ * particles' bounding box). Returns PHIENG_SPH_OK or an error code. */
+int32_t phieng_sph_density_noalloc(const float* xy, uint32_t n, const FluidConfig2Ffi* cfg, float* density,
+                                   float* pressure, void* stream);
 
 /* ---- diagnostics used by the parity tests ---- */
 

@@ -20,6 +20,8 @@ E_NO_DEVICE = 1
 E_CUDA = 2
 E_UNSUPPORTED = 3
 E_ARG = 4
+E_TOO_LARGE = 5
+NOALLOC_MAX_PARTICLES = 65536
 
 
 class FluidConfig2Ffi(C.Structure):
@@ -137,6 +139,7 @@ SIGNATURES = {
     "phieng_sph_front_metrics": (C.c_int32, [_P, _F]),
     "phieng_sph_set_profiling": (C.c_int32, [_P, C.c_int32]),
     "phieng_sph_phase_times": (C.c_uint32, [_P, _F, C.c_uint32]),
+    "phieng_sph_density_noalloc": (C.c_int32, [_P, C.c_uint32, C.POINTER(FluidConfig2Ffi), _P, _P, _P]),
     "phieng_sph_debug_forces": (C.c_uint32, [_P, _F, C.c_uint32]),
     "phieng_sph_debug_sorted": (C.c_uint32, [_P, _U32P, _U32P, C.c_uint32]),
     "phieng_sph_debug_neighbors": (C.c_uint32, [_P, _U32P, _U32P, C.c_uint32, C.c_uint32]),

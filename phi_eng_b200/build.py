@@ -30,6 +30,7 @@ EXACT = ["--fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false"]
 UNITS = [
     ("sph_kernels.cu", EXACT),
     ("sph_world.cu", EXACT),
+    ("sph_noalloc.cu", EXACT),
 ]
 HEADERS = ["sph_device.cuh", "sph_kernels.h"]
 
