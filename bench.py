@@ -116,49 +116,121 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+WORKLOADS = ("dam_break_1m", "dam_break_4k", "batch_512")
+
+
 def make_scene(name: str):
     return {"dam_break_1m": scenes.dam_break_1m, "dam_break_4k": scenes.dam_break_4k}[name]()
 
 
-def workload_desc(sc) -> str:
+def workload_scenes(name: str) -> list:
+    if name == "batch_512":
+        from phi_eng_b200 import batch
+
+        return batch.batched_scenes(512)
+    return [make_scene(name)]
+
+
+def workload_desc(name: str, scs) -> str:
+    sc = scs[0]
+    n = sum(s.n for s in scs)
+    if len(scs) > 1:
+        return (f"{name}: {len(scs)} independent dam-break scenes, {n} particles in total "
+                f"({min(s.n for s in scs)}..{max(s.n for s in scs)} per scene), one CUDA graph per step, "
+                f"h={sc.config.smoothing_length:g} m, Tait gamma={sc.config.gamma:g}, dt={sc.dt:.4e} s")
     return (f"{sc.name}: {sc.n} particles, SPH dam break, h={sc.config.smoothing_length:g} m, "
             f"Tait gamma={sc.config.gamma:g} k={sc.config.stiffness:g}, XSPH {sc.config.viscosity:g}, "
             f"dt={sc.dt:.4e} s, {len(sc.boxes)} static box walls")
 
 
-def cpu_baseline(sc, budget_s: float = 15.0, max_steps: int = 20):
-    """The reference algorithm on one host core (oracle, in-place order)."""
+class Job:
+    """The workload on this GPU: one world, or a batch of scene worlds."""
+
+    def __init__(self, scs):
+        from phi_eng_b200.batch import Batch
+        from phi_eng_b200.world import world_from_scene
+
+        self.scs = scs
+        self.n = sum(sc.n for sc in scs)
+        self.dt = scs[0].dt
+        if len(scs) == 1:
+            self.batch = None
+            self.world = world_from_scene(scs[0])
+        else:
+            self.batch = Batch.from_scenes(scs)
+            self.world = self.batch.world
+
+    def close(self):
+        if self.batch is not None:
+            self.batch.close()
+            for w in self.batch.worlds:
+                w.close()
+        else:
+            self.world.close()
+
+
+def oracle_world(sc):
     from oracle import oracle as orc
 
-    o = orc.OracleWorld(cap=sc.n, libm_pow=True)
+    o = orc.OracleWorld(cap=max(sc.n, 4096), libm_pow=True)
     o.set_gravity(*sc.gravity)
     for (px, py, hx, hy) in sc.boxes:
         o.add_box(px, py, hx, hy, (1.0, 0.0, -0.0, 1.0))
+    for (px, py, r) in sc.circles:
+        o.add_circle(px, py, r, (1.0, 0.0, -0.0, 1.0))
     o.set_config(sc.config)
-    o.add_particles(sc.xy)
-    t = o.steps(sc.dt, 1, orc.REF_SEQ)
-    steps = 1
-    more = int(min(max_steps - 1, max(0, budget_s / max(t, 1e-9) - 1)))
-    if more > 0:
-        t += o.steps(sc.dt, more, orc.REF_SEQ)
-        steps += more
-    return {"value": sc.n * steps / t, "unit": METRIC, "cores": 1, "kind": "port",
-            "sample": f"first {steps} steps of {sc.name} ({sc.n} particles), reference (in-place) order, "
-                      f"C++ restatement of fluid.rs, 1 thread, {t:.1f} s"}
+    o.add_particles(sc.xy, sc.phases)
+    return o
+
+
+def cpu_baseline(scs, budget_s: float = 15.0, max_steps: int = 20):
+    """The reference algorithm on one host core (oracle, in-place order), on
+    the first scene(s) of the workload for a bounded number of steps."""
+    from oracle import oracle as orc
+
+    t = 0.0
+    updates = 0
+    used = 0
+    steps_done = 0
+    for sc in scs:
+        o = oracle_world(sc)
+        dt = o.steps(sc.dt, 1, orc.REF_SEQ)
+        steps = 1
+        left = budget_s / max(len(scs), 1) if len(scs) > 1 else budget_s
+        more = int(min(max_steps - 1, max(0, left / max(dt, 1e-9) - 1)))
+        if more > 0:
+            dt += o.steps(sc.dt, more, orc.REF_SEQ)
+            steps += more
+        t += dt
+        updates += sc.n * steps
+        used += 1
+        steps_done = steps
+        if t > budget_s:
+            break
+    what = (f"first {steps_done} steps of {scs[0].name} ({scs[0].n} particles)" if used == 1 else
+            f"{used} of {len(scs)} scenes, about {steps_done} steps each")
+    return {"value": updates / t, "unit": METRIC, "cores": 1, "kind": "port",
+            "sample": f"{what}, reference (in-place) order, C++ restatement of fluid.rs, 1 thread, {t:.1f} s"}
 
 
 def run_reference(args, rank: int):
     if rank != 0:
         return
-    sc = make_scene(args.workload)
+    scs = workload_scenes(args.workload)
+    if len(scs) > 1:
+        line = cpu_baseline(scs, budget_s=120.0, max_steps=max(args.steps, 1))
+        out = {"impl": "reference", "metric": METRIC, "value": line["value"], "unit": METRIC, "n_gpus": args.gpus,
+               "steps": args.steps, "warmup": 0, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+               "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+               "config": {"workload": workload_desc(args.workload, scs), "particles": sum(x.n for x in scs)},
+               "cpu_baseline": line,
+               "e2e": {"value": line["value"], "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(out), flush=True)
+        return
+    sc = scs[0]
     from oracle import oracle as orc
 
-    o = orc.OracleWorld(cap=sc.n, libm_pow=True)
-    o.set_gravity(*sc.gravity)
-    for (px, py, hx, hy) in sc.boxes:
-        o.add_box(px, py, hx, hy, (1.0, 0.0, -0.0, 1.0))
-    o.set_config(sc.config)
-    o.add_particles(sc.xy)
+    o = oracle_world(sc)
     t1 = o.steps(sc.dt, 1, orc.REF_SEQ)  # one step to size the run
     budget = 150.0
     warm = max(0, min(args.warmup - 1, int(budget * 0.1 / max(t1, 1e-9))))
@@ -173,7 +245,7 @@ def run_reference(args, rank: int):
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": METRIC, "n_gpus": args.gpus,
             "steps": k, "warmup": warm + 1, "ms_per_step": 1000.0 * t / k, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": workload_desc(sc), "particles": sc.n},
+            "config": {"workload": workload_desc(args.workload, scs), "particles": sc.n},
             "cpu_baseline": {"value": v, "unit": METRIC, "cores": 1, "kind": "port", "sample": sample},
             "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -192,16 +264,18 @@ def run_ours(args, rank: int, world: int, local_rank: int):
 
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
 
-    sc = make_scene(args.workload)
+    scs = workload_scenes(args.workload)
+    job = Job(scs)
+    n_total, dt = job.n, job.dt
     stream = torch.cuda.Stream()
-    w = world_from_scene(sc)
+    w = job.world
     w.set_stream(stream.cuda_stream)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
     for _ in range(args.warmup):
-        w.step(sc.dt)
+        w.step(dt)
     w.set_profiling(True)
-    w.step(sc.dt)  # capture the profiled graph outside the timed region
+    w.step(dt)  # capture the profiled graph outside the timed region
     st = w.status()
     buckets = (1 << st.grid_log2_w) * (1 << st.grid_log2_h)
     torch.cuda.synchronize()
@@ -218,7 +292,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         with torch.cuda.stream(stream):
             flush.zero_()
         ev[k][0].record(stream)
-        w.step(sc.dt)
+        w.step(dt)
         ev[k][1].record(stream)
         phases.append(w.phase_times())
     torch.cuda.synchronize()
@@ -229,54 +303,60 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_ms = float(t.item())
-    value = sc.n * args.steps * world / (total_ms / 1000.0)
+    value = n_total * args.steps * world / (total_ms / 1000.0)
 
     ph = np.array(phases)
     ph_mean = ph.mean(axis=0)
     names = ["sort_ranges", "density", "force_integrate"]
-    bytes_pp = [sort_bytes(buckets / sc.n), DENSITY_BYTES, FORCE_BYTES]
+    bytes_pp = [sort_bytes(buckets / n_total), DENSITY_BYTES, FORCE_BYTES]
     top = int(np.argmax(ph_mean))
     peak, peak_kind = hbm_peak()
-    achieved = bytes_pp[top] * sc.n / (ph_mean[top] / 1000.0) / 1e9
+    achieved = bytes_pp[top] * n_total / (ph_mean[top] / 1000.0) / 1e9
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": None, "kernel": names[top], "bytes_per_particle": bytes_pp[top],
                 "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
                 else "fallback 6650 GB/s"}
-    step_bytes = sum(bytes_pp) * sc.n
+    step_bytes = sum(bytes_pp) * n_total
     whole = {"bytes_per_particle": sum(bytes_pp),
              "achieved_gbs": step_bytes / (total_ms / args.steps / 1000.0) / 1e9}
 
-    # end to end through the C ABI from host buffers: world creation, upload,
-    # K steps each followed by the (max x, peak speed) read-back, final state read
+    # end to end through the C ABI from host buffers: the worlds are built and
+    # filled from host arrays outside the timed region; timed: the first
+    # step's upload of the particles, K x (phieng_world_step +
+    # phieng_sph_front_metrics, an 8-byte read-back), and the final read-back
+    # of every particle's state (phieng_world_fluid_get)
+    job.close()
+    job2 = Job(scs)
     torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
     t0 = time.perf_counter()
-    w2 = world_from_scene(sc)
     for _ in range(args.steps):
-        w2.step(sc.dt)
-        w2.front_metrics()
-    final = w2.fluid.particles
+        job2.world.step(dt)
+        job2.world.front_metrics()
+    final = job2.world.fluid.particles
     e2e_s = time.perf_counter() - t0
-    w2.close()
-    e2e = {"value": sc.n * args.steps * world / e2e_s, "unit": METRIC,
-           "h2d_bytes_per_step": int(sc.n * 8 / args.steps),
+    job2.close()
+    e2e = {"value": n_total * args.steps * world / e2e_s, "unit": METRIC,
+           "h2d_bytes_per_step": int(n_total * 8 / args.steps),
            "d2h_bytes_per_step": int(8 + final.nbytes / args.steps),
-           "timed": "phieng_world_new + fluid_add from host arrays + K x (phieng_world_step + "
+           "timed": "first-step upload of the host particle arrays + K x (phieng_world_step + "
                     "phieng_sph_front_metrics) + phieng_world_fluid_get, wall clock"}
     if dist:
         t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e["value"] = sc.n * args.steps * world / float(t.item())
+        e2e["value"] = n_total * args.steps * world / float(t.item())
 
     base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        base = cpu_baseline(sc)
+        base = cpu_baseline(scs)
 
     if rank == 0:
         kernels_per_step = KERNELS_PER_STEP
         line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": {"workload": workload_desc(sc), "particles": sc.n, "parallelism":
+                "config": {"workload": workload_desc(args.workload, scs), "particles": n_total, "parallelism":
                            ("replicas" if world > 1 else "single"),
                            "l2": "flushed between timed steps (256 MiB write, outside the timed events)",
                            "grid": f"{1 << st.grid_log2_w}x{1 << st.grid_log2_h} buckets"},
@@ -285,7 +365,6 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                 "cpu_baseline": base, "e2e": e2e, "gpu_launches": kernels_per_step * args.steps,
                 "clocks": clocks}
         print(json.dumps(line), flush=True)
-    w.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -297,7 +376,7 @@ def main():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", default="dam_break_1m", choices=["dam_break_1m", "dam_break_4k"])
+    ap.add_argument("--workload", default="dam_break_1m", choices=list(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup

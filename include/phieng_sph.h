@@ -230,6 +230,24 @@ uint32_t phieng_sph_phase_times(World2* world, float* ms, uint32_t max);
 int32_t phieng_sph_density_noalloc(const float* xy, uint32_t n, const FluidConfig2Ffi* cfg, float* density,
                                    float* pressure, void* stream);
 
+/* ---- batches of independent scenes ----
+ * A batch is a World2 holding copies of `count` worlds (particles, static
+ * bodies, fluid config, gravity) as independent scenes that advance together:
+ * phieng_world_step(batch, dt) runs one fluid substep of dt in every scene
+ * (one CUDA graph for the whole batch; each scene's results are those of
+ * stepping that world alone). Scenes may differ in size, walls, gravity and
+ * config; CFL substepping is not available in a batch. phieng_world_fluid_get
+ * returns all particles in scene order; particle-adding, clearing, config,
+ * gravity and body calls fail on a batch. Returns null if any world is null,
+ * is itself a batch, uses CFL substeps or an unsupported feature. */
+World2* phieng_sph_batch_new(World2* const* worlds, uint32_t count);
+uint32_t phieng_sph_batch_scenes(const World2* batch);
+/* Particle range [first, first + count) of one scene. 1 ok, 0 invalid. */
+int32_t phieng_sph_batch_scene_range(const World2* batch, uint32_t scene, uint32_t* first, uint32_t* count);
+/* Copy every scene's particle state (and density / pressure) back into the
+ * worlds it came from (same order and sizes). 1 ok, 0 invalid. */
+int32_t phieng_sph_batch_store(World2* batch, World2* const* worlds, uint32_t count);
+
 /* ---- diagnostics used by the parity tests ---- */
 
 /* Run the density + force passes of one substep on the current state without

@@ -139,6 +139,10 @@ SIGNATURES = {
     "phieng_sph_front_metrics": (C.c_int32, [_P, _F]),
     "phieng_sph_set_profiling": (C.c_int32, [_P, C.c_int32]),
     "phieng_sph_phase_times": (C.c_uint32, [_P, _F, C.c_uint32]),
+    "phieng_sph_batch_new": (_P, [C.POINTER(_P), C.c_uint32]),
+    "phieng_sph_batch_scenes": (C.c_uint32, [_P]),
+    "phieng_sph_batch_scene_range": (C.c_int32, [_P, C.c_uint32, _U32P, _U32P]),
+    "phieng_sph_batch_store": (C.c_int32, [_P, C.POINTER(_P), C.c_uint32]),
     "phieng_sph_density_noalloc": (C.c_int32, [_P, C.c_uint32, C.POINTER(FluidConfig2Ffi), _P, _P, _P]),
     "phieng_sph_debug_forces": (C.c_uint32, [_P, _F, C.c_uint32]),
     "phieng_sph_debug_sorted": (C.c_uint32, [_P, _U32P, _U32P, C.c_uint32]),

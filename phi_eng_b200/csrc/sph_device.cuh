@@ -17,18 +17,23 @@ constexpr float kEpsSq = 1e-12f;
 
 // Bucket grid. A particle's cell (cx, cy) = (floor(x/h), floor(y/h)) as
 // saturating i32 (fluid.rs:350-356) maps to bucket
-//   bx = (cx - cx0) mod W, by = (cy - cy0) mod H, key = by * W + bx,
+//   bx = (cx - cx0) mod W, by = (cy - cy0) mod H, key = base + by * W + bx,
 // W = 2^log2w, H = 2^log2h, both >= 4. Particles with a non-finite position
-// get key = nbuckets (sorted last, never visited), as rebuild_grid skips
+// get key = sentinel (sorted last, never visited), as rebuild_grid skips
 // them (fluid.rs:347-349). Cells that alias into one bucket are at least
 // (W - 2) cells apart, so the distance test (d2 < h*h) rejects every aliased
 // candidate and the per-particle visit order stays the reference's.
+// A batch of independent scenes gives each scene its own bucket range
+// [base, base + nbuckets) of one shared key space, so no scene ever sees
+// another's particles; a single world has base 0 and sentinel = nbuckets.
 struct GridPlan {
   int32_t cx0, cy0;
   uint32_t log2w, log2h;
   uint32_t maskw, maskh;
-  uint32_t nbuckets;
-  float hg;  // config.smoothing_length (the raw value rebuild_grid uses)
+  uint32_t nbuckets;  // buckets of this scene (W * H)
+  float hg;           // config.smoothing_length (the raw value rebuild_grid uses)
+  uint32_t base;      // first key of this scene's buckets
+  uint32_t sentinel;  // key of non-finite particles (= total buckets)
 };
 
 enum StepFlags : uint32_t {
@@ -65,8 +70,21 @@ struct StepParams {
   float surface_tension;
   uint32_t flags;
   uint32_t nbodies;
+  uint32_t body_first;     // first of this scene's bodies in the body array
   uint32_t uniform_phase;  // phase used for every particle when !F_PHASE
 };
+
+// Per-launch scene access: a single world passes its parameters by value
+// (constant bank); a batch reads each particle's scene row from a device
+// table.
+template <bool BATCH>
+__device__ __forceinline__ const StepParams& scene_params(const StepParams& P0, const StepParams* __restrict__ ptab,
+                                                          uint32_t scene) {
+  if constexpr (BATCH)
+    return ptab[scene];
+  else
+    return P0;
+}
 
 // Static body as the fluid sees it: shape 0 = circle (a = radius), 1 = box
 // (a, b = half extents); rotation columns x_axis = (xax, xay), y_axis =
@@ -87,13 +105,13 @@ __device__ __forceinline__ bool finitef(float v) { return isfinite(v); }
 __device__ __forceinline__ uint32_t bucket_of_cell(int32_t cx, int32_t cy, const GridPlan& g) {
   uint32_t bx = ((uint32_t)cx - (uint32_t)g.cx0) & g.maskw;
   uint32_t by = ((uint32_t)cy - (uint32_t)g.cy0) & g.maskh;
-  return (by << g.log2w) | bx;
+  return g.base + ((by << g.log2w) | bx);
 }
 
 // cvt.rmi.s32.f32 = floor then saturating conversion with NaN -> 0, the
 // semantics of `(x / h).floor() as i32` (fluid.rs:351-354).
 __device__ __forceinline__ uint32_t bucket_key(float x, float y, const GridPlan& g) {
-  if (!finitef(x) || !finitef(y)) return g.nbuckets;
+  if (!finitef(x) || !finitef(y)) return g.sentinel;
   int32_t cx = __float2int_rd(__fdiv_rn(x, g.hg));
   int32_t cy = __float2int_rd(__fdiv_rn(y, g.hg));
   return bucket_of_cell(cx, cy, g);
@@ -207,7 +225,7 @@ __device__ __forceinline__ bool collide(float px, float py, float pr, const DevB
 __device__ __forceinline__ void walls(float& x, float& y, float& vx, float& vy,
                                       const DevBody* __restrict__ bodies, const StepParams& P) {
   for (uint32_t k = 0; k < P.nbodies; k++) {
-    const DevBody b = bodies[k];
+    const DevBody b = bodies[P.body_first + k];
     if (fabsf(x - b.px) > b.ex + P.pr_pad || fabsf(y - b.py) > b.ey + P.pr_pad) continue;
     float nx, ny, depth;
     if (!collide(x, y, P.pr, b, nx, ny, depth)) continue;

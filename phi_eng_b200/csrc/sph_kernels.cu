@@ -30,10 +30,6 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
   return m;
 }
 
-// ---------------------------------------------------------------- K1 keys
-__global__ void __launch_bounds__(256) k_keys(const float4* __restrict__ state, uint32_t n, GridPlan g,
-                                              uint32_t* __restrict__ keys, uint32_t* __restrict__ count);
-
 // ---------------------------------------------------------------- K2 bucket sort
 // Counting sort over the whole bucket key (a one-digit radix sort with radix
 // = number of buckets), then an in-bucket rank by id, so the final order is
@@ -73,10 +69,13 @@ __device__ __forceinline__ void count_key(uint32_t* __restrict__ count, uint32_t
 }
 
 // K1: key and bucket count of every particle (id order).
-__global__ void __launch_bounds__(256) k_keys(const float4* __restrict__ state, uint32_t n, GridPlan g,
-                                              uint32_t* __restrict__ keys, uint32_t* __restrict__ count) {
+template <bool BATCH>
+__global__ void __launch_bounds__(256) k_keys(const float4* __restrict__ state, uint32_t n, GridPlan g0,
+                                              BatchTab bt, uint32_t* __restrict__ keys,
+                                              uint32_t* __restrict__ count) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
+  const GridPlan& g = BATCH ? bt.ptab[bt.pscene[i]].grid : g0;
   const float4 s = state[i];
   const uint32_t k = bucket_key(s.x, s.y, g);
   keys[i] = k;
@@ -203,6 +202,8 @@ struct GatherArgs {
   float2* svel;
   float* smass;
   uint8_t* sphase;
+  const uint32_t* pscene;  // batch: scene of each particle (id order), else null
+  uint32_t* sscene;
 };
 
 // Final slot = bucket start + rank of the id among the bucket's ids; the
@@ -227,6 +228,7 @@ __global__ void __launch_bounds__(256) k_fixup(const uint32_t* __restrict__ tkey
   ga.svel[f] = make_float2(st.z, st.w);
   if (ga.smass) ga.smass[f] = ga.mass[id];
   if (ga.sphase) ga.sphase[f] = ga.phase[id];
+  if (ga.sscene) ga.sscene[f] = ga.pscene[id];
 }
 
 // ---------------------------------------------------------------- neighbour walk
@@ -238,10 +240,11 @@ __global__ void __launch_bounds__(256) k_fixup(const uint32_t* __restrict__ tkey
 template <class F>
 __device__ __forceinline__ void for_each_candidate(uint32_t key, const uint32_t* __restrict__ start,
                                                    const GridPlan& g, F&& f) {
-  const uint32_t bx = key & g.maskw, by = key >> g.log2w;
+  const uint32_t local = key - g.base;
+  const uint32_t bx = local & g.maskw, by = local >> g.log2w;
 #pragma unroll 1
   for (int oy = -1; oy <= 1; oy++) {
-    const uint32_t row = ((by + (uint32_t)oy) & g.maskh) << g.log2w;
+    const uint32_t row = g.base + (((by + (uint32_t)oy) & g.maskh) << g.log2w);
     if (bx >= 1u && bx < g.maskw) {
       const uint32_t b0 = row + bx - 1;
       const uint32_t e = __ldg(&start[b0 + 3]);
@@ -272,27 +275,29 @@ __device__ __forceinline__ float density_term(float d2, float m, const StepParam
   return d2 < P.hg2 ? __fmul_rn(m, poly6(d2, P)) : 0.0f;
 }
 
-template <bool MASS, bool PHASE>
+template <bool MASS, bool PHASE, bool BATCH>
 __global__ void __launch_bounds__(256) k_density(const float2* __restrict__ spos, const uint32_t* __restrict__ skey,
                                                  const float* __restrict__ smass,
                                                  const uint8_t* __restrict__ sphase, uint32_t n,
-                                                 const uint32_t* __restrict__ start, StepParams P,
+                                                 const uint32_t* __restrict__ start, StepParams P0, BatchTab bt,
                                                  float2* __restrict__ sdq, float* __restrict__ spres,
                                                  uint64_t* __restrict__ nmask) {
   const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n) return;
+  const StepParams& P = scene_params<BATCH>(P0, bt.ptab, BATCH ? bt.sscene[s] : 0u);
   const uint32_t k = skey[s];
   const float2 pi = spos[s];
   float rho = 0.0f;
   uint64_t mrow[3] = {0, 0, 0};
   const GridPlan& g = P.grid;
-  if (k < g.nbuckets) {
-    const uint32_t bx = k & g.maskw, by = k >> g.log2w;
+  if (k != g.sentinel) {
+    const uint32_t local = k - g.base;
+    const uint32_t bx = local & g.maskw, by = local >> g.log2w;
     const bool seam = !(bx >= 1u && bx < g.maskw);
     bool masks_ok = !seam;
 #pragma unroll
     for (int oy = 0; oy < 3; oy++) {
-      const uint32_t row = ((by + (uint32_t)oy - 1u) & g.maskh) << g.log2w;
+      const uint32_t row = g.base + (((by + (uint32_t)oy - 1u) & g.maskh) << g.log2w);
       if (!seam) {
         const uint32_t rs = __ldg(&start[row + bx - 1]);
         const uint32_t re = __ldg(&start[row + bx + 2]);
@@ -400,15 +405,16 @@ __device__ __forceinline__ void pair_terms(uint32_t j, float2 pi, float2 vi, flo
 
 // The neighbour set comes from K5's row masks (bits in ascending slot order =
 // the reference's visit order); particles without masks walk the candidates.
-template <bool MASS, bool DEBUG>
+template <bool MASS, bool DEBUG, bool BATCH>
 __global__ void __launch_bounds__(256) k_force_integrate(
     const float2* __restrict__ spos, const float2* __restrict__ svel, const float2* __restrict__ sdq,
     const uint32_t* __restrict__ skey, const uint32_t* __restrict__ sid, const float* __restrict__ smass,
-    uint32_t n, const uint32_t* __restrict__ start, StepParams P, const DevBody* __restrict__ bodies,
+    uint32_t n, const uint32_t* __restrict__ start, StepParams P0, BatchTab bt, const DevBody* __restrict__ bodies,
     const uint64_t* __restrict__ nmask, float4* __restrict__ state_out, uint32_t* __restrict__ key_out,
     uint32_t* __restrict__ count_out, float2* __restrict__ dbg_force) {
   const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n) return;
+  const StepParams& P = scene_params<BATCH>(P0, bt.ptab, BATCH ? bt.sscene[s] : 0u);
   const uint32_t k = skey[s];
   const uint32_t id = sid[s];
   const float2 pi = spos[s];
@@ -419,14 +425,15 @@ __global__ void __launch_bounds__(256) k_force_integrate(
   const float q_i = dqi.y;  // p_i / (rho_i * rho_i)
   float fx = 0.0f, fy = 0.0f, sx = 0.0f, sy = 0.0f;
   const GridPlan& g = P.grid;
-  if (k < g.nbuckets) {
-    const uint32_t bx = k & g.maskw, by = k >> g.log2w;
+  if (k != g.sentinel) {
+    const uint32_t local = k - g.base;
+    const uint32_t bx = local & g.maskw, by = local >> g.log2w;
     const uint64_t own = nmask[n + s];
     if (own != 0ull) {
       // one loop over the three rows' set bits (ascending slots, row by row)
-      const uint32_t rs0 = __ldg(&start[(((by - 1u) & g.maskh) << g.log2w) + bx - 1]);
-      const uint32_t rs1 = __ldg(&start[((by & g.maskh) << g.log2w) + bx - 1]);
-      const uint32_t rs2 = __ldg(&start[(((by + 1u) & g.maskh) << g.log2w) + bx - 1]);
+      const uint32_t rs0 = __ldg(&start[g.base + (((by - 1u) & g.maskh) << g.log2w) + bx - 1]);
+      const uint32_t rs1 = __ldg(&start[g.base + ((by & g.maskh) << g.log2w) + bx - 1]);
+      const uint32_t rs2 = __ldg(&start[g.base + (((by + 1u) & g.maskh) << g.log2w) + bx - 1]);
       const uint64_t m0 = nmask[s], m2 = nmask[2 * (size_t)n + s];
       uint64_t cur = m0;
       uint32_t row = 0, base = rs0;
@@ -512,7 +519,7 @@ __global__ void __launch_bounds__(256) k_debug_neighbors(const float2* __restric
   const uint32_t id = sid[s];
   const float2 pi = spos[s];
   uint32_t c = 0;
-  if (k < P.grid.nbuckets) {
+  if (k != P.grid.sentinel) {
     for_each_candidate(k, range, P.grid, [&](int j) {
       float2 pj = spos[j];
       float dx = __fsub_rn(pj.x, pi.x);
@@ -578,12 +585,15 @@ inline uint32_t cdiv(uint32_t a, uint32_t b) { return (a + b - 1) / b; }
 void enqueue_keys(const FluidBufs& b, uint32_t n, const GridPlan& g, cudaStream_t st) {
   cudaMemsetAsync(b.count, 0, sizeof(uint32_t) * b.count_len, st);
   if (n == 0) return;
-  k_keys<<<cdiv(n, 256), 256, 0, st>>>(b.state, n, g, b.key, b.count);
+  if (b.batch.ptab)
+    k_keys<true><<<cdiv(n, 256), 256, 0, st>>>(b.state, n, g, b.batch, b.key, b.count);
+  else
+    k_keys<false><<<cdiv(n, 256), 256, 0, st>>>(b.state, n, g, b.batch, b.key, b.count);
 }
 
 void enqueue_sort_and_ranges(const FluidBufs& b, uint32_t n, const StepParams& P, bool by_slot, cudaStream_t st) {
   if (n == 0) return;
-  const uint32_t m = P.grid.nbuckets + 1;  // buckets and the non-finite sentinel
+  const uint32_t m = P.grid.sentinel + 1;  // all buckets and the non-finite sentinel
   const uint32_t nt = cdiv(m, kScanTile);
   k_scan_reduce<<<nt, 256, 0, st>>>(b.count, b.tilesum, nt, b.done);
   k_scan_down<<<nt, 256, 0, st>>>(b.count, b.tilesum, m, b.start);
@@ -599,6 +609,8 @@ void enqueue_sort_and_ranges(const FluidBufs& b, uint32_t n, const StepParams& P
   ga.svel = b.svel;
   ga.smass = (P.flags & F_MASS) ? b.smass : nullptr;
   ga.sphase = (P.flags & F_PHASE) ? b.sphase : nullptr;
+  ga.pscene = b.batch.pscene;
+  ga.sscene = b.batch.ptab ? b.batch.sscene : nullptr;
   k_fixup<<<cdiv(n, 256), 256, 0, st>>>(b.tkey, b.tid, b.start, n, b.skey, b.sid, ga);
   // the counts of the next sort accumulate from zero (K6)
   cudaMemsetAsync(b.count, 0, sizeof(uint32_t) * b.count_len, st);
@@ -606,38 +618,44 @@ void enqueue_sort_and_ranges(const FluidBufs& b, uint32_t n, const StepParams& P
 
 void enqueue_density(const FluidBufs& b, uint32_t n, const StepParams& P, cudaStream_t st) {
   if (n == 0) return;
-  const bool m = (P.flags & F_MASS) != 0, ph = (P.flags & F_PHASE) != 0;
+  const bool m = (P.flags & F_MASS) != 0, ph = (P.flags & F_PHASE) != 0, bat = b.batch.ptab != nullptr;
   const uint32_t g = cdiv(n, 256);
-  if (m && ph)
-    k_density<true, true><<<g, 256, 0, st>>>(b.spos, b.skey, b.smass, b.sphase, n, b.start, P, b.sdq, b.spres, b.nmask);
-  else if (m)
-    k_density<true, false><<<g, 256, 0, st>>>(b.spos, b.skey, b.smass, b.sphase, n, b.start, P, b.sdq, b.spres, b.nmask);
-  else if (ph)
-    k_density<false, true><<<g, 256, 0, st>>>(b.spos, b.skey, b.smass, b.sphase, n, b.start, P, b.sdq, b.spres, b.nmask);
-  else
-    k_density<false, false><<<g, 256, 0, st>>>(b.spos, b.skey, b.smass, b.sphase, n, b.start, P, b.sdq, b.spres, b.nmask);
+#define PHIENG_DENSITY(M, PH, BT)                                                                            \
+  k_density<M, PH, BT><<<g, 256, 0, st>>>(b.spos, b.skey, b.smass, b.sphase, n, b.start, P, b.batch, b.sdq, \
+                                          b.spres, b.nmask)
+  if (bat) {
+    if (m && ph) PHIENG_DENSITY(true, true, true);
+    else if (m) PHIENG_DENSITY(true, false, true);
+    else if (ph) PHIENG_DENSITY(false, true, true);
+    else PHIENG_DENSITY(false, false, true);
+  } else {
+    if (m && ph) PHIENG_DENSITY(true, true, false);
+    else if (m) PHIENG_DENSITY(true, false, false);
+    else if (ph) PHIENG_DENSITY(false, true, false);
+    else PHIENG_DENSITY(false, false, false);
+  }
+#undef PHIENG_DENSITY
 }
 
 void enqueue_force_integrate(const FluidBufs& b, uint32_t n, const StepParams& P, float2* dbg_force,
                              cudaStream_t st) {
   if (n == 0) return;
-  const bool m = (P.flags & F_MASS) != 0;
+  const bool m = (P.flags & F_MASS) != 0, bat = b.batch.ptab != nullptr;
   const uint32_t g = cdiv(n, 256);
+#define PHIENG_FORCE(M, D, BT)                                                                                     \
+  k_force_integrate<M, D, BT><<<g, 256, 0, st>>>(b.spos, b.svel, b.sdq, b.skey, b.sid, b.smass, n, b.start, P,   \
+                                                 b.batch, b.bodies, b.nmask, b.state, b.key, b.count, dbg_force)
   if (dbg_force) {
-    if (m)
-      k_force_integrate<true, true><<<g, 256, 0, st>>>(b.spos, b.svel, b.sdq, b.skey, b.sid, b.smass, n, b.start, P,
-                                                       b.bodies, b.nmask, b.state, b.key, b.count, dbg_force);
-    else
-      k_force_integrate<false, true><<<g, 256, 0, st>>>(b.spos, b.svel, b.sdq, b.skey, b.sid, b.smass, n, b.start,
-                                                        P, b.bodies, b.nmask, b.state, b.key, b.count, dbg_force);
+    if (m) PHIENG_FORCE(true, true, false);
+    else PHIENG_FORCE(false, true, false);
+  } else if (bat) {
+    if (m) PHIENG_FORCE(true, false, true);
+    else PHIENG_FORCE(false, false, true);
   } else {
-    if (m)
-      k_force_integrate<true, false><<<g, 256, 0, st>>>(b.spos, b.svel, b.sdq, b.skey, b.sid, b.smass, n, b.start,
-                                                        P, b.bodies, b.nmask, b.state, b.key, b.count, nullptr);
-    else
-      k_force_integrate<false, false><<<g, 256, 0, st>>>(b.spos, b.svel, b.sdq, b.skey, b.sid, b.smass, n,
-                                                         b.start, P, b.bodies, b.nmask, b.state, b.key, b.count, nullptr);
+    if (m) PHIENG_FORCE(true, false, false);
+    else PHIENG_FORCE(false, false, false);
   }
+#undef PHIENG_FORCE
 }
 
 void enqueue_unsort_dp(const FluidBufs& b, uint32_t n, float* dens, float* pres, cudaStream_t st) {

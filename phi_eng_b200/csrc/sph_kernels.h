@@ -9,6 +9,14 @@
 namespace phieng {
 
 
+// A batch of independent scenes advanced together: per-scene parameters and
+// each particle's scene (ptab == nullptr: a single world).
+struct BatchTab {
+  const StepParams* ptab = nullptr;  // [scenes] device table
+  const uint32_t* pscene = nullptr;  // id order: scene of each particle
+  uint32_t* sscene = nullptr;        // sorted order (gathered by the sort)
+};
+
 // Device arrays of one fluid. "id order" = insertion order (the reference's
 // particle index); "sorted order" = (bucket key, id) order of the last sort.
 struct FluidBufs {
@@ -35,6 +43,7 @@ struct FluidBufs {
   uint32_t* tilesum = nullptr;  // scan tile sums / offsets
   uint32_t range_cap = 0;       // buckets the arrays above can hold
   uint32_t* done = nullptr;     // scan blocks finished (zero between scans)
+  BatchTab batch;
   DevBody* bodies = nullptr;
   uint32_t bodies_cap = 0;
   unsigned int* scalar = nullptr;  // small device scratch (vmax etc.)

@@ -207,6 +207,8 @@ extern "C" int32_t phieng_sph_density_noalloc(const float* xy, uint32_t n, const
   P.grid.maskw = (1u << lw) - 1u;
   P.grid.maskh = (1u << lh) - 1u;
   P.grid.nbuckets = 1u << (lw + lh);
+  P.grid.base = 0;
+  P.grid.sentinel = P.grid.nbuckets;
   P.grid.cx0 = (int32_t)(x0 - 2);
   P.grid.cy0 = (int32_t)(y0 - 2);
   P.grid.hg = hg;

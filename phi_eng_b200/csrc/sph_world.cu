@@ -173,6 +173,27 @@ struct World2 {
 
   int32_t error = PHIENG_SPH_OK;
   uint64_t substeps = 0;
+
+  // Batch of independent scenes (empty for an ordinary world): scene k owns
+  // particles [first, first + count) and bodies [body_first, +nbodies), and
+  // has its own config, gravity and bucket grid; w->plan then spans all
+  // scenes' buckets.
+  struct Scene {
+    uint32_t first = 0, count = 0;
+    FluidConfig2Ffi cfg;
+    float gx = 0.0f, gy = -9.81f;
+    uint32_t body_first = 0, nbodies = 0;
+    bool mass_uniform = true, phase_uniform = true;
+    float mass_value = 0.0f;
+    uint32_t phase_value = 0;
+    GridPlan plan{};
+  };
+  std::vector<Scene> scenes;
+  StepParams* d_ptab = nullptr;
+  uint32_t* d_pscene = nullptr;
+  uint32_t* d_sscene = nullptr;
+  uint32_t batch_cap = 0;
+  bool is_batch() const { return !scenes.empty(); }
 };
 
 namespace {
@@ -264,6 +285,15 @@ bool ensure_capacity(World2* w, uint32_t need) {
             dalloc(w, d.skey, c) && dalloc(w, d.sid, c) && dalloc(w, d.spos, c) && dalloc(w, d.svel, c) &&
             dalloc(w, d.smass, c) && dalloc(w, d.sphase, c) && dalloc(w, d.sdq, c) && dalloc(w, d.spres, c) &&
             dalloc(w, d.nmask, 3 * (size_t)c);
+  if (ok && w->is_batch()) {
+    dfree(w->d_pscene);
+    dfree(w->d_sscene);
+    dfree(w->d_ptab);
+    ok = dalloc(w, w->d_pscene, c) && dalloc(w, w->d_sscene, c) && dalloc(w, w->d_ptab, w->scenes.size());
+    d.batch.ptab = w->d_ptab;
+    d.batch.pscene = w->d_pscene;
+    d.batch.sscene = w->d_sscene;
+  }
   if (!ok) {
     free_particle_buffers(d);
     return false;
@@ -315,11 +345,12 @@ bool ensure_host_dp(World2* w) {
 }
 
 // Bucket grid from the particle bounding box (host copy must be current).
-void plan_grid(World2* w) {
-  const float hg = w->cfg.smoothing_length;
+// Bucket grid covering the cells of n particles (with a margin), ~2 buckets
+// per particle at most.
+GridPlan plan_for(const float4* st, uint32_t n, float hg) {
   int64_t x0 = INT64_MAX, x1 = INT64_MIN, y0 = INT64_MAX, y1 = INT64_MIN;
-  for (uint32_t i = 0; i < w->n; i++) {
-    float4 s = w->h_state[i];
+  for (uint32_t i = 0; i < n; i++) {
+    float4 s = st[i];
     if (!std::isfinite(s.x) || !std::isfinite(s.y)) continue;
     int32_t cx = sat_floor_i32(s.x / hg), cy = sat_floor_i32(s.y / hg);
     x0 = std::min<int64_t>(x0, cx);
@@ -334,7 +365,7 @@ void plan_grid(World2* w) {
   uint32_t H = std::max<uint32_t>(4, next_pow2((uint64_t)(sy + 2 * my)));
   // bucket budget: ~2 buckets per particle (each bucket costs ~20 B of
   // count / scan / range-table traffic per substep)
-  const uint64_t budget = std::min<uint64_t>(1ull << 24, std::max<uint64_t>(1ull << 12, next_pow2(2ull * w->n)));
+  const uint64_t budget = std::min<uint64_t>(1ull << 24, std::max<uint64_t>(1ull << 12, next_pow2(2ull * n)));
   while ((uint64_t)W * H > budget) {
     if (W >= H && W > 4)
       W >>= 1;
@@ -349,10 +380,34 @@ void plan_grid(World2* w) {
   g.maskw = W - 1;
   g.maskh = H - 1;
   g.nbuckets = W * H;
+  g.base = 0;
+  g.sentinel = g.nbuckets;
   g.cx0 = (int32_t)std::max<int64_t>(INT32_MIN, x0 - mx);
   g.cy0 = (int32_t)std::max<int64_t>(INT32_MIN, y0 - my);
   g.hg = hg;
-  w->plan = g;
+  return g;
+}
+
+void plan_grid(World2* w) {
+  if (w->is_batch()) {
+    // one bucket range per scene, laid end to end
+    uint64_t base = 0;
+    for (auto& sc : w->scenes) {
+      GridPlan g = plan_for(w->h_state.data() + sc.first, sc.count, sc.cfg.smoothing_length);
+      g.base = (uint32_t)base;
+      base += g.nbuckets;
+      sc.plan = g;
+    }
+    for (auto& sc : w->scenes) sc.plan.sentinel = (uint32_t)base;
+    GridPlan all{};
+    all.nbuckets = (uint32_t)base;
+    all.sentinel = (uint32_t)base;
+    all.base = 0;
+    all.hg = w->scenes[0].cfg.smoothing_length;
+    w->plan = all;
+  } else {
+    w->plan = plan_for(w->h_state.data(), w->n, w->cfg.smoothing_length);
+  }
   w->plan_valid = true;
   w->keys_valid = false;
 }
@@ -361,7 +416,7 @@ void plan_grid(World2* w) {
 // and the scan tile sums.
 bool ensure_range(World2* w) {
   FluidBufs& d = w->d;
-  const uint32_t m = w->plan.nbuckets + 1;  // buckets + the non-finite sentinel
+  const uint32_t m = w->plan.sentinel + 1;  // buckets + the non-finite sentinel
   const uint32_t tiles = (m + kBucketScanTile - 1) / kBucketScanTile;
   if (d.count && d.range_cap >= w->plan.nbuckets) {
     d.count_len = tiles * kBucketScanTile;
@@ -402,6 +457,8 @@ bool ensure_bodies(World2* w) {
   return true;
 }
 
+bool upload_scene_table(World2* w, float dt);
+
 // Everything a substep needs: device, buffers, current state on the device,
 // a bucket grid, the bodies and valid keys.
 bool prepare(World2* w) {
@@ -414,6 +471,14 @@ bool prepare(World2* w) {
                                             cudaMemcpyHostToDevice, w->stream),
                          "upload state"))
       return false;
+    if (w->is_batch()) {
+      std::vector<uint32_t> ps(w->n);
+      for (uint32_t k = 0; k < w->scenes.size(); k++)
+        for (uint32_t i = 0; i < w->scenes[k].count; i++) ps[w->scenes[k].first + i] = k;
+      if (!cuda_ok(w, cudaMemcpyAsync(w->d_pscene, ps.data(), 4ull * w->n, cudaMemcpyHostToDevice, w->stream),
+                   "upload scene ids"))
+        return false;
+    }
     w->dev_state_valid = true;
     w->keys_valid = false;
   }
@@ -429,17 +494,19 @@ bool prepare(World2* w) {
   if (!ensure_range(w)) return false;
   if (!ensure_bodies(w)) return false;
   if (!w->keys_valid) {
+    if (w->is_batch() && !upload_scene_table(w, 0.0f)) return false;  // the keys read each scene's grid
     enqueue_keys(w->d, w->n, w->plan, w->stream);
     w->keys_valid = true;
   }
   return cuda_ok(w, cudaGetLastError(), "prepare");
 }
 
-StepParams make_params(const World2* w, float dt) {
-  const FluidConfig2Ffi& c = w->cfg;
+StepParams make_params_for(const FluidConfig2Ffi& c, float gx, float gy, bool mass_uniform, float mass_value,
+                           bool phase_uniform, uint32_t phase_value, const GridPlan& plan, uint32_t body_first,
+                           uint32_t nbodies, float dt) {
   StepParams P;
   std::memset(&P, 0, sizeof(P));
-  P.grid = w->plan;
+  P.grid = plan;
   const float hg = c.smoothing_length;
   P.hg2 = hg * hg;
   const float h = rmaxf(hg, kEps);  // substep's h (fluid.rs:908)
@@ -453,12 +520,12 @@ StepParams make_params(const World2* w, float dt) {
   P.stiffness = c.stiffness;
   P.gamma = c.gamma;
   for (int k = 0; k < 4; k++) P.rest[k] = c.phase_rest_density[k];
-  P.mass = w->mass_value;
+  P.mass = mass_value;
   P.visc = c.viscosity;
   P.vmax = c.max_velocity;
   P.dt = dt;
-  P.gx = w->gx;
-  P.gy = w->gy;
+  P.gx = gx;
+  P.gy = gy;
   P.pr = rmaxf(c.particle_radius, 0.0f);
   P.pr_pad = P.pr * 1.001f + 1e-30f;
   float mu = c.wall_friction;
@@ -474,12 +541,40 @@ StepParams make_params(const World2* w, float dt) {
   if (c.surface_tension > 0.0f) f |= F_COHESION;
   if (c.wall_friction > 0.0f) f |= F_FRICTION;
   if (c.gamma != 1.0f) f |= F_TAIT;
-  if (!w->mass_uniform) f |= F_MASS;
-  if (!w->phase_uniform) f |= F_PHASE;
+  if (!mass_uniform) f |= F_MASS;
+  if (!phase_uniform) f |= F_PHASE;
   P.flags = f;
-  P.nbodies = (uint32_t)w->bodies.size();
-  P.uniform_phase = w->phase_value;
+  P.nbodies = nbodies;
+  P.body_first = body_first;
+  P.uniform_phase = phase_value;
   return P;
+}
+
+StepParams make_params(const World2* w, float dt) {
+  if (!w->is_batch())
+    return make_params_for(w->cfg, w->gx, w->gy, w->mass_uniform, w->mass_value, w->phase_uniform, w->phase_value,
+                           w->plan, 0, (uint32_t)w->bodies.size(), dt);
+  // batch: the kernels read each scene's row of the device table; the launch
+  // parameters carry the union of the per-particle array flags and the
+  // global key range
+  StepParams P = make_params_for(w->scenes[0].cfg, 0.0f, 0.0f, true, 0.0f, true, 0, w->plan, 0, 0, dt);
+  for (const auto& sc : w->scenes) {
+    if (!sc.mass_uniform) P.flags |= F_MASS;
+    if (!sc.phase_uniform) P.flags |= F_PHASE;
+  }
+  return P;
+}
+
+// Per-scene parameter rows of a batch for substeps of length dt.
+bool upload_scene_table(World2* w, float dt) {
+  std::vector<StepParams> tab;
+  tab.reserve(w->scenes.size());
+  for (const auto& sc : w->scenes)
+    tab.push_back(make_params_for(sc.cfg, sc.gx, sc.gy, sc.mass_uniform, sc.mass_value, sc.phase_uniform,
+                                  sc.phase_value, sc.plan, sc.body_first, sc.nbodies, dt));
+  return cuda_ok(w, cudaMemcpyAsync(w->d_ptab, tab.data(), sizeof(StepParams) * tab.size(), cudaMemcpyHostToDevice,
+                                    w->stream),
+                 "upload scene table");
 }
 
 void enqueue_substep_body(World2* w, const StepParams& P, cudaStream_t st) {
@@ -576,6 +671,16 @@ bool unsupported(World2* w) {
 
 // World2::step (world.rs:706-732) restricted to the fluid phase (1b).
 bool world_step(World2* w, float dt) {
+  if (w->is_batch()) {
+    // every scene advances one substep of dt (batches take no CFL substeps)
+    if (w->n > 0 && dt > 0.0f) {
+      if (!prepare(w)) return false;
+      if (!upload_scene_table(w, dt)) return false;
+      if (!run_substep(w, make_params(w, dt))) return false;
+    }
+    w->time += dt;
+    return true;
+  }
   if (w->cfg.enabled && w->n > 0 && dt > 0.0f) {  // step_fluid guards (fluid.rs:550-552)
     if (unsupported(w)) return false;
     if (!prepare(w)) return false;
@@ -658,6 +763,9 @@ void phieng_world_free(World2* w) {
     dfree(w->d.start);
     dfree(w->d.tilesum);
     dfree(w->d_tmp);
+    dfree(w->d_pscene);
+    dfree(w->d_sscene);
+    dfree(w->d_ptab);
     for (auto& e : w->ev)
       if (e) cudaEventDestroy(e);
     if (w->h_pinned) cudaFreeHost(w->h_pinned);
@@ -672,7 +780,7 @@ void phieng_world_step(World2* w, float dt) {
 }
 
 void phieng_world_set_gravity(World2* w, float gx, float gy) {
-  if (!w || !std::isfinite(gx) || !std::isfinite(gy)) return;
+  if (!w || w->is_batch() || !std::isfinite(gx) || !std::isfinite(gy)) return;
   w->gx = gx;
   w->gy = gy;
 }
@@ -698,7 +806,7 @@ int32_t phieng_world_add_body(World2* w, float px, float py, uint32_t shape_tag,
                               uint8_t is_static, float friction, float restitution) {
   (void)friction;
   (void)restitution;
-  if (!w || !std::isfinite(px) || !std::isfinite(py)) return -1;
+  if (!w || w->is_batch() || !std::isfinite(px) || !std::isfinite(py)) return -1;
   DevBody bd;
   std::memset(&bd, 0, sizeof(bd));
   auto pos = [](float v) { return std::isfinite(v) && v > 0.0f; };
@@ -735,7 +843,7 @@ int32_t phieng_world_add_body(World2* w, float px, float py, uint32_t shape_tag,
 }
 
 int32_t phieng_world_set_fluid_config(World2* w, const FluidConfig2Ffi* cfg) {
-  if (!w || !cfg) return 0;
+  if (!w || !cfg || w->is_batch()) return 0;
   if (!valid_config(*cfg)) return 0;
   FluidConfig2Ffi c = *cfg;
   c.adaptive_resolution = c.adaptive_resolution ? 1 : 0;
@@ -758,12 +866,12 @@ int32_t phieng_world_get_fluid_config(World2* w, FluidConfig2Ffi* out) {
 }
 
 uint32_t phieng_world_fluid_add(World2* w, const float* positions, uint32_t count) {
-  if (!w || !positions) return 0;
+  if (!w || !positions || w->is_batch()) return 0;
   return add_particles(w, positions, nullptr, count);
 }
 
 uint32_t phieng_world_fluid_add_phase(World2* w, const float* positions, const uint8_t* phases, uint32_t count) {
-  if (!w || !positions || !phases) return 0;
+  if (!w || !positions || !phases || w->is_batch()) return 0;
   return add_particles(w, positions, phases, count);
 }
 
@@ -773,7 +881,7 @@ uint32_t phieng_world_fluid_count(const World2* w) {
 }
 
 int32_t phieng_world_fluid_clear(World2* w) {
-  if (!w) return 0;
+  if (!w || w->is_batch()) return 0;
   if (w->device >= 0) cudaStreamSynchronize(w->stream);
   w->n = 0;
   w->h_state.clear();
@@ -891,13 +999,15 @@ int32_t phieng_sph_replan(World2* w) {
 }
 
 int32_t phieng_sph_set_grid(World2* w, uint32_t log2w, uint32_t log2h, int32_t cx0, int32_t cy0) {
-  if (!w || log2w < 2 || log2h < 2 || log2w + log2h > 24) return 0;
+  if (!w || w->is_batch() || log2w < 2 || log2h < 2 || log2w + log2h > 24) return 0;
   GridPlan g;
   g.log2w = log2w;
   g.log2h = log2h;
   g.maskw = (1u << log2w) - 1u;
   g.maskh = (1u << log2h) - 1u;
   g.nbuckets = 1u << (log2w + log2h);
+  g.base = 0;
+  g.sentinel = g.nbuckets;
   g.cx0 = cx0;
   g.cy0 = cy0;
   g.hg = w->cfg.smoothing_length;
@@ -960,7 +1070,7 @@ int32_t phieng_sph_front_metrics(World2* w, float* out) {
 }
 
 uint32_t phieng_sph_debug_sorted(World2* w, uint32_t* ids, uint32_t* keys, uint32_t max) {
-  if (!w || w->n == 0) return 0;
+  if (!w || w->n == 0 || w->is_batch()) return 0;
   if (!ensure_host_dp(w)) return 0;  // the re-sort below invalidates the sorted density
   if (!prepare(w)) return 0;
   const StepParams P = make_params(w, 0.0f);
@@ -976,7 +1086,7 @@ uint32_t phieng_sph_debug_sorted(World2* w, uint32_t* ids, uint32_t* keys, uint3
 }
 
 uint32_t phieng_sph_debug_neighbors(World2* w, uint32_t* counts, uint32_t* lists, uint32_t max_per, uint32_t max) {
-  if (!w || !counts || !lists || w->n == 0 || max < w->n) return 0;
+  if (!w || !counts || !lists || w->n == 0 || max < w->n || w->is_batch()) return 0;
   if (!ensure_host_dp(w)) return 0;
   if (!prepare(w)) return 0;
   const StepParams P = make_params(w, 0.0f);
@@ -996,7 +1106,7 @@ uint32_t phieng_sph_debug_neighbors(World2* w, uint32_t* counts, uint32_t* lists
 }
 
 uint32_t phieng_sph_debug_forces(World2* w, float* fxy, uint32_t max) {
-  if (!w || !fxy || w->n == 0 || max < w->n) return 0;
+  if (!w || !fxy || w->n == 0 || max < w->n || w->is_batch()) return 0;
   if (!ensure_host_dp(w)) return 0;
   if (!prepare(w)) return 0;
   const StepParams P = make_params(w, 0.0f);
@@ -1011,6 +1121,91 @@ uint32_t phieng_sph_debug_forces(World2* w, float* fxy, uint32_t max) {
   if (!cuda_ok(w, cudaStreamSynchronize(w->stream), "debug_forces")) return 0;
   w->dp_on_device = true;
   return w->n;
+}
+
+// ---------------------------------------------------------------- batches
+World2* phieng_sph_batch_new(World2* const* worlds, uint32_t count) {
+  if (!worlds || count == 0) return nullptr;
+  for (uint32_t k = 0; k < count; k++) {
+    World2* src = worlds[k];
+    if (!src || src->is_batch()) return nullptr;
+    const FluidConfig2Ffi& c = src->cfg;
+    if (!c.enabled || c.adaptive_resolution || c.boundary_particles || (c.cfl > 0.0f && c.max_substeps > 1))
+      return nullptr;
+    if (!ensure_host_state(src) || !ensure_host_dp(src)) return nullptr;
+  }
+  World2* b = new (std::nothrow) World2();
+  if (!b) return nullptr;
+  uint64_t total = 0;
+  for (uint32_t k = 0; k < count; k++) total += worlds[k]->n;
+  if (total > 0xFFFFFFFFull) {
+    delete b;
+    return nullptr;
+  }
+  b->n = (uint32_t)total;
+  b->cap = b->n;
+  b->cfg = worlds[0]->cfg;
+  b->h_state.reserve(b->n);
+  for (uint32_t k = 0; k < count; k++) {
+    World2* src = worlds[k];
+    World2::Scene sc;
+    sc.first = (uint32_t)b->h_state.size();
+    sc.count = src->n;
+    sc.cfg = src->cfg;
+    sc.gx = src->gx;
+    sc.gy = src->gy;
+    sc.body_first = (uint32_t)b->bodies.size();
+    sc.nbodies = (uint32_t)src->bodies.size();
+    sc.mass_uniform = src->mass_uniform;
+    sc.mass_value = src->mass_value;
+    sc.phase_uniform = src->phase_uniform;
+    sc.phase_value = src->phase_value;
+    b->h_state.insert(b->h_state.end(), src->h_state.begin(), src->h_state.end());
+    b->h_mass.insert(b->h_mass.end(), src->h_mass.begin(), src->h_mass.end());
+    b->h_phase.insert(b->h_phase.end(), src->h_phase.begin(), src->h_phase.end());
+    b->h_dens.insert(b->h_dens.end(), src->h_dens.begin(), src->h_dens.end());
+    b->h_pres.insert(b->h_pres.end(), src->h_pres.begin(), src->h_pres.end());
+    b->bodies.insert(b->bodies.end(), src->bodies.begin(), src->bodies.end());
+    b->scenes.push_back(sc);
+  }
+  // the per-particle mass / phase arrays are uploaded when any scene needs them
+  b->mass_uniform = b->phase_uniform = true;
+  for (const auto& sc : b->scenes) {
+    b->mass_uniform = b->mass_uniform && sc.mass_uniform;
+    b->phase_uniform = b->phase_uniform && sc.phase_uniform;
+  }
+  return b;
+}
+
+uint32_t phieng_sph_batch_scenes(const World2* b) {
+  if (!b) return 0;
+  return (uint32_t)b->scenes.size();
+}
+
+int32_t phieng_sph_batch_scene_range(const World2* b, uint32_t scene, uint32_t* first, uint32_t* count) {
+  if (!b || scene >= b->scenes.size() || !first || !count) return 0;
+  *first = b->scenes[scene].first;
+  *count = b->scenes[scene].count;
+  return 1;
+}
+
+int32_t phieng_sph_batch_store(World2* b, World2* const* worlds, uint32_t count) {
+  if (!b || !b->is_batch() || !worlds || count != b->scenes.size()) return 0;
+  for (uint32_t k = 0; k < count; k++)
+    if (!worlds[k] || worlds[k]->is_batch() || worlds[k]->n != b->scenes[k].count) return 0;
+  if (!ensure_host_state(b) || !ensure_host_dp(b)) return 0;
+  for (uint32_t k = 0; k < count; k++) {
+    World2* dst = worlds[k];
+    const World2::Scene& sc = b->scenes[k];
+    if (!ensure_host_state(dst) || !ensure_host_dp(dst)) return 0;
+    std::copy(b->h_state.begin() + sc.first, b->h_state.begin() + sc.first + sc.count, dst->h_state.begin());
+    std::copy(b->h_dens.begin() + sc.first, b->h_dens.begin() + sc.first + sc.count, dst->h_dens.begin());
+    std::copy(b->h_pres.begin() + sc.first, b->h_pres.begin() + sc.first + sc.count, dst->h_pres.begin());
+    dst->dev_state_valid = false;
+    dst->keys_valid = false;
+    if (!dst->plan_locked) dst->plan_valid = false;
+  }
+  return 1;
 }
 
 }  // extern "C"
