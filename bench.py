@@ -46,11 +46,15 @@ HBM_FALLBACK = 6650.0
 #            (20 B per bucket); place: read id 4 + key 4, write (key, id) 8;
 #            fixup: read (key, id) 8 + start 8, write (key, id) 8,
 #            gather state 16 -> write pos 8 + vel 8                = 72 + 20 B/N
-#   density: read pos 8 + key 4, write (density, q) 8 + pressure 4   = 24
-#   force:   read pos 8, vel 8, (density, q) 8, key 4, id 4;
-#            write state 16 + next key 4                             = 52
-DENSITY_BYTES = 24
-FORCE_BYTES = 52
+#   density: read pos 8 + key 4; write (density, q) 8 + pressure 4,
+#            three 64-bit neighbour-row masks 24                    = 48
+#   force:   read pos 8, vel 8, (density, q) 8, key 4, id 4, masks 24;
+#            write state 16 + next key 4                             = 76
+DENSITY_BYTES = 48
+FORCE_BYTES = 76
+# DRAM bytes (read + write) of one launch of the named phase's kernel, from
+# the ncu capture summarised in profiles/<kernel>_<workload>.md.
+PROFILED_TRAFFIC = {("dam_break_1m", "force_integrate"): 60.917248e6 + 4.054272e6}
 KERNELS_PER_STEP = 6  # scan reduce, scan down, place, fixup, density, force
 
 
@@ -68,52 +72,69 @@ def hbm_peak():
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
+    """SM clock and clock-event (throttle) reasons, polled through NVML every
+    ~2 ms on a background thread while the timed steps run (read-only)."""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown",
+               0x40: "hw_thermal_slowdown", 0x80: "hw_power_brake_slowdown"}
 
-    def __init__(self, gpu_index: int):
-        self.gpu = gpu_index
-        self.proc = None
-        self.path = None
+    def __init__(self, cuda_index: int):
+        self.cuda_index = cuda_index
+        self.samples = []
+        self._stop = None
+        self._thread = None
+        self.error = None
+
+    def _handle(self):
+        import pynvml
+        import torch
+
+        pynvml.nvmlInit()
+        try:
+            uuid = str(torch.cuda.get_device_properties(self.cuda_index).uuid)
+            return pynvml.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+        except Exception:
+            return pynvml.nvmlDeviceGetHandleByIndex(self.cuda_index)
 
     def start(self):
-        fd, self.path = tempfile.mkstemp(suffix=".csv")
-        os.close(fd)
+        import threading
+
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
-        except Exception:
-            self.proc = None
+            import pynvml
+
+            h = self._handle()
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+        except Exception as e:  # no NVML: report that instead of numbers
+            self.error = f"nvml unavailable: {e}"
+            return
+        self._stop = threading.Event()
+
+        def run():
+            while not self._stop.is_set():
+                try:
+                    sm = pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)
+                    rs = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
+                    self.samples.append((sm, rs))
+                except Exception:
+                    pass
+                self._stop.wait(0.002)
+
+        self._thread = threading.Thread(target=run, daemon=True)
+        self._thread.start()
 
     def stop(self):
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except Exception:
-            self.proc.kill()
-        sm, mx, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in open(self.path):
-            f = [x.strip() for x in line.split(",")]
-            if len(f) < 9:
-                continue
-            try:
-                sm.append(float(f[1]))
-                mx.append(float(f[2]))
-            except ValueError:
-                continue
-            for name, v in zip(names, f[5:9]):
-                if v.lower().startswith("active"):
+        if self._thread is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [self.error or "not sampled"], "samples": 0}
+        self._stop.set()
+        self._thread.join()
+        sm = [x[0] for x in self.samples]
+        reasons = set()
+        for _, r in self.samples:
+            for bit, name in self.REASONS.items():
+                if r & bit:
                     reasons.add(name)
-        os.unlink(self.path)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(reasons), "samples": len(sm), "source": "nvml"}
 
 
 WORKLOADS = ("dam_break_1m", "dam_break_4k", "batch_512")
@@ -277,7 +298,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     w.set_profiling(True)
     w.step(dt)  # capture the profiled graph outside the timed region
     st = w.status()
-    buckets = (1 << st.grid_log2_w) * (1 << st.grid_log2_h)
+    buckets = st.grid_buckets
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
@@ -313,7 +334,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     peak, peak_kind = hbm_peak()
     achieved = bytes_pp[top] * n_total / (ph_mean[top] / 1000.0) / 1e9
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": None, "kernel": names[top], "bytes_per_particle": bytes_pp[top],
+                "traffic": PROFILED_TRAFFIC.get((args.workload, names[top])), "kernel": names[top], "bytes_per_particle": bytes_pp[top],
                 "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
                 else "fallback 6650 GB/s"}
     step_bytes = sum(bytes_pp) * n_total
@@ -359,7 +380,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                 "config": {"workload": workload_desc(args.workload, scs), "particles": n_total, "parallelism":
                            ("replicas" if world > 1 else "single"),
                            "l2": "flushed between timed steps (256 MiB write, outside the timed events)",
-                           "grid": f"{1 << st.grid_log2_w}x{1 << st.grid_log2_h} buckets"},
+                           "buckets": int(buckets)},
                 "roofline": roofline, "whole_step": whole,
                 "phases_ms": {n: float(v) for n, v in zip(names, ph_mean)},
                 "cpu_baseline": base, "e2e": e2e, "gpu_launches": kernels_per_step * args.steps,

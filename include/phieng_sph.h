@@ -157,7 +157,7 @@ typedef struct PhiengSphStatus {
   uint32_t sort_passes;   /* passes of the bucket sort per substep (1) */
   int32_t grid_cx0;       /* bucket grid origin cell: bucket = ((cy - grid_cy0) mod H) * W */
   int32_t grid_cy0;       /*   + ((cx - grid_cx0) mod W), cx = floor(x / h) as i32 */
-  uint32_t reserved;
+  uint32_t grid_buckets;  /* buckets of all scenes (a batch has one grid per scene) */
 } PhiengSphStatus;
 
 /* Fill *out; 1 ok, 0 null. Does not synchronise. */

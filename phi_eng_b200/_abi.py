@@ -95,7 +95,7 @@ class PhiengSphStatus(C.Structure):
         ("sort_passes", C.c_uint32),
         ("grid_cx0", C.c_int32),
         ("grid_cy0", C.c_int32),
-        ("reserved", C.c_uint32),
+        ("grid_buckets", C.c_uint32),
     ]
 
 

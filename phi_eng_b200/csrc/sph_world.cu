@@ -921,6 +921,7 @@ int32_t phieng_sph_status(const World2* w, PhiengSphStatus* out) {
   out->sort_passes = w->plan_valid ? 1 : 0;
   out->grid_cx0 = w->plan_valid ? w->plan.cx0 : 0;
   out->grid_cy0 = w->plan_valid ? w->plan.cy0 : 0;
+  out->grid_buckets = w->plan_valid ? w->plan.sentinel : 0;
   return 1;
 }
 
