@@ -248,6 +248,93 @@ int32_t phieng_sph_batch_scene_range(const World2* batch, uint32_t scene, uint32
  * worlds it came from (same order and sizes). 1 ok, 0 invalid. */
 int32_t phieng_sph_batch_store(World2* batch, World2* const* worlds, uint32_t count);
 
+/* ---- device-resident state (additive; callers that keep data on the GPU) ----
+ * Pointers are CUDA device pointers on the world's device; the copies are
+ * ordered on the world's stream. */
+
+/* Copy up to max particles' [x, y, vx, vy] (insertion order) into dst.
+ * Returns the count copied. */
+uint32_t phieng_sph_get_state_device(World2* world, float* dst, uint32_t max);
+/* Overwrite the state of all n = fluid_count particles from src. 1 ok, 0 on
+ * a count mismatch or null. Works on batches. */
+int32_t phieng_sph_set_state_device(World2* world, const float* src, uint32_t n);
+
+/* ---- learned closure (additive; no reference counterpart) ----
+ * A per-particle network 16 -> 64 -> 64 -> 2 (SiLU, BF16 weights on the
+ * tensor cores, FP32 accumulate) predicts the displacement correction that
+ * lets one substep of ratio * dt_fine track ratio plain substeps of dt_fine.
+ * Parameters: one flat FP32 vector of PHIENG_MLP_PARAMS values,
+ *   W1[64][16] | b1[64] | W2[64][64] | b2[64] | W3[2][64] | b3[2]
+ * (W[out][in]), and PHIENG_MLP_NORM normalisation values
+ *   mu[16] | isd[16] | out_scale[2]
+ * (input x_hat = (x - mu) * isd; output = network * out_scale, in units of
+ * the smoothing length). */
+#define PHIENG_MLP_PARAMS 5378u
+#define PHIENG_MLP_NORM 34u
+#define PHIENG_MLP_FEATURES 16u
+
+typedef struct PhiengMlp PhiengMlp;
+
+/* New network on the current CUDA device: hidden layers U(-1/sqrt(fan_in),
+ * 1/sqrt(fan_in)) from SplitMix64(seed), output layer zero, identity
+ * normalisation. Never null; check phieng_mlp_status. */
+PhiengMlp* phieng_mlp_new(uint64_t seed);
+void phieng_mlp_free(PhiengMlp* mlp);
+/* PHIENG_SPH_OK or the first error. */
+int32_t phieng_mlp_status(const PhiengMlp* mlp);
+/* Stream for the network's work (null: its own stream). */
+int32_t phieng_mlp_set_stream(PhiengMlp* mlp, void* stream);
+/* Host copies of the parameters / normalisation (either may be null). */
+int32_t phieng_mlp_get_params(PhiengMlp* mlp, float* params, float* norm);
+/* Load parameters and normalisation; resets the Adam state and step count. */
+int32_t phieng_mlp_set_params(PhiengMlp* mlp, const float* params, const float* norm);
+/* Adam steps taken since the last set_params. */
+uint32_t phieng_mlp_step_count(PhiengMlp* mlp);
+/* y[n][2] = network(x[n][16]) (device pointers), asynchronous. */
+int32_t phieng_mlp_forward(PhiengMlp* mlp, const float* x, uint32_t n, float* y);
+/* Loss and gradient (host buffers, PHIENG_MLP_PARAMS values) of the minibatch
+ * that training step `iter` with `seed` would draw from the npairs pairs
+ * (x[npairs][16], t[npairs][2], device); batch a multiple of 128. */
+int32_t phieng_mlp_grad(PhiengMlp* mlp, const float* x, const float* t, uint32_t npairs, uint32_t batch,
+                        uint64_t seed, uint32_t iter, float* grad, float* loss);
+/* iters Adam steps (beta 0.9 / 0.999, eps 1e-8, learning rate lr) on
+ * minibatches of `batch` pairs; loss_hist (host, iters values) may be null. */
+int32_t phieng_mlp_train(PhiengMlp* mlp, const float* x, const float* t, uint32_t npairs, uint32_t batch,
+                         uint32_t iters, float lr, uint64_t seed, float* loss_hist);
+/* The pair indices of one minibatch (device idx[batch]). */
+int32_t phieng_mlp_sample_indices(uint32_t npairs, uint32_t batch, uint64_t seed, uint32_t iter, uint32_t* idx,
+                                  void* stream);
+/* Training targets (x_fine - x_coarse) * inv_h per particle from two
+ * [n][4] states (device). */
+int32_t phieng_mlp_targets(const float* fine, const float* coarse, uint32_t n, float inv_h, float* out,
+                           void* stream);
+
+/* Closure inputs of every particle at the current state for a substep of dt
+ * (device feat[n][16], insertion order). The state is unchanged. */
+int32_t phieng_sph_features(World2* world, float dt, float* feat);
+
+#define PHIENG_CLOSURE_JUMP 0u        /* max_i (rho_i after - rho_i before) / rho0 */
+#define PHIENG_CLOSURE_COMPRESSION 1u /* max_i rho_i after / rho0 - 1 */
+
+/* Attach a network (null detaches) for phieng_sph_closure_step: each coarse
+ * step is one substep of ratio * dt_fine with the network's correction; a
+ * coarse step whose density check exceeds threshold is undone and replaced
+ * by ratio plain substeps of dt_fine. The world keeps the pointer. */
+int32_t phieng_sph_set_closure(World2* world, PhiengMlp* mlp, uint32_t ratio, float threshold, uint32_t criterion);
+
+typedef struct PhiengClosureStats {
+  uint32_t coarse_steps; /* coarse steps attempted */
+  uint32_t accepted;     /* kept */
+  uint32_t fallbacks;    /* replaced by plain substeps */
+  uint32_t reserved;
+  float last_check;      /* density check of the last coarse step */
+  float max_check;       /* largest check seen */
+} PhiengClosureStats;
+
+/* Advance by `coarse_steps` x ratio x dt_fine (a single world, no CFL
+ * substeps). stats (may be null) accumulates. 1 ok, 0 on error. */
+int32_t phieng_sph_closure_step(World2* world, float dt_fine, uint32_t coarse_steps, PhiengClosureStats* stats);
+
 /* ---- diagnostics used by the parity tests ---- */
 
 /* Run the density + force passes of one substep on the current state without

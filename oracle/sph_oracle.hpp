@@ -528,6 +528,137 @@ class Fluid {
     return (uint32_t)k;
   }
 
+  // ---- closure-network inputs (no reference counterpart) ----
+  // The 16 inputs of the learned closure for every particle at the current
+  // state, for a coarse step dt. Restates the GPU closure pass
+  // (feat_pair / wall_feature / feat_finish) operation for operation: the
+  // neighbour aggregates run over j != i in the reference's visit order with
+  // the pressure force's pair arithmetic (fluid.rs:942-997), then the
+  // nearest static body within 3h, then the scaled feature vector.
+  void wall_feature(R x, R y, R h, R& fd, R& fnx, R& fny) const {
+    const R lim = (R)3.0 * h;
+    R best = lim, bnx = 0, bny = 0;
+    for (const Body& b : bodies) {
+      const R ha = (R)b.a, hb = b.shape == 0 ? (R)b.a : (R)b.b;
+      // the world's padded bounding box (phieng_world_add_body)
+      const R ex = (std::fabs((R)b.xax) * ha + std::fabs((R)b.yax) * hb) * (R)1.001f + (R)1e-30f;
+      const R ey = (std::fabs((R)b.xay) * ha + std::fabs((R)b.yay) * hb) * (R)1.001f + (R)1e-30f;
+      if (std::fabs(x - (R)b.px) > ex + lim || std::fabs(y - (R)b.py) > ey + lim) continue;
+      R d, nx, ny;
+      if (b.shape == 0) {
+        const R dx = x - (R)b.px, dy = y - (R)b.py;
+        const R dist = std::sqrt(dx * dx + dy * dy);
+        d = dist - (R)b.a;
+        if (dist > (R)kEps) {
+          nx = dx / dist;
+          ny = dy / dist;
+        } else {
+          nx = 1;
+          ny = 0;
+        }
+      } else {
+        const R rx = x - (R)b.px, ry = y - (R)b.py;
+        const R lx = (R)b.xax * rx + (R)b.yax * ry;
+        const R ly = (R)b.xay * rx + (R)b.yay * ry;
+        const R qx = std::fabs(lx) - (R)b.a, qy = std::fabs(ly) - (R)b.b;
+        R lnx, lny;
+        if (qx > (R)0 || qy > (R)0) {
+          const R ox = qx > (R)0 ? qx : (R)0, oy = qy > (R)0 ? qy : (R)0;
+          d = std::sqrt(ox * ox + oy * oy);
+          lnx = std::copysign(ox, lx) / d;
+          lny = std::copysign(oy, ly) / d;
+        } else if (qx >= qy) {
+          d = qx;
+          lnx = std::copysign((R)1, lx);
+          lny = 0;
+        } else {
+          d = qy;
+          lnx = 0;
+          lny = std::copysign((R)1, ly);
+        }
+        nx = (R)b.xax * lnx + (R)b.yax * lny;
+        ny = (R)b.xay * lnx + (R)b.yay * lny;
+      }
+      if (d < best) {
+        best = d;
+        bnx = nx;
+        bny = ny;
+      }
+    }
+    fd = (best > -h ? best : -h) / h;
+    fnx = bnx;
+    fny = bny;
+  }
+
+  void compute_features(R dt, std::vector<R>& out) {
+    const R h = rmax((R)cfg.smoothing_length, (R)kEps);
+    rebuild_grid();
+    compute_density_pressure(h);
+    const size_t n = particles.size();
+    out.assign(16 * n, (R)0);
+    std::vector<uint32_t> nb;
+    const R ih = (R)1 / h;
+    const R s1 = dt * ih, s2 = s1 * s1, s3 = dt * dt * ih;
+    for (size_t i = 0; i < n; i++) {
+      const auto& pi = particles[i];
+      neighbors_of(pi.x, pi.y, particles, nb);
+      const R rho_i = rmax(pi.density, (R)kEps);
+      const R q_i = pi.pressure / (rho_i * rho_i);
+      R px = 0, py = 0, div = 0, curl = 0, wsum = 0, m1x = 0, m1y = 0, m2xx = 0, m2xy = 0, m2yy = 0;
+      uint32_t cnt = 0;
+      for (uint32_t j : nb) {
+        if (j == i) continue;
+        const auto& pj = particles[j];
+        const R rho_j = rmax(pj.density, (R)kEps);
+        const R dx = pi.x - pj.x, dy = pi.y - pj.y;
+        const R d2 = dx * dx + dy * dy;
+        const R dist = std::sqrt(d2);
+        R gxx, gyy;
+        spiky_grad(dx, dy, dist, h, gxx, gyy);
+        const R w = poly6(d2, h);
+        const R q_j = pj.pressure / (rho_j * rho_j);
+        const R mt = pj.mass * (q_i + q_j);
+        px = px - gxx * mt;
+        py = py - gyy * mt;
+        const R vol = pj.mass / rho_j;
+        const R dvx = pj.vx - pi.vx, dvy = pj.vy - pi.vy;
+        div = div + vol * (dvx * gxx + dvy * gyy);
+        curl = curl + vol * (dvx * gyy - dvy * gxx);
+        const R ww = vol * w;
+        wsum = wsum + ww;
+        const R wx = ww * dvx, wy = ww * dvy;
+        m1x = m1x + wx;
+        m1y = m1y + wy;
+        m2xx = m2xx + wx * dvx;
+        m2xy = m2xy + wx * dvy;
+        m2yy = m2yy + wy * dvy;
+        cnt++;
+      }
+      R wd, wnx, wny;
+      wall_feature(pi.x, pi.y, h, wd, wnx, wny);
+      const R r0 = rmax((R)cfg.phase_rest_density[std::min<int>(pi.phase, 3)], (R)kEps);
+      const R kr = (R)cfg.stiffness * r0;
+      R* f = &out[16 * i];
+      f[0] = pi.density / r0 - (R)1;
+      f[1] = kr > (R)0 ? pi.pressure / kr : (R)0;
+      f[2] = div * dt;
+      f[3] = curl * dt;
+      f[4] = (R)cnt * (R)0.0625f;
+      f[5] = wd;
+      f[6] = wnx;
+      f[7] = wny;
+      const R iw = wsum > (R)0 ? (R)1 / wsum : (R)0;
+      f[8] = m1x * iw * s1;
+      f[9] = m1y * iw * s1;
+      f[10] = m2xx * iw * s2;
+      f[11] = m2xy * iw * s2;
+      f[12] = m2yy * iw * s2;
+      f[13] = px / rho_i * s3;
+      f[14] = py / rho_i * s3;
+      f[15] = std::sqrt(pi.vx * pi.vx + pi.vy * pi.vy) * s1;
+    }
+  }
+
   // ---- one substep (fluid.rs:898-1136) for the dam-break feature set ----
   void substep(R dt, Mode mode) {
     R h = rmax((R)cfg.smoothing_length, (R)kEps);

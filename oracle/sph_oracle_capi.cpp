@@ -7,6 +7,8 @@
 #include <chrono>
 #include <cstdint>
 #include <cstring>
+#include <vector>
+#include <algorithm>
 
 #include "../include/phieng_sph.h"
 #include "sph_oracle.hpp"
@@ -364,6 +366,19 @@ uint32_t orc_cfl_substeps(void* h, float dt) {
 }
 
 // scalar kernels for the reference's kernel-sanity tests (f32)
+// Closure features (16 per particle, insertion order) for a coarse step dt.
+uint32_t orc_features(void* h, float dt, float* out, uint32_t max) {
+  Orc* o = static_cast<Orc*>(h);
+  uint32_t r = 0;
+  DISPATCH(o, {
+    std::vector<decltype(F.time)> f;
+    F.compute_features((decltype(F.time))dt, f);
+    r = (uint32_t)std::min<size_t>(max, f.size() / 16);
+    for (size_t i = 0; i < 16 * (size_t)r; i++) out[i] = (float)f[i];
+  });
+  return r;
+}
+
 float orc_poly6(float r2, float h) { return Fluid<float>::poly6(r2, h); }
 void orc_spiky(float rx, float ry, float r, float h, float* out2) {
   Fluid<float>::spiky_grad(rx, ry, r, h, out2[0], out2[1]);

@@ -99,6 +99,23 @@ class PhiengSphStatus(C.Structure):
     ]
 
 
+class PhiengClosureStats(C.Structure):
+    _fields_ = [
+        ("coarse_steps", C.c_uint32),
+        ("accepted", C.c_uint32),
+        ("fallbacks", C.c_uint32),
+        ("reserved", C.c_uint32),
+        ("last_check", C.c_float),
+        ("max_check", C.c_float),
+    ]
+
+
+MLP_PARAMS = 5378
+MLP_NORM = 34
+MLP_FEATURES = 16
+CLOSURE_JUMP = 0
+CLOSURE_COMPRESSION = 1
+
 _P = C.c_void_p
 _F = C.POINTER(C.c_float)
 _U32P = C.POINTER(C.c_uint32)
@@ -144,6 +161,23 @@ SIGNATURES = {
     "phieng_sph_batch_scene_range": (C.c_int32, [_P, C.c_uint32, _U32P, _U32P]),
     "phieng_sph_batch_store": (C.c_int32, [_P, C.POINTER(_P), C.c_uint32]),
     "phieng_sph_density_noalloc": (C.c_int32, [_P, C.c_uint32, C.POINTER(FluidConfig2Ffi), _P, _P, _P]),
+    "phieng_sph_get_state_device": (C.c_uint32, [_P, _P, C.c_uint32]),
+    "phieng_sph_set_state_device": (C.c_int32, [_P, _P, C.c_uint32]),
+    "phieng_mlp_new": (_P, [C.c_uint64]),
+    "phieng_mlp_free": (None, [_P]),
+    "phieng_mlp_status": (C.c_int32, [_P]),
+    "phieng_mlp_set_stream": (C.c_int32, [_P, _P]),
+    "phieng_mlp_get_params": (C.c_int32, [_P, _F, _F]),
+    "phieng_mlp_set_params": (C.c_int32, [_P, _F, _F]),
+    "phieng_mlp_step_count": (C.c_uint32, [_P]),
+    "phieng_mlp_forward": (C.c_int32, [_P, _P, C.c_uint32, _P]),
+    "phieng_mlp_grad": (C.c_int32, [_P, _P, _P, C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint32, _F, _F]),
+    "phieng_mlp_train": (C.c_int32, [_P, _P, _P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_float, C.c_uint64, _F]),
+    "phieng_mlp_sample_indices": (C.c_int32, [C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint32, _P, _P]),
+    "phieng_mlp_targets": (C.c_int32, [_P, _P, C.c_uint32, C.c_float, _P, _P]),
+    "phieng_sph_features": (C.c_int32, [_P, C.c_float, _P]),
+    "phieng_sph_set_closure": (C.c_int32, [_P, _P, C.c_uint32, C.c_float, C.c_uint32]),
+    "phieng_sph_closure_step": (C.c_int32, [_P, C.c_float, C.c_uint32, C.POINTER(PhiengClosureStats)]),
     "phieng_sph_debug_forces": (C.c_uint32, [_P, _F, C.c_uint32]),
     "phieng_sph_debug_sorted": (C.c_uint32, [_P, _U32P, _U32P, C.c_uint32]),
     "phieng_sph_debug_neighbors": (C.c_uint32, [_P, _U32P, _U32P, C.c_uint32, C.c_uint32]),

@@ -31,8 +31,9 @@ UNITS = [
     ("sph_kernels.cu", EXACT),
     ("sph_world.cu", EXACT),
     ("sph_noalloc.cu", EXACT),
+    ("sph_mlp.cu", EXACT),
 ]
-HEADERS = ["sph_device.cuh", "sph_kernels.h"]
+HEADERS = ["sph_device.cuh", "sph_kernels.h", "sph_mlp.cuh", "sph_mlp_host.h"]
 
 
 def _mtime(p: str) -> float:

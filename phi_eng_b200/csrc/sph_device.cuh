@@ -251,4 +251,133 @@ __device__ __forceinline__ void walls(float& x, float& y, float& vx, float& vy,
   }
 }
 
+// ---------------------------------------------------------------- closure features
+// Neighbour aggregates of one particle for the closure network, accumulated
+// over the same neighbour pairs and in the same order as the pressure force
+// (j != i, the reference's visit order). Per pair, with delta = x_i - x_j,
+// grad = spiky_grad(delta), w = poly6(|delta|^2), V_j = m_j / rho_j and
+// dv = v_j - v_i:
+//   pressure force   P -= grad * (m_j * (q_i + q_j)),  q = p / rho^2
+//   divergence       D += V_j * (dv . grad)
+//   curl (z)         C += V_j * (dv.x grad.y - dv.y grad.x)
+//   kernel moments   S += V_j w, M1 += V_j w dv, M2 += V_j w dv dv^T
+struct FeatAcc {
+  float px = 0.0f, py = 0.0f, div = 0.0f, curl = 0.0f;
+  float wsum = 0.0f, m1x = 0.0f, m1y = 0.0f, m2xx = 0.0f, m2xy = 0.0f, m2yy = 0.0f;
+  uint32_t cnt = 0;
+};
+
+__device__ __forceinline__ void feat_pair(FeatAcc& a, float gxx, float gyy, float w, float m_j, float rho_j,
+                                          float q_i, float q_j, float dvx, float dvy) {
+  const float mt = __fmul_rn(m_j, __fadd_rn(q_i, q_j));
+  a.px = __fsub_rn(a.px, __fmul_rn(gxx, mt));
+  a.py = __fsub_rn(a.py, __fmul_rn(gyy, mt));
+  const float vol = __fdiv_rn(m_j, rho_j);
+  a.div = __fadd_rn(a.div, __fmul_rn(vol, __fadd_rn(__fmul_rn(dvx, gxx), __fmul_rn(dvy, gyy))));
+  a.curl = __fadd_rn(a.curl, __fmul_rn(vol, __fsub_rn(__fmul_rn(dvx, gyy), __fmul_rn(dvy, gxx))));
+  const float ww = __fmul_rn(vol, w);
+  a.wsum = __fadd_rn(a.wsum, ww);
+  const float wx = __fmul_rn(ww, dvx), wy = __fmul_rn(ww, dvy);
+  a.m1x = __fadd_rn(a.m1x, wx);
+  a.m1y = __fadd_rn(a.m1y, wy);
+  a.m2xx = __fadd_rn(a.m2xx, __fmul_rn(wx, dvx));
+  a.m2xy = __fadd_rn(a.m2xy, __fmul_rn(wx, dvy));
+  a.m2yy = __fadd_rn(a.m2yy, __fmul_rn(wy, dvy));
+  a.cnt++;
+}
+
+// Nearest static body within 3h: signed distance to its surface (negative
+// inside, from the box's local frame as collide() builds it) and the
+// outward normal in world axes. d is returned in units of h, clamped to
+// [-1, 3]; the normal is zero when no body is that close. A body whose
+// padded bounding box is farther than 3h along x or y cannot be nearer than
+// 3h and is skipped.
+__device__ __forceinline__ void wall_feature(float x, float y, const DevBody* __restrict__ bodies,
+                                             const StepParams& P, float& fd, float& fnx, float& fny) {
+  const float lim = __fmul_rn(3.0f, P.hk);
+  float best = lim, bnx = 0.0f, bny = 0.0f;
+  for (uint32_t k = 0; k < P.nbodies; k++) {
+    const DevBody b = bodies[P.body_first + k];
+    if (fabsf(__fsub_rn(x, b.px)) > __fadd_rn(b.ex, lim) || fabsf(__fsub_rn(y, b.py)) > __fadd_rn(b.ey, lim)) continue;
+    float d, nx, ny;
+    if (b.shape == 0) {
+      const float dx = __fsub_rn(x, b.px), dy = __fsub_rn(y, b.py);
+      const float dist = __fsqrt_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)));
+      d = __fsub_rn(dist, b.a);
+      if (dist > kEps) {
+        nx = __fdiv_rn(dx, dist);
+        ny = __fdiv_rn(dy, dist);
+      } else {
+        nx = 1.0f;
+        ny = 0.0f;
+      }
+    } else {
+      const float rx = __fsub_rn(x, b.px), ry = __fsub_rn(y, b.py);
+      const float lx = __fadd_rn(__fmul_rn(b.xax, rx), __fmul_rn(b.yax, ry));
+      const float ly = __fadd_rn(__fmul_rn(b.xay, rx), __fmul_rn(b.yay, ry));
+      const float qx = __fsub_rn(fabsf(lx), b.a), qy = __fsub_rn(fabsf(ly), b.b);
+      float lnx, lny;
+      if (qx > 0.0f || qy > 0.0f) {
+        const float ox = fmaxf(qx, 0.0f), oy = fmaxf(qy, 0.0f);
+        d = __fsqrt_rn(__fadd_rn(__fmul_rn(ox, ox), __fmul_rn(oy, oy)));
+        lnx = __fdiv_rn(copysignf(ox, lx), d);
+        lny = __fdiv_rn(copysignf(oy, ly), d);
+      } else if (qx >= qy) {
+        d = qx;
+        lnx = copysignf(1.0f, lx);
+        lny = 0.0f;
+      } else {
+        d = qy;
+        lnx = 0.0f;
+        lny = copysignf(1.0f, ly);
+      }
+      nx = __fadd_rn(__fmul_rn(b.xax, lnx), __fmul_rn(b.yax, lny));
+      ny = __fadd_rn(__fmul_rn(b.xay, lnx), __fmul_rn(b.yay, lny));
+    }
+    if (d < best) {
+      best = d;
+      bnx = nx;
+      bny = ny;
+    }
+  }
+  fd = __fdiv_rn(fmaxf(best, -P.hk), P.hk);
+  fnx = bnx;
+  fny = bny;
+}
+
+// The 16 closure inputs of one particle for a coarse step of P.dt:
+//   0 rho/rho0 - 1          1 p / (k rho0)          2 D dt       3 C dt
+//   4 neighbours / 16       5 wall distance / h     6, 7 wall normal
+//   8, 9 M1/S (dt/h)        10..12 M2/S (dt/h)^2 (xx, xy, yy)
+//   13, 14 (P / rho) dt^2/h (pressure displacement over the step)
+//   15 |v| dt / h
+__device__ __forceinline__ void feat_finish(const FeatAcc& a, float dens, float rho_i, float p, float r0, float vx,
+                                            float vy, float wd, float wnx, float wny, const StepParams& P,
+                                            float (&f)[16]) {
+  const float dt = P.dt;
+  const float ih = __fdiv_rn(1.0f, P.hk);
+  const float s1 = __fmul_rn(dt, ih);
+  const float s2 = __fmul_rn(s1, s1);
+  const float s3 = __fmul_rn(__fmul_rn(dt, dt), ih);
+  const float rr = fmaxf(r0, kEps);
+  const float kr = __fmul_rn(P.stiffness, rr);
+  f[0] = __fsub_rn(__fdiv_rn(dens, rr), 1.0f);
+  f[1] = kr > 0.0f ? __fdiv_rn(p, kr) : 0.0f;
+  f[2] = __fmul_rn(a.div, dt);
+  f[3] = __fmul_rn(a.curl, dt);
+  f[4] = __fmul_rn((float)a.cnt, 0.0625f);
+  f[5] = wd;
+  f[6] = wnx;
+  f[7] = wny;
+  const float iw = a.wsum > 0.0f ? __fdiv_rn(1.0f, a.wsum) : 0.0f;
+  f[8] = __fmul_rn(__fmul_rn(a.m1x, iw), s1);
+  f[9] = __fmul_rn(__fmul_rn(a.m1y, iw), s1);
+  f[10] = __fmul_rn(__fmul_rn(a.m2xx, iw), s2);
+  f[11] = __fmul_rn(__fmul_rn(a.m2xy, iw), s2);
+  f[12] = __fmul_rn(__fmul_rn(a.m2yy, iw), s2);
+  f[13] = __fmul_rn(__fdiv_rn(a.px, rho_i), s3);
+  f[14] = __fmul_rn(__fdiv_rn(a.py, rho_i), s3);
+  f[15] = __fmul_rn(__fsqrt_rn(__fadd_rn(__fmul_rn(vx, vx), __fmul_rn(vy, vy))), s1);
+}
+
 }  // namespace phieng

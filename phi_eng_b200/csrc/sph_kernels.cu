@@ -343,12 +343,14 @@ __global__ void __launch_bounds__(256) k_density(const float2* __restrict__ spos
 
 // ---------------------------------------------------------------- K6 force + integrate
 // One neighbour pair of the force loop (fluid.rs:947-990) and of the XSPH
-// sum (fluid.rs:1022-1033), accumulated in the reference's order.
-template <bool MASS>
+// sum (fluid.rs:1022-1033), accumulated in the reference's order. FEAT also
+// accumulates the closure network's neighbour aggregates (feat_pair).
+template <bool MASS, bool FEAT>
 __device__ __forceinline__ void pair_terms(uint32_t j, float2 pi, float2 vi, float rho_i, float q_i, float m_i,
                                            const float2* __restrict__ spos, const float2* __restrict__ svel,
                                            const float2* __restrict__ sdq, const float* __restrict__ smass,
-                                           const StepParams& P, float& fx, float& fy, float& sx, float& sy) {
+                                           const StepParams& P, float& fx, float& fy, float& sx, float& sy,
+                                           FeatAcc& fa) {
   const float2 pj = __ldg(&spos[j]);
   const float2 dqj = __ldg(&sdq[j]);
   const float2 vj = __ldg(&svel[j]);
@@ -367,6 +369,8 @@ __device__ __forceinline__ void pair_terms(uint32_t j, float2 pi, float2 vi, flo
     gxx = __fmul_rn(__fdiv_rn(dx, dist), sc);
     gyy = __fmul_rn(__fdiv_rn(dy, dist), sc);
   }
+  if constexpr (FEAT)
+    feat_pair(fa, gxx, gyy, poly6(d2, P), m_j, rho_j, q_i, dqj.y, __fsub_rn(vj.x, vi.x), __fsub_rn(vj.y, vi.y));
   float term = __fadd_rn(q_i, dqj.y);
   if ((P.flags & F_AV) && dist > kEps) {
     // Monaghan term (fluid.rs:302-317, called at :963-975)
@@ -403,70 +407,61 @@ __device__ __forceinline__ void pair_terms(uint32_t j, float2 pi, float2 vi, flo
   }
 }
 
-// The neighbour set comes from K5's row masks (bits in ascending slot order =
-// the reference's visit order); particles without masks walk the candidates.
-template <bool MASS, bool DEBUG, bool BATCH>
-__global__ void __launch_bounds__(256) k_force_integrate(
-    const float2* __restrict__ spos, const float2* __restrict__ svel, const float2* __restrict__ sdq,
-    const uint32_t* __restrict__ skey, const uint32_t* __restrict__ sid, const float* __restrict__ smass,
-    uint32_t n, const uint32_t* __restrict__ start, StepParams P0, BatchTab bt, const DevBody* __restrict__ bodies,
-    const uint64_t* __restrict__ nmask, float4* __restrict__ state_out, uint32_t* __restrict__ key_out,
-    uint32_t* __restrict__ count_out, float2* __restrict__ dbg_force) {
-  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= n) return;
-  const StepParams& P = scene_params<BATCH>(P0, bt.ptab, BATCH ? bt.sscene[s] : 0u);
-  const uint32_t k = skey[s];
-  const uint32_t id = sid[s];
-  const float2 pi = spos[s];
-  const float2 vi = svel[s];
-  const float2 dqi = sdq[s];
-  const float m_i = MASS ? smass[s] : P.mass;
-  const float rho_i = fmaxf(dqi.x, kEps);
-  const float q_i = dqi.y;  // p_i / (rho_i * rho_i)
-  float fx = 0.0f, fy = 0.0f, sx = 0.0f, sy = 0.0f;
+// Neighbour sums of sorted slot s: pressure force (fx, fy) and XSPH (sx, sy),
+// plus the closure aggregates when FEAT. The neighbour set comes from K5's
+// row masks (bits in ascending slot order = the reference's visit order);
+// particles without masks walk the candidates.
+template <bool MASS, bool FEAT>
+__device__ __forceinline__ void neighbour_sums(uint32_t s, uint32_t k, uint32_t n, float2 pi, float2 vi, float rho_i,
+                                               float q_i, float m_i, const float2* __restrict__ spos,
+                                               const float2* __restrict__ svel, const float2* __restrict__ sdq,
+                                               const float* __restrict__ smass, const uint32_t* __restrict__ start,
+                                               const uint64_t* __restrict__ nmask, const StepParams& P, float& fx,
+                                               float& fy, float& sx, float& sy, FeatAcc& fa) {
   const GridPlan& g = P.grid;
-  if (k != g.sentinel) {
-    const uint32_t local = k - g.base;
-    const uint32_t bx = local & g.maskw, by = local >> g.log2w;
-    const uint64_t own = nmask[n + s];
-    if (own != 0ull) {
-      // one loop over the three rows' set bits (ascending slots, row by row)
-      const uint32_t rs0 = __ldg(&start[g.base + (((by - 1u) & g.maskh) << g.log2w) + bx - 1]);
-      const uint32_t rs1 = __ldg(&start[g.base + ((by & g.maskh) << g.log2w) + bx - 1]);
-      const uint32_t rs2 = __ldg(&start[g.base + (((by + 1u) & g.maskh) << g.log2w) + bx - 1]);
-      const uint64_t m0 = nmask[s], m2 = nmask[2 * (size_t)n + s];
-      uint64_t cur = m0;
-      uint32_t row = 0, base = rs0;
-      for (;;) {
-        while (cur == 0ull && row < 2) {
-          row++;
-          cur = row == 1 ? own : m2;
-          base = row == 1 ? rs1 : rs2;
-        }
-        if (cur == 0ull) break;
-        const uint32_t j = base + (uint32_t)(__ffsll((long long)cur) - 1);
-        cur &= cur - 1ull;
-        if (j != s) pair_terms<MASS>(j, pi, vi, rho_i, q_i, m_i, spos, svel, sdq, smass, P, fx, fy, sx, sy);
+  if (k == g.sentinel) return;
+  const uint32_t local = k - g.base;
+  const uint32_t bx = local & g.maskw, by = local >> g.log2w;
+  const uint64_t own = nmask[n + s];
+  if (own != 0ull) {
+    // one loop over the three rows' set bits (ascending slots, row by row)
+    const uint32_t rs0 = __ldg(&start[g.base + (((by - 1u) & g.maskh) << g.log2w) + bx - 1]);
+    const uint32_t rs1 = __ldg(&start[g.base + ((by & g.maskh) << g.log2w) + bx - 1]);
+    const uint32_t rs2 = __ldg(&start[g.base + (((by + 1u) & g.maskh) << g.log2w) + bx - 1]);
+    const uint64_t m0 = nmask[s], m2 = nmask[2 * (size_t)n + s];
+    uint64_t cur = m0;
+    uint32_t row = 0, base = rs0;
+    for (;;) {
+      while (cur == 0ull && row < 2) {
+        row++;
+        cur = row == 1 ? own : m2;
+        base = row == 1 ? rs1 : rs2;
       }
-    } else {
-      for_each_candidate(k, start, g, [&](int jj) {
-        const uint32_t j = (uint32_t)jj;
-        const float2 pj = __ldg(&spos[j]);
-        const float ex = __fsub_rn(pj.x, pi.x);
-        const float ey = __fsub_rn(pj.y, pi.y);
-        const float d2 = __fadd_rn(__fmul_rn(ex, ex), __fmul_rn(ey, ey));
-        if (d2 < P.hg2 && j != s)
-          pair_terms<MASS>(j, pi, vi, rho_i, q_i, m_i, spos, svel, sdq, smass, P, fx, fy, sx, sy);
-      });
+      if (cur == 0ull) break;
+      const uint32_t j = base + (uint32_t)(__ffsll((long long)cur) - 1);
+      cur &= cur - 1ull;
+      if (j != s)
+        pair_terms<MASS, FEAT>(j, pi, vi, rho_i, q_i, m_i, spos, svel, sdq, smass, P, fx, fy, sx, sy, fa);
     }
+  } else {
+    for_each_candidate(k, start, g, [&](int jj) {
+      const uint32_t j = (uint32_t)jj;
+      const float2 pj = __ldg(&spos[j]);
+      const float ex = __fsub_rn(pj.x, pi.x);
+      const float ey = __fsub_rn(pj.y, pi.y);
+      const float d2 = __fadd_rn(__fmul_rn(ex, ex), __fmul_rn(ey, ey));
+      if (d2 < P.hg2 && j != s)
+        pair_terms<MASS, FEAT>(j, pi, vi, rho_i, q_i, m_i, spos, svel, sdq, smass, P, fx, fy, sx, sy, fa);
+    });
   }
-  if (DEBUG) {
-    dbg_force[id] = make_float2(fx, fy);
-    return;
-  }
-  // integrate (fluid.rs:1003-1050)
-  const float ax = __fadd_rn(P.gx, __fdiv_rn(fx, rho_i));
-  const float ay = __fadd_rn(P.gy, __fdiv_rn(fy, rho_i));
+}
+
+// integrate (fluid.rs:1003-1050) from acceleration (ax, ay) and the XSPH sum,
+// then the wall pass; writes the new state, the next key and its bucket count.
+__device__ __forceinline__ void integrate_write(uint32_t id, float2 pi, float2 vi, float ax, float ay, float sx,
+                                                float sy, const StepParams& P, const DevBody* __restrict__ bodies,
+                                                float4* __restrict__ state_out, uint32_t* __restrict__ key_out,
+                                                uint32_t* __restrict__ count_out) {
   float vx = __fadd_rn(vi.x, __fmul_rn(ax, P.dt));
   float vy = __fadd_rn(vi.y, __fmul_rn(ay, P.dt));
   if (P.flags & F_VISC) {
@@ -494,6 +489,151 @@ __global__ void __launch_bounds__(256) k_force_integrate(
   const uint32_t nk = bucket_key(x, y, P.grid);
   key_out[id] = nk;
   count_key(count_out, nk);  // bucket counts of the next substep's sort
+}
+
+template <bool MASS, bool DEBUG, bool BATCH>
+__global__ void __launch_bounds__(256) k_force_integrate(
+    const float2* __restrict__ spos, const float2* __restrict__ svel, const float2* __restrict__ sdq,
+    const uint32_t* __restrict__ skey, const uint32_t* __restrict__ sid, const float* __restrict__ smass,
+    uint32_t n, const uint32_t* __restrict__ start, StepParams P0, BatchTab bt, const DevBody* __restrict__ bodies,
+    const uint64_t* __restrict__ nmask, float4* __restrict__ state_out, uint32_t* __restrict__ key_out,
+    uint32_t* __restrict__ count_out, float2* __restrict__ dbg_force) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  const StepParams& P = scene_params<BATCH>(P0, bt.ptab, BATCH ? bt.sscene[s] : 0u);
+  const uint32_t k = skey[s];
+  const uint32_t id = sid[s];
+  const float2 pi = spos[s];
+  const float2 vi = svel[s];
+  const float2 dqi = sdq[s];
+  const float m_i = MASS ? smass[s] : P.mass;
+  const float rho_i = fmaxf(dqi.x, kEps);
+  const float q_i = dqi.y;  // p_i / (rho_i * rho_i)
+  float fx = 0.0f, fy = 0.0f, sx = 0.0f, sy = 0.0f;
+  FeatAcc fa;
+  neighbour_sums<MASS, false>(s, k, n, pi, vi, rho_i, q_i, m_i, spos, svel, sdq, smass, start, nmask, P, fx, fy, sx,
+                              sy, fa);
+  if (DEBUG) {
+    dbg_force[id] = make_float2(fx, fy);
+    return;
+  }
+  const float ax = __fadd_rn(P.gx, __fdiv_rn(fx, rho_i));
+  const float ay = __fadd_rn(P.gy, __fdiv_rn(fy, rho_i));
+  integrate_write(id, pi, vi, ax, ay, sx, sy, P, bodies, state_out, key_out, count_out);
+}
+
+// ---------------------------------------------------------------- closure force pass
+// The coarse step of the learned closure: the K6 neighbour pass also
+// accumulates the 16 closure features; each warp then runs the closure
+// network on its 32 particles on the tensor cores (two 16-row tiles) and the
+// integrate adds the predicted acceleration correction
+//   a_corr = y * out_scale * (h / dt^2)
+// (the network predicts the displacement correction over the coarse step in
+// units of h). It also keeps the pre-step state and density by id for the
+// fallback and the density-jump check.
+// FEATURES mode only writes the features (id order, 16 floats per particle)
+// for the coarse step P.dt and leaves the state untouched.
+constexpr int kModeFeatures = 1;
+constexpr int kModeClosure = 2;
+constexpr int kXRow = 24;  // BF16 elements per staged feature row (16 + pad)
+
+template <bool MASS, bool PHASE, bool BATCH, int MODE>
+__global__ void __launch_bounds__(256, 3) k_force_closure(
+    const float2* __restrict__ spos, const float2* __restrict__ svel, const float2* __restrict__ sdq,
+    const float* __restrict__ spres, const uint32_t* __restrict__ skey, const uint32_t* __restrict__ sid,
+    const float* __restrict__ smass, const uint8_t* __restrict__ sphase, uint32_t n,
+    const uint32_t* __restrict__ start, StepParams P0, BatchTab bt, const DevBody* __restrict__ bodies,
+    const uint64_t* __restrict__ nmask, MlpDev mlp, ClosureIO io, float4* __restrict__ state_out,
+    uint32_t* __restrict__ key_out, uint32_t* __restrict__ count_out) {
+  extern __shared__ __align__(16) unsigned char closure_smem[];
+  MlpSmem& sm = *reinterpret_cast<MlpSmem*>(closure_smem);
+  __nv_bfloat16* sx_all = reinterpret_cast<__nv_bfloat16*>(closure_smem + sizeof(MlpSmem));
+  float* sy_all = reinterpret_cast<float*>(closure_smem + sizeof(MlpSmem) + sizeof(__nv_bfloat16) * 256 * kXRow);
+  if constexpr (MODE == kModeClosure) {
+    mlp_load_smem(sm, mlp);
+    __syncthreads();
+  }
+  const uint32_t s0 = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool active = s0 < n;
+  if (MODE == kModeFeatures && !active) return;
+  const uint32_t s = active ? s0 : 0u;  // idle lanes of the last warp run the network on slot 0's data
+  const StepParams& P = scene_params<BATCH>(P0, bt.ptab, BATCH ? bt.sscene[s] : 0u);
+  const uint32_t k = skey[s];
+  const uint32_t id = sid[s];
+  const float2 pi = spos[s];
+  const float2 vi = svel[s];
+  const float2 dqi = sdq[s];
+  const float m_i = MASS ? smass[s] : P.mass;
+  const float rho_i = fmaxf(dqi.x, kEps);
+  const float q_i = dqi.y;
+  float fx = 0.0f, fy = 0.0f, sx = 0.0f, sy = 0.0f;
+  FeatAcc fa;
+  neighbour_sums<MASS, true>(s, k, n, pi, vi, rho_i, q_i, m_i, spos, svel, sdq, smass, start, nmask, P, fx, fy, sx,
+                             sy, fa);
+  const uint32_t ph = PHASE ? min((uint32_t)sphase[s], 3u) : P.uniform_phase;
+  float wd, wnx, wny;
+  wall_feature(pi.x, pi.y, bodies, P, wd, wnx, wny);
+  float f[kFeat];
+  feat_finish(fa, dqi.x, rho_i, spres[s], P.rest[ph], vi.x, vi.y, wd, wnx, wny, P, f);
+  if constexpr (MODE == kModeFeatures) {
+    float4* o = reinterpret_cast<float4*>(io.feat + (size_t)id * kFeat);
+#pragma unroll
+    for (int q = 0; q < 4; q++) o[q] = make_float4(f[4 * q], f[4 * q + 1], f[4 * q + 2], f[4 * q + 3]);
+    return;
+  } else {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    __nv_bfloat16* xs = sx_all + warp * 32 * kXRow;
+    float* ys = sy_all + warp * 64;
+    mlp_normalise_row(f, sm.norm, xs + lane * kXRow);
+    __syncwarp();
+#pragma unroll
+    for (int mt = 0; mt < 2; mt++) {
+      float y[4];
+      mlp_tile_forward(xs + mt * 16 * kXRow, kXRow, sm, lane, y);
+      if ((lane & 3) == 0) {
+        const int r = mt * 16 + (lane >> 2);
+        ys[2 * r] = y[0];
+        ys[2 * r + 1] = y[1];
+        ys[2 * (r + 8)] = y[2];
+        ys[2 * (r + 8) + 1] = y[3];
+      }
+    }
+    __syncwarp();
+    if (!active) return;
+    const float cx = __fmul_rn(__fmul_rn(ys[2 * lane], sm.norm[2 * kFeat]), io.acc_scale);
+    const float cy = __fmul_rn(__fmul_rn(ys[2 * lane + 1], sm.norm[2 * kFeat + 1]), io.acc_scale);
+    io.save[id] = make_float4(pi.x, pi.y, vi.x, vi.y);
+    io.rho_prev[id] = dqi.x;
+    const float ax = __fadd_rn(__fadd_rn(P.gx, __fdiv_rn(fx, rho_i)), cx);
+    const float ay = __fadd_rn(__fadd_rn(P.gy, __fdiv_rn(fy, rho_i)), cy);
+    integrate_write(id, pi, vi, ax, ay, sx, sy, P, bodies, state_out, key_out, count_out);
+  }
+}
+
+// Density check of an accepted-or-not coarse step, over the new sorted state
+// (after its density pass): criterion 0 = the largest per-particle density
+// increase over the step, max_i (rho'_i - rho_i) / rho0; criterion 1 = the
+// largest compression, max_i (rho'_i / rho0 - 1). Negative values count as 0;
+// a NaN counts as +inf. Result: float bits, atomicMax into *out (>= 0, so the
+// bit order is the value order and the maximum is order independent).
+template <bool PHASE, bool BATCH>
+__global__ void __launch_bounds__(256) k_closure_check(const float2* __restrict__ sdq, const uint32_t* __restrict__ sid,
+                                                       const uint8_t* __restrict__ sphase, uint32_t n, StepParams P0,
+                                                       BatchTab bt, const float* __restrict__ rho_prev,
+                                                       uint32_t criterion, unsigned int* __restrict__ out) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  float v = 0.0f;
+  if (s < n) {
+    const StepParams& P = scene_params<BATCH>(P0, bt.ptab, BATCH ? bt.sscene[s] : 0u);
+    const uint32_t ph = PHASE ? min((uint32_t)sphase[s], 3u) : P.uniform_phase;
+    const float r0 = fmaxf(P.rest[ph], kEps);
+    const float d = sdq[s].x;
+    const float j = criterion == 0 ? __fdiv_rn(__fsub_rn(d, rho_prev[sid[s]]), r0) : __fsub_rn(__fdiv_rn(d, r0), 1.0f);
+    v = (j != j) ? __int_as_float(0x7f800000) : fmaxf(j, 0.0f);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xFFFFFFFFu, v, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(v));
 }
 
 // ---------------------------------------------------------------- helpers
@@ -656,6 +796,60 @@ void enqueue_force_integrate(const FluidBufs& b, uint32_t n, const StepParams& P
     else PHIENG_FORCE(false, false, false);
   }
 #undef PHIENG_FORCE
+}
+
+size_t closure_smem_bytes() { return sizeof(MlpSmem) + sizeof(__nv_bfloat16) * 256 * kXRow + sizeof(float) * 256 * 2; }
+
+template <int MODE>
+void launch_closure(const FluidBufs& b, uint32_t n, const StepParams& P, const MlpDev& mlp, const ClosureIO& io,
+                    cudaStream_t st) {
+  const bool m = (P.flags & F_MASS) != 0, ph = (P.flags & F_PHASE) != 0, bat = b.batch.ptab != nullptr;
+  const uint32_t g = cdiv(n, 256);
+  const size_t sm = MODE == kModeClosure ? closure_smem_bytes() : 0;
+#define PHIENG_CLOSURE(M, PH, BT)                                                                                 \
+  k_force_closure<M, PH, BT, MODE><<<g, 256, sm, st>>>(b.spos, b.svel, b.sdq, b.spres, b.skey, b.sid, b.smass,   \
+                                                       b.sphase, n, b.start, P, b.batch, b.bodies, b.nmask, mlp, \
+                                                       io, b.state, b.key, b.count)
+  if (bat) {
+    if (m && ph) PHIENG_CLOSURE(true, true, true);
+    else if (m) PHIENG_CLOSURE(true, false, true);
+    else if (ph) PHIENG_CLOSURE(false, true, true);
+    else PHIENG_CLOSURE(false, false, true);
+  } else {
+    if (m && ph) PHIENG_CLOSURE(true, true, false);
+    else if (m) PHIENG_CLOSURE(true, false, false);
+    else if (ph) PHIENG_CLOSURE(false, true, false);
+    else PHIENG_CLOSURE(false, false, false);
+  }
+#undef PHIENG_CLOSURE
+}
+
+void enqueue_closure_features(const FluidBufs& b, uint32_t n, const StepParams& P, float* feat, cudaStream_t st) {
+  if (n == 0) return;
+  ClosureIO io;
+  io.feat = feat;
+  launch_closure<kModeFeatures>(b, n, P, MlpDev{}, io, st);
+}
+
+void enqueue_closure_force(const FluidBufs& b, uint32_t n, const StepParams& P, const MlpDev& mlp,
+                           const ClosureIO& io, cudaStream_t st) {
+  if (n == 0) return;
+  launch_closure<kModeClosure>(b, n, P, mlp, io, st);
+}
+
+void enqueue_closure_check(const FluidBufs& b, uint32_t n, const StepParams& P, const float* rho_prev,
+                           uint32_t criterion, unsigned int* out, cudaStream_t st) {
+  cudaMemsetAsync(out, 0, sizeof(unsigned int), st);
+  if (n == 0) return;
+  const bool ph = (P.flags & F_PHASE) != 0, bat = b.batch.ptab != nullptr;
+  const uint32_t g = cdiv(n, 256);
+  if (bat) {
+    if (ph) k_closure_check<true, true><<<g, 256, 0, st>>>(b.sdq, b.sid, b.sphase, n, P, b.batch, rho_prev, criterion, out);
+    else k_closure_check<false, true><<<g, 256, 0, st>>>(b.sdq, b.sid, b.sphase, n, P, b.batch, rho_prev, criterion, out);
+  } else {
+    if (ph) k_closure_check<true, false><<<g, 256, 0, st>>>(b.sdq, b.sid, b.sphase, n, P, b.batch, rho_prev, criterion, out);
+    else k_closure_check<false, false><<<g, 256, 0, st>>>(b.sdq, b.sid, b.sphase, n, P, b.batch, rho_prev, criterion, out);
+  }
 }
 
 void enqueue_unsort_dp(const FluidBufs& b, uint32_t n, float* dens, float* pres, cudaStream_t st) {

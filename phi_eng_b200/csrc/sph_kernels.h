@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include "sph_device.cuh"
+#include "sph_mlp.cuh"
 
 namespace phieng {
 
@@ -71,6 +72,32 @@ void enqueue_density(const FluidBufs& b, uint32_t n, const StepParams& P, cudaSt
 // order) and leaves the state untouched.
 void enqueue_force_integrate(const FluidBufs& b, uint32_t n, const StepParams& P, float2* dbg_force,
                              cudaStream_t st);
+
+// Closure pass buffers: features (id order, 16 per particle) for the
+// features mode; pre-step state and density (id order) kept by the closure
+// step; acc_scale = h / dt^2 turns the network output into an acceleration.
+struct ClosureIO {
+  float* feat = nullptr;
+  float4* save = nullptr;
+  float* rho_prev = nullptr;
+  float acc_scale = 0.0f;
+};
+
+// Closure features of every particle for a coarse step of P.dt (after the
+// sort and density of the current state); state untouched.
+void enqueue_closure_features(const FluidBufs& b, uint32_t n, const StepParams& P, float* feat, cudaStream_t st);
+
+// Coarse step with the closure network: K6 + features + network + corrected
+// integrate. Writes the new state, next keys and counts like K6, plus the
+// pre-step state (io.save) and density (io.rho_prev).
+void enqueue_closure_force(const FluidBufs& b, uint32_t n, const StepParams& P, const MlpDev& mlp,
+                           const ClosureIO& io, cudaStream_t st);
+
+// Density check after the coarse step's new state was sorted and its density
+// computed (criterion 0: largest increase over the step; 1: largest
+// compression), as float bits into *out (zeroed first).
+void enqueue_closure_check(const FluidBufs& b, uint32_t n, const StepParams& P, const float* rho_prev,
+                           uint32_t criterion, unsigned int* out, cudaStream_t st);
 
 // Scatter the sorted density / pressure back to id order.
 void enqueue_unsort_dp(const FluidBufs& b, uint32_t n, float* dens, float* pres, cudaStream_t st);

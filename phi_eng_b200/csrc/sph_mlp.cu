@@ -1,0 +1,774 @@
+// Closure network: parameters on the device, the standalone forward pass,
+// and training (forward + backward + Adam) with hand-written kernels.
+//
+// Training step for a minibatch of B samples drawn from (features, target)
+// pairs, loss L = 1/(2B) sum_b |y_b - t_b / out_scale|^2:
+//   k_mlp_train_tile  each CTA takes B / gridDim samples in rounds of 128:
+//                     every warp runs forward and backward for 32 samples on
+//                     the tensor cores (activations stay in registers or
+//                     shared memory), then the CTA forms its partial weight
+//                     gradients dW2 = dZ2^T H1 and dW1 = dZ1^T X with the
+//                     sample dimension as K (tensor cores), dW3 and the bias
+//                     gradients in FP32; one partial vector per CTA.
+//   k_mlp_adam        per parameter: sum of the CTA partials in CTA order,
+//                     Adam, new FP32 master and its BF16 fragment images.
+//   k_mlp_advance     step counter + 1.
+// No float atomics anywhere: a run is bit-reproducible.
+//
+// Minibatch sample k of step t is pair
+//   idx = (mix64(seed ^ (t << 32) ^ k) >> 32) * npairs >> 32
+// with mix64 the SplitMix64 finaliser (Steele, Lea, Flood 2014).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "phieng_sph.h"
+#include "sph_mlp.cuh"
+#include "sph_mlp_host.h"
+
+namespace phieng {
+namespace {
+
+constexpr int kTrainThreads = 128;
+constexpr int kTileRows = 128;  // samples per CTA round
+constexpr int kXR = 24;         // staged feature row stride (BF16)
+constexpr int kLdT = kTileRows + 8;
+constexpr int kPartStride = 5384;  // kParams gradient entries, then the loss
+constexpr float kBeta1 = 0.9f, kBeta2 = 0.999f, kAdamEps = 1e-8f;
+
+__host__ __device__ inline uint64_t mix64(uint64_t z) {
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+__host__ __device__ inline uint32_t sample_index(uint64_t seed, uint32_t iter, uint32_t k, uint32_t npairs) {
+  const uint64_t h = mix64(seed ^ ((uint64_t)iter << 32) ^ (uint64_t)k);
+  return (uint32_t)(((h >> 32) * (uint64_t)npairs) >> 32);
+}
+
+struct TrainSmem {
+  uint2 f1[kF1];
+  uint2 f2[kF2];
+  uint2 f3[kF3];
+  uint2 f2t[kF2T];
+  float bias[kBias];
+  float w3[kOut * kHidden];
+  float norm[kNorm];
+  float tgt[kTileRows][2];
+  float dy[kTileRows][2];
+  float db[4][2 * kHidden];            // per-warp bias-gradient sums (b1 | b2)
+  alignas(16) float z1[4][2][8][32][4];  // per warp: layer-1 pre-activations in C-fragment order
+  __nv_bfloat16 xs[kTileRows][kXR];    // x_hat, row major
+  __nv_bfloat16 xt[kFeat][kLdT];       // x_hat^T
+  __nv_bfloat16 h1t[kHidden][kLdT];    // H1^T
+  __nv_bfloat16 h2t[kHidden][kLdT];    // H2^T
+  __nv_bfloat16 dz2t[kHidden][kLdT];   // dZ2^T
+  __nv_bfloat16 dz1t[kHidden][kLdT];   // dZ1^T
+};
+
+// Weight p of the flat parameter vector into the BF16 fragment images, the
+// FP32 bias array and the BF16-rounded W3 copy.
+__device__ __forceinline__ void write_weight(int p, float w, __nv_bfloat16* img, float* bias, float* w3) {
+  const __nv_bfloat16 b = __float2bfloat16_rn(w);
+  if (p < kOffB1) {
+    const int n = p / kFeat, k = p % kFeat;
+    img[frag_pos(k, n, 8)] = b;
+  } else if (p < kOffW2) {
+    bias[p - kOffB1] = w;
+  } else if (p < kOffB2) {
+    const int q = p - kOffW2, o = q / kHidden, i = q % kHidden;
+    img[4 * kF1 + frag_pos(i, o, 8)] = b;
+    img[4 * (kF1 + kF2 + kF3) + frag_pos(o, i, 8)] = b;
+  } else if (p < kOffW3) {
+    bias[kHidden + (p - kOffB2)] = w;
+  } else if (p < kOffB3) {
+    const int q = p - kOffW3, o = q / kHidden, n = q % kHidden;
+    img[4 * (kF1 + kF2) + frag_pos(n, o, 1)] = b;
+    w3[q] = __bfloat162float(b);
+  } else {
+    bias[2 * kHidden + (p - kOffB3)] = w;
+  }
+}
+
+__global__ void k_mlp_sync(const float* __restrict__ w, uint2* frag, float* bias, float* w3) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < kParams) write_weight(p, w[p], reinterpret_cast<__nv_bfloat16*>(frag), bias, w3);
+}
+
+__global__ void __launch_bounds__(128) k_mlp_forward(const float* __restrict__ x, uint32_t n, MlpDev mlp,
+                                                     float* __restrict__ y) {
+  __shared__ MlpSmem sm;
+  __shared__ __align__(16) __nv_bfloat16 xs[128 * kXR];
+  __shared__ float ys[128 * 2];
+  mlp_load_smem(sm, mlp);
+  __syncthreads();
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  for (uint32_t base = blockIdx.x * 128u; base < n; base += gridDim.x * 128u) {
+    const uint32_t i = base + tid;
+    float f[kFeat];
+    if (i < n) {
+      const float4* xi = reinterpret_cast<const float4*>(x + (size_t)i * kFeat);
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const float4 v = xi[q];
+        f[4 * q] = v.x;
+        f[4 * q + 1] = v.y;
+        f[4 * q + 2] = v.z;
+        f[4 * q + 3] = v.w;
+      }
+    } else {
+#pragma unroll
+      for (int q = 0; q < kFeat; q++) f[q] = sm.norm[q];  // normalises to zero
+    }
+    mlp_normalise_row(f, sm.norm, xs + tid * kXR);
+    __syncwarp();
+#pragma unroll
+    for (int mt = 0; mt < 2; mt++) {
+      float v[4];
+      mlp_tile_forward(xs + (warp * 32 + mt * 16) * kXR, kXR, sm, lane, v);
+      if ((lane & 3) == 0) {
+        const int r = warp * 32 + mt * 16 + (lane >> 2);
+        ys[2 * r] = v[0];
+        ys[2 * r + 1] = v[1];
+        ys[2 * (r + 8)] = v[2];
+        ys[2 * (r + 8) + 1] = v[3];
+      }
+    }
+    __syncwarp();
+    if (i < n) {
+      y[2 * (size_t)i] = __fmul_rn(ys[2 * tid], sm.norm[2 * kFeat]);
+      y[2 * (size_t)i + 1] = __fmul_rn(ys[2 * tid + 1], sm.norm[2 * kFeat + 1]);
+    }
+    __syncwarp();
+  }
+}
+
+__device__ __forceinline__ void store_bf16(__nv_bfloat16* p, float v) { *p = __float2bfloat16_rn(v); }
+
+// Sum over the 8 row groups of a warp (lanes with equal lane % 4), fixed order.
+__device__ __forceinline__ float group_sum(float v) {
+  v = __fadd_rn(v, __shfl_xor_sync(0xFFFFFFFFu, v, 4));
+  v = __fadd_rn(v, __shfl_xor_sync(0xFFFFFFFFu, v, 8));
+  v = __fadd_rn(v, __shfl_xor_sync(0xFFFFFFFFu, v, 16));
+  return v;
+}
+
+__global__ void __launch_bounds__(kTrainThreads, 1)
+    k_mlp_train_tile(const float* __restrict__ x, const float* __restrict__ tg, uint32_t npairs, uint32_t batch,
+                     uint32_t rounds, uint64_t seed, const uint32_t* __restrict__ iter_ptr, MlpDev mlp,
+                     float* __restrict__ part) {
+  extern __shared__ __align__(16) unsigned char train_smem[];
+  TrainSmem& S = *reinterpret_cast<TrainSmem*>(train_smem);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, g = lane >> 2, t = lane & 3;
+  for (int i = tid; i < kFragAll; i += kTrainThreads) {
+    const uint2 v = mlp.frag[i];
+    if (i < kF1)
+      S.f1[i] = v;
+    else if (i < kF1 + kF2)
+      S.f2[i - kF1] = v;
+    else if (i < kF1 + kF2 + kF3)
+      S.f3[i - kF1 - kF2] = v;
+    else
+      S.f2t[i - kF1 - kF2 - kF3] = v;
+  }
+  for (int i = tid; i < kBias; i += kTrainThreads) S.bias[i] = mlp.bias[i];
+  for (int i = tid; i < kOut * kHidden; i += kTrainThreads) S.w3[i] = mlp.w3[i];
+  for (int i = tid; i < kNorm; i += kTrainThreads) S.norm[i] = mlp.norm[i];
+  for (int i = tid; i < 4 * 2 * kHidden; i += kTrainThreads) (&S.db[0][0])[i] = 0.0f;
+  const uint32_t iter = *iter_ptr;
+  const float inv_b = __fdiv_rn(1.0f, (float)batch);
+  __syncthreads();
+  const float inv_os0 = __fdiv_rn(1.0f, S.norm[2 * kFeat]), inv_os1 = __fdiv_rn(1.0f, S.norm[2 * kFeat + 1]);
+
+  float acc_w2[8][4], acc_w1[2][4];
+#pragma unroll
+  for (int a = 0; a < 8; a++)
+#pragma unroll
+    for (int c = 0; c < 4; c++) acc_w2[a][c] = 0.0f;
+#pragma unroll
+  for (int a = 0; a < 2; a++)
+#pragma unroll
+    for (int c = 0; c < 4; c++) acc_w1[a][c] = 0.0f;
+  float acc_w3 = 0.0f, acc_b3 = 0.0f, loss = 0.0f;
+
+  for (uint32_t r = 0; r < rounds; r++) {
+    // ---- gather 128 samples: row = warp * 32 + lane
+    {
+      const int row = tid;
+      const uint32_t k = (blockIdx.x * rounds + r) * kTileRows + (uint32_t)row;
+      const uint32_t idx = sample_index(seed, iter, k, npairs);
+      const float4* xi = reinterpret_cast<const float4*>(x + (size_t)idx * kFeat);
+      float f[kFeat];
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const float4 v = xi[q];
+        f[4 * q] = v.x;
+        f[4 * q + 1] = v.y;
+        f[4 * q + 2] = v.z;
+        f[4 * q + 3] = v.w;
+      }
+      mlp_normalise_row(f, S.norm, &S.xs[row][0]);
+#pragma unroll
+      for (int q = 0; q < kFeat; q++) S.xt[q][row] = S.xs[row][q];
+      S.tgt[row][0] = __fmul_rn(tg[2 * (size_t)idx], inv_os0);
+      S.tgt[row][1] = __fmul_rn(tg[2 * (size_t)idx + 1], inv_os1);
+    }
+    __syncwarp();
+    // ---- forward + backward, two 16-row tiles per warp
+#pragma unroll 1
+    for (int mt = 0; mt < 2; mt++) {
+      const int r0 = warp * 32 + mt * 16;
+      const int ra = r0 + g, rb = r0 + g + 8;
+      uint32_t a[4];
+      a[0] = lds32(&S.xs[ra][2 * t]);
+      a[1] = lds32(&S.xs[rb][2 * t]);
+      a[2] = lds32(&S.xs[ra][2 * t + 8]);
+      a[3] = lds32(&S.xs[rb][2 * t + 8]);
+      uint32_t h[4][4];
+#pragma unroll
+      for (int nt = 0; nt < 8; nt++) {
+        float c[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+        const uint2 b = S.f1[nt * 32 + lane];
+        mma_bf16(c, a, b.x, b.y);
+        const int c0 = nt * 8 + 2 * t;
+        const float z0 = __fadd_rn(c[0], S.bias[c0]), z1 = __fadd_rn(c[1], S.bias[c0 + 1]);
+        const float z2 = __fadd_rn(c[2], S.bias[c0]), z3 = __fadd_rn(c[3], S.bias[c0 + 1]);
+        *reinterpret_cast<float4*>(&S.z1[warp][mt][nt][lane][0]) = make_float4(z0, z1, z2, z3);
+        const float s0 = silu_hw(z0), s1 = silu_hw(z1), s2 = silu_hw(z2), s3 = silu_hw(z3);
+        h[nt >> 1][(nt & 1) * 2 + 0] = pack_bf16(s0, s1);
+        h[nt >> 1][(nt & 1) * 2 + 1] = pack_bf16(s2, s3);
+        store_bf16(&S.h1t[c0][ra], s0);
+        store_bf16(&S.h1t[c0 + 1][ra], s1);
+        store_bf16(&S.h1t[c0][rb], s2);
+        store_bf16(&S.h1t[c0 + 1][rb], s3);
+      }
+      float z2v[8][4];
+      uint32_t h2[4][4];
+#pragma unroll
+      for (int nt = 0; nt < 8; nt++) {
+        float c[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll
+        for (int kt = 0; kt < 4; kt++) {
+          const uint2 b = S.f2[(kt * 8 + nt) * 32 + lane];
+          mma_bf16(c, h[kt], b.x, b.y);
+        }
+        const int c0 = nt * 8 + 2 * t;
+        z2v[nt][0] = __fadd_rn(c[0], S.bias[kHidden + c0]);
+        z2v[nt][1] = __fadd_rn(c[1], S.bias[kHidden + c0 + 1]);
+        z2v[nt][2] = __fadd_rn(c[2], S.bias[kHidden + c0]);
+        z2v[nt][3] = __fadd_rn(c[3], S.bias[kHidden + c0 + 1]);
+        const float s0 = silu_hw(z2v[nt][0]), s1 = silu_hw(z2v[nt][1]);
+        const float s2 = silu_hw(z2v[nt][2]), s3 = silu_hw(z2v[nt][3]);
+        h2[nt >> 1][(nt & 1) * 2 + 0] = pack_bf16(s0, s1);
+        h2[nt >> 1][(nt & 1) * 2 + 1] = pack_bf16(s2, s3);
+        store_bf16(&S.h2t[c0][ra], s0);
+        store_bf16(&S.h2t[c0 + 1][ra], s1);
+        store_bf16(&S.h2t[c0][rb], s2);
+        store_bf16(&S.h2t[c0 + 1][rb], s3);
+      }
+      float c3[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll
+      for (int kt = 0; kt < 4; kt++) {
+        const uint2 b = S.f3[kt * 32 + lane];
+        mma_bf16(c3, h2[kt], b.x, b.y);
+      }
+      // loss and dY on the lanes holding output columns 0 and 1
+      float dyl[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+      if (t == 0) {
+        const float e0 = __fsub_rn(__fadd_rn(c3[0], S.bias[2 * kHidden]), S.tgt[ra][0]);
+        const float e1 = __fsub_rn(__fadd_rn(c3[1], S.bias[2 * kHidden + 1]), S.tgt[ra][1]);
+        const float e2 = __fsub_rn(__fadd_rn(c3[2], S.bias[2 * kHidden]), S.tgt[rb][0]);
+        const float e3 = __fsub_rn(__fadd_rn(c3[3], S.bias[2 * kHidden + 1]), S.tgt[rb][1]);
+        loss = __fadd_rn(loss, __fadd_rn(__fadd_rn(__fmul_rn(e0, e0), __fmul_rn(e1, e1)),
+                                         __fadd_rn(__fmul_rn(e2, e2), __fmul_rn(e3, e3))));
+        dyl[0] = __fmul_rn(e0, inv_b);
+        dyl[1] = __fmul_rn(e1, inv_b);
+        dyl[2] = __fmul_rn(e2, inv_b);
+        dyl[3] = __fmul_rn(e3, inv_b);
+        S.dy[ra][0] = dyl[0];
+        S.dy[ra][1] = dyl[1];
+        S.dy[rb][0] = dyl[2];
+        S.dy[rb][1] = dyl[3];
+      }
+#pragma unroll
+      for (int q = 0; q < 4; q++) dyl[q] = __shfl_sync(0xFFFFFFFFu, dyl[q], lane & ~3);
+      // dZ2 = (dY W3) * silu'(Z2)
+      uint32_t da[4][4];
+#pragma unroll
+      for (int nt = 0; nt < 8; nt++) {
+        const int c0 = nt * 8 + 2 * t;
+        const float w00 = S.w3[c0], w01 = S.w3[c0 + 1], w10 = S.w3[kHidden + c0], w11 = S.w3[kHidden + c0 + 1];
+        const float d0 = __fmul_rn(__fadd_rn(__fmul_rn(dyl[0], w00), __fmul_rn(dyl[1], w10)), dsilu_hw(z2v[nt][0]));
+        const float d1 = __fmul_rn(__fadd_rn(__fmul_rn(dyl[0], w01), __fmul_rn(dyl[1], w11)), dsilu_hw(z2v[nt][1]));
+        const float d2 = __fmul_rn(__fadd_rn(__fmul_rn(dyl[2], w00), __fmul_rn(dyl[3], w10)), dsilu_hw(z2v[nt][2]));
+        const float d3 = __fmul_rn(__fadd_rn(__fmul_rn(dyl[2], w01), __fmul_rn(dyl[3], w11)), dsilu_hw(z2v[nt][3]));
+        da[nt >> 1][(nt & 1) * 2 + 0] = pack_bf16(d0, d1);
+        da[nt >> 1][(nt & 1) * 2 + 1] = pack_bf16(d2, d3);
+        store_bf16(&S.dz2t[c0][ra], d0);
+        store_bf16(&S.dz2t[c0 + 1][ra], d1);
+        store_bf16(&S.dz2t[c0][rb], d2);
+        store_bf16(&S.dz2t[c0 + 1][rb], d3);
+        const float cs0 = group_sum(__fadd_rn(d0, d2)), cs1 = group_sum(__fadd_rn(d1, d3));
+        if (g == 0) {
+          S.db[warp][kHidden + c0] = __fadd_rn(S.db[warp][kHidden + c0], cs0);
+          S.db[warp][kHidden + c0 + 1] = __fadd_rn(S.db[warp][kHidden + c0 + 1], cs1);
+        }
+      }
+      // dH1 = dZ2 W2, dZ1 = dH1 * silu'(Z1)
+#pragma unroll
+      for (int nt = 0; nt < 8; nt++) {
+        float c[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll
+        for (int kt = 0; kt < 4; kt++) {
+          const uint2 b = S.f2t[(kt * 8 + nt) * 32 + lane];
+          mma_bf16(c, da[kt], b.x, b.y);
+        }
+        const float4 z = *reinterpret_cast<const float4*>(&S.z1[warp][mt][nt][lane][0]);
+        const float d0 = __fmul_rn(c[0], dsilu_hw(z.x)), d1 = __fmul_rn(c[1], dsilu_hw(z.y));
+        const float d2 = __fmul_rn(c[2], dsilu_hw(z.z)), d3 = __fmul_rn(c[3], dsilu_hw(z.w));
+        const int c0 = nt * 8 + 2 * t;
+        store_bf16(&S.dz1t[c0][ra], d0);
+        store_bf16(&S.dz1t[c0 + 1][ra], d1);
+        store_bf16(&S.dz1t[c0][rb], d2);
+        store_bf16(&S.dz1t[c0 + 1][rb], d3);
+        const float cs0 = group_sum(__fadd_rn(d0, d2)), cs1 = group_sum(__fadd_rn(d1, d3));
+        if (g == 0) {
+          S.db[warp][c0] = __fadd_rn(S.db[warp][c0], cs0);
+          S.db[warp][c0 + 1] = __fadd_rn(S.db[warp][c0 + 1], cs1);
+        }
+      }
+    }
+    __syncthreads();
+    // ---- CTA weight gradients over the 128 samples of this round
+    // warp w owns rows [16w, 16w + 16) of dW2 (layer-2 outputs) and of dW1
+#pragma unroll 1
+    for (int kt = 0; kt < kTileRows / 16; kt++) {
+      const int kc = kt * 16 + 2 * t;
+      uint32_t a[4];
+      a[0] = lds32(&S.dz2t[16 * warp + g][kc]);
+      a[1] = lds32(&S.dz2t[16 * warp + g + 8][kc]);
+      a[2] = lds32(&S.dz2t[16 * warp + g][kc + 8]);
+      a[3] = lds32(&S.dz2t[16 * warp + g + 8][kc + 8]);
+#pragma unroll
+      for (int nt = 0; nt < 8; nt++)
+        mma_bf16(acc_w2[nt], a, lds32(&S.h1t[nt * 8 + g][kc]), lds32(&S.h1t[nt * 8 + g][kc + 8]));
+      a[0] = lds32(&S.dz1t[16 * warp + g][kc]);
+      a[1] = lds32(&S.dz1t[16 * warp + g + 8][kc]);
+      a[2] = lds32(&S.dz1t[16 * warp + g][kc + 8]);
+      a[3] = lds32(&S.dz1t[16 * warp + g + 8][kc + 8]);
+#pragma unroll
+      for (int nt = 0; nt < 2; nt++)
+        mma_bf16(acc_w1[nt], a, lds32(&S.xt[nt * 8 + g][kc]), lds32(&S.xt[nt * 8 + g][kc + 8]));
+    }
+    {
+      // dW3[o][n] = sum_k dY[k][o] H2[k][n] and db3 (FP32, sample order)
+      const int o = tid >> 6, n = tid & 63;
+      for (int kk = 0; kk < kTileRows; kk++)
+        acc_w3 = __fadd_rn(acc_w3, __fmul_rn(S.dy[kk][o], __bfloat162float(S.h2t[n][kk])));
+      if (tid < kOut)
+        for (int kk = 0; kk < kTileRows; kk++) acc_b3 = __fadd_rn(acc_b3, S.dy[kk][tid]);
+    }
+    __syncthreads();
+  }
+
+  // ---- this CTA's partial gradient
+  float* P = part + (size_t)blockIdx.x * kPartStride;
+#pragma unroll
+  for (int nt = 0; nt < 8; nt++) {
+    const int i = nt * 8 + 2 * t, oa = 16 * warp + g, ob = oa + 8;
+    P[kOffW2 + oa * kHidden + i] = acc_w2[nt][0];
+    P[kOffW2 + oa * kHidden + i + 1] = acc_w2[nt][1];
+    P[kOffW2 + ob * kHidden + i] = acc_w2[nt][2];
+    P[kOffW2 + ob * kHidden + i + 1] = acc_w2[nt][3];
+  }
+#pragma unroll
+  for (int nt = 0; nt < 2; nt++) {
+    const int k = nt * 8 + 2 * t, na = 16 * warp + g, nb = na + 8;
+    P[kOffW1 + na * kFeat + k] = acc_w1[nt][0];
+    P[kOffW1 + na * kFeat + k + 1] = acc_w1[nt][1];
+    P[kOffW1 + nb * kFeat + k] = acc_w1[nt][2];
+    P[kOffW1 + nb * kFeat + k + 1] = acc_w1[nt][3];
+  }
+  P[kOffW3 + tid] = acc_w3;
+  if (tid < kOut) P[kOffB3 + tid] = acc_b3;
+  {
+    const float s = __fadd_rn(__fadd_rn(S.db[0][tid], S.db[1][tid]), __fadd_rn(S.db[2][tid], S.db[3][tid]));
+    if (tid < kHidden)
+      P[kOffB1 + tid] = s;
+    else
+      P[kOffB2 + tid - kHidden] = s;
+  }
+  // loss: fixed-order tree within each warp, then warps in order
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) loss = __fadd_rn(loss, __shfl_xor_sync(0xFFFFFFFFu, loss, o));
+  __shared__ float wl[4];
+  if (lane == 0) wl[warp] = loss;
+  __syncthreads();
+  if (tid == 0) P[kParams] = __fadd_rn(__fadd_rn(wl[0], wl[1]), __fadd_rn(wl[2], wl[3]));
+}
+
+// Sum of the CTA partials (CTA order) per parameter.
+__device__ __forceinline__ float sum_parts(const float* __restrict__ part, uint32_t nparts, int p) {
+  float g = 0.0f;
+  for (uint32_t c = 0; c < nparts; c++) g = __fadd_rn(g, part[(size_t)c * kPartStride + p]);
+  return g;
+}
+
+__global__ void k_mlp_reduce(const float* __restrict__ part, uint32_t nparts, float inv_2b, float* __restrict__ grad,
+                             float* __restrict__ loss) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < kParams) grad[p] = sum_parts(part, nparts, p);
+  if (p == kParams) *loss = __fmul_rn(sum_parts(part, nparts, kParams), inv_2b);
+}
+
+// Adam (Kingma & Ba 2015) on step t = ctr[0] + 1:
+//   m = b1 m + (1 - b1) g,  v = b2 v + (1 - b2) g^2,
+//   w -= lr * (m / (1 - b1^t)) / (sqrt(v / (1 - b2^t)) + eps)
+__global__ void k_mlp_adam(const float* __restrict__ part, uint32_t nparts, float* __restrict__ w, float* __restrict__ m,
+                           float* __restrict__ v, const uint32_t* __restrict__ ctr, float lr, float inv_2b,
+                           float* __restrict__ loss_hist, uint32_t loss_base, uint32_t loss_cap, uint2* frag,
+                           float* bias, float* w3) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t t0 = ctr[0];
+  if (p == kParams) {
+    if (loss_hist && t0 >= loss_base && t0 - loss_base < loss_cap)
+      loss_hist[t0 - loss_base] = __fmul_rn(sum_parts(part, nparts, kParams), inv_2b);
+    return;
+  }
+  if (p > kParams) return;
+  const float g = sum_parts(part, nparts, p);
+  const double tt = (double)t0 + 1.0;
+  const float bc1 = (float)(1.0 - pow((double)kBeta1, tt));
+  const float bc2 = (float)(1.0 - pow((double)kBeta2, tt));
+  const float mm = __fadd_rn(__fmul_rn(kBeta1, m[p]), __fmul_rn(__fsub_rn(1.0f, kBeta1), g));
+  const float vv = __fadd_rn(__fmul_rn(kBeta2, v[p]), __fmul_rn(__fsub_rn(1.0f, kBeta2), __fmul_rn(g, g)));
+  const float upd = __fdiv_rn(__fdiv_rn(mm, bc1), __fadd_rn(__fsqrt_rn(__fdiv_rn(vv, bc2)), kAdamEps));
+  const float ww = __fsub_rn(w[p], __fmul_rn(lr, upd));
+  m[p] = mm;
+  v[p] = vv;
+  w[p] = ww;
+  write_weight(p, ww, reinterpret_cast<__nv_bfloat16*>(frag), bias, w3);
+}
+
+__global__ void k_mlp_advance(uint32_t* ctr) { ctr[0] += 1u; }
+
+__global__ void k_mlp_indices(uint64_t seed, uint32_t iter, uint32_t batch, uint32_t npairs, uint32_t* out) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < batch) out[k] = sample_index(seed, iter, k, npairs);
+}
+
+__global__ void k_mlp_targets(const float4* __restrict__ fine, const float4* __restrict__ coarse, uint32_t n,
+                              float inv_h, float2* __restrict__ out) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float4 a = fine[i], b = coarse[i];
+  out[i] = make_float2(__fmul_rn(__fsub_rn(a.x, b.x), inv_h), __fmul_rn(__fsub_rn(a.y, b.y), inv_h));
+}
+
+inline uint32_t cdiv(uint32_t a, uint32_t b) { return (a + b - 1) / b; }
+
+}  // namespace
+
+// CTAs and rounds per CTA for a training batch (batch % 128 == 0): rounds
+// grow until the grid is at most two CTAs per SM.
+void mlp_grid(uint32_t batch, uint32_t* ctas, uint32_t* rounds) {
+  uint32_t tiles = batch / kTileRows, r = 1;
+  while (tiles / r > 296u && (tiles % (2 * r)) == 0) r *= 2;
+  *ctas = tiles / r;
+  *rounds = r;
+}
+
+}  // namespace phieng
+
+using namespace phieng;
+
+struct PhiengMlp {
+  int device = -1;
+  cudaStream_t stream = nullptr;
+  cudaStream_t own_stream = nullptr;
+  int32_t error = PHIENG_SPH_OK;
+  float* w = nullptr;
+  float* m = nullptr;
+  float* v = nullptr;
+  uint2* frag = nullptr;
+  float* bias = nullptr;
+  float* w3 = nullptr;
+  float* norm = nullptr;
+  uint32_t* ctr = nullptr;  // [0] Adam step, [1] iteration for a gradient check
+  float* part = nullptr;
+  uint32_t part_cap = 0;
+  float* grad = nullptr;    // kParams + 1 (loss)
+  float* loss_hist = nullptr;
+  uint32_t loss_cap = 0;
+  float* h_pinned = nullptr;
+};
+
+namespace {
+
+bool mlp_ok(PhiengMlp* m, cudaError_t r) {
+  if (r == cudaSuccess) return true;
+  if (m->error == PHIENG_SPH_OK) m->error = PHIENG_SPH_E_CUDA;
+  return false;
+}
+
+template <class T>
+bool mlp_alloc(PhiengMlp* m, T*& p, size_t count) {
+  return mlp_ok(m, cudaMalloc(reinterpret_cast<void**>(&p), sizeof(T) * count));
+}
+
+bool ensure_parts(PhiengMlp* m, uint32_t nparts) {
+  if (m->part_cap >= nparts) return true;
+  if (m->part) cudaFree(m->part);
+  m->part = nullptr;
+  m->part_cap = 0;
+  if (!mlp_alloc(m, m->part, (size_t)nparts * kPartStride)) return false;
+  m->part_cap = nparts;
+  return true;
+}
+
+bool sync_images(PhiengMlp* m) {
+  k_mlp_sync<<<cdiv(kParams, 256), 256, 0, m->stream>>>(m->w, m->frag, m->bias, m->w3);
+  return mlp_ok(m, cudaGetLastError());
+}
+
+bool check_pairs(const float* x, const float* t, uint32_t npairs, uint32_t batch) {
+  return x && t && npairs > 0 && batch > 0 && batch % kTileRows == 0;
+}
+
+bool launch_tile(PhiengMlp* m, const float* x, const float* t, uint32_t npairs, uint32_t batch, uint64_t seed,
+                 const uint32_t* iter_ptr, uint32_t* nparts_out) {
+  uint32_t ctas, rounds;
+  mlp_grid(batch, &ctas, &rounds);
+  if (!ensure_parts(m, ctas)) return false;
+  MlpDev d = phieng_mlp_dev(m);
+  k_mlp_train_tile<<<ctas, kTrainThreads, sizeof(TrainSmem), m->stream>>>(x, t, npairs, batch, rounds, seed, iter_ptr,
+                                                                          d, m->part);
+  *nparts_out = ctas;
+  return mlp_ok(m, cudaGetLastError());
+}
+
+}  // namespace
+
+MlpDev phieng_mlp_dev(const PhiengMlp* m) {
+  MlpDev d;
+  d.frag = m->frag;
+  d.bias = m->bias;
+  d.w3 = m->w3;
+  d.norm = m->norm;
+  return d;
+}
+
+extern "C" {
+
+PhiengMlp* phieng_mlp_new(uint64_t seed) {
+  PhiengMlp* m = new (std::nothrow) PhiengMlp();
+  if (!m) return nullptr;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    m->error = PHIENG_SPH_E_NO_DEVICE;
+    return m;
+  }
+  m->device = dev;
+  if (!mlp_ok(m, cudaStreamCreateWithFlags(&m->own_stream, cudaStreamNonBlocking))) return m;
+  m->stream = m->own_stream;
+  if (!mlp_alloc(m, m->w, kParams) || !mlp_alloc(m, m->m, kParams) || !mlp_alloc(m, m->v, kParams) ||
+      !mlp_alloc(m, m->frag, kFragAll) || !mlp_alloc(m, m->bias, kBias) || !mlp_alloc(m, m->w3, kOut * kHidden) ||
+      !mlp_alloc(m, m->norm, kNorm) || !mlp_alloc(m, m->ctr, 2) || !mlp_alloc(m, m->grad, kParams + 1))
+    return m;
+  if (!mlp_ok(m, cudaMallocHost(reinterpret_cast<void**>(&m->h_pinned), sizeof(float) * (kParams + kNorm + 4))))
+    return m;
+  if (!mlp_ok(m, cudaFuncSetAttribute(k_mlp_train_tile, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)sizeof(TrainSmem))))
+    return m;
+  // Linear-layer initialisation U(-1/sqrt(fan_in), 1/sqrt(fan_in)) from
+  // SplitMix64(seed); the output layer starts at zero (no correction).
+  std::vector<float> w(kParams, 0.0f), norm(kNorm, 0.0f);
+  uint64_t s = seed;
+  auto uni = [&](float bound) {
+    const uint64_t z = mix64(s);
+    s += 0x9E3779B97F4A7C15ull;
+    const double u = (double)(z >> 11) * (1.0 / 9007199254740992.0);
+    return (float)((2.0 * u - 1.0) * bound);
+  };
+  for (int i = 0; i < kHidden * kFeat; i++) w[kOffW1 + i] = uni(0.25f);
+  for (int i = 0; i < kHidden; i++) w[kOffB1 + i] = uni(0.25f);
+  for (int i = 0; i < kHidden * kHidden; i++) w[kOffW2 + i] = uni(0.125f);
+  for (int i = 0; i < kHidden; i++) w[kOffB2 + i] = uni(0.125f);
+  for (int i = 0; i < kFeat; i++) norm[kFeat + i] = 1.0f;
+  norm[2 * kFeat] = norm[2 * kFeat + 1] = 1.0f;
+  phieng_mlp_set_params(m, w.data(), norm.data());
+  return m;
+}
+
+void phieng_mlp_free(PhiengMlp* m) {
+  if (!m) return;
+  if (m->device >= 0) {
+    cudaStreamSynchronize(m->stream);
+    cudaFree(m->w);
+    cudaFree(m->m);
+    cudaFree(m->v);
+    cudaFree(m->frag);
+    cudaFree(m->bias);
+    cudaFree(m->w3);
+    cudaFree(m->norm);
+    cudaFree(m->ctr);
+    cudaFree(m->part);
+    cudaFree(m->grad);
+    cudaFree(m->loss_hist);
+    if (m->h_pinned) cudaFreeHost(m->h_pinned);
+    if (m->own_stream) cudaStreamDestroy(m->own_stream);
+  }
+  delete m;
+}
+
+int32_t phieng_mlp_status(const PhiengMlp* m) { return m ? m->error : PHIENG_SPH_E_ARG; }
+
+int32_t phieng_mlp_set_stream(PhiengMlp* m, void* stream) {
+  if (!m || m->error) return 0;
+  m->stream = stream ? (cudaStream_t)stream : m->own_stream;
+  return 1;
+}
+
+int32_t phieng_mlp_set_params(PhiengMlp* m, const float* params, const float* norm) {
+  if (!m || m->error || !params || !norm) return 0;
+  if (!mlp_ok(m, cudaMemcpyAsync(m->w, params, sizeof(float) * kParams, cudaMemcpyHostToDevice, m->stream)) ||
+      !mlp_ok(m, cudaMemcpyAsync(m->norm, norm, sizeof(float) * kNorm, cudaMemcpyHostToDevice, m->stream)) ||
+      !mlp_ok(m, cudaMemsetAsync(m->m, 0, sizeof(float) * kParams, m->stream)) ||
+      !mlp_ok(m, cudaMemsetAsync(m->v, 0, sizeof(float) * kParams, m->stream)) ||
+      !mlp_ok(m, cudaMemsetAsync(m->frag, 0, sizeof(uint2) * kFragAll, m->stream)) ||
+      !mlp_ok(m, cudaMemsetAsync(m->ctr, 0, sizeof(uint32_t) * 2, m->stream)))
+    return 0;
+  if (!sync_images(m)) return 0;
+  return mlp_ok(m, cudaStreamSynchronize(m->stream)) ? 1 : 0;
+}
+
+int32_t phieng_mlp_get_params(PhiengMlp* m, float* params, float* norm) {
+  if (!m || m->error) return 0;
+  if (params && !mlp_ok(m, cudaMemcpyAsync(params, m->w, sizeof(float) * kParams, cudaMemcpyDeviceToHost, m->stream)))
+    return 0;
+  if (norm && !mlp_ok(m, cudaMemcpyAsync(norm, m->norm, sizeof(float) * kNorm, cudaMemcpyDeviceToHost, m->stream)))
+    return 0;
+  return mlp_ok(m, cudaStreamSynchronize(m->stream)) ? 1 : 0;
+}
+
+uint32_t phieng_mlp_step_count(PhiengMlp* m) {
+  if (!m || m->error) return 0;
+  uint32_t t = 0;
+  if (!mlp_ok(m, cudaMemcpyAsync(m->h_pinned, m->ctr, 4, cudaMemcpyDeviceToHost, m->stream)) ||
+      !mlp_ok(m, cudaStreamSynchronize(m->stream)))
+    return 0;
+  std::memcpy(&t, m->h_pinned, 4);
+  return t;
+}
+
+int32_t phieng_mlp_forward(PhiengMlp* m, const float* x, uint32_t n, float* y) {
+  if (!m || m->error || (n && (!x || !y))) return 0;
+  if (n == 0) return 1;
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, m->device);
+  const uint32_t blocks = std::min<uint32_t>(cdiv(n, 128), (uint32_t)sms * 8u);
+  k_mlp_forward<<<blocks, 128, 0, m->stream>>>(x, n, phieng_mlp_dev(m), y);
+  return mlp_ok(m, cudaGetLastError()) ? 1 : 0;
+}
+
+int32_t phieng_mlp_grad(PhiengMlp* m, const float* x, const float* t, uint32_t npairs, uint32_t batch, uint64_t seed,
+                        uint32_t iter, float* grad_host, float* loss_host) {
+  if (!m || m->error || !check_pairs(x, t, npairs, batch)) return 0;
+  if (!mlp_ok(m, cudaMemcpyAsync(m->ctr + 1, &iter, 4, cudaMemcpyHostToDevice, m->stream))) return 0;
+  uint32_t nparts = 0;
+  if (!launch_tile(m, x, t, npairs, batch, seed, m->ctr + 1, &nparts)) return 0;
+  const float inv_2b = (float)(0.5 / (double)batch);
+  k_mlp_reduce<<<cdiv(kParams + 1, 256), 256, 0, m->stream>>>(m->part, nparts, inv_2b, m->grad, m->grad + kParams);
+  if (!mlp_ok(m, cudaGetLastError())) return 0;
+  if (!mlp_ok(m, cudaMemcpyAsync(m->h_pinned, m->grad, sizeof(float) * (kParams + 1), cudaMemcpyDeviceToHost,
+                                 m->stream)) ||
+      !mlp_ok(m, cudaStreamSynchronize(m->stream)))
+    return 0;
+  if (grad_host) std::memcpy(grad_host, m->h_pinned, sizeof(float) * kParams);
+  if (loss_host) *loss_host = m->h_pinned[kParams];
+  return 1;
+}
+
+int32_t phieng_mlp_train(PhiengMlp* m, const float* x, const float* t, uint32_t npairs, uint32_t batch, uint32_t iters,
+                         float lr, uint64_t seed, float* loss_hist_host) {
+  if (!m || m->error || !check_pairs(x, t, npairs, batch) || !(lr > 0.0f)) return 0;
+  if (iters == 0) return 1;
+  if (loss_hist_host && m->loss_cap < iters) {
+    cudaFree(m->loss_hist);
+    m->loss_hist = nullptr;
+    m->loss_cap = 0;
+    if (!mlp_alloc(m, m->loss_hist, iters)) return 0;
+    m->loss_cap = iters;
+  }
+  const uint32_t t0 = phieng_mlp_step_count(m);
+  const float inv_2b = (float)(0.5 / (double)batch);
+  // one iteration = tile, Adam, advance; replayed from a graph of up to 32
+  const uint32_t per_graph = std::min<uint32_t>(iters, 32u);
+  auto enqueue = [&](uint32_t k, cudaStream_t st) -> bool {
+    cudaStream_t keep = m->stream;
+    m->stream = st;
+    bool ok = true;
+    for (uint32_t i = 0; i < k && ok; i++) {
+      uint32_t nparts = 0;
+      ok = launch_tile(m, x, t, npairs, batch, seed, m->ctr, &nparts);
+      if (ok) {
+        k_mlp_adam<<<cdiv(kParams + 1, 256), 256, 0, st>>>(m->part, nparts, m->w, m->m, m->v, m->ctr, lr, inv_2b,
+                                                            loss_hist_host ? m->loss_hist : nullptr, t0, iters,
+                                                            m->frag, m->bias, m->w3);
+        k_mlp_advance<<<1, 1, 0, st>>>(m->ctr);
+        ok = mlp_ok(m, cudaGetLastError());
+      }
+    }
+    m->stream = keep;
+    return ok;
+  };
+  cudaGraph_t g = nullptr;
+  cudaGraphExec_t ge = nullptr;
+  cudaStream_t cap;
+  if (!mlp_ok(m, cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking))) return 0;
+  bool ok = mlp_ok(m, cudaStreamSynchronize(m->stream)) &&
+            mlp_ok(m, cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
+  if (ok) {
+    const bool body = enqueue(per_graph, cap);
+    ok = mlp_ok(m, cudaStreamEndCapture(cap, &g)) && body && mlp_ok(m, cudaGraphInstantiate(&ge, g, 0));
+  }
+  uint32_t done = 0;
+  while (ok && done + per_graph <= iters) {
+    ok = mlp_ok(m, cudaGraphLaunch(ge, m->stream));
+    done += per_graph;
+  }
+  if (ok && done < iters) ok = enqueue(iters - done, m->stream);
+  if (ge) cudaGraphExecDestroy(ge);
+  if (g) cudaGraphDestroy(g);
+  cudaStreamDestroy(cap);
+  if (ok && loss_hist_host)
+    ok = mlp_ok(m, cudaMemcpyAsync(loss_hist_host, m->loss_hist, sizeof(float) * iters, cudaMemcpyDeviceToHost,
+                                   m->stream));
+  if (ok) ok = mlp_ok(m, cudaStreamSynchronize(m->stream));
+  return ok ? 1 : 0;
+}
+
+int32_t phieng_mlp_sample_indices(uint32_t npairs, uint32_t batch, uint64_t seed, uint32_t iter, uint32_t* idx,
+                                  void* stream) {
+  if (!idx || npairs == 0) return 0;
+  if (batch == 0) return 1;
+  k_mlp_indices<<<cdiv(batch, 256), 256, 0, (cudaStream_t)stream>>>(seed, iter, batch, npairs, idx);
+  return cudaGetLastError() == cudaSuccess ? 1 : 0;
+}
+
+int32_t phieng_mlp_targets(const float* fine, const float* coarse, uint32_t n, float inv_h, float* out, void* stream) {
+  if (n && (!fine || !coarse || !out)) return 0;
+  if (n == 0) return 1;
+  k_mlp_targets<<<cdiv(n, 256), 256, 0, (cudaStream_t)stream>>>(reinterpret_cast<const float4*>(fine),
+                                                                 reinterpret_cast<const float4*>(coarse), n, inv_h,
+                                                                 reinterpret_cast<float2*>(out));
+  return cudaGetLastError() == cudaSuccess ? 1 : 0;
+}
+
+}  // extern "C"

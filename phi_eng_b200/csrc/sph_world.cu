@@ -17,6 +17,7 @@
 
 #include "../../include/phieng_sph.h"
 #include "sph_kernels.h"
+#include "sph_mlp_host.h"
 
 using namespace phieng;
 
@@ -194,6 +195,17 @@ struct World2 {
   uint32_t* d_sscene = nullptr;
   uint32_t batch_cap = 0;
   bool is_batch() const { return !scenes.empty(); }
+
+  // learned closure (phieng_sph_set_closure / phieng_sph_closure_step)
+  PhiengMlp* closure = nullptr;
+  uint32_t closure_ratio = 4;
+  float closure_threshold = 0.03f;
+  uint32_t closure_criterion = 0;
+  float4* d_save = nullptr;     // pre-step state of the last coarse step (id order)
+  float* d_rho_prev = nullptr;  // pre-step density (id order)
+  uint32_t closure_cap = 0;
+  cudaGraphExec_t cexec = nullptr;
+  std::string csig;
 };
 
 namespace {
@@ -244,6 +256,9 @@ void release_graph(World2* w) {
   if (w->gexec) cudaGraphExecDestroy(w->gexec);
   w->gexec = nullptr;
   w->gsig.clear();
+  if (w->cexec) cudaGraphExecDestroy(w->cexec);
+  w->cexec = nullptr;
+  w->csig.clear();
 }
 
 bool ensure_device(World2* w) {
@@ -695,6 +710,60 @@ bool world_step(World2* w, float dt) {
   return true;
 }
 
+
+// ---------------------------------------------------------------- learned closure
+bool ensure_closure_buffers(World2* w) {
+  if (w->closure_cap >= w->d.cap && w->d_save) return true;
+  dfree(w->d_save);
+  dfree(w->d_rho_prev);
+  w->closure_cap = 0;
+  if (!dalloc(w, w->d_save, w->d.cap) || !dalloc(w, w->d_rho_prev, w->d.cap)) return false;
+  w->closure_cap = w->d.cap;
+  release_graph(w);
+  return true;
+}
+
+// Sort + density of the current state with parameters P (the state and its
+// keys / bucket counts are current). Leaves the counts consumed.
+void enqueue_sort_density(World2* w, const StepParams& P) {
+  enqueue_sort_and_ranges(w->d, w->n, P, w->sid_perm_n == w->n, w->stream);
+  enqueue_density(w->d, w->n, P, w->stream);
+  w->sid_perm_n = w->n;
+  w->dp_on_device = true;
+}
+
+// One coarse step from a sorted state with its density: closure force pass,
+// then sort + density of the new state and the density check into
+// scalar[4]; replayed from a cached graph.
+bool run_coarse(World2* w, const StepParams& P, const MlpDev& mlp, const ClosureIO& io) {
+  std::string sig((const char*)&P, sizeof(P));
+  sig.append((const char*)&w->n, sizeof(w->n));
+  sig.append((const char*)&w->closure_criterion, sizeof(w->closure_criterion));
+  sig.append((const char*)&mlp, sizeof(mlp));
+  sig.append((const char*)&io, sizeof(io));
+  if (!w->cexec || sig != w->csig) {
+    if (w->cexec) cudaGraphExecDestroy(w->cexec);
+    w->cexec = nullptr;
+    cudaGraph_t g = nullptr;
+    if (!cuda_ok(w, cudaStreamBeginCapture(w->own_stream, cudaStreamCaptureModeThreadLocal), "begin capture"))
+      return false;
+    enqueue_closure_force(w->d, w->n, P, mlp, io, w->own_stream);
+    enqueue_sort_and_ranges(w->d, w->n, P, true, w->own_stream);
+    enqueue_density(w->d, w->n, P, w->own_stream);
+    enqueue_closure_check(w->d, w->n, P, io.rho_prev, w->closure_criterion, w->d.scalar + 4, w->own_stream);
+    cudaError_t r = cudaStreamEndCapture(w->own_stream, &g);
+    if (!cuda_ok(w, r, "end capture")) return false;
+    r = cudaGraphInstantiate(&w->cexec, g, 0);
+    cudaGraphDestroy(g);
+    if (!cuda_ok(w, r, "graph instantiate")) {
+      w->cexec = nullptr;
+      return false;
+    }
+    w->csig = sig;
+  }
+  return cuda_ok(w, cudaGraphLaunch(w->cexec, w->stream), "graph launch");
+}
+
 void recompute_uniformity(World2* w) {
   w->mass_uniform = true;
   w->phase_uniform = true;
@@ -766,6 +835,9 @@ void phieng_world_free(World2* w) {
     dfree(w->d_pscene);
     dfree(w->d_sscene);
     dfree(w->d_ptab);
+    dfree(w->d_save);
+    dfree(w->d_rho_prev);
+    if (w->cexec) cudaGraphExecDestroy(w->cexec);
     for (auto& e : w->ev)
       if (e) cudaEventDestroy(e);
     if (w->h_pinned) cudaFreeHost(w->h_pinned);
@@ -1068,6 +1140,107 @@ int32_t phieng_sph_front_metrics(World2* w, float* out) {
   }
   std::memcpy(&out[1], &bv, 4);
   return 1;
+}
+
+uint32_t phieng_sph_get_state_device(World2* w, float* dst, uint32_t max) {
+  if (!w || !dst) return 0;
+  const uint32_t n = std::min(max, w->n);
+  if (n == 0) return 0;
+  if (!prepare(w)) return 0;
+  if (!cuda_ok(w, cudaMemcpyAsync(dst, w->d.state, sizeof(float4) * n, cudaMemcpyDeviceToDevice, w->stream),
+               "get state"))
+    return 0;
+  return n;
+}
+
+int32_t phieng_sph_set_state_device(World2* w, const float* src, uint32_t n) {
+  if (!w || !src || n != w->n) return 0;
+  if (n == 0) return 1;
+  if (!prepare(w)) return 0;
+  if (!cuda_ok(w, cudaMemcpyAsync(w->d.state, src, sizeof(float4) * n, cudaMemcpyDeviceToDevice, w->stream),
+               "set state"))
+    return 0;
+  w->host_state_valid = false;
+  w->dp_on_device = false;
+  w->keys_valid = false;  // the bucket grid stays: any grid is exact, it only affects speed
+  return 1;
+}
+
+int32_t phieng_sph_features(World2* w, float dt, float* feat) {
+  if (!w || !feat || !std::isfinite(dt) || dt <= 0.0f) return 0;
+  if (w->n == 0) return 1;
+  if (!w->is_batch() && unsupported(w)) return 0;
+  if (!prepare(w)) return 0;
+  if (w->is_batch() && !upload_scene_table(w, dt)) return 0;
+  const StepParams P = make_params(w, dt);
+  enqueue_sort_density(w, P);
+  enqueue_closure_features(w->d, w->n, P, feat, w->stream);
+  w->keys_valid = false;  // the sort consumed the bucket counts
+  return cuda_ok(w, cudaGetLastError(), "features") ? 1 : 0;
+}
+
+int32_t phieng_sph_set_closure(World2* w, PhiengMlp* mlp, uint32_t ratio, float threshold, uint32_t criterion) {
+  if (!w || w->is_batch() || ratio < 1 || !(threshold >= 0.0f) || criterion > PHIENG_CLOSURE_COMPRESSION) return 0;
+  if (mlp && phieng_mlp_status(mlp) != PHIENG_SPH_OK) return 0;
+  w->closure = mlp;
+  w->closure_ratio = ratio;
+  w->closure_threshold = threshold;
+  w->closure_criterion = criterion;
+  return 1;
+}
+
+int32_t phieng_sph_closure_step(World2* w, float dt_fine, uint32_t coarse_steps, PhiengClosureStats* stats) {
+  if (!w || w->is_batch() || !w->closure || !std::isfinite(dt_fine) || dt_fine <= 0.0f) return 0;
+  const float dtc = dt_fine * (float)w->closure_ratio;
+  if (!w->cfg.enabled || w->n == 0 || coarse_steps == 0) {
+    w->time += dtc * (float)coarse_steps;
+    return 1;
+  }
+  if (unsupported(w)) return 0;
+  if (!prepare(w)) return 0;
+  if (!ensure_closure_buffers(w)) return 0;
+  const StepParams Pc = make_params(w, dtc);
+  const StepParams Pf = make_params(w, dt_fine);
+  const MlpDev mlp = phieng_mlp_dev(w->closure);
+  ClosureIO io;
+  io.save = w->d_save;
+  io.rho_prev = w->d_rho_prev;
+  io.acc_scale = Pc.hk / (dtc * dtc);
+  enqueue_sort_density(w, Pc);
+  for (uint32_t k = 0; k < coarse_steps; k++) {
+    if (!run_coarse(w, Pc, mlp, io)) return 0;
+    w->sid_perm_n = w->n;
+    if (!cuda_ok(w, cudaMemcpyAsync(w->h_pinned, w->d.scalar + 4, 4, cudaMemcpyDeviceToHost, w->stream), "check") ||
+        !cuda_ok(w, cudaStreamSynchronize(w->stream), "sync"))
+      return 0;
+    float chk;
+    std::memcpy(&chk, w->h_pinned, 4);
+    if (stats) {
+      stats->coarse_steps++;
+      stats->last_check = chk;
+      stats->max_check = std::max(stats->max_check, chk);
+    }
+    w->host_state_valid = false;
+    if (chk <= w->closure_threshold) {
+      if (stats) stats->accepted++;
+      w->substeps++;
+    } else {
+      // undo the coarse step, take ratio plain substeps instead
+      if (stats) stats->fallbacks++;
+      if (!cuda_ok(w, cudaMemcpyAsync(w->d.state, w->d_save, sizeof(float4) * w->n, cudaMemcpyDeviceToDevice,
+                                      w->stream),
+                   "restore"))
+        return 0;
+      w->keys_valid = false;
+      if (!prepare(w)) return 0;
+      for (uint32_t r = 0; r < w->closure_ratio; r++)
+        if (!run_substep(w, Pf)) return 0;
+      if (k + 1 < coarse_steps) enqueue_sort_density(w, Pc);
+    }
+    w->time += dtc;
+  }
+  w->keys_valid = false;  // the last sort consumed the bucket counts
+  return cuda_ok(w, cudaGetLastError(), "closure step") ? 1 : 0;
 }
 
 uint32_t phieng_sph_debug_sorted(World2* w, uint32_t* ids, uint32_t* keys, uint32_t max) {

@@ -238,6 +238,40 @@ class World2:
         k = self._lib.phieng_sph_phase_times(self._h, _fptr(out), 3)
         return out[:k].astype(np.float64)
 
+    # ---- device-resident state and the learned closure ----
+    def get_state_device(self, dst_ptr: int, max_count: int) -> int:
+        """Copy [x, y, vx, vy] of up to max_count particles to device memory."""
+        k = self._lib.phieng_sph_get_state_device(self._h, C.c_void_p(dst_ptr), max_count)
+        self.check()
+        return int(k)
+
+    def set_state_device(self, src_ptr: int, n: int) -> None:
+        if self._lib.phieng_sph_set_state_device(self._h, C.c_void_p(src_ptr), n) != 1:
+            self.check()
+            raise ValueError("set_state_device: count mismatch")
+
+    def features(self, dt: float, feat_ptr: int) -> None:
+        """Closure inputs (n x 16 floats, device) at the current state for a step dt."""
+        if self._lib.phieng_sph_features(self._h, dt, C.c_void_p(feat_ptr)) != 1:
+            self.check()
+            raise ValueError("features failed")
+
+    def set_closure(self, mlp, ratio: int = 4, threshold: float = 0.03,
+                    criterion: int = _abi.CLOSURE_JUMP) -> None:
+        h = mlp._h if mlp is not None else None
+        if self._lib.phieng_sph_set_closure(self._h, h, ratio, threshold, criterion) != 1:
+            raise ValueError("set_closure rejected its arguments")
+        self._closure = mlp  # keep the network alive while attached
+
+    def closure_step(self, dt_fine: float, coarse_steps: int = 1, stats=None):
+        """coarse_steps steps of ratio x dt_fine with the attached closure;
+        returns the accumulated PhiengClosureStats."""
+        st = stats if stats is not None else _abi.PhiengClosureStats()
+        if self._lib.phieng_sph_closure_step(self._h, dt_fine, coarse_steps, C.byref(st)) != 1:
+            self.check()
+            raise ValueError("closure_step failed (no network attached?)")
+        return st
+
     # ---- diagnostics ----
     def debug_sorted(self):
         n = len(self.fluid)

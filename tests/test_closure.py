@@ -1,0 +1,387 @@
+"""Learned closure: features, network, training kernels and the coarse step.
+
+CPU: the numpy network oracle's analytic gradient against finite
+differences, its BF16 rounding, the oracle features' basic identities.
+GPU: features bit-exact against the oracle; the network's initialisation,
+minibatch sampling and Adam step exact; forward pass and gradients within the
+BF16 tolerance stated below; training deterministic; the closure step equal
+to the plain coarse step with a zero network and to plain fine steps when
+every coarse step falls back.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import sims
+from oracle import mlp_oracle as mo
+from oracle import oracle as orc
+from phi_eng_b200 import scenes
+
+# ---------------------------------------------------------------- oracle (CPU)
+
+
+def _orc_features(sim, dt):
+    lib = orc._load()
+    if not hasattr(lib.orc_features, "_bound"):
+        lib.orc_features.restype = C.c_uint32
+        lib.orc_features.argtypes = [C.c_void_p, C.c_float, C.POINTER(C.c_float), C.c_uint32]
+        lib.orc_features._bound = True
+    n = sim.count
+    out = np.zeros((n, 16), np.float32)
+    k = lib.orc_features(sim.w._h, dt, out.ctypes.data_as(C.POINTER(C.c_float)), n)
+    assert k == n
+    return out
+
+
+def _random_net(rng, scale_out=0.3):
+    p = mo.init_params(int(rng.integers(1 << 62)))
+    p[mo.OFF_W3:mo.OFF_B3] = (rng.standard_normal(2 * 64) * scale_out).astype(np.float32)
+    p[mo.OFF_B3:] = rng.standard_normal(2).astype(np.float32) * 0.1
+    norm = np.concatenate([rng.standard_normal(16) * 0.1, 1.0 + rng.random(16), [0.7, 1.3]]).astype(np.float32)
+    return p, norm
+
+
+def test_bf16_rounding():
+    x = np.array([1.0, 1.0 + 2.0 ** -8, 1.0 + 3 * 2.0 ** -8, 1.0 + 2.0 ** -9, -2.5, 0.0], np.float32)
+    r = mo.bf16(x)
+    # BF16 keeps 8 significant bits (unit 2^-7 at 1): 1 + 2^-8 ties to 1 (even),
+    # 1 + 3 * 2^-8 ties to 1 + 2^-6 (even)
+    assert r[0] == 1.0 and r[1] == 1.0 and r[3] == 1.0
+    assert r[2] == np.float32(1.0 + 2.0 ** -6) and r[4] == -2.5 and r[5] == 0.0
+
+
+def test_oracle_gradient_matches_finite_differences():
+    rng = np.random.default_rng(1)
+    p, norm = _random_net(rng)
+    x = rng.standard_normal((64, 16)).astype(np.float32)
+    t = rng.standard_normal((64, 2)).astype(np.float32)
+    loss, g = mo.loss_grad(p, norm, x, t, emulate=False)
+    p64 = p.astype(np.float64)
+    idx = rng.choice(mo.NPARAMS, 40, replace=False)
+    eps = 1e-3
+
+    def L(q):
+        # float64 network: evaluate with q in float64 (no float32 cast of parameters)
+        W1, b1, W2, b2, W3, b3 = mo.unpack(q)
+        xh = mo.normalise(x, norm, emulate=False)
+        z1 = xh @ W1.T + b1
+        z2 = mo.silu(z1) @ W2.T + b2
+        y = mo.silu(z2) @ W3.T + b3
+        th = (t.astype(np.float32) * (np.float32(1.0) / norm[32:].astype(np.float32))).astype(np.float64)
+        return float(np.sum((y - th) ** 2) / (2 * x.shape[0]))
+
+    assert abs(L(p64) - loss) < 1e-6 * max(1.0, abs(loss))
+    for i in idx:
+        e = np.zeros_like(p64)
+        e[i] = eps
+        fd = (L(p64 + e) - L(p64 - e)) / (2 * eps)
+        assert abs(fd - g[i]) <= 1e-6 + 1e-4 * abs(fd), (i, fd, g[i])
+
+
+def test_oracle_adam_first_step_moves_by_lr():
+    w = np.ones(8, np.float32)
+    g = np.array([1, -2, 3, -4, 5, -6, 7, 1e-3], np.float32)
+    w1, m, v = mo.adam(w, np.zeros(8, np.float32), np.zeros(8, np.float32), g, 1, 1e-3)
+    # first Adam step is lr * sign(g) up to eps
+    np.testing.assert_allclose(w - w1, 1e-3 * np.sign(g), rtol=1e-4)
+
+
+def test_oracle_sample_indices_in_range_and_deterministic():
+    a = mo.sample_indices(7, 3, 4096, 1000003)
+    b = mo.sample_indices(7, 3, 4096, 1000003)
+    assert a.min() >= 0 and a.max() < 1000003 and np.array_equal(a, b)
+    assert not np.array_equal(a, mo.sample_indices(7, 4, 4096, 1000003))
+    # roughly uniform
+    h = np.bincount(mo.sample_indices(1, 0, 1 << 16, 16), minlength=16)
+    assert h.min() > 3500 and h.max() < 4700
+
+
+def test_oracle_features_identities():
+    """A particle alone far from walls: no neighbours, wall distance at the 3h
+    cap, zero aggregates; a particle beside a wall reads its distance."""
+    sim = sims.OracleSim(orc.JACOBI)
+    cfg = scenes.si_config(0.01)
+    sim.config = cfg
+    sim.add_box(0.0, -0.05, 1.0, 0.05)  # floor: top face at y = 0
+    sim.add_particles(np.array([[0.3, 0.5], [0.6, 0.01]], np.float32))
+    f = _orc_features(sim, 4 * scenes.fine_dt(cfg))
+    h = np.float32(cfg.smoothing_length)
+    assert f[0, 4] == 0.0 and np.all(f[0, [2, 3, 8, 9, 10, 11, 12, 13, 14, 15]] == 0.0)
+    assert f[0, 5] == np.float32(np.float32(3.0) * h) / h and f[0, 6] == 0.0 and f[0, 7] == 0.0
+    # second particle: 0.01 above the floor's top face, normal +y
+    assert abs(f[1, 5] - 0.01 / 0.02) < 1e-5 and f[1, 6] == 0.0 and f[1, 7] == 1.0
+
+
+def test_oracle_features_lattice_at_rest():
+    sim = sims.load_scene(sims.OracleSim(orc.JACOBI), scenes.dam_break_4k())
+    f = _orc_features(sim, 4 * scenes.dam_break_4k().dt)
+    assert np.all(np.isfinite(f))
+    assert np.all(f[:, [2, 3, 8, 9, 10, 11, 12, 15]] == 0.0)  # no velocity yet
+    assert f[:, 4].max() * 16 <= 24 and f[:, 4].min() * 16 >= 2
+
+
+# ---------------------------------------------------------------- GPU
+
+
+def _torch():
+    import torch
+
+    return torch
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("steps", [0, 30])
+def test_features_bit_exact(steps):
+    from phi_eng_b200.world import world_from_scene
+
+    torch = _torch()
+    sc = scenes.dam_break_4k()
+    dtc = 4 * sc.dt
+    o = sims.load_scene(sims.OracleSim(orc.JACOBI), sc)
+    w = world_from_scene(sc)
+    if steps:
+        o.step(sc.dt, steps)
+        w.step_n(sc.dt, steps)
+        np.testing.assert_array_equal(w.fluid.particles, o.state())
+    feat = torch.empty((sc.n, 16), dtype=torch.float32, device="cuda")
+    w.features(dtc, feat.data_ptr())
+    w.sync()
+    np.testing.assert_array_equal(feat.cpu().numpy(), _orc_features(o, dtc))
+    # the state is untouched and stepping continues bit-exactly
+    w.step_n(sc.dt, 3)
+    o.step(sc.dt, 3)
+    np.testing.assert_array_equal(w.fluid.particles, o.state())
+    w.close()
+
+
+@pytest.mark.gpu
+def test_features_bit_exact_circles_and_tank():
+    from phi_eng_b200.world import world_from_scene
+
+    torch = _torch()
+    sc = scenes.reference_tank()
+    sc.circles = [(1.5, 1.0, 0.4)]
+    o = sims.load_scene(sims.OracleSim(orc.JACOBI), sc)
+    w = world_from_scene(sc)
+    o.step(sc.dt, 20)
+    w.step_n(sc.dt, 20)
+    feat = torch.empty((sc.n, 16), dtype=torch.float32, device="cuda")
+    w.features(0.01, feat.data_ptr())
+    w.sync()
+    np.testing.assert_array_equal(feat.cpu().numpy(), _orc_features(o, 0.01))
+    w.close()
+
+
+@pytest.mark.gpu
+def test_batch_features_equal_each_scene():
+    from phi_eng_b200.batch import Batch, batched_scenes
+    from phi_eng_b200.world import world_from_scene
+
+    torch = _torch()
+    scs = batched_scenes(6, n_max=4096)
+    b = Batch.from_scenes(scs)
+    b.step(scs[0].dt, 10)
+    n = sum(s.n for s in scs)
+    feat = torch.empty((n, 16), dtype=torch.float32, device="cuda")
+    b.world.features(4 * scs[0].dt, feat.data_ptr())
+    b.world.sync()
+    allf = feat.cpu().numpy()
+    for k, sc in enumerate(scs):
+        w = world_from_scene(sc)
+        w.step_n(sc.dt, 10)
+        fk = torch.empty((sc.n, 16), dtype=torch.float32, device="cuda")
+        w.features(4 * sc.dt, fk.data_ptr())
+        w.sync()
+        f0, c = b.scene_range(k)
+        np.testing.assert_array_equal(allf[f0:f0 + c], fk.cpu().numpy())
+        w.close()
+    b.close()
+
+
+@pytest.mark.gpu
+def test_mlp_init_and_params_roundtrip():
+    from phi_eng_b200.closure import Mlp
+
+    m = Mlp(seed=1234)
+    p, nrm = m.get()
+    np.testing.assert_array_equal(p, mo.init_params(1234))
+    np.testing.assert_array_equal(nrm[16:], np.ones(18, np.float32))
+    q = np.arange(mo.NPARAMS, dtype=np.float32) * 1e-4
+    m.set(q, nrm)
+    np.testing.assert_array_equal(m.get()[0], q)
+    assert m.steps == 0
+
+
+@pytest.mark.gpu
+def test_sample_indices_exact():
+    from phi_eng_b200.closure import sample_indices
+
+    for (npairs, batch, seed, it) in [(1000003, 65536, 0x5EED, 0), (777, 4096, 3, 12345), (1 << 31, 128, 9, 7)]:
+        np.testing.assert_array_equal(sample_indices(npairs, batch, seed, it), mo.sample_indices(seed, it, batch, npairs))
+
+
+# Tolerance of the BF16 network against the oracle's emulation: both round
+# activations and weights to BF16 at the same points; they differ by the
+# FP32 accumulation order and by the hardware tanh (relative error ~2^-11),
+# which moves a BF16 rounding by one unit (2^-8 relative) now and then.
+FWD_TOL = 2e-2   # max |y_gpu - y_oracle| / rms(y_oracle)
+GRAD_TOL = 3e-2  # |g_gpu - g_oracle| / |g_oracle| per parameter block
+
+
+@pytest.mark.gpu
+def test_mlp_forward_matches_oracle():
+    from phi_eng_b200.closure import Mlp
+
+    torch = _torch()
+    rng = np.random.default_rng(5)
+    p, norm = _random_net(rng)
+    m = Mlp()
+    m.set(p, norm)
+    x = rng.standard_normal((10000, 16)).astype(np.float32) * 2.0
+    y = m.forward(torch.from_numpy(x).cuda()).cpu().numpy()
+    yo, _ = mo.forward(p, norm, x, emulate=True)
+    err = np.abs(y - yo).max() / np.sqrt(np.mean(yo ** 2))
+    assert err < FWD_TOL, err
+    assert np.sqrt(np.mean((y - yo) ** 2)) / np.sqrt(np.mean(yo ** 2)) < 2e-3
+
+
+@pytest.mark.gpu
+def test_mlp_gradient_matches_oracle():
+    from phi_eng_b200.closure import Mlp
+
+    torch = _torch()
+    rng = np.random.default_rng(6)
+    p, norm = _random_net(rng)
+    m = Mlp()
+    m.set(p, norm)
+    npairs, batch, seed, it = 50000, 4096, 0xABC, 3
+    x = rng.standard_normal((npairs, 16)).astype(np.float32)
+    t = rng.standard_normal((npairs, 2)).astype(np.float32)
+    loss, g = m.grad(torch.from_numpy(x).cuda(), torch.from_numpy(t).cuda(), batch, seed, it)
+    idx = mo.sample_indices(seed, it, batch, npairs)
+    lo, go = mo.loss_grad(p, norm, x[idx], t[idx], emulate=True)
+    assert abs(loss - lo) / lo < 1e-3
+    blocks = [(mo.OFF_W1, mo.OFF_B1), (mo.OFF_B1, mo.OFF_W2), (mo.OFF_W2, mo.OFF_B2), (mo.OFF_B2, mo.OFF_W3),
+              (mo.OFF_W3, mo.OFF_B3), (mo.OFF_B3, mo.NPARAMS)]
+    for a, b in blocks:
+        rel = np.linalg.norm(g[a:b] - go[a:b]) / np.linalg.norm(go[a:b])
+        assert rel < GRAD_TOL, (a, b, rel)
+
+
+@pytest.mark.gpu
+def test_adam_step_exact_and_training_deterministic():
+    from phi_eng_b200.closure import Mlp
+
+    torch = _torch()
+    rng = np.random.default_rng(7)
+    p, norm = _random_net(rng)
+    npairs, batch, seed = 20000, 1024, 0x77
+    x = torch.from_numpy(rng.standard_normal((npairs, 16)).astype(np.float32)).cuda()
+    t = torch.from_numpy(rng.standard_normal((npairs, 2)).astype(np.float32)).cuda()
+    m = Mlp()
+    m.set(p, norm)
+    _, g = m.grad(x, t, batch, seed, 0)
+    m.train(x, t, batch=batch, iters=1, lr=1e-3, seed=seed)
+    w1, _ = m.get()
+    wo, mm, vv = mo.adam(p, np.zeros_like(p), np.zeros_like(p), g, 1, 1e-3)
+    np.testing.assert_array_equal(w1, wo)
+    # second step from the moments
+    _, g2 = m.grad(x, t, batch, seed, 1)
+    m.train(x, t, batch=batch, iters=1, lr=1e-3, seed=seed)
+    wo2, _, _ = mo.adam(wo, mm, vv, g2, 2, 1e-3)
+    np.testing.assert_array_equal(m.get()[0], wo2)
+    # two identical runs give identical parameters and loss histories
+    runs = []
+    for _ in range(2):
+        mm_ = Mlp()
+        mm_.set(p, norm)
+        hist = mm_.train(x, t, batch=batch, iters=50, lr=1e-3, seed=seed)
+        runs.append((mm_.get()[0], hist))
+    np.testing.assert_array_equal(runs[0][0], runs[1][0])
+    np.testing.assert_array_equal(runs[0][1], runs[1][1])
+
+
+@pytest.mark.gpu
+def test_training_fits_a_smooth_map():
+    """The training kernels learn: a smooth nonlinear map of the inputs is fit
+    to a small fraction of its variance."""
+    from phi_eng_b200.closure import Mlp
+
+    torch = _torch()
+    rng = np.random.default_rng(8)
+    n = 200000
+    x = rng.standard_normal((n, 16)).astype(np.float32)
+    t = np.stack([np.tanh(x[:, 0] + 0.5 * x[:, 1]) * x[:, 2], np.sin(x[:, 3]) - 0.3 * x[:, 4] * x[:, 5]], 1)
+    t = t.astype(np.float32)
+    m = Mlp(seed=3)
+    p, nrm = m.get()
+    nrm[32:] = t.std(0)
+    m.set(p, nrm)
+    hist = m.train(torch.from_numpy(x).cuda(), torch.from_numpy(t).cuda(), batch=8192, iters=1500, lr=3e-3, seed=11)
+    assert hist[:20].mean() > 0.4 and hist[-50:].mean() < 0.05 * hist[:20].mean(), (hist[:20].mean(), hist[-50:].mean())
+
+
+def _world(sc):
+    from phi_eng_b200.world import world_from_scene
+
+    return world_from_scene(sc)
+
+
+@pytest.mark.gpu
+def test_zero_network_closure_equals_plain_coarse_step():
+    from phi_eng_b200 import _abi
+    from phi_eng_b200.closure import Mlp
+
+    sc = scenes.dam_break_4k()
+    m = Mlp()  # output layer zero: no correction
+    plain, clo = _world(sc), _world(sc)
+    plain.step_n(sc.dt, 20)
+    clo.step_n(sc.dt, 20)
+    clo.set_closure(m, 4, 1e30, _abi.CLOSURE_JUMP)
+    st = None
+    for k in range(3):
+        plain.step(4 * sc.dt)
+        st = clo.closure_step(sc.dt, 1, st)
+        np.testing.assert_array_equal(clo.fluid.particles, plain.fluid.particles)
+    assert st.accepted == 3 and st.fallbacks == 0
+    # and ordinary steps continue from there bit-exactly
+    plain.step_n(sc.dt, 2)
+    clo.step_n(sc.dt, 2)
+    np.testing.assert_array_equal(clo.fluid.particles, plain.fluid.particles)
+
+
+@pytest.mark.gpu
+def test_every_coarse_step_falling_back_equals_fine_steps():
+    from phi_eng_b200 import _abi
+    from phi_eng_b200.closure import Mlp
+
+    sc = scenes.dam_break_4k()
+    rng = np.random.default_rng(9)
+    p, norm = _random_net(rng)
+    m = Mlp()
+    m.set(p, norm)
+    plain, clo = _world(sc), _world(sc)
+    clo.set_closure(m, 4, 0.0, _abi.CLOSURE_COMPRESSION)  # threshold 0: any compression falls back
+    st = clo.closure_step(sc.dt, 5)
+    plain.step_n(sc.dt, 20)
+    assert st.fallbacks + st.accepted == 5
+    if st.fallbacks == 5:
+        np.testing.assert_array_equal(clo.fluid.particles, plain.fluid.particles)
+    assert st.fallbacks >= 4
+
+
+@pytest.mark.gpu
+def test_closure_check_reports_jump():
+    from phi_eng_b200 import _abi
+    from phi_eng_b200.closure import Mlp
+
+    sc = scenes.dam_break_4k()
+    w = _world(sc)
+    w.set_closure(Mlp(), 4, 1e30, _abi.CLOSURE_JUMP)
+    st = w.closure_step(sc.dt, 4)
+    # a plain coarse step from the resting block changes densities by a few
+    # percent at most at first; the check is a finite non-negative number
+    assert np.isfinite(st.max_check) and st.max_check >= 0.0 and st.accepted == 4
