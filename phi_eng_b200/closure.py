@@ -15,7 +15,7 @@ runs in the library's kernels.
 from __future__ import annotations
 
 import ctypes as C
-import math
+import os
 import time
 
 import numpy as np
@@ -323,3 +323,54 @@ def evaluate(scene, mlp: Mlp, coarse_steps: int = 50, ratio: int = 4, threshold:
         max_check=float(stats.max_check), timed_fallbacks=int(st.fallbacks), **err,
         final_plain=rows[-1][1], final_closure=rows[-1][2])
     return out
+
+
+# ---------------------------------------------------------------- command line
+WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "weights", "closure_mlp.npz")
+
+
+def _main(argv=None) -> None:
+    """python -m phi_eng_b200.closure train [--out PATH] [--iters N] ...
+    python -m phi_eng_b200.closure eval [--weights PATH] [--workload NAME] ..."""
+    import argparse
+    import json
+
+    from . import scenes as S
+
+    ap = argparse.ArgumentParser(prog="python -m phi_eng_b200.closure")
+    sub = ap.add_subparsers(dest="cmd", required=True)
+    t = sub.add_parser("train")
+    t.add_argument("--out", default=WEIGHTS)
+    t.add_argument("--scenes", type=int, default=256)
+    t.add_argument("--samples", type=int, default=40)
+    t.add_argument("--every", type=int, default=50)
+    t.add_argument("--iters", type=int, default=20000)
+    t.add_argument("--batch", type=int, default=65536)
+    t.add_argument("--lr", type=float, default=1e-3)
+    t.add_argument("--seed", type=lambda s: int(s, 0), default=0x5EED)
+    e = sub.add_parser("eval")
+    e.add_argument("--weights", default=WEIGHTS)
+    e.add_argument("--workload", default="dam_break_1m", choices=["dam_break_1m", "dam_break_4k"])
+    e.add_argument("--coarse-steps", type=int, default=50)
+    e.add_argument("--threshold", type=float, default=0.03)
+    e.add_argument("--criterion", choices=["jump", "compression"], default="jump")
+    e.add_argument("--zero", action="store_true", help="evaluate a zero network (no correction)")
+    a = ap.parse_args(argv)
+    if a.cmd == "train":
+        from .batch import batched_scenes
+
+        mlp, info = train_closure(batched_scenes(a.scenes), samples=a.samples, every=a.every, batch=a.batch,
+                                  iters=a.iters, lr=a.lr, seed=a.seed, log=None)
+        os.makedirs(os.path.dirname(os.path.abspath(a.out)), exist_ok=True)
+        mlp.save(a.out, **{k: np.asarray(v) for k, v in info.items()})
+        print(json.dumps(dict(trained=a.out, **info)))
+        return
+    sc = S.dam_break_1m() if a.workload == "dam_break_1m" else S.dam_break_4k()
+    mlp = Mlp() if a.zero else Mlp.load(a.weights)
+    crit = _abi.CLOSURE_JUMP if a.criterion == "jump" else _abi.CLOSURE_COMPRESSION
+    r = evaluate(sc, mlp, coarse_steps=a.coarse_steps, threshold=a.threshold, criterion=crit)
+    print(json.dumps(dict(workload=a.workload, weights=None if a.zero else a.weights, **r)))
+
+
+if __name__ == "__main__":
+    _main()

@@ -706,6 +706,13 @@ int32_t phieng_mlp_train(PhiengMlp* m, const float* x, const float* t, uint32_t 
     if (!mlp_alloc(m, m->loss_hist, iters)) return 0;
     m->loss_cap = iters;
   }
+  {
+    // the partial-gradient buffer is sized here: no allocation may happen
+    // while the iteration graph is being captured
+    uint32_t ctas, rounds;
+    mlp_grid(batch, &ctas, &rounds);
+    if (!ensure_parts(m, ctas)) return 0;
+  }
   const uint32_t t0 = phieng_mlp_step_count(m);
   const float inv_2b = (float)(0.5 / (double)batch);
   // one iteration = tile, Adam, advance; replayed from a graph of up to 32
