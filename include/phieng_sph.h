@@ -304,10 +304,14 @@ int32_t phieng_mlp_train(PhiengMlp* mlp, const float* x, const float* t, uint32_
 /* The pair indices of one minibatch (device idx[batch]). */
 int32_t phieng_mlp_sample_indices(uint32_t npairs, uint32_t batch, uint64_t seed, uint32_t iter, uint32_t* idx,
                                   void* stream);
-/* Training targets (x_fine - x_coarse) * inv_h per particle from two
- * [n][4] states (device). */
-int32_t phieng_mlp_targets(const float* fine, const float* coarse, uint32_t n, float inv_h, float* out,
-                           void* stream);
+/* Add uniform noise in [-amp, amp] to x and y of every particle of a [n][4]
+ * device state (deterministic in seed): perturbed states for training pairs. */
+int32_t phieng_mlp_perturb(float* state, uint32_t n, float amp, uint64_t seed, void* stream);
+/* Training targets per particle from two [n][4] states (device): mode 0
+ * (x_fine - x_coarse) * inv_h, mode 1 (v_fine - v_coarse) * dt * inv_h,
+ * mode 2 their mean (dt = the coarse step). */
+int32_t phieng_mlp_targets(const float* fine, const float* coarse, uint32_t n, float inv_h, float dt, uint32_t mode,
+                           float* out, void* stream);
 
 /* Closure inputs of every particle at the current state for a substep of dt
  * (device feat[n][16], insertion order). The state is unchanged. */
@@ -315,6 +319,7 @@ int32_t phieng_sph_features(World2* world, float dt, float* feat);
 
 #define PHIENG_CLOSURE_JUMP 0u        /* max_i (rho_i after - rho_i before) / rho0 */
 #define PHIENG_CLOSURE_COMPRESSION 1u /* max_i rho_i after / rho0 - 1 */
+#define PHIENG_CLOSURE_GROWTH 2u      /* (max_i rho_i after - max_i rho_i before) / rho0 */
 
 /* Attach a network (null detaches) for phieng_sph_closure_step: each coarse
  * step is one substep of ratio * dt_fine with the network's correction; a
@@ -331,8 +336,9 @@ typedef struct PhiengClosureStats {
   float max_check;       /* largest check seen */
 } PhiengClosureStats;
 
-/* Advance by `coarse_steps` x ratio x dt_fine (a single world, no CFL
- * substeps). stats (may be null) accumulates. 1 ok, 0 on error. */
+/* Advance by `coarse_steps` x ratio x dt_fine (no CFL substeps; on a batch
+ * every scene advances and the check and fallback act on the whole batch).
+ * stats (may be null) accumulates. 1 ok, 0 on error. */
 int32_t phieng_sph_closure_step(World2* world, float dt_fine, uint32_t coarse_steps, PhiengClosureStats* stats);
 
 /* ---- diagnostics used by the parity tests ---- */

@@ -67,6 +67,8 @@ def _load():
         "orc_all_neighbors": (None, [P, U32, U32, C.c_uint32]),
         "orc_cells": (None, [P, I32, I32]),
         "orc_cfl_substeps": (C.c_uint32, [P, C.c_float]),
+        "orc_set_extra_accel": (None, [P, F, C.c_uint32]),
+        "orc_features": (C.c_uint32, [P, C.c_float, F, C.c_uint32]),
         "orc_poly6": (C.c_float, [C.c_float, C.c_float]),
         "orc_spiky": (None, [C.c_float, C.c_float, C.c_float, C.c_float, F]),
         "orc_pressure": (C.c_float, [C.c_float, C.c_float, C.c_float, C.c_float]),
@@ -233,6 +235,20 @@ class OracleWorld:
 
     def cfl_substeps(self, dt: float) -> int:
         return int(self._l.orc_cfl_substeps(self._h, dt))
+
+    # ---- learned-closure hooks ----
+    def features(self, dt: float) -> np.ndarray:
+        """Closure inputs [n][16] at the current state for a substep dt."""
+        n = self.count
+        out = np.zeros((n, 16), np.float32)
+        k = self._l.orc_features(self._h, dt, _fp(out), n)
+        assert k == n
+        return out
+
+    def set_extra_accel(self, a) -> None:
+        """Per-particle acceleration [n][2] added in the next substep's integrate."""
+        a = np.ascontiguousarray(a, dtype=np.float32).reshape(-1, 2)
+        self._l.orc_set_extra_accel(self._h, _fp(a), a.shape[0])
 
 
 # scalar kernels (f32) for the reference's kernel-sanity checks

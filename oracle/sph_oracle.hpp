@@ -168,6 +168,9 @@ class Fluid {
 
   // last-substep scratch exposed for per-pass parity dumps
   std::vector<R> fx, fy;
+  // per-particle acceleration added in the integrate (the learned closure's
+  // correction; empty = none), consumed by the next substep
+  std::vector<R> extra_ax, extra_ay;
 
   // ---- kernels (fluid.rs:265-326) ----
   // poly6: 4/(pi h^8)(h^2-r^2)^3, zero beyond h (fluid.rs:265-273)
@@ -359,6 +362,10 @@ class Fluid {
       R rho_i = rmax(src[i].density, (R)kEps);
       R ax = gx + fx[i] / rho_i;
       R ay = gy + fy[i] / rho_i;
+      if (extra_ax.size() == n) {
+        ax = ax + extra_ax[i];
+        ay = ay + extra_ay[i];
+      }
       R vx = src[i].vx + ax * dt;
       R vy = src[i].vy + ay * dt;
       if (visc > (R)0) {
@@ -604,7 +611,7 @@ class Fluid {
       neighbors_of(pi.x, pi.y, particles, nb);
       const R rho_i = rmax(pi.density, (R)kEps);
       const R q_i = pi.pressure / (rho_i * rho_i);
-      R px = 0, py = 0, div = 0, curl = 0, wsum = 0, m1x = 0, m1y = 0, m2xx = 0, m2xy = 0, m2yy = 0;
+      R px = 0, py = 0, div = 0, curl = 0, wsum = 0, m1x = 0, m1y = 0, m2xx = 0, m2yy = 0, pw = 0;
       uint32_t cnt = 0;
       for (uint32_t j : nb) {
         if (j == i) continue;
@@ -630,8 +637,8 @@ class Fluid {
         m1x = m1x + wx;
         m1y = m1y + wy;
         m2xx = m2xx + wx * dvx;
-        m2xy = m2xy + wx * dvy;
         m2yy = m2yy + wy * dvy;
+        pw = pw + ww * (q_j * rho_j * rho_j);
         cnt++;
       }
       R wd, wnx, wny;
@@ -651,7 +658,7 @@ class Fluid {
       f[8] = m1x * iw * s1;
       f[9] = m1y * iw * s1;
       f[10] = m2xx * iw * s2;
-      f[11] = m2xy * iw * s2;
+      f[11] = kr > (R)0 ? (pi.pressure - pw * iw) / kr : (R)0;
       f[12] = m2yy * iw * s2;
       f[13] = px / rho_i * s3;
       f[14] = py / rho_i * s3;
@@ -666,6 +673,8 @@ class Fluid {
     compute_density_pressure(h);
     compute_forces(h);
     integrate(h, dt, mode);
+    extra_ax.clear();
+    extra_ay.clear();
     boundaries();
     // The trailing rebuild_grid + buoyancy pass (fluid.rs:1102-1135) acts
     // on dynamic bodies only and leaves particle state unchanged.

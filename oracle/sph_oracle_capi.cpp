@@ -379,6 +379,20 @@ uint32_t orc_features(void* h, float dt, float* out, uint32_t max) {
   return r;
 }
 
+// Extra acceleration per particle (insertion order, [n][2]) for the next
+// substep only (the closure's correction).
+void orc_set_extra_accel(void* h, const float* a, uint32_t n) {
+  Orc* o = static_cast<Orc*>(h);
+  DISPATCH(o, {
+    F.extra_ax.assign(n, 0);
+    F.extra_ay.assign(n, 0);
+    for (uint32_t i = 0; i < n; i++) {
+      F.extra_ax[i] = a[2 * i];
+      F.extra_ay[i] = a[2 * i + 1];
+    }
+  });
+}
+
 float orc_poly6(float r2, float h) { return Fluid<float>::poly6(r2, h); }
 void orc_spiky(float rx, float ry, float r, float h, float* out2) {
   Fluid<float>::spiky_grad(rx, ry, r, h, out2[0], out2[1]);

@@ -115,6 +115,7 @@ MLP_NORM = 34
 MLP_FEATURES = 16
 CLOSURE_JUMP = 0
 CLOSURE_COMPRESSION = 1
+CLOSURE_GROWTH = 2
 
 _P = C.c_void_p
 _F = C.POINTER(C.c_float)
@@ -174,7 +175,8 @@ SIGNATURES = {
     "phieng_mlp_grad": (C.c_int32, [_P, _P, _P, C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint32, _F, _F]),
     "phieng_mlp_train": (C.c_int32, [_P, _P, _P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_float, C.c_uint64, _F]),
     "phieng_mlp_sample_indices": (C.c_int32, [C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint32, _P, _P]),
-    "phieng_mlp_targets": (C.c_int32, [_P, _P, C.c_uint32, C.c_float, _P, _P]),
+    "phieng_mlp_targets": (C.c_int32, [_P, _P, C.c_uint32, C.c_float, C.c_float, C.c_uint32, _P, _P]),
+    "phieng_mlp_perturb": (C.c_int32, [_P, C.c_uint32, C.c_float, C.c_uint64, _P]),
     "phieng_sph_features": (C.c_int32, [_P, C.c_float, _P]),
     "phieng_sph_set_closure": (C.c_int32, [_P, _P, C.c_uint32, C.c_float, C.c_uint32]),
     "phieng_sph_closure_step": (C.c_int32, [_P, C.c_float, C.c_uint32, C.POINTER(PhiengClosureStats)]),

@@ -40,6 +40,18 @@ def _fp(a: np.ndarray):
     return a.ctypes.data_as(C.POINTER(C.c_float))
 
 
+CUDA_STREAM_LEGACY = 1  # cudaStreamLegacy: the legacy default stream, named explicitly
+
+
+def torch_stream_handle() -> int:
+    """cudaStream_t of torch's current stream for the library's stream
+    arguments. Torch's default stream has handle 0, which the library reads as
+    "use your own stream"; it is passed as cudaStreamLegacy instead, so the
+    library's work and torch's stay ordered on one stream."""
+    torch = _torch()
+    return torch.cuda.current_stream().cuda_stream or CUDA_STREAM_LEGACY
+
+
 class Mlp:
     """The closure network on the current CUDA device."""
 
@@ -99,7 +111,7 @@ class Mlp:
     # ---- compute (device tensors, on torch's current stream) ----
     def _on_current_stream(self):
         torch = _torch()
-        self._lib.phieng_mlp_set_stream(self._h, C.c_void_p(torch.cuda.current_stream().cuda_stream))
+        self._lib.phieng_mlp_set_stream(self._h, C.c_void_p(torch_stream_handle()))
         return torch
 
     def forward(self, x):
@@ -134,55 +146,168 @@ def sample_indices(npairs: int, batch: int, seed: int, it: int):
     torch = _torch()
     out = torch.empty(batch, dtype=torch.int32, device="cuda")
     lib = _abi.load()
-    if lib.phieng_mlp_sample_indices(npairs, batch, seed, it, out.data_ptr(), None) != 1:
+    if lib.phieng_mlp_sample_indices(npairs, batch, seed, it, out.data_ptr(), C.c_void_p(torch_stream_handle())) != 1:
         raise ValueError("sample_indices")
     torch.cuda.synchronize()
     return out.cpu().numpy().view(np.uint32).astype(np.int64)
 
 
 # ---------------------------------------------------------------- training data
-def generate_pairs(scs, ratio: int = 4, samples: int = 40, every: int = 50, first: int = 50):
+TARGETS = {"position": 0, "velocity": 1, "blend": 2}
+
+
+def _pair(b, w, lib, src, n, ratio, dt, h, x_out, t_out, tmp_c, tmp_f, stream, target=1):
+    """One block of training pairs from state `src` (device [n][4]):
+    features for a coarse step, one plain coarse substep, ratio plain fine
+    substeps, target = (x_fine - x_coarse) / h. Leaves the fine result in
+    tmp_f (and in the world)."""
+    w.set_state_device(src.data_ptr(), n)
+    w.features(ratio * dt, x_out.data_ptr())
+    b.step(ratio * dt, 1)
+    w.get_state_device(tmp_c.data_ptr(), n)
+    w.set_state_device(src.data_ptr(), n)
+    b.step(dt, ratio)
+    w.get_state_device(tmp_f.data_ptr(), n)
+    if lib.phieng_mlp_targets(tmp_f.data_ptr(), tmp_c.data_ptr(), n, 1.0 / h, ratio * dt, target,
+                              t_out.data_ptr(), C.c_void_p(stream)) != 1:
+        raise RuntimeError("phieng_mlp_targets")
+
+
+def generate_pairs(scs, ratio: int = 4, samples: int = 40, every: int = 50, first: int = 50,
+                   noise=(0.0, 0.1), mlp=None, rollout: int = 0, seed: int = 0x401,
+                   target: str = "position"):
     """(features, targets) on the device from the plain GPU step.
 
-    The scenes advance together as one batch with the plain fine step dt
-    (the scenes' own). At `samples` instants (after `first` steps, then every
-    `every` steps) the state S is saved and
-      features  = closure inputs at S for a coarse step ratio * dt
-      coarse    = one plain substep of ratio * dt from S
-      fine      = ratio plain substeps of dt from S (the trajectory continues here)
-      target    = (x_fine - x_coarse) / h   per particle
-    """
+    The scenes advance together as one batch along the plain fine trajectory
+    (step dt, the scenes' own). At `samples` instants (after `first` steps,
+    then every `every` steps), with S the state there, pairs come from
+      - S with uniform position noise of each amplitude in `noise` (units of
+        h; 0 = S itself): the fine solver's response to perturbed states is
+        what keeps the corrected coarse step stable (noise injection);
+      - if `mlp` is given, the states the closure itself reaches from S in
+        `rollout` coarse steps (data aggregation on the closure's own
+        distribution).
+    Every target is the plain method's difference between ratio fine
+    substeps and one plain substep of ratio * dt from the same state, as the
+    displacement correction in units of h: "position" (x_fine - x_coarse) / h,
+    "velocity" (v_fine - v_coarse) ratio dt / h, or "blend" their mean."""
     from .batch import Batch
 
     torch = _torch()
     lib = _abi.load()
+    tmode = TARGETS[target]
     dt = scs[0].dt
     h = float(scs[0].config.smoothing_length)
     assert all(s.dt == dt and float(s.config.smoothing_length) == h for s in scs)
     b = Batch.from_scenes(scs)
     w = b.world
     n = sum(s.n for s in scs)
-    S = torch.empty((n, 4), dtype=torch.float32, device="cuda")
-    Cs = torch.empty_like(S)
-    F = torch.empty_like(S)
-    X = torch.empty((samples * n, NFEAT), dtype=torch.float32, device="cuda")
-    T = torch.empty((samples * n, 2), dtype=torch.float32, device="cuda")
-    ws = torch.cuda.current_stream().cuda_stream
+    per = len(noise) + (rollout if mlp is not None else 0)
+    st = [torch.empty((n, 4), dtype=torch.float32, device="cuda") for _ in range(6)]
+    S, P, V, Cs, F, Fc = st
+    X = torch.empty((samples * per * n, NFEAT), dtype=torch.float32, device="cuda")
+    T = torch.empty((samples * per * n, 2), dtype=torch.float32, device="cuda")
+    ws = torch_stream_handle()
     w.set_stream(ws)
     b.step(dt, first)
+    slot = 0
+
+    def blk(k):
+        return X[k * n:(k + 1) * n], T[k * n:(k + 1) * n]
+
     for k in range(samples):
         if k:
             b.step(dt, every)
         w.get_state_device(S.data_ptr(), n)
-        w.features(ratio * dt, X[k * n:(k + 1) * n].data_ptr())
-        b.step(ratio * dt, 1)
-        w.get_state_device(Cs.data_ptr(), n)
-        w.set_state_device(S.data_ptr(), n)
-        b.step(dt, ratio)
-        w.get_state_device(F.data_ptr(), n)
-        if lib.phieng_mlp_targets(F.data_ptr(), Cs.data_ptr(), n, 1.0 / h, T[k * n:(k + 1) * n].data_ptr(),
-                                  C.c_void_p(ws)) != 1:
-            raise RuntimeError("phieng_mlp_targets")
+        have_clean = False
+        for sig in noise:
+            P.copy_(S)
+            if sig > 0 and lib.phieng_mlp_perturb(P.data_ptr(), n, float(sig) * h, seed ^ (slot * 0x9E37 + 1),
+                                                   C.c_void_p(ws)) != 1:
+                raise RuntimeError("phieng_mlp_perturb")
+            _pair(b, w, lib, P, n, ratio, dt, h, *blk(slot), Cs, F, ws, tmode)
+            if sig == 0:
+                Fc.copy_(F)
+                have_clean = True
+            slot += 1
+        if mlp is not None and rollout:
+            w.set_closure(mlp, ratio, 1e30, _abi.CLOSURE_JUMP)
+            V.copy_(S)
+            for r in range(rollout):
+                w.set_state_device(V.data_ptr(), n)
+                w.closure_step(dt, 1)
+                w.get_state_device(V.data_ptr(), n)
+                _pair(b, w, lib, V, n, ratio, dt, h, *blk(slot), Cs, F, ws, tmode)
+                slot += 1
+            w.set_closure(None)
+        if not have_clean:
+            w.set_state_device(S.data_ptr(), n)
+            b.step(dt, ratio)
+            w.get_state_device(Fc.data_ptr(), n)
+        w.set_state_device(Fc.data_ptr(), n)  # the trajectory continues on the plain fine path
+    w.sync()
+    w.set_stream(None)
+    b.close()
+    return X, T
+
+
+def generate_tracking_pairs(scs, mlp, ratio: int = 4, samples: int = 20, rollout: int = 4, every: int = 50,
+                            first: int = 50):
+    """Pairs along the closure's own rollouts, with the plain fine trajectory
+    as the expert (data aggregation, "DAgger").
+
+    At `samples` instants of the plain fine trajectory, with S the state
+    there, the plain fine run is advanced ratio * rollout substeps, keeping
+    F_1 .. F_rollout (one every ratio substeps), and the closure rolls out
+    from S: at its r-th state V_r the pair is
+      features  = closure inputs at V_r
+      target    = (x(F_{r+1}) - x_coarse(V_r)) / h
+    with x_coarse(V_r) one plain substep of ratio * dt from V_r: the
+    displacement correction that would put each particle where the fine
+    trajectory has it, so errors the closure made earlier are corrected
+    rather than amplified."""
+    from .batch import Batch
+
+    torch = _torch()
+    lib = _abi.load()
+    dt = scs[0].dt
+    h = float(scs[0].config.smoothing_length)
+    b = Batch.from_scenes(scs)
+    w = b.world
+    n = sum(s.n for s in scs)
+    S = torch.empty((n, 4), dtype=torch.float32, device="cuda")
+    V = torch.empty_like(S)
+    Cs = torch.empty_like(S)
+    Fs = [torch.empty_like(S) for _ in range(rollout)]
+    X = torch.empty((samples * rollout * n, NFEAT), dtype=torch.float32, device="cuda")
+    T = torch.empty((samples * rollout * n, 2), dtype=torch.float32, device="cuda")
+    ws = torch_stream_handle()
+    w.set_stream(ws)
+    b.step(dt, first)
+    slot = 0
+    for k in range(samples):
+        if k:
+            b.step(dt, max(every - ratio * rollout, 0))
+        w.get_state_device(S.data_ptr(), n)
+        for r in range(rollout):
+            b.step(dt, ratio)
+            w.get_state_device(Fs[r].data_ptr(), n)
+        V.copy_(S)
+        w.set_closure(mlp, ratio, 1e30, _abi.CLOSURE_JUMP)
+        for r in range(rollout):
+            w.set_state_device(V.data_ptr(), n)
+            w.features(ratio * dt, X[slot * n:(slot + 1) * n].data_ptr())
+            b.step(ratio * dt, 1)
+            w.get_state_device(Cs.data_ptr(), n)
+            if lib.phieng_mlp_targets(Fs[r].data_ptr(), Cs.data_ptr(), n, 1.0 / h, ratio * dt, TARGETS["position"],
+                                      T[slot * n:(slot + 1) * n].data_ptr(), C.c_void_p(ws)) != 1:
+                raise RuntimeError("phieng_mlp_targets")
+            slot += 1
+            w.set_state_device(V.data_ptr(), n)
+            w.closure_step(dt, 1)
+            w.get_state_device(V.data_ptr(), n)
+        w.set_closure(None)
+        w.set_state_device(Fs[-1].data_ptr(), n)  # continue on the fine trajectory
     w.sync()
     w.set_stream(None)
     b.close()
@@ -205,15 +330,19 @@ def normalisation(X, T, sample: int = 1 << 20, seed: int = 7) -> np.ndarray:
 
 
 def train_closure(scs=None, ratio: int = 4, samples: int = 40, every: int = 50, batch: int = 65536,
-                  iters: int = 20000, lr: float = 1e-3, seed: int = 0x5EED, log=print):
+                  iters: int = 20000, lr: float = 1e-3, seed: int = 0x5EED, noise=(0.0, 0.1),
+                  dagger_iters: int = 0, dagger_samples: int = 20, rollout: int = 4, target: str = "position",
+                  track_rounds: int = 0, track_iters: int = 5000, log=print):
     """Generate pairs on the batched scenes (the 256-scene slice of the batched
-    workload by default) and train a network; returns (mlp, info)."""
+    workload by default) and train a network; with dagger_iters > 0, a second
+    round adds pairs from the trained closure's own rollouts and continues
+    training on both sets. Returns (mlp, info)."""
     from .batch import batched_scenes
 
     torch = _torch()
     scs = scs if scs is not None else batched_scenes(256)
     t0 = time.perf_counter()
-    X, T = generate_pairs(scs, ratio=ratio, samples=samples, every=every)
+    X, T = generate_pairs(scs, ratio=ratio, samples=samples, every=every, noise=noise, target=target)
     torch.cuda.synchronize()
     t1 = time.perf_counter()
     mlp = Mlp(seed)
@@ -225,7 +354,29 @@ def train_closure(scs=None, ratio: int = 4, samples: int = 40, every: int = 50, 
     t2 = time.perf_counter()
     info = dict(pairs=int(X.shape[0]), scenes=len(scs), gen_s=t1 - t0, train_s=t2 - t1,
                 loss_first=float(hist[:100].mean()), loss_last=float(hist[-100:].mean()), iters=iters,
-                batch=batch, lr=lr, ratio=ratio)
+                batch=batch, lr=lr, ratio=ratio, noise=list(noise), target=target)
+    if dagger_iters > 0:
+        X2, T2 = generate_pairs(scs, ratio=ratio, samples=dagger_samples, every=every * samples // dagger_samples,
+                                noise=(0.0,), mlp=mlp, rollout=rollout, seed=seed ^ 0xDA66, target=target)
+        X = torch.cat([X, X2])
+        T = torch.cat([T, T2])
+        del X2, T2
+        # the normalisation stays: the network's input and output scales are already learnt
+        hist2 = mlp.train(X, T, batch=batch, iters=dagger_iters, lr=lr, seed=seed ^ 0x5A5A)
+        torch.cuda.synchronize()
+        info.update(dagger_pairs=int(X.shape[0]) - info["pairs"], dagger_iters=dagger_iters, rollout=rollout,
+                    dagger_loss_first=float(hist2[:100].mean()), dagger_loss_last=float(hist2[-100:].mean()),
+                    total_s=time.perf_counter() - t0)
+    for rnd in range(track_rounds):
+        X2, T2 = generate_tracking_pairs(scs, mlp, ratio=ratio, samples=dagger_samples, rollout=rollout,
+                                         every=max(every, ratio * rollout))
+        X = torch.cat([X, X2])
+        T = torch.cat([T, T2])
+        del X2, T2
+        hist2 = mlp.train(X, T, batch=batch, iters=track_iters, lr=lr, seed=seed ^ (0x7AC0 + rnd))
+        info[f"track{rnd}_loss"] = [float(hist2[:100].mean()), float(hist2[-100:].mean())]
+    if track_rounds:
+        info.update(track_rounds=track_rounds, track_iters=track_iters, pairs_total=int(X.shape[0]))
     if log:
         log(f"closure training: {info}")
     del X, T
@@ -233,6 +384,42 @@ def train_closure(scs=None, ratio: int = 4, samples: int = 40, every: int = 50, 
 
 
 # ---------------------------------------------------------------- evaluation
+def one_step_errors(scene, mlp: Mlp, warm: int = 100, ratio: int = 4, noise: float = 0.0, seed: int = 1):
+    """RMS position error (units of h) after one coarse step of ratio * dt,
+    against ratio plain fine substeps from the same state, for the plain
+    coarse step and for the closure's coarse step. The state is the scene
+    after `warm` fine substeps, its positions optionally perturbed by uniform
+    noise of amplitude noise * h."""
+    dt = scene.dt
+    h = float(scene.config.smoothing_length)
+    ref = world_from_scene(scene)
+    ref.step_n(dt, warm)
+    s0 = ref.fluid.particles.copy()
+    if noise > 0:
+        rng = np.random.default_rng(seed)
+        s0[:, :2] += (rng.uniform(-1.0, 1.0, s0[:, :2].shape) * noise * h).astype(np.float32)
+        ref.fluid.set_state(s0)
+    ref.step_n(dt, ratio)
+    fine = ref.fluid.particles.copy()
+    plain = world_from_scene(scene)
+    plain.fluid.set_state(s0)
+    plain.step(ratio * dt)
+    clo = world_from_scene(scene)
+    clo.fluid.set_state(s0)
+    clo.set_closure(mlp, ratio, float("inf"), _abi.CLOSURE_JUMP)
+    clo.closure_step(dt, 1)
+
+    def rms(st):
+        d = (st[:, :2].astype(np.float64) - fine[:, :2]) / h
+        return float(np.sqrt(np.mean(np.sum(d * d, 1))))
+
+    out = rms(plain.fluid.particles), rms(clo.fluid.particles)
+    for w in (ref, plain, clo):
+        w.close()
+    return out
+
+
+
 def fluid_metrics(w: World2, mass: float, rho0: float):
     """Dam front (max x), kinetic energy sum(m |v|^2 / 2) and density
     deviation statistics of the current state (density recomputed for it)."""
@@ -316,7 +503,8 @@ def evaluate(scene, mlp: Mlp, coarse_steps: int = 50, ratio: int = 4, threshold:
     sim = coarse_steps * ratio * dt
     out = dict(
         particles=scene.n, coarse_steps=coarse_steps, ratio=ratio, dt_fine=dt, threshold=threshold,
-        criterion="jump" if criterion == _abi.CLOSURE_JUMP else "compression",
+        criterion={_abi.CLOSURE_JUMP: "jump", _abi.CLOSURE_COMPRESSION: "compression",
+                   _abi.CLOSURE_GROWTH: "growth"}[criterion],
         plain_ms=t_plain, closure_ms=t_clo,
         plain_sim_s_per_wall_s=sim / (t_plain / 1000.0), closure_sim_s_per_wall_s=sim / (t_clo / 1000.0),
         speedup=t_plain / t_clo, accepted=int(stats.accepted), fallbacks=int(stats.fallbacks),
@@ -348,26 +536,33 @@ def _main(argv=None) -> None:
     t.add_argument("--batch", type=int, default=65536)
     t.add_argument("--lr", type=float, default=1e-3)
     t.add_argument("--seed", type=lambda s: int(s, 0), default=0x5EED)
+    t.add_argument("--noise", default="0,0.1", help="position noise amplitudes in units of h")
+    t.add_argument("--dagger-iters", type=int, default=0)
+    t.add_argument("--rollout", type=int, default=4)
+    t.add_argument("--target", choices=list(TARGETS), default="position")
+    t.add_argument("--track-rounds", type=int, default=0)
     e = sub.add_parser("eval")
     e.add_argument("--weights", default=WEIGHTS)
     e.add_argument("--workload", default="dam_break_1m", choices=["dam_break_1m", "dam_break_4k"])
     e.add_argument("--coarse-steps", type=int, default=50)
     e.add_argument("--threshold", type=float, default=0.03)
-    e.add_argument("--criterion", choices=["jump", "compression"], default="jump")
+    e.add_argument("--criterion", choices=["jump", "compression", "growth"], default="jump")
     e.add_argument("--zero", action="store_true", help="evaluate a zero network (no correction)")
     a = ap.parse_args(argv)
     if a.cmd == "train":
         from .batch import batched_scenes
 
+        noise = tuple(float(v) for v in a.noise.split(","))
         mlp, info = train_closure(batched_scenes(a.scenes), samples=a.samples, every=a.every, batch=a.batch,
-                                  iters=a.iters, lr=a.lr, seed=a.seed, log=None)
+                                  iters=a.iters, lr=a.lr, seed=a.seed, noise=noise, dagger_iters=a.dagger_iters,
+                                  rollout=a.rollout, target=a.target, track_rounds=a.track_rounds, log=None)
         os.makedirs(os.path.dirname(os.path.abspath(a.out)), exist_ok=True)
         mlp.save(a.out, **{k: np.asarray(v) for k, v in info.items()})
         print(json.dumps(dict(trained=a.out, **info)))
         return
     sc = S.dam_break_1m() if a.workload == "dam_break_1m" else S.dam_break_4k()
     mlp = Mlp() if a.zero else Mlp.load(a.weights)
-    crit = _abi.CLOSURE_JUMP if a.criterion == "jump" else _abi.CLOSURE_COMPRESSION
+    crit = {"jump": _abi.CLOSURE_JUMP, "compression": _abi.CLOSURE_COMPRESSION, "growth": _abi.CLOSURE_GROWTH}[a.criterion]
     r = evaluate(sc, mlp, coarse_steps=a.coarse_steps, threshold=a.threshold, criterion=crit)
     print(json.dumps(dict(workload=a.workload, weights=None if a.zero else a.weights, **r)))
 

@@ -260,10 +260,11 @@ __device__ __forceinline__ void walls(float& x, float& y, float& vx, float& vy,
 //   pressure force   P -= grad * (m_j * (q_i + q_j)),  q = p / rho^2
 //   divergence       D += V_j * (dv . grad)
 //   curl (z)         C += V_j * (dv.x grad.y - dv.y grad.x)
-//   kernel moments   S += V_j w, M1 += V_j w dv, M2 += V_j w dv dv^T
+//   kernel moments   S += V_j w, M1 += V_j w dv, M2 += V_j w (dv.x^2, dv.y^2)
+//   pressure mean    Q += V_j w p_j,  p_j = (q_j rho_j) rho_j
 struct FeatAcc {
   float px = 0.0f, py = 0.0f, div = 0.0f, curl = 0.0f;
-  float wsum = 0.0f, m1x = 0.0f, m1y = 0.0f, m2xx = 0.0f, m2xy = 0.0f, m2yy = 0.0f;
+  float wsum = 0.0f, m1x = 0.0f, m1y = 0.0f, m2xx = 0.0f, m2yy = 0.0f, pw = 0.0f;
   uint32_t cnt = 0;
 };
 
@@ -281,8 +282,8 @@ __device__ __forceinline__ void feat_pair(FeatAcc& a, float gxx, float gyy, floa
   a.m1x = __fadd_rn(a.m1x, wx);
   a.m1y = __fadd_rn(a.m1y, wy);
   a.m2xx = __fadd_rn(a.m2xx, __fmul_rn(wx, dvx));
-  a.m2xy = __fadd_rn(a.m2xy, __fmul_rn(wx, dvy));
   a.m2yy = __fadd_rn(a.m2yy, __fmul_rn(wy, dvy));
+  a.pw = __fadd_rn(a.pw, __fmul_rn(ww, __fmul_rn(__fmul_rn(q_j, rho_j), rho_j)));
   a.cnt++;
 }
 
@@ -348,7 +349,9 @@ __device__ __forceinline__ void wall_feature(float x, float y, const DevBody* __
 // The 16 closure inputs of one particle for a coarse step of P.dt:
 //   0 rho/rho0 - 1          1 p / (k rho0)          2 D dt       3 C dt
 //   4 neighbours / 16       5 wall distance / h     6, 7 wall normal
-//   8, 9 M1/S (dt/h)        10..12 M2/S (dt/h)^2 (xx, xy, yy)
+//   8, 9 M1/S (dt/h)        10, 12 M2/S (dt/h)^2 (xx, yy)
+//   11 (p - Q/S) / (k rho0) (pressure deviation from the neighbour mean:
+//      near zero for a smooth pressure field, large for particle-scale noise)
 //   13, 14 (P / rho) dt^2/h (pressure displacement over the step)
 //   15 |v| dt / h
 __device__ __forceinline__ void feat_finish(const FeatAcc& a, float dens, float rho_i, float p, float r0, float vx,
@@ -373,7 +376,7 @@ __device__ __forceinline__ void feat_finish(const FeatAcc& a, float dens, float 
   f[8] = __fmul_rn(__fmul_rn(a.m1x, iw), s1);
   f[9] = __fmul_rn(__fmul_rn(a.m1y, iw), s1);
   f[10] = __fmul_rn(__fmul_rn(a.m2xx, iw), s2);
-  f[11] = __fmul_rn(__fmul_rn(a.m2xy, iw), s2);
+  f[11] = kr > 0.0f ? __fdiv_rn(__fsub_rn(p, __fmul_rn(a.pw, iw)), kr) : 0.0f;
   f[12] = __fmul_rn(__fmul_rn(a.m2yy, iw), s2);
   f[13] = __fmul_rn(__fdiv_rn(a.px, rho_i), s3);
   f[14] = __fmul_rn(__fdiv_rn(a.py, rho_i), s3);

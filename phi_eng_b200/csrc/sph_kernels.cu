@@ -527,7 +527,7 @@ __global__ void __launch_bounds__(256) k_force_integrate(
 // accumulates the 16 closure features; each warp then runs the closure
 // network on its 32 particles on the tensor cores (two 16-row tiles) and the
 // integrate adds the predicted acceleration correction
-//   a_corr = y * out_scale * (h / dt^2)
+//   a_corr = y * out_scale * (h / dt^2)   (h, dt of the particle's scene)
 // (the network predicts the displacement correction over the coarse step in
 // units of h). It also keeps the pre-step state and density by id for the
 // fallback and the density-jump check.
@@ -600,8 +600,9 @@ __global__ void __launch_bounds__(256, 3) k_force_closure(
     }
     __syncwarp();
     if (!active) return;
-    const float cx = __fmul_rn(__fmul_rn(ys[2 * lane], sm.norm[2 * kFeat]), io.acc_scale);
-    const float cy = __fmul_rn(__fmul_rn(ys[2 * lane + 1], sm.norm[2 * kFeat + 1]), io.acc_scale);
+    const float acc_scale = __fdiv_rn(P.hk, __fmul_rn(P.dt, P.dt));  // h / dt^2 of this particle's scene
+    const float cx = __fmul_rn(__fmul_rn(ys[2 * lane], sm.norm[2 * kFeat]), acc_scale);
+    const float cy = __fmul_rn(__fmul_rn(ys[2 * lane + 1], sm.norm[2 * kFeat + 1]), acc_scale);
     io.save[id] = make_float4(pi.x, pi.y, vi.x, vi.y);
     io.rho_prev[id] = dqi.x;
     const float ax = __fadd_rn(__fadd_rn(P.gx, __fdiv_rn(fx, rho_i)), cx);
@@ -610,30 +611,36 @@ __global__ void __launch_bounds__(256, 3) k_force_closure(
   }
 }
 
-// Density check of an accepted-or-not coarse step, over the new sorted state
-// (after its density pass): criterion 0 = the largest per-particle density
-// increase over the step, max_i (rho'_i - rho_i) / rho0; criterion 1 = the
-// largest compression, max_i (rho'_i / rho0 - 1). Negative values count as 0;
-// a NaN counts as +inf. Result: float bits, atomicMax into *out (>= 0, so the
-// bit order is the value order and the maximum is order independent).
+// Density checks of a coarse step, over the new sorted state after its
+// density pass, each as a maximum over particles (negative values count as
+// 0, a NaN as +inf): out[0] = largest per-particle density increase over the
+// step, (rho'_i - rho_i) / rho0; out[1] = largest compression after the step,
+// rho'_i / rho0 - 1; out[2] = largest compression before it. Float bits,
+// atomicMax (all values >= 0, so the bit order is the value order and the
+// maxima do not depend on the order of the atomics).
 template <bool PHASE, bool BATCH>
 __global__ void __launch_bounds__(256) k_closure_check(const float2* __restrict__ sdq, const uint32_t* __restrict__ sid,
                                                        const uint8_t* __restrict__ sphase, uint32_t n, StepParams P0,
                                                        BatchTab bt, const float* __restrict__ rho_prev,
-                                                       uint32_t criterion, unsigned int* __restrict__ out) {
+                                                       unsigned int* __restrict__ out) {
   const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-  float v = 0.0f;
+  float v[3] = {0.0f, 0.0f, 0.0f};
   if (s < n) {
     const StepParams& P = scene_params<BATCH>(P0, bt.ptab, BATCH ? bt.sscene[s] : 0u);
     const uint32_t ph = PHASE ? min((uint32_t)sphase[s], 3u) : P.uniform_phase;
     const float r0 = fmaxf(P.rest[ph], kEps);
-    const float d = sdq[s].x;
-    const float j = criterion == 0 ? __fdiv_rn(__fsub_rn(d, rho_prev[sid[s]]), r0) : __fsub_rn(__fdiv_rn(d, r0), 1.0f);
-    v = (j != j) ? __int_as_float(0x7f800000) : fmaxf(j, 0.0f);
+    const float d = sdq[s].x, d0 = rho_prev[sid[s]];
+    const float q[3] = {__fdiv_rn(__fsub_rn(d, d0), r0), __fsub_rn(__fdiv_rn(d, r0), 1.0f),
+                        __fsub_rn(__fdiv_rn(d0, r0), 1.0f)};
+#pragma unroll
+    for (int c = 0; c < 3; c++) v[c] = (q[c] != q[c]) ? __int_as_float(0x7f800000) : fmaxf(q[c], 0.0f);
   }
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xFFFFFFFFu, v, o));
-  if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(v));
+  for (int c = 0; c < 3; c++) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[c] = fmaxf(v[c], __shfl_xor_sync(0xFFFFFFFFu, v[c], o));
+    if ((threadIdx.x & 31) == 0) atomicMax(&out[c], __float_as_uint(v[c]));
+  }
 }
 
 // ---------------------------------------------------------------- helpers
@@ -838,17 +845,17 @@ void enqueue_closure_force(const FluidBufs& b, uint32_t n, const StepParams& P, 
 }
 
 void enqueue_closure_check(const FluidBufs& b, uint32_t n, const StepParams& P, const float* rho_prev,
-                           uint32_t criterion, unsigned int* out, cudaStream_t st) {
-  cudaMemsetAsync(out, 0, sizeof(unsigned int), st);
+                           unsigned int* out, cudaStream_t st) {
+  cudaMemsetAsync(out, 0, 3 * sizeof(unsigned int), st);
   if (n == 0) return;
   const bool ph = (P.flags & F_PHASE) != 0, bat = b.batch.ptab != nullptr;
   const uint32_t g = cdiv(n, 256);
   if (bat) {
-    if (ph) k_closure_check<true, true><<<g, 256, 0, st>>>(b.sdq, b.sid, b.sphase, n, P, b.batch, rho_prev, criterion, out);
-    else k_closure_check<false, true><<<g, 256, 0, st>>>(b.sdq, b.sid, b.sphase, n, P, b.batch, rho_prev, criterion, out);
+    if (ph) k_closure_check<true, true><<<g, 256, 0, st>>>(b.sdq, b.sid, b.sphase, n, P, b.batch, rho_prev, out);
+    else k_closure_check<false, true><<<g, 256, 0, st>>>(b.sdq, b.sid, b.sphase, n, P, b.batch, rho_prev, out);
   } else {
-    if (ph) k_closure_check<true, false><<<g, 256, 0, st>>>(b.sdq, b.sid, b.sphase, n, P, b.batch, rho_prev, criterion, out);
-    else k_closure_check<false, false><<<g, 256, 0, st>>>(b.sdq, b.sid, b.sphase, n, P, b.batch, rho_prev, criterion, out);
+    if (ph) k_closure_check<true, false><<<g, 256, 0, st>>>(b.sdq, b.sid, b.sphase, n, P, b.batch, rho_prev, out);
+    else k_closure_check<false, false><<<g, 256, 0, st>>>(b.sdq, b.sid, b.sphase, n, P, b.batch, rho_prev, out);
   }
 }
 

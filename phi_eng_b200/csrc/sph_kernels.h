@@ -75,12 +75,11 @@ void enqueue_force_integrate(const FluidBufs& b, uint32_t n, const StepParams& P
 
 // Closure pass buffers: features (id order, 16 per particle) for the
 // features mode; pre-step state and density (id order) kept by the closure
-// step; acc_scale = h / dt^2 turns the network output into an acceleration.
+// step.
 struct ClosureIO {
   float* feat = nullptr;
   float4* save = nullptr;
   float* rho_prev = nullptr;
-  float acc_scale = 0.0f;
 };
 
 // Closure features of every particle for a coarse step of P.dt (after the
@@ -93,11 +92,12 @@ void enqueue_closure_features(const FluidBufs& b, uint32_t n, const StepParams& 
 void enqueue_closure_force(const FluidBufs& b, uint32_t n, const StepParams& P, const MlpDev& mlp,
                            const ClosureIO& io, cudaStream_t st);
 
-// Density check after the coarse step's new state was sorted and its density
-// computed (criterion 0: largest increase over the step; 1: largest
-// compression), as float bits into *out (zeroed first).
+// Density checks after the coarse step's new state was sorted and its density
+// computed, into out[0..2] (zeroed first): largest per-particle increase over
+// the step, largest compression after it, largest compression before it
+// (relative to the rest density, float bits).
 void enqueue_closure_check(const FluidBufs& b, uint32_t n, const StepParams& P, const float* rho_prev,
-                           uint32_t criterion, unsigned int* out, cudaStream_t st);
+                           unsigned int* out, cudaStream_t st);
 
 // Scatter the sorted density / pressure back to id order.
 void enqueue_unsort_dp(const FluidBufs& b, uint32_t n, float* dens, float* pres, cudaStream_t st);

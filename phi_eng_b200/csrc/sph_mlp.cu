@@ -463,12 +463,39 @@ __global__ void k_mlp_indices(uint64_t seed, uint32_t iter, uint32_t batch, uint
   if (k < batch) out[k] = sample_index(seed, iter, k, npairs);
 }
 
+// Training target per particle from the fine and the coarse state:
+// mode 0 (position) (x_f - x_c) / h; mode 1 (velocity) (v_f - v_c) dt / h,
+// the displacement the velocity difference makes over one coarse step;
+// mode 2 the mean of the two.
 __global__ void k_mlp_targets(const float4* __restrict__ fine, const float4* __restrict__ coarse, uint32_t n,
-                              float inv_h, float2* __restrict__ out) {
+                              float inv_h, float dt, uint32_t mode, float2* __restrict__ out) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const float4 a = fine[i], b = coarse[i];
-  out[i] = make_float2(__fmul_rn(__fsub_rn(a.x, b.x), inv_h), __fmul_rn(__fsub_rn(a.y, b.y), inv_h));
+  const float px = __fmul_rn(__fsub_rn(a.x, b.x), inv_h), py = __fmul_rn(__fsub_rn(a.y, b.y), inv_h);
+  const float s = __fmul_rn(dt, inv_h);
+  const float vx = __fmul_rn(__fsub_rn(a.z, b.z), s), vy = __fmul_rn(__fsub_rn(a.w, b.w), s);
+  if (mode == 0)
+    out[i] = make_float2(px, py);
+  else if (mode == 1)
+    out[i] = make_float2(vx, vy);
+  else
+    out[i] = make_float2(__fmul_rn(0.5f, __fadd_rn(px, vx)), __fmul_rn(0.5f, __fadd_rn(py, vy)));
+}
+
+// Uniform position noise in [-amp, amp] per coordinate, from mix64 of
+// (seed, particle, coordinate): the perturbed states the training pairs are
+// also taken from (noise injection, Sanchez-Gonzalez et al. 2020).
+__global__ void k_mlp_perturb(float4* __restrict__ state, uint32_t n, float amp, uint64_t seed) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint64_t hx = mix64(seed ^ (2ull * i)), hy = mix64(seed ^ (2ull * i + 1ull));
+  const float ux = __fmul_rn((float)(uint32_t)(hx >> 40), 1.0f / 16777216.0f);  // [0, 1)
+  const float uy = __fmul_rn((float)(uint32_t)(hy >> 40), 1.0f / 16777216.0f);
+  float4 s = state[i];
+  s.x = __fadd_rn(s.x, __fmul_rn(amp, __fsub_rn(__fmul_rn(2.0f, ux), 1.0f)));
+  s.y = __fadd_rn(s.y, __fmul_rn(amp, __fsub_rn(__fmul_rn(2.0f, uy), 1.0f)));
+  state[i] = s;
 }
 
 inline uint32_t cdiv(uint32_t a, uint32_t b) { return (a + b - 1) / b; }
@@ -769,12 +796,20 @@ int32_t phieng_mlp_sample_indices(uint32_t npairs, uint32_t batch, uint64_t seed
   return cudaGetLastError() == cudaSuccess ? 1 : 0;
 }
 
-int32_t phieng_mlp_targets(const float* fine, const float* coarse, uint32_t n, float inv_h, float* out, void* stream) {
-  if (n && (!fine || !coarse || !out)) return 0;
+int32_t phieng_mlp_perturb(float* state, uint32_t n, float amp, uint64_t seed, void* stream) {
+  if (n && !state) return 0;
+  if (n == 0) return 1;
+  k_mlp_perturb<<<cdiv(n, 256), 256, 0, (cudaStream_t)stream>>>(reinterpret_cast<float4*>(state), n, amp, seed);
+  return cudaGetLastError() == cudaSuccess ? 1 : 0;
+}
+
+int32_t phieng_mlp_targets(const float* fine, const float* coarse, uint32_t n, float inv_h, float dt, uint32_t mode,
+                           float* out, void* stream) {
+  if ((n && (!fine || !coarse || !out)) || mode > 2) return 0;
   if (n == 0) return 1;
   k_mlp_targets<<<cdiv(n, 256), 256, 0, (cudaStream_t)stream>>>(reinterpret_cast<const float4*>(fine),
                                                                  reinterpret_cast<const float4*>(coarse), n, inv_h,
-                                                                 reinterpret_cast<float2*>(out));
+                                                                 dt, mode, reinterpret_cast<float2*>(out));
   return cudaGetLastError() == cudaSuccess ? 1 : 0;
 }
 

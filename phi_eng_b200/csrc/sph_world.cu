@@ -738,7 +738,6 @@ void enqueue_sort_density(World2* w, const StepParams& P) {
 bool run_coarse(World2* w, const StepParams& P, const MlpDev& mlp, const ClosureIO& io) {
   std::string sig((const char*)&P, sizeof(P));
   sig.append((const char*)&w->n, sizeof(w->n));
-  sig.append((const char*)&w->closure_criterion, sizeof(w->closure_criterion));
   sig.append((const char*)&mlp, sizeof(mlp));
   sig.append((const char*)&io, sizeof(io));
   if (!w->cexec || sig != w->csig) {
@@ -750,7 +749,7 @@ bool run_coarse(World2* w, const StepParams& P, const MlpDev& mlp, const Closure
     enqueue_closure_force(w->d, w->n, P, mlp, io, w->own_stream);
     enqueue_sort_and_ranges(w->d, w->n, P, true, w->own_stream);
     enqueue_density(w->d, w->n, P, w->own_stream);
-    enqueue_closure_check(w->d, w->n, P, io.rho_prev, w->closure_criterion, w->d.scalar + 4, w->own_stream);
+    enqueue_closure_check(w->d, w->n, P, io.rho_prev, w->d.scalar + 4, w->own_stream);
     cudaError_t r = cudaStreamEndCapture(w->own_stream, &g);
     if (!cuda_ok(w, r, "end capture")) return false;
     r = cudaGraphInstantiate(&w->cexec, g, 0);
@@ -1180,7 +1179,7 @@ int32_t phieng_sph_features(World2* w, float dt, float* feat) {
 }
 
 int32_t phieng_sph_set_closure(World2* w, PhiengMlp* mlp, uint32_t ratio, float threshold, uint32_t criterion) {
-  if (!w || w->is_batch() || ratio < 1 || !(threshold >= 0.0f) || criterion > PHIENG_CLOSURE_COMPRESSION) return 0;
+  if (!w || ratio < 1 || !(threshold >= 0.0f) || criterion > PHIENG_CLOSURE_GROWTH) return 0;
   if (mlp && phieng_mlp_status(mlp) != PHIENG_SPH_OK) return 0;
   w->closure = mlp;
   w->closure_ratio = ratio;
@@ -1190,31 +1189,36 @@ int32_t phieng_sph_set_closure(World2* w, PhiengMlp* mlp, uint32_t ratio, float 
 }
 
 int32_t phieng_sph_closure_step(World2* w, float dt_fine, uint32_t coarse_steps, PhiengClosureStats* stats) {
-  if (!w || w->is_batch() || !w->closure || !std::isfinite(dt_fine) || dt_fine <= 0.0f) return 0;
+  if (!w || !w->closure || !std::isfinite(dt_fine) || dt_fine <= 0.0f) return 0;
   const float dtc = dt_fine * (float)w->closure_ratio;
-  if (!w->cfg.enabled || w->n == 0 || coarse_steps == 0) {
+  const bool batch = w->is_batch();
+  if ((!batch && !w->cfg.enabled) || w->n == 0 || coarse_steps == 0) {
     w->time += dtc * (float)coarse_steps;
     return 1;
   }
-  if (unsupported(w)) return 0;
+  if (!batch && unsupported(w)) return 0;
   if (!prepare(w)) return 0;
   if (!ensure_closure_buffers(w)) return 0;
+  // a batch reads each scene's step length from its parameter table
+  if (batch && !upload_scene_table(w, dtc)) return 0;
   const StepParams Pc = make_params(w, dtc);
   const StepParams Pf = make_params(w, dt_fine);
   const MlpDev mlp = phieng_mlp_dev(w->closure);
   ClosureIO io;
   io.save = w->d_save;
   io.rho_prev = w->d_rho_prev;
-  io.acc_scale = Pc.hk / (dtc * dtc);
   enqueue_sort_density(w, Pc);
   for (uint32_t k = 0; k < coarse_steps; k++) {
     if (!run_coarse(w, Pc, mlp, io)) return 0;
     w->sid_perm_n = w->n;
-    if (!cuda_ok(w, cudaMemcpyAsync(w->h_pinned, w->d.scalar + 4, 4, cudaMemcpyDeviceToHost, w->stream), "check") ||
+    if (!cuda_ok(w, cudaMemcpyAsync(w->h_pinned, w->d.scalar + 4, 12, cudaMemcpyDeviceToHost, w->stream), "check") ||
         !cuda_ok(w, cudaStreamSynchronize(w->stream), "sync"))
       return 0;
-    float chk;
-    std::memcpy(&chk, w->h_pinned, 4);
+    float v[3];
+    std::memcpy(v, w->h_pinned, 12);
+    const float chk = w->closure_criterion == PHIENG_CLOSURE_JUMP          ? v[0]
+                      : w->closure_criterion == PHIENG_CLOSURE_COMPRESSION ? v[1]
+                                                                           : v[1] - v[2];
     if (stats) {
       stats->coarse_steps++;
       stats->last_check = chk;
@@ -1233,8 +1237,10 @@ int32_t phieng_sph_closure_step(World2* w, float dt_fine, uint32_t coarse_steps,
         return 0;
       w->keys_valid = false;
       if (!prepare(w)) return 0;
+      if (batch && !upload_scene_table(w, dt_fine)) return 0;
       for (uint32_t r = 0; r < w->closure_ratio; r++)
         if (!run_substep(w, Pf)) return 0;
+      if (batch && !upload_scene_table(w, dtc)) return 0;
       if (k + 1 < coarse_steps) enqueue_sort_density(w, Pc);
     }
     w->time += dtc;
