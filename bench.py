@@ -272,6 +272,41 @@ def run_reference(args, rank: int):
     print(json.dumps(line), flush=True)
 
 
+def apply_tuning(world, mode: str, dt: float) -> dict:
+    """Launch tuning for the timed world: "auto" = the cached / shipped
+    choice for this GPU and workload, else the defaults; "tune" = run the
+    autotuner now (outside the timed region); "default" = the defaults."""
+    from phi_eng_b200 import autotune as at
+
+    if mode == "tune":
+        world.step_n(dt, 2)
+        r = at.autotune(world, dt, steps=10)
+        return dict(r["tuning"], source="autotuned in this run")
+    if mode == "auto":
+        t = at.lookup(world)
+        if t:
+            at.apply(world, t)
+            return dict(t, source="tuning table")
+    return dict(at.DEFAULT, source="defaults")
+
+
+def closure_line(sc) -> dict:
+    """The learned closure against the plain fine run on this workload
+    (50 coarse steps of 4 dt vs 200 fine steps), simulated seconds per wall
+    second of each, with the shipped weights."""
+    from phi_eng_b200 import _abi
+    from phi_eng_b200 import closure as cl
+
+    if not os.path.exists(cl.WEIGHTS):
+        return {"unavailable": "no trained weights"}
+    r = cl.evaluate(sc, cl.Mlp.load(cl.WEIGHTS), coarse_steps=50, threshold=0.03, criterion=_abi.CLOSURE_JUMP,
+                    record_every=10)
+    return {"metric": "simulated s per wall s", "learned": r["closure_sim_s_per_wall_s"],
+            "plain": r["plain_sim_s_per_wall_s"], "ratio": r["speedup"], "front_err": r["front_rel"],
+            "density_err": r["density_dev_abs"], "accepted": r["accepted"], "fallbacks": r["fallbacks"],
+            "threshold": 0.03, "criterion": r["criterion"], "coarse_steps": 50, "dt_ratio": 4}
+
+
 def run_ours(args, rank: int, world: int, local_rank: int):
     import torch
 
@@ -288,6 +323,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     scs = workload_scenes(args.workload)
     job = Job(scs)
     n_total, dt = job.n, job.dt
+    tuning = apply_tuning(job.world, args.tuning, dt)
     stream = torch.cuda.Stream()
     w = job.world
     w.set_stream(stream.cuda_stream)
@@ -348,6 +384,9 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     # of every particle's state (phieng_world_fluid_get)
     job.close()
     job2 = Job(scs)
+    from phi_eng_b200 import autotune as at
+
+    at.apply(job2.world, tuning)
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
@@ -380,11 +419,13 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                 "config": {"workload": workload_desc(args.workload, scs), "particles": n_total, "parallelism":
                            ("replicas" if world > 1 else "single"),
                            "l2": "flushed between timed steps (256 MiB write, outside the timed events)",
-                           "buckets": int(buckets)},
+                           "buckets": int(buckets), "tuning": tuning},
                 "roofline": roofline, "whole_step": whole,
                 "phases_ms": {n: float(v) for n, v in zip(names, ph_mean)},
                 "cpu_baseline": base, "e2e": e2e, "gpu_launches": kernels_per_step * args.steps,
                 "clocks": clocks}
+        if args.closure and len(scs) == 1 and world == 1:
+            line["closure"] = closure_line(scs[0])
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
@@ -399,6 +440,9 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="dam_break_1m", choices=list(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--tuning", choices=["auto", "default", "tune"], default="auto")
+    ap.add_argument("--no-closure", dest="closure", action="store_false",
+                    help="skip the learned-closure comparison line")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     rank = int(os.environ.get("RANK", "0"))

@@ -248,6 +248,22 @@ int32_t phieng_sph_batch_scene_range(const World2* batch, uint32_t scene, uint32
  * worlds it came from (same order and sizes). 1 ok, 0 invalid. */
 int32_t phieng_sph_batch_store(World2* batch, World2* const* worlds, uint32_t count);
 
+/* ---- launch tuning (additive) ----
+ * Launch shapes that change speed, never results (the neighbour visit order
+ * and every sum stay the same). phi_eng_b200/autotune.py picks them per GPU
+ * and workload. */
+typedef struct PhiengSphTuning {
+  uint32_t density_block;     /* threads per block of the density pass: 64, 128, 256 (default 256) */
+  uint32_t force_block;       /* threads per block of the force pass: 64, 128, 256 (default 256) */
+  float buckets_per_particle; /* bucket-grid budget per particle, 0.125..16 (default 2) */
+  uint32_t reserved;
+} PhiengSphTuning;
+
+/* 1 ok, 0 null or out of range (world unchanged). Replans the bucket grid
+ * unless phieng_sph_set_grid fixed it. */
+int32_t phieng_sph_set_tuning(World2* world, const PhiengSphTuning* tuning);
+int32_t phieng_sph_get_tuning(const World2* world, PhiengSphTuning* out);
+
 /* ---- device-resident state (additive; callers that keep data on the GPU) ----
  * Pointers are CUDA device pointers on the world's device; the copies are
  * ordered on the world's stream. */

@@ -110,6 +110,15 @@ class PhiengClosureStats(C.Structure):
     ]
 
 
+class PhiengSphTuning(C.Structure):
+    _fields_ = [
+        ("density_block", C.c_uint32),
+        ("force_block", C.c_uint32),
+        ("buckets_per_particle", C.c_float),
+        ("reserved", C.c_uint32),
+    ]
+
+
 MLP_PARAMS = 5378
 MLP_NORM = 34
 MLP_FEATURES = 16
@@ -162,6 +171,8 @@ SIGNATURES = {
     "phieng_sph_batch_scene_range": (C.c_int32, [_P, C.c_uint32, _U32P, _U32P]),
     "phieng_sph_batch_store": (C.c_int32, [_P, C.POINTER(_P), C.c_uint32]),
     "phieng_sph_density_noalloc": (C.c_int32, [_P, C.c_uint32, C.POINTER(FluidConfig2Ffi), _P, _P, _P]),
+    "phieng_sph_set_tuning": (C.c_int32, [_P, C.POINTER(PhiengSphTuning)]),
+    "phieng_sph_get_tuning": (C.c_int32, [_P, C.POINTER(PhiengSphTuning)]),
     "phieng_sph_get_state_device": (C.c_uint32, [_P, _P, C.c_uint32]),
     "phieng_sph_set_state_device": (C.c_int32, [_P, _P, C.c_uint32]),
     "phieng_mlp_new": (_P, [C.c_uint64]),

@@ -766,10 +766,10 @@ void enqueue_sort_and_ranges(const FluidBufs& b, uint32_t n, const StepParams& P
 void enqueue_density(const FluidBufs& b, uint32_t n, const StepParams& P, cudaStream_t st) {
   if (n == 0) return;
   const bool m = (P.flags & F_MASS) != 0, ph = (P.flags & F_PHASE) != 0, bat = b.batch.ptab != nullptr;
-  const uint32_t g = cdiv(n, 256);
-#define PHIENG_DENSITY(M, PH, BT)                                                                            \
-  k_density<M, PH, BT><<<g, 256, 0, st>>>(b.spos, b.skey, b.smass, b.sphase, n, b.start, P, b.batch, b.sdq, \
-                                          b.spres, b.nmask)
+  const uint32_t bs = b.block_density, g = cdiv(n, bs);
+#define PHIENG_DENSITY(M, PH, BT)                                                                           \
+  k_density<M, PH, BT><<<g, bs, 0, st>>>(b.spos, b.skey, b.smass, b.sphase, n, b.start, P, b.batch, b.sdq, \
+                                         b.spres, b.nmask)
   if (bat) {
     if (m && ph) PHIENG_DENSITY(true, true, true);
     else if (m) PHIENG_DENSITY(true, false, true);
@@ -788,10 +788,10 @@ void enqueue_force_integrate(const FluidBufs& b, uint32_t n, const StepParams& P
                              cudaStream_t st) {
   if (n == 0) return;
   const bool m = (P.flags & F_MASS) != 0, bat = b.batch.ptab != nullptr;
-  const uint32_t g = cdiv(n, 256);
-#define PHIENG_FORCE(M, D, BT)                                                                                     \
-  k_force_integrate<M, D, BT><<<g, 256, 0, st>>>(b.spos, b.svel, b.sdq, b.skey, b.sid, b.smass, n, b.start, P,   \
-                                                 b.batch, b.bodies, b.nmask, b.state, b.key, b.count, dbg_force)
+  const uint32_t bs = b.block_force, g = cdiv(n, bs);
+#define PHIENG_FORCE(M, D, BT)                                                                                    \
+  k_force_integrate<M, D, BT><<<g, bs, 0, st>>>(b.spos, b.svel, b.sdq, b.skey, b.sid, b.smass, n, b.start, P,   \
+                                                b.batch, b.bodies, b.nmask, b.state, b.key, b.count, dbg_force)
   if (dbg_force) {
     if (m) PHIENG_FORCE(true, true, false);
     else PHIENG_FORCE(false, true, false);

@@ -48,6 +48,9 @@ struct FluidBufs {
   DevBody* bodies = nullptr;
   uint32_t bodies_cap = 0;
   unsigned int* scalar = nullptr;  // small device scratch (vmax etc.)
+  // launch shapes (autotuned; results do not depend on them)
+  uint32_t block_density = 256;  // threads per block of K5: 64, 128 or 256
+  uint32_t block_force = 256;    // threads per block of K6: 64, 128 or 256
 };
 
 // Scan tile of the bucket counts; count arrays are padded to a multiple.

@@ -206,6 +206,9 @@ struct World2 {
   uint32_t closure_cap = 0;
   cudaGraphExec_t cexec = nullptr;
   std::string csig;
+
+  // launch tuning (phieng_sph_set_tuning)
+  float buckets_per_particle = 2.0f;
 };
 
 namespace {
@@ -362,7 +365,7 @@ bool ensure_host_dp(World2* w) {
 // Bucket grid from the particle bounding box (host copy must be current).
 // Bucket grid covering the cells of n particles (with a margin), ~2 buckets
 // per particle at most.
-GridPlan plan_for(const float4* st, uint32_t n, float hg) {
+GridPlan plan_for(const float4* st, uint32_t n, float hg, float buckets_per_particle) {
   int64_t x0 = INT64_MAX, x1 = INT64_MIN, y0 = INT64_MAX, y1 = INT64_MIN;
   for (uint32_t i = 0; i < n; i++) {
     float4 s = st[i];
@@ -378,9 +381,11 @@ GridPlan plan_for(const float4* st, uint32_t n, float hg) {
   const int64_t mx = std::max<int64_t>(2, sx / 8), my = std::max<int64_t>(2, sy / 8);
   uint32_t W = std::max<uint32_t>(4, next_pow2((uint64_t)(sx + 2 * mx)));
   uint32_t H = std::max<uint32_t>(4, next_pow2((uint64_t)(sy + 2 * my)));
-  // bucket budget: ~2 buckets per particle (each bucket costs ~20 B of
-  // count / scan / range-table traffic per substep)
-  const uint64_t budget = std::min<uint64_t>(1ull << 24, std::max<uint64_t>(1ull << 12, next_pow2(2ull * n)));
+  // bucket budget: buckets_per_particle (2 by default) per particle, rounded
+  // up to a power of two; each bucket costs ~20 B of count / scan /
+  // range-table traffic per substep, fewer buckets alias more cells into one
+  const uint64_t want = (uint64_t)std::ceil((double)buckets_per_particle * (double)std::max<uint32_t>(n, 1));
+  const uint64_t budget = std::min<uint64_t>(1ull << 24, std::max<uint64_t>(1ull << 12, next_pow2(want)));
   while ((uint64_t)W * H > budget) {
     if (W >= H && W > 4)
       W >>= 1;
@@ -408,7 +413,7 @@ void plan_grid(World2* w) {
     // one bucket range per scene, laid end to end
     uint64_t base = 0;
     for (auto& sc : w->scenes) {
-      GridPlan g = plan_for(w->h_state.data() + sc.first, sc.count, sc.cfg.smoothing_length);
+      GridPlan g = plan_for(w->h_state.data() + sc.first, sc.count, sc.cfg.smoothing_length, w->buckets_per_particle);
       g.base = (uint32_t)base;
       base += g.nbuckets;
       sc.plan = g;
@@ -421,7 +426,7 @@ void plan_grid(World2* w) {
     all.hg = w->scenes[0].cfg.smoothing_length;
     w->plan = all;
   } else {
-    w->plan = plan_for(w->h_state.data(), w->n, w->cfg.smoothing_length);
+    w->plan = plan_for(w->h_state.data(), w->n, w->cfg.smoothing_length, w->buckets_per_particle);
   }
   w->plan_valid = true;
   w->keys_valid = false;
@@ -1138,6 +1143,35 @@ int32_t phieng_sph_front_metrics(World2* w, float* out) {
     std::memcpy(&out[0], &ux, 4);
   }
   std::memcpy(&out[1], &bv, 4);
+  return 1;
+}
+
+int32_t phieng_sph_set_tuning(World2* w, const PhiengSphTuning* t) {
+  if (!w || !t) return 0;
+  auto ok_block = [](uint32_t b) { return b == 64 || b == 128 || b == 256; };
+  if (!ok_block(t->density_block) || !ok_block(t->force_block) || !(t->buckets_per_particle >= 0.125f) ||
+      !(t->buckets_per_particle <= 16.0f))
+    return 0;
+  if (w->device >= 0) cudaStreamSynchronize(w->stream);
+  release_graph(w);
+  w->d.block_density = t->density_block;
+  w->d.block_force = t->force_block;
+  if (w->buckets_per_particle != t->buckets_per_particle) {
+    w->buckets_per_particle = t->buckets_per_particle;
+    if (!w->plan_locked) {
+      if (!ensure_host_state(w)) return 0;
+      plan_grid(w);
+    }
+  }
+  return 1;
+}
+
+int32_t phieng_sph_get_tuning(const World2* w, PhiengSphTuning* t) {
+  if (!w || !t) return 0;
+  t->density_block = w->d.block_density;
+  t->force_block = w->d.block_force;
+  t->buckets_per_particle = w->buckets_per_particle;
+  t->reserved = 0;
   return 1;
 }
 
