@@ -307,6 +307,49 @@ def closure_line(sc) -> dict:
             "threshold": 0.03, "criterion": r["criterion"], "coarse_steps": 50, "dt_ratio": 4}
 
 
+def run_slab(args, rank: int, world: int, local_rank: int) -> None:
+    """The single scene split in x slabs over the ranks (halo exchange and
+    migration over NCCL each substep, phi_eng_b200/slab.py); strong scaling.
+    The timed region is bracketed by barriers and CUDA events on the default
+    stream; the max over ranks is reported."""
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+
+    from phi_eng_b200.slab import GpuEngine, SlabRun
+
+    torch.cuda.set_device(local_rank)
+    dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    sc = workload_scenes(args.workload)[0]
+    eng = GpuEngine(sc, cap=sc.n)
+    run = SlabRun(sc, rank, world, engine=eng, device="cuda")
+    for _ in range(args.warmup):
+        run.step(sc.dt)
+    torch.cuda.synchronize()
+    dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        run.step(sc.dt)
+    e1.record()
+    torch.cuda.synchronize()
+    t = torch.tensor([e0.elapsed_time(e1)], device="cuda", dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms = float(t.item())
+    if rank == 0:
+        value = sc.n * args.steps / (total_ms / 1000.0)
+        line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+                "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": workload_desc(args.workload, [sc]), "particles": sc.n,
+                           "parallelism": f"slab{world}", "l2": "not flushed (inputs move between ranks)"},
+                "gpu_launches": None}
+        print(json.dumps(line), flush=True)
+    eng.close()
+    dist.barrier()
+    dist.destroy_process_group()
+
+
 def run_ours(args, rank: int, world: int, local_rank: int):
     import torch
 
@@ -441,6 +484,8 @@ def main():
     ap.add_argument("--workload", default="dam_break_1m", choices=list(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--tuning", choices=["auto", "default", "tune"], default="auto")
+    ap.add_argument("--parallel", choices=["replicas", "slab"], default="replicas",
+                    help="N > 1: independent replicas (weak scaling) or the scene split in x slabs (strong)")
     ap.add_argument("--no-closure", dest="closure", action="store_false",
                     help="skip the learned-closure comparison line")
     args = ap.parse_args()
@@ -450,6 +495,9 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank)
+        return
+    if args.parallel == "slab" and world > 1:
+        run_slab(args, rank, world, local_rank)
         return
     run_ours(args, rank, world, local_rank)
 

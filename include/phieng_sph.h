@@ -274,6 +274,10 @@ uint32_t phieng_sph_get_state_device(World2* world, float* dst, uint32_t max);
 /* Overwrite the state of all n = fluid_count particles from src. 1 ok, 0 on
  * a count mismatch or null. Works on batches. */
 int32_t phieng_sph_set_state_device(World2* world, const float* src, uint32_t n);
+/* Replace every particle by n phase-0 particles whose [x, y, vx, vy] come
+ * from src (device); n <= the particle cap. Used to rebuild a rank's local
+ * particle set each substep without a host round trip. 1 ok, 0 otherwise. */
+int32_t phieng_sph_load_state_device(World2* world, const float* src, uint32_t n);
 
 /* ---- learned closure (additive; no reference counterpart) ----
  * A per-particle network 16 -> 64 -> 64 -> 2 (SiLU, BF16 weights on the

@@ -175,6 +175,7 @@ SIGNATURES = {
     "phieng_sph_get_tuning": (C.c_int32, [_P, C.POINTER(PhiengSphTuning)]),
     "phieng_sph_get_state_device": (C.c_uint32, [_P, _P, C.c_uint32]),
     "phieng_sph_set_state_device": (C.c_int32, [_P, _P, C.c_uint32]),
+    "phieng_sph_load_state_device": (C.c_int32, [_P, _P, C.c_uint32]),
     "phieng_mlp_new": (_P, [C.c_uint64]),
     "phieng_mlp_free": (None, [_P]),
     "phieng_mlp_status": (C.c_int32, [_P]),

@@ -1175,6 +1175,29 @@ int32_t phieng_sph_get_tuning(const World2* w, PhiengSphTuning* t) {
   return 1;
 }
 
+int32_t phieng_sph_load_state_device(World2* w, const float* src, uint32_t n) {
+  if (!w || w->is_batch() || (n && !src) || n > w->cap) return 0;
+  if (!ensure_device(w)) return 0;
+  cudaStreamSynchronize(w->stream);
+  w->n = n;
+  w->h_state.resize(n);
+  w->h_dens.assign(n, w->cfg.phase_rest_density[0]);
+  w->h_pres.assign(n, 0.0f);
+  w->h_mass.assign(n, rmaxf(w->cfg.phase_mass[0], 0.0f));
+  w->h_phase.assign(n, 0);
+  recompute_uniformity(w);
+  if (n && !ensure_capacity(w, n)) return 0;
+  if (n && !cuda_ok(w, cudaMemcpyAsync(w->d.state, src, sizeof(float4) * n, cudaMemcpyDeviceToDevice, w->stream),
+                    "load state"))
+    return 0;
+  w->dev_state_valid = true;
+  w->host_state_valid = n == 0;
+  w->dev_aux_valid = false;
+  w->dp_on_device = false;
+  w->keys_valid = false;  // the bucket grid stays: any grid is exact
+  return 1;
+}
+
 uint32_t phieng_sph_get_state_device(World2* w, float* dst, uint32_t max) {
   if (!w || !dst) return 0;
   const uint32_t n = std::min(max, w->n);

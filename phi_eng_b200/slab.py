@@ -1,0 +1,301 @@
+"""One SPH scene split over ranks in x slabs, with halo exchange.
+
+Rank r owns the particles whose cell column cx = floor(x / h) lies in
+[edges[r], edges[r+1]). Every substep:
+
+  1. halo: each rank sends its neighbours the particles in the two cell
+     columns next to the shared edge (2h: the neighbours of a particle reach
+     one cell, and their densities need one more);
+  2. the rank steps its owned particles together with the received halo, in
+     ascending global id, on its engine (one substep, no CFL splitting);
+  3. it keeps the owned particles' new states (those are exactly the
+     single-domain results: every neighbour, and every neighbour's density,
+     is present, and the in-cell visit order is ascending global id) and
+     drops the halo's;
+  4. migration: owned particles whose new cell column left the slab go to
+     the adjacent rank (a particle moves less than one cell per substep).
+
+With CFL substeps enabled the substep count comes from the global maximum
+speed (one all-reduce), as the single-domain step computes it. Results are
+bit-identical to the single-domain step; tests/test_slab.py checks that on
+the CPU with gloo ranks and the oracle as the engine.
+
+Communication is neighbour point-to-point (torch.distributed isend / irecv:
+NCCL over NVLink for CUDA tensors, gloo for CPU tensors): first the counts,
+then one float32 payload per direction, [x, y, vx, vy, id bits].
+"""
+from __future__ import annotations
+
+import numpy as np
+
+HALO_CELLS = 2
+
+
+def cell_column(x, h: float):
+    """floor(x / h) in f32 arithmetic, saturated to i32 (NaN -> 0), as the
+    kernels and the reference compute it (fluid.rs:350-356)."""
+    import torch
+
+    q = torch.floor(x.to(torch.float32) / torch.tensor(np.float32(h), device=x.device))
+    q = torch.nan_to_num(q, nan=0.0, posinf=2147483647.0, neginf=-2147483648.0)
+    return q.clamp(-2147483648.0, 2147483647.0).to(torch.int64)
+
+
+def slab_edges(xy: np.ndarray, h: float, size: int) -> list:
+    """Cell-column edges that split the particles into `size` slabs of equal
+    count (each slab at least HALO_CELLS columns wide)."""
+    import torch
+
+    cx = cell_column(torch.from_numpy(np.ascontiguousarray(xy[:, 0])), h).numpy()
+    cols = np.sort(cx)
+    edges = [-(1 << 40)]
+    for r in range(1, size):
+        e = int(cols[min(len(cols) - 1, (len(cols) * r) // size)])
+        e = max(e, edges[-1] + HALO_CELLS if r > 1 else e)
+        edges.append(e)
+    edges.append(1 << 40)
+    return edges
+
+
+def cfl_count(cfg, dt: float, vmax: float) -> int:
+    """cfl_substeps (fluid.rs:562-588) from a global maximum speed, in the
+    f32 arithmetic of the single-domain step."""
+    f = np.float32
+    mx = max(int(cfg.max_substeps), 1)
+    if not (f(cfg.cfl) > 0) or mx <= 1:
+        return 1
+    h = max(f(cfg.smoothing_length), f(1e-6))
+    rho0 = max(f(cfg.rest_density), f(1e-6))
+    k = max(f(cfg.stiffness), f(0))
+    c0 = np.sqrt(k) if f(cfg.gamma) == f(1) else np.sqrt(f(cfg.gamma) * k * rho0)
+    speed = f(c0) + f(vmax)
+    if not np.isfinite(speed) or speed <= f(1e-6):
+        return 1
+    dt_max = f(cfg.cfl) * h / speed
+    if not np.isfinite(dt_max) or dt_max <= 0:
+        return 1
+    q = np.ceil(f(dt) / dt_max)
+    if q != q:
+        return 1
+    return int(max(1, min(float(q), mx)))
+
+
+class OracleEngine:
+    """CPU engine: the oracle in Jacobi order (what the GPU computes)."""
+
+    def __init__(self, scene):
+        self.scene = scene
+
+    def step(self, state, dt: float):
+        import torch
+
+        from oracle import oracle as orc
+
+        sc = self.scene
+        o = orc.OracleWorld(cap=max(state.shape[0], 1))
+        o.set_gravity(*sc.gravity)
+        for (px, py, hx, hy) in sc.boxes:
+            o.add_box(px, py, hx, hy, (1.0, 0.0, -0.0, 1.0))
+        for (px, py, r) in sc.circles:
+            o.add_circle(px, py, r, (1.0, 0.0, -0.0, 1.0))
+        o.set_config(_no_cfl(sc.config))
+        st = state.numpy()
+        if st.shape[0]:
+            o.add_particles(np.ascontiguousarray(st[:, :2]))
+            o.set_state(st)
+            o.step(dt, orc.JACOBI)
+        return torch.from_numpy(o.state().reshape(-1, 4).copy())
+
+
+class GpuEngine:
+    """GPU engine: one library world whose particle set is replaced from
+    device memory each substep."""
+
+    def __init__(self, scene, cap: int):
+        from .world import world_from_scene
+
+        self.world = world_from_scene(_empty_scene(scene))
+        self.world.fluid.config = _no_cfl(scene.config)
+        self.world.fluid.set_cap(cap)
+
+    def close(self) -> None:
+        self.world.close()
+
+    def step(self, state, dt: float):
+        import torch
+
+        n = state.shape[0]
+        w = self.world
+        w.load_state_device(state.data_ptr(), n)
+        w.step(dt)
+        out = torch.empty_like(state)
+        if n:
+            w.get_state_device(out.data_ptr(), n)
+        w.sync()
+        return out
+
+
+def _empty_scene(scene):
+    import copy
+
+    s = copy.copy(scene)
+    s.xy = np.zeros((0, 2), np.float32)
+    s.phases = None
+    return s
+
+
+def _no_cfl(cfg):
+    from ._abi import FluidConfig2Ffi
+    import ctypes as C
+
+    c = FluidConfig2Ffi()
+    C.memmove(C.byref(c), C.byref(cfg), C.sizeof(cfg))
+    c.cfl = 0.0
+    c.max_substeps = 1
+    return c
+
+
+def _pack(state, ids):
+    import torch
+
+    return torch.cat([state, ids.to(torch.int32).view(torch.float32).unsqueeze(1)], 1)
+
+
+def _unpack(buf):
+    import torch
+
+    return buf[:, :4].contiguous(), buf[:, 4].contiguous().view(torch.int32).to(torch.int64)
+
+
+class SlabRun:
+    """This rank's part of one scene (owned particles, their global ids)."""
+
+    def __init__(self, scene, rank: int, size: int, engine=None, device: str = "cpu", edges=None):
+        import torch
+
+        self.scene = scene
+        self.rank, self.size = rank, size
+        self.device = device
+        self.h = float(scene.config.smoothing_length)
+        self.edges = edges or slab_edges(scene.xy, self.h, size)
+        self.lo, self.hi = self.edges[rank], self.edges[rank + 1]
+        xy = torch.from_numpy(np.ascontiguousarray(scene.xy, dtype=np.float32))
+        cx = cell_column(xy[:, 0], self.h)
+        mine = (cx >= self.lo) & (cx < self.hi)
+        ids = torch.nonzero(mine).squeeze(1)
+        st = torch.zeros((ids.shape[0], 4), dtype=torch.float32)
+        st[:, :2] = xy[ids]
+        self.ids = ids.to(device)
+        self.state = st.to(device)
+        self.engine = engine if engine is not None else OracleEngine(scene)
+        self.comm_bytes = 0
+
+    # ---- neighbour exchange ----
+    def _exchange(self, to_left, to_right):
+        """Send packed rows to the neighbours, receive theirs (variable sizes)."""
+        import torch
+        import torch.distributed as dist
+
+        left = self.rank - 1 if self.rank > 0 else None
+        right = self.rank + 1 if self.rank < self.size - 1 else None
+        dev = self.device
+        cnt = {}
+        ops = []
+        for peer, buf in ((left, to_left), (right, to_right)):
+            if peer is None:
+                continue
+            s = torch.tensor([buf.shape[0]], dtype=torch.int64, device=dev)
+            r = torch.zeros(1, dtype=torch.int64, device=dev)
+            cnt[peer] = r
+            ops += [dist.P2POp(dist.isend, s, peer), dist.P2POp(dist.irecv, r, peer)]
+        if ops:
+            for q in dist.batch_isend_irecv(ops):
+                q.wait()
+        got = {}
+        ops = []
+        for peer, buf in ((left, to_left), (right, to_right)):
+            if peer is None:
+                continue
+            k = int(cnt[peer].item())
+            got[peer] = torch.empty((k, 5), dtype=torch.float32, device=dev)
+            if buf.shape[0]:
+                ops.append(dist.P2POp(dist.isend, buf.contiguous(), peer))
+                self.comm_bytes += buf.numel() * 4
+            if k:
+                ops.append(dist.P2POp(dist.irecv, got[peer], peer))
+        if ops:
+            for q in dist.batch_isend_irecv(ops):
+                q.wait()
+        empty = torch.empty((0, 5), dtype=torch.float32, device=dev)
+        return got.get(left, empty), got.get(right, empty)
+
+    def _substep(self, dt: float):
+        import torch
+
+        cx = cell_column(self.state[:, 0], self.h)
+        packed = _pack(self.state, self.ids)
+        to_l = packed[cx < self.lo + HALO_CELLS] if self.size > 1 else packed[:0]
+        to_r = packed[cx >= self.hi - HALO_CELLS] if self.size > 1 else packed[:0]
+        from_l, from_r = self._exchange(to_l, to_r) if self.size > 1 else (packed[:0], packed[:0])
+        hl_s, hl_i = _unpack(from_l)
+        hr_s, hr_i = _unpack(from_r)
+        ids = torch.cat([self.ids, hl_i, hr_i])
+        st = torch.cat([self.state, hl_s, hr_s])
+        order = torch.argsort(ids)
+        new = self.engine.step(st[order].contiguous(), dt).to(self.device)
+        owned = order < self.ids.shape[0]  # rows that came from this rank's own particles
+        self.ids = ids[order][owned]
+        self.state = new[owned]
+        # migration
+        if self.size > 1:
+            cx = cell_column(self.state[:, 0], self.h)
+            go_l, go_r = cx < self.lo, cx >= self.hi
+            if self.rank == 0:
+                go_l = torch.zeros_like(go_l)
+            if self.rank == self.size - 1:
+                go_r = torch.zeros_like(go_r)
+            packed = _pack(self.state, self.ids)
+            in_l, in_r = self._exchange(packed[go_l], packed[go_r])
+            keep = ~(go_l | go_r)
+            a_s, a_i = _unpack(in_l)
+            b_s, b_i = _unpack(in_r)
+            ids = torch.cat([self.ids[keep], a_i, b_i])
+            st = torch.cat([self.state[keep], a_s, b_s])
+            order = torch.argsort(ids)
+            self.ids, self.state = ids[order], st[order].contiguous()
+
+    def step(self, dt: float):
+        """One world step of dt (CFL substeps from the global max speed)."""
+        import torch
+
+        cfg = self.scene.config
+        n_sub = 1
+        if float(cfg.cfl) > 0 and int(cfg.max_substeps) > 1:
+            v = torch.sqrt(self.state[:, 2] ** 2 + self.state[:, 3] ** 2)
+            v = torch.nan_to_num(v, nan=0.0)
+            vmax = v.max() if v.numel() else torch.zeros((), device=self.device)
+            vmax = vmax.reshape(1).to(torch.float32)
+            if self.size > 1:
+                import torch.distributed as dist
+
+                dist.all_reduce(vmax, op=dist.ReduceOp.MAX)
+            n_sub = cfl_count(cfg, dt, float(vmax.item()))
+        sub = float(np.float32(dt) / np.float32(n_sub))
+        for _ in range(n_sub):
+            self._substep(sub)
+
+    def gather(self):
+        """Every particle's state in global id order (all ranks)."""
+        import torch
+
+        if self.size == 1:
+            return self.state.cpu().numpy()
+        import torch.distributed as dist
+
+        parts = [None] * self.size
+        dist.all_gather_object(parts, (self.ids.cpu().numpy(), self.state.cpu().numpy()))
+        n = sum(p[0].shape[0] for p in parts)
+        out = np.zeros((n, 4), np.float32)
+        for ids, st in parts:
+            out[ids] = st
+        return out

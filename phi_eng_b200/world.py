@@ -250,6 +250,12 @@ class World2:
             self.check()
             raise ValueError("set_state_device: count mismatch")
 
+    def load_state_device(self, src_ptr: int, n: int) -> None:
+        """Replace every particle by n phase-0 particles from device memory."""
+        if self._lib.phieng_sph_load_state_device(self._h, C.c_void_p(src_ptr), n) != 1:
+            self.check()
+            raise ValueError("load_state_device rejected its arguments")
+
     def features(self, dt: float, feat_ptr: int) -> None:
         """Closure inputs (n x 16 floats, device) at the current state for a step dt."""
         if self._lib.phieng_sph_features(self._h, dt, C.c_void_p(feat_ptr)) != 1:

@@ -1,0 +1,106 @@
+"""Slab decomposition of one scene over ranks (phi_eng_b200/slab.py).
+
+CPU: gloo ranks (2 and 3) each step their slab plus a 2-cell halo on the
+oracle (Jacobi order, the order the GPU computes) and exchange halos and
+migrating particles with their neighbours; the gathered state equals the
+single-domain oracle run bit for bit, with and without CFL substeps.
+GPU: one rank on the library (no peers) equals the plain world.
+"""
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch.multiprocessing as mp
+
+import sims
+from oracle import oracle as orc
+from phi_eng_b200 import scenes
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    p = s.getsockname()[1]
+    s.close()
+    return p
+
+
+def _scene(cfl: bool):
+    sc = scenes.dam_break_4k()
+    if cfl:
+        cfg = sc.config
+        cfg.cfl = 0.4
+        cfg.max_substeps = 4
+        sc.config = cfg
+        sc.dt = 2.5 * sc.dt
+    return sc
+
+
+def _worker(rank, size, port, steps, cfl, out):
+    import torch.distributed as dist
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=size)
+    from phi_eng_b200.slab import SlabRun
+
+    sc = _scene(cfl)
+    run = SlabRun(sc, rank, size)
+    for _ in range(steps):
+        run.step(sc.dt)
+    full = run.gather()
+    if rank == 0:
+        np.save(out, full)
+    moved = np.array([run.comm_bytes], np.int64)
+    np.save(out + f".bytes{rank}.npy", moved)
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("size,cfl", [(2, False), (3, False), (2, True)])
+def test_slab_ranks_equal_single_domain(tmp_path, size, cfl):
+    steps = 60
+    out = str(tmp_path / "state.npy")
+    mp.start_processes(_worker, args=(size, _free_port(), steps, cfl, out), nprocs=size, start_method="spawn")
+    got = np.load(out)
+    sc = _scene(cfl)
+    o = sims.load_scene(sims.OracleSim(orc.JACOBI), sc)
+    o.step(sc.dt, steps)
+    np.testing.assert_array_equal(got, o.state())
+    for r in range(size):
+        assert np.load(out + f".bytes{r}.npy")[0] > 0  # halos crossed every edge
+
+
+def test_slab_edges_split_evenly():
+    from phi_eng_b200.slab import cell_column, slab_edges
+
+    import torch
+
+    sc = scenes.dam_break_4k()
+    h = float(sc.config.smoothing_length)
+    e = slab_edges(sc.xy, h, 4)
+    cx = cell_column(torch.from_numpy(sc.xy[:, 0].copy()), h).numpy()
+    counts = [int(((cx >= e[r]) & (cx < e[r + 1])).sum()) for r in range(4)]
+    assert sum(counts) == sc.n and max(counts) - min(counts) <= 2 * 64 + 64
+    assert all(e[r + 1] - e[r] >= 2 for r in range(1, 3))
+
+
+@pytest.mark.gpu
+def test_slab_gpu_single_rank_equals_world():
+    import torch
+
+    from phi_eng_b200.slab import GpuEngine, SlabRun
+    from phi_eng_b200.world import world_from_scene
+
+    sc = scenes.dam_break_4k()
+    eng = GpuEngine(sc, cap=sc.n)
+    run = SlabRun(sc, 0, 1, engine=eng, device="cuda")
+    for _ in range(30):
+        run.step(sc.dt)
+    w = world_from_scene(sc)
+    w.step_n(sc.dt, 30)
+    np.testing.assert_array_equal(run.gather(), w.fluid.particles)
+    torch.cuda.synchronize()
+    eng.close()
+    w.close()
