@@ -124,8 +124,11 @@ class GpuEngine:
     def step(self, state, dt: float):
         import torch
 
+        from .closure import torch_stream_handle
+
         n = state.shape[0]
         w = self.world
+        w.set_stream(torch_stream_handle())  # ordered after the torch ops that built `state`
         w.load_state_device(state.data_ptr(), n)
         w.step(dt)
         out = torch.empty_like(state)
