@@ -10,7 +10,8 @@ import ctypes as C
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libphieng_sph.so")
+# PHIENG_SPH_LIBRARY names another build of the same library (same ABI)
+LIB_PATH = os.environ.get("PHIENG_SPH_LIBRARY") or os.path.join(HERE, "libphieng_sph.so")
 
 SHAPE_CIRCLE = 0
 SHAPE_BOX = 1

@@ -265,9 +265,10 @@ __device__ __forceinline__ void for_each_candidate(uint32_t key, const uint32_t*
 // a particle away from the wrap seam, bit t of nmask[oy * n + s] is set iff
 // slot (row start + t) is a neighbour (d2 < h*h, the particle itself
 // included). A zero mask for the particle's own row (which always holds the
-// particle itself) means "no masks": the row was longer than 64 slots or the
-// particle sits on the seam, and K6 walks the candidates itself.
-constexpr uint32_t kMaskBits = 64;
+// particle itself) means "no masks": the row was longer than 32 slots (rows
+// hold ~12 candidates at rest density) or the particle sits on the seam, and
+// K6 walks the candidates itself.
+constexpr uint32_t kMaskBits = 32;
 
 // Candidate j's density contribution m_j * poly6(d2) when d2 < h*h, else +0
 // (adding +0 to a non-negative sum is exact, so skipping and adding agree).
@@ -281,14 +282,14 @@ __global__ void __launch_bounds__(256) k_density(const float2* __restrict__ spos
                                                  const uint8_t* __restrict__ sphase, uint32_t n,
                                                  const uint32_t* __restrict__ start, StepParams P0, BatchTab bt,
                                                  float2* __restrict__ sdq, float* __restrict__ spres,
-                                                 uint64_t* __restrict__ nmask) {
+                                                 uint32_t* __restrict__ nmask) {
   const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n) return;
   const StepParams& P = scene_params<BATCH>(P0, bt.ptab, BATCH ? bt.sscene[s] : 0u);
   const uint32_t k = skey[s];
   const float2 pi = spos[s];
   float rho = 0.0f;
-  uint64_t mrow[3] = {0, 0, 0};
+  uint32_t mrow[3] = {0, 0, 0};
   const GridPlan& g = P.grid;
   if (k != g.sentinel) {
     const uint32_t local = k - g.base;
@@ -301,13 +302,13 @@ __global__ void __launch_bounds__(256) k_density(const float2* __restrict__ spos
       if (!seam) {
         const uint32_t rs = __ldg(&start[row + bx - 1]);
         const uint32_t re = __ldg(&start[row + bx + 2]);
-        uint64_t m = 0;
+        uint32_t m = 0;
         for (uint32_t j = rs; j < re; j++) {
           const float2 a = __ldg(&spos[j]);
           const float dx = __fsub_rn(a.x, pi.x), dy = __fsub_rn(a.y, pi.y);
           const float d2 = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
           rho = __fadd_rn(rho, density_term(d2, MASS ? __ldg(&smass[j]) : P.mass, P));
-          if (j - rs < kMaskBits) m |= (uint64_t)(d2 < P.hg2) << (j - rs);
+          if (j - rs < kMaskBits) m |= (uint32_t)(d2 < P.hg2) << (j - rs);
         }
         mrow[oy] = m;
         if (re - rs > kMaskBits) masks_ok = false;
@@ -416,30 +417,30 @@ __device__ __forceinline__ void neighbour_sums(uint32_t s, uint32_t k, uint32_t 
                                                float q_i, float m_i, const float2* __restrict__ spos,
                                                const float2* __restrict__ svel, const float2* __restrict__ sdq,
                                                const float* __restrict__ smass, const uint32_t* __restrict__ start,
-                                               const uint64_t* __restrict__ nmask, const StepParams& P, float& fx,
+                                               const uint32_t* __restrict__ nmask, const StepParams& P, float& fx,
                                                float& fy, float& sx, float& sy, FeatAcc& fa) {
   const GridPlan& g = P.grid;
   if (k == g.sentinel) return;
   const uint32_t local = k - g.base;
   const uint32_t bx = local & g.maskw, by = local >> g.log2w;
-  const uint64_t own = nmask[n + s];
-  if (own != 0ull) {
+  const uint32_t own = nmask[n + s];
+  if (own != 0u) {
     // one loop over the three rows' set bits (ascending slots, row by row)
     const uint32_t rs0 = __ldg(&start[g.base + (((by - 1u) & g.maskh) << g.log2w) + bx - 1]);
     const uint32_t rs1 = __ldg(&start[g.base + ((by & g.maskh) << g.log2w) + bx - 1]);
     const uint32_t rs2 = __ldg(&start[g.base + (((by + 1u) & g.maskh) << g.log2w) + bx - 1]);
-    const uint64_t m0 = nmask[s], m2 = nmask[2 * (size_t)n + s];
-    uint64_t cur = m0;
+    const uint32_t m0 = nmask[s], m2 = nmask[2 * (size_t)n + s];
+    uint32_t cur = m0;
     uint32_t row = 0, base = rs0;
     for (;;) {
-      while (cur == 0ull && row < 2) {
+      while (cur == 0u && row < 2) {
         row++;
         cur = row == 1 ? own : m2;
         base = row == 1 ? rs1 : rs2;
       }
-      if (cur == 0ull) break;
-      const uint32_t j = base + (uint32_t)(__ffsll((long long)cur) - 1);
-      cur &= cur - 1ull;
+      if (cur == 0u) break;
+      const uint32_t j = base + (uint32_t)(__ffs((int)cur) - 1);
+      cur &= cur - 1u;
       if (j != s)
         pair_terms<MASS, FEAT>(j, pi, vi, rho_i, q_i, m_i, spos, svel, sdq, smass, P, fx, fy, sx, sy, fa);
     }
@@ -496,7 +497,7 @@ __global__ void __launch_bounds__(256) k_force_integrate(
     const float2* __restrict__ spos, const float2* __restrict__ svel, const float2* __restrict__ sdq,
     const uint32_t* __restrict__ skey, const uint32_t* __restrict__ sid, const float* __restrict__ smass,
     uint32_t n, const uint32_t* __restrict__ start, StepParams P0, BatchTab bt, const DevBody* __restrict__ bodies,
-    const uint64_t* __restrict__ nmask, float4* __restrict__ state_out, uint32_t* __restrict__ key_out,
+    const uint32_t* __restrict__ nmask, float4* __restrict__ state_out, uint32_t* __restrict__ key_out,
     uint32_t* __restrict__ count_out, float2* __restrict__ dbg_force) {
   const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n) return;
@@ -543,7 +544,7 @@ __global__ void __launch_bounds__(256, 3) k_force_closure(
     const float* __restrict__ spres, const uint32_t* __restrict__ skey, const uint32_t* __restrict__ sid,
     const float* __restrict__ smass, const uint8_t* __restrict__ sphase, uint32_t n,
     const uint32_t* __restrict__ start, StepParams P0, BatchTab bt, const DevBody* __restrict__ bodies,
-    const uint64_t* __restrict__ nmask, MlpDev mlp, ClosureIO io, float4* __restrict__ state_out,
+    const uint32_t* __restrict__ nmask, MlpDev mlp, ClosureIO io, float4* __restrict__ state_out,
     uint32_t* __restrict__ key_out, uint32_t* __restrict__ count_out) {
   extern __shared__ __align__(16) unsigned char closure_smem[];
   MlpSmem& sm = *reinterpret_cast<MlpSmem*>(closure_smem);

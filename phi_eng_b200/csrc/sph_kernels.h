@@ -36,7 +36,7 @@ struct FluidBufs {
   uint8_t* sphase = nullptr; // sorted phase (F_PHASE)
   float2* sdq = nullptr;     // sorted (density, pressure / max(density,EPS)^2)
   float* spres = nullptr;    // sorted pressure
-  uint64_t* nmask = nullptr; // [3][cap] per-row neighbour masks written by K5, read by K6
+  uint32_t* nmask = nullptr; // [3][cap] per-row neighbour masks written by K5, read by K6
   // per bucket grid (sized by the number of buckets B)
   uint32_t* count = nullptr;    // particles per bucket, then the placement cursor
   uint32_t count_len = 0;       // B + 1 rounded up to the scan tile

@@ -54,7 +54,7 @@ constexpr size_t kOffSpos = align256(kOffSid + 4 * kN);                  // floa
 constexpr size_t kOffSvel = align256(kOffSpos + 8 * kN);                 // float2 [N]
 constexpr size_t kOffSdq = align256(kOffSvel + 8 * kN);                  // float2 [N]
 constexpr size_t kOffSpres = align256(kOffSdq + 8 * kN);                 // float [N]
-constexpr size_t kOffMask = align256(kOffSpres + 4 * kN);                // u64 [3N]
+constexpr size_t kOffMask = align256(kOffSpres + 4 * kN);                // u32 [3N] (room for 8 B each)
 constexpr size_t kOffCount = align256(kOffMask + 24 * kN);               // u32 [kCountLen]
 constexpr size_t kOffStart = align256(kOffCount + 4 * (size_t)kCountLen);  // u32 [kCountLen + 1]
 constexpr size_t kOffTiles = align256(kOffStart + 4 * ((size_t)kCountLen + 1));  // u32 [kScanTiles]
@@ -169,7 +169,7 @@ extern "C" int32_t phieng_sph_density_noalloc(const float* xy, uint32_t n, const
   b.svel = reinterpret_cast<float2*>(base + kOffSvel);
   b.sdq = reinterpret_cast<float2*>(base + kOffSdq);
   b.spres = reinterpret_cast<float*>(base + kOffSpres);
-  b.nmask = reinterpret_cast<uint64_t*>(base + kOffMask);
+  b.nmask = reinterpret_cast<uint32_t*>(base + kOffMask);
   b.count = reinterpret_cast<uint32_t*>(base + kOffCount);
   b.start = reinterpret_cast<uint32_t*>(base + kOffStart);
   b.tilesum = reinterpret_cast<uint32_t*>(base + kOffTiles);
