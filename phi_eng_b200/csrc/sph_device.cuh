@@ -225,8 +225,11 @@ __device__ __forceinline__ bool collide(float px, float py, float pr, const DevB
 __device__ __forceinline__ void walls(float& x, float& y, float& vx, float& vy,
                                       const DevBody* __restrict__ bodies, const StepParams& P) {
   for (uint32_t k = 0; k < P.nbodies; k++) {
-    const DevBody b = bodies[P.body_first + k];
-    if (fabsf(x - b.px) > b.ex + P.pr_pad || fabsf(y - b.py) > b.ey + P.pr_pad) continue;
+    const DevBody* bp = bodies + P.body_first + k;
+    // bounding-box reject first: only the centre and the padded extents are read
+    if (fabsf(x - __ldg(&bp->px)) > __ldg(&bp->ex) + P.pr_pad || fabsf(y - __ldg(&bp->py)) > __ldg(&bp->ey) + P.pr_pad)
+      continue;
+    const DevBody b = *bp;
     float nx, ny, depth;
     if (!collide(x, y, P.pr, b, nx, ny, depth)) continue;
     if (depth <= 0.0f) continue;

@@ -135,8 +135,9 @@ __global__ void __launch_bounds__(256) k_scan_reduce(const uint32_t* __restrict_
 }
 
 // start[i] = exclusive prefix of count[i]; count[i] is overwritten with the
-// same value (the placement cursor). Entries i <= m are written (m = number
-// of keys incl. the sentinel bucket; start[m] = particle count).
+// same value (the placement cursor). Whole scan tiles are written with
+// 16-byte stores (the arrays are padded to whole tiles); m = number of keys
+// incl. the sentinel bucket, start[m] = particle count.
 __global__ void __launch_bounds__(256) k_scan_down(uint32_t* __restrict__ count,
                                                    const uint32_t* __restrict__ tileoff, uint32_t m,
                                                    uint32_t* __restrict__ start) {
@@ -164,11 +165,13 @@ __global__ void __launch_bounds__(256) k_scan_down(uint32_t* __restrict__ count,
     v[q] = run;
     run += x;
   }
+  uint4* s4 = reinterpret_cast<uint4*>(start + base);
 #pragma unroll
-  for (int r = 0; r < 4; r++) c4[r] = make_uint4(v[4 * r], v[4 * r + 1], v[4 * r + 2], v[4 * r + 3]);
-#pragma unroll
-  for (int q = 0; q < 16; q++)
-    if (base + q <= m) start[base + q] = v[q];
+  for (int r = 0; r < 4; r++) {
+    const uint4 q = make_uint4(v[4 * r], v[4 * r + 1], v[4 * r + 2], v[4 * r + 3]);
+    c4[r] = q;
+    s4[r] = q;  // the padded tail past m gets the particle count: never read
+  }
 }
 
 // Slot in the bucket from the cursor. BY_SLOT walks the previous sort's
