@@ -24,12 +24,6 @@ namespace phieng {
 
 namespace {
 
-__device__ __forceinline__ uint32_t lanemask_lt() {
-  uint32_t m;
-  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
-  return m;
-}
-
 // ---------------------------------------------------------------- K2 bucket sort
 // Counting sort over the whole bucket key (a one-digit radix sort with radix
 // = number of buckets), then an in-bucket rank by id, so the final order is
@@ -62,10 +56,35 @@ __device__ __forceinline__ uint32_t block_incl_scan_256(uint32_t v, uint32_t* wa
   return x + add;
 }
 
-// Add a warp's keys to count[] with one atomic per distinct key.
+// Runs of equal keys over the active lanes in lane order (any active set):
+// a lane starts a run unless the nearest active lane below it holds the
+// same key. For the calling lane: *first = its run's first lane, *len = the
+// run's active lanes, *rank = active lanes of the run below this one.
+__device__ __forceinline__ void key_run(uint32_t act, uint32_t k, uint32_t lane, uint32_t* first, uint32_t* len,
+                                        uint32_t* rank) {
+  const uint32_t below = act & ((1u << lane) - 1u);
+  const int src = below ? 31 - __clz(below) : (int)lane;
+  const uint32_t prev = __shfl_sync(act, k, src);
+  const bool head = !below || prev != k;
+  const uint32_t heads = __ballot_sync(act, head);
+  const uint32_t f = 31u - (uint32_t)__clz(heads & (0xFFFFFFFFu >> (31u - lane)));
+  const uint32_t above = heads & ~(0xFFFFFFFFu >> (31u - lane));
+  const uint32_t upper = above ? ((1u << (__ffs(above) - 1)) - 1u) : 0xFFFFFFFFu;  // lanes below the next run
+  const uint32_t run = act & upper & ~((1u << f) - 1u);
+  *first = f;
+  *len = (uint32_t)__popc(run);
+  *rank = (uint32_t)__popc(run & ((1u << lane) - 1u));
+}
+
+// Add a warp's keys to count[] with one atomic per run of equal keys (keys
+// arrive in sorted-slot or id order, so a bucket's particles mostly sit in
+// consecutive lanes; a key split over several runs takes several atomics).
 __device__ __forceinline__ void count_key(uint32_t* __restrict__ count, uint32_t k) {
-  const uint32_t peers = __match_any_sync(__activemask(), k);
-  if ((peers & lanemask_lt()) == 0) atomicAdd(&count[k], (uint32_t)__popc(peers));
+  const uint32_t act = __activemask();
+  const uint32_t lane = threadIdx.x & 31u;
+  uint32_t first, len, rank;
+  key_run(act, k, lane, &first, &len, &rank);
+  if (first == lane) atomicAdd(&count[k], len);
 }
 
 // K1: key and bucket count of every particle (id order).
@@ -175,8 +194,8 @@ __global__ void __launch_bounds__(256) k_scan_down(uint32_t* __restrict__ count,
 }
 
 // Slot in the bucket from the cursor. BY_SLOT walks the previous sort's
-// order (keys nearly sorted: a warp shares few keys, so few atomics);
-// otherwise particles are taken in id order.
+// order (keys nearly sorted: a warp holds few runs of equal keys, so few
+// atomics); otherwise particles are taken in id order.
 template <bool BY_SLOT>
 __global__ void __launch_bounds__(256) k_place(const uint32_t* __restrict__ key,
                                                const uint32_t* __restrict__ sid_prev, uint32_t n,
@@ -186,13 +205,16 @@ __global__ void __launch_bounds__(256) k_place(const uint32_t* __restrict__ key,
   if (s >= n) return;
   const uint32_t id = BY_SLOT ? sid_prev[s] : s;
   const uint32_t k = key[id];
-  const uint32_t peers = __match_any_sync(__activemask(), k);
-  const uint32_t lt = lanemask_lt();
-  const uint32_t leader = __ffs(peers) - 1;
+  // one atomic per run of equal keys in consecutive lanes; a run's lanes take
+  // consecutive slots (any order inside a bucket is fine: k_fixup ranks by id)
+  const uint32_t act = __activemask();
+  const uint32_t lane = threadIdx.x & 31u;
+  uint32_t first, len, rank;
+  key_run(act, k, lane, &first, &len, &rank);
   uint32_t base = 0;
-  if ((peers & lt) == 0) base = atomicAdd(&cursor[k], (uint32_t)__popc(peers));
-  base = __shfl_sync(peers, base, leader);
-  const uint32_t slot = base + (uint32_t)__popc(peers & lt);
+  if (first == lane) base = atomicAdd(&cursor[k], len);
+  base = __shfl_sync(act, base, first);
+  const uint32_t slot = base + rank;
   tkey[slot] = k;
   tid_out[slot] = id;
 }
