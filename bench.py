@@ -47,14 +47,14 @@ HBM_FALLBACK = 6650.0
 #            fixup: read (key, id) 8 + start 8, write (key, id) 8,
 #            gather state 16 -> write pos 8 + vel 8                = 72 + 20 B/N
 #   density: read pos 8 + key 4; write (density, q) 8 + pressure 4,
-#            three 64-bit neighbour-row masks 24                    = 48
-#   force:   read pos 8, vel 8, (density, q) 8, key 4, id 4, masks 24;
-#            write state 16 + next key 4                             = 76
-DENSITY_BYTES = 48
-FORCE_BYTES = 76
+#            three 32-bit neighbour-row masks 12                    = 36
+#   force:   read pos 8, vel 8, (density, q) 8, key 4, id 4, masks 12;
+#            write state 16 + next key 4                             = 64
+DENSITY_BYTES = 36
+FORCE_BYTES = 64
 # DRAM bytes (read + write) of one launch of the named phase's kernel, from
 # the ncu capture summarised in profiles/<kernel>_<workload>.md.
-PROFILED_TRAFFIC = {("dam_break_1m", "force_integrate"): 60.917248e6 + 4.054272e6}
+PROFILED_TRAFFIC = {("dam_break_1m", "force_integrate"): 48.330752e6 + 2.260992e6}
 KERNELS_PER_STEP = 6  # scan reduce, scan down, place, fixup, density, force
 
 
