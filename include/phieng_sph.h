@@ -111,6 +111,28 @@ int32_t phieng_world_add_body(World2* world, float pos_x, float pos_y, uint32_t 
                               float b, float density, uint8_t is_static, float friction,
                               float restitution);
 
+/* ffi.rs:1209-1227 BodyDesc2D: blittable body descriptor for
+ * phieng_world_add_bodies (36 bytes; is_static is one byte + 3 pad bytes). */
+typedef struct BodyDesc2D {
+  float pos_x, pos_y;
+  uint32_t shape_tag;
+  float a, b;
+  float density;
+  uint8_t is_static;
+  uint8_t _pad[3];
+  float friction, restitution;
+} BodyDesc2D;
+#ifdef __cplusplus
+static_assert(sizeof(BodyDesc2D) == 36, "BodyDesc2D must match ffi.rs:1209-1227");
+#endif
+
+/* ffi.rs:1242 phieng_world_add_bodies — n descriptors validated and added
+ * exactly like phieng_world_add_body; out_ids[i] = new id or -1 (rejected,
+ * including dynamic bodies here). Returns the number added; 0 for null
+ * world / descs / out_ids. n capped at 1,000,000. Non-atomic, as the
+ * reference. */
+uint32_t phieng_world_add_bodies(World2* world, const BodyDesc2D* descs, uint32_t n, int32_t* out_ids);
+
 /* ffi.rs:999 / 1017 fluid config. set: 1 ok, 0 null or invalid (the
  * validation of fluid2_from_ffi, ffi.rs:773-855; world unchanged on
  * reject). get: 1 ok, 0 null. */

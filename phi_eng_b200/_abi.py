@@ -86,6 +86,26 @@ def default_config() -> FluidConfig2Ffi:
     return c
 
 
+class BodyDesc2D(C.Structure):
+    """#[repr(C)] BodyDesc2D (crates/engine/src/ffi.rs:1209-1227), 36 bytes."""
+
+    _fields_ = [
+        ("pos_x", C.c_float),
+        ("pos_y", C.c_float),
+        ("shape_tag", C.c_uint32),
+        ("a", C.c_float),
+        ("b", C.c_float),
+        ("density", C.c_float),
+        ("is_static", C.c_uint8),
+        ("_pad", C.c_uint8 * 3),
+        ("friction", C.c_float),
+        ("restitution", C.c_float),
+    ]
+
+
+assert C.sizeof(BodyDesc2D) == 36
+
+
 class PhiengSphStatus(C.Structure):
     _fields_ = [
         ("error", C.c_int32),
@@ -146,6 +166,7 @@ SIGNATURES = {
         [_P, C.c_float, C.c_float, C.c_uint32, C.c_float, C.c_float, C.c_float, C.c_uint8,
          C.c_float, C.c_float],
     ),
+    "phieng_world_add_bodies": (C.c_uint32, [_P, C.POINTER(BodyDesc2D), C.c_uint32, C.POINTER(C.c_int32)]),
     "phieng_world_set_fluid_config": (C.c_int32, [_P, C.POINTER(FluidConfig2Ffi)]),
     "phieng_world_get_fluid_config": (C.c_int32, [_P, C.POINTER(FluidConfig2Ffi)]),
     "phieng_world_fluid_add": (C.c_uint32, [_P, _F, C.c_uint32]),

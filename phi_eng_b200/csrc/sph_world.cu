@@ -918,6 +918,19 @@ int32_t phieng_world_add_body(World2* w, float px, float py, uint32_t shape_tag,
   return (int32_t)(w->bodies.size() - 1);
 }
 
+uint32_t phieng_world_add_bodies(World2* w, const BodyDesc2D* descs, uint32_t n, int32_t* out_ids) {
+  if (!w || !descs || !out_ids) return 0;
+  n = std::min<uint32_t>(n, 1000000u);
+  uint32_t added = 0;
+  for (uint32_t i = 0; i < n; i++) {
+    const BodyDesc2D& d = descs[i];
+    out_ids[i] = phieng_world_add_body(w, d.pos_x, d.pos_y, d.shape_tag, d.a, d.b, d.density, d.is_static,
+                                       d.friction, d.restitution);
+    if (out_ids[i] >= 0) added++;
+  }
+  return added;
+}
+
 int32_t phieng_world_set_fluid_config(World2* w, const FluidConfig2Ffi* cfg) {
   if (!w || !cfg || w->is_batch()) return 0;
   if (!valid_config(*cfg)) return 0;

@@ -245,3 +245,25 @@ def test_python_mirror_without_gpu():
     assert len(w.fluid) == 2
     assert w.fluid.particles.shape == (2, 4)
     w.close()
+
+
+# ffi.rs:1242 phieng_world_add_bodies: bulk add with per-descriptor rejection
+def test_add_bodies_bulk(lib):
+    D = _abi.BodyDesc2D
+    descs = (D * 5)(
+        D(0.0, -1.0, 1, 5.0, 0.5, 1.0, 1, (0, 0, 0), 0.4, 0.1),          # box, ok
+        D(1.0, 2.0, 0, 0.3, 0.0, 1.0, 1, (0, 0, 0), 0.4, 0.1),           # circle, ok
+        D(float("nan"), 0.0, 1, 1.0, 1.0, 1.0, 1, (0, 0, 0), 0.4, 0.1),  # non-finite position
+        D(0.0, 0.0, 7, 1.0, 1.0, 1.0, 1, (0, 0, 0), 0.4, 0.1),           # unknown shape
+        D(0.0, 0.0, 1, 1.0, 1.0, 1.0, 0, (0, 0, 0), 0.4, 0.1),           # dynamic: unsupported here
+    )
+    ids = (C.c_int32 * 5)()
+    w = lib.phieng_world_new()
+    assert lib.phieng_world_add_bodies(w, descs, 5, ids) == 2
+    assert list(ids) == [0, 1, -1, -1, -1]
+    assert lib.phieng_world_body_count(w) == 2
+    assert lib.phieng_world_add_bodies(None, descs, 5, ids) == 0
+    assert lib.phieng_world_add_bodies(w, None, 5, ids) == 0
+    assert lib.phieng_world_add_bodies(w, descs, 5, None) == 0
+    assert C.sizeof(_abi.BodyDesc2D) == 36 and _abi.BodyDesc2D.friction.offset == 28
+    lib.phieng_world_free(w)
