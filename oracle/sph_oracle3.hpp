@@ -1,0 +1,440 @@
+// ORACLE — TEST INFRASTRUCTURE ONLY.
+//
+// CPU restatement of the reference's 3D SPH fluid step
+// (crates/dynamics/src/fluid3.rs), for the static-wall feature set the GPU
+// 3D path implements: particles, hash grid, density + EOS, pressure force
+// (+ Monaghan AV, cohesion), XSPH integrate in the reference's in-place order
+// (REF_SEQ) or in Jacobi order (what the GPU computes), sphere / box / capsule
+// walls with wall friction, CFL substeps. Rigid bodies added through the C
+// ABI (phieng_world3_add_body, crates/engine/src/ffi.rs:3703-3760) carry the
+// identity rotation, so the box and capsule local frames are the world axes:
+// glam's quaternion products with the identity return the vector unchanged.
+// Float arithmetic follows glam 0.29's scalar Vec3 (dot = (x*x + y*y) + z*z,
+// component-wise operators); built with -ffp-contract=off.
+#pragma once
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <unordered_map>
+#include <vector>
+
+#include "sph_oracle.hpp"
+
+namespace oracle {
+
+struct Body3 {
+  int shape = 1;  // 0 sphere (a = radius), 1 box (a, b, c half extents), 2 capsule (a = radius, b = half length along y)
+  float px = 0, py = 0, pz = 0;
+  float a = 0, b = 0, c = 0;
+};
+
+template <class R>
+struct Particle3 {
+  R x, y, z, vx, vy, vz;
+  R density, pressure, mass;
+  uint8_t phase;
+};
+
+template <class R>
+class Fluid3 {
+ public:
+  Config cfg;  // FluidConfig3 has the same fields and defaults as FluidConfig2 (fluid3.rs:51-137)
+  std::vector<Particle3<R>> particles;
+  std::vector<Body3> bodies;
+  R gx = 0, gy = (R)-9.81f, gz = 0;  // World3::new gravity
+  R time = 0;
+  size_t cap = 4096;
+  int pow_mode = 1;
+  std::vector<R> fx, fy, fz;
+
+  static R dot3(R ax, R ay, R az, R bx, R by, R bz) { return ax * bx + ay * by + az * bz; }
+
+  // poly6 (fluid3.rs:220-229): 315/(64 pi h^9) (h^2 - r^2)^3
+  static R poly6(R r2, R h) {
+    if (r2 >= h * h || r2 < (R)0) return (R)0;
+    R h2 = h * h;
+    R t = h2 - r2;
+    return (R)315.0 / ((R)64.0 * Consts<R>::pi() * h2 * h2 * h2 * h2 * h) * t * t * t;
+  }
+  // spiky gradient (fluid3.rs:232-240): -45/(pi h^6) (h - r)^2 r_vec / r
+  static void spiky_grad(R rx, R ry, R rz, R r, R h, R& gx_, R& gy_, R& gz_) {
+    if (r >= h || r < (R)kEps) {
+      gx_ = gy_ = gz_ = 0;
+      return;
+    }
+    R s = (R)-45.0 / (Consts<R>::pi() * h * h * h * h * h * h) * (h - r) * (h - r);
+    gx_ = rx / r * s;
+    gy_ = ry / r * s;
+    gz_ = rz / r * s;
+  }
+  static R pressure(R density, R rest_density, R stiffness, R gamma, int pow_mode = 1) {
+    return Fluid<R>::pressure(density, rest_density, stiffness, gamma, pow_mode);
+  }
+  // Monaghan term (fluid3.rs:254-270)
+  static R artificial_pressure(R dx, R dy, R dz, R vx, R vy, R vz, R r_sq, R h, R rho_bar, R c, R alpha) {
+    R vd = dot3(vx, vy, vz, dx, dy, dz);
+    if (vd >= (R)0) return (R)0;
+    R mu = h * vd / (r_sq + (R)0.01f * h * h);
+    return -alpha * c * mu / rmax(rho_bar, (R)kEps);
+  }
+  static R cohesion(R dist, R h) { return dist >= h ? (R)0 : (R)1.0 - dist / h; }
+
+  size_t add_particles_phase(const float* xyz, const uint8_t* ph, size_t n_in) {
+    size_t room = cap > particles.size() ? cap - particles.size() : 0;
+    size_t n = std::min(room, n_in);
+    for (size_t i = 0; i < n; i++) {
+      uint8_t p = ph ? ph[i] : 0;
+      size_t k = std::min<size_t>(p, 3);
+      Particle3<R> q;
+      q.x = (R)xyz[3 * i];
+      q.y = (R)xyz[3 * i + 1];
+      q.z = (R)xyz[3 * i + 2];
+      q.vx = q.vy = q.vz = 0;
+      q.density = (R)cfg.phase_rest_density[k];
+      q.pressure = 0;
+      q.mass = rmax((R)cfg.phase_mass[k], (R)0);
+      q.phase = p;
+      particles.push_back(q);
+    }
+    return n;
+  }
+
+  // ---- grid (fluid3.rs:282-343) ----
+  struct Key {
+    int32_t x, y, z;
+    bool operator==(const Key& o) const { return x == o.x && y == o.y && z == o.z; }
+  };
+  struct KeyHash {
+    size_t operator()(const Key& k) const {
+      return ((size_t)(uint32_t)k.x * 73856093u) ^ ((size_t)(uint32_t)k.y * 19349663u) ^ ((size_t)(uint32_t)k.z * 83492791u);
+    }
+  };
+  std::unordered_map<Key, std::vector<uint32_t>, KeyHash> grid;
+
+  void cell_of(R x, R y, R z, int32_t& cx, int32_t& cy, int32_t& cz) const {
+    R hg = (R)cfg.smoothing_length;
+    cx = sat_i32(std::floor(x / hg));
+    cy = sat_i32(std::floor(y / hg));
+    cz = sat_i32(std::floor(z / hg));
+  }
+  void rebuild_grid() {
+    for (auto& kv : grid) kv.second.clear();
+    for (size_t i = 0; i < particles.size(); i++) {
+      const auto& p = particles[i];
+      if (!finite(p.x) || !finite(p.y) || !finite(p.z)) continue;
+      Key k;
+      cell_of(p.x, p.y, p.z, k.x, k.y, k.z);
+      grid[k].push_back((uint32_t)i);
+    }
+  }
+  // oz outer, oy, ox inner; ids ascending; keep d2 < h*h (includes i)
+  void neighbors_of(R px, R py, R pz, const std::vector<Particle3<R>>& ps, std::vector<uint32_t>& out) const {
+    out.clear();
+    R hg = (R)cfg.smoothing_length;
+    int32_t cx, cy, cz;
+    cell_of(px, py, pz, cx, cy, cz);
+    for (int oz = -1; oz <= 1; oz++)
+      for (int oy = -1; oy <= 1; oy++)
+        for (int ox = -1; ox <= 1; ox++) {
+          int64_t xx = (int64_t)cx + ox, yy = (int64_t)cy + oy, zz = (int64_t)cz + oz;
+          if (xx < INT32_MIN || xx > INT32_MAX || yy < INT32_MIN || yy > INT32_MAX || zz < INT32_MIN ||
+              zz > INT32_MAX)
+            continue;
+          auto it = grid.find(Key{(int32_t)xx, (int32_t)yy, (int32_t)zz});
+          if (it == grid.end()) continue;
+          for (uint32_t j : it->second) {
+            R dx = ps[j].x - px, dy = ps[j].y - py, dz = ps[j].z - pz;
+            R d2 = dot3(dx, dy, dz, dx, dy, dz);
+            if (d2 < hg * hg) out.push_back(j);
+          }
+        }
+  }
+
+  // ---- density + pressure (fluid3.rs:639-658) ----
+  void compute_density_pressure(R h) {
+    std::vector<uint32_t> nb;
+    R rho_cap = (R)3.0 * rmax((R)cfg.rest_density, (R)kEps);
+    for (size_t i = 0; i < particles.size(); i++) {
+      const auto& pi = particles[i];
+      neighbors_of(pi.x, pi.y, pi.z, particles, nb);
+      R rho = 0;
+      for (uint32_t j : nb) {
+        R dx = particles[j].x - pi.x, dy = particles[j].y - pi.y, dz = particles[j].z - pi.z;
+        rho += particles[j].mass * poly6(dot3(dx, dy, dz, dx, dy, dz), h);
+      }
+      particles[i].density = rclamp(rho, (R)0, rho_cap);
+    }
+    for (auto& p : particles) {
+      R rho0 = (R)cfg.phase_rest_density[std::min<int>(p.phase, 3)];
+      p.pressure = pressure(p.density, rho0, (R)cfg.stiffness, (R)cfg.gamma, pow_mode);
+    }
+  }
+
+  // ---- pressure force (+AV, cohesion) (fluid3.rs:1040-1090) ----
+  void compute_forces(R h) {
+    std::vector<uint32_t> nb;
+    size_t n = particles.size();
+    fx.assign(n, 0);
+    fy.assign(n, 0);
+    fz.assign(n, 0);
+    R c_s = std::sqrt(rmax((R)cfg.stiffness, (R)0));
+    for (size_t i = 0; i < n; i++) {
+      const auto& P = particles[i];
+      neighbors_of(P.x, P.y, P.z, particles, nb);
+      R rho_i = rmax(P.density, (R)kEps);
+      R p_i = P.pressure;
+      R fxi = 0, fyi = 0, fzi = 0;
+      for (uint32_t j : nb) {
+        if (j == i) continue;
+        const auto& pj = particles[j];
+        R rho_j = rmax(pj.density, (R)kEps);
+        R dx = P.x - pj.x, dy = P.y - pj.y, dz = P.z - pj.z;
+        R dist = std::sqrt(dot3(dx, dy, dz, dx, dy, dz));
+        R gx_, gy_, gz_;
+        spiky_grad(dx, dy, dz, dist, h, gx_, gy_, gz_);
+        R term = p_i / (rho_i * rho_i) + pj.pressure / (rho_j * rho_j);
+        if ((R)cfg.artificial_viscosity > (R)0 && dist > (R)kEps) {
+          R rho_bar = (R)0.5 * (rho_i + rho_j);
+          term += artificial_pressure(dx, dy, dz, P.vx - pj.vx, P.vy - pj.vy, P.vz - pj.vz, dist * dist, h, rho_bar,
+                                      c_s, (R)cfg.artificial_viscosity);
+        }
+        R mt = pj.mass * term;
+        fxi -= gx_ * mt;
+        fyi -= gy_ * mt;
+        fzi -= gz_ * mt;
+        if ((R)cfg.surface_tension > (R)0 && dist > (R)kEps) {
+          R coh = cohesion(dist, h);
+          if (coh > (R)0) {
+            R s = (R)cfg.surface_tension * P.mass * pj.mass * coh;
+            fxi -= dx / dist * s;
+            fyi -= dy / dist * s;
+            fzi -= dz / dist * s;
+          }
+        }
+      }
+      fx[i] = fxi;
+      fy[i] = fyi;
+      fz[i] = fzi;
+    }
+  }
+
+  // ---- integrate (fluid3.rs:1092-1138) ----
+  void integrate(R h, R dt, Mode mode) {
+    std::vector<uint32_t> nb;
+    size_t n = particles.size();
+    std::vector<Particle3<R>> snap;
+    if (mode == JACOBI) snap = particles;
+    const std::vector<Particle3<R>>& src = (mode == JACOBI) ? snap : particles;
+    R visc = (R)cfg.viscosity, vmax = (R)cfg.max_velocity;
+    for (size_t i = 0; i < n; i++) {
+      neighbors_of(src[i].x, src[i].y, src[i].z, src, nb);
+      R rho_i = rmax(src[i].density, (R)kEps);
+      R ax = gx + fx[i] / rho_i, ay = gy + fy[i] / rho_i, az = gz + fz[i] / rho_i;
+      R vx = src[i].vx + ax * dt, vy = src[i].vy + ay * dt, vz = src[i].vz + az * dt;
+      if (visc > (R)0) {
+        R sx = 0, sy = 0, sz = 0;
+        for (uint32_t j : nb) {
+          if (j == i) continue;
+          const auto& pj = src[j];
+          R rho_bar = (R)0.5 * (rho_i + rmax(pj.density, (R)kEps));
+          R dx = pj.x - src[i].x, dy = pj.y - src[i].y, dz = pj.z - src[i].z;
+          R w = poly6(dot3(dx, dy, dz, dx, dy, dz), h);
+          R mr = pj.mass / rho_bar;
+          sx += (pj.vx - src[i].vx) * mr * w;
+          sy += (pj.vy - src[i].vy) * mr * w;
+          sz += (pj.vz - src[i].vz) * mr * w;
+        }
+        vx += sx * visc;
+        vy += sy * visc;
+        vz += sz * visc;
+      }
+      R speed = std::sqrt(dot3(vx, vy, vz, vx, vy, vz));
+      if (speed > vmax) {
+        R sc = vmax / speed;
+        vx *= sc;
+        vy *= sc;
+        vz *= sc;
+      }
+      if (!finite(vx) || !finite(vy) || !finite(vz)) vx = vy = vz = 0;
+      R nx = src[i].x + vx * dt, ny = src[i].y + vy * dt, nz = src[i].z + vz * dt;
+      if (!finite(nx) || !finite(ny) || !finite(nz)) {
+        nx = src[i].x;
+        ny = src[i].y;
+        nz = src[i].z;
+      }
+      particles[i].vx = vx;
+      particles[i].vy = vy;
+      particles[i].vz = vz;
+      particles[i].x = nx;
+      particles[i].y = ny;
+      particles[i].z = nz;
+    }
+  }
+
+  // ---- particle vs static body (fluid3.rs:471-590, identity rotation) ----
+  static bool collide(R px, R py, R pz, R pr, const Body3& b, R& nx, R& ny, R& nz, R& depth) {
+    R rx = px - (R)b.px, ry = py - (R)b.py, rz = pz - (R)b.pz;
+    if (b.shape == 0) {
+      R dist = std::sqrt(dot3(rx, ry, rz, rx, ry, rz));
+      R radius = (R)b.a;
+      if (dist >= radius + pr) return false;
+      if (dist > (R)kEps) {
+        nx = rx / dist;
+        ny = ry / dist;
+        nz = rz / dist;
+      } else {
+        nx = 1;
+        ny = 0;
+        nz = 0;
+      }
+      depth = radius + pr - dist;
+      return true;
+    }
+    if (b.shape == 1) {
+      R hx = (R)b.a, hy = (R)b.b, hz = (R)b.c;
+      R cxl = rclamp(rx, -hx, hx), cyl = rclamp(ry, -hy, hy), czl = rclamp(rz, -hz, hz);
+      R ddx = rx - cxl, ddy = ry - cyl, ddz = rz - czl;
+      if (dot3(ddx, ddy, ddz, ddx, ddy, ddz) > (R)kEpsSq) {
+        R dist = std::sqrt(dot3(ddx, ddy, ddz, ddx, ddy, ddz));
+        if (dist >= pr) return false;
+        nx = ddx / dist;
+        ny = ddy / dist;
+        nz = ddz / dist;
+        depth = pr - dist;
+        return true;
+      }
+      R dx = hx - std::fabs(rx), dy = hy - std::fabs(ry), dz = hz - std::fabs(rz);
+      // signum().copysign(1.0) = +1 (a NaN stays a positive NaN)
+      if (dx <= dy && dx <= dz) {
+        nx = (rx != rx) ? std::fabs(rx) : (R)1;
+        ny = 0;
+        nz = 0;
+        depth = pr + dx;
+      } else if (dy <= dz) {
+        nx = 0;
+        ny = (ry != ry) ? std::fabs(ry) : (R)1;
+        nz = 0;
+        depth = pr + dy;
+      } else {
+        nx = 0;
+        ny = 0;
+        nz = (rz != rz) ? std::fabs(rz) : (R)1;
+        depth = pr + dz;
+      }
+      return true;
+    }
+    // capsule along local y
+    R r = (R)b.a, hl = (R)b.b;
+    R sy = rclamp(ry, -hl, hl);
+    R ddx = rx, ddy = ry - sy, ddz = rz;
+    if (dot3(ddx, ddy, ddz, ddx, ddy, ddz) > (R)kEpsSq) {
+      R dist = std::sqrt(dot3(ddx, ddy, ddz, ddx, ddy, ddz));
+      if (dist >= r + pr) return false;
+      nx = ddx / dist;
+      ny = ddy / dist;
+      nz = ddz / dist;
+      depth = r + pr - dist;
+      return true;
+    }
+    // on the axis: radial direction (x, 0, z) by glam's normalize_or_zero
+    // (multiplication by the reciprocal length), else +x
+    R l2 = dot3(rx, (R)0, rz, rx, (R)0, rz);
+    if (l2 > (R)kEpsSq) {
+      R rcp = (R)1 / std::sqrt(l2);
+      if (finite(rcp) && rcp > (R)0) {
+        nx = rx * rcp;
+        ny = (R)0 * rcp;
+        nz = rz * rcp;
+      } else {
+        nx = ny = nz = 0;
+      }
+    } else {
+      nx = 1;
+      ny = 0;
+      nz = 0;
+    }
+    depth = pr + r - std::sqrt(dot3(ddx, ddy, ddz, ddx, ddy, ddz));
+    return true;
+  }
+
+  // boundary pass (fluid3.rs:1140-1176): statics, no impulse
+  void boundaries() {
+    R pr = rmax((R)cfg.particle_radius, (R)0);
+    for (auto& p : particles) {
+      for (const Body3& b : bodies) {
+        R nx, ny, nz, depth;
+        if (!collide(p.x, p.y, p.z, pr, b, nx, ny, nz, depth)) continue;
+        if (depth <= (R)0) continue;
+        p.x = p.x + nx * depth;
+        p.y = p.y + ny * depth;
+        p.z = p.z + nz * depth;
+        R vn = dot3(p.vx, p.vy, p.vz, nx, ny, nz);
+        if (vn < (R)0) {
+          p.vx -= nx * vn;
+          p.vy -= ny * vn;
+          p.vz -= nz * vn;
+          if ((R)cfg.wall_friction > (R)0) {
+            R mu = rclamp((R)cfg.wall_friction, (R)0, (R)1);
+            R vtx = p.vx, vty = p.vy, vtz = p.vz;
+            R wvx = 0, wvy = 0, wvz = 0;
+            R wdot = dot3(wvx, wvy, wvz, nx, ny, nz);
+            R wtx = wvx - nx * wdot, wty = wvy - ny * wdot, wtz = wvz - nz * wdot;
+            R dvx = (wtx - vtx) * mu, dvy = (wty - vty) * mu, dvz = (wtz - vtz) * mu;
+            p.vx += dvx;
+            p.vy += dvy;
+            p.vz += dvz;
+          }
+        }
+      }
+    }
+  }
+
+  // CFL substeps (fluid3.rs:610-637)
+  uint32_t cfl_substeps(R dt) const {
+    uint32_t mx = std::max<uint32_t>(cfg.max_substeps, 1);
+    if ((R)cfg.cfl <= (R)0 || mx <= 1) return 1;
+    R h = rmax((R)cfg.smoothing_length, (R)kEps);
+    R rho0 = rmax((R)cfg.rest_density, (R)kEps);
+    R c0 = ((R)cfg.gamma == (R)1.0) ? std::sqrt(rmax((R)cfg.stiffness, (R)0))
+                                    : std::sqrt((R)cfg.gamma * rmax((R)cfg.stiffness, (R)0) * rho0);
+    R vm = 0;
+    for (const auto& p : particles) vm = rmax(vm, std::sqrt(dot3(p.vx, p.vy, p.vz, p.vx, p.vy, p.vz)));
+    R speed = c0 + vm;
+    if (!finite(speed) || speed <= (R)kEps) return 1;
+    R dt_max = (R)cfg.cfl * h / speed;
+    if (!finite(dt_max) || dt_max <= (R)0) return 1;
+    R q = std::ceil(dt / dt_max);
+    int64_t k;
+    if (q != q)
+      k = 0;
+    else if (q >= (R)9.2233720368547758e18)
+      k = INT64_MAX;
+    else if (q <= (R)-9.2233720368547758e18)
+      k = INT64_MIN;
+    else
+      k = (int64_t)q;
+    k = std::max<int64_t>(1, std::min<int64_t>(k, mx));
+    return (uint32_t)k;
+  }
+
+  void substep(R dt, Mode mode) {
+    R h = rmax((R)cfg.smoothing_length, (R)kEps);
+    rebuild_grid();
+    compute_density_pressure(h);
+    compute_forces(h);
+    integrate(h, dt, mode);
+    boundaries();
+  }
+
+  void world_step(R dt, Mode mode) {
+    if (cfg.enabled && !particles.empty() && dt > (R)0) {
+      uint32_t n = cfl_substeps(dt);
+      R sub = dt / (R)n;
+      for (uint32_t k = 0; k < n; k++) substep(sub, mode);
+    }
+    time += dt;
+  }
+};
+
+}  // namespace oracle

@@ -33,7 +33,7 @@ UNITS = [
     ("sph_noalloc.cu", EXACT),
     ("sph_mlp.cu", EXACT),
 ]
-HEADERS = ["sph_device.cuh", "sph_kernels.h", "sph_mlp.cuh", "sph_mlp_host.h"]
+HEADERS = ["sph_device.cuh", "sph_kernels.h", "sph_mlp.cuh", "sph_mlp_host.h", "sph_warp.cuh", "sph_host.h"]
 
 
 def _mtime(p: str) -> float:

@@ -145,7 +145,8 @@ __device__ __forceinline__ float powf_cr(float x, float g) {
 }
 
 // equation of state (fluid.rs:290-297)
-__device__ __forceinline__ float eos(float density, float rho0, const StepParams& P) {
+template <class PP>
+__device__ __forceinline__ float eos(float density, float rho0, const PP& P) {
   if (!(P.flags & F_TAIT)) {
     return fmaxf(__fmul_rn(P.stiffness, __fsub_rn(density, rho0)), 0.0f);
   }

@@ -19,6 +19,7 @@
 #include <cuda_runtime.h>
 
 #include "sph_kernels.h"
+#include "sph_warp.cuh"
 
 namespace phieng {
 
@@ -54,37 +55,6 @@ __device__ __forceinline__ uint32_t block_incl_scan_256(uint32_t v, uint32_t* wa
   uint32_t add = 0;
   for (uint32_t k = 0; k < w; k++) add += warp_tot[k];
   return x + add;
-}
-
-// Runs of equal keys over the active lanes in lane order (any active set):
-// a lane starts a run unless the nearest active lane below it holds the
-// same key. For the calling lane: *first = its run's first lane, *len = the
-// run's active lanes, *rank = active lanes of the run below this one.
-__device__ __forceinline__ void key_run(uint32_t act, uint32_t k, uint32_t lane, uint32_t* first, uint32_t* len,
-                                        uint32_t* rank) {
-  const uint32_t below = act & ((1u << lane) - 1u);
-  const int src = below ? 31 - __clz(below) : (int)lane;
-  const uint32_t prev = __shfl_sync(act, k, src);
-  const bool head = !below || prev != k;
-  const uint32_t heads = __ballot_sync(act, head);
-  const uint32_t f = 31u - (uint32_t)__clz(heads & (0xFFFFFFFFu >> (31u - lane)));
-  const uint32_t above = heads & ~(0xFFFFFFFFu >> (31u - lane));
-  const uint32_t upper = above ? ((1u << (__ffs(above) - 1)) - 1u) : 0xFFFFFFFFu;  // lanes below the next run
-  const uint32_t run = act & upper & ~((1u << f) - 1u);
-  *first = f;
-  *len = (uint32_t)__popc(run);
-  *rank = (uint32_t)__popc(run & ((1u << lane) - 1u));
-}
-
-// Add a warp's keys to count[] with one atomic per run of equal keys (keys
-// arrive in sorted-slot or id order, so a bucket's particles mostly sit in
-// consecutive lanes; a key split over several runs takes several atomics).
-__device__ __forceinline__ void count_key(uint32_t* __restrict__ count, uint32_t k) {
-  const uint32_t act = __activemask();
-  const uint32_t lane = threadIdx.x & 31u;
-  uint32_t first, len, rank;
-  key_run(act, k, lane, &first, &len, &rank);
-  if (first == lane) atomicAdd(&count[k], len);
 }
 
 // K1: key and bucket count of every particle (id order).
@@ -764,16 +734,30 @@ void enqueue_keys(const FluidBufs& b, uint32_t n, const GridPlan& g, cudaStream_
     k_keys<false><<<cdiv(n, 256), 256, 0, st>>>(b.state, n, g, b.batch, b.key, b.count);
 }
 
+void enqueue_bucket_place(const BucketSort& bs, uint32_t n, uint32_t m, bool by_slot, cudaStream_t st) {
+  if (n == 0) return;
+  const uint32_t nt = cdiv(m, kScanTile);
+  k_scan_reduce<<<nt, 256, 0, st>>>(bs.count, bs.tilesum, nt, bs.done);
+  k_scan_down<<<nt, 256, 0, st>>>(bs.count, bs.tilesum, m, bs.start);
+  if (by_slot)
+    k_place<true><<<cdiv(n, 256), 256, 0, st>>>(bs.key, bs.sid_prev, n, bs.count, bs.tkey, bs.tid);
+  else
+    k_place<false><<<cdiv(n, 256), 256, 0, st>>>(bs.key, bs.sid_prev, n, bs.count, bs.tkey, bs.tid);
+}
+
 void enqueue_sort_and_ranges(const FluidBufs& b, uint32_t n, const StepParams& P, bool by_slot, cudaStream_t st) {
   if (n == 0) return;
   const uint32_t m = P.grid.sentinel + 1;  // all buckets and the non-finite sentinel
-  const uint32_t nt = cdiv(m, kScanTile);
-  k_scan_reduce<<<nt, 256, 0, st>>>(b.count, b.tilesum, nt, b.done);
-  k_scan_down<<<nt, 256, 0, st>>>(b.count, b.tilesum, m, b.start);
-  if (by_slot)
-    k_place<true><<<cdiv(n, 256), 256, 0, st>>>(b.key, b.sid, n, b.count, b.tkey, b.tid);
-  else
-    k_place<false><<<cdiv(n, 256), 256, 0, st>>>(b.key, b.sid, n, b.count, b.tkey, b.tid);
+  BucketSort bs;
+  bs.count = b.count;
+  bs.tilesum = b.tilesum;
+  bs.done = b.done;
+  bs.start = b.start;
+  bs.key = b.key;
+  bs.sid_prev = b.sid;
+  bs.tkey = b.tkey;
+  bs.tid = b.tid;
+  enqueue_bucket_place(bs, n, m, by_slot, st);
   GatherArgs ga;
   ga.state = b.state;
   ga.mass = b.mass;

@@ -67,6 +67,23 @@ void enqueue_keys(const FluidBufs& b, uint32_t n, const GridPlan& g, cudaStream_
 // for locality; otherwise particles are placed in id order.
 void enqueue_sort_and_ranges(const FluidBufs& b, uint32_t n, const StepParams& P, bool by_slot, cudaStream_t st);
 
+// The dimension-independent part of the bucket sort: scan the bucket counts
+// of keys [0, m) into the start table (count becomes the placement cursor),
+// then give every particle a slot inside its bucket (tkey / tid; the in-bucket
+// rank by id and the gather are the caller's). by_slot: sid_prev holds the
+// previous sort's order (walked for locality), else ids are taken in order.
+struct BucketSort {
+  uint32_t* count = nullptr;
+  uint32_t* tilesum = nullptr;
+  uint32_t* done = nullptr;
+  uint32_t* start = nullptr;
+  const uint32_t* key = nullptr;
+  const uint32_t* sid_prev = nullptr;
+  uint32_t* tkey = nullptr;
+  uint32_t* tid = nullptr;
+};
+void enqueue_bucket_place(const BucketSort& bs, uint32_t n, uint32_t m, bool by_slot, cudaStream_t st);
+
 // K5: density + EOS in sorted order.
 void enqueue_density(const FluidBufs& b, uint32_t n, const StepParams& P, cudaStream_t st);
 
