@@ -402,6 +402,123 @@ uint32_t phieng_sph_debug_sorted(World2* world, uint32_t* ids, uint32_t* keys, u
 uint32_t phieng_sph_debug_neighbors(World2* world, uint32_t* counts, uint32_t* lists,
                                     uint32_t max_per, uint32_t max);
 
+/* ======================================================================
+ * 3D SPH world (crates/dynamics/src/fluid3.rs behind ffi.rs:3199-3885).
+ * The fluid step of World3 with static sphere / box / capsule walls; the
+ * other World3 subsystems (rigid dynamics, joints, queries) are not part
+ * of this library.
+ * ====================================================================== */
+
+/* Opaque 3D world handle (reference: Box<World3>, ffi.rs:3199). */
+typedef struct World3 World3;
+
+/* 3D shape tags (ffi.rs:3192-3195). */
+#define PHIENG_SHAPE3_SPHERE 0u
+#define PHIENG_SHAPE3_BOX 1u
+#define PHIENG_SHAPE3_CAPSULE 2u
+
+/* FluidConfig3Ffi (ffi.rs:744-767) has the fields, layout, defaults
+ * (fluid3.rs:108-135) and validation (fluid3_from_ffi, ffi.rs:857) of
+ * the 2D config. */
+typedef FluidConfig2Ffi FluidConfig3Ffi;
+
+/* ffi.rs:3199 / 3209: create / destroy (free(NULL) is a no-op). Gravity
+ * starts at (0, -9.81, 0), the clock at 0. */
+World3* phieng_world3_new(void);
+void phieng_world3_free(World3* world);
+
+/* ffi.rs:3221: advance by min(dt, 1/15); ignored for null, non-finite or
+ * dt <= 0. The fluid phase runs its CFL substeps; the clock advances by dt. */
+void phieng_world3_step(World3* world, float dt);
+
+/* ffi.rs:3234: gravity (ignored when any component is non-finite). */
+void phieng_world3_set_gravity(World3* world, float gx, float gy, float gz);
+
+/* ffi.rs:1091 / 1106: clock. 1 ok, 0 null or non-finite. */
+int32_t phieng_world3_set_time(World3* world, float t);
+int32_t phieng_world3_get_time(World3* world, float* out);
+
+/* ffi.rs:3387: number of bodies, -1 for null. */
+int32_t phieng_world3_body_count(World3* world);
+
+/* ffi.rs:3703 phieng_world3_add_body — PHIENG_SHAPE3_SPHERE (a = radius),
+ * PHIENG_SHAPE3_BOX (a, b, c = half extents), PHIENG_SHAPE3_CAPSULE (a =
+ * radius, b = half length along y); at (pos_x, pos_y, pos_z) with the
+ * identity rotation. Returns the body id or -1 on invalid input. Static
+ * bodies only: is_static == 0 returns -1 here. */
+int32_t phieng_world3_add_body(World3* world, float pos_x, float pos_y, float pos_z, uint32_t shape_tag,
+                               float a, float b, float c, float density, uint8_t is_static, float friction,
+                               float restitution);
+
+/* ffi.rs:3767-3786 BodyDesc3D (44 bytes). */
+typedef struct BodyDesc3D {
+  float pos_x, pos_y, pos_z;
+  uint32_t shape_tag;
+  float a, b, c;
+  float density;
+  uint8_t is_static;
+  uint8_t _pad[3];
+  float friction, restitution;
+} BodyDesc3D;
+#ifdef __cplusplus
+static_assert(sizeof(BodyDesc3D) == 44, "BodyDesc3D must match ffi.rs:3767-3786");
+#endif
+
+/* ffi.rs:3801 phieng_world3_add_bodies — each descriptor as
+ * phieng_world3_add_body; out_ids[i] = id or -1. Returns the number added,
+ * 0 for null world / descs / out_ids; n capped at 1,000,000. */
+uint32_t phieng_world3_add_bodies(World3* world, const BodyDesc3D* descs, uint32_t n, int32_t* out_ids);
+
+/* ffi.rs:1032 / 1050: fluid config. set: 1 ok, 0 null or invalid (world
+ * unchanged). get: 1 ok, 0 null. */
+int32_t phieng_world3_set_fluid_config(World3* world, const FluidConfig3Ffi* cfg);
+int32_t phieng_world3_get_fluid_config(World3* world, FluidConfig3Ffi* out);
+
+/* ffi.rs:3579 / 3609: add `count` particles from xyz triples (phase 0, or
+ * the given phases); 0 when any of the first min(count, 1e6) triples is
+ * non-finite or a pointer is null; at most 4096 particles in total (the
+ * reference's MAX_PARTICLES_3D; phieng_sph3_set_particle_cap raises it).
+ * Returns the number added. */
+uint32_t phieng_world3_fluid_add(World3* world, const float* positions, uint32_t count);
+uint32_t phieng_world3_fluid_add_phase(World3* world, const float* positions, const uint8_t* phases,
+                                       uint32_t count);
+
+/* ffi.rs:3643 / 3656 / 3672: count, clear (1 ok, 0 null), and state out as
+ * [x, y, z, vx, vy, vz] sextuples (returns the number written). */
+uint32_t phieng_world3_fluid_count(const World3* world);
+int32_t phieng_world3_fluid_clear(World3* world);
+uint32_t phieng_world3_fluid_get(const World3* world, float* out, uint32_t max);
+
+/* ---- 3D extensions (no reference counterpart) ---- */
+
+/* As phieng_sph_status (grid_log2_h holds log2 of the rows; depth is not
+ * reported). 1 ok, 0 null. */
+int32_t phieng_sph3_status(const World3* world, PhiengSphStatus* out);
+/* Reset the sticky error (1 ok, 0 null) / its text (never null). */
+int32_t phieng_sph3_clear_error(World3* world);
+const char* phieng_sph3_error_string(const World3* world);
+/* Particle cap in place of 4096 (for workloads past the reference's limit). */
+int32_t phieng_sph3_set_particle_cap(World3* world, uint32_t cap);
+/* `steps` x phieng_world3_step(dt) without synchronising. 1 ok, 0 error. */
+int32_t phieng_sph3_step_n(World3* world, float dt, uint32_t steps);
+/* Launch on this CUDA stream (NULL: the library's own). */
+int32_t phieng_sph3_set_stream(World3* world, void* stream);
+/* Wait for the world's stream; 1 ok, 0 on a (sticky) error. */
+int32_t phieng_sph3_sync(World3* world);
+/* Overwrite the first n particles' state from [x, y, z, vx, vy, vz]
+ * sextuples (non-finite values rejected). 1 ok, 0 bad input. */
+int32_t phieng_sph3_set_state(World3* world, const float* xyzv, uint32_t n);
+/* Density and pressure as the last substep's density pass left them
+ * (fluid3.rs:639-658; insertion order). Returns the number written. */
+uint32_t phieng_sph3_get_density_pressure(World3* world, float* density, float* pressure, uint32_t max);
+/* Density + pressure (and, with fxyz, the pressure force of the next
+ * substep, fluid3.rs:1040-1086) of the current state, insertion order. */
+uint32_t phieng_sph3_debug_forces(World3* world, float* density, float* pressure, float* fxyz, uint32_t max);
+/* CUDA-event times of the sort, density and force passes of the last
+ * substep (after phieng_sph3_set_profiling(world, 1)). */
+int32_t phieng_sph3_set_profiling(World3* world, int32_t on);
+uint32_t phieng_sph3_phase_times(World3* world, float* ms, uint32_t max);
+
 #ifdef __cplusplus
 }
 #endif

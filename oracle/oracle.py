@@ -1,7 +1,7 @@
 """ORACLE — TEST INFRASTRUCTURE ONLY.
 
 ctypes wrapper of oracle/liboracle.so, the C++ restatement of the reference
-2D SPH step (crates/dynamics/src/fluid.rs). Only tests/, the smoke check and
+2D SPH step (crates/dynamics/src/fluid.rs) and 3D step (fluid3.rs). Only tests/, the smoke check and
 the CPU-baseline leg of bench.py import this module; the product library
 never does.
 """
@@ -74,6 +74,28 @@ def _load():
         "orc_pressure": (C.c_float, [C.c_float, C.c_float, C.c_float, C.c_float]),
         "orc_artificial_pressure": (C.c_float, [C.c_float] * 9),
         "orc_cohesion": (C.c_float, [C.c_float, C.c_float]),
+        "orc3_new": (P, [C.c_int]),
+        "orc3_free": (None, [P]),
+        "orc3_set_config": (None, [P, C.POINTER(FluidConfig2Ffi)]),
+        "orc3_set_gravity": (None, [P, C.c_float, C.c_float, C.c_float]),
+        "orc3_set_pow_mode": (None, [P, C.c_int]),
+        "orc3_set_cap": (None, [P, C.c_uint32]),
+        "orc3_add_body": (None, [P, C.c_int] + [C.c_float] * 6),
+        "orc3_add_particles": (C.c_uint32, [P, F, U8, C.c_uint32]),
+        "orc3_count": (C.c_uint32, [P]),
+        "orc3_set_state": (None, [P, F, C.c_uint32]),
+        "orc3_get_state": (C.c_uint32, [P, F, C.c_uint32]),
+        "orc3_get_density_pressure": (C.c_uint32, [P, F, F, C.c_uint32]),
+        "orc3_step": (None, [P, C.c_float, C.c_int]),
+        "orc3_steps": (C.c_double, [P, C.c_float, C.c_int, C.c_uint32]),
+        "orc3_time": (C.c_float, [P]),
+        "orc3_passes": (None, [P, C.c_int]),
+        "orc3_get_forces": (C.c_uint32, [P, F, C.c_uint32]),
+        "orc3_neighbors": (C.c_uint32, [P, C.c_uint32, U32, C.c_uint32]),
+        "orc3_cfl_substeps": (C.c_uint32, [P, C.c_float]),
+        "orc3_collide": (C.c_int, [C.c_int] + [C.c_float] * 7 + [F]),
+        "orc3_poly6": (C.c_float, [C.c_float, C.c_float]),
+        "orc3_spiky": (None, [C.c_float] * 5 + [F]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -251,6 +273,111 @@ class OracleWorld:
         self._l.orc_set_extra_accel(self._h, _fp(a), a.shape[0])
 
 
+class OracleWorld3:
+    """A World3-shaped CPU world: static sphere / box / capsule bodies + one
+    3D SPH fluid (crates/dynamics/src/fluid3.rs). Same modes as OracleWorld."""
+
+    SPHERE, BOX, CAPSULE = 0, 1, 2
+
+    def __init__(self, fp64: bool = False, cap: int = 4096, libm_pow: bool = False):
+        self._l = _load()
+        self._h = self._l.orc3_new(1 if fp64 else 0)
+        self.fp64 = fp64
+        self._l.orc3_set_cap(self._h, cap)
+        self._l.orc3_set_pow_mode(self._h, 0 if libm_pow else 1)
+
+    def __del__(self):
+        try:
+            if self._h:
+                self._l.orc3_free(self._h)
+                self._h = None
+        except Exception:
+            pass
+
+    def set_config(self, cfg: FluidConfig2Ffi) -> None:
+        self._l.orc3_set_config(self._h, C.byref(cfg))
+
+    def set_gravity(self, gx: float, gy: float, gz: float) -> None:
+        self._l.orc3_set_gravity(self._h, gx, gy, gz)
+
+    def add_body(self, shape: int, px, py, pz, a, b=0.0, c=0.0) -> None:
+        self._l.orc3_add_body(self._h, shape, px, py, pz, a, b, c)
+
+    def add_particles(self, xyz, phases=None) -> int:
+        xyz = np.ascontiguousarray(xyz, dtype=np.float32).reshape(-1, 3)
+        ph_p = None
+        if phases is not None:
+            ph = np.ascontiguousarray(phases, dtype=np.uint8)
+            ph_p = ph.ctypes.data_as(C.POINTER(C.c_uint8))
+        return int(self._l.orc3_add_particles(self._h, _fp(xyz), ph_p, xyz.shape[0]))
+
+    @property
+    def count(self) -> int:
+        return int(self._l.orc3_count(self._h))
+
+    @property
+    def time(self) -> float:
+        return float(self._l.orc3_time(self._h))
+
+    def set_state(self, q) -> None:
+        a = np.ascontiguousarray(q, dtype=np.float32).reshape(-1, 6)
+        self._l.orc3_set_state(self._h, _fp(a), a.shape[0])
+
+    def state(self) -> np.ndarray:
+        """[n][6] = x, y, z, vx, vy, vz."""
+        out = np.zeros((self.count, 6), np.float32)
+        self._l.orc3_get_state(self._h, _fp(out), out.shape[0])
+        return out
+
+    def density_pressure(self):
+        n = self.count
+        d = np.zeros(n, np.float32)
+        p = np.zeros(n, np.float32)
+        self._l.orc3_get_density_pressure(self._h, _fp(d), _fp(p), n)
+        return d, p
+
+    def passes(self, forces: bool = True) -> None:
+        """Density (and force) pass on the current state."""
+        self._l.orc3_passes(self._h, 1 if forces else 0)
+
+    def forces(self) -> np.ndarray:
+        out = np.zeros((self.count, 3), np.float32)
+        self._l.orc3_get_forces(self._h, _fp(out), out.shape[0])
+        return out
+
+    def neighbors(self, i: int, max_n: int = 512) -> np.ndarray:
+        out = np.zeros(max_n, np.uint32)
+        k = self._l.orc3_neighbors(self._h, i, out.ctypes.data_as(C.POINTER(C.c_uint32)), max_n)
+        return out[: min(k, max_n)].copy()
+
+    def step(self, dt: float, mode: int = REF_SEQ) -> None:
+        self._l.orc3_step(self._h, dt, mode)
+
+    def steps(self, dt: float, k: int, mode: int = REF_SEQ) -> float:
+        return float(self._l.orc3_steps(self._h, dt, mode, k))
+
+    def cfl_substeps(self, dt: float) -> int:
+        return int(self._l.orc3_cfl_substeps(self._h, dt))
+
+
+def collide3(shape: int, a: float, b: float, c: float, p, pr: float):
+    """Particle at p (body frame, body at the origin) vs one static body:
+    (normal xyz, depth) or None when separated."""
+    out = np.zeros(4, np.float32)
+    hit = _load().orc3_collide(shape, a, b, c, p[0], p[1], p[2], pr, _fp(out))
+    return (tuple(float(v) for v in out[:3]), float(out[3])) if hit else None
+
+
+def poly6_3(r2: float, h: float) -> float:
+    return float(_load().orc3_poly6(r2, h))
+
+
+def spiky_grad3(rx: float, ry: float, rz: float, r: float, h: float):
+    out = np.zeros(3, np.float32)
+    _load().orc3_spiky(rx, ry, rz, r, h, _fp(out))
+    return tuple(float(v) for v in out)
+
+
 # scalar kernels (f32) for the reference's kernel-sanity checks
 def poly6(r2: float, h: float) -> float:
     return float(_load().orc_poly6(r2, h))
@@ -274,4 +401,4 @@ def cohesion(dist: float, h: float) -> float:
     return float(_load().orc_cohesion(dist, h))
 
 
-__all__ = ["OracleWorld", "REF_SEQ", "JACOBI", "default_config", "build", "lib"]
+__all__ = ["OracleWorld", "OracleWorld3", "REF_SEQ", "JACOBI", "default_config", "build", "lib"]

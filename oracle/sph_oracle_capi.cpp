@@ -12,8 +12,10 @@
 
 #include "../include/phieng_sph.h"
 #include "sph_oracle.hpp"
+#include "sph_oracle3.hpp"
 
 using oracle::Fluid;
+using oracle::Fluid3;
 
 namespace {
 
@@ -21,6 +23,12 @@ struct Orc {
   int fp64;
   Fluid<float> f32;
   Fluid<double> f64;
+};
+
+struct Orc3 {
+  int fp64;
+  Fluid3<float> f32;
+  Fluid3<double> f64;
 };
 
 template <class F>
@@ -403,5 +411,211 @@ float orc_artificial_pressure(float dx, float dy, float vrx, float vry, float r_
   return Fluid<float>::artificial_pressure(dx, dy, vrx, vry, r_sq, h, rho_bar, c, alpha);
 }
 float orc_cohesion(float dist, float h) { return Fluid<float>::cohesion(dist, h); }
+
+// ---- 3D (oracle::Fluid3: crates/dynamics/src/fluid3.rs) ----
+
+void* orc3_new(int fp64) {
+  Orc3* o = new Orc3();
+  o->fp64 = fp64 ? 1 : 0;
+  return o;
+}
+
+void orc3_free(void* h) { delete static_cast<Orc3*>(h); }
+
+void orc3_set_config(void* h, const FluidConfig2Ffi* c) {
+  Orc3* o = static_cast<Orc3*>(h);
+  DISPATCH(o, apply_config(F, c));
+}
+
+void orc3_set_gravity(void* h, float gx, float gy, float gz) {
+  Orc3* o = static_cast<Orc3*>(h);
+  o->f32.gx = gx;
+  o->f32.gy = gy;
+  o->f32.gz = gz;
+  o->f64.gx = (double)gx;
+  o->f64.gy = (double)gy;
+  o->f64.gz = (double)gz;
+}
+
+void orc3_set_pow_mode(void* h, int mode) {
+  Orc3* o = static_cast<Orc3*>(h);
+  o->f32.pow_mode = mode;
+  o->f64.pow_mode = mode;
+}
+
+void orc3_set_cap(void* h, uint32_t cap) {
+  Orc3* o = static_cast<Orc3*>(h);
+  o->f32.cap = cap;
+  o->f64.cap = cap;
+}
+
+// shape 0 = sphere (a = radius), 1 = box (a, b, c half extents), 2 = capsule
+// (a = radius, b = half length along y); identity rotation.
+void orc3_add_body(void* h, int shape, float px, float py, float pz, float a, float b, float c) {
+  Orc3* o = static_cast<Orc3*>(h);
+  oracle::Body3 bd;
+  bd.shape = shape;
+  bd.px = px;
+  bd.py = py;
+  bd.pz = pz;
+  bd.a = a;
+  bd.b = b;
+  bd.c = c;
+  o->f32.bodies.push_back(bd);
+  o->f64.bodies.push_back(bd);
+}
+
+uint32_t orc3_add_particles(void* h, const float* xyz, const uint8_t* phases, uint32_t n) {
+  Orc3* o = static_cast<Orc3*>(h);
+  uint32_t r = 0;
+  DISPATCH(o, r = (uint32_t)F.add_particles_phase(xyz, phases, n));
+  return r;
+}
+
+uint32_t orc3_count(void* h) {
+  Orc3* o = static_cast<Orc3*>(h);
+  uint32_t r = 0;
+  DISPATCH(o, r = (uint32_t)F.particles.size());
+  return r;
+}
+
+// position + velocity of the first n particles from sextuples
+void orc3_set_state(void* h, const float* q, uint32_t n) {
+  Orc3* o = static_cast<Orc3*>(h);
+  DISPATCH(o, {
+    for (uint32_t i = 0; i < n && i < F.particles.size(); i++) {
+      F.particles[i].x = q[6 * i];
+      F.particles[i].y = q[6 * i + 1];
+      F.particles[i].z = q[6 * i + 2];
+      F.particles[i].vx = q[6 * i + 3];
+      F.particles[i].vy = q[6 * i + 4];
+      F.particles[i].vz = q[6 * i + 5];
+    }
+  });
+}
+
+uint32_t orc3_get_state(void* h, float* out, uint32_t max) {
+  Orc3* o = static_cast<Orc3*>(h);
+  uint32_t n = 0;
+  DISPATCH(o, {
+    n = (uint32_t)std::min<size_t>(max, F.particles.size());
+    for (uint32_t i = 0; i < n; i++) {
+      const auto& p = F.particles[i];
+      float* r = out + 6 * (size_t)i;
+      r[0] = (float)p.x;
+      r[1] = (float)p.y;
+      r[2] = (float)p.z;
+      r[3] = (float)p.vx;
+      r[4] = (float)p.vy;
+      r[5] = (float)p.vz;
+    }
+  });
+  return n;
+}
+
+uint32_t orc3_get_density_pressure(void* h, float* d, float* p, uint32_t max) {
+  Orc3* o = static_cast<Orc3*>(h);
+  uint32_t n = 0;
+  DISPATCH(o, {
+    n = (uint32_t)std::min<size_t>(max, F.particles.size());
+    for (uint32_t i = 0; i < n; i++) {
+      if (d) d[i] = (float)F.particles[i].density;
+      if (p) p[i] = (float)F.particles[i].pressure;
+    }
+  });
+  return n;
+}
+
+// World3::step's fluid phase (world.rs:2670-2697 with fluid3.rs:591-605).
+void orc3_step(void* h, float dt, int mode) {
+  Orc3* o = static_cast<Orc3*>(h);
+  DISPATCH(o, F.world_step(dt, (oracle::Mode)mode));
+}
+
+double orc3_steps(void* h, float dt, int mode, uint32_t k) {
+  Orc3* o = static_cast<Orc3*>(h);
+  auto t0 = std::chrono::steady_clock::now();
+  for (uint32_t s = 0; s < k; s++) DISPATCH(o, F.world_step(dt, (oracle::Mode)mode));
+  auto t1 = std::chrono::steady_clock::now();
+  return std::chrono::duration<double>(t1 - t0).count();
+}
+
+float orc3_time(void* h) {
+  Orc3* o = static_cast<Orc3*>(h);
+  float t = 0.0f;
+  DISPATCH(o, t = (float)F.time);
+  return t;
+}
+
+// Density pass, then (forces != 0) the force pass, on the current state.
+void orc3_passes(void* h, int forces) {
+  Orc3* o = static_cast<Orc3*>(h);
+  DISPATCH(o, {
+    using R = decltype(F.time);
+    const R hk = oracle::rmax((R)F.cfg.smoothing_length, (R)oracle::kEps);
+    F.rebuild_grid();
+    F.compute_density_pressure(hk);
+    if (forces) F.compute_forces(hk);
+  });
+}
+
+uint32_t orc3_get_forces(void* h, float* fxyz, uint32_t max) {
+  Orc3* o = static_cast<Orc3*>(h);
+  uint32_t n = 0;
+  DISPATCH(o, {
+    n = (uint32_t)std::min<size_t>(max, F.fx.size());
+    for (uint32_t i = 0; i < n; i++) {
+      fxyz[3 * i] = (float)F.fx[i];
+      fxyz[3 * i + 1] = (float)F.fy[i];
+      fxyz[3 * i + 2] = (float)F.fz[i];
+    }
+  });
+  return n;
+}
+
+// Neighbour list of particle i in visit order (rebuilds the grid first).
+uint32_t orc3_neighbors(void* h, uint32_t i, uint32_t* out, uint32_t max) {
+  Orc3* o = static_cast<Orc3*>(h);
+  uint32_t n = 0;
+  DISPATCH(o, {
+    if (i < F.particles.size()) {
+      F.rebuild_grid();
+      std::vector<uint32_t> nb;
+      const auto& p = F.particles[i];
+      F.neighbors_of(p.x, p.y, p.z, F.particles, nb);
+      n = (uint32_t)nb.size();
+      for (uint32_t k = 0; k < n && k < max; k++) out[k] = nb[k];
+    }
+  });
+  return n;
+}
+
+uint32_t orc3_cfl_substeps(void* h, float dt) {
+  Orc3* o = static_cast<Orc3*>(h);
+  uint32_t r = 1;
+  DISPATCH(o, r = F.cfl_substeps(dt));
+  return r;
+}
+
+// Particle vs one static body (fluid3.rs:471-590); returns 1 on contact.
+int orc3_collide(int shape, float a, float b, float c, float px, float py, float pz, float pr, float* out4) {
+  oracle::Body3 bd;
+  bd.shape = shape;
+  bd.a = a;
+  bd.b = b;
+  bd.c = c;
+  float nx = 0, ny = 0, nz = 0, depth = 0;
+  const bool hit = Fluid3<float>::collide(px, py, pz, pr, bd, nx, ny, nz, depth);
+  out4[0] = nx;
+  out4[1] = ny;
+  out4[2] = nz;
+  out4[3] = depth;
+  return hit ? 1 : 0;
+}
+
+float orc3_poly6(float r2, float h) { return Fluid3<float>::poly6(r2, h); }
+void orc3_spiky(float rx, float ry, float rz, float r, float h, float* out3) {
+  Fluid3<float>::spiky_grad(rx, ry, rz, r, h, out3[0], out3[1], out3[2]);
+}
 
 }  // extern "C"

@@ -15,6 +15,10 @@ LIB_PATH = os.environ.get("PHIENG_SPH_LIBRARY") or os.path.join(HERE, "libphieng
 
 SHAPE_CIRCLE = 0
 SHAPE_BOX = 1
+SHAPE3_SPHERE = 0
+SHAPE3_BOX = 1
+SHAPE3_CAPSULE = 2
+MAX_PARTICLES_3D = 4096
 
 OK = 0
 E_NO_DEVICE = 1
@@ -104,6 +108,31 @@ class BodyDesc2D(C.Structure):
 
 
 assert C.sizeof(BodyDesc2D) == 36
+
+
+class BodyDesc3D(C.Structure):
+    """#[repr(C)] BodyDesc3D (crates/engine/src/ffi.rs:3767-3786), 44 bytes."""
+
+    _fields_ = [
+        ("pos_x", C.c_float),
+        ("pos_y", C.c_float),
+        ("pos_z", C.c_float),
+        ("shape_tag", C.c_uint32),
+        ("a", C.c_float),
+        ("b", C.c_float),
+        ("c", C.c_float),
+        ("density", C.c_float),
+        ("is_static", C.c_uint8),
+        ("_pad", C.c_uint8 * 3),
+        ("friction", C.c_float),
+        ("restitution", C.c_float),
+    ]
+
+
+assert C.sizeof(BodyDesc3D) == 44
+
+# FluidConfig3Ffi (ffi.rs:744-767) has the 2D config's fields and layout.
+FluidConfig3Ffi = FluidConfig2Ffi
 
 
 class PhiengSphStatus(C.Structure):
@@ -217,6 +246,38 @@ SIGNATURES = {
     "phieng_sph_debug_forces": (C.c_uint32, [_P, _F, C.c_uint32]),
     "phieng_sph_debug_sorted": (C.c_uint32, [_P, _U32P, _U32P, C.c_uint32]),
     "phieng_sph_debug_neighbors": (C.c_uint32, [_P, _U32P, _U32P, C.c_uint32, C.c_uint32]),
+    "phieng_world3_new": (_P, []),
+    "phieng_world3_free": (None, [_P]),
+    "phieng_world3_step": (None, [_P, C.c_float]),
+    "phieng_world3_set_gravity": (None, [_P, C.c_float, C.c_float, C.c_float]),
+    "phieng_world3_set_time": (C.c_int32, [_P, C.c_float]),
+    "phieng_world3_get_time": (C.c_int32, [_P, _F]),
+    "phieng_world3_body_count": (C.c_int32, [_P]),
+    "phieng_world3_add_body": (
+        C.c_int32,
+        [_P, C.c_float, C.c_float, C.c_float, C.c_uint32, C.c_float, C.c_float, C.c_float, C.c_float,
+         C.c_uint8, C.c_float, C.c_float],
+    ),
+    "phieng_world3_add_bodies": (C.c_uint32, [_P, C.POINTER(BodyDesc3D), C.c_uint32, C.POINTER(C.c_int32)]),
+    "phieng_world3_set_fluid_config": (C.c_int32, [_P, C.POINTER(FluidConfig2Ffi)]),
+    "phieng_world3_get_fluid_config": (C.c_int32, [_P, C.POINTER(FluidConfig2Ffi)]),
+    "phieng_world3_fluid_add": (C.c_uint32, [_P, _F, C.c_uint32]),
+    "phieng_world3_fluid_add_phase": (C.c_uint32, [_P, _F, _U8P, C.c_uint32]),
+    "phieng_world3_fluid_count": (C.c_uint32, [_P]),
+    "phieng_world3_fluid_clear": (C.c_int32, [_P]),
+    "phieng_world3_fluid_get": (C.c_uint32, [_P, _F, C.c_uint32]),
+    "phieng_sph3_status": (C.c_int32, [_P, C.POINTER(PhiengSphStatus)]),
+    "phieng_sph3_clear_error": (C.c_int32, [_P]),
+    "phieng_sph3_error_string": (C.c_char_p, [_P]),
+    "phieng_sph3_set_particle_cap": (C.c_int32, [_P, C.c_uint32]),
+    "phieng_sph3_step_n": (C.c_int32, [_P, C.c_float, C.c_uint32]),
+    "phieng_sph3_set_stream": (C.c_int32, [_P, _P]),
+    "phieng_sph3_sync": (C.c_int32, [_P]),
+    "phieng_sph3_set_state": (C.c_int32, [_P, _F, C.c_uint32]),
+    "phieng_sph3_get_density_pressure": (C.c_uint32, [_P, _F, _F, C.c_uint32]),
+    "phieng_sph3_debug_forces": (C.c_uint32, [_P, _F, _F, _F, C.c_uint32]),
+    "phieng_sph3_set_profiling": (C.c_int32, [_P, C.c_int32]),
+    "phieng_sph3_phase_times": (C.c_uint32, [_P, _F, C.c_uint32]),
 }
 
 _lib = None

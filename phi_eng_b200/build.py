@@ -32,6 +32,7 @@ UNITS = [
     ("sph_world.cu", EXACT),
     ("sph_noalloc.cu", EXACT),
     ("sph_mlp.cu", EXACT),
+    ("sph3d.cu", EXACT),
 ]
 HEADERS = ["sph_device.cuh", "sph_kernels.h", "sph_mlp.cuh", "sph_mlp_host.h", "sph_warp.cuh", "sph_host.h"]
 

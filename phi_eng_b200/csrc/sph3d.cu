@@ -1,0 +1,1298 @@
+// 3D SPH fluid step (crates/dynamics/src/fluid3.rs) on the GPU, behind the
+// engine's phieng_world3_* C ABI (crates/engine/src/ffi.rs:3199-3760).
+//
+// Same design as the 2D chain (sph_kernels.cu): a power-of-two bucket grid
+// over cells of size h, bucket = ((cz - cz0) mod D) * H * W + ((cy - cy0) mod
+// H) * W + ((cx - cx0) mod W); a counting sort by bucket with the in-bucket
+// rank by id (the shared scan + placement of sph_kernels.cu, a 3D gather
+// here), so each particle's candidates are 9 contiguous slot ranges (rows
+// oz, oy = -1..1 of three consecutive x cells) visited in the reference's
+// order (oz outer, oy, ox inner, ascending id, fluid3.rs:319-343); the
+// density pass records one 32-bit neighbour mask per row and the force pass
+// walks them. Arithmetic is glam 0.29's scalar Vec3 in f32 (dot =
+// (x*x + y*y) + z*z, component-wise operators), IEEE division and square
+// root, no FMA contraction: per-pair results are bit-identical to the
+// reference's. The integrate reads pre-step neighbour state (Jacobi), as in
+// 2D. Static sphere / box / capsule walls as phieng_world3_add_body creates
+// them (identity rotation: glam's quaternion products with the identity
+// return the vector unchanged).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/phieng_sph.h"
+#include "sph_host.h"
+#include "sph_kernels.h"
+#include "sph_warp.cuh"
+
+using namespace phieng;
+using namespace phieng::host;
+
+namespace phieng {
+namespace {
+
+constexpr uint32_t kMaxParticles3D = 4096;  // MAX_PARTICLES_3D (fluid3.rs:28)
+constexpr uint32_t kMaskBits3 = 32;
+
+struct GridPlan3 {
+  int32_t cx0, cy0, cz0;
+  uint32_t log2w, log2h, log2d;
+  uint32_t maskw, maskh, maskd;
+  uint32_t nbuckets;
+  float hg;
+  uint32_t sentinel;
+};
+
+struct StepParams3 {
+  GridPlan3 grid;
+  float hg2, hk, hk2;
+  float c_poly6;  // 315/(64 PI h2 h2 h2 h2 h), as fluid3.rs:228 evaluates it
+  float c_spiky;  // -45/(PI h h h h h h), as fluid3.rs:238
+  float rho_cap;
+  float stiffness, gamma;
+  float rest[4];
+  float mass, visc, vmax, dt;
+  float gx, gy, gz;
+  float pr, pr_pad, mu, av_alpha, c_s, surface_tension;
+  uint32_t flags, nbodies, uniform_phase;
+};
+
+// Static body: shape 0 sphere (a = radius), 1 box (a, b, c half extents),
+// 2 capsule (a = radius, b = half length along y); ex, ey, ez = half extents
+// of its axis-aligned bounding box padded by 0.1%.
+struct DevBody3 {
+  int32_t shape;
+  float px, py, pz;
+  float a, b, c;
+  float ex, ey, ez;
+};
+
+__device__ __forceinline__ float dot3(float ax, float ay, float az, float bx, float by, float bz) {
+  return __fadd_rn(__fadd_rn(__fmul_rn(ax, bx), __fmul_rn(ay, by)), __fmul_rn(az, bz));
+}
+
+__device__ __forceinline__ uint32_t bucket_key3(float x, float y, float z, const GridPlan3& g) {
+  if (!isfinite(x) || !isfinite(y) || !isfinite(z)) return g.sentinel;
+  const int32_t cx = __float2int_rd(__fdiv_rn(x, g.hg));
+  const int32_t cy = __float2int_rd(__fdiv_rn(y, g.hg));
+  const int32_t cz = __float2int_rd(__fdiv_rn(z, g.hg));
+  const uint32_t bx = ((uint32_t)cx - (uint32_t)g.cx0) & g.maskw;
+  const uint32_t by = ((uint32_t)cy - (uint32_t)g.cy0) & g.maskh;
+  const uint32_t bz = ((uint32_t)cz - (uint32_t)g.cz0) & g.maskd;
+  return (bz << (g.log2w + g.log2h)) | (by << g.log2w) | bx;
+}
+
+// poly6 (fluid3.rs:220-229): (((c * t) * t) * t)
+__device__ __forceinline__ float poly6_3(float r2, const StepParams3& P) {
+  if (r2 >= P.hk2 || r2 < 0.0f) return 0.0f;
+  const float t = __fsub_rn(P.hk2, r2);
+  return __fmul_rn(__fmul_rn(__fmul_rn(P.c_poly6, t), t), t);
+}
+
+// Candidate j's density term m_j * poly6(d2) when d2 < h*h (a neighbour), else +0
+__device__ __forceinline__ float contrib3(float d2, float m, const StepParams3& P) {
+  return d2 < P.hg2 ? __fmul_rn(m, poly6_3(d2, P)) : 0.0f;
+}
+
+// Particle vs static body (fluid3.rs:471-590) with the identity rotation.
+__device__ __forceinline__ bool collide3(float px, float py, float pz, float pr, const DevBody3& b, float& nx,
+                                         float& ny, float& nz, float& depth) {
+  const float rx = __fsub_rn(px, b.px), ry = __fsub_rn(py, b.py), rz = __fsub_rn(pz, b.pz);
+  if (b.shape == 0) {
+    const float dist = __fsqrt_rn(dot3(rx, ry, rz, rx, ry, rz));
+    const float rr = __fadd_rn(b.a, pr);
+    if (dist >= rr) return false;
+    if (dist > kEps) {
+      nx = __fdiv_rn(rx, dist);
+      ny = __fdiv_rn(ry, dist);
+      nz = __fdiv_rn(rz, dist);
+    } else {
+      nx = 1.0f;
+      ny = 0.0f;
+      nz = 0.0f;
+    }
+    depth = __fsub_rn(rr, dist);
+    return true;
+  }
+  if (b.shape == 1) {
+    float cxl = rx, cyl = ry, czl = rz;  // f32::clamp (NaN passes through)
+    if (cxl < -b.a) cxl = -b.a;
+    if (cxl > b.a) cxl = b.a;
+    if (cyl < -b.b) cyl = -b.b;
+    if (cyl > b.b) cyl = b.b;
+    if (czl < -b.c) czl = -b.c;
+    if (czl > b.c) czl = b.c;
+    const float ddx = __fsub_rn(rx, cxl), ddy = __fsub_rn(ry, cyl), ddz = __fsub_rn(rz, czl);
+    const float l2 = dot3(ddx, ddy, ddz, ddx, ddy, ddz);
+    if (l2 > kEpsSq) {
+      const float dist = __fsqrt_rn(l2);
+      if (dist >= pr) return false;
+      nx = __fdiv_rn(ddx, dist);
+      ny = __fdiv_rn(ddy, dist);
+      nz = __fdiv_rn(ddz, dist);
+      depth = __fsub_rn(pr, dist);
+      return true;
+    }
+    const float dx = __fsub_rn(b.a, fabsf(rx)), dy = __fsub_rn(b.b, fabsf(ry)), dz = __fsub_rn(b.c, fabsf(rz));
+    // signum().copysign(1.0) = +1 (a NaN stays a positive NaN)
+    if (dx <= dy && dx <= dz) {
+      nx = (rx != rx) ? fabsf(rx) : 1.0f;
+      ny = 0.0f;
+      nz = 0.0f;
+      depth = __fadd_rn(pr, dx);
+    } else if (dy <= dz) {
+      nx = 0.0f;
+      ny = (ry != ry) ? fabsf(ry) : 1.0f;
+      nz = 0.0f;
+      depth = __fadd_rn(pr, dy);
+    } else {
+      nx = 0.0f;
+      ny = 0.0f;
+      nz = (rz != rz) ? fabsf(rz) : 1.0f;
+      depth = __fadd_rn(pr, dz);
+    }
+    return true;
+  }
+  // capsule along y: closest point on the segment [-hl, hl]
+  float sy = ry;
+  if (sy < -b.b) sy = -b.b;
+  if (sy > b.b) sy = b.b;
+  const float ddx = rx, ddy = __fsub_rn(ry, sy), ddz = rz;
+  const float l2 = dot3(ddx, ddy, ddz, ddx, ddy, ddz);
+  if (l2 > kEpsSq) {
+    const float dist = __fsqrt_rn(l2);
+    const float rr = __fadd_rn(b.a, pr);
+    if (dist >= rr) return false;
+    nx = __fdiv_rn(ddx, dist);
+    ny = __fdiv_rn(ddy, dist);
+    nz = __fdiv_rn(ddz, dist);
+    depth = __fsub_rn(rr, dist);
+    return true;
+  }
+  // on the axis: push radially, glam normalize_or_zero of (x, 0, z)
+  // (multiplication by the reciprocal length), else +x
+  const float r2 = dot3(rx, 0.0f, rz, rx, 0.0f, rz);
+  if (r2 > kEpsSq) {
+    const float rcp = __fdiv_rn(1.0f, __fsqrt_rn(r2));
+    if (isfinite(rcp) && rcp > 0.0f) {
+      nx = __fmul_rn(rx, rcp);
+      ny = __fmul_rn(0.0f, rcp);
+      nz = __fmul_rn(rz, rcp);
+    } else {
+      nx = ny = nz = 0.0f;
+    }
+  } else {
+    nx = 1.0f;
+    ny = 0.0f;
+    nz = 0.0f;
+  }
+  depth = __fsub_rn(__fadd_rn(pr, b.a), __fsqrt_rn(l2));
+  return true;
+}
+
+// Boundary pass (fluid3.rs:1140-1176); statics take no impulse.
+__device__ __forceinline__ void walls3(float& x, float& y, float& z, float& vx, float& vy, float& vz,
+                                       const DevBody3* __restrict__ bodies, const StepParams3& P) {
+  for (uint32_t k = 0; k < P.nbodies; k++) {
+    const DevBody3* bp = bodies + k;
+    if (fabsf(x - __ldg(&bp->px)) > __ldg(&bp->ex) + P.pr_pad || fabsf(y - __ldg(&bp->py)) > __ldg(&bp->ey) + P.pr_pad ||
+        fabsf(z - __ldg(&bp->pz)) > __ldg(&bp->ez) + P.pr_pad)
+      continue;
+    const DevBody3 b = *bp;
+    float nx, ny, nz, depth;
+    if (!collide3(x, y, z, P.pr, b, nx, ny, nz, depth)) continue;
+    if (depth <= 0.0f) continue;
+    x = __fadd_rn(x, __fmul_rn(nx, depth));
+    y = __fadd_rn(y, __fmul_rn(ny, depth));
+    z = __fadd_rn(z, __fmul_rn(nz, depth));
+    const float vn = dot3(vx, vy, vz, nx, ny, nz);
+    if (vn < 0.0f) {
+      vx = __fsub_rn(vx, __fmul_rn(nx, vn));
+      vy = __fsub_rn(vy, __fmul_rn(ny, vn));
+      vz = __fsub_rn(vz, __fmul_rn(nz, vn));
+      if (P.flags & F_FRICTION) {
+        const float vtx = vx, vty = vy, vtz = vz;
+        const float wdot = dot3(0.0f, 0.0f, 0.0f, nx, ny, nz);
+        const float wtx = __fsub_rn(0.0f, __fmul_rn(nx, wdot));
+        const float wty = __fsub_rn(0.0f, __fmul_rn(ny, wdot));
+        const float wtz = __fsub_rn(0.0f, __fmul_rn(nz, wdot));
+        vx = __fadd_rn(vx, __fmul_rn(__fsub_rn(wtx, vtx), P.mu));
+        vy = __fadd_rn(vy, __fmul_rn(__fsub_rn(wty, vty), P.mu));
+        vz = __fadd_rn(vz, __fmul_rn(__fsub_rn(wtz, vtz), P.mu));
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------- kernels
+__global__ void __launch_bounds__(256) k_keys3(const float4* __restrict__ pos, uint32_t n, GridPlan3 g,
+                                               uint32_t* __restrict__ keys, uint32_t* __restrict__ count) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float4 p = pos[i];
+  const uint32_t k = bucket_key3(p.x, p.y, p.z, g);
+  keys[i] = k;
+  count_key(count, k);
+}
+
+// In-bucket rank by id, then the gather into sorted order.
+__global__ void __launch_bounds__(256) k_fixup3(const uint32_t* __restrict__ tkey, const uint32_t* __restrict__ tid_in,
+                                                const uint32_t* __restrict__ start, uint32_t n,
+                                                uint32_t* __restrict__ skey, uint32_t* __restrict__ sid,
+                                                const float4* __restrict__ pos, const float4* __restrict__ vel,
+                                                const float* __restrict__ mass, const uint8_t* __restrict__ phase,
+                                                float4* __restrict__ spos, float4* __restrict__ svel,
+                                                float* __restrict__ smass, uint8_t* __restrict__ sphase) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  const uint32_t k = tkey[s];
+  const uint32_t id = tid_in[s];
+  const uint32_t lo = start[k], hi = start[k + 1];
+  uint32_t rank = 0;
+  for (uint32_t j = lo; j < hi; j++) rank += __ldg(&tid_in[j]) < id ? 1u : 0u;
+  const uint32_t f = lo + rank;
+  skey[f] = k;
+  sid[f] = id;
+  spos[f] = pos[id];
+  svel[f] = vel[id];
+  if (smass) smass[f] = mass[id];
+  if (sphase) sphase[f] = phase[id];
+}
+
+__device__ __forceinline__ uint32_t row_base3(uint32_t by, uint32_t bz, int r, const GridPlan3& g) {
+  const uint32_t oz = (uint32_t)(r / 3) - 1u, oy = (uint32_t)(r % 3) - 1u;
+  return (((bz + oz) & g.maskd) << (g.log2w + g.log2h)) | (((by + oy) & g.maskh) << g.log2w);
+}
+
+// Density + EOS (fluid3.rs:639-658) in sorted order; per-row neighbour masks
+// (bit t of nmask[r * n + s]: slot row_start + t is a neighbour). A zero mask
+// for the particle's own row (r = 4) means no masks (seam or > 32 slots).
+template <bool MASS, bool PHASE>
+__global__ void __launch_bounds__(256) k_density3(const float4* __restrict__ spos, const uint32_t* __restrict__ skey,
+                                                  const float* __restrict__ smass, const uint8_t* __restrict__ sphase,
+                                                  uint32_t n, const uint32_t* __restrict__ start, StepParams3 P,
+                                                  float2* __restrict__ sdq, float* __restrict__ spres,
+                                                  uint32_t* __restrict__ nmask) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  const uint32_t k = skey[s];
+  const float4 pi = spos[s];
+  float rho = 0.0f;
+  const GridPlan3& g = P.grid;
+  if (k != g.sentinel) {
+    const uint32_t bx = k & g.maskw, by = (k >> g.log2w) & g.maskh, bz = k >> (g.log2w + g.log2h);
+    if (bx >= 1u && bx < g.maskw) {
+      // the three x cells of each row are consecutive buckets: one slot range
+      bool masked = true;
+      uint32_t m_own = 0;
+#pragma unroll 1
+      for (int r = 0; r < 9; r++) {
+        const uint32_t row = row_base3(by, bz, r, g);
+        const uint32_t rs = __ldg(&start[row + bx - 1]), re = __ldg(&start[row + bx + 2]);
+        uint32_t m = 0;
+        for (uint32_t j = rs; j < re; j++) {
+          const float4 a = __ldg(&spos[j]);
+          const float dx = __fsub_rn(a.x, pi.x), dy = __fsub_rn(a.y, pi.y), dz = __fsub_rn(a.z, pi.z);
+          const float d2 = dot3(dx, dy, dz, dx, dy, dz);
+          rho = __fadd_rn(rho, contrib3(d2, MASS ? __ldg(&smass[j]) : P.mass, P));
+          if (j - rs < kMaskBits3) m |= (uint32_t)(d2 < P.hg2) << (j - rs);
+        }
+        if (re - rs > kMaskBits3) masked = false;
+        if (r == 4) m_own = m;
+        else nmask[(size_t)r * n + s] = m;
+      }
+      nmask[4 * (size_t)n + s] = masked ? m_own : 0u;
+    } else {
+      // seam column: the x cells wrap, visit bucket by bucket
+#pragma unroll 1
+      for (int r = 0; r < 9; r++) {
+        const uint32_t row = row_base3(by, bz, r, g);
+#pragma unroll 1
+        for (int ox = -1; ox <= 1; ox++) {
+          const uint32_t bb = row | ((bx + (uint32_t)ox) & g.maskw);
+          const uint32_t e = __ldg(&start[bb + 1]);
+          for (uint32_t j = __ldg(&start[bb]); j < e; j++) {
+            const float4 a = __ldg(&spos[j]);
+            const float dx = __fsub_rn(a.x, pi.x), dy = __fsub_rn(a.y, pi.y), dz = __fsub_rn(a.z, pi.z);
+            rho = __fadd_rn(rho, contrib3(dot3(dx, dy, dz, dx, dy, dz), MASS ? __ldg(&smass[j]) : P.mass, P));
+          }
+        }
+      }
+      nmask[4 * (size_t)n + s] = 0u;
+    }
+  } else {
+    nmask[4 * (size_t)n + s] = 0u;
+  }
+  float dens = rho;
+  if (dens < 0.0f) dens = 0.0f;
+  if (dens > P.rho_cap) dens = P.rho_cap;
+  const uint32_t ph = PHASE ? min((uint32_t)sphase[s], 3u) : P.uniform_phase;
+  const float p = eos(dens, P.rest[ph], P);
+  const float rc = fmaxf(dens, kEps);
+  sdq[s] = make_float2(dens, __fdiv_rn(p, __fmul_rn(rc, rc)));
+  spres[s] = p;
+}
+
+// One neighbour pair of the force loop (fluid3.rs:1040-1084) and of the XSPH
+// sum (fluid3.rs:1111-1123), accumulated in the reference's order.
+template <bool MASS>
+__device__ __forceinline__ void pair3(uint32_t j, float4 pi, float4 vi, float rho_i, float q_i, float m_i,
+                                      const float4* __restrict__ spos, const float4* __restrict__ svel,
+                                      const float2* __restrict__ sdq, const float* __restrict__ smass,
+                                      const StepParams3& P, float (&f)[3], float (&sm)[3]) {
+  const float4 pj = __ldg(&spos[j]);
+  const float2 dqj = __ldg(&sdq[j]);
+  const float4 vj = __ldg(&svel[j]);
+  const float m_j = MASS ? __ldg(&smass[j]) : P.mass;
+  const float rho_j = fmaxf(dqj.x, kEps);
+  const float dx = __fsub_rn(pi.x, pj.x), dy = __fsub_rn(pi.y, pj.y), dz = __fsub_rn(pi.z, pj.z);
+  const float d2 = dot3(dx, dy, dz, dx, dy, dz);
+  const float dist = __fsqrt_rn(d2);
+  float g0 = 0.0f, g1 = 0.0f, g2 = 0.0f;
+  if (!(dist >= P.hk || dist < kEps)) {
+    const float hr = __fsub_rn(P.hk, dist);
+    const float sc = __fmul_rn(__fmul_rn(P.c_spiky, hr), hr);
+    g0 = __fmul_rn(__fdiv_rn(dx, dist), sc);
+    g1 = __fmul_rn(__fdiv_rn(dy, dist), sc);
+    g2 = __fmul_rn(__fdiv_rn(dz, dist), sc);
+  }
+  float term = __fadd_rn(q_i, dqj.y);
+  if ((P.flags & F_AV) && dist > kEps) {
+    const float rho_bar = __fmul_rn(0.5f, __fadd_rn(rho_i, rho_j));
+    const float vd = dot3(__fsub_rn(vi.x, vj.x), __fsub_rn(vi.y, vj.y), __fsub_rn(vi.z, vj.z), dx, dy, dz);
+    if (!(vd >= 0.0f)) {
+      const float r_sq = __fmul_rn(dist, dist);
+      const float mu = __fdiv_rn(__fmul_rn(P.hk, vd), __fadd_rn(r_sq, __fmul_rn(__fmul_rn(0.01f, P.hk), P.hk)));
+      term = __fadd_rn(term, __fdiv_rn(__fmul_rn(__fmul_rn(-P.av_alpha, P.c_s), mu), fmaxf(rho_bar, kEps)));
+    }
+  }
+  const float mt = __fmul_rn(m_j, term);
+  f[0] = __fsub_rn(f[0], __fmul_rn(g0, mt));
+  f[1] = __fsub_rn(f[1], __fmul_rn(g1, mt));
+  f[2] = __fsub_rn(f[2], __fmul_rn(g2, mt));
+  if ((P.flags & F_COHESION) && dist > kEps) {
+    const float c = dist >= P.hk ? 0.0f : __fsub_rn(1.0f, __fdiv_rn(dist, P.hk));
+    if (c > 0.0f) {
+      const float sc = __fmul_rn(__fmul_rn(__fmul_rn(P.surface_tension, m_i), m_j), c);
+      f[0] = __fsub_rn(f[0], __fmul_rn(__fdiv_rn(dx, dist), sc));
+      f[1] = __fsub_rn(f[1], __fmul_rn(__fdiv_rn(dy, dist), sc));
+      f[2] = __fsub_rn(f[2], __fmul_rn(__fdiv_rn(dz, dist), sc));
+    }
+  }
+  if (P.flags & F_VISC) {
+    const float rho_bar = __fmul_rn(0.5f, __fadd_rn(rho_i, rho_j));
+    const float w = poly6_3(d2, P);
+    const float mr = __fdiv_rn(m_j, rho_bar);
+    sm[0] = __fadd_rn(sm[0], __fmul_rn(__fmul_rn(__fsub_rn(vj.x, vi.x), mr), w));
+    sm[1] = __fadd_rn(sm[1], __fmul_rn(__fmul_rn(__fsub_rn(vj.y, vi.y), mr), w));
+    sm[2] = __fadd_rn(sm[2], __fmul_rn(__fmul_rn(__fsub_rn(vj.z, vi.z), mr), w));
+  }
+}
+
+// Force + XSPH + integrate + walls (fluid3.rs:1040-1176); writes the new
+// state (id order), the next key and its bucket count. DEBUG: forces only.
+template <bool MASS, bool DEBUG>
+__global__ void __launch_bounds__(256) k_force3(const float4* __restrict__ spos, const float4* __restrict__ svel,
+                                                const float2* __restrict__ sdq, const uint32_t* __restrict__ skey,
+                                                const uint32_t* __restrict__ sid, const float* __restrict__ smass,
+                                                uint32_t n, const uint32_t* __restrict__ start, StepParams3 P,
+                                                const DevBody3* __restrict__ bodies,
+                                                const uint32_t* __restrict__ nmask, float4* __restrict__ pos_out,
+                                                float4* __restrict__ vel_out, uint32_t* __restrict__ key_out,
+                                                uint32_t* __restrict__ count_out, float4* __restrict__ dbg) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  const uint32_t k = skey[s];
+  const uint32_t id = sid[s];
+  const float4 pi = spos[s];
+  const float4 vi = svel[s];
+  const float2 dqi = sdq[s];
+  const float m_i = MASS ? smass[s] : P.mass;
+  const float rho_i = fmaxf(dqi.x, kEps);
+  const float q_i = dqi.y;
+  float f[3] = {0.0f, 0.0f, 0.0f}, sm[3] = {0.0f, 0.0f, 0.0f};
+  const GridPlan3& g = P.grid;
+  if (k != g.sentinel) {
+    const uint32_t bx = k & g.maskw, by = (k >> g.log2w) & g.maskh, bz = k >> (g.log2w + g.log2h);
+    if (nmask[4 * (size_t)n + s] != 0u) {
+#pragma unroll 1
+      for (int r = 0; r < 9; r++) {
+        uint32_t cur = nmask[(size_t)r * n + s];
+        if (cur == 0u) continue;
+        const uint32_t base = __ldg(&start[row_base3(by, bz, r, g) + bx - 1]);
+        while (cur) {
+          const uint32_t j = base + (uint32_t)(__ffs((int)cur) - 1);
+          cur &= cur - 1u;
+          if (j != s) pair3<MASS>(j, pi, vi, rho_i, q_i, m_i, spos, svel, sdq, smass, P, f, sm);
+        }
+      }
+    } else {
+#pragma unroll 1
+      for (int r = 0; r < 9; r++) {
+        const uint32_t row = row_base3(by, bz, r, g);
+#pragma unroll 1
+        for (int ox = -1; ox <= 1; ox++) {
+          const uint32_t bb = row | ((bx + (uint32_t)ox) & g.maskw);
+          const uint32_t e = __ldg(&start[bb + 1]);
+          for (uint32_t j = __ldg(&start[bb]); j < e; j++) {
+            const float4 a = __ldg(&spos[j]);
+            const float ex = __fsub_rn(a.x, pi.x), ey = __fsub_rn(a.y, pi.y), ez = __fsub_rn(a.z, pi.z);
+            if (dot3(ex, ey, ez, ex, ey, ez) < P.hg2 && j != s)
+              pair3<MASS>(j, pi, vi, rho_i, q_i, m_i, spos, svel, sdq, smass, P, f, sm);
+          }
+        }
+      }
+    }
+  }
+  if (DEBUG) {
+    dbg[id] = make_float4(f[0], f[1], f[2], 0.0f);
+    return;
+  }
+  const float ax = __fadd_rn(P.gx, __fdiv_rn(f[0], rho_i));
+  const float ay = __fadd_rn(P.gy, __fdiv_rn(f[1], rho_i));
+  const float az = __fadd_rn(P.gz, __fdiv_rn(f[2], rho_i));
+  float vx = __fadd_rn(vi.x, __fmul_rn(ax, P.dt));
+  float vy = __fadd_rn(vi.y, __fmul_rn(ay, P.dt));
+  float vz = __fadd_rn(vi.z, __fmul_rn(az, P.dt));
+  if (P.flags & F_VISC) {
+    vx = __fadd_rn(vx, __fmul_rn(sm[0], P.visc));
+    vy = __fadd_rn(vy, __fmul_rn(sm[1], P.visc));
+    vz = __fadd_rn(vz, __fmul_rn(sm[2], P.visc));
+  }
+  const float speed = __fsqrt_rn(dot3(vx, vy, vz, vx, vy, vz));
+  if (speed > P.vmax) {
+    const float sc = __fdiv_rn(P.vmax, speed);
+    vx = __fmul_rn(vx, sc);
+    vy = __fmul_rn(vy, sc);
+    vz = __fmul_rn(vz, sc);
+  }
+  if (!isfinite(vx) || !isfinite(vy) || !isfinite(vz)) vx = vy = vz = 0.0f;
+  float x = __fadd_rn(pi.x, __fmul_rn(vx, P.dt));
+  float y = __fadd_rn(pi.y, __fmul_rn(vy, P.dt));
+  float z = __fadd_rn(pi.z, __fmul_rn(vz, P.dt));
+  if (!isfinite(x) || !isfinite(y) || !isfinite(z)) {
+    x = pi.x;
+    y = pi.y;
+    z = pi.z;
+  }
+  walls3(x, y, z, vx, vy, vz, bodies, P);
+  pos_out[id] = make_float4(x, y, z, 0.0f);
+  vel_out[id] = make_float4(vx, vy, vz, 0.0f);
+  const uint32_t nk = bucket_key3(x, y, z, g);
+  key_out[id] = nk;
+  count_key(count_out, nk);
+}
+
+__global__ void __launch_bounds__(256) k_vmax3(const float4* __restrict__ vel, uint32_t n, unsigned int* out) {
+  float m = 0.0f;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const float4 v = vel[i];
+    const float l = __fsqrt_rn(dot3(v.x, v.y, v.z, v.x, v.y, v.z));
+    if (l > m) m = l;  // NaN never wins (f32::max semantics)
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xFFFFFFFFu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(m));
+}
+
+__global__ void __launch_bounds__(256) k_unsort3(const float2* __restrict__ sdq, const float* __restrict__ spres,
+                                                 const uint32_t* __restrict__ sid, uint32_t n, float* dens,
+                                                 float* pres) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  dens[sid[s]] = sdq[s].x;
+  pres[sid[s]] = spres[s];
+}
+
+inline uint32_t cdiv(uint32_t a, uint32_t b) { return (a + b - 1) / b; }
+
+}  // namespace
+}  // namespace phieng
+
+// ---------------------------------------------------------------- the 3D world
+struct World3 {
+  FluidConfig3Ffi cfg = default_config();
+  float gx = 0.0f, gy = -9.81f, gz = 0.0f;  // World3::new gravity
+  float time = 0.0f;
+  std::vector<DevBody3> bodies;
+  bool bodies_dirty = true;
+  uint32_t cap = kMaxParticles3D;
+  uint32_t n = 0;
+  std::vector<float4> h_pos, h_vel;
+  std::vector<float> h_mass, h_dens, h_pres;  // density / pressure as of dp_dev == false
+  std::vector<uint8_t> h_phase;
+  bool mass_uniform = true, phase_uniform = true;
+  float mass_value = 0.0f;
+  uint32_t phase_value = 0;
+  bool host_valid = true, dev_valid = false, aux_valid = false, keys_valid = false;
+  bool dp_dev = false;  // the sorted density / pressure on the device are newer than h_dens / h_pres
+  bool plan_valid = false;
+  uint32_t sid_perm_n = 0;
+  GridPlan3 plan{};
+  int device = -1;
+  cudaStream_t own_stream = nullptr, stream = nullptr;
+  bool user_stream = false;
+  int32_t error = PHIENG_SPH_OK;
+  uint64_t substeps = 0;
+  // device arrays
+  uint32_t dcap = 0;
+  float4 *pos = nullptr, *vel = nullptr, *spos = nullptr, *svel = nullptr;
+  float *mass = nullptr, *smass = nullptr, *spres = nullptr, *tmp = nullptr;
+  uint8_t *phase = nullptr, *sphase = nullptr;
+  uint32_t *key = nullptr, *tkey = nullptr, *tid = nullptr, *skey = nullptr, *sid = nullptr, *nmask = nullptr;
+  float2* sdq = nullptr;
+  uint32_t *count = nullptr, *start = nullptr, *tilesum = nullptr, *scalar = nullptr;
+  uint32_t count_len = 0, range_cap = 0;
+  DevBody3* dbodies = nullptr;
+  uint32_t bodies_cap = 0;
+  unsigned int* h_pinned = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  std::string gsig;
+  bool profiling = false;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+};
+
+namespace {
+
+bool ok3(World3* w, cudaError_t r) {
+  if (r == cudaSuccess) return true;
+  cudaGetLastError();
+  if (w->error == PHIENG_SPH_OK) w->error = PHIENG_SPH_E_CUDA;
+  return false;
+}
+
+template <class T>
+void dfree3(T*& p) {
+  if (p) cudaFree(p);
+  p = nullptr;
+}
+
+template <class T>
+bool dalloc3(World3* w, T*& p, size_t count) {
+  return ok3(w, cudaMalloc(&p, sizeof(T) * std::max<size_t>(count, 1)));
+}
+
+void release_graph3(World3* w) {
+  if (w->gexec) cudaGraphExecDestroy(w->gexec);
+  w->gexec = nullptr;
+  w->gsig.clear();
+}
+
+void free_particles3(World3* w) {
+  dfree3(w->pos), dfree3(w->vel), dfree3(w->spos), dfree3(w->svel), dfree3(w->mass), dfree3(w->smass);
+  dfree3(w->spres), dfree3(w->tmp), dfree3(w->phase), dfree3(w->sphase), dfree3(w->key), dfree3(w->tkey);
+  dfree3(w->tid), dfree3(w->skey), dfree3(w->sid), dfree3(w->nmask), dfree3(w->sdq);
+  w->dcap = 0;
+}
+
+bool ensure_device3(World3* w) {
+  if (w->device >= 0) return true;
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+    cudaGetLastError();
+    w->error = PHIENG_SPH_E_NO_DEVICE;
+    return false;
+  }
+  int dev = 0;
+  if (!ok3(w, cudaGetDevice(&dev))) return false;
+  if (!ok3(w, cudaStreamCreateWithFlags(&w->own_stream, cudaStreamNonBlocking))) return false;
+  if (!w->user_stream) w->stream = w->own_stream;
+  if (!ok3(w, cudaMalloc(&w->scalar, 64)) || !ok3(w, cudaMemset(w->scalar, 0, 64))) return false;
+  if (!ok3(w, cudaMallocHost(&w->h_pinned, 64))) return false;
+  w->device = dev;
+  return true;
+}
+
+bool ensure_capacity3(World3* w, uint32_t need) {
+  if (need <= w->dcap && w->pos) return true;
+  cudaStreamSynchronize(w->stream);
+  free_particles3(w);
+  release_graph3(w);
+  const uint32_t c = std::max<uint32_t>(need, 1024);
+  const bool ok = dalloc3(w, w->pos, c) && dalloc3(w, w->vel, c) && dalloc3(w, w->spos, c) && dalloc3(w, w->svel, c) &&
+                  dalloc3(w, w->mass, c) && dalloc3(w, w->smass, c) && dalloc3(w, w->spres, c) &&
+                  dalloc3(w, w->tmp, 2 * (size_t)c) && dalloc3(w, w->phase, c) && dalloc3(w, w->sphase, c) &&
+                  dalloc3(w, w->key, c) && dalloc3(w, w->tkey, c) && dalloc3(w, w->tid, c) && dalloc3(w, w->skey, c) &&
+                  dalloc3(w, w->sid, c) && dalloc3(w, w->nmask, 9 * (size_t)c) && dalloc3(w, w->sdq, c);
+  if (!ok) {
+    free_particles3(w);
+    return false;
+  }
+  w->dcap = c;
+  w->dev_valid = w->aux_valid = w->keys_valid = false;
+  w->sid_perm_n = 0;
+  return true;
+}
+
+bool ensure_host3(World3* w) {
+  if (w->host_valid) return true;
+  if (!ok3(w, cudaMemcpyAsync(w->h_pos.data(), w->pos, sizeof(float4) * w->n, cudaMemcpyDeviceToHost, w->stream)) ||
+      !ok3(w, cudaMemcpyAsync(w->h_vel.data(), w->vel, sizeof(float4) * w->n, cudaMemcpyDeviceToHost, w->stream)) ||
+      !ok3(w, cudaStreamSynchronize(w->stream)))
+    return false;
+  w->host_valid = true;
+  return true;
+}
+
+// Bring the density / pressure of the last density pass (sorted order on the
+// device) back to insertion order on the host.
+bool ensure_host_dp3(World3* w) {
+  if (!w->dp_dev) return true;
+  k_unsort3<<<cdiv(w->n, 256), 256, 0, w->stream>>>(w->sdq, w->spres, w->sid, w->n, w->tmp, w->tmp + w->dcap);
+  if (!ok3(w, cudaGetLastError()) ||
+      !ok3(w, cudaMemcpyAsync(w->h_dens.data(), w->tmp, sizeof(float) * w->n, cudaMemcpyDeviceToHost, w->stream)) ||
+      !ok3(w, cudaMemcpyAsync(w->h_pres.data(), w->tmp + w->dcap, sizeof(float) * w->n, cudaMemcpyDeviceToHost,
+                              w->stream)) ||
+      !ok3(w, cudaStreamSynchronize(w->stream)))
+    return false;
+  w->dp_dev = false;
+  return true;
+}
+
+void plan_grid3(World3* w) {
+  const float hg = w->cfg.smoothing_length;
+  int64_t lo[3] = {INT64_MAX, INT64_MAX, INT64_MAX}, hi[3] = {INT64_MIN, INT64_MIN, INT64_MIN};
+  for (uint32_t i = 0; i < w->n; i++) {
+    const float4 p = w->h_pos[i];
+    if (!std::isfinite(p.x) || !std::isfinite(p.y) || !std::isfinite(p.z)) continue;
+    const int32_t c[3] = {sat_floor_i32(p.x / hg), sat_floor_i32(p.y / hg), sat_floor_i32(p.z / hg)};
+    for (int a = 0; a < 3; a++) {
+      lo[a] = std::min<int64_t>(lo[a], c[a]);
+      hi[a] = std::max<int64_t>(hi[a], c[a]);
+    }
+  }
+  if (lo[0] > hi[0]) lo[0] = lo[1] = lo[2] = hi[0] = hi[1] = hi[2] = 0;
+  uint32_t lg[3];  // log2 of the buckets along x, y, z (each >= 2)
+  int64_t mg[3];
+  for (int a = 0; a < 3; a++) {
+    const int64_t ext = hi[a] - lo[a] + 1;
+    mg[a] = std::max<int64_t>(2, ext / 8);
+    lg[a] = std::max<uint32_t>(2, log2u(next_pow2((uint64_t)(ext + 2 * mg[a]))));
+  }
+  // bucket budget: ~2 per particle (each bucket costs ~20 B of scan traffic),
+  // 2^12 .. 2^24; halve the longest axis until the grid fits
+  const uint32_t lb = std::min<uint32_t>(24, std::max<uint32_t>(12, log2u(next_pow2(2ull * w->n))));
+  while (lg[0] + lg[1] + lg[2] > lb) {
+    int a = 0;
+    for (int b = 1; b < 3; b++)
+      if (lg[b] > lg[a]) a = b;
+    if (lg[a] <= 2) break;
+    lg[a]--;
+  }
+  GridPlan3 g;
+  g.log2w = lg[0];
+  g.log2h = lg[1];
+  g.log2d = lg[2];
+  g.maskw = (1u << lg[0]) - 1;
+  g.maskh = (1u << lg[1]) - 1;
+  g.maskd = (1u << lg[2]) - 1;
+  g.nbuckets = 1u << (lg[0] + lg[1] + lg[2]);
+  g.sentinel = g.nbuckets;
+  g.cx0 = (int32_t)std::max<int64_t>(INT32_MIN, lo[0] - mg[0]);
+  g.cy0 = (int32_t)std::max<int64_t>(INT32_MIN, lo[1] - mg[1]);
+  g.cz0 = (int32_t)std::max<int64_t>(INT32_MIN, lo[2] - mg[2]);
+  g.hg = hg;
+  w->plan = g;
+  w->plan_valid = true;
+  w->keys_valid = false;
+}
+
+bool ensure_range3(World3* w) {
+  const uint32_t m = w->plan.sentinel + 1;
+  const uint32_t tiles = (m + kBucketScanTile - 1) / kBucketScanTile;
+  if (w->count && w->range_cap >= w->plan.nbuckets) {
+    w->count_len = tiles * kBucketScanTile;
+    return true;
+  }
+  cudaStreamSynchronize(w->stream);
+  dfree3(w->count), dfree3(w->start), dfree3(w->tilesum);
+  release_graph3(w);
+  const uint32_t len = tiles * kBucketScanTile;
+  if (!dalloc3(w, w->count, len) || !dalloc3(w, w->start, (size_t)len + 1) || !dalloc3(w, w->tilesum, tiles)) return false;
+  if (!ok3(w, cudaMemsetAsync(w->count, 0, sizeof(uint32_t) * len, w->stream))) return false;
+  w->range_cap = w->plan.nbuckets;
+  w->count_len = len;
+  w->keys_valid = false;
+  return true;
+}
+
+bool ensure_bodies3(World3* w) {
+  if (!w->bodies_dirty) return true;
+  const uint32_t nb = (uint32_t)w->bodies.size();
+  if (nb > w->bodies_cap || !w->dbodies) {
+    cudaStreamSynchronize(w->stream);
+    dfree3(w->dbodies);
+    release_graph3(w);
+    const uint32_t c = std::max<uint32_t>(16, nb);
+    if (!dalloc3(w, w->dbodies, c)) return false;
+    w->bodies_cap = c;
+  }
+  if (nb && !ok3(w, cudaMemcpyAsync(w->dbodies, w->bodies.data(), sizeof(DevBody3) * nb, cudaMemcpyHostToDevice,
+                                    w->stream)))
+    return false;
+  w->bodies_dirty = false;
+  return true;
+}
+
+void enqueue_keys3(World3* w, cudaStream_t st) {
+  cudaMemsetAsync(w->count, 0, sizeof(uint32_t) * w->count_len, st);
+  if (w->n) k_keys3<<<cdiv(w->n, 256), 256, 0, st>>>(w->pos, w->n, w->plan, w->key, w->count);
+}
+
+bool prepare3(World3* w) {
+  if (w->error != PHIENG_SPH_OK) return false;
+  if (!ensure_device3(w)) return false;
+  if (!w->dev_valid) {
+    if (!ensure_capacity3(w, w->n)) return false;
+    if (!w->plan_valid) plan_grid3(w);
+    if (w->n && (!ok3(w, cudaMemcpyAsync(w->pos, w->h_pos.data(), sizeof(float4) * w->n, cudaMemcpyHostToDevice,
+                                         w->stream)) ||
+                 !ok3(w, cudaMemcpyAsync(w->vel, w->h_vel.data(), sizeof(float4) * w->n, cudaMemcpyHostToDevice,
+                                         w->stream))))
+      return false;
+    w->dev_valid = true;
+    w->keys_valid = false;
+  }
+  if (!w->aux_valid && (!w->mass_uniform || !w->phase_uniform) && w->n) {
+    if (!ok3(w, cudaMemcpyAsync(w->mass, w->h_mass.data(), sizeof(float) * w->n, cudaMemcpyHostToDevice, w->stream)) ||
+        !ok3(w, cudaMemcpyAsync(w->phase, w->h_phase.data(), w->n, cudaMemcpyHostToDevice, w->stream)))
+      return false;
+    w->aux_valid = true;
+  }
+  if (!w->plan_valid) {
+    if (!ensure_host3(w)) return false;
+    plan_grid3(w);
+  }
+  if (!ensure_range3(w) || !ensure_bodies3(w)) return false;
+  if (!w->keys_valid) {
+    enqueue_keys3(w, w->stream);
+    w->keys_valid = true;
+  }
+  return ok3(w, cudaGetLastError());
+}
+
+StepParams3 make_params3(const World3* w, float dt) {
+  StepParams3 P;
+  std::memset(&P, 0, sizeof(P));
+  const FluidConfig3Ffi& c = w->cfg;
+  P.grid = w->plan;
+  const float hg = c.smoothing_length;
+  P.hg2 = hg * hg;
+  const float h = rmaxf(hg, kEps);
+  P.hk = h;
+  const float h2 = h * h;
+  P.hk2 = h2;
+  const float pi = 3.14159265358979323846f;
+  P.c_poly6 = 315.0f / (64.0f * pi * h2 * h2 * h2 * h2 * h);
+  P.c_spiky = -45.0f / (pi * h * h * h * h * h * h);
+  P.rho_cap = 3.0f * rmaxf(c.rest_density, kEps);
+  P.stiffness = c.stiffness;
+  P.gamma = c.gamma;
+  for (int k = 0; k < 4; k++) P.rest[k] = c.phase_rest_density[k];
+  P.mass = w->mass_value;
+  P.visc = c.viscosity;
+  P.vmax = c.max_velocity;
+  P.dt = dt;
+  P.gx = w->gx;
+  P.gy = w->gy;
+  P.gz = w->gz;
+  P.pr = rmaxf(c.particle_radius, 0.0f);
+  P.pr_pad = P.pr * 1.001f + 1e-30f;
+  float mu = c.wall_friction;
+  if (mu < 0.0f) mu = 0.0f;
+  if (mu > 1.0f) mu = 1.0f;
+  P.mu = mu;
+  P.av_alpha = c.artificial_viscosity;
+  P.c_s = std::sqrt(rmaxf(c.stiffness, 0.0f));
+  P.surface_tension = c.surface_tension;
+  uint32_t f = 0;
+  if (c.viscosity > 0.0f) f |= F_VISC;
+  if (c.artificial_viscosity > 0.0f) f |= F_AV;
+  if (c.surface_tension > 0.0f) f |= F_COHESION;
+  if (c.wall_friction > 0.0f) f |= F_FRICTION;
+  if (c.gamma != 1.0f) f |= F_TAIT;
+  if (!w->mass_uniform) f |= F_MASS;
+  if (!w->phase_uniform) f |= F_PHASE;
+  P.flags = f;
+  P.nbodies = (uint32_t)w->bodies.size();
+  P.uniform_phase = w->phase_value;
+  return P;
+}
+
+void enqueue_sort3(World3* w, const StepParams3& P, cudaStream_t st) {
+  BucketSort bs;
+  bs.count = w->count;
+  bs.tilesum = w->tilesum;
+  bs.done = w->scalar + 8;
+  bs.start = w->start;
+  bs.key = w->key;
+  bs.sid_prev = w->sid;
+  bs.tkey = w->tkey;
+  bs.tid = w->tid;
+  enqueue_bucket_place(bs, w->n, P.grid.sentinel + 1, w->sid_perm_n == w->n, st);
+  const bool m = (P.flags & F_MASS) != 0, ph = (P.flags & F_PHASE) != 0;
+  k_fixup3<<<cdiv(w->n, 256), 256, 0, st>>>(w->tkey, w->tid, w->start, w->n, w->skey, w->sid, w->pos, w->vel, w->mass,
+                                            w->phase, w->spos, w->svel, m ? w->smass : nullptr,
+                                            ph ? w->sphase : nullptr);
+  cudaMemsetAsync(w->count, 0, sizeof(uint32_t) * w->count_len, st);
+}
+
+void enqueue_density3(World3* w, const StepParams3& P, cudaStream_t st) {
+  const bool m = (P.flags & F_MASS) != 0, ph = (P.flags & F_PHASE) != 0;
+  const uint32_t g = cdiv(w->n, 256);
+#define PHIENG_D3(M, PH) \
+  k_density3<M, PH><<<g, 256, 0, st>>>(w->spos, w->skey, w->smass, w->sphase, w->n, w->start, P, w->sdq, w->spres, w->nmask)
+  if (m && ph) PHIENG_D3(true, true);
+  else if (m) PHIENG_D3(true, false);
+  else if (ph) PHIENG_D3(false, true);
+  else PHIENG_D3(false, false);
+#undef PHIENG_D3
+}
+
+void enqueue_force3(World3* w, const StepParams3& P, float4* dbg, cudaStream_t st) {
+  const bool m = (P.flags & F_MASS) != 0;
+  const uint32_t g = cdiv(w->n, 256);
+#define PHIENG_F3(M, D)                                                                                             \
+  k_force3<M, D><<<g, 256, 0, st>>>(w->spos, w->svel, w->sdq, w->skey, w->sid, w->smass, w->n, w->start, P,        \
+                                    w->dbodies, w->nmask, w->pos, w->vel, w->key, w->count, dbg)
+  if (dbg) {
+    if (m) PHIENG_F3(true, true);
+    else PHIENG_F3(false, true);
+  } else {
+    if (m) PHIENG_F3(true, false);
+    else PHIENG_F3(false, false);
+  }
+#undef PHIENG_F3
+}
+
+void enqueue_substep3(World3* w, const StepParams3& P, cudaStream_t st) {
+  if (w->profiling) cudaEventRecordWithFlags(w->ev[0], st, cudaEventRecordExternal);
+  enqueue_sort3(w, P, st);
+  if (w->profiling) cudaEventRecordWithFlags(w->ev[1], st, cudaEventRecordExternal);
+  enqueue_density3(w, P, st);
+  if (w->profiling) cudaEventRecordWithFlags(w->ev[2], st, cudaEventRecordExternal);
+  enqueue_force3(w, P, nullptr, st);
+  if (w->profiling) cudaEventRecordWithFlags(w->ev[3], st, cudaEventRecordExternal);
+}
+
+bool run_substep3(World3* w, const StepParams3& P) {
+  std::string sig((const char*)&P, sizeof(P));
+  sig.append((const char*)&w->n, sizeof(w->n));
+  sig.push_back(w->profiling ? 'p' : '-');
+  sig.push_back(w->sid_perm_n == w->n ? 's' : '-');
+  if (!w->gexec || sig != w->gsig) {
+    release_graph3(w);
+    cudaGraph_t g = nullptr;
+    if (!ok3(w, cudaStreamBeginCapture(w->own_stream, cudaStreamCaptureModeThreadLocal))) return false;
+    enqueue_substep3(w, P, w->own_stream);
+    cudaError_t r = cudaStreamEndCapture(w->own_stream, &g);
+    if (!ok3(w, r)) return false;
+    r = cudaGraphInstantiate(&w->gexec, g, 0);
+    cudaGraphDestroy(g);
+    if (!ok3(w, r)) {
+      w->gexec = nullptr;
+      return false;
+    }
+    w->gsig = sig;
+  }
+  if (!ok3(w, cudaGraphLaunch(w->gexec, w->stream))) return false;
+  w->sid_perm_n = w->n;
+  w->substeps++;
+  w->host_valid = false;
+  w->dp_dev = true;
+  w->keys_valid = true;
+  return true;
+}
+
+bool cfl_substeps3(World3* w, float dt, uint32_t* out) {
+  const FluidConfig3Ffi& c = w->cfg;
+  const uint32_t mx = std::max<uint32_t>(c.max_substeps, 1);
+  *out = 1;
+  if (c.cfl <= 0.0f || mx <= 1) return true;
+  const float h = rmaxf(c.smoothing_length, kEps);
+  const float rho0 = rmaxf(c.rest_density, kEps);
+  const float c0 = (c.gamma == 1.0f) ? std::sqrt(rmaxf(c.stiffness, 0.0f))
+                                     : std::sqrt(c.gamma * rmaxf(c.stiffness, 0.0f) * rho0);
+  float vmax = 0.0f;
+  if (w->host_valid) {
+    for (uint32_t i = 0; i < w->n; i++) {
+      const float4 v = w->h_vel[i];
+      vmax = rmaxf(vmax, std::sqrt(v.x * v.x + v.y * v.y + v.z * v.z));
+    }
+  } else {
+    cudaMemsetAsync(w->scalar, 0, 4, w->stream);
+    k_vmax3<<<std::min(cdiv(w->n, 256), 148u * 8u), 256, 0, w->stream>>>(w->vel, w->n, w->scalar);
+    if (!ok3(w, cudaMemcpyAsync(w->h_pinned, w->scalar, 4, cudaMemcpyDeviceToHost, w->stream)) ||
+        !ok3(w, cudaStreamSynchronize(w->stream)))
+      return false;
+    std::memcpy(&vmax, w->h_pinned, 4);
+  }
+  const float speed = c0 + vmax;
+  if (!std::isfinite(speed) || speed <= kEps) return true;
+  const float dt_max = c.cfl * h / speed;
+  if (!std::isfinite(dt_max) || dt_max <= 0.0f) return true;
+  const float q = std::ceil(dt / dt_max);
+  int64_t k;
+  if (q != q)
+    k = 0;
+  else if (q >= 9.2233720368547758e18f)
+    k = INT64_MAX;
+  else
+    k = (int64_t)q;
+  k = std::max<int64_t>(1, std::min<int64_t>(k, mx));
+  *out = (uint32_t)k;
+  return true;
+}
+
+bool world_step3(World3* w, float dt) {
+  if (w->cfg.enabled && w->n > 0 && dt > 0.0f) {
+    if (w->cfg.adaptive_resolution || w->cfg.boundary_particles) {
+      w->error = PHIENG_SPH_E_UNSUPPORTED;
+      return false;
+    }
+    if (!prepare3(w)) return false;
+    uint32_t ns = 1;
+    if (!cfl_substeps3(w, dt, &ns)) return false;
+    const StepParams3 P = make_params3(w, dt / (float)ns);
+    for (uint32_t k = 0; k < ns; k++)
+      if (!run_substep3(w, P)) return false;
+  }
+  w->time += dt;
+  return true;
+}
+
+void recompute_uniformity3(World3* w) {
+  w->mass_uniform = w->phase_uniform = true;
+  w->mass_value = rmaxf(w->cfg.phase_mass[0], 0.0f);
+  w->phase_value = 0;
+  if (w->n) {
+    w->mass_value = w->h_mass[0];
+    w->phase_value = std::min<uint32_t>(w->h_phase[0], 3);
+  }
+  for (uint32_t i = 1; i < w->n; i++) {
+    if (w->h_mass[i] != w->mass_value) w->mass_uniform = false;
+    if (std::min<uint32_t>(w->h_phase[i], 3) != w->phase_value) w->phase_uniform = false;
+  }
+}
+
+uint32_t add_particles3(World3* w, const float* xyz, const uint8_t* phases, uint32_t count) {
+  uint32_t n = std::min(count, kMaxAddPerCall);
+  for (uint64_t i = 0; i < 3ull * n; i++)
+    if (!std::isfinite(xyz[i])) return 0;
+  const uint32_t room = w->cap > w->n ? w->cap - w->n : 0;
+  n = std::min(n, room);
+  if (n == 0) return 0;
+  if (!ensure_host3(w) || !ensure_host_dp3(w)) return 0;
+  for (uint32_t i = 0; i < n; i++) {
+    const uint8_t ph = phases ? phases[i] : 0;
+    const uint32_t k = std::min<uint32_t>(ph, 3);
+    w->h_pos.push_back(make_float4(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2], 0.0f));
+    w->h_vel.push_back(make_float4(0.0f, 0.0f, 0.0f, 0.0f));
+    w->h_dens.push_back(w->cfg.phase_rest_density[k]);
+    w->h_pres.push_back(0.0f);
+    w->h_mass.push_back(rmaxf(w->cfg.phase_mass[k], 0.0f));
+    w->h_phase.push_back(ph);
+  }
+  w->n += n;
+  recompute_uniformity3(w);
+  w->dev_valid = w->aux_valid = w->plan_valid = w->keys_valid = false;
+  return n;
+}
+
+}  // namespace
+
+extern "C" {
+
+World3* phieng_world3_new(void) { return new (std::nothrow) World3(); }
+
+void phieng_world3_free(World3* w) {
+  if (!w) return;
+  if (w->device >= 0) {
+    cudaStreamSynchronize(w->stream);
+    release_graph3(w);
+    free_particles3(w);
+    dfree3(w->count), dfree3(w->start), dfree3(w->tilesum), dfree3(w->scalar), dfree3(w->dbodies);
+    for (auto& e : w->ev)
+      if (e) cudaEventDestroy(e);
+    if (w->h_pinned) cudaFreeHost(w->h_pinned);
+    if (w->own_stream) cudaStreamDestroy(w->own_stream);
+  }
+  delete w;
+}
+
+void phieng_world3_step(World3* w, float dt) {
+  if (!w || !std::isfinite(dt) || dt <= 0.0f) return;
+  world_step3(w, std::min(dt, kMaxDt));
+}
+
+void phieng_world3_set_gravity(World3* w, float gx, float gy, float gz) {
+  if (!w || !std::isfinite(gx) || !std::isfinite(gy) || !std::isfinite(gz)) return;
+  w->gx = gx;
+  w->gy = gy;
+  w->gz = gz;
+}
+
+int32_t phieng_world3_set_time(World3* w, float t) {
+  if (!w || !std::isfinite(t)) return 0;
+  w->time = t;
+  return 1;
+}
+
+int32_t phieng_world3_get_time(World3* w, float* out) {
+  if (!w || !out) return 0;
+  *out = w->time;
+  return 1;
+}
+
+int32_t phieng_world3_body_count(World3* w) { return w ? (int32_t)w->bodies.size() : -1; }
+
+int32_t phieng_world3_add_body(World3* w, float px, float py, float pz, uint32_t shape_tag, float a, float b, float c,
+                               float density, uint8_t is_static, float friction, float restitution) {
+  (void)friction;
+  (void)restitution;
+  if (!w || !std::isfinite(px) || !std::isfinite(py) || !std::isfinite(pz)) return -1;
+  auto pos = [](float v) { return std::isfinite(v) && v > 0.0f; };
+  DevBody3 bd;
+  std::memset(&bd, 0, sizeof(bd));
+  if (shape_tag == PHIENG_SHAPE3_SPHERE && pos(a)) {
+    bd.shape = 0;
+    bd.a = a;
+  } else if (shape_tag == PHIENG_SHAPE3_BOX && pos(a) && pos(b) && pos(c)) {
+    bd.shape = 1;
+    bd.a = a;
+    bd.b = b;
+    bd.c = c;
+  } else if (shape_tag == PHIENG_SHAPE3_CAPSULE && pos(a) && pos(b)) {
+    bd.shape = 2;
+    bd.a = a;
+    bd.b = b;
+  } else {
+    return -1;
+  }
+  if (!pos(density)) return -1;
+  if (!is_static) return -1;  // dynamic bodies are not part of this library
+  bd.px = px;
+  bd.py = py;
+  bd.pz = pz;
+  // world bounding box half extents of the (unrotated) body, padded by 0.1%
+  const float ex = bd.a;
+  const float ey = bd.shape == 0 ? bd.a : bd.shape == 1 ? bd.b : bd.b + bd.a;
+  const float ez = bd.shape == 1 ? bd.c : bd.a;
+  bd.ex = ex * 1.001f + 1e-30f;
+  bd.ey = ey * 1.001f + 1e-30f;
+  bd.ez = ez * 1.001f + 1e-30f;
+  if (w->bodies.size() >= 0x7FFFFFFF) return -1;
+  w->bodies.push_back(bd);
+  w->bodies_dirty = true;
+  return (int32_t)(w->bodies.size() - 1);
+}
+
+uint32_t phieng_world3_add_bodies(World3* w, const BodyDesc3D* descs, uint32_t n, int32_t* out_ids) {
+  if (!w || !descs || !out_ids) return 0;
+  n = std::min<uint32_t>(n, kMaxAddPerCall);
+  uint32_t added = 0;
+  for (uint32_t i = 0; i < n; i++) {
+    const BodyDesc3D& d = descs[i];
+    out_ids[i] = phieng_world3_add_body(w, d.pos_x, d.pos_y, d.pos_z, d.shape_tag, d.a, d.b, d.c, d.density,
+                                        d.is_static, d.friction, d.restitution);
+    if (out_ids[i] >= 0) added++;
+  }
+  return added;
+}
+
+int32_t phieng_world3_set_fluid_config(World3* w, const FluidConfig3Ffi* cfg) {
+  if (!w || !cfg || !valid_config(*cfg)) return 0;
+  if (w->device >= 0) cudaStreamSynchronize(w->stream);
+  if (!ensure_host3(w)) return 0;
+  w->cfg = *cfg;
+  w->plan_valid = false;
+  release_graph3(w);
+  return 1;
+}
+
+int32_t phieng_world3_get_fluid_config(World3* w, FluidConfig3Ffi* out) {
+  if (!w || !out) return 0;
+  *out = w->cfg;
+  return 1;
+}
+
+uint32_t phieng_world3_fluid_add(World3* w, const float* xyz, uint32_t count) {
+  if (!w || !xyz) return 0;
+  return add_particles3(w, xyz, nullptr, count);
+}
+
+uint32_t phieng_world3_fluid_add_phase(World3* w, const float* xyz, const uint8_t* phases, uint32_t count) {
+  if (!w || !xyz || !phases) return 0;
+  return add_particles3(w, xyz, phases, count);
+}
+
+uint32_t phieng_world3_fluid_count(const World3* w) { return w ? w->n : 0; }
+
+int32_t phieng_world3_fluid_clear(World3* w) {
+  if (!w) return 0;
+  if (w->device >= 0) cudaStreamSynchronize(w->stream);
+  w->n = 0;
+  w->h_pos.clear(), w->h_vel.clear(), w->h_mass.clear(), w->h_phase.clear(), w->h_dens.clear(), w->h_pres.clear();
+  w->dp_dev = false;
+  recompute_uniformity3(w);
+  w->host_valid = true;
+  w->dev_valid = w->aux_valid = w->plan_valid = w->keys_valid = false;
+  return 1;
+}
+
+uint32_t phieng_world3_fluid_get(const World3* cw, float* out, uint32_t max) {
+  if (!cw || !out) return 0;
+  World3* w = const_cast<World3*>(cw);
+  const uint32_t n = std::min(max, w->n);
+  if (n && !ensure_host3(w)) return 0;
+  for (uint32_t i = 0; i < n; i++) {
+    const float4 p = w->h_pos[i], v = w->h_vel[i];
+    float* o = out + 6 * (size_t)i;
+    o[0] = p.x, o[1] = p.y, o[2] = p.z, o[3] = v.x, o[4] = v.y, o[5] = v.z;
+  }
+  return n;
+}
+
+// ---- extension ----
+int32_t phieng_sph3_status(const World3* w, PhiengSphStatus* out) {
+  if (!w || !out) return 0;
+  std::memset(out, 0, sizeof(*out));
+  out->error = w->error;
+  out->particles = w->n;
+  out->substeps = w->substeps;
+  out->grid_log2_w = w->plan.log2w;
+  out->grid_log2_h = w->plan.log2h;
+  out->sort_passes = 1;
+  out->grid_cx0 = w->plan.cx0;
+  out->grid_cy0 = w->plan.cy0;
+  out->grid_buckets = w->plan.nbuckets;
+  return 1;
+}
+
+int32_t phieng_sph3_clear_error(World3* w) {
+  if (!w) return 0;
+  w->error = PHIENG_SPH_OK;
+  return 1;
+}
+
+const char* phieng_sph3_error_string(const World3* w) { return error_text(w ? w->error : PHIENG_SPH_E_ARG); }
+
+int32_t phieng_sph3_set_particle_cap(World3* w, uint32_t cap) {
+  if (!w || cap == 0) return 0;
+  w->cap = cap;
+  return 1;
+}
+
+int32_t phieng_sph3_step_n(World3* w, float dt, uint32_t steps) {
+  if (!w) return 0;
+  if (!std::isfinite(dt) || dt <= 0.0f) return 1;
+  const float d = std::min(dt, kMaxDt);
+  for (uint32_t s = 0; s < steps; s++)
+    if (!world_step3(w, d)) return 0;
+  return 1;
+}
+
+int32_t phieng_sph3_set_stream(World3* w, void* stream) {
+  if (!w) return 0;
+  if (w->device >= 0) cudaStreamSynchronize(w->stream);
+  w->stream = stream ? (cudaStream_t)stream : w->own_stream;
+  w->user_stream = stream != nullptr;
+  return 1;
+}
+
+int32_t phieng_sph3_sync(World3* w) {
+  if (!w) return 0;
+  if (w->device >= 0 && !ok3(w, cudaStreamSynchronize(w->stream))) return 0;
+  return w->error == PHIENG_SPH_OK ? 1 : 0;
+}
+
+int32_t phieng_sph3_set_state(World3* w, const float* xyzv, uint32_t n) {
+  if (!w || !xyzv || n > w->n) return 0;
+  for (uint64_t i = 0; i < 6ull * n; i++)
+    if (!std::isfinite(xyzv[i])) return 0;
+  if (!ensure_host3(w) || !ensure_host_dp3(w)) return 0;
+  for (uint32_t i = 0; i < n; i++) {
+    const float* q = xyzv + 6 * (size_t)i;
+    w->h_pos[i] = make_float4(q[0], q[1], q[2], 0.0f);
+    w->h_vel[i] = make_float4(q[3], q[4], q[5], 0.0f);
+  }
+  w->dev_valid = false;
+  w->keys_valid = false;
+  w->plan_valid = false;
+  return 1;
+}
+
+// Run the density pass (and, with fxyz, the force pass without integrating)
+// on the current state; write density, pressure and force [fx, fy, fz] in
+// insertion order (each output may be null). Returns the number written.
+uint32_t phieng_sph3_debug_forces(World3* w, float* dens, float* pres, float* fxyz, uint32_t max) {
+  if (!w) return 0;
+  const uint32_t n = std::min(max, w->n);
+  if (n == 0) return 0;
+  if (!prepare3(w)) return 0;
+  const StepParams3 P = make_params3(w, 0.0f);
+  float4* dbg = nullptr;
+  if (fxyz && !dalloc3(w, dbg, w->n)) return 0;
+  enqueue_sort3(w, P, w->stream);
+  enqueue_density3(w, P, w->stream);
+  if (fxyz) enqueue_force3(w, P, dbg, w->stream);
+  w->sid_perm_n = w->n;
+  w->keys_valid = false;  // the sort consumed the bucket counts
+  w->dp_dev = true;
+  std::vector<float> f(fxyz ? 4 * (size_t)w->n : 0);
+  bool ok = ok3(w, cudaGetLastError());
+  if (ok && fxyz)
+    ok = ok3(w, cudaMemcpyAsync(f.data(), dbg, sizeof(float4) * w->n, cudaMemcpyDeviceToHost, w->stream));
+  ok = ok && ensure_host_dp3(w);
+  cudaFree(dbg);
+  if (!ok) return 0;
+  if (dens) std::memcpy(dens, w->h_dens.data(), sizeof(float) * n);
+  if (pres) std::memcpy(pres, w->h_pres.data(), sizeof(float) * n);
+  if (fxyz)
+    for (uint32_t i = 0; i < n; i++) {
+      fxyz[3 * i] = f[4 * i];
+      fxyz[3 * i + 1] = f[4 * i + 1];
+      fxyz[3 * i + 2] = f[4 * i + 2];
+    }
+  return n;
+}
+
+// Density and pressure of every particle as the last substep's density pass
+// left them (insertion order; rest density and 0 before the first step).
+uint32_t phieng_sph3_get_density_pressure(World3* w, float* dens, float* pres, uint32_t max) {
+  if (!w) return 0;
+  const uint32_t n = std::min(max, w->n);
+  if (n == 0) return 0;
+  if (!ensure_host_dp3(w)) return 0;
+  if (dens) std::memcpy(dens, w->h_dens.data(), sizeof(float) * n);
+  if (pres) std::memcpy(pres, w->h_pres.data(), sizeof(float) * n);
+  return n;
+}
+
+int32_t phieng_sph3_set_profiling(World3* w, int32_t on) {
+  if (!w) return 0;
+  if (on && !w->ev[0]) {
+    if (!ensure_device3(w)) return 0;
+    for (auto& e : w->ev)
+      if (!ok3(w, cudaEventCreate(&e))) return 0;
+  }
+  w->profiling = on != 0;
+  release_graph3(w);
+  return 1;
+}
+
+uint32_t phieng_sph3_phase_times(World3* w, float* ms, uint32_t max) {
+  if (!w || !ms || !w->profiling || !w->ev[0] || max == 0) return 0;
+  if (!ok3(w, cudaEventSynchronize(w->ev[3]))) return 0;
+  const uint32_t k = std::min<uint32_t>(max, 3);
+  for (uint32_t i = 0; i < k; i++)
+    if (cudaEventElapsedTime(&ms[i], w->ev[i], w->ev[i + 1]) != cudaSuccess) return 0;
+  return k;
+}
+
+}  // extern "C"

@@ -32,7 +32,7 @@ def fp(a):
 def header_symbols():
     txt = open(os.path.join(ROOT, "include", "phieng_sph.h")).read()
     txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
-    return sorted(set(re.findall(r"\b(phieng_(?:world|sph|mlp)_[a-z0-9_]+)\s*\(", txt)))
+    return sorted(set(re.findall(r"\b(phieng_(?:world3?|sph3?|mlp)_[a-z0-9_]+)\s*\(", txt)))
 
 
 def test_header_declares_exactly_the_bound_symbols(lib):

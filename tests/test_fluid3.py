@@ -1,0 +1,575 @@
+"""3D SPH fluid (crates/dynamics/src/fluid3.rs) behind the phieng_world3_* ABI.
+
+CPU part: the oracle restatement against the reference's own 3D tests
+(fluid3.rs:1297-1600: kernel sanity, dam break containment, determinism,
+cohesion, CFL substeps, hydrostatic pressure) and the host side of the ABI
+(validation, counts, caps, loud failure without a device).
+
+GPU part: the CUDA path against the oracle in Jacobi mode, bit-exact: single
+density / force passes (dense rows past the 32-slot masks, wide sparse
+scenes whose bucket grid aliases and wraps), full world steps with walls,
+obstacles and every optional force term, and the reference's behaviour tests
+run on the GPU path.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from oracle.oracle import JACOBI, REF_SEQ, OracleWorld3, collide3, poly6_3, spiky_grad3
+from phi_eng_b200 import _abi
+from phi_eng_b200._abi import BodyDesc3D, default_config
+
+F = C.POINTER(C.c_float)
+SPHERE, BOX, CAPSULE = 0, 1, 2
+
+
+def fp(a):
+    return a.ctypes.data_as(F)
+
+
+def has_gpu():
+    try:
+        import torch
+
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+# ---- scenes --------------------------------------------------------------
+
+# The reference's test tank (fluid3.rs:1228-1247): floor top at y = -0.5,
+# inner walls at x, z = -0.5 and 4.5.
+TANK = [
+    (BOX, (2.0, -1.0, 2.0), (3.0, 0.5, 3.0)),
+    (BOX, (-1.0, 2.0, 2.0), (0.5, 3.5, 3.5)),
+    (BOX, (5.0, 2.0, 2.0), (0.5, 3.5, 3.5)),
+    (BOX, (2.0, 2.0, -1.0), (3.5, 3.5, 0.5)),
+    (BOX, (2.0, 2.0, 5.0), (3.5, 3.5, 0.5)),
+]
+
+
+def lattice(origin, nx, ny, nz, dx):
+    """fluid3.rs:1250-1266: x fastest, then y, then z."""
+    pts = []
+    for iz in range(nz):
+        for iy in range(ny):
+            for ix in range(nx):
+                pts.append(
+                    (
+                        np.float32(origin[0]) + np.float32(ix) * np.float32(dx),
+                        np.float32(origin[1]) + np.float32(iy) * np.float32(dx),
+                        np.float32(origin[2]) + np.float32(iz) * np.float32(dx),
+                    )
+                )
+    return np.array(pts, np.float32)
+
+
+def make_oracle(pts, bodies=TANK, cfg=None, phases=None, gravity=None, cap=4096, mode_fp64=False):
+    o = OracleWorld3(fp64=mode_fp64, cap=cap)
+    if cfg is not None:
+        o.set_config(cfg)
+    if gravity is not None:
+        o.set_gravity(*gravity)
+    for shape, pos, ext in bodies:
+        o.add_body(shape, *pos, *ext)
+    assert o.add_particles(pts, phases) == len(pts)
+    return o
+
+
+def make_gpu(pts, bodies=TANK, cfg=None, phases=None, gravity=None, cap=None):
+    from phi_eng_b200.world3 import World3
+
+    w = World3()
+    if cap is not None:
+        w.fluid.set_cap(cap)
+    if cfg is not None:
+        w.fluid.config = cfg
+    if gravity is not None:
+        w.gravity = gravity
+    for shape, pos, ext in bodies:
+        r = w._lib.phieng_world3_add_body(w._h, *pos, shape, *ext, 1.0, 1, 0.5, 0.0)
+        assert r >= 0
+    if phases is None:
+        assert w.fluid.add_particles(pts) == len(pts)
+    else:
+        assert w.fluid.add_particles_phase(pts, phases) == len(pts)
+    return w
+
+
+def bits(a):
+    return np.ascontiguousarray(a, np.float32).view(np.uint32)
+
+
+def assert_bit_equal(a, b, what):
+    a = np.asarray(a, np.float32)
+    b = np.asarray(b, np.float32)
+    assert a.shape == b.shape, what
+    bad = np.nonzero(bits(a) != bits(b))
+    if bad[0].size:
+        i = bad[0][0]
+        raise AssertionError(f"{what}: {bad[0].size} values differ; first at {i}: {a[i]} vs {b[i]}")
+
+
+def full_cfg():
+    """Every optional term of the 3D step on."""
+    c = default_config()
+    c.gamma = 7.0
+    c.stiffness = 60.0
+    c.cfl = 0.4
+    c.max_substeps = 4
+    c.artificial_viscosity = 0.5
+    c.surface_tension = 0.5
+    c.wall_friction = 0.3
+    c.viscosity = 0.2
+    c.phase_count = 2
+    c.phase_rest_density[1] = 1.5
+    c.phase_mass[1] = 0.09375
+    return c
+
+
+# ---- oracle vs the reference's tests (CPU) --------------------------------
+
+def test_kernels_sane():
+    """fluid3.rs:1297-1311."""
+    h = 0.5
+    peak = poly6_3(0.0, h)
+    assert peak > 0.0
+    assert poly6_3(h * h, h) == 0.0
+    assert poly6_3(h * h * 4.0, h) == 0.0
+    assert poly6_3(h * h * 0.25, h) < peak
+    g = spiky_grad3(0.25, 0.0, 0.0, 0.25, h)
+    assert g[0] < 0.0 and g[1] == 0.0 and g[2] == 0.0
+    assert spiky_grad3(h, 0.0, 0.0, h, h) == (0.0, 0.0, 0.0)
+    assert spiky_grad3(0.0, 0.0, 0.0, 0.0, h) == (0.0, 0.0, 0.0)
+
+
+def test_collide_shapes():
+    """fluid3.rs:471-590 with the identity rotation."""
+    pr = 0.125
+    n, d = collide3(SPHERE, 1.0, 0, 0, (0.0, 1.05, 0.0), pr)
+    assert n == pytest.approx((0.0, 1.0, 0.0)) and d == pytest.approx(0.075, abs=1e-6)
+    assert collide3(SPHERE, 1.0, 0, 0, (0.0, 1.2, 0.0), pr) is None
+    assert collide3(SPHERE, 1.0, 0, 0, (0.0, 0.0, 0.0), pr)[0] == (1.0, 0.0, 0.0)
+    # box: outside a face, inside near the +z face, nearest-face ordering
+    n, d = collide3(BOX, 1.0, 2.0, 3.0, (1.1, 0.0, 0.0), pr)
+    assert n == pytest.approx((1.0, 0.0, 0.0)) and d == pytest.approx(0.025, abs=1e-6)
+    n, d = collide3(BOX, 1.0, 2.0, 3.0, (0.0, 0.0, 2.9), pr)
+    assert n == (0.0, 0.0, 1.0) and d == pytest.approx(0.225, abs=1e-6)
+    n, _ = collide3(BOX, 1.0, 1.0, 1.0, (0.0, 0.0, 0.0), pr)
+    assert n == (1.0, 0.0, 0.0)  # dx <= dy && dx <= dz picks x first
+    # capsule (radius 0.5, half length 1 along y): side, cap, on the axis
+    n, d = collide3(CAPSULE, 0.5, 1.0, 0.0, (0.6, 0.3, 0.0), pr)
+    assert n == pytest.approx((1.0, 0.0, 0.0)) and d == pytest.approx(0.025, abs=1e-6)
+    n, _ = collide3(CAPSULE, 0.5, 1.0, 0.0, (0.0, 1.55, 0.0), pr)
+    assert n == pytest.approx((0.0, 1.0, 0.0))
+    n, d = collide3(CAPSULE, 0.5, 1.0, 0.0, (0.0, 0.5, 0.0), pr)
+    assert n == (1.0, 0.0, 0.0) and d == pytest.approx(0.625)
+
+
+@pytest.mark.parametrize("mode", [REF_SEQ, JACOBI])
+def test_oracle_dam_break_contained(mode):
+    """fluid3.rs:1314-1347 on the oracle (both integrate orders)."""
+    o = make_oracle(lattice((0.0, 0.0, 0.0), 4, 6, 4, 0.25))
+    peak, max_x = 0.0, 0.0
+    for _ in range(400):
+        o.step(1 / 60, mode)
+        s = o.state()
+        peak = max(peak, float(np.sqrt((s[:, 3:] ** 2).sum(1)).max()))
+        max_x = max(max_x, float(s[:, 0].max()))
+    s = o.state()
+    assert np.isfinite(s).all()
+    assert max_x > 1.5
+    assert (s[:, 0] > -1).all() and (s[:, 0] < 5).all() and (s[:, 2] > -1).all() and (s[:, 2] < 5).all()
+    assert (s[:, 1] > -0.6).all()
+    assert peak < 30.0
+    assert o.count == 96
+
+
+def test_oracle_determinism():
+    """fluid3.rs:1399-1416."""
+
+    def run():
+        o = make_oracle(lattice((0.0, 0.0, 0.0), 4, 5, 4, 0.25))
+        for _ in range(80):
+            o.step(1 / 60)
+        return o.state()
+
+    assert_bit_equal(run(), run(), "oracle rerun")
+
+
+def test_oracle_cohesion_attracts():
+    """fluid3.rs:1458-1471."""
+    c = default_config()
+    c.stiffness = 0.0
+    c.viscosity = 0.0
+    c.surface_tension = 1000.0
+    o = make_oracle(np.array([[0, 0, 0], [0.4, 0, 0]], np.float32), bodies=[], cfg=c, gravity=(0, 0, 0))
+    o.step(1 / 60)
+    s = o.state()
+    assert s[0, 3] > 0.0 and s[1, 3] < 0.0
+
+
+def test_oracle_cfl_substeps():
+    """fluid3.rs:1474-1487."""
+    o = make_oracle(np.array([[0, 0, 0], [0.25, 0, 0]], np.float32), bodies=[])
+    assert o.cfl_substeps(1 / 60) == 1
+    c = default_config()
+    c.gamma = 7.0
+    c.stiffness = 200.0
+    c.cfl = 0.4
+    c.max_substeps = 8
+    o.set_config(c)
+    o.set_state(np.array([[0, 0, 0, 20, 0, 0], [0.25, 0, 0, 0, 0, 0]], np.float32))
+    assert 2 <= o.cfl_substeps(1 / 60) <= 8
+
+
+def hydrostatic_check(ys, pres):
+    """The assertions of fluid3.rs:1561-1600 on final heights / pressures."""
+    keep = (ys > -1.0) & (ys < 6.0)
+    ysk = np.sort(ys[keep])
+    n, tenth = ysk.size, ysk.size // 10
+    bottom = ysk[:tenth].mean()
+    surface = ysk[n - tenth:].mean()
+    lo, hi = ysk[tenth], ysk[n - tenth]
+    p_bottom = pres[ys <= lo].mean()
+    p_top = pres[ys >= hi].mean()
+    expected = 1.0 * 9.81 * (surface - bottom)
+    assert p_bottom > p_top
+    assert 0.25 * expected < p_bottom < 3.5 * expected, (p_bottom, expected)
+
+
+@pytest.mark.slow
+def test_oracle_hydrostatic_pressure():
+    """fluid3.rs:1561-1600 on the oracle (Jacobi order, as the GPU runs it)."""
+    o = make_oracle(lattice((0.0, -0.375, 0.0), 8, 10, 8, 0.25))
+    o.steps(1 / 60, 900, JACOBI)
+    s = o.state()
+    assert np.isfinite(s).all()
+    _, p = o.density_pressure()
+    hydrostatic_check(s[:, 1], p)
+
+
+def test_jacobi_tracks_reference_order():
+    """The GPU integrates in Jacobi order; the reference updates in place.
+    Both orders give the same bulk flow: the dam front and the mean height
+    after a second of flow agree closely."""
+    fronts = {}
+    for mode in (REF_SEQ, JACOBI):
+        o = make_oracle(lattice((0.0, 0.0, 0.0), 6, 8, 6, 0.25))
+        o.steps(1 / 60, 60, mode)
+        s = o.state()
+        fronts[mode] = (float(np.percentile(s[:, 0], 95)), float(s[:, 1].mean()))
+    assert abs(fronts[REF_SEQ][0] - fronts[JACOBI][0]) < 0.1 * fronts[REF_SEQ][0]
+    assert abs(fronts[REF_SEQ][1] - fronts[JACOBI][1]) < 0.1
+
+
+# ---- host side of the 3D ABI (CPU, no kernel launches) ---------------------
+
+@pytest.fixture(scope="module")
+def lib():
+    return _abi.load()
+
+
+@pytest.fixture
+def w3(lib):
+    h = lib.phieng_world3_new()
+    yield h
+    lib.phieng_world3_free(h)
+
+
+def test_world3_null_tolerance(lib):
+    lib.phieng_world3_free(None)
+    lib.phieng_world3_step(None, 0.01)
+    lib.phieng_world3_set_gravity(None, 0, 0, 0)
+    assert lib.phieng_world3_body_count(None) == -1
+    assert lib.phieng_world3_fluid_count(None) == 0
+    assert lib.phieng_world3_fluid_clear(None) == 0
+    out = np.zeros(6, np.float32)
+    assert lib.phieng_world3_fluid_get(None, fp(out), 1) == 0
+    assert lib.phieng_world3_fluid_add(None, fp(out), 1) == 0
+    assert lib.phieng_world3_set_time(None, 1.0) == 0
+    assert lib.phieng_world3_add_body(None, 0, 0, 0, 0, 1, 0, 0, 1, 1, 0.5, 0) == -1
+
+
+def test_world3_add_body_validation(lib, w3):
+    """ffi.rs:3703-3760: per-shape positivity and finiteness, density > 0."""
+    nan, inf = float("nan"), float("inf")
+    add = lambda *a: lib.phieng_world3_add_body(w3, *a)  # noqa: E731
+    assert add(0, 0, 0, SPHERE, 1.0, 0, 0, 1.0, 1, 0.5, 0) == 0
+    assert add(0, 0, 0, BOX, 1.0, 2.0, 3.0, 1.0, 1, 0.5, 0) == 1
+    assert add(0, 0, 0, CAPSULE, 0.5, 1.0, 0, 1.0, 1, 0.5, 0) == 2
+    assert add(nan, 0, 0, SPHERE, 1.0, 0, 0, 1.0, 1, 0.5, 0) == -1
+    assert add(0, 0, inf, SPHERE, 1.0, 0, 0, 1.0, 1, 0.5, 0) == -1
+    assert add(0, 0, 0, SPHERE, 0.0, 0, 0, 1.0, 1, 0.5, 0) == -1
+    assert add(0, 0, 0, BOX, 1.0, 2.0, 0.0, 1.0, 1, 0.5, 0) == -1
+    assert add(0, 0, 0, CAPSULE, 0.5, -1.0, 0, 1.0, 1, 0.5, 0) == -1
+    assert add(0, 0, 0, 3, 1.0, 1.0, 1.0, 1.0, 1, 0.5, 0) == -1
+    assert add(0, 0, 0, SPHERE, 1.0, 0, 0, 0.0, 1, 0.5, 0) == -1
+    assert add(0, 0, 0, SPHERE, 1.0, 0, 0, nan, 1, 0.5, 0) == -1
+    assert add(0, 0, 0, SPHERE, 1.0, 0, 0, 1.0, 0, 0.5, 0) == -1  # dynamic: not in this library
+    assert lib.phieng_world3_body_count(w3) == 3
+
+
+def test_world3_add_bodies_bulk(lib, w3):
+    descs = (BodyDesc3D * 3)()
+    descs[0] = BodyDesc3D(0, 0, 0, SPHERE, 1.0, 0, 0, 1.0, 1, (C.c_uint8 * 3)(), 0.5, 0)
+    descs[1] = BodyDesc3D(0, 0, 0, BOX, 1.0, 1.0, 0.0, 1.0, 1, (C.c_uint8 * 3)(), 0.5, 0)  # bad c
+    descs[2] = BodyDesc3D(1, 2, 3, CAPSULE, 0.5, 1.0, 0, 1.0, 1, (C.c_uint8 * 3)(), 0.5, 0)
+    ids = (C.c_int32 * 3)()
+    assert lib.phieng_world3_add_bodies(w3, descs, 3, ids) == 2
+    assert list(ids) == [0, -1, 1]
+    assert lib.phieng_world3_add_bodies(w3, None, 3, ids) == 0
+
+
+def test_world3_config_roundtrip_and_rejection(lib, w3):
+    c = full_cfg()
+    assert lib.phieng_world3_set_fluid_config(w3, C.byref(c)) == 1
+    out = _abi.FluidConfig3Ffi()
+    assert lib.phieng_world3_get_fluid_config(w3, C.byref(out)) == 1
+    assert bytes(out) == bytes(c)
+    bad = full_cfg()
+    bad.gamma = 0.5
+    assert lib.phieng_world3_set_fluid_config(w3, C.byref(bad)) == 0
+    assert lib.phieng_world3_get_fluid_config(w3, C.byref(out)) == 1 and out.gamma == 7.0
+
+
+def test_world3_fluid_add_get_clear(lib, w3):
+    pts = lattice((0.0, 0.0, 0.0), 3, 2, 2, 0.25)
+    assert lib.phieng_world3_fluid_add(w3, fp(pts.ravel()), 12) == 12
+    assert lib.phieng_world3_fluid_count(w3) == 12
+    out = np.zeros((12, 6), np.float32)
+    assert lib.phieng_world3_fluid_get(w3, fp(out), 12) == 12
+    assert_bit_equal(out[:, :3], pts, "positions")
+    assert (out[:, 3:] == 0).all()
+    assert lib.phieng_world3_fluid_get(w3, fp(out), 5) == 5
+    # one non-finite value rejects the whole call
+    bad = pts.copy()
+    bad[7, 2] = np.nan
+    assert lib.phieng_world3_fluid_add(w3, fp(bad.ravel()), 12) == 0
+    assert lib.phieng_world3_fluid_count(w3) == 12
+    ph = np.array([0, 1, 3, 7], np.uint8)
+    assert lib.phieng_world3_fluid_add_phase(w3, fp(pts[:4].ravel()), ph.ctypes.data_as(C.POINTER(C.c_uint8)), 4) == 4
+    assert lib.phieng_world3_fluid_add_phase(w3, fp(pts[:4].ravel()), None, 4) == 0
+    d = np.zeros(16, np.float32)
+    p = np.ones(16, np.float32)
+    assert lib.phieng_sph3_get_density_pressure(w3, fp(d), fp(p), 16) == 16
+    assert (d == 1.0).all() and (p == 0).all()  # rest density before the first step
+    assert lib.phieng_world3_fluid_clear(w3) == 1
+    assert lib.phieng_world3_fluid_count(w3) == 0
+
+
+def test_world3_particle_cap(lib, w3):
+    """MAX_PARTICLES_3D = 4096 (fluid3.rs:28): excess is dropped."""
+    pts = np.zeros((5000, 3), np.float32)
+    pts[:, 0] = np.arange(5000, dtype=np.float32)
+    assert lib.phieng_world3_fluid_add(w3, fp(pts.ravel()), 5000) == 4096
+    assert lib.phieng_world3_fluid_add(w3, fp(pts.ravel()), 10) == 0
+
+
+def test_world3_time(lib, w3):
+    t = C.c_float()
+    assert lib.phieng_world3_get_time(w3, C.byref(t)) == 1 and t.value == 0.0
+    assert lib.phieng_world3_set_time(w3, float("inf")) == 0
+    assert lib.phieng_world3_set_time(w3, 2.5) == 1
+    lib.phieng_world3_step(w3, float("nan"))
+    lib.phieng_world3_step(w3, -1.0)
+    lib.phieng_world3_step(w3, 1.0)  # no particles: only the clock moves, by min(dt, 1/15)
+    assert lib.phieng_world3_get_time(w3, C.byref(t)) == 1
+    assert t.value == np.float32(np.float32(2.5) + np.float32(1 / 15))
+
+
+@pytest.mark.skipif(has_gpu(), reason="checks the no-device error path")
+def test_world3_fails_loudly_without_device(lib, w3):
+    pts = lattice((0.0, 0.0, 0.0), 2, 2, 2, 0.25)
+    assert lib.phieng_world3_fluid_add(w3, fp(pts.ravel()), 8) == 8
+    lib.phieng_world3_step(w3, 1 / 60)
+    st = _abi.PhiengSphStatus()
+    assert lib.phieng_sph3_status(w3, C.byref(st)) == 1
+    assert st.error == _abi.E_NO_DEVICE
+    assert b"CUDA" in lib.phieng_sph3_error_string(w3)
+
+
+# ---- GPU parity ------------------------------------------------------------
+
+def jittered_block(rng, n_side, spacing, origin=(0.0, 0.0, 0.0), jitter=0.3):
+    i, j, k = np.meshgrid(*(np.arange(n_side),) * 3, indexing="ij")
+    p = np.stack([i, j, k], -1).reshape(-1, 3).astype(np.float64) * spacing
+    p += rng.uniform(-jitter, jitter, p.shape) * spacing + np.array(origin)
+    return p.astype(np.float32)
+
+
+def gpu_vs_oracle_passes(pts, cfg=None, phases=None, cap=None):
+    o = make_oracle(pts, bodies=[], cfg=cfg, phases=phases, cap=cap or 4096)
+    o.passes(forces=True)
+    d_ref, p_ref = o.density_pressure()
+    f_ref = o.forces()
+    w = make_gpu(pts, bodies=[], cfg=cfg, phases=phases, cap=cap)
+    d, p, f = w.debug_forces()
+    assert_bit_equal(d, d_ref, "density")
+    assert_bit_equal(p, p_ref, "pressure")
+    assert_bit_equal(f, f_ref, "force")
+    return w
+
+
+@pytest.mark.gpu
+def test_passes_bit_exact_lattice():
+    rng = np.random.default_rng(3)
+    gpu_vs_oracle_passes(jittered_block(rng, 10, 0.25))
+
+
+@pytest.mark.gpu
+def test_passes_bit_exact_all_terms():
+    rng = np.random.default_rng(4)
+    pts = jittered_block(rng, 9, 0.22)
+    phases = rng.integers(0, 2, len(pts)).astype(np.uint8)
+    gpu_vs_oracle_passes(pts, cfg=full_cfg(), phases=phases)
+
+
+@pytest.mark.gpu
+def test_passes_bit_exact_dense_rows():
+    """Rows of three cells holding far more than 32 particles take the
+    unmasked path."""
+    rng = np.random.default_rng(5)
+    w = gpu_vs_oracle_passes(jittered_block(rng, 14, 0.09, jitter=0.45))
+    assert len(w.fluid) == 14**3
+
+
+@pytest.mark.gpu
+def test_passes_bit_exact_aliased_grid():
+    """Particles spread over far more cells than the bucket budget: the grid
+    aliases and particles sit on the wrap seam."""
+    rng = np.random.default_rng(6)
+    pts = rng.uniform(-40.0, 40.0, (3000, 3)).astype(np.float32)
+    pts[:1500] = jittered_block(rng, 12, 0.25, origin=(-1.0, -1.0, -1.0))[:1500]
+    w = gpu_vs_oracle_passes(pts)
+    st = w.status()
+    assert st.grid_buckets < 160**3  # aliasing is in play
+
+
+def run_both(pts, steps, dt=1 / 60, bodies=TANK, cfg=None, phases=None, gravity=None, cap=None):
+    o = make_oracle(pts, bodies=bodies, cfg=cfg, phases=phases, gravity=gravity, cap=cap or 4096)
+    w = make_gpu(pts, bodies=bodies, cfg=cfg, phases=phases, gravity=gravity, cap=cap)
+    for _ in range(steps):
+        o.step(dt, JACOBI)
+        w.step(dt)
+    return o, w
+
+
+@pytest.mark.gpu
+def test_dam_break_bit_exact():
+    o, w = run_both(lattice((0.0, 0.0, 0.0), 4, 6, 4, 0.25), 200)
+    assert_bit_equal(w.fluid.particles, o.state(), "state after 200 steps")
+    d, p = w.fluid.density_pressure()
+    d_ref, p_ref = o.density_pressure()
+    assert_bit_equal(d, d_ref, "density")
+    assert_bit_equal(p, p_ref, "pressure")
+    assert w.time == o.time
+
+
+@pytest.mark.gpu
+def test_all_terms_with_obstacles_bit_exact():
+    """Tait EOS, CFL substeps, AV, cohesion, XSPH, wall friction, two phases
+    of different mass, and sphere / capsule / box obstacles in the tank."""
+    bodies = TANK + [
+        (SPHERE, (2.5, 0.2, 1.0), (0.4, 0.0, 0.0)),
+        (CAPSULE, (1.5, 0.3, 3.0), (0.25, 0.5, 0.0)),
+        (BOX, (3.5, -0.2, 3.2), (0.3, 0.3, 0.6)),
+    ]
+    pts = lattice((0.0, 0.0, 0.0), 6, 8, 6, 0.25)
+    phases = (np.arange(len(pts)) % 3 == 0).astype(np.uint8)
+    o, w = run_both(pts, 150, bodies=bodies, cfg=full_cfg(), phases=phases)
+    assert_bit_equal(w.fluid.particles, o.state(), "state after 150 steps")
+
+
+@pytest.mark.gpu
+def test_large_raised_cap_bit_exact():
+    """32k particles (past the reference's 4096 cap, raised on both sides)."""
+    c = default_config()
+    bodies = [(BOX, (8.0, -1.0, 8.0), (9.0, 0.5, 9.0))]
+    pts = lattice((0.0, 0.0, 0.0), 32, 32, 32, 0.25)
+    o, w = run_both(pts, 5, bodies=bodies, cfg=c, cap=40000)
+    assert_bit_equal(w.fluid.particles, o.state(), "state after 5 steps")
+
+
+@pytest.mark.gpu
+def test_gpu_dam_break_contained():
+    """fluid3.rs:1314-1347 on the GPU path."""
+    from phi_eng_b200.world3 import World3  # noqa: F401
+
+    w = make_gpu(lattice((0.0, 0.0, 0.0), 4, 6, 4, 0.25))
+    peak, max_x = 0.0, 0.0
+    for _ in range(400):
+        w.step(1 / 60)
+        s = w.fluid.particles
+        peak = max(peak, float(np.sqrt((s[:, 3:] ** 2).sum(1)).max()))
+        max_x = max(max_x, float(s[:, 0].max()))
+    s = w.fluid.particles
+    assert np.isfinite(s).all() and max_x > 1.5 and peak < 30.0
+    assert (s[:, 0] > -1).all() and (s[:, 0] < 5).all() and (s[:, 2] > -1).all() and (s[:, 2] < 5).all()
+    assert (s[:, 1] > -0.6).all() and len(w.fluid) == 96
+
+
+@pytest.mark.gpu
+def test_gpu_determinism():
+    def run():
+        w = make_gpu(lattice((0.0, 0.0, 0.0), 4, 5, 4, 0.25))
+        w.step_n(1 / 60, 80)
+        return w.fluid.particles
+
+    assert_bit_equal(run(), run(), "GPU rerun")
+
+
+@pytest.mark.gpu
+def test_gpu_cohesion_attracts():
+    c = default_config()
+    c.stiffness = 0.0
+    c.viscosity = 0.0
+    c.surface_tension = 1000.0
+    w = make_gpu(np.array([[0, 0, 0], [0.4, 0, 0]], np.float32), bodies=[], cfg=c, gravity=(0, 0, 0))
+    w.step(1 / 60)
+    s = w.fluid.particles
+    assert s[0, 3] > 0.0 and s[1, 3] < 0.0
+
+
+@pytest.mark.gpu
+def test_gpu_hydrostatic_pressure():
+    """fluid3.rs:1561-1600 on the GPU path."""
+    w = make_gpu(lattice((0.0, -0.375, 0.0), 8, 10, 8, 0.25))
+    w.step_n(1 / 60, 900)
+    s = w.fluid.particles
+    assert np.isfinite(s).all()
+    _, p = w.fluid.density_pressure()
+    hydrostatic_check(s[:, 1], p)
+
+
+@pytest.mark.gpu
+def test_gpu_add_between_steps_and_set_state():
+    """Particles added after stepping keep the earlier particles' density
+    and pressure; set_state moves particles; both stay bit-exact."""
+    pts = lattice((0.0, 0.0, 0.0), 4, 4, 4, 0.25)
+    o, w = run_both(pts, 30)
+    more = lattice((2.0, 1.0, 2.0), 3, 3, 3, 0.25)
+    assert o.add_particles(more) == 27 and w.fluid.add_particles(more) == 27
+    q = o.state()
+    q[0] = (1.0, 2.0, 1.0, 0.5, -1.0, 0.25)
+    o.set_state(q[:1])
+    w.fluid.set_state(q[:1])
+    for _ in range(30):
+        o.step(1 / 60, JACOBI)
+        w.step(1 / 60)
+    assert_bit_equal(w.fluid.particles, o.state(), "state")
+    d, p = w.fluid.density_pressure()
+    d_ref, p_ref = o.density_pressure()
+    assert_bit_equal(d, d_ref, "density")
+    assert_bit_equal(p, p_ref, "pressure")
+
+
+@pytest.mark.gpu
+def test_gpu_profiling_phase_times():
+    w = make_gpu(lattice((0.0, 0.0, 0.0), 8, 8, 8, 0.25))
+    w.set_profiling(True)
+    w.step(1 / 60)
+    t = w.phase_times()
+    assert t.shape == (3,) and (t > 0).all()
