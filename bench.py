@@ -307,6 +307,88 @@ def closure_line(sc) -> dict:
             "threshold": 0.03, "criterion": r["criterion"], "coarse_steps": 50, "dt_ratio": 4}
 
 
+# 3D (fluid3.rs) chain, bytes per particle of each phase:
+#   sort:    place 16 (read key + previous slot id, write key, id); fixup 64
+#            + 8 (read key, id, start pair; write key, id; gather pos 16 +
+#            vel 16 -> write 32)                                  = 104 + 20 B/N
+#   density: read pos 16 + key 4; write (density, q) 8 + pressure 4 + nine
+#            32-bit row masks 36                                     = 68
+#   force:   read pos 16, vel 16, (density, q) 8, key 4, id 4, masks 36;
+#            write pos 16 + vel 16 + next key 4                       = 120
+DENSITY3_BYTES = 68
+FORCE3_BYTES = 120
+
+
+def fluid3d_line(steps: int, warmup: int, side: int = 100) -> dict:
+    """The 3D step (phieng_world3_*) on a side^3-particle dam break: a block at
+    the reference's lattice spacing 0.25 m in a walled tank 2.5 x 1.5 x 1.5
+    times its size, the reference's default FluidConfig3 and world step
+    dt = 1/60 (its tests' step). Device-timed like the main line (L2 flushed
+    between timed steps), with the oracle's in-place CPU step on the
+    reference's particle cap (4096) beside it."""
+    import torch
+
+    from phi_eng_b200.world3 import World3, dam_break_3d
+
+    L = side * 0.25
+    pts, bodies = dam_break_3d(side, side, side, 0.25, tank=(2.5 * L, 1.5 * L, 1.5 * L))
+    n = len(pts)
+    w = World3()
+    w.fluid.set_cap(n)
+    for pos, sh in bodies:
+        w.add_static_body(pos, sh)
+    assert w.fluid.add_particles(pts) == n
+    stream = torch.cuda.Stream()
+    w.set_stream(stream.cuda_stream)
+    dt = 1.0 / 60.0
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    for _ in range(max(warmup, 3)):
+        w.step(dt)
+    w.set_profiling(True)
+    w.step(dt)
+    buckets = w.status().grid_buckets
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    phases = []
+    for k in range(steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        ev[k][0].record(stream)
+        w.step(dt)
+        ev[k][1].record(stream)
+        phases.append(w.phase_times())
+    torch.cuda.synchronize()
+    ms = sum(a.elapsed_time(b) for a, b in ev) / steps
+    ph = np.array(phases).mean(axis=0)
+    names = ["sort_ranges", "density", "force_integrate"]
+    bytes_pp = [104 + 20 * buckets / n, DENSITY3_BYTES, FORCE3_BYTES]
+    top = int(np.argmax(ph))
+    peak, _ = hbm_peak()
+    achieved = bytes_pp[top] * n / (ph[top] / 1000.0) / 1e9
+    s = w.fluid.particles
+    w.close()
+    # the reference's algorithm on the CPU at its particle cap
+    from oracle.oracle import REF_SEQ, OracleWorld3
+
+    cpts, cbodies = dam_break_3d(16, 16, 16, 0.25, tank=(10.0, 6.0, 6.0))
+    o = OracleWorld3()
+    for pos, sh in cbodies:
+        o.add_body(1, *pos, sh.hx, sh.hy, sh.hz)
+    o.add_particles(cpts)
+    o.steps(dt, 2, REF_SEQ)
+    k = 20
+    secs = o.steps(dt, k, REF_SEQ)
+    return {"metric": METRIC, "value": n / (ms / 1000.0), "ms_per_step": ms, "particles": n,
+            "workload": f"3D dam break, {side}^3 particles at 0.25 m in a {2.5 * L:g} x {1.5 * L:g} x {1.5 * L:g} m "
+                        "tank (floor + 4 walls), FluidConfig3 defaults, dt = 1/60",
+            "phases_ms": {nm: float(v) for nm, v in zip(names, ph)}, "buckets": int(buckets),
+            "roofline": {"bound": "hbm", "kernel": names[top], "bytes_per_particle": bytes_pp[top],
+                         "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak},
+            "finite": bool(np.isfinite(s).all()),
+            "cpu_baseline": {"value": 4096 * k / secs, "unit": METRIC, "cores": 1, "kind": "port",
+                             "sample": f"{k} in-place steps of a 4096-particle 3D dam break (the reference's cap)"}}
+
+
 def run_slab(args, rank: int, world: int, local_rank: int) -> None:
     """The single scene split in x slabs over the ranks (halo exchange and
     migration over NCCL each substep, phi_eng_b200/slab.py); strong scaling.
@@ -469,6 +551,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                 "clocks": clocks}
         if args.closure and len(scs) == 1 and world == 1:
             line["closure"] = closure_line(scs[0])
+        if args.fluid3d and world == 1:
+            line["fluid3d"] = fluid3d_line(args.steps, args.warmup)
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
@@ -488,6 +572,8 @@ def main():
                     help="N > 1: independent replicas (weak scaling) or the scene split in x slabs (strong)")
     ap.add_argument("--no-closure", dest="closure", action="store_false",
                     help="skip the learned-closure comparison line")
+    ap.add_argument("--no-fluid3d", dest="fluid3d", action="store_false",
+                    help="skip the 3D step line")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     rank = int(os.environ.get("RANK", "0"))
