@@ -294,13 +294,18 @@ __global__ void __launch_bounds__(256) k_density3(const float4* __restrict__ spo
       for (int r = 0; r < 9; r++) {
         const uint32_t row = row_base3(by, bz, r, g);
         const uint32_t rs = __ldg(&start[row + bx - 1]), re = __ldg(&start[row + bx + 2]);
-        uint32_t m = 0;
+        uint32_t m = 0, bit = 1u;  // bit shifts out after 32 slots (then masked is false)
         for (uint32_t j = rs; j < re; j++) {
           const float4 a = __ldg(&spos[j]);
           const float dx = __fsub_rn(a.x, pi.x), dy = __fsub_rn(a.y, pi.y), dz = __fsub_rn(a.z, pi.z);
           const float d2 = dot3(dx, dy, dz, dx, dy, dz);
-          rho = __fadd_rn(rho, contrib3(d2, MASS ? __ldg(&smass[j]) : P.mass, P));
-          if (j - rs < kMaskBits3) m |= (uint32_t)(d2 < P.hg2) << (j - rs);
+          const bool nb = d2 < P.hg2;
+          const float t = __fsub_rn(P.hk2, d2);  // poly6 without its range test: 0 <= d2 < h*h <= hk*hk
+          const float w = __fmul_rn(MASS ? __ldg(&smass[j]) : P.mass,
+                                    __fmul_rn(__fmul_rn(__fmul_rn(P.c_poly6, t), t), t));
+          rho = nb ? __fadd_rn(rho, w) : rho;
+          m |= nb ? bit : 0u;
+          bit <<= 1;
         }
         if (re - rs > kMaskBits3) masked = false;
         if (r == 4) m_own = m;
@@ -420,16 +425,20 @@ __global__ void __launch_bounds__(256) k_force3(const float4* __restrict__ spos,
   if (k != g.sentinel) {
     const uint32_t bx = k & g.maskw, by = (k >> g.log2w) & g.maskh, bz = k >> (g.log2w + g.log2h);
     if (nmask[4 * (size_t)n + s] != 0u) {
-#pragma unroll 1
-      for (int r = 0; r < 9; r++) {
-        uint32_t cur = nmask[(size_t)r * n + s];
-        if (cur == 0u) continue;
-        const uint32_t base = __ldg(&start[row_base3(by, bz, r, g) + bx - 1]);
-        while (cur) {
-          const uint32_t j = base + (uint32_t)(__ffs((int)cur) - 1);
-          cur &= cur - 1u;
-          if (j != s) pair3<MASS>(j, pi, vi, rho_i, q_i, m_i, spos, svel, sdq, smass, P, f, sm);
+      // one loop over the nine rows' set bits (ascending slots, row by row), so
+      // a warp runs as many pair iterations as its busiest lane has neighbours
+      uint32_t cur = 0u, base = 0u;
+      int r = -1;
+      for (;;) {
+        while (cur == 0u && r < 8) {
+          r++;
+          cur = nmask[(size_t)r * n + s];
+          if (cur != 0u) base = __ldg(&start[row_base3(by, bz, r, g) + bx - 1]);
         }
+        if (cur == 0u) break;
+        const uint32_t j = base + (uint32_t)(__ffs((int)cur) - 1);
+        cur &= cur - 1u;
+        if (j != s) pair3<MASS>(j, pi, vi, rho_i, q_i, m_i, spos, svel, sdq, smass, P, f, sm);
       }
     } else {
 #pragma unroll 1

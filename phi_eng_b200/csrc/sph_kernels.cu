@@ -271,6 +271,13 @@ __device__ __forceinline__ float density_term(float d2, float m, const StepParam
   return d2 < P.hg2 ? __fmul_rn(m, poly6(d2, P)) : 0.0f;
 }
 
+// m_j * poly6(d2) for a candidate known to be a neighbour: d2 < h*h <= hk*hk
+// and d2 >= 0 (a sum of squares), so poly6's range test always passes.
+__device__ __forceinline__ float neighbour_density_term(float d2, float m, const StepParams& P) {
+  const float t = __fsub_rn(P.hk2, d2);
+  return __fmul_rn(m, __fmul_rn(__fmul_rn(__fmul_rn(P.c_poly6, t), t), t));
+}
+
 template <bool MASS, bool PHASE, bool BATCH>
 __global__ void __launch_bounds__(256) k_density(const float2* __restrict__ spos, const uint32_t* __restrict__ skey,
                                                  const float* __restrict__ smass,
@@ -297,13 +304,16 @@ __global__ void __launch_bounds__(256) k_density(const float2* __restrict__ spos
       if (!seam) {
         const uint32_t rs = __ldg(&start[row + bx - 1]);
         const uint32_t re = __ldg(&start[row + bx + 2]);
-        uint32_t m = 0;
+        uint32_t m = 0, bit = 1u;  // bit shifts out after 32 slots (then masks_ok is false)
         for (uint32_t j = rs; j < re; j++) {
           const float2 a = __ldg(&spos[j]);
           const float dx = __fsub_rn(a.x, pi.x), dy = __fsub_rn(a.y, pi.y);
           const float d2 = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
-          rho = __fadd_rn(rho, density_term(d2, MASS ? __ldg(&smass[j]) : P.mass, P));
-          if (j - rs < kMaskBits) m |= (uint32_t)(d2 < P.hg2) << (j - rs);
+          const bool nb = d2 < P.hg2;
+          const float w = neighbour_density_term(d2, MASS ? __ldg(&smass[j]) : P.mass, P);
+          rho = nb ? __fadd_rn(rho, w) : rho;
+          m |= nb ? bit : 0u;
+          bit <<= 1;
         }
         mrow[oy] = m;
         if (re - rs > kMaskBits) masks_ok = false;
