@@ -402,6 +402,29 @@ uint32_t phieng_sph_debug_sorted(World2* world, uint32_t* ids, uint32_t* keys, u
 uint32_t phieng_sph_debug_neighbors(World2* world, uint32_t* counts, uint32_t* lists,
                                     uint32_t max_per, uint32_t max);
 
+/* ---- snapshot fluid block (crates/dynamics/src/snapshot.rs) ----
+ * The fluid section of the reference's binary world snapshot: config, then
+ * per particle position, velocity, mass and phase, little-endian, in the
+ * layout of encode_fluid2 (snapshot.rs:6478) for schema `version` (1 ..
+ * PHIENG_SNAPSHOT_SCHEMA; schema 5 and later carry the EOS / CFL / phase
+ * fields). A host that writes or reads world snapshots splices this block
+ * where the reference's encode_world2 / decode place the fluid. */
+#define PHIENG_SNAPSHOT_SCHEMA 17u
+
+/* Encode the world's fluid. Returns the block size in bytes and writes it to
+ * out when out is not null and cap >= the size; -1 for a null world, a batch
+ * or an unknown version. */
+int64_t phieng_sph_fluid_block_save(World2* world, uint32_t version, uint8_t* out, uint64_t cap);
+/* Replace the world's fluid config and particles by a decoded block with the
+ * rules of the reference's load (apply_fluid2, snapshot.rs:4471): finite
+ * config scalars and particle values, at most the particle cap (4096 by
+ * default), a single phase resets the phase tables, mass = stored mass if
+ * positive else particle_mass, density = rest_density and pressure = 0 until
+ * the next step. Continuing to step after a save and a load is bit-identical
+ * to never having saved. Returns the bytes consumed; -1 for null / bad
+ * version; -2 for a malformed block (the world is then unchanged). */
+int64_t phieng_sph_fluid_block_load(World2* world, uint32_t version, const uint8_t* data, uint64_t len);
+
 /* ======================================================================
  * 3D SPH world (crates/dynamics/src/fluid3.rs behind ffi.rs:3199-3885).
  * The fluid step of World3 with static sphere / box / capsule walls; the
@@ -488,6 +511,11 @@ uint32_t phieng_world3_fluid_add_phase(World3* world, const float* positions, co
 uint32_t phieng_world3_fluid_count(const World3* world);
 int32_t phieng_world3_fluid_clear(World3* world);
 uint32_t phieng_world3_fluid_get(const World3* world, float* out, uint32_t max);
+
+/* The 3D fluid block (encode_fluid3 / apply_fluid3, snapshot.rs:6662,
+ * :4545): as the 2D one with z components. */
+int64_t phieng_sph3_fluid_block_save(World3* world, uint32_t version, uint8_t* out, uint64_t cap);
+int64_t phieng_sph3_fluid_block_load(World3* world, uint32_t version, const uint8_t* data, uint64_t len);
 
 /* ---- 3D extensions (no reference counterpart) ---- */
 

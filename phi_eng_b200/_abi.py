@@ -19,6 +19,7 @@ SHAPE3_SPHERE = 0
 SHAPE3_BOX = 1
 SHAPE3_CAPSULE = 2
 MAX_PARTICLES_3D = 4096
+SNAPSHOT_SCHEMA = 17
 
 OK = 0
 E_NO_DEVICE = 1
@@ -246,6 +247,10 @@ SIGNATURES = {
     "phieng_sph_debug_forces": (C.c_uint32, [_P, _F, C.c_uint32]),
     "phieng_sph_debug_sorted": (C.c_uint32, [_P, _U32P, _U32P, C.c_uint32]),
     "phieng_sph_debug_neighbors": (C.c_uint32, [_P, _U32P, _U32P, C.c_uint32, C.c_uint32]),
+    "phieng_sph_fluid_block_save": (C.c_int64, [_P, C.c_uint32, _U8P, C.c_uint64]),
+    "phieng_sph_fluid_block_load": (C.c_int64, [_P, C.c_uint32, _U8P, C.c_uint64]),
+    "phieng_sph3_fluid_block_save": (C.c_int64, [_P, C.c_uint32, _U8P, C.c_uint64]),
+    "phieng_sph3_fluid_block_load": (C.c_int64, [_P, C.c_uint32, _U8P, C.c_uint64]),
     "phieng_world3_new": (_P, []),
     "phieng_world3_free": (None, [_P]),
     "phieng_world3_step": (None, [_P, C.c_float]),

@@ -28,6 +28,7 @@
 #include "../../include/phieng_sph.h"
 #include "sph_host.h"
 #include "sph_kernels.h"
+#include "sph_snapshot.h"
 #include "sph_warp.cuh"
 
 using namespace phieng;
@@ -1165,6 +1166,50 @@ uint32_t phieng_world3_fluid_get(const World3* cw, float* out, uint32_t max) {
     o[0] = p.x, o[1] = p.y, o[2] = p.z, o[3] = v.x, o[4] = v.y, o[5] = v.z;
   }
   return n;
+}
+
+int64_t phieng_sph3_fluid_block_save(World3* w, uint32_t version, uint8_t* out, uint64_t cap) {
+  if (!w || version == 0 || version > snap::kSchemaLatest) return -1;
+  if (w->n && !ensure_host3(w)) return -1;
+  std::vector<snap::Particle> ps(w->n);
+  for (uint32_t i = 0; i < w->n; i++) {
+    const float4 p = w->h_pos[i], v = w->h_vel[i];
+    ps[i] = snap::Particle{p.x, p.y, p.z, v.x, v.y, v.z, w->h_mass[i], w->h_phase[i]};
+  }
+  std::vector<uint8_t> o;
+  snap::encode(o, w->cfg, ps, 3, version);
+  if (out && cap >= o.size()) std::memcpy(out, o.data(), o.size());
+  return (int64_t)o.size();
+}
+
+int64_t phieng_sph3_fluid_block_load(World3* w, uint32_t version, const uint8_t* data, uint64_t len) {
+  if (!w || !data || version == 0 || version > snap::kSchemaLatest) return -1;
+  snap::Reader r(data, len);
+  snap::Block b;
+  if (!snap::decode(r, version, 3, w->cap, b)) return -2;
+  if (w->device >= 0) cudaStreamSynchronize(w->stream);
+  w->cfg = b.cfg;
+  const uint32_t n = (uint32_t)b.particles.size();
+  w->h_pos.resize(n);
+  w->h_vel.resize(n);
+  w->h_mass.resize(n);
+  w->h_phase.resize(n);
+  w->h_dens.assign(n, b.cfg.rest_density);  // density / pressure are recomputed by the next step
+  w->h_pres.assign(n, 0.0f);
+  for (uint32_t i = 0; i < n; i++) {
+    const snap::Particle& q = b.particles[i];
+    w->h_pos[i] = make_float4(q.x, q.y, q.z, 0.0f);
+    w->h_vel[i] = make_float4(q.vx, q.vy, q.vz, 0.0f);
+    w->h_mass[i] = q.mass;
+    w->h_phase[i] = q.phase;
+  }
+  w->n = n;
+  recompute_uniformity3(w);
+  w->host_valid = true;
+  w->dp_dev = false;
+  w->dev_valid = w->aux_valid = w->plan_valid = w->keys_valid = false;
+  release_graph3(w);
+  return (int64_t)r.off;
 }
 
 // ---- extension ----

@@ -19,6 +19,7 @@
 #include "sph_kernels.h"
 #include "sph_mlp_host.h"
 #include "sph_host.h"
+#include "sph_snapshot.h"
 
 using namespace phieng;
 
@@ -846,6 +847,55 @@ int32_t phieng_world_set_fluid_config(World2* w, const FluidConfig2Ffi* cfg) {
     w->keys_valid = false;
   }
   return 1;
+}
+
+int64_t phieng_sph_fluid_block_save(World2* w, uint32_t version, uint8_t* out, uint64_t cap) {
+  if (!w || w->is_batch() || version == 0 || version > snap::kSchemaLatest) return -1;
+  if (w->n && !ensure_host_state(w)) return -1;
+  std::vector<snap::Particle> ps(w->n);
+  for (uint32_t i = 0; i < w->n; i++) {
+    const float4 q = w->h_state[i];
+    ps[i] = snap::Particle{q.x, q.y, 0.0f, q.z, q.w, 0.0f, w->h_mass[i], w->h_phase[i]};
+  }
+  std::vector<uint8_t> o;
+  snap::encode(o, w->cfg, ps, 2, version);
+  if (out && cap >= o.size()) std::memcpy(out, o.data(), o.size());
+  return (int64_t)o.size();
+}
+
+int64_t phieng_sph_fluid_block_load(World2* w, uint32_t version, const uint8_t* data, uint64_t len) {
+  if (!w || w->is_batch() || !data || version == 0 || version > snap::kSchemaLatest) return -1;
+  snap::Reader r(data, len);
+  snap::Block b;
+  if (!snap::decode(r, version, 2, w->cap, b)) return -2;
+  if (w->device >= 0) cudaStreamSynchronize(w->stream);
+  const bool regrid = b.cfg.smoothing_length != w->cfg.smoothing_length;
+  w->cfg = b.cfg;
+  const uint32_t n = (uint32_t)b.particles.size();
+  w->h_state.resize(n);
+  w->h_mass.resize(n);
+  w->h_phase.resize(n);
+  w->h_dens.assign(n, b.cfg.rest_density);  // density / pressure are recomputed by the next step
+  w->h_pres.assign(n, 0.0f);
+  for (uint32_t i = 0; i < n; i++) {
+    const snap::Particle& q = b.particles[i];
+    w->h_state[i] = make_float4(q.x, q.y, q.vx, q.vy);
+    w->h_mass[i] = q.mass;
+    w->h_phase[i] = q.phase;
+  }
+  w->n = n;
+  recompute_uniformity(w);
+  w->host_state_valid = true;
+  w->dev_state_valid = false;
+  w->dev_aux_valid = false;
+  w->dp_on_device = false;
+  if (w->plan_locked) {
+    if (regrid) w->plan.hg = b.cfg.smoothing_length;
+  } else {
+    w->plan_valid = false;
+  }
+  w->keys_valid = false;
+  return (int64_t)r.off;
 }
 
 int32_t phieng_world_get_fluid_config(World2* w, FluidConfig2Ffi* out) {

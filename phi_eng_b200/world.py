@@ -304,6 +304,26 @@ class World2:
         self.check()
         return out
 
+    def save_fluid_block(self, version: int = _abi.SNAPSHOT_SCHEMA) -> bytes:
+        """The fluid section of the reference's binary world snapshot
+        (snapshot.rs encode_fluid2) for this world's fluid."""
+        n = self._lib.phieng_sph_fluid_block_save(self._h, version, None, 0)
+        if n < 0:
+            self.check()
+            raise ValueError("fluid block save failed (version or world)")
+        buf = (C.c_uint8 * n)()
+        self._lib.phieng_sph_fluid_block_save(self._h, version, buf, n)
+        return bytes(buf)
+
+    def load_fluid_block(self, data: bytes, version: int = _abi.SNAPSHOT_SCHEMA) -> int:
+        """Replace the fluid by a snapshot fluid block (the reference's load
+        rules); returns the bytes consumed."""
+        buf = (C.c_uint8 * max(len(data), 1)).from_buffer_copy(bytes(data) or b"\0")
+        r = self._lib.phieng_sph_fluid_block_load(self._h, version, buf, len(data))
+        if r < 0:
+            raise ValueError("malformed fluid block" if r == -2 else "bad arguments")
+        return int(r)
+
     def replan(self) -> None:
         self._lib.phieng_sph_replan(self._h)
 

@@ -226,6 +226,26 @@ class World3:
         k = self._lib.phieng_sph3_phase_times(self._h, _fptr(out), 3)
         return out[:k].astype(np.float64)
 
+    def save_fluid_block(self, version: int = _abi.SNAPSHOT_SCHEMA) -> bytes:
+        """The fluid section of the reference's binary world snapshot
+        (snapshot.rs encode_fluid3) for this world's fluid."""
+        n = self._lib.phieng_sph3_fluid_block_save(self._h, version, None, 0)
+        if n < 0:
+            self.check()
+            raise ValueError("fluid block save failed (version or world)")
+        buf = (C.c_uint8 * n)()
+        self._lib.phieng_sph3_fluid_block_save(self._h, version, buf, n)
+        return bytes(buf)
+
+    def load_fluid_block(self, data: bytes, version: int = _abi.SNAPSHOT_SCHEMA) -> int:
+        """Replace the fluid by a snapshot fluid block (the reference's load
+        rules); returns the bytes consumed."""
+        buf = (C.c_uint8 * max(len(data), 1)).from_buffer_copy(bytes(data) or b"\0")
+        r = self._lib.phieng_sph3_fluid_block_load(self._h, version, buf, len(data))
+        if r < 0:
+            raise ValueError("malformed fluid block" if r == -2 else "bad arguments")
+        return int(r)
+
     def debug_forces(self):
         """(density, pressure, force [n][3]) of a density + force pass on the
         current state (no integration)."""
