@@ -402,6 +402,37 @@ uint32_t phieng_sph_debug_sorted(World2* world, uint32_t* ids, uint32_t* keys, u
 uint32_t phieng_sph_debug_neighbors(World2* world, uint32_t* counts, uint32_t* lists,
                                     uint32_t max_per, uint32_t max);
 
+/* ---- the fluid phase with the engine's rigid bodies (two-way coupling) ----
+ * A rigid body as the fluid phase sees it (RigidBody2, body.rs:560-700):
+ * shape, transform, velocity and inverse mass / inertia. 60 bytes. */
+typedef struct PhiengBody2 {
+  uint32_t shape_tag;        /* PHIENG_SHAPE_CIRCLE (a = radius) or PHIENG_SHAPE_BOX (a, b = half extents) */
+  float a, b;
+  float px, py;              /* transform.position */
+  float xax, xay, yax, yay;  /* transform.rotation columns x_axis, y_axis */
+  float vx, vy, w;           /* velocity, angular velocity: updated for dynamic bodies */
+  float inv_mass, inv_inertia;
+  uint8_t is_static;         /* statics take no reaction */
+  uint8_t is_sleeping;       /* cleared when the fluid pushes or floats the body */
+  uint8_t _pad[2];
+} PhiengBody2;
+#ifdef __cplusplus
+static_assert(sizeof(PhiengBody2) == 60, "PhiengBody2 layout");
+#endif
+
+/* FluidState2::step_fluid(bodies, gravity, ambient, time, dt) (fluid.rs:541-557),
+ * the fluid phase of World2::step_inner (world.rs:843-849): CFL substeps of
+ * the world's fluid against `bodies` in their order (in place of the world's
+ * own static bodies), with the reactions of fluid.rs:1056-1094 (impulse
+ * n * (vn * m) and the no-slip reaction on each body, applied in particle
+ * order) and the buoyancy + drag pass of fluid.rs:1103-1135 on dynamic
+ * circles and boxes; vx, vy, w and is_sleeping of `bodies` are updated in
+ * place. The ambient wind and turbulence are zero. Does not advance the
+ * world clock and does not clamp dt (the caller's World2::step does both).
+ * 1 ok; 0 for a null world, a batch, a body with an unknown shape or a
+ * non-finite field, more than 65536 bodies, or an error (phieng_sph_status). */
+int32_t phieng_sph_step_fluid(World2* world, PhiengBody2* bodies, uint32_t nbodies, float dt);
+
 /* ---- snapshot fluid block (crates/dynamics/src/snapshot.rs) ----
  * The fluid section of the reference's binary world snapshot: config, then
  * per particle position, velocity, mass and phase, little-endian, in the

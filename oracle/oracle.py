@@ -48,6 +48,7 @@ def _load():
         "orc_add_body": (None, [P, C.c_int, C.c_float, C.c_float, C.c_float, C.c_float,
                                 C.c_float, C.c_float, C.c_float, C.c_float]),
         "orc_add_particles": (C.c_uint32, [P, F, U8, C.c_uint32]),
+        "orc_step_fluid": (None, [P, C.c_void_p, C.c_uint32, C.c_float, C.c_int]),
         "orc_count": (C.c_uint32, [P]),
         "orc_clear": (None, [P]),
         "orc_set_state": (None, [P, F, C.c_uint32]),
@@ -257,6 +258,11 @@ class OracleWorld:
 
     def cfl_substeps(self, dt: float) -> int:
         return int(self._l.orc_cfl_substeps(self._h, dt))
+
+    def step_fluid(self, bodies, dt: float, mode: int = REF_SEQ) -> None:
+        """FluidState2::step_fluid with `bodies` (a ctypes PhiengBody2 array,
+        updated in place) in place of the world's bodies; no clock."""
+        self._l.orc_step_fluid(self._h, C.cast(bodies, C.c_void_p), len(bodies), dt, mode)
 
     # ---- learned-closure hooks ----
     def features(self, dt: float) -> np.ndarray:

@@ -73,6 +73,30 @@ struct Body {
   float px = 0, py = 0;
   float xax = 1, xay = 0, yax = 0, yay = 1;  // rotation columns x_axis, y_axis
   float a = 0, b = 0;
+  // RigidBody2 velocity state (body.rs:560-700): statics take no reaction
+  bool is_static = true, sleeping = false;
+  float vx = 0, vy = 0, w = 0, inv_mass = 0, inv_inertia = 0;
+
+  // apply_impulse (body.rs:675-687)
+  void apply_impulse(float jx, float jy, float qx, float qy) {
+    if (is_static) return;
+    sleeping = false;
+    vx = vx + jx * inv_mass;
+    vy = vy + jy * inv_mass;
+    float rx = qx - px, ry = qy - py;
+    float torque = rx * jy - ry * jx;
+    w = w + torque * inv_inertia;
+  }
+  // apply_force (body.rs:657-673)
+  void apply_force(float fx, float fy, float qx, float qy, float dt) {
+    if (is_static) return;
+    sleeping = false;
+    vx = vx + fx * inv_mass * dt;
+    vy = vy + fy * inv_mass * dt;
+    float rx = qx - px, ry = qy - py;
+    float torque = rx * fy - ry * fx;
+    w = w + torque * inv_inertia * dt;
+  }
 };
 
 template <class R>
@@ -411,6 +435,12 @@ class Fluid {
   // ---- particle vs static body (fluid.rs:463-533, circle + box) ----
   // Returns false when separated; else the normal and depth.
   static bool collide(R px, R py, R pr, const Body& b, R& nx, R& ny, R& depth) {
+    R qx, qy;
+    return collide_pt(px, py, pr, b, nx, ny, depth, qx, qy);
+  }
+  // ... and the contact point on the body surface (circle: position +
+  // normal * radius; box: transform_point(clamped))
+  static bool collide_pt(R px, R py, R pr, const Body& b, R& nx, R& ny, R& depth, R& qx, R& qy) {
     if (b.shape == 0) {
       R dx = px - (R)b.px;
       R dy = py - (R)b.py;
@@ -425,6 +455,8 @@ class Fluid {
         ny = 0;
       }
       depth = radius + pr - dist;
+      qx = (R)b.px + nx * radius;
+      qy = (R)b.py + ny * radius;
       return true;
     }
     R hx = (R)b.a, hy = (R)b.b;
@@ -447,6 +479,8 @@ class Fluid {
       nx = xax * lnx + yax * lny;
       ny = xay * lnx + yay * lny;
       depth = pr - dist;
+      qx = (xax * cxl + yax * cyl) + (R)b.px;
+      qy = (xay * cxl + yay * cyl) + (R)b.py;
       return true;
     }
     R dxp = hx - std::fabs(lx);
@@ -467,18 +501,21 @@ class Fluid {
     if (lny != lny) lny = std::fabs(lny);
     nx = xax * lnx + yax * lny;
     ny = xay * lnx + yay * lny;
+    qx = (xax * cxl + yax * cyl) + (R)b.px;
+    qy = (xay * cxl + yay * cyl) + (R)b.py;
     return true;
   }
 
-  // boundary pass (fluid.rs:1056-1094); statics take no impulse
-  // (body.rs:675-687), so only the particle side changes. Static walls
-  // have zero velocity, which the friction branch reads.
+  // boundary pass (fluid.rs:1056-1094): push out, remove the approach
+  // velocity, impulse n * (vn * m) on the body, then the no-slip pull toward
+  // the body's tangential velocity with its reaction -dv * m. Statics take
+  // no impulse (body.rs:675-687) and walls have zero velocity.
   void boundaries() {
     R pr = rmax((R)cfg.particle_radius, (R)0);
     for (auto& p : particles) {
-      for (const Body& b : bodies) {
-        R nx, ny, depth;
-        if (!collide(p.x, p.y, pr, b, nx, ny, depth)) continue;
+      for (Body& b : bodies) {
+        R nx, ny, depth, qx, qy;
+        if (!collide_pt(p.x, p.y, pr, b, nx, ny, depth, qx, qy)) continue;
         if (depth <= (R)0) continue;
         p.x = p.x + nx * depth;
         p.y = p.y + ny * depth;
@@ -486,10 +523,12 @@ class Fluid {
         if (vn < (R)0) {
           p.vx -= nx * vn;
           p.vy -= ny * vn;
+          if (!b.is_static) b.sleeping = false;
+          b.apply_impulse((float)(nx * (vn * p.mass)), (float)(ny * (vn * p.mass)), (float)qx, (float)qy);
           if ((R)cfg.wall_friction > (R)0) {
             R mu = rclamp((R)cfg.wall_friction, (R)0, (R)1);
             R vtx = p.vx, vty = p.vy;
-            R wvx = 0, wvy = 0;
+            R wvx = (R)b.vx, wvy = (R)b.vy;
             R wdot = wvx * nx + wvy * ny;
             R wtx = wvx - nx * wdot;
             R wty = wvy - ny * wdot;
@@ -497,10 +536,102 @@ class Fluid {
             R dvy = (wty - vty) * mu;
             p.vx += dvx;
             p.vy += dvy;
+            b.apply_impulse((float)(-dvx * p.mass), (float)(-dvy * p.mass), (float)qx, (float)qy);
           }
         }
       }
     }
+  }
+
+  // ---- buoyancy + drag (fluid.rs:388-458, :1103-1135) ----
+  // sample_pressure: p(x) = sum m_j (p_j / max(rho_j, EPS)) poly6(|x - x_j|^2)
+  // over the grid cells around floor(x / h), h = max(smoothing_length, EPS)
+  R sample_pressure(R ptx, R pty) const {
+    R h = rmax((R)cfg.smoothing_length, (R)kEps);
+    int32_t cx = sat_i32(std::floor(ptx / h)), cy = sat_i32(std::floor(pty / h));
+    R p = 0;
+    for (int oy = -1; oy <= 1; oy++)
+      for (int ox = -1; ox <= 1; ox++) {
+        int64_t xx = (int64_t)cx + ox, yy = (int64_t)cy + oy;
+        if (xx < INT32_MIN || xx > INT32_MAX || yy < INT32_MIN || yy > INT32_MAX) continue;
+        auto it = grid.find(cell_key((int32_t)xx, (int32_t)yy));
+        if (it == grid.end()) continue;
+        for (uint32_t j : it->second) {
+          const auto& pj = particles[j];
+          R dx = pj.x - ptx, dy = pj.y - pty;
+          R r2 = dx * dx + dy * dy;
+          if (r2 < h * h) p += pj.mass * (pj.pressure / rmax(pj.density, (R)kEps)) * poly6(r2, h);
+        }
+      }
+    return rmax(p, (R)0);
+  }
+  // surface_samples: circles 12 perimeter points, boxes 4 per edge
+  static void surface_samples(const Body& b, std::vector<float>& out) {  // (x, y, nx, ny, area) each
+    const float pi = Consts<float>::pi();
+    auto push = [&](float lx, float ly, float nlx, float nly, float area) {
+      out.push_back((b.xax * lx + b.yax * ly) + b.px);
+      out.push_back((b.xay * lx + b.yay * ly) + b.py);
+      out.push_back(b.xax * nlx + b.yax * nly);
+      out.push_back(b.xay * nlx + b.yay * nly);
+      out.push_back(area);
+    };
+    if (b.shape == 0) {
+      const int n = 12;
+      float area = 2.0f * pi * b.a / (float)n;
+      for (int k = 0; k < n; k++) {
+        float a = 2.0f * pi * (float)k / (float)n;
+        float c = cosf(a), sn = sinf(a);
+        push(c * b.a, sn * b.a, c, sn, area);
+      }
+    } else {
+      float hx = b.a, hy = b.b;
+      float area = 4.0f * (hx + hy) / 16.0f;
+      const float e[4][5] = {{0, -1, -hx, -hy, 1}, {0, 1, -hx, hy, 1}, {-1, 0, -hx, -hy, 0}, {1, 0, hx, -hy, 0}};
+      for (int q = 0; q < 4; q++)
+        for (int k = 0; k < 4; k++) {
+          float t = ((float)k + 0.5f) / 4.0f;
+          bool along_x = e[q][4] != 0;
+          float extent = along_x ? hx : hy;
+          float sc = 2.0f * extent * t;
+          float tx = along_x ? 1.0f : 0.0f, ty = along_x ? 0.0f : 1.0f;
+          push(e[q][2] + tx * sc, e[q][3] + ty * sc, e[q][0], e[q][1], area);
+        }
+    }
+  }
+  void buoyancy(R dt) {
+    rebuild_grid();
+    std::vector<float> smp;
+    for (Body& b : bodies) {
+      if (b.is_static) continue;
+      smp.clear();
+      surface_samples(b, smp);
+      if (smp.empty()) continue;
+      float drag = std::max(cfg.drag, 0.0f);
+      bool wet = false;
+      for (size_t q = 0; q < smp.size(); q += 5) {
+        float ptx = smp[q], pty = smp[q + 1], nx = smp[q + 2], ny = smp[q + 3], area = smp[q + 4];
+        float p = (float)sample_pressure((R)ptx, (R)pty);
+        if (p <= 0.0f) continue;
+        wet = true;
+        float rx = ptx - b.px, ry = pty - b.py;
+        float vrx = (b.vx + (-b.w * ry)) - 0.0f;
+        float vry = (b.vy + (b.w * rx)) - 0.0f;
+        float speed = std::sqrt(vrx * vrx + vry * vry);
+        float fx = -nx * (p * area), fy = -ny * (p * area);
+        if (speed > kEps) {
+          float c = drag * area * speed;
+          fx -= vrx * c;
+          fy -= vry * c;
+        }
+        b.apply_force(fx, fy, ptx, pty, (float)dt);
+      }
+      if (wet) b.sleeping = false;
+    }
+  }
+  bool any_dynamic() const {
+    for (const Body& b : bodies)
+      if (!b.is_static) return true;
+    return false;
   }
 
   // ---- CFL substeps (fluid.rs:562-588) ----
@@ -676,8 +807,17 @@ class Fluid {
     extra_ax.clear();
     extra_ay.clear();
     boundaries();
-    // The trailing rebuild_grid + buoyancy pass (fluid.rs:1102-1135) acts
-    // on dynamic bodies only and leaves particle state unchanged.
+    // the trailing rebuild_grid + buoyancy pass (fluid.rs:1102-1135) acts on
+    // dynamic bodies only and leaves the particle state unchanged
+    if (any_dynamic()) buoyancy(dt);
+  }
+
+  // FluidState2::step_fluid (fluid.rs:541-557): no clock
+  void step_fluid(R dt, Mode mode) {
+    if (!cfg.enabled || particles.empty() || dt <= (R)0) return;
+    uint32_t n = cfl_substeps(dt);
+    R sub = dt / (R)n;
+    for (uint32_t k = 0; k < n; k++) substep(sub, mode);
   }
 
   // ---- step_fluid (fluid.rs:541-557) inside World2::step (world.rs:706-732) ----

@@ -163,6 +163,44 @@ void orc_add_body(void* h, int shape, float px, float py, float a, float b, floa
   o->f64.bodies.push_back(bd);
 }
 
+// step_fluid with the caller's bodies in place of the world's (f32 oracle):
+// the bodies' velocity state is updated in place (PhiengBody2 layout).
+void orc_step_fluid(void* h, PhiengBody2* bodies, uint32_t nb, float dt, int mode) {
+  Orc* o = static_cast<Orc*>(h);
+  std::vector<oracle::Body> keep = o->f32.bodies;
+  o->f32.bodies.clear();
+  for (uint32_t k = 0; k < nb; k++) {
+    const PhiengBody2& q = bodies[k];
+    oracle::Body b;
+    b.shape = q.shape_tag == PHIENG_SHAPE_CIRCLE ? 0 : 1;
+    b.px = q.px;
+    b.py = q.py;
+    b.xax = q.xax;
+    b.xay = q.xay;
+    b.yax = q.yax;
+    b.yay = q.yay;
+    b.a = q.a;
+    b.b = q.b;
+    b.is_static = q.is_static != 0;
+    b.sleeping = q.is_sleeping != 0;
+    b.vx = q.vx;
+    b.vy = q.vy;
+    b.w = q.w;
+    b.inv_mass = q.inv_mass;
+    b.inv_inertia = q.inv_inertia;
+    o->f32.bodies.push_back(b);
+  }
+  o->f32.step_fluid(dt, (oracle::Mode)mode);
+  for (uint32_t k = 0; k < nb; k++) {
+    const oracle::Body& b = o->f32.bodies[k];
+    bodies[k].vx = b.vx;
+    bodies[k].vy = b.vy;
+    bodies[k].w = b.w;
+    bodies[k].is_sleeping = b.sleeping ? 1 : 0;
+  }
+  o->f32.bodies = keep;
+}
+
 uint32_t orc_add_particles(void* h, const float* xy, const uint8_t* phases, uint32_t n) {
   Orc* o = static_cast<Orc*>(h);
   uint32_t r = 0;

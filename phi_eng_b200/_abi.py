@@ -132,6 +132,32 @@ class BodyDesc3D(C.Structure):
 
 assert C.sizeof(BodyDesc3D) == 44
 
+class PhiengBody2(C.Structure):
+    """A rigid body as the fluid phase sees it (phieng_sph_step_fluid), 60 bytes."""
+
+    _fields_ = [
+        ("shape_tag", C.c_uint32),
+        ("a", C.c_float),
+        ("b", C.c_float),
+        ("px", C.c_float),
+        ("py", C.c_float),
+        ("xax", C.c_float),
+        ("xay", C.c_float),
+        ("yax", C.c_float),
+        ("yay", C.c_float),
+        ("vx", C.c_float),
+        ("vy", C.c_float),
+        ("w", C.c_float),
+        ("inv_mass", C.c_float),
+        ("inv_inertia", C.c_float),
+        ("is_static", C.c_uint8),
+        ("is_sleeping", C.c_uint8),
+        ("_pad", C.c_uint8 * 2),
+    ]
+
+
+assert C.sizeof(PhiengBody2) == 60
+
 # FluidConfig3Ffi (ffi.rs:744-767) has the 2D config's fields and layout.
 FluidConfig3Ffi = FluidConfig2Ffi
 
@@ -247,6 +273,7 @@ SIGNATURES = {
     "phieng_sph_debug_forces": (C.c_uint32, [_P, _F, C.c_uint32]),
     "phieng_sph_debug_sorted": (C.c_uint32, [_P, _U32P, _U32P, C.c_uint32]),
     "phieng_sph_debug_neighbors": (C.c_uint32, [_P, _U32P, _U32P, C.c_uint32, C.c_uint32]),
+    "phieng_sph_step_fluid": (C.c_int32, [_P, C.POINTER(PhiengBody2), C.c_uint32, C.c_float]),
     "phieng_sph_fluid_block_save": (C.c_int64, [_P, C.c_uint32, _U8P, C.c_uint64]),
     "phieng_sph_fluid_block_load": (C.c_int64, [_P, C.c_uint32, _U8P, C.c_uint64]),
     "phieng_sph3_fluid_block_save": (C.c_int64, [_P, C.c_uint32, _U8P, C.c_uint64]),

@@ -44,6 +44,7 @@ enum StepFlags : uint32_t {
   F_TAIT = 1u << 4,      // gamma != 1
   F_MASS = 1u << 5,      // per-particle mass array (non-uniform)
   F_PHASE = 1u << 6,     // per-particle phase array (non-uniform rest density)
+  F_DYNAMIC = 1u << 7,   // bodies with impulses or velocity: their contacts run in the ordered pass
 };
 
 struct StepParams {
@@ -98,7 +99,21 @@ struct DevBody {
   // particle farther than this plus its radius from the centre along x or
   // y cannot touch the body, so the exact test is skipped for it
   float ex, ey;
+  // 1: a contact with this body reads or changes the body's velocity (a
+  // dynamic body, or a static one given a velocity), so it is resolved in
+  // particle order by the ordered pass instead of in parallel
+  uint32_t dyn;
 };
+
+// A body's velocity state during one fluid phase (phieng_sph_step_fluid).
+struct DynBody {
+  float vx, vy, w;  // velocity, angular velocity
+  float inv_mass, inv_inertia;
+  uint32_t is_static, sleeping;
+  uint32_t sample_first, sample_count;  // buoyancy surface samples (point, normal) and areas
+};
+
+constexpr uint32_t kNoDefer = 0xFFFFFFFFu;
 
 __device__ __forceinline__ bool finitef(float v) { return isfinite(v); }
 
@@ -156,10 +171,11 @@ __device__ __forceinline__ float eos(float density, float rho0, const PP& P) {
   return fmaxf(__fmul_rn(__fmul_rn(P.stiffness, r0), __fsub_rn(pw, 1.0f)), 0.0f);
 }
 
-// Particle vs static body (fluid.rs:463-533, circle and box branches).
-// Returns false when separated.
+// Particle vs body (fluid.rs:463-533, circle and box branches). Returns
+// false when separated. With cp: the contact point on the body surface
+// (circle: position + normal * radius; box: transform_point(clamped)).
 __device__ __forceinline__ bool collide(float px, float py, float pr, const DevBody& b, float& nx,
-                                        float& ny, float& depth) {
+                                        float& ny, float& depth, float2* cp = nullptr) {
   if (b.shape == 0) {
     float dx = __fsub_rn(px, b.px);
     float dy = __fsub_rn(py, b.py);
@@ -174,6 +190,7 @@ __device__ __forceinline__ bool collide(float px, float py, float pr, const DevB
       ny = 0.0f;
     }
     depth = __fsub_rn(rr, dist);
+    if (cp) *cp = make_float2(__fadd_rn(b.px, __fmul_rn(nx, b.a)), __fadd_rn(b.py, __fmul_rn(ny, b.a)));
     return true;
   }
   float rx = __fsub_rn(px, b.px);
@@ -217,14 +234,19 @@ __device__ __forceinline__ bool collide(float px, float py, float pr, const DevB
   // glam Mat2 * Vec2 = x_axis * v.x + y_axis * v.y
   nx = __fadd_rn(__fmul_rn(b.xax, lnx), __fmul_rn(b.yax, lny));
   ny = __fadd_rn(__fmul_rn(b.xay, lnx), __fmul_rn(b.yay, lny));
+  if (cp)
+    *cp = make_float2(__fadd_rn(__fadd_rn(__fmul_rn(b.xax, cxl), __fmul_rn(b.yax, cyl)), b.px),
+                      __fadd_rn(__fadd_rn(__fmul_rn(b.xay, cxl), __fmul_rn(b.yay, cyl)), b.py));
   return true;
 }
 
 // Boundary response for one particle against every body in order
 // (fluid.rs:1056-1094). Statics take no impulse (body.rs:675-687) and have
-// zero velocity, which the no-slip branch reads.
-__device__ __forceinline__ void walls(float& x, float& y, float& vx, float& vy,
-                                      const DevBody* __restrict__ bodies, const StepParams& P) {
+// zero velocity, which the no-slip branch reads. Returns kNoDefer, or the
+// index of the first body marked dyn that the particle touches: the state is
+// then left as it was before that body, for the ordered pass to resume.
+__device__ __forceinline__ uint32_t walls(float& x, float& y, float& vx, float& vy,
+                                          const DevBody* __restrict__ bodies, const StepParams& P) {
   for (uint32_t k = 0; k < P.nbodies; k++) {
     const DevBody* bp = bodies + P.body_first + k;
     // bounding-box reject first: only the centre and the padded extents are read
@@ -234,6 +256,7 @@ __device__ __forceinline__ void walls(float& x, float& y, float& vx, float& vy,
     float nx, ny, depth;
     if (!collide(x, y, P.pr, b, nx, ny, depth)) continue;
     if (depth <= 0.0f) continue;
+    if (b.dyn) return k;
     x = __fadd_rn(x, __fmul_rn(nx, depth));
     y = __fadd_rn(y, __fmul_rn(ny, depth));
     float vn = __fadd_rn(__fmul_rn(vx, nx), __fmul_rn(vy, ny));
@@ -250,6 +273,71 @@ __device__ __forceinline__ void walls(float& x, float& y, float& vx, float& vy,
         float dvy = __fmul_rn(__fsub_rn(wty, vty), P.mu);
         vx = __fadd_rn(vx, dvx);
         vy = __fadd_rn(vy, dvy);
+      }
+    }
+  }
+  return kNoDefer;
+}
+
+// RigidBody2::apply_impulse (body.rs:675-687): statics ignore it; a
+// dynamic body wakes, v += J * inv_mass, w += (r x J) * inv_inertia.
+__device__ __forceinline__ void apply_impulse(DynBody& d, float bpx, float bpy, float jx, float jy, float qx,
+                                              float qy) {
+  if (d.is_static) return;
+  d.sleeping = 0;
+  d.vx = __fadd_rn(d.vx, __fmul_rn(jx, d.inv_mass));
+  d.vy = __fadd_rn(d.vy, __fmul_rn(jy, d.inv_mass));
+  const float rx = __fsub_rn(qx, bpx), ry = __fsub_rn(qy, bpy);
+  const float torque = __fsub_rn(__fmul_rn(rx, jy), __fmul_rn(ry, jx));
+  d.w = __fadd_rn(d.w, __fmul_rn(torque, d.inv_inertia));
+}
+
+// The full body loop of one particle from body k0 on, with the reactions on
+// the bodies (fluid.rs:1056-1094): push out, remove the approach velocity,
+// impulse n * (vn * m) on the body, then the no-slip pull toward the body's
+// tangential velocity and its reaction -dv * m. Run in particle order.
+__device__ __forceinline__ void walls_ordered(float& x, float& y, float& vx, float& vy, float m, uint32_t k0,
+                                              const DevBody* __restrict__ bodies, DynBody* __restrict__ dyn,
+                                              const StepParams& P) {
+  for (uint32_t k = k0; k < P.nbodies; k++) {
+    const DevBody b = bodies[P.body_first + k];
+    if (fabsf(x - b.px) > b.ex + P.pr_pad || fabsf(y - b.py) > b.ey + P.pr_pad) continue;
+    float nx, ny, depth;
+    float2 cp;
+    if (!collide(x, y, P.pr, b, nx, ny, depth, &cp)) continue;
+    if (depth <= 0.0f) continue;
+    x = __fadd_rn(x, __fmul_rn(nx, depth));
+    y = __fadd_rn(y, __fmul_rn(ny, depth));
+    const float vn = __fadd_rn(__fmul_rn(vx, nx), __fmul_rn(vy, ny));
+    if (vn < 0.0f) {
+      vx = __fsub_rn(vx, __fmul_rn(nx, vn));
+      vy = __fsub_rn(vy, __fmul_rn(ny, vn));
+      if (!b.dyn) {
+        // a plain wall: no reaction, zero velocity
+        if (P.flags & F_FRICTION) {
+          const float wdot = __fadd_rn(__fmul_rn(0.0f, nx), __fmul_rn(0.0f, ny));
+          const float wtx = __fsub_rn(0.0f, __fmul_rn(nx, wdot));
+          const float wty = __fsub_rn(0.0f, __fmul_rn(ny, wdot));
+          vx = __fadd_rn(vx, __fmul_rn(__fsub_rn(wtx, vx), P.mu));
+          vy = __fadd_rn(vy, __fmul_rn(__fsub_rn(wty, vy), P.mu));
+        }
+        continue;
+      }
+      DynBody& d = dyn[k];
+      if (!d.is_static) d.sleeping = 0;
+      const float vm = __fmul_rn(vn, m);
+      apply_impulse(d, b.px, b.py, __fmul_rn(nx, vm), __fmul_rn(ny, vm), cp.x, cp.y);
+      if (P.flags & F_FRICTION) {
+        const float vtx = vx, vty = vy;
+        const float wvx = d.vx, wvy = d.vy;
+        const float wdot = __fadd_rn(__fmul_rn(wvx, nx), __fmul_rn(wvy, ny));
+        const float wtx = __fsub_rn(wvx, __fmul_rn(nx, wdot));
+        const float wty = __fsub_rn(wvy, __fmul_rn(ny, wdot));
+        const float dvx = __fmul_rn(__fsub_rn(wtx, vtx), P.mu);
+        const float dvy = __fmul_rn(__fsub_rn(wty, vty), P.mu);
+        vx = __fadd_rn(vx, dvx);
+        vy = __fadd_rn(vy, dvy);
+        apply_impulse(d, b.px, b.py, __fmul_rn(-dvx, m), __fmul_rn(-dvy, m), cp.x, cp.y);
       }
     }
   }

@@ -467,7 +467,9 @@ __device__ __forceinline__ void neighbour_sums(uint32_t s, uint32_t k, uint32_t 
 __device__ __forceinline__ void integrate_write(uint32_t id, float2 pi, float2 vi, float ax, float ay, float sx,
                                                 float sy, const StepParams& P, const DevBody* __restrict__ bodies,
                                                 float4* __restrict__ state_out, uint32_t* __restrict__ key_out,
-                                                uint32_t* __restrict__ count_out) {
+                                                uint32_t* __restrict__ count_out,
+                                                uint32_t* __restrict__ defer = nullptr,
+                                                uint32_t* __restrict__ dcount = nullptr) {
   float vx = __fadd_rn(vi.x, __fmul_rn(ax, P.dt));
   float vy = __fadd_rn(vi.y, __fmul_rn(ay, P.dt));
   if (P.flags & F_VISC) {
@@ -490,8 +492,16 @@ __device__ __forceinline__ void integrate_write(uint32_t id, float2 pi, float2 v
     x = pi.x;
     y = pi.y;
   }
-  walls(x, y, vx, vy, bodies, P);
+  const uint32_t r = walls(x, y, vx, vy, bodies, P);
   state_out[id] = make_float4(x, y, vx, vy);
+  if (P.flags & F_DYNAMIC) {
+    // contacts with bodies that react run in particle order (enqueue_dynamic_walls)
+    dcount[id] = r != kNoDefer ? 1u : 0u;
+    if (r != kNoDefer) {
+      defer[id] = r;
+      return;
+    }
+  }
   const uint32_t nk = bucket_key(x, y, P.grid);
   key_out[id] = nk;
   count_key(count_out, nk);  // bucket counts of the next substep's sort
@@ -503,7 +513,8 @@ __global__ void __launch_bounds__(256) k_force_integrate(
     const uint32_t* __restrict__ skey, const uint32_t* __restrict__ sid, const float* __restrict__ smass,
     uint32_t n, const uint32_t* __restrict__ start, StepParams P0, BatchTab bt, const DevBody* __restrict__ bodies,
     const uint32_t* __restrict__ nmask, float4* __restrict__ state_out, uint32_t* __restrict__ key_out,
-    uint32_t* __restrict__ count_out, float2* __restrict__ dbg_force) {
+    uint32_t* __restrict__ count_out, float2* __restrict__ dbg_force, uint32_t* __restrict__ defer,
+    uint32_t* __restrict__ dcount) {
   const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n) return;
   const StepParams& P = scene_params<BATCH>(P0, bt.ptab, BATCH ? bt.sscene[s] : 0u);
@@ -525,7 +536,7 @@ __global__ void __launch_bounds__(256) k_force_integrate(
   }
   const float ax = __fadd_rn(P.gx, __fdiv_rn(fx, rho_i));
   const float ay = __fadd_rn(P.gy, __fdiv_rn(fy, rho_i));
-  integrate_write(id, pi, vi, ax, ay, sx, sy, P, bodies, state_out, key_out, count_out);
+  integrate_write(id, pi, vi, ax, ay, sx, sy, P, bodies, state_out, key_out, count_out, defer, dcount);
 }
 
 // ---------------------------------------------------------------- closure force pass
@@ -811,7 +822,8 @@ void enqueue_force_integrate(const FluidBufs& b, uint32_t n, const StepParams& P
   const uint32_t bs = b.block_force, g = cdiv(n, bs);
 #define PHIENG_FORCE(M, D, BT)                                                                                    \
   k_force_integrate<M, D, BT><<<g, bs, 0, st>>>(b.spos, b.svel, b.sdq, b.skey, b.sid, b.smass, n, b.start, P,   \
-                                                b.batch, b.bodies, b.nmask, b.state, b.key, b.count, dbg_force)
+                                                b.batch, b.bodies, b.nmask, b.state, b.key, b.count, dbg_force, \
+                                                b.defer, b.dcount)
   if (dbg_force) {
     if (m) PHIENG_FORCE(true, true, false);
     else PHIENG_FORCE(false, true, false);
@@ -877,6 +889,166 @@ void enqueue_closure_check(const FluidBufs& b, uint32_t n, const StepParams& P, 
     if (ph) k_closure_check<true, false><<<g, 256, 0, st>>>(b.sdq, b.sid, b.sphase, n, P, b.batch, rho_prev, out);
     else k_closure_check<false, false><<<g, 256, 0, st>>>(b.sdq, b.sid, b.sphase, n, P, b.batch, rho_prev, out);
   }
+}
+
+// ---------------------------------------------------------------- bodies that react
+// Ordered compaction of the deferred particles: list[dstart[i]] = i.
+__global__ void __launch_bounds__(256) k_compact_deferred(const uint32_t* __restrict__ dcount,
+                                                          const uint32_t* __restrict__ dstart, uint32_t n,
+                                                          uint32_t* __restrict__ list) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n && dcount[i]) list[dstart[i]] = i;
+}
+
+// The rest of the body loop of every deferred particle, one particle after
+// the other in id order (the reference's loop order: a body's velocity after
+// particle i's reactions is what particle i+1's no-slip term reads); then the
+// particle's next key and bucket count.
+__global__ void k_dynamic_walls(const uint32_t* __restrict__ list, const uint32_t* __restrict__ total,
+                                const uint32_t* __restrict__ defer, float4* __restrict__ state,
+                                const float* __restrict__ mass, uint32_t* __restrict__ key,
+                                uint32_t* __restrict__ count, const DevBody* __restrict__ bodies,
+                                DynBody* __restrict__ dyn, StepParams P) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  const uint32_t m = *total;
+  for (uint32_t t = 0; t < m; t++) {
+    const uint32_t id = list[t];
+    const float4 q = state[id];
+    float x = q.x, y = q.y, vx = q.z, vy = q.w;
+    const float mi = (P.flags & F_MASS) ? mass[id] : P.mass;
+    walls_ordered(x, y, vx, vy, mi, defer[id], bodies, dyn, P);
+    state[id] = make_float4(x, y, vx, vy);
+    const uint32_t nk = bucket_key(x, y, P.grid);
+    key[id] = nk;
+    atomicAdd(&count[nk], 1u);
+  }
+}
+
+// Sorted (density, q) and pressure to id order and back into the order of a
+// newer sort (the buoyancy pass samples the pressure on the re-sorted grid).
+__global__ void __launch_bounds__(256) k_dp_to_id(const float2* __restrict__ sdq, const float* __restrict__ spres,
+                                                  const uint32_t* __restrict__ sid, uint32_t n,
+                                                  float2* __restrict__ dq_id, float* __restrict__ p_id) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  const uint32_t id = sid[s];
+  dq_id[id] = sdq[s];
+  p_id[id] = spres[s];
+}
+
+__global__ void __launch_bounds__(256) k_dp_from_id(const float2* __restrict__ dq_id, const float* __restrict__ p_id,
+                                                    const uint32_t* __restrict__ sid, uint32_t n,
+                                                    float2* __restrict__ sdq, float* __restrict__ spres) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  const uint32_t id = sid[s];
+  sdq[s] = dq_id[id];
+  spres[s] = p_id[id];
+}
+
+// FluidState2::sample_pressure (fluid.rs:392-410) at a point over the sorted
+// grid: h = max(smoothing_length, EPS); cells oy, ox = -1..1 around
+// floor(point / h); p += m_j * (p_j / max(rho_j, EPS)) * poly6(r^2) for
+// r^2 < h*h in visit order; max(p, 0).
+__device__ float sample_pressure(float ptx, float pty, const float2* __restrict__ spos,
+                                 const float2* __restrict__ sdq, const float* __restrict__ spres,
+                                 const float* __restrict__ smass, const uint32_t* __restrict__ start,
+                                 const StepParams& P) {
+  const GridPlan& g = P.grid;
+  const int32_t cx = __float2int_rd(__fdiv_rn(ptx, P.hk));
+  const int32_t cy = __float2int_rd(__fdiv_rn(pty, P.hk));
+  float p = 0.0f;
+  for (int oy = -1; oy <= 1; oy++) {
+    const uint32_t by = ((uint32_t)cy + (uint32_t)oy - (uint32_t)g.cy0) & g.maskh;
+    for (int ox = -1; ox <= 1; ox++) {
+      const uint32_t bx = ((uint32_t)cx + (uint32_t)ox - (uint32_t)g.cx0) & g.maskw;
+      const uint32_t bb = g.base + (by << g.log2w) + bx;
+      const uint32_t e = start[bb + 1];
+      for (uint32_t j = start[bb]; j < e; j++) {
+        const float2 pj = spos[j];
+        const float dx = __fsub_rn(pj.x, ptx), dy = __fsub_rn(pj.y, pty);
+        const float r2 = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
+        if (r2 < P.hk2) {
+          const float mj = (P.flags & F_MASS) ? smass[j] : P.mass;
+          const float pr = __fdiv_rn(spres[j], fmaxf(sdq[j].x, kEps));
+          p = __fadd_rn(p, __fmul_rn(__fmul_rn(mj, pr), poly6(r2, P)));
+        }
+      }
+    }
+  }
+  return fmaxf(p, 0.0f);  // f32::max(0.0); a NaN sum gives 0
+}
+
+// Buoyancy + drag on one dynamic body (fluid.rs:1103-1135): for each surface
+// sample in order, the sampled pressure p > 0 gives the force
+// -n * (p * area) - v_rel * (drag * area * |v_rel|) (the latter when
+// |v_rel| > EPS), applied at the sample point for dt (body.rs:657-673).
+__global__ void k_buoyancy(const uint32_t* __restrict__ which, uint32_t nb, const DevBody* __restrict__ bodies,
+                           DynBody* __restrict__ dyn, const float4* __restrict__ samples,
+                           const float* __restrict__ areas, const float2* __restrict__ spos,
+                           const float2* __restrict__ sdq, const float* __restrict__ spres,
+                           const float* __restrict__ smass, const uint32_t* __restrict__ start, StepParams P,
+                           float drag, float dt) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nb) return;
+  const uint32_t k = which[t];
+  const DevBody b = bodies[P.body_first + k];
+  DynBody d = dyn[k];
+  bool wet = false;
+  for (uint32_t q = 0; q < d.sample_count; q++) {
+    const float4 sp = samples[d.sample_first + q];
+    const float area = areas[d.sample_first + q];
+    const float p = sample_pressure(sp.x, sp.y, spos, sdq, spres, smass, start, P);
+    if (p <= 0.0f) continue;
+    wet = true;
+    const float rx = __fsub_rn(sp.x, b.px), ry = __fsub_rn(sp.y, b.py);
+    // v + (-w r.y, w r.x) - wind (the ambient wind is zero here)
+    const float vrx = __fsub_rn(__fadd_rn(d.vx, __fmul_rn(-d.w, ry)), 0.0f);
+    const float vry = __fsub_rn(__fadd_rn(d.vy, __fmul_rn(d.w, rx)), 0.0f);
+    const float speed = __fsqrt_rn(__fadd_rn(__fmul_rn(vrx, vrx), __fmul_rn(vry, vry)));
+    const float pa = __fmul_rn(p, area);
+    float fx = __fmul_rn(-sp.z, pa), fy = __fmul_rn(-sp.w, pa);
+    if (speed > kEps) {
+      const float c = __fmul_rn(__fmul_rn(drag, area), speed);
+      fx = __fsub_rn(fx, __fmul_rn(vrx, c));
+      fy = __fsub_rn(fy, __fmul_rn(vry, c));
+    }
+    if (!d.is_static) {  // RigidBody2::apply_force
+      d.sleeping = 0;
+      d.vx = __fadd_rn(d.vx, __fmul_rn(__fmul_rn(fx, d.inv_mass), dt));
+      d.vy = __fadd_rn(d.vy, __fmul_rn(__fmul_rn(fy, d.inv_mass), dt));
+      const float torque = __fsub_rn(__fmul_rn(rx, fy), __fmul_rn(ry, fx));
+      d.w = __fadd_rn(d.w, __fmul_rn(__fmul_rn(torque, d.inv_inertia), dt));
+    }
+  }
+  if (wet) d.sleeping = 0;
+  dyn[k] = d;
+}
+
+void enqueue_dynamic_walls(const FluidBufs& b, const DynBufs& y, uint32_t n, const StepParams& P, cudaStream_t st) {
+  if (n == 0) return;
+  const uint32_t nt = cdiv(n + 1, kScanTile);
+  k_scan_reduce<<<nt, 256, 0, st>>>(y.dcount, y.dtile, nt, y.done);
+  k_scan_down<<<nt, 256, 0, st>>>(y.dcount, y.dtile, n + 1, y.dstart);
+  k_compact_deferred<<<cdiv(n, 256), 256, 0, st>>>(y.dcount, y.dstart, n, y.list);
+  k_dynamic_walls<<<1, 32, 0, st>>>(y.list, y.dstart + n, b.defer, b.state, b.mass, b.key, b.count, b.bodies, y.dyn,
+                                    P);
+}
+
+void enqueue_buoyancy(const FluidBufs& b, const DynBufs& y, uint32_t n, const StepParams& P, float drag, float dt,
+                      cudaStream_t st) {
+  if (n == 0 || y.nbuoy == 0) return;
+  // the density pass's values by id, the grid rebuilt on the new positions
+  // (from a copy of the bucket counts, which the next substep's sort needs),
+  // the values gathered into the new order, then the sampling
+  k_dp_to_id<<<cdiv(n, 256), 256, 0, st>>>(b.sdq, b.spres, b.sid, n, y.dq_id, y.p_id);
+  cudaMemcpyAsync(y.count2, b.count, sizeof(uint32_t) * b.count_len, cudaMemcpyDeviceToDevice, st);
+  FluidBufs b2 = b;
+  b2.count = y.count2;
+  enqueue_sort_and_ranges(b2, n, P, true, st);
+  k_dp_from_id<<<cdiv(n, 256), 256, 0, st>>>(y.dq_id, y.p_id, b.sid, n, b.sdq, b.spres);
+  k_buoyancy<<<cdiv(y.nbuoy, 32), 32, 0, st>>>(y.buoy, y.nbuoy, b.bodies, y.dyn, y.samples, y.areas, b.spos, b.sdq,
+                                               b.spres, b.smass, b.start, P, drag, dt);
 }
 
 void enqueue_unsort_dp(const FluidBufs& b, uint32_t n, float* dens, float* pres, cudaStream_t st) {

@@ -47,6 +47,10 @@ struct FluidBufs {
   BatchTab batch;
   DevBody* bodies = nullptr;
   uint32_t bodies_cap = 0;
+  // bodies that react (F_DYNAMIC): per id, the body index the ordered pass
+  // resumes from, and 1 / 0 = deferred or not (padded to a scan tile)
+  uint32_t* defer = nullptr;
+  uint32_t* dcount = nullptr;
   unsigned int* scalar = nullptr;  // small device scratch (vmax etc.)
   // launch shapes (autotuned; results do not depend on them)
   uint32_t block_density = 256;  // threads per block of K5: 64, 128 or 256
@@ -118,6 +122,33 @@ void enqueue_closure_force(const FluidBufs& b, uint32_t n, const StepParams& P, 
 // (relative to the rest density, float bits).
 void enqueue_closure_check(const FluidBufs& b, uint32_t n, const StepParams& P, const float* rho_prev,
                            unsigned int* out, cudaStream_t st);
+
+// Device buffers of a fluid phase with bodies that react (phieng_sph_step_fluid).
+struct DynBufs {
+  DynBody* dyn = nullptr;        // [bodies] velocity state, updated in place
+  float4* samples = nullptr;     // buoyancy surface samples: point (x, y), outward normal (z, w)
+  float* areas = nullptr;        // their areas
+  uint32_t* buoy = nullptr;      // indices of the dynamic bodies with samples
+  uint32_t nbuoy = 0;
+  uint32_t* dcount = nullptr;    // = FluidBufs::dcount
+  uint32_t* dstart = nullptr;    // exclusive prefix of dcount; dstart[n] = deferred count
+  uint32_t* dtile = nullptr;     // scan tile sums
+  uint32_t* done = nullptr;      // scan blocks finished (zero between scans)
+  uint32_t* list = nullptr;      // deferred ids in id order
+  float2* dq_id = nullptr;       // density pass values by id
+  float* p_id = nullptr;
+  uint32_t* count2 = nullptr;    // copy of the bucket counts for the buoyancy sort
+};
+
+// After K6 with F_DYNAMIC: finish the body loop of the deferred particles in
+// particle order with the bodies' reactions, and their keys / counts.
+void enqueue_dynamic_walls(const FluidBufs& b, const DynBufs& y, uint32_t n, const StepParams& P, cudaStream_t st);
+
+// Buoyancy + drag of the dynamic bodies (fluid.rs:1103-1135): re-sort on the
+// new positions, then each body's samples in order. Leaves the sorted arrays
+// and the density-pass values in the new order and the bucket counts intact.
+void enqueue_buoyancy(const FluidBufs& b, const DynBufs& y, uint32_t n, const StepParams& P, float drag, float dt,
+                      cudaStream_t st);
 
 // Scatter the sorted density / pressure back to id order.
 void enqueue_unsort_dp(const FluidBufs& b, uint32_t n, float* dens, float* pres, cudaStream_t st);

@@ -108,6 +108,11 @@ struct World2 {
   cudaGraphExec_t cexec = nullptr;
   std::string csig;
 
+  // bodies of the last phieng_sph_step_fluid call and their buffers
+  DynBufs dynb;
+  DevBody* d_cbodies = nullptr;
+  uint32_t cbody_cap = 0, sample_cap = 0, dyn_pcap = 0, count2_cap = 0;
+
   // launch tuning (phieng_sph_set_tuning)
   float buckets_per_particle = 2.0f;
 };
@@ -617,6 +622,226 @@ bool world_step(World2* w, float dt) {
 }
 
 
+// ---------------------------------------------------------------- bodies that react
+// FluidState2::step_fluid (fluid.rs:541-557) with the caller's bodies: the
+// fluid phase of World2::step_inner (world.rs:843-849), where the engine
+// passes its rigid bodies and keeps the updated velocities.
+constexpr uint32_t kMaxCallBodies = 65536;
+
+bool ensure_dyn_buffers(World2* w, uint32_t nb, uint32_t ns) {
+  DynBufs& y = w->dynb;
+  if (nb > w->cbody_cap) {
+    cudaStreamSynchronize(w->stream);
+    dfree(w->d_cbodies), dfree(y.dyn), dfree(y.buoy);
+    const uint32_t c = std::max<uint32_t>(16, nb);
+    if (!dalloc(w, w->d_cbodies, c) || !dalloc(w, y.dyn, c) || !dalloc(w, y.buoy, c)) return false;
+    w->cbody_cap = c;
+  }
+  if (ns > w->sample_cap) {
+    cudaStreamSynchronize(w->stream);
+    dfree(y.samples), dfree(y.areas);
+    const uint32_t c = std::max<uint32_t>(64, ns);
+    if (!dalloc(w, y.samples, c) || !dalloc(w, y.areas, c)) return false;
+    w->sample_cap = c;
+  }
+  if (w->n > w->dyn_pcap || !w->d.defer) {
+    cudaStreamSynchronize(w->stream);
+    dfree(w->d.defer), dfree(w->d.dcount), dfree(y.dstart), dfree(y.dtile), dfree(y.list), dfree(y.dq_id),
+        dfree(y.p_id);
+    const uint32_t c = std::max<uint32_t>(1024, w->n);
+    const uint32_t tiles = (c + 1 + kBucketScanTile - 1) / kBucketScanTile;
+    const size_t len = (size_t)tiles * kBucketScanTile;
+    if (!dalloc(w, w->d.defer, c) || !dalloc(w, w->d.dcount, len) || !dalloc(w, y.dstart, len + 1) ||
+        !dalloc(w, y.dtile, tiles) || !dalloc(w, y.list, c) || !dalloc(w, y.dq_id, c) || !dalloc(w, y.p_id, c))
+      return false;
+    w->dyn_pcap = c;
+  }
+  if (w->d.count_len > w->count2_cap) {
+    cudaStreamSynchronize(w->stream);
+    dfree(y.count2);
+    if (!dalloc(w, y.count2, w->d.count_len)) return false;
+    w->count2_cap = w->d.count_len;
+  }
+  y.dcount = w->d.dcount;
+  y.done = w->d.scalar + 10;
+  return true;
+}
+
+// Surface samples of a dynamic body for buoyancy (fluid.rs:417-458): circles
+// 12 perimeter points, boxes 4 per edge; (point, outward normal) in world
+// axes and the sample's area. The angles' cosines and sines come from the C
+// library, as f32::cos / f32::sin do.
+void surface_samples(const PhiengBody2& b, std::vector<float4>& pts, std::vector<float>& areas) {
+  const float pi = 3.14159265358979323846f;
+  auto rot = [&](float x, float y, float& ox, float& oy) {  // glam Mat2 * Vec2
+    ox = b.xax * x + b.yax * y;
+    oy = b.xay * x + b.yay * y;
+  };
+  if (b.shape_tag == PHIENG_SHAPE_CIRCLE) {
+    const int n = 12;
+    const float r = b.a;
+    const float area = 2.0f * pi * r / (float)n;
+    for (int k = 0; k < n; k++) {
+      const float a = 2.0f * pi * (float)k / (float)n;
+      const float c = std::cos(a), sn = std::sin(a);
+      float qx, qy, nx, ny;
+      rot(c * r, sn * r, qx, qy);
+      rot(c, sn, nx, ny);
+      pts.push_back(make_float4(qx + b.px, qy + b.py, nx, ny));
+      areas.push_back(area);
+    }
+  } else if (b.shape_tag == PHIENG_SHAPE_BOX) {
+    const float hx = b.a, hy = b.b;
+    const float perimeter = 4.0f * (hx + hy);
+    const float area = perimeter / 16.0f;
+    struct Edge {
+      float nx, ny, ox, oy;
+      bool along_x;
+    };
+    const Edge edges[4] = {{0.0f, -1.0f, -hx, -hy, true},
+                           {0.0f, 1.0f, -hx, hy, true},
+                           {-1.0f, 0.0f, -hx, -hy, false},
+                           {1.0f, 0.0f, hx, -hy, false}};
+    for (const Edge& e : edges) {
+      for (int k = 0; k < 4; k++) {
+        const float t = ((float)k + 0.5f) / 4.0f;
+        const float extent = e.along_x ? hx : hy;
+        const float sc = 2.0f * extent * t;
+        const float tx = e.along_x ? 1.0f : 0.0f, ty = e.along_x ? 0.0f : 1.0f;  // Vec2::X / Vec2::Y
+        const float lx = e.ox + tx * sc, ly = e.oy + ty * sc;
+        float qx, qy, nx, ny;
+        rot(lx, ly, qx, qy);
+        rot(e.nx, e.ny, nx, ny);
+        pts.push_back(make_float4(qx + b.px, qy + b.py, nx, ny));
+        areas.push_back(area);
+      }
+    }
+  }
+}
+
+bool body_valid(const PhiengBody2& b) {
+  if (b.shape_tag != PHIENG_SHAPE_CIRCLE && b.shape_tag != PHIENG_SHAPE_BOX) return false;
+  const float v[] = {b.a, b.b, b.px, b.py, b.xax, b.xay, b.yax, b.yay, b.vx, b.vy, b.w, b.inv_mass, b.inv_inertia};
+  for (float x : v)
+    if (!std::isfinite(x)) return false;
+  return b.a > 0.0f && (b.shape_tag == PHIENG_SHAPE_CIRCLE || b.b > 0.0f);
+}
+
+DevBody dev_body(const PhiengBody2& b) {
+  DevBody d;
+  std::memset(&d, 0, sizeof(d));
+  d.shape = b.shape_tag == PHIENG_SHAPE_CIRCLE ? 0 : 1;
+  d.px = b.px;
+  d.py = b.py;
+  d.xax = b.xax;
+  d.xay = b.xay;
+  d.yax = b.yax;
+  d.yay = b.yay;
+  d.a = b.a;
+  d.b = b.b;
+  if (d.shape == 0) {
+    d.ex = d.ey = b.a * 1.001f + 1e-30f;
+  } else {
+    // the box test maps rel to x_axis.x*rel.x + y_axis.x*rel.y, ... (fluid.rs:483-489),
+    // i.e. the box sits at R^T: both candidate extents for a rotation, none
+    // for a matrix that is not one
+    const float det = b.xax * b.yay - b.yax * b.xay;
+    const float c0 = b.xax * b.xax + b.xay * b.xay, c1 = b.yax * b.yax + b.yay * b.yay;
+    if (std::fabs(det - 1.0f) > 1e-3f || std::fabs(c0 - 1.0f) > 1e-3f || std::fabs(c1 - 1.0f) > 1e-3f) {
+      d.ex = d.ey = INFINITY;
+    } else {
+      const float ax = std::fabs(b.xax), ay = std::fabs(b.xay), bx = std::fabs(b.yax), by = std::fabs(b.yay);
+      d.ex = std::max(ax * b.a + bx * b.b, ax * b.a + ay * b.b) * 1.001f + 1e-30f;
+      d.ey = std::max(ay * b.a + by * b.b, bx * b.a + by * b.b) * 1.001f + 1e-30f;
+    }
+  }
+  d.dyn = (!b.is_static || b.vx != 0.0f || b.vy != 0.0f) ? 1u : 0u;
+  return d;
+}
+
+bool step_fluid_bodies(World2* w, PhiengBody2* bodies, uint32_t nb, float dt) {
+  if (!w->cfg.enabled || w->n == 0 || dt <= 0.0f) return true;  // step_fluid guards (fluid.rs:550-552)
+  if (unsupported(w)) return false;
+  if (!prepare(w)) return false;
+  std::vector<DevBody> db(nb);
+  std::vector<DynBody> dy(nb);
+  std::vector<float4> pts;
+  std::vector<float> areas;
+  std::vector<uint32_t> buoy;
+  bool any_dyn = false;
+  for (uint32_t k = 0; k < nb; k++) {
+    const PhiengBody2& b = bodies[k];
+    db[k] = dev_body(b);
+    any_dyn = any_dyn || db[k].dyn;
+    DynBody& d = dy[k];
+    d.vx = b.vx;
+    d.vy = b.vy;
+    d.w = b.w;
+    d.inv_mass = b.inv_mass;
+    d.inv_inertia = b.inv_inertia;
+    d.is_static = b.is_static ? 1u : 0u;
+    d.sleeping = b.is_sleeping ? 1u : 0u;
+    d.sample_first = (uint32_t)pts.size();
+    if (!b.is_static) surface_samples(b, pts, areas);
+    d.sample_count = (uint32_t)pts.size() - d.sample_first;
+    if (d.sample_count) buoy.push_back(k);
+  }
+  if (!ensure_dyn_buffers(w, nb, (uint32_t)pts.size())) return false;
+  DynBufs y = w->dynb;
+  y.nbuoy = (uint32_t)buoy.size();
+  cudaStream_t st = w->stream;
+  if (nb && (!cuda_ok(w, cudaMemcpyAsync(w->d_cbodies, db.data(), sizeof(DevBody) * nb, cudaMemcpyHostToDevice, st),
+                      "upload bodies") ||
+             !cuda_ok(w, cudaMemcpyAsync(y.dyn, dy.data(), sizeof(DynBody) * nb, cudaMemcpyHostToDevice, st),
+                      "upload body state") ||
+             !cuda_ok(w, cudaMemcpyAsync(y.buoy, buoy.data(), 4 * buoy.size(), cudaMemcpyHostToDevice, st),
+                      "upload body list")))
+    return false;
+  if (!pts.empty() &&
+      (!cuda_ok(w, cudaMemcpyAsync(y.samples, pts.data(), sizeof(float4) * pts.size(), cudaMemcpyHostToDevice, st),
+                "upload samples") ||
+       !cuda_ok(w, cudaMemcpyAsync(y.areas, areas.data(), 4 * areas.size(), cudaMemcpyHostToDevice, st),
+                "upload sample areas")))
+    return false;
+  uint32_t ns = 1;
+  if (!cfl_substeps(w, dt, &ns)) return false;
+  const float sub = dt / (float)ns;
+  StepParams P = make_params_for(w->cfg, w->gx, w->gy, w->mass_uniform, w->mass_value, w->phase_uniform,
+                                 w->phase_value, w->plan, 0, nb, sub);
+  if (any_dyn) P.flags |= F_DYNAMIC;
+  FluidBufs dB = w->d;
+  dB.bodies = w->d_cbodies;
+  const float drag = rmaxf(w->cfg.drag, 0.0f);
+  const size_t dlen = (size_t)((w->n + 1 + kBucketScanTile - 1) / kBucketScanTile) * kBucketScanTile;
+  for (uint32_t k = 0; k < ns; k++) {
+    enqueue_sort_and_ranges(dB, w->n, P, w->sid_perm_n == w->n, st);
+    w->sid_perm_n = w->n;
+    enqueue_density(dB, w->n, P, st);
+    if (any_dyn) cudaMemsetAsync(dB.dcount, 0, sizeof(uint32_t) * dlen, st);
+    enqueue_force_integrate(dB, w->n, P, nullptr, st);
+    if (any_dyn) enqueue_dynamic_walls(dB, y, w->n, P, st);
+    if (y.nbuoy) enqueue_buoyancy(dB, y, w->n, P, drag, sub, st);
+    w->substeps++;
+  }
+  if (!cuda_ok(w, cudaGetLastError(), "step_fluid")) return false;
+  w->host_state_valid = false;
+  w->dp_on_device = true;
+  w->keys_valid = true;
+  if (nb) {
+    if (!cuda_ok(w, cudaMemcpyAsync(dy.data(), y.dyn, sizeof(DynBody) * nb, cudaMemcpyDeviceToHost, st),
+                 "download body state") ||
+        !cuda_ok(w, cudaStreamSynchronize(st), "sync"))
+      return false;
+    for (uint32_t k = 0; k < nb; k++) {
+      bodies[k].vx = dy[k].vx;
+      bodies[k].vy = dy[k].vy;
+      bodies[k].w = dy[k].w;
+      bodies[k].is_sleeping = dy[k].sleeping ? 1 : 0;
+    }
+  }
+  return true;
+}
+
 // ---------------------------------------------------------------- learned closure
 bool ensure_closure_buffers(World2* w) {
   if (w->closure_cap >= w->d.cap && w->d_save) return true;
@@ -742,6 +967,19 @@ void phieng_world_free(World2* w) {
     dfree(w->d_ptab);
     dfree(w->d_save);
     dfree(w->d_rho_prev);
+    dfree(w->d_cbodies);
+    dfree(w->dynb.dyn);
+    dfree(w->dynb.samples);
+    dfree(w->dynb.areas);
+    dfree(w->dynb.buoy);
+    dfree(w->d.defer);
+    dfree(w->d.dcount);
+    dfree(w->dynb.dstart);
+    dfree(w->dynb.dtile);
+    dfree(w->dynb.list);
+    dfree(w->dynb.dq_id);
+    dfree(w->dynb.p_id);
+    dfree(w->dynb.count2);
     if (w->cexec) cudaGraphExecDestroy(w->cexec);
     for (auto& e : w->ev)
       if (e) cudaEventDestroy(e);
@@ -830,6 +1068,13 @@ uint32_t phieng_world_add_bodies(World2* w, const BodyDesc2D* descs, uint32_t n,
     if (out_ids[i] >= 0) added++;
   }
   return added;
+}
+
+int32_t phieng_sph_step_fluid(World2* w, PhiengBody2* bodies, uint32_t nbodies, float dt) {
+  if (!w || w->is_batch() || (nbodies && !bodies) || nbodies > kMaxCallBodies) return 0;
+  for (uint32_t k = 0; k < nbodies; k++)
+    if (!body_valid(bodies[k])) return 0;
+  return step_fluid_bodies(w, bodies, nbodies, dt) ? 1 : 0;
 }
 
 int32_t phieng_world_set_fluid_config(World2* w, const FluidConfig2Ffi* cfg) {
