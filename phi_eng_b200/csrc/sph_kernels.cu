@@ -892,12 +892,13 @@ void enqueue_closure_check(const FluidBufs& b, uint32_t n, const StepParams& P, 
 }
 
 // ---------------------------------------------------------------- bodies that react
-// Ordered compaction of the deferred particles: list[dstart[i]] = i.
-__global__ void __launch_bounds__(256) k_compact_deferred(const uint32_t* __restrict__ dcount,
-                                                          const uint32_t* __restrict__ dstart, uint32_t n,
+// Ordered compaction of the deferred particles: list[dstart[i]] = i for
+// every i whose flag was 1 (the scan turned the flags into their exclusive
+// prefix, so a flag shows as a step between dstart[i] and dstart[i + 1]).
+__global__ void __launch_bounds__(256) k_compact_deferred(const uint32_t* __restrict__ dstart, uint32_t n,
                                                           uint32_t* __restrict__ list) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n && dcount[i]) list[dstart[i]] = i;
+  if (i < n && dstart[i + 1] != dstart[i]) list[dstart[i]] = i;
 }
 
 // The rest of the body loop of every deferred particle, one particle after
@@ -1030,7 +1031,7 @@ void enqueue_dynamic_walls(const FluidBufs& b, const DynBufs& y, uint32_t n, con
   const uint32_t nt = cdiv(n + 1, kScanTile);
   k_scan_reduce<<<nt, 256, 0, st>>>(y.dcount, y.dtile, nt, y.done);
   k_scan_down<<<nt, 256, 0, st>>>(y.dcount, y.dtile, n + 1, y.dstart);
-  k_compact_deferred<<<cdiv(n, 256), 256, 0, st>>>(y.dcount, y.dstart, n, y.list);
+  k_compact_deferred<<<cdiv(n, 256), 256, 0, st>>>(y.dstart, n, y.list);
   k_dynamic_walls<<<1, 32, 0, st>>>(y.list, y.dstart + n, b.defer, b.state, b.mass, b.key, b.count, b.bodies, y.dyn,
                                     P);
 }
