@@ -273,7 +273,7 @@ __device__ __forceinline__ uint32_t row_base3(uint32_t by, uint32_t bz, int r, c
 // Density + EOS (fluid3.rs:639-658) in sorted order; per-row neighbour masks
 // (bit t of nmask[r * n + s]: slot row_start + t is a neighbour). A zero mask
 // for the particle's own row (r = 4) means no masks (seam or > 32 slots).
-template <bool MASS, bool PHASE>
+template <bool MASS, bool PHASE, bool WIDE>
 __global__ void __launch_bounds__(256) k_density3(const float4* __restrict__ spos, const uint32_t* __restrict__ skey,
                                                   const float* __restrict__ smass, const uint8_t* __restrict__ sphase,
                                                   uint32_t n, const uint32_t* __restrict__ start, StepParams3 P,
@@ -301,9 +301,7 @@ __global__ void __launch_bounds__(256) k_density3(const float4* __restrict__ spo
           const float dx = __fsub_rn(a.x, pi.x), dy = __fsub_rn(a.y, pi.y), dz = __fsub_rn(a.z, pi.z);
           const float d2 = dot3(dx, dy, dz, dx, dy, dz);
           const bool nb = d2 < P.hg2;
-          const float t = __fsub_rn(P.hk2, d2);  // poly6 without its range test: 0 <= d2 < h*h <= hk*hk
-          const float w = __fmul_rn(MASS ? __ldg(&smass[j]) : P.mass,
-                                    __fmul_rn(__fmul_rn(__fmul_rn(P.c_poly6, t), t), t));
+          const float w = __fmul_rn(MASS ? __ldg(&smass[j]) : P.mass, poly6_nb<WIDE>(d2, P));
           rho = nb ? __fadd_rn(rho, w) : rho;
           m |= nb ? bit : 0u;
           bit <<= 1;
@@ -434,12 +432,15 @@ __global__ void __launch_bounds__(256) k_force3(const float4* __restrict__ spos,
         while (cur == 0u && r < 8) {
           r++;
           cur = nmask[(size_t)r * n + s];
-          if (cur != 0u) base = __ldg(&start[row_base3(by, bz, r, g) + bx - 1]);
+          if (cur != 0u) {
+            base = __ldg(&start[row_base3(by, bz, r, g) + bx - 1]);
+            if (r == 4) cur &= ~(1u << (s - base));  // the particle's own bit: j != i
+          }
         }
         if (cur == 0u) break;
         const uint32_t j = base + (uint32_t)(__ffs((int)cur) - 1);
         cur &= cur - 1u;
-        if (j != s) pair3<MASS>(j, pi, vi, rho_i, q_i, m_i, spos, svel, sdq, smass, P, f, sm);
+        pair3<MASS>(j, pi, vi, rho_i, q_i, m_i, spos, svel, sdq, smass, P, f, sm);
       }
     } else {
 #pragma unroll 1
@@ -828,6 +829,7 @@ StepParams3 make_params3(const World3* w, float dt) {
   if (c.gamma != 1.0f) f |= F_TAIT;
   if (!w->mass_uniform) f |= F_MASS;
   if (!w->phase_uniform) f |= F_PHASE;
+  if (!(P.hg2 <= P.hk2)) f |= F_WIDE_NB;
   P.flags = f;
   P.nbodies = (uint32_t)w->bodies.size();
   P.uniform_phase = w->phase_value;
@@ -855,8 +857,16 @@ void enqueue_sort3(World3* w, const StepParams3& P, cudaStream_t st) {
 void enqueue_density3(World3* w, const StepParams3& P, cudaStream_t st) {
   const bool m = (P.flags & F_MASS) != 0, ph = (P.flags & F_PHASE) != 0;
   const uint32_t g = cdiv(w->n, 256);
-#define PHIENG_D3(M, PH) \
-  k_density3<M, PH><<<g, 256, 0, st>>>(w->spos, w->skey, w->smass, w->sphase, w->n, w->start, P, w->sdq, w->spres, w->nmask)
+  const bool wide = (P.flags & F_WIDE_NB) != 0;
+#define PHIENG_D3(M, PH)                                                                                     \
+  do {                                                                                                       \
+    if (wide)                                                                                                \
+      k_density3<M, PH, true><<<g, 256, 0, st>>>(w->spos, w->skey, w->smass, w->sphase, w->n, w->start, P,  \
+                                                 w->sdq, w->spres, w->nmask);                                \
+    else                                                                                                     \
+      k_density3<M, PH, false><<<g, 256, 0, st>>>(w->spos, w->skey, w->smass, w->sphase, w->n, w->start, P, \
+                                                  w->sdq, w->spres, w->nmask);                               \
+  } while (0)
   if (m && ph) PHIENG_D3(true, true);
   else if (m) PHIENG_D3(true, false);
   else if (ph) PHIENG_D3(false, true);

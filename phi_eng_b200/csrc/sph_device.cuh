@@ -45,6 +45,7 @@ enum StepFlags : uint32_t {
   F_MASS = 1u << 5,      // per-particle mass array (non-uniform)
   F_PHASE = 1u << 6,     // per-particle phase array (non-uniform rest density)
   F_DYNAMIC = 1u << 7,   // bodies with impulses or velocity: their contacts run in the ordered pass
+  F_WIDE_NB = 1u << 8,   // h*h > max(h, EPS)^2 (h <= 0 from a snapshot): poly6 keeps its range test for neighbours
 };
 
 struct StepParams {
@@ -137,6 +138,15 @@ __device__ __forceinline__ uint32_t bucket_key(float x, float y, const GridPlan&
 __device__ __forceinline__ float poly6(float r2, const StepParams& P) {
   if (r2 >= P.hk2 || r2 < 0.0f) return 0.0f;
   float t = __fsub_rn(P.hk2, r2);
+  return __fmul_rn(__fmul_rn(__fmul_rn(P.c_poly6, t), t), t);
+}
+
+// poly6 of a neighbour (d2 < h*h, d2 >= 0 as a sum of squares): unless WIDE
+// (h*h > hk*hk, F_WIDE_NB) the range test always passes and is skipped.
+template <bool WIDE, class PP>
+__device__ __forceinline__ float poly6_nb(float d2, const PP& P) {
+  if (WIDE && (d2 >= P.hk2 || d2 < 0.0f)) return 0.0f;
+  const float t = __fsub_rn(P.hk2, d2);
   return __fmul_rn(__fmul_rn(__fmul_rn(P.c_poly6, t), t), t);
 }
 

@@ -271,14 +271,13 @@ __device__ __forceinline__ float density_term(float d2, float m, const StepParam
   return d2 < P.hg2 ? __fmul_rn(m, poly6(d2, P)) : 0.0f;
 }
 
-// m_j * poly6(d2) for a candidate known to be a neighbour: d2 < h*h <= hk*hk
-// and d2 >= 0 (a sum of squares), so poly6's range test always passes.
+// m_j * poly6(d2) for a candidate known to be a neighbour (poly6_nb).
+template <bool WIDE>
 __device__ __forceinline__ float neighbour_density_term(float d2, float m, const StepParams& P) {
-  const float t = __fsub_rn(P.hk2, d2);
-  return __fmul_rn(m, __fmul_rn(__fmul_rn(__fmul_rn(P.c_poly6, t), t), t));
+  return __fmul_rn(m, poly6_nb<WIDE>(d2, P));
 }
 
-template <bool MASS, bool PHASE, bool BATCH>
+template <bool MASS, bool PHASE, bool BATCH, bool WIDE>
 __global__ void __launch_bounds__(256) k_density(const float2* __restrict__ spos, const uint32_t* __restrict__ skey,
                                                  const float* __restrict__ smass,
                                                  const uint8_t* __restrict__ sphase, uint32_t n,
@@ -310,7 +309,7 @@ __global__ void __launch_bounds__(256) k_density(const float2* __restrict__ spos
           const float dx = __fsub_rn(a.x, pi.x), dy = __fsub_rn(a.y, pi.y);
           const float d2 = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
           const bool nb = d2 < P.hg2;
-          const float w = neighbour_density_term(d2, MASS ? __ldg(&smass[j]) : P.mass, P);
+          const float w = neighbour_density_term<WIDE>(d2, MASS ? __ldg(&smass[j]) : P.mass, P);
           rho = nb ? __fadd_rn(rho, w) : rho;
           m |= nb ? bit : 0u;
           bit <<= 1;
@@ -435,19 +434,21 @@ __device__ __forceinline__ void neighbour_sums(uint32_t s, uint32_t k, uint32_t 
     const uint32_t rs1 = __ldg(&start[g.base + ((by & g.maskh) << g.log2w) + bx - 1]);
     const uint32_t rs2 = __ldg(&start[g.base + (((by + 1u) & g.maskh) << g.log2w) + bx - 1]);
     const uint32_t m0 = nmask[s], m2 = nmask[2 * (size_t)n + s];
+    // the particle's own bit (its slot in its own row, < 32 when the masks
+    // are valid) is cleared: j != i (fluid.rs:947-950)
+    const uint32_t own_nb = own & ~(1u << (s - rs1));
     uint32_t cur = m0;
     uint32_t row = 0, base = rs0;
     for (;;) {
       while (cur == 0u && row < 2) {
         row++;
-        cur = row == 1 ? own : m2;
+        cur = row == 1 ? own_nb : m2;
         base = row == 1 ? rs1 : rs2;
       }
       if (cur == 0u) break;
       const uint32_t j = base + (uint32_t)(__ffs((int)cur) - 1);
       cur &= cur - 1u;
-      if (j != s)
-        pair_terms<MASS, FEAT>(j, pi, vi, rho_i, q_i, m_i, spos, svel, sdq, smass, P, fx, fy, sx, sy, fa);
+      pair_terms<MASS, FEAT>(j, pi, vi, rho_i, q_i, m_i, spos, svel, sdq, smass, P, fx, fy, sx, sy, fa);
     }
   } else {
     for_each_candidate(k, start, g, [&](int jj) {
@@ -797,21 +798,30 @@ void enqueue_sort_and_ranges(const FluidBufs& b, uint32_t n, const StepParams& P
 void enqueue_density(const FluidBufs& b, uint32_t n, const StepParams& P, cudaStream_t st) {
   if (n == 0) return;
   const bool m = (P.flags & F_MASS) != 0, ph = (P.flags & F_PHASE) != 0, bat = b.batch.ptab != nullptr;
+  const bool wide = (P.flags & F_WIDE_NB) != 0;  // h <= 0, which only a snapshot can carry
   const uint32_t bs = b.block_density, g = cdiv(n, bs);
-#define PHIENG_DENSITY(M, PH, BT)                                                                           \
-  k_density<M, PH, BT><<<g, bs, 0, st>>>(b.spos, b.skey, b.smass, b.sphase, n, b.start, P, b.batch, b.sdq, \
-                                         b.spres, b.nmask)
+#define PHIENG_DENSITY(M, PH, BT, WD)                                                                          \
+  k_density<M, PH, BT, WD><<<g, bs, 0, st>>>(b.spos, b.skey, b.smass, b.sphase, n, b.start, P, b.batch, b.sdq, \
+                                             b.spres, b.nmask)
+#define PHIENG_DENSITY_W(M, PH, BT)       \
+  do {                                    \
+    if (wide)                             \
+      PHIENG_DENSITY(M, PH, BT, true);    \
+    else                                  \
+      PHIENG_DENSITY(M, PH, BT, false);   \
+  } while (0)
   if (bat) {
-    if (m && ph) PHIENG_DENSITY(true, true, true);
-    else if (m) PHIENG_DENSITY(true, false, true);
-    else if (ph) PHIENG_DENSITY(false, true, true);
-    else PHIENG_DENSITY(false, false, true);
+    if (m && ph) PHIENG_DENSITY_W(true, true, true);
+    else if (m) PHIENG_DENSITY_W(true, false, true);
+    else if (ph) PHIENG_DENSITY_W(false, true, true);
+    else PHIENG_DENSITY_W(false, false, true);
   } else {
-    if (m && ph) PHIENG_DENSITY(true, true, false);
-    else if (m) PHIENG_DENSITY(true, false, false);
-    else if (ph) PHIENG_DENSITY(false, true, false);
-    else PHIENG_DENSITY(false, false, false);
+    if (m && ph) PHIENG_DENSITY_W(true, true, false);
+    else if (m) PHIENG_DENSITY_W(true, false, false);
+    else if (ph) PHIENG_DENSITY_W(false, true, false);
+    else PHIENG_DENSITY_W(false, false, false);
   }
+#undef PHIENG_DENSITY_W
 #undef PHIENG_DENSITY
 }
 

@@ -469,6 +469,7 @@ StepParams make_params_for(const FluidConfig2Ffi& c, float gx, float gy, bool ma
   if (c.gamma != 1.0f) f |= F_TAIT;
   if (!mass_uniform) f |= F_MASS;
   if (!phase_uniform) f |= F_PHASE;
+  if (!(P.hg2 <= P.hk2)) f |= F_WIDE_NB;
   P.flags = f;
   P.nbodies = nbodies;
   P.body_first = body_first;
@@ -487,6 +488,8 @@ StepParams make_params(const World2* w, float dt) {
   for (const auto& sc : w->scenes) {
     if (!sc.mass_uniform) P.flags |= F_MASS;
     if (!sc.phase_uniform) P.flags |= F_PHASE;
+    const float hg = sc.cfg.smoothing_length, hk = rmaxf(hg, kEps);
+    if (!(hg * hg <= hk * hk)) P.flags |= F_WIDE_NB;
   }
   return P;
 }

@@ -318,3 +318,32 @@ def test_continuation_after_reload_3d(lib):
     assert (a.view(np.uint32) == b.view(np.uint32)).all()
     lib.phieng_world3_free(w)
     lib.phieng_world3_free(w2)
+
+
+@pytest.mark.gpu
+def test_negative_smoothing_length_from_a_block(lib):
+    """A block may carry h <= 0 (the load checks finiteness only). The
+    kernels then keep poly6's range test for neighbours (h*h > max(h, EPS)^2);
+    the step stays bit-exact with the oracle fed the same config."""
+    from oracle.oracle import JACOBI, OracleWorld
+
+    w = world2(lib, grid_pts(6, 4))
+    data = bytearray(save(lib, w))
+    struct.pack_into("<f", data, 8, -0.5)  # smoothing_length
+    w2 = lib.phieng_world_new()
+    lib.phieng_world_add_body(w2, 0.0, -1.0, _abi.SHAPE_BOX, 10.0, 0.5, 1.0, 1, 0.5, 0.0)
+    assert load(lib, w2, bytes(data)) == len(data)
+    cfg = _abi.FluidConfig2Ffi()
+    lib.phieng_world_get_fluid_config(w2, C.byref(cfg))
+    assert cfg.smoothing_length == -0.5
+    o = OracleWorld()
+    o.set_config(cfg)
+    o.add_box(0.0, -1.0, 10.0, 0.5)
+    o.add_particles(grid_pts(6, 4))
+    for _ in range(20):
+        o.step(1 / 60, JACOBI)
+        lib.phieng_world_step(w2, 1 / 60)
+    a, b = o.state(), state2(lib, w2)
+    assert (a.view(np.uint32) == b.view(np.uint32)).all()
+    lib.phieng_world_free(w)
+    lib.phieng_world_free(w2)
