@@ -291,10 +291,17 @@ __global__ void __launch_bounds__(256) k_density3(const float4* __restrict__ spo
       // the three x cells of each row are consecutive buckets: one slot range
       bool masked = true;
       uint32_t m_own = 0;
-#pragma unroll 1
+      // the rows' slot ranges, loaded up front
+      uint32_t rsa[9], rea[9];
+#pragma unroll
       for (int r = 0; r < 9; r++) {
         const uint32_t row = row_base3(by, bz, r, g);
-        const uint32_t rs = __ldg(&start[row + bx - 1]), re = __ldg(&start[row + bx + 2]);
+        rsa[r] = __ldg(&start[row + bx - 1]);
+        rea[r] = __ldg(&start[row + bx + 2]);
+      }
+#pragma unroll
+      for (int r = 0; r < 9; r++) {
+        const uint32_t rs = rsa[r], re = rea[r];
         uint32_t m = 0, bit = 1u;  // bit shifts out after 32 slots (then masked is false)
         for (uint32_t j = rs; j < re; j++) {
           const float4 a = __ldg(&spos[j]);
@@ -424,18 +431,29 @@ __global__ void __launch_bounds__(256) k_force3(const float4* __restrict__ spos,
   if (k != g.sentinel) {
     const uint32_t bx = k & g.maskw, by = (k >> g.log2w) & g.maskh, bz = k >> (g.log2w + g.log2h);
     if (nmask[4 * (size_t)n + s] != 0u) {
-      // one loop over the nine rows' set bits (ascending slots, row by row), so
-      // a warp runs as many pair iterations as its busiest lane has neighbours
-      uint32_t cur = 0u, base = 0u;
-      int r = -1;
+      // the nine rows' masks and first slots, loaded up front (independent
+      // loads; none inside the divergent row advance below)
+      uint32_t mk[9], bs[9];
+#pragma unroll
+      for (int r = 0; r < 9; r++) {
+        mk[r] = nmask[(size_t)r * n + s];
+        bs[r] = __ldg(&start[row_base3(by, bz, r, g) + bx - 1]);
+      }
+      mk[4] &= ~(1u << (s - bs[4]));  // the particle's own bit: j != i
+      // one loop over the set bits of all rows (ascending slots, row by row),
+      // so a warp runs as many pair iterations as its busiest lane has
+      // neighbours
+      uint32_t cur = mk[0], base = bs[0];
+      int r = 0;
       for (;;) {
         while (cur == 0u && r < 8) {
           r++;
-          cur = nmask[(size_t)r * n + s];
-          if (cur != 0u) {
-            base = __ldg(&start[row_base3(by, bz, r, g) + bx - 1]);
-            if (r == 4) cur &= ~(1u << (s - base));  // the particle's own bit: j != i
-          }
+#pragma unroll
+          for (int t = 1; t < 9; t++)
+            if (t == r) {
+              cur = mk[t];
+              base = bs[t];
+            }
         }
         if (cur == 0u) break;
         const uint32_t j = base + (uint32_t)(__ffs((int)cur) - 1);
