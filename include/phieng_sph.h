@@ -402,6 +402,11 @@ uint32_t phieng_sph_debug_sorted(World2* world, uint32_t* ids, uint32_t* keys, u
 uint32_t phieng_sph_debug_neighbors(World2* world, uint32_t* counts, uint32_t* lists,
                                     uint32_t max_per, uint32_t max);
 
+/* Allocate the device arrays for n particles now (as std::vector::reserve),
+ * so the first step does not. 1 ok, 0 for a null world, a batch, no device
+ * or an allocation error. */
+int32_t phieng_sph_reserve(World2* world, uint32_t n);
+
 /* ---- the fluid phase with the engine's rigid bodies (two-way coupling) ----
  * A rigid body as the fluid phase sees it (RigidBody2, body.rs:560-700):
  * shape, transform, velocity and inverse mass / inertia. 60 bytes. */

@@ -273,6 +273,7 @@ SIGNATURES = {
     "phieng_sph_debug_forces": (C.c_uint32, [_P, _F, C.c_uint32]),
     "phieng_sph_debug_sorted": (C.c_uint32, [_P, _U32P, _U32P, C.c_uint32]),
     "phieng_sph_debug_neighbors": (C.c_uint32, [_P, _U32P, _U32P, C.c_uint32, C.c_uint32]),
+    "phieng_sph_reserve": (C.c_int32, [_P, C.c_uint32]),
     "phieng_sph_step_fluid": (C.c_int32, [_P, C.POINTER(PhiengBody2), C.c_uint32, C.c_float]),
     "phieng_sph_fluid_block_save": (C.c_int64, [_P, C.c_uint32, _U8P, C.c_uint64]),
     "phieng_sph_fluid_block_load": (C.c_int64, [_P, C.c_uint32, _U8P, C.c_uint64]),

@@ -351,7 +351,7 @@ __global__ void __launch_bounds__(256) k_density3(const float4* __restrict__ spo
 
 // One neighbour pair of the force loop (fluid3.rs:1040-1084) and of the XSPH
 // sum (fluid3.rs:1111-1123), accumulated in the reference's order.
-template <bool MASS>
+template <bool MASS, bool PLAIN>
 __device__ __forceinline__ void pair3(uint32_t j, float4 pi, float4 vi, float rho_i, float q_i, float m_i,
                                       const float4* __restrict__ spos, const float4* __restrict__ svel,
                                       const float2* __restrict__ sdq, const float* __restrict__ smass,
@@ -373,7 +373,7 @@ __device__ __forceinline__ void pair3(uint32_t j, float4 pi, float4 vi, float rh
     g2 = __fmul_rn(__fdiv_rn(dz, dist), sc);
   }
   float term = __fadd_rn(q_i, dqj.y);
-  if ((P.flags & F_AV) && dist > kEps) {
+  if (!PLAIN && (P.flags & F_AV) && dist > kEps) {
     const float rho_bar = __fmul_rn(0.5f, __fadd_rn(rho_i, rho_j));
     const float vd = dot3(__fsub_rn(vi.x, vj.x), __fsub_rn(vi.y, vj.y), __fsub_rn(vi.z, vj.z), dx, dy, dz);
     if (!(vd >= 0.0f)) {
@@ -386,7 +386,7 @@ __device__ __forceinline__ void pair3(uint32_t j, float4 pi, float4 vi, float rh
   f[0] = __fsub_rn(f[0], __fmul_rn(g0, mt));
   f[1] = __fsub_rn(f[1], __fmul_rn(g1, mt));
   f[2] = __fsub_rn(f[2], __fmul_rn(g2, mt));
-  if ((P.flags & F_COHESION) && dist > kEps) {
+  if (!PLAIN && (P.flags & F_COHESION) && dist > kEps) {
     const float c = dist >= P.hk ? 0.0f : __fsub_rn(1.0f, __fdiv_rn(dist, P.hk));
     if (c > 0.0f) {
       const float sc = __fmul_rn(__fmul_rn(__fmul_rn(P.surface_tension, m_i), m_j), c);
@@ -395,9 +395,9 @@ __device__ __forceinline__ void pair3(uint32_t j, float4 pi, float4 vi, float rh
       f[2] = __fsub_rn(f[2], __fmul_rn(__fdiv_rn(dz, dist), sc));
     }
   }
-  if (P.flags & F_VISC) {
+  if (PLAIN || (P.flags & F_VISC)) {
     const float rho_bar = __fmul_rn(0.5f, __fadd_rn(rho_i, rho_j));
-    const float w = poly6_3(d2, P);
+    const float w = PLAIN ? poly6_nb<false>(d2, P) : poly6_3(d2, P);
     const float mr = __fdiv_rn(m_j, rho_bar);
     sm[0] = __fadd_rn(sm[0], __fmul_rn(__fmul_rn(__fsub_rn(vj.x, vi.x), mr), w));
     sm[1] = __fadd_rn(sm[1], __fmul_rn(__fmul_rn(__fsub_rn(vj.y, vi.y), mr), w));
@@ -407,7 +407,7 @@ __device__ __forceinline__ void pair3(uint32_t j, float4 pi, float4 vi, float rh
 
 // Force + XSPH + integrate + walls (fluid3.rs:1040-1176); writes the new
 // state (id order), the next key and its bucket count. DEBUG: forces only.
-template <bool MASS, bool DEBUG>
+template <bool MASS, bool DEBUG, bool PLAIN>
 __global__ void __launch_bounds__(256) k_force3(const float4* __restrict__ spos, const float4* __restrict__ svel,
                                                 const float2* __restrict__ sdq, const uint32_t* __restrict__ skey,
                                                 const uint32_t* __restrict__ sid, const float* __restrict__ smass,
@@ -458,7 +458,7 @@ __global__ void __launch_bounds__(256) k_force3(const float4* __restrict__ spos,
         if (cur == 0u) break;
         const uint32_t j = base + (uint32_t)(__ffs((int)cur) - 1);
         cur &= cur - 1u;
-        pair3<MASS>(j, pi, vi, rho_i, q_i, m_i, spos, svel, sdq, smass, P, f, sm);
+        pair3<MASS, PLAIN>(j, pi, vi, rho_i, q_i, m_i, spos, svel, sdq, smass, P, f, sm);
       }
     } else {
 #pragma unroll 1
@@ -472,7 +472,7 @@ __global__ void __launch_bounds__(256) k_force3(const float4* __restrict__ spos,
             const float4 a = __ldg(&spos[j]);
             const float ex = __fsub_rn(a.x, pi.x), ey = __fsub_rn(a.y, pi.y), ez = __fsub_rn(a.z, pi.z);
             if (dot3(ex, ey, ez, ex, ey, ez) < P.hg2 && j != s)
-              pair3<MASS>(j, pi, vi, rho_i, q_i, m_i, spos, svel, sdq, smass, P, f, sm);
+              pair3<MASS, PLAIN>(j, pi, vi, rho_i, q_i, m_i, spos, svel, sdq, smass, P, f, sm);
           }
         }
       }
@@ -895,15 +895,21 @@ void enqueue_density3(World3* w, const StepParams3& P, cudaStream_t st) {
 void enqueue_force3(World3* w, const StepParams3& P, float4* dbg, cudaStream_t st) {
   const bool m = (P.flags & F_MASS) != 0;
   const uint32_t g = cdiv(w->n, 256);
-#define PHIENG_F3(M, D)                                                                                             \
-  k_force3<M, D><<<g, 256, 0, st>>>(w->spos, w->svel, w->sdq, w->skey, w->sid, w->smass, w->n, w->start, P,        \
-                                    w->dbodies, w->nmask, w->pos, w->vel, w->key, w->count, dbg)
+  // XSPH on, artificial viscosity and cohesion off, h*h <= hk*hk: the
+  // optional pair terms compiled out
+  const bool plain = (P.flags & F_VISC) && !(P.flags & (F_AV | F_COHESION | F_WIDE_NB));
+#define PHIENG_F3(M, D, PL)                                                                                         \
+  k_force3<M, D, PL><<<g, 256, 0, st>>>(w->spos, w->svel, w->sdq, w->skey, w->sid, w->smass, w->n, w->start, P,    \
+                                        w->dbodies, w->nmask, w->pos, w->vel, w->key, w->count, dbg)
   if (dbg) {
-    if (m) PHIENG_F3(true, true);
-    else PHIENG_F3(false, true);
+    if (m) PHIENG_F3(true, true, false);
+    else PHIENG_F3(false, true, false);
+  } else if (plain) {
+    if (m) PHIENG_F3(true, false, true);
+    else PHIENG_F3(false, false, true);
   } else {
-    if (m) PHIENG_F3(true, false);
-    else PHIENG_F3(false, false);
+    if (m) PHIENG_F3(true, false, false);
+    else PHIENG_F3(false, false, false);
   }
 #undef PHIENG_F3
 }

@@ -6,7 +6,11 @@
 
 #include <cmath>
 #include <cstdint>
+#include <cstdlib>
 #include <cstring>
+#include <new>
+
+#include <cuda_runtime.h>
 
 #include "../../include/phieng_sph.h"
 
@@ -14,6 +18,45 @@ namespace phieng {
 namespace host {
 constexpr uint32_t kMaxAddPerCall = 1000000;    // ffi.rs:2493
 constexpr float kMaxDt = 1.0f / 15.0f;          // ffi.rs:80
+
+// Page-locked host memory when a CUDA device can be used (the particle state
+// then crosses PCIe as a direct DMA, not through the driver's bounce buffer),
+// ordinary memory otherwise; a 64-byte header records which.
+template <class T>
+struct PinnedAlloc {
+  using value_type = T;
+  PinnedAlloc() = default;
+  template <class U>
+  PinnedAlloc(const PinnedAlloc<U>&) {}
+  T* allocate(size_t n) {
+    const size_t bytes = n * sizeof(T) + 64;
+    void* p = nullptr;
+    uint8_t kind = 1;
+    if (cudaHostAlloc(&p, bytes, cudaHostAllocPortable) != cudaSuccess) {
+      cudaGetLastError();
+      kind = 0;
+      p = std::malloc(bytes);
+      if (!p) throw std::bad_alloc();
+    }
+    static_cast<uint8_t*>(p)[0] = kind;
+    return reinterpret_cast<T*>(static_cast<uint8_t*>(p) + 64);
+  }
+  void deallocate(T* q, size_t) {
+    uint8_t* p = reinterpret_cast<uint8_t*>(q) - 64;
+    if (p[0] == 1)
+      cudaFreeHost(p);
+    else
+      std::free(p);
+  }
+  template <class U>
+  bool operator==(const PinnedAlloc<U>&) const {
+    return true;
+  }
+  template <class U>
+  bool operator!=(const PinnedAlloc<U>&) const {
+    return false;
+  }
+};
 
 inline float rmaxf(float a, float b) {  // f32::max: a NaN operand loses
   if (a != a) return b;

@@ -349,8 +349,10 @@ __global__ void __launch_bounds__(256) k_density(const float2* __restrict__ spos
 // ---------------------------------------------------------------- K6 force + integrate
 // One neighbour pair of the force loop (fluid.rs:947-990) and of the XSPH
 // sum (fluid.rs:1022-1033), accumulated in the reference's order. FEAT also
-// accumulates the closure network's neighbour aggregates (feat_pair).
-template <bool MASS, bool FEAT>
+// accumulates the closure network's neighbour aggregates (feat_pair). PLAIN:
+// the launch's flags are known to be XSPH on, artificial viscosity and
+// cohesion off, h*h <= hk*hk (plain_flags), so those tests are compiled out.
+template <bool MASS, bool FEAT, bool PLAIN = false>
 __device__ __forceinline__ void pair_terms(uint32_t j, float2 pi, float2 vi, float rho_i, float q_i, float m_i,
                                            const float2* __restrict__ spos, const float2* __restrict__ svel,
                                            const float2* __restrict__ sdq, const float* __restrict__ smass,
@@ -377,7 +379,7 @@ __device__ __forceinline__ void pair_terms(uint32_t j, float2 pi, float2 vi, flo
   if constexpr (FEAT)
     feat_pair(fa, gxx, gyy, poly6(d2, P), m_j, rho_j, q_i, dqj.y, __fsub_rn(vj.x, vi.x), __fsub_rn(vj.y, vi.y));
   float term = __fadd_rn(q_i, dqj.y);
-  if ((P.flags & F_AV) && dist > kEps) {
+  if (!PLAIN && (P.flags & F_AV) && dist > kEps) {
     // Monaghan term (fluid.rs:302-317, called at :963-975)
     const float rho_bar = __fmul_rn(0.5f, __fadd_rn(rho_i, rho_j));
     const float vrx = __fsub_rn(vi.x, vj.x), vry = __fsub_rn(vi.y, vj.y);
@@ -393,7 +395,7 @@ __device__ __forceinline__ void pair_terms(uint32_t j, float2 pi, float2 vi, flo
   const float mt = __fmul_rn(m_j, term);
   fx = __fsub_rn(fx, __fmul_rn(gxx, mt));
   fy = __fsub_rn(fy, __fmul_rn(gyy, mt));
-  if ((P.flags & F_COHESION) && dist > kEps) {
+  if (!PLAIN && (P.flags & F_COHESION) && dist > kEps) {
     // cohesion (fluid.rs:320-326, applied at :979-985)
     const float c = dist >= P.hk ? 0.0f : __fsub_rn(1.0f, __fdiv_rn(dist, P.hk));
     if (c > 0.0f) {
@@ -402,10 +404,10 @@ __device__ __forceinline__ void pair_terms(uint32_t j, float2 pi, float2 vi, flo
       fy = __fsub_rn(fy, __fmul_rn(__fdiv_rn(dy, dist), sc));
     }
   }
-  if (P.flags & F_VISC) {
+  if (PLAIN || (P.flags & F_VISC)) {
     // XSPH (fluid.rs:1022-1033) against pre-integrate neighbours
     const float rho_bar = __fmul_rn(0.5f, __fadd_rn(rho_i, rho_j));
-    const float w = poly6(d2, P);
+    const float w = PLAIN ? poly6_nb<false>(d2, P) : poly6(d2, P);
     const float mr = __fdiv_rn(m_j, rho_bar);
     sx = __fadd_rn(sx, __fmul_rn(__fmul_rn(__fsub_rn(vj.x, vi.x), mr), w));
     sy = __fadd_rn(sy, __fmul_rn(__fmul_rn(__fsub_rn(vj.y, vi.y), mr), w));
@@ -416,7 +418,7 @@ __device__ __forceinline__ void pair_terms(uint32_t j, float2 pi, float2 vi, flo
 // plus the closure aggregates when FEAT. The neighbour set comes from K5's
 // row masks (bits in ascending slot order = the reference's visit order);
 // particles without masks walk the candidates.
-template <bool MASS, bool FEAT>
+template <bool MASS, bool FEAT, bool PLAIN = false>
 __device__ __forceinline__ void neighbour_sums(uint32_t s, uint32_t k, uint32_t n, float2 pi, float2 vi, float rho_i,
                                                float q_i, float m_i, const float2* __restrict__ spos,
                                                const float2* __restrict__ svel, const float2* __restrict__ sdq,
@@ -448,7 +450,7 @@ __device__ __forceinline__ void neighbour_sums(uint32_t s, uint32_t k, uint32_t 
       if (cur == 0u) break;
       const uint32_t j = base + (uint32_t)(__ffs((int)cur) - 1);
       cur &= cur - 1u;
-      pair_terms<MASS, FEAT>(j, pi, vi, rho_i, q_i, m_i, spos, svel, sdq, smass, P, fx, fy, sx, sy, fa);
+      pair_terms<MASS, FEAT, PLAIN>(j, pi, vi, rho_i, q_i, m_i, spos, svel, sdq, smass, P, fx, fy, sx, sy, fa);
     }
   } else {
     for_each_candidate(k, start, g, [&](int jj) {
@@ -458,7 +460,7 @@ __device__ __forceinline__ void neighbour_sums(uint32_t s, uint32_t k, uint32_t 
       const float ey = __fsub_rn(pj.y, pi.y);
       const float d2 = __fadd_rn(__fmul_rn(ex, ex), __fmul_rn(ey, ey));
       if (d2 < P.hg2 && j != s)
-        pair_terms<MASS, FEAT>(j, pi, vi, rho_i, q_i, m_i, spos, svel, sdq, smass, P, fx, fy, sx, sy, fa);
+        pair_terms<MASS, FEAT, PLAIN>(j, pi, vi, rho_i, q_i, m_i, spos, svel, sdq, smass, P, fx, fy, sx, sy, fa);
     });
   }
 }
@@ -508,7 +510,7 @@ __device__ __forceinline__ void integrate_write(uint32_t id, float2 pi, float2 v
   count_key(count_out, nk);  // bucket counts of the next substep's sort
 }
 
-template <bool MASS, bool DEBUG, bool BATCH>
+template <bool MASS, bool DEBUG, bool BATCH, bool PLAIN>
 __global__ void __launch_bounds__(256) k_force_integrate(
     const float2* __restrict__ spos, const float2* __restrict__ svel, const float2* __restrict__ sdq,
     const uint32_t* __restrict__ skey, const uint32_t* __restrict__ sid, const float* __restrict__ smass,
@@ -529,7 +531,7 @@ __global__ void __launch_bounds__(256) k_force_integrate(
   const float q_i = dqi.y;  // p_i / (rho_i * rho_i)
   float fx = 0.0f, fy = 0.0f, sx = 0.0f, sy = 0.0f;
   FeatAcc fa;
-  neighbour_sums<MASS, false>(s, k, n, pi, vi, rho_i, q_i, m_i, spos, svel, sdq, smass, start, nmask, P, fx, fy, sx,
+  neighbour_sums<MASS, false, PLAIN>(s, k, n, pi, vi, rho_i, q_i, m_i, spos, svel, sdq, smass, start, nmask, P, fx, fy, sx,
                               sy, fa);
   if (DEBUG) {
     dbg_force[id] = make_float2(fx, fy);
@@ -723,23 +725,34 @@ __device__ __forceinline__ unsigned int f2ord(float f) {
 
 __global__ void __launch_bounds__(256) k_front_metrics(const float4* __restrict__ state, uint32_t n,
                                                        unsigned int* __restrict__ out) {
+  __shared__ unsigned int smx[8], smv[8];
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   unsigned int mx = 0u;  // below every ordered float
-  float mv = 0.0f;
+  float m2 = 0.0f;       // max |v|^2: sqrt is monotonic, so sqrt(max) = max(sqrt)
   for (; i < n; i += gridDim.x * blockDim.x) {
-    float4 s = state[i];
+    const float4 s = state[i];
     if (s.x == s.x) mx = max(mx, f2ord(s.x));
-    float l = __fsqrt_rn(__fadd_rn(__fmul_rn(s.z, s.z), __fmul_rn(s.w, s.w)));
-    if (l > mv) mv = l;
+    const float l2 = __fadd_rn(__fmul_rn(s.z, s.z), __fmul_rn(s.w, s.w));
+    if (l2 > m2) m2 = l2;
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
     mx = max(mx, __shfl_xor_sync(0xFFFFFFFFu, mx, o));
-    mv = fmaxf(mv, __shfl_xor_sync(0xFFFFFFFFu, mv, o));
+    m2 = fmaxf(m2, __shfl_xor_sync(0xFFFFFFFFu, m2, o));
   }
-  if ((threadIdx.x & 31) == 0) {
+  const uint32_t lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
+  if (lane == 0) {
+    smx[wid] = mx;
+    smv[wid] = __float_as_uint(m2);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (uint32_t k = 1; k < (blockDim.x >> 5); k++) {
+      mx = max(mx, smx[k]);
+      m2 = fmaxf(m2, __uint_as_float(smv[k]));
+    }
     atomicMax(&out[0], mx);
-    atomicMax(&out[1], __float_as_uint(mv));
+    atomicMax(&out[1], __float_as_uint(__fsqrt_rn(m2)));  // non-negative floats order as their bits
   }
 }
 
@@ -825,24 +838,32 @@ void enqueue_density(const FluidBufs& b, uint32_t n, const StepParams& P, cudaSt
 #undef PHIENG_DENSITY
 }
 
+// The launch's flags for which the force pass compiles out the optional pair
+// terms: XSPH on, artificial viscosity and cohesion off, h*h <= hk*hk (a
+// batch's launch parameters carry the union of its scenes' flags).
+inline bool plain_flags(uint32_t f) { return (f & F_VISC) && !(f & (F_AV | F_COHESION | F_WIDE_NB)); }
+
 void enqueue_force_integrate(const FluidBufs& b, uint32_t n, const StepParams& P, float2* dbg_force,
                              cudaStream_t st) {
   if (n == 0) return;
-  const bool m = (P.flags & F_MASS) != 0, bat = b.batch.ptab != nullptr;
+  const bool m = (P.flags & F_MASS) != 0, bat = b.batch.ptab != nullptr, plain = plain_flags(P.flags);
   const uint32_t bs = b.block_force, g = cdiv(n, bs);
-#define PHIENG_FORCE(M, D, BT)                                                                                    \
-  k_force_integrate<M, D, BT><<<g, bs, 0, st>>>(b.spos, b.svel, b.sdq, b.skey, b.sid, b.smass, n, b.start, P,   \
-                                                b.batch, b.bodies, b.nmask, b.state, b.key, b.count, dbg_force, \
-                                                b.defer, b.dcount)
+#define PHIENG_FORCE(M, D, BT, PL)                                                                                  \
+  k_force_integrate<M, D, BT, PL><<<g, bs, 0, st>>>(b.spos, b.svel, b.sdq, b.skey, b.sid, b.smass, n, b.start, P, \
+                                                    b.batch, b.bodies, b.nmask, b.state, b.key, b.count, dbg_force, \
+                                                    b.defer, b.dcount)
   if (dbg_force) {
-    if (m) PHIENG_FORCE(true, true, false);
-    else PHIENG_FORCE(false, true, false);
+    if (m) PHIENG_FORCE(true, true, false, false);
+    else PHIENG_FORCE(false, true, false, false);
   } else if (bat) {
-    if (m) PHIENG_FORCE(true, false, true);
-    else PHIENG_FORCE(false, false, true);
+    if (m) PHIENG_FORCE(true, false, true, false);
+    else PHIENG_FORCE(false, false, true, false);
+  } else if (plain) {
+    if (m) PHIENG_FORCE(true, false, false, true);
+    else PHIENG_FORCE(false, false, false, true);
   } else {
-    if (m) PHIENG_FORCE(true, false, false);
-    else PHIENG_FORCE(false, false, false);
+    if (m) PHIENG_FORCE(true, false, false, false);
+    else PHIENG_FORCE(false, false, false, false);
   }
 #undef PHIENG_FORCE
 }
@@ -1076,7 +1097,7 @@ void enqueue_debug_neighbors(const FluidBufs& b, uint32_t n, const StepParams& P
 void enqueue_front_metrics(const FluidBufs& b, uint32_t n, cudaStream_t st) {
   cudaMemsetAsync(b.scalar + 2, 0, 2 * sizeof(unsigned int), st);
   if (n == 0) return;
-  uint32_t g = min(cdiv(n, 256), 148u * 8u);
+  uint32_t g = min(cdiv(n, 256), 148u * 2u);
   k_front_metrics<<<g, 256, 0, st>>>(b.state, n, b.scalar + 2);
 }
 

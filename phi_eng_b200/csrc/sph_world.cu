@@ -38,7 +38,11 @@ struct World2 {
 
   // particles (host mirror); mass and phase are fixed at insertion
   uint32_t n = 0;
-  std::vector<float4> h_state;
+  std::vector<float4, PinnedAlloc<float4>> h_state;  // (x, y, vx, vy) by id
+  // bounding box of the finite host positions, kept while particles are
+  // added so the first grid plan needs no pass over a large state
+  bool bbox_valid = true;
+  float bx0 = INFINITY, bx1 = -INFINITY, by0 = INFINITY, by1 = -INFINITY;
   std::vector<float> h_mass;
   std::vector<uint8_t> h_phase;
   std::vector<float> h_dens, h_pres;
@@ -249,6 +253,7 @@ bool ensure_host_state(World2* w) {
     return false;
   if (!cuda_ok(w, cudaStreamSynchronize(w->stream), "sync")) return false;
   w->host_state_valid = true;
+  w->bbox_valid = false;
   return true;
 }
 
@@ -271,6 +276,9 @@ bool ensure_host_dp(World2* w) {
 // Bucket grid from the particle bounding box (host copy must be current).
 // Bucket grid covering the cells of n particles (with a margin), ~2 buckets
 // per particle at most.
+GridPlan plan_cells(int64_t x0, int64_t x1, int64_t y0, int64_t y1, uint32_t n, float hg,
+                    float buckets_per_particle);
+
 GridPlan plan_for(const float4* st, uint32_t n, float hg, float buckets_per_particle) {
   int64_t x0 = INT64_MAX, x1 = INT64_MIN, y0 = INT64_MAX, y1 = INT64_MIN;
   for (uint32_t i = 0; i < n; i++) {
@@ -282,6 +290,12 @@ GridPlan plan_for(const float4* st, uint32_t n, float hg, float buckets_per_part
     y0 = std::min<int64_t>(y0, cy);
     y1 = std::max<int64_t>(y1, cy);
   }
+  return plan_cells(x0, x1, y0, y1, n, hg, buckets_per_particle);
+}
+
+// The plan from the cell bounds of the particles (x0 > x1: none).
+GridPlan plan_cells(int64_t x0, int64_t x1, int64_t y0, int64_t y1, uint32_t n, float hg,
+                    float buckets_per_particle) {
   if (x0 > x1) x0 = x1 = y0 = y1 = 0;
   const int64_t sx = x1 - x0 + 1, sy = y1 - y0 + 1;
   const int64_t mx = std::max<int64_t>(2, sx / 8), my = std::max<int64_t>(2, sy / 8);
@@ -331,6 +345,15 @@ void plan_grid(World2* w) {
     all.base = 0;
     all.hg = w->scenes[0].cfg.smoothing_length;
     w->plan = all;
+  } else if (w->bbox_valid && w->cfg.smoothing_length > 0.0f) {
+    // floor(x / h) is monotonic in x for h > 0: the bounding box's cells
+    // bound every particle's cell
+    const float hg = w->cfg.smoothing_length;
+    if (w->n == 0 || !(w->bx0 <= w->bx1))
+      w->plan = plan_cells(1, 0, 1, 0, w->n, hg, w->buckets_per_particle);
+    else
+      w->plan = plan_cells(sat_floor_i32(w->bx0 / hg), sat_floor_i32(w->bx1 / hg), sat_floor_i32(w->by0 / hg),
+                           sat_floor_i32(w->by1 / hg), w->n, hg, w->buckets_per_particle);
   } else {
     w->plan = plan_for(w->h_state.data(), w->n, w->cfg.smoothing_length, w->buckets_per_particle);
   }
@@ -930,6 +953,10 @@ uint32_t add_particles(World2* w, const float* xy, const uint8_t* phases, uint32
     uint8_t ph = phases ? phases[i] : 0;
     uint32_t k = std::min<uint32_t>(ph, 3);
     w->h_state.push_back(make_float4(xy[2 * i], xy[2 * i + 1], 0.0f, 0.0f));
+    w->bx0 = std::min(w->bx0, xy[2 * i]);
+    w->bx1 = std::max(w->bx1, xy[2 * i]);
+    w->by0 = std::min(w->by0, xy[2 * i + 1]);
+    w->by1 = std::max(w->by1, xy[2 * i + 1]);
     w->h_dens.push_back(w->cfg.phase_rest_density[k]);
     w->h_pres.push_back(0.0f);
     w->h_mass.push_back(rmaxf(w->cfg.phase_mass[k], 0.0f));
@@ -1073,6 +1100,12 @@ uint32_t phieng_world_add_bodies(World2* w, const BodyDesc2D* descs, uint32_t n,
   return added;
 }
 
+int32_t phieng_sph_reserve(World2* w, uint32_t n) {
+  if (!w || w->is_batch()) return 0;
+  if (w->error != PHIENG_SPH_OK || !ensure_device(w)) return 0;
+  return ensure_capacity(w, std::max(n, w->n)) ? 1 : 0;
+}
+
 int32_t phieng_sph_step_fluid(World2* w, PhiengBody2* bodies, uint32_t nbodies, float dt) {
   if (!w || w->is_batch() || (nbodies && !bodies) || nbodies > kMaxCallBodies) return 0;
   for (uint32_t k = 0; k < nbodies; k++)
@@ -1128,6 +1161,7 @@ int64_t phieng_sph_fluid_block_load(World2* w, uint32_t version, const uint8_t* 
   for (uint32_t i = 0; i < n; i++) {
     const snap::Particle& q = b.particles[i];
     w->h_state[i] = make_float4(q.x, q.y, q.vx, q.vy);
+    w->bbox_valid = false;
     w->h_mass[i] = q.mass;
     w->h_phase[i] = q.phase;
   }
@@ -1172,6 +1206,9 @@ int32_t phieng_world_fluid_clear(World2* w) {
   if (w->device >= 0) cudaStreamSynchronize(w->stream);
   w->n = 0;
   w->h_state.clear();
+  w->bbox_valid = true;
+  w->bx0 = w->by0 = INFINITY;
+  w->bx1 = w->by1 = -INFINITY;
   w->h_mass.clear();
   w->h_phase.clear();
   w->h_dens.clear();
@@ -1191,7 +1228,16 @@ uint32_t phieng_world_fluid_get(const World2* cw, float* out, uint32_t max) {
   World2* w = const_cast<World2*>(cw);
   uint32_t n = std::min(max, w->n);
   if (n == 0) return 0;
-  if (!ensure_host_state(w)) return 0;
+  if (!w->host_state_valid) {
+    // straight from the device into the caller's buffer (a DMA when it is
+    // page-locked)
+    if (w->device < 0) return 0;
+    if (!cuda_ok(w, cudaMemcpyAsync(out, w->d.state, sizeof(float4) * n, cudaMemcpyDeviceToHost, w->stream),
+                 "download state") ||
+        !cuda_ok(w, cudaStreamSynchronize(w->stream), "sync"))
+      return 0;
+    return n;
+  }
   std::memcpy(out, w->h_state.data(), sizeof(float4) * n);
   return n;
 }
@@ -1261,6 +1307,7 @@ int32_t phieng_sph_set_state(World2* w, const float* xyvv, uint32_t n) {
     if (!std::isfinite(xyvv[i])) return 0;
   if (!ensure_host_state(w)) return 0;
   std::memcpy(w->h_state.data(), xyvv, sizeof(float4) * n);
+  w->bbox_valid = false;
   w->dev_state_valid = false;
   w->keys_valid = false;
   if (!w->plan_locked) w->plan_valid = false;
@@ -1647,6 +1694,7 @@ int32_t phieng_sph_batch_store(World2* b, World2* const* worlds, uint32_t count)
     const World2::Scene& sc = b->scenes[k];
     if (!ensure_host_state(dst) || !ensure_host_dp(dst)) return 0;
     std::copy(b->h_state.begin() + sc.first, b->h_state.begin() + sc.first + sc.count, dst->h_state.begin());
+    dst->bbox_valid = false;
     std::copy(b->h_dens.begin() + sc.first, b->h_dens.begin() + sc.first + sc.count, dst->h_dens.begin());
     std::copy(b->h_pres.begin() + sc.first, b->h_pres.begin() + sc.first + sc.count, dst->h_pres.begin());
     dst->dev_state_valid = false;

@@ -117,6 +117,17 @@ class FluidState2:
                 self._world.check()
         return out
 
+    def read_into(self, out: np.ndarray) -> int:
+        """phieng_world_fluid_get into a caller buffer of (>= n, 4) float32
+        (page-locked memory makes the read-back a direct DMA)."""
+        if out.dtype != np.float32 or not out.flags.c_contiguous or out.ndim != 2 or out.shape[1] != 4:
+            raise ValueError("out must be a C-contiguous (n, 4) float32 array")
+        n = min(len(self), out.shape[0])
+        k = self._lib.phieng_world_fluid_get(self._h, _fptr(out), n) if n else 0
+        if k != n:
+            self._world.check()
+        return int(k)
+
     def set_state(self, xyvv) -> None:
         a = np.ascontiguousarray(xyvv, dtype=np.float32).reshape(-1, 4)
         if self._lib.phieng_sph_set_state(self._h, _fptr(a), a.shape[0]) != 1:
@@ -198,6 +209,12 @@ class World2:
     def step(self, dt: float) -> None:
         self._lib.phieng_world_step(self._h, dt)
         self.check()
+
+    def reserve(self, n: int) -> None:
+        """Allocate the device arrays for n particles ahead of the first step."""
+        if self._lib.phieng_sph_reserve(self._h, n) != 1:
+            self.check()
+            raise SphError("phieng_sph_reserve failed")
 
     def step_n(self, dt: float, n: int) -> None:
         if self._lib.phieng_sph_step_n(self._h, dt, n) != 1:
