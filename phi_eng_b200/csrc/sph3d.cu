@@ -576,6 +576,7 @@ struct World3 {
   uint32_t *key = nullptr, *tkey = nullptr, *tid = nullptr, *skey = nullptr, *sid = nullptr, *nmask = nullptr;
   float2* sdq = nullptr;
   uint32_t *count = nullptr, *start = nullptr, *tilesum = nullptr, *scalar = nullptr;
+  unsigned long long* tstate = nullptr;  // single-pass scan tile states
   uint32_t count_len = 0, range_cap = 0;
   DevBody3* dbodies = nullptr;
   uint32_t bodies_cap = 0;
@@ -739,11 +740,15 @@ bool ensure_range3(World3* w) {
     return true;
   }
   cudaStreamSynchronize(w->stream);
-  dfree3(w->count), dfree3(w->start), dfree3(w->tilesum);
+  dfree3(w->count), dfree3(w->start), dfree3(w->tilesum), dfree3(w->tstate);
   release_graph3(w);
   const uint32_t len = tiles * kBucketScanTile;
-  if (!dalloc3(w, w->count, len) || !dalloc3(w, w->start, (size_t)len + 1) || !dalloc3(w, w->tilesum, tiles)) return false;
-  if (!ok3(w, cudaMemsetAsync(w->count, 0, sizeof(uint32_t) * len, w->stream))) return false;
+  if (!dalloc3(w, w->count, len) || !dalloc3(w, w->start, (size_t)len + 1) || !dalloc3(w, w->tilesum, tiles) ||
+      !dalloc3(w, w->tstate, tiles))
+    return false;
+  if (!ok3(w, cudaMemsetAsync(w->count, 0, sizeof(uint32_t) * len, w->stream)) ||
+      !ok3(w, cudaMemsetAsync(w->tstate, 0, sizeof(unsigned long long) * tiles, w->stream)))
+    return false;
   w->range_cap = w->plan.nbuckets;
   w->count_len = len;
   w->keys_valid = false;
@@ -858,7 +863,9 @@ void enqueue_sort3(World3* w, const StepParams3& P, cudaStream_t st) {
   BucketSort bs;
   bs.count = w->count;
   bs.tilesum = w->tilesum;
-  bs.done = w->scalar + 8;
+  bs.done = w->scalar + 8;  // scan counters [8], [9]
+  bs.tstate = w->tstate;
+  bs.err = w->scalar + 12;
   bs.start = w->start;
   bs.key = w->key;
   bs.sid_prev = w->sid;
@@ -1060,7 +1067,7 @@ void phieng_world3_free(World3* w) {
     cudaStreamSynchronize(w->stream);
     release_graph3(w);
     free_particles3(w);
-    dfree3(w->count), dfree3(w->start), dfree3(w->tilesum), dfree3(w->scalar), dfree3(w->dbodies);
+    dfree3(w->count), dfree3(w->start), dfree3(w->tilesum), dfree3(w->tstate), dfree3(w->scalar), dfree3(w->dbodies);
     for (auto& e : w->ev)
       if (e) cudaEventDestroy(e);
     if (w->h_pinned) cudaFreeHost(w->h_pinned);
@@ -1295,7 +1302,12 @@ int32_t phieng_sph3_set_stream(World3* w, void* stream) {
 
 int32_t phieng_sph3_sync(World3* w) {
   if (!w) return 0;
-  if (w->device >= 0 && !ok3(w, cudaStreamSynchronize(w->stream))) return 0;
+  if (w->device >= 0) {
+    if (!ok3(w, cudaStreamSynchronize(w->stream)) ||
+        !ok3(w, cudaMemcpy(w->h_pinned + 8, w->scalar + 12, 4, cudaMemcpyDeviceToHost)))
+      return 0;
+    if (w->h_pinned[8] != 0u && w->error == PHIENG_SPH_OK) w->error = PHIENG_SPH_E_CUDA;  // a scan wait gave up
+  }
   return w->error == PHIENG_SPH_OK ? 1 : 0;
 }
 

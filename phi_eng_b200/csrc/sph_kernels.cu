@@ -163,6 +163,115 @@ __global__ void __launch_bounds__(256) k_scan_down(uint32_t* __restrict__ count,
   }
 }
 
+// Single-pass variant of k_scan_reduce + k_scan_down (decoupled look-back,
+// Merrill & Garland, "Single-pass Parallel Prefix Scan with Decoupled
+// Look-back", 2016): tiles are taken in ticket order; each publishes its sum
+// (flag 1) at once, then walks back over its predecessors' published values
+// until it meets an inclusive prefix (flag 2), and publishes its own
+// inclusive prefix. A block only waits for tiles that took an earlier ticket,
+// so are already running; each wait is still bounded (kScanSpinLimit reads,
+// then *err = 1 and the scan goes on with a wrong prefix). The last block to
+// finish clears the tile states and counters for the next scan. ctr[0] =
+// ticket, ctr[1] = finished blocks; both zero between scans.
+constexpr uint32_t kScanSpinLimit = 1u << 22;
+constexpr unsigned long long kTileAgg = 1ull << 32, kTileIncl = 2ull << 32;
+
+__global__ void __launch_bounds__(256) k_scan_lookback(uint32_t* __restrict__ count, uint32_t ntiles,
+                                                       uint32_t* __restrict__ start,
+                                                       unsigned long long* __restrict__ tstate,
+                                                       uint32_t* __restrict__ ctr, uint32_t* __restrict__ err) {
+  __shared__ uint32_t warp_tot[8];
+  __shared__ uint32_t s_tile, s_prefix;
+  __shared__ bool s_last;
+  if (threadIdx.x == 0) s_tile = atomicAdd(&ctr[0], 1u);
+  __syncthreads();
+  const uint32_t t = s_tile;
+  const uint32_t base = t * kScanTile + threadIdx.x * 16;
+  uint4* c4 = reinterpret_cast<uint4*>(count + base);
+  uint32_t v[16];
+#pragma unroll
+  for (int r = 0; r < 4; r++) {
+    const uint4 q = c4[r];
+    v[4 * r] = q.x;
+    v[4 * r + 1] = q.y;
+    v[4 * r + 2] = q.z;
+    v[4 * r + 3] = q.w;
+  }
+  uint32_t sum = 0;
+#pragma unroll
+  for (int q = 0; q < 16; q++) sum += v[q];
+  const uint32_t incl = block_incl_scan_256(sum, warp_tot);
+  if (threadIdx.x < 32) {
+    // warp 0: publish this tile's sum, then look back 32 predecessors at a
+    // time (lane k reads tile t-1-k; tiles before 0 count as an inclusive 0)
+    const uint32_t lane = threadIdx.x;
+    uint32_t total = 0;
+    for (int k = 0; k < 8; k++) total += warp_tot[k];
+    uint32_t excl = 0;
+    if (t == 0) {
+      if (lane == 0) atomicExch(&tstate[0], kTileIncl | total);
+    } else {
+      if (lane == 0) atomicExch(&tstate[t], kTileAgg | total);
+      __syncwarp();
+      volatile unsigned long long* vs = tstate;
+      int64_t top = (int64_t)t - 1;
+      uint32_t spins = 0;
+      for (;;) {
+        const int64_t idx = top - (int64_t)lane;
+        unsigned long long sv;
+        for (;;) {
+          sv = idx >= 0 ? (unsigned long long)vs[idx] : (unsigned long long)kTileIncl;
+          if (__all_sync(0xFFFFFFFFu, (sv >> 32) != 0ull)) break;
+          if (++spins > kScanSpinLimit) {  // bounded: give up with a wrong prefix
+            if (lane == 0) atomicExch(err, 1u);
+            sv = (unsigned long long)kTileIncl;
+            break;
+          }
+        }
+        const uint32_t flag = (uint32_t)(sv >> 32);
+        const uint32_t incl_lanes = __ballot_sync(0xFFFFFFFFu, flag == 2u);
+        // lanes up to the nearest inclusive prefix (all 32 if none)
+        const uint32_t upto = incl_lanes ? (uint32_t)(__ffs((int)incl_lanes) - 1) : 31u;
+        uint32_t v = lane <= upto ? (uint32_t)sv : 0u;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+        excl += v;
+        if (incl_lanes) break;
+        top -= 32;
+      }
+      if (lane == 0) atomicExch(&tstate[t], kTileIncl | (excl + total));
+    }
+    if (lane == 0) s_prefix = excl;
+  }
+  __syncthreads();
+  uint32_t run = s_prefix + incl - sum;
+#pragma unroll
+  for (int q = 0; q < 16; q++) {
+    const uint32_t x = v[q];
+    v[q] = run;
+    run += x;
+  }
+  uint4* s4 = reinterpret_cast<uint4*>(start + base);
+#pragma unroll
+  for (int r = 0; r < 4; r++) {
+    const uint4 q = make_uint4(v[4 * r], v[4 * r + 1], v[4 * r + 2], v[4 * r + 3]);
+    c4[r] = q;
+    s4[r] = q;  // the padded tail past the last key gets the particle count: never read
+  }
+  if (threadIdx.x == 0) {
+    __threadfence();
+    s_last = atomicAdd(&ctr[1], 1u) + 1u == gridDim.x;
+  }
+  __syncthreads();
+  if (s_last) {
+    for (uint32_t i = threadIdx.x; i < ntiles; i += blockDim.x) tstate[i] = 0ull;
+    if (threadIdx.x == 0) {
+      ctr[0] = 0u;
+      ctr[1] = 0u;
+    }
+  }
+}
+
 // Slot in the bucket from the cursor. BY_SLOT walks the previous sort's
 // order (keys nearly sorted: a warp holds few runs of equal keys, so few
 // atomics); otherwise particles are taken in id order.
@@ -772,8 +881,12 @@ void enqueue_keys(const FluidBufs& b, uint32_t n, const GridPlan& g, cudaStream_
 void enqueue_bucket_place(const BucketSort& bs, uint32_t n, uint32_t m, bool by_slot, cudaStream_t st) {
   if (n == 0) return;
   const uint32_t nt = cdiv(m, kScanTile);
-  k_scan_reduce<<<nt, 256, 0, st>>>(bs.count, bs.tilesum, nt, bs.done);
-  k_scan_down<<<nt, 256, 0, st>>>(bs.count, bs.tilesum, m, bs.start);
+  if (bs.tstate) {
+    k_scan_lookback<<<nt, 256, 0, st>>>(bs.count, nt, bs.start, bs.tstate, bs.done, bs.err);
+  } else {
+    k_scan_reduce<<<nt, 256, 0, st>>>(bs.count, bs.tilesum, nt, bs.done);
+    k_scan_down<<<nt, 256, 0, st>>>(bs.count, bs.tilesum, m, bs.start);
+  }
   if (by_slot)
     k_place<true><<<cdiv(n, 256), 256, 0, st>>>(bs.key, bs.sid_prev, n, bs.count, bs.tkey, bs.tid);
   else
@@ -787,6 +900,8 @@ void enqueue_sort_and_ranges(const FluidBufs& b, uint32_t n, const StepParams& P
   bs.count = b.count;
   bs.tilesum = b.tilesum;
   bs.done = b.done;
+  bs.tstate = b.tstate;
+  bs.err = b.scan_err;
   bs.start = b.start;
   bs.key = b.key;
   bs.sid_prev = b.sid;

@@ -43,7 +43,11 @@ struct FluidBufs {
   uint32_t* start = nullptr;    // bucket b holds sorted slots [start[b], start[b+1])
   uint32_t* tilesum = nullptr;  // scan tile sums / offsets
   uint32_t range_cap = 0;       // buckets the arrays above can hold
-  uint32_t* done = nullptr;     // scan blocks finished (zero between scans)
+  uint32_t* done = nullptr;     // scan counters (two words, zero between scans)
+  // single-pass scan: per-tile (flag, value) states, zero between scans, and a
+  // sticky flag set when a look-back wait gave up (null: the two-kernel scan)
+  unsigned long long* tstate = nullptr;
+  uint32_t* scan_err = nullptr;
   BatchTab batch;
   DevBody* bodies = nullptr;
   uint32_t bodies_cap = 0;
@@ -80,6 +84,8 @@ struct BucketSort {
   uint32_t* count = nullptr;
   uint32_t* tilesum = nullptr;
   uint32_t* done = nullptr;
+  unsigned long long* tstate = nullptr;  // single-pass scan when set (see FluidBufs)
+  uint32_t* err = nullptr;
   uint32_t* start = nullptr;
   const uint32_t* key = nullptr;
   const uint32_t* sid_prev = nullptr;

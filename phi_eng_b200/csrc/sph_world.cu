@@ -140,6 +140,20 @@ bool cuda_ok(World2* w, cudaError_t r, const char* what) {
   return false;
 }
 
+// A look-back wait of the scan that gave up leaves a sticky device flag
+// (a wrong grid order): read it where the host synchronises anyway.
+bool scan_flag_ok(World2* w) {
+  if (w->device < 0 || !w->d.scalar) return true;
+  if (!cuda_ok(w, cudaMemcpyAsync(w->h_pinned + 8, w->d.scan_err, 4, cudaMemcpyDeviceToHost, w->stream), "flag") ||
+      !cuda_ok(w, cudaStreamSynchronize(w->stream), "sync"))
+    return false;
+  if (w->h_pinned[8] != 0u) {
+    set_error(w, PHIENG_SPH_E_CUDA, "bucket scan wait gave up");
+    return false;
+  }
+  return true;
+}
+
 template <class T>
 void dfree(T*& p) {
   if (p) cudaFree(p);
@@ -190,7 +204,8 @@ bool ensure_device(World2* w) {
   if (!w->user_stream) w->stream = w->own_stream;
   if (!cuda_ok(w, cudaMalloc(&w->d.scalar, 64), "cudaMalloc(scalar)")) return false;
   if (!cuda_ok(w, cudaMemset(w->d.scalar, 0, 64), "cudaMemset(scalar)")) return false;
-  w->d.done = w->d.scalar + 8;
+  w->d.done = w->d.scalar + 8;       // scan counters [8], [9]
+  w->d.scan_err = w->d.scalar + 12;  // set when a scan's look-back wait gave up
   if (!cuda_ok(w, cudaMallocHost(&w->h_pinned, 64), "cudaMallocHost")) return false;
   w->device = dev;
   return true;
@@ -252,6 +267,7 @@ bool ensure_host_state(World2* w) {
                "download state"))
     return false;
   if (!cuda_ok(w, cudaStreamSynchronize(w->stream), "sync")) return false;
+  if (!scan_flag_ok(w)) return false;
   w->host_state_valid = true;
   w->bbox_valid = false;
   return true;
@@ -375,11 +391,16 @@ bool ensure_range(World2* w) {
   dfree(d.count);
   dfree(d.start);
   dfree(d.tilesum);
+  dfree(d.tstate);
   d.range_cap = 0;
   release_graph(w);
   const uint32_t len = tiles * kBucketScanTile;
-  if (!dalloc(w, d.count, len) || !dalloc(w, d.start, (size_t)len + 1) || !dalloc(w, d.tilesum, tiles)) return false;
-  if (!cuda_ok(w, cudaMemsetAsync(d.count, 0, sizeof(uint32_t) * len, w->stream), "memset")) return false;
+  if (!dalloc(w, d.count, len) || !dalloc(w, d.start, (size_t)len + 1) || !dalloc(w, d.tilesum, tiles) ||
+      !dalloc(w, d.tstate, tiles))
+    return false;
+  if (!cuda_ok(w, cudaMemsetAsync(d.count, 0, sizeof(uint32_t) * len, w->stream), "memset") ||
+      !cuda_ok(w, cudaMemsetAsync(d.tstate, 0, sizeof(unsigned long long) * tiles, w->stream), "memset"))
+    return false;
   d.range_cap = w->plan.nbuckets;
   d.count_len = len;
   w->keys_valid = false;
@@ -991,6 +1012,7 @@ void phieng_world_free(World2* w) {
     dfree(w->d.count);
     dfree(w->d.start);
     dfree(w->d.tilesum);
+    dfree(w->d.tstate);
     dfree(w->d_tmp);
     dfree(w->d_pscene);
     dfree(w->d_sscene);
@@ -1234,7 +1256,7 @@ uint32_t phieng_world_fluid_get(const World2* cw, float* out, uint32_t max) {
     if (w->device < 0) return 0;
     if (!cuda_ok(w, cudaMemcpyAsync(out, w->d.state, sizeof(float4) * n, cudaMemcpyDeviceToHost, w->stream),
                  "download state") ||
-        !cuda_ok(w, cudaStreamSynchronize(w->stream), "sync"))
+        !cuda_ok(w, cudaStreamSynchronize(w->stream), "sync") || !scan_flag_ok(w))
       return 0;
     return n;
   }
@@ -1298,6 +1320,7 @@ int32_t phieng_sph_sync(World2* w) {
   if (!w) return 0;
   if (w->device < 0) return w->error == PHIENG_SPH_OK ? 1 : 0;
   if (!cuda_ok(w, cudaStreamSynchronize(w->stream), "sync")) return 0;
+  if (!scan_flag_ok(w)) return 0;
   return w->error == PHIENG_SPH_OK ? 1 : 0;
 }
 
