@@ -391,6 +391,13 @@ int32_t phieng_sph_closure_step(World2* world, float dt_fine, uint32_t coarse_st
  * Returns the number written. */
 uint32_t phieng_sph_debug_forces(World2* world, float* fxy, uint32_t max);
 
+/* Run one bucket scan in which the first tile never publishes its prefix
+ * (the grid must span at least two scan tiles): the other tiles' bounded
+ * look-back waits run out, the device flag is set and read back, and the
+ * world reports PHIENG_SPH_E_CUDA. Returns 1 if no wait ran out (then the
+ * bound failed to trigger), 0 otherwise. Test hook for the bounded waits. */
+int32_t phieng_sph_debug_scan_timeout(World2* world);
+
 /* Rebuild the grid from the current state and write the sorted order:
  * ids[s] = particle id at sorted slot s, keys[s] = its bucket key (either may
  * be null). Returns n. */

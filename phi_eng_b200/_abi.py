@@ -271,6 +271,7 @@ SIGNATURES = {
     "phieng_sph_set_closure": (C.c_int32, [_P, _P, C.c_uint32, C.c_float, C.c_uint32]),
     "phieng_sph_closure_step": (C.c_int32, [_P, C.c_float, C.c_uint32, C.POINTER(PhiengClosureStats)]),
     "phieng_sph_debug_forces": (C.c_uint32, [_P, _F, C.c_uint32]),
+    "phieng_sph_debug_scan_timeout": (C.c_int32, [_P]),
     "phieng_sph_debug_sorted": (C.c_uint32, [_P, _U32P, _U32P, C.c_uint32]),
     "phieng_sph_debug_neighbors": (C.c_uint32, [_P, _U32P, _U32P, C.c_uint32, C.c_uint32]),
     "phieng_sph_reserve": (C.c_int32, [_P, C.c_uint32]),

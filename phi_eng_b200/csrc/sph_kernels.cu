@@ -172,14 +172,17 @@ __global__ void __launch_bounds__(256) k_scan_down(uint32_t* __restrict__ count,
 // so are already running; each wait is still bounded (kScanSpinLimit reads,
 // then *err = 1 and the scan goes on with a wrong prefix). The last block to
 // finish clears the tile states and counters for the next scan. ctr[0] =
-// ticket, ctr[1] = finished blocks; both zero between scans.
-constexpr uint32_t kScanSpinLimit = 1u << 22;
+// ticket, ctr[1] = finished blocks; both zero between scans. The tile whose
+// ticket equals silent publishes nothing (a test of the bounded waits; the
+// step passes 0xFFFFFFFF).
+constexpr uint32_t kScanSpinLimit = 1u << 20;
 constexpr unsigned long long kTileAgg = 1ull << 32, kTileIncl = 2ull << 32;
 
 __global__ void __launch_bounds__(256) k_scan_lookback(uint32_t* __restrict__ count, uint32_t ntiles,
                                                        uint32_t* __restrict__ start,
                                                        unsigned long long* __restrict__ tstate,
-                                                       uint32_t* __restrict__ ctr, uint32_t* __restrict__ err) {
+                                                       uint32_t* __restrict__ ctr, uint32_t* __restrict__ err,
+                                                       uint32_t silent) {
   __shared__ uint32_t warp_tot[8];
   __shared__ uint32_t s_tile, s_prefix;
   __shared__ bool s_last;
@@ -209,9 +212,9 @@ __global__ void __launch_bounds__(256) k_scan_lookback(uint32_t* __restrict__ co
     for (int k = 0; k < 8; k++) total += warp_tot[k];
     uint32_t excl = 0;
     if (t == 0) {
-      if (lane == 0) atomicExch(&tstate[0], kTileIncl | total);
+      if (lane == 0 && t != silent) atomicExch(&tstate[0], kTileIncl | total);
     } else {
-      if (lane == 0) atomicExch(&tstate[t], kTileAgg | total);
+      if (lane == 0 && t != silent) atomicExch(&tstate[t], kTileAgg | total);
       __syncwarp();
       volatile unsigned long long* vs = tstate;
       int64_t top = (int64_t)t - 1;
@@ -239,7 +242,7 @@ __global__ void __launch_bounds__(256) k_scan_lookback(uint32_t* __restrict__ co
         if (incl_lanes) break;
         top -= 32;
       }
-      if (lane == 0) atomicExch(&tstate[t], kTileIncl | (excl + total));
+      if (lane == 0 && t != silent) atomicExch(&tstate[t], kTileIncl | (excl + total));
     }
     if (lane == 0) s_prefix = excl;
   }
@@ -882,7 +885,7 @@ void enqueue_bucket_place(const BucketSort& bs, uint32_t n, uint32_t m, bool by_
   if (n == 0) return;
   const uint32_t nt = cdiv(m, kScanTile);
   if (bs.tstate) {
-    k_scan_lookback<<<nt, 256, 0, st>>>(bs.count, nt, bs.start, bs.tstate, bs.done, bs.err);
+    k_scan_lookback<<<nt, 256, 0, st>>>(bs.count, nt, bs.start, bs.tstate, bs.done, bs.err, 0xFFFFFFFFu);
   } else {
     k_scan_reduce<<<nt, 256, 0, st>>>(bs.count, bs.tilesum, nt, bs.done);
     k_scan_down<<<nt, 256, 0, st>>>(bs.count, bs.tilesum, m, bs.start);
@@ -1196,6 +1199,12 @@ void enqueue_buoyancy(const FluidBufs& b, const DynBufs& y, uint32_t n, const St
   k_dp_from_id<<<cdiv(n, 256), 256, 0, st>>>(y.dq_id, y.p_id, b.sid, n, b.sdq, b.spres);
   k_buoyancy<<<cdiv(y.nbuoy, 32), 32, 0, st>>>(y.buoy, y.nbuoy, b.bodies, y.dyn, y.samples, y.areas, b.spos, b.sdq,
                                                b.spres, b.smass, b.start, P, drag, dt);
+}
+
+void enqueue_scan_silent_tile(const FluidBufs& b, uint32_t m, cudaStream_t st) {
+  const uint32_t nt = cdiv(m, kScanTile);
+  if (!b.tstate || nt < 2) return;
+  k_scan_lookback<<<nt, 256, 0, st>>>(b.count, nt, b.start, b.tstate, b.done, b.scan_err, 0u);
 }
 
 void enqueue_unsort_dp(const FluidBufs& b, uint32_t n, float* dens, float* pres, cudaStream_t st) {

@@ -156,6 +156,11 @@ void enqueue_dynamic_walls(const FluidBufs& b, const DynBufs& y, uint32_t n, con
 void enqueue_buoyancy(const FluidBufs& b, const DynBufs& y, uint32_t n, const StepParams& P, float drag, float dt,
                       cudaStream_t st);
 
+// One bucket scan in which tile 0 never publishes its prefix: every other
+// tile's look-back wait runs out, sets b.scan_err and ends (the test of the
+// bounded waits). Leaves the bucket ranges wrong.
+void enqueue_scan_silent_tile(const FluidBufs& b, uint32_t m, cudaStream_t st);
+
 // Scatter the sorted density / pressure back to id order.
 void enqueue_unsort_dp(const FluidBufs& b, uint32_t n, float* dens, float* pres, cudaStream_t st);
 

@@ -1587,6 +1587,16 @@ int32_t phieng_sph_closure_step(World2* w, float dt_fine, uint32_t coarse_steps,
   return cuda_ok(w, cudaGetLastError(), "closure step") ? 1 : 0;
 }
 
+int32_t phieng_sph_debug_scan_timeout(World2* w) {
+  if (!w || !prepare(w)) return 0;
+  const uint32_t m = w->plan.sentinel + 1;
+  if ((m + kBucketScanTile - 1) / kBucketScanTile < 2) return 0;
+  enqueue_scan_silent_tile(w->d, m, w->stream);
+  if (!cuda_ok(w, cudaGetLastError(), "scan")) return 0;
+  w->keys_valid = false;  // the counts became cursors
+  return scan_flag_ok(w) ? 1 : 0;
+}
+
 uint32_t phieng_sph_debug_sorted(World2* w, uint32_t* ids, uint32_t* keys, uint32_t max) {
   if (!w || w->n == 0 || w->is_batch()) return 0;
   if (!ensure_host_dp(w)) return 0;  // the re-sort below invalidates the sorted density
