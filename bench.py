@@ -54,7 +54,8 @@ DENSITY_BYTES = 36
 FORCE_BYTES = 64
 # DRAM bytes (read + write) of one launch of the named phase's kernel, from
 # the ncu capture summarised in profiles/<kernel>_<workload>.md.
-PROFILED_TRAFFIC = {("dam_break_1m", "force_integrate"): 48.330752e6 + 2.260992e6}
+PROFILED_TRAFFIC = {("dam_break_1m", "force_integrate"): 48.333312e6 + 1.921792e6}
+PROFILED_TRAFFIC_3D = {"force_integrate": 85.545216e6 + 14.838528e6}  # 100^3 3D dam break
 KERNELS_PER_STEP = 6  # scan reduce, scan down, place, fixup, density, force
 
 
@@ -383,7 +384,8 @@ def fluid3d_line(steps: int, warmup: int, side: int = 100) -> dict:
                         "tank (floor + 4 walls), FluidConfig3 defaults, dt = 1/60",
             "phases_ms": {nm: float(v) for nm, v in zip(names, ph)}, "buckets": int(buckets),
             "roofline": {"bound": "hbm", "kernel": names[top], "bytes_per_particle": bytes_pp[top],
-                         "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak},
+                         "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": PROFILED_TRAFFIC_3D.get(names[top]) if side == 100 else None},
             "finite": bool(np.isfinite(s).all()),
             "cpu_baseline": {"value": 4096 * k / secs, "unit": METRIC, "cores": 1, "kind": "port",
                              "sample": f"{k} in-place steps of a 4096-particle 3D dam break (the reference's cap)"}}

@@ -1221,7 +1221,7 @@ void enqueue_debug_neighbors(const FluidBufs& b, uint32_t n, const StepParams& P
 void enqueue_front_metrics(const FluidBufs& b, uint32_t n, cudaStream_t st) {
   cudaMemsetAsync(b.scalar + 2, 0, 2 * sizeof(unsigned int), st);
   if (n == 0) return;
-  uint32_t g = min(cdiv(n, 256), 148u * 2u);
+  uint32_t g = min(cdiv(n, 256), 148u * 8u);
   k_front_metrics<<<g, 256, 0, st>>>(b.state, n, b.scalar + 2);
 }
 
