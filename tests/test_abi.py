@@ -267,3 +267,32 @@ def test_add_bodies_bulk(lib):
     assert lib.phieng_world_add_bodies(w, descs, 5, None) == 0
     assert C.sizeof(_abi.BodyDesc2D) == 36 and _abi.BodyDesc2D.friction.offset == 28
     lib.phieng_world_free(w)
+
+
+def _has_gpu():
+    try:
+        import torch
+
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+def test_reserve_and_read_into_host_paths(lib):
+    """phieng_sph_reserve needs a device (loud failure without one); the host
+    mirror read-back works without one."""
+    from phi_eng_b200.world import World2
+
+    w = World2()
+    pts = np.array([[0.0, 0.0], [0.25, 0.0], [0.5, 0.25]], np.float32)
+    assert w.fluid.add_particles(pts) == 3
+    out = np.full((3, 4), np.nan, np.float32)
+    assert w.fluid.read_into(out) == 3
+    assert (out[:, :2] == pts).all() and (out[:, 2:] == 0).all()
+    with pytest.raises(ValueError):
+        w.fluid.read_into(np.zeros((3, 2), np.float32))
+    if not _has_gpu():
+        assert lib.phieng_sph_reserve(w._h, 1000) == 0
+        assert w.status().error == _abi.E_NO_DEVICE
+    w.close()
+    assert lib.phieng_sph_reserve(None, 10) == 0
