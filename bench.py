@@ -530,7 +530,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     e2e_s = time.perf_counter() - t0
     job2.close()
     e2e = {"value": n_total * args.steps * world / e2e_s, "unit": METRIC,
-           "h2d_bytes_per_step": int(n_total * 8 / args.steps),
+           "h2d_bytes_per_step": int(n_total * 16 / args.steps),
            "d2h_bytes_per_step": int(8 + final.nbytes / args.steps),
            "timed": "(device arrays reserved beforehand) first-step upload of the page-locked host particle "
                     "arrays, grid plan and graph capture + K x (phieng_world_step + "

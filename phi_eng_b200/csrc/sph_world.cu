@@ -379,14 +379,10 @@ void plan_grid(World2* w) {
 
 // Bucket-grid arrays: counts (padded to whole scan tiles), the range table
 // and the scan tile sums.
-bool ensure_range(World2* w) {
+// Bucket arrays for up to nbuckets buckets (+ the sentinel), zeroed.
+bool alloc_range(World2* w, uint32_t nbuckets) {
   FluidBufs& d = w->d;
-  const uint32_t m = w->plan.sentinel + 1;  // buckets + the non-finite sentinel
-  const uint32_t tiles = (m + kBucketScanTile - 1) / kBucketScanTile;
-  if (d.count && d.range_cap >= w->plan.nbuckets) {
-    d.count_len = tiles * kBucketScanTile;
-    return true;
-  }
+  const uint32_t tiles = (nbuckets + 1 + kBucketScanTile - 1) / kBucketScanTile;
   cudaStreamSynchronize(w->stream);
   dfree(d.count);
   dfree(d.start);
@@ -401,9 +397,22 @@ bool ensure_range(World2* w) {
   if (!cuda_ok(w, cudaMemsetAsync(d.count, 0, sizeof(uint32_t) * len, w->stream), "memset") ||
       !cuda_ok(w, cudaMemsetAsync(d.tstate, 0, sizeof(unsigned long long) * tiles, w->stream), "memset"))
     return false;
-  d.range_cap = w->plan.nbuckets;
+  d.range_cap = nbuckets;
   d.count_len = len;
   w->keys_valid = false;
+  return true;
+}
+
+bool ensure_range(World2* w) {
+  FluidBufs& d = w->d;
+  const uint32_t m = w->plan.sentinel + 1;  // buckets + the non-finite sentinel
+  const uint32_t tiles = (m + kBucketScanTile - 1) / kBucketScanTile;
+  if (d.count && d.range_cap >= w->plan.sentinel) {
+    d.count_len = tiles * kBucketScanTile;
+    return true;
+  }
+  if (!alloc_range(w, w->plan.sentinel)) return false;
+  d.count_len = tiles * kBucketScanTile;
   return true;
 }
 
@@ -1125,7 +1134,14 @@ uint32_t phieng_world_add_bodies(World2* w, const BodyDesc2D* descs, uint32_t n,
 int32_t phieng_sph_reserve(World2* w, uint32_t n) {
   if (!w || w->is_batch()) return 0;
   if (w->error != PHIENG_SPH_OK || !ensure_device(w)) return 0;
-  return ensure_capacity(w, std::max(n, w->n)) ? 1 : 0;
+  n = std::max(n, w->n);
+  if (!ensure_capacity(w, n)) return 0;
+  // the bucket arrays for the largest grid a plan for n particles can take
+  // (plan_cells: a power of two of buckets_per_particle * n, 2^12 .. 2^24)
+  const uint64_t want = (uint64_t)std::ceil((double)w->buckets_per_particle * (double)std::max<uint32_t>(n, 1));
+  const uint32_t budget = (uint32_t)std::min<uint64_t>(1ull << 24, std::max<uint64_t>(1ull << 12, next_pow2(want)));
+  if (w->d.count && w->d.range_cap >= budget) return 1;
+  return alloc_range(w, budget) ? 1 : 0;
 }
 
 int32_t phieng_sph_step_fluid(World2* w, PhiengBody2* bodies, uint32_t nbodies, float dt) {
