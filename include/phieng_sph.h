@@ -410,8 +410,9 @@ uint32_t phieng_sph_debug_neighbors(World2* world, uint32_t* counts, uint32_t* l
                                     uint32_t max_per, uint32_t max);
 
 /* Allocate the device arrays for n particles now (as std::vector::reserve),
- * so the first step does not. 1 ok, 0 for a null world, a batch, no device
- * or an allocation error. */
+ * and the bucket arrays of the largest grid a plan for n particles can use,
+ * so the first step allocates nothing. 1 ok, 0 for a null world, a batch, no
+ * device or an allocation error. */
 int32_t phieng_sph_reserve(World2* world, uint32_t n);
 
 /* ---- the fluid phase with the engine's rigid bodies (two-way coupling) ----
