@@ -56,7 +56,7 @@ FORCE_BYTES = 64
 # the ncu capture summarised in profiles/<kernel>_<workload>.md.
 PROFILED_TRAFFIC = {("dam_break_1m", "force_integrate"): 48.333312e6 + 1.921792e6}
 PROFILED_TRAFFIC_3D = {"force_integrate": 85.545216e6 + 14.838528e6}  # 100^3 3D dam break
-KERNELS_PER_STEP = 6  # scan reduce, scan down, place, fixup, density, force
+KERNELS_PER_STEP = 5  # single-pass scan, place, fixup, density, force
 
 
 def sort_bytes(buckets_per_particle: float) -> float:
