@@ -314,6 +314,20 @@ def generate_tracking_pairs(scs, mlp, ratio: int = 4, samples: int = 20, rollout
     return X, T
 
 
+def damped_targets(X, T, damp=(0.75, 1.0)):
+    """Project position targets onto pressure damping: the coarse step's
+    pressure displacement is P = a_p (ratio dt)^2 / h (features 13, 14); the
+    per-particle damping s that best explains the target in least squares,
+    s = -(T . P) / |P|^2, is clipped to `damp`, and the target becomes -s P.
+    A coarse step whose pressure response is damped far enough is stable
+    under iteration (its acoustic CFL number is 1.6 undamped), so the
+    network learns the fine trajectory's correction only within that range."""
+    P = X[:, 13:15]
+    pp = (P * P).sum(1).clamp_min(1e-30)
+    s = (-(T * P).sum(1) / pp).clamp(float(damp[0]), float(damp[1]))
+    return -s[:, None] * P
+
+
 def normalisation(X, T, sample: int = 1 << 20, seed: int = 7) -> np.ndarray:
     """mu / isd of the features and out_scale of the targets (per-component
     standard deviations) from a seeded subsample of the pairs."""
@@ -332,7 +346,7 @@ def normalisation(X, T, sample: int = 1 << 20, seed: int = 7) -> np.ndarray:
 def train_closure(scs=None, ratio: int = 4, samples: int = 40, every: int = 50, batch: int = 65536,
                   iters: int = 20000, lr: float = 1e-3, seed: int = 0x5EED, noise=(0.0, 0.1),
                   dagger_iters: int = 0, dagger_samples: int = 20, rollout: int = 4, target: str = "position",
-                  track_rounds: int = 0, track_iters: int = 5000, log=print):
+                  track_rounds: int = 0, track_iters: int = 5000, damp=(0.75, 1.0), log=print):
     """Generate pairs on the batched scenes (the 256-scene slice of the batched
     workload by default) and train a network; with dagger_iters > 0, a second
     round adds pairs from the trained closure's own rollouts and continues
@@ -342,7 +356,10 @@ def train_closure(scs=None, ratio: int = 4, samples: int = 40, every: int = 50, 
     torch = _torch()
     scs = scs if scs is not None else batched_scenes(256)
     t0 = time.perf_counter()
-    X, T = generate_pairs(scs, ratio=ratio, samples=samples, every=every, noise=noise, target=target)
+    gen_target = "position" if target == "damped" else target
+    X, T = generate_pairs(scs, ratio=ratio, samples=samples, every=every, noise=noise, target=gen_target)
+    if target == "damped":
+        T = damped_targets(X, T, damp)
     torch.cuda.synchronize()
     t1 = time.perf_counter()
     mlp = Mlp(seed)
@@ -354,10 +371,13 @@ def train_closure(scs=None, ratio: int = 4, samples: int = 40, every: int = 50, 
     t2 = time.perf_counter()
     info = dict(pairs=int(X.shape[0]), scenes=len(scs), gen_s=t1 - t0, train_s=t2 - t1,
                 loss_first=float(hist[:100].mean()), loss_last=float(hist[-100:].mean()), iters=iters,
-                batch=batch, lr=lr, ratio=ratio, noise=list(noise), target=target)
+                batch=batch, lr=lr, ratio=ratio, noise=list(noise), target=target,
+                damp=list(damp) if target == "damped" else None)
     if dagger_iters > 0:
         X2, T2 = generate_pairs(scs, ratio=ratio, samples=dagger_samples, every=every * samples // dagger_samples,
-                                noise=(0.0,), mlp=mlp, rollout=rollout, seed=seed ^ 0xDA66, target=target)
+                                noise=(0.0,), mlp=mlp, rollout=rollout, seed=seed ^ 0xDA66, target=gen_target)
+        if target == "damped":
+            T2 = damped_targets(X2, T2, damp)
         X = torch.cat([X, X2])
         T = torch.cat([T, T2])
         del X2, T2
@@ -481,7 +501,9 @@ def evaluate(scene, mlp: Mlp, coarse_steps: int = 50, ratio: int = 4, threshold:
             w.set_stream(s.cuda_stream)
             if run is not None:
                 w.set_closure(mlp, ratio, threshold, criterion)
-            w.step_n(dt, 1)  # upload, plan, first graphs outside the timing
+                w.closure_step(dt, 1)  # upload, plan, closure buffers and graphs outside the timing
+            else:
+                w.step_n(dt, 1)  # upload, plan, first graphs outside the timing
             w.sync()
             st = _abi.PhiengClosureStats()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -539,7 +561,8 @@ def _main(argv=None) -> None:
     t.add_argument("--noise", default="0,0.1", help="position noise amplitudes in units of h")
     t.add_argument("--dagger-iters", type=int, default=0)
     t.add_argument("--rollout", type=int, default=4)
-    t.add_argument("--target", choices=list(TARGETS), default="position")
+    t.add_argument("--target", choices=list(TARGETS) + ["damped"], default="position")
+    t.add_argument("--damp", default="0.75,1.0", help="damped target: the range of the pressure damping")
     t.add_argument("--track-rounds", type=int, default=0)
     e = sub.add_parser("eval")
     e.add_argument("--weights", default=WEIGHTS)
@@ -555,7 +578,8 @@ def _main(argv=None) -> None:
         noise = tuple(float(v) for v in a.noise.split(","))
         mlp, info = train_closure(batched_scenes(a.scenes), samples=a.samples, every=a.every, batch=a.batch,
                                   iters=a.iters, lr=a.lr, seed=a.seed, noise=noise, dagger_iters=a.dagger_iters,
-                                  rollout=a.rollout, target=a.target, track_rounds=a.track_rounds, log=None)
+                                  rollout=a.rollout, target=a.target, track_rounds=a.track_rounds,
+                                  damp=tuple(float(v) for v in a.damp.split(",")), log=None)
         os.makedirs(os.path.dirname(os.path.abspath(a.out)), exist_ok=True)
         mlp.save(a.out, **{k: np.asarray(v) for k, v in info.items()})
         print(json.dumps(dict(trained=a.out, **info)))

@@ -755,9 +755,11 @@ __global__ void __launch_bounds__(256) k_closure_check(const float2* __restrict_
                                                        const uint8_t* __restrict__ sphase, uint32_t n, StepParams P0,
                                                        BatchTab bt, const float* __restrict__ rho_prev,
                                                        unsigned int* __restrict__ out) {
-  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  __shared__ float red[3][8];
   float v[3] = {0.0f, 0.0f, 0.0f};
-  if (s < n) {
+  // grid-stride, then warp and block maxima: one atomic per block and value
+  // (per-warp atomics on three addresses serialised to ~67 us at 2^20)
+  for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
     const StepParams& P = scene_params<BATCH>(P0, bt.ptab, BATCH ? bt.sscene[s] : 0u);
     const uint32_t ph = PHASE ? min((uint32_t)sphase[s], 3u) : P.uniform_phase;
     const float r0 = fmaxf(P.rest[ph], kEps);
@@ -765,13 +767,21 @@ __global__ void __launch_bounds__(256) k_closure_check(const float2* __restrict_
     const float q[3] = {__fdiv_rn(__fsub_rn(d, d0), r0), __fsub_rn(__fdiv_rn(d, r0), 1.0f),
                         __fsub_rn(__fdiv_rn(d0, r0), 1.0f)};
 #pragma unroll
-    for (int c = 0; c < 3; c++) v[c] = (q[c] != q[c]) ? __int_as_float(0x7f800000) : fmaxf(q[c], 0.0f);
+    for (int c = 0; c < 3; c++)
+      v[c] = fmaxf(v[c], (q[c] != q[c]) ? __int_as_float(0x7f800000) : fmaxf(q[c], 0.0f));
   }
+  const uint32_t lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
 #pragma unroll
   for (int c = 0; c < 3; c++) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v[c] = fmaxf(v[c], __shfl_xor_sync(0xFFFFFFFFu, v[c], o));
-    if ((threadIdx.x & 31) == 0) atomicMax(&out[c], __float_as_uint(v[c]));
+    if (lane == 0) red[c][wid] = v[c];
+  }
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    float m = 0.0f;
+    for (uint32_t k = 0; k < (blockDim.x >> 5); k++) m = fmaxf(m, red[threadIdx.x][k]);
+    atomicMax(&out[threadIdx.x], __float_as_uint(m));
   }
 }
 
@@ -1025,12 +1035,31 @@ void enqueue_closure_force(const FluidBufs& b, uint32_t n, const StepParams& P, 
   launch_closure<kModeClosure>(b, n, P, mlp, io, st);
 }
 
+// Running maxima of the three closure checks over a block of coarse steps:
+// acc = (max out[0], max out[1], max (out[1] - out[2])), the per-step value
+// of each criterion (jump, compression, growth); reset to -inf.
+__global__ void k_check_fold(const unsigned int* __restrict__ out, float* __restrict__ acc, int reset) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  if (reset) {
+    acc[0] = acc[1] = acc[2] = -INFINITY;
+    return;
+  }
+  const float v0 = __uint_as_float(out[0]), v1 = __uint_as_float(out[1]), v2 = __uint_as_float(out[2]);
+  acc[0] = fmaxf(acc[0], v0);
+  acc[1] = fmaxf(acc[1], v1);
+  acc[2] = fmaxf(acc[2], __fsub_rn(v1, v2));
+}
+
+void enqueue_check_fold(const unsigned int* out, float* acc, bool reset, cudaStream_t st) {
+  k_check_fold<<<1, 32, 0, st>>>(out, acc, reset ? 1 : 0);
+}
+
 void enqueue_closure_check(const FluidBufs& b, uint32_t n, const StepParams& P, const float* rho_prev,
                            unsigned int* out, cudaStream_t st) {
   cudaMemsetAsync(out, 0, 3 * sizeof(unsigned int), st);
   if (n == 0) return;
   const bool ph = (P.flags & F_PHASE) != 0, bat = b.batch.ptab != nullptr;
-  const uint32_t g = cdiv(n, 256);
+  const uint32_t g = min(cdiv(n, 256), 148u * 8u);
   if (bat) {
     if (ph) k_closure_check<true, true><<<g, 256, 0, st>>>(b.sdq, b.sid, b.sphase, n, P, b.batch, rho_prev, out);
     else k_closure_check<false, true><<<g, 256, 0, st>>>(b.sdq, b.sid, b.sphase, n, P, b.batch, rho_prev, out);

@@ -161,6 +161,10 @@ void enqueue_buoyancy(const FluidBufs& b, const DynBufs& y, uint32_t n, const St
 // bounded waits). Leaves the bucket ranges wrong.
 void enqueue_scan_silent_tile(const FluidBufs& b, uint32_t m, cudaStream_t st);
 
+// Fold one coarse step's checks (out[0..2] of enqueue_closure_check) into
+// the block maxima acc[0..2] (jump, compression, growth), or reset them.
+void enqueue_check_fold(const unsigned int* out, float* acc, bool reset, cudaStream_t st);
+
 // Scatter the sorted density / pressure back to id order.
 void enqueue_unsort_dp(const FluidBufs& b, uint32_t n, float* dens, float* pres, cudaStream_t st);
 

@@ -108,6 +108,7 @@ struct World2 {
   uint32_t closure_criterion = 0;
   float4* d_save = nullptr;     // pre-step state of the last coarse step (id order)
   float* d_rho_prev = nullptr;  // pre-step density (id order)
+  float4* d_block_save = nullptr;  // state at the start of an optimistic block of coarse steps
   uint32_t closure_cap = 0;
   cudaGraphExec_t cexec = nullptr;
   std::string csig;
@@ -903,8 +904,11 @@ bool ensure_closure_buffers(World2* w) {
   if (w->closure_cap >= w->d.cap && w->d_save) return true;
   dfree(w->d_save);
   dfree(w->d_rho_prev);
+  dfree(w->d_block_save);
   w->closure_cap = 0;
-  if (!dalloc(w, w->d_save, w->d.cap) || !dalloc(w, w->d_rho_prev, w->d.cap)) return false;
+  if (!dalloc(w, w->d_save, w->d.cap) || !dalloc(w, w->d_rho_prev, w->d.cap) ||
+      !dalloc(w, w->d_block_save, w->d.cap))
+    return false;
   w->closure_cap = w->d.cap;
   release_graph(w);
   return true;
@@ -1028,6 +1032,7 @@ void phieng_world_free(World2* w) {
     dfree(w->d_ptab);
     dfree(w->d_save);
     dfree(w->d_rho_prev);
+    dfree(w->d_block_save);
     dfree(w->d_cbodies);
     dfree(w->dynb.dyn);
     dfree(w->dynb.samples);
@@ -1562,42 +1567,100 @@ int32_t phieng_sph_closure_step(World2* w, float dt_fine, uint32_t coarse_steps,
   io.save = w->d_save;
   io.rho_prev = w->d_rho_prev;
   enqueue_sort_density(w, Pc);
-  for (uint32_t k = 0; k < coarse_steps; k++) {
-    if (!run_coarse(w, Pc, mlp, io)) return 0;
-    w->sid_perm_n = w->n;
-    if (!cuda_ok(w, cudaMemcpyAsync(w->h_pinned, w->d.scalar + 4, 12, cudaMemcpyDeviceToHost, w->stream), "check") ||
-        !cuda_ok(w, cudaStreamSynchronize(w->stream), "sync"))
-      return 0;
-    float v[3];
-    std::memcpy(v, w->h_pinned, 12);
-    const float chk = w->closure_criterion == PHIENG_CLOSURE_JUMP          ? v[0]
-                      : w->closure_criterion == PHIENG_CLOSURE_COMPRESSION ? v[1]
-                                                                           : v[1] - v[2];
-    if (stats) {
-      stats->coarse_steps++;
-      stats->last_check = chk;
-      stats->max_check = std::max(stats->max_check, chk);
-    }
-    w->host_state_valid = false;
-    if (chk <= w->closure_threshold) {
-      if (stats) stats->accepted++;
-      w->substeps++;
-    } else {
-      // undo the coarse step, take ratio plain substeps instead
-      if (stats) stats->fallbacks++;
-      if (!cuda_ok(w, cudaMemcpyAsync(w->d.state, w->d_save, sizeof(float4) * w->n, cudaMemcpyDeviceToDevice,
+  // Coarse steps run in optimistic blocks: kBlock steps back to back with the
+  // checks folded on the device and one read of their maxima. If every step
+  // passes, the block stands exactly as step-by-step acceptance would have
+  // left it; otherwise the block's start is restored and its steps are taken
+  // one at a time with the per-step check and fallback, so the result is the
+  // same as that of the per-step rule in every case.
+  constexpr uint32_t kBlock = 8;
+  float* acc = reinterpret_cast<float*>(w->d.scalar + 13);
+  uint32_t k = 0;
+  while (k < coarse_steps) {
+    const uint32_t nb = std::min(kBlock, coarse_steps - k);
+    if (nb > 1) {
+      if (!cuda_ok(w, cudaMemcpyAsync(w->d_block_save, w->d.state, sizeof(float4) * w->n, cudaMemcpyDeviceToDevice,
                                       w->stream),
-                   "restore"))
+                   "block save"))
+        return 0;
+      enqueue_check_fold(w->d.scalar + 4, acc, true, w->stream);
+      for (uint32_t b = 0; b < nb; b++) {
+        if (!run_coarse(w, Pc, mlp, io)) return 0;
+        w->sid_perm_n = w->n;
+        enqueue_check_fold(w->d.scalar + 4, acc, false, w->stream);
+      }
+      if (!cuda_ok(w, cudaMemcpyAsync(w->h_pinned, w->d.scalar + 4, 12 * sizeof(unsigned int), cudaMemcpyDeviceToHost,
+                                      w->stream),
+                   "check") ||
+          !cuda_ok(w, cudaStreamSynchronize(w->stream), "sync"))
+        return 0;
+      float last[3], mx[3];
+      std::memcpy(last, w->h_pinned, 12);
+      std::memcpy(mx, w->h_pinned + 9, 12);  // scalar[13..15]
+      const int c = (int)w->closure_criterion;
+      const float chk = c == PHIENG_CLOSURE_JUMP ? mx[0] : c == PHIENG_CLOSURE_COMPRESSION ? mx[1] : mx[2];
+      w->host_state_valid = false;
+      if (chk <= w->closure_threshold) {
+        if (stats) {
+          stats->coarse_steps += nb;
+          stats->accepted += nb;
+          stats->last_check = c == PHIENG_CLOSURE_JUMP          ? last[0]
+                              : c == PHIENG_CLOSURE_COMPRESSION ? last[1]
+                                                                : last[1] - last[2];
+          stats->max_check = std::max(stats->max_check, chk);
+        }
+        w->substeps += nb;
+        for (uint32_t b = 0; b < nb; b++) w->time += dtc;
+        k += nb;
+        continue;
+      }
+      // a step of the block failed: back to its start, then step by step
+      if (!cuda_ok(w, cudaMemcpyAsync(w->d.state, w->d_block_save, sizeof(float4) * w->n, cudaMemcpyDeviceToDevice,
+                                      w->stream),
+                   "block restore"))
         return 0;
       w->keys_valid = false;
       if (!prepare(w)) return 0;
-      if (batch && !upload_scene_table(w, dt_fine)) return 0;
-      for (uint32_t r = 0; r < w->closure_ratio; r++)
-        if (!run_substep(w, Pf)) return 0;
-      if (batch && !upload_scene_table(w, dtc)) return 0;
-      if (k + 1 < coarse_steps) enqueue_sort_density(w, Pc);
+      enqueue_sort_density(w, Pc);
     }
-    w->time += dtc;
+    const uint32_t kend = k + nb;
+    for (; k < kend; k++) {
+      if (!run_coarse(w, Pc, mlp, io)) return 0;
+      w->sid_perm_n = w->n;
+      if (!cuda_ok(w, cudaMemcpyAsync(w->h_pinned, w->d.scalar + 4, 12, cudaMemcpyDeviceToHost, w->stream), "check") ||
+          !cuda_ok(w, cudaStreamSynchronize(w->stream), "sync"))
+        return 0;
+      float v[3];
+      std::memcpy(v, w->h_pinned, 12);
+      const float chk = w->closure_criterion == PHIENG_CLOSURE_JUMP          ? v[0]
+                        : w->closure_criterion == PHIENG_CLOSURE_COMPRESSION ? v[1]
+                                                                             : v[1] - v[2];
+      if (stats) {
+        stats->coarse_steps++;
+        stats->last_check = chk;
+        stats->max_check = std::max(stats->max_check, chk);
+      }
+      w->host_state_valid = false;
+      if (chk <= w->closure_threshold) {
+        if (stats) stats->accepted++;
+        w->substeps++;
+      } else {
+        // undo the coarse step, take ratio plain substeps instead
+        if (stats) stats->fallbacks++;
+        if (!cuda_ok(w, cudaMemcpyAsync(w->d.state, w->d_save, sizeof(float4) * w->n, cudaMemcpyDeviceToDevice,
+                                        w->stream),
+                     "restore"))
+          return 0;
+        w->keys_valid = false;
+        if (!prepare(w)) return 0;
+        if (batch && !upload_scene_table(w, dt_fine)) return 0;
+        for (uint32_t r = 0; r < w->closure_ratio; r++)
+          if (!run_substep(w, Pf)) return 0;
+        if (batch && !upload_scene_table(w, dtc)) return 0;
+        if (k + 1 < coarse_steps) enqueue_sort_density(w, Pc);
+      }
+      w->time += dtc;
+    }
   }
   w->keys_valid = false;  // the last sort consumed the bucket counts
   return cuda_ok(w, cudaGetLastError(), "closure step") ? 1 : 0;
