@@ -6,12 +6,16 @@ its minibatch sampling, used by tests/ to check the GPU kernels
 counterpart; this file states its definition:
 
   x_hat = bf16((x - mu) * isd)                      (float32 ops, then BF16)
-  z1 = W1 x_hat + b1,  h1 = bf16(silu(z1))
-  z2 = W2 h1 + b2,     h2 = bf16(silu(z2))
+  z1 = W1 x_hat + b1,  h1 = silu(z1)
+  z2 = W2 h1 + b2,     h2 = silu(z2)
   y  = W3 h2 + b3,     output = y * out_scale
   W1, W2, W3 rounded to BF16; biases FP32; products accumulated exactly here
   (FP32 on the tensor cores).
   loss = 1/(2B) sum_b |y_b - t_b / out_scale|^2
+
+The kernels evaluate silu(z) = u + u tanh(u), u = z / 2 (the hidden layers
+run on halved weights and biases, so the accumulators hold u), in FP32 with
+the hardware tanh, then round to BF16 (act_bf16).
 
 emulate=True reproduces the GPU's BF16 rounding points (to compare against
 the kernels within a tolerance: accumulation order and the hardware tanh
@@ -70,6 +74,13 @@ def dsilu(z):
     return s + z * s * (1.0 - s)
 
 
+def act_bf16(z):
+    """silu(z) at the kernels' rounding point: u = z / 2, u + u tanh(u)
+    (one fused multiply-add), rounded to BF16."""
+    u = 0.5 * z
+    return bf16((u + u * np.tanh(u)).astype(np.float32)).astype(np.float64)
+
+
 def normalise(x, norm, emulate=True):
     x32 = np.asarray(x, dtype=np.float32)
     mu = np.asarray(norm[:FEAT], dtype=np.float32)
@@ -85,11 +96,9 @@ def forward(params, norm, x, emulate=True):
     W1b, W2b, W3b = (r(W).astype(np.float64) for W in (W1, W2, W3))
     xh = normalise(x, norm, emulate)
     z1 = xh @ W1b.T + b1.astype(np.float64)
-    a1 = silu(z1)
-    h1 = bf16(a1.astype(np.float32)).astype(np.float64) if emulate else a1
+    h1 = act_bf16(z1) if emulate else silu(z1)
     z2 = h1 @ W2b.T + b2.astype(np.float64)
-    a2 = silu(z2)
-    h2 = bf16(a2.astype(np.float32)).astype(np.float64) if emulate else a2
+    h2 = act_bf16(z2) if emulate else silu(z2)
     y = h2 @ W3b.T + b3.astype(np.float64)
     os_ = np.asarray(norm[2 * FEAT:], dtype=np.float64)
     cache = dict(xh=xh, z1=z1, h1=h1, z2=z2, h2=h2, y=y, W1b=W1b, W2b=W2b, W3b=W3b)

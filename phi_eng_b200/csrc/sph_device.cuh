@@ -370,12 +370,19 @@ struct FeatAcc {
   uint32_t cnt = 0;
 };
 
-__device__ __forceinline__ void feat_pair(FeatAcc& a, float gxx, float gyy, float w, float m_j, float rho_j,
+// vol = V_j = m_j / rho_j and pj = (q_j rho_j) rho_j come precomputed per
+// particle (the density pass's closure factors). PXY: accumulate the pressure
+// sum P here; a caller whose force sum has no other terms (no artificial
+// viscosity, no cohesion) takes P from it instead, which is the same sum of
+// the same products in the same order.
+template <bool PXY>
+__device__ __forceinline__ void feat_pair(FeatAcc& a, float gxx, float gyy, float w, float vol, float pj, float m_j,
                                           float q_i, float q_j, float dvx, float dvy) {
-  const float mt = __fmul_rn(m_j, __fadd_rn(q_i, q_j));
-  a.px = __fsub_rn(a.px, __fmul_rn(gxx, mt));
-  a.py = __fsub_rn(a.py, __fmul_rn(gyy, mt));
-  const float vol = __fdiv_rn(m_j, rho_j);
+  if constexpr (PXY) {
+    const float mt = __fmul_rn(m_j, __fadd_rn(q_i, q_j));
+    a.px = __fsub_rn(a.px, __fmul_rn(gxx, mt));
+    a.py = __fsub_rn(a.py, __fmul_rn(gyy, mt));
+  }
   a.div = __fadd_rn(a.div, __fmul_rn(vol, __fadd_rn(__fmul_rn(dvx, gxx), __fmul_rn(dvy, gyy))));
   a.curl = __fadd_rn(a.curl, __fmul_rn(vol, __fsub_rn(__fmul_rn(dvx, gyy), __fmul_rn(dvy, gxx))));
   const float ww = __fmul_rn(vol, w);
@@ -385,7 +392,7 @@ __device__ __forceinline__ void feat_pair(FeatAcc& a, float gxx, float gyy, floa
   a.m1y = __fadd_rn(a.m1y, wy);
   a.m2xx = __fadd_rn(a.m2xx, __fmul_rn(wx, dvx));
   a.m2yy = __fadd_rn(a.m2yy, __fmul_rn(wy, dvy));
-  a.pw = __fadd_rn(a.pw, __fmul_rn(ww, __fmul_rn(__fmul_rn(q_j, rho_j), rho_j)));
+  a.pw = __fadd_rn(a.pw, __fmul_rn(ww, pj));
   a.cnt++;
 }
 

@@ -395,7 +395,7 @@ __global__ void __launch_bounds__(256) k_density(const float2* __restrict__ spos
                                                  const uint8_t* __restrict__ sphase, uint32_t n,
                                                  const uint32_t* __restrict__ start, StepParams P0, BatchTab bt,
                                                  float2* __restrict__ sdq, float* __restrict__ spres,
-                                                 uint32_t* __restrict__ nmask) {
+                                                 uint32_t* __restrict__ nmask, float2* __restrict__ svp) {
   const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n) return;
   const StepParams& P = scene_params<BATCH>(P0, bt.ptab, BATCH ? bt.sscene[s] : 0u);
@@ -454,8 +454,12 @@ __global__ void __launch_bounds__(256) k_density(const float2* __restrict__ spos
   const uint32_t ph = PHASE ? min((uint32_t)sphase[s], 3u) : P.uniform_phase;
   const float p = eos(dens, P.rest[ph], P);
   const float rc = fmaxf(dens, kEps);
-  sdq[s] = make_float2(dens, __fdiv_rn(p, __fmul_rn(rc, rc)));
+  const float q = __fdiv_rn(p, __fmul_rn(rc, rc));
+  sdq[s] = make_float2(dens, q);
   spres[s] = p;
+  // closure passes: the per-neighbour factors of the feature sums, once per
+  // particle instead of once per pair (same expressions as feat_pair's)
+  if (svp) svp[s] = make_float2(__fdiv_rn(MASS ? smass[s] : P.mass, rc), __fmul_rn(__fmul_rn(q, rc), rc));
 }
 
 // ---------------------------------------------------------------- K6 force + integrate
@@ -468,8 +472,8 @@ template <bool MASS, bool FEAT, bool PLAIN = false>
 __device__ __forceinline__ void pair_terms(uint32_t j, float2 pi, float2 vi, float rho_i, float q_i, float m_i,
                                            const float2* __restrict__ spos, const float2* __restrict__ svel,
                                            const float2* __restrict__ sdq, const float* __restrict__ smass,
-                                           const StepParams& P, float& fx, float& fy, float& sx, float& sy,
-                                           FeatAcc& fa) {
+                                           const float2* __restrict__ svp, const StepParams& P, float& fx,
+                                           float& fy, float& sx, float& sy, FeatAcc& fa) {
   const float2 pj = __ldg(&spos[j]);
   const float2 dqj = __ldg(&sdq[j]);
   const float2 vj = __ldg(&svel[j]);
@@ -488,8 +492,13 @@ __device__ __forceinline__ void pair_terms(uint32_t j, float2 pi, float2 vi, flo
     gxx = __fmul_rn(__fdiv_rn(dx, dist), sc);
     gyy = __fmul_rn(__fdiv_rn(dy, dist), sc);
   }
-  if constexpr (FEAT)
-    feat_pair(fa, gxx, gyy, poly6(d2, P), m_j, rho_j, q_i, dqj.y, __fsub_rn(vj.x, vi.x), __fsub_rn(vj.y, vi.y));
+  if constexpr (FEAT) {
+    // PLAIN: d2 < hg2 <= hk2, so poly6's range test passes (and the XSPH
+    // term's poly6_nb is the same value)
+    const float2 vp = __ldg(&svp[j]);
+    feat_pair<!PLAIN>(fa, gxx, gyy, PLAIN ? poly6_nb<false>(d2, P) : poly6(d2, P), vp.x, vp.y, m_j, q_i, dqj.y,
+                      __fsub_rn(vj.x, vi.x), __fsub_rn(vj.y, vi.y));
+  }
   float term = __fadd_rn(q_i, dqj.y);
   if (!PLAIN && (P.flags & F_AV) && dist > kEps) {
     // Monaghan term (fluid.rs:302-317, called at :963-975)
@@ -534,7 +543,8 @@ template <bool MASS, bool FEAT, bool PLAIN = false>
 __device__ __forceinline__ void neighbour_sums(uint32_t s, uint32_t k, uint32_t n, float2 pi, float2 vi, float rho_i,
                                                float q_i, float m_i, const float2* __restrict__ spos,
                                                const float2* __restrict__ svel, const float2* __restrict__ sdq,
-                                               const float* __restrict__ smass, const uint32_t* __restrict__ start,
+                                               const float* __restrict__ smass, const float2* __restrict__ svp,
+                                               const uint32_t* __restrict__ start,
                                                const uint32_t* __restrict__ nmask, const StepParams& P, float& fx,
                                                float& fy, float& sx, float& sy, FeatAcc& fa) {
   const GridPlan& g = P.grid;
@@ -562,7 +572,7 @@ __device__ __forceinline__ void neighbour_sums(uint32_t s, uint32_t k, uint32_t 
       if (cur == 0u) break;
       const uint32_t j = base + (uint32_t)(__ffs((int)cur) - 1);
       cur &= cur - 1u;
-      pair_terms<MASS, FEAT, PLAIN>(j, pi, vi, rho_i, q_i, m_i, spos, svel, sdq, smass, P, fx, fy, sx, sy, fa);
+      pair_terms<MASS, FEAT, PLAIN>(j, pi, vi, rho_i, q_i, m_i, spos, svel, sdq, smass, svp, P, fx, fy, sx, sy, fa);
     }
   } else {
     for_each_candidate(k, start, g, [&](int jj) {
@@ -572,7 +582,7 @@ __device__ __forceinline__ void neighbour_sums(uint32_t s, uint32_t k, uint32_t 
       const float ey = __fsub_rn(pj.y, pi.y);
       const float d2 = __fadd_rn(__fmul_rn(ex, ex), __fmul_rn(ey, ey));
       if (d2 < P.hg2 && j != s)
-        pair_terms<MASS, FEAT, PLAIN>(j, pi, vi, rho_i, q_i, m_i, spos, svel, sdq, smass, P, fx, fy, sx, sy, fa);
+        pair_terms<MASS, FEAT, PLAIN>(j, pi, vi, rho_i, q_i, m_i, spos, svel, sdq, smass, svp, P, fx, fy, sx, sy, fa);
     });
   }
 }
@@ -643,8 +653,8 @@ __global__ void __launch_bounds__(256) k_force_integrate(
   const float q_i = dqi.y;  // p_i / (rho_i * rho_i)
   float fx = 0.0f, fy = 0.0f, sx = 0.0f, sy = 0.0f;
   FeatAcc fa;
-  neighbour_sums<MASS, false, PLAIN>(s, k, n, pi, vi, rho_i, q_i, m_i, spos, svel, sdq, smass, start, nmask, P, fx, fy, sx,
-                              sy, fa);
+  neighbour_sums<MASS, false, PLAIN>(s, k, n, pi, vi, rho_i, q_i, m_i, spos, svel, sdq, smass, nullptr, start, nmask,
+                                     P, fx, fy, sx, sy, fa);
   if (DEBUG) {
     dbg_force[id] = make_float2(fx, fy);
     return;
@@ -664,13 +674,17 @@ __global__ void __launch_bounds__(256) k_force_integrate(
 // units of h). It also keeps the pre-step state and density by id for the
 // fallback and the density-jump check.
 // FEATURES mode only writes the features (id order, 16 floats per particle)
-// for the coarse step P.dt and leaves the state untouched.
+// for the coarse step P.dt and leaves the state untouched. PLAIN as for K6
+// (plain_flags); both variants give the same features and state.
+// io.svp: the density pass's per-particle closure factors of this sort.
 constexpr int kModeFeatures = 1;
 constexpr int kModeClosure = 2;
 constexpr int kXRow = 24;  // BF16 elements per staged feature row (16 + pad)
 
-template <bool MASS, bool PHASE, bool BATCH, int MODE>
-__global__ void __launch_bounds__(256, 3) k_force_closure(
+// 4 blocks per SM (64 registers, a few bytes spilled): 171 -> 152 us per
+// coarse step at 2^20 particles against 3 blocks (80 registers, no spills).
+template <bool MASS, bool PHASE, bool BATCH, bool PLAIN, int MODE>
+__global__ void __launch_bounds__(256, 4) k_force_closure(
     const float2* __restrict__ spos, const float2* __restrict__ svel, const float2* __restrict__ sdq,
     const float* __restrict__ spres, const uint32_t* __restrict__ skey, const uint32_t* __restrict__ sid,
     const float* __restrict__ smass, const uint8_t* __restrict__ sphase, uint32_t n,
@@ -700,8 +714,12 @@ __global__ void __launch_bounds__(256, 3) k_force_closure(
   const float q_i = dqi.y;
   float fx = 0.0f, fy = 0.0f, sx = 0.0f, sy = 0.0f;
   FeatAcc fa;
-  neighbour_sums<MASS, true>(s, k, n, pi, vi, rho_i, q_i, m_i, spos, svel, sdq, smass, start, nmask, P, fx, fy, sx,
-                             sy, fa);
+  neighbour_sums<MASS, true, PLAIN>(s, k, n, pi, vi, rho_i, q_i, m_i, spos, svel, sdq, smass, io.svp, start, nmask,
+                                    P, fx, fy, sx, sy, fa);
+  if constexpr (PLAIN) {
+    fa.px = fx;  // the force sum is the pressure sum alone (feat_pair<false>)
+    fa.py = fy;
+  }
   const uint32_t ph = PHASE ? min((uint32_t)sphase[s], 3u) : P.uniform_phase;
   float wd, wnx, wny;
   wall_feature(pi.x, pi.y, bodies, P, wd, wnx, wny);
@@ -936,14 +954,14 @@ void enqueue_sort_and_ranges(const FluidBufs& b, uint32_t n, const StepParams& P
   cudaMemsetAsync(b.count, 0, sizeof(uint32_t) * b.count_len, st);
 }
 
-void enqueue_density(const FluidBufs& b, uint32_t n, const StepParams& P, cudaStream_t st) {
+void enqueue_density(const FluidBufs& b, uint32_t n, const StepParams& P, cudaStream_t st, float2* svp) {
   if (n == 0) return;
   const bool m = (P.flags & F_MASS) != 0, ph = (P.flags & F_PHASE) != 0, bat = b.batch.ptab != nullptr;
   const bool wide = (P.flags & F_WIDE_NB) != 0;  // h <= 0, which only a snapshot can carry
   const uint32_t bs = b.block_density, g = cdiv(n, bs);
 #define PHIENG_DENSITY(M, PH, BT, WD)                                                                          \
   k_density<M, PH, BT, WD><<<g, bs, 0, st>>>(b.spos, b.skey, b.smass, b.sphase, n, b.start, P, b.batch, b.sdq, \
-                                             b.spres, b.nmask)
+                                             b.spres, b.nmask, svp)
 #define PHIENG_DENSITY_W(M, PH, BT)       \
   do {                                    \
     if (wide)                             \
@@ -1002,13 +1020,18 @@ template <int MODE>
 void launch_closure(const FluidBufs& b, uint32_t n, const StepParams& P, const MlpDev& mlp, const ClosureIO& io,
                     cudaStream_t st) {
   const bool m = (P.flags & F_MASS) != 0, ph = (P.flags & F_PHASE) != 0, bat = b.batch.ptab != nullptr;
+  const bool plain = plain_flags(P.flags) && !m && !ph;
   const uint32_t g = cdiv(n, 256);
   const size_t sm = MODE == kModeClosure ? closure_smem_bytes() : 0;
-#define PHIENG_CLOSURE(M, PH, BT)                                                                                 \
-  k_force_closure<M, PH, BT, MODE><<<g, 256, sm, st>>>(b.spos, b.svel, b.sdq, b.spres, b.skey, b.sid, b.smass,   \
-                                                       b.sphase, n, b.start, P, b.batch, b.bodies, b.nmask, mlp, \
-                                                       io, b.state, b.key, b.count)
-  if (bat) {
+#define PHIENG_CLOSURE_V(M, PH, BT, PL)                                                                           \
+  k_force_closure<M, PH, BT, PL, MODE><<<g, 256, sm, st>>>(b.spos, b.svel, b.sdq, b.spres, b.skey, b.sid,         \
+                                                           b.smass, b.sphase, n, b.start, P, b.batch, b.bodies,   \
+                                                           b.nmask, mlp, io, b.state, b.key, b.count)
+#define PHIENG_CLOSURE(M, PH, BT) PHIENG_CLOSURE_V(M, PH, BT, false)
+  if (plain) {
+    if (bat) PHIENG_CLOSURE_V(false, false, true, true);
+    else PHIENG_CLOSURE_V(false, false, false, true);
+  } else if (bat) {
     if (m && ph) PHIENG_CLOSURE(true, true, true);
     else if (m) PHIENG_CLOSURE(true, false, true);
     else if (ph) PHIENG_CLOSURE(false, true, true);
@@ -1020,12 +1043,15 @@ void launch_closure(const FluidBufs& b, uint32_t n, const StepParams& P, const M
     else PHIENG_CLOSURE(false, false, false);
   }
 #undef PHIENG_CLOSURE
+#undef PHIENG_CLOSURE_V
 }
 
-void enqueue_closure_features(const FluidBufs& b, uint32_t n, const StepParams& P, float* feat, cudaStream_t st) {
+void enqueue_closure_features(const FluidBufs& b, uint32_t n, const StepParams& P, float* feat, const float2* svp,
+                              cudaStream_t st) {
   if (n == 0) return;
   ClosureIO io;
   io.feat = feat;
+  io.svp = svp;
   launch_closure<kModeFeatures>(b, n, P, MlpDev{}, io, st);
 }
 

@@ -94,8 +94,10 @@ struct BucketSort {
 };
 void enqueue_bucket_place(const BucketSort& bs, uint32_t n, uint32_t m, bool by_slot, cudaStream_t st);
 
-// K5: density + EOS in sorted order.
-void enqueue_density(const FluidBufs& b, uint32_t n, const StepParams& P, cudaStream_t st);
+// K5: density + EOS in sorted order. svp (optional, sorted order): also
+// (m / max(density, EPS), q max(density, EPS)^2) per particle, the
+// neighbour factors of the closure feature sums.
+void enqueue_density(const FluidBufs& b, uint32_t n, const StepParams& P, cudaStream_t st, float2* svp = nullptr);
 
 // K6: pressure force + XSPH + integrate + walls; writes state and next keys
 // in id order. With dbg_force != nullptr it only writes the forces (id
@@ -110,11 +112,13 @@ struct ClosureIO {
   float* feat = nullptr;
   float4* save = nullptr;
   float* rho_prev = nullptr;
+  const float2* svp = nullptr;  // K5's closure factors of the current sort (required)
 };
 
 // Closure features of every particle for a coarse step of P.dt (after the
 // sort and density of the current state); state untouched.
-void enqueue_closure_features(const FluidBufs& b, uint32_t n, const StepParams& P, float* feat, cudaStream_t st);
+void enqueue_closure_features(const FluidBufs& b, uint32_t n, const StepParams& P, float* feat, const float2* svp,
+                              cudaStream_t st);
 
 // Coarse step with the closure network: K6 + features + network + corrected
 // integrate. Writes the new state, next keys and counts like K6, plus the

@@ -63,7 +63,7 @@ struct TrainSmem {
   float tgt[kTileRows][2];
   float dy[kTileRows][2];
   float db[4][2 * kHidden];            // per-warp bias-gradient sums (b1 | b2)
-  alignas(16) float z1[4][2][8][32][4];  // per warp: layer-1 pre-activations in C-fragment order
+  alignas(16) float z1[4][2][8][32][4];  // per warp: halved layer-1 pre-activations (z1 / 2), C-fragment order
   __nv_bfloat16 xs[kTileRows][kXR];    // x_hat, row major
   __nv_bfloat16 xt[kFeat][kLdT];       // x_hat^T
   __nv_bfloat16 h1t[kHidden][kLdT];    // H1^T
@@ -76,17 +76,18 @@ struct TrainSmem {
 // FP32 bias array and the BF16-rounded W3 copy.
 __device__ __forceinline__ void write_weight(int p, float w, __nv_bfloat16* img, float* bias, float* w3) {
   const __nv_bfloat16 b = __float2bfloat16_rn(w);
+  const __nv_bfloat16 bh = __float2bfloat16_rn(__fmul_rn(0.5f, w));  // = b / 2 exactly
   if (p < kOffB1) {
     const int n = p / kFeat, k = p % kFeat;
-    img[frag_pos(k, n, 8)] = b;
+    img[frag_pos(k, n, 8)] = bh;
   } else if (p < kOffW2) {
-    bias[p - kOffB1] = w;
+    bias[p - kOffB1] = __fmul_rn(0.5f, w);
   } else if (p < kOffB2) {
     const int q = p - kOffW2, o = q / kHidden, i = q % kHidden;
-    img[4 * kF1 + frag_pos(i, o, 8)] = b;
+    img[4 * kF1 + frag_pos(i, o, 8)] = bh;
     img[4 * (kF1 + kF2 + kF3) + frag_pos(o, i, 8)] = b;
   } else if (p < kOffW3) {
-    bias[kHidden + (p - kOffB2)] = w;
+    bias[kHidden + (p - kOffB2)] = __fmul_rn(0.5f, w);
   } else if (p < kOffB3) {
     const int q = p - kOffW3, o = q / kHidden, n = q % kHidden;
     img[4 * (kF1 + kF2) + frag_pos(n, o, 1)] = b;
@@ -150,6 +151,17 @@ __global__ void __launch_bounds__(128) k_mlp_forward(const float* __restrict__ x
 }
 
 __device__ __forceinline__ void store_bf16(__nv_bfloat16* p, float v) { *p = __float2bfloat16_rn(v); }
+
+// A packed BF16 pair of columns (c0, c0 + 1) of row r into a transposed
+// [column][row] array.
+template <int LD>
+__device__ __forceinline__ void store_pair_t(__nv_bfloat16 (*m)[LD], int c0, int r, uint32_t v) {
+  *reinterpret_cast<uint16_t*>(&m[c0][r]) = (uint16_t)(v & 0xFFFFu);
+  *reinterpret_cast<uint16_t*>(&m[c0 + 1][r]) = (uint16_t)(v >> 16);
+}
+
+// silu'(z) from the halved pre-activation u = z / 2 (z = 2u exactly).
+__device__ __forceinline__ float dsilu_half(float u) { return dsilu_hw(__fmul_rn(2.0f, u)); }
 
 // Sum over the 8 row groups of a warp (lanes with equal lane % 4), fixed order.
 __device__ __forceinline__ float group_sum(float v) {
@@ -233,46 +245,39 @@ __global__ void __launch_bounds__(kTrainThreads, 1)
       uint32_t h[4][4];
 #pragma unroll
       for (int nt = 0; nt < 8; nt++) {
-        float c[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+        const int c0 = nt * 8 + 2 * t;
+        float c[4] = {S.bias[c0], S.bias[c0 + 1], S.bias[c0], S.bias[c0 + 1]};
         const uint2 b = S.f1[nt * 32 + lane];
         mma_bf16(c, a, b.x, b.y);
-        const int c0 = nt * 8 + 2 * t;
-        const float z0 = __fadd_rn(c[0], S.bias[c0]), z1 = __fadd_rn(c[1], S.bias[c0 + 1]);
-        const float z2 = __fadd_rn(c[2], S.bias[c0]), z3 = __fadd_rn(c[3], S.bias[c0 + 1]);
-        *reinterpret_cast<float4*>(&S.z1[warp][mt][nt][lane][0]) = make_float4(z0, z1, z2, z3);
-        const float s0 = silu_hw(z0), s1 = silu_hw(z1), s2 = silu_hw(z2), s3 = silu_hw(z3);
-        h[nt >> 1][(nt & 1) * 2 + 0] = pack_bf16(s0, s1);
-        h[nt >> 1][(nt & 1) * 2 + 1] = pack_bf16(s2, s3);
-        store_bf16(&S.h1t[c0][ra], s0);
-        store_bf16(&S.h1t[c0 + 1][ra], s1);
-        store_bf16(&S.h1t[c0][rb], s2);
-        store_bf16(&S.h1t[c0 + 1][rb], s3);
+        // halved pre-activations u = z1 / 2, kept for the backward pass
+        *reinterpret_cast<float4*>(&S.z1[warp][mt][nt][lane][0]) = make_float4(c[0], c[1], c[2], c[3]);
+        const uint32_t ha = silu_half_bf16x2(c[0], c[1]), hb = silu_half_bf16x2(c[2], c[3]);
+        h[nt >> 1][(nt & 1) * 2 + 0] = ha;
+        h[nt >> 1][(nt & 1) * 2 + 1] = hb;
+        store_pair_t(S.h1t, c0, ra, ha);
+        store_pair_t(S.h1t, c0, rb, hb);
       }
       float z2v[8][4];
       uint32_t h2[4][4];
 #pragma unroll
       for (int nt = 0; nt < 8; nt++) {
-        float c[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+        const int c0 = nt * 8 + 2 * t;
+        float c[4] = {S.bias[kHidden + c0], S.bias[kHidden + c0 + 1], S.bias[kHidden + c0], S.bias[kHidden + c0 + 1]};
 #pragma unroll
         for (int kt = 0; kt < 4; kt++) {
           const uint2 b = S.f2[(kt * 8 + nt) * 32 + lane];
           mma_bf16(c, h[kt], b.x, b.y);
         }
-        const int c0 = nt * 8 + 2 * t;
-        z2v[nt][0] = __fadd_rn(c[0], S.bias[kHidden + c0]);
-        z2v[nt][1] = __fadd_rn(c[1], S.bias[kHidden + c0 + 1]);
-        z2v[nt][2] = __fadd_rn(c[2], S.bias[kHidden + c0]);
-        z2v[nt][3] = __fadd_rn(c[3], S.bias[kHidden + c0 + 1]);
-        const float s0 = silu_hw(z2v[nt][0]), s1 = silu_hw(z2v[nt][1]);
-        const float s2 = silu_hw(z2v[nt][2]), s3 = silu_hw(z2v[nt][3]);
-        h2[nt >> 1][(nt & 1) * 2 + 0] = pack_bf16(s0, s1);
-        h2[nt >> 1][(nt & 1) * 2 + 1] = pack_bf16(s2, s3);
-        store_bf16(&S.h2t[c0][ra], s0);
-        store_bf16(&S.h2t[c0 + 1][ra], s1);
-        store_bf16(&S.h2t[c0][rb], s2);
-        store_bf16(&S.h2t[c0 + 1][rb], s3);
+#pragma unroll
+        for (int q = 0; q < 4; q++) z2v[nt][q] = c[q];  // u = z2 / 2
+        const uint32_t ha = silu_half_bf16x2(c[0], c[1]), hb = silu_half_bf16x2(c[2], c[3]);
+        h2[nt >> 1][(nt & 1) * 2 + 0] = ha;
+        h2[nt >> 1][(nt & 1) * 2 + 1] = hb;
+        store_pair_t(S.h2t, c0, ra, ha);
+        store_pair_t(S.h2t, c0, rb, hb);
       }
-      float c3[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+      const float b30 = t == 0 ? S.bias[2 * kHidden] : 0.0f, b31 = t == 0 ? S.bias[2 * kHidden + 1] : 0.0f;
+      float c3[4] = {b30, b31, b30, b31};
 #pragma unroll
       for (int kt = 0; kt < 4; kt++) {
         const uint2 b = S.f3[kt * 32 + lane];
@@ -281,10 +286,10 @@ __global__ void __launch_bounds__(kTrainThreads, 1)
       // loss and dY on the lanes holding output columns 0 and 1
       float dyl[4] = {0.0f, 0.0f, 0.0f, 0.0f};
       if (t == 0) {
-        const float e0 = __fsub_rn(__fadd_rn(c3[0], S.bias[2 * kHidden]), S.tgt[ra][0]);
-        const float e1 = __fsub_rn(__fadd_rn(c3[1], S.bias[2 * kHidden + 1]), S.tgt[ra][1]);
-        const float e2 = __fsub_rn(__fadd_rn(c3[2], S.bias[2 * kHidden]), S.tgt[rb][0]);
-        const float e3 = __fsub_rn(__fadd_rn(c3[3], S.bias[2 * kHidden + 1]), S.tgt[rb][1]);
+        const float e0 = __fsub_rn(c3[0], S.tgt[ra][0]);
+        const float e1 = __fsub_rn(c3[1], S.tgt[ra][1]);
+        const float e2 = __fsub_rn(c3[2], S.tgt[rb][0]);
+        const float e3 = __fsub_rn(c3[3], S.tgt[rb][1]);
         loss = __fadd_rn(loss, __fadd_rn(__fadd_rn(__fmul_rn(e0, e0), __fmul_rn(e1, e1)),
                                          __fadd_rn(__fmul_rn(e2, e2), __fmul_rn(e3, e3))));
         dyl[0] = __fmul_rn(e0, inv_b);
@@ -304,10 +309,10 @@ __global__ void __launch_bounds__(kTrainThreads, 1)
       for (int nt = 0; nt < 8; nt++) {
         const int c0 = nt * 8 + 2 * t;
         const float w00 = S.w3[c0], w01 = S.w3[c0 + 1], w10 = S.w3[kHidden + c0], w11 = S.w3[kHidden + c0 + 1];
-        const float d0 = __fmul_rn(__fadd_rn(__fmul_rn(dyl[0], w00), __fmul_rn(dyl[1], w10)), dsilu_hw(z2v[nt][0]));
-        const float d1 = __fmul_rn(__fadd_rn(__fmul_rn(dyl[0], w01), __fmul_rn(dyl[1], w11)), dsilu_hw(z2v[nt][1]));
-        const float d2 = __fmul_rn(__fadd_rn(__fmul_rn(dyl[2], w00), __fmul_rn(dyl[3], w10)), dsilu_hw(z2v[nt][2]));
-        const float d3 = __fmul_rn(__fadd_rn(__fmul_rn(dyl[2], w01), __fmul_rn(dyl[3], w11)), dsilu_hw(z2v[nt][3]));
+        const float d0 = __fmul_rn(__fadd_rn(__fmul_rn(dyl[0], w00), __fmul_rn(dyl[1], w10)), dsilu_half(z2v[nt][0]));
+        const float d1 = __fmul_rn(__fadd_rn(__fmul_rn(dyl[0], w01), __fmul_rn(dyl[1], w11)), dsilu_half(z2v[nt][1]));
+        const float d2 = __fmul_rn(__fadd_rn(__fmul_rn(dyl[2], w00), __fmul_rn(dyl[3], w10)), dsilu_half(z2v[nt][2]));
+        const float d3 = __fmul_rn(__fadd_rn(__fmul_rn(dyl[2], w01), __fmul_rn(dyl[3], w11)), dsilu_half(z2v[nt][3]));
         da[nt >> 1][(nt & 1) * 2 + 0] = pack_bf16(d0, d1);
         da[nt >> 1][(nt & 1) * 2 + 1] = pack_bf16(d2, d3);
         store_bf16(&S.dz2t[c0][ra], d0);
@@ -330,8 +335,8 @@ __global__ void __launch_bounds__(kTrainThreads, 1)
           mma_bf16(c, da[kt], b.x, b.y);
         }
         const float4 z = *reinterpret_cast<const float4*>(&S.z1[warp][mt][nt][lane][0]);
-        const float d0 = __fmul_rn(c[0], dsilu_hw(z.x)), d1 = __fmul_rn(c[1], dsilu_hw(z.y));
-        const float d2 = __fmul_rn(c[2], dsilu_hw(z.z)), d3 = __fmul_rn(c[3], dsilu_hw(z.w));
+        const float d0 = __fmul_rn(c[0], dsilu_half(z.x)), d1 = __fmul_rn(c[1], dsilu_half(z.y));
+        const float d2 = __fmul_rn(c[2], dsilu_half(z.z)), d3 = __fmul_rn(c[3], dsilu_half(z.w));
         const int c0 = nt * 8 + 2 * t;
         store_bf16(&S.dz1t[c0][ra], d0);
         store_bf16(&S.dz1t[c0 + 1][ra], d1);

@@ -11,10 +11,14 @@
 //   weight fragment images (BF16, the B operand of m16n8k16 in register
 //   order): one uint2 per lane per (k-tile, n-tile), so a warp loads a whole
 //   B fragment with one conflict-free 64-bit shared-memory read per lane.
-//     F1  B(k, n) = W1[n][k]   1 k-tile  x 8 n-tiles
-//     F2  B(k, n) = W2[n][k]   4 k-tiles x 8 n-tiles
-//     F3  B(k, n) = W3[n][k]   4 k-tiles x 1 n-tile (outputs 2..7 are zero)
-//     F2T B(k, n) = W2[k][n]   4 k-tiles x 8 n-tiles (backward dH1 = dZ2 W2)
+//     F1  B(k, n) = W1[n][k] / 2   1 k-tile  x 8 n-tiles
+//     F2  B(k, n) = W2[n][k] / 2   4 k-tiles x 8 n-tiles
+//     F3  B(k, n) = W3[n][k]       4 k-tiles x 1 n-tile (outputs 2..7 are zero)
+//     F2T B(k, n) = W2[k][n]       4 k-tiles x 8 n-tiles (backward dH1 = dZ2 W2)
+//   The hidden layers run on halved weights and biases, so their accumulators
+//   hold u = z / 2 (exact: a power-of-two scale commutes with the rounding)
+//   and the activation is silu(z) = u + u tanh(u) (silu_half_bf16x2). Each
+//   layer's bias is the accumulator's initial value.
 //
 // m16n8k16 register layout (PTX ISA, "Matrix Fragments for mma.m16n8k16"),
 // g = lane / 4, t = lane % 4:
@@ -52,8 +56,9 @@ constexpr int kF2T = 32 * 32;
 constexpr int kFragAll = kF1 + kF2 + kF3 + kF2T;
 constexpr int kBias = 2 * kHidden + kOut;  // b1 | b2 | b3
 
-// Device view of a network. frag: F1 | F2 | F3 | F2T; bias (FP32): b1 | b2 |
-// b3; w3 (BF16-rounded, as FP32): W3[2][64]; norm: mu | isd | out_scale.
+// Device view of a network. frag: F1 | F2 | F3 | F2T; bias (FP32): b1/2 |
+// b2/2 | b3; w3 (BF16-rounded, as FP32): W3[2][64]; norm: mu | isd |
+// out_scale.
 struct MlpDev {
   const uint2* frag;
   const float* bias;
@@ -70,6 +75,8 @@ __host__ __device__ inline uint32_t frag_pos(int k, int n, int nt_count) {
 }
 
 __device__ __forceinline__ void mma_bf16(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+  // volatile keeps the MMAs in program order: without it the compiler hoists
+  // every fragment load ahead and spills
   asm volatile(
       "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
       "{%0,%1,%2,%3};\n"
@@ -92,7 +99,16 @@ __device__ __forceinline__ float tanh_hw(float x) {
   return y;
 }
 __device__ __forceinline__ float sigmoid_hw(float z) { return __fadd_rn(__fmul_rn(0.5f, tanh_hw(__fmul_rn(0.5f, z))), 0.5f); }
-__device__ __forceinline__ float silu_hw(float z) { return __fmul_rn(z, sigmoid_hw(z)); }
+
+// Activation of two hidden units from their halved pre-activations u = z / 2,
+// packed as a BF16 pair (first unit in the low half):
+//   silu(z) = z sigmoid(z) = z (1 + tanh(z / 2)) / 2 = u + u tanh(u)
+// one hardware tanh and one fused multiply-add per unit in FP32, then one
+// conversion per pair. (BF16 arithmetic would be cheaper still, but a BF16
+// tanh near -1 loses 1 + tanh(u) to cancellation: ~6 % output error.)
+__device__ __forceinline__ uint32_t silu_half_bf16x2(float u0, float u1) {
+  return pack_bf16(__fmaf_rn(u0, tanh_hw(u0), u0), __fmaf_rn(u1, tanh_hw(u1), u1));
+}
 // d silu / dz = s + z s (1 - s)
 __device__ __forceinline__ float dsilu_hw(float z) {
   const float s = sigmoid_hw(z);
@@ -139,38 +155,40 @@ __device__ __forceinline__ void mlp_tile_forward(const __nv_bfloat16* xs, int ld
   uint32_t h[4][4];
 #pragma unroll
   for (int nt = 0; nt < 8; nt++) {
-    float c[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    const float2 bb = *reinterpret_cast<const float2*>(&s.bias[nt * 8 + 2 * t]);
+    float c[4] = {bb.x, bb.y, bb.x, bb.y};
     const uint2 b = s.f1[nt * 32 + lane];
     mma_bf16(c, a, b.x, b.y);
-    const float b0 = s.bias[nt * 8 + 2 * t], b1 = s.bias[nt * 8 + 2 * t + 1];
-    h[nt >> 1][(nt & 1) * 2 + 0] = pack_bf16(silu_hw(__fadd_rn(c[0], b0)), silu_hw(__fadd_rn(c[1], b1)));
-    h[nt >> 1][(nt & 1) * 2 + 1] = pack_bf16(silu_hw(__fadd_rn(c[2], b0)), silu_hw(__fadd_rn(c[3], b1)));
-  }
-  uint32_t h2[4][4];
-#pragma unroll
-  for (int nt = 0; nt < 8; nt++) {
-    float c[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-#pragma unroll
-    for (int kt = 0; kt < 4; kt++) {
-      const uint2 b = s.f2[(kt * 8 + nt) * 32 + lane];
-      mma_bf16(c, h[kt], b.x, b.y);
-    }
-    const float b0 = s.bias[kHidden + nt * 8 + 2 * t], b1 = s.bias[kHidden + nt * 8 + 2 * t + 1];
-    h2[nt >> 1][(nt & 1) * 2 + 0] = pack_bf16(silu_hw(__fadd_rn(c[0], b0)), silu_hw(__fadd_rn(c[1], b1)));
-    h2[nt >> 1][(nt & 1) * 2 + 1] = pack_bf16(silu_hw(__fadd_rn(c[2], b0)), silu_hw(__fadd_rn(c[3], b1)));
-  }
-  float c[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-#pragma unroll
-  for (int kt = 0; kt < 4; kt++) {
-    const uint2 b = s.f3[kt * 32 + lane];
-    mma_bf16(c, h2[kt], b.x, b.y);
+    h[nt >> 1][(nt & 1) * 2 + 0] = silu_half_bf16x2(c[0], c[1]);
+    h[nt >> 1][(nt & 1) * 2 + 1] = silu_half_bf16x2(c[2], c[3]);
   }
   const float b30 = t == 0 ? s.bias[2 * kHidden] : 0.0f;
   const float b31 = t == 0 ? s.bias[2 * kHidden + 1] : 0.0f;
-  y[0] = __fadd_rn(c[0], b30);
-  y[1] = __fadd_rn(c[1], b31);
-  y[2] = __fadd_rn(c[2], b30);
-  y[3] = __fadd_rn(c[3], b31);
+  y[0] = b30;
+  y[1] = b31;
+  y[2] = b30;
+  y[3] = b31;
+  // layer 2 two n-tiles at a time, each pair (one k-tile of layer 3) fed to
+  // the output straight away: 4 live activation registers instead of 16
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    uint32_t h2[4];
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+      const int nt = 2 * j + q;
+      const float2 bb = *reinterpret_cast<const float2*>(&s.bias[kHidden + nt * 8 + 2 * t]);
+      float c[4] = {bb.x, bb.y, bb.x, bb.y};
+#pragma unroll
+      for (int kt = 0; kt < 4; kt++) {
+        const uint2 b = s.f2[(kt * 8 + nt) * 32 + lane];
+        mma_bf16(c, h[kt], b.x, b.y);
+      }
+      h2[q * 2 + 0] = silu_half_bf16x2(c[0], c[1]);
+      h2[q * 2 + 1] = silu_half_bf16x2(c[2], c[3]);
+    }
+    const uint2 b = s.f3[j * 32 + lane];
+    mma_bf16(y, h2, b.x, b.y);
+  }
 }
 
 // x_hat = bf16((x - mu) * isd) for one row of 16 features, stored as BF16.

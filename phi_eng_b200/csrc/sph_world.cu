@@ -109,6 +109,7 @@ struct World2 {
   float4* d_save = nullptr;     // pre-step state of the last coarse step (id order)
   float* d_rho_prev = nullptr;  // pre-step density (id order)
   float4* d_block_save = nullptr;  // state at the start of an optimistic block of coarse steps
+  float2* d_svp = nullptr;         // sorted closure factors of the last closure density pass
   uint32_t closure_cap = 0;
   cudaGraphExec_t cexec = nullptr;
   std::string csig;
@@ -905,9 +906,10 @@ bool ensure_closure_buffers(World2* w) {
   dfree(w->d_save);
   dfree(w->d_rho_prev);
   dfree(w->d_block_save);
+  dfree(w->d_svp);
   w->closure_cap = 0;
   if (!dalloc(w, w->d_save, w->d.cap) || !dalloc(w, w->d_rho_prev, w->d.cap) ||
-      !dalloc(w, w->d_block_save, w->d.cap))
+      !dalloc(w, w->d_block_save, w->d.cap) || !dalloc(w, w->d_svp, w->d.cap))
     return false;
   w->closure_cap = w->d.cap;
   release_graph(w);
@@ -915,10 +917,11 @@ bool ensure_closure_buffers(World2* w) {
 }
 
 // Sort + density of the current state with parameters P (the state and its
-// keys / bucket counts are current). Leaves the counts consumed.
-void enqueue_sort_density(World2* w, const StepParams& P) {
+// keys / bucket counts are current). Leaves the counts consumed. svp: also
+// the closure factors (closure passes).
+void enqueue_sort_density(World2* w, const StepParams& P, float2* svp = nullptr) {
   enqueue_sort_and_ranges(w->d, w->n, P, w->sid_perm_n == w->n, w->stream);
-  enqueue_density(w->d, w->n, P, w->stream);
+  enqueue_density(w->d, w->n, P, w->stream, svp);
   w->sid_perm_n = w->n;
   w->dp_on_device = true;
 }
@@ -939,7 +942,7 @@ bool run_coarse(World2* w, const StepParams& P, const MlpDev& mlp, const Closure
       return false;
     enqueue_closure_force(w->d, w->n, P, mlp, io, w->own_stream);
     enqueue_sort_and_ranges(w->d, w->n, P, true, w->own_stream);
-    enqueue_density(w->d, w->n, P, w->own_stream);
+    enqueue_density(w->d, w->n, P, w->own_stream, w->d_svp);
     enqueue_closure_check(w->d, w->n, P, io.rho_prev, w->d.scalar + 4, w->own_stream);
     cudaError_t r = cudaStreamEndCapture(w->own_stream, &g);
     if (!cuda_ok(w, r, "end capture")) return false;
@@ -1033,6 +1036,7 @@ void phieng_world_free(World2* w) {
     dfree(w->d_save);
     dfree(w->d_rho_prev);
     dfree(w->d_block_save);
+    dfree(w->d_svp);
     dfree(w->d_cbodies);
     dfree(w->dynb.dyn);
     dfree(w->dynb.samples);
@@ -1530,9 +1534,10 @@ int32_t phieng_sph_features(World2* w, float dt, float* feat) {
   if (!w->is_batch() && unsupported(w)) return 0;
   if (!prepare(w)) return 0;
   if (w->is_batch() && !upload_scene_table(w, dt)) return 0;
+  if (!ensure_closure_buffers(w)) return 0;
   const StepParams P = make_params(w, dt);
-  enqueue_sort_density(w, P);
-  enqueue_closure_features(w->d, w->n, P, feat, w->stream);
+  enqueue_sort_density(w, P, w->d_svp);
+  enqueue_closure_features(w->d, w->n, P, feat, w->d_svp, w->stream);
   w->keys_valid = false;  // the sort consumed the bucket counts
   return cuda_ok(w, cudaGetLastError(), "features") ? 1 : 0;
 }
@@ -1566,7 +1571,8 @@ int32_t phieng_sph_closure_step(World2* w, float dt_fine, uint32_t coarse_steps,
   ClosureIO io;
   io.save = w->d_save;
   io.rho_prev = w->d_rho_prev;
-  enqueue_sort_density(w, Pc);
+  io.svp = w->d_svp;
+  enqueue_sort_density(w, Pc, w->d_svp);
   // Coarse steps run in optimistic blocks: kBlock steps back to back with the
   // checks folded on the device and one read of their maxima. If every step
   // passes, the block stands exactly as step-by-step acceptance would have
@@ -1621,7 +1627,7 @@ int32_t phieng_sph_closure_step(World2* w, float dt_fine, uint32_t coarse_steps,
         return 0;
       w->keys_valid = false;
       if (!prepare(w)) return 0;
-      enqueue_sort_density(w, Pc);
+      enqueue_sort_density(w, Pc, w->d_svp);
     }
     const uint32_t kend = k + nb;
     for (; k < kend; k++) {
@@ -1657,7 +1663,7 @@ int32_t phieng_sph_closure_step(World2* w, float dt_fine, uint32_t coarse_steps,
         for (uint32_t r = 0; r < w->closure_ratio; r++)
           if (!run_substep(w, Pf)) return 0;
         if (batch && !upload_scene_table(w, dtc)) return 0;
-        if (k + 1 < coarse_steps) enqueue_sort_density(w, Pc);
+        if (k + 1 < coarse_steps) enqueue_sort_density(w, Pc, w->d_svp);
       }
       w->time += dtc;
     }
