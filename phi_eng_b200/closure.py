@@ -345,7 +345,7 @@ def normalisation(X, T, sample: int = 1 << 20, seed: int = 7) -> np.ndarray:
 
 def train_closure(scs=None, ratio: int = 4, samples: int = 40, every: int = 50, batch: int = 65536,
                   iters: int = 20000, lr: float = 1e-3, seed: int = 0x5EED, noise=(0.0, 0.1),
-                  dagger_iters: int = 0, dagger_samples: int = 20, rollout: int = 4, target: str = "position",
+                  dagger_iters: int = 0, dagger_samples: int = 20, rollout: int = 4, target: str = "damped",
                   track_rounds: int = 0, track_iters: int = 5000, damp=(0.75, 1.0), log=print):
     """Generate pairs on the batched scenes (the 256-scene slice of the batched
     workload by default) and train a network; with dagger_iters > 0, a second
@@ -561,7 +561,7 @@ def _main(argv=None) -> None:
     t.add_argument("--noise", default="0,0.1", help="position noise amplitudes in units of h")
     t.add_argument("--dagger-iters", type=int, default=0)
     t.add_argument("--rollout", type=int, default=4)
-    t.add_argument("--target", choices=list(TARGETS) + ["damped"], default="position")
+    t.add_argument("--target", choices=list(TARGETS) + ["damped"], default="damped")
     t.add_argument("--damp", default="0.75,1.0", help="damped target: the range of the pressure damping")
     t.add_argument("--track-rounds", type=int, default=0)
     e = sub.add_parser("eval")
