@@ -9,13 +9,15 @@ counterpart; this file states its definition:
   z1 = W1 x_hat + b1,  h1 = silu(z1)
   z2 = W2 h1 + b2,     h2 = silu(z2)
   y  = W3 h2 + b3,     output = y * out_scale
-  W1, W2, W3 rounded to BF16; biases FP32; products accumulated exactly here
-  (FP32 on the tensor cores).
+  W1 rounded to BF16, W2 and W3 to FP16 (the backward's W2 to BF16); biases
+  FP32; products accumulated exactly here (FP32 on the tensor cores).
   loss = 1/(2B) sum_b |y_b - t_b / out_scale|^2
 
 The kernels evaluate silu(z) = u + u tanh(u), u = z / 2 (the hidden layers
-run on halved weights and biases, so the accumulators hold u), in FP32 with
-the hardware tanh, then round to BF16 (act_bf16).
+run on halved weights and biases, so the accumulators hold u), on FP16
+pairs: u rounded to FP16, the hardware's FP16 tanh, one FP16 fused
+multiply-add (act_f16). Layers 2 and 3 take those FP16 activations; dW2
+takes them rounded to BF16.
 
 emulate=True reproduces the GPU's BF16 rounding points (to compare against
 the kernels within a tolerance: accumulation order and the hardware tanh
@@ -74,11 +76,17 @@ def dsilu(z):
     return s + z * s * (1.0 - s)
 
 
-def act_bf16(z):
-    """silu(z) at the kernels' rounding point: u = z / 2, u + u tanh(u)
-    (one fused multiply-add), rounded to BF16."""
-    u = 0.5 * z
-    return bf16((u + u * np.tanh(u)).astype(np.float32)).astype(np.float64)
+def f16(x) -> np.ndarray:
+    """Round to the nearest FP16, ties to even (as float64)."""
+    return np.asarray(x, dtype=np.float64).astype(np.float16).astype(np.float64)
+
+
+def act_f16(z):
+    """silu(z) at the kernels' rounding points: u = f16(z / 2),
+    f16(u + u * f16(tanh(u))) (the last a fused multiply-add)."""
+    u = f16(np.clip(0.5 * z, -65504.0, 65504.0))
+    t = f16(np.tanh(u))
+    return f16(u + u * t)
 
 
 def normalise(x, norm, emulate=True):
@@ -93,15 +101,18 @@ def forward(params, norm, x, emulate=True):
     """Network output (times out_scale) and the intermediates."""
     W1, b1, W2, b2, W3, b3 = unpack(np.asarray(params, dtype=np.float32))
     r = bf16 if emulate else (lambda a: np.asarray(a, dtype=np.float32))
-    W1b, W2b, W3b = (r(W).astype(np.float64) for W in (W1, W2, W3))
+    h = f16 if emulate else (lambda a: np.asarray(a, dtype=np.float32).astype(np.float64))
+    W1b, W2b = (r(W).astype(np.float64) for W in (W1, W2))
+    W2h, W3h = h(W2), h(W3)
     xh = normalise(x, norm, emulate)
     z1 = xh @ W1b.T + b1.astype(np.float64)
-    h1 = act_bf16(z1) if emulate else silu(z1)
-    z2 = h1 @ W2b.T + b2.astype(np.float64)
-    h2 = act_bf16(z2) if emulate else silu(z2)
-    y = h2 @ W3b.T + b3.astype(np.float64)
+    h1 = act_f16(z1) if emulate else silu(z1)
+    z2 = h1 @ W2h.T + b2.astype(np.float64)
+    h2 = act_f16(z2) if emulate else silu(z2)
+    y = h2 @ W3h.T + b3.astype(np.float64)
     os_ = np.asarray(norm[2 * FEAT:], dtype=np.float64)
-    cache = dict(xh=xh, z1=z1, h1=h1, z2=z2, h2=h2, y=y, W1b=W1b, W2b=W2b, W3b=W3b)
+    h1g = bf16(h1.astype(np.float32)).astype(np.float64) if emulate else h1
+    cache = dict(xh=xh, z1=z1, h1=h1, h1g=h1g, z2=z2, h2=h2, y=y, W1b=W1b, W2b=W2b, W3b=W3h)
     return y * os_, cache
 
 
@@ -119,7 +130,7 @@ def loss_grad(params, norm, x, t, emulate=True):
     db3 = dy.sum(0)
     dz2 = (dy @ c["W3b"]) * dsilu(c["z2"])
     dz2g = bf16(dz2.astype(np.float32)).astype(np.float64) if emulate else dz2
-    dW2 = dz2g.T @ c["h1"]
+    dW2 = dz2g.T @ c["h1g"]
     db2 = dz2.sum(0)
     dz1 = (dz2g @ c["W2b"]) * dsilu(c["z1"])
     dz1g = bf16(dz1.astype(np.float32)).astype(np.float64) if emulate else dz1

@@ -67,31 +67,32 @@ struct TrainSmem {
   __nv_bfloat16 xs[kTileRows][kXR];    // x_hat, row major
   __nv_bfloat16 xt[kFeat][kLdT];       // x_hat^T
   __nv_bfloat16 h1t[kHidden][kLdT];    // H1^T
-  __nv_bfloat16 h2t[kHidden][kLdT];    // H2^T
+  __half h2t[kHidden][kLdT];           // H2^T (FP16, as the forward)
   __nv_bfloat16 dz2t[kHidden][kLdT];   // dZ2^T
   __nv_bfloat16 dz1t[kHidden][kLdT];   // dZ1^T
 };
 
-// Weight p of the flat parameter vector into the BF16 fragment images, the
-// FP32 bias array and the BF16-rounded W3 copy.
+// Weight p of the flat parameter vector into the fragment images (F1, F2T
+// BF16; F2, F3 FP16), the FP32 bias array and the FP16-rounded W3 copy (the
+// forward's W3, for the backward pass).
 __device__ __forceinline__ void write_weight(int p, float w, __nv_bfloat16* img, float* bias, float* w3) {
-  const __nv_bfloat16 b = __float2bfloat16_rn(w);
-  const __nv_bfloat16 bh = __float2bfloat16_rn(__fmul_rn(0.5f, w));  // = b / 2 exactly
+  __half* himg = reinterpret_cast<__half*>(img);
   if (p < kOffB1) {
     const int n = p / kFeat, k = p % kFeat;
-    img[frag_pos(k, n, 8)] = bh;
+    img[frag_pos(k, n, 8)] = __float2bfloat16_rn(__fmul_rn(0.5f, w));  // = bf16(w) / 2 exactly
   } else if (p < kOffW2) {
     bias[p - kOffB1] = __fmul_rn(0.5f, w);
   } else if (p < kOffB2) {
     const int q = p - kOffW2, o = q / kHidden, i = q % kHidden;
-    img[4 * kF1 + frag_pos(i, o, 8)] = bh;
-    img[4 * (kF1 + kF2 + kF3) + frag_pos(o, i, 8)] = b;
+    himg[4 * kF1 + frag_pos(i, o, 8)] = __float2half_rn(__fmul_rn(0.5f, w));
+    img[4 * (kF1 + kF2 + kF3) + frag_pos(o, i, 8)] = __float2bfloat16_rn(w);
   } else if (p < kOffW3) {
     bias[kHidden + (p - kOffB2)] = __fmul_rn(0.5f, w);
   } else if (p < kOffB3) {
     const int q = p - kOffW3, o = q / kHidden, n = q % kHidden;
-    img[4 * (kF1 + kF2) + frag_pos(n, o, 1)] = b;
-    w3[q] = __bfloat162float(b);
+    const __half h = __float2half_rn(w);
+    himg[4 * (kF1 + kF2) + frag_pos(n, o, 1)] = h;
+    w3[q] = __half2float(h);
   } else {
     bias[2 * kHidden + (p - kOffB3)] = w;
   }
@@ -152,12 +153,19 @@ __global__ void __launch_bounds__(128) k_mlp_forward(const float* __restrict__ x
 
 __device__ __forceinline__ void store_bf16(__nv_bfloat16* p, float v) { *p = __float2bfloat16_rn(v); }
 
-// A packed BF16 pair of columns (c0, c0 + 1) of row r into a transposed
+// A packed 16-bit pair of columns (c0, c0 + 1) of row r into a transposed
 // [column][row] array.
-template <int LD>
-__device__ __forceinline__ void store_pair_t(__nv_bfloat16 (*m)[LD], int c0, int r, uint32_t v) {
+template <class T, int LD>
+__device__ __forceinline__ void store_pair_t(T (*m)[LD], int c0, int r, uint32_t v) {
+  static_assert(sizeof(T) == 2, "16-bit elements");
   *reinterpret_cast<uint16_t*>(&m[c0][r]) = (uint16_t)(v & 0xFFFFu);
   *reinterpret_cast<uint16_t*>(&m[c0 + 1][r]) = (uint16_t)(v >> 16);
+}
+
+// An FP16 pair as a BF16 pair (round to nearest even).
+__device__ __forceinline__ uint32_t f16x2_to_bf16x2(uint32_t v) {
+  const float2 f = __half22float2(*reinterpret_cast<const __half2*>(&v));
+  return pack_bf16(f.x, f.y);
 }
 
 // silu'(z) from the halved pre-activation u = z / 2 (z = 2u exactly).
@@ -251,11 +259,12 @@ __global__ void __launch_bounds__(kTrainThreads, 1)
         mma_bf16(c, a, b.x, b.y);
         // halved pre-activations u = z1 / 2, kept for the backward pass
         *reinterpret_cast<float4*>(&S.z1[warp][mt][nt][lane][0]) = make_float4(c[0], c[1], c[2], c[3]);
-        const uint32_t ha = silu_half_bf16x2(c[0], c[1]), hb = silu_half_bf16x2(c[2], c[3]);
+        const uint32_t ha = silu_half_f16x2(c[0], c[1]), hb = silu_half_f16x2(c[2], c[3]);
         h[nt >> 1][(nt & 1) * 2 + 0] = ha;
         h[nt >> 1][(nt & 1) * 2 + 1] = hb;
-        store_pair_t(S.h1t, c0, ra, ha);
-        store_pair_t(S.h1t, c0, rb, hb);
+        // H1^T feeds dW2 = dZ2^T H1 on BF16 tensor cores
+        store_pair_t(S.h1t, c0, ra, f16x2_to_bf16x2(ha));
+        store_pair_t(S.h1t, c0, rb, f16x2_to_bf16x2(hb));
       }
       float z2v[8][4];
       uint32_t h2[4][4];
@@ -266,11 +275,11 @@ __global__ void __launch_bounds__(kTrainThreads, 1)
 #pragma unroll
         for (int kt = 0; kt < 4; kt++) {
           const uint2 b = S.f2[(kt * 8 + nt) * 32 + lane];
-          mma_bf16(c, h[kt], b.x, b.y);
+          mma_f16(c, h[kt], b.x, b.y);
         }
 #pragma unroll
         for (int q = 0; q < 4; q++) z2v[nt][q] = c[q];  // u = z2 / 2
-        const uint32_t ha = silu_half_bf16x2(c[0], c[1]), hb = silu_half_bf16x2(c[2], c[3]);
+        const uint32_t ha = silu_half_f16x2(c[0], c[1]), hb = silu_half_f16x2(c[2], c[3]);
         h2[nt >> 1][(nt & 1) * 2 + 0] = ha;
         h2[nt >> 1][(nt & 1) * 2 + 1] = hb;
         store_pair_t(S.h2t, c0, ra, ha);
@@ -281,7 +290,7 @@ __global__ void __launch_bounds__(kTrainThreads, 1)
 #pragma unroll
       for (int kt = 0; kt < 4; kt++) {
         const uint2 b = S.f3[kt * 32 + lane];
-        mma_bf16(c3, h2[kt], b.x, b.y);
+        mma_f16(c3, h2[kt], b.x, b.y);
       }
       // loss and dY on the lanes holding output columns 0 and 1
       float dyl[4] = {0.0f, 0.0f, 0.0f, 0.0f};
@@ -375,7 +384,7 @@ __global__ void __launch_bounds__(kTrainThreads, 1)
       // dW3[o][n] = sum_k dY[k][o] H2[k][n] and db3 (FP32, sample order)
       const int o = tid >> 6, n = tid & 63;
       for (int kk = 0; kk < kTileRows; kk++)
-        acc_w3 = __fadd_rn(acc_w3, __fmul_rn(S.dy[kk][o], __bfloat162float(S.h2t[n][kk])));
+        acc_w3 = __fadd_rn(acc_w3, __fmul_rn(S.dy[kk][o], __half2float(S.h2t[n][kk])));
       if (tid < kOut)
         for (int kk = 0; kk < kTileRows; kk++) acc_b3 = __fadd_rn(acc_b3, S.dy[kk][tid]);
     }

@@ -1,5 +1,6 @@
-// Per-particle closure network: 16 -> 64 -> 64 -> 2, SiLU, BF16 weights and
-// activations on the tensor cores (mma.sync m16n8k16, FP32 accumulate).
+// Per-particle closure network: 16 -> 64 -> 64 -> 2, SiLU, on the tensor
+// cores (mma.sync m16n8k16, FP32 accumulate): layer 1 on BF16 inputs and
+// weights, layers 2 and 3 on FP16 activations and weights.
 //
 // Layout conventions shared by the inference path (fused into the coarse
 // force pass), the standalone forward kernel and the training kernels:
@@ -8,16 +9,16 @@
 //     (W[out][in]; z = W x + b)
 //   normalisation: mu[16] | isd[16] | out_scale[2]; the network sees
 //     x_hat = bf16((x - mu) * isd) and the caller gets y * out_scale.
-//   weight fragment images (BF16, the B operand of m16n8k16 in register
-//   order): one uint2 per lane per (k-tile, n-tile), so a warp loads a whole
-//   B fragment with one conflict-free 64-bit shared-memory read per lane.
-//     F1  B(k, n) = W1[n][k] / 2   1 k-tile  x 8 n-tiles
-//     F2  B(k, n) = W2[n][k] / 2   4 k-tiles x 8 n-tiles
-//     F3  B(k, n) = W3[n][k]       4 k-tiles x 1 n-tile (outputs 2..7 are zero)
-//     F2T B(k, n) = W2[k][n]       4 k-tiles x 8 n-tiles (backward dH1 = dZ2 W2)
+//   weight fragment images (the B operand of m16n8k16 in register order):
+//   one uint2 per lane per (k-tile, n-tile), so a warp loads a whole B
+//   fragment with one conflict-free 64-bit shared-memory read per lane.
+//     F1  B(k, n) = W1[n][k] / 2   BF16, 1 k-tile  x 8 n-tiles
+//     F2  B(k, n) = W2[n][k] / 2   FP16, 4 k-tiles x 8 n-tiles
+//     F3  B(k, n) = W3[n][k]       FP16, 4 k-tiles x 1 n-tile (outputs 2..7 are zero)
+//     F2T B(k, n) = W2[k][n]       BF16, 4 k-tiles x 8 n-tiles (backward dH1 = dZ2 W2)
 //   The hidden layers run on halved weights and biases, so their accumulators
 //   hold u = z / 2 (exact: a power-of-two scale commutes with the rounding)
-//   and the activation is silu(z) = u + u tanh(u) (silu_half_bf16x2). Each
+//   and the activation is silu(z) = u + u tanh(u) (silu_half_f16x2). Each
 //   layer's bias is the accumulator's initial value.
 //
 // m16n8k16 register layout (PTX ISA, "Matrix Fragments for mma.m16n8k16"),
@@ -26,13 +27,14 @@
 //     cols; a2 = row g, cols 2t+8..2t+9; a3 = row g+8, cols 2t+8..2t+9
 //   B (16x8): b0 = k 2t..2t+1, col g; b1 = k 2t+8..2t+9, col g
 //   C (16x8, f32): c0, c1 = row g, cols 2t, 2t+1; c2, c3 = row g+8
-// The C fragments of n-tiles 2j and 2j+1 are, packed to BF16 pairs, exactly
+// The C fragments of n-tiles 2j and 2j+1 are, packed to FP16 pairs, exactly
 // the A fragment of k-tile j of the next layer, so hidden activations stay in
 // registers between layers.
 #pragma once
 
 #include <cstdint>
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 namespace phieng {
@@ -74,6 +76,14 @@ __host__ __device__ inline uint32_t frag_pos(int k, int n, int nt_count) {
   return (uint32_t)(((((kt * nt_count + nt) * 32 + lane) * 2 + reg) * 2) + half);
 }
 
+__device__ __forceinline__ void mma_f16(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
 __device__ __forceinline__ void mma_bf16(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
   // volatile keeps the MMAs in program order: without it the compiler hoists
   // every fragment load ahead and spills
@@ -101,13 +111,19 @@ __device__ __forceinline__ float tanh_hw(float x) {
 __device__ __forceinline__ float sigmoid_hw(float z) { return __fadd_rn(__fmul_rn(0.5f, tanh_hw(__fmul_rn(0.5f, z))), 0.5f); }
 
 // Activation of two hidden units from their halved pre-activations u = z / 2,
-// packed as a BF16 pair (first unit in the low half):
+// as an FP16 pair (first unit in the low half):
 //   silu(z) = z sigmoid(z) = z (1 + tanh(z / 2)) / 2 = u + u tanh(u)
-// one hardware tanh and one fused multiply-add per unit in FP32, then one
-// conversion per pair. (BF16 arithmetic would be cheaper still, but a BF16
-// tanh near -1 loses 1 + tanh(u) to cancellation: ~6 % output error.)
-__device__ __forceinline__ uint32_t silu_half_bf16x2(float u0, float u1) {
-  return pack_bf16(__fmaf_rn(u0, tanh_hw(u0), u0), __fmaf_rn(u1, tanh_hw(u1), u1));
+// u converted to FP16 (saturating at +-65504, so the result stays finite),
+// then PTX tanh.approx.f16x2 and one fma.rn.f16x2: three instructions and one
+// special-function op per pair, where FP32 takes two special-function ops.
+// FP16 keeps 1 + tanh(u) near u << 0 to about the FP32 tanh.approx error;
+// BF16 there loses it to cancellation (~6 % output error).
+__device__ __forceinline__ uint32_t silu_half_f16x2(float u0, float u1) {
+  uint32_t u, t, h;
+  asm("cvt.rn.satfinite.f16x2.f32 %0, %1, %2;" : "=r"(u) : "f"(u1), "f"(u0));
+  asm("tanh.approx.f16x2 %0, %1;" : "=r"(t) : "r"(u));
+  asm("fma.rn.f16x2 %0, %1, %2, %1;" : "=r"(h) : "r"(u), "r"(t));
+  return h;
 }
 // d silu / dz = s + z s (1 - s)
 __device__ __forceinline__ float dsilu_hw(float z) {
@@ -159,8 +175,8 @@ __device__ __forceinline__ void mlp_tile_forward(const __nv_bfloat16* xs, int ld
     float c[4] = {bb.x, bb.y, bb.x, bb.y};
     const uint2 b = s.f1[nt * 32 + lane];
     mma_bf16(c, a, b.x, b.y);
-    h[nt >> 1][(nt & 1) * 2 + 0] = silu_half_bf16x2(c[0], c[1]);
-    h[nt >> 1][(nt & 1) * 2 + 1] = silu_half_bf16x2(c[2], c[3]);
+    h[nt >> 1][(nt & 1) * 2 + 0] = silu_half_f16x2(c[0], c[1]);
+    h[nt >> 1][(nt & 1) * 2 + 1] = silu_half_f16x2(c[2], c[3]);
   }
   const float b30 = t == 0 ? s.bias[2 * kHidden] : 0.0f;
   const float b31 = t == 0 ? s.bias[2 * kHidden + 1] : 0.0f;
@@ -169,25 +185,35 @@ __device__ __forceinline__ void mlp_tile_forward(const __nv_bfloat16* xs, int ld
   y[2] = b30;
   y[3] = b31;
   // layer 2 two n-tiles at a time, each pair (one k-tile of layer 3) fed to
-  // the output straight away: 4 live activation registers instead of 16
+  // the output straight away: 4 live activation registers instead of 16. The
+  // pair's two accumulation chains alternate (k outer), so each MMA waits on
+  // the one two issues back.
 #pragma unroll
   for (int j = 0; j < 4; j++) {
+    float c[2][4];
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+      const float2 bb = *reinterpret_cast<const float2*>(&s.bias[kHidden + (2 * j + q) * 8 + 2 * t]);
+      c[q][0] = bb.x;
+      c[q][1] = bb.y;
+      c[q][2] = bb.x;
+      c[q][3] = bb.y;
+    }
+#pragma unroll
+    for (int kt = 0; kt < 4; kt++)
+#pragma unroll
+      for (int q = 0; q < 2; q++) {
+        const uint2 b = s.f2[(kt * 8 + 2 * j + q) * 32 + lane];
+        mma_f16(c[q], h[kt], b.x, b.y);
+      }
     uint32_t h2[4];
 #pragma unroll
     for (int q = 0; q < 2; q++) {
-      const int nt = 2 * j + q;
-      const float2 bb = *reinterpret_cast<const float2*>(&s.bias[kHidden + nt * 8 + 2 * t]);
-      float c[4] = {bb.x, bb.y, bb.x, bb.y};
-#pragma unroll
-      for (int kt = 0; kt < 4; kt++) {
-        const uint2 b = s.f2[(kt * 8 + nt) * 32 + lane];
-        mma_bf16(c, h[kt], b.x, b.y);
-      }
-      h2[q * 2 + 0] = silu_half_bf16x2(c[0], c[1]);
-      h2[q * 2 + 1] = silu_half_bf16x2(c[2], c[3]);
+      h2[q * 2 + 0] = silu_half_f16x2(c[q][0], c[q][1]);
+      h2[q * 2 + 1] = silu_half_f16x2(c[q][2], c[q][3]);
     }
     const uint2 b = s.f3[j * 32 + lane];
-    mma_bf16(y, h2, b.x, b.y);
+    mma_f16(y, h2, b.x, b.y);
   }
 }
 
