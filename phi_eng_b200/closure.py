@@ -564,6 +564,7 @@ def _main(argv=None) -> None:
     t.add_argument("--target", choices=list(TARGETS) + ["damped"], default="damped")
     t.add_argument("--damp", default="0.75,1.0", help="damped target: the range of the pressure damping")
     t.add_argument("--track-rounds", type=int, default=0)
+    t.add_argument("--ratio", type=int, default=4, help="coarse step = ratio * dt")
     e = sub.add_parser("eval")
     e.add_argument("--weights", default=WEIGHTS)
     e.add_argument("--workload", default="dam_break_1m", choices=["dam_break_1m", "dam_break_4k"])
@@ -571,12 +572,14 @@ def _main(argv=None) -> None:
     e.add_argument("--threshold", type=float, default=0.03)
     e.add_argument("--criterion", choices=["jump", "compression", "growth"], default="jump")
     e.add_argument("--zero", action="store_true", help="evaluate a zero network (no correction)")
+    e.add_argument("--ratio", type=int, default=0, help="coarse step = ratio * dt (0: the weights' own ratio)")
     a = ap.parse_args(argv)
     if a.cmd == "train":
         from .batch import batched_scenes
 
         noise = tuple(float(v) for v in a.noise.split(","))
-        mlp, info = train_closure(batched_scenes(a.scenes), samples=a.samples, every=a.every, batch=a.batch,
+        mlp, info = train_closure(batched_scenes(a.scenes), ratio=a.ratio, samples=a.samples, every=a.every,
+                                  batch=a.batch,
                                   iters=a.iters, lr=a.lr, seed=a.seed, noise=noise, dagger_iters=a.dagger_iters,
                                   rollout=a.rollout, target=a.target, track_rounds=a.track_rounds,
                                   damp=tuple(float(v) for v in a.damp.split(",")), log=None)
@@ -587,7 +590,13 @@ def _main(argv=None) -> None:
     sc = S.dam_break_1m() if a.workload == "dam_break_1m" else S.dam_break_4k()
     mlp = Mlp() if a.zero else Mlp.load(a.weights)
     crit = {"jump": _abi.CLOSURE_JUMP, "compression": _abi.CLOSURE_COMPRESSION, "growth": _abi.CLOSURE_GROWTH}[a.criterion]
-    r = evaluate(sc, mlp, coarse_steps=a.coarse_steps, threshold=a.threshold, criterion=crit)
+    ratio = a.ratio
+    if ratio <= 0:
+        ratio = 4
+        if not a.zero:
+            with np.load(a.weights) as z:
+                ratio = int(z["ratio"]) if "ratio" in z.files else 4
+    r = evaluate(sc, mlp, coarse_steps=a.coarse_steps, ratio=ratio, threshold=a.threshold, criterion=crit)
     print(json.dumps(dict(workload=a.workload, weights=None if a.zero else a.weights, **r)))
 
 
