@@ -77,6 +77,36 @@ static_assert(offsetof(FluidConfig2Ffi, phase_mass) == 84, "layout");
 static_assert(offsetof(FluidConfig2Ffi, enabled) == 108, "layout");
 #endif
 
+/* 2D ambient-force config, #[repr(C)] mirror of AmbientConfig2Ffi
+ * (ffi.rs:231-276): spring / drag / wind act on rigid bodies only and are
+ * kept for the round trip; the fluid reads the turbulence fields
+ * (fluid.rs:1001-1019). Flags are u32 (0 = off). Size 80, align 4. */
+typedef struct AmbientConfig2Ffi {
+  uint32_t spring_enabled;            /* 0  */
+  float spring_ax, spring_ay;         /* 4  */
+  float spring_stiffness;             /* 12 */
+  float spring_damping;               /* 16 */
+  float spring_max_displacement;      /* 20 */
+  uint32_t drag_enabled;              /* 24 */
+  float drag_linear;                  /* 28 */
+  float drag_quadratic;               /* 32 */
+  float air_density;                  /* 36 */
+  float drag_angular;                 /* 40 */
+  float wind_x, wind_y;               /* 44 */
+  uint32_t turbulence_enabled;        /* 52 */
+  float turbulence_amplitude;         /* 56 */
+  float turbulence_frequency;         /* 60 */
+  float turbulence_time_scale;        /* 64 */
+  uint32_t turbulence_seed;           /* 68 */
+  uint32_t turbulence_octaves;        /* 72: stored as min(v, 255); the noise clamps to 1..8 */
+  uint32_t turbulence_divergence_free;/* 76 */
+} AmbientConfig2Ffi;
+
+#ifdef __cplusplus
+static_assert(sizeof(AmbientConfig2Ffi) == 80, "AmbientConfig2Ffi must match ffi.rs:231-276");
+static_assert(offsetof(AmbientConfig2Ffi, turbulence_enabled) == 52, "layout");
+#endif
+
 /* ---------------- reference entry points (ffi.rs) ---------------- */
 
 /* ffi.rs:51 phieng_world_new — never returns null. No GPU work happens here;
@@ -97,6 +127,19 @@ void phieng_world_set_gravity(World2* world, float gx, float gy);
 /* ffi.rs:1067 / 1079 world clock. 1 ok, 0 null or non-finite. */
 int32_t phieng_world_set_time(World2* world, float t);
 int32_t phieng_world_get_time(World2* world, float* out);
+
+/* ffi.rs:512 phieng_world_set_ambient_config — 1 ok; 0 for a null world or
+ * config, a non-finite float, or a negative spring stiffness / damping / max
+ * displacement, drag coefficient, air density or turbulence amplitude (world
+ * unchanged). Turbulence (enabled and amplitude > 0) adds the reference's
+ * value-noise acceleration to every particle in the integrate, sampled at
+ * the world clock of the step's start. */
+int32_t phieng_world_set_ambient_config(World2* world, const AmbientConfig2Ffi* cfg);
+
+/* ffi.rs:533 phieng_world_get_ambient_config — 1 ok, 0 for null world / out.
+ * A new world holds the reference's defaults (ambient.rs: everything off,
+ * air density 1, turbulence frequency 1, time scale 1, 3 octaves). */
+int32_t phieng_world_get_ambient_config(World2* world, AmbientConfig2Ffi* out);
 
 /* ffi.rs:1123 body count, -1 for null. */
 int32_t phieng_world_body_count(World2* world);

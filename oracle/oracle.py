@@ -43,6 +43,8 @@ def _load():
         "orc_set_config": (None, [P, C.POINTER(FluidConfig2Ffi)]),
         "orc_get_config": (None, [P, C.POINTER(FluidConfig2Ffi)]),
         "orc_set_gravity": (None, [P, C.c_float, C.c_float]),
+        "orc_set_turbulence": (None, [P, C.c_int, C.c_float, C.c_float, C.c_float, C.c_uint32, C.c_uint32, C.c_int]),
+        "orc_noise2": (None, [C.c_int, C.c_float, C.c_float, C.c_float, C.c_uint32, C.c_uint32, C.POINTER(C.c_float)]),
         "orc_set_cap": (None, [P, C.c_uint32]),
         "orc_set_pow_mode": (None, [P, C.c_int]),
         "orc_add_body": (None, [P, C.c_int, C.c_float, C.c_float, C.c_float, C.c_float,
@@ -149,6 +151,13 @@ class OracleWorld:
 
     def set_gravity(self, gx: float, gy: float) -> None:
         self._l.orc_set_gravity(self._h, gx, gy)
+
+    def set_turbulence(self, amplitude: float, frequency: float = 1.0, time_scale: float = 1.0, seed: int = 0,
+                       octaves: int = 3, divergence_free: bool = False, enabled: bool = True) -> None:
+        """world.ambient.turbulence (ambient.rs:108-126), read by the integrate
+        at the world clock of each step's start."""
+        self._l.orc_set_turbulence(self._h, 1 if enabled else 0, amplitude, frequency, time_scale,
+                                   seed & 0xFFFFFFFF, octaves, 1 if divergence_free else 0)
 
     def set_cap(self, cap: int) -> None:
         self._l.orc_set_cap(self._h, cap)
@@ -408,3 +417,12 @@ def cohesion(dist: float, h: float) -> float:
 
 
 __all__ = ["OracleWorld", "OracleWorld3", "REF_SEQ", "JACOBI", "default_config", "build", "lib"]
+
+
+def noise2(kind: str, x: float, y: float, t: float = 0.0, seed: int = 0, octaves: int = 3):
+    """The oracle's f32 restatement of noise.rs: kind "value" (value_noise_2),
+    "fbm" (fbm_2) or "curl" (curl_2, a pair)."""
+    out = (C.c_float * 2)()
+    k = {"value": 0, "fbm": 1, "curl": 2}[kind]
+    _load().orc_noise2(k, x, y, t, seed & 0xFFFFFFFF, octaves, out)
+    return (out[0], out[1]) if k == 2 else out[0]

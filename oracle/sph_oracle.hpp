@@ -29,6 +29,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <limits>
 #include <unordered_map>
 #include <vector>
 
@@ -179,6 +180,111 @@ inline double rpow<double>(double a, double b, int) {
   return pow(a, b);
 }
 
+// ---- ambient turbulence (crates/dynamics/src/noise.rs, fluid.rs:1001-1019) ----
+struct Turbulence {
+  bool on = false;  // enabled && amplitude > 0 (fluid.rs:1002)
+  float amp = 0, freq = 1, tscale = 1;
+  uint32_t seed = 0, oct = 3;  // octaves as stored (u8); clamped to 1..8 where used
+  bool curl = false;
+};
+
+// integer avalanche hash (noise.rs:27-35)
+inline uint32_t nz_hash(uint32_t x) {
+  x ^= x >> 16;
+  x *= 0x7feb352du;
+  x ^= x >> 15;
+  x *= 0x846ca68bu;
+  x ^= x >> 16;
+  return x;
+}
+
+// Rust's `f as i32` / `f as i64`: truncate, saturate, NaN -> 0
+template <class I, class R>
+inline I rust_as_int(R v) {
+  if (v != v) return 0;
+  const R lo = (R)std::numeric_limits<I>::min(), hi = (R)std::numeric_limits<I>::max();
+  if (v <= lo) return std::numeric_limits<I>::min();
+  if (v >= hi) return std::numeric_limits<I>::max();
+  return (I)v;
+}
+
+template <class R>
+inline R nz_lattice(int32_t ix, int32_t iy, uint32_t seed) {  // noise.rs:38-47
+  const uint32_t h = nz_hash((uint32_t)ix * 0x1f1f1f1fu + (uint32_t)iy * 0x9e3779b9u + seed);
+  return (R)(h >> 8) * (R)(1.0f / 16777216.0f);
+}
+
+template <class R>
+inline R nz_fade(R t) {  // noise.rs:64-67
+  return t * t * t * (t * (t * (R)6 - (R)15) + (R)10);
+}
+
+template <class R>
+inline R nz_lerp(R a, R b, R t) {
+  return a + (b - a) * t;
+}
+
+template <class R>
+inline R nz_value2(R x, R y, uint32_t seed) {  // noise.rs:75-87
+  const R x0 = std::floor(x), y0 = std::floor(y);
+  const int32_t xi = rust_as_int<int32_t>(x0), yi = rust_as_int<int32_t>(y0);
+  const R tx = nz_fade(x - x0), ty = nz_fade(y - y0);
+  const int32_t xi1 = (int32_t)((uint32_t)xi + 1u), yi1 = (int32_t)((uint32_t)yi + 1u);
+  const R v00 = nz_lattice<R>(xi, yi, seed), v10 = nz_lattice<R>(xi1, yi, seed);
+  const R v01 = nz_lattice<R>(xi, yi1, seed), v11 = nz_lattice<R>(xi1, yi1, seed);
+  return nz_lerp(nz_lerp(v00, v10, tx), nz_lerp(v01, v11, tx), ty);
+}
+
+template <class R>
+inline R nz_fbm2_static(R x, R y, uint32_t seed, uint32_t oct) {  // noise.rs:115-132
+  R sum = 0, amp = 1, freq = 1, norm = 0;
+  for (uint32_t o = 0; o < oct; o++) {
+    sum += amp * (nz_value2(x * freq, y * freq, seed + o) * (R)2 - (R)1);
+    norm += amp;
+    amp *= (R)0.5;
+    freq *= (R)2;
+  }
+  return norm > (R)0 ? sum / norm : (R)0;
+}
+
+template <class R>
+inline R nz_fbm2(R x, R y, R t, uint32_t seed, uint32_t octaves) {  // noise.rs:160-170
+  const uint32_t oct = std::min<uint32_t>(std::max<uint32_t>(octaves, 1u), 8u);
+  const R t0 = std::floor(t);
+  const R ft = nz_fade(t - t0);
+  const int64_t sl = rust_as_int<int64_t>(t0);
+  const uint32_t s0 = seed + (uint32_t)sl * 0x9e3779b9u;
+  const uint32_t s1 = seed + (uint32_t)((uint64_t)sl + 1u) * 0x9e3779b9u;
+  return nz_lerp(nz_fbm2_static(x, y, s0, oct), nz_fbm2_static(x, y, s1, oct), ft);
+}
+
+// acceleration added at (px, py) and clock `time` (fluid.rs:1007-1018);
+// clamp_length_max(1.0) as glam 0.29 (v / sqrt(|v|^2) when |v|^2 > 1)
+template <class R>
+inline void turbulence_accel(const Turbulence& tb, R px, R py, R time, R& ax, R& ay) {
+  const R x = px * (R)tb.freq, y = py * (R)tb.freq;
+  const R t = time * (R)tb.tscale;
+  R nx, ny;
+  if (tb.curl) {  // noise.rs:186-193
+    const R e = (R)1e-3f, e2 = (R)(2.0f * 1e-3f);
+    const R dpdy = (nz_fbm2(x, y + e, t, tb.seed, tb.oct) - nz_fbm2(x, y - e, t, tb.seed, tb.oct)) / e2;
+    const R dpdx = (nz_fbm2(x + e, y, t, tb.seed, tb.oct) - nz_fbm2(x - e, y, t, tb.seed, tb.oct)) / e2;
+    nx = dpdy;
+    ny = -dpdx;
+  } else {
+    nx = nz_fbm2(x, y, t, tb.seed, tb.oct);
+    ny = nz_fbm2(x, y, t, tb.seed ^ 0x55aa55aau, tb.oct);
+  }
+  const R ls = nx * nx + ny * ny;
+  if (ls > (R)1) {
+    const R l = std::sqrt(ls);
+    nx = nx / l;
+    ny = ny / l;
+  }
+  ax = ax + nx * (R)tb.amp;
+  ay = ay + ny * (R)tb.amp;
+}
+
 template <class R>
 class Fluid {
  public:
@@ -187,6 +293,7 @@ class Fluid {
   std::vector<Body> bodies;
   R gx = (R)0.0f, gy = (R)-9.81f;  // World2::new gravity (world.rs:338)
   R time = 0;
+  Turbulence turb;    // world.ambient.turbulence
   size_t cap = 4096;  // MAX_PARTICLES_2D (fluid.rs:30); lifted by the caller
   int pow_mode = 1;   // see powf_cr
 
@@ -390,6 +497,7 @@ class Fluid {
         ax = ax + extra_ax[i];
         ay = ay + extra_ay[i];
       }
+      if (turb.on) turbulence_accel(turb, src[i].x, src[i].y, time, ax, ay);
       R vx = src[i].vx + ax * dt;
       R vy = src[i].vy + ay * dt;
       if (visc > (R)0) {

@@ -131,6 +131,38 @@ void orc_set_gravity(void* h, float gx, float gy) {
   o->f64.gy = (double)gy;
 }
 
+// world.ambient.turbulence (TurbulenceConfig2, ambient.rs:108-126)
+void orc_set_turbulence(void* h, int enabled, float amp, float freq, float tscale, uint32_t seed, uint32_t octaves,
+                        int divergence_free) {
+  Orc* o = static_cast<Orc*>(h);
+  oracle::Turbulence t;
+  t.on = enabled != 0 && amp > 0.0f;
+  t.amp = amp;
+  t.freq = freq;
+  t.tscale = tscale;
+  t.seed = seed;
+  t.oct = std::min<uint32_t>(octaves, 255u);
+  t.curl = divergence_free != 0;
+  o->f32.turb = t;
+  o->f64.turb = t;
+}
+
+// noise.rs entry points in f32, for the restatement's own tests: kind 0
+// value_noise_2(x, y, seed) -> out[0]; 1 fbm_2(x, y, t, seed, octaves) ->
+// out[0]; 2 curl_2(x, y, t, seed, octaves) -> out[0..1]
+void orc_noise2(int kind, float x, float y, float t, uint32_t seed, uint32_t octaves, float* out) {
+  if (kind == 0) {
+    out[0] = oracle::nz_value2<float>(x, y, seed);
+  } else if (kind == 1) {
+    out[0] = oracle::nz_fbm2<float>(x, y, t, seed, std::min<uint32_t>(octaves, 255u));
+  } else {
+    const uint32_t oct = std::min<uint32_t>(octaves, 255u);
+    const float e = 1e-3f, e2 = 2.0f * 1e-3f;  // noise.rs:189-192
+    out[0] = (oracle::nz_fbm2<float>(x, y + e, t, seed, oct) - oracle::nz_fbm2<float>(x, y - e, t, seed, oct)) / e2;
+    out[1] = -((oracle::nz_fbm2<float>(x + e, y, t, seed, oct) - oracle::nz_fbm2<float>(x - e, y, t, seed, oct)) / e2);
+  }
+}
+
 // 1 = correctly rounded power (the GPU's), 0 = the platform libm powf
 void orc_set_pow_mode(void* h, int mode) {
   Orc* o = static_cast<Orc*>(h);

@@ -46,6 +46,8 @@ enum StepFlags : uint32_t {
   F_PHASE = 1u << 6,     // per-particle phase array (non-uniform rest density)
   F_DYNAMIC = 1u << 7,   // bodies with impulses or velocity: their contacts run in the ordered pass
   F_WIDE_NB = 1u << 8,   // h*h > max(h, EPS)^2 (h <= 0 from a snapshot): poly6 keeps its range test for neighbours
+  F_TURB = 1u << 9,      // ambient turbulence on (enabled and amplitude > 0)
+  F_TURB_CURL = 1u << 10,  // turbulence as divergence-free curl noise
 };
 
 struct StepParams {
@@ -74,6 +76,10 @@ struct StepParams {
   uint32_t nbodies;
   uint32_t body_first;     // first of this scene's bodies in the body array
   uint32_t uniform_phase;  // phase used for every particle when !F_PHASE
+  // ambient turbulence (F_TURB; TurbulenceConfig2, ambient.rs:108-126)
+  float turb_amp, turb_freq, turb_tscale;
+  uint32_t turb_seed, turb_oct;  // octaves already clamped to 1..8
+  const float* clock;            // device word holding the world clock of the current step
 };
 
 // Per-launch scene access: a single world passes its parameters by value

@@ -19,6 +19,7 @@
 #include <cuda_runtime.h>
 
 #include "sph_kernels.h"
+#include "sph_noise.cuh"
 #include "sph_warp.cuh"
 
 namespace phieng {
@@ -589,12 +590,20 @@ __device__ __forceinline__ void neighbour_sums(uint32_t s, uint32_t k, uint32_t 
 
 // integrate (fluid.rs:1003-1050) from acceleration (ax, ay) and the XSPH sum,
 // then the wall pass; writes the new state, the next key and its bucket count.
+// Ambient turbulence (F_TURB) joins the acceleration first, at the particle's
+// pre-step position and the step's world clock.
 __device__ __forceinline__ void integrate_write(uint32_t id, float2 pi, float2 vi, float ax, float ay, float sx,
                                                 float sy, const StepParams& P, const DevBody* __restrict__ bodies,
                                                 float4* __restrict__ state_out, uint32_t* __restrict__ key_out,
                                                 uint32_t* __restrict__ count_out,
                                                 uint32_t* __restrict__ defer = nullptr,
                                                 uint32_t* __restrict__ dcount = nullptr) {
+  if (P.flags & F_TURB) {
+    const float2 tb = turbulence_accel(pi.x, pi.y, *P.clock, P.turb_freq, P.turb_tscale, P.turb_seed, P.turb_oct,
+                                       P.flags & F_TURB_CURL, P.turb_amp);
+    ax = __fadd_rn(ax, tb.x);
+    ay = __fadd_rn(ay, tb.y);
+  }
   float vx = __fadd_rn(vi.x, __fmul_rn(ax, P.dt));
   float vy = __fadd_rn(vi.y, __fmul_rn(ay, P.dt));
   if (P.flags & F_VISC) {
@@ -1079,6 +1088,10 @@ __global__ void k_check_fold(const unsigned int* __restrict__ out, float* __rest
 void enqueue_check_fold(const unsigned int* out, float* acc, bool reset, cudaStream_t st) {
   k_check_fold<<<1, 32, 0, st>>>(out, acc, reset ? 1 : 0);
 }
+
+__global__ void k_set_word(unsigned int* p, unsigned int v) { *p = v; }
+
+void enqueue_set_word(unsigned int* p, uint32_t v, cudaStream_t st) { k_set_word<<<1, 1, 0, st>>>(p, v); }
 
 void enqueue_closure_check(const FluidBufs& b, uint32_t n, const StepParams& P, const float* rho_prev,
                            unsigned int* out, cudaStream_t st) {

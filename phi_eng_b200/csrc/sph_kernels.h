@@ -169,6 +169,11 @@ void enqueue_scan_silent_tile(const FluidBufs& b, uint32_t m, cudaStream_t st);
 // the block maxima acc[0..2] (jump, compression, growth), or reset them.
 void enqueue_check_fold(const unsigned int* out, float* acc, bool reset, cudaStream_t st);
 
+// *p = v, in stream order (the value travels as a launch argument, so the
+// host may reuse its copy at once): the world clock word read by the
+// turbulence term of cached step graphs.
+void enqueue_set_word(unsigned int* p, uint32_t v, cudaStream_t st);
+
 // Scatter the sorted density / pressure back to id order.
 void enqueue_unsort_dp(const FluidBufs& b, uint32_t n, float* dens, float* pres, cudaStream_t st);
 

@@ -26,10 +26,24 @@ using namespace phieng;
 namespace {
 using namespace phieng::host;
 constexpr uint32_t kMaxParticles2D = 4096;  // MAX_PARTICLES_2D (fluid.rs:30)
+constexpr uint32_t kClockWord = 16;         // scalar word holding the step's world clock (turbulence)
+
+// AmbientConfig2::default (ambient.rs): springs, drag and turbulence off, air
+// density 1, turbulence frequency 1, time scale 1, 3 octaves.
+AmbientConfig2Ffi default_ambient() {
+  AmbientConfig2Ffi a;
+  std::memset(&a, 0, sizeof(a));
+  a.air_density = 1.0f;
+  a.turbulence_frequency = 1.0f;
+  a.turbulence_time_scale = 1.0f;
+  a.turbulence_octaves = 3;
+  return a;
+}
 }  // namespace
 
 struct World2 {
   FluidConfig2Ffi cfg = default_config();
+  AmbientConfig2Ffi ambient = default_ambient();
   float gx = 0.0f, gy = -9.81f;  // World2::new (world.rs:338)
   float time = 0.0f;
   std::vector<DevBody> bodies;
@@ -204,8 +218,8 @@ bool ensure_device(World2* w) {
   if (!cuda_ok(w, cudaStreamCreateWithFlags(&w->own_stream, cudaStreamNonBlocking), "cudaStreamCreate"))
     return false;
   if (!w->user_stream) w->stream = w->own_stream;
-  if (!cuda_ok(w, cudaMalloc(&w->d.scalar, 64), "cudaMalloc(scalar)")) return false;
-  if (!cuda_ok(w, cudaMemset(w->d.scalar, 0, 64), "cudaMemset(scalar)")) return false;
+  if (!cuda_ok(w, cudaMalloc(&w->d.scalar, 128), "cudaMalloc(scalar)")) return false;
+  if (!cuda_ok(w, cudaMemset(w->d.scalar, 0, 128), "cudaMemset(scalar)")) return false;
   w->d.done = w->d.scalar + 8;       // scan counters [8], [9]
   w->d.scan_err = w->d.scalar + 12;  // set when a scan's look-back wait gave up
   if (!cuda_ok(w, cudaMallocHost(&w->h_pinned, 64), "cudaMallocHost")) return false;
@@ -532,10 +546,39 @@ StepParams make_params_for(const FluidConfig2Ffi& c, float gx, float gy, bool ma
   return P;
 }
 
+// Ambient turbulence of a single world (fluid.rs:1001-1002: on when enabled
+// with a positive amplitude). The kernels read the step's clock from a device
+// word (set_clock), so cached graphs stay valid as the clock advances.
+void apply_ambient(const World2* w, StepParams& P) {
+  const AmbientConfig2Ffi& a = w->ambient;
+  if (!(a.turbulence_enabled != 0 && a.turbulence_amplitude > 0.0f) || !w->d.scalar) return;
+  P.flags |= F_TURB;
+  if (a.turbulence_divergence_free) P.flags |= F_TURB_CURL;
+  P.turb_amp = a.turbulence_amplitude;
+  P.turb_freq = a.turbulence_frequency;
+  P.turb_tscale = a.turbulence_time_scale;
+  P.turb_seed = a.turbulence_seed;
+  P.turb_oct = std::min<uint32_t>(std::max<uint32_t>(a.turbulence_octaves, 1u), 8u);  // (octaves as u32).clamp(1, 8)
+  P.clock = reinterpret_cast<const float*>(w->d.scalar + kClockWord);
+}
+
+// The clock the next substeps' turbulence reads (the world time at the start
+// of the step, fluid.rs:1009 with world.rs:848), in stream order.
+void set_clock(World2* w, const StepParams& P, float t) {
+  if (P.flags & F_TURB) {
+    uint32_t bits;
+    std::memcpy(&bits, &t, 4);
+    enqueue_set_word(w->d.scalar + kClockWord, bits, w->stream);
+  }
+}
+
 StepParams make_params(const World2* w, float dt) {
-  if (!w->is_batch())
-    return make_params_for(w->cfg, w->gx, w->gy, w->mass_uniform, w->mass_value, w->phase_uniform, w->phase_value,
-                           w->plan, 0, (uint32_t)w->bodies.size(), dt);
+  if (!w->is_batch()) {
+    StepParams P = make_params_for(w->cfg, w->gx, w->gy, w->mass_uniform, w->mass_value, w->phase_uniform,
+                                   w->phase_value, w->plan, 0, (uint32_t)w->bodies.size(), dt);
+    apply_ambient(w, P);
+    return P;
+  }
   // batch: the kernels read each scene's row of the device table; the launch
   // parameters carry the union of the per-particle array flags and the
   // global key range
@@ -672,6 +715,7 @@ bool world_step(World2* w, float dt) {
     if (!cfl_substeps(w, dt, &ns)) return false;
     const float sub = dt / (float)ns;
     const StepParams P = make_params(w, sub);
+    set_clock(w, P, w->time);  // every CFL substep sees the step's start time
     for (uint32_t k = 0; k < ns; k++)
       if (!run_substep(w, P)) return false;
   }
@@ -867,6 +911,8 @@ bool step_fluid_bodies(World2* w, PhiengBody2* bodies, uint32_t nb, float dt) {
   StepParams P = make_params_for(w->cfg, w->gx, w->gy, w->mass_uniform, w->mass_value, w->phase_uniform,
                                  w->phase_value, w->plan, 0, nb, sub);
   if (any_dyn) P.flags |= F_DYNAMIC;
+  apply_ambient(w, P);
+  set_clock(w, P, w->time);
   FluidBufs dB = w->d;
   dB.bodies = w->d_cbodies;
   const float drag = rmaxf(w->cfg.drag, 0.0f);
@@ -1079,6 +1125,35 @@ int32_t phieng_world_set_time(World2* w, float t) {
 int32_t phieng_world_get_time(World2* w, float* out) {
   if (!w || !out) return 0;
   *out = w->time;
+  return 1;
+}
+
+int32_t phieng_world_set_ambient_config(World2* w, const AmbientConfig2Ffi* cfg) {
+  if (!w || !cfg) return 0;
+  const AmbientConfig2Ffi& c = *cfg;
+  // ambient2_from_ffi (ffi.rs:328-386): finite floats, non-negative
+  // coefficients, octaves stored as min(v, 255)
+  for (float v : {c.spring_ax, c.spring_ay, c.spring_stiffness, c.spring_damping, c.spring_max_displacement,
+                  c.drag_linear, c.drag_quadratic, c.air_density, c.drag_angular, c.wind_x, c.wind_y,
+                  c.turbulence_amplitude, c.turbulence_frequency, c.turbulence_time_scale})
+    if (!std::isfinite(v)) return 0;
+  if (c.spring_stiffness < 0.0f || c.spring_damping < 0.0f || c.spring_max_displacement < 0.0f ||
+      c.drag_linear < 0.0f || c.drag_quadratic < 0.0f || c.air_density < 0.0f || c.drag_angular < 0.0f ||
+      c.turbulence_amplitude < 0.0f)
+    return 0;
+  AmbientConfig2Ffi a = c;
+  a.spring_enabled = c.spring_enabled != 0;
+  a.drag_enabled = c.drag_enabled != 0;
+  a.turbulence_enabled = c.turbulence_enabled != 0;
+  a.turbulence_divergence_free = c.turbulence_divergence_free != 0;
+  a.turbulence_octaves = std::min<uint32_t>(c.turbulence_octaves, 255u);
+  w->ambient = a;
+  return 1;
+}
+
+int32_t phieng_world_get_ambient_config(World2* w, AmbientConfig2Ffi* out) {
+  if (!w || !out) return 0;
+  *out = w->ambient;
   return 1;
 }
 
@@ -1590,7 +1665,10 @@ int32_t phieng_sph_closure_step(World2* w, float dt_fine, uint32_t coarse_steps,
                    "block save"))
         return 0;
       enqueue_check_fold(w->d.scalar + 4, acc, true, w->stream);
+      float tb = w->time;
       for (uint32_t b = 0; b < nb; b++) {
+        set_clock(w, Pc, tb);
+        tb += dtc;
         if (!run_coarse(w, Pc, mlp, io)) return 0;
         w->sid_perm_n = w->n;
         enqueue_check_fold(w->d.scalar + 4, acc, false, w->stream);
@@ -1631,6 +1709,7 @@ int32_t phieng_sph_closure_step(World2* w, float dt_fine, uint32_t coarse_steps,
     }
     const uint32_t kend = k + nb;
     for (; k < kend; k++) {
+      set_clock(w, Pc, w->time);
       if (!run_coarse(w, Pc, mlp, io)) return 0;
       w->sid_perm_n = w->n;
       if (!cuda_ok(w, cudaMemcpyAsync(w->h_pinned, w->d.scalar + 4, 12, cudaMemcpyDeviceToHost, w->stream), "check") ||
@@ -1660,8 +1739,12 @@ int32_t phieng_sph_closure_step(World2* w, float dt_fine, uint32_t coarse_steps,
         w->keys_valid = false;
         if (!prepare(w)) return 0;
         if (batch && !upload_scene_table(w, dt_fine)) return 0;
-        for (uint32_t r = 0; r < w->closure_ratio; r++)
+        float tf = w->time;
+        for (uint32_t r = 0; r < w->closure_ratio; r++) {
+          set_clock(w, Pf, tf);
+          tf += dt_fine;
           if (!run_substep(w, Pf)) return 0;
+        }
         if (batch && !upload_scene_table(w, dtc)) return 0;
         if (k + 1 < coarse_steps) enqueue_sort_density(w, Pc, w->d_svp);
       }
