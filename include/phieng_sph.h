@@ -551,6 +551,41 @@ int32_t phieng_world3_get_time(World3* world, float* out);
 /* ffi.rs:3387: number of bodies, -1 for null. */
 int32_t phieng_world3_body_count(World3* world);
 
+/* 3D ambient-force config, #[repr(C)] mirror of AmbientConfig3Ffi
+ * (ffi.rs:278-326): as AmbientConfig2Ffi with 3D anchor and wind. Size 88,
+ * align 4. */
+typedef struct AmbientConfig3Ffi {
+  uint32_t spring_enabled;                 /* 0  */
+  float spring_ax, spring_ay, spring_az;   /* 4  */
+  float spring_stiffness;                  /* 16 */
+  float spring_damping;                    /* 20 */
+  float spring_max_displacement;           /* 24 */
+  uint32_t drag_enabled;                   /* 28 */
+  float drag_linear;                       /* 32 */
+  float drag_quadratic;                    /* 36 */
+  float air_density;                       /* 40 */
+  float drag_angular;                      /* 44 */
+  float wind_x, wind_y, wind_z;            /* 48 */
+  uint32_t turbulence_enabled;             /* 60 */
+  float turbulence_amplitude;              /* 64 */
+  float turbulence_frequency;              /* 68 */
+  float turbulence_time_scale;             /* 72 */
+  uint32_t turbulence_seed;                /* 76 */
+  uint32_t turbulence_octaves;             /* 80 */
+  uint32_t turbulence_divergence_free;     /* 84 */
+} AmbientConfig3Ffi;
+
+#ifdef __cplusplus
+static_assert(sizeof(AmbientConfig3Ffi) == 88, "AmbientConfig3Ffi must match ffi.rs:278-326");
+static_assert(offsetof(AmbientConfig3Ffi, turbulence_enabled) == 60, "layout");
+#endif
+
+/* ffi.rs:549 / 568 phieng_world3_set/get_ambient_config — as the 2D pair
+ * (ambient3_from_ffi, ffi.rs:414-475); turbulence acts on the 3D fluid
+ * (fluid3.rs:1090-1108). */
+int32_t phieng_world3_set_ambient_config(World3* world, const AmbientConfig3Ffi* cfg);
+int32_t phieng_world3_get_ambient_config(World3* world, AmbientConfig3Ffi* out);
+
 /* ffi.rs:3703 phieng_world3_add_body — PHIENG_SHAPE3_SPHERE (a = radius),
  * PHIENG_SHAPE3_BOX (a, b, c = half extents), PHIENG_SHAPE3_CAPSULE (a =
  * radius, b = half length along y); at (pos_x, pos_y, pos_z) with the

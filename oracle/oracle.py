@@ -44,6 +44,7 @@ def _load():
         "orc_get_config": (None, [P, C.POINTER(FluidConfig2Ffi)]),
         "orc_set_gravity": (None, [P, C.c_float, C.c_float]),
         "orc_set_turbulence": (None, [P, C.c_int, C.c_float, C.c_float, C.c_float, C.c_uint32, C.c_uint32, C.c_int]),
+        "orc3_set_turbulence": (None, [P, C.c_int, C.c_float, C.c_float, C.c_float, C.c_uint32, C.c_uint32, C.c_int]),
         "orc_noise2": (None, [C.c_int, C.c_float, C.c_float, C.c_float, C.c_uint32, C.c_uint32, C.POINTER(C.c_float)]),
         "orc_set_cap": (None, [P, C.c_uint32]),
         "orc_set_pow_mode": (None, [P, C.c_int]),
@@ -311,6 +312,13 @@ class OracleWorld3:
 
     def set_config(self, cfg: FluidConfig2Ffi) -> None:
         self._l.orc3_set_config(self._h, C.byref(cfg))
+
+    def set_turbulence(self, amplitude: float, frequency: float = 1.0, time_scale: float = 1.0, seed: int = 0,
+                       octaves: int = 3, divergence_free: bool = False, enabled: bool = True) -> None:
+        """world.ambient.turbulence (TurbulenceConfig3), read by the integrate
+        at the world clock of each step's start."""
+        self._l.orc3_set_turbulence(self._h, 1 if enabled else 0, amplitude, frequency, time_scale,
+                                    seed & 0xFFFFFFFF, octaves, 1 if divergence_free else 0)
 
     def set_gravity(self, gx: float, gy: float, gz: float) -> None:
         self._l.orc3_set_gravity(self._h, gx, gy, gz)

@@ -23,6 +23,85 @@
 
 namespace oracle {
 
+// ---- 3D ambient turbulence (noise.rs:50-222, fluid3.rs:1090-1108) ----
+template <class R>
+inline R nz_lattice3(int32_t ix, int32_t iy, int32_t iz, uint32_t seed) {  // noise.rs:50-60
+  const uint32_t h = nz_hash((uint32_t)ix * 0x1f1f1f1fu + (uint32_t)iy * 0x9e3779b9u + (uint32_t)iz * 0x85ebca6bu + seed);
+  return (R)(h >> 8) * (R)(1.0f / 16777216.0f);
+}
+
+template <class R>
+inline R nz_value3(R x, R y, R z, uint32_t seed) {  // noise.rs:90-111
+  const R x0 = std::floor(x), y0 = std::floor(y), z0 = std::floor(z);
+  const int32_t xi = rust_as_int<int32_t>(x0), yi = rust_as_int<int32_t>(y0), zi = rust_as_int<int32_t>(z0);
+  const R tx = nz_fade(x - x0), ty = nz_fade(y - y0), tz = nz_fade(z - z0);
+  const int32_t x1 = (int32_t)((uint32_t)xi + 1u), y1 = (int32_t)((uint32_t)yi + 1u), z1 = (int32_t)((uint32_t)zi + 1u);
+  const R v000 = nz_lattice3<R>(xi, yi, zi, seed), v100 = nz_lattice3<R>(x1, yi, zi, seed);
+  const R v010 = nz_lattice3<R>(xi, y1, zi, seed), v110 = nz_lattice3<R>(x1, y1, zi, seed);
+  const R v001 = nz_lattice3<R>(xi, yi, z1, seed), v101 = nz_lattice3<R>(x1, yi, z1, seed);
+  const R v011 = nz_lattice3<R>(xi, y1, z1, seed), v111 = nz_lattice3<R>(x1, y1, z1, seed);
+  const R a = nz_lerp(nz_lerp(v000, v100, tx), nz_lerp(v010, v110, tx), ty);
+  const R b = nz_lerp(nz_lerp(v001, v101, tx), nz_lerp(v011, v111, tx), ty);
+  return nz_lerp(a, b, tz);
+}
+
+template <class R>
+inline R nz_fbm3_static(R x, R y, R z, uint32_t seed, uint32_t oct) {  // noise.rs:135-152
+  R sum = 0, amp = 1, freq = 1, norm = 0;
+  for (uint32_t o = 0; o < oct; o++) {
+    sum += amp * (nz_value3(x * freq, y * freq, z * freq, seed + o) * (R)2 - (R)1);
+    norm += amp;
+    amp *= (R)0.5;
+    freq *= (R)2;
+  }
+  return norm > (R)0 ? sum / norm : (R)0;
+}
+
+template <class R>
+inline R nz_fbm3(R x, R y, R z, R t, uint32_t seed, uint32_t octaves) {  // noise.rs:173-183
+  const uint32_t oct = std::min<uint32_t>(std::max<uint32_t>(octaves, 1u), 8u);
+  const R t0 = std::floor(t);
+  const R ft = nz_fade(t - t0);
+  const int64_t sl = rust_as_int<int64_t>(t0);
+  const uint32_t s0 = seed + (uint32_t)sl * 0x9e3779b9u;
+  const uint32_t s1 = seed + (uint32_t)((uint64_t)sl + 1u) * 0x9e3779b9u;
+  return nz_lerp(nz_fbm3_static(x, y, z, s0, oct), nz_fbm3_static(x, y, z, s1, oct), ft);
+}
+
+template <class R>
+inline void turbulence_accel3(const Turbulence& tb, R px, R py, R pz, R time, R& ax, R& ay, R& az) {
+  const R x = px * (R)tb.freq, y = py * (R)tb.freq, z = pz * (R)tb.freq;
+  const R t = time * (R)tb.tscale;
+  R nx, ny, nz;
+  if (tb.curl) {  // curl_3 (noise.rs:198-222), components exactly as written there
+    const R e = (R)1e-3f, e2 = (R)(2.0f * 1e-3f);
+    const uint32_t oc = tb.oct;
+    auto px_ = [&](R a, R b, R c) { return nz_fbm3(a, b, c, t, tb.seed ^ 0x11111111u, oc); };
+    auto py_ = [&](R a, R b, R c) { return nz_fbm3(a, b, c, t, tb.seed ^ 0x22222222u, oc); };
+    auto pz_ = [&](R a, R b, R c) { return nz_fbm3(a, b, c, t, tb.seed ^ 0x33333333u, oc); };
+    auto ddx = [&](auto f) { return (f(x + e, y, z) - f(x - e, y, z)) / e2; };
+    auto ddy = [&](auto f) { return (f(x, y + e, z) - f(x, y - e, z)) / e2; };
+    auto ddz = [&](auto f) { return (f(x, y, z + e) - f(x, y, z - e)) / e2; };
+    nx = ddy(pz_) - ddz(py_);
+    ny = ddx(px_) - ddz(pz_);
+    nz = ddx(py_) - ddy(px_);
+  } else {
+    nx = nz_fbm3(x, y, z, t, tb.seed, tb.oct);
+    ny = nz_fbm3(x, y, z, t, tb.seed ^ 0x55aa55aau, tb.oct);
+    nz = nz_fbm3(x, y, z, t, tb.seed ^ 0xaa55aa55u, tb.oct);
+  }
+  const R ls = nx * nx + ny * ny + nz * nz;  // glam Vec3 dot: (x*x + y*y) + z*z
+  if (ls > (R)1) {
+    const R l = std::sqrt(ls);
+    nx = nx / l;
+    ny = ny / l;
+    nz = nz / l;
+  }
+  ax = ax + nx * (R)tb.amp;
+  ay = ay + ny * (R)tb.amp;
+  az = az + nz * (R)tb.amp;
+}
+
 struct Body3 {
   int shape = 1;  // 0 sphere (a = radius), 1 box (a, b, c half extents), 2 capsule (a = radius, b = half length along y)
   float px = 0, py = 0, pz = 0;
@@ -44,6 +123,7 @@ class Fluid3 {
   std::vector<Body3> bodies;
   R gx = 0, gy = (R)-9.81f, gz = 0;  // World3::new gravity
   R time = 0;
+  Turbulence turb;  // world.ambient.turbulence
   size_t cap = 4096;
   int pow_mode = 1;
   std::vector<R> fx, fy, fz;
@@ -231,6 +311,7 @@ class Fluid3 {
       neighbors_of(src[i].x, src[i].y, src[i].z, src, nb);
       R rho_i = rmax(src[i].density, (R)kEps);
       R ax = gx + fx[i] / rho_i, ay = gy + fy[i] / rho_i, az = gz + fz[i] / rho_i;
+      if (turb.on) turbulence_accel3(turb, src[i].x, src[i].y, src[i].z, time, ax, ay, az);
       R vx = src[i].vx + ax * dt, vy = src[i].vy + ay * dt, vz = src[i].vz + az * dt;
       if (visc > (R)0) {
         R sx = 0, sy = 0, sz = 0;

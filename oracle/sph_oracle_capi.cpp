@@ -497,6 +497,21 @@ void orc3_set_config(void* h, const FluidConfig2Ffi* c) {
   DISPATCH(o, apply_config(F, c));
 }
 
+void orc3_set_turbulence(void* h, int enabled, float amp, float freq, float tscale, uint32_t seed, uint32_t octaves,
+                         int divergence_free) {
+  Orc3* o = static_cast<Orc3*>(h);
+  oracle::Turbulence t;
+  t.on = enabled != 0 && amp > 0.0f;
+  t.amp = amp;
+  t.freq = freq;
+  t.tscale = tscale;
+  t.seed = seed;
+  t.oct = std::min<uint32_t>(octaves, 255u);
+  t.curl = divergence_free != 0;
+  o->f32.turb = t;
+  o->f64.turb = t;
+}
+
 void orc3_set_gravity(void* h, float gx, float gy, float gz) {
   Orc3* o = static_cast<Orc3*>(h);
   o->f32.gx = gx;

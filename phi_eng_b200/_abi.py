@@ -118,6 +118,45 @@ class AmbientConfig2Ffi(C.Structure):
     ]
 
 
+class AmbientConfig3Ffi(C.Structure):
+    """#[repr(C)] AmbientConfig3Ffi (crates/engine/src/ffi.rs:278-326), 88 bytes."""
+
+    _fields_ = [
+        ("spring_enabled", C.c_uint32),
+        ("spring_ax", C.c_float),
+        ("spring_ay", C.c_float),
+        ("spring_az", C.c_float),
+        ("spring_stiffness", C.c_float),
+        ("spring_damping", C.c_float),
+        ("spring_max_displacement", C.c_float),
+        ("drag_enabled", C.c_uint32),
+        ("drag_linear", C.c_float),
+        ("drag_quadratic", C.c_float),
+        ("air_density", C.c_float),
+        ("drag_angular", C.c_float),
+        ("wind_x", C.c_float),
+        ("wind_y", C.c_float),
+        ("wind_z", C.c_float),
+        ("turbulence_enabled", C.c_uint32),
+        ("turbulence_amplitude", C.c_float),
+        ("turbulence_frequency", C.c_float),
+        ("turbulence_time_scale", C.c_float),
+        ("turbulence_seed", C.c_uint32),
+        ("turbulence_octaves", C.c_uint32),
+        ("turbulence_divergence_free", C.c_uint32),
+    ]
+
+
+def default_ambient3() -> AmbientConfig3Ffi:
+    """AmbientConfig3::default (crates/dynamics/src/ambient.rs)."""
+    a = AmbientConfig3Ffi()
+    a.air_density = 1.0
+    a.turbulence_frequency = 1.0
+    a.turbulence_time_scale = 1.0
+    a.turbulence_octaves = 3
+    return a
+
+
 def default_ambient() -> AmbientConfig2Ffi:
     """AmbientConfig2::default (crates/dynamics/src/ambient.rs)."""
     a = AmbientConfig2Ffi()
@@ -326,6 +365,8 @@ SIGNATURES = {
     "phieng_world3_set_time": (C.c_int32, [_P, C.c_float]),
     "phieng_world3_get_time": (C.c_int32, [_P, _F]),
     "phieng_world3_body_count": (C.c_int32, [_P]),
+    "phieng_world3_set_ambient_config": (C.c_int32, [_P, C.POINTER(AmbientConfig3Ffi)]),
+    "phieng_world3_get_ambient_config": (C.c_int32, [_P, C.POINTER(AmbientConfig3Ffi)]),
     "phieng_world3_add_body": (
         C.c_int32,
         [_P, C.c_float, C.c_float, C.c_float, C.c_uint32, C.c_float, C.c_float, C.c_float, C.c_float,

@@ -34,7 +34,8 @@ UNITS = [
     ("sph_mlp.cu", EXACT),
     ("sph3d.cu", EXACT),
 ]
-HEADERS = ["sph_device.cuh", "sph_kernels.h", "sph_mlp.cuh", "sph_mlp_host.h", "sph_warp.cuh", "sph_host.h", "sph_snapshot.h"]
+HEADERS = ["sph_device.cuh", "sph_kernels.h", "sph_mlp.cuh", "sph_mlp_host.h", "sph_warp.cuh", "sph_host.h", "sph_snapshot.h",
+           "sph_noise.cuh"]
 
 
 def _mtime(p: str) -> float:

@@ -28,6 +28,7 @@
 #include "../../include/phieng_sph.h"
 #include "sph_host.h"
 #include "sph_kernels.h"
+#include "sph_noise.cuh"
 #include "sph_snapshot.h"
 #include "sph_warp.cuh"
 
@@ -61,6 +62,10 @@ struct StepParams3 {
   float gx, gy, gz;
   float pr, pr_pad, mu, av_alpha, c_s, surface_tension;
   uint32_t flags, nbodies, uniform_phase;
+  // ambient turbulence (F_TURB; TurbulenceConfig3, ambient.rs:251-266)
+  float turb_amp, turb_freq, turb_tscale;
+  uint32_t turb_seed, turb_oct;  // octaves already clamped to 1..8
+  const float* clock;            // device word holding the world clock of the current step
 };
 
 // Static body: shape 0 sphere (a = radius), 1 box (a, b, c half extents),
@@ -482,9 +487,16 @@ __global__ void __launch_bounds__(256) k_force3(const float4* __restrict__ spos,
     dbg[id] = make_float4(f[0], f[1], f[2], 0.0f);
     return;
   }
-  const float ax = __fadd_rn(P.gx, __fdiv_rn(f[0], rho_i));
-  const float ay = __fadd_rn(P.gy, __fdiv_rn(f[1], rho_i));
-  const float az = __fadd_rn(P.gz, __fdiv_rn(f[2], rho_i));
+  float ax = __fadd_rn(P.gx, __fdiv_rn(f[0], rho_i));
+  float ay = __fadd_rn(P.gy, __fdiv_rn(f[1], rho_i));
+  float az = __fadd_rn(P.gz, __fdiv_rn(f[2], rho_i));
+  if (P.flags & F_TURB) {  // fluid3.rs:1096-1108, at the pre-step position and the step's clock
+    const float3 tb = turbulence_accel3(pi.x, pi.y, pi.z, *P.clock, P.turb_freq, P.turb_tscale, P.turb_seed,
+                                        P.turb_oct, P.flags & F_TURB_CURL, P.turb_amp);
+    ax = __fadd_rn(ax, tb.x);
+    ay = __fadd_rn(ay, tb.y);
+    az = __fadd_rn(az, tb.z);
+  }
   float vx = __fadd_rn(vi.x, __fmul_rn(ax, P.dt));
   float vy = __fadd_rn(vi.y, __fmul_rn(ay, P.dt));
   float vz = __fadd_rn(vi.z, __fmul_rn(az, P.dt));
@@ -544,8 +556,23 @@ inline uint32_t cdiv(uint32_t a, uint32_t b) { return (a + b - 1) / b; }
 }  // namespace phieng
 
 // ---------------------------------------------------------------- the 3D world
+// AmbientConfig3::default (ambient.rs): everything off, air density 1,
+// turbulence frequency 1, time scale 1, 3 octaves.
+AmbientConfig3Ffi default_ambient3() {
+  AmbientConfig3Ffi a;
+  std::memset(&a, 0, sizeof(a));
+  a.air_density = 1.0f;
+  a.turbulence_frequency = 1.0f;
+  a.turbulence_time_scale = 1.0f;
+  a.turbulence_octaves = 3;
+  return a;
+}
+
+constexpr uint32_t kClockWord3 = 16;  // scalar word holding the step's world clock (turbulence)
+
 struct World3 {
   FluidConfig3Ffi cfg = default_config();
+  AmbientConfig3Ffi ambient = default_ambient3();
   float gx = 0.0f, gy = -9.81f, gz = 0.0f;  // World3::new gravity
   float time = 0.0f;
   std::vector<DevBody3> bodies;
@@ -632,7 +659,7 @@ bool ensure_device3(World3* w) {
   if (!ok3(w, cudaGetDevice(&dev))) return false;
   if (!ok3(w, cudaStreamCreateWithFlags(&w->own_stream, cudaStreamNonBlocking))) return false;
   if (!w->user_stream) w->stream = w->own_stream;
-  if (!ok3(w, cudaMalloc(&w->scalar, 64)) || !ok3(w, cudaMemset(w->scalar, 0, 64))) return false;
+  if (!ok3(w, cudaMalloc(&w->scalar, 128)) || !ok3(w, cudaMemset(w->scalar, 0, 128))) return false;
   if (!ok3(w, cudaMallocHost(&w->h_pinned, 64))) return false;
   w->device = dev;
   return true;
@@ -853,6 +880,17 @@ StepParams3 make_params3(const World3* w, float dt) {
   if (!w->mass_uniform) f |= F_MASS;
   if (!w->phase_uniform) f |= F_PHASE;
   if (!(P.hg2 <= P.hk2)) f |= F_WIDE_NB;
+  const AmbientConfig3Ffi& a = w->ambient;
+  if (a.turbulence_enabled != 0 && a.turbulence_amplitude > 0.0f && w->scalar) {  // fluid3.rs:1090-1091
+    f |= F_TURB;
+    if (a.turbulence_divergence_free) f |= F_TURB_CURL;
+    P.turb_amp = a.turbulence_amplitude;
+    P.turb_freq = a.turbulence_frequency;
+    P.turb_tscale = a.turbulence_time_scale;
+    P.turb_seed = a.turbulence_seed;
+    P.turb_oct = std::min<uint32_t>(std::max<uint32_t>(a.turbulence_octaves, 1u), 8u);
+    P.clock = reinterpret_cast<const float*>(w->scalar + kClockWord3);
+  }
   P.flags = f;
   P.nbodies = (uint32_t)w->bodies.size();
   P.uniform_phase = w->phase_value;
@@ -1010,6 +1048,11 @@ bool world_step3(World3* w, float dt) {
     uint32_t ns = 1;
     if (!cfl_substeps3(w, dt, &ns)) return false;
     const StepParams3 P = make_params3(w, dt / (float)ns);
+    if (P.flags & F_TURB) {  // every CFL substep sees the step's start time (world.rs:2811)
+      uint32_t bits;
+      std::memcpy(&bits, &w->time, 4);
+      enqueue_set_word(w->scalar + kClockWord3, bits, w->stream);
+    }
     for (uint32_t k = 0; k < ns; k++)
       if (!run_substep3(w, P)) return false;
   }
@@ -1101,6 +1144,36 @@ int32_t phieng_world3_get_time(World3* w, float* out) {
 }
 
 int32_t phieng_world3_body_count(World3* w) { return w ? (int32_t)w->bodies.size() : -1; }
+
+int32_t phieng_world3_set_ambient_config(World3* w, const AmbientConfig3Ffi* cfg) {
+  if (!w || !cfg) return 0;
+  const AmbientConfig3Ffi& c = *cfg;
+  // ambient3_from_ffi (ffi.rs:414-475): finite floats, non-negative
+  // coefficients, octaves stored as min(v, 255)
+  for (float v : {c.spring_ax, c.spring_ay, c.spring_az, c.spring_stiffness, c.spring_damping,
+                  c.spring_max_displacement, c.drag_linear, c.drag_quadratic, c.air_density, c.drag_angular,
+                  c.wind_x, c.wind_y, c.wind_z, c.turbulence_amplitude, c.turbulence_frequency,
+                  c.turbulence_time_scale})
+    if (!std::isfinite(v)) return 0;
+  if (c.spring_stiffness < 0.0f || c.spring_damping < 0.0f || c.spring_max_displacement < 0.0f ||
+      c.drag_linear < 0.0f || c.drag_quadratic < 0.0f || c.air_density < 0.0f || c.drag_angular < 0.0f ||
+      c.turbulence_amplitude < 0.0f)
+    return 0;
+  AmbientConfig3Ffi a = c;
+  a.spring_enabled = c.spring_enabled != 0;
+  a.drag_enabled = c.drag_enabled != 0;
+  a.turbulence_enabled = c.turbulence_enabled != 0;
+  a.turbulence_divergence_free = c.turbulence_divergence_free != 0;
+  a.turbulence_octaves = std::min<uint32_t>(c.turbulence_octaves, 255u);
+  w->ambient = a;
+  return 1;
+}
+
+int32_t phieng_world3_get_ambient_config(World3* w, AmbientConfig3Ffi* out) {
+  if (!w || !out) return 0;
+  *out = w->ambient;
+  return 1;
+}
 
 int32_t phieng_world3_add_body(World3* w, float px, float py, float pz, uint32_t shape_tag, float a, float b, float c,
                                float density, uint8_t is_static, float friction, float restitution) {

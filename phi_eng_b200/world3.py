@@ -171,6 +171,28 @@ class World3:
         self._lib.phieng_world3_get_time(self._h, C.byref(t))
         return float(t.value)
 
+    @property
+    def ambient(self) -> "_abi.AmbientConfig3Ffi":
+        """The world's AmbientConfig3Ffi (phieng_world3_get_ambient_config)."""
+        a = _abi.AmbientConfig3Ffi()
+        self._lib.phieng_world3_get_ambient_config(self._h, C.byref(a))
+        return a
+
+    def set_turbulence(self, amplitude: float, frequency: float = 1.0, time_scale: float = 1.0, seed: int = 0,
+                       octaves: int = 3, divergence_free: bool = False, enabled: bool = True) -> None:
+        """world.ambient.turbulence (TurbulenceConfig3, ambient.rs:251-266) through
+        phieng_world3_set_ambient_config, the other ambient fields kept."""
+        a = self.ambient
+        a.turbulence_enabled = 1 if enabled else 0
+        a.turbulence_amplitude = amplitude
+        a.turbulence_frequency = frequency
+        a.turbulence_time_scale = time_scale
+        a.turbulence_seed = seed & 0xFFFFFFFF
+        a.turbulence_octaves = octaves
+        a.turbulence_divergence_free = 1 if divergence_free else 0
+        if self._lib.phieng_world3_set_ambient_config(self._h, C.byref(a)) != 1:
+            raise ValueError("ambient config rejected")
+
     def add_static_body(self, position, shape) -> int:
         """A static body through phieng_world3_add_body (identity rotation)."""
         px, py, pz = (float(v) for v in position)

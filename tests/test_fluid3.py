@@ -573,3 +573,79 @@ def test_gpu_profiling_phase_times():
     w.step(1 / 60)
     t = w.phase_times()
     assert t.shape == (3,) and (t > 0).all()
+
+
+# ---------------------------------------------------------------- ambient turbulence (fluid3.rs:1090-1108)
+TURB3 = dict(amplitude=5.0, frequency=0.5, seed=7, octaves=3)
+
+
+def test_ambient3_layout_roundtrip_and_validation():
+    """phieng_world3_set/get_ambient_config (ffi.rs:549-577) on the CPU."""
+    import math
+
+    assert C.sizeof(_abi.AmbientConfig3Ffi) == 88
+    assert _abi.AmbientConfig3Ffi.turbulence_enabled.offset == 60
+    lib = _abi.load()
+    w = lib.phieng_world3_new()
+    try:
+        a = _abi.AmbientConfig3Ffi()
+        assert lib.phieng_world3_get_ambient_config(w, C.byref(a)) == 1
+        d = _abi.default_ambient3()
+        for name, _ in _abi.AmbientConfig3Ffi._fields_:
+            assert getattr(a, name) == getattr(d, name), name
+        a.turbulence_enabled, a.turbulence_amplitude, a.turbulence_octaves, a.wind_z = 3, 2.0, 999, 1.5
+        assert lib.phieng_world3_set_ambient_config(w, C.byref(a)) == 1
+        b = _abi.AmbientConfig3Ffi()
+        lib.phieng_world3_get_ambient_config(w, C.byref(b))
+        assert (b.turbulence_enabled, b.turbulence_amplitude, b.turbulence_octaves, b.wind_z) == (1, 2.0, 255, 1.5)
+        for field, value in (("turbulence_amplitude", -1.0), ("wind_z", math.nan), ("spring_az", math.inf),
+                             ("drag_angular", -1.0)):
+            bad = _abi.default_ambient3()
+            setattr(bad, field, value)
+            assert lib.phieng_world3_set_ambient_config(w, C.byref(bad)) == 0
+        lib.phieng_world3_get_ambient_config(w, C.byref(b))
+        assert b.turbulence_amplitude == 2.0
+        assert lib.phieng_world3_set_ambient_config(None, C.byref(b)) == 0
+        assert lib.phieng_world3_get_ambient_config(w, None) == 0
+    finally:
+        lib.phieng_world3_free(w)
+
+
+@pytest.mark.parametrize("curl", [False, True])
+def test_turbulence3_deterministic_oracle(curl):
+    """The 3D counterpart of test_fluid_turbulence_deterministic
+    (fluid.rs:1497-1516) on the oracle: bit-identical reruns, and the field
+    moves the fluid."""
+    def run(turb):
+        o = make_oracle(lattice((0.0, 0.0, 0.0), 4, 6, 4, 0.25))
+        if turb:
+            o.set_turbulence(**turb, divergence_free=curl)
+        for _ in range(60):
+            o.step(1 / 60, REF_SEQ)
+        return o.state()
+
+    a, b, c = run(TURB3), run(TURB3), run(None)
+    assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+    assert np.isfinite(a).all()
+    assert not np.array_equal(a, c)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("curl", [False, True])
+def test_turbulence3_bit_exact(curl):
+    """3D dam break with turbulence (both modes; CFL substeps share a step's
+    clock), 120 steps: GPU equals the oracle's Jacobi integrate bit for bit."""
+    cfg = default_config()
+    cfg.cfl = 0.3
+    cfg.max_substeps = 3
+    pts = lattice((0.0, 0.0, 0.0), 5, 7, 5, 0.25)
+    o = make_oracle(pts, cfg=cfg)
+    w = make_gpu(pts, cfg=cfg)
+    o.set_turbulence(**TURB3, time_scale=2.0, divergence_free=curl)
+    w.set_turbulence(**TURB3, time_scale=2.0, divergence_free=curl)
+    for k in range(120):
+        o.step(1 / 60, JACOBI)
+        w.step(1 / 60)
+        if k % 40 == 39:
+            assert_bit_equal(w.fluid.particles, o.state(), f"state after {k + 1} steps")
+    assert w.time == o.time
