@@ -38,6 +38,9 @@ typedef struct World2 World2;
 /* Shape tags (ffi.rs:26-28). */
 #define PHIENG_SHAPE_CIRCLE 0u
 #define PHIENG_SHAPE_BOX 1u
+/* Shape2::Polygon (body.rs): accepted by phieng_sph_step_fluid_poly only
+ * (the reference's add_body takes circles and boxes). */
+#define PHIENG_SHAPE_POLYGON 2u
 
 /* 2D SPH fluid config, #[repr(C)] mirror of FluidConfig2Ffi (ffi.rs:712-739).
  * Rust `bool` fields are one byte (0 or 1). Size 112, align 4. */
@@ -462,7 +465,8 @@ int32_t phieng_sph_reserve(World2* world, uint32_t n);
  * A rigid body as the fluid phase sees it (RigidBody2, body.rs:560-700):
  * shape, transform, velocity and inverse mass / inertia. 60 bytes. */
 typedef struct PhiengBody2 {
-  uint32_t shape_tag;        /* PHIENG_SHAPE_CIRCLE (a = radius) or PHIENG_SHAPE_BOX (a, b = half extents) */
+  uint32_t shape_tag;        /* PHIENG_SHAPE_CIRCLE (a = radius), PHIENG_SHAPE_BOX (a, b = half extents) or
+                                PHIENG_SHAPE_POLYGON (phieng_sph_step_fluid_poly) */
   float a, b;
   float px, py;              /* transform.position */
   float xax, xay, yax, yay;  /* transform.rotation columns x_axis, y_axis */
@@ -483,11 +487,29 @@ static_assert(sizeof(PhiengBody2) == 60, "PhiengBody2 layout");
  * n * (vn * m) and the no-slip reaction on each body, applied in particle
  * order) and the buoyancy + drag pass of fluid.rs:1103-1135 on dynamic
  * circles and boxes; vx, vy, w and is_sleeping of `bodies` are updated in
- * place. The ambient wind and turbulence are zero. Does not advance the
- * world clock and does not clamp dt (the caller's World2::step does both).
+ * place. The world's ambient config applies as World2::step_inner passes
+ * it: turbulence at the world clock (phieng_world_set_time), the wind in the
+ * buoyancy drag (fluid.rs:1121-1124). Does not advance the world clock and
+ * does not clamp dt (the caller's World2::step does both).
  * 1 ok; 0 for a null world, a batch, a body with an unknown shape or a
  * non-finite field, more than 65536 bodies, or an error (phieng_sph_status). */
 int32_t phieng_sph_step_fluid(World2* world, PhiengBody2* bodies, uint32_t nbodies, float dt);
+
+/* phieng_sph_step_fluid with polygon bodies as well: a body with shape_tag
+ * PHIENG_SHAPE_POLYGON (a, b unused) has poly_count[k] >= 3 vertices in its
+ * own frame at poly_xy[2 * poly_first[k] ...] (Shape2::Polygon; the arrays
+ * are indexed by body and read for polygons only). The fluid tests it as
+ * fluid.rs:518-530 does: the vertices moved by the body's transform, SAT
+ * circle-polygon (collision/src/sat.rs:104-200), the axis oriented from the
+ * vertex centroid to the particle, contact point particle - normal * r.
+ * Polygons are impulse-coupled only, as in the reference: no buoyancy
+ * samples (fluid.rs:415-418). Each particle tests every polygon (a non-convex
+ * polygon's SAT can report a contact outside its bounding box, so no box
+ * reject applies). 0 also for a polygon with fewer than 3 vertices, a vertex
+ * range outside poly_nverts or a non-finite vertex. */
+int32_t phieng_sph_step_fluid_poly(World2* world, PhiengBody2* bodies, uint32_t nbodies, const float* poly_xy,
+                                   const uint32_t* poly_first, const uint32_t* poly_count, uint32_t poly_nverts,
+                                   float dt);
 
 /* ---- snapshot fluid block (crates/dynamics/src/snapshot.rs) ----
  * The fluid section of the reference's binary world snapshot: config, then

@@ -44,6 +44,7 @@ def _load():
         "orc_get_config": (None, [P, C.POINTER(FluidConfig2Ffi)]),
         "orc_set_gravity": (None, [P, C.c_float, C.c_float]),
         "orc_set_turbulence": (None, [P, C.c_int, C.c_float, C.c_float, C.c_float, C.c_uint32, C.c_uint32, C.c_int]),
+        "orc_set_wind": (None, [P, C.c_float, C.c_float]),
         "orc3_set_turbulence": (None, [P, C.c_int, C.c_float, C.c_float, C.c_float, C.c_uint32, C.c_uint32, C.c_int]),
         "orc_noise2": (None, [C.c_int, C.c_float, C.c_float, C.c_float, C.c_uint32, C.c_uint32, C.POINTER(C.c_float)]),
         "orc_set_cap": (None, [P, C.c_uint32]),
@@ -52,6 +53,8 @@ def _load():
                                 C.c_float, C.c_float, C.c_float, C.c_float]),
         "orc_add_particles": (C.c_uint32, [P, F, U8, C.c_uint32]),
         "orc_step_fluid": (None, [P, C.c_void_p, C.c_uint32, C.c_float, C.c_int]),
+        "orc_step_fluid_poly": (None, [P, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_float,
+                                       C.c_int]),
         "orc_count": (C.c_uint32, [P]),
         "orc_clear": (None, [P]),
         "orc_set_state": (None, [P, F, C.c_uint32]),
@@ -152,6 +155,10 @@ class OracleWorld:
 
     def set_gravity(self, gx: float, gy: float) -> None:
         self._l.orc_set_gravity(self._h, gx, gy)
+
+    def set_wind(self, wx: float, wy: float) -> None:
+        """world.ambient.drag.wind, against which the buoyancy drag acts."""
+        self._l.orc_set_wind(self._h, wx, wy)
 
     def set_turbulence(self, amplitude: float, frequency: float = 1.0, time_scale: float = 1.0, seed: int = 0,
                        octaves: int = 3, divergence_free: bool = False, enabled: bool = True) -> None:
@@ -269,10 +276,17 @@ class OracleWorld:
     def cfl_substeps(self, dt: float) -> int:
         return int(self._l.orc_cfl_substeps(self._h, dt))
 
-    def step_fluid(self, bodies, dt: float, mode: int = REF_SEQ) -> None:
+    def step_fluid(self, bodies, dt: float, mode: int = REF_SEQ, poly=None) -> None:
         """FluidState2::step_fluid with `bodies` (a ctypes PhiengBody2 array,
-        updated in place) in place of the world's bodies; no clock."""
-        self._l.orc_step_fluid(self._h, C.cast(bodies, C.c_void_p), len(bodies), dt, mode)
+        updated in place) in place of the world's bodies; no clock. poly =
+        (xy float32 [m][2], first uint32 [nb], count uint32 [nb]): the local
+        vertices of the PHIENG_SHAPE_POLYGON bodies."""
+        if poly is None:
+            self._l.orc_step_fluid(self._h, C.cast(bodies, C.c_void_p), len(bodies), dt, mode)
+            return
+        xy, first, count = (np.ascontiguousarray(a) for a in poly)
+        self._l.orc_step_fluid_poly(self._h, C.cast(bodies, C.c_void_p), len(bodies), xy.ctypes.data,
+                                    first.ctypes.data, count.ctypes.data, dt, mode)
 
     # ---- learned-closure hooks ----
     def features(self, dt: float) -> np.ndarray:

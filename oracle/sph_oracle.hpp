@@ -70,7 +70,8 @@ struct Config {
 // A static rigid body as the fluid sees it (body.rs:573-607): a circle or a
 // box with a Transform2 (math.rs:34-60: position + glam Mat2 columns).
 struct Body {
-  int shape = 1;  // 0 = circle (a = radius), 1 = box (a, b = half extents)
+  int shape = 1;  // 0 = circle (a = radius), 1 = box (a, b = half extents), 2 = polygon
+  std::vector<float> poly;  // polygon: world-space vertices x0, y0, x1, y1, ... (transform_point of the local ones)
   float px = 0, py = 0;
   float xax = 1, xay = 0, yax = 0, yay = 1;  // rotation columns x_axis, y_axis
   float a = 0, b = 0;
@@ -294,6 +295,7 @@ class Fluid {
   R gx = (R)0.0f, gy = (R)-9.81f;  // World2::new gravity (world.rs:338)
   R time = 0;
   Turbulence turb;    // world.ambient.turbulence
+  float wind_x = 0, wind_y = 0;  // world.ambient.drag.wind
   size_t cap = 4096;  // MAX_PARTICLES_2D (fluid.rs:30); lifted by the caller
   int pow_mode = 1;   // see powf_cr
 
@@ -548,7 +550,131 @@ class Fluid {
   }
   // ... and the contact point on the body surface (circle: position +
   // normal * radius; box: transform_point(clamped))
+  // ---- polygon bodies: fluid.rs:518-530 and crates/collision/src/sat.rs ----
+  // glam Vec2::normalize_or_zero: v * (1 / |v|) if that is finite and > 0
+  static void unit_or_zero(R x, R y, R& ox, R& oy) {
+    const R rcp = (R)1 / std::sqrt(x * x + y * y);
+    if (std::isfinite(rcp) && rcp > (R)0) {
+      ox = x * rcp;
+      oy = y * rcp;
+    } else {
+      ox = 0;
+      oy = 0;
+    }
+  }
+  // project_polygon (sat.rs:88-99); std::fmin / fmax keep the non-NaN, as f32::min / max
+  static void poly_extent(const std::vector<float>& v, R ax, R ay, R& lo, R& hi) {
+    lo = (R)std::numeric_limits<float>::max();
+    hi = -(R)std::numeric_limits<float>::max();
+    for (size_t i = 0; i + 1 < v.size(); i += 2) {
+      const R d = ax * (R)v[i] + ay * (R)v[i + 1];
+      lo = std::fmin(lo, d);
+      hi = std::fmax(hi, d);
+    }
+  }
+  // edge k's normalised (-e.y, e.x); false for |e|^2 < EPS_SQ
+  static bool edge_unit_normal(const std::vector<float>& v, size_t k, R& nx, R& ny) {
+    const size_t n = v.size() / 2, j = (k + 1) % n;
+    const R ex = (R)v[2 * j] - (R)v[2 * k], ey = (R)v[2 * j + 1] - (R)v[2 * k + 1];
+    if (ex * ex + ey * ey < (R)kEpsSq) return false;
+    unit_or_zero(-ey, ex, nx, ny);
+    return true;
+  }
+  // point_in_polygon (sat.rs:203-220), even-odd rule
+  static bool inside_poly(R x, R y, const std::vector<float>& v) {
+    const size_t n = v.size() / 2;
+    bool in = false;
+    for (size_t i = 0, j = n - 1; i < n; j = i++) {
+      const R xi = v[2 * i], yi = v[2 * i + 1], xj = v[2 * j], yj = v[2 * j + 1];
+      if ((yi > y) != (yj > y) && x < (xj - xi) * (y - yi) / (yj - yi) + xi) in = !in;
+    }
+    return in;
+  }
+  // sat_circle_polygon (sat.rs:104-200)
+  static bool circle_poly_sat(R cx, R cy, R r, const std::vector<float>& v, R& ax, R& ay, R& pen) {
+    const size_t n = v.size() / 2;
+    if (n < 3 || r <= (R)0) return false;
+    R best = (R)std::numeric_limits<float>::max(), bx = 0, by = 0;
+    for (size_t k = 0; k < n; k++) {
+      R ux, uy, lo, hi;
+      if (!edge_unit_normal(v, k, ux, uy)) continue;
+      poly_extent(v, ux, uy, lo, hi);
+      const R c = ux * cx + uy * cy;
+      if (hi < c - r || c + r < lo) return false;
+      const R ov = std::fmin(hi, c + r) - std::fmax(lo, c - r);
+      if (ov < best) {
+        best = ov;
+        bx = ux;
+        by = uy;
+      }
+    }
+    size_t kc = 0;  // the closest vertex (first of equals)
+    R dbest = (cx - (R)v[0]) * (cx - (R)v[0]) + (cy - (R)v[1]) * (cy - (R)v[1]);
+    for (size_t k = 1; k < n; k++) {
+      const R dx = cx - (R)v[2 * k], dy = cy - (R)v[2 * k + 1];
+      const R d = dx * dx + dy * dy;
+      if (d < dbest) {
+        dbest = d;
+        kc = k;
+      }
+    }
+    const R wx = cx - (R)v[2 * kc], wy = cy - (R)v[2 * kc + 1];
+    if (wx * wx + wy * wy >= (R)kEpsSq) {
+      R ux, uy, lo, hi;
+      unit_or_zero(wx, wy, ux, uy);
+      if (!(ux == (R)0 && uy == (R)0)) {
+        poly_extent(v, ux, uy, lo, hi);
+        const R c = ux * cx + uy * cy;
+        if (hi < c - r || c + r < lo) return false;
+      }
+    }
+    if (inside_poly(cx, cy, v)) {
+      R far = -(R)std::numeric_limits<float>::max(), fx = 0, fy = 0;
+      for (size_t k = 0; k < n; k++) {
+        R ux, uy;
+        if (!edge_unit_normal(v, k, ux, uy)) continue;
+        const R d = ux * ((R)v[2 * k] - cx) + uy * ((R)v[2 * k + 1] - cy);
+        if (d > far) {
+          far = d;
+          fx = ux;
+          fy = uy;
+        }
+      }
+      if (fx == (R)0 && fy == (R)0) return false;
+      ax = -fx;
+      ay = -fy;
+      pen = r - far;
+      return true;
+    }
+    if (bx == (R)0 && by == (R)0) return false;
+    ax = bx;
+    ay = by;
+    pen = best;
+    return true;
+  }
+
   static bool collide_pt(R px, R py, R pr, const Body& b, R& nx, R& ny, R& depth, R& qx, R& qy) {
+    if (b.shape == 2) {
+      R ax, ay, pen;
+      if (!circle_poly_sat(px, py, pr, b.poly, ax, ay, pen)) return false;
+      R sx = 0, sy = 0;  // polygon_centroid: sum from zero, divided by the count
+      for (size_t i = 0; i + 1 < b.poly.size(); i += 2) {
+        sx = sx + (R)b.poly[i];
+        sy = sy + (R)b.poly[i + 1];
+      }
+      const R cnt = (R)(float)(b.poly.size() / 2);
+      const R cenx = sx / cnt, ceny = sy / cnt;
+      if ((px - cenx) * ax + (py - ceny) * ay < (R)0) {  // orient_normal(axis, centroid, particle)
+        ax = -ax;
+        ay = -ay;
+      }
+      nx = ax;
+      ny = ay;
+      depth = pen;
+      qx = px - ax * pr;
+      qy = py - ay * pr;
+      return true;
+    }
     if (b.shape == 0) {
       R dx = px - (R)b.px;
       R dy = py - (R)b.py;
@@ -675,6 +801,7 @@ class Fluid {
   }
   // surface_samples: circles 12 perimeter points, boxes 4 per edge
   static void surface_samples(const Body& b, std::vector<float>& out) {  // (x, y, nx, ny, area) each
+    if (b.shape == 2) return;  // polygons are impulse-coupled only (fluid.rs:415-418)
     const float pi = Consts<float>::pi();
     auto push = [&](float lx, float ly, float nlx, float nly, float area) {
       out.push_back((b.xax * lx + b.yax * ly) + b.px);
@@ -722,8 +849,8 @@ class Fluid {
         if (p <= 0.0f) continue;
         wet = true;
         float rx = ptx - b.px, ry = pty - b.py;
-        float vrx = (b.vx + (-b.w * ry)) - 0.0f;
-        float vry = (b.vy + (b.w * rx)) - 0.0f;
+        float vrx = (b.vx + (-b.w * ry)) - wind_x;  // against ambient.drag.wind (fluid.rs:1121-1124)
+        float vry = (b.vy + (b.w * rx)) - wind_y;
         float speed = std::sqrt(vrx * vrx + vry * vry);
         float fx = -nx * (p * area), fy = -ny * (p * area);
         if (speed > kEps) {

@@ -131,6 +131,13 @@ void orc_set_gravity(void* h, float gx, float gy) {
   o->f64.gy = (double)gy;
 }
 
+// world.ambient.drag.wind (read by the buoyancy drag)
+void orc_set_wind(void* h, float wx, float wy) {
+  Orc* o = static_cast<Orc*>(h);
+  o->f32.wind_x = o->f64.wind_x = wx;
+  o->f32.wind_y = o->f64.wind_y = wy;
+}
+
 // world.ambient.turbulence (TurbulenceConfig2, ambient.rs:108-126)
 void orc_set_turbulence(void* h, int enabled, float amp, float freq, float tscale, uint32_t seed, uint32_t octaves,
                         int divergence_free) {
@@ -197,14 +204,24 @@ void orc_add_body(void* h, int shape, float px, float py, float a, float b, floa
 
 // step_fluid with the caller's bodies in place of the world's (f32 oracle):
 // the bodies' velocity state is updated in place (PhiengBody2 layout).
-void orc_step_fluid(void* h, PhiengBody2* bodies, uint32_t nb, float dt, int mode) {
+// FluidState2::step_fluid with the caller's bodies; polygon bodies
+// (PHIENG_SHAPE_POLYGON) take their local vertices from poly_xy
+// [2 * first[k], 2 * (first[k] + count[k])), moved by the body's transform.
+void orc_step_fluid_poly(void* h, PhiengBody2* bodies, uint32_t nb, const float* poly_xy, const uint32_t* first,
+                         const uint32_t* count, float dt, int mode) {
   Orc* o = static_cast<Orc*>(h);
   std::vector<oracle::Body> keep = o->f32.bodies;
   o->f32.bodies.clear();
   for (uint32_t k = 0; k < nb; k++) {
     const PhiengBody2& q = bodies[k];
     oracle::Body b;
-    b.shape = q.shape_tag == PHIENG_SHAPE_CIRCLE ? 0 : 1;
+    b.shape = q.shape_tag == PHIENG_SHAPE_CIRCLE ? 0 : q.shape_tag == PHIENG_SHAPE_POLYGON ? 2 : 1;
+    if (b.shape == 2)
+      for (uint32_t i = first[k]; i < first[k] + count[k]; i++) {
+        const float lx = poly_xy[2 * i], ly = poly_xy[2 * i + 1];
+        b.poly.push_back((q.xax * lx + q.yax * ly) + q.px);  // rotation * v + position (math.rs:58-60)
+        b.poly.push_back((q.xay * lx + q.yay * ly) + q.py);
+      }
     b.px = q.px;
     b.py = q.py;
     b.xax = q.xax;
@@ -231,6 +248,10 @@ void orc_step_fluid(void* h, PhiengBody2* bodies, uint32_t nb, float dt, int mod
     bodies[k].is_sleeping = b.sleeping ? 1 : 0;
   }
   o->f32.bodies = keep;
+}
+
+void orc_step_fluid(void* h, PhiengBody2* bodies, uint32_t nb, float dt, int mode) {
+  orc_step_fluid_poly(h, bodies, nb, nullptr, nullptr, nullptr, dt, mode);
 }
 
 uint32_t orc_add_particles(void* h, const float* xy, const uint8_t* phases, uint32_t n) {

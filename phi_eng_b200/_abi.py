@@ -15,6 +15,7 @@ LIB_PATH = os.environ.get("PHIENG_SPH_LIBRARY") or os.path.join(HERE, "libphieng
 
 SHAPE_CIRCLE = 0
 SHAPE_BOX = 1
+SHAPE_POLYGON = 2  # phieng_sph_step_fluid_poly only
 SHAPE3_SPHERE = 0
 SHAPE3_BOX = 1
 SHAPE3_CAPSULE = 2
@@ -354,6 +355,10 @@ SIGNATURES = {
     "phieng_sph_debug_neighbors": (C.c_uint32, [_P, _U32P, _U32P, C.c_uint32, C.c_uint32]),
     "phieng_sph_reserve": (C.c_int32, [_P, C.c_uint32]),
     "phieng_sph_step_fluid": (C.c_int32, [_P, C.POINTER(PhiengBody2), C.c_uint32, C.c_float]),
+    "phieng_sph_step_fluid_poly": (
+        C.c_int32,
+        [_P, C.POINTER(PhiengBody2), C.c_uint32, _F, _U32P, _U32P, C.c_uint32, C.c_float],
+    ),
     "phieng_sph_fluid_block_save": (C.c_int64, [_P, C.c_uint32, _U8P, C.c_uint64]),
     "phieng_sph_fluid_block_load": (C.c_int64, [_P, C.c_uint32, _U8P, C.c_uint64]),
     "phieng_sph3_fluid_block_save": (C.c_int64, [_P, C.c_uint32, _U8P, C.c_uint64]),

@@ -76,6 +76,8 @@ struct StepParams {
   uint32_t nbodies;
   uint32_t body_first;     // first of this scene's bodies in the body array
   uint32_t uniform_phase;  // phase used for every particle when !F_PHASE
+  float wind_x, wind_y;  // ambient.drag.wind, against which the buoyancy drag acts (fluid.rs:1121-1124)
+  const float2* poly;    // world-space vertices of the polygon bodies
   // ambient turbulence (F_TURB; TurbulenceConfig2, ambient.rs:108-126)
   float turb_amp, turb_freq, turb_tscale;
   uint32_t turb_seed, turb_oct;  // octaves already clamped to 1..8
@@ -95,13 +97,15 @@ __device__ __forceinline__ const StepParams& scene_params(const StepParams& P0, 
 }
 
 // Static body as the fluid sees it: shape 0 = circle (a = radius), 1 = box
-// (a, b = half extents); rotation columns x_axis = (xax, xay), y_axis =
-// (yax, yay) (crates/math/src/math.rs:34-60).
+// (a, b = half extents), 2 = polygon (vertices [vfirst, vfirst + vcount) of
+// StepParams::poly, already in world space; a, b = their centroid); rotation
+// columns x_axis = (xax, xay), y_axis = (yax, yay) (crates/math/src/math.rs:34-60).
 struct DevBody {
   int32_t shape;
   float px, py;
   float xax, xay, yax, yay;
   float a, b;
+  uint32_t vfirst, vcount;
   // half extents of the body's world-space bounding box, padded by 0.1%: a
   // particle farther than this plus its radius from the centre along x or
   // y cannot touch the body, so the exact test is skipped for it
@@ -190,8 +194,153 @@ __device__ __forceinline__ float eos(float density, float rho0, const PP& P) {
 // Particle vs body (fluid.rs:463-533, circle and box branches). Returns
 // false when separated. With cp: the contact point on the body surface
 // (circle: position + normal * radius; box: transform_point(clamped)).
+// ---- polygon walls: fluid.rs:518-530 with crates/collision/src/sat.rs ----
+// glam 0.29 Vec2::normalize_or_zero: v * (1 / |v|) when that reciprocal is
+// finite and positive, else zero.
+__device__ __forceinline__ void normalize_or_zero2(float x, float y, float& ox, float& oy) {
+  const float rcp = __fdiv_rn(1.0f, __fsqrt_rn(__fadd_rn(__fmul_rn(x, x), __fmul_rn(y, y))));
+  if (isfinite(rcp) && rcp > 0.0f) {
+    ox = __fmul_rn(x, rcp);
+    oy = __fmul_rn(y, rcp);
+  } else {
+    ox = 0.0f;
+    oy = 0.0f;
+  }
+}
+
+// project_polygon (sat.rs:88-99): min / max of axis . v, folded from
+// (f32::MAX, f32::MIN) with f32::min / max (a NaN loses).
+__device__ __forceinline__ void project_poly(const float2* __restrict__ v, uint32_t n, float ax, float ay, float& mn,
+                                             float& mx) {
+  mn = 3.40282347e38f;
+  mx = -3.40282347e38f;
+  for (uint32_t i = 0; i < n; i++) {
+    const float2 p = v[i];
+    const float d = __fadd_rn(__fmul_rn(ax, p.x), __fmul_rn(ay, p.y));
+    mn = fminf(mn, d);
+    mx = fmaxf(mx, d);
+  }
+}
+
+// point_in_polygon (sat.rs:203-220): even-odd crossing test.
+__device__ __forceinline__ bool point_in_poly(float px, float py, const float2* __restrict__ v, uint32_t n) {
+  bool inside = false;
+  uint32_t j = n - 1;
+  for (uint32_t i = 0; i < n; i++) {
+    const float2 a = v[i], b = v[j];
+    if (((a.y > py) != (b.y > py)) &&
+        (px < __fadd_rn(__fdiv_rn(__fmul_rn(__fsub_rn(b.x, a.x), __fsub_rn(py, a.y)), __fsub_rn(b.y, a.y)), a.x)))
+      inside = !inside;
+    j = i;
+  }
+  return inside;
+}
+
+// Edge i's unit normal (-e.y, e.x) of a polygon, false for an edge shorter
+// than sqrt(EPS_SQ) (sat.rs:112-116).
+__device__ __forceinline__ bool poly_edge_normal(const float2* __restrict__ v, uint32_t n, uint32_t i, float& nx,
+                                                 float& ny) {
+  const float2 a = v[i], b = v[i + 1 == n ? 0 : i + 1];
+  const float ex = __fsub_rn(b.x, a.x), ey = __fsub_rn(b.y, a.y);
+  if (__fadd_rn(__fmul_rn(ex, ex), __fmul_rn(ey, ey)) < kEpsSq) return false;
+  normalize_or_zero2(-ey, ex, nx, ny);
+  return true;
+}
+
+// sat_circle_polygon (sat.rs:104-200): the edge-normal axes (least overlap
+// wins), the closest-vertex axis (can only separate), and for a centre
+// inside the polygon the closest edge (largest signed distance). Returns the
+// axis (orientation undefined) and the penetration, or false.
+__device__ __forceinline__ bool sat_circle_poly(float cx, float cy, float r, const float2* __restrict__ v, uint32_t n,
+                                                float& axx, float& axy, float& pen) {
+  if (n < 3 || r <= 0.0f) return false;
+  float best = 3.40282347e38f, bx = 0.0f, by = 0.0f;
+  for (uint32_t i = 0; i < n; i++) {
+    float nx, ny;
+    if (!poly_edge_normal(v, n, i, nx, ny)) continue;
+    float mn, mx;
+    project_poly(v, n, nx, ny, mn, mx);
+    const float cp = __fadd_rn(__fmul_rn(nx, cx), __fmul_rn(ny, cy));
+    const float lo = __fsub_rn(cp, r), hi = __fadd_rn(cp, r);
+    if (mx < lo || hi < mn) return false;
+    const float ov = __fsub_rn(fminf(mx, hi), fmaxf(mn, lo));
+    if (ov < best) {
+      best = ov;
+      bx = nx;
+      by = ny;
+    }
+  }
+  {
+    float2 cl = v[0];
+    float dx = __fsub_rn(cx, cl.x), dy = __fsub_rn(cy, cl.y);
+    float bd = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
+    for (uint32_t i = 1; i < n; i++) {
+      const float2 q = v[i];
+      const float ex = __fsub_rn(cx, q.x), ey = __fsub_rn(cy, q.y);
+      const float d = __fadd_rn(__fmul_rn(ex, ex), __fmul_rn(ey, ey));
+      if (d < bd) {
+        bd = d;
+        cl = q;
+      }
+    }
+    dx = __fsub_rn(cx, cl.x);
+    dy = __fsub_rn(cy, cl.y);
+    if (__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)) >= kEpsSq) {
+      float ux, uy;
+      normalize_or_zero2(dx, dy, ux, uy);
+      if (!(ux == 0.0f && uy == 0.0f)) {
+        float mn, mx;
+        project_poly(v, n, ux, uy, mn, mx);
+        const float cp = __fadd_rn(__fmul_rn(ux, cx), __fmul_rn(uy, cy));
+        if (mx < __fsub_rn(cp, r) || __fadd_rn(cp, r) < mn) return false;
+      }
+    }
+  }
+  if (point_in_poly(cx, cy, v, n)) {
+    float bd = -3.40282347e38f, cnx = 0.0f, cny = 0.0f;
+    for (uint32_t i = 0; i < n; i++) {
+      float nx, ny;
+      if (!poly_edge_normal(v, n, i, nx, ny)) continue;
+      const float2 q = v[i];
+      const float dist = __fadd_rn(__fmul_rn(nx, __fsub_rn(q.x, cx)), __fmul_rn(ny, __fsub_rn(q.y, cy)));
+      if (dist > bd) {
+        bd = dist;
+        cnx = nx;
+        cny = ny;
+      }
+    }
+    if (cnx == 0.0f && cny == 0.0f) return false;
+    axx = -cnx;
+    axy = -cny;
+    pen = __fsub_rn(r, bd);
+    return true;
+  }
+  if (bx == 0.0f && by == 0.0f) return false;
+  axx = bx;
+  axy = by;
+  pen = best;
+  return true;
+}
+
 __device__ __forceinline__ bool collide(float px, float py, float pr, const DevBody& b, float& nx,
-                                        float& ny, float& depth, float2* cp = nullptr) {
+                                        float& ny, float& depth, float2* cp = nullptr,
+                                        const float2* __restrict__ poly = nullptr) {
+  if (b.shape == 2) {
+    // fluid.rs:518-530: SAT on the world-space vertices, the axis oriented
+    // from the vertex centroid towards the particle, contact point
+    // particle - normal * pr
+    float ax, ay, pen;
+    if (!sat_circle_poly(px, py, pr, poly + b.vfirst, b.vcount, ax, ay, pen)) return false;
+    if (__fadd_rn(__fmul_rn(__fsub_rn(px, b.a), ax), __fmul_rn(__fsub_rn(py, b.b), ay)) < 0.0f) {
+      ax = -ax;
+      ay = -ay;
+    }
+    nx = ax;
+    ny = ay;
+    depth = pen;
+    if (cp) *cp = make_float2(__fsub_rn(px, __fmul_rn(ax, pr)), __fsub_rn(py, __fmul_rn(ay, pr)));
+    return true;
+  }
   if (b.shape == 0) {
     float dx = __fsub_rn(px, b.px);
     float dy = __fsub_rn(py, b.py);
@@ -270,7 +419,7 @@ __device__ __forceinline__ uint32_t walls(float& x, float& y, float& vx, float& 
       continue;
     const DevBody b = *bp;
     float nx, ny, depth;
-    if (!collide(x, y, P.pr, b, nx, ny, depth)) continue;
+    if (!collide(x, y, P.pr, b, nx, ny, depth, nullptr, P.poly)) continue;
     if (depth <= 0.0f) continue;
     if (b.dyn) return k;
     x = __fadd_rn(x, __fmul_rn(nx, depth));
@@ -320,7 +469,7 @@ __device__ __forceinline__ void walls_ordered(float& x, float& y, float& vx, flo
     if (fabsf(x - b.px) > b.ex + P.pr_pad || fabsf(y - b.py) > b.ey + P.pr_pad) continue;
     float nx, ny, depth;
     float2 cp;
-    if (!collide(x, y, P.pr, b, nx, ny, depth, &cp)) continue;
+    if (!collide(x, y, P.pr, b, nx, ny, depth, &cp, P.poly)) continue;
     if (depth <= 0.0f) continue;
     x = __fadd_rn(x, __fmul_rn(nx, depth));
     y = __fadd_rn(y, __fmul_rn(ny, depth));
@@ -414,6 +563,7 @@ __device__ __forceinline__ void wall_feature(float x, float y, const DevBody* __
   float best = lim, bnx = 0.0f, bny = 0.0f;
   for (uint32_t k = 0; k < P.nbodies; k++) {
     const DevBody b = bodies[P.body_first + k];
+    if (b.shape == 2) continue;  // polygons (fluid-phase bodies only) are not part of the feature
     if (fabsf(__fsub_rn(x, b.px)) > __fadd_rn(b.ex, lim) || fabsf(__fsub_rn(y, b.py)) > __fadd_rn(b.ey, lim)) continue;
     float d, nx, ny;
     if (b.shape == 0) {

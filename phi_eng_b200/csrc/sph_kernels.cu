@@ -1220,9 +1220,9 @@ __global__ void k_buoyancy(const uint32_t* __restrict__ which, uint32_t nb, cons
     if (p <= 0.0f) continue;
     wet = true;
     const float rx = __fsub_rn(sp.x, b.px), ry = __fsub_rn(sp.y, b.py);
-    // v + (-w r.y, w r.x) - wind (the ambient wind is zero here)
-    const float vrx = __fsub_rn(__fadd_rn(d.vx, __fmul_rn(-d.w, ry)), 0.0f);
-    const float vry = __fsub_rn(__fadd_rn(d.vy, __fmul_rn(d.w, rx)), 0.0f);
+    // v + (-w r.y, w r.x) - wind
+    const float vrx = __fsub_rn(__fadd_rn(d.vx, __fmul_rn(-d.w, ry)), P.wind_x);
+    const float vry = __fsub_rn(__fadd_rn(d.vy, __fmul_rn(d.w, rx)), P.wind_y);
     const float speed = __fsqrt_rn(__fadd_rn(__fmul_rn(vrx, vrx), __fmul_rn(vry, vry)));
     const float pa = __fmul_rn(p, area);
     float fx = __fmul_rn(-sp.z, pa), fy = __fmul_rn(-sp.w, pa);

@@ -132,6 +132,8 @@ struct World2 {
   DynBufs dynb;
   DevBody* d_cbodies = nullptr;
   uint32_t cbody_cap = 0, sample_cap = 0, dyn_pcap = 0, count2_cap = 0;
+  float2* d_poly = nullptr;  // world-space polygon vertices of the last fluid-phase call
+  uint32_t poly_cap = 0;
 
   // launch tuning (phieng_sph_set_tuning)
   float buckets_per_particle = 2.0f;
@@ -551,6 +553,8 @@ StepParams make_params_for(const FluidConfig2Ffi& c, float gx, float gy, bool ma
 // word (set_clock), so cached graphs stay valid as the clock advances.
 void apply_ambient(const World2* w, StepParams& P) {
   const AmbientConfig2Ffi& a = w->ambient;
+  P.wind_x = a.wind_x;  // read by the buoyancy drag whether or not drag is enabled (fluid.rs:1124)
+  P.wind_y = a.wind_y;
   if (!(a.turbulence_enabled != 0 && a.turbulence_amplitude > 0.0f) || !w->d.scalar) return;
   P.flags |= F_TURB;
   if (a.turbulence_divergence_free) P.flags |= F_TURB_CURL;
@@ -774,6 +778,7 @@ bool ensure_dyn_buffers(World2* w, uint32_t nb, uint32_t ns) {
 // axes and the sample's area. The angles' cosines and sines come from the C
 // library, as f32::cos / f32::sin do.
 void surface_samples(const PhiengBody2& b, std::vector<float4>& pts, std::vector<float>& areas) {
+  if (b.shape_tag == PHIENG_SHAPE_POLYGON) return;  // impulse-coupled only (fluid.rs:415-418)
   const float pi = 3.14159265358979323846f;
   auto rot = [&](float x, float y, float& ox, float& oy) {  // glam Mat2 * Vec2
     ox = b.xax * x + b.yax * y;
@@ -861,10 +866,21 @@ DevBody dev_body(const PhiengBody2& b) {
   return d;
 }
 
-bool step_fluid_bodies(World2* w, PhiengBody2* bodies, uint32_t nb, float dt) {
+// Polygon vertices of one call (validated by the caller): local vertices
+// moved by each polygon body's transform (Transform2::transform_point,
+// math.rs:58-60: rotation * v + position, glam Mat2 * Vec2 = x_axis * v.x +
+// y_axis * v.y), as fluid.rs:519-523 builds poly_scratch for every test.
+struct PolyIn {
+  const float* xy = nullptr;
+  const uint32_t* first = nullptr;
+  const uint32_t* count = nullptr;
+};
+
+bool step_fluid_bodies(World2* w, PhiengBody2* bodies, uint32_t nb, float dt, const PolyIn& pin = PolyIn()) {
   if (!w->cfg.enabled || w->n == 0 || dt <= 0.0f) return true;  // step_fluid guards (fluid.rs:550-552)
   if (unsupported(w)) return false;
   if (!prepare(w)) return false;
+  std::vector<float2> wv;  // world-space polygon vertices
   std::vector<DevBody> db(nb);
   std::vector<DynBody> dy(nb);
   std::vector<float4> pts;
@@ -874,6 +890,23 @@ bool step_fluid_bodies(World2* w, PhiengBody2* bodies, uint32_t nb, float dt) {
   for (uint32_t k = 0; k < nb; k++) {
     const PhiengBody2& b = bodies[k];
     db[k] = dev_body(b);
+    if (b.shape_tag == PHIENG_SHAPE_POLYGON) {
+      DevBody& d = db[k];
+      d.shape = 2;
+      d.vfirst = (uint32_t)wv.size();
+      d.vcount = pin.count[k];
+      float sx = 0.0f, sy = 0.0f;  // polygon_centroid (sat.rs:77-83): fold from zero, then / len
+      for (uint32_t i = 0; i < pin.count[k]; i++) {
+        const float lx = pin.xy[2 * ((size_t)pin.first[k] + i)], ly = pin.xy[2 * ((size_t)pin.first[k] + i) + 1];
+        const float2 v = make_float2((b.xax * lx + b.yax * ly) + b.px, (b.xay * lx + b.yay * ly) + b.py);
+        wv.push_back(v);
+        sx = sx + v.x;
+        sy = sy + v.y;
+      }
+      d.a = sx / (float)pin.count[k];
+      d.b = sy / (float)pin.count[k];
+      d.ex = d.ey = INFINITY;  // no bounding-box reject for polygons
+    }
     any_dyn = any_dyn || db[k].dyn;
     DynBody& d = dy[k];
     d.vx = b.vx;
@@ -889,6 +922,17 @@ bool step_fluid_bodies(World2* w, PhiengBody2* bodies, uint32_t nb, float dt) {
     if (d.sample_count) buoy.push_back(k);
   }
   if (!ensure_dyn_buffers(w, nb, (uint32_t)pts.size())) return false;
+  if (wv.size() > w->poly_cap) {
+    cudaStreamSynchronize(w->stream);
+    dfree(w->d_poly);
+    const uint32_t c = std::max<uint32_t>(64, (uint32_t)wv.size());
+    if (!dalloc(w, w->d_poly, c)) return false;
+    w->poly_cap = c;
+  }
+  if (!wv.empty() && !cuda_ok(w, cudaMemcpyAsync(w->d_poly, wv.data(), sizeof(float2) * wv.size(),
+                                                  cudaMemcpyHostToDevice, w->stream),
+                              "upload polygon vertices"))
+    return false;
   DynBufs y = w->dynb;
   y.nbuoy = (uint32_t)buoy.size();
   cudaStream_t st = w->stream;
@@ -911,6 +955,7 @@ bool step_fluid_bodies(World2* w, PhiengBody2* bodies, uint32_t nb, float dt) {
   StepParams P = make_params_for(w->cfg, w->gx, w->gy, w->mass_uniform, w->mass_value, w->phase_uniform,
                                  w->phase_value, w->plan, 0, nb, sub);
   if (any_dyn) P.flags |= F_DYNAMIC;
+  P.poly = w->d_poly;
   apply_ambient(w, P);
   set_clock(w, P, w->time);
   FluidBufs dB = w->d;
@@ -1084,6 +1129,7 @@ void phieng_world_free(World2* w) {
     dfree(w->d_block_save);
     dfree(w->d_svp);
     dfree(w->d_cbodies);
+    dfree(w->d_poly);
     dfree(w->dynb.dyn);
     dfree(w->dynb.samples);
     dfree(w->dynb.areas);
@@ -1233,6 +1279,38 @@ int32_t phieng_sph_step_fluid(World2* w, PhiengBody2* bodies, uint32_t nbodies, 
   for (uint32_t k = 0; k < nbodies; k++)
     if (!body_valid(bodies[k])) return 0;
   return step_fluid_bodies(w, bodies, nbodies, dt) ? 1 : 0;
+}
+
+constexpr uint32_t kMaxPolyVerts = 1u << 20;
+
+int32_t phieng_sph_step_fluid_poly(World2* w, PhiengBody2* bodies, uint32_t nbodies, const float* poly_xy,
+                                   const uint32_t* poly_first, const uint32_t* poly_count, uint32_t poly_nverts,
+                                   float dt) {
+  if (!w || w->is_batch() || (nbodies && !bodies) || nbodies > kMaxCallBodies || poly_nverts > kMaxPolyVerts)
+    return 0;
+  uint64_t total = 0;
+  for (uint32_t k = 0; k < nbodies; k++) {
+    const PhiengBody2& b = bodies[k];
+    if (b.shape_tag != PHIENG_SHAPE_POLYGON) {
+      if (!body_valid(b)) return 0;
+      continue;
+    }
+    if (!poly_xy || !poly_first || !poly_count) return 0;
+    const float t[] = {b.px, b.py, b.xax, b.xay, b.yax, b.yay, b.vx, b.vy, b.w, b.inv_mass, b.inv_inertia};
+    for (float x : t)
+      if (!std::isfinite(x)) return 0;
+    const uint64_t f = poly_first[k], c = poly_count[k];
+    if (c < 3 || f + c > poly_nverts) return 0;
+    for (uint64_t i = 2 * f; i < 2 * (f + c); i++)
+      if (!std::isfinite(poly_xy[i])) return 0;
+    total += c;
+  }
+  if (total > kMaxPolyVerts) return 0;
+  PolyIn pin;
+  pin.xy = poly_xy;
+  pin.first = poly_first;
+  pin.count = poly_count;
+  return step_fluid_bodies(w, bodies, nbodies, dt, pin) ? 1 : 0;
 }
 
 int32_t phieng_world_set_fluid_config(World2* w, const FluidConfig2Ffi* cfg) {

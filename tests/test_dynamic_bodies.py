@@ -100,7 +100,7 @@ def drift(arr, dt, angles):
             b.px = f32(b.px) + f32(b.vx) * f32(dt)
             b.py = f32(b.py) + f32(b.vy) * f32(dt)
             angles[k] = f32(angles[k]) + f32(b.w) * f32(dt)
-            if b.shape_tag == _abi.SHAPE_BOX:
+            if b.shape_tag in (_abi.SHAPE_BOX, _abi.SHAPE_POLYGON):
                 set_angle(b, float(angles[k]))
 
 
@@ -118,12 +118,52 @@ def oracle_world(pts, cfg=None):
     return o
 
 
-def run_oracle(o, arr, frames, dt=1 / 60, mode=REF_SEQ):
+def run_oracle(o, arr, frames, dt=1 / 60, mode=REF_SEQ, poly=None):
     angles = [0.0] * len(arr)
     for _ in range(frames):
         kick(arr, dt)
-        o.step_fluid(arr, dt, mode)
+        o.step_fluid(arr, dt, mode, poly)
         drift(arr, dt, angles)
+
+
+def polygon_body(px, py, verts, dynamic=False, inv_mass=2.0, inv_inertia=6.0, angle=0.0):
+    """A Shape2::Polygon body; returns (body, local vertices)."""
+    b = PhiengBody2()
+    b.shape_tag = _abi.SHAPE_POLYGON
+    b.px, b.py = px, py
+    set_angle(b, angle)
+    b.is_static = 0 if dynamic else 1
+    if dynamic:
+        b.inv_mass, b.inv_inertia = inv_mass, inv_inertia
+    return b, np.asarray(verts, np.float32)
+
+
+def poly_arrays(entries):
+    """(xy, first, count) for phieng_sph_step_fluid_poly from per-body vertex
+    arrays (None for non-polygons)."""
+    xy, first, count = [], [], []
+    for v in entries:
+        first.append(sum(len(a) for a in xy))
+        count.append(0 if v is None else len(v))
+        if v is not None:
+            xy.append(v)
+    flat = np.concatenate(xy).astype(np.float32) if xy else np.zeros((0, 2), np.float32)
+    return np.ascontiguousarray(flat), np.asarray(first, np.uint32), np.asarray(count, np.uint32)
+
+
+def point_in_poly(x, y, v):
+    inside = False
+    j = len(v) - 1
+    for i in range(len(v)):
+        if (v[i][1] > y) != (v[j][1] > y) and x < (v[j][0] - v[i][0]) * (y - v[i][1]) / (v[j][1] - v[i][1]) + v[i][0]:
+            inside = not inside
+        j = i
+    return inside
+
+
+RAMP = [(-1.0, -0.4), (1.0, -0.4), (-1.0, 0.6)]          # triangle, counter-clockwise
+ELL = [(0.0, 0.0), (0.8, 0.0), (0.8, 0.2), (0.2, 0.2), (0.2, 0.7), (0.0, 0.7)]  # concave L
+PENTAGON = [(0.25 * math.cos(2 * math.pi * k / 5), 0.25 * math.sin(2 * math.pi * k / 5)) for k in range(5)]
 
 
 # ---- oracle (CPU) -----------------------------------------------------------
@@ -153,6 +193,51 @@ def test_oracle_heavy_box_sinks_light_box_floats():
         run_oracle(o, arr, 200)
         ends[density] = float(arr[3].py)
     assert ends[3.0] < ends[0.3] - 0.2, ends
+
+
+def test_oracle_wind_drifts_floating_body():
+    """fluid.rs:1467-1494 on the oracle: a box floating in the settled tank
+    drifts downwind under ambient.drag.wind = (3, 0)."""
+    o = oracle_world(lattice(-0.5, -0.5, 12, 6, 0.25))
+    for _ in range(200):
+        o.step(1 / 60, REF_SEQ)
+    o.set_wind(3.0, 0.0)
+    arr = body_list([static_box(*p, *e) for p, e in TANK] + [dynamic_box(2.0, 1.6, 0.3, 0.3, 0.5)])
+    x0 = arr[3].px
+    run_oracle(o, arr, 400)
+    assert arr[3].px > x0 + 0.05, (x0, arr[3].px)
+
+
+def test_oracle_polygon_ramp_holds_and_deflects_fluid():
+    """A static triangular ramp in the tank (fluid.rs:518-530): fluid poured
+    on it ends outside the triangle and runs down its slope."""
+    o = OracleWorld()
+    for (px, py), (hx, hy) in TANK:
+        o.add_box(px, py, hx, hy)
+    o.add_particles(lattice(-0.2, 1.0, 8, 4, 0.2))
+    ramp, v = polygon_body(1.0, 0.2, RAMP)
+    arr = body_list([static_box(*p, *e) for p, e in TANK] + [ramp])
+    poly = poly_arrays([None, None, None, v])
+    run_oracle(o, arr, 240, poly=poly)
+    s = o.state()
+    world = [(x + 1.0, y + 0.2) for x, y in RAMP]
+    assert np.isfinite(s).all()
+    assert sum(point_in_poly(x, y, world) for x, y in s[:, :2]) == 0
+    assert s[:, 0].mean() > 0.9  # ran down the slope towards +x
+
+
+def test_oracle_polygon_body_takes_impulses():
+    """A dynamic pentagon hit by falling fluid picks up velocity and spin
+    from the boundary impulses (polygons get no buoyancy, fluid.rs:415-418)."""
+    o = oracle_world(lattice(1.5, 1.2, 6, 3, 0.2))
+    pent, v = polygon_body(2.0, 0.6, PENTAGON, dynamic=True)
+    arr = body_list([static_box(*p, *e) for p, e in TANK] + [pent])
+    poly = poly_arrays([None, None, None, v])
+    vy0 = []
+    for _ in range(40):
+        o.step_fluid(arr, 1 / 60, REF_SEQ, poly)  # no kick: only the fluid moves the body
+        vy0.append(arr[3].vy)
+    assert min(vy0) < 0.0 and arr[3].is_sleeping == 0
 
 
 def test_oracle_reaction_hand_computed():
@@ -191,6 +276,25 @@ def test_step_fluid_arguments(lib=None):
     bad = body_list([dynamic_circle(0.0, 0.0, 1.0, 1.0)])
     bad[0].vx = float("nan")
     assert lib.phieng_sph_step_fluid(w, bad, 1, 0.01) == 0
+    # polygons: only through phieng_sph_step_fluid_poly, with a valid vertex range
+    pb, v = polygon_body(0.0, 0.0, RAMP)
+    arr = body_list([pb])
+    xy, first, count = poly_arrays([v])
+    U = C.POINTER(C.c_uint32)
+
+    def call(xy_, first_, count_, nverts):
+        return lib.phieng_sph_step_fluid_poly(w, arr, 1, None if xy_ is None else fp(xy_),
+                                             None if first_ is None else first_.ctypes.data_as(U),
+                                             None if count_ is None else count_.ctypes.data_as(U), nverts, 0.01)
+
+    assert lib.phieng_sph_step_fluid(w, arr, 1, 0.01) == 0
+    assert call(xy, first, count, 3) == 1
+    assert call(None, first, count, 3) == 0
+    assert call(xy, first, count, 2) == 0  # range past the vertex count
+    assert call(xy, first, np.asarray([2], np.uint32), 3) == 0  # fewer than 3 vertices
+    xy_bad = xy.copy()
+    xy_bad[1, 0] = np.inf
+    assert call(xy_bad, first, count, 3) == 0
     lib.phieng_world_free(w)
 
 
@@ -225,10 +329,27 @@ def body_bits(arr):
     return np.array([[b.vx, b.vy, b.w, b.px, b.py] for b in arr], np.float32).view(np.uint32)
 
 
-def coupled_parity(cfg, bodies, frames, settle=60, pts=None):
+def set_gpu_ambient(lib, w, wind=(0.0, 0.0), turb=None):
+    a = _abi.default_ambient()
+    a.wind_x, a.wind_y = wind
+    if turb:
+        a.turbulence_enabled = 1
+        a.turbulence_amplitude = turb["amplitude"]
+        a.turbulence_frequency = turb.get("frequency", 1.0)
+        a.turbulence_seed = turb.get("seed", 0)
+        a.turbulence_divergence_free = 1 if turb.get("divergence_free") else 0
+    assert lib.phieng_world_set_ambient_config(w, C.byref(a)) == 1
+
+
+def coupled_parity(cfg, bodies, frames, settle=60, pts=None, wind=None, turb=None, poly=None):
     pts = lattice(-0.5, -0.5, 16, 8, 0.25) if pts is None else pts
     o = oracle_world(pts, cfg)
     lib, w = gpu_world(pts, cfg)
+    if wind or turb:
+        set_gpu_ambient(lib, w, wind or (0.0, 0.0), turb)
+        o.set_wind(*(wind or (0.0, 0.0)))
+        if turb:
+            o.set_turbulence(**turb)
     for _ in range(settle):
         o.step(1 / 60, JACOBI)
         lib.phieng_world_step(w, 1 / 60)
@@ -239,8 +360,14 @@ def coupled_parity(cfg, bodies, frames, settle=60, pts=None):
     for f in range(frames):
         kick(a, dt)
         kick(b, dt)
-        o.step_fluid(a, dt, JACOBI)
-        assert lib.phieng_sph_step_fluid(w, b, len(b), dt) == 1
+        o.step_fluid(a, dt, JACOBI, poly)
+        if poly is None:
+            assert lib.phieng_sph_step_fluid(w, b, len(b), dt) == 1
+        else:
+            xy, first, count = poly
+            U = C.POINTER(C.c_uint32)
+            assert lib.phieng_sph_step_fluid_poly(w, b, len(b), fp(xy), first.ctypes.data_as(U),
+                                                  count.ctypes.data_as(U), len(xy), dt) == 1
         drift(a, dt, angles_a)
         drift(b, dt, angles_b)
         assert (body_bits(a) == body_bits(b)).all(), f"bodies differ at frame {f}"
@@ -276,6 +403,33 @@ def test_step_fluid_bit_exact_friction_and_substeps():
     c.max_substeps = 4
     c.drag = 2.0
     coupled_parity(c, floating_bodies(), 100)
+
+
+@pytest.mark.gpu
+def test_step_fluid_bit_exact_wind_and_turbulence():
+    """The world's ambient config in the fluid phase: the wind in the
+    buoyancy drag (fluid.rs:1121-1124) and curl turbulence at the world clock,
+    bodies and particles bit for bit against the oracle."""
+    c = default_config()
+    c.drag = 2.0
+    coupled_parity(c, floating_bodies(), 90, wind=(3.0, -0.5),
+                   turb=dict(amplitude=3.0, frequency=0.7, seed=11, divergence_free=True))
+
+
+@pytest.mark.gpu
+def test_step_fluid_bit_exact_polygons():
+    """A static triangular ramp, a static concave L and a dynamic rotating
+    pentagon among the walls, with friction: bodies and particles bit for bit
+    against the oracle."""
+    c = default_config()
+    c.wall_friction = 0.3
+    ramp, vr = polygon_body(1.2, 0.3, RAMP, angle=0.2)
+    ell, ve = polygon_body(2.8, -0.45, ELL)
+    pent, vp = polygon_body(3.6, 1.2, PENTAGON, dynamic=True, angle=0.4)
+    bodies = [static_box(*p, *e) for p, e in TANK] + [ramp, ell, pent, dynamic_circle(0.6, 1.8, 0.2, 0.5)]
+    poly = poly_arrays([None, None, None, vr, ve, vp, None])
+    a = coupled_parity(c, bodies, 100, pts=lattice(-0.4, 0.8, 16, 10, 0.2), poly=poly)
+    assert abs(a[5].vx) + abs(a[5].vy) > 0  # the pentagon took impulses
 
 
 @pytest.mark.gpu
