@@ -455,6 +455,14 @@ uint32_t phieng_sph_debug_sorted(World2* world, uint32_t* ids, uint32_t* keys, u
 uint32_t phieng_sph_debug_neighbors(World2* world, uint32_t* counts, uint32_t* lists,
                                     uint32_t max_per, uint32_t max);
 
+/* Boundary ghosts (FluidConfig2Ffi.boundary_particles, fluid.rs:617-818):
+ * the count of the last generated set, and up to max positions (x, y pairs,
+ * grouped by grid cell, generation order inside a cell) into xy (may be
+ * null); *regens (may be null) = how many times they were generated
+ * (boundary_regens: once per change of the static bodies or of h, mass, rest
+ * density). 0 for a null world. */
+uint32_t phieng_sph_ghosts(World2* world, float* xy, uint32_t max, uint64_t* regens);
+
 /* Allocate the device arrays for n particles now (as std::vector::reserve),
  * and the bucket arrays of the largest grid a plan for n particles can use,
  * so the first step allocates nothing. 1 ok, 0 for a null world, a batch, no

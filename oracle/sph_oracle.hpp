@@ -72,6 +72,7 @@ struct Config {
 struct Body {
   int shape = 1;  // 0 = circle (a = radius), 1 = box (a, b = half extents), 2 = polygon
   std::vector<float> poly;  // polygon: world-space vertices x0, y0, x1, y1, ... (transform_point of the local ones)
+  std::vector<float> poly_local;  // polygon: the body-frame vertices (boundary ghosts sample these)
   float px = 0, py = 0;
   float xax = 1, xay = 0, yax = 0, yay = 1;  // rotation columns x_axis, y_axis
   float a = 0, b = 0;
@@ -363,6 +364,120 @@ class Fluid {
     return n;
   }
 
+  // ---- boundary ghosts (fluid.rs:617-818) ----
+  struct Ghost {
+    float x, y;
+    R density, pressure;
+  };
+  std::vector<Ghost> ghosts;
+  std::unordered_map<uint64_t, std::vector<uint32_t>> ghost_grid;
+
+  // refresh_boundaries (fluid.rs:665-741) + rebuild_boundary_grid
+  // (fluid.rs:744-756) from the static bodies, in f32 as the reference. Its
+  // output is a function of the bodies and the config only, so regenerating
+  // every substep gives what the reference's fingerprint-triggered refresh
+  // keeps.
+  void refresh_ghosts() {
+    ghosts.clear();
+    ghost_grid.clear();
+    const float hk = std::max(cfg.smoothing_length, kEps);
+    const float spacing = std::max(hk * 0.5f, kEps);
+    const float pi = Consts<float>::pi();
+    auto cnt = [](float v) -> uint64_t {  // `as usize`, at least 1
+      uint64_t n = (v > 0.0f) ? (v >= 1.8446744e19f ? UINT64_MAX : (uint64_t)v) : 0;
+      return std::max<uint64_t>(n, 1);
+    };
+    for (const Body& b : bodies) {
+      if (!b.is_static) continue;
+      auto put = [&](float lx, float ly) {
+        ghosts.push_back({(b.xax * lx + b.yax * ly) + b.px, (b.xay * lx + b.yay * ly) + b.py, 0, 0});
+      };
+      if (b.shape == 0) {
+        const uint64_t n = cnt(std::ceil((2.0f * pi * b.a) / spacing));
+        for (uint64_t k = 0; k < n; k++) {
+          const float a = 2.0f * pi * (float)k / (float)n;
+          put(std::cos(a) * b.a, std::sin(a) * b.a);
+        }
+      } else if (b.shape == 1) {
+        const float hx = b.a, hy = b.b;
+        // fluid.rs:686-691: (origin, tangent) per edge, in this order
+        const float o[4][2] = {{-hx, -hy}, {-hx, hy}, {-hx, -hy}, {hx, -hy}};
+        const float tg[4][2] = {{0, 1}, {0, 1}, {1, 0}, {1, 0}};
+        for (int e = 0; e < 4; e++) {
+          const float ext = (tg[e][0] == 1.0f) ? hx : hy;
+          const uint64_t n = cnt(std::ceil((2.0f * ext) / spacing));
+          for (uint64_t k = 0; k < n; k++) {
+            const float t = ((float)k + 0.5f) / (float)n;
+            const float sc = 2.0f * ext * t;
+            put(o[e][0] + tg[e][0] * sc, o[e][1] + tg[e][1] * sc);
+          }
+        }
+      } else {
+        const size_t nv = b.poly_local.size() / 2;
+        for (size_t e = 0; e < nv; e++) {
+          const size_t f = (e + 1) % nv;
+          const float ax = b.poly_local[2 * e], ay = b.poly_local[2 * e + 1];
+          const float ex = b.poly_local[2 * f] - ax, ey = b.poly_local[2 * f + 1] - ay;
+          const float len = std::sqrt(ex * ex + ey * ey);
+          if (len < kEps) continue;
+          const uint64_t n = cnt(std::ceil(len / spacing));
+          for (uint64_t k = 0; k < n; k++) {
+            const float t = ((float)k + 0.5f) / (float)n;
+            put(ax + ex * t, ay + ey * t);
+          }
+        }
+      }
+    }
+    for (uint32_t i = 0; i < ghosts.size(); i++) {
+      const Ghost& g = ghosts[i];
+      if (!std::isfinite(g.x) || !std::isfinite(g.y)) continue;
+      ghost_grid[cell_key(sat_i32(std::floor(g.x / hk)), sat_i32(std::floor(g.y / hk)))].push_back(i);
+    }
+  }
+
+  // compute_boundary_density_pressure (fluid.rs:804-818)
+  void ghost_density(R h) {
+    std::vector<uint32_t> nb;
+    for (Ghost& g : ghosts) {
+      neighbors_of((R)g.x, (R)g.y, particles, nb);
+      R rho = 0;
+      for (uint32_t j : nb) {
+        const R dx = particles[j].x - (R)g.x, dy = particles[j].y - (R)g.y;
+        rho += particles[j].mass * poly6(dx * dx + dy * dy, h);
+      }
+      g.density = rclamp(rho, (R)0, (R)3 * rmax((R)cfg.rest_density, (R)kEps));
+      g.pressure = pressure(rho, (R)cfg.rest_density, (R)cfg.stiffness, (R)cfg.gamma, pow_mode);
+    }
+  }
+
+  // ghost pressure on a fluid particle (fluid.rs:977-988), after its fluid
+  // pairs: boundary_near's cells and filter, -grad W * (m_g (q_i + q_g))
+  void ghost_pressure_force(R px, R py, R q_i, R h, R& fxi, R& fyi) const {
+    const R hg = (R)cfg.smoothing_length;
+    const R m = (R)std::max(cfg.particle_mass, kEps);
+    int32_t cx, cy;
+    cell_of(px, py, cx, cy);
+    for (int oy = -1; oy <= 1; oy++) {
+      for (int ox = -1; ox <= 1; ox++) {
+        auto it = ghost_grid.find(cell_key((int32_t)((uint32_t)cx + (uint32_t)ox), (int32_t)((uint32_t)cy + (uint32_t)oy)));
+        if (it == ghost_grid.end()) continue;
+        for (uint32_t k : it->second) {
+          const Ghost& g = ghosts[k];
+          const R ex = (R)g.x - px, ey = (R)g.y - py;
+          if (!(ex * ex + ey * ey < hg * hg)) continue;
+          const R dx = px - (R)g.x, dy = py - (R)g.y;
+          const R dist = std::sqrt(dx * dx + dy * dy);
+          R gx, gy;
+          spiky_grad(dx, dy, dist, h, gx, gy);
+          const R rb = rmax(g.density, (R)kEps);
+          const R s = m * (q_i + g.pressure / (rb * rb));
+          fxi -= gx * s;
+          fyi -= gy * s;
+        }
+      }
+    }
+  }
+
   // ---- grid (fluid.rs:330-386) ----
   static uint64_t cell_key(int32_t cx, int32_t cy) {
     return ((uint64_t)(uint32_t)cx << 32) | (uint64_t)(uint32_t)cy;
@@ -475,6 +590,7 @@ class Fluid {
           }
         }
       }
+      if (cfg.boundary_particles) ghost_pressure_force(pix, piy, p_i / (rho_i * rho_i), h, fxi, fyi);
       fx[i] = fxi;
       fy[i] = fyi;
     }
@@ -1037,6 +1153,10 @@ class Fluid {
     R h = rmax((R)cfg.smoothing_length, (R)kEps);
     rebuild_grid();
     compute_density_pressure(h);
+    if (cfg.boundary_particles) {  // fluid.rs:929-937
+      refresh_ghosts();
+      ghost_density(h);
+    }
     compute_forces(h);
     integrate(h, dt, mode);
     extra_ax.clear();

@@ -131,6 +131,17 @@ void orc_set_gravity(void* h, float gx, float gy) {
   o->f64.gy = (double)gy;
 }
 
+// the boundary ghosts of the last substep, generation order
+uint32_t orc_ghosts(void* h, float* xy, uint32_t max) {
+  Orc* o = static_cast<Orc*>(h);
+  const auto& g = o->f32.ghosts;
+  for (uint32_t i = 0; xy && i < std::min<size_t>(g.size(), max); i++) {
+    xy[2 * i] = g[i].x;
+    xy[2 * i + 1] = g[i].y;
+  }
+  return (uint32_t)g.size();
+}
+
 // world.ambient.drag.wind (read by the buoyancy drag)
 void orc_set_wind(void* h, float wx, float wy) {
   Orc* o = static_cast<Orc*>(h);
@@ -221,6 +232,8 @@ void orc_step_fluid_poly(void* h, PhiengBody2* bodies, uint32_t nb, const float*
         const float lx = poly_xy[2 * i], ly = poly_xy[2 * i + 1];
         b.poly.push_back((q.xax * lx + q.yax * ly) + q.px);  // rotation * v + position (math.rs:58-60)
         b.poly.push_back((q.xay * lx + q.yay * ly) + q.py);
+        b.poly_local.push_back(lx);
+        b.poly_local.push_back(ly);
       }
     b.px = q.px;
     b.py = q.py;

@@ -48,7 +48,22 @@ enum StepFlags : uint32_t {
   F_WIDE_NB = 1u << 8,   // h*h > max(h, EPS)^2 (h <= 0 from a snapshot): poly6 keeps its range test for neighbours
   F_TURB = 1u << 9,      // ambient turbulence on (enabled and amplitude > 0)
   F_TURB_CURL = 1u << 10,  // turbulence as divergence-free curl noise
+  F_GHOST = 1u << 11,      // boundary ghost particles (boundary_particles)
 };
+
+// One cell of the boundary ghosts' hash grid: ghosts [start, start + count)
+// of the cell-sorted ghost array lie in cell (cx, cy); count 0 = empty slot.
+struct GhostCell {
+  int32_t cx, cy;
+  uint32_t start, count;
+};
+
+// Open-addressing slot of a ghost cell (linear probing from here).
+__host__ __device__ inline uint32_t ghost_cell_hash(int32_t cx, int32_t cy, uint32_t mask) {
+  uint32_t h = (uint32_t)cx * 0x9E3779B1u ^ ((uint32_t)cy * 0x85EBCA77u + 0x165667B1u);
+  h ^= h >> 15;
+  return h & mask;
+}
 
 struct StepParams {
   GridPlan grid;
@@ -78,6 +93,14 @@ struct StepParams {
   uint32_t uniform_phase;  // phase used for every particle when !F_PHASE
   float wind_x, wind_y;  // ambient.drag.wind, against which the buoyancy drag acts (fluid.rs:1121-1124)
   const float2* poly;    // world-space vertices of the polygon bodies
+  // boundary ghosts (F_GHOST, fluid.rs:617-818): cell-sorted positions, their
+  // q = p / max(rho, EPS)^2 of the current substep, the cell table
+  const float2* gpos;
+  float* gq;
+  const GhostCell* gtab;
+  uint32_t gtab_mask, nghost;
+  float gmass;  // particle_mass.max(EPS)
+  float rest0;  // config rest_density (the ghosts' EOS reference)
   // ambient turbulence (F_TURB; TurbulenceConfig2, ambient.rs:108-126)
   float turb_amp, turb_freq, turb_tscale;
   uint32_t turb_seed, turb_oct;  // octaves already clamped to 1..8

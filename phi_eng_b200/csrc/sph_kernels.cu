@@ -641,6 +641,80 @@ __device__ __forceinline__ void integrate_write(uint32_t id, float2 pi, float2 v
   count_key(count_out, nk);  // bucket counts of the next substep's sort
 }
 
+// ---------------------------------------------------------------- boundary ghosts
+// Ghost pressure on a fluid particle (fluid.rs:977-988): after its fluid
+// pairs, every ghost within h of it, visited as boundary_near does (cells
+// (floor(x / h) + ox, floor(y / h) + oy) for oy, ox = -1..1, h the config's
+// smoothing length; each cell's ghosts in generation order), adds
+// -grad W(p_i - g) * (m_g * (q_i + q_g)). Out of line: only worlds with
+// ghosts pay for it.
+static __device__ __noinline__ float2 ghost_force(float px, float py, float q_i, float fx, float fy,
+                                                  const float2* __restrict__ gpos, const float* __restrict__ gq,
+                                                  const GhostCell* __restrict__ tab, uint32_t mask, float gmass,
+                                                  float hg, float hg2, float hk, float c_spiky) {
+  const int32_t cx = __float2int_rd(__fdiv_rn(px, hg)), cy = __float2int_rd(__fdiv_rn(py, hg));
+  for (int oy = -1; oy <= 1; oy++) {
+    for (int ox = -1; ox <= 1; ox++) {
+      const int32_t qx = (int32_t)((uint32_t)cx + (uint32_t)ox), qy = (int32_t)((uint32_t)cy + (uint32_t)oy);
+      uint32_t slot = ghost_cell_hash(qx, qy, mask);
+      GhostCell c = tab[slot];
+      for (uint32_t probe = 0; probe <= mask && c.count != 0 && (c.cx != qx || c.cy != qy); probe++) {
+        slot = (slot + 1) & mask;
+        c = tab[slot];
+      }
+      if (c.count == 0 || c.cx != qx || c.cy != qy) continue;
+      for (uint32_t k = c.start; k < c.start + c.count; k++) {
+        const float2 g = gpos[k];
+        const float ex = __fsub_rn(g.x, px), ey = __fsub_rn(g.y, py);
+        if (!(__fadd_rn(__fmul_rn(ex, ex), __fmul_rn(ey, ey)) < hg2)) continue;
+        const float dx = __fsub_rn(px, g.x), dy = __fsub_rn(py, g.y);
+        const float dist = __fsqrt_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)));
+        float gx = 0.0f, gy = 0.0f;  // spiky_grad, zero outside (EPS, h) (fluid.rs:278-285)
+        if (!(dist >= hk || dist < kEps)) {
+          const float hr = __fsub_rn(hk, dist);
+          const float sc = __fmul_rn(__fmul_rn(c_spiky, hr), hr);
+          gx = __fmul_rn(__fdiv_rn(dx, dist), sc);
+          gy = __fmul_rn(__fdiv_rn(dy, dist), sc);
+        }
+        const float mt = __fmul_rn(gmass, __fadd_rn(q_i, gq[k]));
+        fx = __fsub_rn(fx, __fmul_rn(gx, mt));
+        fy = __fsub_rn(fy, __fmul_rn(gy, mt));
+      }
+    }
+  }
+  return make_float2(fx, fy);
+}
+
+// Ghost density and pressure from the fluid (compute_boundary_density_pressure,
+// fluid.rs:804-818): the fluid candidates around the ghost in the reference's
+// cell order, m_j * poly6 for those within h; density clamped to
+// [0, 3 max(rest, EPS)], the pressure from the unclamped sum with the
+// config's rest density; stored as q = p / max(density, EPS)^2.
+__global__ void __launch_bounds__(256) k_ghost_density(const float2* __restrict__ spos,
+                                                       const float* __restrict__ smass,
+                                                       const uint32_t* __restrict__ start, StepParams P) {
+  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= P.nghost) return;
+  const float2 b = P.gpos[g];
+  float rho = 0.0f;
+  const uint32_t key = bucket_key(b.x, b.y, P.grid);
+  if (key != P.grid.sentinel) {
+    const bool mass = (P.flags & F_MASS) != 0;
+    for_each_candidate(key, start, P.grid, [&](int j) {
+      const float2 a = __ldg(&spos[j]);
+      const float dx = __fsub_rn(a.x, b.x), dy = __fsub_rn(a.y, b.y);
+      rho = __fadd_rn(rho, density_term(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)),
+                                        mass ? __ldg(&smass[j]) : P.mass, P));
+    });
+  }
+  float dens = rho;
+  if (dens < 0.0f) dens = 0.0f;
+  if (dens > P.rho_cap) dens = P.rho_cap;
+  const float p = eos(rho, P.rest0, P);
+  const float rc = fmaxf(dens, kEps);
+  P.gq[g] = __fdiv_rn(p, __fmul_rn(rc, rc));
+}
+
 template <bool MASS, bool DEBUG, bool BATCH, bool PLAIN>
 __global__ void __launch_bounds__(256) k_force_integrate(
     const float2* __restrict__ spos, const float2* __restrict__ svel, const float2* __restrict__ sdq,
@@ -664,6 +738,12 @@ __global__ void __launch_bounds__(256) k_force_integrate(
   FeatAcc fa;
   neighbour_sums<MASS, false, PLAIN>(s, k, n, pi, vi, rho_i, q_i, m_i, spos, svel, sdq, smass, nullptr, start, nmask,
                                      P, fx, fy, sx, sy, fa);
+  if (!BATCH && (P.flags & F_GHOST)) {
+    const float2 f = ghost_force(pi.x, pi.y, q_i, fx, fy, P.gpos, P.gq, P.gtab, P.gtab_mask, P.gmass, P.grid.hg,
+                                 P.hg2, P.hk, P.c_spiky);
+    fx = f.x;
+    fy = f.y;
+  }
   if (DEBUG) {
     dbg_force[id] = make_float2(fx, fy);
     return;
@@ -961,6 +1041,11 @@ void enqueue_sort_and_ranges(const FluidBufs& b, uint32_t n, const StepParams& P
   k_fixup<<<cdiv(n, 256), 256, 0, st>>>(b.tkey, b.tid, b.start, n, b.skey, b.sid, ga);
   // the counts of the next sort accumulate from zero (K6)
   cudaMemsetAsync(b.count, 0, sizeof(uint32_t) * b.count_len, st);
+}
+
+void enqueue_ghost_density(const FluidBufs& b, const StepParams& P, cudaStream_t st) {
+  if (!(P.flags & F_GHOST) || P.nghost == 0) return;
+  k_ghost_density<<<cdiv(P.nghost, 256), 256, 0, st>>>(b.spos, b.smass, b.start, P);
 }
 
 void enqueue_density(const FluidBufs& b, uint32_t n, const StepParams& P, cudaStream_t st, float2* svp) {

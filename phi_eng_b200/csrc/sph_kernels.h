@@ -94,6 +94,10 @@ struct BucketSort {
 };
 void enqueue_bucket_place(const BucketSort& bs, uint32_t n, uint32_t m, bool by_slot, cudaStream_t st);
 
+// Boundary ghosts' density / pressure from the fluid of the current sort
+// (after K5, before K6); no-op unless P has F_GHOST.
+void enqueue_ghost_density(const FluidBufs& b, const StepParams& P, cudaStream_t st);
+
 // K5: density + EOS in sorted order. svp (optional, sorted order): also
 // (m / max(density, EPS), q max(density, EPS)^2) per particle, the
 // neighbour factors of the closure feature sums.

@@ -134,6 +134,14 @@ struct World2 {
   uint32_t cbody_cap = 0, sample_cap = 0, dyn_pcap = 0, count2_cap = 0;
   float2* d_poly = nullptr;  // world-space polygon vertices of the last fluid-phase call
   uint32_t poly_cap = 0;
+  // boundary ghosts (boundary_particles): regenerated when their inputs change
+  std::string ghost_sig;
+  std::vector<float2> h_gpos;  // host copy of the device ghosts (cell-grouped order)
+  uint64_t ghost_regens = 0;   // boundary_regens (fluid.rs:207)
+  uint32_t nghost = 0, ghost_cap = 0, gtab_mask = 0, gtab_cap = 0;
+  float2* d_gpos = nullptr;
+  float* d_gq = nullptr;
+  GhostCell* d_gtab = nullptr;
 
   // launch tuning (phieng_sph_set_tuning)
   float buckets_per_particle = 2.0f;
@@ -566,6 +574,8 @@ void apply_ambient(const World2* w, StepParams& P) {
   P.clock = reinterpret_cast<const float*>(w->d.scalar + kClockWord);
 }
 
+void apply_ghosts(const World2* w, StepParams& P);  // boundary ghosts, below
+
 // The clock the next substeps' turbulence reads (the world time at the start
 // of the step, fluid.rs:1009 with world.rs:848), in stream order.
 void set_clock(World2* w, const StepParams& P, float t) {
@@ -581,6 +591,7 @@ StepParams make_params(const World2* w, float dt) {
     StepParams P = make_params_for(w->cfg, w->gx, w->gy, w->mass_uniform, w->mass_value, w->phase_uniform,
                                    w->phase_value, w->plan, 0, (uint32_t)w->bodies.size(), dt);
     apply_ambient(w, P);
+    apply_ghosts(w, P);
     return P;
   }
   // batch: the kernels read each scene's row of the device table; the launch
@@ -613,6 +624,7 @@ void enqueue_substep_body(World2* w, const StepParams& P, cudaStream_t st) {
   enqueue_sort_and_ranges(w->d, w->n, P, w->sid_perm_n == w->n, st);
   if (w->profiling) cudaEventRecordWithFlags(w->ev[1], st, cudaEventRecordExternal);
   enqueue_density(w->d, w->n, P, st);
+  enqueue_ghost_density(w->d, P, st);
   if (w->profiling) cudaEventRecordWithFlags(w->ev[2], st, cudaEventRecordExternal);
   enqueue_force_integrate(w->d, w->n, P, nullptr, st);
   if (w->profiling) cudaEventRecordWithFlags(w->ev[3], st, cudaEventRecordExternal);
@@ -692,12 +704,201 @@ bool cfl_substeps(World2* w, float dt, uint32_t* out) {
   return true;
 }
 
-bool unsupported(World2* w) {
-  if (w->cfg.adaptive_resolution || w->cfg.boundary_particles) {
+// Features the closure and feature passes do not take: adaptive resolution
+// and boundary ghosts; the world step and the fluid phase take ghosts
+// (ghosts_ok).
+bool unsupported(World2* w, bool ghosts_ok = false) {
+  if (w->cfg.adaptive_resolution || (w->cfg.boundary_particles && !ghosts_ok)) {
     set_error(w, PHIENG_SPH_E_UNSUPPORTED, "step");
     return true;
   }
   return false;
+}
+
+// ---- boundary ghosts (fluid.rs:617-818) ----
+// A static body as the ghost generator reads it.
+struct GhostSource {
+  int shape;  // 0 circle, 1 box, 2 polygon
+  float px, py, xax, xay, yax, yay, a, b;
+  const float* verts = nullptr;  // polygon: local vertices (x, y pairs)
+  uint32_t nverts = 0;
+};
+
+constexpr size_t kMaxGhosts = 1u << 22;
+
+// f32 -> usize / i32 as Rust's `as` (truncate, saturate, NaN -> 0).
+uint64_t as_usize(float v) {
+  if (!(v > 0.0f)) return 0;
+  if (v >= 1.8446744e19f) return UINT64_MAX;
+  return (uint64_t)v;
+}
+int32_t as_i32(float v) {
+  if (v != v) return 0;
+  if (v <= -2147483648.0f) return INT32_MIN;
+  if (v >= 2147483648.0f) return INT32_MAX;
+  return (int32_t)v;
+}
+
+// refresh_boundaries (fluid.rs:665-741) at spacing max(h * 0.5, EPS): circles
+// n = ceil(2 pi r / s) points at angles 2 pi k / n; boxes 4 edges (bottom,
+// top, left, right) of ceil(2 extent / s) points at (k + 0.5) / n; polygons
+// each edge of length >= EPS at (k + 0.5) / n; every point moved by the
+// body's transform (rotation * local + position). false past kMaxGhosts.
+bool generate_ghosts(const std::vector<GhostSource>& src, float hk, std::vector<float2>& out) {
+  const float spacing = std::max(hk * 0.5f, kEps);
+  const float pi = 3.14159265358979323846f;
+  out.clear();
+  auto push = [&](const GhostSource& b, float lx, float ly) {
+    out.push_back(make_float2((b.xax * lx + b.yax * ly) + b.px, (b.xay * lx + b.yay * ly) + b.py));
+  };
+  for (const GhostSource& b : src) {
+    if (b.shape == 0) {
+      const uint64_t n = std::max<uint64_t>(as_usize(std::ceil((2.0f * pi * b.a) / spacing)), 1);
+      if (n > kMaxGhosts || out.size() + n > kMaxGhosts) return false;
+      for (uint64_t k = 0; k < n; k++) {
+        const float ang = 2.0f * pi * (float)k / (float)n;
+        push(b, std::cos(ang) * b.a, std::sin(ang) * b.a);
+      }
+    } else if (b.shape == 1) {
+      const float hx = b.a, hy = b.b;
+      // (origin, tangent) of the bottom, top, left and right edges
+      const float edges[4][4] = {{-hx, -hy, 0.0f, 1.0f}, {-hx, hy, 0.0f, 1.0f}, {-hx, -hy, 1.0f, 0.0f},
+                                 {hx, -hy, 1.0f, 0.0f}};
+      for (const auto& e : edges) {
+        const float extent = e[2] == 1.0f ? hx : hy;
+        const uint64_t n = std::max<uint64_t>(as_usize(std::ceil((2.0f * extent) / spacing)), 1);
+        if (n > kMaxGhosts || out.size() + n > kMaxGhosts) return false;
+        for (uint64_t k = 0; k < n; k++) {
+          const float t = ((float)k + 0.5f) / (float)n;
+          const float sc = 2.0f * extent * t;
+          push(b, e[0] + e[2] * sc, e[1] + e[3] * sc);
+        }
+      }
+    } else {
+      for (uint32_t e = 0; e < b.nverts; e++) {
+        const uint32_t f = (e + 1) % b.nverts;
+        const float ax = b.verts[2 * e], ay = b.verts[2 * e + 1];
+        const float ex = b.verts[2 * f] - ax, ey = b.verts[2 * f + 1] - ay;
+        const float len = std::sqrt(ex * ex + ey * ey);
+        if (len < kEps) continue;
+        const uint64_t n = std::max<uint64_t>(as_usize(std::ceil(len / spacing)), 1);
+        if (n > kMaxGhosts || out.size() + n > kMaxGhosts) return false;
+        for (uint64_t k = 0; k < n; k++) {
+          const float t = ((float)k + 0.5f) / (float)n;
+          push(b, ax + ex * t, ay + ey * t);
+        }
+      }
+    }
+  }
+  return true;
+}
+
+// Make the device ghosts current for these static bodies (regenerated when
+// the inputs of boundary_fingerprint change, fluid.rs:614-660, 929-936):
+// positions grouped by cell (floor(p / hk), rebuild_boundary_grid,
+// fluid.rs:744-756; generation order within a cell; non-finite ghosts are in
+// no cell and are dropped), and the open-addressing cell table.
+bool refresh_ghosts(World2* w, const std::vector<GhostSource>& src) {
+  const FluidConfig2Ffi& c = w->cfg;
+  std::string sig;
+  auto add = [&](const void* p, size_t n) { sig.append((const char*)p, n); };
+  add(&c.smoothing_length, 4);
+  add(&c.particle_mass, 4);
+  add(&c.rest_density, 4);
+  for (const GhostSource& b : src) {
+    add(&b.shape, 4);
+    add(&b.px, 4 * 8);
+    add(&b.nverts, 4);
+    if (b.nverts) add(b.verts, 8 * (size_t)b.nverts);
+  }
+  if (sig == w->ghost_sig && w->d_gtab) return true;
+  const float hk = std::max(c.smoothing_length, kEps);
+  std::vector<float2> raw;
+  if (!generate_ghosts(src, hk, raw)) {
+    set_error(w, PHIENG_SPH_E_ARG, "too many boundary ghosts");
+    return false;
+  }
+  // group by cell, keeping generation order inside each cell
+  std::vector<std::pair<int64_t, uint32_t>> order;  // (cell key, generation index)
+  std::vector<std::pair<int32_t, int32_t>> cell_of(raw.size());
+  for (uint32_t i = 0; i < raw.size(); i++) {
+    const float2 g = raw[i];
+    if (!std::isfinite(g.x) || !std::isfinite(g.y)) continue;
+    const int32_t cx = as_i32(std::floor(g.x / hk)), cy = as_i32(std::floor(g.y / hk));
+    cell_of[i] = {cx, cy};
+    order.push_back({((int64_t)cx << 32) | (uint32_t)cy, i});
+  }
+  std::stable_sort(order.begin(), order.end(),
+                   [](const std::pair<int64_t, uint32_t>& x, const std::pair<int64_t, uint32_t>& y) {
+                     return x.first < y.first;
+                   });
+  std::vector<float2> gpos(order.size());
+  std::vector<GhostCell> cells;
+  for (size_t k = 0; k < order.size(); k++) {
+    gpos[k] = raw[order[k].second];
+    const auto cc = cell_of[order[k].second];
+    if (cells.empty() || cells.back().cx != cc.first || cells.back().cy != cc.second)
+      cells.push_back({cc.first, cc.second, (uint32_t)k, 0});
+    cells.back().count++;
+  }
+  uint32_t tsize = 16;
+  while (tsize < 2 * cells.size()) tsize <<= 1;
+  std::vector<GhostCell> tab(tsize, GhostCell{0, 0, 0, 0});
+  for (const GhostCell& gc : cells) {
+    uint32_t slot = ghost_cell_hash(gc.cx, gc.cy, tsize - 1);
+    while (tab[slot].count != 0) slot = (slot + 1) & (tsize - 1);
+    tab[slot] = gc;
+  }
+  const uint32_t ng = (uint32_t)gpos.size();
+  if (ng > w->ghost_cap) {
+    cudaStreamSynchronize(w->stream);
+    dfree(w->d_gpos), dfree(w->d_gq);
+    if (!dalloc(w, w->d_gpos, std::max<uint32_t>(ng, 64)) || !dalloc(w, w->d_gq, std::max<uint32_t>(ng, 64)))
+      return false;
+    w->ghost_cap = std::max<uint32_t>(ng, 64);
+  }
+  if (tsize > w->gtab_cap) {
+    cudaStreamSynchronize(w->stream);
+    dfree(w->d_gtab);
+    if (!dalloc(w, w->d_gtab, tsize)) return false;
+    w->gtab_cap = tsize;
+  }
+  if ((ng && !cuda_ok(w, cudaMemcpyAsync(w->d_gpos, gpos.data(), sizeof(float2) * ng, cudaMemcpyHostToDevice,
+                                          w->stream), "upload ghosts")) ||
+      !cuda_ok(w, cudaMemcpyAsync(w->d_gtab, tab.data(), sizeof(GhostCell) * tsize, cudaMemcpyHostToDevice, w->stream),
+               "upload ghost cells") ||
+      !cuda_ok(w, cudaStreamSynchronize(w->stream), "sync"))  // the host vectors go out of scope
+    return false;
+  w->nghost = ng;
+  w->gtab_mask = tsize - 1;
+  w->ghost_sig = sig;
+  w->h_gpos = std::move(gpos);
+  w->ghost_regens++;
+  return true;
+}
+
+// The world's static bodies as ghost sources (all of them are static).
+std::vector<GhostSource> world_ghost_sources(const World2* w) {
+  std::vector<GhostSource> v;
+  for (const DevBody& b : w->bodies) {
+    GhostSource g;
+    g.shape = b.shape;
+    g.px = b.px, g.py = b.py, g.xax = b.xax, g.xay = b.xay, g.yax = b.yax, g.yay = b.yay, g.a = b.a, g.b = b.b;
+    v.push_back(g);
+  }
+  return v;
+}
+
+void apply_ghosts(const World2* w, StepParams& P) {
+  if (!w->cfg.boundary_particles || w->nghost == 0 || !w->d_gtab) return;
+  P.flags |= F_GHOST;
+  P.gpos = w->d_gpos;
+  P.gq = w->d_gq;
+  P.gtab = w->d_gtab;
+  P.gtab_mask = w->gtab_mask;
+  P.nghost = w->nghost;
+  P.gmass = std::max(w->cfg.particle_mass, kEps);
+  P.rest0 = w->cfg.rest_density;
 }
 
 // World2::step (world.rs:706-732) restricted to the fluid phase (1b).
@@ -713,8 +914,9 @@ bool world_step(World2* w, float dt) {
     return true;
   }
   if (w->cfg.enabled && w->n > 0 && dt > 0.0f) {  // step_fluid guards (fluid.rs:550-552)
-    if (unsupported(w)) return false;
+    if (unsupported(w, true)) return false;
     if (!prepare(w)) return false;
+    if (w->cfg.boundary_particles && !refresh_ghosts(w, world_ghost_sources(w))) return false;
     uint32_t ns = 1;
     if (!cfl_substeps(w, dt, &ns)) return false;
     const float sub = dt / (float)ns;
@@ -878,8 +1080,24 @@ struct PolyIn {
 
 bool step_fluid_bodies(World2* w, PhiengBody2* bodies, uint32_t nb, float dt, const PolyIn& pin = PolyIn()) {
   if (!w->cfg.enabled || w->n == 0 || dt <= 0.0f) return true;  // step_fluid guards (fluid.rs:550-552)
-  if (unsupported(w)) return false;
+  if (unsupported(w, true)) return false;
   if (!prepare(w)) return false;
+  if (w->cfg.boundary_particles) {  // ghosts of the call's static bodies (fluid.rs:929-936)
+    std::vector<GhostSource> src;
+    for (uint32_t k = 0; k < nb; k++) {
+      const PhiengBody2& b = bodies[k];
+      if (!b.is_static) continue;
+      GhostSource g;
+      g.shape = b.shape_tag == PHIENG_SHAPE_CIRCLE ? 0 : b.shape_tag == PHIENG_SHAPE_POLYGON ? 2 : 1;
+      g.px = b.px, g.py = b.py, g.xax = b.xax, g.xay = b.xay, g.yax = b.yax, g.yay = b.yay, g.a = b.a, g.b = b.b;
+      if (g.shape == 2) {
+        g.verts = pin.xy + 2 * (size_t)pin.first[k];
+        g.nverts = pin.count[k];
+      }
+      src.push_back(g);
+    }
+    if (!refresh_ghosts(w, src)) return false;
+  }
   std::vector<float2> wv;  // world-space polygon vertices
   std::vector<DevBody> db(nb);
   std::vector<DynBody> dy(nb);
@@ -957,6 +1175,7 @@ bool step_fluid_bodies(World2* w, PhiengBody2* bodies, uint32_t nb, float dt, co
   if (any_dyn) P.flags |= F_DYNAMIC;
   P.poly = w->d_poly;
   apply_ambient(w, P);
+  apply_ghosts(w, P);
   set_clock(w, P, w->time);
   FluidBufs dB = w->d;
   dB.bodies = w->d_cbodies;
@@ -966,6 +1185,7 @@ bool step_fluid_bodies(World2* w, PhiengBody2* bodies, uint32_t nb, float dt, co
     enqueue_sort_and_ranges(dB, w->n, P, w->sid_perm_n == w->n, st);
     w->sid_perm_n = w->n;
     enqueue_density(dB, w->n, P, st);
+    enqueue_ghost_density(dB, P, st);
     if (any_dyn) cudaMemsetAsync(dB.dcount, 0, sizeof(uint32_t) * dlen, st);
     enqueue_force_integrate(dB, w->n, P, nullptr, st);
     if (any_dyn) enqueue_dynamic_walls(dB, y, w->n, P, st);
@@ -1130,6 +1350,9 @@ void phieng_world_free(World2* w) {
     dfree(w->d_svp);
     dfree(w->d_cbodies);
     dfree(w->d_poly);
+    dfree(w->d_gpos);
+    dfree(w->d_gq);
+    dfree(w->d_gtab);
     dfree(w->dynb.dyn);
     dfree(w->dynb.samples);
     dfree(w->dynb.areas);
@@ -1201,6 +1424,18 @@ int32_t phieng_world_get_ambient_config(World2* w, AmbientConfig2Ffi* out) {
   if (!w || !out) return 0;
   *out = w->ambient;
   return 1;
+}
+
+uint32_t phieng_sph_ghosts(World2* w, float* xy, uint32_t max, uint64_t* regens) {
+  if (!w) return 0;
+  if (regens) *regens = w->ghost_regens;
+  const uint32_t n = (uint32_t)w->h_gpos.size();
+  if (xy)
+    for (uint32_t i = 0; i < std::min(n, max); i++) {
+      xy[2 * i] = w->h_gpos[i].x;
+      xy[2 * i + 1] = w->h_gpos[i].y;
+    }
+  return n;
 }
 
 int32_t phieng_world_body_count(World2* w) {

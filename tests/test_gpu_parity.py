@@ -397,7 +397,7 @@ def test_unsupported_feature_fails_cleanly():
     w = World2()
     w.fluid.add_particles(np.array([[0.0, 0.0], [0.1, 0.0]], np.float32))
     c = w.fluid.config
-    c.boundary_particles = 1
+    c.adaptive_resolution = 1  # resample (fluid.rs:826-893) is the one fluid feature not built
     w.fluid.config = c
     before = w.fluid.particles.copy()
     with pytest.raises(SphError):
