@@ -455,6 +455,10 @@ uint32_t phieng_sph_debug_sorted(World2* world, uint32_t* ids, uint32_t* keys, u
 uint32_t phieng_sph_debug_neighbors(World2* world, uint32_t* counts, uint32_t* lists,
                                     uint32_t max_per, uint32_t max);
 
+/* Particle masses by id (set at insertion; merges and splits of adaptive
+ * resolution change them). Returns the particle count; writes up to max. */
+uint32_t phieng_sph_fluid_masses(World2* world, float* out, uint32_t max);
+
 /* Boundary ghosts (FluidConfig2Ffi.boundary_particles, fluid.rs:617-818):
  * the count of the last generated set, and up to max positions (x, y pairs,
  * grouped by grid cell, generation order inside a cell) into xy (may be

@@ -46,6 +46,7 @@ def _load():
         "orc_set_turbulence": (None, [P, C.c_int, C.c_float, C.c_float, C.c_float, C.c_uint32, C.c_uint32, C.c_int]),
         "orc_set_wind": (None, [P, C.c_float, C.c_float]),
         "orc_ghosts": (C.c_uint32, [P, C.c_void_p, C.c_uint32]),
+        "orc_masses": (C.c_uint32, [P, C.c_void_p, C.c_uint32]),
         "orc3_set_turbulence": (None, [P, C.c_int, C.c_float, C.c_float, C.c_float, C.c_uint32, C.c_uint32, C.c_int]),
         "orc_noise2": (None, [C.c_int, C.c_float, C.c_float, C.c_float, C.c_uint32, C.c_uint32, C.POINTER(C.c_float)]),
         "orc_set_cap": (None, [P, C.c_uint32]),
@@ -156,6 +157,13 @@ class OracleWorld:
 
     def set_gravity(self, gx: float, gy: float) -> None:
         self._l.orc_set_gravity(self._h, gx, gy)
+
+    def masses(self) -> np.ndarray:
+        """Particle masses by index."""
+        n = self._l.orc_masses(self._h, None, 0)
+        out = np.zeros(n, np.float32)
+        self._l.orc_masses(self._h, out.ctypes.data, n)
+        return out
 
     def ghosts(self) -> np.ndarray:
         """Boundary ghost positions of the last substep [m][2], generation order."""

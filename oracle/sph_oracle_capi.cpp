@@ -131,6 +131,14 @@ void orc_set_gravity(void* h, float gx, float gy) {
   o->f64.gy = (double)gy;
 }
 
+// particle masses by index
+uint32_t orc_masses(void* h, float* out, uint32_t max) {
+  Orc* o = static_cast<Orc*>(h);
+  const auto& ps = o->f32.particles;
+  for (uint32_t i = 0; out && i < std::min<size_t>(ps.size(), max); i++) out[i] = ps[i].mass;
+  return (uint32_t)ps.size();
+}
+
 // the boundary ghosts of the last substep, generation order
 uint32_t orc_ghosts(void* h, float* xy, uint32_t max) {
   Orc* o = static_cast<Orc*>(h);

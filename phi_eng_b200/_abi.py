@@ -295,6 +295,7 @@ SIGNATURES = {
     "phieng_world_get_time": (C.c_int32, [_P, _F]),
     "phieng_world_body_count": (C.c_int32, [_P]),
     "phieng_sph_ghosts": (C.c_uint32, [_P, _F, C.c_uint32, C.POINTER(C.c_uint64)]),
+    "phieng_sph_fluid_masses": (C.c_uint32, [_P, _F, C.c_uint32]),
     "phieng_world_set_ambient_config": (C.c_int32, [_P, C.POINTER(AmbientConfig2Ffi)]),
     "phieng_world_get_ambient_config": (C.c_int32, [_P, C.POINTER(AmbientConfig2Ffi)]),
     "phieng_world_add_body": (

@@ -1043,6 +1043,98 @@ void enqueue_sort_and_ranges(const FluidBufs& b, uint32_t n, const StepParams& P
   cudaMemsetAsync(b.count, 0, sizeof(uint32_t) * b.count_len, st);
 }
 
+// ---------------------------------------------------------------- adaptive resolution
+// FluidState2::resample (fluid.rs:826-893) after the first density pass.
+// Merge: each particle i in index order whose density exceeds merge_hi takes
+// in the highest-index j < i that is not yet absorbed, also exceeds merge_hi
+// and lies within 0.25 h (mass and momentum conserved: v_i = (v_i m_i +
+// v_j m_j) / m_t, m_i = m_t when m_t > EPS). j is found among the grid
+// candidates, which hold every particle within h. Split: in index order, a
+// kept particle under split_lo heavier than particle_mass / 8 becomes two
+// half-mass children at x +- (0.25 h, 0) while the output holds fewer than
+// MAX_PARTICLES_2D - 1. One thread: every decision depends on the earlier
+// ones. Writes the new state / mass / phase to out_*, the count to *n_out.
+__global__ void k_resample(uint32_t n, float4* __restrict__ state, float* __restrict__ mass,
+                           const uint8_t* __restrict__ phase, const float2* __restrict__ sdq,
+                           const uint32_t* __restrict__ sid, const uint32_t* __restrict__ skey,
+                           const uint32_t* __restrict__ slot_of, const uint32_t* __restrict__ start, StepParams P,
+                           float merge_hi, float split_lo, float min_mass, uint8_t* __restrict__ absorbed,
+                           float4* __restrict__ out_state, float* __restrict__ out_mass, uint8_t* __restrict__ out_phase,
+                           uint32_t* __restrict__ n_out) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  const float h = P.hk;
+  const float md = __fmul_rn(0.25f, h);
+  const float merge_d2 = __fmul_rn(md, md);
+  for (uint32_t i = 0; i < n; i++) absorbed[i] = 0;
+  for (uint32_t i = 0; i < n; i++) {
+    const uint32_t si = slot_of[i];
+    if (absorbed[i] || sdq[si].x <= merge_hi) continue;
+    const float4 pi = state[i];
+    int64_t best = -1;
+    const uint32_t key = skey[si];
+    if (key != P.grid.sentinel)
+      for_each_candidate(key, start, P.grid, [&](int js) {
+        const uint32_t j = sid[js];
+        if (j >= i || absorbed[j] || sdq[js].x <= merge_hi || (int64_t)j <= best) return;
+        const float4 pj = state[j];
+        const float dx = __fsub_rn(pi.x, pj.x), dy = __fsub_rn(pi.y, pj.y);
+        if (__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)) < merge_d2) best = j;
+      });
+    if (best < 0) continue;
+    const uint32_t j = (uint32_t)best;
+    const float mi = mass[i], mj = mass[j];
+    const float mt = __fadd_rn(mi, mj);
+    if (mt > kEps) {
+      const float4 pj = state[j];
+      state[i].z = __fdiv_rn(__fadd_rn(__fmul_rn(pi.z, mi), __fmul_rn(pj.z, mj)), mt);
+      state[i].w = __fdiv_rn(__fadd_rn(__fmul_rn(pi.w, mi), __fmul_rn(pj.w, mj)), mt);
+      mass[i] = mt;
+    }
+    absorbed[j] = 1;
+  }
+  uint32_t out = 0;
+  const float off = __fmul_rn(0.25f, h);
+  for (uint32_t i = 0; i < n; i++) {
+    if (absorbed[i]) continue;
+    const float4 p = state[i];
+    const float m = mass[i];
+    if (sdq[slot_of[i]].x < split_lo && m > min_mass && out + 1 < 4096u) {  // MAX_PARTICLES_2D (fluid.rs:30)
+      const float half = __fmul_rn(m, 0.5f);
+      out_state[out] = make_float4(__fadd_rn(p.x, off), __fadd_rn(p.y, 0.0f), p.z, p.w);
+      out_mass[out] = half;
+      out_phase[out++] = phase[i];
+      out_state[out] = make_float4(__fsub_rn(p.x, off), __fsub_rn(p.y, 0.0f), p.z, p.w);
+      out_mass[out] = half;
+      out_phase[out++] = phase[i];
+    } else {
+      out_state[out] = p;
+      out_mass[out] = m;
+      out_phase[out++] = phase[i];
+    }
+  }
+  *n_out = out;
+}
+
+// slot_of[sid[s]] = s; uniform mass / phase written out per particle first.
+__global__ void k_resample_prep(const uint32_t* __restrict__ sid, uint32_t n, uint32_t* __restrict__ slot_of,
+                                float* __restrict__ mass, uint8_t* __restrict__ phase, int mass_uniform,
+                                float mass_value, int phase_uniform, uint8_t phase_value) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  slot_of[sid[s]] = s;
+  if (mass_uniform) mass[s] = mass_value;
+  if (phase_uniform) phase[s] = phase_value;
+}
+
+void enqueue_resample(const FluidBufs& b, uint32_t n, const StepParams& P, const ResampleBufs& r, float merge_hi,
+                      float split_lo, float min_mass, bool mass_uniform, bool phase_uniform, cudaStream_t st) {
+  if (n == 0) return;
+  k_resample_prep<<<cdiv(n, 256), 256, 0, st>>>(b.sid, n, r.slot_of, b.mass, b.phase, mass_uniform ? 1 : 0, P.mass,
+                                                 phase_uniform ? 1 : 0, (uint8_t)P.uniform_phase);
+  k_resample<<<1, 1, 0, st>>>(n, b.state, b.mass, b.phase, b.sdq, b.sid, b.skey, r.slot_of, b.start, P, merge_hi,
+                              split_lo, min_mass, r.absorbed, r.state, r.mass, r.phase, r.n_out);
+}
+
 void enqueue_ghost_density(const FluidBufs& b, const StepParams& P, cudaStream_t st) {
   if (!(P.flags & F_GHOST) || P.nghost == 0) return;
   k_ghost_density<<<cdiv(P.nghost, 256), 256, 0, st>>>(b.spos, b.smass, b.start, P);

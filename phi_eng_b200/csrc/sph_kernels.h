@@ -94,6 +94,24 @@ struct BucketSort {
 };
 void enqueue_bucket_place(const BucketSort& bs, uint32_t n, uint32_t m, bool by_slot, cudaStream_t st);
 
+// Adaptive resolution scratch: inverse sort permutation, merge flags, the
+// resampled particles (capacity >= max(n, 4096)) and their count.
+struct ResampleBufs {
+  uint32_t* slot_of = nullptr;
+  uint8_t* absorbed = nullptr;
+  float4* state = nullptr;
+  float* mass = nullptr;
+  uint8_t* phase = nullptr;
+  uint32_t* n_out = nullptr;
+};
+
+// resample (fluid.rs:826-893) after a sort and density pass: merges and
+// splits into r.state / r.mass / r.phase (id order), the new count into
+// *r.n_out. Overwrites b.mass / b.phase with per-particle values when they
+// were uniform, and the merged particles' velocity and mass in b.
+void enqueue_resample(const FluidBufs& b, uint32_t n, const StepParams& P, const ResampleBufs& r, float merge_hi,
+                      float split_lo, float min_mass, bool mass_uniform, bool phase_uniform, cudaStream_t st);
+
 // Boundary ghosts' density / pressure from the fluid of the current sort
 // (after K5, before K6); no-op unless P has F_GHOST.
 void enqueue_ghost_density(const FluidBufs& b, const StepParams& P, cudaStream_t st);

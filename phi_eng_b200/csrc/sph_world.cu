@@ -142,6 +142,9 @@ struct World2 {
   float2* d_gpos = nullptr;
   float* d_gq = nullptr;
   GhostCell* d_gtab = nullptr;
+  // adaptive resolution scratch (capacity = d.cap when allocated)
+  ResampleBufs rs;
+  uint32_t rs_cap = 0;
 
   // launch tuning (phieng_sph_set_tuning)
   float buckets_per_particle = 2.0f;
@@ -470,7 +473,8 @@ bool prepare(World2* w) {
   if (w->error != PHIENG_SPH_OK) return false;
   if (!ensure_device(w)) return false;
   if (!w->dev_state_valid) {
-    if (!ensure_capacity(w, w->n)) return false;
+    // adaptive resolution may split up to MAX_PARTICLES_2D particles
+    if (!ensure_capacity(w, w->cfg.adaptive_resolution ? std::max(w->n, kMaxParticles2D) : w->n)) return false;
     if (!w->plan_valid) plan_grid(w);
     if (w->n && !cuda_ok(w, cudaMemcpyAsync(w->d.state, w->h_state.data(), sizeof(float4) * w->n,
                                             cudaMemcpyHostToDevice, w->stream),
@@ -705,10 +709,10 @@ bool cfl_substeps(World2* w, float dt, uint32_t* out) {
 }
 
 // Features the closure and feature passes do not take: adaptive resolution
-// and boundary ghosts; the world step and the fluid phase take ghosts
-// (ghosts_ok).
-bool unsupported(World2* w, bool ghosts_ok = false) {
-  if (w->cfg.adaptive_resolution || (w->cfg.boundary_particles && !ghosts_ok)) {
+// and boundary ghosts; the fluid phase takes ghosts (ghosts_ok), the world
+// step both (world_ok).
+bool unsupported(World2* w, bool ghosts_ok = false, bool world_ok = false) {
+  if ((w->cfg.adaptive_resolution && !world_ok) || (w->cfg.boundary_particles && !ghosts_ok)) {
     set_error(w, PHIENG_SPH_E_UNSUPPORTED, "step");
     return true;
   }
@@ -901,6 +905,84 @@ void apply_ghosts(const World2* w, StepParams& P) {
   P.rest0 = w->cfg.rest_density;
 }
 
+void recompute_uniformity(World2* w);
+
+// One substep with adaptive resolution (fluid.rs:909-920): sort and density,
+// resample, then the new particle set's sort and density and the rest of the
+// substep. The count changes mid-substep, so it runs as plain launches with
+// one read of the new count; the host mirrors of mass and phase follow the
+// device, and the uniform-mass shortcut ends once masses differ.
+bool ensure_resample_buffers(World2* w) {
+  const uint32_t c = w->d.cap;
+  if (w->rs_cap >= c && w->rs.state) return true;
+  ResampleBufs& r = w->rs;
+  cudaStreamSynchronize(w->stream);
+  dfree(r.slot_of), dfree(r.absorbed), dfree(r.state), dfree(r.mass), dfree(r.phase);
+  if (!dalloc(w, r.slot_of, c) || !dalloc(w, r.absorbed, c) || !dalloc(w, r.state, c) || !dalloc(w, r.mass, c) ||
+      !dalloc(w, r.phase, c))
+    return false;
+  r.n_out = w->d.scalar + 18;
+  w->rs_cap = c;
+  return true;
+}
+
+bool run_substep_adaptive(World2* w, float dt) {
+  if (!ensure_resample_buffers(w)) return false;
+  cudaStream_t st = w->stream;
+  StepParams P = make_params(w, dt);
+  enqueue_sort_and_ranges(w->d, w->n, P, w->sid_perm_n == w->n, st);
+  w->sid_perm_n = w->n;
+  enqueue_density(w->d, w->n, P, st);
+  const FluidConfig2Ffi& c = w->cfg;
+  const float rest = std::max(c.rest_density, kEps);
+  enqueue_resample(w->d, w->n, P, w->rs, c.merge_density_ratio * rest, c.split_density_ratio * rest,
+                   std::max(c.particle_mass, kEps) * 0.125f, w->mass_uniform, w->phase_uniform, st);
+  if (!cuda_ok(w, cudaMemcpyAsync(w->h_pinned, w->rs.n_out, 4, cudaMemcpyDeviceToHost, st), "resample count") ||
+      !cuda_ok(w, cudaStreamSynchronize(st), "sync"))
+    return false;
+  uint32_t n2;
+  std::memcpy(&n2, w->h_pinned, 4);
+  if (n2 > w->d.cap) {
+    set_error(w, PHIENG_SPH_E_CUDA, "resample count");
+    return false;
+  }
+  w->h_state.resize(n2);
+  w->h_mass.resize(n2);
+  w->h_phase.resize(n2);
+  w->h_dens.resize(n2);
+  w->h_pres.resize(n2);
+  if (n2 &&
+      (!cuda_ok(w, cudaMemcpyAsync(w->d.state, w->rs.state, sizeof(float4) * n2, cudaMemcpyDeviceToDevice, st),
+                "resample state") ||
+       !cuda_ok(w, cudaMemcpyAsync(w->d.mass, w->rs.mass, sizeof(float) * n2, cudaMemcpyDeviceToDevice, st),
+                "resample mass") ||
+       !cuda_ok(w, cudaMemcpyAsync(w->d.phase, w->rs.phase, n2, cudaMemcpyDeviceToDevice, st), "resample phase") ||
+       !cuda_ok(w, cudaMemcpyAsync(w->h_mass.data(), w->rs.mass, sizeof(float) * n2, cudaMemcpyDeviceToHost, st),
+                "resample mass down") ||
+       !cuda_ok(w, cudaMemcpyAsync(w->h_phase.data(), w->rs.phase, n2, cudaMemcpyDeviceToHost, st),
+                "resample phase down") ||
+       !cuda_ok(w, cudaStreamSynchronize(st), "sync")))
+    return false;
+  w->n = n2;
+  recompute_uniformity(w);
+  w->dev_aux_valid = true;
+  w->host_state_valid = false;
+  w->bbox_valid = false;
+  // the second density pass on the resampled set, then the rest
+  P = make_params(w, dt);
+  enqueue_keys(w->d, w->n, w->plan, st);
+  enqueue_sort_and_ranges(w->d, w->n, P, false, st);
+  w->sid_perm_n = w->n;
+  enqueue_density(w->d, w->n, P, st);
+  enqueue_ghost_density(w->d, P, st);
+  enqueue_force_integrate(w->d, w->n, P, nullptr, st);
+  if (!cuda_ok(w, cudaGetLastError(), "adaptive substep")) return false;
+  w->substeps++;
+  w->dp_on_device = true;
+  w->keys_valid = true;
+  return true;
+}
+
 // World2::step (world.rs:706-732) restricted to the fluid phase (1b).
 bool world_step(World2* w, float dt) {
   if (w->is_batch()) {
@@ -914,7 +996,12 @@ bool world_step(World2* w, float dt) {
     return true;
   }
   if (w->cfg.enabled && w->n > 0 && dt > 0.0f) {  // step_fluid guards (fluid.rs:550-552)
-    if (unsupported(w, true)) return false;
+    if (unsupported(w, true, true)) return false;
+    if (w->cfg.adaptive_resolution && w->d.state && w->d.cap < std::max(w->n, kMaxParticles2D)) {
+      // room for the splits: bring the state home and upload it into larger buffers
+      if (!ensure_host_state(w)) return false;
+      w->dev_state_valid = false;
+    }
     if (!prepare(w)) return false;
     if (w->cfg.boundary_particles && !refresh_ghosts(w, world_ghost_sources(w))) return false;
     uint32_t ns = 1;
@@ -923,7 +1010,7 @@ bool world_step(World2* w, float dt) {
     const StepParams P = make_params(w, sub);
     set_clock(w, P, w->time);  // every CFL substep sees the step's start time
     for (uint32_t k = 0; k < ns; k++)
-      if (!run_substep(w, P)) return false;
+      if (!(w->cfg.adaptive_resolution ? run_substep_adaptive(w, sub) : run_substep(w, P))) return false;
   }
   w->time += dt;
   return true;
@@ -1353,6 +1440,7 @@ void phieng_world_free(World2* w) {
     dfree(w->d_gpos);
     dfree(w->d_gq);
     dfree(w->d_gtab);
+    dfree(w->rs.slot_of), dfree(w->rs.absorbed), dfree(w->rs.state), dfree(w->rs.mass), dfree(w->rs.phase);
     dfree(w->dynb.dyn);
     dfree(w->dynb.samples);
     dfree(w->dynb.areas);
@@ -1424,6 +1512,12 @@ int32_t phieng_world_get_ambient_config(World2* w, AmbientConfig2Ffi* out) {
   if (!w || !out) return 0;
   *out = w->ambient;
   return 1;
+}
+
+uint32_t phieng_sph_fluid_masses(World2* w, float* out, uint32_t max) {
+  if (!w) return 0;
+  for (uint32_t i = 0; out && i < std::min(w->n, max); i++) out[i] = w->h_mass[i];
+  return w->n;
 }
 
 uint32_t phieng_sph_ghosts(World2* w, float* xy, uint32_t max, uint64_t* regens) {

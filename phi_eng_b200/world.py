@@ -106,6 +106,13 @@ class FluidState2:
     def __len__(self) -> int:
         return int(self._lib.phieng_world_fluid_count(self._h))
 
+    def masses(self) -> np.ndarray:
+        """Particle masses by id (phieng_sph_fluid_masses)."""
+        n = len(self)
+        out = np.zeros(n, np.float32)
+        self._lib.phieng_sph_fluid_masses(self._h, out.ctypes.data_as(C.POINTER(C.c_float)), n)
+        return out
+
     @property
     def particles(self) -> np.ndarray:
         """(n, 4) float32 [x, y, vx, vy] in insertion order (ffi.rs:2575)."""

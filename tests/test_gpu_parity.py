@@ -392,16 +392,20 @@ def test_step_guards_and_clock():
 
 
 def test_unsupported_feature_fails_cleanly():
-    from phi_eng_b200.world import SphError, World2
+    """The fluid phase with the engine's bodies (phieng_sph_step_fluid) does
+    not take adaptive resolution (the world step does): it reports
+    PHIENG_SPH_E_UNSUPPORTED and leaves the particles unchanged."""
+    from phi_eng_b200._abi import PhiengBody2
+    from phi_eng_b200.world import World2
 
     w = World2()
     w.fluid.add_particles(np.array([[0.0, 0.0], [0.1, 0.0]], np.float32))
     c = w.fluid.config
-    c.adaptive_resolution = 1  # resample (fluid.rs:826-893) is the one fluid feature not built
+    c.adaptive_resolution = 1
     w.fluid.config = c
     before = w.fluid.particles.copy()
-    with pytest.raises(SphError):
-        w.step(0.01)
+    assert w._lib.phieng_sph_step_fluid(w._h, (PhiengBody2 * 1)(), 0, 0.01) == 0
+    assert w.status().error == 3  # PHIENG_SPH_E_UNSUPPORTED
     assert np.array_equal(before, w.fluid.particles)
 
 
