@@ -49,6 +49,7 @@ enum StepFlags : uint32_t {
   F_TURB = 1u << 9,      // ambient turbulence on (enabled and amplitude > 0)
   F_TURB_CURL = 1u << 10,  // turbulence as divergence-free curl noise
   F_GHOST = 1u << 11,      // boundary ghost particles (boundary_particles)
+  F_POLY = 1u << 12,       // polygon bodies among the launch's bodies
 };
 
 // One cell of the boundary ghosts' hash grid: ghosts [start, start + count)
@@ -345,10 +346,13 @@ __device__ __forceinline__ bool sat_circle_poly(float cx, float cy, float r, con
   return true;
 }
 
+// POLY = false compiles the polygon branch out: launches without polygon
+// bodies (F_POLY clear) keep the registers of the circle / box tests alone.
+template <bool POLY = true>
 __device__ __forceinline__ bool collide(float px, float py, float pr, const DevBody& b, float& nx,
                                         float& ny, float& depth, float2* cp = nullptr,
                                         const float2* __restrict__ poly = nullptr) {
-  if (b.shape == 2) {
+  if (POLY && b.shape == 2) {
     // fluid.rs:518-530: SAT on the world-space vertices, the axis oriented
     // from the vertex centroid towards the particle, contact point
     // particle - normal * pr
@@ -433,6 +437,7 @@ __device__ __forceinline__ bool collide(float px, float py, float pr, const DevB
 // zero velocity, which the no-slip branch reads. Returns kNoDefer, or the
 // index of the first body marked dyn that the particle touches: the state is
 // then left as it was before that body, for the ordered pass to resume.
+template <bool POLY = true>
 __device__ __forceinline__ uint32_t walls(float& x, float& y, float& vx, float& vy,
                                           const DevBody* __restrict__ bodies, const StepParams& P) {
   for (uint32_t k = 0; k < P.nbodies; k++) {
@@ -442,7 +447,7 @@ __device__ __forceinline__ uint32_t walls(float& x, float& y, float& vx, float& 
       continue;
     const DevBody b = *bp;
     float nx, ny, depth;
-    if (!collide(x, y, P.pr, b, nx, ny, depth, nullptr, P.poly)) continue;
+    if (!collide<POLY>(x, y, P.pr, b, nx, ny, depth, nullptr, P.poly)) continue;
     if (depth <= 0.0f) continue;
     if (b.dyn) return k;
     x = __fadd_rn(x, __fmul_rn(nx, depth));

@@ -591,14 +591,16 @@ __device__ __forceinline__ void neighbour_sums(uint32_t s, uint32_t k, uint32_t 
 // integrate (fluid.rs:1003-1050) from acceleration (ax, ay) and the XSPH sum,
 // then the wall pass; writes the new state, the next key and its bucket count.
 // Ambient turbulence (F_TURB) joins the acceleration first, at the particle's
-// pre-step position and the step's world clock.
+// pre-step position and the step's world clock. EXTRA = false compiles it and
+// the polygon wall test out (the PLAIN variants, whose flags exclude both).
+template <bool EXTRA = true>
 __device__ __forceinline__ void integrate_write(uint32_t id, float2 pi, float2 vi, float ax, float ay, float sx,
                                                 float sy, const StepParams& P, const DevBody* __restrict__ bodies,
                                                 float4* __restrict__ state_out, uint32_t* __restrict__ key_out,
                                                 uint32_t* __restrict__ count_out,
                                                 uint32_t* __restrict__ defer = nullptr,
                                                 uint32_t* __restrict__ dcount = nullptr) {
-  if (P.flags & F_TURB) {
+  if (EXTRA && (P.flags & F_TURB)) {
     const float2 tb = turbulence_accel(pi.x, pi.y, *P.clock, P.turb_freq, P.turb_tscale, P.turb_seed, P.turb_oct,
                                        P.flags & F_TURB_CURL, P.turb_amp);
     ax = __fadd_rn(ax, tb.x);
@@ -626,7 +628,7 @@ __device__ __forceinline__ void integrate_write(uint32_t id, float2 pi, float2 v
     x = pi.x;
     y = pi.y;
   }
-  const uint32_t r = walls(x, y, vx, vy, bodies, P);
+  const uint32_t r = walls<EXTRA>(x, y, vx, vy, bodies, P);
   state_out[id] = make_float4(x, y, vx, vy);
   if (P.flags & F_DYNAMIC) {
     // contacts with bodies that react run in particle order (enqueue_dynamic_walls)
@@ -738,7 +740,7 @@ __global__ void __launch_bounds__(256) k_force_integrate(
   FeatAcc fa;
   neighbour_sums<MASS, false, PLAIN>(s, k, n, pi, vi, rho_i, q_i, m_i, spos, svel, sdq, smass, nullptr, start, nmask,
                                      P, fx, fy, sx, sy, fa);
-  if (!BATCH && (P.flags & F_GHOST)) {
+  if (!BATCH && !PLAIN && (P.flags & F_GHOST)) {  // PLAIN launches exclude F_GHOST (plain_flags)
     const float2 f = ghost_force(pi.x, pi.y, q_i, fx, fy, P.gpos, P.gq, P.gtab, P.gtab_mask, P.gmass, P.grid.hg,
                                  P.hg2, P.hk, P.c_spiky);
     fx = f.x;
@@ -750,7 +752,7 @@ __global__ void __launch_bounds__(256) k_force_integrate(
   }
   const float ax = __fadd_rn(P.gx, __fdiv_rn(fx, rho_i));
   const float ay = __fadd_rn(P.gy, __fdiv_rn(fy, rho_i));
-  integrate_write(id, pi, vi, ax, ay, sx, sy, P, bodies, state_out, key_out, count_out, defer, dcount);
+  integrate_write<!PLAIN>(id, pi, vi, ax, ay, sx, sy, P, bodies, state_out, key_out, count_out, defer, dcount);
 }
 
 // ---------------------------------------------------------------- closure force pass
@@ -846,7 +848,7 @@ __global__ void __launch_bounds__(256, 4) k_force_closure(
     io.rho_prev[id] = dqi.x;
     const float ax = __fadd_rn(__fadd_rn(P.gx, __fdiv_rn(fx, rho_i)), cx);
     const float ay = __fadd_rn(__fadd_rn(P.gy, __fdiv_rn(fy, rho_i)), cy);
-    integrate_write(id, pi, vi, ax, ay, sx, sy, P, bodies, state_out, key_out, count_out);
+    integrate_write<!PLAIN>(id, pi, vi, ax, ay, sx, sy, P, bodies, state_out, key_out, count_out);
   }
 }
 
@@ -1173,7 +1175,9 @@ void enqueue_density(const FluidBufs& b, uint32_t n, const StepParams& P, cudaSt
 // The launch's flags for which the force pass compiles out the optional pair
 // terms: XSPH on, artificial viscosity and cohesion off, h*h <= hk*hk (a
 // batch's launch parameters carry the union of its scenes' flags).
-inline bool plain_flags(uint32_t f) { return (f & F_VISC) && !(f & (F_AV | F_COHESION | F_WIDE_NB)); }
+inline bool plain_flags(uint32_t f) {
+  return (f & F_VISC) && !(f & (F_AV | F_COHESION | F_WIDE_NB | F_TURB | F_GHOST | F_POLY));
+}
 
 void enqueue_force_integrate(const FluidBufs& b, uint32_t n, const StepParams& P, float2* dbg_force,
                              cudaStream_t st) {

@@ -1260,6 +1260,7 @@ bool step_fluid_bodies(World2* w, PhiengBody2* bodies, uint32_t nb, float dt, co
   StepParams P = make_params_for(w->cfg, w->gx, w->gy, w->mass_uniform, w->mass_value, w->phase_uniform,
                                  w->phase_value, w->plan, 0, nb, sub);
   if (any_dyn) P.flags |= F_DYNAMIC;
+  if (!wv.empty()) P.flags |= F_POLY;
   P.poly = w->d_poly;
   apply_ambient(w, P);
   apply_ghosts(w, P);
