@@ -614,6 +614,10 @@ static_assert(sizeof(AmbientConfig3Ffi) == 88, "AmbientConfig3Ffi must match ffi
 static_assert(offsetof(AmbientConfig3Ffi, turbulence_enabled) == 60, "layout");
 #endif
 
+/* 3D boundary ghosts (fluid3.rs:719-922), as phieng_sph_ghosts: count,
+ * up to max (x, y, z) triples (cell-grouped), generation count. */
+uint32_t phieng_sph3_ghosts(World3* world, float* xyz, uint32_t max, uint64_t* regens);
+
 /* ffi.rs:549 / 568 phieng_world3_set/get_ambient_config — as the 2D pair
  * (ambient3_from_ffi, ffi.rs:414-475); turbulence acts on the 3D fluid
  * (fluid3.rs:1090-1108). */

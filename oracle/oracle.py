@@ -47,6 +47,7 @@ def _load():
         "orc_set_wind": (None, [P, C.c_float, C.c_float]),
         "orc_ghosts": (C.c_uint32, [P, C.c_void_p, C.c_uint32]),
         "orc_masses": (C.c_uint32, [P, C.c_void_p, C.c_uint32]),
+        "orc3_ghosts": (C.c_uint32, [P, C.c_void_p, C.c_uint32]),
         "orc3_set_turbulence": (None, [P, C.c_int, C.c_float, C.c_float, C.c_float, C.c_uint32, C.c_uint32, C.c_int]),
         "orc_noise2": (None, [C.c_int, C.c_float, C.c_float, C.c_float, C.c_uint32, C.c_uint32, C.POINTER(C.c_float)]),
         "orc_set_cap": (None, [P, C.c_uint32]),
@@ -342,6 +343,13 @@ class OracleWorld3:
 
     def set_config(self, cfg: FluidConfig2Ffi) -> None:
         self._l.orc3_set_config(self._h, C.byref(cfg))
+
+    def ghosts(self) -> np.ndarray:
+        """3D boundary ghost positions of the last substep [m][3], generation order."""
+        n = self._l.orc3_ghosts(self._h, None, 0)
+        out = np.zeros((n, 3), np.float32)
+        self._l.orc3_ghosts(self._h, out.ctypes.data, n)
+        return out
 
     def set_turbulence(self, amplitude: float, frequency: float = 1.0, time_scale: float = 1.0, seed: int = 0,
                        octaves: int = 3, divergence_free: bool = False, enabled: bool = True) -> None:

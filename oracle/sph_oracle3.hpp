@@ -14,6 +14,8 @@
 #pragma once
 
 #include <algorithm>
+#include <map>
+#include <tuple>
 #include <cmath>
 #include <cstdint>
 #include <unordered_map>
@@ -124,6 +126,129 @@ class Fluid3 {
   R gx = 0, gy = (R)-9.81f, gz = 0;  // World3::new gravity
   R time = 0;
   Turbulence turb;  // world.ambient.turbulence
+
+  // ---- boundary ghosts (fluid3.rs:719-922), regenerated every substep (a
+  // function of the static bodies and the config only) ----
+  struct Ghost3 {
+    float x, y, z;
+    R density, pressure;
+  };
+  std::vector<Ghost3> ghosts;
+  std::map<std::tuple<int32_t, int32_t, int32_t>, std::vector<uint32_t>> ghost_grid;
+
+  static int32_t as_i32(float v) {
+    if (v != v) return 0;
+    if (v <= -2147483648.0f) return INT32_MIN;
+    if (v >= 2147483648.0f) return INT32_MAX;
+    return (int32_t)v;
+  }
+  void refresh_ghosts() {
+    ghosts.clear();
+    ghost_grid.clear();
+    const float hk = std::max(cfg.smoothing_length, kEps);
+    const float sp = std::max(hk * 0.5f, kEps), sp2 = sp * sp;
+    const float pi = Consts<float>::pi();
+    auto count = [](float v, float hi) -> uint64_t {  // .ceil().clamp(1, hi) as usize
+      return v != v ? 0 : (uint64_t)std::min(std::max(std::ceil(v), 1.0f), hi);
+    };
+    for (const Body3& b : bodies) {
+      // identity rotation: glam Mat3 * Vec3 = (x_axis*x + y_axis*y) + z_axis*z, then + position
+      auto put = [&](float x, float y, float z) {
+        ghosts.push_back({((1.0f * x + 0.0f * y) + 0.0f * z) + b.px, ((0.0f * x + 1.0f * y) + 0.0f * z) + b.py,
+                          ((0.0f * x + 0.0f * y) + 1.0f * z) + b.pz, 0, 0});
+      };
+      if (b.shape == 0) {
+        const float r = b.a;
+        const uint64_t n = count((4.0f * pi * r * r) / sp2, 512.0f);
+        const float golden = pi * (3.0f - std::sqrt(5.0f));
+        for (uint64_t k = 0; k < n; k++) {
+          const float z = 1.0f - 2.0f * ((float)k + 0.5f) / (float)n;
+          const float rr = std::sqrt(1.0f - z * z);
+          const float th = golden * (float)k;
+          put(std::cos(th) * rr * r, z * r, std::sin(th) * rr * r);
+        }
+      } else if (b.shape == 1) {
+        const float he[3] = {b.a, b.b, b.c};
+        const struct { float fixed; int axis; } faces[6] = {{-he[1], 0}, {-he[1], 0}, {-he[0], 1},
+                                                            {-he[0], 1}, {-he[2], 2}, {-he[2], 2}};
+        for (const auto& f : faces) {
+          const float area = f.axis == 0 ? 4.0f * he[1] * he[2] : f.axis == 1 ? 4.0f * he[0] * he[2] : 4.0f * he[0] * he[1];
+          const uint64_t n = count(area / sp2, 512.0f);
+          for (uint64_t k = 0; k < n; k++) {
+            const float t = ((float)k + 0.5f) / (float)n;
+            float l[3] = {0.0f, 0.0f, f.fixed};
+            const float u = (2.0f * t - 1.0f), v = (2.0f * std::fmod(t * 7.0f, 1.0f) - 1.0f);
+            if (f.axis == 0) {
+              l[1] = u * he[1];
+              l[2] = v * he[2];
+            } else if (f.axis == 1) {
+              l[0] = u * he[0];
+              l[2] = v * he[2];
+            } else {
+              l[0] = u * he[0];
+              l[1] = v * he[1];
+            }
+            put(l[0], l[1], l[2]);
+          }
+        }
+      } else {
+        const float r = b.a, hl = b.b;
+        const uint64_t n = count((4.0f * pi * r * hl) / sp2, 256.0f);
+        const float ys[2] = {-hl * 0.5f, hl * 0.5f};
+        for (float sy : ys)
+          for (uint64_t k = 0; k < n; k++) {
+            const float a = 2.0f * pi * (float)k / (float)n;
+            put(std::cos(a) * r, sy, std::sin(a) * r);
+          }
+        const float ss[2] = {-1.0f, 1.0f};
+        for (float s : ss) put((0.0f * s) * (hl + r), (1.0f * s) * (hl + r), (0.0f * s) * (hl + r));
+      }
+    }
+    for (uint32_t i = 0; i < ghosts.size(); i++) {
+      const Ghost3& g = ghosts[i];
+      if (!std::isfinite(g.x)) continue;
+      ghost_grid[{as_i32(std::floor(g.x / hk)), as_i32(std::floor(g.y / hk)), as_i32(std::floor(g.z / hk))}].push_back(i);
+    }
+  }
+  void ghost_density(R h) {
+    std::vector<uint32_t> nb;
+    for (Ghost3& g : ghosts) {
+      neighbors_of((R)g.x, (R)g.y, (R)g.z, particles, nb);
+      R rho = 0;
+      for (uint32_t j : nb) {
+        const R dx = particles[j].x - (R)g.x, dy = particles[j].y - (R)g.y, dz = particles[j].z - (R)g.z;
+        rho += particles[j].mass * poly6(dx * dx + dy * dy + dz * dz, h);
+      }
+      g.density = rclamp(rho, (R)0, (R)3 * rmax((R)cfg.rest_density, (R)kEps));
+      g.pressure = Fluid<R>::pressure(rho, (R)cfg.rest_density, (R)cfg.stiffness, (R)cfg.gamma, pow_mode);
+    }
+  }
+  void ghost_force(R px, R py, R pz, R q_i, R h, R& f0, R& f1, R& f2) const {
+    const R hg = (R)cfg.smoothing_length;
+    const R m = (R)std::max(cfg.particle_mass, kEps);
+    const int32_t cx = sat_i32(std::floor(px / hg)), cy = sat_i32(std::floor(py / hg)), cz = sat_i32(std::floor(pz / hg));
+    for (int oz = -1; oz <= 1; oz++)
+      for (int oy = -1; oy <= 1; oy++)
+        for (int ox = -1; ox <= 1; ox++) {
+          auto it = ghost_grid.find({(int32_t)((uint32_t)cx + (uint32_t)ox), (int32_t)((uint32_t)cy + (uint32_t)oy),
+                                     (int32_t)((uint32_t)cz + (uint32_t)oz)});
+          if (it == ghost_grid.end()) continue;
+          for (uint32_t k : it->second) {
+            const Ghost3& g = ghosts[k];
+            const R ex = (R)g.x - px, ey = (R)g.y - py, ez = (R)g.z - pz;
+            if (!(ex * ex + ey * ey + ez * ez < hg * hg)) continue;
+            const R dx = px - (R)g.x, dy = py - (R)g.y, dz = pz - (R)g.z;
+            const R dist = std::sqrt(dx * dx + dy * dy + dz * dz);
+            R g0, g1, g2;
+            spiky_grad(dx, dy, dz, dist, h, g0, g1, g2);
+            const R rb = rmax(g.density, (R)kEps);
+            const R s = m * (q_i + g.pressure / (rb * rb));
+            f0 -= g0 * s;
+            f1 -= g1 * s;
+            f2 -= g2 * s;
+          }
+        }
+  }
   size_t cap = 4096;
   int pow_mode = 1;
   std::vector<R> fx, fy, fz;
@@ -293,6 +418,7 @@ class Fluid3 {
           }
         }
       }
+      if (cfg.boundary_particles) ghost_force(P.x, P.y, P.z, p_i / (rho_i * rho_i), h, fxi, fyi, fzi);
       fx[i] = fxi;
       fy[i] = fyi;
       fz[i] = fzi;
@@ -503,6 +629,10 @@ class Fluid3 {
     R h = rmax((R)cfg.smoothing_length, (R)kEps);
     rebuild_grid();
     compute_density_pressure(h);
+    if (cfg.boundary_particles) {  // fluid3.rs:1018-1026
+      refresh_ghosts();
+      ghost_density(h);
+    }
     compute_forces(h);
     integrate(h, dt, mode);
     boundaries();

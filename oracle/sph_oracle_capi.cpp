@@ -554,6 +554,17 @@ void orc3_set_turbulence(void* h, int enabled, float amp, float freq, float tsca
   o->f64.turb = t;
 }
 
+uint32_t orc3_ghosts(void* h, float* xyz, uint32_t max) {
+  Orc3* o = static_cast<Orc3*>(h);
+  const auto& g = o->f32.ghosts;
+  for (uint32_t i = 0; xyz && i < std::min<size_t>(g.size(), max); i++) {
+    xyz[3 * i] = g[i].x;
+    xyz[3 * i + 1] = g[i].y;
+    xyz[3 * i + 2] = g[i].z;
+  }
+  return (uint32_t)g.size();
+}
+
 void orc3_set_gravity(void* h, float gx, float gy, float gz) {
   Orc3* o = static_cast<Orc3*>(h);
   o->f32.gx = gx;

@@ -50,6 +50,18 @@ struct GridPlan3 {
   uint32_t sentinel;
 };
 
+// One cell of the 3D boundary ghosts' hash grid (count 0 = empty slot).
+struct GhostCell3 {
+  int32_t cx, cy, cz;
+  uint32_t start, count;
+};
+
+__host__ __device__ inline uint32_t ghost_cell_hash3(int32_t cx, int32_t cy, int32_t cz, uint32_t mask) {
+  uint32_t h = (uint32_t)cx * 0x9E3779B1u ^ ((uint32_t)cy * 0x85EBCA77u) ^ ((uint32_t)cz * 0xC2B2AE3Du + 0x165667B1u);
+  h ^= h >> 15;
+  return h & mask;
+}
+
 struct StepParams3 {
   GridPlan3 grid;
   float hg2, hk, hk2;
@@ -66,6 +78,13 @@ struct StepParams3 {
   float turb_amp, turb_freq, turb_tscale;
   uint32_t turb_seed, turb_oct;  // octaves already clamped to 1..8
   const float* clock;            // device word holding the world clock of the current step
+  // boundary ghosts (F_GHOST, fluid3.rs:719-922): cell-grouped positions,
+  // their q = p / max(rho, EPS)^2 this substep, the cell table
+  const float4* gpos;
+  float* gq;
+  const GhostCell3* gtab;
+  uint32_t gtab_mask, nghost;
+  float gmass, rest0;
 };
 
 // Static body: shape 0 sphere (a = radius), 1 box (a, b, c half extents),
@@ -410,6 +429,89 @@ __device__ __forceinline__ void pair3(uint32_t j, float4 pi, float4 vi, float rh
   }
 }
 
+// Ghost pressure on a fluid particle (fluid3.rs:1073-1083), after its fluid
+// pairs: boundary_near's cells (oz, oy, ox = -1..1 around floor(p / h), h
+// the config's smoothing length) and filter, -grad W * (m_g (q_i + q_g)).
+static __device__ __noinline__ float3 ghost_force3(float4 pi, float q_i, float f0, float f1, float f2,
+                                                   const StepParams3 P) {
+  const float hg = P.grid.hg;
+  const int32_t cx = __float2int_rd(__fdiv_rn(pi.x, hg)), cy = __float2int_rd(__fdiv_rn(pi.y, hg));
+  const int32_t cz = __float2int_rd(__fdiv_rn(pi.z, hg));
+  for (int oz = -1; oz <= 1; oz++)
+    for (int oy = -1; oy <= 1; oy++)
+      for (int ox = -1; ox <= 1; ox++) {
+        const int32_t qx = (int32_t)((uint32_t)cx + (uint32_t)ox), qy = (int32_t)((uint32_t)cy + (uint32_t)oy);
+        const int32_t qz = (int32_t)((uint32_t)cz + (uint32_t)oz);
+        uint32_t slot = ghost_cell_hash3(qx, qy, qz, P.gtab_mask);
+        GhostCell3 c = P.gtab[slot];
+        for (uint32_t probe = 0; probe <= P.gtab_mask && c.count != 0 && (c.cx != qx || c.cy != qy || c.cz != qz);
+             probe++) {
+          slot = (slot + 1) & P.gtab_mask;
+          c = P.gtab[slot];
+        }
+        if (c.count == 0 || c.cx != qx || c.cy != qy || c.cz != qz) continue;
+        for (uint32_t k = c.start; k < c.start + c.count; k++) {
+          const float4 g = P.gpos[k];
+          const float ex = __fsub_rn(g.x, pi.x), ey = __fsub_rn(g.y, pi.y), ez = __fsub_rn(g.z, pi.z);
+          if (!(dot3(ex, ey, ez, ex, ey, ez) < P.hg2)) continue;
+          const float dx = __fsub_rn(pi.x, g.x), dy = __fsub_rn(pi.y, g.y), dz = __fsub_rn(pi.z, g.z);
+          const float dist = __fsqrt_rn(dot3(dx, dy, dz, dx, dy, dz));
+          float g0 = 0.0f, g1 = 0.0f, g2 = 0.0f;
+          if (!(dist >= P.hk || dist < kEps)) {
+            const float hr = __fsub_rn(P.hk, dist);
+            const float sc = __fmul_rn(__fmul_rn(P.c_spiky, hr), hr);
+            g0 = __fmul_rn(__fdiv_rn(dx, dist), sc);
+            g1 = __fmul_rn(__fdiv_rn(dy, dist), sc);
+            g2 = __fmul_rn(__fdiv_rn(dz, dist), sc);
+          }
+          const float mt = __fmul_rn(P.gmass, __fadd_rn(q_i, P.gq[k]));
+          f0 = __fsub_rn(f0, __fmul_rn(g0, mt));
+          f1 = __fsub_rn(f1, __fmul_rn(g1, mt));
+          f2 = __fsub_rn(f2, __fmul_rn(g2, mt));
+        }
+      }
+  return make_float3(f0, f1, f2);
+}
+
+// Ghost density and pressure from the fluid (fluid3.rs:906-921): the 27
+// cells around the ghost bucket by bucket in the reference's order, m_j *
+// poly6 for candidates within h; density clamped, pressure from the
+// unclamped sum with the config's rest density; stored as q.
+template <bool MASS>
+__global__ void __launch_bounds__(256) k_ghost_density3(const float4* __restrict__ spos,
+                                                        const float* __restrict__ smass,
+                                                        const uint32_t* __restrict__ start, StepParams3 P) {
+  const uint32_t gi = blockIdx.x * blockDim.x + threadIdx.x;
+  if (gi >= P.nghost) return;
+  const float4 b = P.gpos[gi];
+  const GridPlan3& g = P.grid;
+  float rho = 0.0f;
+  const uint32_t k = bucket_key3(b.x, b.y, b.z, g);
+  if (k != g.sentinel) {
+    const uint32_t bx = k & g.maskw, by = (k >> g.log2w) & g.maskh, bz = k >> (g.log2w + g.log2h);
+#pragma unroll 1
+    for (int r = 0; r < 9; r++) {
+      const uint32_t row = row_base3(by, bz, r, g);
+#pragma unroll 1
+      for (int ox = -1; ox <= 1; ox++) {
+        const uint32_t bb = row | ((bx + (uint32_t)ox) & g.maskw);
+        const uint32_t e = __ldg(&start[bb + 1]);
+        for (uint32_t j = __ldg(&start[bb]); j < e; j++) {
+          const float4 a = __ldg(&spos[j]);
+          const float dx = __fsub_rn(a.x, b.x), dy = __fsub_rn(a.y, b.y), dz = __fsub_rn(a.z, b.z);
+          rho = __fadd_rn(rho, contrib3(dot3(dx, dy, dz, dx, dy, dz), MASS ? __ldg(&smass[j]) : P.mass, P));
+        }
+      }
+    }
+  }
+  float dens = rho;
+  if (dens < 0.0f) dens = 0.0f;
+  if (dens > P.rho_cap) dens = P.rho_cap;
+  const float p = eos(rho, P.rest0, P);
+  const float rc = fmaxf(dens, kEps);
+  P.gq[gi] = __fdiv_rn(p, __fmul_rn(rc, rc));
+}
+
 // Force + XSPH + integrate + walls (fluid3.rs:1040-1176); writes the new
 // state (id order), the next key and its bucket count. DEBUG: forces only.
 template <bool MASS, bool DEBUG, bool PLAIN>
@@ -483,6 +585,12 @@ __global__ void __launch_bounds__(256) k_force3(const float4* __restrict__ spos,
       }
     }
   }
+  if (!PLAIN && (P.flags & F_GHOST)) {  // PLAIN launches exclude F_GHOST
+    const float3 gf = ghost_force3(pi, q_i, f[0], f[1], f[2], P);
+    f[0] = gf.x;
+    f[1] = gf.y;
+    f[2] = gf.z;
+  }
   if (DEBUG) {
     dbg[id] = make_float4(f[0], f[1], f[2], 0.0f);
     return;
@@ -490,7 +598,7 @@ __global__ void __launch_bounds__(256) k_force3(const float4* __restrict__ spos,
   float ax = __fadd_rn(P.gx, __fdiv_rn(f[0], rho_i));
   float ay = __fadd_rn(P.gy, __fdiv_rn(f[1], rho_i));
   float az = __fadd_rn(P.gz, __fdiv_rn(f[2], rho_i));
-  if (P.flags & F_TURB) {  // fluid3.rs:1096-1108, at the pre-step position and the step's clock
+  if (!PLAIN && (P.flags & F_TURB)) {  // fluid3.rs:1096-1108, at the pre-step position and the step's clock
     const float3 tb = turbulence_accel3(pi.x, pi.y, pi.z, *P.clock, P.turb_freq, P.turb_tscale, P.turb_seed,
                                         P.turb_oct, P.flags & F_TURB_CURL, P.turb_amp);
     ax = __fadd_rn(ax, tb.x);
@@ -576,6 +684,14 @@ struct World3 {
   float gx = 0.0f, gy = -9.81f, gz = 0.0f;  // World3::new gravity
   float time = 0.0f;
   std::vector<DevBody3> bodies;
+  // boundary ghosts (boundary_particles): regenerated when their inputs change
+  std::string ghost_sig;
+  std::vector<float4> h_gpos;
+  uint64_t ghost_regens = 0;
+  uint32_t nghost = 0, ghost_cap = 0, gtab_cap = 0, gtab_mask = 0;
+  float4* d_gpos = nullptr;
+  float* d_gq = nullptr;
+  GhostCell3* d_gtab = nullptr;
   bool bodies_dirty = true;
   uint32_t cap = kMaxParticles3D;
   uint32_t n = 0;
@@ -837,6 +953,151 @@ bool prepare3(World3* w) {
   return ok3(w, cudaGetLastError());
 }
 
+// ---- boundary ghosts (fluid3.rs:719-922) ----
+int32_t as_i32_3(float v) {  // Rust `as i32`: truncate, saturate, NaN -> 0
+  if (v != v) return 0;
+  if (v <= -2147483648.0f) return INT32_MIN;
+  if (v >= 2147483648.0f) return INT32_MAX;
+  return (int32_t)v;
+}
+uint64_t ghost_count3(float v, float hi) {  // `.ceil().clamp(1.0, hi) as usize` (NaN -> 0)
+  if (v != v) return 0;
+  return (uint64_t)std::min(std::max(std::ceil(v), 1.0f), hi);
+}
+
+// refresh_boundaries (fluid3.rs:719-855) for the world's static spheres,
+// boxes and capsules (identity rotation: transform_point = (x_axis * v.x +
+// y_axis * v.y + z_axis * v.z) + position, evaluated as glam's Mat3 * Vec3),
+// at spacing max(h * 0.5, EPS).
+void generate_ghosts3(const World3* w, float hk, std::vector<float4>& out) {
+  const float spacing = std::max(hk * 0.5f, kEps);
+  const float sp2 = spacing * spacing;  // powi(2)
+  const float pi = 3.14159265358979323846f;
+  out.clear();
+  for (const DevBody3& b : w->bodies) {
+    auto put = [&](float x, float y, float z) {
+      const float wx = ((1.0f * x + 0.0f * y) + 0.0f * z) + b.px;
+      const float wy = ((0.0f * x + 1.0f * y) + 0.0f * z) + b.py;
+      const float wz = ((0.0f * x + 0.0f * y) + 1.0f * z) + b.pz;
+      out.push_back(make_float4(wx, wy, wz, 0.0f));
+    };
+    if (b.shape == 0) {  // sphere: golden-angle spiral
+      const float r = b.a;
+      const uint64_t n = ghost_count3((4.0f * pi * r * r) / sp2, 512.0f);
+      const float golden = pi * (3.0f - std::sqrt(5.0f));
+      for (uint64_t k = 0; k < n; k++) {
+        const float z = 1.0f - 2.0f * ((float)k + 0.5f) / (float)n;
+        const float rr = std::sqrt(1.0f - z * z);
+        const float th = golden * (float)k;
+        put(std::cos(th) * rr * r, z * r, std::sin(th) * rr * r);
+      }
+    } else if (b.shape == 1) {  // box: six faces, (7 t) mod 1 across each
+      const float hx = b.a, hy = b.b, hz = b.c;
+      const float fixed[6] = {-hy, -hy, -hx, -hx, -hz, -hz};
+      const int axis[6] = {0, 0, 1, 1, 2, 2};
+      for (int f = 0; f < 6; f++) {
+        const int ax = axis[f];
+        const float area = ax == 0 ? 4.0f * hy * hz : ax == 1 ? 4.0f * hx * hz : 4.0f * hx * hy;
+        const uint64_t n = ghost_count3(area / sp2, 512.0f);
+        for (uint64_t k = 0; k < n; k++) {
+          const float t = ((float)k + 0.5f) / (float)n;
+          const float u = 2.0f * t - 1.0f, v = 2.0f * std::fmod(t * 7.0f, 1.0f) - 1.0f;
+          float lx = 0.0f, ly = 0.0f, lz = fixed[f];
+          if (ax == 0) {
+            ly = u * hy;
+            lz = v * hz;
+          } else if (ax == 1) {
+            lx = u * hx;
+            lz = v * hz;
+          } else {
+            lx = u * hx;
+            ly = v * hy;
+          }
+          put(lx, ly, lz);
+        }
+      }
+    } else {  // capsule along y: two rings at +-hl / 2, then the two poles
+      const float r = b.a, hl = b.b;
+      const uint64_t n = ghost_count3((4.0f * pi * r * hl) / sp2, 256.0f);
+      for (float sy : {-hl * 0.5f, hl * 0.5f})
+        for (uint64_t k = 0; k < n; k++) {
+          const float a = 2.0f * pi * (float)k / (float)n;
+          put(std::cos(a) * r, sy, std::sin(a) * r);
+        }
+      for (float sg : {-1.0f, 1.0f}) {
+        const float len = hl + r;
+        put((0.0f * sg) * len, (1.0f * sg) * len, (0.0f * sg) * len);  // Vec3::Y * s * (hl + r)
+      }
+    }
+  }
+}
+
+bool refresh_ghosts3(World3* w) {
+  const FluidConfig3Ffi& c = w->cfg;
+  std::string sig;
+  auto add = [&](const void* p, size_t n) { sig.append((const char*)p, n); };
+  add(&c.smoothing_length, 4);
+  add(&c.particle_mass, 4);
+  add(&c.rest_density, 4);
+  for (const DevBody3& b : w->bodies) add(&b, sizeof(DevBody3));
+  if (sig == w->ghost_sig && w->d_gtab) return true;
+  const float hk = std::max(c.smoothing_length, kEps);
+  std::vector<float4> raw;
+  generate_ghosts3(w, hk, raw);
+  std::vector<std::pair<std::pair<int64_t, int32_t>, uint32_t>> order;  // ((x, y), z) cell key, index
+  std::vector<int32_t> cell(3 * raw.size());
+  for (uint32_t i = 0; i < raw.size(); i++) {
+    if (!std::isfinite(raw[i].x)) continue;  // rebuild_boundary_grid checks x only (fluid3.rs:842-844)
+    const int32_t cx = as_i32_3(std::floor(raw[i].x / hk)), cy = as_i32_3(std::floor(raw[i].y / hk));
+    const int32_t cz = as_i32_3(std::floor(raw[i].z / hk));
+    cell[3 * i] = cx, cell[3 * i + 1] = cy, cell[3 * i + 2] = cz;
+    order.push_back({{((int64_t)cx << 32) | (uint32_t)cy, cz}, i});
+  }
+  std::stable_sort(order.begin(), order.end(), [](const auto& x, const auto& y) { return x.first < y.first; });
+  std::vector<float4> gpos(order.size());
+  std::vector<GhostCell3> cells;
+  for (size_t k = 0; k < order.size(); k++) {
+    const uint32_t i = order[k].second;
+    gpos[k] = raw[i];
+    if (cells.empty() || cells.back().cx != cell[3 * i] || cells.back().cy != cell[3 * i + 1] ||
+        cells.back().cz != cell[3 * i + 2])
+      cells.push_back({cell[3 * i], cell[3 * i + 1], cell[3 * i + 2], (uint32_t)k, 0});
+    cells.back().count++;
+  }
+  uint32_t tsize = 16;
+  while (tsize < 2 * cells.size()) tsize <<= 1;
+  std::vector<GhostCell3> tab(tsize, GhostCell3{0, 0, 0, 0, 0});
+  for (const GhostCell3& gc : cells) {
+    uint32_t slot = ghost_cell_hash3(gc.cx, gc.cy, gc.cz, tsize - 1);
+    while (tab[slot].count != 0) slot = (slot + 1) & (tsize - 1);
+    tab[slot] = gc;
+  }
+  const uint32_t ng = (uint32_t)gpos.size();
+  if (ng > w->ghost_cap || !w->d_gpos) {
+    cudaStreamSynchronize(w->stream);
+    dfree3(w->d_gpos), dfree3(w->d_gq);
+    const uint32_t cp = std::max<uint32_t>(ng, 64);
+    if (!dalloc3(w, w->d_gpos, cp) || !dalloc3(w, w->d_gq, cp)) return false;
+    w->ghost_cap = cp;
+  }
+  if (tsize > w->gtab_cap) {
+    cudaStreamSynchronize(w->stream);
+    dfree3(w->d_gtab);
+    if (!dalloc3(w, w->d_gtab, tsize)) return false;
+    w->gtab_cap = tsize;
+  }
+  if ((ng && !ok3(w, cudaMemcpyAsync(w->d_gpos, gpos.data(), sizeof(float4) * ng, cudaMemcpyHostToDevice, w->stream))) ||
+      !ok3(w, cudaMemcpyAsync(w->d_gtab, tab.data(), sizeof(GhostCell3) * tsize, cudaMemcpyHostToDevice, w->stream)) ||
+      !ok3(w, cudaStreamSynchronize(w->stream)))
+    return false;
+  w->nghost = ng;
+  w->gtab_mask = tsize - 1;
+  w->ghost_sig = sig;
+  w->h_gpos = std::move(gpos);
+  w->ghost_regens++;
+  return true;
+}
+
 StepParams3 make_params3(const World3* w, float dt) {
   StepParams3 P;
   std::memset(&P, 0, sizeof(P));
@@ -880,6 +1141,16 @@ StepParams3 make_params3(const World3* w, float dt) {
   if (!w->mass_uniform) f |= F_MASS;
   if (!w->phase_uniform) f |= F_PHASE;
   if (!(P.hg2 <= P.hk2)) f |= F_WIDE_NB;
+  if (c.boundary_particles && w->nghost && w->d_gtab) {
+    f |= F_GHOST;
+    P.gpos = w->d_gpos;
+    P.gq = w->d_gq;
+    P.gtab = w->d_gtab;
+    P.gtab_mask = w->gtab_mask;
+    P.nghost = w->nghost;
+    P.gmass = std::max(c.particle_mass, kEps);
+    P.rest0 = c.rest_density;
+  }
   const AmbientConfig3Ffi& a = w->ambient;
   if (a.turbulence_enabled != 0 && a.turbulence_amplitude > 0.0f && w->scalar) {  // fluid3.rs:1090-1091
     f |= F_TURB;
@@ -942,7 +1213,7 @@ void enqueue_force3(World3* w, const StepParams3& P, float4* dbg, cudaStream_t s
   const uint32_t g = cdiv(w->n, 128);  // 128-thread blocks: 286 -> 280 us at 1M (256, 5-block cap: 329 us)
   // XSPH on, artificial viscosity and cohesion off, h*h <= hk*hk: the
   // optional pair terms compiled out
-  const bool plain = (P.flags & F_VISC) && !(P.flags & (F_AV | F_COHESION | F_WIDE_NB));
+  const bool plain = (P.flags & F_VISC) && !(P.flags & (F_AV | F_COHESION | F_WIDE_NB | F_TURB | F_GHOST));
 #define PHIENG_F3(M, D, PL)                                                                                         \
   k_force3<M, D, PL><<<g, 128, 0, st>>>(w->spos, w->svel, w->sdq, w->skey, w->sid, w->smass, w->n, w->start, P,    \
                                         w->dbodies, w->nmask, w->pos, w->vel, w->key, w->count, dbg)
@@ -964,6 +1235,12 @@ void enqueue_substep3(World3* w, const StepParams3& P, cudaStream_t st) {
   enqueue_sort3(w, P, st);
   if (w->profiling) cudaEventRecordWithFlags(w->ev[1], st, cudaEventRecordExternal);
   enqueue_density3(w, P, st);
+  if ((P.flags & F_GHOST) && P.nghost) {
+    if (P.flags & F_MASS)
+      k_ghost_density3<true><<<cdiv(P.nghost, 256), 256, 0, st>>>(w->spos, w->smass, w->start, P);
+    else
+      k_ghost_density3<false><<<cdiv(P.nghost, 256), 256, 0, st>>>(w->spos, w->smass, w->start, P);
+  }
   if (w->profiling) cudaEventRecordWithFlags(w->ev[2], st, cudaEventRecordExternal);
   enqueue_force3(w, P, nullptr, st);
   if (w->profiling) cudaEventRecordWithFlags(w->ev[3], st, cudaEventRecordExternal);
@@ -1040,11 +1317,12 @@ bool cfl_substeps3(World3* w, float dt, uint32_t* out) {
 
 bool world_step3(World3* w, float dt) {
   if (w->cfg.enabled && w->n > 0 && dt > 0.0f) {
-    if (w->cfg.adaptive_resolution || w->cfg.boundary_particles) {
+    if (w->cfg.adaptive_resolution) {
       w->error = PHIENG_SPH_E_UNSUPPORTED;
       return false;
     }
     if (!prepare3(w)) return false;
+    if (w->cfg.boundary_particles && !refresh_ghosts3(w)) return false;
     uint32_t ns = 1;
     if (!cfl_substeps3(w, dt, &ns)) return false;
     const StepParams3 P = make_params3(w, dt / (float)ns);
@@ -1111,6 +1389,7 @@ void phieng_world3_free(World3* w) {
     release_graph3(w);
     free_particles3(w);
     dfree3(w->count), dfree3(w->start), dfree3(w->tilesum), dfree3(w->tstate), dfree3(w->scalar), dfree3(w->dbodies);
+    dfree3(w->d_gpos), dfree3(w->d_gq), dfree3(w->d_gtab);
     for (auto& e : w->ev)
       if (e) cudaEventDestroy(e);
     if (w->h_pinned) cudaFreeHost(w->h_pinned);
@@ -1144,6 +1423,18 @@ int32_t phieng_world3_get_time(World3* w, float* out) {
 }
 
 int32_t phieng_world3_body_count(World3* w) { return w ? (int32_t)w->bodies.size() : -1; }
+
+uint32_t phieng_sph3_ghosts(World3* w, float* xyz, uint32_t max, uint64_t* regens) {
+  if (!w) return 0;
+  if (regens) *regens = w->ghost_regens;
+  const uint32_t n = (uint32_t)w->h_gpos.size();
+  for (uint32_t i = 0; xyz && i < std::min(n, max); i++) {
+    xyz[3 * i] = w->h_gpos[i].x;
+    xyz[3 * i + 1] = w->h_gpos[i].y;
+    xyz[3 * i + 2] = w->h_gpos[i].z;
+  }
+  return n;
+}
 
 int32_t phieng_world3_set_ambient_config(World3* w, const AmbientConfig3Ffi* cfg) {
   if (!w || !cfg) return 0;

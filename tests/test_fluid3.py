@@ -649,3 +649,65 @@ def test_turbulence3_bit_exact(curl):
         if k % 40 == 39:
             assert_bit_equal(w.fluid.particles, o.state(), f"state after {k + 1} steps")
     assert w.time == o.time
+
+
+# ---------------------------------------------------------------- boundary ghosts (fluid3.rs:719-922)
+def ghost_cfg():
+    c = default_config()
+    c.boundary_particles = 1
+    return c
+
+
+def test_oracle3_ghosts_contained():
+    """fluid3.rs:1488-1518 on the oracle (the reference's in-place order)."""
+    o = make_oracle(lattice((0.0, 0.0, 0.0), 4, 6, 4, 0.25), cfg=ghost_cfg())
+    peak = 0.0
+    for _ in range(200):
+        o.step(1 / 60, REF_SEQ)
+        st = o.state()
+        peak = max(peak, float(np.sqrt((st[:, 3:6] ** 2).sum(1)).max()))
+    st = o.state()
+    assert np.isfinite(st).all() and len(o.ghosts()) > 0
+    assert (st[:, 0] > -1.0).all() and (st[:, 0] < 5.0).all() and (st[:, 2] > -1.0).all() and (st[:, 2] < 5.0).all()
+    assert peak < 30.0
+
+
+def gpu_ghosts3(w):
+    regens = C.c_uint64()
+    n = w._lib.phieng_sph3_ghosts(w._h, None, 0, C.byref(regens))
+    xyz = np.zeros((n, 3), np.float32)
+    w._lib.phieng_sph3_ghosts(w._h, xyz.ctypes.data_as(C.POINTER(C.c_float)), n, None)
+    return xyz, regens.value
+
+
+OBSTACLES3 = [
+    (SPHERE, (2.5, 0.2, 1.0), (0.4, 0.0, 0.0)),
+    (CAPSULE, (1.5, 0.3, 3.0), (0.25, 0.5, 0.0)),
+    (BOX, (3.5, -0.2, 3.2), (0.3, 0.3, 0.6)),
+]
+
+
+@pytest.mark.gpu
+def test_ghosts3_equal_oracle_persist_and_bit_exact():
+    """The GPU's ghost set equals the oracle's (tank boxes, a sphere, a
+    capsule, a box), is generated once for the static scene, and 120 steps
+    with ghosts (and CFL substeps) match the oracle bit for bit."""
+    cfg = ghost_cfg()
+    cfg.cfl = 0.3
+    cfg.max_substeps = 3
+    pts = lattice((0.0, 0.0, 0.0), 5, 7, 5, 0.25)
+    bodies = TANK + OBSTACLES3
+    o = make_oracle(pts, bodies=bodies, cfg=cfg)
+    w = make_gpu(pts, bodies=bodies, cfg=cfg)
+    for k in range(120):
+        o.step(1 / 60, JACOBI)
+        w.step(1 / 60)
+        if k == 0:
+            xyz, regens = gpu_ghosts3(w)
+            ref = o.ghosts()
+            assert len(xyz) == len(ref) > 0 and regens == 1
+            key = lambda a: a[np.lexsort((a[:, 2], a[:, 1], a[:, 0]))]  # noqa: E731
+            assert np.array_equal(key(xyz).view(np.uint32), key(ref).view(np.uint32))
+        if k % 40 == 39:
+            assert_bit_equal(w.fluid.particles, o.state(), f"state after {k + 1} steps")
+    assert gpu_ghosts3(w)[1] == 1
