@@ -618,6 +618,10 @@ static_assert(offsetof(AmbientConfig3Ffi, turbulence_enabled) == 60, "layout");
  * up to max (x, y, z) triples (cell-grouped), generation count. */
 uint32_t phieng_sph3_ghosts(World3* world, float* xyz, uint32_t max, uint64_t* regens);
 
+/* 3D particle masses by id (adaptive resolution changes them), as
+ * phieng_sph_fluid_masses. */
+uint32_t phieng_sph3_fluid_masses(World3* world, float* out, uint32_t max);
+
 /* ffi.rs:549 / 568 phieng_world3_set/get_ambient_config — as the 2D pair
  * (ambient3_from_ffi, ffi.rs:414-475); turbulence acts on the 3D fluid
  * (fluid3.rs:1090-1108). */

@@ -48,6 +48,7 @@ def _load():
         "orc_ghosts": (C.c_uint32, [P, C.c_void_p, C.c_uint32]),
         "orc_masses": (C.c_uint32, [P, C.c_void_p, C.c_uint32]),
         "orc3_ghosts": (C.c_uint32, [P, C.c_void_p, C.c_uint32]),
+        "orc3_masses": (C.c_uint32, [P, C.c_void_p, C.c_uint32]),
         "orc3_set_turbulence": (None, [P, C.c_int, C.c_float, C.c_float, C.c_float, C.c_uint32, C.c_uint32, C.c_int]),
         "orc_noise2": (None, [C.c_int, C.c_float, C.c_float, C.c_float, C.c_uint32, C.c_uint32, C.POINTER(C.c_float)]),
         "orc_set_cap": (None, [P, C.c_uint32]),
@@ -343,6 +344,13 @@ class OracleWorld3:
 
     def set_config(self, cfg: FluidConfig2Ffi) -> None:
         self._l.orc3_set_config(self._h, C.byref(cfg))
+
+    def masses(self) -> np.ndarray:
+        """Particle masses by index."""
+        n = self._l.orc3_masses(self._h, None, 0)
+        out = np.zeros(n, np.float32)
+        self._l.orc3_masses(self._h, out.ctypes.data, n)
+        return out
 
     def ghosts(self) -> np.ndarray:
         """3D boundary ghost positions of the last substep [m][3], generation order."""

@@ -625,10 +625,61 @@ class Fluid3 {
     return (uint32_t)k;
   }
 
+  // FluidState3::resample (fluid3.rs:923-990)
+  void resample(R h) {
+    const float rest = std::max(cfg.rest_density, kEps);
+    const R split_lo = (R)(cfg.split_density_ratio * rest), merge_hi = (R)(cfg.merge_density_ratio * rest);
+    const R min_mass = (R)(std::max(cfg.particle_mass, kEps) * 0.125f);
+    const size_t n = particles.size();
+    std::vector<char> absorbed(n, 0);
+    const R md = (R)0.25 * h, merge_d2 = md * md;
+    for (size_t i = 0; i < n; i++) {
+      if (absorbed[i] || particles[i].density <= merge_hi) continue;
+      for (size_t j = i; j-- > 0;) {
+        if (absorbed[j] || particles[j].density <= merge_hi) continue;
+        const R dx = particles[i].x - particles[j].x, dy = particles[i].y - particles[j].y;
+        const R dz = particles[i].z - particles[j].z;
+        if (dx * dx + dy * dy + dz * dz < merge_d2) {
+          const R mi = particles[i].mass, mj = particles[j].mass, mt = mi + mj;
+          if (mt > (R)kEps) {
+            particles[i].vx = (particles[i].vx * mi + particles[j].vx * mj) / mt;
+            particles[i].vy = (particles[i].vy * mi + particles[j].vy * mj) / mt;
+            particles[i].vz = (particles[i].vz * mi + particles[j].vz * mj) / mt;
+            particles[i].mass = mt;
+          }
+          absorbed[j] = 1;
+          break;
+        }
+      }
+    }
+    std::vector<Particle3<R>> out;
+    const R off = (R)0.25 * h;
+    for (size_t i = 0; i < n; i++) {
+      if (absorbed[i]) continue;
+      const Particle3<R>& p = particles[i];
+      if (p.density < split_lo && p.mass > min_mass && out.size() + 1 < 4096) {  // MAX_PARTICLES_3D
+        Particle3<R> a = p, b = p;
+        a.mass = b.mass = p.mass * (R)0.5;
+        a.x = p.x + off, a.y = p.y + (R)0, a.z = p.z + (R)0;
+        b.x = p.x - off, b.y = p.y - (R)0, b.z = p.z - (R)0;
+        out.push_back(a);
+        out.push_back(b);
+      } else {
+        out.push_back(p);
+      }
+    }
+    particles.swap(out);
+  }
+
   void substep(R dt, Mode mode) {
     R h = rmax((R)cfg.smoothing_length, (R)kEps);
     rebuild_grid();
     compute_density_pressure(h);
+    if (cfg.adaptive_resolution) {  // fluid3.rs:1008-1016
+      resample(h);
+      rebuild_grid();
+      compute_density_pressure(h);
+    }
     if (cfg.boundary_particles) {  // fluid3.rs:1018-1026
       refresh_ghosts();
       ghost_density(h);

@@ -554,6 +554,13 @@ void orc3_set_turbulence(void* h, int enabled, float amp, float freq, float tsca
   o->f64.turb = t;
 }
 
+uint32_t orc3_masses(void* h, float* out, uint32_t max) {
+  Orc3* o = static_cast<Orc3*>(h);
+  const auto& ps = o->f32.particles;
+  for (uint32_t i = 0; out && i < std::min<size_t>(ps.size(), max); i++) out[i] = ps[i].mass;
+  return (uint32_t)ps.size();
+}
+
 uint32_t orc3_ghosts(void* h, float* xyz, uint32_t max) {
   Orc3* o = static_cast<Orc3*>(h);
   const auto& g = o->f32.ghosts;

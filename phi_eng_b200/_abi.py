@@ -374,6 +374,7 @@ SIGNATURES = {
     "phieng_world3_body_count": (C.c_int32, [_P]),
     "phieng_world3_set_ambient_config": (C.c_int32, [_P, C.POINTER(AmbientConfig3Ffi)]),
     "phieng_sph3_ghosts": (C.c_uint32, [_P, _F, C.c_uint32, C.POINTER(C.c_uint64)]),
+    "phieng_sph3_fluid_masses": (C.c_uint32, [_P, _F, C.c_uint32]),
     "phieng_world3_get_ambient_config": (C.c_int32, [_P, C.POINTER(AmbientConfig3Ffi)]),
     "phieng_world3_add_body": (
         C.c_int32,

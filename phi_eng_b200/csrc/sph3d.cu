@@ -512,6 +512,93 @@ __global__ void __launch_bounds__(256) k_ghost_density3(const float4* __restrict
   P.gq[gi] = __fdiv_rn(p, __fmul_rn(rc, rc));
 }
 
+// FluidState3::resample (fluid3.rs:923-990), one thread as the 2D pass:
+// merges (index order, highest-index dense neighbour j < i within 0.25 h
+// among the 27-cell grid candidates, mass and momentum conserved), then
+// splits into half-mass children at x +- (0.25 h, 0, 0) while the output
+// holds fewer than MAX_PARTICLES_3D - 1.
+__global__ void k_resample3(uint32_t n, float4* __restrict__ pos, float4* __restrict__ vel, float* __restrict__ mass,
+                            const uint8_t* __restrict__ phase, const float2* __restrict__ sdq,
+                            const uint32_t* __restrict__ sid, const uint32_t* __restrict__ skey,
+                            const uint32_t* __restrict__ slot_of, const uint32_t* __restrict__ start, StepParams3 P,
+                            float merge_hi, float split_lo, float min_mass, uint8_t* __restrict__ absorbed,
+                            float4* __restrict__ out_pos, float4* __restrict__ out_vel, float* __restrict__ out_mass,
+                            uint8_t* __restrict__ out_phase, uint32_t* __restrict__ n_out) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  const GridPlan3& g = P.grid;
+  const float md = __fmul_rn(0.25f, P.hk), merge_d2 = __fmul_rn(md, md);
+  for (uint32_t i = 0; i < n; i++) absorbed[i] = 0;
+  for (uint32_t i = 0; i < n; i++) {
+    const uint32_t si = slot_of[i];
+    if (absorbed[i] || sdq[si].x <= merge_hi) continue;
+    const float4 pi = pos[i];
+    int64_t best = -1;
+    const uint32_t k = skey[si];
+    if (k != g.sentinel) {
+      const uint32_t bx = k & g.maskw, by = (k >> g.log2w) & g.maskh, bz = k >> (g.log2w + g.log2h);
+      for (int r = 0; r < 9; r++) {
+        const uint32_t row = row_base3(by, bz, r, g);
+        for (int ox = -1; ox <= 1; ox++) {
+          const uint32_t bb = row | ((bx + (uint32_t)ox) & g.maskw);
+          for (uint32_t js = start[bb]; js < start[bb + 1]; js++) {
+            const uint32_t j = sid[js];
+            if (j >= i || absorbed[j] || sdq[js].x <= merge_hi || (int64_t)j <= best) continue;
+            const float4 pj = pos[j];
+            const float dx = __fsub_rn(pi.x, pj.x), dy = __fsub_rn(pi.y, pj.y), dz = __fsub_rn(pi.z, pj.z);
+            if (dot3(dx, dy, dz, dx, dy, dz) < merge_d2) best = j;
+          }
+        }
+      }
+    }
+    if (best < 0) continue;
+    const uint32_t j = (uint32_t)best;
+    const float mi = mass[i], mj = mass[j];
+    const float mt = __fadd_rn(mi, mj);
+    if (mt > kEps) {
+      const float4 vi = vel[i], vj = vel[j];
+      vel[i] = make_float4(__fdiv_rn(__fadd_rn(__fmul_rn(vi.x, mi), __fmul_rn(vj.x, mj)), mt),
+                           __fdiv_rn(__fadd_rn(__fmul_rn(vi.y, mi), __fmul_rn(vj.y, mj)), mt),
+                           __fdiv_rn(__fadd_rn(__fmul_rn(vi.z, mi), __fmul_rn(vj.z, mj)), mt), vi.w);
+      mass[i] = mt;
+    }
+    absorbed[j] = 1;
+  }
+  uint32_t out = 0;
+  const float off = __fmul_rn(0.25f, P.hk);
+  for (uint32_t i = 0; i < n; i++) {
+    if (absorbed[i]) continue;
+    const float4 p = pos[i], v = vel[i];
+    const float m = mass[i];
+    if (sdq[slot_of[i]].x < split_lo && m > min_mass && out + 1 < 4096u) {  // MAX_PARTICLES_3D (fluid3.rs:28)
+      const float half = __fmul_rn(m, 0.5f);
+      out_pos[out] = make_float4(__fadd_rn(p.x, off), __fadd_rn(p.y, 0.0f), __fadd_rn(p.z, 0.0f), p.w);
+      out_vel[out] = v;
+      out_mass[out] = half;
+      out_phase[out++] = phase[i];
+      out_pos[out] = make_float4(__fsub_rn(p.x, off), __fsub_rn(p.y, 0.0f), __fsub_rn(p.z, 0.0f), p.w);
+      out_vel[out] = v;
+      out_mass[out] = half;
+      out_phase[out++] = phase[i];
+    } else {
+      out_pos[out] = p;
+      out_vel[out] = v;
+      out_mass[out] = m;
+      out_phase[out++] = phase[i];
+    }
+  }
+  *n_out = out;
+}
+
+__global__ void k_resample_prep3(const uint32_t* __restrict__ sid, uint32_t n, uint32_t* __restrict__ slot_of,
+                                 float* __restrict__ mass, uint8_t* __restrict__ phase, int mass_uniform,
+                                 float mass_value, int phase_uniform, uint8_t phase_value) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  slot_of[sid[s]] = s;
+  if (mass_uniform) mass[s] = mass_value;
+  if (phase_uniform) phase[s] = phase_value;
+}
+
 // Force + XSPH + integrate + walls (fluid3.rs:1040-1176); writes the new
 // state (id order), the next key and its bucket count. DEBUG: forces only.
 template <bool MASS, bool DEBUG, bool PLAIN>
@@ -692,6 +779,13 @@ struct World3 {
   float4* d_gpos = nullptr;
   float* d_gq = nullptr;
   GhostCell3* d_gtab = nullptr;
+  // adaptive resolution scratch (capacity = dcap when allocated)
+  uint32_t* rs_slot = nullptr;
+  uint8_t* rs_absorbed = nullptr;
+  float4 *rs_pos = nullptr, *rs_vel = nullptr;
+  float* rs_mass = nullptr;
+  uint8_t* rs_phase = nullptr;
+  uint32_t rs_cap = 0;
   bool bodies_dirty = true;
   uint32_t cap = kMaxParticles3D;
   uint32_t n = 0;
@@ -925,7 +1019,8 @@ bool prepare3(World3* w) {
   if (w->error != PHIENG_SPH_OK) return false;
   if (!ensure_device3(w)) return false;
   if (!w->dev_valid) {
-    if (!ensure_capacity3(w, w->n)) return false;
+    // adaptive resolution may split up to MAX_PARTICLES_3D particles
+    if (!ensure_capacity3(w, w->cfg.adaptive_resolution ? std::max(w->n, kMaxParticles3D) : w->n)) return false;
     if (!w->plan_valid) plan_grid3(w);
     if (w->n && (!ok3(w, cudaMemcpyAsync(w->pos, w->h_pos.data(), sizeof(float4) * w->n, cudaMemcpyHostToDevice,
                                          w->stream)) ||
@@ -1315,11 +1410,80 @@ bool cfl_substeps3(World3* w, float dt, uint32_t* out) {
   return true;
 }
 
+void recompute_uniformity3(World3* w);
+
+// One 3D substep with adaptive resolution (fluid3.rs:1008-1016), as the 2D
+// one: sort and density, resample (one thread), one read of the new count,
+// then the new set's keys and the whole substep body.
+bool run_substep3_adaptive(World3* w, float dt) {
+  const uint32_t c = w->dcap;
+  if (w->rs_cap < c || !w->rs_pos) {
+    cudaStreamSynchronize(w->stream);
+    dfree3(w->rs_slot), dfree3(w->rs_absorbed), dfree3(w->rs_pos), dfree3(w->rs_vel), dfree3(w->rs_mass),
+        dfree3(w->rs_phase);
+    if (!dalloc3(w, w->rs_slot, c) || !dalloc3(w, w->rs_absorbed, c) || !dalloc3(w, w->rs_pos, c) ||
+        !dalloc3(w, w->rs_vel, c) || !dalloc3(w, w->rs_mass, c) || !dalloc3(w, w->rs_phase, c))
+      return false;
+    w->rs_cap = c;
+  }
+  cudaStream_t st = w->stream;
+  StepParams3 P = make_params3(w, dt);
+  enqueue_sort3(w, P, st);
+  w->sid_perm_n = w->n;
+  enqueue_density3(w, P, st);
+  const FluidConfig3Ffi& cf = w->cfg;
+  const float rest = std::max(cf.rest_density, kEps);
+  uint32_t* n_out = w->scalar + 18;
+  if (w->n) {
+    k_resample_prep3<<<cdiv(w->n, 256), 256, 0, st>>>(w->sid, w->n, w->rs_slot, w->mass, w->phase,
+                                                       w->mass_uniform ? 1 : 0, P.mass, w->phase_uniform ? 1 : 0,
+                                                       (uint8_t)P.uniform_phase);
+    k_resample3<<<1, 1, 0, st>>>(w->n, w->pos, w->vel, w->mass, w->phase, w->sdq, w->sid, w->skey, w->rs_slot,
+                                 w->start, P, cf.merge_density_ratio * rest, cf.split_density_ratio * rest,
+                                 std::max(cf.particle_mass, kEps) * 0.125f, w->rs_absorbed, w->rs_pos, w->rs_vel,
+                                 w->rs_mass, w->rs_phase, n_out);
+  } else {
+    cudaMemsetAsync(n_out, 0, 4, st);
+  }
+  if (!ok3(w, cudaMemcpyAsync(w->h_pinned, n_out, 4, cudaMemcpyDeviceToHost, st)) || !ok3(w, cudaStreamSynchronize(st)))
+    return false;
+  uint32_t n2;
+  std::memcpy(&n2, w->h_pinned, 4);
+  if (n2 > c) {
+    w->error = PHIENG_SPH_E_CUDA;
+    return false;
+  }
+  w->h_pos.resize(n2), w->h_vel.resize(n2), w->h_mass.resize(n2), w->h_phase.resize(n2);
+  w->h_dens.resize(n2), w->h_pres.resize(n2);
+  if (n2 && (!ok3(w, cudaMemcpyAsync(w->pos, w->rs_pos, sizeof(float4) * n2, cudaMemcpyDeviceToDevice, st)) ||
+             !ok3(w, cudaMemcpyAsync(w->vel, w->rs_vel, sizeof(float4) * n2, cudaMemcpyDeviceToDevice, st)) ||
+             !ok3(w, cudaMemcpyAsync(w->mass, w->rs_mass, sizeof(float) * n2, cudaMemcpyDeviceToDevice, st)) ||
+             !ok3(w, cudaMemcpyAsync(w->phase, w->rs_phase, n2, cudaMemcpyDeviceToDevice, st)) ||
+             !ok3(w, cudaMemcpyAsync(w->h_mass.data(), w->rs_mass, sizeof(float) * n2, cudaMemcpyDeviceToHost, st)) ||
+             !ok3(w, cudaMemcpyAsync(w->h_phase.data(), w->rs_phase, n2, cudaMemcpyDeviceToHost, st)) ||
+             !ok3(w, cudaStreamSynchronize(st))))
+    return false;
+  w->n = n2;
+  recompute_uniformity3(w);
+  w->aux_valid = true;
+  w->host_valid = false;
+  P = make_params3(w, dt);
+  enqueue_keys3(w, st);
+  w->sid_perm_n = 0;
+  enqueue_substep3(w, P, st);
+  if (!ok3(w, cudaGetLastError())) return false;
+  w->sid_perm_n = w->n;
+  w->substeps++;
+  w->dp_dev = true;
+  w->keys_valid = true;
+  return true;
+}
+
 bool world_step3(World3* w, float dt) {
   if (w->cfg.enabled && w->n > 0 && dt > 0.0f) {
-    if (w->cfg.adaptive_resolution) {
-      w->error = PHIENG_SPH_E_UNSUPPORTED;
-      return false;
+    if (w->cfg.adaptive_resolution && w->pos && w->dcap < std::max(w->n, kMaxParticles3D)) {
+      if (!ensure_host3(w)) return false;  // room for the splits: re-upload into larger buffers
+      w->dev_valid = false;
     }
     if (!prepare3(w)) return false;
     if (w->cfg.boundary_particles && !refresh_ghosts3(w)) return false;
@@ -1332,7 +1496,7 @@ bool world_step3(World3* w, float dt) {
       enqueue_set_word(w->scalar + kClockWord3, bits, w->stream);
     }
     for (uint32_t k = 0; k < ns; k++)
-      if (!run_substep3(w, P)) return false;
+      if (!(w->cfg.adaptive_resolution ? run_substep3_adaptive(w, dt / (float)ns) : run_substep3(w, P))) return false;
   }
   w->time += dt;
   return true;
@@ -1390,6 +1554,8 @@ void phieng_world3_free(World3* w) {
     free_particles3(w);
     dfree3(w->count), dfree3(w->start), dfree3(w->tilesum), dfree3(w->tstate), dfree3(w->scalar), dfree3(w->dbodies);
     dfree3(w->d_gpos), dfree3(w->d_gq), dfree3(w->d_gtab);
+    dfree3(w->rs_slot), dfree3(w->rs_absorbed), dfree3(w->rs_pos), dfree3(w->rs_vel), dfree3(w->rs_mass),
+        dfree3(w->rs_phase);
     for (auto& e : w->ev)
       if (e) cudaEventDestroy(e);
     if (w->h_pinned) cudaFreeHost(w->h_pinned);
@@ -1423,6 +1589,12 @@ int32_t phieng_world3_get_time(World3* w, float* out) {
 }
 
 int32_t phieng_world3_body_count(World3* w) { return w ? (int32_t)w->bodies.size() : -1; }
+
+uint32_t phieng_sph3_fluid_masses(World3* w, float* out, uint32_t max) {
+  if (!w) return 0;
+  for (uint32_t i = 0; out && i < std::min(w->n, max); i++) out[i] = w->h_mass[i];
+  return w->n;
+}
 
 uint32_t phieng_sph3_ghosts(World3* w, float* xyz, uint32_t max, uint64_t* regens) {
   if (!w) return 0;
