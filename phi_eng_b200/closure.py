@@ -314,7 +314,7 @@ def generate_tracking_pairs(scs, mlp, ratio: int = 4, samples: int = 20, rollout
     return X, T
 
 
-def damped_targets(X, T, damp=(0.75, 1.0)):
+def damped_targets(X, T, damp=(0.95, 1.0)):
     """Project position targets onto pressure damping: the coarse step's
     pressure displacement is P = a_p (ratio dt)^2 / h (features 13, 14); the
     per-particle damping s that best explains the target in least squares,
@@ -346,7 +346,7 @@ def normalisation(X, T, sample: int = 1 << 20, seed: int = 7) -> np.ndarray:
 def train_closure(scs=None, ratio: int = 4, samples: int = 40, every: int = 50, batch: int = 65536,
                   iters: int = 20000, lr: float = 1e-3, seed: int = 0x5EED, noise=(0.0, 0.1),
                   dagger_iters: int = 0, dagger_samples: int = 20, rollout: int = 4, target: str = "damped",
-                  track_rounds: int = 0, track_iters: int = 5000, damp=(0.75, 1.0), log=print):
+                  track_rounds: int = 0, track_iters: int = 5000, damp=(0.95, 1.0), log=print):
     """Generate pairs on the batched scenes (the 256-scene slice of the batched
     workload by default) and train a network; with dagger_iters > 0, a second
     round adds pairs from the trained closure's own rollouts and continues
@@ -562,7 +562,7 @@ def _main(argv=None) -> None:
     t.add_argument("--dagger-iters", type=int, default=0)
     t.add_argument("--rollout", type=int, default=4)
     t.add_argument("--target", choices=list(TARGETS) + ["damped"], default="damped")
-    t.add_argument("--damp", default="0.75,1.0", help="damped target: the range of the pressure damping")
+    t.add_argument("--damp", default="0.95,1.0", help="damped target: the range of the pressure damping")
     t.add_argument("--track-rounds", type=int, default=0)
     t.add_argument("--ratio", type=int, default=4, help="coarse step = ratio * dt")
     e = sub.add_parser("eval")
