@@ -2,11 +2,16 @@
 """SPH dam-break throughput on B200: particle-updates/s.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload dam_break_1m|dam_break_4k] [--no-cpu-baseline]
+                    [--workload dam_break_1m|dam_break_4k|batch_512]
+                    [--precision tolerance|exact] [--no-cpu-baseline]
 
 One step = one fluid substep of the whole scene (sort, ranges, density,
 force + integrate + walls). Default workload: 1,048,576 particles (1024 x
-1024 lattice, 1 mm spacing) in a 10 x 6 m box, dt = 0.4 h / sqrt(gamma k).
+1024 lattice, 1 mm spacing) in a 10 x 6 m box, dt = 0.4 h / sqrt(gamma k),
+in the tolerance mode (phieng_sph_set_precision: reassociated density and
+force sums within the stated tolerances); the exact mode (the reference's
+f32 arithmetic bit for bit) is timed beside it, and so are steps 150..200 of
+the workload and the 512-scene batched workload.
 Inputs are resident in HBM when timing starts; L2 is flushed (256 MiB write)
 between timed steps, outside the timed events. Under torchrun each rank runs
 its own replica of the scene (the single-scene step has no exchange), so
@@ -40,8 +45,23 @@ from phi_eng_b200 import scenes  # noqa: E402
 METRIC = "particle-updates/s"
 HBM_FALLBACK = 6650.0
 
-# Algorithmic bytes per particle of each phase (every array read or written
-# once; neighbour re-reads not counted). B/N = buckets per particle.
+# Algorithmic bytes per particle-update of the reference's step (payload
+# bytes only, each array read or written once, neighbour re-reads not
+# counted): K1 hash 16 (read pos 8, write key + id 8); K2 radix sort of
+# (key, id) with 3 digit passes 16 * 3 + 4 = 52; K3 cell ranges 4 + 8 c
+# (c = occupied cells per particle, 0.25 at rest density) = 6; K4 reorder 32
+# (read pos + vel 16, write them sorted 16); K5 density 16 (read pos 8,
+# write density + pressure 8); K6 force + integrate 40 (read pos, vel,
+# density, pressure 24, write pos + vel 16). Whole step 162.
+ALG_BYTES = dict(hash=16, sort=52, ranges=6, reorder=32, density=16, force=40)
+STEP_ALG_BYTES = sum(ALG_BYTES.values())
+# the bench's phases: the library's sort phase holds K2-K4, its force pass
+# also writes the next keys (K1, counted nowhere else)
+PHASE_ALG_BYTES = dict(sort_ranges=ALG_BYTES["sort"] + ALG_BYTES["ranges"] + ALG_BYTES["reorder"],
+                       density=ALG_BYTES["density"], force_integrate=ALG_BYTES["force"] + ALG_BYTES["hash"])
+
+# What this implementation moves per particle (each of its arrays read or
+# written once; B/N = buckets per particle):
 #   sort:    scan: read counts twice, write start + cursor, clear counts
 #            (20 B per bucket); place: read id 4 + key 4, write (key, id) 8;
 #            fixup: read (key, id) 8 + start 8, write (key, id) 8,
@@ -52,9 +72,9 @@ HBM_FALLBACK = 6650.0
 #            write state 16 + next key 4                             = 64
 DENSITY_BYTES = 36
 FORCE_BYTES = 64
-# DRAM bytes (read + write) of one launch of the named phase's kernel, from
-# the ncu capture summarised in profiles/<kernel>_<workload>.md.
-PROFILED_TRAFFIC = {("dam_break_1m", "force_integrate"): 48.333312e6 + 1.921792e6}
+# DRAM bytes (read + write) of one launch of the named kernel on the named
+# workload and precision mode, from an ncu capture (profiles/).
+PROFILED_TRAFFIC = {("dam_break_1m", "exact", "force_integrate"): 48.333312e6 + 1.921792e6}
 PROFILED_TRAFFIC_3D = {"force_integrate": 85.545216e6 + 14.838528e6}  # 100^3 3D dam break
 KERNELS_PER_STEP = 5  # single-pass scan, place, fixup, density, force
 
@@ -434,10 +454,94 @@ def run_slab(args, rank: int, world: int, local_rank: int) -> None:
     dist.destroy_process_group()
 
 
+def timed_steps(w, dt: float, steps: int, stream, flush, phases: bool = True):
+    """Device time of `steps` world steps on `stream` (CUDA events around each
+    step, L2 flushed before each one outside the events); returns
+    (ms per step list, per-phase ms array of shape (steps, 3) or None)."""
+    import torch
+
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    ph = []
+    for k in range(steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        ev[k][0].record(stream)
+        w.step(dt)
+        ev[k][1].record(stream)
+        if phases:
+            ph.append(w.phase_times())
+    torch.cuda.synchronize()
+    return [a.elapsed_time(b) for a, b in ev], (np.array(ph) if phases else None)
+
+
+def roofline_of(phase_ms, n: int, workload: str, precision: str, buckets: int) -> dict:
+    """Roofline of the dominant phase's kernel at its algorithmic bytes per
+    particle (ALG_BYTES; the force pass is held to the reference's K6 bytes,
+    40, although it also writes the next keys), with this implementation's
+    own bytes and the profiled DRAM traffic beside it."""
+    names = ["sort_ranges", "density", "force_integrate"]
+    alg = [PHASE_ALG_BYTES["sort_ranges"], ALG_BYTES["density"], ALG_BYTES["force"]]
+    impl = [sort_bytes(buckets / n), DENSITY_BYTES, FORCE_BYTES]
+    top = int(np.argmax(phase_ms))
+    peak, peak_kind = hbm_peak()
+    achieved = alg[top] * n / (phase_ms[top] / 1000.0) / 1e9
+    traffic = PROFILED_TRAFFIC.get((workload, precision, names[top]))
+    return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": traffic, "kernel": names[top], "bytes_per_particle": alg[top],
+            "implementation_bytes_per_particle": impl[top],
+            "traffic_over_algorithmic": (traffic / (alg[top] * n)) if traffic else None,
+            "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+            else "fallback 6650 GB/s"}
+
+
+def whole_step_of(ms_per_step: float, n: int) -> dict:
+    peak, _ = hbm_peak()
+    gbs = STEP_ALG_BYTES * n / (ms_per_step / 1000.0) / 1e9
+    return {"bytes_per_particle": STEP_ALG_BYTES, "achieved_gbs": gbs, "frac": gbs / peak,
+            "bytes": "K1 hash 16 + K2 sort (3 digit passes) 52 + K3 ranges 6 + K4 reorder 32 + K5 density 16 + "
+                     "K6 force 40"}
+
+
+def batch_line(steps: int, warmup: int, tuning_mode: str, cpu: bool) -> dict:
+    """The batched workload (512 independent scenes, one CUDA graph of the
+    step's kernels for all of them per step), device-timed like the main
+    line, with the oracle's in-place CPU step on a sample of its scenes."""
+    import torch
+
+    scs = workload_scenes("batch_512")
+    job = Job(scs)
+    n = job.n
+    w = job.world
+    tuning = apply_tuning(w, tuning_mode, job.dt)
+    stream = torch.cuda.Stream()
+    w.set_stream(stream.cuda_stream)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    for _ in range(max(warmup, 3)):
+        w.step(job.dt)
+    w.set_profiling(True)
+    w.step(job.dt)
+    buckets = w.status().grid_buckets
+    torch.cuda.synchronize()
+    step_ms, ph = timed_steps(w, job.dt, steps, stream, flush)
+    ms = sum(step_ms) / steps
+    ph_mean = ph.mean(axis=0)
+    job.close()
+    out = {"metric": METRIC, "value": n / (ms / 1000.0), "ms_per_step": ms, "particles": n,
+           "scenes": len(scs), "workload": workload_desc("batch_512", scs), "buckets": int(buckets),
+           "tuning": tuning, "precision": "exact (batches run the exact passes)",
+           "phases_ms": {k: float(v) for k, v in zip(["sort_ranges", "density", "force_integrate"], ph_mean)},
+           "roofline": roofline_of(ph_mean, n, "batch_512", "exact", buckets), "whole_step": whole_step_of(ms, n),
+           "step_ms_min_max": [float(min(step_ms)), float(max(step_ms))]}
+    if cpu:
+        sample = [scs[i] for i in range(0, len(scs), 64)]  # 8 scenes spread over the size range
+        out["cpu_baseline"] = cpu_baseline(sample, budget_s=15.0, max_steps=10)
+    return out
+
+
 def run_ours(args, rank: int, world: int, local_rank: int):
     import torch
 
-    from phi_eng_b200.world import world_from_scene
+    from phi_eng_b200 import _abi
 
     torch.cuda.set_device(local_rank)
     dist = None
@@ -448,11 +552,15 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
 
     scs = workload_scenes(args.workload)
+    single = len(scs) == 1
+    mode = _abi.TOLERANCE if args.precision == "tolerance" else _abi.EXACT
     job = Job(scs)
     n_total, dt = job.n, job.dt
-    tuning = apply_tuning(job.world, args.tuning, dt)
-    stream = torch.cuda.Stream()
     w = job.world
+    if single:
+        w.precision = mode
+    tuning = apply_tuning(w, args.tuning, dt)
+    stream = torch.cuda.Stream()
     w.set_stream(stream.cuda_stream)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
@@ -470,39 +578,51 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     sampler = ClockSampler(local_rank) if rank == 0 else None
     if sampler:
         sampler.start()
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    phases = []
-    for k in range(args.steps):
-        with torch.cuda.stream(stream):
-            flush.zero_()
-        ev[k][0].record(stream)
-        w.step(dt)
-        ev[k][1].record(stream)
-        phases.append(w.phase_times())
-    torch.cuda.synchronize()
+    step_ms, ph = timed_steps(w, dt, args.steps, stream, flush)
     clocks = sampler.stop() if sampler else None
-    step_ms = [a.elapsed_time(b) for a, b in ev]
     total_ms = sum(step_ms)
     if dist:
         t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_ms = float(t.item())
     value = n_total * args.steps * world / (total_ms / 1000.0)
-
-    ph = np.array(phases)
     ph_mean = ph.mean(axis=0)
     names = ["sort_ranges", "density", "force_integrate"]
-    bytes_pp = [sort_bytes(buckets / n_total), DENSITY_BYTES, FORCE_BYTES]
-    top = int(np.argmax(ph_mean))
-    peak, peak_kind = hbm_peak()
-    achieved = bytes_pp[top] * n_total / (ph_mean[top] / 1000.0) / 1e9
-    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": PROFILED_TRAFFIC.get((args.workload, names[top])), "kernel": names[top], "bytes_per_particle": bytes_pp[top],
-                "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
-                else "fallback 6650 GB/s"}
-    step_bytes = sum(bytes_pp) * n_total
-    whole = {"bytes_per_particle": sum(bytes_pp),
-             "achieved_gbs": step_bytes / (total_ms / args.steps / 1000.0) / 1e9}
+    precision = "tolerance" if (single and mode == _abi.TOLERANCE) else "exact"
+    roofline = roofline_of(ph_mean, n_total, args.workload, precision, buckets)
+    whole = whole_step_of(total_ms / args.steps, n_total)
+
+    # the exact mode (the reference's f32 arithmetic bit for bit) on the same
+    # world, from where the timed steps left it
+    exact = None
+    if single and mode == _abi.TOLERANCE and not args.no_exact:
+        w.precision = _abi.EXACT
+        for _ in range(3):
+            w.step(dt)
+        e_ms, e_ph = timed_steps(w, dt, args.steps, stream, flush)
+        e_mean = e_ph.mean(axis=0)
+        em = sum(e_ms) / args.steps
+        exact = {"value": n_total / (em / 1000.0), "ms_per_step": em,
+                 "phases_ms": {k: float(v) for k, v in zip(names, e_mean)},
+                 "roofline": roofline_of(e_mean, n_total, args.workload, "exact", buckets),
+                 "whole_step": whole_step_of(em, n_total)}
+        w.precision = mode
+
+    # later in the flow: steps 150..200 of the 200-step workload
+    late = None
+    if single and args.workload == "dam_break_1m" and not args.no_late:
+        w.set_profiling(False)
+        done = args.warmup + 1 + args.steps + (args.steps + 3 if exact else 0)
+        if done < 150:
+            w.step_n(dt, 150 - done)
+        w.set_profiling(True)
+        w.step(dt)
+        l_ms, l_ph = timed_steps(w, dt, 50, stream, flush)
+        lm = sum(l_ms) / 50
+        late = {"steps": f"{max(done, 150) + 1}..{max(done, 150) + 50}", "ms_per_step": lm,
+                "value": n_total / (lm / 1000.0),
+                "phases_ms": {k: float(v) for k, v in zip(names, l_ph.mean(axis=0))},
+                "front_x": w.front_metrics()[0]}
 
     # end to end through the C ABI from host buffers: the worlds are built and
     # filled from host arrays outside the timed region; timed: the first
@@ -513,6 +633,8 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     job2 = Job(scs)
     from phi_eng_b200 import autotune as at
 
+    if single:
+        job2.world.precision = mode
     at.apply(job2.world, tuning)
     if job2.batch is None:
         job2.world.reserve(n_total)  # device arrays allocated before the clock starts
@@ -546,19 +668,24 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         base = cpu_baseline(scs)
 
     if rank == 0:
-        kernels_per_step = KERNELS_PER_STEP
         line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
                 "config": {"workload": workload_desc(args.workload, scs), "particles": n_total, "parallelism":
                            ("replicas" if world > 1 else "single"),
                            "l2": "flushed between timed steps (256 MiB write, outside the timed events)",
-                           "buckets": int(buckets), "tuning": tuning},
+                           "buckets": int(buckets), "tuning": tuning, "precision": precision},
                 "roofline": roofline, "whole_step": whole,
                 "phases_ms": {n: float(v) for n, v in zip(names, ph_mean)},
-                "cpu_baseline": base, "e2e": e2e, "gpu_launches": kernels_per_step * args.steps,
+                "cpu_baseline": base, "e2e": e2e, "gpu_launches": KERNELS_PER_STEP * args.steps,
                 "clocks": clocks}
-        if args.closure and len(scs) == 1 and world == 1:
+        if exact:
+            line["exact_mode"] = exact
+        if late:
+            line["late_flow"] = late
+        if args.batch and world == 1 and args.workload != "batch_512":
+            line["batch"] = batch_line(args.steps, args.warmup, args.tuning, not args.no_cpu_baseline)
+        if args.closure and single and world == 1:
             line["closure"] = closure_line(scs[0])
         if args.fluid3d and world == 1:
             line["fluid3d"] = fluid3d_line(args.steps, args.warmup)
@@ -583,6 +710,13 @@ def main():
                     help="skip the learned-closure comparison line")
     ap.add_argument("--no-fluid3d", dest="fluid3d", action="store_false",
                     help="skip the 3D step line")
+    ap.add_argument("--no-batch", dest="batch", action="store_false",
+                    help="skip the batched-scenes line (512 scenes)")
+    ap.add_argument("--precision", choices=["tolerance", "exact"], default="tolerance",
+                    help="arithmetic of the plain passes (phieng_sph_set_precision); the other mode is "
+                         "timed beside it unless --no-exact")
+    ap.add_argument("--no-exact", action="store_true", help="skip the exact-mode comparison")
+    ap.add_argument("--no-late", action="store_true", help="skip the late-flow timing (steps 150..200)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     rank = int(os.environ.get("RANK", "0"))

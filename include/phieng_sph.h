@@ -292,9 +292,14 @@ uint32_t phieng_sph_phase_times(World2* world, float* ms, uint32_t max);
  * 6 MiB inside this library (held on every GPU that loads it until exit),
  * which limits n to 65536 (more returns PHIENG_SPH_E_TOO_LARGE). The first
  * call on a device resolves that array's address; make it before any stream
- * capture. Calls share the array, so calls whose GPU work overlaps race:
- * order them on the device. Synchronises the stream once (to read the
- * particles' bounding box). Returns PHIENG_SPH_OK or an error code. */
+ * capture. The address is kept per device for the life of the process: after
+ * cudaDeviceReset the process must be restarted before the next call. Calls
+ * share the array, so calls whose GPU work overlaps race: order them on the
+ * device. Every call blocks the calling thread once, until `stream` has
+ * finished the particles' bounding-box pass (a 20-byte read-back that sizes
+ * the bucket grid); the remaining work is queued on `stream` when it returns.
+ * Every particle is phase 0 (cfg's phase_rest_density[0] and phase_mass[0]).
+ * Returns PHIENG_SPH_OK or an error code. */
 int32_t phieng_sph_density_noalloc(const float* xy, uint32_t n, const FluidConfig2Ffi* cfg, float* density,
                                    float* pressure, void* stream);
 
@@ -324,13 +329,32 @@ typedef struct PhiengSphTuning {
   uint32_t density_block;     /* threads per block of the density pass: 64, 128, 256 (default 256) */
   uint32_t force_block;       /* threads per block of the force pass: 64, 128, 256 (default 256) */
   float buckets_per_particle; /* bucket-grid budget per particle, 0.125..16 (default 2) */
-  uint32_t reserved;
+  uint32_t stage;             /* tolerance-mode passes: bit 0 = the density pass stages its neighbour
+                                 rows in shared memory, bit 1 = the force pass does (default 3) */
 } PhiengSphTuning;
 
 /* 1 ok, 0 null or out of range (world unchanged). Replans the bucket grid
  * unless phieng_sph_set_grid fixed it. */
 int32_t phieng_sph_set_tuning(World2* world, const PhiengSphTuning* tuning);
 int32_t phieng_sph_get_tuning(const World2* world, PhiengSphTuning* out);
+
+/* ---- arithmetic mode of the density and force passes (additive) ----
+ * EXACT (default): every pair term in the reference's f32 expression order
+ * with IEEE division and square root (fluid.rs:265-297, 592-611, 942-1050):
+ * bit-identical to the reference's arithmetic in the Jacobi integrate order.
+ * TOLERANCE: for the plain flag set (uniform mass and phase, XSPH on, no
+ * artificial viscosity, cohesion, turbulence, ghosts or polygons) the
+ * density, force and XSPH sums are reassociated with fused multiply-adds,
+ * one approximate reciprocal square root and one approximate reciprocal per
+ * neighbour pair. Neighbour sets, sort order and visit order stay exact and
+ * runs stay bit-reproducible; from identical state, density agrees with the
+ * exact mode within 1e-5 and force within 1e-4 of their RMS. Other flag sets
+ * and batches run the exact passes in either mode. */
+#define PHIENG_SPH_EXACT 0u
+#define PHIENG_SPH_TOLERANCE 1u
+/* 1 ok, 0 null or an unknown mode (world unchanged). */
+int32_t phieng_sph_set_precision(World2* world, uint32_t mode);
+uint32_t phieng_sph_get_precision(const World2* world);
 
 /* ---- device-resident state (additive; callers that keep data on the GPU) ----
  * Pointers are CUDA device pointers on the world's device; the copies are

@@ -269,9 +269,12 @@ class PhiengSphTuning(C.Structure):
         ("density_block", C.c_uint32),
         ("force_block", C.c_uint32),
         ("buckets_per_particle", C.c_float),
-        ("reserved", C.c_uint32),
+        ("stage", C.c_uint32),
     ]
 
+
+EXACT = 0  # PHIENG_SPH_EXACT: the reference's f32 arithmetic, bit for bit
+TOLERANCE = 1  # PHIENG_SPH_TOLERANCE: reassociated plain passes, within the stated tolerances
 
 MLP_PARAMS = 5378
 MLP_NORM = 34
@@ -332,6 +335,8 @@ SIGNATURES = {
     "phieng_sph_density_noalloc": (C.c_int32, [_P, C.c_uint32, C.POINTER(FluidConfig2Ffi), _P, _P, _P]),
     "phieng_sph_set_tuning": (C.c_int32, [_P, C.POINTER(PhiengSphTuning)]),
     "phieng_sph_get_tuning": (C.c_int32, [_P, C.POINTER(PhiengSphTuning)]),
+    "phieng_sph_set_precision": (C.c_int32, [_P, C.c_uint32]),
+    "phieng_sph_get_precision": (C.c_uint32, [_P]),
     "phieng_sph_get_state_device": (C.c_uint32, [_P, _P, C.c_uint32]),
     "phieng_sph_set_state_device": (C.c_int32, [_P, _P, C.c_uint32]),
     "phieng_sph_load_state_device": (C.c_int32, [_P, _P, C.c_uint32]),

@@ -26,8 +26,11 @@ from . import _abi
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 SHIPPED = os.path.join(HERE, "tuning_b200.json")
-DEFAULT = dict(density_block=256, force_block=256, buckets_per_particle=2.0)
-CANDIDATES = dict(density_block=(128, 256), force_block=(64, 128, 256), buckets_per_particle=(0.5, 1.0, 2.0, 4.0))
+DEFAULT = dict(density_block=256, force_block=256, buckets_per_particle=2.0, stage=3)
+CANDIDATES = dict(density_block=(128, 256), force_block=(64, 128, 256), buckets_per_particle=(0.5, 1.0, 2.0, 4.0),
+                  stage=(3,))
+# tolerance-mode worlds also try the passes without shared-memory staging
+CANDIDATES_TOLERANCE = dict(CANDIDATES, stage=(0, 1, 2, 3))
 
 
 def cache_path() -> str:
@@ -51,7 +54,8 @@ def signature(world) -> str:
     n2 = int(float(f"{n:.2g}")) if n else 0
     scenes = int(world._lib.phieng_sph_batch_scenes(world._h)) or 1
     h = float(world.fluid.config.smoothing_length) if scenes == 1 else 0.0
-    return f"n{n2}|s{scenes}|h{h:.3g}"
+    mode = "|tol" if int(world._lib.phieng_sph_get_precision(world._h)) == _abi.TOLERANCE else ""
+    return f"n{n2}|s{scenes}|h{h:.3g}{mode}"
 
 
 def _load(path: str) -> dict:
@@ -74,7 +78,7 @@ def lookup(world, gpu: str | None = None):
 
 def apply(world, tuning: dict) -> None:
     t = _abi.PhiengSphTuning(int(tuning["density_block"]), int(tuning["force_block"]),
-                             float(tuning["buckets_per_particle"]), 0)
+                             float(tuning["buckets_per_particle"]), int(tuning.get("stage", 3)))
     if world._lib.phieng_sph_set_tuning(world._h, C.byref(t)) != 1:
         raise ValueError(f"invalid tuning {tuning}")
 
@@ -83,7 +87,7 @@ def current(world) -> dict:
     t = _abi.PhiengSphTuning()
     world._lib.phieng_sph_get_tuning(world._h, C.byref(t))
     return dict(density_block=int(t.density_block), force_block=int(t.force_block),
-                buckets_per_particle=float(t.buckets_per_particle))
+                buckets_per_particle=float(t.buckets_per_particle), stage=int(t.stage))
 
 
 def time_steps(world, dt: float, steps: int, warmup: int = 2) -> float:
@@ -108,14 +112,16 @@ def autotune(world, dt: float, steps: int = 20, candidates: dict | None = None, 
     candidates) and leave the fastest applied. Returns {tuning, ms, table}."""
     import torch
 
-    cand = candidates or CANDIDATES
+    tol = int(world._lib.phieng_sph_get_precision(world._h)) == _abi.TOLERANCE
+    cand = candidates or (CANDIDATES_TOLERANCE if tol else CANDIDATES)
     n = int(world.status().particles)
     saved = torch.empty((max(n, 1), 4), dtype=torch.float32, device="cuda")
     world.get_state_device(saved.data_ptr(), n)
     world.sync()
     table = []
-    for db, fb, bpp in itertools.product(cand["density_block"], cand["force_block"], cand["buckets_per_particle"]):
-        t = dict(density_block=db, force_block=fb, buckets_per_particle=bpp)
+    for db, fb, bpp, stg in itertools.product(cand["density_block"], cand["force_block"],
+                                              cand["buckets_per_particle"], cand.get("stage", (3,))):
+        t = dict(density_block=db, force_block=fb, buckets_per_particle=bpp, stage=stg)
         apply(world, t)
         world.set_state_device(saved.data_ptr(), n)
         ms = time_steps(world, dt, steps)

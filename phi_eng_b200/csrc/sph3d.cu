@@ -39,6 +39,11 @@ namespace phieng {
 namespace {
 
 constexpr uint32_t kMaxParticles3D = 4096;  // MAX_PARTICLES_3D (fluid3.rs:28)
+
+// Most particles one 3D resample pass (fluid3.rs:923-990) can leave from n:
+// a split only happens while the output holds fewer than MAX_PARTICLES_3D - 1
+// particles, so at most MAX_PARTICLES_3D / 2 particles split.
+inline uint32_t resample_bound3(uint32_t n) { return n + std::min(n, kMaxParticles3D / 2); }
 constexpr uint32_t kMaskBits3 = 32;
 
 struct GridPlan3 {
@@ -523,7 +528,7 @@ __global__ void k_resample3(uint32_t n, float4* __restrict__ pos, float4* __rest
                             const uint32_t* __restrict__ slot_of, const uint32_t* __restrict__ start, StepParams3 P,
                             float merge_hi, float split_lo, float min_mass, uint8_t* __restrict__ absorbed,
                             float4* __restrict__ out_pos, float4* __restrict__ out_vel, float* __restrict__ out_mass,
-                            uint8_t* __restrict__ out_phase, uint32_t* __restrict__ n_out) {
+                            uint8_t* __restrict__ out_phase, uint32_t out_cap, uint32_t* __restrict__ n_out) {
   if (blockIdx.x != 0 || threadIdx.x != 0) return;
   const GridPlan3& g = P.grid;
   const float md = __fmul_rn(0.25f, P.hk), merge_d2 = __fmul_rn(md, md);
@@ -569,7 +574,12 @@ __global__ void k_resample3(uint32_t n, float4* __restrict__ pos, float4* __rest
     if (absorbed[i]) continue;
     const float4 p = pos[i], v = vel[i];
     const float m = mass[i];
-    if (sdq[slot_of[i]].x < split_lo && m > min_mass && out + 1 < 4096u) {  // MAX_PARTICLES_3D (fluid3.rs:28)
+    const bool split = sdq[slot_of[i]].x < split_lo && m > min_mass && out + 1 < 4096u;  // MAX_PARTICLES_3D (fluid3.rs:28)
+    if (out + (split ? 2u : 1u) > out_cap) {  // never with buffers sized for the bound: report, write nothing past
+      *n_out = out_cap + 1u;
+      return;
+    }
+    if (split) {
       const float half = __fmul_rn(m, 0.5f);
       out_pos[out] = make_float4(__fadd_rn(p.x, off), __fadd_rn(p.y, 0.0f), __fadd_rn(p.z, 0.0f), p.w);
       out_vel[out] = v;
@@ -1019,8 +1029,9 @@ bool prepare3(World3* w) {
   if (w->error != PHIENG_SPH_OK) return false;
   if (!ensure_device3(w)) return false;
   if (!w->dev_valid) {
-    // adaptive resolution may split up to MAX_PARTICLES_3D particles
-    if (!ensure_capacity3(w, w->cfg.adaptive_resolution ? std::max(w->n, kMaxParticles3D) : w->n)) return false;
+    // adaptive resolution: room for what a resample pass can output
+    if (!ensure_capacity3(w, w->cfg.adaptive_resolution ? std::max(resample_bound3(w->n), kMaxParticles3D) : w->n))
+      return false;
     if (!w->plan_valid) plan_grid3(w);
     if (w->n && (!ok3(w, cudaMemcpyAsync(w->pos, w->h_pos.data(), sizeof(float4) * w->n, cudaMemcpyHostToDevice,
                                          w->stream)) ||
@@ -1416,6 +1427,13 @@ void recompute_uniformity3(World3* w);
 // one: sort and density, resample (one thread), one read of the new count,
 // then the new set's keys and the whole substep body.
 bool run_substep3_adaptive(World3* w, float dt) {
+  if (w->dcap < resample_bound3(w->n)) {
+    // an earlier CFL substep of this step grew the set: bring the state home
+    // and upload it into buffers with room for this pass's output
+    if (!ensure_host3(w)) return false;
+    w->dev_valid = false;
+    if (!prepare3(w)) return false;
+  }
   const uint32_t c = w->dcap;
   if (w->rs_cap < c || !w->rs_pos) {
     cudaStreamSynchronize(w->stream);
@@ -1441,7 +1459,7 @@ bool run_substep3_adaptive(World3* w, float dt) {
     k_resample3<<<1, 1, 0, st>>>(w->n, w->pos, w->vel, w->mass, w->phase, w->sdq, w->sid, w->skey, w->rs_slot,
                                  w->start, P, cf.merge_density_ratio * rest, cf.split_density_ratio * rest,
                                  std::max(cf.particle_mass, kEps) * 0.125f, w->rs_absorbed, w->rs_pos, w->rs_vel,
-                                 w->rs_mass, w->rs_phase, n_out);
+                                 w->rs_mass, w->rs_phase, c, n_out);
   } else {
     cudaMemsetAsync(n_out, 0, 4, st);
   }
@@ -1481,7 +1499,7 @@ bool run_substep3_adaptive(World3* w, float dt) {
 
 bool world_step3(World3* w, float dt) {
   if (w->cfg.enabled && w->n > 0 && dt > 0.0f) {
-    if (w->cfg.adaptive_resolution && w->pos && w->dcap < std::max(w->n, kMaxParticles3D)) {
+    if (w->cfg.adaptive_resolution && w->pos && w->dcap < std::max(resample_bound3(w->n), kMaxParticles3D)) {
       if (!ensure_host3(w)) return false;  // room for the splits: re-upload into larger buffers
       w->dev_valid = false;
     }

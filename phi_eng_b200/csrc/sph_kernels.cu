@@ -987,7 +987,22 @@ __global__ void __launch_bounds__(256) k_front_metrics(const float4* __restrict_
   }
 }
 
+#include "sph_fast.cuh"
+
 inline uint32_t cdiv(uint32_t a, uint32_t b) { return (a + b - 1) / b; }
+
+// The launch's flags for which the force pass compiles out the optional pair
+// terms: XSPH on, artificial viscosity and cohesion off, h*h <= hk*hk (a
+// batch's launch parameters carry the union of its scenes' flags).
+inline bool plain_flags(uint32_t f) {
+  return (f & F_VISC) && !(f & (F_AV | F_COHESION | F_WIDE_NB | F_TURB | F_GHOST | F_POLY));
+}
+
+// Tolerance-mode passes apply: requested, the plain flag set, uniform mass
+// and phase, a single world.
+inline bool fast_flags(uint32_t f, bool batch) {
+  return (f & F_FAST) && plain_flags(f) && !(f & (F_MASS | F_PHASE)) && !batch;
+}
 
 }  // namespace
 
@@ -1062,7 +1077,7 @@ __global__ void k_resample(uint32_t n, float4* __restrict__ state, float* __rest
                            const uint32_t* __restrict__ slot_of, const uint32_t* __restrict__ start, StepParams P,
                            float merge_hi, float split_lo, float min_mass, uint8_t* __restrict__ absorbed,
                            float4* __restrict__ out_state, float* __restrict__ out_mass, uint8_t* __restrict__ out_phase,
-                           uint32_t* __restrict__ n_out) {
+                           uint32_t out_cap, uint32_t* __restrict__ n_out) {
   if (blockIdx.x != 0 || threadIdx.x != 0) return;
   const float h = P.hk;
   const float md = __fmul_rn(0.25f, h);
@@ -1100,7 +1115,12 @@ __global__ void k_resample(uint32_t n, float4* __restrict__ state, float* __rest
     if (absorbed[i]) continue;
     const float4 p = state[i];
     const float m = mass[i];
-    if (sdq[slot_of[i]].x < split_lo && m > min_mass && out + 1 < 4096u) {  // MAX_PARTICLES_2D (fluid.rs:30)
+    const bool split = sdq[slot_of[i]].x < split_lo && m > min_mass && out + 1 < 4096u;  // MAX_PARTICLES_2D (fluid.rs:30)
+    if (out + (split ? 2u : 1u) > out_cap) {  // never with buffers sized for the bound: report, write nothing past
+      *n_out = out_cap + 1u;
+      return;
+    }
+    if (split) {
       const float half = __fmul_rn(m, 0.5f);
       out_state[out] = make_float4(__fadd_rn(p.x, off), __fadd_rn(p.y, 0.0f), p.z, p.w);
       out_mass[out] = half;
@@ -1134,7 +1154,7 @@ void enqueue_resample(const FluidBufs& b, uint32_t n, const StepParams& P, const
   k_resample_prep<<<cdiv(n, 256), 256, 0, st>>>(b.sid, n, r.slot_of, b.mass, b.phase, mass_uniform ? 1 : 0, P.mass,
                                                  phase_uniform ? 1 : 0, (uint8_t)P.uniform_phase);
   k_resample<<<1, 1, 0, st>>>(n, b.state, b.mass, b.phase, b.sdq, b.sid, b.skey, r.slot_of, b.start, P, merge_hi,
-                              split_lo, min_mass, r.absorbed, r.state, r.mass, r.phase, r.n_out);
+                              split_lo, min_mass, r.absorbed, r.state, r.mass, r.phase, r.cap, r.n_out);
 }
 
 void enqueue_ghost_density(const FluidBufs& b, const StepParams& P, cudaStream_t st) {
@@ -1147,6 +1167,14 @@ void enqueue_density(const FluidBufs& b, uint32_t n, const StepParams& P, cudaSt
   const bool m = (P.flags & F_MASS) != 0, ph = (P.flags & F_PHASE) != 0, bat = b.batch.ptab != nullptr;
   const bool wide = (P.flags & F_WIDE_NB) != 0;  // h <= 0, which only a snapshot can carry
   const uint32_t bs = b.block_density, g = cdiv(n, bs);
+  if (svp == nullptr && fast_flags(P.flags, bat)) {
+    if (b.stage & 1u)
+      k_density_fast<true><<<g, bs, 3 * fast_stage_cap(bs) * sizeof(float2), st>>>(b.spos, b.skey, n, b.start, P,
+                                                                                    b.sdq, b.spres, b.nmask);
+    else
+      k_density_fast<false><<<g, bs, 0, st>>>(b.spos, b.skey, n, b.start, P, b.sdq, b.spres, b.nmask);
+    return;
+  }
 #define PHIENG_DENSITY(M, PH, BT, WD)                                                                          \
   k_density<M, PH, BT, WD><<<g, bs, 0, st>>>(b.spos, b.skey, b.smass, b.sphase, n, b.start, P, b.batch, b.sdq, \
                                              b.spres, b.nmask, svp)
@@ -1172,18 +1200,27 @@ void enqueue_density(const FluidBufs& b, uint32_t n, const StepParams& P, cudaSt
 #undef PHIENG_DENSITY
 }
 
-// The launch's flags for which the force pass compiles out the optional pair
-// terms: XSPH on, artificial viscosity and cohesion off, h*h <= hk*hk (a
-// batch's launch parameters carry the union of its scenes' flags).
-inline bool plain_flags(uint32_t f) {
-  return (f & F_VISC) && !(f & (F_AV | F_COHESION | F_WIDE_NB | F_TURB | F_GHOST | F_POLY));
-}
-
 void enqueue_force_integrate(const FluidBufs& b, uint32_t n, const StepParams& P, float2* dbg_force,
                              cudaStream_t st) {
   if (n == 0) return;
   const bool m = (P.flags & F_MASS) != 0, bat = b.batch.ptab != nullptr, plain = plain_flags(P.flags);
   const uint32_t bs = b.block_force, g = cdiv(n, bs);
+  if (fast_flags(P.flags, bat)) {
+    const size_t sm = 9 * fast_stage_cap(bs) * sizeof(float2);
+#define PHIENG_FORCE_FAST(STG, D)                                                                               \
+  k_force_fast<STG, D><<<g, bs, STG ? sm : 0, st>>>(b.spos, b.svel, b.sdq, b.skey, b.sid, n, b.start, P, b.bodies, \
+                                                    b.nmask, b.state, b.key, b.count, dbg_force, b.defer, b.dcount)
+    const bool stg = (b.stage & 2u) != 0;
+    if (dbg_force) {
+      if (stg) PHIENG_FORCE_FAST(true, true);
+      else PHIENG_FORCE_FAST(false, true);
+    } else {
+      if (stg) PHIENG_FORCE_FAST(true, false);
+      else PHIENG_FORCE_FAST(false, false);
+    }
+#undef PHIENG_FORCE_FAST
+    return;
+  }
 #define PHIENG_FORCE(M, D, BT, PL)                                                                                  \
   k_force_integrate<M, D, BT, PL><<<g, bs, 0, st>>>(b.spos, b.svel, b.sdq, b.skey, b.sid, b.smass, n, b.start, P, \
                                                     b.batch, b.bodies, b.nmask, b.state, b.key, b.count, dbg_force, \

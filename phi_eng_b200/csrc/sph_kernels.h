@@ -59,6 +59,9 @@ struct FluidBufs {
   // launch shapes (autotuned; results do not depend on them)
   uint32_t block_density = 256;  // threads per block of K5: 64, 128 or 256
   uint32_t block_force = 256;    // threads per block of K6: 64, 128 or 256
+  // tolerance-mode passes: bit 0 = K5 stages its neighbour rows in shared
+  // memory, bit 1 = K6 does (results do not depend on it)
+  uint32_t stage = 3;
 };
 
 // Scan tile of the bucket counts; count arrays are padded to a multiple.
@@ -95,13 +98,15 @@ struct BucketSort {
 void enqueue_bucket_place(const BucketSort& bs, uint32_t n, uint32_t m, bool by_slot, cudaStream_t st);
 
 // Adaptive resolution scratch: inverse sort permutation, merge flags, the
-// resampled particles (capacity >= max(n, 4096)) and their count.
+// resampled particles (cap rows; a pass over n particles writes at most
+// n + min(n, 2048)) and their count (cap + 1 if the output would not fit).
 struct ResampleBufs {
   uint32_t* slot_of = nullptr;
   uint8_t* absorbed = nullptr;
   float4* state = nullptr;
   float* mass = nullptr;
   uint8_t* phase = nullptr;
+  uint32_t cap = 0;
   uint32_t* n_out = nullptr;
 };
 

@@ -19,7 +19,11 @@
 //
 // The first call on a device looks up the array's device address with
 // cudaGetSymbolAddress (which can trigger module loading); make that first
-// call before any stream capture.
+// call before any stream capture. The address is cached per device for the
+// life of the process, so a cudaDeviceReset (which unloads the module) needs
+// a process restart before the next call. Each call blocks once on the
+// bounding-box read-back that sizes the bucket grid; every particle is
+// phase 0.
 #include <cmath>
 #include <cstdio>
 #include <cstring>

@@ -26,6 +26,13 @@ using namespace phieng;
 namespace {
 using namespace phieng::host;
 constexpr uint32_t kMaxParticles2D = 4096;  // MAX_PARTICLES_2D (fluid.rs:30)
+
+// Most particles one resample pass (fluid.rs:826-893) can leave from n: every
+// particle is kept or split in two, and a split only happens while the output
+// holds fewer than MAX_PARTICLES_2D - 1 particles, so at most
+// MAX_PARTICLES_2D / 2 particles split. The output is a Vec in the reference
+// and has no cap of its own.
+inline uint32_t resample_bound(uint32_t n) { return n + std::min(n, kMaxParticles2D / 2); }
 constexpr uint32_t kClockWord = 16;         // scalar word holding the step's world clock (turbulence)
 
 // AmbientConfig2::default (ambient.rs): springs, drag and turbulence off, air
@@ -148,6 +155,8 @@ struct World2 {
 
   // launch tuning (phieng_sph_set_tuning)
   float buckets_per_particle = 2.0f;
+  // arithmetic of the plain density / force passes (phieng_sph_set_precision)
+  uint32_t precision = PHIENG_SPH_EXACT;
 };
 
 namespace {
@@ -473,8 +482,9 @@ bool prepare(World2* w) {
   if (w->error != PHIENG_SPH_OK) return false;
   if (!ensure_device(w)) return false;
   if (!w->dev_state_valid) {
-    // adaptive resolution may split up to MAX_PARTICLES_2D particles
-    if (!ensure_capacity(w, w->cfg.adaptive_resolution ? std::max(w->n, kMaxParticles2D) : w->n)) return false;
+    // adaptive resolution: room for what a resample pass can output
+    if (!ensure_capacity(w, w->cfg.adaptive_resolution ? std::max(resample_bound(w->n), kMaxParticles2D) : w->n))
+      return false;
     if (!w->plan_valid) plan_grid(w);
     if (w->n && !cuda_ok(w, cudaMemcpyAsync(w->d.state, w->h_state.data(), sizeof(float4) * w->n,
                                             cudaMemcpyHostToDevice, w->stream),
@@ -596,6 +606,7 @@ StepParams make_params(const World2* w, float dt) {
                                    w->phase_value, w->plan, 0, (uint32_t)w->bodies.size(), dt);
     apply_ambient(w, P);
     apply_ghosts(w, P);
+    if (w->precision == PHIENG_SPH_TOLERANCE) P.flags |= F_FAST;
     return P;
   }
   // batch: the kernels read each scene's row of the device table; the launch
@@ -922,11 +933,19 @@ bool ensure_resample_buffers(World2* w) {
       !dalloc(w, r.phase, c))
     return false;
   r.n_out = w->d.scalar + 18;
+  r.cap = c;
   w->rs_cap = c;
   return true;
 }
 
 bool run_substep_adaptive(World2* w, float dt) {
+  if (w->d.cap < resample_bound(w->n)) {
+    // an earlier CFL substep of this step grew the set: bring the state home
+    // and upload it into buffers with room for this pass's output
+    if (!ensure_host_state(w)) return false;
+    w->dev_state_valid = false;
+    if (!prepare(w)) return false;
+  }
   if (!ensure_resample_buffers(w)) return false;
   cudaStream_t st = w->stream;
   StepParams P = make_params(w, dt);
@@ -942,8 +961,8 @@ bool run_substep_adaptive(World2* w, float dt) {
     return false;
   uint32_t n2;
   std::memcpy(&n2, w->h_pinned, 4);
-  if (n2 > w->d.cap) {
-    set_error(w, PHIENG_SPH_E_CUDA, "resample count");
+  if (n2 > w->d.cap) {  // the kernel stopped at the buffer's end (cannot happen with resample_bound)
+    set_error(w, PHIENG_SPH_E_CUDA, "resample output exceeds the particle buffers");
     return false;
   }
   w->h_state.resize(n2);
@@ -997,7 +1016,7 @@ bool world_step(World2* w, float dt) {
   }
   if (w->cfg.enabled && w->n > 0 && dt > 0.0f) {  // step_fluid guards (fluid.rs:550-552)
     if (unsupported(w, true, true)) return false;
-    if (w->cfg.adaptive_resolution && w->d.state && w->d.cap < std::max(w->n, kMaxParticles2D)) {
+    if (w->cfg.adaptive_resolution && w->d.state && w->d.cap < std::max(resample_bound(w->n), kMaxParticles2D)) {
       // room for the splits: bring the state home and upload it into larger buffers
       if (!ensure_host_state(w)) return false;
       w->dev_state_valid = false;
@@ -1939,12 +1958,13 @@ int32_t phieng_sph_set_tuning(World2* w, const PhiengSphTuning* t) {
   if (!w || !t) return 0;
   auto ok_block = [](uint32_t b) { return b == 64 || b == 128 || b == 256; };
   if (!ok_block(t->density_block) || !ok_block(t->force_block) || !(t->buckets_per_particle >= 0.125f) ||
-      !(t->buckets_per_particle <= 16.0f))
+      !(t->buckets_per_particle <= 16.0f) || t->stage > 3u)
     return 0;
   if (w->device >= 0) cudaStreamSynchronize(w->stream);
   release_graph(w);
   w->d.block_density = t->density_block;
   w->d.block_force = t->force_block;
+  w->d.stage = t->stage;
   if (w->buckets_per_particle != t->buckets_per_particle) {
     w->buckets_per_particle = t->buckets_per_particle;
     if (!w->plan_locked) {
@@ -1960,9 +1980,20 @@ int32_t phieng_sph_get_tuning(const World2* w, PhiengSphTuning* t) {
   t->density_block = w->d.block_density;
   t->force_block = w->d.block_force;
   t->buckets_per_particle = w->buckets_per_particle;
-  t->reserved = 0;
+  t->stage = w->d.stage;
   return 1;
 }
+
+int32_t phieng_sph_set_precision(World2* w, uint32_t mode) {
+  if (!w || (mode != PHIENG_SPH_EXACT && mode != PHIENG_SPH_TOLERANCE)) return 0;
+  if (mode == w->precision) return 1;
+  if (w->device >= 0) cudaStreamSynchronize(w->stream);
+  release_graph(w);
+  w->precision = mode;
+  return 1;
+}
+
+uint32_t phieng_sph_get_precision(const World2* w) { return w ? w->precision : PHIENG_SPH_EXACT; }
 
 int32_t phieng_sph_load_state_device(World2* w, const float* src, uint32_t n) {
   if (!w || w->is_batch() || (n && !src) || n > w->cap) return 0;

@@ -17,8 +17,7 @@ Rank r owns the particles whose cell column cx = floor(x / h) lies in
 
 With CFL substeps enabled the substep count comes from the global maximum
 speed (one all-reduce), as the single-domain step computes it. Results are
-bit-identical to the single-domain step; tests/test_slab.py checks that on
-the CPU with gloo ranks and the oracle as the engine.
+bit-identical to the single-domain step.
 
 Communication is neighbour point-to-point (torch.distributed isend / irecv:
 NCCL over NVLink for CUDA tensors, gloo for CPU tensors): first the counts,
@@ -80,36 +79,11 @@ def cfl_count(cfg, dt: float, vmax: float) -> int:
     return int(max(1, min(float(q), mx)))
 
 
-class OracleEngine:
-    """CPU engine: the oracle in Jacobi order (what the GPU computes)."""
-
-    def __init__(self, scene):
-        self.scene = scene
-
-    def step(self, state, dt: float):
-        import torch
-
-        from oracle import oracle as orc
-
-        sc = self.scene
-        o = orc.OracleWorld(cap=max(state.shape[0], 1))
-        o.set_gravity(*sc.gravity)
-        for (px, py, hx, hy) in sc.boxes:
-            o.add_box(px, py, hx, hy, (1.0, 0.0, -0.0, 1.0))
-        for (px, py, r) in sc.circles:
-            o.add_circle(px, py, r, (1.0, 0.0, -0.0, 1.0))
-        o.set_config(_no_cfl(sc.config))
-        st = state.numpy()
-        if st.shape[0]:
-            o.add_particles(np.ascontiguousarray(st[:, :2]))
-            o.set_state(st)
-            o.step(dt, orc.JACOBI)
-        return torch.from_numpy(o.state().reshape(-1, 4).copy())
-
-
 class GpuEngine:
-    """GPU engine: one library world whose particle set is replaced from
-    device memory each substep."""
+    """The rank's engine: one library world whose particle set is replaced
+    from device memory each substep. `state` may live on the host (gloo
+    exchange) or on the GPU (NCCL exchange); the result comes back on the
+    same device."""
 
     def __init__(self, scene, cap: int):
         from .world import world_from_scene
@@ -126,16 +100,18 @@ class GpuEngine:
 
         from .closure import torch_stream_handle
 
-        n = state.shape[0]
+        home = state.device
+        dev = state if state.is_cuda else state.to("cuda")
+        n = dev.shape[0]
         w = self.world
         w.set_stream(torch_stream_handle())  # ordered after the torch ops that built `state`
-        w.load_state_device(state.data_ptr(), n)
+        w.load_state_device(dev.data_ptr(), n)
         w.step(dt)
-        out = torch.empty_like(state)
+        out = torch.empty_like(dev)
         if n:
             w.get_state_device(out.data_ptr(), n)
         w.sync()
-        return out
+        return out if home == out.device else out.to(home)
 
 
 def _empty_scene(scene):
@@ -190,7 +166,7 @@ class SlabRun:
         st[:, :2] = xy[ids]
         self.ids = ids.to(device)
         self.state = st.to(device)
-        self.engine = engine if engine is not None else OracleEngine(scene)
+        self.engine = engine if engine is not None else GpuEngine(scene, cap=max(scene.n, 1))
         self.comm_bytes = 0
 
     # ---- neighbour exchange ----

@@ -245,6 +245,16 @@ class World2:
             self.check()
             raise SphError("phieng_sph_reserve failed")
 
+    @property
+    def precision(self) -> int:
+        """_abi.EXACT (default) or _abi.TOLERANCE (phieng_sph_set_precision)."""
+        return int(self._lib.phieng_sph_get_precision(self._h))
+
+    @precision.setter
+    def precision(self, mode: int) -> None:
+        if self._lib.phieng_sph_set_precision(self._h, int(mode)) != 1:
+            raise ValueError(f"unknown precision mode {mode}")
+
     def step_n(self, dt: float, n: int) -> None:
         if self._lib.phieng_sph_step_n(self._h, dt, n) != 1:
             self.check()

@@ -83,3 +83,50 @@ def test_adaptive_bit_exact(cfg_name):
         assert bad.size == 0, f"step {15 * (k + 1)}: {bad.size} words differ, first particle {bad[0] // 4}"
         assert np.array_equal(masses(g).view(np.uint32), masses(o).view(np.uint32))
     assert counts != {n0}  # the resampling changed the particle count
+
+
+def _sparse_points(n, spacing, x0=0.0, y0=0.5):
+    """n isolated particles on a row-major grid `spacing` apart (> h, so each
+    one's density is its own kernel weight: under split_density_ratio)."""
+    nx = int(np.ceil(np.sqrt(n)))
+    i = np.arange(n)
+    return np.stack([x0 + (i % nx) * spacing, y0 + (i // nx) * spacing], axis=1).astype(np.float32)
+
+
+def test_oracle_split_output_exceeds_the_add_cap():
+    """More than MAX_PARTICLES_2D / 2 under-dense particles: the first 2048
+    split (the output reaches 4096), the rest are kept, so one pass leaves
+    n + 2048 particles, beyond the 4096 cap of add_particles (the reference's
+    output is a Vec with no cap of its own, fluid.rs:873-889)."""
+    s = sims.OracleSim(orc.JACOBI)
+    c = sims.default_cfg()
+    c.adaptive_resolution = 1
+    s.config = c
+    s.set_gravity(0.0, 0.0)
+    assert s.add_particles(_sparse_points(3000, 2.0)) == 3000
+    s.step(1 / 60)
+    assert s.count == 3000 + 2048
+
+
+@pytest.mark.gpu
+def test_adaptive_split_beyond_cap_bit_exact():
+    """The same pass on the GPU: the world's buffers hold the n + 2048 output
+    (no write past them), and counts, states and masses equal the oracle's
+    over further steps in which the grown set resamples again."""
+    c = sims.default_cfg()
+    c.adaptive_resolution = 1
+    pts = _sparse_points(3000, 2.0)
+    g, o = sims.GpuSim(), sims.OracleSim(orc.JACOBI)
+    for s in (g, o):
+        s.set_gravity(0.0, -9.81)
+        s.config = c
+        assert s.add_particles(pts) == 3000
+    for k in range(4):
+        g.step(1 / 60)
+        o.step(1 / 60)
+        assert g.count == o.count, f"step {k + 1}: counts {g.count} vs {o.count}"
+        a, b = g.state(), o.state()
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), f"step {k + 1}: states differ"
+        assert np.array_equal(masses(g).view(np.uint32), masses(o).view(np.uint32))
+    assert o.count > 5000
+    assert g.w.status().error == 0

@@ -23,8 +23,8 @@ def test_tuning_validation_and_roundtrip():
         t = _abi.PhiengSphTuning(bad[0], bad[1], bad[2], 0)
         assert lib.phieng_sph_set_tuning(w._h, C.byref(t)) == 0
     assert autotune.current(w) == autotune.DEFAULT
-    autotune.apply(w, dict(density_block=128, force_block=64, buckets_per_particle=0.5))
-    assert autotune.current(w) == dict(density_block=128, force_block=64, buckets_per_particle=0.5)
+    autotune.apply(w, dict(density_block=128, force_block=64, buckets_per_particle=0.5, stage=1))
+    assert autotune.current(w) == dict(density_block=128, force_block=64, buckets_per_particle=0.5, stage=1)
     assert lib.phieng_sph_set_tuning(None, None) == 0
     w.close()
 

@@ -153,3 +153,33 @@ def test_batch_rejects_bad_input():
     w.fluid.config = c
     with pytest.raises(ValueError):
         batch.Batch([w])
+
+
+def workload_slice():
+    """32 scenes of the 512-scene workload generator itself: its 8 largest
+    (32,768-particle end of the log-uniform range) and 24 spread over the rest
+    by index."""
+    scs = batch.batched_scenes(512)
+    by_size = sorted(range(len(scs)), key=lambda i: (-scs[i].n, i))
+    largest = by_size[:8]
+    rest = [i for i in range(0, 512, 21) if i not in largest][:24]
+    idx = sorted(largest + rest)
+    return [scs[i] for i in idx]
+
+
+def test_workload_slice_covers_the_range():
+    scs = workload_slice()
+    n = [sc.n for sc in scs]
+    assert len(scs) == 32
+    assert max(n) >= 32000 and min(n) < 2048
+
+
+@pytest.mark.gpu
+def test_batch_workload_slice_matches_oracle():
+    """The slice advanced together in one batch for 20 steps: every scene bit
+    for bit equal to the oracle's Jacobi step of that scene alone."""
+    scs = workload_slice()
+    got = batch.gpu_stepper(scs, 20)
+    want = oracle_stepper(scs, 20)
+    for k in range(len(scs)):
+        assert np.array_equal(got[k].view(np.uint32), want[k].view(np.uint32)), (k, scs[k].n)

@@ -753,3 +753,24 @@ def test_adaptive3_bit_exact():
             assert_bit_equal(w.fluid.particles, o.state(), f"state after {k + 1} steps")
             assert np.array_equal(gpu_masses3(w).view(np.uint32), o.masses().view(np.uint32))
     assert o.count != n0
+
+
+@pytest.mark.gpu
+def test_adaptive3_split_beyond_cap_bit_exact():
+    """More than MAX_PARTICLES_3D / 2 isolated (under-dense) particles: one
+    pass leaves n + 2048 of them, more than the add cap; the GPU's buffers
+    hold them and counts, states and masses equal the oracle's."""
+    c = default_config()
+    c.adaptive_resolution = 1
+    c.split_density_ratio = 2.5  # an isolated particle's own kernel weight is below it
+    side = 15  # 3375 particles, 4 h apart
+    pts = lattice((0.0, 0.0, 0.0), side, side, side, 2.0)
+    o = make_oracle(pts, bodies=(), cfg=c)
+    w = make_gpu(pts, bodies=(), cfg=c)
+    for k in range(3):
+        o.step(1 / 60, JACOBI)
+        w.step(1 / 60)
+        assert len(w.fluid) == o.count, f"step {k + 1}: counts {len(w.fluid)} vs {o.count}"
+        assert_bit_equal(w.fluid.particles, o.state(), f"state after {k + 1} steps")
+        assert np.array_equal(gpu_masses3(w).view(np.uint32), o.masses().view(np.uint32))
+    assert o.count > 5000

@@ -1,7 +1,9 @@
 """phieng_sph_density_noalloc: the density pass for callers that may not
 allocate GPU memory (e.g. a game engine's simulation thread, where cudaMalloc
 can stall the frame). It must give the same density and pressure as the
-world's own density pass, on repeated calls that reuse its fixed scratch.
+world's own density pass and as the oracle's, on repeated calls that reuse
+its fixed scratch, also when the particles lie so far apart that its bucket
+grid is clamped to 2^16 buckets and distant cells share buckets.
 
 This file is collected last so that a run stopping at the first failure has
 already run every other test.
@@ -11,10 +13,33 @@ import ctypes as C
 import numpy as np
 import pytest
 
+import sims
+from oracle import oracle as orc
 from phi_eng_b200 import _abi, scenes
 from phi_eng_b200.world import world_from_scene
 
 pytestmark = pytest.mark.gpu
+
+
+def two_clusters():
+    """Two 64 x 64 blocks of the 4k dam break's lattice, one shifted by
+    (1500 h, 900 h): the cell bounding box needs 2^11 x 2^10 buckets, more
+    than the scratch's 2^16, so the grid is clamped and cells 2^8 apart
+    share a bucket."""
+    sc = scenes.dam_break_4k()
+    h = float(sc.config.smoothing_length)
+    far = sc.xy + np.array([1500 * h, 900 * h], np.float32)
+    sc.xy = np.concatenate([sc.xy, far]).astype(np.float32)
+    sc.boxes = []
+    return sc
+
+
+def oracle_density(sc):
+    o = sims.OracleSim(orc.JACOBI)
+    o.config = sc.config
+    assert o.add_particles(sc.xy) == sc.n
+    o.w.pass_density()
+    return o.density_pressure()
 
 
 def rel_rms(a, b):
@@ -23,7 +48,7 @@ def rel_rms(a, b):
     return float(np.sqrt(((a - b) ** 2).mean()) / max(np.sqrt((b ** 2).mean()), 1e-30))
 
 
-@pytest.mark.parametrize("make", [scenes.dam_break_4k, lambda: scenes.dam_break_scaled(256, 256)])
+@pytest.mark.parametrize("make", [scenes.dam_break_4k, lambda: scenes.dam_break_scaled(256, 256), two_clusters])
 def test_noalloc_density_matches_world_twice(make):
     import torch
 
@@ -34,6 +59,9 @@ def test_noalloc_density_matches_world_twice(make):
     w.debug_forces()
     d_ref, p_ref = w.fluid.density_pressure()
     w.close()
+    # and the oracle's density pass (the reference's arithmetic)
+    d_o, p_o = oracle_density(sc)
+    assert np.array_equal(d_ref, d_o) and np.array_equal(p_ref, p_o)
 
     lib = _abi.load()
     xy = torch.from_numpy(np.ascontiguousarray(sc.xy)).cuda()
