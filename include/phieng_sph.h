@@ -404,6 +404,17 @@ int32_t phieng_mlp_set_params(PhiengMlp* mlp, const float* params, const float* 
 uint32_t phieng_mlp_step_count(PhiengMlp* mlp);
 /* y[n][2] = network(x[n][16]) (device pointers), asynchronous. */
 int32_t phieng_mlp_forward(PhiengMlp* mlp, const float* x, uint32_t n, float* y);
+/* The same forward pass on the 5th-generation tensor cores (tcgen05.mma
+ * with TMEM accumulators, 128 particles per CTA), same layer numerics:
+ * results agree with phieng_mlp_forward within the network's tolerance,
+ * not bit for bit (the tensor core's accumulation order differs).
+ * Asynchronous; its waits for the tensor core are bounded, and one that
+ * runs out is reported by phieng_mlp_check_waits. */
+int32_t phieng_mlp_forward_tc(PhiengMlp* mlp, const float* x, uint32_t n, float* y);
+/* Synchronise the network's stream; 1 if no bounded wait of a tcgen05 kernel
+ * ran out since creation, else 0 (and the network reports
+ * PHIENG_SPH_E_CUDA). */
+int32_t phieng_mlp_check_waits(PhiengMlp* mlp);
 /* Loss and gradient (host buffers, PHIENG_MLP_PARAMS values) of the minibatch
  * that training step `iter` with `seed` would draw from the npairs pairs
  * (x[npairs][16], t[npairs][2], device); batch a multiple of 128. */

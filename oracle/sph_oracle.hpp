@@ -9,7 +9,7 @@
 // Parity status: the reference's Rust step cannot be compiled in this
 // environment (no cargo/rustc) and its own tests pin no numeric results of
 // the SPH step, so this restatement is pinned by (a) the reference's
-// behavioural tests re-run on it (tests/test_oracle.py), (b) the one
+// behavioural tests re-run on it (tests/test_behaviour.py), (b) the one
 // bit-pinned arithmetic identity of the reference (linear EOS,
 // fluid.rs:1326-1329), and (c) an FP64 twin that bounds its f32 error.
 //

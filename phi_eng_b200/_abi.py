@@ -348,6 +348,8 @@ SIGNATURES = {
     "phieng_mlp_set_params": (C.c_int32, [_P, _F, _F]),
     "phieng_mlp_step_count": (C.c_uint32, [_P]),
     "phieng_mlp_forward": (C.c_int32, [_P, _P, C.c_uint32, _P]),
+    "phieng_mlp_forward_tc": (C.c_int32, [_P, _P, C.c_uint32, _P]),
+    "phieng_mlp_check_waits": (C.c_int32, [_P]),
     "phieng_mlp_grad": (C.c_int32, [_P, _P, _P, C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint32, _F, _F]),
     "phieng_mlp_train": (C.c_int32, [_P, _P, _P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_float, C.c_uint64, _F]),
     "phieng_mlp_sample_indices": (C.c_int32, [C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint32, _P, _P]),

@@ -122,6 +122,19 @@ class Mlp:
             self.check()
         return y
 
+    def forward_tc(self, x):
+        """forward() on the tcgen05 tensor cores (TMEM accumulators)."""
+        torch = self._on_current_stream()
+        x = x.contiguous()
+        y = torch.empty((x.shape[0], 2), dtype=torch.float32, device=x.device)
+        if self._lib.phieng_mlp_forward_tc(self._h, x.data_ptr(), x.shape[0], y.data_ptr()) != 1:
+            self.check()
+        return y
+
+    def check_waits(self) -> bool:
+        """True if no bounded tensor-core wait ran out (synchronises)."""
+        return self._lib.phieng_mlp_check_waits(self._h) == 1
+
     def grad(self, x, t, batch: int, seed: int, it: int):
         self._on_current_stream()
         g = np.zeros(NPARAMS, np.float32)

@@ -2,9 +2,9 @@
 // sph_kernels.cu inside its anonymous namespace: they use its neighbour walk
 // (for_each_candidate) and integrate (integrate_write).
 //
-// Scope: the plain flag set of a single world (uniform mass and phase, XSPH
-// on, no artificial viscosity, cohesion, turbulence, ghosts or polygons,
-// h > 0). The neighbour sets, the sort order and the per-particle visit order
+// Scope: the plain flag set (uniform mass and phase, XSPH on, no artificial
+// viscosity, cohesion, turbulence, ghosts or polygons, h > 0) of a single
+// world or of every scene of a batch. The neighbour sets, the sort order and the per-particle visit order
 // are the exact passes': the neighbour test d2 < h*h keeps the reference's
 // rounding (fluid.rs:383), so the neighbour lists and the row masks are the
 // same bits. What changes is the arithmetic of the sums over those
@@ -130,17 +130,19 @@ __device__ __forceinline__ bool candidate_rows(uint32_t k, const uint32_t* __res
 }
 
 // ---------------------------------------------------------------- K5 (tolerance mode)
-template <bool STAGE>
+template <bool STAGE, bool BATCH>
 __global__ void __launch_bounds__(256) k_density_fast(const float2* __restrict__ spos,
                                                       const uint32_t* __restrict__ skey, uint32_t n,
-                                                      const uint32_t* __restrict__ start, StepParams P,
+                                                      const uint32_t* __restrict__ start, StepParams P0, BatchTab bt,
                                                       float2* __restrict__ sdq, float* __restrict__ spres,
                                                       uint32_t* __restrict__ nmask) {
   extern __shared__ __align__(16) float2 fast_win[];
   const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   const bool active = s < n;
+  // a batch: the particle's scene row (its own bucket range inside the shared key space)
+  const StepParams& P = scene_params<BATCH>(P0, bt.ptab, BATCH && active ? bt.sscene[s] : 0u);
   const GridPlan& g = P.grid;
-  const uint32_t k = active ? skey[s] : g.sentinel;
+  const uint32_t k = active ? skey[s] : P0.grid.sentinel;
   uint32_t lo[3], hi[3];
   const bool rows = candidate_rows(k, start, g, lo, hi);
   RowWindows win;
@@ -229,19 +231,20 @@ struct FastPair {
   }
 };
 
-template <bool STAGE, bool DEBUG>
+template <bool STAGE, bool DEBUG, bool BATCH>
 __global__ void __launch_bounds__(256) k_force_fast(
     const float2* __restrict__ spos, const float2* __restrict__ svel, const float2* __restrict__ sdq,
     const uint32_t* __restrict__ skey, const uint32_t* __restrict__ sid, uint32_t n,
-    const uint32_t* __restrict__ start, StepParams P, const DevBody* __restrict__ bodies,
+    const uint32_t* __restrict__ start, StepParams P0, BatchTab bt, const DevBody* __restrict__ bodies,
     const uint32_t* __restrict__ nmask, float4* __restrict__ state_out, uint32_t* __restrict__ key_out,
     uint32_t* __restrict__ count_out, float2* __restrict__ dbg_force, uint32_t* __restrict__ defer,
     uint32_t* __restrict__ dcount) {
   extern __shared__ __align__(16) float2 fast_win[];
   const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   const bool active = s < n;
+  const StepParams& P = scene_params<BATCH>(P0, bt.ptab, BATCH && active ? bt.sscene[s] : 0u);
   const GridPlan& g = P.grid;
-  const uint32_t k = active ? skey[s] : g.sentinel;
+  const uint32_t k = active ? skey[s] : P0.grid.sentinel;
   const uint32_t own = active ? nmask[n + s] : 0u;
   uint32_t lo[3], hi[3];
   const bool rows = candidate_rows(k, start, g, lo, hi) && own != 0u;

@@ -999,10 +999,8 @@ inline bool plain_flags(uint32_t f) {
 }
 
 // Tolerance-mode passes apply: requested, the plain flag set, uniform mass
-// and phase, a single world.
-inline bool fast_flags(uint32_t f, bool batch) {
-  return (f & F_FAST) && plain_flags(f) && !(f & (F_MASS | F_PHASE)) && !batch;
-}
+// and phase (for a batch: the union of its scenes' flags).
+inline bool fast_flags(uint32_t f) { return (f & F_FAST) && plain_flags(f) && !(f & (F_MASS | F_PHASE)); }
 
 }  // namespace
 
@@ -1167,12 +1165,19 @@ void enqueue_density(const FluidBufs& b, uint32_t n, const StepParams& P, cudaSt
   const bool m = (P.flags & F_MASS) != 0, ph = (P.flags & F_PHASE) != 0, bat = b.batch.ptab != nullptr;
   const bool wide = (P.flags & F_WIDE_NB) != 0;  // h <= 0, which only a snapshot can carry
   const uint32_t bs = b.block_density, g = cdiv(n, bs);
-  if (svp == nullptr && fast_flags(P.flags, bat)) {
-    if (b.stage & 1u)
-      k_density_fast<true><<<g, bs, 3 * fast_stage_cap(bs) * sizeof(float2), st>>>(b.spos, b.skey, n, b.start, P,
-                                                                                    b.sdq, b.spres, b.nmask);
-    else
-      k_density_fast<false><<<g, bs, 0, st>>>(b.spos, b.skey, n, b.start, P, b.sdq, b.spres, b.nmask);
+  if (svp == nullptr && fast_flags(P.flags)) {
+    const size_t sm = 3 * fast_stage_cap(bs) * sizeof(float2);
+#define PHIENG_DENSITY_FAST(STG, BT) \
+  k_density_fast<STG, BT><<<g, bs, STG ? sm : 0, st>>>(b.spos, b.skey, n, b.start, P, b.batch, b.sdq, b.spres, b.nmask)
+    const bool stg = (b.stage & 1u) != 0;
+    if (bat) {
+      if (stg) PHIENG_DENSITY_FAST(true, true);
+      else PHIENG_DENSITY_FAST(false, true);
+    } else {
+      if (stg) PHIENG_DENSITY_FAST(true, false);
+      else PHIENG_DENSITY_FAST(false, false);
+    }
+#undef PHIENG_DENSITY_FAST
     return;
   }
 #define PHIENG_DENSITY(M, PH, BT, WD)                                                                          \
@@ -1205,18 +1210,22 @@ void enqueue_force_integrate(const FluidBufs& b, uint32_t n, const StepParams& P
   if (n == 0) return;
   const bool m = (P.flags & F_MASS) != 0, bat = b.batch.ptab != nullptr, plain = plain_flags(P.flags);
   const uint32_t bs = b.block_force, g = cdiv(n, bs);
-  if (fast_flags(P.flags, bat)) {
+  if (fast_flags(P.flags)) {
     const size_t sm = 9 * fast_stage_cap(bs) * sizeof(float2);
-#define PHIENG_FORCE_FAST(STG, D)                                                                               \
-  k_force_fast<STG, D><<<g, bs, STG ? sm : 0, st>>>(b.spos, b.svel, b.sdq, b.skey, b.sid, n, b.start, P, b.bodies, \
-                                                    b.nmask, b.state, b.key, b.count, dbg_force, b.defer, b.dcount)
+#define PHIENG_FORCE_FAST(STG, D, BT)                                                                              \
+  k_force_fast<STG, D, BT><<<g, bs, STG ? sm : 0, st>>>(b.spos, b.svel, b.sdq, b.skey, b.sid, n, b.start, P, b.batch, \
+                                                        b.bodies, b.nmask, b.state, b.key, b.count, dbg_force,       \
+                                                        b.defer, b.dcount)
     const bool stg = (b.stage & 2u) != 0;
-    if (dbg_force) {
-      if (stg) PHIENG_FORCE_FAST(true, true);
-      else PHIENG_FORCE_FAST(false, true);
+    if (dbg_force) {  // single worlds only
+      if (stg) PHIENG_FORCE_FAST(true, true, false);
+      else PHIENG_FORCE_FAST(false, true, false);
+    } else if (bat) {
+      if (stg) PHIENG_FORCE_FAST(true, false, true);
+      else PHIENG_FORCE_FAST(false, false, true);
     } else {
-      if (stg) PHIENG_FORCE_FAST(true, false);
-      else PHIENG_FORCE_FAST(false, false);
+      if (stg) PHIENG_FORCE_FAST(true, false, false);
+      else PHIENG_FORCE_FAST(false, false, false);
     }
 #undef PHIENG_FORCE_FAST
     return;

@@ -619,6 +619,19 @@ StepParams make_params(const World2* w, float dt) {
     const float hg = sc.cfg.smoothing_length, hk = rmaxf(hg, kEps);
     if (!(hg * hg <= hk * hk)) P.flags |= F_WIDE_NB;
   }
+  if (w->precision == PHIENG_SPH_TOLERANCE) {
+    // the tolerance-mode kernels take a batch only if every scene has the
+    // plain flag set (XSPH on; no artificial viscosity, cohesion, per-particle
+    // mass or phase, h > 0): the launch's own flags are scene 0's
+    bool all_plain = true;
+    for (const auto& sc : w->scenes) {
+      const uint32_t f = make_params_for(sc.cfg, sc.gx, sc.gy, sc.mass_uniform, sc.mass_value, sc.phase_uniform,
+                                         sc.phase_value, sc.plan, sc.body_first, sc.nbodies, dt)
+                             .flags;
+      all_plain = all_plain && (f & F_VISC) && !(f & (F_AV | F_COHESION | F_WIDE_NB | F_MASS | F_PHASE));
+    }
+    if (all_plain) P.flags |= F_FAST;
+  }
   return P;
 }
 

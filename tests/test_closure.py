@@ -249,6 +249,36 @@ def test_mlp_forward_matches_oracle():
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("n", [128, 10000, 1 << 20])
+def test_mlp_forward_tcgen05_matches_oracle_and_mma_sync(n):
+    """The forward pass on the tcgen05 tensor cores (TMEM accumulators)
+    against the oracle's emulation of the same rounding points (the bar of
+    the mma.sync path) and against the mma.sync path itself; 1M rows cover
+    the persistent loop over many tiles, and ragged sizes the idle rows of
+    the last tile."""
+    from phi_eng_b200.closure import Mlp
+
+    torch = _torch()
+    rng = np.random.default_rng(11)
+    p, norm = _random_net(rng)
+    m = Mlp()
+    m.set(p, norm)
+    for rows in (n, n - 37 if n > 128 else 1):
+        x = rng.standard_normal((rows, 16)).astype(np.float32) * 2.0
+        xd = torch.from_numpy(x).cuda()
+        y_tc = m.forward_tc(xd).cpu().numpy()
+        assert m.check_waits()
+        y_ms = m.forward(xd).cpu().numpy()
+        k = min(rows, 20000)
+        yo, _ = mo.forward(p, norm, x[:k], emulate=True)
+        rms = np.sqrt(np.mean(yo ** 2))
+        assert np.abs(y_tc[:k] - yo).max() / rms < FWD_TOL
+        assert np.sqrt(np.mean((y_tc[:k] - yo) ** 2)) / rms < 2e-3
+        assert np.abs(y_tc - y_ms).max() / np.sqrt(np.mean(y_ms ** 2)) < FWD_TOL
+        assert np.isfinite(y_tc).all()
+
+
+@pytest.mark.gpu
 def test_mlp_gradient_matches_oracle():
     from phi_eng_b200.closure import Mlp
 

@@ -170,3 +170,25 @@ def test_full_size_step_within_tolerance():
     assert rel_rms(d_gpu, d_o) <= 1e-5
     assert rel_rms(p_gpu, p_o) <= 1e-5
     assert rel_rms(f_gpu, f_o) <= 1e-4
+
+
+@pytest.mark.gpu
+def test_batch_scenes_equal_each_world_alone():
+    """A batch in tolerance mode: every scene bit for bit equal to its world
+    stepped alone in tolerance mode (the reassociated arithmetic is per
+    particle; block and staging windows may span scenes without effect)."""
+    from phi_eng_b200 import batch
+    from phi_eng_b200.world import world_from_scene
+
+    scs = batch.batched_scenes(12, n_min=256, n_max=4096)
+    dt = scs[0].dt
+    b = batch.Batch.from_scenes(scs)
+    b.world.precision = _abi.TOLERANCE
+    b.step(dt, 40)
+    for k, sc in enumerate(scs):
+        w = world_from_scene(sc)
+        w.precision = _abi.TOLERANCE
+        w.step_n(dt, 40)
+        assert np.array_equal(b.scene_particles(k).view(np.uint32), w.fluid.particles.view(np.uint32)), k
+        w.close()
+    b.close()
