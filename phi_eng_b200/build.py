@@ -35,7 +35,8 @@ UNITS = [
     ("sph3d.cu", EXACT),
 ]
 HEADERS = ["sph_device.cuh", "sph_kernels.h", "sph_mlp.cuh", "sph_mlp_host.h", "sph_warp.cuh", "sph_host.h", "sph_snapshot.h",
-           "sph_noise.cuh", "sph_fast.cuh", "sph_tc.cuh"]
+           "sph_noise.cuh", "sph_fast.cuh", "sph_tc.cuh", "sph_tc_net.cuh",
+           "sph_closure_tc.cuh"]
 
 
 def _mtime(p: str) -> float:

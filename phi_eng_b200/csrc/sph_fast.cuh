@@ -135,7 +135,7 @@ __global__ void __launch_bounds__(256) k_density_fast(const float2* __restrict__
                                                       const uint32_t* __restrict__ skey, uint32_t n,
                                                       const uint32_t* __restrict__ start, StepParams P0, BatchTab bt,
                                                       float2* __restrict__ sdq, float* __restrict__ spres,
-                                                      uint32_t* __restrict__ nmask) {
+                                                      uint32_t* __restrict__ nmask, float2* __restrict__ svp) {
   extern __shared__ __align__(16) float2 fast_win[];
   const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   const bool active = s < n;
@@ -201,8 +201,11 @@ __global__ void __launch_bounds__(256) k_density_fast(const float2* __restrict__
   if (dens > P.rho_cap) dens = P.rho_cap;
   const float p = eos_fast(dens, P.rest[P.uniform_phase], P);
   const float rc = fmaxf(dens, kEps);
-  sdq[s] = make_float2(dens, __fdiv_rn(p, __fmul_rn(rc, rc)));
+  const float q = __fdiv_rn(p, __fmul_rn(rc, rc));
+  sdq[s] = make_float2(dens, q);
   spres[s] = p;
+  // closure passes: the per-neighbour factors of the feature sums, m / rho and p
+  if (svp) svp[s] = make_float2(__fdiv_rn(P.mass, rc), __fmul_rn(__fmul_rn(q, rc), rc));
 }
 
 // ---------------------------------------------------------------- K6 (tolerance mode)

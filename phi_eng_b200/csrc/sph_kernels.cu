@@ -20,6 +20,7 @@
 
 #include "sph_kernels.h"
 #include "sph_noise.cuh"
+#include "sph_tc_net.cuh"
 #include "sph_warp.cuh"
 
 namespace phieng {
@@ -988,6 +989,7 @@ __global__ void __launch_bounds__(256) k_front_metrics(const float4* __restrict_
 }
 
 #include "sph_fast.cuh"
+#include "sph_closure_tc.cuh"
 
 inline uint32_t cdiv(uint32_t a, uint32_t b) { return (a + b - 1) / b; }
 
@@ -1165,10 +1167,11 @@ void enqueue_density(const FluidBufs& b, uint32_t n, const StepParams& P, cudaSt
   const bool m = (P.flags & F_MASS) != 0, ph = (P.flags & F_PHASE) != 0, bat = b.batch.ptab != nullptr;
   const bool wide = (P.flags & F_WIDE_NB) != 0;  // h <= 0, which only a snapshot can carry
   const uint32_t bs = b.block_density, g = cdiv(n, bs);
-  if (svp == nullptr && fast_flags(P.flags)) {
+  if (fast_flags(P.flags)) {
     const size_t sm = 3 * fast_stage_cap(bs) * sizeof(float2);
-#define PHIENG_DENSITY_FAST(STG, BT) \
-  k_density_fast<STG, BT><<<g, bs, STG ? sm : 0, st>>>(b.spos, b.skey, n, b.start, P, b.batch, b.sdq, b.spres, b.nmask)
+#define PHIENG_DENSITY_FAST(STG, BT)                                                                           \
+  k_density_fast<STG, BT><<<g, bs, STG ? sm : 0, st>>>(b.spos, b.skey, n, b.start, P, b.batch, b.sdq, b.spres, \
+                                                       b.nmask, svp)
     const bool stg = (b.stage & 1u) != 0;
     if (bat) {
       if (stg) PHIENG_DENSITY_FAST(true, true);
@@ -1257,6 +1260,20 @@ void launch_closure(const FluidBufs& b, uint32_t n, const StepParams& P, const M
                     cudaStream_t st) {
   const bool m = (P.flags & F_MASS) != 0, ph = (P.flags & F_PHASE) != 0, bat = b.batch.ptab != nullptr;
   const bool plain = plain_flags(P.flags) && !m && !ph;
+  if (MODE == kModeClosure && fast_flags(P.flags) && io.err) {
+    // tolerance mode: fused pass with the network on the tcgen05 tensor cores
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const uint32_t blocks = min(cdiv(n, 128), (uint32_t)sms * 6u);
+#define PHIENG_CLOSURE_TC(BT)                                                                                       \
+  k_closure_tc<BT><<<blocks, 128, kNetSmem, st>>>(b.spos, b.svel, b.sdq, b.spres, b.skey, b.sid, n, b.start, P,     \
+                                                  b.batch, b.bodies, b.nmask, mlp, io, b.state, b.key, b.count, io.err)
+    if (bat) PHIENG_CLOSURE_TC(true);
+    else PHIENG_CLOSURE_TC(false);
+#undef PHIENG_CLOSURE_TC
+    return;
+  }
   const uint32_t g = cdiv(n, 256);
   const size_t sm = MODE == kModeClosure ? closure_smem_bytes() : 0;
 #define PHIENG_CLOSURE_V(M, PH, BT, PL)                                                                           \

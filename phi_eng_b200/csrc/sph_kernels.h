@@ -140,6 +140,7 @@ struct ClosureIO {
   float4* save = nullptr;
   float* rho_prev = nullptr;
   const float2* svp = nullptr;  // K5's closure factors of the current sort (required)
+  uint32_t* err = nullptr;       // sticky flag: a tensor-core wait of the tolerance-mode pass ran out
 };
 
 // Closure features of every particle for a coarse step of P.dt (after the

@@ -29,7 +29,7 @@
 #include "phieng_sph.h"
 #include "sph_mlp.cuh"
 #include "sph_mlp_host.h"
-#include "sph_tc.cuh"
+#include "sph_tc_net.cuh"
 
 namespace phieng {
 namespace {
@@ -153,111 +153,15 @@ __global__ void __launch_bounds__(128) k_mlp_forward(const float* __restrict__ x
 }
 
 // ---------------------------------------------------------------- tcgen05 forward
-// The same network on the 5th-generation tensor cores: one CTA of 128 threads
-// per tile of 128 particles (M = 128), persistent over the tiles. Operands
-// live in shared memory in the K-major no-swizzle layout of sph_tc.cuh (x_hat
-// and W1 / 2 as BF16, hidden activations and W2 / 2, W3 as FP16: the
-// numerics of the mma.sync path), accumulators in 128 TMEM columns:
-//   layer 1  D[:, 0:64)   = x_hat (W1/2)^T        1 MMA  (K = 16)
-//   layer 2  D[:, 64:128) = H1 (W2/2)^T           4 MMAs (K = 64)
-//   layer 3  D[:, 0:16)   = H2 W3pad^T            4 MMAs (N = 16, rows 2..15 of W3pad zero)
-// Thread t reads row t of each result from TMEM (warp w: lanes 32w..),
-// adds the bias, applies silu(z) = u + u tanh(u) on u = z / 2 as FP16 pairs
-// and writes row t of the next layer's operand. One thread issues the MMAs;
-// each layer's completion arrives on an mbarrier. Dynamic shared memory is
-// sized so that at most 4 CTAs share an SM: 4 x 128 TMEM columns = the SM's
-// 512, so an allocation never waits on a CTA that is not running.
-constexpr uint32_t kTcX = 0;                         // x_hat   [128][16] bf16
-constexpr uint32_t kTcA = kTcX + 128 * 16 * 2;       // H1 / H2 [128][64] fp16
-constexpr uint32_t kTcW1 = kTcA + 128 * 64 * 2;      // W1 / 2  [64][16]  bf16
-constexpr uint32_t kTcW2 = kTcW1 + 64 * 16 * 2;      // W2 / 2  [64][64]  fp16
-constexpr uint32_t kTcW3 = kTcW2 + 64 * 64 * 2;      // W3      [16][64]  fp16 (rows 2..15 zero)
-constexpr uint32_t kTcBias = kTcW3 + 16 * 64 * 2;    // b1 / 2 | b2 / 2 | b3 (f32)
-constexpr uint32_t kTcNorm = kTcBias + 4 * 256;      // mu | isd | out_scale (f32)
-constexpr uint32_t kTcBar = kTcNorm + 4 * 64;        // mbarrier
-constexpr uint32_t kTcSlot = kTcBar + 8;             // TMEM address
-constexpr uint32_t kTcUsed = kTcSlot + 8;
-constexpr uint32_t kTcSmem = 56 * 1024;  // requested: 4 x (56 + 1) KB fit the SM's 228 KB, 5 do not
-static_assert(kTcUsed <= kTcSmem, "tcgen05 forward shared memory");
-constexpr uint32_t kTcCols = 128;
-constexpr uint32_t kTcWaitLimit = 1u << 20;
-
-__global__ void __launch_bounds__(128, 4) k_mlp_forward_tc(const float* __restrict__ x, uint32_t n, MlpDev mlp,
-                                                            float* __restrict__ y, uint32_t* __restrict__ err) {
+// The same network on the 5th-generation tensor cores (sph_tc_net.cuh): one
+// CTA of 128 threads per tile of 128 rows, persistent over the tiles.
+__global__ void __launch_bounds__(128) k_mlp_forward_tc(const float* __restrict__ x, uint32_t n, MlpDev mlp,
+                                                         float* __restrict__ y, uint32_t* __restrict__ err) {
   extern __shared__ __align__(1024) unsigned char tsm[];
-  const uint32_t tid = threadIdx.x, warp = tid >> 5;
-  unsigned char* X = tsm + kTcX;
-  unsigned char* A = tsm + kTcA;
-  float* bias = reinterpret_cast<float*>(tsm + kTcBias);
-  float* norm = reinterpret_cast<float*>(tsm + kTcNorm);
-  uint64_t* bar = reinterpret_cast<uint64_t*>(tsm + kTcBar);
-  uint32_t* slot = reinterpret_cast<uint32_t*>(tsm + kTcSlot);
-  // weights from the fragment images into the UMMA layout
-  const __nv_bfloat16* img = reinterpret_cast<const __nv_bfloat16*>(mlp.frag);
-  const __half* himg = reinterpret_cast<const __half*>(mlp.frag);
-  for (uint32_t i = tid; i < 64 * 16; i += 128) {
-    const uint32_t o = i >> 4, k = i & 15;
-    *reinterpret_cast<__nv_bfloat16*>(tsm + kTcW1 + tc::kmajor_offset(o, k, 16)) = img[frag_pos(k, o, 8)];
-  }
-  for (uint32_t i = tid; i < 64 * 64; i += 128) {
-    const uint32_t o = i >> 6, k = i & 63;
-    *reinterpret_cast<__half*>(tsm + kTcW2 + tc::kmajor_offset(o, k, 64)) = himg[4 * kF1 + frag_pos(k, o, 8)];
-  }
-  for (uint32_t i = tid; i < 16 * 64; i += 128) {
-    const uint32_t o = i >> 6, k = i & 63;
-    *reinterpret_cast<__half*>(tsm + kTcW3 + tc::kmajor_offset(o, k, 64)) =
-        o < 2 ? himg[4 * (kF1 + kF2) + frag_pos(k, o, 1)] : __float2half_rn(0.0f);
-  }
-  for (uint32_t i = tid; i < kBias; i += 128) bias[i] = mlp.bias[i];
-  for (uint32_t i = tid; i < kNorm; i += 128) norm[i] = mlp.norm[i];
-  if (tid == 0) tc::mbar_init(bar, 1);
-  if (warp == 0) tc::tmem_alloc(slot, kTcCols);
-  tc::fence_async_smem();
-  tc::fence_before_sync();
-  __syncthreads();
-  tc::fence_after_sync();
-  const uint32_t tmem = *slot;
-  const uint32_t lanes = (warp * 32u) << 16;  // this warp's TMEM lanes
-  const uint64_t dX = tc::smem_desc(tc::smem_u32(X), 128, 256);
-  const uint64_t dW1 = tc::smem_desc(tc::smem_u32(tsm + kTcW1), 128, 256);
-  const uint32_t aA = tc::smem_u32(A), aW2 = tc::smem_u32(tsm + kTcW2), aW3 = tc::smem_u32(tsm + kTcW3);
-  uint32_t phase = 0;
+  TcNet net = tc_net_init(tsm, mlp);
   bool ok = true;
-  // hidden layer epilogue: TMEM columns [c0, c0 + 64) of this thread's row,
-  // plus the halved bias, through silu, as FP16 into row tid of A
-  auto hidden = [&](uint32_t c0, const float* b) {
-    float v[4][16];
-#pragma unroll
-    for (int q = 0; q < 4; q++) tc::tmem_ld16(tmem + lanes + c0 + 16 * q, v[q]);
-    tc::tmem_wait_ld();
-#pragma unroll
-    for (int q = 0; q < 4; q++) {
-      uint32_t h[8];
-#pragma unroll
-      for (int j = 0; j < 8; j++)
-        h[j] = silu_half_f16x2(__fadd_rn(v[q][2 * j], b[16 * q + 2 * j]), __fadd_rn(v[q][2 * j + 1], b[16 * q + 2 * j + 1]));
-      *reinterpret_cast<uint4*>(A + tc::kmajor_offset(tid, 16 * q, 64)) = make_uint4(h[0], h[1], h[2], h[3]);
-      *reinterpret_cast<uint4*>(A + tc::kmajor_offset(tid, 16 * q + 8, 64)) = make_uint4(h[4], h[5], h[6], h[7]);
-    }
-  };
-  // operand writes -> tensor core; one thread issues, all wait for the commit
-  auto run = [&](auto issue) -> bool {
-    tc::fence_async_smem();
-    tc::fence_before_sync();
-    __syncthreads();
-    if (tid == 0) {
-      tc::fence_after_sync();
-      issue();
-      tc::commit(bar);
-    }
-    const bool done = tc::mbar_wait(bar, phase, kTcWaitLimit);
-    if (__syncthreads_or(!done)) return false;
-    phase ^= 1u;
-    tc::fence_after_sync();
-    return true;
-  };
-  for (uint32_t base = blockIdx.x * 128u; base < n && ok; base += gridDim.x * 128u) {
-    const uint32_t i = base + tid;
+  for (uint32_t base = blockIdx.x * 128u; base < n; base += gridDim.x * 128u) {
+    const uint32_t i = base + threadIdx.x;
     float f[kFeat];
     if (i < n) {
       const float4* xi = reinterpret_cast<const float4*>(x + (size_t)i * kFeat);
@@ -271,53 +175,17 @@ __global__ void __launch_bounds__(128, 4) k_mlp_forward_tc(const float* __restri
       }
     } else {
 #pragma unroll
-      for (int q = 0; q < kFeat; q++) f[q] = norm[q];  // normalises to zero
+      for (int q = 0; q < kFeat; q++) f[q] = net.norm()[q];  // normalises to zero
     }
-    uint32_t xp[8];
-#pragma unroll
-    for (int k = 0; k < kFeat; k += 2)
-      xp[k / 2] = pack_bf16(__fmul_rn(__fsub_rn(f[k], norm[k]), norm[kFeat + k]),
-                            __fmul_rn(__fsub_rn(f[k + 1], norm[k + 1]), norm[kFeat + k + 1]));
-    *reinterpret_cast<uint4*>(X + tc::kmajor_offset(tid, 0, 16)) = make_uint4(xp[0], xp[1], xp[2], xp[3]);
-    *reinterpret_cast<uint4*>(X + tc::kmajor_offset(tid, 8, 16)) = make_uint4(xp[4], xp[5], xp[6], xp[7]);
-    ok = run([&] { tc::mma_f16(tmem, dX, dW1, tc::idesc_f16(tc::kFmtBF16, 64), 0u); });
-    if (!ok) break;
-    hidden(0, bias);
-    ok = run([&] {
-#pragma unroll
-      for (uint32_t kk = 0; kk < 4; kk++)
-        tc::mma_f16(tmem + 64, tc::smem_desc(aA + 256 * kk, 128, 1024), tc::smem_desc(aW2 + 256 * kk, 128, 1024),
-                    tc::idesc_f16(tc::kFmtF16, 64), kk);
-    });
-    if (!ok) break;
-    hidden(64, bias + kHidden);
-    ok = run([&] {
-#pragma unroll
-      for (uint32_t kk = 0; kk < 4; kk++)
-        tc::mma_f16(tmem, tc::smem_desc(aA + 256 * kk, 128, 1024), tc::smem_desc(aW3 + 256 * kk, 128, 1024),
-                    tc::idesc_f16(tc::kFmtF16, 16), kk);
-    });
-    if (!ok) break;
     float o[2];
-    tc::tmem_ld2(tmem + lanes, o);
-    tc::tmem_wait_ld();
+    ok = tc_net_forward(net, f, o);
+    if (!ok) break;
     if (i < n) {
-      y[2 * (size_t)i] = __fmul_rn(__fadd_rn(o[0], bias[2 * kHidden]), norm[2 * kFeat]);
-      y[2 * (size_t)i + 1] = __fmul_rn(__fadd_rn(o[1], bias[2 * kHidden + 1]), norm[2 * kFeat + 1]);
+      y[2 * (size_t)i] = o[0];
+      y[2 * (size_t)i + 1] = o[1];
     }
   }
-  if (!ok) {
-    // a wait ran out: report it, give the MMA in flight one more bounded
-    // wait, then release the tensor memory
-    if (tid == 0) atomicExch(err, 1u);
-    tc::mbar_wait(bar, phase, kTcWaitLimit);
-  }
-  tc::fence_before_sync();
-  __syncthreads();
-  if (warp == 0) {
-    tc::fence_after_sync();
-    tc::tmem_free(tmem, kTcCols);
-  }
+  tc_net_finish(net, ok, err);
 }
 
 __device__ __forceinline__ void store_bf16(__nv_bfloat16* p, float v) { *p = __float2bfloat16_rn(v); }
@@ -793,8 +661,7 @@ PhiengMlp* phieng_mlp_new(uint64_t seed) {
     return m;
   // ctr[2]: set by the tcgen05 forward when one of its waits ran out
   if (!mlp_ok(m, cudaMemsetAsync(m->ctr, 0, sizeof(uint32_t) * 4, m->stream))) return m;
-  if (!mlp_ok(m, cudaFuncSetAttribute(k_mlp_forward_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem)))
-    return m;
+
   if (!mlp_ok(m, cudaMallocHost(reinterpret_cast<void**>(&m->h_pinned), sizeof(float) * (kParams + kNorm + 4))))
     return m;
   if (!mlp_ok(m, cudaFuncSetAttribute(k_mlp_train_tile, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -896,8 +763,8 @@ int32_t phieng_mlp_forward_tc(PhiengMlp* m, const float* x, uint32_t n, float* y
   if (n == 0) return 1;
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, m->device);
-  const uint32_t blocks = std::min<uint32_t>(cdiv(n, 128), (uint32_t)sms * 4u);
-  k_mlp_forward_tc<<<blocks, 128, kTcSmem, m->stream>>>(x, n, phieng_mlp_dev(m), y, m->ctr + 2);
+  const uint32_t blocks = std::min<uint32_t>(cdiv(n, 128), (uint32_t)sms * 6u);
+  k_mlp_forward_tc<<<blocks, 128, kNetSmem, m->stream>>>(x, n, phieng_mlp_dev(m), y, m->ctr + 2);
   return mlp_ok(m, cudaGetLastError()) ? 1 : 0;
 }
 

@@ -186,7 +186,7 @@ bool scan_flag_ok(World2* w) {
       !cuda_ok(w, cudaStreamSynchronize(w->stream), "sync"))
     return false;
   if (w->h_pinned[8] != 0u) {
-    set_error(w, PHIENG_SPH_E_CUDA, "bucket scan wait gave up");
+    set_error(w, PHIENG_SPH_E_CUDA, "a bounded device wait gave up (bucket scan or tensor core)");
     return false;
   }
   return true;
@@ -243,7 +243,7 @@ bool ensure_device(World2* w) {
   if (!cuda_ok(w, cudaMalloc(&w->d.scalar, 128), "cudaMalloc(scalar)")) return false;
   if (!cuda_ok(w, cudaMemset(w->d.scalar, 0, 128), "cudaMemset(scalar)")) return false;
   w->d.done = w->d.scalar + 8;       // scan counters [8], [9]
-  w->d.scan_err = w->d.scalar + 12;  // set when a scan's look-back wait gave up
+  w->d.scan_err = w->d.scalar + 12;  // set when a scan's look-back wait or a tensor-core wait gave up
   if (!cuda_ok(w, cudaMallocHost(&w->h_pinned, 64), "cudaMallocHost")) return false;
   w->device = dev;
   return true;
@@ -2099,6 +2099,7 @@ int32_t phieng_sph_closure_step(World2* w, float dt_fine, uint32_t coarse_steps,
   io.save = w->d_save;
   io.rho_prev = w->d_rho_prev;
   io.svp = w->d_svp;
+  io.err = w->d.scan_err;  // tolerance mode: the tensor-core waits of the fused pass report here
   enqueue_sort_density(w, Pc, w->d_svp);
   // Coarse steps run in optimistic blocks: kBlock steps back to back with the
   // checks folded on the device and one read of their maxima. If every step

@@ -384,6 +384,58 @@ def test_zero_network_closure_equals_plain_coarse_step():
 
 
 @pytest.mark.gpu
+def test_tolerance_zero_network_closure_equals_plain_coarse_step():
+    """Tolerance mode: the fused coarse pass (tolerance-mode pair arithmetic,
+    network on the tcgen05 tensor cores) with a zero network equals the
+    plain tolerance-mode substep of 4 dt bit for bit."""
+    from phi_eng_b200 import _abi
+    from phi_eng_b200.closure import Mlp
+
+    sc = scenes.dam_break_4k()
+    m = Mlp()
+    plain, clo = _world(sc), _world(sc)
+    for w in (plain, clo):
+        w.precision = _abi.TOLERANCE
+        w.step_n(sc.dt, 20)
+    clo.set_closure(m, 4, 1e30, _abi.CLOSURE_JUMP)
+    st = None
+    for k in range(3):
+        plain.step(4 * sc.dt)
+        st = clo.closure_step(sc.dt, 1, st)
+        np.testing.assert_array_equal(clo.fluid.particles, plain.fluid.particles)
+    assert st.accepted == 3 and st.fallbacks == 0
+    assert clo.status().error == 0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["dam_break_4k", "dam_break_128x128"])
+def test_tolerance_closure_step_close_to_exact(name):
+    """One coarse step with the shipped network from the same state, in the
+    tolerance mode (fused tcgen05 pass) and in the exact mode (mma.sync
+    network): positions agree to a small fraction of h, and the check values
+    agree closely."""
+    from phi_eng_b200 import _abi
+    from phi_eng_b200 import closure as cl
+
+    sc = scenes.dam_break_4k() if name == "dam_break_4k" else scenes.dam_break_scaled(128, 128)
+    m = cl.Mlp.load(cl.WEIGHTS)
+    h = float(sc.config.smoothing_length)
+    ws = []
+    for mode in (_abi.EXACT, _abi.TOLERANCE):
+        w = _world(sc)
+        w.step_n(sc.dt, 40)
+        w.precision = mode
+        w.set_closure(m, 4, 1e30, _abi.CLOSURE_JUMP)
+        st = w.closure_step(sc.dt, 2)
+        ws.append((w.fluid.particles, st.max_check))
+        assert w.status().error == 0
+        w.close()
+    (a, ca), (b, cb) = ws
+    assert np.abs(a[:, :2] - b[:, :2]).max() < 1e-3 * h
+    assert abs(ca - cb) <= 1e-3 + 1e-2 * abs(ca)
+
+
+@pytest.mark.gpu
 def test_every_coarse_step_falling_back_equals_fine_steps():
     from phi_eng_b200 import _abi
     from phi_eng_b200.closure import Mlp
