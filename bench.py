@@ -311,7 +311,7 @@ def apply_tuning(world, mode: str, dt: float) -> dict:
     return dict(at.DEFAULT, source="defaults")
 
 
-def closure_line(sc) -> dict:
+def closure_line(sc, precision: int) -> dict:
     """The learned closure against the plain fine run on this workload, with
     the shipped weights: 50 coarse steps of 4 dt against 200 fine steps
     (speed and accuracy), under the per-particle jump criterion and under the
@@ -329,7 +329,8 @@ def closure_line(sc) -> dict:
     mlp = cl.Mlp.load(cl.WEIGHTS)
 
     def run(steps, crit, every):
-        r = cl.evaluate(sc, mlp, coarse_steps=steps, threshold=0.03, criterion=crit, record_every=every)
+        r = cl.evaluate(sc, mlp, coarse_steps=steps, threshold=0.03, criterion=crit, record_every=every,
+                        precision=precision)
         fp, fc = r["final_plain"], r["final_closure"]
         return {"ratio": r["speedup"], "learned": r["closure_sim_s_per_wall_s"],
                 "plain": r["plain_sim_s_per_wall_s"], "accepted": r["accepted"], "fallbacks": r["fallbacks"],
@@ -339,7 +340,9 @@ def closure_line(sc) -> dict:
                           "closure": {"front": fc["front"], "ke": fc["ke"], "dev_mean": fc["dev_mean"]}},
                 "front_travel_plain": fp["front"] - float(np.max(sc.xy[:, 0])), "coarse_steps": steps}
 
-    out = {"metric": "simulated s per wall s", "dt_ratio": 4, "threshold": 0.03}
+    out = {"metric": "simulated s per wall s", "dt_ratio": 4, "threshold": 0.03,
+           "precision": "tolerance (network on the tcgen05 tensor cores)" if precision == _abi.TOLERANCE
+           else "exact (network on mma.sync)"}
     jump = run(50, _abi.CLOSURE_JUMP, 10)
     out.update(jump, criterion="jump (largest per-particle density increase over the coarse step)")
     out["literal_rule"] = dict(run(50, _abi.CLOSURE_COMPRESSION, 10),
@@ -708,7 +711,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         if args.batch and world == 1 and args.workload != "batch_512":
             line["batch"] = batch_line(args.steps, args.warmup, args.tuning, not args.no_cpu_baseline, mode)
         if args.closure and single and world == 1:
-            line["closure"] = closure_line(scs[0])
+            line["closure"] = closure_line(scs[0], mode)
         if args.fluid3d and world == 1:
             line["fluid3d"] = fluid3d_line(args.steps, args.warmup)
         print(json.dumps(line), flush=True)

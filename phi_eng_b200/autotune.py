@@ -26,9 +26,9 @@ from . import _abi
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 SHIPPED = os.path.join(HERE, "tuning_b200.json")
-DEFAULT = dict(density_block=256, force_block=256, buckets_per_particle=2.0, stage=3)
+DEFAULT = dict(density_block=256, force_block=256, buckets_per_particle=2.0, stage=0)
 CANDIDATES = dict(density_block=(128, 256), force_block=(64, 128, 256), buckets_per_particle=(0.5, 1.0, 2.0, 4.0),
-                  stage=(3,))
+                  stage=(0,))
 # tolerance-mode worlds also try the passes without shared-memory staging
 CANDIDATES_TOLERANCE = dict(CANDIDATES, stage=(0, 1, 2, 3))
 
@@ -78,7 +78,7 @@ def lookup(world, gpu: str | None = None):
 
 def apply(world, tuning: dict) -> None:
     t = _abi.PhiengSphTuning(int(tuning["density_block"]), int(tuning["force_block"]),
-                             float(tuning["buckets_per_particle"]), int(tuning.get("stage", 3)))
+                             float(tuning["buckets_per_particle"]), int(tuning.get("stage", 0)))
     if world._lib.phieng_sph_set_tuning(world._h, C.byref(t)) != 1:
         raise ValueError(f"invalid tuning {tuning}")
 
@@ -120,7 +120,7 @@ def autotune(world, dt: float, steps: int = 20, candidates: dict | None = None, 
     world.sync()
     table = []
     for db, fb, bpp, stg in itertools.product(cand["density_block"], cand["force_block"],
-                                              cand["buckets_per_particle"], cand.get("stage", (3,))):
+                                              cand["buckets_per_particle"], cand.get("stage", (0,))):
         t = dict(density_block=db, force_block=fb, buckets_per_particle=bpp, stage=stg)
         apply(world, t)
         world.set_state_device(saved.data_ptr(), n)
@@ -144,7 +144,7 @@ def autotune(world, dt: float, steps: int = 20, candidates: dict | None = None, 
 
 
 def _main(argv=None) -> None:
-    """python -m phi_eng_b200.autotune [--workload NAME] [--out PATH]: tune the
+    """python -m phi_eng_b200.autotune [--workload NAME] [--out PATH] [--precision MODE]: tune the
     benchmark workloads and write their entries (GPU name + signature) to a
     JSON table."""
     import argparse
@@ -157,7 +157,10 @@ def _main(argv=None) -> None:
     ap.add_argument("--workload", action="append", choices=["dam_break_1m", "dam_break_4k", "batch_512"])
     ap.add_argument("--out", default=None, help="JSON table to update (default: the user cache)")
     ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--precision", choices=["exact", "tolerance"], default="exact",
+                    help="tune the worlds in this arithmetic mode (phieng_sph_set_precision)")
     a = ap.parse_args(argv)
+    mode = _abi.TOLERANCE if a.precision == "tolerance" else _abi.EXACT
     out = {}
     for name in a.workload or ["dam_break_1m", "dam_break_4k", "batch_512"]:
         if name == "batch_512":
@@ -167,6 +170,7 @@ def _main(argv=None) -> None:
         else:
             sc = S.dam_break_1m() if name == "dam_break_1m" else S.dam_break_4k()
             w, dt, keep = world_from_scene(sc), sc.dt, None
+        w.precision = mode
         w.step_n(dt, 3)
         r = autotune(w, dt, steps=a.steps)
         key = f"{gpu_name()}|{signature(w)}"

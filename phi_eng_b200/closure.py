@@ -22,6 +22,7 @@ import numpy as np
 
 from . import _abi
 from .world import World2, world_from_scene
+from .world import world_from_scene as _world_from_scene
 
 NPARAMS = _abi.MLP_PARAMS
 NNORM = _abi.MLP_NORM
@@ -466,7 +467,8 @@ def fluid_metrics(w: World2, mass: float, rho0: float):
 
 
 def evaluate(scene, mlp: Mlp, coarse_steps: int = 50, ratio: int = 4, threshold: float = 0.03,
-             criterion: int = _abi.CLOSURE_JUMP, record_every: int = 1, timing_reps: int = 1):
+             criterion: int = _abi.CLOSURE_JUMP, record_every: int = 1, timing_reps: int = 1,
+             precision: int = _abi.EXACT):
     """Closure (coarse_steps x ratio*dt) against the plain run (coarse_steps x
     ratio plain steps of dt) from the same initial state.
 
@@ -475,8 +477,17 @@ def evaluate(scene, mlp: Mlp, coarse_steps: int = 50, ratio: int = 4, threshold:
     travel), kinetic energy, mean |rho/rho0 - 1| and the largest compression.
     Speed: simulated seconds per wall second of each run, timed on the device
     with CUDA events over the whole run (metric reads excluded; the closure's
-    per-step density check and its host read are included)."""
+    per-step density check and its host read are included). Both runs use
+    the arithmetic mode `precision` (phieng_sph_set_precision); in the
+    tolerance mode the closure's coarse pass runs its network on the tcgen05
+    tensor cores."""
     torch = _torch()
+
+    def world_from_scene(sc):
+        w = _world_from_scene(sc)
+        w.precision = precision
+        return w
+
     dt = scene.dt
     mass = float(scene.config.particle_mass)
     rho0 = float(scene.config.rest_density)
@@ -586,6 +597,7 @@ def _main(argv=None) -> None:
     e.add_argument("--criterion", choices=["jump", "compression", "growth"], default="jump")
     e.add_argument("--zero", action="store_true", help="evaluate a zero network (no correction)")
     e.add_argument("--ratio", type=int, default=0, help="coarse step = ratio * dt (0: the weights' own ratio)")
+    e.add_argument("--precision", choices=["exact", "tolerance"], default="exact")
     a = ap.parse_args(argv)
     if a.cmd == "train":
         from .batch import batched_scenes
@@ -609,7 +621,8 @@ def _main(argv=None) -> None:
         if not a.zero:
             with np.load(a.weights) as z:
                 ratio = int(z["ratio"]) if "ratio" in z.files else 4
-    r = evaluate(sc, mlp, coarse_steps=a.coarse_steps, ratio=ratio, threshold=a.threshold, criterion=crit)
+    r = evaluate(sc, mlp, coarse_steps=a.coarse_steps, ratio=ratio, threshold=a.threshold, criterion=crit,
+                 precision=_abi.TOLERANCE if a.precision == "tolerance" else _abi.EXACT)
     print(json.dumps(dict(workload=a.workload, weights=None if a.zero else a.weights, **r)))
 
 

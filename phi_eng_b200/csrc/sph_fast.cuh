@@ -9,8 +9,8 @@
 // rounding (fluid.rs:383), so the neighbour lists and the row masks are the
 // same bits. What changes is the arithmetic of the sums over those
 // neighbours:
-//   density  rho_i = (m c_poly6) * sum t^3, t = h^2 - d2   (fluid.rs:592-611);
-//            Tait power x^gamma by f32 multiplies for an integer gamma;
+//   density  rho_i = (m c_poly6) * sum t^3, t = h^2 - d2   (fluid.rs:592-611),
+//            then the exact pass's clamp and EOS;
 //   force    one approximate reciprocal square root per pair gives the
 //            distance and the direction of the spiky gradient (fluid.rs:278-285),
 //            m (q_i + q_j) as one fused multiply-add, the sum accumulated
@@ -28,9 +28,13 @@
 // particles (row r's window = the union of the block's slot ranges of that
 // row: contiguous, since slots are sorted by bucket and a row's three buckets
 // are consecutive keys) from the sorted arrays into shared memory with
-// 16-byte loads, and the loops read them there. A window longer than the
-// block's capacity (a block across a wrapped bucket row, a crowded aliased
-// row) is not staged; that row's loops read global memory.
+// 16-byte loads, and the loops read them there. If any window is longer than
+// the block's capacity (a block across a wrapped bucket row, a crowded
+// aliased row), nothing is staged and the block reads global memory.
+//
+// Each thread walks its three rows as one flattened loop (the next row's
+// range starts as soon as the current one ends), so a warp's trip count is
+// the largest per-lane total, not the sum of the per-row maxima.
 
 // Staged slots per row window for a block of `threads` threads: a block of
 // B consecutive particles of one bucket row spans about B / 4 cells, i.e.
@@ -42,7 +46,8 @@ __host__ __device__ constexpr uint32_t fast_stage_cap(uint32_t threads) { return
 // float2 pairs).
 struct RowWindows {
   uint32_t base[3];
-  uint32_t len[3];  // 0: row not staged
+  uint32_t len[3];  // all 0: nothing staged
+  __device__ __forceinline__ bool staged() const { return len[0] != 0u; }
 };
 
 // Block-wide min / max of the per-thread row ranges (threads without masks
@@ -66,12 +71,15 @@ __device__ __forceinline__ RowWindows block_row_windows(const uint32_t lo[3], co
   }
   __syncthreads();
   RowWindows w;
+  bool all = true;
 #pragma unroll
   for (int r = 0; r < 3; r++) {
     const uint32_t l = s_lo[r], h = s_hi[r];
     w.base[r] = l & ~1u;
-    w.len[r] = (h > l && h - w.base[r] <= cap) ? h - w.base[r] : 0u;
+    w.len[r] = h > l ? h - w.base[r] : 0u;
+    all = all && h > l && w.len[r] <= cap;
   }
+  if (!all) w.len[0] = w.len[1] = w.len[2] = 0u;  // stage all three rows or none
   return w;
 }
 
@@ -84,29 +92,6 @@ __device__ __forceinline__ void stage_rows(float2* __restrict__ dst, const float
   const uint32_t pairs = len >> 1;
   for (uint32_t i = threadIdx.x; i < pairs; i += blockDim.x) d4[i] = __ldg(&s4[i]);
   if ((len & 1u) && threadIdx.x == 0) dst[len - 1] = __ldg(&src[base + len - 1]);
-}
-
-// x^g for the Tait power: binary exponentiation in f32 for an integer
-// g in [1, 64], else the correctly rounded power of the exact pass.
-__device__ __forceinline__ float powf_fast(float x, float g) {
-  if (g >= 1.0f && g <= 64.0f && g == floorf(g)) {
-    unsigned e = (unsigned)g;
-    float b = x, r = 1.0f;
-    while (e) {
-      if (e & 1u) r = __fmul_rn(r, b);
-      e >>= 1;
-      if (e) b = __fmul_rn(b, b);
-    }
-    return r;
-  }
-  return powf_cr(x, g);
-}
-
-__device__ __forceinline__ float eos_fast(float density, float rho0, const StepParams& P) {
-  if (!(P.flags & F_TAIT)) return fmaxf(__fmul_rn(P.stiffness, __fsub_rn(density, rho0)), 0.0f);
-  const float r0 = fmaxf(rho0, kEps);
-  const float pw = powf_fast(__fdiv_rn(density, r0), P.gamma);
-  return fmaxf(__fmul_rn(__fmul_rn(P.stiffness, r0), __fsub_rn(pw, 1.0f)), 0.0f);
 }
 
 // The three candidate rows of a particle in bucket k away from the x seam:
@@ -149,9 +134,10 @@ __global__ void __launch_bounds__(256) k_density_fast(const float2* __restrict__
   const uint32_t cap = fast_stage_cap(blockDim.x);
   if constexpr (STAGE) {
     win = block_row_windows(lo, hi, cap);
+    if (win.staged()) {
 #pragma unroll
-    for (int r = 0; r < 3; r++)
-      if (win.len[r]) stage_rows(fast_win + r * cap, spos, win.base[r], win.len[r]);
+      for (int r = 0; r < 3; r++) stage_rows(fast_win + r * cap, spos, win.base[r], win.len[r]);
+    }
     __syncthreads();
   }
   if (!active) return;
@@ -160,28 +146,47 @@ __global__ void __launch_bounds__(256) k_density_fast(const float2* __restrict__
   uint32_t mrow[3] = {0, 0, 0};
   bool masks_ok = rows;
   if (rows) {
-#pragma unroll
-    for (int r = 0; r < 3; r++) {
-      uint32_t m = 0, bit = 1u;
-      auto visit = [&](const float2 a) {
-        const float dx = __fsub_rn(a.x, pi.x), dy = __fsub_rn(a.y, pi.y);
-        const float d2 = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));  // the reference's rounding
-        const bool nb = d2 < P.hg2;
-        const float t = __fsub_rn(P.hk2, d2);
-        const float t3 = __fmul_rn(__fmul_rn(t, t), t);
-        acc = nb ? __fadd_rn(acc, t3) : acc;
-        m |= nb ? bit : 0u;
+    auto visit = [&](const float2 a, uint32_t& m, uint32_t bit) {
+      const float dx = __fsub_rn(a.x, pi.x), dy = __fsub_rn(a.y, pi.y);
+      const float d2 = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));  // the reference's rounding
+      const bool nb = d2 < P.hg2;
+      const float t = __fsub_rn(P.hk2, d2);
+      const float t3 = __fmul_rn(__fmul_rn(t, t), t);
+      acc = nb ? __fadd_rn(acc, t3) : acc;
+      m |= nb ? bit : 0u;
+    };
+    // rows 0, 1, 2 in one loop; a row's mask bit shifts out after 32 slots
+    // (then masks_ok is false)
+    auto walk = [&](auto load, uint32_t o0, uint32_t o1, uint32_t o2) {
+      uint32_t row = 0, j = lo[0], e = hi[0], o = o0, m = 0u, bit = 1u;
+      for (;;) {
+        if (j >= e) {
+          if (row == 2u) break;
+          if (row == 0u)
+            mrow[0] = m;
+          else
+            mrow[1] = m;
+          row++;
+          j = row == 1u ? lo[1] : lo[2];
+          e = row == 1u ? hi[1] : hi[2];
+          o = row == 1u ? o1 : o2;
+          m = 0u;
+          bit = 1u;
+          continue;
+        }
+        visit(load(o + j), m, bit);
         bit <<= 1;
-      };
-      if (STAGE && win.len[r]) {
-        const uint32_t o = r * cap - win.base[r];  // shared index of slot j: o + j (mod 2^32)
-        for (uint32_t j = lo[r]; j < hi[r]; j++) visit(fast_win[o + j]);
-      } else {
-        for (uint32_t j = lo[r]; j < hi[r]; j++) visit(__ldg(&spos[j]));
+        j++;
       }
-      mrow[r] = m;
+      mrow[2] = m;
+    };
+    if (STAGE && win.staged())  // shared index of slot j of row r: r * cap - base[r] + j (mod 2^32)
+      walk([&](uint32_t i) { return fast_win[i]; }, 0u - win.base[0], cap - win.base[1], 2u * cap - win.base[2]);
+    else
+      walk([&](uint32_t i) { return __ldg(&spos[i]); }, 0u, 0u, 0u);
+#pragma unroll
+    for (int r = 0; r < 3; r++)
       if (hi[r] - lo[r] > kMaskBits) masks_ok = false;
-    }
   } else if (k != g.sentinel) {
     // x seam: the reference's cell-by-cell walk
     for_each_candidate(k, start, g, [&](int j) {
@@ -199,7 +204,7 @@ __global__ void __launch_bounds__(256) k_density_fast(const float2* __restrict__
   float dens = __fmul_rn(__fmul_rn(P.mass, P.c_poly6), acc);
   if (dens < 0.0f) dens = 0.0f;  // f32::clamp(0, 3 * max(rest_density, EPS)) (fluid.rs:605)
   if (dens > P.rho_cap) dens = P.rho_cap;
-  const float p = eos_fast(dens, P.rest[P.uniform_phase], P);
+  const float p = eos(dens, P.rest[P.uniform_phase], P);  // the exact pass's EOS (correctly rounded power)
   const float rc = fmaxf(dens, kEps);
   const float q = __fdiv_rn(p, __fmul_rn(rc, rc));
   sdq[s] = make_float2(dens, q);
@@ -262,13 +267,14 @@ __global__ void __launch_bounds__(256) k_force_fast(
   float2* wq = fast_win + 6 * cap;  // [3][cap] (density, q)
   if constexpr (STAGE) {
     win = block_row_windows(lo, hi, cap);
+    if (win.staged()) {
 #pragma unroll
-    for (int r = 0; r < 3; r++)
-      if (win.len[r]) {
+      for (int r = 0; r < 3; r++) {
         stage_rows(wp + r * cap, spos, win.base[r], win.len[r]);
         stage_rows(wv + r * cap, svel, win.base[r], win.len[r]);
         stage_rows(wq + r * cap, sdq, win.base[r], win.len[r]);
       }
+    }
     __syncthreads();
   }
   if (!active) return;
@@ -283,25 +289,28 @@ __global__ void __launch_bounds__(256) k_force_fast(
   if (rows) {
     // the three rows' neighbour bits in ascending slot order, the particle's
     // own bit cleared (j != i, fluid.rs:947-950)
-    uint32_t m[3] = {nmask[s], own & ~(1u << (s - lo[1])), nmask[2 * (size_t)n + s]};
-#pragma unroll
-    for (int r = 0; r < 3; r++) {
-      uint32_t cur = m[r];
-      if (STAGE && win.len[r]) {
-        const uint32_t o = r * cap + lo[r] - win.base[r];
-        while (cur) {
-          const uint32_t j = o + (uint32_t)(__ffs((int)cur) - 1);
-          cur &= cur - 1u;
-          pair(wp[j], wv[j], wq[j], P, fx, fy, sx, sy);
+    const uint32_t m1 = own & ~(1u << (s - lo[1])), m2 = nmask[2 * (size_t)n + s];
+    // the three rows' set bits as one loop (ascending slots, row by row)
+    auto walk = [&](auto pair_at, uint32_t o0, uint32_t o1, uint32_t o2) {
+      uint32_t cur = nmask[s], row = 0, o = o0;
+      for (;;) {
+        while (cur == 0u && row < 2u) {
+          row++;
+          cur = row == 1u ? m1 : m2;
+          o = row == 1u ? o1 : o2;
         }
-      } else {
-        while (cur) {
-          const uint32_t j = lo[r] + (uint32_t)(__ffs((int)cur) - 1);
-          cur &= cur - 1u;
-          pair(__ldg(&spos[j]), __ldg(&svel[j]), __ldg(&sdq[j]), P, fx, fy, sx, sy);
-        }
+        if (cur == 0u) break;
+        const uint32_t j = o + (uint32_t)(__ffs((int)cur) - 1);
+        cur &= cur - 1u;
+        pair_at(j);
       }
-    }
+    };
+    if (STAGE && win.staged())
+      walk([&](uint32_t j) { pair(wp[j], wv[j], wq[j], P, fx, fy, sx, sy); }, lo[0] - win.base[0],
+           cap + lo[1] - win.base[1], 2u * cap + lo[2] - win.base[2]);
+    else
+      walk([&](uint32_t j) { pair(__ldg(&spos[j]), __ldg(&svel[j]), __ldg(&sdq[j]), P, fx, fy, sx, sy); }, lo[0],
+           lo[1], lo[2]);
   } else if (k != g.sentinel) {
     // no masks (x seam, or a row longer than 32 slots): walk the candidates
     for_each_candidate(k, start, g, [&](int jj) {

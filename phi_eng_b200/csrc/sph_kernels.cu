@@ -277,6 +277,76 @@ __global__ void __launch_bounds__(256) k_scan_lookback(uint32_t* __restrict__ co
   }
 }
 
+struct GatherArgs {
+  const float4* state;
+  const float* mass;
+  const uint8_t* phase;
+  float2* spos;
+  float2* svel;
+  float* smass;
+  uint8_t* sphase;
+  const uint32_t* pscene;  // batch: scene of each particle (id order), else null
+  uint32_t* sscene;
+};
+
+// The particle's sorted entries at final slot f (sid only when given: the
+// placement pass reads the previous sort's sid while it runs).
+__device__ __forceinline__ void gather_slot(uint32_t f, uint32_t k, uint32_t id, const GatherArgs& ga,
+                                            uint32_t* __restrict__ skey, uint32_t* __restrict__ sid) {
+  skey[f] = k;
+  if (sid) sid[f] = id;
+  const float4 st = ga.state[id];
+  ga.spos[f] = make_float2(st.x, st.y);
+  ga.svel[f] = make_float2(st.z, st.w);
+  if (ga.smass) ga.smass[f] = ga.mass[id];
+  if (ga.sphase) ga.sphase[f] = ga.phase[id];
+  if (ga.sscene) ga.sscene[f] = ga.pscene[id];
+}
+
+// tid entry of a slot whose particle k_place_final already put in its final
+// place (ids are below 2^31)
+constexpr uint32_t kPlacedFinal = 0x80000000u;
+
+// Placement for the 2D sort, with the common case finished in place: when a
+// run of equal keys in consecutive lanes is the whole bucket (its length
+// equals the bucket's count) and its ids ascend lane by lane, the run's
+// slots are already the final (key, id) order, so its particles are
+// gathered into sorted order here and their tid entries flagged; k_fixup
+// ranks only the other buckets and writes the flagged slots' sid (read here
+// as the previous order). Particles keep their cell from one substep
+// to the next almost always, and a bucket's particles arrive as one run in
+// the previous sort's order, so most buckets finish here.
+template <bool BY_SLOT>
+__global__ void __launch_bounds__(256) k_place_final(const uint32_t* __restrict__ key,
+                                                     const uint32_t* __restrict__ sid_prev, uint32_t n,
+                                                     uint32_t* __restrict__ cursor, const uint32_t* __restrict__ start,
+                                                     uint32_t* __restrict__ tkey, uint32_t* __restrict__ tid_out,
+                                                     uint32_t* __restrict__ skey, GatherArgs ga) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  const uint32_t id = BY_SLOT ? sid_prev[s] : s;
+  const uint32_t k = key[id];
+  const uint32_t act = __activemask();  // a prefix of the warp's lanes
+  const uint32_t lane = threadIdx.x & 31u;
+  uint32_t first, len, rank;
+  key_run(act, k, lane, &first, &len, &rank);
+  uint32_t base = 0;
+  if (first == lane) base = atomicAdd(&cursor[k], len);
+  base = __shfl_sync(act, base, first);
+  const uint32_t slot = base + rank;
+  const uint32_t pid = __shfl_sync(act, id, lane ? lane - 1u : 0u);
+  const bool asc = lane == first || pid < id;
+  const uint32_t bad = __ballot_sync(act, !asc);
+  const uint32_t run = (len >= 32u ? 0xFFFFFFFFu : ((1u << len) - 1u)) << first;
+  if (len == __ldg(&start[k + 1]) - __ldg(&start[k]) && (bad & run) == 0u) {
+    gather_slot(slot, k, id, ga, skey, nullptr);
+    tid_out[slot] = id | kPlacedFinal;
+  } else {
+    tkey[slot] = k;
+    tid_out[slot] = id;
+  }
+}
+
 // Slot in the bucket from the cursor. BY_SLOT walks the previous sort's
 // order (keys nearly sorted: a warp holds few runs of equal keys, so few
 // atomics); otherwise particles are taken in id order.
@@ -303,18 +373,6 @@ __global__ void __launch_bounds__(256) k_place(const uint32_t* __restrict__ key,
   tid_out[slot] = id;
 }
 
-struct GatherArgs {
-  const float4* state;
-  const float* mass;
-  const uint8_t* phase;
-  float2* spos;
-  float2* svel;
-  float* smass;
-  uint8_t* sphase;
-  const uint32_t* pscene;  // batch: scene of each particle (id order), else null
-  uint32_t* sscene;
-};
-
 // Final slot = bucket start + rank of the id among the bucket's ids; the
 // particle's state is gathered into that slot.
 __global__ void __launch_bounds__(256) k_fixup(const uint32_t* __restrict__ tkey,
@@ -324,20 +382,16 @@ __global__ void __launch_bounds__(256) k_fixup(const uint32_t* __restrict__ tkey
                                                GatherArgs ga) {
   const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n) return;
-  const uint32_t k = tkey[s];
   const uint32_t id = tid_in[s];
+  if (id & kPlacedFinal) {  // k_place_final finished this bucket but its sid
+    sid[s] = id & ~kPlacedFinal;
+    return;
+  }
+  const uint32_t k = tkey[s];
   const uint32_t lo = start[k], hi = start[k + 1];
   uint32_t rank = 0;
   for (uint32_t j = lo; j < hi; j++) rank += __ldg(&tid_in[j]) < id ? 1u : 0u;
-  const uint32_t f = lo + rank;
-  skey[f] = k;
-  sid[f] = id;
-  const float4 st = ga.state[id];
-  ga.spos[f] = make_float2(st.x, st.y);
-  ga.svel[f] = make_float2(st.z, st.w);
-  if (ga.smass) ga.smass[f] = ga.mass[id];
-  if (ga.sphase) ga.sphase[f] = ga.phase[id];
-  if (ga.sscene) ga.sscene[f] = ga.pscene[id];
+  gather_slot(lo + rank, k, id, ga, skey, sid);
 }
 
 // ---------------------------------------------------------------- neighbour walk
@@ -1015,8 +1069,8 @@ void enqueue_keys(const FluidBufs& b, uint32_t n, const GridPlan& g, cudaStream_
     k_keys<false><<<cdiv(n, 256), 256, 0, st>>>(b.state, n, g, b.batch, b.key, b.count);
 }
 
-void enqueue_bucket_place(const BucketSort& bs, uint32_t n, uint32_t m, bool by_slot, cudaStream_t st) {
-  if (n == 0) return;
+// Bucket counts -> start table (count becomes the placement cursor).
+void enqueue_bucket_scan(const BucketSort& bs, uint32_t m, cudaStream_t st) {
   const uint32_t nt = cdiv(m, kScanTile);
   if (bs.tstate) {
     k_scan_lookback<<<nt, 256, 0, st>>>(bs.count, nt, bs.start, bs.tstate, bs.done, bs.err, 0xFFFFFFFFu);
@@ -1024,6 +1078,11 @@ void enqueue_bucket_place(const BucketSort& bs, uint32_t n, uint32_t m, bool by_
     k_scan_reduce<<<nt, 256, 0, st>>>(bs.count, bs.tilesum, nt, bs.done);
     k_scan_down<<<nt, 256, 0, st>>>(bs.count, bs.tilesum, m, bs.start);
   }
+}
+
+void enqueue_bucket_place(const BucketSort& bs, uint32_t n, uint32_t m, bool by_slot, cudaStream_t st) {
+  if (n == 0) return;
+  enqueue_bucket_scan(bs, m, st);
   if (by_slot)
     k_place<true><<<cdiv(n, 256), 256, 0, st>>>(bs.key, bs.sid_prev, n, bs.count, bs.tkey, bs.tid);
   else
@@ -1044,7 +1103,6 @@ void enqueue_sort_and_ranges(const FluidBufs& b, uint32_t n, const StepParams& P
   bs.sid_prev = b.sid;
   bs.tkey = b.tkey;
   bs.tid = b.tid;
-  enqueue_bucket_place(bs, n, m, by_slot, st);
   GatherArgs ga;
   ga.state = b.state;
   ga.mass = b.mass;
@@ -1055,6 +1113,11 @@ void enqueue_sort_and_ranges(const FluidBufs& b, uint32_t n, const StepParams& P
   ga.sphase = (P.flags & F_PHASE) ? b.sphase : nullptr;
   ga.pscene = b.batch.pscene;
   ga.sscene = b.batch.ptab ? b.batch.sscene : nullptr;
+  enqueue_bucket_scan(bs, m, st);
+  if (by_slot)
+    k_place_final<true><<<cdiv(n, 256), 256, 0, st>>>(b.key, b.sid, n, b.count, b.start, b.tkey, b.tid, b.skey, ga);
+  else
+    k_place_final<false><<<cdiv(n, 256), 256, 0, st>>>(b.key, b.sid, n, b.count, b.start, b.tkey, b.tid, b.skey, ga);
   k_fixup<<<cdiv(n, 256), 256, 0, st>>>(b.tkey, b.tid, b.start, n, b.skey, b.sid, ga);
   // the counts of the next sort accumulate from zero (K6)
   cudaMemsetAsync(b.count, 0, sizeof(uint32_t) * b.count_len, st);
