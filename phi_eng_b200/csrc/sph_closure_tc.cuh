@@ -53,8 +53,9 @@ struct FastFeatPair {
   }
 };
 
+// At most 6 CTAs share an SM (shared memory), so 80 registers cost nothing.
 template <bool BATCH>
-__global__ void __launch_bounds__(128) k_closure_tc(
+__global__ void __launch_bounds__(128, 6) k_closure_tc(
     const float2* __restrict__ spos, const float2* __restrict__ svel, const float2* __restrict__ sdq,
     const float* __restrict__ spres, const uint32_t* __restrict__ skey, const uint32_t* __restrict__ sid, uint32_t n,
     const uint32_t* __restrict__ start, StepParams P0, BatchTab bt, const DevBody* __restrict__ bodies,

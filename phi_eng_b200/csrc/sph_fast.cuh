@@ -32,9 +32,9 @@
 // the block's capacity (a block across a wrapped bucket row, a crowded
 // aliased row), nothing is staged and the block reads global memory.
 //
-// Each thread walks its three rows as one flattened loop (the next row's
-// range starts as soon as the current one ends), so a warp's trip count is
-// the largest per-lane total, not the sum of the per-row maxima.
+// The force pass walks a thread's three rows as one flattened loop (the next
+// row's range starts as soon as the current one ends), so a warp's trip count
+// is the largest per-lane total, not the sum of the per-row maxima.
 
 // Staged slots per row window for a block of `threads` threads: a block of
 // B consecutive particles of one bucket row spans about B / 4 cells, i.e.
@@ -155,35 +155,21 @@ __global__ void __launch_bounds__(256) k_density_fast(const float2* __restrict__
       acc = nb ? __fadd_rn(acc, t3) : acc;
       m |= nb ? bit : 0u;
     };
-    // rows 0, 1, 2 in one loop; a row's mask bit shifts out after 32 slots
-    // (then masks_ok is false)
-    auto walk = [&](auto load, uint32_t o0, uint32_t o1, uint32_t o2) {
-      uint32_t row = 0, j = lo[0], e = hi[0], o = o0, m = 0u, bit = 1u;
-      for (;;) {
-        if (j >= e) {
-          if (row == 2u) break;
-          if (row == 0u)
-            mrow[0] = m;
-          else
-            mrow[1] = m;
-          row++;
-          j = row == 1u ? lo[1] : lo[2];
-          e = row == 1u ? hi[1] : hi[2];
-          o = row == 1u ? o1 : o2;
-          m = 0u;
-          bit = 1u;
-          continue;
-        }
-        visit(load(o + j), m, bit);
-        bit <<= 1;
-        j++;
+    // row by row (a flattened loop over the three rows measured slower here:
+    // the candidate loop is short and its row switch costs more than the
+    // lanes it keeps busy); a row's mask bit shifts out after 32 slots (then
+    // masks_ok is false)
+#pragma unroll
+    for (int r = 0; r < 3; r++) {
+      uint32_t m = 0u, bit = 1u;
+      if (STAGE && win.staged()) {
+        const uint32_t o = r * cap - win.base[r];  // shared index of slot j: o + j (mod 2^32)
+        for (uint32_t j = lo[r]; j < hi[r]; j++, bit <<= 1) visit(fast_win[o + j], m, bit);
+      } else {
+        for (uint32_t j = lo[r]; j < hi[r]; j++, bit <<= 1) visit(__ldg(&spos[j]), m, bit);
       }
-      mrow[2] = m;
-    };
-    if (STAGE && win.staged())  // shared index of slot j of row r: r * cap - base[r] + j (mod 2^32)
-      walk([&](uint32_t i) { return fast_win[i]; }, 0u - win.base[0], cap - win.base[1], 2u * cap - win.base[2]);
-    else
-      walk([&](uint32_t i) { return __ldg(&spos[i]); }, 0u, 0u, 0u);
+      mrow[r] = m;
+    }
 #pragma unroll
     for (int r = 0; r < 3; r++)
       if (hi[r] - lo[r] > kMaskBits) masks_ok = false;

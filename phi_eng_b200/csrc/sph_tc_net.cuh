@@ -112,21 +112,26 @@ __device__ __forceinline__ bool tc_net_layer(TcNet& net, F&& issue) {
 
 // Hidden-layer epilogue: TMEM columns [0, 64) of this thread's row plus the
 // halved bias b, through silu, as FP16 into row threadIdx.x of the A operand.
+// Two halves of 32 columns, to keep the registers of a fused caller low.
 __device__ __forceinline__ void tc_net_hidden(const TcNet& net, const float* b) {
   const uint32_t lanes = ((threadIdx.x >> 5) * 32u) << 16;
   unsigned char* A = net.sm + kNetA;
-  float v[4][16];
 #pragma unroll
-  for (int q = 0; q < 4; q++) tc::tmem_ld16(net.tmem + lanes + 16 * q, v[q]);
-  tc::tmem_wait_ld();
+  for (int half = 0; half < 2; half++) {
+    float v[2][16];
 #pragma unroll
-  for (int q = 0; q < 4; q++) {
-    uint32_t h[8];
+    for (int q = 0; q < 2; q++) tc::tmem_ld16(net.tmem + lanes + 32 * half + 16 * q, v[q]);
+    tc::tmem_wait_ld();
 #pragma unroll
-    for (int j = 0; j < 8; j++)
-      h[j] = silu_half_f16x2(__fadd_rn(v[q][2 * j], b[16 * q + 2 * j]), __fadd_rn(v[q][2 * j + 1], b[16 * q + 2 * j + 1]));
-    *reinterpret_cast<uint4*>(A + tc::kmajor_offset(threadIdx.x, 16 * q, 64)) = make_uint4(h[0], h[1], h[2], h[3]);
-    *reinterpret_cast<uint4*>(A + tc::kmajor_offset(threadIdx.x, 16 * q + 8, 64)) = make_uint4(h[4], h[5], h[6], h[7]);
+    for (int q = 0; q < 2; q++) {
+      const int c = 32 * half + 16 * q;  // first unit of this group of 16
+      uint32_t h[8];
+#pragma unroll
+      for (int j = 0; j < 8; j++)
+        h[j] = silu_half_f16x2(__fadd_rn(v[q][2 * j], b[c + 2 * j]), __fadd_rn(v[q][2 * j + 1], b[c + 2 * j + 1]));
+      *reinterpret_cast<uint4*>(A + tc::kmajor_offset(threadIdx.x, c, 64)) = make_uint4(h[0], h[1], h[2], h[3]);
+      *reinterpret_cast<uint4*>(A + tc::kmajor_offset(threadIdx.x, c + 8, 64)) = make_uint4(h[4], h[5], h[6], h[7]);
+    }
   }
 }
 
