@@ -343,13 +343,15 @@ int32_t phieng_sph_get_tuning(const World2* world, PhiengSphTuning* out);
  * with IEEE division and square root (fluid.rs:265-297, 592-611, 942-1050):
  * bit-identical to the reference's arithmetic in the Jacobi integrate order.
  * TOLERANCE: for the plain flag set (uniform mass and phase, XSPH on, no
- * artificial viscosity, cohesion, turbulence, ghosts or polygons) the
- * density, force and XSPH sums are reassociated with fused multiply-adds,
- * one approximate reciprocal square root and one approximate reciprocal per
- * neighbour pair. Neighbour sets, sort order and visit order stay exact and
- * runs stay bit-reproducible; from identical state, density agrees with the
- * exact mode within 1e-5 and force within 1e-4 of their RMS. Other flag sets
- * and batches run the exact passes in either mode. */
+ * artificial viscosity, cohesion, turbulence, ghosts or polygons) the force
+ * and XSPH sums are reassociated with fused multiply-adds, one approximate
+ * reciprocal square root and one approximate reciprocal per neighbour pair
+ * (the density pass stays exact unless PhiengSphTuning.stage bit 0 selects
+ * its shared-memory-staged, reassociated variant). Neighbour sets, sort
+ * order and visit order stay exact and runs stay bit-reproducible; from
+ * identical state, density agrees with the exact mode within 1e-5 and force
+ * within 1e-4 of their RMS. Other flag sets run the exact passes in either
+ * mode. */
 #define PHIENG_SPH_EXACT 0u
 #define PHIENG_SPH_TOLERANCE 1u
 /* 1 ok, 0 null or an unknown mode (world unchanged). */

@@ -4,11 +4,14 @@
 //
 // Scope: the plain flag set (uniform mass and phase, XSPH on, no artificial
 // viscosity, cohesion, turbulence, ghosts or polygons, h > 0) of a single
-// world or of every scene of a batch. The neighbour sets, the sort order and the per-particle visit order
-// are the exact passes': the neighbour test d2 < h*h keeps the reference's
-// rounding (fluid.rs:383), so the neighbour lists and the row masks are the
-// same bits. What changes is the arithmetic of the sums over those
-// neighbours:
+// world or of every scene of a batch. The force pass below is the tolerance
+// mode's; its density pass is the exact k_density, except when the tuning
+// asks for the shared-memory-staged density variant here (measured slower
+// on B200; kept selectable). The neighbour sets, the sort order and the
+// per-particle visit order are the exact passes': the neighbour test
+// d2 < h*h keeps the reference's rounding (fluid.rs:383), so the neighbour
+// lists and the row masks are the same bits. What changes is the arithmetic
+// of the sums over those neighbours:
 //   density  rho_i = (m c_poly6) * sum t^3, t = h^2 - d2   (fluid.rs:592-611),
 //            then the exact pass's clamp and EOS;
 //   force    one approximate reciprocal square root per pair gives the

@@ -1230,20 +1230,18 @@ void enqueue_density(const FluidBufs& b, uint32_t n, const StepParams& P, cudaSt
   const bool m = (P.flags & F_MASS) != 0, ph = (P.flags & F_PHASE) != 0, bat = b.batch.ptab != nullptr;
   const bool wide = (P.flags & F_WIDE_NB) != 0;  // h <= 0, which only a snapshot can carry
   const uint32_t bs = b.block_density, g = cdiv(n, bs);
-  if (fast_flags(P.flags)) {
+  // Tolerance mode: the density pass stays the exact one (its neighbour test
+  // must keep the reference's rounding, which leaves the reassociated sum
+  // nothing to save: measured slower), unless the tuning asks for the
+  // shared-memory-staged variant.
+  if (fast_flags(P.flags) && (b.stage & 1u)) {
     const size_t sm = 3 * fast_stage_cap(bs) * sizeof(float2);
-#define PHIENG_DENSITY_FAST(STG, BT)                                                                           \
-  k_density_fast<STG, BT><<<g, bs, STG ? sm : 0, st>>>(b.spos, b.skey, n, b.start, P, b.batch, b.sdq, b.spres, \
-                                                       b.nmask, svp)
-    const bool stg = (b.stage & 1u) != 0;
-    if (bat) {
-      if (stg) PHIENG_DENSITY_FAST(true, true);
-      else PHIENG_DENSITY_FAST(false, true);
-    } else {
-      if (stg) PHIENG_DENSITY_FAST(true, false);
-      else PHIENG_DENSITY_FAST(false, false);
-    }
-#undef PHIENG_DENSITY_FAST
+    if (bat)
+      k_density_fast<true, true><<<g, bs, sm, st>>>(b.spos, b.skey, n, b.start, P, b.batch, b.sdq, b.spres, b.nmask,
+                                                    svp);
+    else
+      k_density_fast<true, false><<<g, bs, sm, st>>>(b.spos, b.skey, n, b.start, P, b.batch, b.sdq, b.spres, b.nmask,
+                                                     svp);
     return;
   }
 #define PHIENG_DENSITY(M, PH, BT, WD)                                                                          \
