@@ -329,8 +329,9 @@ typedef struct PhiengSphTuning {
   uint32_t density_block;     /* threads per block of the density pass: 64, 128, 256 (default 256) */
   uint32_t force_block;       /* threads per block of the force pass: 64, 128, 256 (default 256) */
   float buckets_per_particle; /* bucket-grid budget per particle, 0.125..16 (default 2) */
-  uint32_t stage;             /* tolerance-mode passes: bit 0 = the density pass stages its neighbour
-                                 rows in shared memory, bit 1 = the force pass does (default 0) */
+  uint32_t stage;             /* tolerance mode: bit 0 = the density pass stages its neighbour rows in
+                                 shared memory, bit 1 = the force pass does (default 0; no effect on
+                                 results) */
 } PhiengSphTuning;
 
 /* 1 ok, 0 null or out of range (world unchanged). Replans the bucket grid
@@ -345,9 +346,8 @@ int32_t phieng_sph_get_tuning(const World2* world, PhiengSphTuning* out);
  * TOLERANCE: for the plain flag set (uniform mass and phase, XSPH on, no
  * artificial viscosity, cohesion, turbulence, ghosts or polygons) the force
  * and XSPH sums are reassociated with fused multiply-adds, one approximate
- * reciprocal square root and one approximate reciprocal per neighbour pair
- * (the density pass stays exact unless PhiengSphTuning.stage bit 0 selects
- * its shared-memory-staged, reassociated variant). Neighbour sets, sort
+ * reciprocal square root and one approximate reciprocal per neighbour pair;
+ * the density pass stays exact (bit-identical). Neighbour sets, sort
  * order and visit order stay exact and runs stay bit-reproducible; from
  * identical state, density agrees with the exact mode within 1e-5 and force
  * within 1e-4 of their RMS. Other flag sets run the exact passes in either

@@ -4,16 +4,17 @@
 //
 // Scope: the plain flag set (uniform mass and phase, XSPH on, no artificial
 // viscosity, cohesion, turbulence, ghosts or polygons, h > 0) of a single
-// world or of every scene of a batch. The force pass below is the tolerance
-// mode's; its density pass is the exact k_density, except when the tuning
-// asks for the shared-memory-staged density variant here (measured slower
-// on B200; kept selectable). The neighbour sets, the sort order and the
-// per-particle visit order are the exact passes': the neighbour test
+// world or of every scene of a batch. The neighbour sets, the sort order and
+// the per-particle visit order are the exact passes': the neighbour test
 // d2 < h*h keeps the reference's rounding (fluid.rs:383), so the neighbour
-// lists and the row masks are the same bits. What changes is the arithmetic
-// of the sums over those neighbours:
-//   density  rho_i = (m c_poly6) * sum t^3, t = h^2 - d2   (fluid.rs:592-611),
-//            then the exact pass's clamp and EOS;
+// lists and the row masks are the same bits.
+//   density  k_density_fast is the exact density pass (the same products in
+//            the same order: bit-identical results) with its neighbour rows
+//            staged in shared memory, a launch shape (PhiengSphTuning.stage
+//            bit 0); without staging the mode runs k_density itself.
+//            Reassociating the density sum does not pay: the neighbour test
+//            needs the reference's d2, which leaves one multiply per
+//            candidate to save (measured slower);
 //   force    one approximate reciprocal square root per pair gives the
 //            distance and the direction of the spiky gradient (fluid.rs:278-285),
 //            m (q_i + q_j) as one fused multiply-add, the sum accumulated
@@ -23,9 +24,8 @@
 //            (fluid.rs:1022-1033).
 // Every operation is an explicit intrinsic in a fixed order, so a run is
 // bit-reproducible; the parity tests bound the difference to the reference's
-// arithmetic (density 1e-5, force 1e-4 of the RMS from identical state).
-// The per-particle epilogue (clamp, EOS division, integrate, walls, next key)
-// is the exact pass's.
+// arithmetic (force 1e-4 of the RMS from identical state). The per-particle
+// epilogue (integrate, walls, next key) is the exact pass's.
 //
 // STAGE: the block first copies the three neighbour-row windows of its
 // particles (row r's window = the union of the block's slot ranges of that
@@ -34,6 +34,8 @@
 // 16-byte loads, and the loops read them there. If any window is longer than
 // the block's capacity (a block across a wrapped bucket row, a crowded
 // aliased row), nothing is staged and the block reads global memory.
+// Staging measured slower on B200 (the rows are L1 / L2 resident) and is off
+// by default.
 //
 // The force pass walks a thread's three rows as one flattened loop (the next
 // row's range starts as soon as the current one ends), so a warp's trip count
@@ -117,7 +119,7 @@ __device__ __forceinline__ bool candidate_rows(uint32_t k, const uint32_t* __res
   return true;
 }
 
-// ---------------------------------------------------------------- K5 (tolerance mode)
+// ---------------------------------------------------------------- K5, shared-memory-staged
 template <bool STAGE, bool BATCH>
 __global__ void __launch_bounds__(256) k_density_fast(const float2* __restrict__ spos,
                                                       const uint32_t* __restrict__ skey, uint32_t n,
@@ -145,7 +147,7 @@ __global__ void __launch_bounds__(256) k_density_fast(const float2* __restrict__
   }
   if (!active) return;
   const float2 pi = spos[s];
-  float acc = 0.0f;  // sum of t^3 over the neighbours
+  float rho = 0.0f;
   uint32_t mrow[3] = {0, 0, 0};
   bool masks_ok = rows;
   if (rows) {
@@ -153,9 +155,8 @@ __global__ void __launch_bounds__(256) k_density_fast(const float2* __restrict__
       const float dx = __fsub_rn(a.x, pi.x), dy = __fsub_rn(a.y, pi.y);
       const float d2 = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));  // the reference's rounding
       const bool nb = d2 < P.hg2;
-      const float t = __fsub_rn(P.hk2, d2);
-      const float t3 = __fmul_rn(__fmul_rn(t, t), t);
-      acc = nb ? __fadd_rn(acc, t3) : acc;
+      const float w = neighbour_density_term<false>(d2, P.mass, P);  // m * poly6, the exact pass's order
+      rho = nb ? __fadd_rn(rho, w) : rho;
       m |= nb ? bit : 0u;
     };
     // row by row (a flattened loop over the three rows measured slower here:
@@ -181,19 +182,17 @@ __global__ void __launch_bounds__(256) k_density_fast(const float2* __restrict__
     for_each_candidate(k, start, g, [&](int j) {
       const float2 a = __ldg(&spos[j]);
       const float dx = __fsub_rn(a.x, pi.x), dy = __fsub_rn(a.y, pi.y);
-      const float d2 = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
-      const float t = __fsub_rn(P.hk2, d2);
-      if (d2 < P.hg2) acc = __fadd_rn(acc, __fmul_rn(__fmul_rn(t, t), t));
+      rho = __fadd_rn(rho, density_term(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), P.mass, P));
     });
   }
   if (!masks_ok) mrow[1] = 0;  // the force pass walks the candidates itself
   nmask[s] = mrow[0];
   nmask[n + s] = mrow[1];
   nmask[2 * (size_t)n + s] = mrow[2];
-  float dens = __fmul_rn(__fmul_rn(P.mass, P.c_poly6), acc);
+  float dens = rho;
   if (dens < 0.0f) dens = 0.0f;  // f32::clamp(0, 3 * max(rest_density, EPS)) (fluid.rs:605)
   if (dens > P.rho_cap) dens = P.rho_cap;
-  const float p = eos(dens, P.rest[P.uniform_phase], P);  // the exact pass's EOS (correctly rounded power)
+  const float p = eos(dens, P.rest[P.uniform_phase], P);
   const float rc = fmaxf(dens, kEps);
   const float q = __fdiv_rn(p, __fmul_rn(rc, rc));
   sdq[s] = make_float2(dens, q);

@@ -1230,10 +1230,8 @@ void enqueue_density(const FluidBufs& b, uint32_t n, const StepParams& P, cudaSt
   const bool m = (P.flags & F_MASS) != 0, ph = (P.flags & F_PHASE) != 0, bat = b.batch.ptab != nullptr;
   const bool wide = (P.flags & F_WIDE_NB) != 0;  // h <= 0, which only a snapshot can carry
   const uint32_t bs = b.block_density, g = cdiv(n, bs);
-  // Tolerance mode: the density pass stays the exact one (its neighbour test
-  // must keep the reference's rounding, which leaves the reassociated sum
-  // nothing to save: measured slower), unless the tuning asks for the
-  // shared-memory-staged variant.
+  // Tolerance mode with staging asked for: the exact density pass with its
+  // neighbour rows staged in shared memory (same bits).
   if (fast_flags(P.flags) && (b.stage & 1u)) {
     const size_t sm = 3 * fast_stage_cap(bs) * sizeof(float2);
     if (bat)
