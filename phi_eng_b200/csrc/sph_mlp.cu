@@ -155,28 +155,39 @@ __global__ void __launch_bounds__(128) k_mlp_forward(const float* __restrict__ x
 // ---------------------------------------------------------------- tcgen05 forward
 // The same network on the 5th-generation tensor cores (sph_tc_net.cuh): one
 // CTA of 128 threads per tile of 128 rows, persistent over the tiles.
+// Row i's 16 features, or the normalisation's mean (a zero input) past n.
+__device__ __forceinline__ void load_features(const float* __restrict__ x, uint32_t i, uint32_t n, const float* mu,
+                                              float (&f)[kFeat]) {
+  if (i < n) {
+    const float4* xi = reinterpret_cast<const float4*>(x + (size_t)i * kFeat);
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const float4 v = xi[q];
+      f[4 * q] = v.x;
+      f[4 * q + 1] = v.y;
+      f[4 * q + 2] = v.z;
+      f[4 * q + 3] = v.w;
+    }
+  } else {
+#pragma unroll
+    for (int q = 0; q < kFeat; q++) f[q] = mu[q];
+  }
+}
+
 __global__ void __launch_bounds__(128) k_mlp_forward_tc(const float* __restrict__ x, uint32_t n, MlpDev mlp,
                                                          float* __restrict__ y, uint32_t* __restrict__ err) {
   extern __shared__ __align__(1024) unsigned char tsm[];
   TcNet net = tc_net_init(tsm, mlp);
   bool ok = true;
-  for (uint32_t base = blockIdx.x * 128u; base < n; base += gridDim.x * 128u) {
+  const uint32_t stride = gridDim.x * 128u;
+  float f[kFeat];
+  load_features(x, blockIdx.x * 128u + threadIdx.x, n, net.norm(), f);
+  for (uint32_t base = blockIdx.x * 128u; base < n; base += stride) {
     const uint32_t i = base + threadIdx.x;
-    float f[kFeat];
-    if (i < n) {
-      const float4* xi = reinterpret_cast<const float4*>(x + (size_t)i * kFeat);
-#pragma unroll
-      for (int q = 0; q < 4; q++) {
-        const float4 v = xi[q];
-        f[4 * q] = v.x;
-        f[4 * q + 1] = v.y;
-        f[4 * q + 2] = v.z;
-        f[4 * q + 3] = v.w;
-      }
-    } else {
-#pragma unroll
-      for (int q = 0; q < kFeat; q++) f[q] = net.norm()[q];  // normalises to zero
-    }
+    // the next tile's features are loaded before this tile's network runs,
+    // so their memory latency overlaps the tensor-core round trips
+    float fn[kFeat];
+    load_features(x, i + stride, n, net.norm(), fn);
     float o[2];
     ok = tc_net_forward(net, f, o);
     if (!ok) break;
@@ -184,6 +195,8 @@ __global__ void __launch_bounds__(128) k_mlp_forward_tc(const float* __restrict_
       y[2 * (size_t)i] = o[0];
       y[2 * (size_t)i + 1] = o[1];
     }
+#pragma unroll
+    for (int q = 0; q < kFeat; q++) f[q] = fn[q];
   }
   tc_net_finish(net, ok, err);
 }
