@@ -272,6 +272,16 @@ int32_t phieng_sph_set_grid(World2* world, uint32_t log2w, uint32_t log2h, int32
  * reference's fluid_dam example, fluid_dam.rs:46-52) into out[0], out[1];
  * reduced on the GPU, 8 bytes copied back. 1 ok, 0 error. Synchronises. */
 int32_t phieng_sph_front_metrics(World2* world, float* out);
+/* The same reduction without waiting: enqueues it and an 8-byte copy of its
+ * raw result into raw[0..1] (host memory, page-locked for the copy to be
+ * asynchronous) on the world's stream, and returns at once. raw must stay
+ * valid until the stream has passed the copy (phieng_sph_sync, or any call
+ * that synchronises: phieng_world_fluid_get). A host that reads a metric
+ * every step can so keep the GPU busy with the next steps meanwhile.
+ * phieng_sph_front_metrics_decode turns raw into (max x, max |v|). 1 ok,
+ * 0 error. No counterpart in the reference. */
+int32_t phieng_sph_front_metrics_async(World2* world, uint32_t* raw);
+void phieng_sph_front_metrics_decode(const uint32_t* raw, float* out);
 
 /* Record CUDA events between the substep phases (sort + ranges, density,
  * force + integrate) of every following substep. 1 ok, 0 error. */

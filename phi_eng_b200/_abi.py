@@ -326,6 +326,8 @@ SIGNATURES = {
     "phieng_sph_replan": (C.c_int32, [_P]),
     "phieng_sph_set_grid": (C.c_int32, [_P, C.c_uint32, C.c_uint32, C.c_int32, C.c_int32]),
     "phieng_sph_front_metrics": (C.c_int32, [_P, _F]),
+    "phieng_sph_front_metrics_async": (C.c_int32, [_P, _P]),
+    "phieng_sph_front_metrics_decode": (None, [_P, _P]),
     "phieng_sph_set_profiling": (C.c_int32, [_P, C.c_int32]),
     "phieng_sph_phase_times": (C.c_uint32, [_P, _F, C.c_uint32]),
     "phieng_sph_batch_new": (_P, [C.POINTER(_P), C.c_uint32]),

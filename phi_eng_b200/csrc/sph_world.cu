@@ -1967,6 +1967,40 @@ int32_t phieng_sph_front_metrics(World2* w, float* out) {
   return 1;
 }
 
+int32_t phieng_sph_front_metrics_async(World2* w, uint32_t* raw) {
+  if (!w || !raw) return 0;
+  if (w->n == 0) {
+    raw[0] = 0u;
+    raw[1] = 0u;
+    return 1;
+  }
+  if (w->host_state_valid) {
+    float m[2];
+    if (!phieng_sph_front_metrics(w, m)) return 0;
+    uint32_t bx, bv;
+    std::memcpy(&bx, &m[0], 4);
+    std::memcpy(&bv, &m[1], 4);
+    raw[0] = (bx & 0x80000000u) ? ~bx : (bx | 0x80000000u);  // the device reduction's order-preserving map
+    raw[1] = bv;
+    return 1;
+  }
+  if (w->device < 0) return 0;
+  enqueue_front_metrics(w->d, w->n, w->stream);
+  return cuda_ok(w, cudaMemcpyAsync(raw, w->d.scalar + 2, 8, cudaMemcpyDeviceToHost, w->stream), "metrics") ? 1 : 0;
+}
+
+void phieng_sph_front_metrics_decode(const uint32_t* raw, float* out) {
+  if (!raw || !out) return;
+  const uint32_t bx = raw[0], bv = raw[1];
+  if (bx == 0u) {
+    out[0] = -INFINITY;
+  } else {
+    const uint32_t ux = (bx & 0x80000000u) ? (bx & 0x7FFFFFFFu) : ~bx;
+    std::memcpy(&out[0], &ux, 4);
+  }
+  std::memcpy(&out[1], &bv, 4);
+}
+
 int32_t phieng_sph_set_tuning(World2* w, const PhiengSphTuning* t) {
   if (!w || !t) return 0;
   auto ok_block = [](uint32_t b) { return b == 64 || b == 128 || b == 256; };

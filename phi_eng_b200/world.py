@@ -284,6 +284,21 @@ class World2:
             self.check()
         return float(out[0]), float(out[1])
 
+    def front_metrics_async(self, raw: np.ndarray) -> None:
+        """Enqueue the front metrics' reduction and an 8-byte copy of its raw
+        result into raw (a uint32 array of 2, page-locked for the copy to be
+        asynchronous) without waiting; decode after the stream has passed it
+        (decode_front_metrics)."""
+        if raw.dtype != np.uint32 or raw.size < 2 or not raw.flags.c_contiguous:
+            raise ValueError("raw must be a contiguous uint32 array of 2")
+        if self._lib.phieng_sph_front_metrics_async(self._h, C.c_void_p(raw.ctypes.data)) != 1:
+            self.check()
+
+    def decode_front_metrics(self, raw: np.ndarray):
+        out = np.zeros(2, np.float32)
+        self._lib.phieng_sph_front_metrics_decode(C.c_void_p(raw.ctypes.data), _fptr(out))
+        return float(out[0]), float(out[1])
+
     def set_profiling(self, on: bool) -> None:
         if self._lib.phieng_sph_set_profiling(self._h, 1 if on else 0) != 1:
             self.check()

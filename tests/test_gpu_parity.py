@@ -444,3 +444,24 @@ def test_forced_tiny_grid_exact(log2):
     g.step(sc.dt, 40)
     o.step(sc.dt, 40)
     assert np.array_equal(g.state(), o.state())
+
+
+def test_front_metrics_async_equal_sync():
+    """phieng_sph_front_metrics_async: the metric of every step copied into
+    its own page-locked slot without waiting equals the synchronous read of
+    the same state."""
+    import torch
+
+    sc = scenes.dam_break_4k()
+    a = sims.load_scene(sims.make("gpu"), sc).w
+    b = sims.load_scene(sims.make("gpu"), sc).w
+    ring = torch.zeros((6, 2), dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
+    want = []
+    for k in range(6):
+        a.step(sc.dt)
+        a.front_metrics_async(ring[k])
+        b.step(sc.dt)
+        want.append(b.front_metrics())
+    a.sync()
+    got = [a.decode_front_metrics(ring[k]) for k in range(6)]
+    assert got == want
