@@ -606,7 +606,34 @@ def _main(argv=None) -> None:
     e.add_argument("--zero", action="store_true", help="evaluate a zero network (no correction)")
     e.add_argument("--ratio", type=int, default=0, help="coarse step = ratio * dt (0: the weights' own ratio)")
     e.add_argument("--precision", choices=["exact", "tolerance"], default="exact")
+    fb = sub.add_parser("forward-bench", help="time the network's forward pass, mma.sync against tcgen05")
+    fb.add_argument("--weights", default=WEIGHTS)
+    fb.add_argument("--rows", default="262144,1048576,4194304")
+    fb.add_argument("--reps", type=int, default=20)
     a = ap.parse_args(argv)
+    if a.cmd == "forward-bench":
+        torch = _torch()
+        mlp = Mlp.load(a.weights)
+        out = []
+        for n in (int(v) for v in a.rows.split(",")):
+            x = torch.randn((n, NFEAT), device="cuda", generator=torch.Generator(device="cuda").manual_seed(n))
+            row = dict(rows=n)
+            for name, f in (("mma_sync_us", mlp.forward), ("tcgen05_us", mlp.forward_tc)):
+                for _ in range(3):
+                    f(x)
+                torch.cuda.synchronize()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                for _ in range(a.reps):
+                    f(x)
+                e1.record()
+                e1.synchronize()
+                row[name] = 1000.0 * e0.elapsed_time(e1) / a.reps
+            if not mlp.check_waits():
+                raise RuntimeError("a tensor-core wait ran out")
+            out.append(row)
+            print(json.dumps(row), flush=True)
+        return
     if a.cmd == "train":
         from .batch import batched_scenes
 
