@@ -11,7 +11,12 @@
 // the SPH step, so this restatement is pinned by (a) the reference's
 // behavioural tests re-run on it (tests/test_behaviour.py), (b) the one
 // bit-pinned arithmetic identity of the reference (linear EOS,
-// fluid.rs:1326-1329), and (c) an FP64 twin that bounds its f32 error.
+// fluid.rs:1326-1329), (c) an FP64 twin that bounds its f32 error, and
+// (d) a second restatement written from the reference's C# solver
+// (oracle/fluid_cs.py, src/PhiEng.Dynamics/FluidSolver.cs), which this one
+// matches bit for bit on the scene of the reference's own C#-vs-Rust
+// equivalence test (tests/PhiEng.Tests/EquivalenceTests.cs:122-176;
+// tests/test_oracle_pin.py).
 //
 // Arithmetic contract: every expression keeps the reference's evaluation
 // order (glam 0.29 Vec2 ops are component-wise IEEE f32; Rust never
