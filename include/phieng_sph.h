@@ -436,6 +436,23 @@ int32_t phieng_mlp_grad(PhiengMlp* mlp, const float* x, const float* t, uint32_t
  * minibatches of `batch` pairs; loss_hist (host, iters values) may be null. */
 int32_t phieng_mlp_train(PhiengMlp* mlp, const float* x, const float* t, uint32_t npairs, uint32_t batch,
                          uint32_t iters, float lr, uint64_t seed, float* loss_hist);
+/* Tensor-core path of phieng_mlp_grad / phieng_mlp_train (default
+ * PHIENG_MLP_TCGEN05). Both draw the
+ * same minibatches and round at the same points (BF16 / FP16 operands, f32
+ * accumulation); their gradients agree within the network's tolerance, not
+ * bit for bit (different accumulation order). Each is bit-reproducible.
+ *   PHIENG_MLP_TCGEN05   5th-generation tensor cores: per 128-sample round
+ *                        the forward layers, dH1 = dZ2 W2 and one weight-
+ *                        gradient GEMM (both hidden layers' weights and
+ *                        biases, accumulated in TMEM over the CTA's rounds)
+ *                        as tcgen05.mma chains; bounded waits, reported
+ *                        like phieng_mlp_check_waits (the call returns 0)
+ *   PHIENG_MLP_MMA_SYNC  warp-level mma.sync m16n8k16 tiles */
+#define PHIENG_MLP_TCGEN05 0
+#define PHIENG_MLP_MMA_SYNC 1
+int32_t phieng_mlp_set_train_engine(PhiengMlp* mlp, int32_t engine);
+/* The current training path (-1 for a null network). */
+int32_t phieng_mlp_get_train_engine(const PhiengMlp* mlp);
 /* The pair indices of one minibatch (device idx[batch]). */
 int32_t phieng_mlp_sample_indices(uint32_t npairs, uint32_t batch, uint64_t seed, uint32_t iter, uint32_t* idx,
                                   void* stream);

@@ -275,6 +275,8 @@ class PhiengSphTuning(C.Structure):
 
 EXACT = 0  # PHIENG_SPH_EXACT: the reference's f32 arithmetic, bit for bit
 TOLERANCE = 1  # PHIENG_SPH_TOLERANCE: reassociated plain passes, within the stated tolerances
+MLP_TCGEN05 = 0  # PHIENG_MLP_TCGEN05: training GEMMs on the 5th-generation tensor cores
+MLP_MMA_SYNC = 1  # PHIENG_MLP_MMA_SYNC: training GEMMs on warp-level mma.sync tiles
 
 MLP_PARAMS = 5378
 MLP_NORM = 34
@@ -352,6 +354,8 @@ SIGNATURES = {
     "phieng_mlp_forward": (C.c_int32, [_P, _P, C.c_uint32, _P]),
     "phieng_mlp_forward_tc": (C.c_int32, [_P, _P, C.c_uint32, _P]),
     "phieng_mlp_check_waits": (C.c_int32, [_P]),
+    "phieng_mlp_set_train_engine": (C.c_int32, [_P, C.c_int32]),
+    "phieng_mlp_get_train_engine": (C.c_int32, [_P]),
     "phieng_mlp_grad": (C.c_int32, [_P, _P, _P, C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint32, _F, _F]),
     "phieng_mlp_train": (C.c_int32, [_P, _P, _P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_float, C.c_uint64, _F]),
     "phieng_mlp_sample_indices": (C.c_int32, [C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint32, _P, _P]),

@@ -136,6 +136,17 @@ class Mlp:
         """True if no bounded tensor-core wait ran out (synchronises)."""
         return self._lib.phieng_mlp_check_waits(self._h) == 1
 
+    @property
+    def train_engine(self) -> str:
+        """Tensor-core path of grad() / train(): "tcgen05" or "mma.sync"."""
+        return "tcgen05" if self._lib.phieng_mlp_get_train_engine(self._h) == _abi.MLP_TCGEN05 else "mma.sync"
+
+    @train_engine.setter
+    def train_engine(self, name: str) -> None:
+        code = {"tcgen05": _abi.MLP_TCGEN05, "mma.sync": _abi.MLP_MMA_SYNC}.get(name)
+        if code is None or self._lib.phieng_mlp_set_train_engine(self._h, code) != 1:
+            raise ValueError(f"training engine {name!r}: 'tcgen05' or 'mma.sync'")
+
     def grad(self, x, t, batch: int, seed: int, it: int):
         self._on_current_stream()
         g = np.zeros(NPARAMS, np.float32)
@@ -360,7 +371,8 @@ def normalisation(X, T, sample: int = 1 << 20, seed: int = 7) -> np.ndarray:
 def train_closure(scs=None, ratio: int = 4, samples: int = 40, every: int = 50, batch: int = 65536,
                   iters: int = 20000, lr: float = 1e-3, seed: int = 0x5EED, noise=(0.0, 0.1),
                   dagger_iters: int = 0, dagger_samples: int = 20, rollout: int = 4, target: str = "damped",
-                  track_rounds: int = 0, track_iters: int = 5000, damp=(0.95, 1.0), log=print):
+                  track_rounds: int = 0, track_iters: int = 5000, damp=(0.95, 1.0), engine: str = "tcgen05",
+                  log=print):
     """Generate pairs on the batched scenes (the 256-scene slice of the batched
     workload by default) and train a network; with dagger_iters > 0, a second
     round adds pairs from the trained closure's own rollouts and continues
@@ -377,6 +389,7 @@ def train_closure(scs=None, ratio: int = 4, samples: int = 40, every: int = 50, 
     torch.cuda.synchronize()
     t1 = time.perf_counter()
     mlp = Mlp(seed)
+    mlp.train_engine = engine
     p, _ = mlp.get()
     nrm = normalisation(X, T)
     mlp.set(p, nrm)
@@ -595,6 +608,7 @@ def _main(argv=None) -> None:
     t.add_argument("--rollout", type=int, default=4)
     t.add_argument("--target", choices=list(TARGETS) + ["damped"], default="damped")
     t.add_argument("--damp", default="0.95,1.0", help="damped target: the range of the pressure damping")
+    t.add_argument("--engine", default="tcgen05", choices=["tcgen05", "mma.sync"], help="training tensor-core path")
     t.add_argument("--track-rounds", type=int, default=0)
     t.add_argument("--ratio", type=int, default=4, help="coarse step = ratio * dt")
     e = sub.add_parser("eval")
@@ -610,7 +624,35 @@ def _main(argv=None) -> None:
     fb.add_argument("--weights", default=WEIGHTS)
     fb.add_argument("--rows", default="262144,1048576,4194304")
     fb.add_argument("--reps", type=int, default=20)
+    tb = sub.add_parser("train-bench", help="time training iterations, mma.sync against tcgen05")
+    tb.add_argument("--pairs", type=int, default=1 << 20)
+    tb.add_argument("--batch", default="8192,65536")
+    tb.add_argument("--iters", type=int, default=200)
     a = ap.parse_args(argv)
+    if a.cmd == "train-bench":
+        torch = _torch()
+        g = torch.Generator(device="cuda").manual_seed(5)
+        x = torch.randn((a.pairs, NFEAT), device="cuda", generator=g)
+        t = torch.randn((a.pairs, 2), device="cuda", generator=g)
+        for b in (int(v) for v in a.batch.split(",")):
+            row = dict(pairs=a.pairs, batch=b, iters=a.iters)
+            grads = {}
+            for eng in ("mma.sync", "tcgen05"):
+                m = Mlp(seed=3)
+                m.train_engine = eng
+                grads[eng] = m.grad(x, t, b, 7, 0)[1]
+                m.train(x, t, batch=b, iters=3, lr=1e-3, seed=9)
+                torch.cuda.synchronize()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                m.train(x, t, batch=b, iters=a.iters, lr=1e-3, seed=9)
+                e1.record()
+                e1.synchronize()
+                row[eng.replace(".", "_") + "_us_per_iter"] = 1000.0 * e0.elapsed_time(e1) / a.iters
+            d = grads["tcgen05"] - grads["mma.sync"]
+            row["grad_rel_diff"] = float(np.linalg.norm(d) / np.linalg.norm(grads["mma.sync"]))
+            print(json.dumps(row), flush=True)
+        return
     if a.cmd == "forward-bench":
         torch = _torch()
         mlp = Mlp.load(a.weights)
@@ -642,7 +684,7 @@ def _main(argv=None) -> None:
                                   batch=a.batch,
                                   iters=a.iters, lr=a.lr, seed=a.seed, noise=noise, dagger_iters=a.dagger_iters,
                                   rollout=a.rollout, target=a.target, track_rounds=a.track_rounds,
-                                  damp=tuple(float(v) for v in a.damp.split(",")), log=None)
+                                  damp=tuple(float(v) for v in a.damp.split(",")), engine=a.engine, log=None)
         os.makedirs(os.path.dirname(os.path.abspath(a.out)), exist_ok=True)
         mlp.save(a.out, **{k: np.asarray(v) for k, v in info.items()})
         print(json.dumps(dict(trained=a.out, **info)))

@@ -3,7 +3,12 @@
 //
 // Training step for a minibatch of B samples drawn from (features, target)
 // pairs, loss L = 1/(2B) sum_b |y_b - t_b / out_scale|^2:
-//   k_mlp_train_tile  each CTA takes B / gridDim samples in rounds of 128:
+//   k_mlp_train_tc    (default) each CTA takes B / gridDim samples in rounds
+//                     of 128 on the 5th-generation tensor cores: forward,
+//                     dH1 and the hidden layers' weight and bias gradients as
+//                     tcgen05.mma chains with TMEM accumulators (the layout
+//                     is described above the kernel).
+//   k_mlp_train_tile  the same on warp-level mma.sync tiles:
 //                     every warp runs forward and backward for 32 samples on
 //                     the tensor cores (activations stay in registers or
 //                     shared memory), then the CTA forms its partial weight
@@ -477,6 +482,341 @@ __global__ void __launch_bounds__(kTrainThreads, 1)
   if (tid == 0) P[kParams] = __fadd_rn(__fadd_rn(wl[0], wl[1]), __fadd_rn(wl[2], wl[3]));
 }
 
+// ---- the training tile on the 5th-generation tensor cores (tcgen05)
+//
+// Same sampling, numerics and partial-gradient layout as k_mlp_train_tile;
+// thread t owns sample row t of each 128-sample round, and every GEMM is one
+// M = 128 tcgen05.mma chain from K-major shared-memory operands (sph_tc.cuh)
+// into f32 TMEM columns:
+//   Z1  [0, 64)     x_hat (W1/2)^T                       K = 16   bf16
+//   Z2  [64, 128)   H1 (W2/2)^T                          K = 64   fp16
+//   Y   [224, 240)  H2 W3pad^T                           K = 64   fp16
+//   dH1 [64, 128)   dZ2 W2 (over Z2, once it is read)    K = 64   bf16
+//   G   [128, 224)  [dZ2^T ; dZ1^T] [H1^T ; x_hat^T ; 1 ; 0]^T   K = 128 samples, bf16,
+//                   accumulated over all rounds of the CTA
+// G's row m < 64 holds dW2[m][:] (columns 0..63) and db2[m] (column 80, the
+// ones row); row 64 + o holds dW1[o][:] (columns 64..79) and db1[o] (column
+// 80); the two off-diagonal blocks are unused. dW3 and db3 are f32 sums in
+// sample order from dY and the FP16 H2 tile.
+constexpr uint32_t kTrW1 = 0;                       // W1 / 2   [64][16]  bf16
+constexpr uint32_t kTrW2 = kTrW1 + 64 * 16 * 2;     // W2 / 2   [64][64]  fp16
+constexpr uint32_t kTrW3 = kTrW2 + 64 * 64 * 2;     // W3       [16][64]  fp16 (rows 2..15 zero)
+constexpr uint32_t kTrW2T = kTrW3 + 16 * 64 * 2;    // W2^T     [64][64]  bf16 (row = layer-1 unit)
+constexpr uint32_t kTrX = kTrW2T + 64 * 64 * 2;     // x_hat    [128][16] bf16
+constexpr uint32_t kTrA = kTrX + 128 * 16 * 2;      // H1, H2 (fp16), then dZ2 (bf16) [128][64]
+constexpr uint32_t kTrGA = kTrA + 128 * 64 * 2;     // [dZ2^T ; dZ1^T]              [128][128] bf16
+constexpr uint32_t kTrGB = kTrGA + 128 * 128 * 2;   // [H1^T ; x_hat^T ; 1 ; 0]     [96][128]  bf16
+constexpr uint32_t kTrBias = kTrGB + 96 * 128 * 2;  // b1/2 | b2/2 | b3 (f32)
+constexpr uint32_t kTrNorm = kTrBias + 4 * 256;     // mu | isd | out_scale
+constexpr uint32_t kTrW3f = kTrNorm + 4 * 64;       // W3 (FP16-rounded) as f32 [2][64]
+constexpr uint32_t kTrTgt = kTrW3f + 4 * 128;       // targets / out_scale [128][2]
+constexpr uint32_t kTrDy = kTrTgt + 4 * 256;        // dL/dy [128][2]
+constexpr uint32_t kTrLoss = kTrDy + 4 * 256;       // per-warp loss [4]
+constexpr uint32_t kTrBar = kTrLoss + 16;           // mbarrier
+constexpr uint32_t kTrSlot = kTrBar + 8;            // TMEM address
+constexpr uint32_t kTrSmem = kTrSlot + 8;           // ~100 KB: two CTAs per SM
+constexpr uint32_t kTrCols = 256;                   // two CTAs per SM use all 512 columns
+constexpr uint32_t kColZ1 = 0, kColZ2 = 64, kColG = 128, kColY = 224;
+constexpr uint32_t kGradN = 96;
+constexpr uint32_t kTrWaitLimit = 1u << 20;
+static_assert(kTrSmem % 16 == 0 && kTrBar % 8 == 0, "shared-memory layout");
+
+// 16-bit element (row, col) of a K-major operand with 128 columns (col = sample).
+__device__ __forceinline__ void st_t16(unsigned char* m, uint32_t row, uint32_t col, uint32_t v) {
+  *reinterpret_cast<uint16_t*>(m + tc::kmajor_offset(row, col, 128)) = (uint16_t)v;
+}
+
+__global__ void __launch_bounds__(kTrainThreads, 1)
+    k_mlp_train_tc(const float* __restrict__ x, const float* __restrict__ tg, uint32_t npairs, uint32_t batch,
+                   uint32_t rounds, uint64_t seed, const uint32_t* __restrict__ iter_ptr, MlpDev mlp,
+                   float* __restrict__ part, uint32_t* __restrict__ err) {
+  extern __shared__ __align__(1024) unsigned char tsm[];
+  const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const __nv_bfloat16* img = reinterpret_cast<const __nv_bfloat16*>(mlp.frag);
+  const __half* himg = reinterpret_cast<const __half*>(mlp.frag);
+  for (uint32_t i = tid; i < 64 * 16; i += kTrainThreads) {
+    const uint32_t o = i >> 4, k = i & 15;
+    *reinterpret_cast<__nv_bfloat16*>(tsm + kTrW1 + tc::kmajor_offset(o, k, 16)) = img[frag_pos(k, o, 8)];
+  }
+  for (uint32_t i = tid; i < 64 * 64; i += kTrainThreads) {
+    const uint32_t o = i >> 6, k = i & 63;
+    *reinterpret_cast<__half*>(tsm + kTrW2 + tc::kmajor_offset(o, k, 64)) = himg[4 * kF1 + frag_pos(k, o, 8)];
+    // W2^T row o (a layer-1 unit), column k (a layer-2 unit) = W2[k][o], from F2T
+    *reinterpret_cast<__nv_bfloat16*>(tsm + kTrW2T + tc::kmajor_offset(o, k, 64)) =
+        img[4 * (kF1 + kF2 + kF3) + frag_pos(k, o, 8)];
+  }
+  for (uint32_t i = tid; i < 16 * 64; i += kTrainThreads) {
+    const uint32_t o = i >> 6, k = i & 63;
+    *reinterpret_cast<__half*>(tsm + kTrW3 + tc::kmajor_offset(o, k, 64)) =
+        o < 2 ? himg[4 * (kF1 + kF2) + frag_pos(k, o, 1)] : __float2half_rn(0.0f);
+  }
+  unsigned char* X = tsm + kTrX;
+  unsigned char* A = tsm + kTrA;
+  unsigned char* GA = tsm + kTrGA;
+  unsigned char* GB = tsm + kTrGB;
+  // rows 80..95 of G's B operand: ones (the bias gradients), then zeros
+  for (uint32_t i = tid; i < 16 * kTileRows; i += kTrainThreads) {
+    const uint32_t row = 80 + (i >> 7);
+    st_t16(GB, row, i & 127, row == 80 ? 0x3F80u : 0u);  // bf16 1.0 / 0.0
+  }
+  float* bias = reinterpret_cast<float*>(tsm + kTrBias);
+  float* norm = reinterpret_cast<float*>(tsm + kTrNorm);
+  float* w3f = reinterpret_cast<float*>(tsm + kTrW3f);
+  float* tgt = reinterpret_cast<float*>(tsm + kTrTgt);
+  float* dy = reinterpret_cast<float*>(tsm + kTrDy);
+  float* wl = reinterpret_cast<float*>(tsm + kTrLoss);
+  for (uint32_t i = tid; i < kBias; i += kTrainThreads) bias[i] = mlp.bias[i];
+  for (uint32_t i = tid; i < kNorm; i += kTrainThreads) norm[i] = mlp.norm[i];
+  for (uint32_t i = tid; i < kOut * kHidden; i += kTrainThreads) w3f[i] = mlp.w3[i];
+  uint64_t* bar = reinterpret_cast<uint64_t*>(tsm + kTrBar);
+  uint32_t* slot = reinterpret_cast<uint32_t*>(tsm + kTrSlot);
+  if (tid == 0) tc::mbar_init(bar, 1);
+  if (warp == 0) tc::tmem_alloc(slot, kTrCols);
+  tc::fence_async_smem();
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tm = *slot, lanes = (warp * 32u) << 16;
+  uint32_t phase = 0;
+  const uint32_t iter = *iter_ptr;
+  const float inv_b = __fdiv_rn(1.0f, (float)batch);
+  const float inv_os0 = __fdiv_rn(1.0f, norm[2 * kFeat]), inv_os1 = __fdiv_rn(1.0f, norm[2 * kFeat + 1]);
+  const uint32_t aX = tc::smem_u32(X), aA = tc::smem_u32(A), aGA = tc::smem_u32(GA), aGB = tc::smem_u32(GB);
+  const uint32_t aW1 = tc::smem_u32(tsm + kTrW1), aW2 = tc::smem_u32(tsm + kTrW2), aW3 = tc::smem_u32(tsm + kTrW3),
+                 aW2T = tc::smem_u32(tsm + kTrW2T);
+
+  float acc_w3 = 0.0f, acc_b3 = 0.0f, loss = 0.0f;
+  bool ok = true;
+  for (uint32_t r = 0; r < rounds; r++) {
+    // ---- sample row tid: x_hat into X (row) and GB rows 64..79 (column), scaled target
+    {
+      const uint32_t k = (blockIdx.x * rounds + r) * kTileRows + tid;
+      const uint32_t idx = sample_index(seed, iter, k, npairs);
+      const float4* xi = reinterpret_cast<const float4*>(x + (size_t)idx * kFeat);
+      float f[kFeat];
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const float4 v = xi[q];
+        f[4 * q] = v.x;
+        f[4 * q + 1] = v.y;
+        f[4 * q + 2] = v.z;
+        f[4 * q + 3] = v.w;
+      }
+      uint32_t xp[8];
+#pragma unroll
+      for (int q = 0; q < 8; q++)
+        xp[q] = pack_bf16(__fmul_rn(__fsub_rn(f[2 * q], norm[2 * q]), norm[kFeat + 2 * q]),
+                          __fmul_rn(__fsub_rn(f[2 * q + 1], norm[2 * q + 1]), norm[kFeat + 2 * q + 1]));
+      *reinterpret_cast<uint4*>(X + tc::kmajor_offset(tid, 0, 16)) = make_uint4(xp[0], xp[1], xp[2], xp[3]);
+      *reinterpret_cast<uint4*>(X + tc::kmajor_offset(tid, 8, 16)) = make_uint4(xp[4], xp[5], xp[6], xp[7]);
+#pragma unroll
+      for (int q = 0; q < 8; q++) {
+        st_t16(GB, 64 + 2 * q, tid, xp[q] & 0xFFFFu);
+        st_t16(GB, 65 + 2 * q, tid, xp[q] >> 16);
+      }
+      tgt[2 * tid] = __fmul_rn(tg[2 * (size_t)idx], inv_os0);
+      tgt[2 * tid + 1] = __fmul_rn(tg[2 * (size_t)idx + 1], inv_os1);
+    }
+    // ---- layer 1
+    ok = tc::mma_step(bar, phase, kTrWaitLimit, [&] {
+      tc::mma_f16(tm + kColZ1, tc::smem_desc(aX, 128, 256), tc::smem_desc(aW1, 128, 256),
+                  tc::idesc_f16(tc::kFmtBF16, 64), 0u);
+    });
+    if (!ok) break;
+    // H1 = silu(z1): row tid of A (fp16) and column tid of GB rows 0..63 (bf16)
+#pragma unroll
+    for (int half = 0; half < 2; half++) {
+      float v[2][16];
+#pragma unroll
+      for (int q = 0; q < 2; q++) tc::tmem_ld16(tm + lanes + kColZ1 + 32 * half + 16 * q, v[q]);
+      tc::tmem_wait_ld();
+#pragma unroll
+      for (int q = 0; q < 2; q++) {
+        const int c = 32 * half + 16 * q;
+        uint32_t hp[8];
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+          hp[j] = silu_half_f16x2(__fadd_rn(v[q][2 * j], bias[c + 2 * j]), __fadd_rn(v[q][2 * j + 1], bias[c + 2 * j + 1]));
+          const uint32_t b = f16x2_to_bf16x2(hp[j]);
+          st_t16(GB, c + 2 * j, tid, b & 0xFFFFu);
+          st_t16(GB, c + 2 * j + 1, tid, b >> 16);
+        }
+        *reinterpret_cast<uint4*>(A + tc::kmajor_offset(tid, c, 64)) = make_uint4(hp[0], hp[1], hp[2], hp[3]);
+        *reinterpret_cast<uint4*>(A + tc::kmajor_offset(tid, c + 8, 64)) = make_uint4(hp[4], hp[5], hp[6], hp[7]);
+      }
+    }
+    // ---- layer 2
+    ok = tc::mma_step(bar, phase, kTrWaitLimit, [&] {
+#pragma unroll
+      for (uint32_t kk = 0; kk < 4; kk++)
+        tc::mma_f16(tm + kColZ2, tc::smem_desc(aA + 256 * kk, 128, 1024), tc::smem_desc(aW2 + 256 * kk, 128, 1024),
+                    tc::idesc_f16(tc::kFmtF16, 64), kk);
+    });
+    if (!ok) break;
+    // H2 = silu(z2): row tid of A (fp16)
+#pragma unroll
+    for (int half = 0; half < 2; half++) {
+      float v[2][16];
+#pragma unroll
+      for (int q = 0; q < 2; q++) tc::tmem_ld16(tm + lanes + kColZ2 + 32 * half + 16 * q, v[q]);
+      tc::tmem_wait_ld();
+#pragma unroll
+      for (int q = 0; q < 2; q++) {
+        const int c = 32 * half + 16 * q;
+        const float* b = bias + kHidden + c;
+        uint32_t hp[8];
+#pragma unroll
+        for (int j = 0; j < 8; j++)
+          hp[j] = silu_half_f16x2(__fadd_rn(v[q][2 * j], b[2 * j]), __fadd_rn(v[q][2 * j + 1], b[2 * j + 1]));
+        *reinterpret_cast<uint4*>(A + tc::kmajor_offset(tid, c, 64)) = make_uint4(hp[0], hp[1], hp[2], hp[3]);
+        *reinterpret_cast<uint4*>(A + tc::kmajor_offset(tid, c + 8, 64)) = make_uint4(hp[4], hp[5], hp[6], hp[7]);
+      }
+    }
+    // ---- layer 3, loss and dY = (y - t) / B
+    ok = tc::mma_step(bar, phase, kTrWaitLimit, [&] {
+#pragma unroll
+      for (uint32_t kk = 0; kk < 4; kk++)
+        tc::mma_f16(tm + kColY, tc::smem_desc(aA + 256 * kk, 128, 1024), tc::smem_desc(aW3 + 256 * kk, 128, 1024),
+                    tc::idesc_f16(tc::kFmtF16, 16), kk);
+    });
+    if (!ok) break;
+    {
+      float o[2];
+      tc::tmem_ld2(tm + lanes + kColY, o);
+      tc::tmem_wait_ld();
+      const float e0 = __fsub_rn(__fadd_rn(o[0], bias[2 * kHidden]), tgt[2 * tid]);
+      const float e1 = __fsub_rn(__fadd_rn(o[1], bias[2 * kHidden + 1]), tgt[2 * tid + 1]);
+      loss = __fadd_rn(loss, __fadd_rn(__fmul_rn(e0, e0), __fmul_rn(e1, e1)));
+      dy[2 * tid] = __fmul_rn(e0, inv_b);
+      dy[2 * tid + 1] = __fmul_rn(e1, inv_b);
+    }
+    __syncthreads();
+    // ---- dW3[o][n] = sum_k dY[k][o] H2[k][n] and db3 (f32, sample order; H2 from A)
+    {
+      const uint32_t o = tid >> 6, n = tid & 63;
+      for (uint32_t kk = 0; kk < kTileRows; kk++)
+        acc_w3 = __fadd_rn(acc_w3, __fmul_rn(dy[2 * kk + o],
+                                             __half2float(*reinterpret_cast<const __half*>(A + tc::kmajor_offset(kk, n, 64)))));
+      if (tid < kOut)
+        for (uint32_t kk = 0; kk < kTileRows; kk++) acc_b3 = __fadd_rn(acc_b3, dy[2 * kk + tid]);
+    }
+    __syncthreads();
+    // ---- dZ2 = (dY W3) silu'(z2): row tid of A (bf16) and column tid of GA rows 0..63
+    {
+      const float dy0 = dy[2 * tid], dy1 = dy[2 * tid + 1];
+#pragma unroll
+      for (int half = 0; half < 2; half++) {
+        float v[2][16];
+#pragma unroll
+        for (int q = 0; q < 2; q++) tc::tmem_ld16(tm + lanes + kColZ2 + 32 * half + 16 * q, v[q]);
+        tc::tmem_wait_ld();
+#pragma unroll
+        for (int q = 0; q < 2; q++) {
+          const int c = 32 * half + 16 * q;
+          uint32_t dp[8];
+#pragma unroll
+          for (int j = 0; j < 8; j++) {
+            const int c0 = c + 2 * j;
+            const float d0 = __fmul_rn(__fadd_rn(__fmul_rn(dy0, w3f[c0]), __fmul_rn(dy1, w3f[kHidden + c0])),
+                                       dsilu_half(__fadd_rn(v[q][2 * j], bias[kHidden + c0])));
+            const float d1 = __fmul_rn(__fadd_rn(__fmul_rn(dy0, w3f[c0 + 1]), __fmul_rn(dy1, w3f[kHidden + c0 + 1])),
+                                       dsilu_half(__fadd_rn(v[q][2 * j + 1], bias[kHidden + c0 + 1])));
+            dp[j] = pack_bf16(d0, d1);
+            st_t16(GA, c0, tid, dp[j] & 0xFFFFu);
+            st_t16(GA, c0 + 1, tid, dp[j] >> 16);
+          }
+          *reinterpret_cast<uint4*>(A + tc::kmajor_offset(tid, c, 64)) = make_uint4(dp[0], dp[1], dp[2], dp[3]);
+          *reinterpret_cast<uint4*>(A + tc::kmajor_offset(tid, c + 8, 64)) = make_uint4(dp[4], dp[5], dp[6], dp[7]);
+        }
+      }
+    }
+    // ---- dH1 = dZ2 W2 (over Z2, which every thread has read)
+    ok = tc::mma_step(bar, phase, kTrWaitLimit, [&] {
+#pragma unroll
+      for (uint32_t kk = 0; kk < 4; kk++)
+        tc::mma_f16(tm + kColZ2, tc::smem_desc(aA + 256 * kk, 128, 1024), tc::smem_desc(aW2T + 256 * kk, 128, 1024),
+                    tc::idesc_f16(tc::kFmtBF16, 64), kk);
+    });
+    if (!ok) break;
+    // ---- dZ1 = dH1 silu'(z1): column tid of GA rows 64..127
+#pragma unroll
+    for (int half = 0; half < 2; half++) {
+      float v[2][16], z[2][16];
+#pragma unroll
+      for (int q = 0; q < 2; q++) {
+        tc::tmem_ld16(tm + lanes + kColZ2 + 32 * half + 16 * q, v[q]);
+        tc::tmem_ld16(tm + lanes + kColZ1 + 32 * half + 16 * q, z[q]);
+      }
+      tc::tmem_wait_ld();
+#pragma unroll
+      for (int q = 0; q < 2; q++) {
+        const int c = 32 * half + 16 * q;
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+          const int c0 = c + 2 * j;
+          const float d0 = __fmul_rn(v[q][2 * j], dsilu_half(__fadd_rn(z[q][2 * j], bias[c0])));
+          const float d1 = __fmul_rn(v[q][2 * j + 1], dsilu_half(__fadd_rn(z[q][2 * j + 1], bias[c0 + 1])));
+          const uint32_t p = pack_bf16(d0, d1);
+          st_t16(GA, 64 + c0, tid, p & 0xFFFFu);
+          st_t16(GA, 65 + c0, tid, p >> 16);
+        }
+      }
+    }
+    // ---- G (+)= GA GB^T over this round's 128 samples; the next round's
+    // operand writes wait for it
+    ok = tc::mma_step(bar, phase, kTrWaitLimit, [&] {
+#pragma unroll
+      for (uint32_t kk = 0; kk < kTileRows / 16; kk++)
+        tc::mma_f16(tm + kColG, tc::smem_desc(aGA + 256 * kk, 128, 2048), tc::smem_desc(aGB + 256 * kk, 128, 2048),
+                    tc::idesc_f16(tc::kFmtBF16, kGradN), (r | kk) != 0u ? 1u : 0u);
+    });
+    if (!ok) break;
+  }
+
+  // ---- this CTA's partial gradient
+  float* P = part + (size_t)blockIdx.x * kPartStride;
+  if (ok) {
+    float g[16];
+    if (warp < 2) {
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        tc::tmem_ld16(tm + lanes + kColG + 16 * q, g);
+        tc::tmem_wait_ld();
+#pragma unroll
+        for (int j = 0; j < 16; j++) P[kOffW2 + tid * kHidden + 16 * q + j] = g[j];
+      }
+    } else {
+      tc::tmem_ld16(tm + lanes + kColG + 64, g);
+      tc::tmem_wait_ld();
+#pragma unroll
+      for (int j = 0; j < 16; j++) P[kOffW1 + (tid - 64) * kFeat + j] = g[j];
+    }
+    tc::tmem_ld16(tm + lanes + kColG + 80, g);
+    tc::tmem_wait_ld();
+    if (warp < 2)
+      P[kOffB2 + tid] = g[0];
+    else
+      P[kOffB1 + tid - 64] = g[0];
+  }
+  P[kOffW3 + tid] = acc_w3;
+  if (tid < kOut) P[kOffB3 + tid] = acc_b3;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) loss = __fadd_rn(loss, __shfl_xor_sync(0xFFFFFFFFu, loss, o));
+  if (lane == 0) wl[warp] = loss;
+  __syncthreads();
+  if (tid == 0) P[kParams] = __fadd_rn(__fadd_rn(wl[0], wl[1]), __fadd_rn(wl[2], wl[3]));
+  if (!ok) {
+    if (tid == 0) atomicExch(err, 1u);
+    tc::mbar_wait(bar, phase, kTrWaitLimit);
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) {
+    tc::fence_after_sync();
+    tc::tmem_free(tm, kTrCols);
+  }
+}
+
 // Sum of the CTA partials (CTA order) per parameter.
 __device__ __forceinline__ float sum_parts(const float* __restrict__ part, uint32_t nparts, int p) {
   float g = 0.0f;
@@ -598,6 +938,7 @@ struct PhiengMlp {
   float* loss_hist = nullptr;
   uint32_t loss_cap = 0;
   float* h_pinned = nullptr;
+  int32_t train_engine = PHIENG_MLP_TCGEN05;
 };
 
 namespace {
@@ -628,6 +969,16 @@ bool sync_images(PhiengMlp* m) {
   return mlp_ok(m, cudaGetLastError());
 }
 
+// After a stream synchronisation: fail (and poison the network) if a bounded
+// tensor-core wait of any tcgen05 kernel of this network ran out.
+bool waits_clean(PhiengMlp* m) {
+  uint32_t e = 0;
+  if (!mlp_ok(m, cudaMemcpy(&e, m->ctr + 2, 4, cudaMemcpyDeviceToHost))) return false;
+  if (e == 0) return true;
+  if (m->error == PHIENG_SPH_OK) m->error = PHIENG_SPH_E_CUDA;
+  return false;
+}
+
 bool check_pairs(const float* x, const float* t, uint32_t npairs, uint32_t batch) {
   return x && t && npairs > 0 && batch > 0 && batch % kTileRows == 0;
 }
@@ -638,8 +989,12 @@ bool launch_tile(PhiengMlp* m, const float* x, const float* t, uint32_t npairs, 
   mlp_grid(batch, &ctas, &rounds);
   if (!ensure_parts(m, ctas)) return false;
   MlpDev d = phieng_mlp_dev(m);
-  k_mlp_train_tile<<<ctas, kTrainThreads, sizeof(TrainSmem), m->stream>>>(x, t, npairs, batch, rounds, seed, iter_ptr,
-                                                                          d, m->part);
+  if (m->train_engine == PHIENG_MLP_TCGEN05)
+    k_mlp_train_tc<<<ctas, kTrainThreads, kTrSmem, m->stream>>>(x, t, npairs, batch, rounds, seed, iter_ptr, d,
+                                                                 m->part, m->ctr + 2);
+  else
+    k_mlp_train_tile<<<ctas, kTrainThreads, sizeof(TrainSmem), m->stream>>>(x, t, npairs, batch, rounds, seed,
+                                                                            iter_ptr, d, m->part);
   *nparts_out = ctas;
   return mlp_ok(m, cudaGetLastError());
 }
@@ -678,7 +1033,8 @@ PhiengMlp* phieng_mlp_new(uint64_t seed) {
   if (!mlp_ok(m, cudaMallocHost(reinterpret_cast<void**>(&m->h_pinned), sizeof(float) * (kParams + kNorm + 4))))
     return m;
   if (!mlp_ok(m, cudaFuncSetAttribute(k_mlp_train_tile, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)sizeof(TrainSmem))))
+                                      (int)sizeof(TrainSmem))) ||
+      !mlp_ok(m, cudaFuncSetAttribute(k_mlp_train_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrSmem)))
     return m;
   // Linear-layer initialisation U(-1/sqrt(fan_in), 1/sqrt(fan_in)) from
   // SplitMix64(seed); the output layer starts at zero (no correction).
@@ -803,7 +1159,7 @@ int32_t phieng_mlp_grad(PhiengMlp* m, const float* x, const float* t, uint32_t n
   if (!mlp_ok(m, cudaGetLastError())) return 0;
   if (!mlp_ok(m, cudaMemcpyAsync(m->h_pinned, m->grad, sizeof(float) * (kParams + 1), cudaMemcpyDeviceToHost,
                                  m->stream)) ||
-      !mlp_ok(m, cudaStreamSynchronize(m->stream)))
+      !mlp_ok(m, cudaStreamSynchronize(m->stream)) || !waits_clean(m))
     return 0;
   if (grad_host) std::memcpy(grad_host, m->h_pinned, sizeof(float) * kParams);
   if (loss_host) *loss_host = m->h_pinned[kParams];
@@ -872,9 +1228,17 @@ int32_t phieng_mlp_train(PhiengMlp* m, const float* x, const float* t, uint32_t 
   if (ok && loss_hist_host)
     ok = mlp_ok(m, cudaMemcpyAsync(loss_hist_host, m->loss_hist, sizeof(float) * iters, cudaMemcpyDeviceToHost,
                                    m->stream));
-  if (ok) ok = mlp_ok(m, cudaStreamSynchronize(m->stream));
+  if (ok) ok = mlp_ok(m, cudaStreamSynchronize(m->stream)) && waits_clean(m);
   return ok ? 1 : 0;
 }
+
+int32_t phieng_mlp_set_train_engine(PhiengMlp* m, int32_t engine) {
+  if (!m || m->error || (engine != PHIENG_MLP_TCGEN05 && engine != PHIENG_MLP_MMA_SYNC)) return 0;
+  m->train_engine = engine;
+  return 1;
+}
+
+int32_t phieng_mlp_get_train_engine(const PhiengMlp* m) { return m ? m->train_engine : -1; }
 
 int32_t phieng_mlp_sample_indices(uint32_t npairs, uint32_t batch, uint64_t seed, uint32_t iter, uint32_t* idx,
                                   void* stream) {

@@ -133,5 +133,28 @@ __host__ __device__ constexpr uint32_t kmajor_offset(uint32_t row, uint32_t k, u
   return (row >> 3) * (kcols * 16u) + (k >> 3) * 128u + (row & 7u) * 16u + (k & 7u) * 2u;
 }
 
+// One CTA-wide MMA step: every thread's operand writes (generic proxy) are
+// made visible to the tensor core, thread 0 issues `issue` and commits to
+// `bar`, and every thread waits for the completion (at most `limit` polls).
+// The caller's TMEM reads must have completed (tmem_wait_ld) before. Returns
+// false for every thread if the wait ran out; `phase` then stays at the
+// incomplete phase.
+template <class F>
+__device__ __forceinline__ bool mma_step(uint64_t* bar, uint32_t& phase, uint32_t limit, F&& issue) {
+  fence_async_smem();
+  fence_before_sync();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    fence_after_sync();
+    issue();
+    commit(bar);
+  }
+  const bool done = mbar_wait(bar, phase, limit);
+  if (__syncthreads_or(!done)) return false;
+  phase ^= 1u;
+  fence_after_sync();
+  return true;
+}
+
 }  // namespace tc
 }  // namespace phieng

@@ -95,19 +95,7 @@ __device__ __forceinline__ TcNet tc_net_init(unsigned char* sm, const MlpDev& ml
 // out; the phase is then left at the incomplete one.
 template <class F>
 __device__ __forceinline__ bool tc_net_layer(TcNet& net, F&& issue) {
-  tc::fence_async_smem();
-  tc::fence_before_sync();
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    tc::fence_after_sync();
-    issue();
-    tc::commit(net.bar());
-  }
-  const bool done = tc::mbar_wait(net.bar(), net.phase, kNetWaitLimit);
-  if (__syncthreads_or(!done)) return false;
-  net.phase ^= 1u;
-  tc::fence_after_sync();
-  return true;
+  return tc::mma_step(net.bar(), net.phase, kNetWaitLimit, issue);
 }
 
 // Hidden-layer epilogue: TMEM columns [0, 64) of this thread's row plus the

@@ -278,14 +278,20 @@ def test_mlp_forward_tcgen05_matches_oracle_and_mma_sync(n):
         assert np.isfinite(y_tc).all()
 
 
+ENGINES = ["mma.sync", "tcgen05"]
+
+
 @pytest.mark.gpu
-def test_mlp_gradient_matches_oracle():
+@pytest.mark.parametrize("engine", ENGINES)
+def test_mlp_gradient_matches_oracle(engine):
     from phi_eng_b200.closure import Mlp
 
     torch = _torch()
     rng = np.random.default_rng(6)
     p, norm = _random_net(rng)
     m = Mlp()
+    m.train_engine = engine
+    assert m.train_engine == engine
     m.set(p, norm)
     npairs, batch, seed, it = 50000, 4096, 0xABC, 3
     x = rng.standard_normal((npairs, 16)).astype(np.float32)
@@ -302,7 +308,46 @@ def test_mlp_gradient_matches_oracle():
 
 
 @pytest.mark.gpu
-def test_adam_step_exact_and_training_deterministic():
+@pytest.mark.parametrize("batch", [128, 1024, 65536])
+def test_training_engines_agree(batch):
+    """The tcgen05 and mma.sync training tiles compute the same gradient of
+    the same minibatch (one round per CTA at 128 and 1024 samples; several
+    rounds accumulated in TMEM at 65536) within the network's tolerance."""
+    from phi_eng_b200.closure import Mlp
+
+    torch = _torch()
+    rng = np.random.default_rng(9)
+    p, norm = _random_net(rng)
+    npairs = 100000
+    x = torch.from_numpy(rng.standard_normal((npairs, 16)).astype(np.float32)).cuda()
+    t = torch.from_numpy(rng.standard_normal((npairs, 2)).astype(np.float32)).cuda()
+    out = {}
+    for eng in ENGINES:
+        m = Mlp()
+        m.train_engine = eng
+        m.set(p, norm)
+        out[eng] = m.grad(x, t, batch, 0x51, 2)
+        assert m.check_waits()
+    (la, ga), (lb, gb) = out["mma.sync"], out["tcgen05"]
+    assert abs(la - lb) / la < 1e-3
+    blocks = [(mo.OFF_W1, mo.OFF_B1), (mo.OFF_B1, mo.OFF_W2), (mo.OFF_W2, mo.OFF_B2), (mo.OFF_B2, mo.OFF_W3),
+              (mo.OFF_W3, mo.OFF_B3), (mo.OFF_B3, mo.NPARAMS)]
+    for a, b in blocks:
+        assert np.linalg.norm(gb[a:b] - ga[a:b]) / np.linalg.norm(ga[a:b]) < GRAD_TOL, (a, b)
+
+
+@pytest.mark.gpu
+def test_training_engine_rejects_unknown():
+    from phi_eng_b200.closure import Mlp
+
+    m = Mlp()
+    with pytest.raises(ValueError):
+        m.train_engine = "wmma"
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("engine", ENGINES)
+def test_adam_step_exact_and_training_deterministic(engine):
     from phi_eng_b200.closure import Mlp
 
     torch = _torch()
@@ -312,6 +357,7 @@ def test_adam_step_exact_and_training_deterministic():
     x = torch.from_numpy(rng.standard_normal((npairs, 16)).astype(np.float32)).cuda()
     t = torch.from_numpy(rng.standard_normal((npairs, 2)).astype(np.float32)).cuda()
     m = Mlp()
+    m.train_engine = engine
     m.set(p, norm)
     _, g = m.grad(x, t, batch, seed, 0)
     m.train(x, t, batch=batch, iters=1, lr=1e-3, seed=seed)
@@ -327,6 +373,7 @@ def test_adam_step_exact_and_training_deterministic():
     runs = []
     for _ in range(2):
         mm_ = Mlp()
+        mm_.train_engine = engine
         mm_.set(p, norm)
         hist = mm_.train(x, t, batch=batch, iters=50, lr=1e-3, seed=seed)
         runs.append((mm_.get()[0], hist))
@@ -335,7 +382,8 @@ def test_adam_step_exact_and_training_deterministic():
 
 
 @pytest.mark.gpu
-def test_training_fits_a_smooth_map():
+@pytest.mark.parametrize("engine", ENGINES)
+def test_training_fits_a_smooth_map(engine):
     """The training kernels learn: a smooth nonlinear map of the inputs is fit
     to a small fraction of its variance."""
     from phi_eng_b200.closure import Mlp
@@ -347,6 +395,7 @@ def test_training_fits_a_smooth_map():
     t = np.stack([np.tanh(x[:, 0] + 0.5 * x[:, 1]) * x[:, 2], np.sin(x[:, 3]) - 0.3 * x[:, 4] * x[:, 5]], 1)
     t = t.astype(np.float32)
     m = Mlp(seed=3)
+    m.train_engine = engine
     p, nrm = m.get()
     nrm[32:] = t.std(0)
     m.set(p, nrm)
