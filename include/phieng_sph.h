@@ -436,6 +436,20 @@ int32_t phieng_mlp_grad(PhiengMlp* mlp, const float* x, const float* t, uint32_t
  * minibatches of `batch` pairs; loss_hist (host, iters values) may be null. */
 int32_t phieng_mlp_train(PhiengMlp* mlp, const float* x, const float* t, uint32_t npairs, uint32_t batch,
                          uint32_t iters, float lr, uint64_t seed, float* loss_hist);
+/* Data-parallel training, one rank's share of an iteration (asynchronous on
+ * the network's stream; x, t, grad on the device): grad[PHIENG_MLP_PARAMS + 1]
+ * = the gradient over samples [first, first + batch) of the total-sample
+ * minibatch that Adam step phieng_mlp_step_count() draws with `seed` (the
+ * sampling of phieng_mlp_train; each sample's dL/dy carries 1 / total), then
+ * those samples' sum of squared errors. Summed over ranks whose slices tile
+ * [0, total) (an all-reduce), it is the minibatch gradient, and the loss is
+ * the last entry / (2 total). batch a multiple of 128, first + batch <= total. */
+int32_t phieng_mlp_shard_grad(PhiengMlp* mlp, const float* x, const float* t, uint32_t npairs, uint32_t first,
+                              uint32_t batch, uint32_t total, uint64_t seed, float* grad);
+/* One Adam step (as phieng_mlp_train's) from a device gradient laid out as
+ * phieng_mlp_shard_grad writes it; asynchronous. Ranks that apply the same
+ * all-reduced gradient keep bit-identical parameters. */
+int32_t phieng_mlp_apply_grad(PhiengMlp* mlp, const float* grad, float lr);
 /* Tensor-core path of phieng_mlp_grad / phieng_mlp_train (default
  * PHIENG_MLP_TCGEN05). Both draw the
  * same minibatches and round at the same points (BF16 / FP16 operands, f32

@@ -355,6 +355,9 @@ SIGNATURES = {
     "phieng_mlp_forward_tc": (C.c_int32, [_P, _P, C.c_uint32, _P]),
     "phieng_mlp_check_waits": (C.c_int32, [_P]),
     "phieng_mlp_set_train_engine": (C.c_int32, [_P, C.c_int32]),
+    "phieng_mlp_shard_grad": (C.c_int32, [_P, _P, _P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64,
+                                          _P]),
+    "phieng_mlp_apply_grad": (C.c_int32, [_P, _P, C.c_float]),
     "phieng_mlp_get_train_engine": (C.c_int32, [_P]),
     "phieng_mlp_grad": (C.c_int32, [_P, _P, _P, C.c_uint32, C.c_uint32, C.c_uint64, C.c_uint32, _F, _F]),
     "phieng_mlp_train": (C.c_int32, [_P, _P, _P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_float, C.c_uint64, _F]),

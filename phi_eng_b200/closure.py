@@ -167,6 +167,58 @@ class Mlp:
         return hist
 
 
+    def shard_grad(self, x, t, first: int, batch: int, total: int, seed: int, out=None):
+        """This rank's slice [first, first + batch) of the total-sample
+        minibatch of the next Adam step: a device vector of NPARAMS gradient
+        entries (each sample's dL/dy carries 1 / total) and the slice's sum of
+        squared errors; asynchronous."""
+        torch = self._on_current_stream()
+        g = out if out is not None else torch.empty(NPARAMS + 1, dtype=torch.float32, device=x.device)
+        if self._lib.phieng_mlp_shard_grad(self._h, x.data_ptr(), t.data_ptr(), x.shape[0], first, batch, total, seed,
+                                           g.data_ptr()) != 1:
+            self.check()
+            raise ValueError("phieng_mlp_shard_grad rejected its arguments")
+        return g
+
+    def apply_grad(self, g, lr: float) -> None:
+        """One Adam step from a device gradient laid out as shard_grad's."""
+        self._on_current_stream()
+        if self._lib.phieng_mlp_apply_grad(self._h, g.data_ptr(), lr) != 1:
+            self.check()
+            raise ValueError("phieng_mlp_apply_grad rejected its arguments")
+
+
+def train_data_parallel(mlp: Mlp, x, t, batch: int, iters: int, lr: float = 1e-3, seed: int = 0xC105E,
+                        group=None):
+    """Data-parallel training, this rank's part (every rank of `group` calls
+    it with the same network, pairs and arguments). Each iteration the rank
+    computes the gradient of its slice [rank * batch, (rank + 1) * batch) of
+    the size * batch minibatch that a single-GPU phieng_mlp_train with that
+    batch would draw, the ranks sum the vectors with one all-reduce (NCCL on
+    the GPU; gloo through a host copy), and every rank takes the same Adam
+    step, so all ranks keep identical parameters. Returns the loss history
+    (host, one synchronisation at the end)."""
+    import torch.distributed as dist
+
+    torch = _torch()
+    rank, size = dist.get_rank(group), dist.get_world_size(group)
+    total = batch * size
+    on_device = dist.get_backend(group) == "nccl"
+    g = torch.empty(NPARAMS + 1, dtype=torch.float32, device=x.device)
+    losses = torch.empty(iters, dtype=torch.float32, device=x.device)
+    for it in range(iters):
+        mlp.shard_grad(x, t, rank * batch, batch, total, seed, out=g)
+        if on_device:
+            dist.all_reduce(g, group=group)
+        else:
+            h = g.cpu()
+            dist.all_reduce(h, group=group)
+            g.copy_(h)
+        losses[it] = g[NPARAMS] / (2.0 * total)
+        mlp.apply_grad(g, lr)
+    return losses.cpu().numpy()
+
+
 def sample_indices(npairs: int, batch: int, seed: int, it: int):
     torch = _torch()
     out = torch.empty(batch, dtype=torch.int32, device="cuda")

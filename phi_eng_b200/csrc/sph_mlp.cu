@@ -235,8 +235,8 @@ __device__ __forceinline__ float group_sum(float v) {
 }
 
 __global__ void __launch_bounds__(kTrainThreads, 1)
-    k_mlp_train_tile(const float* __restrict__ x, const float* __restrict__ tg, uint32_t npairs, uint32_t batch,
-                     uint32_t rounds, uint64_t seed, const uint32_t* __restrict__ iter_ptr, MlpDev mlp,
+    k_mlp_train_tile(const float* __restrict__ x, const float* __restrict__ tg, uint32_t npairs, uint32_t k0,
+                     uint32_t total, uint32_t rounds, uint64_t seed, const uint32_t* __restrict__ iter_ptr, MlpDev mlp,
                      float* __restrict__ part) {
   extern __shared__ __align__(16) unsigned char train_smem[];
   TrainSmem& S = *reinterpret_cast<TrainSmem*>(train_smem);
@@ -257,7 +257,7 @@ __global__ void __launch_bounds__(kTrainThreads, 1)
   for (int i = tid; i < kNorm; i += kTrainThreads) S.norm[i] = mlp.norm[i];
   for (int i = tid; i < 4 * 2 * kHidden; i += kTrainThreads) (&S.db[0][0])[i] = 0.0f;
   const uint32_t iter = *iter_ptr;
-  const float inv_b = __fdiv_rn(1.0f, (float)batch);
+  const float inv_b = __fdiv_rn(1.0f, (float)total);
   __syncthreads();
   const float inv_os0 = __fdiv_rn(1.0f, S.norm[2 * kFeat]), inv_os1 = __fdiv_rn(1.0f, S.norm[2 * kFeat + 1]);
 
@@ -276,7 +276,7 @@ __global__ void __launch_bounds__(kTrainThreads, 1)
     // ---- gather 128 samples: row = warp * 32 + lane
     {
       const int row = tid;
-      const uint32_t k = (blockIdx.x * rounds + r) * kTileRows + (uint32_t)row;
+      const uint32_t k = k0 + (blockIdx.x * rounds + r) * kTileRows + (uint32_t)row;
       const uint32_t idx = sample_index(seed, iter, k, npairs);
       const float4* xi = reinterpret_cast<const float4*>(x + (size_t)idx * kFeat);
       float f[kFeat];
@@ -527,8 +527,8 @@ __device__ __forceinline__ void st_t16(unsigned char* m, uint32_t row, uint32_t 
 }
 
 __global__ void __launch_bounds__(kTrainThreads, 1)
-    k_mlp_train_tc(const float* __restrict__ x, const float* __restrict__ tg, uint32_t npairs, uint32_t batch,
-                   uint32_t rounds, uint64_t seed, const uint32_t* __restrict__ iter_ptr, MlpDev mlp,
+    k_mlp_train_tc(const float* __restrict__ x, const float* __restrict__ tg, uint32_t npairs, uint32_t k0,
+                   uint32_t total, uint32_t rounds, uint64_t seed, const uint32_t* __restrict__ iter_ptr, MlpDev mlp,
                    float* __restrict__ part, uint32_t* __restrict__ err) {
   extern __shared__ __align__(1024) unsigned char tsm[];
   const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -579,7 +579,7 @@ __global__ void __launch_bounds__(kTrainThreads, 1)
   const uint32_t tm = *slot, lanes = (warp * 32u) << 16;
   uint32_t phase = 0;
   const uint32_t iter = *iter_ptr;
-  const float inv_b = __fdiv_rn(1.0f, (float)batch);
+  const float inv_b = __fdiv_rn(1.0f, (float)total);
   const float inv_os0 = __fdiv_rn(1.0f, norm[2 * kFeat]), inv_os1 = __fdiv_rn(1.0f, norm[2 * kFeat + 1]);
   const uint32_t aX = tc::smem_u32(X), aA = tc::smem_u32(A), aGA = tc::smem_u32(GA), aGB = tc::smem_u32(GB);
   const uint32_t aW1 = tc::smem_u32(tsm + kTrW1), aW2 = tc::smem_u32(tsm + kTrW2), aW3 = tc::smem_u32(tsm + kTrW3),
@@ -590,7 +590,7 @@ __global__ void __launch_bounds__(kTrainThreads, 1)
   for (uint32_t r = 0; r < rounds; r++) {
     // ---- sample row tid: x_hat into X (row) and GB rows 64..79 (column), scaled target
     {
-      const uint32_t k = (blockIdx.x * rounds + r) * kTileRows + tid;
+      const uint32_t k = k0 + (blockIdx.x * rounds + r) * kTileRows + tid;
       const uint32_t idx = sample_index(seed, iter, k, npairs);
       const float4* xi = reinterpret_cast<const float4*>(x + (size_t)idx * kFeat);
       float f[kFeat];
@@ -983,17 +983,19 @@ bool check_pairs(const float* x, const float* t, uint32_t npairs, uint32_t batch
   return x && t && npairs > 0 && batch > 0 && batch % kTileRows == 0;
 }
 
+// Samples [k0, k0 + batch) of a minibatch of `total` (dL/dy scaled by 1 / total).
 bool launch_tile(PhiengMlp* m, const float* x, const float* t, uint32_t npairs, uint32_t batch, uint64_t seed,
-                 const uint32_t* iter_ptr, uint32_t* nparts_out) {
+                 const uint32_t* iter_ptr, uint32_t* nparts_out, uint32_t k0 = 0, uint32_t total = 0) {
   uint32_t ctas, rounds;
   mlp_grid(batch, &ctas, &rounds);
   if (!ensure_parts(m, ctas)) return false;
   MlpDev d = phieng_mlp_dev(m);
+  if (total == 0) total = batch;
   if (m->train_engine == PHIENG_MLP_TCGEN05)
-    k_mlp_train_tc<<<ctas, kTrainThreads, kTrSmem, m->stream>>>(x, t, npairs, batch, rounds, seed, iter_ptr, d,
+    k_mlp_train_tc<<<ctas, kTrainThreads, kTrSmem, m->stream>>>(x, t, npairs, k0, total, rounds, seed, iter_ptr, d,
                                                                  m->part, m->ctr + 2);
   else
-    k_mlp_train_tile<<<ctas, kTrainThreads, sizeof(TrainSmem), m->stream>>>(x, t, npairs, batch, rounds, seed,
+    k_mlp_train_tile<<<ctas, kTrainThreads, sizeof(TrainSmem), m->stream>>>(x, t, npairs, k0, total, rounds, seed,
                                                                             iter_ptr, d, m->part);
   *nparts_out = ctas;
   return mlp_ok(m, cudaGetLastError());
@@ -1230,6 +1232,26 @@ int32_t phieng_mlp_train(PhiengMlp* m, const float* x, const float* t, uint32_t 
                                    m->stream));
   if (ok) ok = mlp_ok(m, cudaStreamSynchronize(m->stream)) && waits_clean(m);
   return ok ? 1 : 0;
+}
+
+int32_t phieng_mlp_shard_grad(PhiengMlp* m, const float* x, const float* t, uint32_t npairs, uint32_t first,
+                              uint32_t batch, uint32_t total, uint64_t seed, float* grad) {
+  if (!m || m->error || !grad || !check_pairs(x, t, npairs, batch) || total < batch || first > total - batch)
+    return 0;
+  uint32_t nparts = 0;
+  if (!launch_tile(m, x, t, npairs, batch, seed, m->ctr, &nparts, first, total)) return 0;
+  // raw sums: the gradient already carries 1 / total, the loss is the sum of squared errors
+  k_mlp_reduce<<<cdiv(kParams + 1, 256), 256, 0, m->stream>>>(m->part, nparts, 1.0f, grad, grad + kParams);
+  return mlp_ok(m, cudaGetLastError()) ? 1 : 0;
+}
+
+int32_t phieng_mlp_apply_grad(PhiengMlp* m, const float* grad, float lr) {
+  if (!m || m->error || !grad || !(lr > 0.0f)) return 0;
+  // a single gradient vector is a partial list of length one
+  k_mlp_adam<<<cdiv(kParams + 1, 256), 256, 0, m->stream>>>(grad, 1, m->w, m->m, m->v, m->ctr, lr, 0.0f, nullptr, 0,
+                                                              0, m->frag, m->bias, m->w3);
+  k_mlp_advance<<<1, 1, 0, m->stream>>>(m->ctr);
+  return mlp_ok(m, cudaGetLastError()) ? 1 : 0;
 }
 
 int32_t phieng_mlp_set_train_engine(PhiengMlp* m, int32_t engine) {
