@@ -379,9 +379,57 @@ uint32_t phieng_sph_get_state_device(World2* world, float* dst, uint32_t max);
  * a count mismatch or null. Works on batches. */
 int32_t phieng_sph_set_state_device(World2* world, const float* src, uint32_t n);
 /* Replace every particle by n phase-0 particles whose [x, y, vx, vy] come
- * from src (device); n <= the particle cap. Used to rebuild a rank's local
- * particle set each substep without a host round trip. 1 ok, 0 otherwise. */
+ * from src (device); n <= the particle cap. 1 ok, 0 otherwise. */
 int32_t phieng_sph_load_state_device(World2* world, const float* src, uint32_t n);
+
+/* ---- x-slab decomposition of one scene over ranks (additive) ----
+ * A rank world holds own_cap owned slots, then halo_cap slots for the left
+ * neighbour's halo and halo_cap for the right's (n = own_cap + 2 halo_cap,
+ * loaded with phieng_sph_load_state_device); an unused slot holds
+ * [NaN, NaN, 0, 0] and the order tag PHIENG_SPH_SLAB_FREE. Each substep the
+ * host calls pack(0), moves the send buffers to the neighbours' receive
+ * buffers (point-to-point, whole buffers: the count travels inside), calls
+ * unpack(0), phieng_world_step, pack(1), exchanges again and calls
+ * unpack(1). Everything is ordered on the world's stream and nothing is read
+ * on the host, so with NCCL on that stream a substep never synchronises. The
+ * owned particles' results are bit-identical to the single-domain step's. */
+#define PHIENG_SPH_SLAB_FREE 0xFFFFFFFFu
+/* Bytes of one exchange buffer for halo_cap rows: header (count, overflow
+ * flag, 2 x 0; uint32), float [halo_cap][4] states, uint32 [halo_cap] tags. */
+#define PHIENG_SPH_SLAB_BUFFER_BYTES(halo_cap) (16u + 20u * (uint32_t)(halo_cap))
+/* Per-particle order tags (n = fluid_count values; host or device memory):
+ * each cell's particles are visited in ascending tag instead of ascending
+ * index. Tags of finite particles must be distinct; with the global ids of
+ * the single domain, a world that holds any subset of its particles in any
+ * order visits neighbours in the single domain's order. Cleared when the
+ * particle buffers are reallocated. 1 ok, 0 otherwise. */
+int32_t phieng_sph_set_order(World2* world, const uint32_t* tags, uint32_t n);
+/* Make the world a slab rank: owned cell columns [lo, hi) (column =
+ * floor(x / smoothing_length)), neighbours bit 0 = left rank exists, bit 1 =
+ * right; device buffers of PHIENG_SPH_SLAB_BUFFER_BYTES(halo_cap) each (a
+ * side without a neighbour may pass null). Requires order tags, one substep
+ * per step (cfl 0 or max_substeps 1), no adaptive resolution or ghosts.
+ * Owned slots whose tag is PHIENG_SPH_SLAB_FREE form the free-slot stack. */
+int32_t phieng_sph_slab_setup(World2* world, int32_t lo, int32_t hi, uint32_t neighbours, uint32_t own_cap,
+                              uint32_t halo_cap, void* send_left, void* send_right, const void* recv_left,
+                              const void* recv_right);
+/* phase 0: owned particles within two cell columns of a shared edge into
+ * that side's send buffer (the halo); phase 1: owned particles whose column
+ * left [lo, hi) into that side's send buffer, their slots freed. */
+int32_t phieng_sph_slab_pack(World2* world, uint32_t phase);
+/* phase 0: each side's received halo into its halo slots (the remaining
+ * halo slots emptied); phase 1: received particles into free owned slots.
+ * A buffer that overflowed or a full owned region sets the slab error that
+ * phieng_sph_slab_status reports. */
+int32_t phieng_sph_slab_unpack(World2* world, uint32_t phase);
+/* *out (device float) = max |v| over the owned particles (for the ranks'
+ * all-reduce of the CFL substep count). */
+int32_t phieng_sph_slab_vmax(World2* world, float* out);
+/* Synchronise; 1 if no exchange overflowed since set-up, else 0. */
+int32_t phieng_sph_slab_status(World2* world);
+/* Synchronise; the owned particles' [x, y, vx, vy] and tags (host buffers,
+ * up to max rows, slot order). Returns the number of owned particles. */
+uint32_t phieng_sph_slab_owned(World2* world, float* state, uint32_t* tags, uint32_t max);
 
 /* ---- learned closure (additive; no reference counterpart) ----
  * A per-particle network 16 -> 64 -> 64 -> 2 (SiLU, BF16 weights on the

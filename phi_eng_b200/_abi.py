@@ -344,6 +344,14 @@ SIGNATURES = {
     "phieng_sph_get_state_device": (C.c_uint32, [_P, _P, C.c_uint32]),
     "phieng_sph_set_state_device": (C.c_int32, [_P, _P, C.c_uint32]),
     "phieng_sph_load_state_device": (C.c_int32, [_P, _P, C.c_uint32]),
+    "phieng_sph_set_order": (C.c_int32, [_P, _P, C.c_uint32]),
+    "phieng_sph_slab_setup": (C.c_int32, [_P, C.c_int32, C.c_int32, C.c_uint32, C.c_uint32, C.c_uint32, _P, _P, _P,
+                                          _P]),
+    "phieng_sph_slab_pack": (C.c_int32, [_P, C.c_uint32]),
+    "phieng_sph_slab_unpack": (C.c_int32, [_P, C.c_uint32]),
+    "phieng_sph_slab_vmax": (C.c_int32, [_P, _P]),
+    "phieng_sph_slab_status": (C.c_int32, [_P]),
+    "phieng_sph_slab_owned": (C.c_uint32, [_P, _P, _P, C.c_uint32]),
     "phieng_mlp_new": (_P, [C.c_uint64]),
     "phieng_mlp_free": (None, [_P]),
     "phieng_mlp_status": (C.c_int32, [_P]),

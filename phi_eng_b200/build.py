@@ -33,6 +33,7 @@ UNITS = [
     ("sph_noalloc.cu", EXACT),
     ("sph_mlp.cu", EXACT),
     ("sph3d.cu", EXACT),
+    ("sph_slab.cu", EXACT),
 ]
 HEADERS = ["sph_device.cuh", "sph_kernels.h", "sph_mlp.cuh", "sph_mlp_host.h", "sph_warp.cuh", "sph_host.h", "sph_snapshot.h",
            "sph_noise.cuh", "sph_fast.cuh", "sph_tc.cuh", "sph_tc_net.cuh",

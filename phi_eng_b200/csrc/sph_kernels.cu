@@ -321,7 +321,8 @@ __global__ void __launch_bounds__(256) k_place_final(const uint32_t* __restrict_
                                                      const uint32_t* __restrict__ sid_prev, uint32_t n,
                                                      uint32_t* __restrict__ cursor, const uint32_t* __restrict__ start,
                                                      uint32_t* __restrict__ tkey, uint32_t* __restrict__ tid_out,
-                                                     uint32_t* __restrict__ skey, GatherArgs ga) {
+                                                     uint32_t* __restrict__ skey, const uint32_t* __restrict__ order,
+                                                     GatherArgs ga) {
   const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n) return;
   const uint32_t id = BY_SLOT ? sid_prev[s] : s;
@@ -334,8 +335,9 @@ __global__ void __launch_bounds__(256) k_place_final(const uint32_t* __restrict_
   if (first == lane) base = atomicAdd(&cursor[k], len);
   base = __shfl_sync(act, base, first);
   const uint32_t slot = base + rank;
-  const uint32_t pid = __shfl_sync(act, id, lane ? lane - 1u : 0u);
-  const bool asc = lane == first || pid < id;
+  const uint32_t tag = order ? __ldg(&order[id]) : id;
+  const uint32_t ptag = __shfl_sync(act, tag, lane ? lane - 1u : 0u);
+  const bool asc = lane == first || ptag < tag;
   const uint32_t bad = __ballot_sync(act, !asc);
   const uint32_t run = (len >= 32u ? 0xFFFFFFFFu : ((1u << len) - 1u)) << first;
   if (len == __ldg(&start[k + 1]) - __ldg(&start[k]) && (bad & run) == 0u) {
@@ -373,12 +375,16 @@ __global__ void __launch_bounds__(256) k_place(const uint32_t* __restrict__ key,
   tid_out[slot] = id;
 }
 
-// Final slot = bucket start + rank of the id among the bucket's ids; the
-// particle's state is gathered into that slot.
+// Final slot = bucket start + rank of the id (or its order tag) among the
+// bucket's; the particle's state is gathered into that slot. With order
+// tags, the sentinel bucket of non-finite particles keeps its placement
+// slots: no walk visits it, and its size (a rank world's unused slots) would
+// make ranking quadratic.
 __global__ void __launch_bounds__(256) k_fixup(const uint32_t* __restrict__ tkey,
                                                const uint32_t* __restrict__ tid_in,
                                                const uint32_t* __restrict__ start, uint32_t n,
                                                uint32_t* __restrict__ skey, uint32_t* __restrict__ sid,
+                                               const uint32_t* __restrict__ order, uint32_t sentinel,
                                                GatherArgs ga) {
   const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n) return;
@@ -390,7 +396,16 @@ __global__ void __launch_bounds__(256) k_fixup(const uint32_t* __restrict__ tkey
   const uint32_t k = tkey[s];
   const uint32_t lo = start[k], hi = start[k + 1];
   uint32_t rank = 0;
-  for (uint32_t j = lo; j < hi; j++) rank += __ldg(&tid_in[j]) < id ? 1u : 0u;
+  if (order) {
+    if (k == sentinel) {
+      gather_slot(s, k, id, ga, skey, sid);
+      return;
+    }
+    const uint32_t tag = __ldg(&order[id]);
+    for (uint32_t j = lo; j < hi; j++) rank += __ldg(&order[__ldg(&tid_in[j])]) < tag ? 1u : 0u;
+  } else {
+    for (uint32_t j = lo; j < hi; j++) rank += __ldg(&tid_in[j]) < id ? 1u : 0u;
+  }
   gather_slot(lo + rank, k, id, ga, skey, sid);
 }
 
@@ -1115,10 +1130,12 @@ void enqueue_sort_and_ranges(const FluidBufs& b, uint32_t n, const StepParams& P
   ga.sscene = b.batch.ptab ? b.batch.sscene : nullptr;
   enqueue_bucket_scan(bs, m, st);
   if (by_slot)
-    k_place_final<true><<<cdiv(n, 256), 256, 0, st>>>(b.key, b.sid, n, b.count, b.start, b.tkey, b.tid, b.skey, ga);
+    k_place_final<true><<<cdiv(n, 256), 256, 0, st>>>(b.key, b.sid, n, b.count, b.start, b.tkey, b.tid, b.skey,
+                                                       b.order, ga);
   else
-    k_place_final<false><<<cdiv(n, 256), 256, 0, st>>>(b.key, b.sid, n, b.count, b.start, b.tkey, b.tid, b.skey, ga);
-  k_fixup<<<cdiv(n, 256), 256, 0, st>>>(b.tkey, b.tid, b.start, n, b.skey, b.sid, ga);
+    k_place_final<false><<<cdiv(n, 256), 256, 0, st>>>(b.key, b.sid, n, b.count, b.start, b.tkey, b.tid, b.skey,
+                                                        b.order, ga);
+  k_fixup<<<cdiv(n, 256), 256, 0, st>>>(b.tkey, b.tid, b.start, n, b.skey, b.sid, b.order, P.grid.sentinel, ga);
   // the counts of the next sort accumulate from zero (K6)
   cudaMemsetAsync(b.count, 0, sizeof(uint32_t) * b.count_len, st);
 }

@@ -37,6 +37,12 @@ struct FluidBufs {
   float2* sdq = nullptr;     // sorted (density, pressure / max(density,EPS)^2)
   float* spres = nullptr;    // sorted pressure
   uint32_t* nmask = nullptr; // [3][cap] per-row neighbour masks written by K5, read by K6
+  // per id: the tag that orders a bucket's particles (null: the id itself).
+  // Tags of finite particles are distinct; the x-slab decomposition sets the
+  // global ids, so a rank world visits its neighbours in the single domain's
+  // order whatever slot a particle occupies. With tags, the non-finite
+  // sentinel bucket keeps its placement order (nothing visits it).
+  uint32_t* order = nullptr;
   // per bucket grid (sized by the number of buckets B)
   uint32_t* count = nullptr;    // particles per bucket, then the placement cursor
   uint32_t count_len = 0;       // B + 1 rounded up to the scan tile
@@ -215,5 +221,41 @@ void enqueue_vmax(const FluidBufs& b, uint32_t n, cudaStream_t st);
 
 // b.scalar[2] = order-preserving bits of max_i x_i, b.scalar[3] = bits of max_i |v_i|.
 void enqueue_front_metrics(const FluidBufs& b, uint32_t n, cudaStream_t st);
+
+// ---------------------------------------------------------------- x-slab ranks
+// A rank world of the x-slab decomposition holds own_cap owned slots, then
+// halo_cap slots for the left neighbour's halo and halo_cap for the right's;
+// an unused slot holds (NaN, NaN, 0, 0) with order tag kSlabFree (its key is
+// the sentinel, so no walk visits it). Exchange buffers (one per direction)
+// are 16 + 20 * halo_cap bytes: uint32 header [count, overflow, 0, 0], then
+// float4 rows [halo_cap], then uint32 tags [halo_cap]; the host moves them
+// between neighbours without reading them.
+constexpr uint32_t kSlabFree = 0xFFFFFFFFu;
+constexpr int32_t kSlabHaloColumns = 2;
+
+struct SlabPlan {
+  int32_t lo = 0, hi = 0;             // owned cell columns [lo, hi)
+  uint32_t has_left = 0, has_right = 0;
+  float h = 1.0f;                     // cell width (config smoothing_length)
+  uint32_t own_cap = 0, halo_cap = 0;
+  unsigned char* send[2] = {nullptr, nullptr};        // to the left (0) / right (1) neighbour
+  const unsigned char* recv[2] = {nullptr, nullptr};  // from the left / right neighbour
+  uint32_t* free_stack = nullptr;     // [own_cap] owned slots not in use
+  uint32_t* words = nullptr;          // [0] free slots, [1] error (sticky), [2] slots taken
+};
+
+constexpr size_t slab_buffer_bytes(uint32_t cap) { return 16 + 20 * (size_t)cap; }
+
+// Stack of the owned slots whose tag is kSlabFree (slab set-up).
+void enqueue_slab_init(const FluidBufs& b, const SlabPlan& sp, cudaStream_t st);
+// phase 0: halo (owned particles within kSlabHaloColumns of a shared edge, to
+// that neighbour); phase 1: migrants (owned particles whose column left the
+// slab, to that neighbour; their slots become free). Resets the send headers.
+void enqueue_slab_pack(const FluidBufs& b, const SlabPlan& sp, const GridPlan& g, uint32_t phase, cudaStream_t st);
+// phase 0: each side's received halo into its halo slots, the rest of them
+// emptied; phase 1: received migrants into free owned slots. Keys and bucket
+// counts follow every replaced slot; an overflowing buffer or a full owned
+// region sets words[1].
+void enqueue_slab_unpack(const FluidBufs& b, const SlabPlan& sp, const GridPlan& g, uint32_t phase, cudaStream_t st);
 
 }  // namespace phieng

@@ -122,6 +122,13 @@ struct World2 {
   uint32_t batch_cap = 0;
   bool is_batch() const { return !scenes.empty(); }
 
+  // x-slab rank world (phieng_sph_slab_*): slots, exchange buffers and the
+  // free-slot stack [own_cap] + words [4] (d_slab)
+  bool slab = false;
+  SlabPlan slab_plan{};
+  uint32_t* d_slab = nullptr;
+  uint32_t slab_cap = 0;
+
   // learned closure (phieng_sph_set_closure / phieng_sph_closure_step)
   PhiengMlp* closure = nullptr;
   uint32_t closure_ratio = 4;
@@ -199,6 +206,7 @@ void dfree(T*& p) {
 }
 
 void free_particle_buffers(FluidBufs& d) {
+  dfree(d.order);  // order tags do not survive a reallocation
   dfree(d.state);
   dfree(d.mass);
   dfree(d.phase);
@@ -1461,6 +1469,7 @@ void phieng_world_free(World2* w) {
     dfree(w->d.tilesum);
     dfree(w->d.tstate);
     dfree(w->d_tmp);
+    dfree(w->d_slab);
     dfree(w->d_pscene);
     dfree(w->d_sscene);
     dfree(w->d_ptab);
@@ -2041,6 +2050,114 @@ int32_t phieng_sph_set_precision(World2* w, uint32_t mode) {
 }
 
 uint32_t phieng_sph_get_precision(const World2* w) { return w ? w->precision : PHIENG_SPH_EXACT; }
+
+int32_t phieng_sph_set_order(World2* w, const uint32_t* tags, uint32_t n) {
+  if (!w || w->is_batch() || !tags || n == 0 || n != w->n) return 0;
+  if (!prepare(w)) return 0;
+  if (!w->d.order && !dalloc(w, w->d.order, w->d.cap)) return 0;
+  if (!cuda_ok(w, cudaMemcpyAsync(w->d.order, tags, sizeof(uint32_t) * n, cudaMemcpyDefault, w->stream),
+               "order tags"))
+    return 0;
+  release_graph(w);  // the captured sort reads the tag array
+  return 1;
+}
+
+int32_t phieng_sph_slab_setup(World2* w, int32_t lo, int32_t hi, uint32_t neighbours, uint32_t own_cap,
+                              uint32_t halo_cap, void* send_left, void* send_right, const void* recv_left,
+                              const void* recv_right) {
+  if (!w || w->is_batch() || !w->d.order || hi <= lo || halo_cap == 0 || neighbours > 3u ||
+      (uint64_t)own_cap + 2ull * halo_cap != w->n)
+    return 0;
+  if ((neighbours & 1u) && (!send_left || !recv_left)) return 0;
+  if ((neighbours & 2u) && (!send_right || !recv_right)) return 0;
+  // one substep per world step (the ranks agree on the substep count), and
+  // none of the passes that change the particle set or add particles
+  if ((w->cfg.cfl > 0.0f && w->cfg.max_substeps > 1) || w->cfg.adaptive_resolution || w->cfg.boundary_particles)
+    return 0;
+  if (!prepare(w)) return 0;  // keys and bucket counts of the current slots
+  if (w->slab_cap < own_cap + 4u) {
+    cudaStreamSynchronize(w->stream);
+    dfree(w->d_slab);
+    w->slab_cap = 0;
+    if (!dalloc(w, w->d_slab, (size_t)own_cap + 4u)) return 0;
+    w->slab_cap = own_cap + 4u;
+  }
+  SlabPlan& sp = w->slab_plan;
+  sp.lo = lo;
+  sp.hi = hi;
+  sp.has_left = neighbours & 1u;
+  sp.has_right = (neighbours >> 1) & 1u;
+  sp.h = w->cfg.smoothing_length;
+  sp.own_cap = own_cap;
+  sp.halo_cap = halo_cap;
+  sp.send[0] = sp.has_left ? static_cast<unsigned char*>(send_left) : nullptr;
+  sp.send[1] = sp.has_right ? static_cast<unsigned char*>(send_right) : nullptr;
+  sp.recv[0] = sp.has_left ? static_cast<const unsigned char*>(recv_left) : nullptr;
+  sp.recv[1] = sp.has_right ? static_cast<const unsigned char*>(recv_right) : nullptr;
+  sp.free_stack = w->d_slab;
+  sp.words = w->d_slab + own_cap;
+  enqueue_slab_init(w->d, sp, w->stream);
+  w->slab = true;
+  return cuda_ok(w, cudaGetLastError(), "slab setup") ? 1 : 0;
+}
+
+int32_t phieng_sph_slab_pack(World2* w, uint32_t phase) {
+  if (!w || !w->slab || phase > 1 || !w->d.order) return 0;
+  if (!prepare(w)) return 0;
+  enqueue_slab_pack(w->d, w->slab_plan, w->plan, phase, w->stream);
+  return cuda_ok(w, cudaGetLastError(), "slab pack") ? 1 : 0;
+}
+
+int32_t phieng_sph_slab_unpack(World2* w, uint32_t phase) {
+  if (!w || !w->slab || phase > 1 || !w->d.order) return 0;
+  if (!prepare(w)) return 0;
+  enqueue_slab_unpack(w->d, w->slab_plan, w->plan, phase, w->stream);
+  w->host_state_valid = false;
+  w->dp_on_device = false;
+  return cuda_ok(w, cudaGetLastError(), "slab unpack") ? 1 : 0;
+}
+
+int32_t phieng_sph_slab_vmax(World2* w, float* out) {
+  if (!w || !w->slab || !out) return 0;
+  if (!prepare(w)) return 0;
+  FluidBufs b = w->d;
+  b.scalar = reinterpret_cast<unsigned int*>(out);
+  enqueue_vmax(b, w->slab_plan.own_cap, w->stream);
+  return cuda_ok(w, cudaGetLastError(), "slab vmax") ? 1 : 0;
+}
+
+int32_t phieng_sph_slab_status(World2* w) {
+  if (!w || !w->slab) return 0;
+  uint32_t e = 1;
+  if (!cuda_ok(w, cudaMemcpyAsync(&e, w->slab_plan.words + 1, 4, cudaMemcpyDeviceToHost, w->stream), "slab status") ||
+      !cuda_ok(w, cudaStreamSynchronize(w->stream), "sync"))
+    return 0;
+  return e == 0 ? 1 : 0;
+}
+
+uint32_t phieng_sph_slab_owned(World2* w, float* state, uint32_t* tags, uint32_t max) {
+  if (!w || !w->slab || !state || !tags) return 0;
+  const uint32_t oc = w->slab_plan.own_cap;
+  std::vector<float4> st(oc);
+  std::vector<uint32_t> tg(oc);
+  if (oc && (!cuda_ok(w, cudaMemcpyAsync(st.data(), w->d.state, sizeof(float4) * oc, cudaMemcpyDeviceToHost,
+                                          w->stream),
+                      "slab owned") ||
+             !cuda_ok(w, cudaMemcpyAsync(tg.data(), w->d.order, 4ull * oc, cudaMemcpyDeviceToHost, w->stream),
+                      "slab owned") ||
+             !cuda_ok(w, cudaStreamSynchronize(w->stream), "sync")))
+    return 0;
+  uint32_t k = 0;
+  for (uint32_t i = 0; i < oc; i++) {
+    if (tg[i] == kSlabFree) continue;
+    if (k < max) {
+      std::memcpy(state + 4ull * k, &st[i], sizeof(float4));
+      tags[k] = tg[i];
+    }
+    k++;
+  }
+  return k;
+}
 
 int32_t phieng_sph_load_state_device(World2* w, const float* src, uint32_t n) {
   if (!w || w->is_batch() || (n && !src) || n > w->cap) return 0;

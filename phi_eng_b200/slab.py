@@ -114,6 +114,173 @@ class GpuEngine:
         return out if home == out.device else out.to(home)
 
 
+class DeviceSlabRun:
+    """This rank's part of one scene on a persistent rank world with the
+    exchange on the device (phieng_sph_slab_*): the world holds the owned
+    slots and two halo regions at a fixed capacity (unused slots are NaN
+    particles, which no neighbour walk visits, so the step's CUDA graph never
+    changes), buckets are ordered by global id (order tags), and each
+    substep packs, exchanges whole fixed-size buffers, unpacks, steps, then
+    does the same for the migrants. With NCCL the buffers move on the
+    world's stream and a substep never waits on the host; with CFL substeps
+    one all-reduced maximum speed is read per step. gloo moves host copies of
+    the same buffers (tests on one GPU)."""
+
+    def __init__(self, scene, rank: int, size: int, edges=None, own_cap: int | None = None,
+                 halo_cap: int | None = None):
+        import torch
+
+        from . import _abi
+        from .closure import torch_stream_handle
+        from .world import world_from_scene
+
+        self.scene = scene
+        self.rank, self.size = rank, size
+        self.h = float(scene.config.smoothing_length)
+        self.edges = edges or slab_edges(scene.xy, self.h, size)
+        self.lo, self.hi = self.edges[rank], self.edges[rank + 1]
+        xy = torch.from_numpy(np.ascontiguousarray(scene.xy, dtype=np.float32))
+        cx = cell_column(xy[:, 0], self.h)
+        ids = torch.nonzero((cx >= self.lo) & (cx < self.hi)).squeeze(1)
+        n0 = int(ids.shape[0])
+        if halo_cap is None:
+            # particles within four columns of an inner edge, with room for the flow to pile up there
+            near = 0
+            for e in self.edges[1:-1]:
+                near = max(near, int(((cx >= e - 2 * HALO_CELLS) & (cx < e + 2 * HALO_CELLS)).sum()))
+            halo_cap = max(1024, 4 * near)
+        halo_cap = max(1, min(int(halo_cap), max(scene.n, 1)))
+        if own_cap is None:
+            own_cap = min(max(scene.n, 1), n0 + max(n0 // 4, 4 * halo_cap))
+        own_cap = max(int(own_cap), n0)
+        self.own_cap, self.halo_cap = own_cap, halo_cap
+        cap = own_cap + 2 * halo_cap
+        st = torch.zeros((cap, 4), dtype=torch.float32)
+        st[:, :2] = float("nan")
+        st[:n0, :2] = xy[ids]
+        tags = torch.full((cap,), -1, dtype=torch.int32)  # PHIENG_SPH_SLAB_FREE
+        tags[:n0] = ids.to(torch.int32)
+        self.world = world_from_scene(_empty_scene(scene))
+        self.world.fluid.config = _no_cfl(scene.config)
+        self.world.fluid.set_cap(cap)
+        self.world.set_stream(torch_stream_handle())
+        self._lib = _abi.load()
+        st_d, tags_d = st.cuda(), tags.cuda()
+        self.world.load_state_device(st_d.data_ptr(), cap)
+        if self._lib.phieng_sph_set_order(self.world._h, tags_d.data_ptr(), cap) != 1:
+            self.world.check()
+            raise RuntimeError("phieng_sph_set_order")
+        nbytes = 16 + 20 * halo_cap
+        self.send = [torch.zeros(nbytes, dtype=torch.uint8, device="cuda") for _ in range(2)]
+        self.recv = [torch.zeros(nbytes, dtype=torch.uint8, device="cuda") for _ in range(2)]
+        self.left = rank - 1 if rank > 0 else None
+        self.right = rank + 1 if rank < size - 1 else None
+        nb = (1 if self.left is not None else 0) | (2 if self.right is not None else 0)
+        i32 = lambda v: int(max(-(1 << 31), min((1 << 31) - 1, v)))
+        ok = self._lib.phieng_sph_slab_setup(self.world._h, i32(self.lo), i32(self.hi), nb, own_cap, halo_cap,
+                                             self.send[0].data_ptr(), self.send[1].data_ptr(),
+                                             self.recv[0].data_ptr(), self.recv[1].data_ptr())
+        if ok != 1:
+            self.world.check()
+            raise RuntimeError("phieng_sph_slab_setup")
+        torch.cuda.current_stream().synchronize()  # st_d / tags_d were read on the stream
+        self.backend = None
+        if size > 1:
+            import torch.distributed as dist
+
+            self.backend = dist.get_backend()
+        self.vmax = torch.zeros(1, dtype=torch.float32, device="cuda")
+        self.comm_bytes = 0
+
+    def close(self) -> None:
+        self.world.close()
+
+    def _exchange(self):
+        if self.size == 1:
+            return
+        import torch
+        import torch.distributed as dist
+
+        peers = [(k, p) for k, p in ((0, self.left), (1, self.right)) if p is not None]
+        if self.backend == "nccl":
+            ops = []
+            for k, p in peers:
+                ops += [dist.P2POp(dist.isend, self.send[k], p), dist.P2POp(dist.irecv, self.recv[k], p)]
+            for q in dist.batch_isend_irecv(ops):
+                q.wait()
+        else:
+            hs = {k: self.send[k].cpu() for k, _ in peers}
+            hr = {k: torch.empty_like(hs[k]) for k, _ in peers}
+            ops = []
+            for k, p in peers:
+                ops += [dist.P2POp(dist.isend, hs[k], p), dist.P2POp(dist.irecv, hr[k], p)]
+            for q in dist.batch_isend_irecv(ops):
+                q.wait()
+            for k, _ in peers:
+                self.recv[k].copy_(hr[k])
+        self.comm_bytes += sum(self.send[k].numel() for k, _ in peers)
+
+    def _call(self, name: str, *args) -> None:
+        if getattr(self._lib, name)(self.world._h, *args) != 1:
+            self.world.check()
+            raise RuntimeError(name)
+
+    def _substep(self, dt: float) -> None:
+        self._call("phieng_sph_slab_pack", 0)
+        self._exchange()
+        self._call("phieng_sph_slab_unpack", 0)
+        self.world.step(dt)
+        self._call("phieng_sph_slab_pack", 1)
+        self._exchange()
+        self._call("phieng_sph_slab_unpack", 1)
+
+    def step(self, dt: float) -> None:
+        """One world step of dt (CFL substeps from the global maximum speed)."""
+        cfg = self.scene.config
+        n_sub = 1
+        if float(cfg.cfl) > 0 and int(cfg.max_substeps) > 1:
+            self._call("phieng_sph_slab_vmax", self.vmax.data_ptr())
+            v = self.vmax
+            if self.size > 1:
+                import torch.distributed as dist
+
+                if self.backend == "nccl":
+                    dist.all_reduce(v, op=dist.ReduceOp.MAX)
+                else:
+                    v = v.cpu()
+                    dist.all_reduce(v, op=dist.ReduceOp.MAX)
+            n_sub = cfl_count(cfg, dt, float(v.item()))
+        sub = float(np.float32(dt) / np.float32(n_sub))
+        for _ in range(n_sub):
+            self._substep(sub)
+
+    def owned(self):
+        """(state [k][4], global ids [k]) of this rank's particles (host)."""
+        st = np.zeros((self.own_cap, 4), np.float32)
+        tg = np.zeros(self.own_cap, np.uint32)
+        k = self._lib.phieng_sph_slab_owned(self.world._h, st.ctypes.data, tg.ctypes.data, self.own_cap)
+        if self._lib.phieng_sph_slab_status(self.world._h) != 1:
+            raise RuntimeError("a slab exchange overflowed its buffers or the owned slots")
+        return st[:k], tg[:k].astype(np.int64)
+
+    def gather(self):
+        """Every particle's state in global id order (all ranks)."""
+        st, ids = self.owned()
+        if self.size == 1:
+            out = np.zeros((ids.shape[0], 4), np.float32)
+            out[ids] = st
+            return out
+        import torch.distributed as dist
+
+        parts = [None] * self.size
+        dist.all_gather_object(parts, (ids, st))
+        n = sum(p[0].shape[0] for p in parts)
+        out = np.zeros((n, 4), np.float32)
+        for i, s in parts:
+            out[i] = s
+        return out
+
+
 def _empty_scene(scene):
     import copy
 
