@@ -438,27 +438,34 @@ def fluid3d_line(steps: int, warmup: int, side: int = 100) -> dict:
                              "sample": f"{k} in-place steps of a 4096-particle 3D dam break (the reference's cap)"}}
 
 
+# kernels per substep of a slab rank: halo pack + unpack, the world's five
+# (scan, placement, fixup, density, force), migrant pack + unpack + settle
+SLAB_KERNELS_PER_SUBSTEP = 10
+
+
 def run_slab(args, rank: int, world: int, local_rank: int) -> None:
-    """The single scene split in x slabs over the ranks (halo exchange and
-    migration over NCCL each substep, phi_eng_b200/slab.py); strong scaling.
-    The timed region is bracketed by barriers and CUDA events on the default
-    stream; the max over ranks is reported."""
+    """The single scene split in x slabs over the ranks, each a persistent
+    rank world with the device-side exchange (pack / unpack kernels, whole
+    fixed-size buffers over NCCL point-to-point on the world's stream,
+    phi_eng_b200/slab.py DeviceSlabRun); strong scaling. The timed region is
+    bracketed by barriers and CUDA events on the default stream; the max over
+    ranks is reported."""
     import torch
     import torch.distributed as dist
     from datetime import timedelta
 
-    from phi_eng_b200.slab import GpuEngine, SlabRun
+    from phi_eng_b200.slab import DeviceSlabRun
 
     torch.cuda.set_device(local_rank)
     dist.init_process_group("nccl", timeout=timedelta(seconds=120))
     sc = workload_scenes(args.workload)[0]
-    eng = GpuEngine(sc, cap=sc.n)
-    run = SlabRun(sc, rank, world, engine=eng, device="cuda")
+    run = DeviceSlabRun(sc, rank, world)
     for _ in range(args.warmup):
         run.step(sc.dt)
     torch.cuda.synchronize()
     dist.barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    sub0 = run.substeps
     e0.record()
     for _ in range(args.steps):
         run.step(sc.dt)
@@ -474,11 +481,18 @@ def run_slab(args, rank: int, world: int, local_rank: int) -> None:
                 "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
                 "config": {"workload": workload_desc(args.workload, [sc]), "particles": sc.n,
                            "parallelism": f"slab{world}", "l2": "not flushed (inputs move between ranks)"},
-                "gpu_launches": None}
+                "gpu_launches": SLAB_KERNELS_PER_SUBSTEP * (run.substeps - sub0)}
         print(json.dumps(line), flush=True)
-    eng.close()
+    try:
+        run.owned()  # raises if an exchange overflowed
+        ok = True
+    except RuntimeError:
+        ok = False
+    run.close()
     dist.barrier()
     dist.destroy_process_group()
+    if not ok:
+        raise RuntimeError("slab exchange")
 
 
 def timed_steps(w, dt: float, steps: int, stream, flush, phases: bool = True):

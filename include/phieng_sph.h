@@ -383,16 +383,19 @@ int32_t phieng_sph_set_state_device(World2* world, const float* src, uint32_t n)
 int32_t phieng_sph_load_state_device(World2* world, const float* src, uint32_t n);
 
 /* ---- x-slab decomposition of one scene over ranks (additive) ----
- * A rank world holds own_cap owned slots, then halo_cap slots for the left
- * neighbour's halo and halo_cap for the right's (n = own_cap + 2 halo_cap,
- * loaded with phieng_sph_load_state_device); an unused slot holds
- * [NaN, NaN, 0, 0] and the order tag PHIENG_SPH_SLAB_FREE. Each substep the
- * host calls pack(0), moves the send buffers to the neighbours' receive
- * buffers (point-to-point, whole buffers: the count travels inside), calls
- * unpack(0), phieng_world_step, pack(1), exchanges again and calls
- * unpack(1). Everything is ordered on the world's stream and nothing is read
- * on the host, so with NCCL on that stream a substep never synchronises. The
- * owned particles' results are bit-identical to the single-domain step's. */
+ * A rank world holds own_cap owned slots, then 2 halo_cap halo slots for the
+ * left side and 2 halo_cap for the right (n = own_cap + 4 halo_cap, loaded
+ * with phieng_sph_load_state_device); an unused slot holds [NaN, NaN, 0, 0]
+ * and the order tag PHIENG_SPH_SLAB_FREE. Once before the first step the
+ * host calls pack(0), moves each send buffer to the neighbour's receive
+ * buffer (point-to-point, whole buffers: the count travels inside) and calls
+ * unpack(0); then every substep is phieng_world_step, pack(1), the same
+ * exchange, unpack(1): one exchange per substep carries the particles that
+ * left the slab and the halo of those that stayed. Everything is ordered on
+ * the world's stream and nothing is read on the host, so with NCCL on that
+ * stream a substep never synchronises. The owned particles' results are
+ * bit-identical to the single-domain step's. Global ids are below 2^31 - 1;
+ * a particle moves less than one cell column per substep. */
 #define PHIENG_SPH_SLAB_FREE 0xFFFFFFFFu
 /* Bytes of one exchange buffer for halo_cap rows: header (count, overflow
  * flag, 2 x 0; uint32), float [halo_cap][4] states, uint32 [halo_cap] tags. */
@@ -406,21 +409,24 @@ int32_t phieng_sph_load_state_device(World2* world, const float* src, uint32_t n
 int32_t phieng_sph_set_order(World2* world, const uint32_t* tags, uint32_t n);
 /* Make the world a slab rank: owned cell columns [lo, hi) (column =
  * floor(x / smoothing_length)), neighbours bit 0 = left rank exists, bit 1 =
- * right; device buffers of PHIENG_SPH_SLAB_BUFFER_BYTES(halo_cap) each (a
- * side without a neighbour may pass null). Requires order tags, one substep
- * per step (cfl 0 or max_substeps 1), no adaptive resolution or ghosts.
- * Owned slots whose tag is PHIENG_SPH_SLAB_FREE form the free-slot stack. */
+ * right (with both, hi - lo >= 4); device buffers of
+ * PHIENG_SPH_SLAB_BUFFER_BYTES(halo_cap) each (a side without a neighbour
+ * may pass null). Requires order tags, one substep per step (cfl 0 or
+ * max_substeps 1), no adaptive resolution or ghosts. Owned slots whose tag is
+ * PHIENG_SPH_SLAB_FREE form the free-slot stack. */
 int32_t phieng_sph_slab_setup(World2* world, int32_t lo, int32_t hi, uint32_t neighbours, uint32_t own_cap,
                               uint32_t halo_cap, void* send_left, void* send_right, const void* recv_left,
                               const void* recv_right);
-/* phase 0: owned particles within two cell columns of a shared edge into
- * that side's send buffer (the halo); phase 1: owned particles whose column
- * left [lo, hi) into that side's send buffer, their slots freed. */
+/* phase 1 (after a step): owned particles whose column left [lo, hi) into
+ * that side's send buffer as migrants (their slots freed), the others within
+ * two cell columns of a shared edge as halo; phase 0 (before the first step):
+ * the halo only. */
 int32_t phieng_sph_slab_pack(World2* world, uint32_t phase);
-/* phase 0: each side's received halo into its halo slots (the remaining
- * halo slots emptied); phase 1: received particles into free owned slots.
- * A buffer that overflowed or a full owned region sets the slab error that
- * phieng_sph_slab_status reports. */
+/* After the exchange: received migrants into free owned slots, each side's
+ * halo (its received halo rows and this rank's own migrants to that side)
+ * into the halo slots, the others emptied. A buffer that overflowed or a
+ * full owned region sets the slab error that phieng_sph_slab_status
+ * reports. */
 int32_t phieng_sph_slab_unpack(World2* world, uint32_t phase);
 /* *out (device float) = max |v| over the owned particles (for the ranks'
  * all-reduce of the CFL substep count). */

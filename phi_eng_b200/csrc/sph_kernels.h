@@ -224,38 +224,46 @@ void enqueue_front_metrics(const FluidBufs& b, uint32_t n, cudaStream_t st);
 
 // ---------------------------------------------------------------- x-slab ranks
 // A rank world of the x-slab decomposition holds own_cap owned slots, then
-// halo_cap slots for the left neighbour's halo and halo_cap for the right's;
+// 2 * halo_cap halo slots for the left side and 2 * halo_cap for the right;
 // an unused slot holds (NaN, NaN, 0, 0) with order tag kSlabFree (its key is
 // the sentinel, so no walk visits it). Exchange buffers (one per direction)
 // are 16 + 20 * halo_cap bytes: uint32 header [count, overflow, 0, 0], then
-// float4 rows [halo_cap], then uint32 tags [halo_cap]; the host moves them
-// between neighbours without reading them.
+// float4 rows [halo_cap], then uint32 tags [halo_cap] (a migrant's tag
+// carries kSlabMigrant); the host moves them between neighbours without
+// reading them. Global ids (the tags) are below 2^31 - 1.
 constexpr uint32_t kSlabFree = 0xFFFFFFFFu;
+constexpr uint32_t kSlabMigrant = 0x80000000u;
 constexpr int32_t kSlabHaloColumns = 2;
+constexpr uint32_t kSlabWords = 8;
 
 struct SlabPlan {
   int32_t lo = 0, hi = 0;             // owned cell columns [lo, hi)
   uint32_t has_left = 0, has_right = 0;
   float h = 1.0f;                     // cell width (config smoothing_length)
   uint32_t own_cap = 0, halo_cap = 0;
+  uint32_t pack_blocks = 592;         // grid of the pack (4 blocks per SM)
   unsigned char* send[2] = {nullptr, nullptr};        // to the left (0) / right (1) neighbour
   const unsigned char* recv[2] = {nullptr, nullptr};  // from the left / right neighbour
   uint32_t* free_stack = nullptr;     // [own_cap] owned slots not in use
-  uint32_t* words = nullptr;          // [0] free slots, [1] error (sticky), [2] slots taken
+  // [0] free slots on the stack, [1] error (sticky), [2] pack blocks done,
+  // [4], [5] rows appended to send[0] / send[1] by the running pack
+  uint32_t* words = nullptr;
 };
 
 constexpr size_t slab_buffer_bytes(uint32_t cap) { return 16 + 20 * (size_t)cap; }
 
-// Stack of the owned slots whose tag is kSlabFree (slab set-up).
+// Stack of the owned slots whose tag is kSlabFree, zeroed counters (set-up).
 void enqueue_slab_init(const FluidBufs& b, const SlabPlan& sp, cudaStream_t st);
-// phase 0: halo (owned particles within kSlabHaloColumns of a shared edge, to
-// that neighbour); phase 1: migrants (owned particles whose column left the
-// slab, to that neighbour; their slots become free). Resets the send headers.
+// After the rank's step (phase 1): migrants (owned particles whose column
+// left the slab; their slots become free) and the halo of the others (within
+// kSlabHaloColumns of a shared edge) into that side's send buffer. phase 0,
+// before the first step: the halo only.
 void enqueue_slab_pack(const FluidBufs& b, const SlabPlan& sp, const GridPlan& g, uint32_t phase, cudaStream_t st);
-// phase 0: each side's received halo into its halo slots, the rest of them
-// emptied; phase 1: received migrants into free owned slots. Keys and bucket
-// counts follow every replaced slot; an overflowing buffer or a full owned
-// region sets words[1].
+// After the exchange: received migrants into free owned slots, each side's
+// halo (received halo rows and this rank's own migrants to that side) into
+// its halo slots, the rest of them emptied. Keys and bucket counts follow
+// every replaced slot; an overflowing buffer or a full owned region sets
+// words[1].
 void enqueue_slab_unpack(const FluidBufs& b, const SlabPlan& sp, const GridPlan& g, uint32_t phase, cudaStream_t st);
 
 }  // namespace phieng

@@ -11,6 +11,7 @@
 // by the particles' global ids (FluidBufs::order).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 
 #include "sph_device.cuh"
@@ -40,14 +41,28 @@ __device__ __forceinline__ SlabView slab_view(const unsigned char* p, uint32_t c
   return v;
 }
 
-__device__ __forceinline__ void slab_append(unsigned char* buf, uint32_t cap, float4 s, uint32_t tag) {
-  SlabView v = slab_view(buf, cap);
-  const uint32_t j = atomicAdd(&v.hdr[0], 1u);
-  if (j < cap) {
+// Index of this lane's entry among the warp's `want` lanes in an array whose
+// length counter is *ctr: one atomic per warp (every lane of the warp calls
+// it). Returns the index (undefined where want is false).
+__device__ __forceinline__ uint32_t warp_reserve(uint32_t* ctr, bool want) {
+  const uint32_t m = __ballot_sync(0xFFFFFFFFu, want);
+  if (m == 0u) return 0u;
+  const uint32_t lane = threadIdx.x & 31u, leader = __ffs(m) - 1u;
+  uint32_t base = 0;
+  if (lane == leader) base = atomicAdd(ctr, __popc(m));
+  base = __shfl_sync(0xFFFFFFFFu, base, leader);
+  return base + __popc(m & ((1u << lane) - 1u));
+}
+
+// Append (s, tag) to send[side] for the lanes with want (every lane of the
+// warp calls it); rows past the capacity are dropped and show up as an
+// overflowing count.
+__device__ __forceinline__ void slab_append(const SlabPlan& sp, int side, bool want, float4 s, uint32_t tag) {
+  SlabView v = slab_view(sp.send[side], sp.halo_cap);
+  const uint32_t j = warp_reserve(&sp.words[4 + side], want);
+  if (want && j < sp.halo_cap) {
     v.rows[j] = s;
     v.tags[j] = tag;
-  } else {
-    v.hdr[1] = 1u;
   }
 }
 
@@ -102,78 +117,121 @@ __global__ void k_slab_init(const uint32_t* __restrict__ order, SlabPlan sp) {
   }
   if (threadIdx.x == 0) {
     sp.words[0] = base;
-    sp.words[1] = 0u;
+    for (int k = 1; k < 8; k++) sp.words[k] = 0u;
+  }
+}
+
+// Blocks of whole warps, no early return: the appends are warp-collective.
+// One pack per substep, after the rank's step: owned particles whose column
+// left [lo, hi) go to that side as migrants (tag | kSlabMigrant; their slots
+// are freed), the others within kSlabHaloColumns of a shared edge go as halo.
+// phase 0 (before the first step) packs the halo only. The appends count
+// into words[4 + side]; the last block to finish writes the headers. Blocks
+// of whole warps and no early return: the appends are warp-collective.
+__global__ void k_slab_pack(FluidBufs d, SlabPlan sp, GridPlan g, uint32_t phase) {
+  // grid-stride over the owned slots (the loop bound is uniform per block)
+  for (uint32_t base = blockIdx.x * blockDim.x; base < sp.own_cap; base += gridDim.x * blockDim.x) {
+    const uint32_t i = base + threadIdx.x;
+    const uint32_t tag = i < sp.own_cap ? d.order[i] : kSlabFree;
+    const bool live = tag != kSlabFree;
+    const float4 s = live ? d.state[i] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    const int64_t cx = cell_column(s.x, sp.h);
+    const bool gl = phase && live && sp.has_left && cx < (int64_t)sp.lo;
+    const bool gr = phase && live && !gl && sp.has_right && cx >= (int64_t)sp.hi;
+    const bool stay = live && !gl && !gr;
+    const bool hl = stay && sp.has_left && cx < (int64_t)sp.lo + kSlabHaloColumns;
+    const bool hr = stay && sp.has_right && cx >= (int64_t)sp.hi - kSlabHaloColumns;
+    if (sp.has_left) slab_append(sp, 0, gl || hl, s, gl ? (tag | kSlabMigrant) : tag);
+    if (sp.has_right) slab_append(sp, 1, gr || hr, s, gr ? (tag | kSlabMigrant) : tag);
+    const bool go = gl || gr;
+    const uint32_t top = warp_reserve(&sp.words[0], go);  // below own_cap: each slot is on the stack at most once
+    if (go) {
+      slab_set_slot(d, g, i, empty_slot(), kSlabFree);
+      if (top < sp.own_cap)
+        sp.free_stack[top] = i;
+      else
+        atomicExch(&sp.words[1], 1u);
+    }
+  }
+  __shared__ bool last;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    last = atomicAdd(&sp.words[2], 1u) + 1u == gridDim.x;
+  }
+  __syncthreads();
+  if (last && threadIdx.x == 0) {
+    __threadfence();
+    for (int k = 0; k < 2; k++)
+      if (sp.send[k]) {
+        const uint32_t c = atomicAdd(&sp.words[4 + k], 0u);
+        uint32_t* h = reinterpret_cast<uint32_t*>(sp.send[k]);
+        h[0] = c;
+        h[1] = c > sp.halo_cap ? 1u : 0u;
+      }
     sp.words[2] = 0u;
   }
 }
 
-__global__ void k_slab_pack_halo(FluidBufs d, SlabPlan sp) {
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= sp.own_cap) return;
-  const uint32_t tag = d.order[i];
-  if (tag == kSlabFree) return;
-  const float4 s = d.state[i];
-  const int64_t cx = cell_column(s.x, sp.h);
-  if (sp.has_left && cx < (int64_t)sp.lo + kSlabHaloColumns) slab_append(sp.send[0], sp.halo_cap, s, tag);
-  if (sp.has_right && cx >= (int64_t)sp.hi - kSlabHaloColumns) slab_append(sp.send[1], sp.halo_cap, s, tag);
-}
-
-__global__ void k_slab_unpack_halo(FluidBufs d, SlabPlan sp, GridPlan g) {
+// One unpack per substep, after the exchange. Each side's halo region has
+// 2 * halo_cap slots: slot q < halo_cap takes received row q if it is halo
+// (a received migrant instead takes a free owned slot), slot halo_cap + q
+// takes the row q this rank sent to that side if it was a migrant (it now
+// lies within the neighbour's edge band, so it belongs to this rank's halo;
+// the neighbour could not send it back in the same exchange). Every other
+// halo slot is emptied. Slabs are at least 2 * kSlabHaloColumns wide, so a
+// migrant from the far side never lands in the band sent to the near one.
+__global__ void k_slab_unpack(FluidBufs d, SlabPlan sp, GridPlan g, uint32_t phase) {
   const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= 2 * sp.halo_cap) return;
-  const uint32_t side = j >= sp.halo_cap ? 1u : 0u, r = j - side * sp.halo_cap;
-  const SlabView v = slab_view(sp.recv[side], sp.halo_cap);
-  const uint32_t cnt = slab_received(sp, side, v, r == 0);
-  const uint32_t i = sp.own_cap + j;
-  if (r < cnt)
-    slab_set_slot(d, g, i, v.rows[r], v.tags[r]);
-  else if (d.order[i] != kSlabFree || finitef(d.state[i].x))
-    slab_set_slot(d, g, i, empty_slot(), kSlabFree);
-}
-
-__global__ void k_slab_pack_migrants(FluidBufs d, SlabPlan sp, GridPlan g) {
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= sp.own_cap) return;
-  const uint32_t tag = d.order[i];
-  if (tag == kSlabFree) return;
-  const float4 s = d.state[i];
-  const int64_t cx = cell_column(s.x, sp.h);
-  int side = -1;
-  if (sp.has_left && cx < (int64_t)sp.lo)
-    side = 0;
-  else if (sp.has_right && cx >= (int64_t)sp.hi)
-    side = 1;
-  if (side < 0) return;
-  slab_append(sp.send[side], sp.halo_cap, s, tag);
-  slab_set_slot(d, g, i, empty_slot(), kSlabFree);
-  const uint32_t top = atomicAdd(&sp.words[0], 1u);  // below own_cap: each slot is on the stack at most once
-  if (top < sp.own_cap)
-    sp.free_stack[top] = i;
-  else
-    atomicExch(&sp.words[1], 1u);
-}
-
-__global__ void k_slab_unpack_migrants(FluidBufs d, SlabPlan sp, GridPlan g) {
-  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= 2 * sp.halo_cap) return;
-  const uint32_t side = j >= sp.halo_cap ? 1u : 0u, r = j - side * sp.halo_cap;
-  const SlabView v = slab_view(sp.recv[side], sp.halo_cap);
-  const uint32_t cnt = slab_received(sp, side, v, r == 0);
-  if (r >= cnt) return;
-  const uint32_t size = min(sp.words[0], sp.own_cap);  // not changed by this kernel
-  const uint32_t p = atomicAdd(&sp.words[2], 1u);
-  if (p >= size) {  // the owned region is full: the particle is lost, the run reports it
-    atomicExch(&sp.words[1], 1u);
-    return;
+  const uint32_t cap = sp.halo_cap;
+  if (j == 0) {  // the pack counters start from zero again (the pack has finished)
+    sp.words[4] = 0u;
+    sp.words[5] = 0u;
   }
-  slab_set_slot(d, g, sp.free_stack[size - 1u - p], v.rows[r], v.tags[r]);
-}
-
-// Pop the slots k_slab_unpack_migrants took.
-__global__ void k_slab_settle(SlabPlan sp) {
-  const uint32_t size = min(sp.words[0], sp.own_cap), p = sp.words[2];
-  sp.words[0] = p < size ? size - p : 0u;
-  sp.words[2] = 0u;
+  if (j >= 4 * cap) return;
+  const uint32_t side = j >= 2 * cap ? 1u : 0u, q = j - side * 2 * cap;
+  const uint32_t slot = sp.own_cap + j;
+  const uint32_t has = side ? sp.has_right : sp.has_left;
+  float4 row = empty_slot();
+  uint32_t tag = kSlabFree;
+  bool halo = false;
+  if (has && q < cap) {
+    const SlabView v = slab_view(sp.recv[side], cap);
+    const uint32_t cnt = slab_received(sp, side, v, q == 0);
+    if (q < cnt) {
+      const uint32_t t = v.tags[q];
+      const float4 r = v.rows[q];
+      if (!(t & kSlabMigrant)) {
+        row = r;
+        tag = t;
+        halo = true;
+      } else if (phase == 0) {
+        atomicExch(&sp.words[1], 1u);  // no particle migrates before the first step
+      } else {
+        // pop a free owned slot (no push runs concurrently); an empty stack is reported
+        const uint32_t p = atomicSub(&sp.words[0], 1u);
+        if (p == 0u || p > sp.own_cap) {
+          atomicAdd(&sp.words[0], 1u);
+          atomicExch(&sp.words[1], 1u);
+        } else {
+          slab_set_slot(d, g, sp.free_stack[p - 1u], r, t & ~kSlabMigrant);
+        }
+      }
+    }
+  } else if (has && phase == 1) {
+    const uint32_t r = q - cap;
+    const SlabView v = slab_view(sp.send[side], cap);
+    const uint32_t cnt = min(v.hdr[0], cap);
+    if (r < cnt && (v.tags[r] & kSlabMigrant)) {
+      row = v.rows[r];
+      tag = v.tags[r] & ~kSlabMigrant;
+      halo = true;
+    }
+  }
+  if (halo)
+    slab_set_slot(d, g, slot, row, tag);
+  else if (d.order[slot] != kSlabFree || finitef(d.state[slot].x))
+    slab_set_slot(d, g, slot, empty_slot(), kSlabFree);
 }
 
 }  // namespace
@@ -183,23 +241,14 @@ void enqueue_slab_init(const FluidBufs& b, const SlabPlan& sp, cudaStream_t st) 
 }
 
 void enqueue_slab_pack(const FluidBufs& b, const SlabPlan& sp, const GridPlan& g, uint32_t phase, cudaStream_t st) {
-  for (int k = 0; k < 2; k++)
-    if (sp.send[k]) cudaMemsetAsync(sp.send[k], 0, 16, st);
-  if (sp.own_cap == 0) return;
-  if (phase == 0)
-    k_slab_pack_halo<<<cdiv(sp.own_cap, 256), 256, 0, st>>>(b, sp);
-  else
-    k_slab_pack_migrants<<<cdiv(sp.own_cap, 256), 256, 0, st>>>(b, sp, g);
+  // at most sp.pack_blocks blocks: each block takes one ticket of the last-block hand-off
+  const uint32_t blocks = std::min<uint32_t>(cdiv(sp.own_cap > 0 ? sp.own_cap : 1u, 256), sp.pack_blocks);
+  k_slab_pack<<<blocks, 256, 0, st>>>(b, sp, g, phase);
 }
 
 void enqueue_slab_unpack(const FluidBufs& b, const SlabPlan& sp, const GridPlan& g, uint32_t phase, cudaStream_t st) {
   if (sp.halo_cap == 0) return;
-  if (phase == 0) {
-    k_slab_unpack_halo<<<cdiv(2 * sp.halo_cap, 256), 256, 0, st>>>(b, sp, g);
-  } else {
-    k_slab_unpack_migrants<<<cdiv(2 * sp.halo_cap, 256), 256, 0, st>>>(b, sp, g);
-    k_slab_settle<<<1, 1, 0, st>>>(sp);
-  }
+  k_slab_unpack<<<cdiv(4 * sp.halo_cap, 256), 256, 0, st>>>(b, sp, g, phase);
 }
 
 }  // namespace phieng

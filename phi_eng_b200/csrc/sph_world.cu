@@ -123,7 +123,7 @@ struct World2 {
   bool is_batch() const { return !scenes.empty(); }
 
   // x-slab rank world (phieng_sph_slab_*): slots, exchange buffers and the
-  // free-slot stack [own_cap] + words [4] (d_slab)
+  // free-slot stack [own_cap] + words [kSlabWords] (d_slab)
   bool slab = false;
   SlabPlan slab_plan{};
   uint32_t* d_slab = nullptr;
@@ -2066,8 +2066,10 @@ int32_t phieng_sph_slab_setup(World2* w, int32_t lo, int32_t hi, uint32_t neighb
                               uint32_t halo_cap, void* send_left, void* send_right, const void* recv_left,
                               const void* recv_right) {
   if (!w || w->is_batch() || !w->d.order || hi <= lo || halo_cap == 0 || neighbours > 3u ||
-      (uint64_t)own_cap + 2ull * halo_cap != w->n)
+      (uint64_t)own_cap + 4ull * halo_cap != w->n)
     return 0;
+  // a slab between two neighbours spans at least two halo bands
+  if (neighbours == 3u && (int64_t)hi - (int64_t)lo < 2 * kSlabHaloColumns) return 0;
   if ((neighbours & 1u) && (!send_left || !recv_left)) return 0;
   if ((neighbours & 2u) && (!send_right || !recv_right)) return 0;
   // one substep per world step (the ranks agree on the substep count), and
@@ -2075,12 +2077,12 @@ int32_t phieng_sph_slab_setup(World2* w, int32_t lo, int32_t hi, uint32_t neighb
   if ((w->cfg.cfl > 0.0f && w->cfg.max_substeps > 1) || w->cfg.adaptive_resolution || w->cfg.boundary_particles)
     return 0;
   if (!prepare(w)) return 0;  // keys and bucket counts of the current slots
-  if (w->slab_cap < own_cap + 4u) {
+  if (w->slab_cap < own_cap + kSlabWords) {
     cudaStreamSynchronize(w->stream);
     dfree(w->d_slab);
     w->slab_cap = 0;
-    if (!dalloc(w, w->d_slab, (size_t)own_cap + 4u)) return 0;
-    w->slab_cap = own_cap + 4u;
+    if (!dalloc(w, w->d_slab, (size_t)own_cap + kSlabWords)) return 0;
+    w->slab_cap = own_cap + kSlabWords;
   }
   SlabPlan& sp = w->slab_plan;
   sp.lo = lo;
@@ -2096,6 +2098,9 @@ int32_t phieng_sph_slab_setup(World2* w, int32_t lo, int32_t hi, uint32_t neighb
   sp.recv[1] = sp.has_right ? static_cast<const unsigned char*>(recv_right) : nullptr;
   sp.free_stack = w->d_slab;
   sp.words = w->d_slab + own_cap;
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, w->device);
+  sp.pack_blocks = 4u * (uint32_t)std::max(sms, 1);
   enqueue_slab_init(w->d, sp, w->stream);
   w->slab = true;
   return cuda_ok(w, cudaGetLastError(), "slab setup") ? 1 : 0;

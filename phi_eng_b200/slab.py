@@ -42,7 +42,8 @@ def cell_column(x, h: float):
 
 def slab_edges(xy: np.ndarray, h: float, size: int) -> list:
     """Cell-column edges that split the particles into `size` slabs of equal
-    count (each slab at least HALO_CELLS columns wide)."""
+    count (each inner slab at least two halo bands, 2 * HALO_CELLS columns,
+    wide)."""
     import torch
 
     cx = cell_column(torch.from_numpy(np.ascontiguousarray(xy[:, 0])), h).numpy()
@@ -50,7 +51,7 @@ def slab_edges(xy: np.ndarray, h: float, size: int) -> list:
     edges = [-(1 << 40)]
     for r in range(1, size):
         e = int(cols[min(len(cols) - 1, (len(cols) * r) // size)])
-        e = max(e, edges[-1] + HALO_CELLS if r > 1 else e)
+        e = max(e, edges[-1] + 2 * HALO_CELLS if r > 1 else e)
         edges.append(e)
     edges.append(1 << 40)
     return edges
@@ -144,17 +145,19 @@ class DeviceSlabRun:
         ids = torch.nonzero((cx >= self.lo) & (cx < self.hi)).squeeze(1)
         n0 = int(ids.shape[0])
         if halo_cap is None:
-            # particles within four columns of an inner edge, with room for the flow to pile up there
-            near = 0
+            # twice the fullest halo band at the start (the HALO_CELLS columns on either side of an inner
+            # edge), plus a margin; an exchange that overflows is reported, never written past the end
+            band = 0
             for e in self.edges[1:-1]:
-                near = max(near, int(((cx >= e - 2 * HALO_CELLS) & (cx < e + 2 * HALO_CELLS)).sum()))
-            halo_cap = max(1024, 4 * near)
+                band = max(band, int(((cx >= e - HALO_CELLS) & (cx < e)).sum()),
+                           int(((cx >= e) & (cx < e + HALO_CELLS)).sum()))
+            halo_cap = 2 * band + 1024
         halo_cap = max(1, min(int(halo_cap), max(scene.n, 1)))
         if own_cap is None:
-            own_cap = min(max(scene.n, 1), n0 + max(n0 // 4, 4 * halo_cap))
+            own_cap = min(max(scene.n, 1), n0 + n0 // 8 + 2 * halo_cap)
         own_cap = max(int(own_cap), n0)
         self.own_cap, self.halo_cap = own_cap, halo_cap
-        cap = own_cap + 2 * halo_cap
+        cap = own_cap + 4 * halo_cap
         st = torch.zeros((cap, 4), dtype=torch.float32)
         st[:, :2] = float("nan")
         st[:n0, :2] = xy[ids]
@@ -188,9 +191,12 @@ class DeviceSlabRun:
         if size > 1:
             import torch.distributed as dist
 
-            self.backend = dist.get_backend()
+            if dist.is_available() and dist.is_initialized():
+                self.backend = dist.get_backend()
         self.vmax = torch.zeros(1, dtype=torch.float32, device="cuda")
         self.comm_bytes = 0
+        self.substeps = 0
+        self.primed = False
 
     def close(self) -> None:
         self.world.close()
@@ -225,22 +231,39 @@ class DeviceSlabRun:
             self.world.check()
             raise RuntimeError(name)
 
+    def pack(self, phase: int) -> None:
+        self._call("phieng_sph_slab_pack", phase)
+
+    def unpack(self, phase: int) -> None:
+        self._call("phieng_sph_slab_unpack", phase)
+
+    def local_vmax(self):
+        """Max |v| over the owned particles (device tensor of one float)."""
+        self._call("phieng_sph_slab_vmax", self.vmax.data_ptr())
+        return self.vmax
+
+    def prime(self) -> None:
+        """The first halo (before the first step)."""
+        self.pack(0)
+        self._exchange()
+        self.unpack(0)
+        self.primed = True
+
     def _substep(self, dt: float) -> None:
-        self._call("phieng_sph_slab_pack", 0)
-        self._exchange()
-        self._call("phieng_sph_slab_unpack", 0)
+        self.substeps += 1
         self.world.step(dt)
-        self._call("phieng_sph_slab_pack", 1)
+        self.pack(1)
         self._exchange()
-        self._call("phieng_sph_slab_unpack", 1)
+        self.unpack(1)
 
     def step(self, dt: float) -> None:
         """One world step of dt (CFL substeps from the global maximum speed)."""
+        if not self.primed:
+            self.prime()
         cfg = self.scene.config
         n_sub = 1
         if float(cfg.cfl) > 0 and int(cfg.max_substeps) > 1:
-            self._call("phieng_sph_slab_vmax", self.vmax.data_ptr())
-            v = self.vmax
+            v = self.local_vmax()
             if self.size > 1:
                 import torch.distributed as dist
 
@@ -278,6 +301,71 @@ class DeviceSlabRun:
         out = np.zeros((n, 4), np.float32)
         for i, s in parts:
             out[i] = s
+        return out
+
+
+class LocalSlabGroup:
+    """All ranks of a slab decomposition in one process on one GPU: the host
+    runs each phase on every rank world in turn and moves the exchange
+    buffers with device-to-device copies (no kernel waits on another rank).
+    Bit-identical to the single-domain step, like the ranks of a real run;
+    used to test the decomposition without a process group and to measure
+    what the device-side exchange adds per substep."""
+
+    def __init__(self, scene, size: int, halo_cap: int | None = None):
+        edges = slab_edges(scene.xy, float(scene.config.smoothing_length), size)
+        self.scene = scene
+        self.ranks = [DeviceSlabRun(scene, r, size, edges=edges, halo_cap=halo_cap) for r in range(size)]
+        self.copied = 0
+
+    def close(self) -> None:
+        for r in self.ranks:
+            r.close()
+
+    def _exchange(self) -> None:
+        rk = self.ranks
+        for i, r in enumerate(rk):
+            if r.left is not None:
+                r.recv[0].copy_(rk[i - 1].send[1])
+                self.copied += r.recv[0].numel()
+            if r.right is not None:
+                r.recv[1].copy_(rk[i + 1].send[0])
+                self.copied += r.recv[1].numel()
+
+    def _phase(self, phase: int) -> None:
+        for r in self.ranks:
+            r.pack(phase)
+        self._exchange()
+        for r in self.ranks:
+            r.unpack(phase)
+
+    def _substep(self, dt: float) -> None:
+        for r in self.ranks:
+            r.world.step(dt)
+        self._phase(1)
+
+    def step(self, dt: float) -> None:
+        import torch
+
+        if not self.ranks[0].primed:
+            self._phase(0)
+            for r in self.ranks:
+                r.primed = True
+        cfg = self.scene.config
+        n_sub = 1
+        if float(cfg.cfl) > 0 and int(cfg.max_substeps) > 1:
+            v = torch.stack([r.local_vmax().clone() for r in self.ranks]).max()
+            n_sub = cfl_count(cfg, dt, float(v.item()))
+        sub = float(np.float32(dt) / np.float32(n_sub))
+        for _ in range(n_sub):
+            self._substep(sub)
+
+    def gather(self):
+        parts = [r.owned() for r in self.ranks]
+        n = sum(p[1].shape[0] for p in parts)
+        out = np.zeros((n, 4), np.float32)
+        for st, ids in parts:
+            out[ids] = st
         return out
 
 
@@ -445,3 +533,128 @@ class SlabRun:
         for ids, st in parts:
             out[ids] = st
         return out
+
+
+def bench_local(workload: str = "dam_break_1m", ranks: int = 2, steps: int = 20, warmup: int = 3) -> dict:
+    """Device time per step of the single-domain world and of `ranks` rank
+    worlds run one after another on this GPU (LocalSlabGroup), split into the
+    rank worlds' steps and the exchange (pack, buffer copies, unpack); CUDA
+    events on the current stream, L2 not flushed."""
+    import torch
+
+    from . import scenes
+    from .closure import torch_stream_handle
+    from .world import world_from_scene
+
+    sc = {"dam_break_1m": scenes.dam_break_1m, "dam_break_4k": scenes.dam_break_4k}[workload]()
+    w = world_from_scene(sc)
+    w.set_stream(torch_stream_handle())
+    for _ in range(warmup):
+        w.step(sc.dt)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(steps):
+        w.step(sc.dt)
+    e1.record()
+    e1.synchronize()
+    single = e0.elapsed_time(e1) / steps
+    w.close()
+
+    g = LocalSlabGroup(sc, ranks)
+    for _ in range(warmup):
+        g.step(sc.dt)
+    torch.cuda.synchronize()
+
+    def n_substeps():
+        if float(sc.config.cfl) > 0 and int(sc.config.max_substeps) > 1:
+            v = torch.stack([r.local_vmax().clone() for r in g.ranks]).max()
+            return cfl_count(sc.config, sc.dt, float(v.item()))
+        return 1
+
+    # LocalSlabGroup.step with CUDA events around the rank worlds' steps and the exchange
+    marks = []
+    substeps = 0
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record()
+    for _ in range(steps):
+        n_sub = n_substeps()
+        sub = float(np.float32(sc.dt) / np.float32(n_sub))
+        for _ in range(n_sub):
+            substeps += 1
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+            ev[0].record()
+            for r in g.ranks:
+                r.world.step(sub)
+            ev[1].record()
+            g._phase(1)
+            ev[2].record()
+            marks.append(ev)
+    t1.record()
+    t1.synchronize()
+    total = t0.elapsed_time(t1) / steps
+    world = sum(e[0].elapsed_time(e[1]) for e in marks)
+    exch = sum(e[1].elapsed_time(e[2]) for e in marks)
+    # the same exchange captured once in a CUDA graph (all ranks' packs, the buffer copies, all
+    # unpacks): its device time without the host's per-call launch latency
+    cap_stream = torch.cuda.Stream()
+    torch.cuda.synchronize()
+    for r in g.ranks:  # outside the capture: switching streams synchronises the old one
+        r.world.set_stream(cap_stream.cuda_stream)
+    gr = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(gr, stream=cap_stream):
+        g._phase(1)
+    for r in g.ranks:
+        r.world.set_stream(torch_stream_handle())
+    torch.cuda.synchronize()
+    gexch = 0.0
+    gsub = 0
+    for _ in range(steps):
+        n_sub = n_substeps()
+        sub = float(np.float32(sc.dt) / np.float32(n_sub))
+        for _ in range(n_sub):
+            gsub += 1
+            for r in g.ranks:
+                r.world.step(sub)
+            a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a0.record()
+            gr.replay()
+            a1.record()
+            a1.synchronize()
+            gexch += a0.elapsed_time(a1)
+    rows = int(sum(r.own_cap for r in g.ranks))
+    halo = [r.halo_cap for r in g.ranks]
+    status = all(r._lib.phieng_sph_slab_status(r.world._h) == 1 for r in g.ranks)
+    gathered = g.gather()
+    g.close()
+    # the graph-replayed substeps continue the same trajectory: still the single domain's, bit for bit
+    w = world_from_scene(sc)
+    for _ in range(warmup + 2 * steps):
+        w.step(sc.dt)
+    same = bool(np.array_equal(gathered.view(np.uint32), w.fluid.particles.view(np.uint32)))
+    w.close()
+    return {"workload": workload, "particles": sc.n, "ranks": ranks, "steps": steps, "substeps": substeps,
+            "single_ms_per_step": single, "ranks_ms_per_step": total,
+            "rank_worlds_ms_per_step": world / steps, "exchange_ms_per_step": exch / steps,
+            "exchange_us_per_substep": 1000.0 * exch / substeps,
+            "exchange_graph_us_per_substep": 1000.0 * gexch / gsub,
+            "owned_slots": rows, "halo_cap": halo, "buffer_bytes": 16 + 20 * halo[0], "clean": status,
+            "bit_identical_to_single_domain": same}
+
+
+def main(argv=None) -> None:
+    import argparse
+    import json
+
+    ap = argparse.ArgumentParser(description="slab decomposition on one GPU: rank worlds run in turn")
+    ap.add_argument("cmd", choices=["bench"])
+    ap.add_argument("--workload", default="dam_break_1m")
+    ap.add_argument("--ranks", type=int, default=2)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    a = ap.parse_args(argv)
+    print(json.dumps(bench_local(a.workload, a.ranks, a.steps, a.warmup)), flush=True)
+
+
+if __name__ == "__main__":
+    main()

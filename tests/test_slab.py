@@ -231,3 +231,25 @@ def test_device_slab_reports_overflow(tmp_path):
     mp.start_processes(_worker, args=(size, _free_port(), steps, False, out, "device", 8), nprocs=size,
                        start_method="spawn")
     assert [int(np.load(out + f".ok{r}.npy")[0]) for r in range(size)] == [0, 0]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("size,cfl", [(2, False), (3, True)])
+def test_local_slab_group_equals_world(size, cfl):
+    """All ranks in one process on the one GPU, buffers moved by device
+    copies: the same bit-identical result as the process-group ranks."""
+    from phi_eng_b200.slab import LocalSlabGroup
+    from phi_eng_b200.world import world_from_scene
+
+    sc = _scene(cfl)
+    g = LocalSlabGroup(sc, size)
+    w = world_from_scene(sc)
+    for _ in range(40):
+        g.step(sc.dt)
+        w.step(sc.dt)
+    got = g.gather()
+    assert g.copied > 0
+    g.close()
+    ref = w.fluid.particles
+    w.close()
+    assert np.array_equal(got.view(np.uint32), ref.view(np.uint32))
