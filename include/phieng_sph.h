@@ -570,7 +570,8 @@ int32_t phieng_sph_closure_step(World2* world, float dt_fine, uint32_t coarse_st
 uint32_t phieng_sph_debug_forces(World2* world, float* fxy, uint32_t max);
 
 /* Run one bucket scan in which the first tile never publishes its prefix
- * (the grid must span at least two scan tiles): the other tiles' bounded
+ * (the grid must span at least two look-back blocks of the bucket scan,
+ * i.e. more than 4096 buckets): the other blocks' bounded
  * look-back waits run out, the device flag is set and read back, and the
  * world reports PHIENG_SPH_E_CUDA. Returns 1 if no wait ran out (then the
  * bound failed to trigger), 0 otherwise. Test hook for the bounded waits. */

@@ -167,7 +167,8 @@ __global__ void __launch_bounds__(256) k_scan_down(uint32_t* __restrict__ count,
 
 // Single-pass variant of k_scan_reduce + k_scan_down (decoupled look-back,
 // Merrill & Garland, "Single-pass Parallel Prefix Scan with Decoupled
-// Look-back", 2016): tiles are taken in ticket order; each publishes its sum
+// Look-back", 2016), one block per supertile of kBucketScanSuper scan tiles:
+// supertiles are taken in ticket order; each publishes its sum
 // (flag 1) at once, then walks back over its predecessors' published values
 // until it meets an inclusive prefix (flag 2), and publishes its own
 // inclusive prefix. A block only waits for tiles that took an earlier ticket,
@@ -180,38 +181,68 @@ __global__ void __launch_bounds__(256) k_scan_down(uint32_t* __restrict__ count,
 constexpr uint32_t kScanSpinLimit = 1u << 20;
 constexpr unsigned long long kTileAgg = 1ull << 32, kTileIncl = 2ull << 32;
 
-__global__ void __launch_bounds__(256) k_scan_lookback(uint32_t* __restrict__ count, uint32_t ntiles,
-                                                       uint32_t* __restrict__ start,
-                                                       unsigned long long* __restrict__ tstate,
-                                                       uint32_t* __restrict__ ctr, uint32_t* __restrict__ err,
-                                                       uint32_t silent) {
-  __shared__ uint32_t warp_tot[8];
+// Each look-back block of 256 * kLookbackSub threads scans kLookbackSub
+// consecutive scan tiles (a "supertile"), 16 counts per thread: every count
+// is loaded at once, as with one tile per 256-thread block, but the
+// look-back chain (a block walks its predecessors 32 at a time) is
+// kLookbackSub times shorter. The count arrays keep their padding to whole
+// scan tiles: a thread whose tile lies past the last does nothing.
+constexpr uint32_t kLookbackSub = kBucketScanSuper;
+constexpr uint32_t kLookbackThreads = 256 * kLookbackSub;
+
+// Block-wide inclusive scan of one value per thread (kLookbackThreads).
+__device__ __forceinline__ uint32_t block_incl_scan_big(uint32_t v, uint32_t* warp_tot) {
+  const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  uint32_t x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+    if (lane >= (uint32_t)o) x += y;
+  }
+  if (lane == 31) warp_tot[w] = x;
+  __syncthreads();
+  uint32_t add = 0;
+  for (uint32_t k = 0; k < w; k++) add += warp_tot[k];
+  return x + add;
+}
+
+__global__ void __launch_bounds__(kLookbackThreads) k_scan_lookback(uint32_t* __restrict__ count, uint32_t nsub,
+                                                                    uint32_t* __restrict__ start,
+                                                                    unsigned long long* __restrict__ tstate,
+                                                                    uint32_t* __restrict__ ctr,
+                                                                    uint32_t* __restrict__ err, uint32_t silent) {
+  constexpr uint32_t kWarps = kLookbackThreads / 32;
+  __shared__ uint32_t warp_tot[kWarps];
   __shared__ uint32_t s_tile, s_prefix;
   __shared__ bool s_last;
   if (threadIdx.x == 0) s_tile = atomicAdd(&ctr[0], 1u);
   __syncthreads();
   const uint32_t t = s_tile;
-  const uint32_t base = t * kScanTile + threadIdx.x * 16;
-  uint4* c4 = reinterpret_cast<uint4*>(count + base);
+  const bool mine = t * kLookbackSub + threadIdx.x / 256 < nsub;  // this thread's scan tile exists
+  const size_t base = (size_t)t * kLookbackThreads * 16 + threadIdx.x * 16;
   uint32_t v[16];
-#pragma unroll
-  for (int r = 0; r < 4; r++) {
-    const uint4 q = c4[r];
-    v[4 * r] = q.x;
-    v[4 * r + 1] = q.y;
-    v[4 * r + 2] = q.z;
-    v[4 * r + 3] = q.w;
-  }
   uint32_t sum = 0;
+  if (mine) {
+    const uint4* c4 = reinterpret_cast<const uint4*>(count + base);
 #pragma unroll
-  for (int q = 0; q < 16; q++) sum += v[q];
-  const uint32_t incl = block_incl_scan_256(sum, warp_tot);
+    for (int r = 0; r < 4; r++) {
+      const uint4 q = c4[r];
+      v[4 * r] = q.x;
+      v[4 * r + 1] = q.y;
+      v[4 * r + 2] = q.z;
+      v[4 * r + 3] = q.w;
+    }
+#pragma unroll
+    for (int q = 0; q < 16; q++) sum += v[q];
+  }
+  const uint32_t incl = block_incl_scan_big(sum, warp_tot);
   if (threadIdx.x < 32) {
-    // warp 0: publish this tile's sum, then look back 32 predecessors at a
-    // time (lane k reads tile t-1-k; tiles before 0 count as an inclusive 0)
+    // warp 0: publish this supertile's sum, then look back 32 predecessors
+    // at a time (lane k reads supertile t-1-k; before 0 counts as an
+    // inclusive 0)
     const uint32_t lane = threadIdx.x;
     uint32_t total = 0;
-    for (int k = 0; k < 8; k++) total += warp_tot[k];
+    for (uint32_t k = 0; k < kWarps; k++) total += warp_tot[k];
     uint32_t excl = 0;
     if (t == 0) {
       if (lane == 0 && t != silent) atomicExch(&tstate[0], kTileIncl | total);
@@ -237,10 +268,10 @@ __global__ void __launch_bounds__(256) k_scan_lookback(uint32_t* __restrict__ co
         const uint32_t incl_lanes = __ballot_sync(0xFFFFFFFFu, flag == 2u);
         // lanes up to the nearest inclusive prefix (all 32 if none)
         const uint32_t upto = incl_lanes ? (uint32_t)(__ffs((int)incl_lanes) - 1) : 31u;
-        uint32_t v = lane <= upto ? (uint32_t)sv : 0u;
+        uint32_t val = lane <= upto ? (uint32_t)sv : 0u;
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
-        excl += v;
+        for (int o = 16; o > 0; o >>= 1) val += __shfl_xor_sync(0xFFFFFFFFu, val, o);
+        excl += val;
         if (incl_lanes) break;
         top -= 32;
       }
@@ -249,19 +280,22 @@ __global__ void __launch_bounds__(256) k_scan_lookback(uint32_t* __restrict__ co
     if (lane == 0) s_prefix = excl;
   }
   __syncthreads();
-  uint32_t run = s_prefix + incl - sum;
+  if (mine) {
+    uint32_t run = s_prefix + incl - sum;
 #pragma unroll
-  for (int q = 0; q < 16; q++) {
-    const uint32_t x = v[q];
-    v[q] = run;
-    run += x;
-  }
-  uint4* s4 = reinterpret_cast<uint4*>(start + base);
+    for (int q = 0; q < 16; q++) {
+      const uint32_t x = v[q];
+      v[q] = run;
+      run += x;
+    }
+    uint4* c4 = reinterpret_cast<uint4*>(count + base);
+    uint4* s4 = reinterpret_cast<uint4*>(start + base);
 #pragma unroll
-  for (int r = 0; r < 4; r++) {
-    const uint4 q = make_uint4(v[4 * r], v[4 * r + 1], v[4 * r + 2], v[4 * r + 3]);
-    c4[r] = q;
-    s4[r] = q;  // the padded tail past the last key gets the particle count: never read
+    for (int r = 0; r < 4; r++) {
+      const uint4 q = make_uint4(v[4 * r], v[4 * r + 1], v[4 * r + 2], v[4 * r + 3]);
+      c4[r] = q;
+      s4[r] = q;  // the padded tail past the last key gets the particle count: never read
+    }
   }
   if (threadIdx.x == 0) {
     __threadfence();
@@ -269,7 +303,7 @@ __global__ void __launch_bounds__(256) k_scan_lookback(uint32_t* __restrict__ co
   }
   __syncthreads();
   if (s_last) {
-    for (uint32_t i = threadIdx.x; i < ntiles; i += blockDim.x) tstate[i] = 0ull;
+    for (uint32_t i = threadIdx.x; i < gridDim.x; i += blockDim.x) tstate[i] = 0ull;
     if (threadIdx.x == 0) {
       ctr[0] = 0u;
       ctr[1] = 0u;
@@ -380,15 +414,11 @@ __global__ void __launch_bounds__(256) k_place(const uint32_t* __restrict__ key,
 // tags, the sentinel bucket of non-finite particles keeps its placement
 // slots: no walk visits it, and its size (a rank world's unused slots) would
 // make ranking quadratic.
-__global__ void __launch_bounds__(256) k_fixup(const uint32_t* __restrict__ tkey,
-                                               const uint32_t* __restrict__ tid_in,
-                                               const uint32_t* __restrict__ start, uint32_t n,
-                                               uint32_t* __restrict__ skey, uint32_t* __restrict__ sid,
-                                               const uint32_t* __restrict__ order, uint32_t sentinel,
-                                               GatherArgs ga) {
-  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= n) return;
-  const uint32_t id = tid_in[s];
+__device__ __forceinline__ void fixup_slot(uint32_t s, uint32_t id, const uint32_t* __restrict__ tkey,
+                                           const uint32_t* __restrict__ tid_in, const uint32_t* __restrict__ start,
+                                           uint32_t* __restrict__ skey, uint32_t* __restrict__ sid,
+                                           const uint32_t* __restrict__ order, uint32_t sentinel,
+                                           const GatherArgs& ga) {
   if (id & kPlacedFinal) {  // k_place_final finished this bucket but its sid
     sid[s] = id & ~kPlacedFinal;
     return;
@@ -407,6 +437,36 @@ __global__ void __launch_bounds__(256) k_fixup(const uint32_t* __restrict__ tkey
     for (uint32_t j = lo; j < hi; j++) rank += __ldg(&tid_in[j]) < id ? 1u : 0u;
   }
   gather_slot(lo + rank, k, id, ga, skey, sid);
+}
+
+// Four slots per thread: where all four were finished by k_place_final (the
+// common case) one 16-byte load and store; the others one by one. The same
+// threads clear the bucket counts for the next sort (the placement, which
+// used them as cursors, has finished): count_len is a multiple of the scan
+// tile, so whole uint4 stores.
+__global__ void __launch_bounds__(256) k_fixup(const uint32_t* __restrict__ tkey,
+                                               const uint32_t* __restrict__ tid_in,
+                                               const uint32_t* __restrict__ start, uint32_t n,
+                                               uint32_t* __restrict__ skey, uint32_t* __restrict__ sid,
+                                               const uint32_t* __restrict__ order, uint32_t sentinel,
+                                               uint32_t* __restrict__ count, uint32_t count_len, GatherArgs ga) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (4u * t < count_len) reinterpret_cast<uint4*>(count)[t] = make_uint4(0u, 0u, 0u, 0u);
+  const uint32_t s0 = 4u * t;
+  if (s0 >= n) return;
+  if (s0 + 3u < n) {
+    const uint4 v = *reinterpret_cast<const uint4*>(tid_in + s0);
+    if ((v.x & v.y & v.z & v.w) & kPlacedFinal) {
+      *reinterpret_cast<uint4*>(sid + s0) =
+          make_uint4(v.x & ~kPlacedFinal, v.y & ~kPlacedFinal, v.z & ~kPlacedFinal, v.w & ~kPlacedFinal);
+      return;
+    }
+    const uint32_t ids[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+    for (int q = 0; q < 4; q++) fixup_slot(s0 + q, ids[q], tkey, tid_in, start, skey, sid, order, sentinel, ga);
+    return;
+  }
+  for (uint32_t s = s0; s < n; s++) fixup_slot(s, tid_in[s], tkey, tid_in, start, skey, sid, order, sentinel, ga);
 }
 
 // ---------------------------------------------------------------- neighbour walk
@@ -1088,7 +1148,8 @@ void enqueue_keys(const FluidBufs& b, uint32_t n, const GridPlan& g, cudaStream_
 void enqueue_bucket_scan(const BucketSort& bs, uint32_t m, cudaStream_t st) {
   const uint32_t nt = cdiv(m, kScanTile);
   if (bs.tstate) {
-    k_scan_lookback<<<nt, 256, 0, st>>>(bs.count, nt, bs.start, bs.tstate, bs.done, bs.err, 0xFFFFFFFFu);
+    k_scan_lookback<<<cdiv(nt, kLookbackSub), kLookbackThreads, 0, st>>>(bs.count, nt, bs.start, bs.tstate, bs.done,
+                                                                          bs.err, 0xFFFFFFFFu);
   } else {
     k_scan_reduce<<<nt, 256, 0, st>>>(bs.count, bs.tilesum, nt, bs.done);
     k_scan_down<<<nt, 256, 0, st>>>(bs.count, bs.tilesum, m, bs.start);
@@ -1135,9 +1196,10 @@ void enqueue_sort_and_ranges(const FluidBufs& b, uint32_t n, const StepParams& P
   else
     k_place_final<false><<<cdiv(n, 256), 256, 0, st>>>(b.key, b.sid, n, b.count, b.start, b.tkey, b.tid, b.skey,
                                                         b.order, ga);
-  k_fixup<<<cdiv(n, 256), 256, 0, st>>>(b.tkey, b.tid, b.start, n, b.skey, b.sid, b.order, P.grid.sentinel, ga);
-  // the counts of the next sort accumulate from zero (K6)
-  cudaMemsetAsync(b.count, 0, sizeof(uint32_t) * b.count_len, st);
+  // the fixup also clears the counts: the next sort's accumulate from zero (K6)
+  const uint32_t quads = std::max(cdiv(n, 4), cdiv(b.count_len, 4));
+  k_fixup<<<cdiv(quads, 256), 256, 0, st>>>(b.tkey, b.tid, b.start, n, b.skey, b.sid, b.order, P.grid.sentinel,
+                                             b.count, b.count_len, ga);
 }
 
 // ---------------------------------------------------------------- adaptive resolution
@@ -1591,8 +1653,9 @@ void enqueue_buoyancy(const FluidBufs& b, const DynBufs& y, uint32_t n, const St
 
 void enqueue_scan_silent_tile(const FluidBufs& b, uint32_t m, cudaStream_t st) {
   const uint32_t nt = cdiv(m, kScanTile);
-  if (!b.tstate || nt < 2) return;
-  k_scan_lookback<<<nt, 256, 0, st>>>(b.count, nt, b.start, b.tstate, b.done, b.scan_err, 0u);
+  if (!b.tstate || cdiv(nt, kLookbackSub) < 2) return;
+  k_scan_lookback<<<cdiv(nt, kLookbackSub), kLookbackThreads, 0, st>>>(b.count, nt, b.start, b.tstate, b.done,
+                                                                        b.scan_err, 0u);
 }
 
 void enqueue_unsort_dp(const FluidBufs& b, uint32_t n, float* dens, float* pres, cudaStream_t st) {

@@ -2367,7 +2367,8 @@ int32_t phieng_sph_closure_step(World2* w, float dt_fine, uint32_t coarse_steps,
 int32_t phieng_sph_debug_scan_timeout(World2* w) {
   if (!w || !prepare(w)) return 0;
   const uint32_t m = w->plan.sentinel + 1;
-  if ((m + kBucketScanTile - 1) / kBucketScanTile < 2) return 0;
+  // at least two look-back blocks
+  if ((m + kBucketScanTile * kBucketScanSuper - 1) / (kBucketScanTile * kBucketScanSuper) < 2) return 0;
   enqueue_scan_silent_tile(w->d, m, w->stream);
   if (!cuda_ok(w, cudaGetLastError(), "scan")) return 0;
   w->keys_valid = false;  // the counts became cursors

@@ -16,6 +16,7 @@ F = C.POINTER(C.c_float)
 
 def make_world(lib, nx=64, ny=64):
     w = lib.phieng_world_new()
+    lib.phieng_sph_set_particle_cap(w, max(nx * ny, 4096))
     pts = np.array([(ix * 0.25, iy * 0.25) for iy in range(ny) for ix in range(nx)], np.float32)
     assert lib.phieng_world_fluid_add(w, pts.ctypes.data_as(F), len(pts)) == len(pts)
     return w
@@ -24,12 +25,12 @@ def make_world(lib, nx=64, ny=64):
 @pytest.mark.gpu
 def test_scan_wait_runs_out_and_is_reported():
     lib = _abi.load()
-    w = make_world(lib)
+    w = make_world(lib, 128, 128)
     lib.phieng_world_step(w, 1 / 60)
     assert lib.phieng_sph_sync(w) == 1
     st = _abi.PhiengSphStatus()
     lib.phieng_sph_status(w, C.byref(st))
-    assert st.grid_buckets + 1 > 4096  # at least two scan tiles
+    assert st.grid_buckets + 1 > 4 * 4096  # at least two look-back blocks (of up to four scan tiles)
     assert lib.phieng_sph_debug_scan_timeout(w) == 0
     lib.phieng_sph_status(w, C.byref(st))
     assert st.error == _abi.E_CUDA
