@@ -345,8 +345,8 @@ def closure_line(sc, precision: int) -> dict:
                 "front_travel_plain": fp["front"] - float(np.max(sc.xy[:, 0])), "coarse_steps": steps}
 
     out = {"metric": "simulated s per wall s", "dt_ratio": 4, "threshold": 0.03,
-           "precision": "tolerance (network on the tcgen05 tensor cores)" if precision == _abi.TOLERANCE
-           else "exact (network on mma.sync)"}
+           "precision": f"tolerance (fast pair arithmetic, network on {mlp.closure_engine})"
+           if precision == _abi.TOLERANCE else "exact (network on mma.sync)"}
     jump = run(50, _abi.CLOSURE_JUMP, 10)
     out.update(jump, criterion="jump (largest per-particle density increase over the coarse step)")
     out["literal_rule"] = dict(run(50, _abi.CLOSURE_COMPRESSION, 10),

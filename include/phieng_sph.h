@@ -521,6 +521,16 @@ int32_t phieng_mlp_apply_grad(PhiengMlp* mlp, const float* grad, float lr);
 int32_t phieng_mlp_set_train_engine(PhiengMlp* mlp, int32_t engine);
 /* The current training path (-1 for a null network). */
 int32_t phieng_mlp_get_train_engine(const PhiengMlp* mlp);
+/* Network of the tolerance-mode coarse pass of phieng_sph_closure_step
+ * (PHIENG_SPH_TOLERANCE worlds with the plain flag set): PHIENG_MLP_MMA_SYNC
+ * (default: 256-particle blocks, warp-level mma.sync tiles; 132 us per
+ * coarse pass at 2^20 particles on B200) or PHIENG_MLP_TCGEN05 (one
+ * persistent pass, 128-particle tiles through the tcgen05 tensor cores; 167
+ * us: each tile's three dependent MMA round trips are latency-bound). The
+ * same numerics; results agree within the network's tolerance. The exact
+ * mode's coarse pass always uses mma.sync. */
+int32_t phieng_mlp_set_closure_engine(PhiengMlp* mlp, int32_t engine);
+int32_t phieng_mlp_get_closure_engine(const PhiengMlp* mlp);
 /* The pair indices of one minibatch (device idx[batch]). */
 int32_t phieng_mlp_sample_indices(uint32_t npairs, uint32_t batch, uint64_t seed, uint32_t iter, uint32_t* idx,
                                   void* stream);

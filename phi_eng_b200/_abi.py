@@ -363,6 +363,8 @@ SIGNATURES = {
     "phieng_mlp_forward_tc": (C.c_int32, [_P, _P, C.c_uint32, _P]),
     "phieng_mlp_check_waits": (C.c_int32, [_P]),
     "phieng_mlp_set_train_engine": (C.c_int32, [_P, C.c_int32]),
+    "phieng_mlp_set_closure_engine": (C.c_int32, [_P, C.c_int32]),
+    "phieng_mlp_get_closure_engine": (C.c_int32, [_P]),
     "phieng_mlp_shard_grad": (C.c_int32, [_P, _P, _P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64,
                                           _P]),
     "phieng_mlp_apply_grad": (C.c_int32, [_P, _P, C.c_float]),

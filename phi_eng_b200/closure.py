@@ -147,6 +147,17 @@ class Mlp:
         if code is None or self._lib.phieng_mlp_set_train_engine(self._h, code) != 1:
             raise ValueError(f"training engine {name!r}: 'tcgen05' or 'mma.sync'")
 
+    @property
+    def closure_engine(self) -> str:
+        """Network of the tolerance-mode coarse pass: "tcgen05" or "mma.sync"."""
+        return "tcgen05" if self._lib.phieng_mlp_get_closure_engine(self._h) == _abi.MLP_TCGEN05 else "mma.sync"
+
+    @closure_engine.setter
+    def closure_engine(self, name: str) -> None:
+        code = {"tcgen05": _abi.MLP_TCGEN05, "mma.sync": _abi.MLP_MMA_SYNC}.get(name)
+        if code is None or self._lib.phieng_mlp_set_closure_engine(self._h, code) != 1:
+            raise ValueError(f"closure engine {name!r}: 'tcgen05' or 'mma.sync'")
+
     def grad(self, x, t, batch: int, seed: int, it: int):
         self._on_current_stream()
         g = np.zeros(NPARAMS, np.float32)
@@ -672,6 +683,8 @@ def _main(argv=None) -> None:
     e.add_argument("--zero", action="store_true", help="evaluate a zero network (no correction)")
     e.add_argument("--ratio", type=int, default=0, help="coarse step = ratio * dt (0: the weights' own ratio)")
     e.add_argument("--precision", choices=["exact", "tolerance"], default="exact")
+    e.add_argument("--net-engine", choices=["tcgen05", "mma.sync"], default=None,
+                   help="network of the tolerance-mode coarse pass (default: the network's setting)")
     fb = sub.add_parser("forward-bench", help="time the network's forward pass, mma.sync against tcgen05")
     fb.add_argument("--weights", default=WEIGHTS)
     fb.add_argument("--rows", default="262144,1048576,4194304")
@@ -743,6 +756,8 @@ def _main(argv=None) -> None:
         return
     sc = S.dam_break_1m() if a.workload == "dam_break_1m" else S.dam_break_4k()
     mlp = Mlp() if a.zero else Mlp.load(a.weights)
+    if a.net_engine:
+        mlp.closure_engine = a.net_engine
     crit = {"jump": _abi.CLOSURE_JUMP, "compression": _abi.CLOSURE_COMPRESSION, "growth": _abi.CLOSURE_GROWTH}[a.criterion]
     ratio = a.ratio
     if ratio <= 0:
@@ -752,7 +767,8 @@ def _main(argv=None) -> None:
                 ratio = int(z["ratio"]) if "ratio" in z.files else 4
     r = evaluate(sc, mlp, coarse_steps=a.coarse_steps, ratio=ratio, threshold=a.threshold, criterion=crit,
                  precision=_abi.TOLERANCE if a.precision == "tolerance" else _abi.EXACT)
-    print(json.dumps(dict(workload=a.workload, weights=None if a.zero else a.weights, **r)))
+    print(json.dumps(dict(workload=a.workload, weights=None if a.zero else a.weights,
+                          closure_engine=mlp.closure_engine, **r)))
 
 
 if __name__ == "__main__":

@@ -1398,6 +1398,17 @@ void launch_closure(const FluidBufs& b, uint32_t n, const StepParams& P, const M
                     cudaStream_t st) {
   const bool m = (P.flags & F_MASS) != 0, ph = (P.flags & F_PHASE) != 0, bat = b.batch.ptab != nullptr;
   const bool plain = plain_flags(P.flags) && !m && !ph;
+  if (MODE == kModeClosure && fast_flags(P.flags) && mlp.engine == kMlpInferMmaSync) {
+    // tolerance mode, network on mma.sync warp tiles
+#define PHIENG_CLOSURE_F(BT)                                                                                       \
+  k_closure_fast<BT><<<cdiv(n, 256), 256, closure_smem_bytes(), st>>>(b.spos, b.svel, b.sdq, b.spres, b.skey,     \
+                                                                      b.sid, n, b.start, P, b.batch, b.bodies,    \
+                                                                      b.nmask, mlp, io, b.state, b.key, b.count)
+    if (bat) PHIENG_CLOSURE_F(true);
+    else PHIENG_CLOSURE_F(false);
+#undef PHIENG_CLOSURE_F
+    return;
+  }
   if (MODE == kModeClosure && fast_flags(P.flags) && io.err) {
     // tolerance mode: fused pass with the network on the tcgen05 tensor cores
     int dev = 0, sms = 148;

@@ -36,6 +36,9 @@
 #include "sph_mlp_host.h"
 #include "sph_tc_net.cuh"
 
+static_assert(phieng::kMlpInferTcgen05 == PHIENG_MLP_TCGEN05 && phieng::kMlpInferMmaSync == PHIENG_MLP_MMA_SYNC,
+              "engine codes");
+
 namespace phieng {
 namespace {
 
@@ -939,6 +942,7 @@ struct PhiengMlp {
   uint32_t loss_cap = 0;
   float* h_pinned = nullptr;
   int32_t train_engine = PHIENG_MLP_TCGEN05;
+  int32_t infer_engine = PHIENG_MLP_MMA_SYNC;  // network of the tolerance-mode coarse pass (measured faster)
 };
 
 namespace {
@@ -1004,11 +1008,12 @@ bool launch_tile(PhiengMlp* m, const float* x, const float* t, uint32_t npairs, 
 }  // namespace
 
 MlpDev phieng_mlp_dev(const PhiengMlp* m) {
-  MlpDev d;
+  MlpDev d{};
   d.frag = m->frag;
   d.bias = m->bias;
   d.w3 = m->w3;
   d.norm = m->norm;
+  d.engine = m->infer_engine;
   return d;
 }
 
@@ -1261,6 +1266,14 @@ int32_t phieng_mlp_set_train_engine(PhiengMlp* m, int32_t engine) {
 }
 
 int32_t phieng_mlp_get_train_engine(const PhiengMlp* m) { return m ? m->train_engine : -1; }
+
+int32_t phieng_mlp_set_closure_engine(PhiengMlp* m, int32_t engine) {
+  if (!m || m->error || (engine != PHIENG_MLP_TCGEN05 && engine != PHIENG_MLP_MMA_SYNC)) return 0;
+  m->infer_engine = engine;
+  return 1;
+}
+
+int32_t phieng_mlp_get_closure_engine(const PhiengMlp* m) { return m ? m->infer_engine : -1; }
 
 int32_t phieng_mlp_sample_indices(uint32_t npairs, uint32_t batch, uint64_t seed, uint32_t iter, uint32_t* idx,
                                   void* stream) {

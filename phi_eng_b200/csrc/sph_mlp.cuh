@@ -66,7 +66,15 @@ struct MlpDev {
   const float* bias;
   const float* w3;
   const float* norm;
+  // network of the tolerance-mode coarse pass: kMlpInferTcgen05 or
+  // kMlpInferMmaSync (64-bit: no padding bytes, the struct is part of a graph
+  // signature)
+  int64_t engine;
 };
+
+// (the values of PHIENG_MLP_TCGEN05 / PHIENG_MLP_MMA_SYNC)
+constexpr int32_t kMlpInferTcgen05 = 0;
+constexpr int32_t kMlpInferMmaSync = 1;
 
 // Position (in BF16 elements) of B(k, n) inside an image with nt n-tiles.
 __host__ __device__ inline uint32_t frag_pos(int k, int n, int nt_count) {

@@ -433,15 +433,19 @@ def test_zero_network_closure_equals_plain_coarse_step():
 
 
 @pytest.mark.gpu
-def test_tolerance_zero_network_closure_equals_plain_coarse_step():
+@pytest.mark.parametrize("engine", ENGINES)
+def test_tolerance_zero_network_closure_equals_plain_coarse_step(engine):
     """Tolerance mode: the fused coarse pass (tolerance-mode pair arithmetic,
-    network on the tcgen05 tensor cores) with a zero network equals the
-    plain tolerance-mode substep of 4 dt bit for bit."""
+    network on the tcgen05 tensor cores or on mma.sync warp tiles) with a
+    zero network equals the plain tolerance-mode substep of 4 dt bit for
+    bit."""
     from phi_eng_b200 import _abi
     from phi_eng_b200.closure import Mlp
 
     sc = scenes.dam_break_4k()
     m = Mlp()
+    m.closure_engine = engine
+    assert m.closure_engine == engine
     plain, clo = _world(sc), _world(sc)
     for w in (plain, clo):
         w.precision = _abi.TOLERANCE
@@ -457,17 +461,19 @@ def test_tolerance_zero_network_closure_equals_plain_coarse_step():
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("engine", ENGINES)
 @pytest.mark.parametrize("name", ["dam_break_4k", "dam_break_128x128"])
-def test_tolerance_closure_step_close_to_exact(name):
+def test_tolerance_closure_step_close_to_exact(name, engine):
     """One coarse step with the shipped network from the same state, in the
-    tolerance mode (fused tcgen05 pass) and in the exact mode (mma.sync
-    network): positions agree to a small fraction of h, and the check values
-    agree closely."""
+    tolerance mode (fused pass, network on either engine) and in the exact
+    mode (mma.sync network): positions agree to a small fraction of h, and
+    the check values agree closely."""
     from phi_eng_b200 import _abi
     from phi_eng_b200 import closure as cl
 
     sc = scenes.dam_break_4k() if name == "dam_break_4k" else scenes.dam_break_scaled(128, 128)
     m = cl.Mlp.load(cl.WEIGHTS)
+    m.closure_engine = engine
     h = float(sc.config.smoothing_length)
     ws = []
     for mode in (_abi.EXACT, _abi.TOLERANCE):
