@@ -244,11 +244,15 @@ def test_local_slab_group_equals_world(size, cfl):
     sc = _scene(cfl)
     g = LocalSlabGroup(sc, size)
     w = world_from_scene(sc)
+    before = [set(r.owned()[1].tolist()) for r in g.ranks]
     for _ in range(40):
         g.step(sc.dt)
         w.step(sc.dt)
+    after = [set(r.owned()[1].tolist()) for r in g.ranks]
     got = g.gather()
     assert g.copied > 0
+    assert any(a != b for a, b in zip(before, after))  # particles changed rank on the way
+    assert sum(len(a) for a in after) == sc.n
     g.close()
     ref = w.fluid.particles
     w.close()
