@@ -272,7 +272,7 @@ def test_local_slab_group_migrants_cross_the_edge():
     g = LocalSlabGroup(sc, 2, edges=[-(1 << 40), edge, 1 << 40])
     w = world_from_scene(sc)
     before = [set(r.owned()[1].tolist()) for r in g.ranks]
-    for _ in range(60):
+    for _ in range(80):  # on the oracle, 43 particles have crossed by step 60
         g.step(sc.dt)
         w.step(sc.dt)
     after = [set(r.owned()[1].tolist()) for r in g.ranks]
