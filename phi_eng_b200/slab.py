@@ -312,10 +312,11 @@ class LocalSlabGroup:
     used to test the decomposition without a process group and to measure
     what the device-side exchange adds per substep."""
 
-    def __init__(self, scene, size: int, halo_cap: int | None = None, edges=None):
+    def __init__(self, scene, size: int, halo_cap: int | None = None, edges=None, own_cap: int | None = None):
         edges = edges or slab_edges(scene.xy, float(scene.config.smoothing_length), size)
         self.scene = scene
-        self.ranks = [DeviceSlabRun(scene, r, size, edges=edges, halo_cap=halo_cap) for r in range(size)]
+        self.ranks = [DeviceSlabRun(scene, r, size, edges=edges, halo_cap=halo_cap, own_cap=own_cap)
+                      for r in range(size)]
         self.copied = 0
 
     def close(self) -> None:

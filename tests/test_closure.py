@@ -343,6 +343,9 @@ def test_training_engine_rejects_unknown():
     m = Mlp()
     with pytest.raises(ValueError):
         m.train_engine = "wmma"
+    with pytest.raises(ValueError):
+        m.closure_engine = "wmma"
+    assert m.train_engine == "tcgen05" and m.closure_engine == "mma.sync"  # the defaults
 
 
 @pytest.mark.gpu

@@ -283,3 +283,26 @@ def test_local_slab_group_migrants_cross_the_edge():
     assert len(after[1] - before[1]) > 0  # particles moved into the right rank
     assert sum(len(a) for a in after) == sc.n
     assert np.array_equal(got.view(np.uint32), ref.view(np.uint32))
+
+
+@pytest.mark.gpu
+def test_local_slab_group_reports_a_full_owned_region():
+    """An owned region with no spare slot (the right rank's own_cap is its
+    initial count): the migrants that arrive there find no free slot, which
+    is reported (the unpack drops them), not written past the region."""
+    import torch
+
+    from phi_eng_b200.slab import LocalSlabGroup, cell_column
+
+    sc = _scene(False)
+    h = float(sc.config.smoothing_length)
+    cx = cell_column(torch.from_numpy(np.ascontiguousarray(sc.xy[:, 0])), h)
+    edge = int(cx.max()) - 4
+    n_right = int((cx >= edge).sum())
+    # the right rank starts full (own_cap = its initial count; the left one's region is its own count)
+    g = LocalSlabGroup(sc, 2, edges=[-(1 << 40), edge, 1 << 40], own_cap=n_right)
+    for _ in range(80):
+        g.step(sc.dt)
+    with pytest.raises(RuntimeError):
+        g.ranks[1].owned()
+    g.close()
