@@ -376,6 +376,7 @@ def fluid3d_line(steps: int, warmup: int, side: int = 100) -> dict:
     reference's particle cap (4096) beside it."""
     import torch
 
+    from phi_eng_b200 import _abi
     from phi_eng_b200.world3 import World3, dam_break_3d
 
     L = side * 0.25
@@ -390,24 +391,36 @@ def fluid3d_line(steps: int, warmup: int, side: int = 100) -> dict:
     w.set_stream(stream.cuda_stream)
     dt = 1.0 / 60.0
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
     for _ in range(max(warmup, 3)):
         w.step(dt)
-    w.set_profiling(True)
-    w.step(dt)
-    buckets = w.status().grid_buckets
-    torch.cuda.synchronize()
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
-    phases = []
-    for k in range(steps):
-        with torch.cuda.stream(stream):
-            flush.zero_()
-        ev[k][0].record(stream)
+    s0 = w.fluid.particles  # both modes are timed from this state
+
+    def timed():
+        w.fluid.set_state(s0)
+        for _ in range(3):
+            w.step(dt)
+        w.set_profiling(True)
         w.step(dt)
-        ev[k][1].record(stream)
-        phases.append(w.phase_times())
-    torch.cuda.synchronize()
-    ms = sum(a.elapsed_time(b) for a, b in ev) / steps
-    ph = np.array(phases).mean(axis=0)
+        torch.cuda.synchronize()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        phases = []
+        for k in range(steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+            ev[k][0].record(stream)
+            w.step(dt)
+            ev[k][1].record(stream)
+            phases.append(w.phase_times())
+        torch.cuda.synchronize()
+        w.set_profiling(False)
+        return sum(a.elapsed_time(b) for a, b in ev) / steps, np.array(phases).mean(axis=0)
+
+    # the exact mode, then the tolerance mode (the line's value), each from s0
+    ms_exact, ph_exact = timed()
+    w.precision = _abi.TOLERANCE
+    ms, ph = timed()
+    buckets = w.status().grid_buckets
     names = ["sort_ranges", "density", "force_integrate"]
     bytes_pp = [104 + 20 * buckets / n, DENSITY3_BYTES, FORCE3_BYTES]
     top = int(np.argmax(ph))
@@ -429,7 +442,10 @@ def fluid3d_line(steps: int, warmup: int, side: int = 100) -> dict:
     return {"metric": METRIC, "value": n / (ms / 1000.0), "ms_per_step": ms, "particles": n,
             "workload": f"3D dam break, {side}^3 particles at 0.25 m in a {2.5 * L:g} x {1.5 * L:g} x {1.5 * L:g} m "
                         "tank (floor + 4 walls), FluidConfig3 defaults, dt = 1/60",
+            "precision": "tolerance",
             "phases_ms": {nm: float(v) for nm, v in zip(names, ph)}, "buckets": int(buckets),
+            "exact_mode": {"value": n / (ms_exact / 1000.0), "ms_per_step": ms_exact,
+                           "phases_ms": {nm: float(v) for nm, v in zip(names, ph_exact)}},
             "roofline": {"bound": "hbm", "kernel": names[top], "bytes_per_particle": bytes_pp[top],
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": PROFILED_TRAFFIC_3D.get(names[top]) if side == 100 else None},

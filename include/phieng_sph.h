@@ -849,6 +849,15 @@ uint32_t phieng_sph3_get_density_pressure(World3* world, float* density, float* 
 /* Density + pressure (and, with fxyz, the pressure force of the next
  * substep, fluid3.rs:1040-1086) of the current state, insertion order. */
 uint32_t phieng_sph3_debug_forces(World3* world, float* density, float* pressure, float* fxyz, uint32_t max);
+/* Arithmetic mode of the 3D step, as phieng_sph_set_precision's: in
+ * PHIENG_SPH_TOLERANCE the plain force pass (XSPH on, no artificial
+ * viscosity, cohesion, ghosts or turbulence, uniform mass) reassociates its
+ * pair terms (one approximate reciprocal square root and one approximate
+ * reciprocal per pair, fused multiply-adds); the density pass, the neighbour
+ * sets and the visit order stay exact, and runs stay bit-reproducible. 1 ok,
+ * 0 for a null world or an unknown mode. */
+int32_t phieng_sph3_set_precision(World3* world, uint32_t mode);
+uint32_t phieng_sph3_get_precision(const World3* world);
 /* CUDA-event times of the sort, density and force passes of the last
  * substep (after phieng_sph3_set_profiling(world, 1)). */
 int32_t phieng_sph3_set_profiling(World3* world, int32_t on);

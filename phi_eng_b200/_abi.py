@@ -425,6 +425,8 @@ SIGNATURES = {
     "phieng_sph3_set_state": (C.c_int32, [_P, _F, C.c_uint32]),
     "phieng_sph3_get_density_pressure": (C.c_uint32, [_P, _F, _F, C.c_uint32]),
     "phieng_sph3_debug_forces": (C.c_uint32, [_P, _F, _F, _F, C.c_uint32]),
+    "phieng_sph3_set_precision": (C.c_int32, [_P, C.c_uint32]),
+    "phieng_sph3_get_precision": (C.c_uint32, [_P]),
     "phieng_sph3_set_profiling": (C.c_int32, [_P, C.c_int32]),
     "phieng_sph3_phase_times": (C.c_uint32, [_P, _F, C.c_uint32]),
 }

@@ -434,6 +434,38 @@ __device__ __forceinline__ void pair3(uint32_t j, float4 pi, float4 vi, float rh
   }
 }
 
+// The tolerance mode's pair (plain flag set, uniform mass): the same pairs
+// in the same order as pair3 with reassociated arithmetic, as the 2D pass
+// does: one approximate reciprocal square root for the spiky direction and
+// one approximate reciprocal for the XSPH weight 1 / (rho_i + rho_j) per
+// pair, fused multiply-adds. The XSPH sum leaves out its constant factor
+// 2 m c_poly6 (m / rho_bar * poly6 = 2 m c_poly6 t^3 / (rho_i + rho_j)),
+// which k_force3 applies once per particle. mq_i = m q_i.
+__device__ __forceinline__ void pair3_fast(uint32_t j, float4 pi, float4 vi, float rho_i, float mq_i,
+                                           const float4* __restrict__ spos, const float4* __restrict__ svel,
+                                           const float2* __restrict__ sdq, const StepParams3& P, float (&f)[3],
+                                           float (&sm)[3]) {
+  const float4 pj = __ldg(&spos[j]);
+  const float2 dqj = __ldg(&sdq[j]);
+  const float4 vj = __ldg(&svel[j]);
+  const float dx = __fsub_rn(pi.x, pj.x), dy = __fsub_rn(pi.y, pj.y), dz = __fsub_rn(pi.z, pj.z);
+  const float d2 = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, __fmul_rn(dz, dz)));
+  const float rinv = rsqrtf(d2);  // d2 = 0 (coincident): inf, and r below is NaN -> no gradient
+  const float r = __fmul_rn(d2, rinv);
+  const float hr = __fsub_rn(P.hk, r);
+  const bool grad = r < P.hk && r >= kEps;  // spiky_grad's support
+  const float gs = grad ? __fmul_rn(__fmul_rn(__fmul_rn(P.c_spiky, hr), hr), rinv) : 0.0f;
+  const float c = __fmul_rn(gs, __fmaf_rn(P.mass, dqj.y, mq_i));  // m (q_i + q_j)
+  f[0] = __fmaf_rn(-dx, c, f[0]);
+  f[1] = __fmaf_rn(-dy, c, f[1]);
+  f[2] = __fmaf_rn(-dz, c, f[2]);
+  const float t = __fsub_rn(P.hk2, d2);
+  const float w = __fmul_rn(__fmul_rn(__fmul_rn(t, t), t), __fdividef(1.0f, __fadd_rn(rho_i, fmaxf(dqj.x, kEps))));
+  sm[0] = __fmaf_rn(__fsub_rn(vj.x, vi.x), w, sm[0]);
+  sm[1] = __fmaf_rn(__fsub_rn(vj.y, vi.y), w, sm[1]);
+  sm[2] = __fmaf_rn(__fsub_rn(vj.z, vi.z), w, sm[2]);
+}
+
 // Ghost pressure on a fluid particle (fluid3.rs:1073-1083), after its fluid
 // pairs: boundary_near's cells (oz, oy, ox = -1..1 around floor(p / h), h
 // the config's smoothing length) and filter, -grad W * (m_g (q_i + q_g)).
@@ -611,7 +643,8 @@ __global__ void k_resample_prep3(const uint32_t* __restrict__ sid, uint32_t n, u
 
 // Force + XSPH + integrate + walls (fluid3.rs:1040-1176); writes the new
 // state (id order), the next key and its bucket count. DEBUG: forces only.
-template <bool MASS, bool DEBUG, bool PLAIN>
+// FAST (tolerance mode; PLAIN, uniform mass): pair3_fast's arithmetic.
+template <bool MASS, bool DEBUG, bool PLAIN, bool FAST = false>
 __global__ void __launch_bounds__(256) k_force3(const float4* __restrict__ spos, const float4* __restrict__ svel,
                                                 const float2* __restrict__ sdq, const uint32_t* __restrict__ skey,
                                                 const uint32_t* __restrict__ sid, const float* __restrict__ smass,
@@ -630,6 +663,7 @@ __global__ void __launch_bounds__(256) k_force3(const float4* __restrict__ spos,
   const float m_i = MASS ? smass[s] : P.mass;
   const float rho_i = fmaxf(dqi.x, kEps);
   const float q_i = dqi.y;
+  const float mq_i = __fmul_rn(P.mass, q_i);
   float f[3] = {0.0f, 0.0f, 0.0f}, sm[3] = {0.0f, 0.0f, 0.0f};
   const GridPlan3& g = P.grid;
   if (k != g.sentinel) {
@@ -662,7 +696,10 @@ __global__ void __launch_bounds__(256) k_force3(const float4* __restrict__ spos,
         if (cur == 0u) break;
         const uint32_t j = base + (uint32_t)(__ffs((int)cur) - 1);
         cur &= cur - 1u;
-        pair3<MASS, PLAIN>(j, pi, vi, rho_i, q_i, m_i, spos, svel, sdq, smass, P, f, sm);
+        if constexpr (FAST)
+          pair3_fast(j, pi, vi, rho_i, mq_i, spos, svel, sdq, P, f, sm);
+        else
+          pair3<MASS, PLAIN>(j, pi, vi, rho_i, q_i, m_i, spos, svel, sdq, smass, P, f, sm);
       }
     } else {
 #pragma unroll 1
@@ -675,12 +712,22 @@ __global__ void __launch_bounds__(256) k_force3(const float4* __restrict__ spos,
           for (uint32_t j = __ldg(&start[bb]); j < e; j++) {
             const float4 a = __ldg(&spos[j]);
             const float ex = __fsub_rn(a.x, pi.x), ey = __fsub_rn(a.y, pi.y), ez = __fsub_rn(a.z, pi.z);
-            if (dot3(ex, ey, ez, ex, ey, ez) < P.hg2 && j != s)
-              pair3<MASS, PLAIN>(j, pi, vi, rho_i, q_i, m_i, spos, svel, sdq, smass, P, f, sm);
+            if (dot3(ex, ey, ez, ex, ey, ez) < P.hg2 && j != s) {
+              if constexpr (FAST)
+                pair3_fast(j, pi, vi, rho_i, mq_i, spos, svel, sdq, P, f, sm);
+              else
+                pair3<MASS, PLAIN>(j, pi, vi, rho_i, q_i, m_i, spos, svel, sdq, smass, P, f, sm);
+            }
           }
         }
       }
     }
+  }
+  if constexpr (FAST) {
+    const float xs = __fmul_rn(__fmul_rn(2.0f, P.mass), P.c_poly6);  // pair3_fast's XSPH factor
+    sm[0] = __fmul_rn(sm[0], xs);
+    sm[1] = __fmul_rn(sm[1], xs);
+    sm[2] = __fmul_rn(sm[2], xs);
   }
   if (!PLAIN && (P.flags & F_GHOST)) {  // PLAIN launches exclude F_GHOST
     const float3 gf = ghost_force3(pi, q_i, f[0], f[1], f[2], P);
@@ -777,6 +824,8 @@ constexpr uint32_t kClockWord3 = 16;  // scalar word holding the step's world cl
 
 struct World3 {
   FluidConfig3Ffi cfg = default_config();
+  // arithmetic of the plain force pass (phieng_sph3_set_precision)
+  uint32_t precision = PHIENG_SPH_EXACT;
   AmbientConfig3Ffi ambient = default_ambient3();
   float gx = 0.0f, gy = -9.81f, gz = 0.0f;  // World3::new gravity
   float time = 0.0f;
@@ -1271,6 +1320,7 @@ StepParams3 make_params3(const World3* w, float dt) {
   P.flags = f;
   P.nbodies = (uint32_t)w->bodies.size();
   P.uniform_phase = w->phase_value;
+  if (w->precision == PHIENG_SPH_TOLERANCE) P.flags |= F_FAST;
   return P;
 }
 
@@ -1320,10 +1370,16 @@ void enqueue_force3(World3* w, const StepParams3& P, float4* dbg, cudaStream_t s
   // XSPH on, artificial viscosity and cohesion off, h*h <= hk*hk: the
   // optional pair terms compiled out
   const bool plain = (P.flags & F_VISC) && !(P.flags & (F_AV | F_COHESION | F_WIDE_NB | F_TURB | F_GHOST));
-#define PHIENG_F3(M, D, PL)                                                                                         \
-  k_force3<M, D, PL><<<g, 128, 0, st>>>(w->spos, w->svel, w->sdq, w->skey, w->sid, w->smass, w->n, w->start, P,    \
-                                        w->dbodies, w->nmask, w->pos, w->vel, w->key, w->count, dbg)
-  if (dbg) {
+  // tolerance mode: the plain pass with uniform mass runs pair3_fast
+  const bool fast = plain && !m && (P.flags & F_FAST);
+#define PHIENG_F3X(M, D, PL, FA)                                                                                    \
+  k_force3<M, D, PL, FA><<<g, 128, 0, st>>>(w->spos, w->svel, w->sdq, w->skey, w->sid, w->smass, w->n, w->start, \
+                                            P, w->dbodies, w->nmask, w->pos, w->vel, w->key, w->count, dbg)
+#define PHIENG_F3(M, D, PL) PHIENG_F3X(M, D, PL, false)
+  if (fast) {
+    if (dbg) PHIENG_F3X(false, true, true, true);
+    else PHIENG_F3X(false, false, true, true);
+  } else if (dbg) {
     if (m) PHIENG_F3(true, true, false);
     else PHIENG_F3(false, true, false);
   } else if (plain) {
@@ -1334,6 +1390,7 @@ void enqueue_force3(World3* w, const StepParams3& P, float4* dbg, cudaStream_t s
     else PHIENG_F3(false, false, false);
   }
 #undef PHIENG_F3
+#undef PHIENG_F3X
 }
 
 void enqueue_substep3(World3* w, const StepParams3& P, cudaStream_t st) {
@@ -1884,6 +1941,17 @@ int32_t phieng_sph3_set_state(World3* w, const float* xyzv, uint32_t n) {
 // Run the density pass (and, with fxyz, the force pass without integrating)
 // on the current state; write density, pressure and force [fx, fy, fz] in
 // insertion order (each output may be null). Returns the number written.
+int32_t phieng_sph3_set_precision(World3* w, uint32_t mode) {
+  if (!w || (mode != PHIENG_SPH_EXACT && mode != PHIENG_SPH_TOLERANCE)) return 0;
+  if (mode == w->precision) return 1;
+  if (w->device >= 0) cudaStreamSynchronize(w->stream);
+  release_graph3(w);
+  w->precision = mode;
+  return 1;
+}
+
+uint32_t phieng_sph3_get_precision(const World3* w) { return w ? w->precision : PHIENG_SPH_EXACT; }
+
 uint32_t phieng_sph3_debug_forces(World3* w, float* dens, float* pres, float* fxyz, uint32_t max) {
   if (!w) return 0;
   const uint32_t n = std::min(max, w->n);

@@ -268,6 +268,16 @@ class World3:
             raise ValueError("malformed fluid block" if r == -2 else "bad arguments")
         return int(r)
 
+    @property
+    def precision(self) -> int:
+        """_abi.EXACT (default) or _abi.TOLERANCE (phieng_sph3_set_precision)."""
+        return int(self._lib.phieng_sph3_get_precision(self._h))
+
+    @precision.setter
+    def precision(self, mode: int) -> None:
+        if self._lib.phieng_sph3_set_precision(self._h, int(mode)) != 1:
+            raise ValueError(f"unknown precision mode {mode}")
+
     def debug_forces(self):
         """(density, pressure, force [n][3]) of a density + force pass on the
         current state (no integration)."""
