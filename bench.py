@@ -448,7 +448,9 @@ def fluid3d_line(steps: int, warmup: int, side: int = 100) -> dict:
                            "phases_ms": {nm: float(v) for nm, v in zip(names, ph_exact)}},
             "roofline": {"bound": "hbm", "kernel": names[top], "bytes_per_particle": bytes_pp[top],
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": PROFILED_TRAFFIC_3D.get(names[top]) if side == 100 else None},
+                         "traffic": PROFILED_TRAFFIC_3D.get(names[top]) if side == 100 else None,
+                         "traffic_source": "ncu capture of the exact-mode force pass (the tolerance-mode pass "
+                                           "reads and writes the same arrays)"},
             "finite": bool(np.isfinite(s).all()),
             "cpu_baseline": {"value": 4096 * k / secs, "unit": METRIC, "cores": 1, "kind": "port",
                              "sample": f"{k} in-place steps of a 4096-particle 3D dam break (the reference's cap)"}}
