@@ -417,7 +417,7 @@ __global__ void __launch_bounds__(kTrainThreads, 1)
       }
     }
     __syncthreads();
-    // ---- CTA weight gradients over the 128 samples of this round
+    // ---- CTA weight gradients over the 128 samples of this pass
     // warp w owns rows [16w, 16w + 16) of dW2 (layer-2 outputs) and of dW1
 #pragma unroll 1
     for (int kt = 0; kt < kTileRows / 16; kt++) {
@@ -765,7 +765,7 @@ __global__ void __launch_bounds__(kTrainThreads, 1)
         }
       }
     }
-    // ---- G (+)= GA GB^T over this round's 128 samples; the next round's
+    // ---- G (+)= GA GB^T over this pass's 128 samples; the next pass's
     // operand writes wait for it
     ok = tc::mma_step(bar, phase, kTrWaitLimit, [&] {
 #pragma unroll
