@@ -476,8 +476,11 @@ def run_slab(args, rank: int, world: int, local_rank: int) -> None:
 
     torch.cuda.set_device(local_rank)
     dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    from phi_eng_b200 import _abi
+
     sc = workload_scenes(args.workload)[0]
-    run = DeviceSlabRun(sc, rank, world)
+    run = DeviceSlabRun(sc, rank, world,
+                        precision=_abi.TOLERANCE if args.precision == "tolerance" else _abi.EXACT)
     for _ in range(args.warmup):
         run.step(sc.dt)
     torch.cuda.synchronize()

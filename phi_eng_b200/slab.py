@@ -128,7 +128,7 @@ class DeviceSlabRun:
     the same buffers (tests on one GPU)."""
 
     def __init__(self, scene, rank: int, size: int, edges=None, own_cap: int | None = None,
-                 halo_cap: int | None = None):
+                 halo_cap: int | None = None, precision: int | None = None):
         import torch
 
         from . import _abi
@@ -166,6 +166,8 @@ class DeviceSlabRun:
         self.world = world_from_scene(_empty_scene(scene))
         self.world.fluid.config = _no_cfl(scene.config)
         self.world.fluid.set_cap(cap)
+        if precision is not None:
+            self.world.precision = precision  # the owned results equal a single-domain world's in either mode
         self.world.set_stream(torch_stream_handle())
         self._lib = _abi.load()
         st_d, tags_d = st.cuda(), tags.cuda()
@@ -312,11 +314,12 @@ class LocalSlabGroup:
     used to test the decomposition without a process group and to measure
     what the device-side exchange adds per substep."""
 
-    def __init__(self, scene, size: int, halo_cap: int | None = None, edges=None, own_cap: int | None = None):
+    def __init__(self, scene, size: int, halo_cap: int | None = None, edges=None, own_cap: int | None = None,
+                 precision: int | None = None):
         edges = edges or slab_edges(scene.xy, float(scene.config.smoothing_length), size)
         self.scene = scene
-        self.ranks = [DeviceSlabRun(scene, r, size, edges=edges, halo_cap=halo_cap, own_cap=own_cap)
-                      for r in range(size)]
+        self.ranks = [DeviceSlabRun(scene, r, size, edges=edges, halo_cap=halo_cap, own_cap=own_cap,
+                                    precision=precision) for r in range(size)]
         self.copied = 0
 
     def close(self) -> None:
@@ -536,7 +539,8 @@ class SlabRun:
         return out
 
 
-def bench_local(workload: str = "dam_break_1m", ranks: int = 2, steps: int = 20, warmup: int = 3) -> dict:
+def bench_local(workload: str = "dam_break_1m", ranks: int = 2, steps: int = 20, warmup: int = 3,
+                precision: str = "tolerance") -> dict:
     """Device time per step of the single-domain world and of `ranks` rank
     worlds run one after another on this GPU (LocalSlabGroup), split into the
     rank worlds' steps and the exchange (pack, buffer copies, unpack); CUDA
@@ -547,8 +551,12 @@ def bench_local(workload: str = "dam_break_1m", ranks: int = 2, steps: int = 20,
     from .closure import torch_stream_handle
     from .world import world_from_scene
 
+    from . import _abi
+
+    mode = _abi.TOLERANCE if precision == "tolerance" else _abi.EXACT
     sc = {"dam_break_1m": scenes.dam_break_1m, "dam_break_4k": scenes.dam_break_4k}[workload]()
     w = world_from_scene(sc)
+    w.precision = mode
     w.set_stream(torch_stream_handle())
     for _ in range(warmup):
         w.step(sc.dt)
@@ -562,7 +570,7 @@ def bench_local(workload: str = "dam_break_1m", ranks: int = 2, steps: int = 20,
     single = e0.elapsed_time(e1) / steps
     w.close()
 
-    g = LocalSlabGroup(sc, ranks)
+    g = LocalSlabGroup(sc, ranks, precision=mode)
     for _ in range(warmup):
         g.step(sc.dt)
     torch.cuda.synchronize()
@@ -630,11 +638,13 @@ def bench_local(workload: str = "dam_break_1m", ranks: int = 2, steps: int = 20,
     g.close()
     # the graph-replayed substeps continue the same trajectory: still the single domain's, bit for bit
     w = world_from_scene(sc)
+    w.precision = mode
     for _ in range(warmup + 2 * steps):
         w.step(sc.dt)
     same = bool(np.array_equal(gathered.view(np.uint32), w.fluid.particles.view(np.uint32)))
     w.close()
-    return {"workload": workload, "particles": sc.n, "ranks": ranks, "steps": steps, "substeps": substeps,
+    return {"workload": workload, "precision": precision, "particles": sc.n, "ranks": ranks, "steps": steps,
+            "substeps": substeps,
             "single_ms_per_step": single, "ranks_ms_per_step": total,
             "rank_worlds_ms_per_step": world / steps, "exchange_ms_per_step": exch / steps,
             "exchange_us_per_substep": 1000.0 * exch / substeps,
@@ -653,8 +663,9 @@ def main(argv=None) -> None:
     ap.add_argument("--ranks", type=int, default=2)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--precision", choices=["tolerance", "exact"], default="tolerance")
     a = ap.parse_args(argv)
-    print(json.dumps(bench_local(a.workload, a.ranks, a.steps, a.warmup)), flush=True)
+    print(json.dumps(bench_local(a.workload, a.ranks, a.steps, a.warmup, a.precision)), flush=True)
 
 
 if __name__ == "__main__":

@@ -306,3 +306,26 @@ def test_local_slab_group_reports_a_full_owned_region():
     with pytest.raises(RuntimeError):
         g.ranks[1].owned()
     g.close()
+
+
+@pytest.mark.gpu
+def test_local_slab_group_tolerance_mode_equals_world():
+    """In the tolerance mode too, the rank worlds visit every owned
+    particle's neighbours in the single domain's order, so the gathered
+    state equals a single-domain tolerance-mode world bit for bit."""
+    from phi_eng_b200 import _abi
+    from phi_eng_b200.slab import LocalSlabGroup
+    from phi_eng_b200.world import world_from_scene
+
+    sc = _scene(False)
+    g = LocalSlabGroup(sc, 3, precision=_abi.TOLERANCE)
+    w = world_from_scene(sc)
+    w.precision = _abi.TOLERANCE
+    for _ in range(40):
+        g.step(sc.dt)
+        w.step(sc.dt)
+    got = g.gather()
+    g.close()
+    ref = w.fluid.particles
+    w.close()
+    assert np.array_equal(got.view(np.uint32), ref.view(np.uint32))
