@@ -340,8 +340,9 @@ typedef struct PhiengSphTuning {
   uint32_t force_block;       /* threads per block of the force pass: 64, 128, 256 (default 256) */
   float buckets_per_particle; /* bucket-grid budget per particle, 0.125..16 (default 2) */
   uint32_t stage;             /* tolerance mode: bit 0 = the density pass stages its neighbour rows in
-                                 shared memory, bit 1 = the force pass does (default 0; no effect on
-                                 results) */
+                                 shared memory, bit 1 = the force pass does, bit 2 = the force pass
+                                 reassigns each block's particles to its lanes by neighbour count
+                                 (ignored with bit 1); 0..7, default 0; no effect on results */
 } PhiengSphTuning;
 
 /* 1 ok, 0 null or out of range (world unchanged). Replans the bucket grid

@@ -30,7 +30,7 @@ DEFAULT = dict(density_block=256, force_block=256, buckets_per_particle=2.0, sta
 CANDIDATES = dict(density_block=(128, 256), force_block=(64, 128, 256), buckets_per_particle=(0.5, 1.0, 2.0, 4.0),
                   stage=(0,))
 # tolerance-mode worlds also try the passes without shared-memory staging
-CANDIDATES_TOLERANCE = dict(CANDIDATES, stage=(0, 1, 2, 3))
+CANDIDATES_TOLERANCE = dict(CANDIDATES, stage=(0, 1, 2, 3, 4, 5))
 
 
 def cache_path() -> str:

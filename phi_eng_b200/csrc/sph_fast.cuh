@@ -227,7 +227,46 @@ struct FastPair {
   }
 };
 
-template <bool STAGE, bool DEBUG, bool BATCH>
+// The slot a thread of a BALANCE launch takes: the block's slots ordered by
+// their neighbour count (the three rows' mask bits; a slot without masks,
+// which walks its candidates, counts as the largest), so the lanes of a warp
+// run about as many pair iterations each. Only the lane that computes a
+// particle changes, not its arithmetic or its order: results are the same.
+// blockDim.x <= 256; every thread of the block calls it.
+__device__ __forceinline__ uint32_t balanced_slot(const uint32_t* __restrict__ nmask, uint32_t n) {
+  __shared__ uint32_t hist[64];
+  __shared__ uint32_t perm[256];
+  const uint32_t tid = threadIdx.x, s0 = blockIdx.x * blockDim.x + tid;
+  uint32_t c = 0;
+  if (s0 < n) {
+    const uint32_t own = nmask[n + s0];
+    c = own ? min(__popc(nmask[s0]) + __popc(own) + __popc(nmask[2 * (size_t)n + s0]), 63u) : 63u;
+  }
+  if (tid < 64) hist[tid] = 0u;
+  __syncthreads();
+  const uint32_t r = atomicAdd(&hist[c], 1u);  // rank inside the count's bin (any order will do)
+  __syncthreads();
+  if (tid < 32) {  // exclusive scan of the 64 bins, two per lane
+    const uint32_t a = hist[2 * tid], b = hist[2 * tid + 1];
+    uint32_t x = a + b;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+      if (tid >= (uint32_t)o) x += y;
+    }
+    const uint32_t ex = x - a - b;
+    hist[2 * tid] = ex;
+    hist[2 * tid + 1] = ex + a;
+  }
+  __syncthreads();
+  perm[hist[c] + r] = s0;
+  __syncthreads();
+  return perm[tid];
+}
+
+// BALANCE: the block's slots reassigned to its lanes by neighbour count
+// (balanced_slot); not combined with STAGE.
+template <bool STAGE, bool DEBUG, bool BATCH, bool BALANCE = false>
 __global__ void __launch_bounds__(256) k_force_fast(
     const float2* __restrict__ spos, const float2* __restrict__ svel, const float2* __restrict__ sdq,
     const uint32_t* __restrict__ skey, const uint32_t* __restrict__ sid, uint32_t n,
@@ -235,8 +274,9 @@ __global__ void __launch_bounds__(256) k_force_fast(
     const uint32_t* __restrict__ nmask, float4* __restrict__ state_out, uint32_t* __restrict__ key_out,
     uint32_t* __restrict__ count_out, float2* __restrict__ dbg_force, uint32_t* __restrict__ defer,
     uint32_t* __restrict__ dcount) {
+  static_assert(!(STAGE && BALANCE), "staging windows assume the block's own slot order");
   extern __shared__ __align__(16) float2 fast_win[];
-  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t s = BALANCE ? balanced_slot(nmask, n) : blockIdx.x * blockDim.x + threadIdx.x;
   const bool active = s < n;
   const StepParams& P = scene_params<BATCH>(P0, bt.ptab, BATCH && active ? bt.sscene[s] : 0u);
   const GridPlan& g = P.grid;

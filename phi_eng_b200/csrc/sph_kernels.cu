@@ -1353,22 +1353,28 @@ void enqueue_force_integrate(const FluidBufs& b, uint32_t n, const StepParams& P
   const uint32_t bs = b.block_force, g = cdiv(n, bs);
   if (fast_flags(P.flags)) {
     const size_t sm = 9 * fast_stage_cap(bs) * sizeof(float2);
-#define PHIENG_FORCE_FAST(STG, D, BT)                                                                              \
-  k_force_fast<STG, D, BT><<<g, bs, STG ? sm : 0, st>>>(b.spos, b.svel, b.sdq, b.skey, b.sid, n, b.start, P, b.batch, \
-                                                        b.bodies, b.nmask, b.state, b.key, b.count, dbg_force,       \
-                                                        b.defer, b.dcount)
+#define PHIENG_FORCE_FAST_B(STG, D, BT, BAL)                                                                       \
+  k_force_fast<STG, D, BT, BAL><<<g, bs, STG ? sm : 0, st>>>(b.spos, b.svel, b.sdq, b.skey, b.sid, n, b.start, P,  \
+                                                             b.batch, b.bodies, b.nmask, b.state, b.key, b.count,  \
+                                                             dbg_force, b.defer, b.dcount)
+#define PHIENG_FORCE_FAST(STG, D, BT) PHIENG_FORCE_FAST_B(STG, D, BT, false)
     const bool stg = (b.stage & 2u) != 0;
+    const bool bal = !stg && (b.stage & 4u) != 0;  // lanes balanced by neighbour count
     if (dbg_force) {  // single worlds only
       if (stg) PHIENG_FORCE_FAST(true, true, false);
+      else if (bal) PHIENG_FORCE_FAST_B(false, true, false, true);
       else PHIENG_FORCE_FAST(false, true, false);
     } else if (bat) {
       if (stg) PHIENG_FORCE_FAST(true, false, true);
+      else if (bal) PHIENG_FORCE_FAST_B(false, false, true, true);
       else PHIENG_FORCE_FAST(false, false, true);
     } else {
       if (stg) PHIENG_FORCE_FAST(true, false, false);
+      else if (bal) PHIENG_FORCE_FAST_B(false, false, false, true);
       else PHIENG_FORCE_FAST(false, false, false);
     }
 #undef PHIENG_FORCE_FAST
+#undef PHIENG_FORCE_FAST_B
     return;
   }
 #define PHIENG_FORCE(M, D, BT, PL)                                                                                  \

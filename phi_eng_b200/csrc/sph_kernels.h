@@ -66,8 +66,9 @@ struct FluidBufs {
   uint32_t block_density = 256;  // threads per block of K5: 64, 128 or 256
   uint32_t block_force = 256;    // threads per block of K6: 64, 128 or 256
   // tolerance-mode passes: bit 0 = K5 stages its neighbour rows in shared
-  // memory, bit 1 = K6 does (results do not depend on it; off by default:
-  // measured slower on B200, the rows being L1 / L2 resident)
+  // memory, bit 1 = K6 does, bit 2 = K6 reassigns each block's particles to
+  // its lanes by neighbour count (not with bit 1). Results do not depend on
+  // them.
   uint32_t stage = 0;
 };
 

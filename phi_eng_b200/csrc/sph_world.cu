@@ -2014,7 +2014,7 @@ int32_t phieng_sph_set_tuning(World2* w, const PhiengSphTuning* t) {
   if (!w || !t) return 0;
   auto ok_block = [](uint32_t b) { return b == 64 || b == 128 || b == 256; };
   if (!ok_block(t->density_block) || !ok_block(t->force_block) || !(t->buckets_per_particle >= 0.125f) ||
-      !(t->buckets_per_particle <= 16.0f) || t->stage > 3u)
+      !(t->buckets_per_particle <= 16.0f) || t->stage > 7u)
     return 0;
   if (w->device >= 0) cudaStreamSynchronize(w->stream);
   release_graph(w);

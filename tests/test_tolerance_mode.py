@@ -49,8 +49,10 @@ def test_precision_mode_abi():
     lib = w._lib
     assert lib.phieng_sph_set_precision(None, 0) == 0
     assert lib.phieng_sph_get_precision(None) == _abi.EXACT
-    t = _abi.PhiengSphTuning(128, 128, 2.0, 4)  # stage bits beyond 3 are refused
+    t = _abi.PhiengSphTuning(128, 128, 2.0, 8)  # stage bits beyond 2 are refused
     assert lib.phieng_sph_set_tuning(w._h, C.byref(t)) == 0
+    t = _abi.PhiengSphTuning(128, 128, 2.0, 4)  # bit 2: the force pass's lane balancing
+    assert lib.phieng_sph_set_tuning(w._h, C.byref(t)) == 1
     w.close()
 
 
@@ -90,7 +92,7 @@ def _gpu(sc, tolerance=True, stage=3):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("name", list(SCENES))
-@pytest.mark.parametrize("stage", [0, 3])
+@pytest.mark.parametrize("stage", [0, 3, 4])
 def test_identical_state_within_tolerance(name, stage):
     make, steps = SCENES[name]
     sc = make()
@@ -145,7 +147,7 @@ def test_fp64_error_of_both_paths():
 def test_bit_reproducible_and_staging_invariant():
     sc = scenes.dam_break_4k()
     runs = []
-    for stage in (3, 3, 0, 1, 2):
+    for stage in (3, 3, 0, 1, 2, 4, 5, 6):
         g = _gpu(sc, stage=stage)
         g.step(sc.dt, 150)
         runs.append(g.state())
