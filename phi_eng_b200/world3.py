@@ -326,10 +326,12 @@ def main(argv=None) -> None:
     ap.add_argument("--side", type=int, default=32)
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--every", type=int, default=0, help="print the front every k steps (0: only at the end)")
+    ap.add_argument("--precision", choices=["exact", "tolerance"], default="exact")
     a = ap.parse_args(argv)
     L = a.side * 0.25
     pts, bodies = dam_break_3d(a.side, a.side, a.side, 0.25, tank=(2.5 * L, 1.5 * L, 1.5 * L))
     w = World3()
+    w.precision = _abi.TOLERANCE if a.precision == "tolerance" else _abi.EXACT
     w.fluid.set_cap(len(pts))
     for pos, sh in bodies:
         w.add_static_body(pos, sh)
