@@ -439,11 +439,12 @@ __device__ __forceinline__ void fixup_slot(uint32_t s, uint32_t id, const uint32
   gather_slot(lo + rank, k, id, ga, skey, sid);
 }
 
-// Four slots per thread: where all four were finished by k_place_final (the
-// common case) one 16-byte load and store; the others one by one. The same
-// threads clear the bucket counts for the next sort (the placement, which
-// used them as cursors, has finished): count_len is a multiple of the scan
-// tile, so whole uint4 stores.
+// SLOTS = 4: four slots per thread; where all four were finished by
+// k_place_final (the common case) one 16-byte load and store, the others one
+// by one. SLOTS = 1: one slot per thread. The same threads clear the bucket
+// counts for the next sort (the placement, which used them as cursors, has
+// finished): count_len is a multiple of the scan tile, so whole uint4 stores.
+template <int SLOTS>
 __global__ void __launch_bounds__(256) k_fixup(const uint32_t* __restrict__ tkey,
                                                const uint32_t* __restrict__ tid_in,
                                                const uint32_t* __restrict__ start, uint32_t n,
@@ -452,6 +453,10 @@ __global__ void __launch_bounds__(256) k_fixup(const uint32_t* __restrict__ tkey
                                                uint32_t* __restrict__ count, uint32_t count_len, GatherArgs ga) {
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (4u * t < count_len) reinterpret_cast<uint4*>(count)[t] = make_uint4(0u, 0u, 0u, 0u);
+  if constexpr (SLOTS == 1) {
+    if (t < n) fixup_slot(t, tid_in[t], tkey, tid_in, start, skey, sid, order, sentinel, ga);
+    return;
+  }
   const uint32_t s0 = 4u * t;
   if (s0 >= n) return;
   if (s0 + 3u < n) {
@@ -1196,10 +1201,18 @@ void enqueue_sort_and_ranges(const FluidBufs& b, uint32_t n, const StepParams& P
   else
     k_place_final<false><<<cdiv(n, 256), 256, 0, st>>>(b.key, b.sid, n, b.count, b.start, b.tkey, b.tid, b.skey,
                                                         b.order, ga);
-  // the fixup also clears the counts: the next sort's accumulate from zero (K6)
-  const uint32_t quads = std::max(cdiv(n, 4), cdiv(b.count_len, 4));
-  k_fixup<<<cdiv(quads, 256), 256, 0, st>>>(b.tkey, b.tid, b.start, n, b.skey, b.sid, b.order, P.grid.sentinel,
-                                             b.count, b.count_len, ga);
+  // the fixup also clears the counts: the next sort's accumulate from zero
+  // (K6). Four slots per thread for one world (sort 31.6 against 32.1 us at
+  // 2^20 particles), one for a batch, whose many small buckets leave more
+  // slots to rank (sort 160 against 168 us for 512 scenes)
+  const uint32_t slots = b.batch.ptab ? 1u : 4u;
+  const uint32_t threads = std::max(cdiv(n, slots), cdiv(b.count_len, 4));
+  if (slots == 1)
+    k_fixup<1><<<cdiv(threads, 256), 256, 0, st>>>(b.tkey, b.tid, b.start, n, b.skey, b.sid, b.order, P.grid.sentinel,
+                                                   b.count, b.count_len, ga);
+  else
+    k_fixup<4><<<cdiv(threads, 256), 256, 0, st>>>(b.tkey, b.tid, b.start, n, b.skey, b.sid, b.order, P.grid.sentinel,
+                                                   b.count, b.count_len, ga);
 }
 
 // ---------------------------------------------------------------- adaptive resolution
