@@ -134,7 +134,12 @@ def test_slab_edges_split_evenly():
     cx = cell_column(torch.from_numpy(sc.xy[:, 0].copy()), h).numpy()
     counts = [int(((cx >= e[r]) & (cx < e[r + 1])).sum()) for r in range(4)]
     assert sum(counts) == sc.n and max(counts) - min(counts) <= 2 * 64 + 64
-    assert all(e[r + 1] - e[r] >= 2 for r in range(1, 3))
+    # inner slabs span two halo bands: a migrant from the far side never lands in the near band
+    assert all(e[r + 1] - e[r] >= 4 for r in range(1, 3))
+    # many ranks on a narrow block: the edges still keep that width, and the outer slabs absorb the rest
+    e8 = slab_edges(sc.xy, h, 8)
+    assert all(e8[r + 1] - e8[r] >= 4 for r in range(1, 7))
+    assert e8 == sorted(e8)
 
 
 @pytest.mark.gpu
