@@ -825,6 +825,66 @@ uint32_t phieng_world3_fluid_get(const World3* world, float* out, uint32_t max);
 int64_t phieng_sph3_fluid_block_save(World3* world, uint32_t version, uint8_t* out, uint64_t cap);
 int64_t phieng_sph3_fluid_block_load(World3* world, uint32_t version, const uint8_t* data, uint64_t len);
 
+/* ---- the 3D fluid phase with the engine's rigid bodies (two-way coupling) ----
+ * A rigid body as the 3D fluid phase sees it (RigidBody3, body.rs:902-956):
+ * shape, transform (position and unit-quaternion rotation), velocity,
+ * angular velocity (world frame), inverse mass and the body-frame inverse
+ * inertia tensor. 112 bytes. */
+#define PHIENG_SHAPE3_HULL 3u /* Shape3::ConvexHull / ConvexMesh vertices (phieng_sph3_step_fluid_hull only) */
+typedef struct PhiengBody3 {
+  uint32_t shape_tag;       /* PHIENG_SHAPE3_SPHERE (a = radius), _BOX (a, b, c = half extents), _CAPSULE (a =
+                               radius, b = half length along the body's y axis) or _HULL */
+  float a, b, c;
+  float px, py, pz;         /* transform.position */
+  float qx, qy, qz, qw;     /* transform.rotation */
+  float vx, vy, vz;         /* velocity: updated for dynamic bodies */
+  float wx, wy, wz;         /* angular velocity: updated for dynamic bodies */
+  float inv_mass;
+  float inv_inertia[9];     /* body-frame inverse inertia (glam Mat3, column-major: x_axis, y_axis, z_axis) */
+  uint8_t is_static;        /* statics take no reaction */
+  uint8_t is_sleeping;      /* cleared when the fluid pushes or floats the body */
+  uint8_t _pad[2];
+} PhiengBody3;
+#ifdef __cplusplus
+static_assert(sizeof(PhiengBody3) == 112, "PhiengBody3 layout");
+#endif
+
+/* FluidState3::step_fluid(bodies, gravity, ambient, time, dt)
+ * (fluid3.rs:591-607), the fluid phase of World3::step (world.rs:2805-2812):
+ * CFL substeps of the world's 3D fluid against `bodies` in their order (in
+ * place of the world's own static bodies). Per substep (fluid3.rs:990-1214):
+ * sort, density, ghosts, force and integrate, then the boundary pass of
+ * fluid3.rs:1140-1178 in particle order (push-out, approach velocity removed,
+ * impulse n * (vn * m) on a dynamic body, the no-slip pull toward the body's
+ * velocity and its reaction -dv * m; RigidBody3::apply_impulse with the
+ * world-frame inverse inertia R I^-1 R^T, body.rs:1324-1361), then the
+ * buoyancy + drag pass of fluid3.rs:1180-1213 over the surface samples of
+ * dynamic spheres (14), boxes (24) and capsules (18) (fluid3.rs:371-467:
+ * pressure sampled on the re-sorted grid, force -n (p A) - v_rel (drag A
+ * |v_rel|) against the ambient wind, RigidBody3::apply_force). vx .. wz and
+ * is_sleeping of `bodies` are updated in place; the transforms are the
+ * caller's (the host engine integrates them). Turbulence uses the world
+ * clock (phieng_world3_set_time). Does not advance the clock.
+ * 1 ok; 0 for a null world, a body with an unknown shape, a non-finite
+ * field or a rotation whose norm is not 1 within 1e-3, more than 65536
+ * bodies, adaptive resolution on, boundary particles on with a static body
+ * that is rotated (its ghosts are generated for the identity rotation
+ * only), or an error (phieng_sph3_status). */
+int32_t phieng_sph3_step_fluid(World3* world, PhiengBody3* bodies, uint32_t nbodies, float dt);
+
+/* phieng_sph3_step_fluid with convex hulls as well: a body with shape_tag
+ * PHIENG_SHAPE3_HULL (a, b, c unused) has hull_count[k] >= 1 vertices in its
+ * own frame at hull_xyz[3 * hull_first[k] ...] (the arrays are indexed by
+ * body and read for hulls only). A particle tests a hull as fluid3.rs:568-585
+ * does: the nearest vertex sphere of radius particle_radius among the
+ * vertices moved by the body's transform (the first of equal depths), contact
+ * point the vertex. Hulls are impulse-coupled only: no buoyancy samples
+ * (fluid3.rs:464). 0 also for a hull with no vertex, a vertex range outside
+ * hull_nverts or a non-finite vertex. */
+int32_t phieng_sph3_step_fluid_hull(World3* world, PhiengBody3* bodies, uint32_t nbodies, const float* hull_xyz,
+                                    const uint32_t* hull_first, const uint32_t* hull_count, uint32_t hull_nverts,
+                                    float dt);
+
 /* ---- 3D extensions (no reference counterpart) ---- */
 
 /* As phieng_sph_status (grid_log2_h holds log2 of the rows; depth is not

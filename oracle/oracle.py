@@ -107,6 +107,12 @@ def _load():
         "orc3_collide": (C.c_int, [C.c_int] + [C.c_float] * 7 + [F]),
         "orc3_poly6": (C.c_float, [C.c_float, C.c_float]),
         "orc3_spiky": (None, [C.c_float] * 5 + [F]),
+        "orc3_step_fluid": (None, [P, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_float,
+                                   C.c_int]),
+        "orc3_set_wind": (None, [P, C.c_float, C.c_float, C.c_float]),
+        "orc3_qrot": (None, [C.c_float] * 4 + [F, F]),
+        "orc3_world_inv_inertia": (None, [C.c_float] * 4 + [F, F]),
+        "orc3_surface_samples": (C.c_uint32, [C.c_void_p, F, C.c_uint32]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -428,6 +434,22 @@ class OracleWorld3:
     def cfl_substeps(self, dt: float) -> int:
         return int(self._l.orc3_cfl_substeps(self._h, dt))
 
+    def set_wind(self, x: float, y: float, z: float) -> None:
+        """world.ambient.drag.wind, read by the buoyancy drag (fluid3.rs:1196)."""
+        self._l.orc3_set_wind(self._h, x, y, z)
+
+    def step_fluid(self, bodies, dt: float, mode: int = REF_SEQ, hulls=None) -> None:
+        """FluidState3::step_fluid with `bodies` (a ctypes PhiengBody3 array,
+        updated in place) in place of the world's bodies; no clock. hulls =
+        (xyz float32 [m][3], first uint32 [nb], count uint32 [nb]): the local
+        vertices of the PHIENG_SHAPE3_HULL bodies."""
+        if hulls is None:
+            self._l.orc3_step_fluid(self._h, C.cast(bodies, C.c_void_p), len(bodies), None, None, None, dt, mode)
+            return
+        xyz, first, count = (np.ascontiguousarray(a) for a in hulls)
+        self._l.orc3_step_fluid(self._h, C.cast(bodies, C.c_void_p), len(bodies), xyz.ctypes.data,
+                                first.ctypes.data, count.ctypes.data, dt, mode)
+
 
 def collide3(shape: int, a: float, b: float, c: float, p, pr: float):
     """Particle at p (body frame, body at the origin) vs one static body:
@@ -435,6 +457,31 @@ def collide3(shape: int, a: float, b: float, c: float, p, pr: float):
     out = np.zeros(4, np.float32)
     hit = _load().orc3_collide(shape, a, b, c, p[0], p[1], p[2], pr, _fp(out))
     return (tuple(float(v) for v in out[:3]), float(out[3])) if hit else None
+
+
+def qrot3(q, v):
+    """v rotated by the unit quaternion q = (x, y, z, w), in the fluid
+    phase's f32 evaluation order."""
+    vv = np.ascontiguousarray(v, np.float32)
+    out = np.zeros(3, np.float32)
+    _load().orc3_qrot(q[0], q[1], q[2], q[3], _fp(vv), _fp(out))
+    return out
+
+
+def world_inv_inertia3(q, inv_inertia) -> np.ndarray:
+    """(R I^-1) R^T, column-major [9], for R = Mat3::from_quat(q)."""
+    ii = np.ascontiguousarray(inv_inertia, np.float32).ravel()
+    out = np.zeros(9, np.float32)
+    _load().orc3_world_inv_inertia(q[0], q[1], q[2], q[3], _fp(ii), _fp(out))
+    return out
+
+
+def surface_samples3(body) -> np.ndarray:
+    """Buoyancy samples of one PhiengBody3: [k][7] = point, outward normal, area."""
+    n = _load().orc3_surface_samples(C.addressof(body), None, 0)
+    out = np.zeros((n, 7), np.float32)
+    _load().orc3_surface_samples(C.addressof(body), _fp(out), n)
+    return out
 
 
 def poly6_3(r2: float, h: float) -> float:

@@ -104,11 +104,152 @@ inline void turbulence_accel3(const Turbulence& tb, R px, R py, R pz, R time, R&
   az = az + nz * (R)tb.amp;
 }
 
+// ---- rigid bodies of the fluid phase (RigidBody3, body.rs:902-956, 1324-1361) ----
+// Rotation of v by the unit quaternion (b, w) = (qx, qy, qz, qw), the
+// expansion of q v q* for |q| = 1:
+//   v' = (v (w^2 - b.b) + b (2 (v.b))) + (b x v) (2 w)
+// evaluated in this order. glam 0.29's Quat * Vec3 sums the same three
+// terms; its association is not pinned here (no Rust toolchain on this
+// image), so rotated bodies are checked against this restatement only.
+template <class R>
+inline R vdot3(R ax, R ay, R az, R bx, R by, R bz) {  // glam Vec3::dot: (x x' + y y') + z z'
+  return ax * bx + ay * by + az * bz;
+}
+template <class R>
+inline void qrot(R qx, R qy, R qz, R qw, R vx, R vy, R vz, R& ox, R& oy, R& oz) {
+  const R s = qw * qw - vdot3(qx, qy, qz, qx, qy, qz);
+  const R d = vdot3(vx, vy, vz, qx, qy, qz) * (R)2;
+  const R w2 = qw * (R)2;
+  const R cx = qy * vz - qz * vy, cy = qz * vx - qx * vz, cz = qx * vy - qy * vx;
+  ox = (vx * s + qx * d) + cx * w2;
+  oy = (vy * s + qy * d) + cy * w2;
+  oz = (vz * s + qz * d) + cz * w2;
+}
+
+// Mat3::from_quat for a unit quaternion (column-major: x_axis, y_axis,
+// z_axis), with x2 = x + x etc.: the standard rotation matrix.
+inline void mat3_from_quat(float x, float y, float z, float w, float m[9]) {
+  const float x2 = x + x, y2 = y + y, z2 = z + z;
+  const float xx = x * x2, xy = x * y2, xz = x * z2, yy = y * y2, yz = y * z2, zz = z * z2;
+  const float wx = w * x2, wy = w * y2, wz = w * z2;
+  m[0] = 1.0f - (yy + zz), m[1] = xy + wz, m[2] = xz - wy;
+  m[3] = xy - wz, m[4] = 1.0f - (xx + zz), m[5] = yz + wx;
+  m[6] = xz + wy, m[7] = yz - wx, m[8] = 1.0f - (xx + yy);
+}
+// c = a * b, column by column: a * v = (x_axis v.x + y_axis v.y) + z_axis v.z
+inline void mat3_mul(const float a[9], const float b[9], float c[9]) {
+  for (int j = 0; j < 3; j++)
+    for (int i = 0; i < 3; i++) c[3 * j + i] = (a[i] * b[3 * j] + a[3 + i] * b[3 * j + 1]) + a[6 + i] * b[3 * j + 2];
+}
+// RigidBody3::world_inv_inertia (body.rs:1328-1331): (R I^-1) R^T
+inline void world_inv_inertia(float qx, float qy, float qz, float qw, const float inv_i[9], float out[9]) {
+  float r[9], rt[9], t[9];
+  mat3_from_quat(qx, qy, qz, qw, r);
+  for (int j = 0; j < 3; j++)
+    for (int i = 0; i < 3; i++) rt[3 * j + i] = r[3 * i + j];
+  mat3_mul(r, inv_i, t);
+  mat3_mul(t, rt, out);
+}
+
 struct Body3 {
-  int shape = 1;  // 0 sphere (a = radius), 1 box (a, b, c half extents), 2 capsule (a = radius, b = half length along y)
+  int shape = 1;  // 0 sphere (a = radius), 1 box (a, b, c half extents), 2 capsule (a = radius, b = half length along y), 3 hull
   float px = 0, py = 0, pz = 0;
   float a = 0, b = 0, c = 0;
+  // a body of the fluid phase with the engine's bodies (step_fluid): its
+  // rotation, motion and mass properties; hull vertices moved by the
+  // transform (rotation * v + position, math.rs:94-96)
+  bool rotated = false;
+  float qx = 0, qy = 0, qz = 0, qw = 1;
+  bool is_static = true, sleeping = false;
+  float vx = 0, vy = 0, vz = 0, wx = 0, wy = 0, wz = 0;
+  float inv_mass = 0;
+  float inv_inertia[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  std::vector<float> hull;  // world-space xyz
+
+  // RigidBody3::apply_impulse (body.rs:1349-1361)
+  void apply_impulse(float jx, float jy, float jz, float ptx, float pty, float ptz) {
+    if (is_static) return;
+    sleeping = false;
+    vx = vx + jx * inv_mass;
+    vy = vy + jy * inv_mass;
+    vz = vz + jz * inv_mass;
+    const float rx = ptx - px, ry = pty - py, rz = ptz - pz;
+    const float tx = ry * jz - rz * jy, ty = rz * jx - rx * jz, tz = rx * jy - ry * jx;
+    float iw[9];
+    world_inv_inertia(qx, qy, qz, qw, inv_inertia, iw);
+    wx = wx + ((iw[0] * tx + iw[3] * ty) + iw[6] * tz);
+    wy = wy + ((iw[1] * tx + iw[4] * ty) + iw[7] * tz);
+    wz = wz + ((iw[2] * tx + iw[5] * ty) + iw[8] * tz);
+  }
+  // RigidBody3::apply_force (body.rs:1334-1346): impulse F dt at the point
+  void apply_force(float fx, float fy, float fz, float ptx, float pty, float ptz, float dt) {
+    if (is_static) return;
+    sleeping = false;
+    vx = vx + (fx * inv_mass) * dt;
+    vy = vy + (fy * inv_mass) * dt;
+    vz = vz + (fz * inv_mass) * dt;
+    const float rx = ptx - px, ry = pty - py, rz = ptz - pz;
+    const float tx = ry * fz - rz * fy, ty = rz * fx - rx * fz, tz = rx * fy - ry * fx;
+    float iw[9];
+    world_inv_inertia(qx, qy, qz, qw, inv_inertia, iw);
+    wx = wx + ((iw[0] * tx + iw[3] * ty) + iw[6] * tz) * dt;
+    wy = wy + ((iw[1] * tx + iw[4] * ty) + iw[7] * tz) * dt;
+    wz = wz + ((iw[2] * tx + iw[5] * ty) + iw[8] * tz) * dt;
+  }
 };
+
+// Surface samples (point, outward normal, area) of a dynamic body for the
+// buoyancy pass (fluid3.rs:371-467): 14 sphere directions, 4 per box face
+// (every face's points at its fixed coordinate -he, as written), two rings
+// of 8 plus the poles for a capsule; none for hulls. Appends 7 floats each.
+inline void surface_samples3(const Body3& b, std::vector<float>& out) {
+  const float pi = 3.14159265358979323846f;
+  auto push = [&](float lx, float ly, float lz, float nlx, float nly, float nlz, float area) {
+    float x, y, z, nx, ny, nz;
+    qrot(b.qx, b.qy, b.qz, b.qw, lx, ly, lz, x, y, z);  // transform_point
+    qrot(b.qx, b.qy, b.qz, b.qw, nlx, nly, nlz, nx, ny, nz);
+    out.insert(out.end(), {x + b.px, y + b.py, z + b.pz, nx, ny, nz, area});
+  };
+  if (b.shape == 0) {
+    const float r = b.a;
+    float dirs[14][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+    const float sg[8][3] = {{1, 1, 1}, {1, 1, -1}, {1, -1, 1}, {1, -1, -1},
+                            {-1, 1, 1}, {-1, 1, -1}, {-1, -1, 1}, {-1, -1, -1}};
+    for (int k = 0; k < 8; k++) {  // normalize_or_zero: v * (1 / |v|)
+      const float rcp = 1.0f / std::sqrt(vdot3(sg[k][0], sg[k][1], sg[k][2], sg[k][0], sg[k][1], sg[k][2]));
+      for (int a = 0; a < 3; a++) dirs[6 + k][a] = sg[k][a] * rcp;
+    }
+    const float area = 4.0f * pi * r * r / 14.0f;
+    for (auto& d : dirs) push(d[0] * r, d[1] * r, d[2] * r, d[0], d[1], d[2], area);
+  } else if (b.shape == 1) {
+    const float hx = b.a, hy = b.b, hz = b.c;
+    const float area = 8.0f * (hx * hy + hy * hz + hz * hx) / 24.0f;
+    const struct { float n[3]; float fixed; int axis; } faces[6] = {
+        {{0, 1, 0}, -hy, 0}, {{0, -1, 0}, -hy, 0}, {{1, 0, 0}, -hx, 1},
+        {{-1, 0, 0}, -hx, 1}, {{0, 0, 1}, -hz, 2}, {{0, 0, -1}, -hz, 2}};
+    const float ts[4][2] = {{-0.75f, -0.75f}, {0.75f, -0.75f}, {-0.75f, 0.75f}, {0.75f, 0.75f}};
+    for (const auto& f : faces)
+      for (const auto& t : ts) {
+        if (f.axis == 0) push(hx * t[0], f.fixed, hz * t[1], f.n[0], f.n[1], f.n[2], area);
+        else if (f.axis == 1) push(f.fixed, hy * t[0], hz * t[1], f.n[0], f.n[1], f.n[2], area);
+        else push(hx * t[0], hy * t[1], f.fixed, f.n[0], f.n[1], f.n[2], area);
+      }
+  } else if (b.shape == 2) {
+    const float r = b.a, hl = b.b;
+    const float side = 4.0f * pi * r * hl / 16.0f, cap = 2.0f * pi * r * r;
+    for (float sy : {-hl * 0.5f, hl * 0.5f})
+      for (int k = 0; k < 8; k++) {
+        const float a = 2.0f * pi * (float)k / 8.0f;
+        const float c = std::cos(a), s = std::sin(a);
+        // dir * r + Y * sy
+        push(c * r + 0.0f * sy, 0.0f * r + 1.0f * sy, s * r + 0.0f * sy, c, 0.0f, s, side);
+      }
+    for (float s : {-1.0f, 1.0f}) {
+      const float len = hl + r;
+      push((0.0f * s) * len, (1.0f * s) * len, (0.0f * s) * len, 0.0f * s, 1.0f * s, 0.0f * s, cap);
+    }
+  }
+}
 
 template <class R>
 struct Particle3 {
@@ -126,6 +267,7 @@ class Fluid3 {
   R gx = 0, gy = (R)-9.81f, gz = 0;  // World3::new gravity
   R time = 0;
   Turbulence turb;  // world.ambient.turbulence
+  float wind_x = 0, wind_y = 0, wind_z = 0;  // world.ambient.drag.wind (buoyancy drag)
 
   // ---- boundary ghosts (fluid3.rs:719-922), regenerated every substep (a
   // function of the static bodies and the config only) ----
@@ -595,6 +737,240 @@ class Fluid3 {
         }
       }
     }
+  }
+
+  // ---- the fluid phase with the engine's bodies (fluid3.rs:591-607, 1140-1213) ----
+  // Particle vs a body with its transform (fluid3.rs:471-586); also the
+  // contact point on the body. local = inverse(rotation) * (p - position),
+  // the inverse of a unit quaternion being its conjugate.
+  static bool collide_q(R px, R py, R pz, R pr, const Body3& b, R& nx, R& ny, R& nz, R& depth, R& cx, R& cy,
+                        R& cz) {
+    const R qx = (R)b.qx, qy = (R)b.qy, qz = (R)b.qz, qw = (R)b.qw;
+    const R bx = (R)b.px, by = (R)b.py, bz = (R)b.pz;
+    R rx = px - bx, ry = py - by, rz = pz - bz;
+    if (b.shape == 0) {
+      R dist = std::sqrt(dot3(rx, ry, rz, rx, ry, rz));
+      R radius = (R)b.a;
+      if (dist >= radius + pr) return false;
+      if (dist > (R)kEps) {
+        nx = rx / dist, ny = ry / dist, nz = rz / dist;
+      } else {
+        nx = 1, ny = 0, nz = 0;
+      }
+      depth = radius + pr - dist;
+      cx = bx + nx * radius, cy = by + ny * radius, cz = bz + nz * radius;
+      return true;
+    }
+    if (b.shape == 3) {  // nearest vertex sphere; the first of equal depths
+      bool hit = false;
+      R best = 0;
+      for (size_t k = 0; k + 2 < b.hull.size(); k += 3) {
+        const R vx = (R)b.hull[k], vy = (R)b.hull[k + 1], vz = (R)b.hull[k + 2];
+        const R dx = px - vx, dy = py - vy, dz = pz - vz;
+        const R dist = std::sqrt(dot3(dx, dy, dz, dx, dy, dz));
+        if (!(dist < pr)) continue;
+        const R d = pr - dist;
+        if (hit && best >= d) continue;
+        hit = true;
+        best = d;
+        if (dist > (R)kEps) {
+          nx = dx / dist, ny = dy / dist, nz = dz / dist;
+        } else {
+          nx = 1, ny = 0, nz = 0;
+        }
+        depth = d;
+        cx = vx, cy = vy, cz = vz;
+      }
+      return hit;
+    }
+    R lx, ly, lz;
+    qrot(-qx, -qy, -qz, qw, rx, ry, rz, lx, ly, lz);
+    if (b.shape == 1) {
+      const R hx = (R)b.a, hy = (R)b.b, hz = (R)b.c;
+      const R kx = rclamp(lx, -hx, hx), ky = rclamp(ly, -hy, hy), kz = rclamp(lz, -hz, hz);
+      const R ddx = lx - kx, ddy = ly - ky, ddz = lz - kz;
+      if (dot3(ddx, ddy, ddz, ddx, ddy, ddz) > (R)kEpsSq) {
+        const R dist = std::sqrt(dot3(ddx, ddy, ddz, ddx, ddy, ddz));
+        if (dist >= pr) return false;
+        qrot(qx, qy, qz, qw, ddx / dist, ddy / dist, ddz / dist, nx, ny, nz);
+        depth = pr - dist;
+      } else {
+        // least-penetration axis, sign signum().copysign(1.0) = +1 (NaN: |NaN|)
+        const R dx = hx - std::fabs(lx), dy = hy - std::fabs(ly), dz = hz - std::fabs(lz);
+        R ax = 0, ay = 0, az = 0, s, d;
+        if (dx <= dy && dx <= dz) {
+          ax = 1, s = (lx != lx) ? std::fabs(lx) : (R)1, d = dx;
+        } else if (dy <= dz) {
+          ay = 1, s = (ly != ly) ? std::fabs(ly) : (R)1, d = dy;
+        } else {
+          az = 1, s = (lz != lz) ? std::fabs(lz) : (R)1, d = dz;
+        }
+        qrot(qx, qy, qz, qw, ax * s, ay * s, az * s, nx, ny, nz);
+        depth = pr + d;
+      }
+      qrot(qx, qy, qz, qw, kx, ky, kz, cx, cy, cz);
+      cx = cx + bx, cy = cy + by, cz = cz + bz;
+      return true;
+    }
+    // capsule along the local y axis
+    const R r = (R)b.a, hl = (R)b.b;
+    const R sy = rclamp(ly, -hl, hl);
+    const R ddx = lx - (R)0, ddy = ly - sy, ddz = lz - (R)0;
+    const R l2 = dot3(ddx, ddy, ddz, ddx, ddy, ddz);
+    R ox, oy, oz;  // local contact point seg + dir * r
+    if (l2 > (R)kEpsSq) {
+      const R dist = std::sqrt(l2);
+      if (dist >= r + pr) return false;
+      qrot(qx, qy, qz, qw, ddx / dist, ddy / dist, ddz / dist, nx, ny, nz);
+      depth = r + pr - dist;
+      R ux = 0, uy = 0, uz = 0;  // diff.normalize_or_zero()
+      const R rcp = (R)1 / std::sqrt(l2);
+      if (finite(rcp) && rcp > (R)0) ux = ddx * rcp, uy = ddy * rcp, uz = ddz * rcp;
+      ox = (R)0 + ux * r, oy = sy + uy * r, oz = (R)0 + uz * r;
+    } else {
+      // on the axis: the radial direction (x, 0, z), else +x
+      R ux = 1, uy = 0, uz = 0;
+      const R q2 = dot3(lx, (R)0, lz, lx, (R)0, lz);
+      if (q2 > (R)kEpsSq) {
+        const R rcp = (R)1 / std::sqrt(q2);
+        if (finite(rcp) && rcp > (R)0) {
+          ux = lx * rcp, uy = (R)0 * rcp, uz = lz * rcp;
+        } else {
+          ux = uy = uz = 0;
+        }
+      }
+      qrot(qx, qy, qz, qw, ux, uy, uz, nx, ny, nz);
+      depth = pr + r - std::sqrt(l2);
+      ox = (R)0 + ux * r, oy = sy + uy * r, oz = (R)0 + uz * r;
+    }
+    qrot(qx, qy, qz, qw, ox, oy, oz, cx, cy, cz);
+    cx = cx + bx, cy = cy + by, cz = cz + bz;
+    return true;
+  }
+
+  // boundary pass with reactions (fluid3.rs:1140-1178), particle by particle
+  void boundaries_q() {
+    R pr = rmax((R)cfg.particle_radius, (R)0);
+    for (auto& p : particles) {
+      for (Body3& b : bodies) {
+        R nx, ny, nz, depth, cx, cy, cz;
+        if (!collide_q(p.x, p.y, p.z, pr, b, nx, ny, nz, depth, cx, cy, cz)) continue;
+        if (depth <= (R)0) continue;
+        p.x = p.x + nx * depth;
+        p.y = p.y + ny * depth;
+        p.z = p.z + nz * depth;
+        R vn = dot3(p.vx, p.vy, p.vz, nx, ny, nz);
+        if (vn < (R)0) {
+          p.vx -= nx * vn;
+          p.vy -= ny * vn;
+          p.vz -= nz * vn;
+          if (!b.is_static) b.sleeping = false;
+          const R vm = vn * p.mass;
+          b.apply_impulse((float)(nx * vm), (float)(ny * vm), (float)(nz * vm), (float)cx, (float)cy, (float)cz);
+          if ((R)cfg.wall_friction > (R)0) {
+            R mu = rclamp((R)cfg.wall_friction, (R)0, (R)1);
+            R vtx = p.vx, vty = p.vy, vtz = p.vz;
+            R wvx = (R)b.vx, wvy = (R)b.vy, wvz = (R)b.vz;
+            R wdot = dot3(wvx, wvy, wvz, nx, ny, nz);
+            R wtx = wvx - nx * wdot, wty = wvy - ny * wdot, wtz = wvz - nz * wdot;
+            R dvx = (wtx - vtx) * mu, dvy = (wty - vty) * mu, dvz = (wtz - vtz) * mu;
+            p.vx += dvx;
+            p.vy += dvy;
+            p.vz += dvz;
+            b.apply_impulse((float)(-dvx * p.mass), (float)(-dvy * p.mass), (float)(-dvz * p.mass), (float)cx,
+                            (float)cy, (float)cz);
+          }
+        }
+      }
+    }
+  }
+
+  // FluidState3::sample_pressure (fluid3.rs:345-369): sum over the 27 cells
+  // around floor(point / h), h = max(smoothing_length, EPS), of
+  // m_j (p_j / max(rho_j, EPS)) poly6(r^2) for r^2 < h*h; max(p, 0)
+  R sample_pressure3(R ptx, R pty, R ptz) const {
+    const R h = rmax((R)cfg.smoothing_length, (R)kEps);
+    const int32_t cx = sat_i32(std::floor(ptx / h)), cy = sat_i32(std::floor(pty / h)), cz = sat_i32(std::floor(ptz / h));
+    R p = 0;
+    for (int oz = -1; oz <= 1; oz++)
+      for (int oy = -1; oy <= 1; oy++)
+        for (int ox = -1; ox <= 1; ox++) {
+          const int64_t xx = (int64_t)cx + ox, yy = (int64_t)cy + oy, zz = (int64_t)cz + oz;
+          if (xx < INT32_MIN || xx > INT32_MAX || yy < INT32_MIN || yy > INT32_MAX || zz < INT32_MIN ||
+              zz > INT32_MAX)
+            continue;
+          auto it = grid.find(Key{(int32_t)xx, (int32_t)yy, (int32_t)zz});
+          if (it == grid.end()) continue;
+          for (uint32_t j : it->second) {
+            const auto& pj = particles[j];
+            const R dx = pj.x - ptx, dy = pj.y - pty, dz = pj.z - ptz;
+            const R r2 = dot3(dx, dy, dz, dx, dy, dz);
+            if (r2 < h * h) p += pj.mass * (pj.pressure / rmax(pj.density, (R)kEps)) * poly6(r2, h);
+          }
+        }
+    return rmax(p, (R)0);
+  }
+
+  // buoyancy + drag over the dynamic bodies' surfaces (fluid3.rs:1180-1213)
+  void buoyancy3(R dt) {
+    rebuild_grid();
+    std::vector<float> smp;
+    for (Body3& b : bodies) {
+      if (b.is_static) continue;
+      smp.clear();
+      surface_samples3(b, smp);
+      if (smp.empty()) continue;
+      const float drag = std::max(cfg.drag, 0.0f);
+      bool wet = false;
+      for (size_t q = 0; q < smp.size(); q += 7) {
+        const float ptx = smp[q], pty = smp[q + 1], ptz = smp[q + 2];
+        const float nx = smp[q + 3], ny = smp[q + 4], nz = smp[q + 5], area = smp[q + 6];
+        const float p = (float)sample_pressure3((R)ptx, (R)pty, (R)ptz);
+        if (p <= 0.0f) continue;
+        wet = true;
+        const float rx = ptx - b.px, ry = pty - b.py, rz = ptz - b.pz;
+        // (velocity + angular_velocity x r) - wind
+        const float vrx = (b.vx + (b.wy * rz - b.wz * ry)) - wind_x;
+        const float vry = (b.vy + (b.wz * rx - b.wx * rz)) - wind_y;
+        const float vrz = (b.vz + (b.wx * ry - b.wy * rx)) - wind_z;
+        const float speed = std::sqrt(vrx * vrx + vry * vry + vrz * vrz);
+        const float pa = p * area;
+        float fx = -nx * pa, fy = -ny * pa, fz = -nz * pa;
+        if (speed > kEps) {
+          const float c = drag * area * speed;
+          fx -= vrx * c;
+          fy -= vry * c;
+          fz -= vrz * c;
+        }
+        b.apply_force(fx, fy, fz, ptx, pty, ptz, (float)dt);
+      }
+      if (wet) b.sleeping = false;
+    }
+  }
+
+  void substep_bodies(R dt, Mode mode) {
+    R h = rmax((R)cfg.smoothing_length, (R)kEps);
+    rebuild_grid();
+    compute_density_pressure(h);
+    if (cfg.boundary_particles) {
+      refresh_ghosts();
+      ghost_density(h);
+    }
+    compute_forces(h);
+    integrate(h, dt, mode);
+    boundaries_q();
+    bool dyn = false;
+    for (const Body3& b : bodies) dyn = dyn || !b.is_static;
+    if (dyn) buoyancy3(dt);
+  }
+
+  // FluidState3::step_fluid (fluid3.rs:591-607) with `bodies` as the
+  // engine's bodies: no clock
+  void step_fluid(R dt, Mode mode) {
+    if (!cfg.enabled || particles.empty() || !(dt > (R)0)) return;
+    uint32_t n = cfl_substeps(dt);
+    R sub = dt / (R)n;
+    for (uint32_t k = 0; k < n; k++) substep_bodies(sub, mode);
   }
 
   // CFL substeps (fluid3.rs:610-637)

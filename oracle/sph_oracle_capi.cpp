@@ -758,6 +758,77 @@ int orc3_collide(int shape, float a, float b, float c, float px, float py, float
   return hit ? 1 : 0;
 }
 
+// FluidState3::step_fluid with the caller's bodies (PhiengBody3 layout), in
+// place of the world's statics; vx .. wz and is_sleeping are updated in
+// place. Hull bodies (PHIENG_SHAPE3_HULL) take their local vertices from
+// hull_xyz [3 * first[k], 3 * (first[k] + count[k])), moved by the body's
+// transform (rotation * v + position, math.rs:94-96).
+void orc3_step_fluid(void* h, PhiengBody3* bodies, uint32_t nb, const float* hull_xyz, const uint32_t* first,
+                     const uint32_t* count, float dt, int mode) {
+  Orc3* o = static_cast<Orc3*>(h);
+  std::vector<oracle::Body3> keep = o->f32.bodies;
+  o->f32.bodies.clear();
+  for (uint32_t k = 0; k < nb; k++) {
+    const PhiengBody3& q = bodies[k];
+    oracle::Body3 b;
+    b.shape = (int)q.shape_tag;
+    b.px = q.px, b.py = q.py, b.pz = q.pz;
+    b.a = q.a, b.b = q.b, b.c = q.c;
+    b.rotated = true;
+    b.qx = q.qx, b.qy = q.qy, b.qz = q.qz, b.qw = q.qw;
+    b.is_static = q.is_static != 0;
+    b.sleeping = q.is_sleeping != 0;
+    b.vx = q.vx, b.vy = q.vy, b.vz = q.vz;
+    b.wx = q.wx, b.wy = q.wy, b.wz = q.wz;
+    b.inv_mass = q.inv_mass;
+    for (int i = 0; i < 9; i++) b.inv_inertia[i] = q.inv_inertia[i];
+    if (b.shape == 3)
+      for (uint32_t i = first[k]; i < first[k] + count[k]; i++) {
+        float x, y, z;
+        oracle::qrot(q.qx, q.qy, q.qz, q.qw, hull_xyz[3 * i], hull_xyz[3 * i + 1], hull_xyz[3 * i + 2], x, y, z);
+        b.hull.push_back(x + q.px);
+        b.hull.push_back(y + q.py);
+        b.hull.push_back(z + q.pz);
+      }
+    o->f32.bodies.push_back(b);
+  }
+  o->f32.step_fluid(dt, (oracle::Mode)mode);
+  for (uint32_t k = 0; k < nb; k++) {
+    const oracle::Body3& b = o->f32.bodies[k];
+    bodies[k].vx = b.vx, bodies[k].vy = b.vy, bodies[k].vz = b.vz;
+    bodies[k].wx = b.wx, bodies[k].wy = b.wy, bodies[k].wz = b.wz;
+    bodies[k].is_sleeping = b.sleeping ? 1 : 0;
+  }
+  o->f32.bodies = keep;
+}
+
+void orc3_set_wind(void* h, float x, float y, float z) {
+  Orc3* o = static_cast<Orc3*>(h);
+  o->f32.wind_x = o->f64.wind_x = x;
+  o->f32.wind_y = o->f64.wind_y = y;
+  o->f32.wind_z = o->f64.wind_z = z;
+}
+
+// Rotation of a vector by a quaternion, the world inverse inertia and the
+// buoyancy samples of one body, as the fluid phase computes them.
+void orc3_qrot(float qx, float qy, float qz, float qw, const float* v, float* out) {
+  oracle::qrot(qx, qy, qz, qw, v[0], v[1], v[2], out[0], out[1], out[2]);
+}
+void orc3_world_inv_inertia(float qx, float qy, float qz, float qw, const float* inv_i, float* out) {
+  oracle::world_inv_inertia(qx, qy, qz, qw, inv_i, out);
+}
+uint32_t orc3_surface_samples(const PhiengBody3* q, float* out, uint32_t max) {
+  oracle::Body3 b;
+  b.shape = (int)q->shape_tag;
+  b.px = q->px, b.py = q->py, b.pz = q->pz;
+  b.a = q->a, b.b = q->b, b.c = q->c;
+  b.qx = q->qx, b.qy = q->qy, b.qz = q->qz, b.qw = q->qw;
+  std::vector<float> s;
+  oracle::surface_samples3(b, s);
+  for (size_t i = 0; out && i < std::min<size_t>(s.size(), 7 * (size_t)max); i++) out[i] = s[i];
+  return (uint32_t)(s.size() / 7);
+}
+
 float orc3_poly6(float r2, float h) { return Fluid3<float>::poly6(r2, h); }
 void orc3_spiky(float rx, float ry, float rz, float r, float h, float* out3) {
   Fluid3<float>::spiky_grad(rx, ry, rz, r, h, out3[0], out3[1], out3[2]);

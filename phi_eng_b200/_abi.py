@@ -19,6 +19,7 @@ SHAPE_POLYGON = 2  # phieng_sph_step_fluid_poly only
 SHAPE3_SPHERE = 0
 SHAPE3_BOX = 1
 SHAPE3_CAPSULE = 2
+SHAPE3_HULL = 3  # phieng_sph3_step_fluid_hull only
 MAX_PARTICLES_3D = 4096
 SNAPSHOT_SCHEMA = 17
 
@@ -235,6 +236,38 @@ class PhiengBody2(C.Structure):
 
 assert C.sizeof(PhiengBody2) == 60
 
+
+class PhiengBody3(C.Structure):
+    """A rigid body as the 3D fluid phase sees it (phieng_sph3_step_fluid), 112 bytes."""
+
+    _fields_ = [
+        ("shape_tag", C.c_uint32),
+        ("a", C.c_float),
+        ("b", C.c_float),
+        ("c", C.c_float),
+        ("px", C.c_float),
+        ("py", C.c_float),
+        ("pz", C.c_float),
+        ("qx", C.c_float),
+        ("qy", C.c_float),
+        ("qz", C.c_float),
+        ("qw", C.c_float),
+        ("vx", C.c_float),
+        ("vy", C.c_float),
+        ("vz", C.c_float),
+        ("wx", C.c_float),
+        ("wy", C.c_float),
+        ("wz", C.c_float),
+        ("inv_mass", C.c_float),
+        ("inv_inertia", C.c_float * 9),
+        ("is_static", C.c_uint8),
+        ("is_sleeping", C.c_uint8),
+        ("_pad", C.c_uint8 * 2),
+    ]
+
+
+assert C.sizeof(PhiengBody3) == 112
+
 # FluidConfig3Ffi (ffi.rs:744-767) has the 2D config's fields and layout.
 FluidConfig3Ffi = FluidConfig2Ffi
 
@@ -426,6 +459,11 @@ SIGNATURES = {
     "phieng_sph3_get_density_pressure": (C.c_uint32, [_P, _F, _F, C.c_uint32]),
     "phieng_sph3_debug_forces": (C.c_uint32, [_P, _F, _F, _F, C.c_uint32]),
     "phieng_sph3_set_precision": (C.c_int32, [_P, C.c_uint32]),
+    "phieng_sph3_step_fluid": (C.c_int32, [_P, C.POINTER(PhiengBody3), C.c_uint32, C.c_float]),
+    "phieng_sph3_step_fluid_hull": (
+        C.c_int32,
+        [_P, C.POINTER(PhiengBody3), C.c_uint32, C.POINTER(C.c_float), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
+         C.c_uint32, C.c_float]),
     "phieng_sph3_get_precision": (C.c_uint32, [_P]),
     "phieng_sph3_set_profiling": (C.c_int32, [_P, C.c_int32]),
     "phieng_sph3_phase_times": (C.c_uint32, [_P, _F, C.c_uint32]),

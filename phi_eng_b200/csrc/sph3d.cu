@@ -67,6 +67,32 @@ __host__ __device__ inline uint32_t ghost_cell_hash3(int32_t cx, int32_t cy, int
   return h & mask;
 }
 
+// A body of phieng_sph3_step_fluid as the boundary pass reads it: shape (0
+// sphere, 1 box, 2 capsule, 3 hull), position, rotation (unit quaternion),
+// shape sizes, the half extents of its padded world bounding box, dyn = the
+// body takes reactions or moves (its contacts run in the ordered pass), and
+// for a hull its world-space vertices [vfirst, vfirst + vcount).
+struct DevBodyQ3 {
+  int32_t shape;
+  uint32_t dyn;
+  float px, py, pz;
+  float qx, qy, qz, qw;
+  float a, b, c;
+  float ex, ey, ez;
+  uint32_t vfirst, vcount;
+};
+
+// The motion state of a body in the fluid phase (RigidBody3): velocity,
+// angular velocity, inverse mass, the world inverse inertia R I^-1 R^T
+// (column-major, fixed over the call: the transform does not change), the
+// flags, and its buoyancy samples [sample_first, sample_first + sample_count).
+struct DynBody3 {
+  float vx, vy, vz, wx, wy, wz;
+  float inv_mass;
+  float iw[9];
+  uint32_t is_static, sleeping, sample_first, sample_count;
+};
+
 struct StepParams3 {
   GridPlan3 grid;
   float hg2, hk, hk2;
@@ -90,6 +116,14 @@ struct StepParams3 {
   const GhostCell3* gtab;
   uint32_t gtab_mask, nghost;
   float gmass, rest0;
+  // the engine's bodies (F_QBODIES, phieng_sph3_step_fluid): replace the
+  // world's statics; with F_DYNAMIC a particle's contact with a body that
+  // reacts defers the rest of its body loop to the ordered pass (defer[id] =
+  // the body it resumes from, dcount[id] = 1)
+  const DevBodyQ3* qbodies;
+  const float4* hullv;
+  uint32_t* defer;
+  uint32_t* dcount;
 };
 
 // Static body: shape 0 sphere (a = radius), 1 box (a, b, c half extents),
@@ -255,6 +289,251 @@ __device__ __forceinline__ void walls3(float& x, float& y, float& z, float& vx, 
         vy = __fadd_rn(vy, __fmul_rn(__fsub_rn(wty, vty), P.mu));
         vz = __fadd_rn(vz, __fmul_rn(__fsub_rn(wtz, vtz), P.mu));
       }
+    }
+  }
+}
+
+// ---------------------------------------------------------------- the engine's bodies
+// Rotation of v by the unit quaternion (b, w) = (qx, qy, qz, qw), the
+// expansion of q v q*: (v (w^2 - b.b) + b (2 (v.b))) + (b x v) (2 w), in this
+// order (the host restates it for hull vertices and buoyancy samples).
+__device__ __forceinline__ void qrot3(float qx, float qy, float qz, float qw, float vx, float vy, float vz, float& ox,
+                                      float& oy, float& oz) {
+  const float s = __fsub_rn(__fmul_rn(qw, qw), dot3(qx, qy, qz, qx, qy, qz));
+  const float d = __fmul_rn(dot3(vx, vy, vz, qx, qy, qz), 2.0f);
+  const float w2 = __fmul_rn(qw, 2.0f);
+  const float cx = __fsub_rn(__fmul_rn(qy, vz), __fmul_rn(qz, vy));
+  const float cy = __fsub_rn(__fmul_rn(qz, vx), __fmul_rn(qx, vz));
+  const float cz = __fsub_rn(__fmul_rn(qx, vy), __fmul_rn(qy, vx));
+  ox = __fadd_rn(__fadd_rn(__fmul_rn(vx, s), __fmul_rn(qx, d)), __fmul_rn(cx, w2));
+  oy = __fadd_rn(__fadd_rn(__fmul_rn(vy, s), __fmul_rn(qy, d)), __fmul_rn(cy, w2));
+  oz = __fadd_rn(__fadd_rn(__fmul_rn(vz, s), __fmul_rn(qz, d)), __fmul_rn(cz, w2));
+}
+
+__device__ __forceinline__ float clampf_rs(float x, float lo, float hi) {  // f32::clamp: NaN passes through
+  if (x < lo) x = lo;
+  if (x > hi) x = hi;
+  return x;
+}
+
+// Particle vs a body with its transform (fluid3.rs:471-586): outward normal,
+// depth and the contact point on the body. The local frame is
+// inverse(rotation) * (p - position), the conjugate for a unit quaternion.
+__device__ __noinline__ bool collide_q3(float px, float py, float pz, float pr, const DevBodyQ3& b,
+                                        const float4* __restrict__ hullv, float& nx, float& ny, float& nz,
+                                        float& depth, float& cx, float& cy, float& cz) {
+  const float rx = __fsub_rn(px, b.px), ry = __fsub_rn(py, b.py), rz = __fsub_rn(pz, b.pz);
+  if (b.shape == 0) {
+    const float dist = __fsqrt_rn(dot3(rx, ry, rz, rx, ry, rz));
+    if (dist >= __fadd_rn(b.a, pr)) return false;
+    if (dist > kEps) {
+      nx = __fdiv_rn(rx, dist), ny = __fdiv_rn(ry, dist), nz = __fdiv_rn(rz, dist);
+    } else {
+      nx = 1.0f, ny = 0.0f, nz = 0.0f;
+    }
+    depth = __fsub_rn(__fadd_rn(b.a, pr), dist);
+    cx = __fadd_rn(b.px, __fmul_rn(nx, b.a));
+    cy = __fadd_rn(b.py, __fmul_rn(ny, b.a));
+    cz = __fadd_rn(b.pz, __fmul_rn(nz, b.a));
+    return true;
+  }
+  if (b.shape == 3) {  // nearest vertex sphere of radius pr; the first of equal depths
+    bool hit = false;
+    float best = 0.0f;
+    for (uint32_t k = 0; k < b.vcount; k++) {
+      const float4 v = hullv[b.vfirst + k];
+      const float dx = __fsub_rn(px, v.x), dy = __fsub_rn(py, v.y), dz = __fsub_rn(pz, v.z);
+      const float dist = __fsqrt_rn(dot3(dx, dy, dz, dx, dy, dz));
+      if (!(dist < pr)) continue;
+      const float d = __fsub_rn(pr, dist);
+      if (hit && best >= d) continue;
+      hit = true;
+      best = d;
+      if (dist > kEps) {
+        nx = __fdiv_rn(dx, dist), ny = __fdiv_rn(dy, dist), nz = __fdiv_rn(dz, dist);
+      } else {
+        nx = 1.0f, ny = 0.0f, nz = 0.0f;
+      }
+      depth = d;
+      cx = v.x, cy = v.y, cz = v.z;
+    }
+    return hit;
+  }
+  float lx, ly, lz;
+  qrot3(-b.qx, -b.qy, -b.qz, b.qw, rx, ry, rz, lx, ly, lz);
+  float ox, oy, oz;  // local contact point
+  if (b.shape == 1) {
+    const float kx = clampf_rs(lx, -b.a, b.a), ky = clampf_rs(ly, -b.b, b.b), kz = clampf_rs(lz, -b.c, b.c);
+    const float ddx = __fsub_rn(lx, kx), ddy = __fsub_rn(ly, ky), ddz = __fsub_rn(lz, kz);
+    const float l2 = dot3(ddx, ddy, ddz, ddx, ddy, ddz);
+    if (l2 > kEpsSq) {
+      const float dist = __fsqrt_rn(l2);
+      if (dist >= pr) return false;
+      qrot3(b.qx, b.qy, b.qz, b.qw, __fdiv_rn(ddx, dist), __fdiv_rn(ddy, dist), __fdiv_rn(ddz, dist), nx, ny, nz);
+      depth = __fsub_rn(pr, dist);
+    } else {
+      // least-penetration axis, sign signum().copysign(1.0) = +1 (NaN: |NaN|)
+      const float dx = __fsub_rn(b.a, fabsf(lx)), dy = __fsub_rn(b.b, fabsf(ly)), dz = __fsub_rn(b.c, fabsf(lz));
+      float ax = 0.0f, ay = 0.0f, az = 0.0f, sg, d;
+      if (dx <= dy && dx <= dz) {
+        ax = 1.0f, sg = (lx != lx) ? fabsf(lx) : 1.0f, d = dx;
+      } else if (dy <= dz) {
+        ay = 1.0f, sg = (ly != ly) ? fabsf(ly) : 1.0f, d = dy;
+      } else {
+        az = 1.0f, sg = (lz != lz) ? fabsf(lz) : 1.0f, d = dz;
+      }
+      qrot3(b.qx, b.qy, b.qz, b.qw, __fmul_rn(ax, sg), __fmul_rn(ay, sg), __fmul_rn(az, sg), nx, ny, nz);
+      depth = __fadd_rn(pr, d);
+    }
+    ox = kx, oy = ky, oz = kz;
+  } else {
+    // capsule along the local y axis: closest point on the segment [-hl, hl]
+    const float r = b.a, sy = clampf_rs(ly, -b.b, b.b);
+    const float ddx = __fsub_rn(lx, 0.0f), ddy = __fsub_rn(ly, sy), ddz = __fsub_rn(lz, 0.0f);
+    const float l2 = dot3(ddx, ddy, ddz, ddx, ddy, ddz);
+    float ux, uy, uz;  // diff.normalize_or_zero(), or the radial direction on the axis
+    if (l2 > kEpsSq) {
+      const float dist = __fsqrt_rn(l2);
+      if (dist >= __fadd_rn(r, pr)) return false;
+      qrot3(b.qx, b.qy, b.qz, b.qw, __fdiv_rn(ddx, dist), __fdiv_rn(ddy, dist), __fdiv_rn(ddz, dist), nx, ny, nz);
+      depth = __fsub_rn(__fadd_rn(r, pr), dist);
+      const float rcp = __fdiv_rn(1.0f, __fsqrt_rn(l2));
+      if (isfinite(rcp) && rcp > 0.0f) {
+        ux = __fmul_rn(ddx, rcp), uy = __fmul_rn(ddy, rcp), uz = __fmul_rn(ddz, rcp);
+      } else {
+        ux = uy = uz = 0.0f;
+      }
+    } else {
+      ux = 1.0f, uy = 0.0f, uz = 0.0f;
+      const float q2 = dot3(lx, 0.0f, lz, lx, 0.0f, lz);
+      if (q2 > kEpsSq) {
+        const float rcp = __fdiv_rn(1.0f, __fsqrt_rn(q2));
+        if (isfinite(rcp) && rcp > 0.0f) {
+          ux = __fmul_rn(lx, rcp), uy = __fmul_rn(0.0f, rcp), uz = __fmul_rn(lz, rcp);
+        } else {
+          ux = uy = uz = 0.0f;
+        }
+      }
+      qrot3(b.qx, b.qy, b.qz, b.qw, ux, uy, uz, nx, ny, nz);
+      depth = __fsub_rn(__fadd_rn(pr, r), __fsqrt_rn(l2));
+    }
+    ox = __fadd_rn(0.0f, __fmul_rn(ux, r)), oy = __fadd_rn(sy, __fmul_rn(uy, r)), oz = __fadd_rn(0.0f, __fmul_rn(uz, r));
+  }
+  qrot3(b.qx, b.qy, b.qz, b.qw, ox, oy, oz, cx, cy, cz);
+  cx = __fadd_rn(cx, b.px), cy = __fadd_rn(cy, b.py), cz = __fadd_rn(cz, b.pz);
+  return true;
+}
+
+// The parallel part of the boundary pass over the engine's bodies
+// (fluid3.rs:1140-1178): plain walls (statics at rest) in body order;
+// returns kNoDefer, or the index of the first body marked dyn that the
+// particle touches, the state left as it was before that body.
+__device__ __forceinline__ uint32_t walls3q(float& x, float& y, float& z, float& vx, float& vy, float& vz,
+                                            const StepParams3& P) {
+  for (uint32_t k = 0; k < P.nbodies; k++) {
+    const DevBodyQ3* bp = P.qbodies + k;
+    // bounding-box reject (the extents include the particle radius)
+    if (fabsf(x - __ldg(&bp->px)) > __ldg(&bp->ex) || fabsf(y - __ldg(&bp->py)) > __ldg(&bp->ey) ||
+        fabsf(z - __ldg(&bp->pz)) > __ldg(&bp->ez))
+      continue;
+    const DevBodyQ3 b = *bp;
+    float nx, ny, nz, depth, cx, cy, cz;
+    if (!collide_q3(x, y, z, P.pr, b, P.hullv, nx, ny, nz, depth, cx, cy, cz)) continue;
+    if (depth <= 0.0f) continue;
+    if (b.dyn) return k;
+    x = __fadd_rn(x, __fmul_rn(nx, depth));
+    y = __fadd_rn(y, __fmul_rn(ny, depth));
+    z = __fadd_rn(z, __fmul_rn(nz, depth));
+    const float vn = dot3(vx, vy, vz, nx, ny, nz);
+    if (vn < 0.0f) {
+      vx = __fsub_rn(vx, __fmul_rn(nx, vn));
+      vy = __fsub_rn(vy, __fmul_rn(ny, vn));
+      vz = __fsub_rn(vz, __fmul_rn(nz, vn));
+      if (P.flags & F_FRICTION) {  // the wall's velocity is zero
+        const float wdot = dot3(0.0f, 0.0f, 0.0f, nx, ny, nz);
+        const float wtx = __fsub_rn(0.0f, __fmul_rn(nx, wdot));
+        const float wty = __fsub_rn(0.0f, __fmul_rn(ny, wdot));
+        const float wtz = __fsub_rn(0.0f, __fmul_rn(nz, wdot));
+        vx = __fadd_rn(vx, __fmul_rn(__fsub_rn(wtx, vx), P.mu));
+        vy = __fadd_rn(vy, __fmul_rn(__fsub_rn(wty, vy), P.mu));
+        vz = __fadd_rn(vz, __fmul_rn(__fsub_rn(wtz, vz), P.mu));
+      }
+    }
+  }
+  return kNoDefer;
+}
+
+// (Iw * t): (x_axis t.x + y_axis t.y) + z_axis t.z
+__device__ __forceinline__ void mat3_vec(const float* m, float tx, float ty, float tz, float& ox, float& oy,
+                                         float& oz) {
+  ox = __fadd_rn(__fadd_rn(__fmul_rn(m[0], tx), __fmul_rn(m[3], ty)), __fmul_rn(m[6], tz));
+  oy = __fadd_rn(__fadd_rn(__fmul_rn(m[1], tx), __fmul_rn(m[4], ty)), __fmul_rn(m[7], tz));
+  oz = __fadd_rn(__fadd_rn(__fmul_rn(m[2], tx), __fmul_rn(m[5], ty)), __fmul_rn(m[8], tz));
+}
+
+// RigidBody3::apply_impulse (body.rs:1349-1361): statics ignore it; a
+// dynamic body wakes, v += J * inv_mass, w += Iw (r x J).
+__device__ __forceinline__ void apply_impulse3(DynBody3& d, float bpx, float bpy, float bpz, float jx, float jy,
+                                               float jz, float qx, float qy, float qz) {
+  if (d.is_static) return;
+  d.sleeping = 0;
+  d.vx = __fadd_rn(d.vx, __fmul_rn(jx, d.inv_mass));
+  d.vy = __fadd_rn(d.vy, __fmul_rn(jy, d.inv_mass));
+  d.vz = __fadd_rn(d.vz, __fmul_rn(jz, d.inv_mass));
+  const float rx = __fsub_rn(qx, bpx), ry = __fsub_rn(qy, bpy), rz = __fsub_rn(qz, bpz);
+  const float tx = __fsub_rn(__fmul_rn(ry, jz), __fmul_rn(rz, jy));
+  const float ty = __fsub_rn(__fmul_rn(rz, jx), __fmul_rn(rx, jz));
+  const float tz = __fsub_rn(__fmul_rn(rx, jy), __fmul_rn(ry, jx));
+  float ax, ay, az;
+  mat3_vec(d.iw, tx, ty, tz, ax, ay, az);
+  d.wx = __fadd_rn(d.wx, ax);
+  d.wy = __fadd_rn(d.wy, ay);
+  d.wz = __fadd_rn(d.wz, az);
+}
+
+// The body loop of one particle from body k0 on with the reactions
+// (fluid3.rs:1140-1178): push out, remove the approach velocity, impulse
+// n * (vn * m), then the no-slip pull toward the body's velocity and its
+// reaction -dv * m. Run in particle order.
+__device__ void walls3q_ordered(float& x, float& y, float& z, float& vx, float& vy, float& vz, float m, uint32_t k0,
+                                DynBody3* __restrict__ dyn, const StepParams3& P) {
+  for (uint32_t k = k0; k < P.nbodies; k++) {
+    const DevBodyQ3 b = P.qbodies[k];
+    if (fabsf(x - b.px) > b.ex || fabsf(y - b.py) > b.ey || fabsf(z - b.pz) > b.ez) continue;
+    float nx, ny, nz, depth, cx, cy, cz;
+    if (!collide_q3(x, y, z, P.pr, b, P.hullv, nx, ny, nz, depth, cx, cy, cz)) continue;
+    if (depth <= 0.0f) continue;
+    x = __fadd_rn(x, __fmul_rn(nx, depth));
+    y = __fadd_rn(y, __fmul_rn(ny, depth));
+    z = __fadd_rn(z, __fmul_rn(nz, depth));
+    const float vn = dot3(vx, vy, vz, nx, ny, nz);
+    if (!(vn < 0.0f)) continue;
+    vx = __fsub_rn(vx, __fmul_rn(nx, vn));
+    vy = __fsub_rn(vy, __fmul_rn(ny, vn));
+    vz = __fsub_rn(vz, __fmul_rn(nz, vn));
+    float wvx = 0.0f, wvy = 0.0f, wvz = 0.0f;
+    DynBody3* d = b.dyn ? dyn + k : nullptr;
+    if (d) {
+      if (!d->is_static) d->sleeping = 0;
+      const float vm = __fmul_rn(vn, m);
+      apply_impulse3(*d, b.px, b.py, b.pz, __fmul_rn(nx, vm), __fmul_rn(ny, vm), __fmul_rn(nz, vm), cx, cy, cz);
+      wvx = d->vx, wvy = d->vy, wvz = d->vz;
+    }
+    if (P.flags & F_FRICTION) {
+      const float vtx = vx, vty = vy, vtz = vz;
+      const float wdot = dot3(wvx, wvy, wvz, nx, ny, nz);
+      const float wtx = __fsub_rn(wvx, __fmul_rn(nx, wdot));
+      const float wty = __fsub_rn(wvy, __fmul_rn(ny, wdot));
+      const float wtz = __fsub_rn(wvz, __fmul_rn(nz, wdot));
+      const float dvx = __fmul_rn(__fsub_rn(wtx, vtx), P.mu);
+      const float dvy = __fmul_rn(__fsub_rn(wty, vty), P.mu);
+      const float dvz = __fmul_rn(__fsub_rn(wtz, vtz), P.mu);
+      vx = __fadd_rn(vx, dvx);
+      vy = __fadd_rn(vy, dvy);
+      vz = __fadd_rn(vz, dvz);
+      if (d)
+        apply_impulse3(*d, b.px, b.py, b.pz, __fmul_rn(-dvx, m), __fmul_rn(-dvy, m), __fmul_rn(-dvz, m), cx, cy,
+                       cz);
     }
   }
 }
@@ -773,9 +1052,24 @@ __global__ void __launch_bounds__(256) k_force3(const float4* __restrict__ spos,
     y = pi.y;
     z = pi.z;
   }
-  walls3(x, y, z, vx, vy, vz, bodies, P);
-  pos_out[id] = make_float4(x, y, z, 0.0f);
-  vel_out[id] = make_float4(vx, vy, vz, 0.0f);
+  if (P.flags & F_QBODIES) {
+    // the engine's bodies (phieng_sph3_step_fluid)
+    const uint32_t r = walls3q(x, y, z, vx, vy, vz, P);
+    pos_out[id] = make_float4(x, y, z, 0.0f);
+    vel_out[id] = make_float4(vx, vy, vz, 0.0f);
+    if (P.flags & F_DYNAMIC) {
+      // contacts with bodies that react run in particle order (k_dynamic_walls3)
+      P.dcount[id] = r != kNoDefer ? 1u : 0u;
+      if (r != kNoDefer) {
+        P.defer[id] = r;
+        return;
+      }
+    }
+  } else {
+    walls3(x, y, z, vx, vy, vz, bodies, P);
+    pos_out[id] = make_float4(x, y, z, 0.0f);
+    vel_out[id] = make_float4(vx, vy, vz, 0.0f);
+  }
   const uint32_t nk = bucket_key3(x, y, z, g);
   key_out[id] = nk;
   count_key(count_out, nk);
@@ -800,6 +1094,145 @@ __global__ void __launch_bounds__(256) k_unsort3(const float2* __restrict__ sdq,
   if (s >= n) return;
   dens[sid[s]] = sdq[s].x;
   pres[sid[s]] = spres[s];
+}
+
+// The rest of the body loop of every deferred particle, one after the other
+// in id order (a body's velocity after particle i's reactions is what
+// particle i+1's no-slip term reads); then its next key and bucket count.
+__global__ void k_dynamic_walls3(const uint32_t* __restrict__ list, const uint32_t* __restrict__ total,
+                                 float4* __restrict__ pos, float4* __restrict__ vel, const float* __restrict__ mass,
+                                 uint32_t* __restrict__ key, uint32_t* __restrict__ count, DynBody3* __restrict__ dyn,
+                                 StepParams3 P) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  const uint32_t m = *total;
+  for (uint32_t t = 0; t < m; t++) {
+    const uint32_t id = list[t];
+    const float4 p = pos[id], v = vel[id];
+    float x = p.x, y = p.y, z = p.z, vx = v.x, vy = v.y, vz = v.z;
+    const float mi = (P.flags & F_MASS) ? mass[id] : P.mass;
+    walls3q_ordered(x, y, z, vx, vy, vz, mi, P.defer[id], dyn, P);
+    pos[id] = make_float4(x, y, z, 0.0f);
+    vel[id] = make_float4(vx, vy, vz, 0.0f);
+    const uint32_t nk = bucket_key3(x, y, z, P.grid);
+    key[id] = nk;
+    count_key(count, nk);
+  }
+}
+
+// Sorted (density, q) and pressure to id order, and back into the order of
+// a newer sort (the buoyancy pass samples the pressure on the re-sorted grid).
+__global__ void __launch_bounds__(256) k_dp_to_id3(const float2* __restrict__ sdq, const float* __restrict__ spres,
+                                                   const uint32_t* __restrict__ sid, uint32_t n,
+                                                   float2* __restrict__ dq_id, float* __restrict__ p_id) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  const uint32_t id = sid[s];
+  dq_id[id] = sdq[s];
+  p_id[id] = spres[s];
+}
+
+__global__ void __launch_bounds__(256) k_dp_from_id3(const float2* __restrict__ dq_id,
+                                                     const float* __restrict__ p_id,
+                                                     const uint32_t* __restrict__ sid, uint32_t n,
+                                                     float2* __restrict__ sdq, float* __restrict__ spres) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  const uint32_t id = sid[s];
+  sdq[s] = dq_id[id];
+  spres[s] = p_id[id];
+}
+
+// FluidState3::sample_pressure (fluid3.rs:345-369) over the sorted grid:
+// cells oz, oy, ox = -1..1 around floor(point / h), h = max(smoothing_length,
+// EPS), each bucket's particles in id order (others aliased into the bucket
+// lie at least 3 h away); p += m_j (p_j / max(rho_j, EPS)) poly6(r^2) for
+// r^2 < h*h; max(p, 0).
+__device__ float sample_pressure3(float ptx, float pty, float ptz, const float4* __restrict__ spos,
+                                  const float2* __restrict__ sdq, const float* __restrict__ spres,
+                                  const float* __restrict__ smass, const uint32_t* __restrict__ start,
+                                  const StepParams3& P) {
+  const GridPlan3& g = P.grid;
+  const int32_t cx = __float2int_rd(__fdiv_rn(ptx, P.hk));
+  const int32_t cy = __float2int_rd(__fdiv_rn(pty, P.hk));
+  const int32_t cz = __float2int_rd(__fdiv_rn(ptz, P.hk));
+  float p = 0.0f;
+  for (int oz = -1; oz <= 1; oz++) {
+    const uint32_t bz = ((uint32_t)cz + (uint32_t)oz - (uint32_t)g.cz0) & g.maskd;
+    for (int oy = -1; oy <= 1; oy++) {
+      const uint32_t by = ((uint32_t)cy + (uint32_t)oy - (uint32_t)g.cy0) & g.maskh;
+      for (int ox = -1; ox <= 1; ox++) {
+        const uint32_t bx = ((uint32_t)cx + (uint32_t)ox - (uint32_t)g.cx0) & g.maskw;
+        const uint32_t bb = (bz << (g.log2w + g.log2h)) | (by << g.log2w) | bx;
+        const uint32_t e = start[bb + 1];
+        for (uint32_t j = start[bb]; j < e; j++) {
+          const float4 pj = spos[j];
+          const float dx = __fsub_rn(pj.x, ptx), dy = __fsub_rn(pj.y, pty), dz = __fsub_rn(pj.z, ptz);
+          const float r2 = dot3(dx, dy, dz, dx, dy, dz);
+          if (r2 < P.hk2) {
+            const float mj = (P.flags & F_MASS) ? smass[j] : P.mass;
+            const float pr = __fdiv_rn(spres[j], fmaxf(sdq[j].x, kEps));
+            p = __fadd_rn(p, __fmul_rn(__fmul_rn(mj, pr), poly6_3(r2, P)));
+          }
+        }
+      }
+    }
+  }
+  return fmaxf(p, 0.0f);  // f32::max(0.0): a NaN sum gives 0
+}
+
+// Buoyancy + drag on one dynamic body (fluid3.rs:1180-1213): for each
+// surface sample in order (point and area in samples[2 q], outward normal in
+// samples[2 q + 1]), a sampled pressure p > 0 gives the force
+// -n (p A) - v_rel (drag A |v_rel|) (the latter when |v_rel| > EPS), v_rel =
+// (v + w x r) - wind, applied at the point for dt (RigidBody3::apply_force,
+// body.rs:1334-1346).
+__global__ void k_buoyancy3(const uint32_t* __restrict__ which, uint32_t nb, DynBody3* __restrict__ dyn,
+                            const float4* __restrict__ samples, const float4* __restrict__ spos,
+                            const float2* __restrict__ sdq, const float* __restrict__ spres,
+                            const float* __restrict__ smass, const uint32_t* __restrict__ start, StepParams3 P,
+                            float drag, float dt, float wind_x, float wind_y, float wind_z) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nb) return;
+  const uint32_t k = which[t];
+  const DevBodyQ3 b = P.qbodies[k];
+  DynBody3 d = dyn[k];
+  bool wet = false;
+  for (uint32_t q = 0; q < d.sample_count; q++) {
+    const float4 sp = samples[2 * (size_t)(d.sample_first + q)];
+    const float4 sn = samples[2 * (size_t)(d.sample_first + q) + 1];
+    const float p = sample_pressure3(sp.x, sp.y, sp.z, spos, sdq, spres, smass, start, P);
+    if (p <= 0.0f) continue;
+    wet = true;
+    const float rx = __fsub_rn(sp.x, b.px), ry = __fsub_rn(sp.y, b.py), rz = __fsub_rn(sp.z, b.pz);
+    const float vrx = __fsub_rn(__fadd_rn(d.vx, __fsub_rn(__fmul_rn(d.wy, rz), __fmul_rn(d.wz, ry))), wind_x);
+    const float vry = __fsub_rn(__fadd_rn(d.vy, __fsub_rn(__fmul_rn(d.wz, rx), __fmul_rn(d.wx, rz))), wind_y);
+    const float vrz = __fsub_rn(__fadd_rn(d.vz, __fsub_rn(__fmul_rn(d.wx, ry), __fmul_rn(d.wy, rx))), wind_z);
+    const float speed = __fsqrt_rn(dot3(vrx, vry, vrz, vrx, vry, vrz));
+    const float pa = __fmul_rn(p, sp.w);
+    float fx = __fmul_rn(-sn.x, pa), fy = __fmul_rn(-sn.y, pa), fz = __fmul_rn(-sn.z, pa);
+    if (speed > kEps) {
+      const float c = __fmul_rn(__fmul_rn(drag, sp.w), speed);
+      fx = __fsub_rn(fx, __fmul_rn(vrx, c));
+      fy = __fsub_rn(fy, __fmul_rn(vry, c));
+      fz = __fsub_rn(fz, __fmul_rn(vrz, c));
+    }
+    if (!d.is_static) {  // RigidBody3::apply_force
+      d.sleeping = 0;
+      d.vx = __fadd_rn(d.vx, __fmul_rn(__fmul_rn(fx, d.inv_mass), dt));
+      d.vy = __fadd_rn(d.vy, __fmul_rn(__fmul_rn(fy, d.inv_mass), dt));
+      d.vz = __fadd_rn(d.vz, __fmul_rn(__fmul_rn(fz, d.inv_mass), dt));
+      const float tx = __fsub_rn(__fmul_rn(ry, fz), __fmul_rn(rz, fy));
+      const float ty = __fsub_rn(__fmul_rn(rz, fx), __fmul_rn(rx, fz));
+      const float tz = __fsub_rn(__fmul_rn(rx, fy), __fmul_rn(ry, fx));
+      float ax, ay, az;
+      mat3_vec(d.iw, tx, ty, tz, ax, ay, az);
+      d.wx = __fadd_rn(d.wx, __fmul_rn(ax, dt));
+      d.wy = __fadd_rn(d.wy, __fmul_rn(ay, dt));
+      d.wz = __fadd_rn(d.wz, __fmul_rn(az, dt));
+    }
+  }
+  if (wet) d.sleeping = 0;
+  dyn[k] = d;
 }
 
 inline uint32_t cdiv(uint32_t a, uint32_t b) { return (a + b - 1) / b; }
@@ -881,6 +1314,21 @@ struct World3 {
   std::string gsig;
   bool profiling = false;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  // the fluid phase with the engine's bodies (phieng_sph3_step_fluid)
+  DevBodyQ3* d_qbodies = nullptr;
+  DynBody3* d_dyn = nullptr;
+  uint32_t* d_buoy = nullptr;
+  uint32_t qbody_cap = 0;
+  float4* d_samples = nullptr;  // two per sample: (point, area), (normal, 0)
+  uint32_t sample_cap = 0;
+  float4* d_hullv = nullptr;
+  uint32_t hull_cap = 0;
+  uint32_t *d_defer = nullptr, *d_dcount = nullptr, *d_dstart = nullptr, *d_dtile = nullptr, *d_list = nullptr;
+  float2* d_dq_id = nullptr;
+  float* d_p_id = nullptr;
+  uint32_t dyn_pcap = 0;
+  uint32_t* d_count2 = nullptr;
+  uint32_t count2_cap = 0;
 };
 
 namespace {
@@ -1124,12 +1572,12 @@ uint64_t ghost_count3(float v, float hi) {  // `.ceil().clamp(1.0, hi) as usize`
 // boxes and capsules (identity rotation: transform_point = (x_axis * v.x +
 // y_axis * v.y + z_axis * v.z) + position, evaluated as glam's Mat3 * Vec3),
 // at spacing max(h * 0.5, EPS).
-void generate_ghosts3(const World3* w, float hk, std::vector<float4>& out) {
+void generate_ghosts3(const std::vector<DevBody3>& bodies, float hk, std::vector<float4>& out) {
   const float spacing = std::max(hk * 0.5f, kEps);
   const float sp2 = spacing * spacing;  // powi(2)
   const float pi = 3.14159265358979323846f;
   out.clear();
-  for (const DevBody3& b : w->bodies) {
+  for (const DevBody3& b : bodies) {
     auto put = [&](float x, float y, float z) {
       const float wx = ((1.0f * x + 0.0f * y) + 0.0f * z) + b.px;
       const float wy = ((0.0f * x + 1.0f * y) + 0.0f * z) + b.py;
@@ -1187,18 +1635,20 @@ void generate_ghosts3(const World3* w, float hk, std::vector<float4>& out) {
   }
 }
 
-bool refresh_ghosts3(World3* w) {
+// Ghosts of the static bodies `bodies` (the world's own, or the statics of a
+// fluid-phase call), regenerated when they or the kernel config change.
+bool refresh_ghosts3(World3* w, const std::vector<DevBody3>& bodies) {
   const FluidConfig3Ffi& c = w->cfg;
   std::string sig;
   auto add = [&](const void* p, size_t n) { sig.append((const char*)p, n); };
   add(&c.smoothing_length, 4);
   add(&c.particle_mass, 4);
   add(&c.rest_density, 4);
-  for (const DevBody3& b : w->bodies) add(&b, sizeof(DevBody3));
+  for (const DevBody3& b : bodies) add(&b, sizeof(DevBody3));
   if (sig == w->ghost_sig && w->d_gtab) return true;
   const float hk = std::max(c.smoothing_length, kEps);
   std::vector<float4> raw;
-  generate_ghosts3(w, hk, raw);
+  generate_ghosts3(bodies, hk, raw);
   std::vector<std::pair<std::pair<int64_t, int32_t>, uint32_t>> order;  // ((x, y), z) cell key, index
   std::vector<int32_t> cell(3 * raw.size());
   for (uint32_t i = 0; i < raw.size(); i++) {
@@ -1561,7 +2011,7 @@ bool world_step3(World3* w, float dt) {
       w->dev_valid = false;
     }
     if (!prepare3(w)) return false;
-    if (w->cfg.boundary_particles && !refresh_ghosts3(w)) return false;
+    if (w->cfg.boundary_particles && !refresh_ghosts3(w, w->bodies)) return false;
     uint32_t ns = 1;
     if (!cfl_substeps3(w, dt, &ns)) return false;
     const StepParams3 P = make_params3(w, dt / (float)ns);
@@ -1615,6 +2065,351 @@ uint32_t add_particles3(World3* w, const float* xyz, const uint8_t* phases, uint
   return n;
 }
 
+// ---------------------------------------------------------------- the fluid phase with the engine's bodies
+// Host restatements of the rotation arithmetic the device and the buoyancy
+// samples use (f32, no contraction): q v q* as in qrot3, Mat3::from_quat,
+// column-major products, RigidBody3::world_inv_inertia (body.rs:1328-1331).
+void qrot_h(float qx, float qy, float qz, float qw, float vx, float vy, float vz, float& ox, float& oy, float& oz) {
+  const float s = qw * qw - ((qx * qx + qy * qy) + qz * qz);
+  const float d = ((vx * qx + vy * qy) + vz * qz) * 2.0f;
+  const float w2 = qw * 2.0f;
+  const float cx = qy * vz - qz * vy, cy = qz * vx - qx * vz, cz = qx * vy - qy * vx;
+  ox = (vx * s + qx * d) + cx * w2;
+  oy = (vy * s + qy * d) + cy * w2;
+  oz = (vz * s + qz * d) + cz * w2;
+}
+
+void mat3_from_quat_h(float x, float y, float z, float w, float m[9]) {
+  const float x2 = x + x, y2 = y + y, z2 = z + z;
+  const float xx = x * x2, xy = x * y2, xz = x * z2, yy = y * y2, yz = y * z2, zz = z * z2;
+  const float wx = w * x2, wy = w * y2, wz = w * z2;
+  m[0] = 1.0f - (yy + zz), m[1] = xy + wz, m[2] = xz - wy;
+  m[3] = xy - wz, m[4] = 1.0f - (xx + zz), m[5] = yz + wx;
+  m[6] = xz + wy, m[7] = yz - wx, m[8] = 1.0f - (xx + yy);
+}
+
+void world_inv_inertia_h(const PhiengBody3& b, float out[9]) {
+  float r[9], rt[9], t[9];
+  mat3_from_quat_h(b.qx, b.qy, b.qz, b.qw, r);
+  for (int j = 0; j < 3; j++)
+    for (int i = 0; i < 3; i++) rt[3 * j + i] = r[3 * i + j];
+  auto mul = [](const float* a, const float* c, float* o) {
+    for (int j = 0; j < 3; j++)
+      for (int i = 0; i < 3; i++) o[3 * j + i] = (a[i] * c[3 * j] + a[3 + i] * c[3 * j + 1]) + a[6 + i] * c[3 * j + 2];
+  };
+  mul(r, b.inv_inertia, t);
+  mul(t, rt, out);
+}
+
+// Buoyancy surface samples of a dynamic body (fluid3.rs:371-467): 14 sphere
+// directions, 4 per box face (each face's points at its fixed coordinate -he,
+// as the reference writes them), two rings of 8 and the two poles of a
+// capsule; none for hulls. Two float4 per sample: (point, area), (normal, 0).
+// The ring angles' cosines and sines come from the C library, as f32::cos /
+// f32::sin do.
+void surface_samples3_h(const PhiengBody3& b, std::vector<float4>& out) {
+  const float pi = 3.14159265358979323846f;
+  auto push = [&](float lx, float ly, float lz, float nlx, float nly, float nlz, float area) {
+    float x, y, z, nx, ny, nz;
+    qrot_h(b.qx, b.qy, b.qz, b.qw, lx, ly, lz, x, y, z);
+    qrot_h(b.qx, b.qy, b.qz, b.qw, nlx, nly, nlz, nx, ny, nz);
+    out.push_back(make_float4(x + b.px, y + b.py, z + b.pz, area));
+    out.push_back(make_float4(nx, ny, nz, 0.0f));
+  };
+  if (b.shape_tag == PHIENG_SHAPE3_SPHERE) {
+    const float r = b.a;
+    float dirs[14][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+    const float sg[8][3] = {{1, 1, 1}, {1, 1, -1}, {1, -1, 1}, {1, -1, -1},
+                            {-1, 1, 1}, {-1, 1, -1}, {-1, -1, 1}, {-1, -1, -1}};
+    for (int k = 0; k < 8; k++) {  // normalize_or_zero: v * (1 / |v|)
+      const float rcp = 1.0f / std::sqrt((sg[k][0] * sg[k][0] + sg[k][1] * sg[k][1]) + sg[k][2] * sg[k][2]);
+      for (int a = 0; a < 3; a++) dirs[6 + k][a] = sg[k][a] * rcp;
+    }
+    const float area = 4.0f * pi * r * r / 14.0f;
+    for (auto& d : dirs) push(d[0] * r, d[1] * r, d[2] * r, d[0], d[1], d[2], area);
+  } else if (b.shape_tag == PHIENG_SHAPE3_BOX) {
+    const float hx = b.a, hy = b.b, hz = b.c;
+    const float area = 8.0f * (hx * hy + hy * hz + hz * hx) / 24.0f;
+    struct Face {
+      float n[3];
+      float fixed;
+      int axis;
+    };
+    const Face faces[6] = {{{0, 1, 0}, -hy, 0},  {{0, -1, 0}, -hy, 0}, {{1, 0, 0}, -hx, 1},
+                           {{-1, 0, 0}, -hx, 1}, {{0, 0, 1}, -hz, 2},  {{0, 0, -1}, -hz, 2}};
+    const float ts[4][2] = {{-0.75f, -0.75f}, {0.75f, -0.75f}, {-0.75f, 0.75f}, {0.75f, 0.75f}};
+    for (const Face& f : faces)
+      for (const auto& t : ts) {
+        if (f.axis == 0) push(hx * t[0], f.fixed, hz * t[1], f.n[0], f.n[1], f.n[2], area);
+        else if (f.axis == 1) push(f.fixed, hy * t[0], hz * t[1], f.n[0], f.n[1], f.n[2], area);
+        else push(hx * t[0], hy * t[1], f.fixed, f.n[0], f.n[1], f.n[2], area);
+      }
+  } else if (b.shape_tag == PHIENG_SHAPE3_CAPSULE) {
+    const float r = b.a, hl = b.b;
+    const float side = 4.0f * pi * r * hl / 16.0f, cap = 2.0f * pi * r * r;
+    for (float sy : {-hl * 0.5f, hl * 0.5f})
+      for (int k = 0; k < 8; k++) {
+        const float a = 2.0f * pi * (float)k / 8.0f;
+        const float c = std::cos(a), sn = std::sin(a);
+        push(c * r + 0.0f * sy, 0.0f * r + 1.0f * sy, sn * r + 0.0f * sy, c, 0.0f, sn, side);  // dir * r + Y * sy
+      }
+    for (float sg : {-1.0f, 1.0f}) {
+      const float len = hl + r;
+      push((0.0f * sg) * len, (1.0f * sg) * len, (0.0f * sg) * len, 0.0f * sg, 1.0f * sg, 0.0f * sg, cap);
+    }
+  }
+}
+
+struct HullIn {
+  const float* xyz = nullptr;
+  const uint32_t* first = nullptr;
+  const uint32_t* count = nullptr;
+};
+
+bool identity_rotation(const PhiengBody3& b) { return b.qx == 0.0f && b.qy == 0.0f && b.qz == 0.0f && b.qw == 1.0f; }
+
+bool ensure_body_buffers3(World3* w, uint32_t nb, uint32_t nsamples, uint32_t nhull) {
+  auto grow = [&](auto*& p, uint32_t& cap, uint32_t need, uint32_t floor_) {
+    if (need <= cap && p) return true;
+    cudaStreamSynchronize(w->stream);
+    dfree3(p);
+    const uint32_t c = std::max(need, floor_);
+    if (!dalloc3(w, p, c)) return false;
+    cap = c;
+    return true;
+  };
+  if (nb > w->qbody_cap || !w->d_qbodies) {
+    cudaStreamSynchronize(w->stream);
+    dfree3(w->d_qbodies), dfree3(w->d_dyn), dfree3(w->d_buoy);
+    const uint32_t c = std::max<uint32_t>(16, nb);
+    if (!dalloc3(w, w->d_qbodies, c) || !dalloc3(w, w->d_dyn, c) || !dalloc3(w, w->d_buoy, c)) return false;
+    w->qbody_cap = c;
+  }
+  if (!grow(w->d_samples, w->sample_cap, 2 * nsamples, 64) || !grow(w->d_hullv, w->hull_cap, nhull, 64)) return false;
+  if (w->n > w->dyn_pcap || !w->d_defer) {
+    cudaStreamSynchronize(w->stream);
+    dfree3(w->d_defer), dfree3(w->d_dcount), dfree3(w->d_dstart), dfree3(w->d_dtile), dfree3(w->d_list);
+    dfree3(w->d_dq_id), dfree3(w->d_p_id);
+    const uint32_t c = std::max<uint32_t>(1024, w->n);
+    const uint32_t tiles = (c + 1 + kBucketScanTile - 1) / kBucketScanTile;
+    const size_t len = (size_t)tiles * kBucketScanTile;
+    if (!dalloc3(w, w->d_defer, c) || !dalloc3(w, w->d_dcount, len) || !dalloc3(w, w->d_dstart, len + 1) ||
+        !dalloc3(w, w->d_dtile, tiles) || !dalloc3(w, w->d_list, c) || !dalloc3(w, w->d_dq_id, c) ||
+        !dalloc3(w, w->d_p_id, c))
+      return false;
+    w->dyn_pcap = c;
+  }
+  return grow(w->d_count2, w->count2_cap, w->count_len, 1);
+}
+
+// The grid on the post-boundary positions for the buoyancy pass, from a copy
+// of the bucket counts (the next substep's sort needs the originals), with
+// the density pass's values carried into the new order.
+void enqueue_resort3(World3* w, const StepParams3& P, cudaStream_t st) {
+  const uint32_t g = cdiv(w->n, 256);
+  k_dp_to_id3<<<g, 256, 0, st>>>(w->sdq, w->spres, w->sid, w->n, w->d_dq_id, w->d_p_id);
+  cudaMemcpyAsync(w->d_count2, w->count, sizeof(uint32_t) * w->count_len, cudaMemcpyDeviceToDevice, st);
+  BucketSort bs;
+  bs.count = w->d_count2;
+  bs.tilesum = w->tilesum;
+  bs.done = w->scalar + 8;
+  bs.tstate = w->tstate;
+  bs.err = w->scalar + 12;
+  bs.start = w->start;
+  bs.key = w->key;
+  bs.sid_prev = w->sid;
+  bs.tkey = w->tkey;
+  bs.tid = w->tid;
+  enqueue_bucket_place(bs, w->n, P.grid.sentinel + 1, true, st);
+  const bool m = (P.flags & F_MASS) != 0, ph = (P.flags & F_PHASE) != 0;
+  k_fixup3<<<g, 256, 0, st>>>(w->tkey, w->tid, w->start, w->n, w->skey, w->sid, w->pos, w->vel, w->mass, w->phase,
+                              w->spos, w->svel, m ? w->smass : nullptr, ph ? w->sphase : nullptr);
+  k_dp_from_id3<<<g, 256, 0, st>>>(w->d_dq_id, w->d_p_id, w->sid, w->n, w->sdq, w->spres);
+}
+
+// FluidState3::step_fluid with the caller's bodies (fluid3.rs:591-607,
+// 990-1213). Bodies are validated by the caller.
+bool step_fluid_bodies3(World3* w, PhiengBody3* bodies, uint32_t nb, float dt, const HullIn& hin = HullIn()) {
+  if (!w->cfg.enabled || w->n == 0 || !(dt > 0.0f)) return true;  // step_fluid guards (fluid3.rs:599-601)
+  if (w->error != PHIENG_SPH_OK) return false;
+  if (w->cfg.adaptive_resolution) {
+    w->error = PHIENG_SPH_E_UNSUPPORTED;
+    return false;
+  }
+  std::vector<DevBodyQ3> qb(nb);
+  std::vector<DynBody3> dy(nb);
+  std::vector<float4> samples, hullv;
+  std::vector<uint32_t> buoy;
+  std::vector<DevBody3> statics;  // ghost sources
+  bool any_dyn = false, ghost_ok = true;
+  const float pr = rmaxf(w->cfg.particle_radius, 0.0f);
+  for (uint32_t k = 0; k < nb; k++) {
+    const PhiengBody3& b = bodies[k];
+    DevBodyQ3& d = qb[k];
+    std::memset(&d, 0, sizeof(d));
+    d.shape = (int32_t)b.shape_tag;
+    d.px = b.px, d.py = b.py, d.pz = b.pz;
+    d.qx = b.qx, d.qy = b.qy, d.qz = b.qz, d.qw = b.qw;
+    d.a = b.a, d.b = b.b, d.c = b.c;
+    d.dyn = (!b.is_static || b.vx != 0.0f || b.vy != 0.0f || b.vz != 0.0f) ? 1u : 0u;
+    any_dyn = any_dyn || d.dyn;
+    // world bounding box half extents around the position, the particle
+    // radius included, padded by 1% (the rotation is unit within 1e-3)
+    float m[9];
+    mat3_from_quat_h(b.qx, b.qy, b.qz, b.qw, m);
+    float he[3] = {b.a + pr, b.a + pr, b.a + pr};
+    if (b.shape_tag == PHIENG_SHAPE3_BOX) he[1] = b.b + pr, he[2] = b.c + pr;
+    if (b.shape_tag == PHIENG_SHAPE3_CAPSULE) he[1] = b.b + b.a + pr;
+    float ext[3] = {0.0f, 0.0f, 0.0f};
+    if (b.shape_tag == PHIENG_SHAPE3_SPHERE) {
+      ext[0] = ext[1] = ext[2] = he[0];
+    } else if (b.shape_tag == PHIENG_SHAPE3_HULL) {
+      d.vfirst = (uint32_t)hullv.size();
+      d.vcount = hin.count[k];
+      for (uint32_t i = hin.first[k]; i < hin.first[k] + hin.count[k]; i++) {
+        float x, y, z;
+        qrot_h(b.qx, b.qy, b.qz, b.qw, hin.xyz[3 * (size_t)i], hin.xyz[3 * (size_t)i + 1], hin.xyz[3 * (size_t)i + 2],
+               x, y, z);
+        const float4 v = make_float4(x + b.px, y + b.py, z + b.pz, 0.0f);
+        hullv.push_back(v);
+        ext[0] = std::max(ext[0], std::fabs(v.x - b.px) + pr);
+        ext[1] = std::max(ext[1], std::fabs(v.y - b.py) + pr);
+        ext[2] = std::max(ext[2], std::fabs(v.z - b.pz) + pr);
+      }
+    } else {
+      for (int i = 0; i < 3; i++)
+        ext[i] = std::fabs(m[i]) * he[0] + std::fabs(m[3 + i]) * he[1] + std::fabs(m[6 + i]) * he[2];
+    }
+    d.ex = ext[0] * 1.01f + 1e-30f;
+    d.ey = ext[1] * 1.01f + 1e-30f;
+    d.ez = ext[2] * 1.01f + 1e-30f;
+    DynBody3& y = dy[k];
+    std::memset(&y, 0, sizeof(y));
+    y.vx = b.vx, y.vy = b.vy, y.vz = b.vz, y.wx = b.wx, y.wy = b.wy, y.wz = b.wz;
+    y.inv_mass = b.inv_mass;
+    world_inv_inertia_h(b, y.iw);
+    y.is_static = b.is_static ? 1u : 0u;
+    y.sleeping = b.is_sleeping ? 1u : 0u;
+    y.sample_first = (uint32_t)(samples.size() / 2);
+    if (!b.is_static) surface_samples3_h(b, samples);
+    y.sample_count = (uint32_t)(samples.size() / 2) - y.sample_first;
+    if (y.sample_count) buoy.push_back(k);
+    if (b.is_static && w->cfg.boundary_particles) {
+      // ghosts are generated for static spheres, boxes and capsules at the
+      // identity rotation (generate_ghosts3)
+      if (b.shape_tag == PHIENG_SHAPE3_HULL || !identity_rotation(b)) ghost_ok = false;
+      DevBody3 g;
+      std::memset(&g, 0, sizeof(g));
+      g.shape = (int32_t)b.shape_tag;
+      g.px = b.px, g.py = b.py, g.pz = b.pz;
+      g.a = b.a, g.b = b.b, g.c = b.c;
+      statics.push_back(g);
+    }
+  }
+  if (!ghost_ok) {
+    w->error = PHIENG_SPH_E_UNSUPPORTED;
+    return false;
+  }
+  if (!prepare3(w)) return false;
+  if (w->cfg.boundary_particles && !refresh_ghosts3(w, statics)) return false;
+  if (!ensure_body_buffers3(w, nb, (uint32_t)(samples.size() / 2), (uint32_t)hullv.size())) return false;
+  cudaStream_t st = w->stream;
+  if (nb && (!ok3(w, cudaMemcpyAsync(w->d_qbodies, qb.data(), sizeof(DevBodyQ3) * nb, cudaMemcpyHostToDevice, st)) ||
+             !ok3(w, cudaMemcpyAsync(w->d_dyn, dy.data(), sizeof(DynBody3) * nb, cudaMemcpyHostToDevice, st))))
+    return false;
+  if (!buoy.empty() &&
+      !ok3(w, cudaMemcpyAsync(w->d_buoy, buoy.data(), 4 * buoy.size(), cudaMemcpyHostToDevice, st)))
+    return false;
+  if (!samples.empty() && !ok3(w, cudaMemcpyAsync(w->d_samples, samples.data(), sizeof(float4) * samples.size(),
+                                                  cudaMemcpyHostToDevice, st)))
+    return false;
+  if (!hullv.empty() &&
+      !ok3(w, cudaMemcpyAsync(w->d_hullv, hullv.data(), sizeof(float4) * hullv.size(), cudaMemcpyHostToDevice, st)))
+    return false;
+  uint32_t ns = 1;
+  if (!cfl_substeps3(w, dt, &ns)) return false;
+  const float sub = dt / (float)ns;
+  StepParams3 P = make_params3(w, sub);
+  P.flags |= F_QBODIES;
+  if (any_dyn) P.flags |= F_DYNAMIC;
+  P.nbodies = nb;
+  P.qbodies = w->d_qbodies;
+  P.hullv = w->d_hullv;
+  P.defer = w->d_defer;
+  P.dcount = w->d_dcount;
+  if (P.flags & F_TURB) {  // the world clock (world.rs:2811)
+    uint32_t bits;
+    std::memcpy(&bits, &w->time, 4);
+    enqueue_set_word(w->scalar + kClockWord3, bits, st);
+  }
+  const float drag = rmaxf(w->cfg.drag, 0.0f);
+  const size_t dlen = (size_t)((w->n + 1 + kBucketScanTile - 1) / kBucketScanTile) * kBucketScanTile;
+  for (uint32_t k = 0; k < ns; k++) {
+    enqueue_sort3(w, P, st);
+    w->sid_perm_n = w->n;
+    enqueue_density3(w, P, st);
+    if ((P.flags & F_GHOST) && P.nghost) {
+      if (P.flags & F_MASS)
+        k_ghost_density3<true><<<cdiv(P.nghost, 256), 256, 0, st>>>(w->spos, w->smass, w->start, P);
+      else
+        k_ghost_density3<false><<<cdiv(P.nghost, 256), 256, 0, st>>>(w->spos, w->smass, w->start, P);
+    }
+    if (any_dyn) cudaMemsetAsync(w->d_dcount, 0, sizeof(uint32_t) * dlen, st);
+    enqueue_force3(w, P, nullptr, st);
+    if (any_dyn) {
+      enqueue_flag_compact(w->d_dcount, w->n, w->d_dtile, w->scalar + 20, w->d_dstart, w->d_list, st);
+      k_dynamic_walls3<<<1, 32, 0, st>>>(w->d_list, w->d_dstart + w->n, w->pos, w->vel, w->mass, w->key, w->count,
+                                         w->d_dyn, P);
+    }
+    if (!buoy.empty()) {
+      enqueue_resort3(w, P, st);
+      k_buoyancy3<<<cdiv((uint32_t)buoy.size(), 32), 32, 0, st>>>(
+          w->d_buoy, (uint32_t)buoy.size(), w->d_dyn, w->d_samples, w->spos, w->sdq, w->spres, w->smass, w->start, P,
+          drag, sub, w->ambient.wind_x, w->ambient.wind_y, w->ambient.wind_z);
+    }
+    w->substeps++;
+  }
+  if (!ok3(w, cudaGetLastError())) return false;
+  w->host_valid = false;
+  w->dp_dev = true;
+  w->keys_valid = true;
+  if (nb) {
+    if (!ok3(w, cudaMemcpyAsync(dy.data(), w->d_dyn, sizeof(DynBody3) * nb, cudaMemcpyDeviceToHost, st)) ||
+        !ok3(w, cudaStreamSynchronize(st)))
+      return false;
+    for (uint32_t k = 0; k < nb; k++) {
+      bodies[k].vx = dy[k].vx, bodies[k].vy = dy[k].vy, bodies[k].vz = dy[k].vz;
+      bodies[k].wx = dy[k].wx, bodies[k].wy = dy[k].wy, bodies[k].wz = dy[k].wz;
+      bodies[k].is_sleeping = dy[k].sleeping ? 1 : 0;
+    }
+  }
+  return true;
+}
+
+// Fields a body of the fluid phase must have: a known shape with positive
+// finite sizes (hulls: phieng_sph3_step_fluid_hull), finite transform and
+// motion state, a rotation of norm 1 within 1e-3.
+bool body3_valid(const PhiengBody3& b, bool hull_ok) {
+  const float f[] = {b.px, b.py, b.pz, b.qx, b.qy, b.qz, b.qw, b.vx, b.vy, b.vz, b.wx, b.wy, b.wz, b.inv_mass};
+  for (float x : f)
+    if (!std::isfinite(x)) return false;
+  for (float x : b.inv_inertia)
+    if (!std::isfinite(x)) return false;
+  const float n2 = ((b.qx * b.qx + b.qy * b.qy) + b.qz * b.qz) + b.qw * b.qw;
+  if (!(std::fabs(n2 - 1.0f) <= 1e-3f)) return false;
+  auto pos = [](float v) { return std::isfinite(v) && v > 0.0f; };
+  switch (b.shape_tag) {
+    case PHIENG_SHAPE3_SPHERE: return pos(b.a);
+    case PHIENG_SHAPE3_BOX: return pos(b.a) && pos(b.b) && pos(b.c);
+    case PHIENG_SHAPE3_CAPSULE: return pos(b.a) && pos(b.b);
+    case PHIENG_SHAPE3_HULL: return hull_ok;
+    default: return false;
+  }
+}
+
+constexpr uint32_t kMaxCallBodies3 = 65536;
+constexpr uint32_t kMaxHullVerts3 = 1u << 20;
+
 }  // namespace
 
 extern "C" {
@@ -1631,6 +2426,9 @@ void phieng_world3_free(World3* w) {
     dfree3(w->d_gpos), dfree3(w->d_gq), dfree3(w->d_gtab);
     dfree3(w->rs_slot), dfree3(w->rs_absorbed), dfree3(w->rs_pos), dfree3(w->rs_vel), dfree3(w->rs_mass),
         dfree3(w->rs_phase);
+    dfree3(w->d_qbodies), dfree3(w->d_dyn), dfree3(w->d_buoy), dfree3(w->d_samples), dfree3(w->d_hullv);
+    dfree3(w->d_defer), dfree3(w->d_dcount), dfree3(w->d_dstart), dfree3(w->d_dtile), dfree3(w->d_list);
+    dfree3(w->d_dq_id), dfree3(w->d_p_id), dfree3(w->d_count2);
     for (auto& e : w->ev)
       if (e) cudaEventDestroy(e);
     if (w->h_pinned) cudaFreeHost(w->h_pinned);
@@ -1920,6 +2718,37 @@ int32_t phieng_sph3_sync(World3* w) {
     if (w->h_pinned[8] != 0u && w->error == PHIENG_SPH_OK) w->error = PHIENG_SPH_E_CUDA;  // a scan wait gave up
   }
   return w->error == PHIENG_SPH_OK ? 1 : 0;
+}
+
+int32_t phieng_sph3_step_fluid(World3* w, PhiengBody3* bodies, uint32_t nbodies, float dt) {
+  if (!w || (nbodies && !bodies) || nbodies > kMaxCallBodies3) return 0;
+  for (uint32_t k = 0; k < nbodies; k++)
+    if (!body3_valid(bodies[k], false)) return 0;
+  return step_fluid_bodies3(w, bodies, nbodies, dt) ? 1 : 0;
+}
+
+int32_t phieng_sph3_step_fluid_hull(World3* w, PhiengBody3* bodies, uint32_t nbodies, const float* hull_xyz,
+                                    const uint32_t* hull_first, const uint32_t* hull_count, uint32_t hull_nverts,
+                                    float dt) {
+  if (!w || (nbodies && !bodies) || nbodies > kMaxCallBodies3 || hull_nverts > kMaxHullVerts3) return 0;
+  uint64_t total = 0;
+  for (uint32_t k = 0; k < nbodies; k++) {
+    const PhiengBody3& b = bodies[k];
+    if (!body3_valid(b, true)) return 0;
+    if (b.shape_tag != PHIENG_SHAPE3_HULL) continue;
+    if (!hull_xyz || !hull_first || !hull_count) return 0;
+    const uint64_t f = hull_first[k], c = hull_count[k];
+    if (c < 1 || f + c > hull_nverts) return 0;
+    for (uint64_t i = 3 * f; i < 3 * (f + c); i++)
+      if (!std::isfinite(hull_xyz[i])) return 0;
+    total += c;
+  }
+  if (total > kMaxHullVerts3) return 0;
+  HullIn hin;
+  hin.xyz = hull_xyz;
+  hin.first = hull_first;
+  hin.count = hull_count;
+  return step_fluid_bodies3(w, bodies, nbodies, dt, hin) ? 1 : 0;
 }
 
 int32_t phieng_sph3_set_state(World3* w, const float* xyzv, uint32_t n) {

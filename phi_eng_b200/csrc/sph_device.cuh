@@ -51,6 +51,7 @@ enum StepFlags : uint32_t {
   F_GHOST = 1u << 11,      // boundary ghost particles (boundary_particles)
   F_POLY = 1u << 12,       // polygon bodies among the launch's bodies
   F_FAST = 1u << 13,       // tolerance mode: the plain passes may run the reassociated kernels (sph_fast.cuh)
+  F_QBODIES = 1u << 14,    // 3D: the boundary pass runs over the engine's bodies (rotations, reactions)
 };
 
 // One cell of the boundary ghosts' hash grid: ghosts [start, start + count)

@@ -1655,12 +1655,18 @@ __global__ void k_buoyancy(const uint32_t* __restrict__ which, uint32_t nb, cons
   dyn[k] = d;
 }
 
-void enqueue_dynamic_walls(const FluidBufs& b, const DynBufs& y, uint32_t n, const StepParams& P, cudaStream_t st) {
+void enqueue_flag_compact(uint32_t* flags, uint32_t n, uint32_t* tile, uint32_t* done, uint32_t* start,
+                          uint32_t* list, cudaStream_t st) {
   if (n == 0) return;
   const uint32_t nt = cdiv(n + 1, kScanTile);
-  k_scan_reduce<<<nt, 256, 0, st>>>(y.dcount, y.dtile, nt, y.done);
-  k_scan_down<<<nt, 256, 0, st>>>(y.dcount, y.dtile, n + 1, y.dstart);
-  k_compact_deferred<<<cdiv(n, 256), 256, 0, st>>>(y.dstart, n, y.list);
+  k_scan_reduce<<<nt, 256, 0, st>>>(flags, tile, nt, done);
+  k_scan_down<<<nt, 256, 0, st>>>(flags, tile, n + 1, start);
+  k_compact_deferred<<<cdiv(n, 256), 256, 0, st>>>(start, n, list);
+}
+
+void enqueue_dynamic_walls(const FluidBufs& b, const DynBufs& y, uint32_t n, const StepParams& P, cudaStream_t st) {
+  if (n == 0) return;
+  enqueue_flag_compact(y.dcount, n, y.dtile, y.done, y.dstart, y.list, st);
   k_dynamic_walls<<<1, 32, 0, st>>>(y.list, y.dstart + n, b.defer, b.state, b.mass, b.key, b.count, b.bodies, y.dyn,
                                     P);
 }

@@ -192,6 +192,13 @@ struct DynBufs {
   uint32_t* count2 = nullptr;    // copy of the bucket counts for the buoyancy sort
 };
 
+// Ordered compaction of flagged ids: flags[0, n) hold 0 / 1 and are zero up
+// to the next whole scan tile past n; start becomes their exclusive prefix
+// (start[n] = the flagged count) and list[0, start[n]) the flagged ids in
+// ascending order. done: a zeroed device word (left zero).
+void enqueue_flag_compact(uint32_t* flags, uint32_t n, uint32_t* tile, uint32_t* done, uint32_t* start,
+                          uint32_t* list, cudaStream_t st);
+
 // After K6 with F_DYNAMIC: finish the body loop of the deferred particles in
 // particle order with the bodies' reactions, and their keys / counts.
 void enqueue_dynamic_walls(const FluidBufs& b, const DynBufs& y, uint32_t n, const StepParams& P, cudaStream_t st);

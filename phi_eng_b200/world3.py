@@ -52,6 +52,47 @@ class Capsule:
     half_length: float
 
 
+def body3(shape, position, rotation=(0.0, 0.0, 0.0, 1.0), density: float | None = None, velocity=(0.0, 0.0, 0.0),
+          angular_velocity=(0.0, 0.0, 0.0)) -> "_abi.PhiengBody3":
+    """A PhiengBody3 for World3.step_fluid: static when density is None, else
+    dynamic with the mass and diagonal inertia of mass_properties_3d
+    (body.rs:811-830) for a Sphere or Box3 (inverse inertia 1 / I per axis)."""
+    b = _abi.PhiengBody3()
+    if isinstance(shape, Sphere):
+        b.shape_tag, b.a = _abi.SHAPE3_SPHERE, shape.radius
+    elif isinstance(shape, Box3):
+        b.shape_tag, b.a, b.b, b.c = _abi.SHAPE3_BOX, shape.hx, shape.hy, shape.hz
+    elif isinstance(shape, Capsule):
+        b.shape_tag, b.a, b.b = _abi.SHAPE3_CAPSULE, shape.radius, shape.half_length
+    else:
+        raise TypeError("shape must be Sphere, Box3 or Capsule")
+    b.px, b.py, b.pz = (float(v) for v in position)
+    b.qx, b.qy, b.qz, b.qw = (float(v) for v in rotation)
+    b.vx, b.vy, b.vz = (float(v) for v in velocity)
+    b.wx, b.wy, b.wz = (float(v) for v in angular_velocity)
+    if density is None:
+        b.is_static = 1
+        return b
+    f = np.float32
+    d = f(density)
+    if isinstance(shape, Sphere):
+        r = f(shape.radius)
+        m = ((f(4.0) / f(3.0)) * f(np.pi) * r * r * r) * d
+        i = f(0.4) * m * r * r
+        diag = (i, i, i)
+    elif isinstance(shape, Box3):
+        w, h, dd = f(shape.hx) * f(2), f(shape.hy) * f(2), f(shape.hz) * f(2)
+        m = (w * h * dd) * d
+        diag = (m * (h * h + dd * dd) / f(12), m * (w * w + dd * dd) / f(12), m * (w * w + h * h) / f(12))
+    else:
+        raise TypeError("dynamic bodies here: Sphere or Box3 (pass inv_mass / inv_inertia yourself for others)")
+    b.is_static = 0
+    b.inv_mass = f(1) / m
+    for k in range(3):
+        b.inv_inertia[4 * k] = f(1) / diag[k]
+    return b
+
+
 class FluidState3:
     """world.fluid of a World3: config, particle insertion and read-back."""
 
@@ -211,6 +252,26 @@ class World3:
 
     def body_count(self) -> int:
         return int(self._lib.phieng_world3_body_count(self._h))
+
+    def step_fluid(self, bodies, dt: float, hulls=None) -> None:
+        """FluidState3::step_fluid with the engine's bodies (a ctypes
+        PhiengBody3 array, updated in place: velocities and sleep flags), in
+        place of the world's static bodies; the clock does not advance.
+        hulls = (xyz float32 [m][3], first uint32 [nb], count uint32 [nb]) for
+        PHIENG_SHAPE3_HULL bodies."""
+        n = len(bodies)
+        if hulls is None:
+            ok = self._lib.phieng_sph3_step_fluid(self._h, bodies, n, dt)
+        else:
+            xyz = np.ascontiguousarray(hulls[0], np.float32).reshape(-1, 3)
+            first = np.ascontiguousarray(hulls[1], np.uint32)
+            count = np.ascontiguousarray(hulls[2], np.uint32)
+            U = C.POINTER(C.c_uint32)
+            ok = self._lib.phieng_sph3_step_fluid_hull(self._h, bodies, n, _fptr(xyz), first.ctypes.data_as(U),
+                                                       count.ctypes.data_as(U), xyz.shape[0], dt)
+        if ok != 1:
+            self.check()
+            raise ValueError("invalid bodies for the fluid phase")
 
     def step(self, dt: float) -> None:
         self._lib.phieng_world3_step(self._h, dt)
