@@ -305,6 +305,9 @@ def coupled_parity3(cfg, bodies, frames, settle=40, pts=None, wind=None, turb=No
         w.step_fluid(b, f32(DT), hulls)
         drift(a, DT)
         drift(b, DT)
+        # a body that blows up turns NaN on both sides with different NaN
+        # bits; say so instead of reporting a bit difference
+        assert np.isfinite(body_bits(a).view(np.float32)).all(), f"oracle bodies non-finite at frame {f}"
         assert (body_bits(a) == body_bits(b)).all(), f"bodies differ at frame {f}"
         assert [x.is_sleeping for x in a] == [x.is_sleeping for x in b]
         if f % 10 == 9 or f == frames - 1:
@@ -341,7 +344,13 @@ def test_step_fluid3_statics_equal_world_step():
 
 @pytest.mark.gpu
 def test_step_fluid3_bit_exact_frictionless():
-    a = coupled_parity3(default_config(), floating_bodies3(), 80)
+    # drag 1 instead of the default 4: the buoyancy pass applies the
+    # quadratic drag explicitly, sample after sample, and the light box
+    # (inverse inertia ~275) spins up without bound under drag 4 (the
+    # oracle's box goes to inf at frame 35, as the reference's would)
+    c = default_config()
+    c.drag = 1.0
+    a = coupled_parity3(c, floating_bodies3(), 80)
     assert any(abs(b.wx) + abs(b.wy) + abs(b.wz) > 0 for b in a[5:8])  # the coupling produced torque
     assert any(b.vy != 0 for b in a[5:8])
 
