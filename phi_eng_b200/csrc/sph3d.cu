@@ -1072,7 +1072,7 @@ __global__ void __launch_bounds__(256) k_force3(const float4* __restrict__ spos,
   }
   const uint32_t nk = bucket_key3(x, y, z, g);
   key_out[id] = nk;
-  count_key(count_out, nk);
+  atomicAdd(&count_out[nk], 1u);  // one atomic per particle, as the 2D force pass
 }
 
 __global__ void __launch_bounds__(256) k_vmax3(const float4* __restrict__ vel, uint32_t n, unsigned int* out) {
