@@ -52,6 +52,7 @@ enum StepFlags : uint32_t {
   F_POLY = 1u << 12,       // polygon bodies among the launch's bodies
   F_FAST = 1u << 13,       // tolerance mode: the plain passes may run the reassociated kernels (sph_fast.cuh)
   F_QBODIES = 1u << 14,    // 3D: the boundary pass runs over the engine's bodies (rotations, reactions)
+  F_WBOX = 1u << 15,       // StepParams::wbox holds every body's padded bounding box (at most kWallBoxes bodies)
 };
 
 // One cell of the boundary ghosts' hash grid: ghosts [start, start + count)
@@ -67,6 +68,9 @@ __host__ __device__ inline uint32_t ghost_cell_hash(int32_t cx, int32_t cy, uint
   h ^= h >> 15;
   return h & mask;
 }
+
+// Bodies whose bounding boxes a launch can carry in its parameters.
+constexpr uint32_t kWallBoxes = 4;
 
 struct StepParams {
   GridPlan grid;
@@ -108,6 +112,9 @@ struct StepParams {
   float turb_amp, turb_freq, turb_tscale;
   uint32_t turb_seed, turb_oct;  // octaves already clamped to 1..8
   const float* clock;            // device word holding the world clock of the current step
+  // F_WBOX: body k's bounding box as (px, py, ex + pr_pad, ey + pr_pad), the
+  // values of the wall pass's reject test; unused slots never pass it
+  float4 wbox[kWallBoxes];
 };
 
 // Per-launch scene access: a single world passes its parameters by value
@@ -442,6 +449,18 @@ __device__ __forceinline__ bool collide(float px, float py, float pr, const DevB
 template <bool POLY = true>
 __device__ __forceinline__ uint32_t walls(float& x, float& y, float& vx, float& vy,
                                           const DevBody* __restrict__ bodies, const StepParams& P) {
+  if (P.flags & F_WBOX) {
+    // the reject test below for every body at once, from the launch
+    // parameters: a particle it rejects for every body touches none, and
+    // nothing moves it between bodies, so the loop would change nothing
+    bool near = false;
+#pragma unroll
+    for (uint32_t k = 0; k < kWallBoxes; k++) {
+      const float4 wb = P.wbox[k];
+      near = near || !(fabsf(x - wb.x) > wb.z || fabsf(y - wb.y) > wb.w);
+    }
+    if (!near) return kNoDefer;
+  }
   for (uint32_t k = 0; k < P.nbodies; k++) {
     const DevBody* bp = bodies + P.body_first + k;
     // bounding-box reject first: only the centre and the padded extents are read

@@ -578,6 +578,19 @@ StepParams make_params_for(const FluidConfig2Ffi& c, float gx, float gy, bool ma
   return P;
 }
 
+// The launch's copy of the wall pass's bounding-box reject (F_WBOX), for
+// the P.nbodies bodies at `bodies` (the array the kernels read from
+// P.body_first on): each box is the test's (px, py, ex + pr_pad, ey + pr_pad),
+// summed in f32 as the device sums it; unused slots hold an extent of -1,
+// which every finite position exceeds.
+void set_wall_boxes(StepParams& P, const DevBody* bodies) {
+  if (P.nbodies > kWallBoxes || (P.nbodies && !bodies)) return;
+  for (uint32_t k = 0; k < kWallBoxes; k++)
+    P.wbox[k] = k < P.nbodies ? make_float4(bodies[k].px, bodies[k].py, bodies[k].ex + P.pr_pad, bodies[k].ey + P.pr_pad)
+                              : make_float4(0.0f, 0.0f, -1.0f, -1.0f);
+  P.flags |= F_WBOX;
+}
+
 // Ambient turbulence of a single world (fluid.rs:1001-1002: on when enabled
 // with a positive amplitude). The kernels read the step's clock from a device
 // word (set_clock), so cached graphs stay valid as the clock advances.
@@ -612,6 +625,7 @@ StepParams make_params(const World2* w, float dt) {
   if (!w->is_batch()) {
     StepParams P = make_params_for(w->cfg, w->gx, w->gy, w->mass_uniform, w->mass_value, w->phase_uniform,
                                    w->phase_value, w->plan, 0, (uint32_t)w->bodies.size(), dt);
+    set_wall_boxes(P, w->bodies.data());
     apply_ambient(w, P);
     apply_ghosts(w, P);
     if (w->precision == PHIENG_SPH_TOLERANCE) P.flags |= F_FAST;
@@ -647,9 +661,11 @@ StepParams make_params(const World2* w, float dt) {
 bool upload_scene_table(World2* w, float dt) {
   std::vector<StepParams> tab;
   tab.reserve(w->scenes.size());
-  for (const auto& sc : w->scenes)
+  for (const auto& sc : w->scenes) {
     tab.push_back(make_params_for(sc.cfg, sc.gx, sc.gy, sc.mass_uniform, sc.mass_value, sc.phase_uniform,
                                   sc.phase_value, sc.plan, sc.body_first, sc.nbodies, dt));
+    set_wall_boxes(tab.back(), w->bodies.data() + sc.body_first);
+  }
   return cuda_ok(w, cudaMemcpyAsync(w->d_ptab, tab.data(), sizeof(StepParams) * tab.size(), cudaMemcpyHostToDevice,
                                     w->stream),
                  "upload scene table");
@@ -1299,6 +1315,7 @@ bool step_fluid_bodies(World2* w, PhiengBody2* bodies, uint32_t nb, float dt, co
   const float sub = dt / (float)ns;
   StepParams P = make_params_for(w->cfg, w->gx, w->gy, w->mass_uniform, w->mass_value, w->phase_uniform,
                                  w->phase_value, w->plan, 0, nb, sub);
+  set_wall_boxes(P, db.data());
   if (any_dyn) P.flags |= F_DYNAMIC;
   if (!wv.empty()) P.flags |= F_POLY;
   P.poly = w->d_poly;
