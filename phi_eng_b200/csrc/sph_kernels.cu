@@ -31,7 +31,8 @@ namespace {
 // Counting sort over the whole bucket key (a one-digit radix sort with radix
 // = number of buckets), then an in-bucket rank by id, so the final order is
 // exactly (key, id):
-//   count   K1 / K6 add each particle to count[key] (warp-aggregated)
+//   count   K1 / K6 add each particle to count[key] (K1 warp-aggregated,
+//           K6 one atomic per particle)
 //   scan    count -> start (exclusive; start doubles as the bucket range
 //           table: bucket b holds slots [start[b], start[b+1])), and count
 //           becomes the placement cursor
