@@ -11,6 +11,12 @@
 // glam's quaternion products with the identity return the vector unchanged.
 // Float arithmetic follows glam 0.29's scalar Vec3 (dot = (x*x + y*y) + z*z,
 // component-wise operators); built with -ffp-contract=off.
+// Pinned against a second statement of the algorithm by the reference's
+// authors, the C# solver (src/PhiEng.Dynamics/FluidSolver3.cs, restated in
+// oracle/fluid3_cs.py): bit-identical in REF_SEQ order on the reference's
+// own 3D equivalence scene (tests/PhiEng.Tests/EquivalenceTests.cs:177-225,
+// 30 steps) and on a five-box tank with CFL substeps and wall friction
+// (tests/test_oracle_pin.py).
 #pragma once
 
 #include <algorithm>

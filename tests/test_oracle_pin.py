@@ -10,6 +10,11 @@ position and 1e-3 in velocity per particle. The C++ oracle in the
 reference's own (in-place) order must agree with the C# restatement on that
 scene within the same bar; it does so bit for bit where both are IEEE f32 in
 the same order, which this test also records.
+
+The 3D oracle (oracle/sph_oracle3.hpp, from fluid3.rs) is pinned the same
+way to the C# 3D solver (src/PhiEng.Dynamics/FluidSolver3.cs, restated in
+oracle/fluid3_cs.py), on the scene of EquivalenceTests.cs:177-225 (30 steps,
+1e-4 in position) and on the reference's five-box test tank.
 """
 import numpy as np
 
@@ -61,4 +66,63 @@ def test_oracle_matches_csharp_solver_tait():
     a, b = run_both(cfg, 40, pts)
     dp = np.sqrt(((a[:, :2] - b[:, :2]).astype(np.float64) ** 2).sum(1)).max()
     dv = np.sqrt(((a[:, 2:] - b[:, 2:]).astype(np.float64) ** 2).sum(1)).max()
+    assert dp < 1e-4 and dv < 1e-3, (dp, dv)
+
+
+# ---- 3D: crates/dynamics/src/fluid3.rs against src/PhiEng.Dynamics/FluidSolver3.cs ----
+
+from oracle import fluid3_cs  # noqa: E402
+from phi_eng_b200._abi import default_config  # noqa: E402
+from test_fluid3 import BOX, TANK as TANK3, lattice, make_oracle  # noqa: E402
+
+
+def run_both3(cfg, steps, pts, bodies):
+    cs = fluid3_cs.CsFluid3(cfg, [(*p, *e) for _, p, e in bodies])
+    cs.add_particles(pts)
+    o = make_oracle(pts, bodies=bodies, cfg=cfg, gravity=(0.0, -9.81, 0.0))
+    for _ in range(steps):
+        cs.step(1.0 / 60.0)
+        o.step(1.0 / 60.0, orc.REF_SEQ)
+    a, b = cs.state(), o.state()
+    dp = np.sqrt(((a[:, :3] - b[:, :3]).astype(np.float64) ** 2).sum(1)).max()
+    dv = np.sqrt(((a[:, 3:] - b[:, 3:]).astype(np.float64) ** 2).sum(1)).max()
+    return a, b, dp, dv
+
+
+def test_oracle3_matches_csharp_solver_on_the_equivalence_scene():
+    """EquivalenceTests.cs:177-225: a 3 x 3 x 3 lattice at 0.25 (iz, iy, ix
+    loops) over one static box (centre (1, -1, 1), half extents (2, 0.5, 2)),
+    default config, 30 steps of 1/60 s; the reference's bar is 1e-4 in
+    position. The two restatements agree bit for bit."""
+    pts = np.array([(ix * 0.25, iy * 0.25, iz * 0.25) for iz in range(3) for iy in range(3) for ix in range(3)],
+                   np.float32)
+    a, b, dp, dv = run_both3(default_config(), 30, pts, [(BOX, (1.0, -1.0, 1.0), (2.0, 0.5, 2.0))])
+    assert dp < 1e-4, dp
+    assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+
+
+def test_oracle3_matches_csharp_solver_tank_cfl_friction():
+    """A 6 x 5 x 6 lattice in the reference's five-box test tank, linear EOS,
+    CFL substeps and wall friction, 40 steps: bit for bit."""
+    cfg = default_config()
+    cfg.cfl = 0.4
+    cfg.max_substeps = 4
+    cfg.wall_friction = 0.5
+    pts = lattice((0.125, -0.375, 0.125), 6, 5, 6, 0.25)
+    a, b, dp, dv = run_both3(cfg, 40, pts, TANK3)
+    assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), (dp, dv)
+
+
+def test_oracle3_matches_csharp_solver_tait():
+    """Tait EOS (gamma 7, k 10) with CFL substeps, 20 steps: the power
+    functions differ by an ulp at times (the oracle's correctly rounded power,
+    numpy's float32 power for MathF.Pow); the runs stay within the
+    reference's bars (1e-4 position, 1e-3 velocity)."""
+    cfg = default_config()
+    cfg.gamma = 7.0
+    cfg.stiffness = 10.0
+    cfg.cfl = 0.4
+    cfg.max_substeps = 4
+    pts = lattice((0.125, -0.375, 0.125), 6, 5, 6, 0.25)
+    a, b, dp, dv = run_both3(cfg, 20, pts, TANK3)
     assert dp < 1e-4 and dv < 1e-3, (dp, dv)
