@@ -12,8 +12,8 @@ the 3D oracle to a statement of the algorithm written by the reference's
 authors.
 
 Scope: the default flag set (linear or Tait EOS, XSPH, CFL substeps, static
-boxes at the identity rotation; no artificial viscosity, cohesion, ghosts,
-resampling, turbulence or dynamic bodies). System.Numerics operations are
+boxes at the identity rotation) plus Monaghan artificial viscosity, cohesion
+and wall friction; no ghosts, resampling, turbulence or dynamic bodies. System.Numerics operations are
 restated component-wise in the C# source's order on numpy float32 scalars:
 Vector3.Dot and LengthSquared as (x x' + y y') + z z', Length as the square
 root of that, a vector divided by a scalar component by component, and the
@@ -192,6 +192,7 @@ class CsFluid3:
         h = max(F(c.smoothing_length), EPS)
         self.rebuild_grid()
         self.density_pressure(h)
+        cs = F(np.sqrt(max(F(c.stiffness), F(0))))
         n = len(self.pos)
         forces = []
         for i in range(n):
@@ -206,8 +207,22 @@ class CsFluid3:
                 dist = length(delta)
                 grad = spiky_grad(delta, dist, h)
                 term = p_i / (rho_i * rho_i) + self.pres[j] / (rho_j * rho_j)
+                if F(c.artificial_viscosity) > F(0) and dist > EPS:
+                    # FluidSolver3.cs:75-85, called at :983-987
+                    rho_bar = F(0.5) * (rho_i + rho_j)
+                    vrel = tuple(a - b for a, b in zip(self.vel[i], self.vel[j]))
+                    vd = dot(vrel, delta)
+                    if not vd >= F(0):
+                        mu = h * vd / (dist * dist + F(0.01) * h * h)
+                        term = term + -F(c.artificial_viscosity) * cs * mu / max(rho_bar, EPS)
                 mt = self.mass[j] * term
                 f = [fa - g * mt for fa, g in zip(f, grad)]
+                if F(c.surface_tension) > F(0) and dist > EPS:
+                    # FluidSolver3.cs:87-94, applied at :989-996
+                    coh = F(0) if dist >= h else F(1) - dist / h
+                    if coh > F(0):
+                        sc = F(c.surface_tension) * self.mass[i] * self.mass[j] * coh
+                        f = [fa - (d / dist) * sc for fa, d in zip(f, delta)]
             forces.append(f)
         # integrate in place: later particles see the earlier ones' new state
         visc, vmax = F(c.viscosity), F(c.max_velocity)

@@ -11,8 +11,8 @@ the C++ oracle on that scene with that bar, which ties the oracle to a
 statement of the algorithm written by the reference's authors.
 
 Scope: the default flag set of that scene (linear or Tait EOS, XSPH, static
-boxes and circles; no artificial viscosity, cohesion, ghosts, resampling,
-turbulence or dynamic bodies). Every operation is an IEEE f32 operation on
+boxes and circles) plus Monaghan artificial viscosity and cohesion; no
+ghosts, resampling, turbulence or dynamic bodies. Every operation is an IEEE f32 operation on
 numpy float32 scalars in the C# source's evaluation order (System.Numerics
 vector ops restated component-wise); slow, for scenes of a few hundred
 particles.
@@ -67,6 +67,8 @@ class CsFluid:
         self.k = F(cfg.stiffness)
         self.gamma = F(cfg.gamma)
         self.visc = F(cfg.viscosity)
+        self.av = F(cfg.artificial_viscosity)
+        self.st = F(cfg.surface_tension)
         self.vmax = F(cfg.max_velocity)
         self.pr = max(F(cfg.particle_radius), F(0))
         self.mass0 = F(cfg.phase_mass[0])
@@ -164,6 +166,7 @@ class CsFluid:
         n = len(self.pos)
         self._rebuild()
         self._density_pressure(h)
+        self.cs = F(np.sqrt(max(self.k, F(0))))
         forces = []
         for i in range(n):
             px, py = self.pos[i]
@@ -178,9 +181,24 @@ class CsFluid:
                 dist = length(dx, dy)
                 gx, gy = spiky_grad(dx, dy, dist, h)
                 term = p_i / (rho_i * rho_i) + self.pres[j] / (rho_j * rho_j)
+                if self.av > F(0) and dist > EPS:
+                    # FluidSolver.cs:89-98, called at :858-862
+                    rho_bar = F(0.5) * (rho_i + rho_j)
+                    vrx, vry = self.vel[i][0] - self.vel[j][0], self.vel[i][1] - self.vel[j][1]
+                    vd = vrx * dx + vry * dy
+                    if not vd >= F(0):
+                        mu = h * vd / (dist * dist + F(0.01) * h * h)
+                        term = term + -self.av * self.cs * mu / max(rho_bar, EPS)
                 mt = self.mass[j] * term
                 fx = fx - gx * mt
                 fy = fy - gy * mt
+                if self.st > F(0) and dist > EPS:
+                    # FluidSolver.cs:101-108, applied at :864-871
+                    coh = F(0) if dist >= h else F(1) - dist / h
+                    if coh > F(0):
+                        sc = self.st * self.mass[i] * self.mass[j] * coh
+                        fx = fx - dx / dist * sc
+                        fy = fy - dy / dist * sc
             forces.append((fx, fy))
         for i in range(n):
             nb = self._neighbors(i)  # from the grid of this substep, positions as they are now

@@ -126,3 +126,30 @@ def test_oracle3_matches_csharp_solver_tait():
     pts = lattice((0.125, -0.375, 0.125), 6, 5, 6, 0.25)
     a, b, dp, dv = run_both3(cfg, 20, pts, TANK3)
     assert dp < 1e-4 and dv < 1e-3, (dp, dv)
+
+
+def test_oracle_matches_csharp_solver_av_cohesion():
+    """Monaghan artificial viscosity (alpha 0.5) and cohesion (surface
+    tension 2) on the 2D equivalence scene, 60 steps: bit for bit, and the
+    terms change the run."""
+    cfg = sims.default_cfg()
+    cfg.artificial_viscosity = 0.5
+    cfg.surface_tension = 2.0
+    a, b = run_both(cfg, 60)
+    assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+    plain, _ = run_both(sims.default_cfg(), 60)
+    assert not np.array_equal(a, plain)
+
+
+def test_oracle3_matches_csharp_solver_av_cohesion():
+    """The same terms (and wall friction) in the 3D tank, 40 steps: bit for
+    bit, and the terms change the run."""
+    cfg = default_config()
+    cfg.artificial_viscosity = 0.5
+    cfg.surface_tension = 2.0
+    cfg.wall_friction = 0.3
+    pts = lattice((0.125, -0.375, 0.125), 6, 5, 6, 0.25)
+    a, b, dp, dv = run_both3(cfg, 40, pts, TANK3)
+    assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), (dp, dv)
+    plain, _, _, _ = run_both3(default_config(), 40, pts, TANK3)
+    assert not np.array_equal(a, plain)
