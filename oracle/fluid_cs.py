@@ -11,8 +11,9 @@ the C++ oracle on that scene with that bar, which ties the oracle to a
 statement of the algorithm written by the reference's authors.
 
 Scope: the default flag set of that scene (linear or Tait EOS, XSPH, static
-boxes and circles) plus Monaghan artificial viscosity and cohesion; no
-ghosts, resampling, turbulence or dynamic bodies. Every operation is an IEEE f32 operation on
+boxes and circles, CFL substeps) plus Monaghan artificial viscosity,
+cohesion and wall friction; no ghosts, resampling, turbulence or dynamic
+bodies. Every operation is an IEEE f32 operation on
 numpy float32 scalars in the C# source's evaluation order (System.Numerics
 vector ops restated component-wise); slow, for scenes of a few hundred
 particles.
@@ -68,6 +69,9 @@ class CsFluid:
         self.gamma = F(cfg.gamma)
         self.visc = F(cfg.viscosity)
         self.av = F(cfg.artificial_viscosity)
+        self.friction = F(cfg.wall_friction)
+        self.cfl = F(cfg.cfl)
+        self.max_substeps = int(cfg.max_substeps)
         self.st = F(cfg.surface_tension)
         self.vmax = F(cfg.max_velocity)
         self.pr = max(F(cfg.particle_radius), F(0))
@@ -159,8 +163,37 @@ class CsFluid:
             return copysign1(lx), F(0), pr + dxp
         return F(0), copysign1(ly), pr + dyp
 
-    # ---- FluidSolver.cs:793-948 + the boundary loop
+    # ---- FluidSolver.cs:381-410
+    def cfl_substeps(self, dt):
+        mx = 1 if self.max_substeps < 1 else self.max_substeps
+        if self.cfl <= F(0) or mx <= 1:
+            return 1
+        h = max(self.h_cfg, EPS)
+        rho0 = max(self.rest, EPS)
+        k = max(self.k, F(0))
+        c0 = F(np.sqrt(k)) if self.gamma == F(1) else F(np.sqrt(self.gamma * k * rho0))
+        vmax = F(0)
+        for v in self.vel:
+            vmax = max(vmax, length(v[0], v[1]))
+        speed = c0 + vmax
+        if not math.isfinite(speed) or speed <= EPS:
+            return 1
+        dt_max = self.cfl * h / speed
+        if not math.isfinite(dt_max) or dt_max <= F(0):
+            return 1
+        return max(1, min(int(math.ceil(F(dt) / dt_max)), mx))
+
+    # ---- FluidSolver.cs:27-45: CFL substeps of Substep2
     def step(self, dt):
+        if not self.pos or not F(dt) > F(0):
+            return
+        k = self.cfl_substeps(dt)
+        sub = F(dt) / F(k)
+        for _ in range(k):
+            self.substep(sub)
+
+    # ---- FluidSolver.cs:793-948 + the boundary loop
+    def substep(self, dt):
         dt = F(dt)
         h = max(self.h_cfg, EPS)
         n = len(self.pos)
@@ -243,7 +276,14 @@ class CsFluid:
                 self.pos[i] = [px + nx * depth, py + ny * depth]
                 vn = self.vel[i][0] * nx + self.vel[i][1] * ny
                 if vn < F(0):
-                    self.vel[i] = [self.vel[i][0] - nx * vn, self.vel[i][1] - ny * vn]
+                    vx, vy = self.vel[i][0] - nx * vn, self.vel[i][1] - ny * vn
+                    if self.friction > F(0):
+                        # FluidSolver.cs:973-982 against a static body (velocity zero)
+                        mu = min(max(self.friction, F(0)), F(1))
+                        wn = F(0) * nx + F(0) * ny
+                        wtx, wty = F(0) - nx * wn, F(0) - ny * wn
+                        vx, vy = vx + (wtx - vx) * mu, vy + (wty - vy) * mu
+                    self.vel[i] = [vx, vy]
 
     def state(self):
         return np.array([[p[0], p[1], v[0], v[1]] for p, v in zip(self.pos, self.vel)], np.float32)

@@ -102,13 +102,18 @@ def test_oracle3_matches_csharp_solver_on_the_equivalence_scene():
 
 
 def test_oracle3_matches_csharp_solver_tank_cfl_friction():
-    """A 6 x 5 x 6 lattice in the reference's five-box test tank, linear EOS,
-    CFL substeps and wall friction, 40 steps: bit for bit."""
+    """A 6 x 5 x 6 lattice in the reference's five-box test tank, linear EOS
+    (k 400: two CFL substeps per step from the start), wall friction, 40
+    steps: bit for bit."""
     cfg = default_config()
+    cfg.stiffness = 400.0
     cfg.cfl = 0.4
     cfg.max_substeps = 4
     cfg.wall_friction = 0.5
     pts = lattice((0.125, -0.375, 0.125), 6, 5, 6, 0.25)
+    cs = fluid3_cs.CsFluid3(cfg, [(*p, *e) for _, p, e in TANK3])
+    cs.add_particles(pts)
+    assert cs.cfl_substeps(1.0 / 60.0) >= 2
     a, b, dp, dv = run_both3(cfg, 40, pts, TANK3)
     assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), (dp, dv)
 
@@ -153,3 +158,18 @@ def test_oracle3_matches_csharp_solver_av_cohesion():
     assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), (dp, dv)
     plain, _, _, _ = run_both3(default_config(), 40, pts, TANK3)
     assert not np.array_equal(a, plain)
+
+
+def test_oracle_matches_csharp_solver_cfl_friction():
+    """CFL substeps (k 400: two substeps per 1/60 s step from the start) and
+    wall friction on the 2D equivalence scene, 60 steps: bit for bit."""
+    cfg = sims.default_cfg()
+    cfg.stiffness = 400.0
+    cfg.cfl = 0.4
+    cfg.max_substeps = 4
+    cfg.wall_friction = 0.5
+    cs = fluid_cs.CsFluid(cfg, TANK)
+    cs.add_particles(equivalence_points())
+    assert cs.cfl_substeps(1.0 / 60.0) >= 2
+    a, b = run_both(cfg, 60)
+    assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
