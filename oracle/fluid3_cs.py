@@ -12,7 +12,7 @@ the 3D oracle to a statement of the algorithm written by the reference's
 authors.
 
 Scope: the default flag set (linear or Tait EOS, XSPH, CFL substeps, static
-boxes at the identity rotation) plus Monaghan artificial viscosity, cohesion
+spheres, boxes and capsules at the identity rotation) plus Monaghan artificial viscosity, cohesion
 and wall friction; no ghosts, resampling, turbulence or dynamic bodies. System.Numerics operations are
 restated component-wise in the C# source's order on numpy float32 scalars:
 Vector3.Dot and LengthSquared as (x x' + y y') + z z', Length as the square
@@ -80,13 +80,23 @@ def clamp(x, lo, hi):
     return x
 
 
+SPHERE, BOX, CAPSULE = 0, 1, 2
+
+
 class CsFluid3:
     """FluidState3 + FluidIntegration3.StepFluid3 with static identity-rotation
-    boxes (px, py, pz, hx, hy, hz) in body order."""
+    bodies (shape, (px, py, pz), (a, b, c)) in body order: SPHERE (a =
+    radius), BOX (half extents), CAPSULE (a = radius, b = half length along
+    y)."""
 
-    def __init__(self, cfg, boxes, gravity=(0.0, -9.81, 0.0)):
+    def __init__(self, cfg, bodies, gravity=(0.0, -9.81, 0.0), rust_sign=False):
+        # rust_sign: a particle inside a box is pushed out along +axis, as the
+        # Rust step's signum().copysign(1.0) does (fluid3.rs), instead of the
+        # C# Copysign1's -axis for a negative coordinate: the one place where
+        # the reference's two statements differ
+        self.rust_sign = rust_sign
         self.cfg = cfg
-        self.boxes = [tuple(F(v) for v in b) for b in boxes]
+        self.bodies = [(int(sh), tuple(F(v) for v in p), tuple(F(v) for v in e)) for sh, p, e in bodies]
         self.g = tuple(F(v) for v in gravity)
         self.pos, self.vel, self.mass, self.dens, self.pres = [], [], [], [], []
         self.grid = {}
@@ -163,7 +173,36 @@ class CsFluid3:
         for i in range(len(self.pos)):
             self.pres[i] = pressure(self.dens[i], F(c.phase_rest_density[0]), F(c.stiffness), F(c.gamma))
 
-    # CollideParticleBody3, BoxShape3 branch (FluidSolver3.cs:343-385), identity rotation
+    # CollideParticleBody3 (FluidSolver3.cs:325-443), identity rotation
+    def collide(self, p, pr, body):
+        shape, bp, ext = body
+        if shape == SPHERE:  # :330-342
+            delta = tuple(a - c for a, c in zip(p, bp))
+            dist = length(delta)
+            if dist >= ext[0] + pr:
+                return None
+            normal = tuple(d / dist for d in delta) if dist > EPS else (F(1), F(0), F(0))
+            return normal, ext[0] + pr - dist
+        if shape == CAPSULE:  # :386-413
+            r, hl = ext[0], ext[1]
+            local = tuple(a - c for a, c in zip(p, bp))
+            sy = clamp(local[1], -hl, hl)
+            diff = (local[0] - F(0), local[1] - sy, local[2] - F(0))
+            if dot(diff, diff) > EPS_SQ:
+                dist = length(diff)
+                if dist >= r + pr:
+                    return None
+                return tuple(d / dist for d in diff), r + pr - dist
+            radial = (local[0], F(0), local[2])
+            if dot(radial, radial) > EPS_SQ:
+                ln = length(radial)  # NormalizeOrZero
+                d = tuple(c / ln for c in radial) if ln > F(0) and np.isfinite(ln) else (F(0), F(0), F(0))
+            else:
+                d = (F(1), F(0), F(0))
+            return d, pr + r - length(diff)
+        return self.collide_box(p, pr, bp + ext)
+
+    # BoxShape3 branch (FluidSolver3.cs:343-385)
     def collide_box(self, p, pr, b):
         bp, he = b[:3], b[3:]
         local = tuple(a - c for a, c in zip(p, bp))
@@ -182,7 +221,8 @@ class CsFluid3:
         else:
             ax = 2
         n = [F(0), F(0), F(0)]
-        n[ax] = F(1) * copysign1(local[ax])
+        sg = (abs(local[ax]) if np.isnan(local[ax]) else F(1)) if self.rust_sign else copysign1(local[ax])
+        n[ax] = F(1) * sg
         return tuple(n), pr + d[ax]
 
     # FluidSolver3.cs:923-1161
@@ -256,8 +296,8 @@ class CsFluid3:
         # boundary pass, particle by particle, bodies in order (statics take no impulse)
         pr = max(F(c.particle_radius), F(0))
         for i in range(n):
-            for b in self.boxes:
-                hit = self.collide_box(self.pos[i], pr, b)
+            for b in self.bodies:
+                hit = self.collide(self.pos[i], pr, b)
                 if hit is None:
                     continue
                 normal, depth = hit

@@ -76,8 +76,8 @@ from phi_eng_b200._abi import default_config  # noqa: E402
 from test_fluid3 import BOX, TANK as TANK3, lattice, make_oracle  # noqa: E402
 
 
-def run_both3(cfg, steps, pts, bodies):
-    cs = fluid3_cs.CsFluid3(cfg, [(*p, *e) for _, p, e in bodies])
+def run_both3(cfg, steps, pts, bodies, rust_sign=False):
+    cs = fluid3_cs.CsFluid3(cfg, bodies, rust_sign=rust_sign)
     cs.add_particles(pts)
     o = make_oracle(pts, bodies=bodies, cfg=cfg, gravity=(0.0, -9.81, 0.0))
     for _ in range(steps):
@@ -111,7 +111,7 @@ def test_oracle3_matches_csharp_solver_tank_cfl_friction():
     cfg.max_substeps = 4
     cfg.wall_friction = 0.5
     pts = lattice((0.125, -0.375, 0.125), 6, 5, 6, 0.25)
-    cs = fluid3_cs.CsFluid3(cfg, [(*p, *e) for _, p, e in TANK3])
+    cs = fluid3_cs.CsFluid3(cfg, TANK3)
     cs.add_particles(pts)
     assert cs.cfl_substeps(1.0 / 60.0) >= 2
     a, b, dp, dv = run_both3(cfg, 40, pts, TANK3)
@@ -173,3 +173,21 @@ def test_oracle_matches_csharp_solver_cfl_friction():
     assert cs.cfl_substeps(1.0 / 60.0) >= 2
     a, b = run_both(cfg, 60)
     assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+
+
+def test_oracle3_matches_csharp_solver_sphere_capsule():
+    """A static sphere and an upright capsule in the 3D tank under a falling
+    block, 40 steps: bit for bit. At step 30 a fast particle ends a step just
+    inside the right wall, where the reference's two statements differ (the
+    C# Copysign1 pushes it out along -x, the Rust step along +x); the C#
+    restatement takes the Rust sign there (rust_sign), and without it the
+    runs part at that particle."""
+    from test_fluid3 import CAPSULE, SPHERE
+
+    bodies = TANK3 + [(SPHERE, (1.0, 0.2, 1.0), (0.45, 0.0, 0.0)), (CAPSULE, (3.0, 0.4, 3.0), (0.3, 0.5, 0.0))]
+    pts = lattice((0.125, 1.0, 0.125), 6, 4, 6, 0.25)
+    pts = np.concatenate([pts, np.array([[3.0, 1.2, 3.0]], np.float32)])
+    a, b, dp, dv = run_both3(default_config(), 40, pts, bodies, rust_sign=True)
+    assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), (dp, dv)
+    a, b, dp, dv = run_both3(default_config(), 40, pts, bodies)
+    assert not np.array_equal(a, b)
