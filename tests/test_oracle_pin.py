@@ -191,3 +191,28 @@ def test_oracle3_matches_csharp_solver_sphere_capsule():
     assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), (dp, dv)
     a, b, dp, dv = run_both3(default_config(), 40, pts, bodies)
     assert not np.array_equal(a, b)
+
+
+def test_oracle_matches_csharp_solver_circle_obstacle():
+    """A static circle in the 2D tank under a falling 10 x 6 block, with wall
+    friction, 60 steps: bit for bit."""
+    cfg = sims.default_cfg()
+    cfg.wall_friction = 0.3
+    pts = np.array([(0.125 + ix * 0.25, 1.0 + iy * 0.25) for iy in range(6) for ix in range(10)], np.float32)
+    cs = fluid_cs.CsFluid(cfg, TANK + [("circle", 1.2, 0.3, 0.35)])
+    cs.add_particles(pts)
+    o = sims.OracleSim(orc.REF_SEQ)
+    sims.tank(o)
+    o.add_circle(1.2, 0.3, 0.35)
+    o.config = cfg
+    assert o.add_particles(pts) == len(pts)
+    touched = False
+    for _ in range(60):
+        cs.step(1.0 / 60.0)
+        o.step(1.0 / 60.0)
+        s = cs.state()
+        d = np.sqrt((s[:, 0] - 1.2) ** 2 + (s[:, 1] - 0.3) ** 2)
+        touched = touched or bool((d < 0.35 + cfg.particle_radius + 1e-3).any())
+    a, b = cs.state(), o.state()
+    assert touched  # the block reached the circle
+    assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
